@@ -1,0 +1,800 @@
+/*
+ * ns_oracle.c -- CPU restatement of TubularFlowIGA's body-fitted IGA
+ * Navier-Stokes hot path.  TEST INFRASTRUCTURE ONLY: the parity tests, the
+ * smoke check and the bench's CPU-baseline leg call it as the checker; the
+ * product library never links it.
+ *
+ * Every function restates one reference routine (file:line in the reference
+ * project) in plain C.  Element data use the reference's layout:
+ *   C[a*64+p]   dense Bezier extraction row of basis a (p = i + 4j + 16k)
+ *   X[p*3+d]    Bezier control points
+ *   state[a*4+f], f = (u, v, w, p)
+ * Matrices are 4x4 row-major blocks in node-graph block CSR, the layout of
+ * solvers/cuda/include/BlockCsr.hpp:15-100.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define TFO_OK 0
+#define TFO_SINGULAR_JACOBIAN -2
+#define TFO_NONPOSITIVE_JACOBIAN -3
+#define TFO_BAD_INPUT -4
+#define TFO_NO_MEMORY -5
+#define TFO_NOT_CONVERGED -6
+
+/* Four-point Gauss-Legendre rule on [0,1]: Quadrature.hpp:63-66. */
+static const double kGaussPoint[4] = {0.06943184420297371, 0.33000947820757187,
+	0.6699905217924281, 0.9305681557970262};
+static const double kGaussWeight[4] = {0.3478548451374539, 0.6521451548625461,
+	0.6521451548625461, 0.3478548451374539};
+
+void tfo_gauss_rule(double* points, double* weights)
+{
+	/* FullCell4x4x4VolumeQuadratureProvider::BuildRule, Quadrature.hpp:193-204:
+	 * qx fastest, reference weight = wx*wy*wz/8. */
+	int q = 0;
+	for (int qz = 0; qz < 4; ++qz)
+		for (int qy = 0; qy < 4; ++qy)
+			for (int qx = 0; qx < 4; ++qx, ++q) {
+				points[3*q] = kGaussPoint[qx];
+				points[3*q+1] = kGaussPoint[qy];
+				points[3*q+2] = kGaussPoint[qz];
+				weights[q] = kGaussWeight[qx]*kGaussWeight[qy]*kGaussWeight[qz]/8.0;
+			}
+}
+
+/* Cubic Bernstein polynomials and derivatives: TransportElement.hpp:120-134. */
+static void bernstein1(double t, double b[4], double db[4], double d2b[4])
+{
+	const double s = 1.0-t;
+	b[0] = s*s*s; b[1] = 3.0*s*s*t; b[2] = 3.0*s*t*t; b[3] = t*t*t;
+	db[0] = -3.0*s*s; db[1] = 3.0-12.0*t+9.0*t*t; db[2] = 3.0*(2.0-3.0*t)*t; db[3] = 3.0*t*t;
+	d2b[0] = 6.0*s; d2b[1] = -12.0+18.0*t; d2b[2] = 6.0-18.0*t; d2b[3] = 6.0*t;
+}
+
+static void bernstein3(double u, double v, double w, double* B, double (*dB)[3], double (*d2B)[3][3])
+{
+	double b[3][4], db[3][4], d2b[3][4];
+	bernstein1(u, b[0], db[0], d2b[0]);
+	bernstein1(v, b[1], db[1], d2b[1]);
+	bernstein1(w, b[2], db[2], d2b[2]);
+	int p = 0;
+	for (int k = 0; k < 4; ++k)
+		for (int j = 0; j < 4; ++j)
+			for (int i = 0; i < 4; ++i, ++p) {
+				B[p] = b[0][i]*b[1][j]*b[2][k];
+				dB[p][0] = db[0][i]*b[1][j]*b[2][k];
+				dB[p][1] = b[0][i]*db[1][j]*b[2][k];
+				dB[p][2] = b[0][i]*b[1][j]*db[2][k];
+				if (d2B) {
+					d2B[p][0][0] = d2b[0][i]*b[1][j]*b[2][k];
+					d2B[p][0][1] = db[0][i]*db[1][j]*b[2][k];
+					d2B[p][0][2] = db[0][i]*b[1][j]*db[2][k];
+					d2B[p][1][0] = d2B[p][0][1];
+					d2B[p][1][1] = b[0][i]*d2b[1][j]*b[2][k];
+					d2B[p][1][2] = b[0][i]*db[1][j]*db[2][k];
+					d2B[p][2][0] = d2B[p][0][2];
+					d2B[p][2][1] = d2B[p][1][2];
+					d2B[p][2][2] = b[0][i]*b[1][j]*d2b[2][k];
+				}
+			}
+}
+
+static double det3(const double a[3][3])
+{
+	/* Determinant: TransportElement.hpp:33-37. */
+	return a[0][0]*a[1][1]*a[2][2]+a[0][1]*a[1][2]*a[2][0]+a[0][2]*a[1][0]*a[2][1]
+		-a[0][2]*a[1][1]*a[2][0]-a[0][0]*a[1][2]*a[2][1]-a[0][1]*a[1][0]*a[2][2];
+}
+
+static int inverse3(const double a[3][3], double inv[3][3], double* determinant)
+{
+	/* Inverse by cofactors with the singularity guard: TransportElement.hpp:39-53. */
+	const double d = det3(a);
+	*determinant = d;
+	if (!isfinite(d) || fabs(d) < 1e-14) return TFO_SINGULAR_JACOBIAN;
+	inv[0][0] = (a[1][1]*a[2][2]-a[1][2]*a[2][1])/d;
+	inv[0][1] = (a[2][1]*a[0][2]-a[0][1]*a[2][2])/d;
+	inv[0][2] = (a[0][1]*a[1][2]-a[1][1]*a[0][2])/d;
+	inv[1][0] = (a[2][0]*a[1][2]-a[1][0]*a[2][2])/d;
+	inv[1][1] = (a[0][0]*a[2][2]-a[0][2]*a[2][0])/d;
+	inv[1][2] = (a[1][0]*a[0][2]-a[0][0]*a[1][2])/d;
+	inv[2][0] = (a[1][0]*a[2][1]-a[1][1]*a[2][0])/d;
+	inv[2][1] = (a[0][1]*a[2][0]-a[0][0]*a[2][1])/d;
+	inv[2][2] = (a[0][0]*a[1][1]-a[0][1]*a[1][0])/d;
+	return TFO_OK;
+}
+
+/*
+ * EvaluateBasis (TransportElement.hpp:118-206): values, physical gradients
+ * and (optionally) physical Hessians of the nen extracted basis functions at
+ * parametric point (u,v,w), plus J^{-1} (inverse[parameter][physical]) and
+ * the raw determinant det(dx/dxi).
+ */
+int tfo_basis(const double* C, const double* X, int nen, double u, double v, double w,
+	int with_hessian, double* N, double* dN, double* H, double* inverse_out, double* raw_det)
+{
+	double B[64], dB[64][3], d2B[64][3][3];
+	bernstein3(u, v, w, B, dB, with_hessian ? d2B : NULL);
+	double jac[3][3] = {{0}};
+	for (int p = 0; p < 64; ++p)
+		for (int phys = 0; phys < 3; ++phys)
+			for (int par = 0; par < 3; ++par)
+				jac[phys][par] += X[p*3+phys]*dB[p][par];
+	double inv[3][3], det = 0.0;
+	if (inverse3(jac, inv, &det) != TFO_OK) return TFO_SINGULAR_JACOBIAN;
+	if (!(0.125*det > 0.0)) return TFO_NONPOSITIVE_JACOBIAN;
+	double pg[64][3];
+	for (int p = 0; p < 64; ++p)
+		for (int phys = 0; phys < 3; ++phys) {
+			double s = 0.0;
+			for (int par = 0; par < 3; ++par) s += dB[p][par]*inv[par][phys];
+			pg[p][phys] = s;
+		}
+	for (int a = 0; a < nen; ++a) {
+		double value = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0;
+		for (int p = 0; p < 64; ++p) {
+			const double c = C[a*64+p];
+			value += c*B[p];
+			g0 += c*pg[p][0]; g1 += c*pg[p][1]; g2 += c*pg[p][2];
+		}
+		N[a] = value;
+		dN[a*3] = g0; dN[a*3+1] = g1; dN[a*3+2] = g2;
+	}
+	if (inverse_out)
+		for (int i = 0; i < 3; ++i)
+			for (int j = 0; j < 3; ++j) inverse_out[i*3+j] = inv[i][j];
+	*raw_det = det;
+	if (!with_hessian) return TFO_OK;
+	double gs[3][3][3] = {{{0}}};
+	for (int phys = 0; phys < 3; ++phys)
+		for (int p = 0; p < 64; ++p)
+			for (int a = 0; a < 3; ++a)
+				for (int b = 0; b < 3; ++b)
+					gs[phys][a][b] += X[p*3+phys]*d2B[p][a][b];
+	double is[3][3][3] = {{{0}}};
+	for (int c = 0; c < 3; ++c)
+		for (int i = 0; i < 3; ++i)
+			for (int j = 0; j < 3; ++j)
+				for (int phys = 0; phys < 3; ++phys)
+					for (int a = 0; a < 3; ++a)
+						for (int b = 0; b < 3; ++b)
+							is[c][i][j] -= gs[phys][a][b]*inv[a][i]*inv[b][j]*inv[c][phys];
+	/* Per Bernstein function, its physical Hessian; then extract. */
+	double ph[64][9];
+	for (int p = 0; p < 64; ++p)
+		for (int i = 0; i < 3; ++i)
+			for (int j = 0; j < 3; ++j) {
+				double value = 0.0;
+				for (int a = 0; a < 3; ++a) {
+					for (int b = 0; b < 3; ++b) value += d2B[p][a][b]*inv[a][i]*inv[b][j];
+					value += dB[p][a]*is[a][i][j];
+				}
+				ph[p][i*3+j] = value;
+			}
+	for (int a = 0; a < nen; ++a) {
+		double h[9] = {0};
+		for (int p = 0; p < 64; ++p) {
+			const double c = C[a*64+p];
+			if (c == 0.0) continue;
+			for (int k = 0; k < 9; ++k) h[k] += c*ph[p][k];
+		}
+		for (int k = 0; k < 9; ++k) H[a*9+k] = h[k];
+	}
+	return TFO_OK;
+}
+
+/* Stabilization parameters: NavierStokesElement.hpp:121-144. */
+static void stabilization(const double inv[3][3], const double state[4], double nu, double dt,
+	double* tau_m, double* tau_c)
+{
+	double metric[3][3] = {{0}}, direction[3] = {0};
+	for (int i = 0; i < 3; ++i)
+		for (int j = 0; j < 3; ++j) {
+			for (int k = 0; k < 3; ++k) metric[i][j] += inv[k][i]*inv[k][j];
+			direction[i] += inv[j][i];
+		}
+	double metric_norm = 0.0, direction_norm = 0.0, velocity_metric = 0.0;
+	for (int i = 0; i < 3; ++i) {
+		direction_norm += direction[i]*direction[i];
+		for (int j = 0; j < 3; ++j) {
+			metric_norm += metric[i][j]*metric[i][j];
+			velocity_metric += state[i]*metric[i][j]*state[j];
+		}
+	}
+	const double temporal = dt > 0.0 ? 4.0*(1.0/dt)*(1.0/dt) : 0.0;
+	*tau_m = 1.0/sqrt(temporal+velocity_metric+(1.0/12.0)*nu*nu*metric_norm);
+	*tau_c = 1.0/(*tau_m*direction_norm);
+}
+
+/*
+ * BuildNavierStokesElementFromPreparedPoints (NavierStokesElement.hpp:149-317),
+ * LegacyBodyFitted weak form, zero body force: the VMS residual (stored as
+ * negres = -r) and its exact Newton tangent jac = dr/du (row 4a+i, column
+ * 4b+f, dense (4 nen)^2).  jac may be NULL for the residual-only request.
+ * prev may be NULL when dt == 0 (steady).
+ */
+int tfo_ns_element(const double* C, const double* X, int nen, const double* state,
+	const double* prev, double density, double viscosity, double dt,
+	const double* qpoints, const double* qweights, int nq, double* jac, double* negres)
+{
+	if (!(density > 0.0) || !(viscosity > 0.0) || !isfinite(dt) || dt < 0.0 || nen <= 0 || nen > 80)
+		return TFO_BAD_INPUT;
+	const double nu = viscosity/density;
+	const int ndof = 4*nen;
+	if (jac) memset(jac, 0, sizeof(double)*(size_t)ndof*ndof);
+	memset(negres, 0, sizeof(double)*(size_t)ndof);
+	double N[80], dN[80*3], H[80*9];
+	for (int q = 0; q < nq; ++q) {
+		double inv_flat[9], raw = 0.0;
+		const int status = tfo_basis(C, X, nen, qpoints[3*q], qpoints[3*q+1], qpoints[3*q+2], 1,
+			N, dN, H, inv_flat, &raw);
+		if (status != TFO_OK) return status;
+		double inv[3][3];
+		for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) inv[i][j] = inv_flat[i*3+j];
+		const double measure = qweights[q]*raw;
+		double st[4] = {0}, grad[4][3] = {{0}}, hess[4][3][3] = {{{0}}}, pv[3] = {0};
+		for (int a = 0; a < nen; ++a)
+			for (int f = 0; f < 4; ++f) {
+				const double c = state[a*4+f];
+				st[f] += c*N[a];
+				for (int i = 0; i < 3; ++i) {
+					grad[f][i] += c*dN[a*3+i];
+					for (int j = 0; j < 3; ++j) hess[f][i][j] += c*H[a*9+i*3+j];
+				}
+			}
+		if (dt > 0.0)
+			for (int a = 0; a < nen; ++a)
+				for (int c = 0; c < 3; ++c) pv[c] += prev[a*4+c]*N[a];
+		double dudt[3] = {0};
+		if (dt > 0.0) for (int c = 0; c < 3; ++c) dudt[c] = (st[c]-pv[c])/dt;
+		double tau_m = 0.0, tau_c = 0.0;
+		stabilization(inv, st, nu, dt, &tau_m, &tau_c);
+		double fine[3];
+		for (int c = 0; c < 3; ++c) {
+			const double conv = st[0]*grad[c][0]+st[1]*grad[c][1]+st[2]*grad[c][2];
+			const double lap = hess[c][0][0]+hess[c][1][1]+hess[c][2][2];
+			fine[c] = -tau_m*(dudt[c]+conv+grad[3][c]/density-nu*lap);
+		}
+		const double divu = grad[0][0]+grad[1][1]+grad[2][2];
+		const double fine_p = -density*tau_c*divu;
+		double metric[3][3] = {{0}};
+		if (jac)
+			for (int i = 0; i < 3; ++i)
+				for (int j = 0; j < 3; ++j)
+					for (int k = 0; k < 3; ++k) metric[i][j] += inv[k][i]*inv[k][j];
+		/* Strong momentum residual (without tau), reused by the tangent. */
+		double strong[3];
+		for (int c = 0; c < 3; ++c)
+			strong[c] = dudt[c]+st[0]*grad[c][0]+st[1]*grad[c][1]+st[2]*grad[c][2]
+				+grad[3][c]/density-nu*(hess[c][0][0]+hess[c][1][1]+hess[c][2][2]);
+		for (int a = 0; a < nen; ++a) {
+			const double na = N[a];
+			const double* ga = dN+a*3;
+			double r[4];
+			for (int c = 0; c < 3; ++c) {
+				r[c] = density*na*dudt[c]-ga[c]*fine_p;
+				r[c] -= ga[c]*st[3];
+				for (int d = 0; d < 3; ++d) {
+					r[c] += viscosity*ga[d]*(grad[c][d]+grad[d][c]);
+					r[c] += density*na*(st[d]+fine[d])*grad[c][d];
+					r[c] -= density*ga[d]*fine[c]*(st[d]+fine[d]);
+				}
+			}
+			r[3] = na*divu-ga[0]*fine[0]-ga[1]*fine[1]-ga[2]*fine[2];
+			for (int f = 0; f < 4; ++f) negres[4*a+f] -= r[f]*measure;
+			if (!jac) continue;
+			for (int b = 0; b < nen; ++b) {
+				const double nb = N[b];
+				const double* gb = dN+b*3;
+				const double lap_b = H[b*9]+H[b*9+4]+H[b*9+8];
+				for (int f = 0; f < 4; ++f) {
+					double du[3] = {0}, dlap[3] = {0}, dgp[3] = {0};
+					const double dp = f == 3 ? nb : 0.0;
+					if (f < 3) { du[f] = nb; dlap[f] = lap_b; }
+					else { dgp[0] = gb[0]; dgp[1] = gb[1]; dgp[2] = gb[2]; }
+					double vmd = 0.0;
+					for (int i = 0; i < 3; ++i)
+						for (int j = 0; j < 3; ++j) vmd += du[i]*metric[i][j]*st[j];
+					const double dtau_m = -tau_m*tau_m*tau_m*vmd;
+					const double dtau_c = tau_c*tau_m*tau_m*vmd;
+					const double ddiv = f < 3 ? gb[f] : 0.0;
+					double dfine[3];
+					for (int c = 0; c < 3; ++c) {
+						double ds = 0.0;
+						for (int d = 0; d < 3; ++d)
+							ds += du[d]*grad[c][d]+st[d]*(f == c ? gb[d] : 0.0);
+						if (dt > 0.0 && f == c) ds += nb/dt;
+						ds += dgp[c]/density-nu*dlap[c];
+						dfine[c] = -dtau_m*strong[c]-tau_m*ds;
+					}
+					const double dfine_p = -density*(dtau_c*divu+tau_c*ddiv);
+					for (int i = 0; i < 3; ++i) {
+						double t = density*na*(dt > 0.0 && f == i ? nb/dt : 0.0)-ga[i]*dfine_p;
+						t -= ga[i]*dp;
+						for (int d = 0; d < 3; ++d) {
+							t += viscosity*ga[d]*((f == i ? gb[d] : 0.0)+(f == d ? gb[i] : 0.0));
+							t += density*na*((du[d]+dfine[d])*grad[i][d]
+								+(st[d]+fine[d])*(f == i ? gb[d] : 0.0));
+							t -= density*ga[d]*(dfine[i]*(st[d]+fine[d])+fine[i]*(du[d]+dfine[d]));
+						}
+						jac[(size_t)(4*a+i)*ndof+4*b+f] += t*measure;
+					}
+					double ct = na*ddiv;
+					for (int d = 0; d < 3; ++d) ct -= ga[d]*dfine[d];
+					jac[(size_t)(4*a+3)*ndof+4*b+f] += ct*measure;
+				}
+			}
+		}
+	}
+	return TFO_OK;
+}
+
+/* 0.125 det(dx/dxi) at the 4x4x4 Gauss points (InspectGeometry,
+ * TransportElement.hpp:55-90): returns the minimum and counts bad samples. */
+double tfo_min_determinant(const double* X, int* bad_samples)
+{
+	double minimum = INFINITY;
+	int bad = 0;
+	for (int k = 0; k < 4; ++k)
+		for (int j = 0; j < 4; ++j)
+			for (int i = 0; i < 4; ++i) {
+				double B[64], dB[64][3];
+				bernstein3(kGaussPoint[i], kGaussPoint[j], kGaussPoint[k], B, dB, NULL);
+				double jac[3][3] = {{0}};
+				for (int p = 0; p < 64; ++p)
+					for (int phys = 0; phys < 3; ++phys)
+						for (int par = 0; par < 3; ++par) jac[phys][par] += X[p*3+phys]*dB[p][par];
+				const double d = 0.125*det3(jac);
+				if (d < minimum) minimum = d;
+				if (!isfinite(d) || d <= 0.0) ++bad;
+			}
+	if (bad_samples) *bad_samples = bad;
+	return minimum;
+}
+
+/* Face tables of the body-fitted surface rule: BoundaryFlow.hpp:175-180. */
+static const int kFixedAxis[6] = {2, 1, 0, 1, 0, 2};
+static const int kVaryingAxes[6][2] = {{0, 1}, {0, 2}, {1, 2}, {0, 2}, {1, 2}, {0, 1}};
+static const double kFixedValue[6] = {0.0, 0.0, 1.0, 1.0, 0.0, 1.0};
+static const double kOutwardSign[6] = {-1.0, -1.0, 1.0, 1.0, -1.0, 1.0};
+
+/*
+ * Per-face flow coefficients F[a*3+c] such that the outward boundary flow of
+ * face `face` is sum_a sum_c F[a*3+c] u_a[c] (IntegrateBoundaryFlow,
+ * BoundaryFlow.hpp:165-200) and the pressure traction of pressure p adds
+ * -p F[a*3+c] to rhs (IntegrateBoundaryPressureTraction, :445-475).
+ */
+int tfo_face_coefficients(const double* C, const double* X, int nen, int face, double* F)
+{
+	if (face < 0 || face >= 6) return TFO_BAD_INPUT;
+	memset(F, 0, sizeof(double)*(size_t)nen*3);
+	double N[80], dN[240];
+	for (int qi = 0; qi < 4; ++qi)
+		for (int qj = 0; qj < 4; ++qj) {
+			double coordinate[3] = {0, 0, 0};
+			coordinate[kFixedAxis[face]] = kFixedValue[face];
+			coordinate[kVaryingAxes[face][0]] = kGaussPoint[qi];
+			coordinate[kVaryingAxes[face][1]] = kGaussPoint[qj];
+			double inv[9], raw = 0.0;
+			const int status = tfo_basis(C, X, nen, coordinate[0], coordinate[1], coordinate[2], 0,
+				N, dN, NULL, inv, &raw);
+			if (status != TFO_OK) return status;
+			const double scale = kOutwardSign[face]*kGaussWeight[qi]*kGaussWeight[qj]*2.0*(0.125*raw);
+			for (int a = 0; a < nen; ++a)
+				for (int c = 0; c < 3; ++c)
+					F[a*3+c] += scale*inv[kFixedAxis[face]*3+c]*N[a];
+		}
+	return TFO_OK;
+}
+
+double tfo_boundary_flow(const double* C, const double* X, int nen, int face, const double* state)
+{
+	double F[240];
+	if (tfo_face_coefficients(C, X, nen, face, F) != TFO_OK) return NAN;
+	double flow = 0.0;
+	for (int a = 0; a < nen; ++a)
+		for (int c = 0; c < 3; ++c) flow += F[a*3+c]*state[a*4+c];
+	return flow;
+}
+
+/* Outlet 0D models (EvaluateOutletModel, OutletModel.hpp:70-90).
+ * kind: 0 resistance, 1 windkessel RC, 2 windkessel RCR. */
+int tfo_outlet_model(int kind, double resistance, double proximal, double distal, double capacitance,
+	double reference_pressure, double capacitor_pressure, double flow, double dt,
+	double* pressure, double* new_capacitor_pressure)
+{
+	if (!isfinite(flow)) return TFO_BAD_INPUT;
+	if (kind == 0) {
+		*pressure = reference_pressure+resistance*flow;
+		*new_capacitor_pressure = capacitor_pressure;
+		return TFO_OK;
+	}
+	if (!(dt > 0.0)) return TFO_BAD_INPUT;
+	const double r = kind == 1 ? resistance : distal;
+	const double pc = (capacitance*capacitor_pressure/dt+flow+reference_pressure/r)/(capacitance/dt+1.0/r);
+	*new_capacitor_pressure = pc;
+	*pressure = pc+(kind == 2 ? proximal*flow : 0.0);
+	return TFO_OK;
+}
+
+/* Temporal waveforms (EvaluateTemporalFunction, TemporalFunction.hpp:97-112).
+ * kind: 0 constant, 1 sinusoid, 2 fourier. */
+double tfo_temporal(int kind, double value, double mean, double amplitude, double period, double phase,
+	const double* cosine, const double* sine, int harmonics, double time)
+{
+	const double pi = 3.141592653589793238462643383279502884;
+	if (kind == 0) return value;
+	double wrapped = fmod(time, period);
+	if (wrapped < 0.0) wrapped += period;
+	const double theta = 2.0*pi*wrapped/period+phase;
+	if (kind == 1) return mean+amplitude*sin(theta);
+	double result = mean;
+	for (int h = 0; h < harmonics; ++h) {
+		const double angle = (double)(h+1)*theta;
+		result += cosine[h]*cos(angle)+sine[h]*sin(angle);
+	}
+	return result;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Global (mesh-level) restatements.                                      */
+/* ---------------------------------------------------------------------- */
+
+static int compare_int(const void* a, const void* b)
+{
+	const int x = *(const int*)a, y = *(const int*)b;
+	return (x > y)-(x < y);
+}
+
+/*
+ * Node-graph block pattern (BlockPattern, BlockCsr.hpp:15-55): sorted unique
+ * columns per node row.  Call with columns == NULL to get the block count in
+ * *blocks; then call again with arrays of that size.
+ */
+int tfo_block_pattern(int nodes, int elements, const int* element_offsets, const int* connectivity,
+	int* row_offsets, int* columns, int* diagonal, long long* blocks)
+{
+	int* count = (int*)calloc((size_t)nodes+1, sizeof(int));
+	if (!count) return TFO_NO_MEMORY;
+	for (int e = 0; e < elements; ++e) {
+		const int nen = element_offsets[e+1]-element_offsets[e];
+		for (int a = element_offsets[e]; a < element_offsets[e+1]; ++a) {
+			const int node = connectivity[a];
+			if (node < 0 || node >= nodes) { free(count); return TFO_BAD_INPUT; }
+			count[node] += nen;
+		}
+	}
+	long long* start = (long long*)malloc(sizeof(long long)*((size_t)nodes+1));
+	start[0] = 0;
+	for (int i = 0; i < nodes; ++i) start[i+1] = start[i]+count[i];
+	int* raw = (int*)malloc(sizeof(int)*(size_t)(start[nodes] > 0 ? start[nodes] : 1));
+	memset(count, 0, sizeof(int)*((size_t)nodes+1));
+	for (int e = 0; e < elements; ++e)
+		for (int a = element_offsets[e]; a < element_offsets[e+1]; ++a) {
+			const int node = connectivity[a];
+			for (int b = element_offsets[e]; b < element_offsets[e+1]; ++b)
+				raw[start[node]+count[node]++] = connectivity[b];
+		}
+	long long total = 0;
+	for (int i = 0; i < nodes; ++i) {
+		int* row = raw+start[i];
+		const int length = count[i];
+		qsort(row, (size_t)length, sizeof(int), compare_int);
+		int unique = 0;
+		for (int k = 0; k < length; ++k)
+			if (unique == 0 || row[unique-1] != row[k]) row[unique++] = row[k];
+		int has_diagonal = 0;
+		if (columns) {
+			row_offsets[i] = (int)total;
+			for (int k = 0; k < unique; ++k) {
+				if (row[k] == i) { diagonal[i] = (int)(total+k); has_diagonal = 1; }
+				columns[total+k] = row[k];
+			}
+			if (!has_diagonal) { free(raw); free(start); free(count); return TFO_BAD_INPUT; }
+		}
+		total += unique;
+	}
+	if (columns) row_offsets[nodes] = (int)total;
+	*blocks = total;
+	free(raw); free(start); free(count);
+	return TFO_OK;
+}
+
+static long long find_block(const int* row_offsets, const int* columns, int row, int column)
+{
+	/* FindBlock: SparseKernels.cuh:13-23. */
+	int first = row_offsets[row], last = row_offsets[row+1];
+	while (first < last) {
+		const int middle = first+(last-first)/2;
+		if (columns[middle] < column) first = middle+1;
+		else last = middle;
+	}
+	return first;
+}
+
+/*
+ * Global assembly: every element's exact tangent and -r scatter-added into
+ * the block-CSR Jacobian and rhs (AddElementMatrix semantics,
+ * OwnedRowAssembler.hpp:210-236; the loop of iga_cuda.cu:959-965).  The
+ * element extraction is passed in the flattened sparse layout of FlatMesh
+ * (DeviceMesh.hpp:16-57).  values may be NULL for a residual-only pass.
+ * Element failures are reported through *failed_element (-1 = none).
+ */
+int tfo_assemble(int nodes, int elements, const int* element_offsets, const int* connectivity,
+	const int* extraction_offsets, const uint8_t* extraction_columns, const double* extraction_values,
+	const double* bezier_points, const int* row_offsets, const int* columns,
+	const double* state, const double* previous, double density, double viscosity, double dt,
+	double* values, double* rhs, int* failed_element)
+{
+	(void)nodes;
+	double qp[64*3], qw[64];
+	tfo_gauss_rule(qp, qw);
+	int failure = -1, status_out = TFO_OK;
+#pragma omp parallel
+	{
+		double* C = (double*)malloc(sizeof(double)*80*64);
+		double* jac = values ? (double*)malloc(sizeof(double)*320*320) : NULL;
+		double negres[320], st[320], pv[320];
+		long long blocks[80];
+#pragma omp for schedule(dynamic, 4)
+		for (int e = 0; e < elements; ++e) {
+			const int begin = element_offsets[e];
+			const int nen = element_offsets[e+1]-begin;
+			memset(C, 0, sizeof(double)*(size_t)nen*64);
+			for (int a = 0; a < nen; ++a)
+				for (int k = extraction_offsets[begin+a]; k < extraction_offsets[begin+a+1]; ++k)
+					C[a*64+extraction_columns[k]] = extraction_values[k];
+			for (int a = 0; a < nen; ++a) {
+				const int node = connectivity[begin+a];
+				for (int f = 0; f < 4; ++f) {
+					st[4*a+f] = state[4*(size_t)node+f];
+					pv[4*a+f] = previous ? previous[4*(size_t)node+f] : 0.0;
+				}
+			}
+			const int status = tfo_ns_element(C, bezier_points+(size_t)e*192, nen, st, pv,
+				density, viscosity, dt, qp, qw, 64, jac, negres);
+			if (status != TFO_OK) {
+#pragma omp critical
+				{ failure = e; status_out = status; }
+				continue;
+			}
+			for (int a = 0; a < nen; ++a) {
+				const int row = connectivity[begin+a];
+				for (int f = 0; f < 4; ++f) {
+#pragma omp atomic
+					rhs[4*(size_t)row+f] += negres[4*a+f];
+				}
+			}
+			if (!values) continue;
+			const int ndof = 4*nen;
+			for (int a = 0; a < nen; ++a) {
+				const int row = connectivity[begin+a];
+				for (int b = 0; b < nen; ++b)
+					blocks[b] = find_block(row_offsets, columns, row, connectivity[begin+b]);
+				for (int b = 0; b < nen; ++b) {
+					double* block = values+blocks[b]*16;
+					for (int i = 0; i < 4; ++i)
+						for (int f = 0; f < 4; ++f) {
+#pragma omp atomic
+							block[i*4+f] += jac[(size_t)(4*a+i)*ndof+4*b+f];
+						}
+				}
+			}
+		}
+		free(C);
+		free(jac);
+	}
+	if (failed_element) *failed_element = failure;
+	return status_out;
+}
+
+/*
+ * Dirichlet rows (ApplyNavierStokesBoundaryKernel / SetNavierStokesBoundaryRhsKernel,
+ * IgaCudaKernels.cuh:436-463): zero the constrained rows, put 1 on the
+ * diagonal, rhs = target - state.
+ */
+void tfo_apply_dirichlet(int nodes, const int* row_offsets, const int* diagonal,
+	const int* velocity_mask, const int* pressure_mask, const double* velocity, const double* pressure,
+	const double* state, double* values, double* rhs)
+{
+	for (int node = 0; node < nodes; ++node)
+		for (int f = 0; f < 4; ++f) {
+			const int constrained = f < 3 ? velocity_mask[node] : pressure_mask[node];
+			if (!constrained) continue;
+			if (values) {
+				for (int b = row_offsets[node]; b < row_offsets[node+1]; ++b)
+					for (int g = 0; g < 4; ++g) values[(size_t)b*16+f*4+g] = 0.0;
+				values[(size_t)diagonal[node]*16+f*4+f] = 1.0;
+			}
+			const double target = f < 3 ? velocity[3*(size_t)node+f] : pressure[node];
+			rhs[4*(size_t)node+f] = target-state[4*(size_t)node+f];
+		}
+}
+
+/* y = A x over 4x4 blocks (BlockSpmvKernel, SparseKernels.cuh:25-40). */
+void tfo_spmv(int nodes, const int* row_offsets, const int* columns, const double* values,
+	const double* x, double* y)
+{
+#pragma omp parallel for schedule(static)
+	for (int row = 0; row < nodes; ++row) {
+		double r[4] = {0, 0, 0, 0};
+		for (int b = row_offsets[row]; b < row_offsets[row+1]; ++b) {
+			const double* blk = values+(size_t)b*16;
+			const double* xc = x+4*(size_t)columns[b];
+			for (int i = 0; i < 4; ++i)
+				r[i] += blk[i*4]*xc[0]+blk[i*4+1]*xc[1]+blk[i*4+2]*xc[2]+blk[i*4+3]*xc[3];
+		}
+		for (int i = 0; i < 4; ++i) y[4*(size_t)row+i] = r[i];
+	}
+}
+
+/* Diagonal-block Gauss-Jordan inverse with partial pivoting and the
+ * singular fallback (BuildBlockInverseKernel, SparseKernels.cuh:42-89). */
+int tfo_block_inverse(int nodes, const int* diagonal, const double* values, double* inverse)
+{
+	int singular = 0;
+#pragma omp parallel for schedule(static) reduction(+:singular)
+	for (int node = 0; node < nodes; ++node) {
+		const double* s = values+(size_t)diagonal[node]*16;
+		double m[4][8];
+		for (int i = 0; i < 4; ++i)
+			for (int j = 0; j < 8; ++j) m[i][j] = j < 4 ? s[i*4+j] : (j-4 == i ? 1.0 : 0.0);
+		int failed = 0;
+		for (int pivot = 0; pivot < 4; ++pivot) {
+			int best = pivot;
+			for (int row = pivot+1; row < 4; ++row)
+				if (fabs(m[row][pivot]) > fabs(m[best][pivot])) best = row;
+			if (!isfinite(m[best][pivot]) || fabs(m[best][pivot]) < 1e-14) { failed = 1; break; }
+			if (best != pivot)
+				for (int c = 0; c < 8; ++c) { const double t = m[pivot][c]; m[pivot][c] = m[best][c]; m[best][c] = t; }
+			const double scale = 1.0/m[pivot][pivot];
+			for (int c = 0; c < 8; ++c) m[pivot][c] *= scale;
+			for (int row = 0; row < 4; ++row) {
+				if (row == pivot) continue;
+				const double factor = m[row][pivot];
+				for (int c = 0; c < 8; ++c) m[row][c] -= factor*m[pivot][c];
+			}
+		}
+		double* d = inverse+(size_t)node*16;
+		if (!failed) {
+			for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) d[i*4+j] = m[i][4+j];
+		} else {
+			++singular;
+			for (int i = 0; i < 4; ++i)
+				for (int j = 0; j < 4; ++j)
+					d[i*4+j] = i == j && fabs(s[i*4+i]) > 1e-14 ? 1.0/s[i*4+i] : (i == j ? 1.0 : 0.0);
+		}
+	}
+	return singular;
+}
+
+static void apply_block_inverse(int nodes, const double* inverse, const double* x, double* y)
+{
+#pragma omp parallel for schedule(static)
+	for (int node = 0; node < nodes; ++node)
+		for (int i = 0; i < 4; ++i) {
+			double r = 0.0;
+			for (int j = 0; j < 4; ++j) r += inverse[((size_t)node*4+i)*4+j]*x[4*(size_t)node+j];
+			y[4*(size_t)node+i] = r;
+		}
+}
+
+static double dot(long long n, const double* x, const double* y)
+{
+	double s = 0.0;
+#pragma omp parallel for schedule(static) reduction(+:s)
+	for (long long i = 0; i < n; ++i) s += x[i]*y[i];
+	return s;
+}
+
+static void axpy(long long n, double alpha, const double* x, double* y)
+{
+#pragma omp parallel for schedule(static)
+	for (long long i = 0; i < n; ++i) y[i] += alpha*x[i];
+}
+
+/*
+ * Restarted left-preconditioned GMRES(m) with modified Gram-Schmidt,
+ * Givens rotations and the true-residual restart check, block-Jacobi
+ * preconditioned (SolveGmres, Gmres.hpp:192-336, zero polynomial sweeps).
+ * Tolerance: max(1e-30, rtol * ||D^{-1} (b - A x0)||).  Returns the
+ * iteration count (>= 0) or TFO_NOT_CONVERGED; *residual gets the final
+ * preconditioned residual norm.
+ */
+int tfo_gmres_bjacobi(int nodes, const int* row_offsets, const int* columns, const int* diagonal,
+	const double* values, const double* rhs, double* x, int restart, int maximum_iterations,
+	double rtol, double* residual_out, int* singular_out)
+{
+	const long long n = 4LL*nodes;
+	double* inverse = (double*)malloc(sizeof(double)*(size_t)n*4);
+	double* raw = (double*)malloc(sizeof(double)*(size_t)n);
+	double* res = (double*)malloc(sizeof(double)*(size_t)n);
+	double* work = (double*)malloc(sizeof(double)*(size_t)n);
+	double* V = (double*)malloc(sizeof(double)*(size_t)n*(size_t)(restart+1));
+	double* h = (double*)calloc((size_t)(restart+1)*restart, sizeof(double));
+	double* cs = (double*)calloc((size_t)restart, sizeof(double));
+	double* sn = (double*)calloc((size_t)restart, sizeof(double));
+	double* g = (double*)calloc((size_t)restart+1, sizeof(double));
+	double* y = (double*)calloc((size_t)restart, sizeof(double));
+	if (!inverse || !raw || !res || !work || !V || !h || !cs || !sn || !g || !y) return TFO_NO_MEMORY;
+	const int singular = tfo_block_inverse(nodes, diagonal, values, inverse);
+	if (singular_out) *singular_out = singular;
+	tfo_spmv(nodes, row_offsets, columns, values, x, raw);
+	for (long long i = 0; i < n; ++i) res[i] = rhs[i]-raw[i];
+	apply_block_inverse(nodes, inverse, res, work);
+	const double initial = sqrt(dot(n, work, work));
+	int iterations = 0, converged = 0;
+	double residual = initial;
+	if (initial == 0.0) converged = 1;
+	const double tolerance = fmax(1e-30, rtol*initial);
+	double beta = initial;
+	while (!converged && iterations < maximum_iterations) {
+		for (long long i = 0; i < n; ++i) V[i] = work[i]/beta;
+		memset(h, 0, sizeof(double)*(size_t)(restart+1)*restart);
+		memset(g, 0, sizeof(double)*((size_t)restart+1));
+		g[0] = beta;
+		int used = 0;
+		for (int j = 0; j < restart && iterations < maximum_iterations; ++j) {
+			tfo_spmv(nodes, row_offsets, columns, values, V+(size_t)j*n, raw);
+			apply_block_inverse(nodes, inverse, raw, work);
+			for (int i = 0; i <= j; ++i) {
+				const double value = dot(n, V+(size_t)i*n, work);
+				h[(size_t)i*restart+j] = value;
+				axpy(n, -value, V+(size_t)i*n, work);
+			}
+			const double next = sqrt(dot(n, work, work));
+			h[(size_t)(j+1)*restart+j] = next;
+			if (next > 1e-30)
+				for (long long i = 0; i < n; ++i) V[(size_t)(j+1)*n+i] = work[i]/next;
+			for (int i = 0; i < j; ++i) {
+				const double a = h[(size_t)i*restart+j], b = h[(size_t)(i+1)*restart+j];
+				h[(size_t)i*restart+j] = cs[i]*a+sn[i]*b;
+				h[(size_t)(i+1)*restart+j] = -sn[i]*a+cs[i]*b;
+			}
+			const double a = h[(size_t)j*restart+j], b = h[(size_t)(j+1)*restart+j];
+			const double mag = hypot(a, b);
+			cs[j] = mag > 0.0 ? a/mag : 1.0;
+			sn[j] = mag > 0.0 ? b/mag : 0.0;
+			h[(size_t)j*restart+j] = mag;
+			h[(size_t)(j+1)*restart+j] = 0.0;
+			const double old = g[j];
+			g[j] = cs[j]*old;
+			g[j+1] = -sn[j]*old;
+			++iterations;
+			used = j+1;
+			residual = fabs(g[j+1]);
+			if (residual <= tolerance || next <= 1e-30) break;
+		}
+		for (int row = used-1; row >= 0; --row) {
+			double value = g[row];
+			for (int c = row+1; c < used; ++c) value -= h[(size_t)row*restart+c]*y[c];
+			y[row] = value/h[(size_t)row*restart+row];
+		}
+		for (int i = 0; i < used; ++i) axpy(n, y[i], V+(size_t)i*n, x);
+		tfo_spmv(nodes, row_offsets, columns, values, x, raw);
+		for (long long i = 0; i < n; ++i) res[i] = rhs[i]-raw[i];
+		apply_block_inverse(nodes, inverse, res, work);
+		beta = sqrt(dot(n, work, work));
+		residual = beta;
+		if (beta <= tolerance) converged = 1;
+	}
+	if (residual_out) *residual_out = residual;
+	free(inverse); free(raw); free(res); free(work); free(V); free(h); free(cs); free(sn); free(g); free(y);
+	return converged ? iterations : TFO_NOT_CONVERGED;
+}
+
+int tfo_max_threads(void)
+{
+#ifdef _OPENMP
+	return omp_get_max_threads();
+#else
+	return 1;
+#endif
+}

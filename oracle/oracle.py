@@ -1,0 +1,288 @@
+"""ctypes access to the CPU oracle (test infrastructure only).
+
+Two libraries live here:
+
+* ``liboracle.so`` -- the C restatement in ``ns_oracle.c`` of the reference's
+  element arithmetic, block pattern, Dirichlet rows and block-Jacobi GMRES.
+* ``_ref/libtfiga_ref.so`` -- the reference's own header-only element code
+  compiled unmodified (``ref_shim.cpp``); present where it was built.
+
+Only the tests, the smoke check and the bench's CPU-baseline leg import this
+module, and only as the checker.  ``newton_step`` restates one iteration of
+the reference Newton loop (solvers/cuda/src/iga_cuda.cu:956-1033) with a
+direct sparse solve so the parity tests can use a linear solve far tighter
+than the reference's GMRES tolerance.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_up = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+def _load(path: Path):
+    if not path.exists():
+        raise FileNotFoundError(f"{path} is not built; run `make -C {HERE}`")
+    return C.CDLL(str(path))
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = _load(HERE / "liboracle.so")
+        L = _lib
+        L.tfo_gauss_rule.argtypes = [_dp, _dp]
+        L.tfo_basis.argtypes = [_dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
+                                _dp, _dp, _dp, _dp, C.POINTER(C.c_double)]
+        L.tfo_ns_element.argtypes = [_dp, _dp, C.c_int, _dp, C.c_void_p, C.c_double, C.c_double,
+                                     C.c_double, _dp, _dp, C.c_int, C.c_void_p, _dp]
+        L.tfo_min_determinant.argtypes = [_dp, C.POINTER(C.c_int)]
+        L.tfo_min_determinant.restype = C.c_double
+        L.tfo_face_coefficients.argtypes = [_dp, _dp, C.c_int, C.c_int, _dp]
+        L.tfo_boundary_flow.argtypes = [_dp, _dp, C.c_int, C.c_int, _dp]
+        L.tfo_boundary_flow.restype = C.c_double
+        L.tfo_outlet_model.argtypes = [C.c_int] + [C.c_double] * 8 + [C.POINTER(C.c_double)] * 2
+        L.tfo_temporal.argtypes = [C.c_int] + [C.c_double] * 5 + [_dp, _dp, C.c_int, C.c_double]
+        L.tfo_temporal.restype = C.c_double
+        L.tfo_block_pattern.argtypes = [C.c_int, C.c_int, _ip, _ip, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.POINTER(C.c_longlong)]
+        L.tfo_assemble.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip, _up, _dp, _dp, _ip, _ip, _dp, _dp,
+                                   C.c_double, C.c_double, C.c_double, C.c_void_p, _dp, C.POINTER(C.c_int)]
+        L.tfo_apply_dirichlet.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, _dp, C.c_void_p, _dp]
+        L.tfo_spmv.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp]
+        L.tfo_gmres_bjacobi.argtypes = [C.c_int, _ip, _ip, _ip, _dp, _dp, _dp, C.c_int, C.c_int, C.c_double,
+                                        C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.tfo_max_threads.restype = C.c_int
+    return _lib
+
+
+def ref_available() -> bool:
+    return (HERE / "_ref" / "libtfiga_ref.so").exists()
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        _ref = _load(HERE / "_ref" / "libtfiga_ref.so")
+        R = _ref
+        R.ref_last_error.restype = C.c_char_p
+        R.ref_ns_element.argtypes = [_dp, _dp, C.c_int, _dp, C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                     C.c_void_p, _dp]
+        R.ref_ns_element_points.argtypes = [_dp, _dp, C.c_int, _dp, C.c_void_p, C.c_double, C.c_double,
+                                            C.c_double, _dp, _dp, C.c_int, C.c_void_p, _dp]
+        R.ref_basis.argtypes = [_dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp,
+                                C.POINTER(C.c_double)]
+        R.ref_boundary_flow.argtypes = [_dp, _dp, C.c_int, C.c_int, _dp]
+        R.ref_boundary_flow.restype = C.c_double
+        R.ref_pressure_traction.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, _dp]
+        R.ref_outlet_model.argtypes = [C.c_int] + [C.c_double] * 8 + [C.POINTER(C.c_double)] * 2
+        R.ref_ntiga_header.argtypes = [C.c_char_p, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")]
+        R.ref_ntiga_element.argtypes = [C.c_char_p, C.c_uint64, C.POINTER(C.c_int), _ip, _ip, _dp, _dp]
+        R.ref_wall_trace.argtypes = [C.c_char_p, C.c_char_p, _ip, C.c_longlong]
+        R.ref_wall_trace.restype = C.c_longlong
+    return _ref
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def gauss_rule():
+    p = np.zeros(64 * 3)
+    w = np.zeros(64)
+    lib().tfo_gauss_rule(p, w)
+    return p.reshape(64, 3), w
+
+
+# --------------------------------------------------------------------------
+# Element level
+# --------------------------------------------------------------------------
+
+def basis(Cx, X, u, v, w, hessian=True, use_ref=False):
+    Cx = np.ascontiguousarray(Cx, dtype=np.float64)
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    nen = Cx.shape[0]
+    N = np.zeros(nen); dN = np.zeros(nen * 3); H = np.zeros(nen * 9); inv = np.zeros(9)
+    det = C.c_double()
+    if use_ref:
+        st = ref().ref_basis(Cx.ravel(), X.ravel(), nen, u, v, w, N, dN, H, inv, C.byref(det))
+    else:
+        st = lib().tfo_basis(Cx.ravel(), X.ravel(), nen, u, v, w, int(hessian), N, dN, H, inv, C.byref(det))
+    if st != 0:
+        raise RuntimeError(f"basis evaluation failed ({st})")
+    return N, dN.reshape(nen, 3), H.reshape(nen, 3, 3), inv.reshape(3, 3), det.value
+
+
+def ns_element(Cx, X, state, previous, density, viscosity, dt, jacobian=True, use_ref=False,
+               points=None, weights=None):
+    """Element (-r, dr/du) of the reference VMS formulation; jac is (4nen, 4nen)."""
+    Cx = np.ascontiguousarray(Cx, dtype=np.float64)
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    pv = None if previous is None else np.ascontiguousarray(previous, dtype=np.float64)
+    nen = Cx.shape[0]
+    negres = np.zeros(4 * nen)
+    jac = np.zeros((4 * nen, 4 * nen)) if jacobian else None
+    if points is None:
+        points, weights = gauss_rule()
+    points = np.ascontiguousarray(points, dtype=np.float64).ravel()
+    weights = np.ascontiguousarray(weights, dtype=np.float64).ravel()
+    if use_ref:
+        R = ref()
+        if len(weights) == 64 and np.allclose(points.reshape(-1, 3), gauss_rule()[0]):
+            s = R.ref_ns_element(Cx.ravel(), X.ravel(), nen, st.ravel(), _ptr(pv), density, viscosity, dt,
+                                 _ptr(jac), negres)
+        else:
+            s = R.ref_ns_element_points(Cx.ravel(), X.ravel(), nen, st.ravel(), _ptr(pv), density, viscosity,
+                                        dt, points, weights, len(weights), _ptr(jac), negres)
+        if s != 0:
+            raise RuntimeError(R.ref_last_error().decode())
+    else:
+        s = lib().tfo_ns_element(Cx.ravel(), X.ravel(), nen, st.ravel(), _ptr(pv), density, viscosity, dt,
+                                 points, weights, len(weights), _ptr(jac), negres)
+        if s != 0:
+            raise RuntimeError(f"oracle element failed ({s})")
+    return negres, jac
+
+
+def face_coefficients(Cx, X, face):
+    Cx = np.ascontiguousarray(Cx, dtype=np.float64)
+    nen = Cx.shape[0]
+    F = np.zeros(nen * 3)
+    if lib().tfo_face_coefficients(Cx.ravel(), np.ascontiguousarray(X, dtype=np.float64).ravel(), nen, face, F):
+        raise RuntimeError("face coefficients failed")
+    return F.reshape(nen, 3)
+
+
+def boundary_flow(Cx, X, face, state, use_ref=False):
+    Cx = np.ascontiguousarray(Cx, dtype=np.float64)
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    st = np.ascontiguousarray(state, dtype=np.float64).ravel()
+    f = ref().ref_boundary_flow if use_ref else lib().tfo_boundary_flow
+    return f(Cx.ravel(), X.ravel(), Cx.shape[0], face, st)
+
+
+def outlet_model(kind, resistance, proximal, distal, capacitance, reference_pressure, capacitor_pressure,
+                 flow, dt, use_ref=False):
+    p = C.c_double(); pc = C.c_double()
+    f = ref().ref_outlet_model if use_ref else lib().tfo_outlet_model
+    if f(kind, resistance, proximal, distal, capacitance, reference_pressure, capacitor_pressure, flow, dt,
+         C.byref(p), C.byref(pc)):
+        raise RuntimeError("outlet model rejected its input")
+    return p.value, pc.value
+
+
+def temporal(kind, value=0.0, mean=0.0, amplitude=0.0, period=1.0, phase=0.0, cosine=(), sine=(), time=0.0):
+    c = np.ascontiguousarray(cosine, dtype=np.float64)
+    s = np.ascontiguousarray(sine, dtype=np.float64)
+    if c.size == 0:
+        c = np.zeros(1); s = np.zeros(1); h = 0
+    else:
+        h = len(cosine)
+    return lib().tfo_temporal(kind, value, mean, amplitude, period, phase, c, s, h, time)
+
+
+# --------------------------------------------------------------------------
+# Mesh level
+# --------------------------------------------------------------------------
+
+class Pattern:
+    def __init__(self, nodes, element_offsets, connectivity):
+        L = lib()
+        eo = np.ascontiguousarray(element_offsets, dtype=np.int32)
+        cn = np.ascontiguousarray(connectivity, dtype=np.int32)
+        blocks = C.c_longlong()
+        st = L.tfo_block_pattern(nodes, len(eo) - 1, eo, cn, None, None, None, C.byref(blocks))
+        if st:
+            raise RuntimeError("block pattern failed")
+        self.nodes = nodes
+        self.row_offsets = np.zeros(nodes + 1, np.int32)
+        self.columns = np.zeros(blocks.value, np.int32)
+        self.diagonal = np.zeros(nodes, np.int32)
+        st = L.tfo_block_pattern(nodes, len(eo) - 1, eo, cn, _ptr(self.row_offsets), _ptr(self.columns),
+                                 _ptr(self.diagonal), C.byref(blocks))
+        if st:
+            raise RuntimeError("block pattern failed (missing diagonal)")
+        self.blocks = int(blocks.value)
+
+    def to_scipy(self, values):
+        import scipy.sparse as sp
+        v = np.asarray(values).reshape(-1, 4, 4)
+        return sp.bsr_matrix((v, self.columns, self.row_offsets),
+                             shape=(4 * self.nodes, 4 * self.nodes)).tocsr()
+
+
+def assemble(mesh, pattern, state, previous, density, viscosity, dt, jacobian=True):
+    """Global assembly of (block-CSR values, rhs = -r) over a FlatMesh-like object."""
+    L = lib()
+    values = np.zeros(pattern.blocks * 16) if jacobian else None
+    rhs = np.zeros(4 * mesh.nodes)
+    failed = C.c_int(-1)
+    prev = np.ascontiguousarray(previous if previous is not None else np.zeros(4 * mesh.nodes), np.float64)
+    st = L.tfo_assemble(mesh.nodes, mesh.elements, mesh.element_offsets, mesh.connectivity,
+                        mesh.extraction_offsets, mesh.extraction_columns, mesh.extraction_values,
+                        mesh.bezier_points, pattern.row_offsets, pattern.columns,
+                        np.ascontiguousarray(state, np.float64).ravel(), prev.ravel(),
+                        density, viscosity, dt, _ptr(values), rhs, C.byref(failed))
+    if st:
+        raise RuntimeError(f"oracle assembly failed at element {failed.value} ({st})")
+    return values, rhs
+
+
+def apply_dirichlet(pattern, vmask, pmask, velocity, pressure, state, values, rhs):
+    lib().tfo_apply_dirichlet(pattern.nodes, pattern.row_offsets, pattern.diagonal,
+                              np.ascontiguousarray(vmask, np.int32), np.ascontiguousarray(pmask, np.int32),
+                              np.ascontiguousarray(velocity, np.float64).ravel(),
+                              np.ascontiguousarray(pressure, np.float64).ravel(),
+                              np.ascontiguousarray(state, np.float64).ravel(), _ptr(values), rhs)
+
+
+def spmv(pattern, values, x):
+    y = np.zeros(4 * pattern.nodes)
+    lib().tfo_spmv(pattern.nodes, pattern.row_offsets, pattern.columns, values,
+                   np.ascontiguousarray(x, np.float64), y)
+    return y
+
+
+def gmres_bjacobi(pattern, values, rhs, x0=None, restart=200, maxit=5000, rtol=1e-8):
+    x = np.zeros(4 * pattern.nodes) if x0 is None else np.array(x0, np.float64)
+    res = C.c_double(); singular = C.c_int()
+    it = lib().tfo_gmres_bjacobi(pattern.nodes, pattern.row_offsets, pattern.columns, pattern.diagonal,
+                                 values, np.ascontiguousarray(rhs, np.float64), x, restart, maxit, rtol,
+                                 C.byref(res), C.byref(singular))
+    return x, it, res.value, singular.value
+
+
+def newton_step(mesh, pattern, state, previous, density, viscosity, dt, vmask, pmask, velocity, pressure,
+                traction_rhs=None):
+    """One reference Newton iteration (iga_cuda.cu:959-1033) with a direct solve.
+
+    Returns (new_state, residual_norm_after_bc, raw_rhs_before_bc)."""
+    import scipy.sparse.linalg as spla
+    values, rhs = assemble(mesh, pattern, state, previous, density, viscosity, dt)
+    if traction_rhs is not None:
+        rhs += traction_rhs
+    raw = rhs.copy()
+    apply_dirichlet(pattern, vmask, pmask, velocity, pressure, state, values, rhs)
+    norm = float(np.linalg.norm(rhs))
+    A = pattern.to_scipy(values)
+    update = spla.spsolve(A.tocsc(), rhs)
+    return np.asarray(state, np.float64).ravel() + update, norm, raw
+
+
+def max_threads() -> int:
+    return int(lib().tfo_max_threads())
+
+
+os.environ.setdefault("OMP_PROC_BIND", "false")

@@ -1,0 +1,225 @@
+// ref_shim.cpp -- C entry points around the reference's own header-only
+// element code, compiled unmodified from the reference sources (see
+// oracle/Makefile) into oracle/_ref/libtfiga_ref.so.  TEST INFRASTRUCTURE
+// ONLY: it pins the C restatement in ns_oracle.c and serves as the reference
+// CPU arm of the bench.  Nothing in the product links it.
+//
+// Wrapped reference routines:
+//   iga::BuildNavierStokesElement      solvers/cpu/include/NavierStokesElement.hpp:390-397
+//   iga::EvaluateBasis                 solvers/cpu/include/TransportElement.hpp:118-206
+//   iga::IntegrateBoundaryFlow         solvers/cpu/include/BoundaryFlow.hpp:165-200
+//   iga::IntegrateBoundaryPressureTraction solvers/cpu/include/BoundaryFlow.hpp:445-475
+//   iga::EvaluateOutletModel           include/OutletModel.hpp:70-90
+//   iga::Database::Load                solvers/cpu/include/IgaDatabase.hpp:124-161
+//   iga::WallTraceBasis                solvers/cpu/include/BoundarySupport.hpp:134-150
+#include "BoundaryFlow.hpp"
+#include "BoundarySupport.hpp"
+#include "NavierStokesElement.hpp"
+#include "OutletModel.hpp"
+
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+namespace {
+
+iga::Element MakeElement(const double* C, const double* X, int nen)
+{
+	iga::Element element;
+	element.connectivity.resize(static_cast<std::size_t>(nen));
+	element.extraction.resize(static_cast<std::size_t>(nen));
+	for (int a = 0; a < nen; ++a) {
+		element.connectivity[static_cast<std::size_t>(a)] = a;
+		for (int p = 0; p < 64; ++p) element.extraction[static_cast<std::size_t>(a)][static_cast<std::size_t>(p)] = C[a*64+p];
+	}
+	for (int p = 0; p < 64; ++p)
+		for (int d = 0; d < 3; ++d) element.bezier_points[static_cast<std::size_t>(p)][static_cast<std::size_t>(d)] = X[p*3+d];
+	return element;
+}
+
+std::vector<std::array<double, 4>> Nodal(const double* values, int nen)
+{
+	std::vector<std::array<double, 4>> result(static_cast<std::size_t>(nen));
+	for (int a = 0; a < nen; ++a)
+		for (int f = 0; f < 4; ++f) result[static_cast<std::size_t>(a)][static_cast<std::size_t>(f)] = values ? values[a*4+f] : 0.0;
+	return result;
+}
+
+thread_local std::string last_error;
+
+} // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return last_error.c_str(); }
+
+// Element residual (-r) and exact tangent at the reference 4x4x4 rule.
+// jac may be null (residual only).  Returns 0 or -1 on a reference exception.
+int ref_ns_element(const double* C, const double* X, int nen, const double* state,
+	const double* previous, double density, double viscosity, double dt, double* jac, double* negres)
+{
+	try {
+		const auto element = MakeElement(C, X, nen);
+		const auto nodal = Nodal(state, nen);
+		const auto prev = dt > 0.0 ? Nodal(previous, nen) : std::vector<std::array<double, 4>>{};
+		iga::FullCell4x4x4VolumeQuadratureProvider quadrature(element);
+		const auto system = iga::BuildNavierStokesElement(element, nodal, prev,
+			{density, viscosity, dt}, quadrature.Rule(),
+			jac ? iga::NavierStokesAssemblyRequest::ResidualAndJacobian
+				: iga::NavierStokesAssemblyRequest::ResidualOnly);
+		if (jac) std::memcpy(jac, system.jacobian.data(), sizeof(double)*system.jacobian.size());
+		std::memcpy(negres, system.negative_residual.data(), sizeof(double)*system.negative_residual.size());
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+// Element residual with an explicit single-point rule (reference test form).
+int ref_ns_element_points(const double* C, const double* X, int nen, const double* state,
+	const double* previous, double density, double viscosity, double dt,
+	const double* points, const double* weights, int count, double* jac, double* negres)
+{
+	try {
+		const auto element = MakeElement(C, X, nen);
+		std::vector<iga::VolumeQuadraturePoint> rule;
+		for (int q = 0; q < count; ++q)
+			rule.push_back({{points[3*q], points[3*q+1], points[3*q+2]}, weights[q]});
+		const auto system = iga::BuildNavierStokesElement(element, Nodal(state, nen),
+			dt > 0.0 ? Nodal(previous, nen) : std::vector<std::array<double, 4>>{},
+			{density, viscosity, dt}, iga::VolumeQuadratureRule(rule));
+		if (jac) std::memcpy(jac, system.jacobian.data(), sizeof(double)*system.jacobian.size());
+		std::memcpy(negres, system.negative_residual.data(), sizeof(double)*system.negative_residual.size());
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+int ref_basis(const double* C, const double* X, int nen, double u, double v, double w,
+	double* N, double* dN, double* H, double* inverse, double* raw_det)
+{
+	try {
+		const auto basis = iga::EvaluateBasis(MakeElement(C, X, nen), u, v, w, true);
+		for (int a = 0; a < nen; ++a) {
+			N[a] = basis.value[static_cast<std::size_t>(a)];
+			for (int i = 0; i < 3; ++i) {
+				dN[a*3+i] = basis.gradient[static_cast<std::size_t>(a)][static_cast<std::size_t>(i)];
+				for (int j = 0; j < 3; ++j)
+					H[a*9+i*3+j] = basis.hessian[static_cast<std::size_t>(a)][static_cast<std::size_t>(i)][static_cast<std::size_t>(j)];
+			}
+		}
+		for (int i = 0; i < 3; ++i)
+			for (int j = 0; j < 3; ++j) inverse[i*3+j] = basis.inverse_jacobian[static_cast<std::size_t>(i)][static_cast<std::size_t>(j)];
+		*raw_det = basis.raw_determinant;
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+double ref_boundary_flow(const double* C, const double* X, int nen, int face, const double* state)
+{
+	return iga::IntegrateBoundaryFlow(MakeElement(C, X, nen), static_cast<std::size_t>(face), Nodal(state, nen));
+}
+
+int ref_pressure_traction(const double* C, const double* X, int nen, int face, double pressure, double* out)
+{
+	try {
+		const auto local = iga::IntegrateBoundaryPressureTraction(MakeElement(C, X, nen),
+			static_cast<std::size_t>(face), pressure);
+		std::memcpy(out, local.data(), sizeof(double)*local.size());
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+int ref_outlet_model(int kind, double resistance, double proximal, double distal, double capacitance,
+	double reference_pressure, double capacitor_pressure, double flow, double dt,
+	double* pressure, double* new_capacitor_pressure)
+{
+	try {
+		iga::OutletModelState model;
+		model.kind = kind == 0 ? iga::FieldBoundaryKind::Resistance
+			: kind == 1 ? iga::FieldBoundaryKind::WindkesselRC : iga::FieldBoundaryKind::WindkesselRCR;
+		model.resistance = resistance;
+		model.proximal_resistance = proximal;
+		model.distal_resistance = distal;
+		model.capacitance = capacitance;
+		model.reference_pressure = reference_pressure;
+		model.capacitor_pressure = capacitor_pressure;
+		const auto result = iga::EvaluateOutletModel(model, flow, dt);
+		*pressure = result.pressure;
+		*new_capacitor_pressure = result.capacitor_pressure;
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+// Database header (version, ranks, elements, nodes) through iga::Database.
+int ref_ntiga_header(const char* path, std::uint64_t* out)
+{
+	try {
+		iga::Database database(path);
+		const auto& h = database.header();
+		out[0] = h.version; out[1] = h.ranks; out[2] = h.elements; out[3] = h.nodes;
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+// One element through iga::Database::Load: nen, labels[6], connectivity,
+// dense extraction [nen*64] and Bezier points [192].
+int ref_ntiga_element(const char* path, std::uint64_t index, int* nen, int* labels,
+	int* connectivity, double* extraction, double* bezier)
+{
+	try {
+		iga::Database database(path);
+		const auto element = database.Load(index);
+		*nen = static_cast<int>(element.connectivity.size());
+		for (int k = 0; k < 6; ++k) labels[k] = element.boundary_labels[static_cast<std::size_t>(k)];
+		for (std::size_t a = 0; a < element.connectivity.size(); ++a) {
+			connectivity[a] = element.connectivity[a];
+			for (std::size_t p = 0; p < 64; ++p) extraction[a*64+p] = element.extraction[a][p];
+		}
+		for (std::size_t p = 0; p < 64; ++p)
+			for (std::size_t d = 0; d < 3; ++d) bezier[p*3+d] = element.bezier_points[p][d];
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+// Wall-trace no-slip basis set (iga_cuda.cu:748 -> BoundarySupport.hpp:134-150).
+// Writes up to `capacity` node ids (sorted) and returns the count, or -1.
+long long ref_wall_trace(const char* database_path, const char* vtk_path, int* out, long long capacity)
+{
+	try {
+		iga::Database database(database_path);
+		const auto mesh = iga::ReadLabeledHexMesh(vtk_path, database.header().nodes, database.header().elements);
+		const auto nodes = iga::WallTraceBasis(database, mesh);
+		long long count = 0;
+		for (const auto node : nodes) {
+			if (count < capacity) out[count] = node;
+			++count;
+		}
+		return count;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+} // extern "C"
