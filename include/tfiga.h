@@ -1,0 +1,203 @@
+/*
+ * tfiga.h -- C ABI of the B200 body-fitted IGA Navier-Stokes hot path.
+ *
+ * This is the drop-in boundary for the solve behind the reference's
+ * `iga_cuda navier-stokes` command (solvers/cuda/src/iga_cuda.cu:734-1153).
+ * The reference has no FFI of its own: its host loop includes CUDA templates
+ * directly.  Each entry point below replaces one of those in-process
+ * interfaces; the reference file:line it stands in for is given beside it.
+ *
+ * Conventions
+ *  - Every call returns an int status: 0 on success, a negative TFIGA_E_*
+ *    code on failure; tfiga_last_error() gives the message of the calling
+ *    thread's last failure.  No C++ exception crosses this boundary.
+ *  - Arrays are plain caller-owned host pointers unless the name says
+ *    "device"; sizes are explicit.  Nodal vectors are node-major with 4
+ *    fields (u, v, w, p): value[4*node + field].
+ *  - A tfiga_ns handle owns device state on the current CUDA device and its
+ *    own stream; a handle is not thread-safe, use one per host thread.
+ *  - Every device-side wait is bounded and reports a status.
+ *  - There is no CPU fallback: without a usable sm_100 device the create
+ *    calls fail with TFIGA_E_CUDA.
+ */
+#ifndef TFIGA_H
+#define TFIGA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TFIGA_OK 0
+#define TFIGA_E_INVALID (-1)       /* bad argument or inconsistent sizes */
+#define TFIGA_E_CUDA (-2)          /* CUDA runtime / device failure */
+#define TFIGA_E_IO (-3)            /* file could not be read or written */
+#define TFIGA_E_FORMAT (-4)        /* malformed .ntiga / case input */
+#define TFIGA_E_GEOMETRY (-5)      /* non-positive element Jacobian */
+#define TFIGA_E_NOT_CONVERGED (-6) /* linear or nonlinear solve did not converge */
+#define TFIGA_E_UNSUPPORTED (-7)   /* valid input outside what this build supports */
+#define TFIGA_E_MEMORY (-8)        /* device or host allocation failed */
+
+typedef struct tfiga_mesh tfiga_mesh;
+typedef struct tfiga_ns tfiga_ns;
+
+/* Flattened mesh, the layout of iga::cuda::FlatMesh
+ * (solvers/cuda/include/DeviceMesh.hpp:16-57). */
+typedef struct tfiga_mesh_desc {
+	int64_t nodes;
+	int64_t elements;
+	const int32_t* element_offsets;    /* [elements+1] */
+	const int32_t* connectivity;       /* [element_offsets[elements]] */
+	const int32_t* extraction_offsets; /* [element_offsets[elements]+1] */
+	const uint8_t* extraction_columns; /* [nnz] Bernstein index i+4j+16k */
+	const double* extraction_values;   /* [nnz] */
+	const double* bezier_points;       /* [elements*64*3] */
+	const int32_t* boundary_labels;    /* [elements*6] face labels, -1 = none; may be NULL */
+} tfiga_mesh_desc;
+
+typedef struct tfiga_mesh_info {
+	int64_t nodes;
+	int64_t elements;
+	int32_t max_basis;
+	int64_t basis_entries;
+	int64_t extraction_nonzeros;
+	int64_t block_nonzeros;       /* 4x4 blocks of the node-graph pattern */
+	int32_t max_block_row;
+	double min_detj;              /* min 0.125 det(dx/dxi) over the 4x4x4 Gauss points */
+	int64_t bad_samples;          /* Gauss points with det <= 0 or non-finite */
+	int64_t device_bytes;         /* resident mesh + pattern + basis tables */
+} tfiga_mesh_info;
+
+/* Solver parameters (the options of iga_cuda.cu:402-417 and the fixed
+ * GMRES settings of :858 and :1015). */
+typedef struct tfiga_ns_params {
+	double density;
+	double viscosity;              /* dynamic viscosity */
+	double dt;                     /* backward-Euler step; 0 = steady */
+	int32_t max_newton;            /* default 12 */
+	double nonlinear_rtol;         /* default 1e-5 */
+	double nonlinear_atol;         /* default 1e-10 (scaled by sqrt(4n)) */
+	double mass_rtol;              /* default 1e-3 */
+	int32_t gmres_restart;         /* default 200 */
+	int32_t gmres_max_iterations;  /* default 5000 */
+	double gmres_rtol;             /* default 1e-8 (preconditioned residual) */
+} tfiga_ns_params;
+
+/* One Newton iteration's log record (iga_cuda.cu:1000-1009, 1034-1045). */
+typedef struct tfiga_newton_report {
+	int32_t converged;             /* 1 when the convergence test passed before solving */
+	int32_t linear_iterations;
+	int32_t singular_diagonal_blocks;
+	double residual_l2;            /* ||rhs|| after the Dirichlet rows */
+	double tolerance;
+	double continuity_l2;          /* from the raw rhs before Dirichlet rows */
+	double continuity_sum;
+	double net_boundary_flow;
+	double absolute_boundary_flow;
+	double relative_mass_imbalance;
+	double update_l2;
+	double linear_residual;
+	double assembly_ms;
+	double linear_ms;
+} tfiga_newton_report;
+
+/* One physical step (the Newton loop of iga_cuda.cu:956-1054). */
+typedef struct tfiga_step_report {
+	int32_t converged;
+	int32_t newton_iterations;
+	int32_t linear_iterations;
+	double residual_l2;
+	double initial_residual_l2;
+	double relative_mass_imbalance;
+	double assembly_ms;
+	double linear_ms;
+} tfiga_step_report;
+
+/* ---- errors ------------------------------------------------------------ */
+/* Copies the calling thread's last error message; returns its full length. */
+size_t tfiga_last_error(char* buffer, size_t capacity);
+/* Library build string (arch, version). */
+const char* tfiga_version(void);
+
+/* ---- mesh -------------------------------------------------------------- */
+/* Replaces FlatMesh + DeviceMesh + BlockPattern + DevicePattern + ReferenceData
+ * + GeometryData (iga_cuda.cu:820-851; DeviceMesh.hpp:27-114; BlockCsr.hpp:15-55;
+ * iga_cuda.cu:73-220): uploads the mesh, builds the block pattern and the
+ * per-element basis tables on the device, and checks the geometry. */
+int tfiga_mesh_create(const tfiga_mesh_desc* desc, tfiga_mesh** out);
+/* Same from a packed .ntiga file (iga::Database, IgaDatabase.hpp:95-161). */
+int tfiga_mesh_load_ntiga(const char* path, tfiga_mesh** out);
+int tfiga_mesh_destroy(tfiga_mesh* mesh);
+/* mesh-check numbers (iga_cuda.cu:604-617). */
+int tfiga_mesh_info_get(const tfiga_mesh* mesh, tfiga_mesh_info* info);
+/* Block-CSR pattern (BlockPattern, BlockCsr.hpp:15-55): row_offsets[nodes+1],
+ * columns[blocks], diagonal[nodes]; any pointer may be NULL. */
+int tfiga_mesh_pattern(const tfiga_mesh* mesh, int32_t* row_offsets, int32_t* columns, int32_t* diagonal);
+
+/* ---- Navier-Stokes solver -------------------------------------------- */
+void tfiga_ns_default_params(tfiga_ns_params* params);
+/* Allocates matrix, vectors and the GMRES workspace (iga_cuda.cu:858-865, 899). */
+int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out);
+int tfiga_ns_destroy(tfiga_ns* ns);
+/* Dirichlet masks and values (ResolvedBoundaryConditions after the wall trace,
+ * iga_cuda.cu:750-797 and :854-857): masks [nodes] (nonzero = constrained),
+ * velocity [3*nodes], pressure [nodes]; pressure may be NULL (all zero). */
+int tfiga_ns_set_dirichlet(tfiga_ns* ns, const int32_t* velocity_mask, const int32_t* pressure_mask,
+	const double* velocity, const double* pressure);
+/* Dirichlet values only (per-step waveform update, iga_cuda.cu:944-946). */
+int tfiga_ns_set_dirichlet_values(tfiga_ns* ns, const double* velocity, const double* pressure);
+/* Natural pressure traction on labelled faces (IntegratePressureTractionForces,
+ * PressureTractionFlow.hpp:41-64; iga_cuda.cu:948-951), computed on the device. */
+int tfiga_ns_set_tractions(tfiga_ns* ns, const int32_t* labels, const double* pressures, int32_t count);
+/* State and previous state [4*nodes]; previous may be NULL (= state). */
+int tfiga_ns_set_state(tfiga_ns* ns, const double* state, const double* previous);
+int tfiga_ns_get_state(tfiga_ns* ns, double* state);
+/* previous <- state (start of a physical step, iga_cuda.cu:918-920). */
+int tfiga_ns_commit_step(tfiga_ns* ns);
+/* Raw assembly for parity tests: Jacobian values [blocks*16] (row-major 4x4
+ * blocks) and rhs = -r + traction [4*nodes], before the Dirichlet rows;
+ * either output may be NULL (AssembleNavierStokesKernel + the traction axpy,
+ * iga_cuda.cu:959-969, with the exact tangent of NavierStokesElement.hpp:244-312). */
+int tfiga_ns_assemble(tfiga_ns* ns, double* values, double* rhs);
+/* Dirichlet rows applied to the last assembly (IgaCudaKernels.cuh:436-463):
+ * copies back values/rhs after the rows were applied; either may be NULL. */
+int tfiga_ns_apply_dirichlet(tfiga_ns* ns, double* values, double* rhs);
+/* Block-Jacobi GMRES on the current (Dirichlet-applied) system
+ * (SolveGmres, Gmres.hpp:192-336): update = A^{-1} rhs. */
+int tfiga_ns_solve_linear(tfiga_ns* ns, double rtol, int32_t max_iterations, double* update,
+	int32_t* iterations, double* residual);
+/* One full Newton iteration: assemble, diagnostics, Dirichlet rows, norm and
+ * convergence test, GMRES, state += update (iga_cuda.cu:956-1046).
+ * initial_residual is the step's first residual norm (<0 on the first iteration). */
+int tfiga_ns_newton_iteration(tfiga_ns* ns, double initial_residual, tfiga_newton_report* report);
+/* One physical step: the Newton loop to convergence (iga_cuda.cu:952-1054). */
+int tfiga_ns_step(tfiga_ns* ns, tfiga_step_report* report);
+/* Outward flow through each labelled boundary (IntegrateBoundaryFlow,
+ * BoundaryFlow.hpp:165-200; MeasureFlowConvergence iga_cuda.cu:520-557). */
+int tfiga_ns_boundary_flows(tfiga_ns* ns, const int32_t* labels, int32_t count, double* flows);
+
+/* ---- raw kernels on device pointers (measurement and integration) ------ */
+/* y = A x over the mesh pattern (BlockSpmvKernel<4>, SparseKernels.cuh:25-40). */
+int tfiga_ns_spmv_device(tfiga_ns* ns, const double* x_device, double* y_device);
+/* Device pointers of the handle's matrix values and state (for in-HBM timing). */
+int tfiga_ns_device_buffers(tfiga_ns* ns, double** values, double** state, double** rhs);
+/* Counters of kernel launches issued by this handle (for launch accounting). */
+int64_t tfiga_ns_launch_count(const tfiga_ns* ns);
+/* Waits for the handle's stream (bounded by the driver). */
+int tfiga_ns_synchronize(tfiga_ns* ns);
+
+/* ---- drop-in command ------------------------------------------------- */
+/* `navier-stokes DATABASE CASE_DIR [MAX_NEWTON] [OUTPUT] [options]`, the argv of
+ * iga_cuda's navier-stokes command (ParseCudaFlowOptions iga_cuda.cu:447-498,
+ * NavierStokes :734-1153).  argv[0] is the program name, argv[1] the command
+ * ("navier-stokes", "mesh-check" or "device-info").  Prints the reference's
+ * key=value lines to stdout; returns the process exit code (0 or 1). */
+int tfiga_main(int argc, char** argv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

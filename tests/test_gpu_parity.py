@@ -1,0 +1,168 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerances (FP64 throughout):
+* assembly (Jacobian blocks, rhs): 1e-12 relative in norm per field pair;
+* boundary flows / tractions: 1e-12 relative;
+* linear solve: true residual <= 1e-10 ||b|| and 1e-8 against a direct solve;
+* Newton steps on the 1,280-element cylinder: velocity and pressure within
+  1e-10 relative L2 of the oracle after every Newton step (both linear solves
+  far below the production GMRES tolerance, as parity at this level needs).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RHO, MU, DT = 1060.0, 3.5e-3, 1e-3
+
+
+@pytest.fixture(scope="module")
+def api():
+    from tubularflowiga_b200 import api as a
+    return a
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+def random_state(nodes, seed, speed=0.2, pressure=20.0):
+    rng = np.random.default_rng(seed)
+    s = rng.normal(size=(nodes, 4))
+    s[:, :3] *= speed
+    s[:, 3] *= pressure
+    return s.ravel()
+
+
+def blockwise_rel(values, ref):
+    v = values.reshape(-1, 4, 4)
+    r = ref.reshape(-1, 4, 4)
+    return max(rel(v[:, i, f], r[:, i, f]) for i in range(4) for f in range(4))
+
+
+def check_assembly(api, flat, rho, mu, dt, seed):
+    mesh = api.Mesh(flat)
+    ns = api.NavierStokes(mesh, density=rho, viscosity=mu, dt=dt)
+    st = random_state(flat.nodes, seed)
+    pv = random_state(flat.nodes, seed + 1)
+    ns.set_state(st, pv)
+    values, rhs = ns.assemble()
+    P = O.Pattern(flat.nodes, flat.element_offsets, flat.connectivity)
+    ro, cols, diag = mesh.pattern()
+    assert np.array_equal(ro, P.row_offsets) and np.array_equal(cols, P.columns) and np.array_equal(diag, P.diagonal)
+    ov, orhs = O.assemble(flat, P, st, pv, rho, mu, dt)
+    assert blockwise_rel(values, ov) < 1e-12
+    for f in range(4):
+        assert rel(rhs[f::4], orhs[f::4]) < 1e-12
+    return mesh, ns, P
+
+
+def test_assembly_small_tube(api, small_tube):
+    check_assembly(api, small_tube.mesh, RHO, MU, DT, 0)
+
+
+def test_assembly_steady(api, small_tube):
+    check_assembly(api, small_tube.mesh, RHO, MU, 0.0, 3)
+
+
+def test_assembly_reference_tube_ragged(api, reference_tube):
+    """The reference-generated mesh: nen in {36, 42, 48, 56, 64}, normalised units."""
+    from tubularflowiga_b200 import ntiga
+    flat = ntiga.read(reference_tube / "tube-1.ntiga")
+    assert len(set(np.diff(flat.element_offsets))) >= 4
+    check_assembly(api, flat, 1.0, 1.0, 0.1, 5)
+
+
+def test_assembly_cylinder_1280(api, cylinder_1280):
+    check_assembly(api, cylinder_1280.mesh, RHO, MU, DT, 7)
+
+
+def test_mesh_load_ntiga_and_geometry(api, reference_tube):
+    from tubularflowiga_b200 import ntiga
+    import ctypes
+    flat = ntiga.read(reference_tube / "tube-1.ntiga")
+    mesh = api.Mesh(reference_tube / "tube-1.ntiga")
+    assert mesh.info["elements"] == flat.elements and mesh.info["nodes"] == flat.nodes
+    bad = ctypes.c_int()
+    mins = [O.lib().tfo_min_determinant(np.ascontiguousarray(flat.element(e)[2].ravel()), ctypes.byref(bad))
+            for e in range(flat.elements)]
+    assert abs(mesh.info["min_detj"] - min(mins)) <= 1e-12 * abs(min(mins))
+    assert mesh.info["bad_samples"] == 0
+
+
+def test_boundary_flows_and_traction(api, small_tube):
+    flat = small_tube.mesh
+    mesh = api.Mesh(flat)
+    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT)
+    st = random_state(flat.nodes, 11)
+    ns.set_state(st, st)
+    flows = ns.boundary_flows([0, 1, 2, 7])
+    expect = np.zeros(3)
+    trac = np.zeros(4 * flat.nodes)
+    for e in range(flat.elements):
+        conn, C, X, labels = flat.element(e)
+        for face, label in enumerate(labels):
+            if label < 0:
+                continue
+            F = O.face_coefficients(C, X, face)
+            expect[label] += float((F * st.reshape(-1, 4)[conn, :3]).sum())
+            if label == 2:
+                np.add.at(trac.reshape(-1, 4), (conn, slice(0, 3)), -13.0 * F)
+    assert flows[3] == 0.0
+    for k in range(3):
+        assert abs(flows[k] - expect[k]) <= 1e-12 * max(1e-30, np.abs(expect).max())
+    _, r0 = ns.assemble(values=False)
+    ns.set_tractions({2: 13.0})
+    _, r1 = ns.assemble(values=False)
+    assert rel(r1 - r0, trac) < 1e-12
+
+
+def test_spmv_and_gmres(api, small_tube):
+    import scipy.sparse.linalg as spla
+    import torch
+    flat = small_tube.mesh
+    vmask, pmask, vel = api.tube_boundary_conditions(small_tube, 0.2)
+    mesh, ns, P = check_assembly(api, flat, RHO, MU, DT, 13)
+    ns.set_dirichlet(vmask, pmask, vel)
+    values, rhs = ns.apply_dirichlet()
+    A = P.to_scipy(values)
+    x = torch.randn(4 * flat.nodes, dtype=torch.float64, device="cuda")
+    y = torch.zeros_like(x)
+    ns.spmv_device(x.data_ptr(), y.data_ptr())
+    ns.synchronize()
+    assert rel(y.cpu().numpy(), A @ x.cpu().numpy()) < 1e-14
+    u, iterations, residual = ns.solve_linear(rtol=1e-12, max_iterations=20000)
+    assert iterations > 0
+    assert np.linalg.norm(A @ u - rhs) <= 1e-10 * np.linalg.norm(rhs)
+    direct = spla.spsolve(A.tocsc(), rhs)
+    assert rel(u, direct) < 1e-8
+
+
+def test_newton_steps_match_oracle_cylinder_1280(api, cylinder_1280):
+    """C1: parity within 1e-10 relative L2 on velocity and pressure after every Newton step."""
+    tube = cylinder_1280
+    flat = tube.mesh
+    vmask, pmask, vel = api.tube_boundary_conditions(tube, 0.2)
+    state0 = api.initial_state(vmask, vel)
+    mesh = api.Mesh(flat)
+    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, gmres_rtol=1e-14,
+                          gmres_max_iterations=50000, gmres_restart=200)
+    ns.set_dirichlet(vmask, pmask, vel)
+    ns.set_tractions({2: 0.0})
+    ns.set_state(state0, state0)
+    P = O.Pattern(flat.nodes, flat.element_offsets, flat.connectivity)
+    oracle_state = state0.copy()
+    initial = -1.0
+    for it in range(3):
+        report = ns.newton_iteration(initial)
+        oracle_state, norm, _ = O.newton_step(flat, P, oracle_state, state0, RHO, MU, DT, vmask, pmask,
+                                              vel.ravel(), np.zeros(flat.nodes))
+        assert abs(report["residual_l2"] - norm) <= 1e-9 * max(norm, 1e-30)
+        if initial < 0:
+            initial = report["residual_l2"]
+        gpu = ns.get_state().reshape(-1, 4)
+        ref = oracle_state.reshape(-1, 4)
+        assert rel(gpu[:, :3], ref[:, :3]) < 1e-10, it
+        assert rel(gpu[:, 3], ref[:, 3]) < 1e-10, it

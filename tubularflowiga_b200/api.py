@@ -1,0 +1,302 @@
+"""Python binding of the C ABI in include/tfiga.h (ctypes, no torch types).
+
+The product path is the CUDA library ``lib/libtfiga_b200.so``; there is no
+CPU fallback: loading fails loudly when the library is missing, and the
+create calls fail without an sm_100 device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from .ntiga import FlatMesh
+
+LIBRARY = Path(__file__).resolve().parent / "lib" / "libtfiga_b200.so"
+
+
+class TfigaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"tfiga error {status}: {message}")
+        self.status = status
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("nodes", C.c_int64), ("elements", C.c_int64), ("element_offsets", C.c_void_p),
+                ("connectivity", C.c_void_p), ("extraction_offsets", C.c_void_p),
+                ("extraction_columns", C.c_void_p), ("extraction_values", C.c_void_p),
+                ("bezier_points", C.c_void_p), ("boundary_labels", C.c_void_p)]
+
+
+class MeshInfo(C.Structure):
+    _fields_ = [("nodes", C.c_int64), ("elements", C.c_int64), ("max_basis", C.c_int32),
+                ("basis_entries", C.c_int64), ("extraction_nonzeros", C.c_int64), ("block_nonzeros", C.c_int64),
+                ("max_block_row", C.c_int32), ("min_detj", C.c_double), ("bad_samples", C.c_int64),
+                ("device_bytes", C.c_int64)]
+
+
+class NsParams(C.Structure):
+    _fields_ = [("density", C.c_double), ("viscosity", C.c_double), ("dt", C.c_double),
+                ("max_newton", C.c_int32), ("nonlinear_rtol", C.c_double), ("nonlinear_atol", C.c_double),
+                ("mass_rtol", C.c_double), ("gmres_restart", C.c_int32), ("gmres_max_iterations", C.c_int32),
+                ("gmres_rtol", C.c_double)]
+
+
+class NewtonReport(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("linear_iterations", C.c_int32),
+                ("singular_diagonal_blocks", C.c_int32), ("residual_l2", C.c_double), ("tolerance", C.c_double),
+                ("continuity_l2", C.c_double), ("continuity_sum", C.c_double), ("net_boundary_flow", C.c_double),
+                ("absolute_boundary_flow", C.c_double), ("relative_mass_imbalance", C.c_double),
+                ("update_l2", C.c_double), ("linear_residual", C.c_double), ("assembly_ms", C.c_double),
+                ("linear_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class StepReport(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("newton_iterations", C.c_int32), ("linear_iterations", C.c_int32),
+                ("residual_l2", C.c_double), ("initial_residual_l2", C.c_double),
+                ("relative_mass_imbalance", C.c_double), ("assembly_ms", C.c_double), ("linear_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# Every exported symbol of include/tfiga.h with its signature.
+SIGNATURES = {
+    "tfiga_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "tfiga_version": (C.c_char_p, []),
+    "tfiga_mesh_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(C.c_void_p)]),
+    "tfiga_mesh_load_ntiga": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "tfiga_mesh_destroy": (C.c_int, [C.c_void_p]),
+    "tfiga_mesh_info_get": (C.c_int, [C.c_void_p, C.POINTER(MeshInfo)]),
+    "tfiga_mesh_pattern": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_ns_default_params": (None, [C.POINTER(NsParams)]),
+    "tfiga_ns_create": (C.c_int, [C.c_void_p, C.POINTER(NsParams), C.POINTER(C.c_void_p)]),
+    "tfiga_ns_destroy": (C.c_int, [C.c_void_p]),
+    "tfiga_ns_set_dirichlet": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_ns_set_dirichlet_values": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_ns_set_tractions": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "tfiga_ns_set_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_ns_get_state": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tfiga_ns_commit_step": (C.c_int, [C.c_void_p]),
+    "tfiga_ns_assemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_ns_apply_dirichlet": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_ns_solve_linear": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, C.c_void_p, C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_double)]),
+    "tfiga_ns_newton_iteration": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(NewtonReport)]),
+    "tfiga_ns_step": (C.c_int, [C.c_void_p, C.POINTER(StepReport)]),
+    "tfiga_ns_boundary_flows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "tfiga_ns_spmv_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_ns_device_buffers": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                          C.POINTER(C.c_void_p)]),
+    "tfiga_ns_launch_count": (C.c_int64, [C.c_void_p]),
+    "tfiga_ns_synchronize": (C.c_int, [C.c_void_p]),
+    "tfiga_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIBRARY.exists():
+            raise ImportError(f"{LIBRARY} is not built: run `python -m tubularflowiga_b200.build` "
+                              "(there is no CPU fallback)")
+        L = C.CDLL(str(LIBRARY))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(4096)
+    lib().tfiga_last_error(buf, 4096)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int):
+    if status != 0:
+        raise TfigaError(status, last_error())
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def default_params(**overrides) -> NsParams:
+    p = NsParams()
+    lib().tfiga_ns_default_params(C.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+class Mesh:
+    """Device-resident mesh (tfiga_mesh)."""
+
+    def __init__(self, source):
+        L = lib()
+        self._h = C.c_void_p()
+        if isinstance(source, (str, Path)):
+            check(L.tfiga_mesh_load_ntiga(str(source).encode(), C.byref(self._h)))
+        else:
+            m: FlatMesh = source.contiguous()
+            self._keep = m
+            d = MeshDesc(m.nodes, m.elements, _p(m.element_offsets), _p(m.connectivity),
+                         _p(m.extraction_offsets), _p(m.extraction_columns), _p(m.extraction_values),
+                         _p(m.bezier_points), _p(m.boundary_labels))
+            check(L.tfiga_mesh_create(C.byref(d), C.byref(self._h)))
+        info = MeshInfo()
+        check(L.tfiga_mesh_info_get(self._h, C.byref(info)))
+        self.info = {k: getattr(info, k) for k, _ in MeshInfo._fields_}
+        self.nodes = int(info.nodes)
+        self.blocks = int(info.block_nonzeros)
+
+    def pattern(self):
+        ro = np.zeros(self.nodes + 1, np.int32)
+        cols = np.zeros(self.blocks, np.int32)
+        diag = np.zeros(self.nodes, np.int32)
+        check(lib().tfiga_mesh_pattern(self._h, _p(ro), _p(cols), _p(diag)))
+        return ro, cols, diag
+
+    def close(self):
+        if self._h:
+            lib().tfiga_mesh_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class NavierStokes:
+    """Device-resident Navier-Stokes solver (tfiga_ns)."""
+
+    def __init__(self, mesh: Mesh, **params):
+        self.mesh = mesh
+        self.params = default_params(**params)
+        self._h = C.c_void_p()
+        check(lib().tfiga_ns_create(mesh._h, C.byref(self.params), C.byref(self._h)))
+        self.nodes = mesh.nodes
+
+    def set_dirichlet(self, velocity_mask, pressure_mask, velocity, pressure=None):
+        vm = np.ascontiguousarray(velocity_mask, np.int32)
+        pm = np.ascontiguousarray(pressure_mask if pressure_mask is not None else np.zeros(self.nodes), np.int32)
+        v = np.ascontiguousarray(velocity, np.float64).ravel()
+        p = None if pressure is None else np.ascontiguousarray(pressure, np.float64)
+        check(lib().tfiga_ns_set_dirichlet(self._h, _p(vm), _p(pm), _p(v), _p(p)))
+
+    def set_dirichlet_values(self, velocity, pressure=None):
+        v = np.ascontiguousarray(velocity, np.float64).ravel()
+        p = None if pressure is None else np.ascontiguousarray(pressure, np.float64)
+        check(lib().tfiga_ns_set_dirichlet_values(self._h, _p(v), _p(p)))
+
+    def set_tractions(self, tractions: dict):
+        labels = np.array(list(tractions.keys()), np.int32)
+        pressures = np.array(list(tractions.values()), np.float64)
+        check(lib().tfiga_ns_set_tractions(self._h, _p(labels), _p(pressures), len(labels)))
+
+    def set_state(self, state, previous=None):
+        s = np.ascontiguousarray(state, np.float64).ravel()
+        p = None if previous is None else np.ascontiguousarray(previous, np.float64).ravel()
+        check(lib().tfiga_ns_set_state(self._h, _p(s), _p(p)))
+
+    def get_state(self, out=None):
+        out = np.zeros(4 * self.nodes) if out is None else out
+        check(lib().tfiga_ns_get_state(self._h, _p(out)))
+        return out
+
+    def commit_step(self):
+        check(lib().tfiga_ns_commit_step(self._h))
+
+    def assemble(self, values=True, rhs=True):
+        v = np.zeros(self.mesh.blocks * 16) if values else None
+        r = np.zeros(4 * self.nodes) if rhs else None
+        check(lib().tfiga_ns_assemble(self._h, _p(v), _p(r)))
+        return v, r
+
+    def apply_dirichlet(self, values=True, rhs=True):
+        v = np.zeros(self.mesh.blocks * 16) if values else None
+        r = np.zeros(4 * self.nodes) if rhs else None
+        check(lib().tfiga_ns_apply_dirichlet(self._h, _p(v), _p(r)))
+        return v, r
+
+    def solve_linear(self, rtol=1e-8, max_iterations=5000):
+        u = np.zeros(4 * self.nodes)
+        it = C.c_int32(); res = C.c_double()
+        check(lib().tfiga_ns_solve_linear(self._h, rtol, max_iterations, _p(u), C.byref(it), C.byref(res)))
+        return u, it.value, res.value
+
+    def newton_iteration(self, initial_residual=-1.0) -> dict:
+        r = NewtonReport()
+        check(lib().tfiga_ns_newton_iteration(self._h, initial_residual, C.byref(r)))
+        return r.as_dict()
+
+    def step(self) -> dict:
+        r = StepReport()
+        check(lib().tfiga_ns_step(self._h, C.byref(r)))
+        return r.as_dict()
+
+    def boundary_flows(self, labels):
+        lab = np.ascontiguousarray(labels, np.int32)
+        out = np.zeros(len(lab))
+        check(lib().tfiga_ns_boundary_flows(self._h, _p(lab), len(lab), _p(out)))
+        return out
+
+    def device_buffers(self):
+        v, s, r = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(lib().tfiga_ns_device_buffers(self._h, C.byref(v), C.byref(s), C.byref(r)))
+        return v.value, s.value, r.value
+
+    def spmv_device(self, x_ptr: int, y_ptr: int):
+        check(lib().tfiga_ns_spmv_device(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr)))
+
+    def launches(self) -> int:
+        return int(lib().tfiga_ns_launch_count(self._h))
+
+    def synchronize(self):
+        check(lib().tfiga_ns_synchronize(self._h))
+
+    def close(self):
+        if self._h:
+            lib().tfiga_ns_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tube_boundary_conditions(tube, inlet_scale: float):
+    """Dirichlet masks/values of a generated tube: wall (label 0) no-slip, inlet (label 1) scaled profile.
+
+    Mirrors ResolveFlowBoundaries (solvers/cpu/include/GenericCaseInput.hpp:174-259) for the generator's
+    simulation_config, plus the wall-trace basis, which for the generator tubes is exactly the label-0
+    vertex set."""
+    labels = tube.labels
+    vmask = ((labels == 0) | (labels == 1)).astype(np.int32)
+    vel = np.zeros((len(labels), 3))
+    inlet = labels == 1
+    vel[inlet] = inlet_scale * tube.profile[inlet]
+    return vmask, np.zeros(len(labels), np.int32), vel
+
+
+def initial_state(vmask, velocity, pmask=None, pressure=None):
+    """Initial state of a transient run (iga_cuda.cu:879-889): constrained values, zero elsewhere."""
+    n = len(vmask)
+    s = np.zeros((n, 4))
+    s[vmask != 0, :3] = np.asarray(velocity).reshape(n, 3)[vmask != 0]
+    if pmask is not None and pressure is not None:
+        s[pmask != 0, 3] = np.asarray(pressure)[pmask != 0]
+    return s.ravel()

@@ -1,0 +1,337 @@
+// extern "C" boundary: every entry point converts exceptions into a status
+// code plus a thread-local message (tfiga_last_error).
+#include "mesh.hpp"
+#include "ns.hpp"
+
+#include "../../include/tfiga.h"
+
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
+#include <string>
+
+struct tfiga_mesh {
+	std::unique_ptr<tfiga::Mesh> mesh;
+};
+
+struct tfiga_ns {
+	tfiga_mesh* mesh = nullptr;
+	std::unique_ptr<tfiga::NsSolver> solver;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+template <class F>
+int Guard(F&& body)
+{
+	try {
+		body();
+		return TFIGA_OK;
+	} catch (const tfiga::Error& error) {
+		g_error = error.what();
+		return error.status;
+	} catch (const std::bad_alloc&) {
+		g_error = "host allocation failed";
+		return TFIGA_E_MEMORY;
+	} catch (const std::exception& error) {
+		g_error = error.what();
+		return TFIGA_E_INVALID;
+	} catch (...) {
+		g_error = "unknown error";
+		return TFIGA_E_INVALID;
+	}
+}
+
+void Require(bool condition, const char* message)
+{
+	if (!condition) tfiga::Fail(TFIGA_E_INVALID, message);
+}
+
+tfiga::HostMesh FromDesc(const tfiga_mesh_desc* d)
+{
+	Require(d && d->nodes > 0 && d->elements > 0, "mesh descriptor needs nodes and elements");
+	Require(d->element_offsets && d->connectivity && d->extraction_offsets && d->extraction_columns
+		&& d->extraction_values && d->bezier_points, "mesh descriptor has a null array");
+	tfiga::HostMesh m;
+	m.nodes = d->nodes;
+	const int64_t E = d->elements;
+	m.element_offsets.assign(d->element_offsets, d->element_offsets+E+1);
+	Require(m.element_offsets[0] == 0, "element_offsets must start at 0");
+	const int64_t entries = m.element_offsets[E];
+	m.connectivity.assign(d->connectivity, d->connectivity+entries);
+	m.extraction_offsets.assign(d->extraction_offsets, d->extraction_offsets+entries+1);
+	const int64_t nnz = m.extraction_offsets[entries];
+	m.extraction_columns.assign(d->extraction_columns, d->extraction_columns+nnz);
+	m.extraction_values.assign(d->extraction_values, d->extraction_values+nnz);
+	m.bezier_points.assign(d->bezier_points, d->bezier_points+E*192);
+	if (d->boundary_labels) m.boundary_labels.assign(d->boundary_labels, d->boundary_labels+E*6);
+	else m.boundary_labels.assign(E*6, -1);
+	for (int64_t e = 0; e < E; ++e)
+		m.max_basis = std::max<int32_t>(m.max_basis, m.element_offsets[e+1]-m.element_offsets[e]);
+	return m;
+}
+
+} // namespace
+
+extern "C" {
+
+size_t tfiga_last_error(char* buffer, size_t capacity)
+{
+	if (buffer && capacity) {
+		const size_t n = std::min(capacity-1, g_error.size());
+		std::memcpy(buffer, g_error.data(), n);
+		buffer[n] = '\0';
+	}
+	return g_error.size();
+}
+
+const char* tfiga_version(void)
+{
+	return "tubularflowiga-b200 0.1 sm_100a fp64";
+}
+
+int tfiga_mesh_create(const tfiga_mesh_desc* desc, tfiga_mesh** out)
+{
+	return Guard([&] {
+		Require(out != nullptr, "out is null");
+		*out = nullptr;
+		auto handle = std::make_unique<tfiga_mesh>();
+		handle->mesh = std::make_unique<tfiga::Mesh>(FromDesc(desc));
+		*out = handle.release();
+	});
+}
+
+int tfiga_mesh_load_ntiga(const char* path, tfiga_mesh** out)
+{
+	return Guard([&] {
+		Require(path && out, "null argument");
+		*out = nullptr;
+		auto handle = std::make_unique<tfiga_mesh>();
+		handle->mesh = std::make_unique<tfiga::Mesh>(tfiga::ReadNtiga(path));
+		*out = handle.release();
+	});
+}
+
+int tfiga_mesh_destroy(tfiga_mesh* mesh)
+{
+	return Guard([&] { delete mesh; });
+}
+
+int tfiga_mesh_info_get(const tfiga_mesh* mesh, tfiga_mesh_info* info)
+{
+	return Guard([&] {
+		Require(mesh && info, "null argument");
+		const auto& m = *mesh->mesh;
+		info->nodes = m.host().nodes;
+		info->elements = m.host().elements();
+		info->max_basis = m.host().max_basis;
+		info->basis_entries = (int64_t)m.host().connectivity.size();
+		info->extraction_nonzeros = (int64_t)m.host().extraction_values.size();
+		info->block_nonzeros = (int64_t)m.pattern().columns.size();
+		info->max_block_row = m.pattern().max_row;
+		info->min_detj = m.min_detj();
+		info->bad_samples = m.bad_samples();
+		info->device_bytes = m.device_bytes();
+	});
+}
+
+int tfiga_mesh_pattern(const tfiga_mesh* mesh, int32_t* row_offsets, int32_t* columns, int32_t* diagonal)
+{
+	return Guard([&] {
+		Require(mesh != nullptr, "null mesh");
+		const auto& p = mesh->mesh->pattern();
+		if (row_offsets) std::memcpy(row_offsets, p.row_offsets.data(), p.row_offsets.size()*sizeof(int32_t));
+		if (columns) std::memcpy(columns, p.columns.data(), p.columns.size()*sizeof(int32_t));
+		if (diagonal) std::memcpy(diagonal, p.diagonal.data(), p.diagonal.size()*sizeof(int32_t));
+	});
+}
+
+void tfiga_ns_default_params(tfiga_ns_params* p)
+{
+	if (!p) return;
+	p->density = 1.0;
+	p->viscosity = 0.1;
+	p->dt = 0.0;
+	p->max_newton = 12;
+	p->nonlinear_rtol = 1e-5;
+	p->nonlinear_atol = 1e-10;
+	p->mass_rtol = 1e-3;
+	p->gmres_restart = 200;
+	p->gmres_max_iterations = 5000;
+	p->gmres_rtol = 1e-8;
+}
+
+int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out)
+{
+	return Guard([&] {
+		Require(mesh && params && out, "null argument");
+		*out = nullptr;
+		auto handle = std::make_unique<tfiga_ns>();
+		handle->mesh = mesh;
+		handle->solver = std::make_unique<tfiga::NsSolver>(*mesh->mesh, *params);
+		*out = handle.release();
+	});
+}
+
+int tfiga_ns_destroy(tfiga_ns* ns)
+{
+	return Guard([&] { delete ns; });
+}
+
+int tfiga_ns_set_dirichlet(tfiga_ns* ns, const int32_t* vmask, const int32_t* pmask, const double* velocity,
+	const double* pressure)
+{
+	return Guard([&] {
+		Require(ns && vmask && velocity, "null argument");
+		std::vector<double> zeros;
+		if (!pressure) { zeros.assign(ns->solver->nodes(), 0.0); pressure = zeros.data(); }
+		ns->solver->SetDirichlet(vmask, pmask, velocity, pressure);
+	});
+}
+
+int tfiga_ns_set_dirichlet_values(tfiga_ns* ns, const double* velocity, const double* pressure)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		ns->solver->SetDirichletValues(velocity, pressure);
+	});
+}
+
+int tfiga_ns_set_tractions(tfiga_ns* ns, const int32_t* labels, const double* pressures, int32_t count)
+{
+	return Guard([&] {
+		Require(ns && (count == 0 || (labels && pressures)), "null argument");
+		ns->solver->SetTractions(labels, pressures, count);
+	});
+}
+
+int tfiga_ns_set_state(tfiga_ns* ns, const double* state, const double* previous)
+{
+	return Guard([&] {
+		Require(ns && state, "null argument");
+		ns->solver->SetState(state, previous);
+	});
+}
+
+int tfiga_ns_get_state(tfiga_ns* ns, double* state)
+{
+	return Guard([&] {
+		Require(ns && state, "null argument");
+		ns->solver->GetState(state);
+	});
+}
+
+int tfiga_ns_commit_step(tfiga_ns* ns)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		ns->solver->CommitStep();
+	});
+}
+
+int tfiga_ns_assemble(tfiga_ns* ns, double* values, double* rhs)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		auto& s = *ns->solver;
+		s.Assemble();
+		if (values) tfiga::CudaCheck(cudaMemcpyAsync(values, s.values(), (size_t)s.blocks()*16*sizeof(double),
+			cudaMemcpyDeviceToHost, s.stream()), "download values");
+		if (rhs) tfiga::CudaCheck(cudaMemcpyAsync(rhs, s.rhs(), (size_t)s.nodes()*4*sizeof(double),
+			cudaMemcpyDeviceToHost, s.stream()), "download rhs");
+		s.Synchronize();
+	});
+}
+
+int tfiga_ns_apply_dirichlet(tfiga_ns* ns, double* values, double* rhs)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		auto& s = *ns->solver;
+		s.ApplyDirichlet();
+		if (values) tfiga::CudaCheck(cudaMemcpyAsync(values, s.values(), (size_t)s.blocks()*16*sizeof(double),
+			cudaMemcpyDeviceToHost, s.stream()), "download values");
+		if (rhs) tfiga::CudaCheck(cudaMemcpyAsync(rhs, s.rhs(), (size_t)s.nodes()*4*sizeof(double),
+			cudaMemcpyDeviceToHost, s.stream()), "download rhs");
+		s.Synchronize();
+	});
+}
+
+int tfiga_ns_solve_linear(tfiga_ns* ns, double rtol, int32_t max_iterations, double* update, int32_t* iterations,
+	double* residual)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		auto& s = *ns->solver;
+		const auto result = s.SolveLinear(rtol, max_iterations);
+		if (iterations) *iterations = result.iterations;
+		if (residual) *residual = result.residual;
+		if (update) {
+			tfiga::CudaCheck(cudaMemcpyAsync(update, s.update(), (size_t)s.nodes()*4*sizeof(double),
+				cudaMemcpyDeviceToHost, s.stream()), "download update");
+			s.Synchronize();
+		}
+		if (!result.converged) tfiga::Fail(TFIGA_E_NOT_CONVERGED, "GMRES did not reach the requested tolerance");
+	});
+}
+
+int tfiga_ns_newton_iteration(tfiga_ns* ns, double initial_residual, tfiga_newton_report* report)
+{
+	return Guard([&] {
+		Require(ns && report, "null argument");
+		*report = ns->solver->NewtonIteration(initial_residual);
+	});
+}
+
+int tfiga_ns_step(tfiga_ns* ns, tfiga_step_report* report)
+{
+	return Guard([&] {
+		Require(ns && report, "null argument");
+		*report = ns->solver->Step();
+	});
+}
+
+int tfiga_ns_boundary_flows(tfiga_ns* ns, const int32_t* labels, int32_t count, double* flows)
+{
+	return Guard([&] {
+		Require(ns && (count == 0 || (labels && flows)), "null argument");
+		ns->solver->BoundaryFlows(labels, count, flows);
+	});
+}
+
+int tfiga_ns_spmv_device(tfiga_ns* ns, const double* x, double* y)
+{
+	return Guard([&] {
+		Require(ns && x && y, "null argument");
+		tfiga::LaunchSpmv(ns->solver->pattern(), ns->solver->values(), x, y, ns->solver->stream());
+		ns->solver->AddLaunches(1);
+	});
+}
+
+int tfiga_ns_device_buffers(tfiga_ns* ns, double** values, double** state, double** rhs)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		if (values) *values = ns->solver->values();
+		if (state) *state = ns->solver->state();
+		if (rhs) *rhs = ns->solver->rhs();
+	});
+}
+
+int64_t tfiga_ns_launch_count(const tfiga_ns* ns)
+{
+	return ns ? ns->solver->launches() : -1;
+}
+
+int tfiga_ns_synchronize(tfiga_ns* ns)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		ns->solver->Synchronize();
+	});
+}
+
+} // extern "C"

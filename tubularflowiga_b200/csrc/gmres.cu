@@ -1,0 +1,319 @@
+// Device kernels and host driver of the block-Jacobi GMRES (see gmres.hpp).
+#include "gmres.hpp"
+
+#include <algorithm>
+#include <cmath>
+
+namespace tfiga {
+namespace {
+
+constexpr int kBlocks = 296;          // 2 CTAs per SM for the streaming passes
+constexpr int kThreads = 256;
+constexpr int kBatch = 8;             // Arnoldi steps launched per host wait
+
+// partial[i*blocks + cta] = scale[i] * <V_i, w> over this CTA's chunk.
+__global__ void __launch_bounds__(kThreads) MultiDotKernel(const double* __restrict__ V, long long n,
+	const double* __restrict__ scale, int count, const double* __restrict__ w, double* __restrict__ partial,
+	int chunk, const int* __restrict__ stop)
+{
+	if (*stop) return;
+	extern __shared__ double wchunk[];
+	const long long lo = (long long)blockIdx.x*chunk;
+	const long long rest = n-lo;
+	const int len = rest <= 0 ? 0 : (rest < chunk ? (int)rest : chunk);
+	for (int k = threadIdx.x; k < len; k += blockDim.x) wchunk[k] = w[lo+k];
+	__syncthreads();
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	for (int i = warp; i < count; i += kThreads/32) {
+		const double* vi = V+(size_t)i*n+lo;
+		double s0 = 0.0, s1 = 0.0;
+		int k = lane;
+		for (; k+32 < len; k += 64) { s0 = fma(vi[k], wchunk[k], s0); s1 = fma(vi[k+32], wchunk[k+32], s1); }
+		if (k < len) s0 = fma(vi[k], wchunk[k], s0);
+		double s = s0+s1;
+		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+		if (lane == 0) partial[(size_t)i*gridDim.x+blockIdx.x] = s*scale[i];
+	}
+}
+
+// hpass[i] = sum over CTAs; H[i][j] = (pass == 0 ? hpass : H + hpass).
+__global__ void __launch_bounds__(kThreads) DotFinalizeKernel(const double* __restrict__ partial, int blocks,
+	int count, double* __restrict__ hpass, double* __restrict__ H, int restart, int j, int pass,
+	const int* __restrict__ stop)
+{
+	if (*stop) return;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	for (int i = warp; i < count; i += kThreads/32) {
+		double s = 0.0;
+		for (int b = lane; b < blocks; b += 32) s += partial[(size_t)i*blocks+b];
+		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+		if (lane == 0) {
+			hpass[i] = s;
+			double& h = H[(size_t)i*restart+j];
+			h = pass == 0 ? s : h+s;
+		}
+	}
+}
+
+// out = w - sum_i scale_i hpass_i V_i; norm_partial[cta] = sum out^2 (if non-null).
+__global__ void __launch_bounds__(kThreads) UpdateKernel(const double* __restrict__ V, long long n,
+	const double* __restrict__ scale, int count, const double* __restrict__ hpass, const double* win, double* out,
+	double* __restrict__ norm_partial, const int* __restrict__ stop)
+{
+	if (*stop) return;
+	extern __shared__ double coef[];
+	for (int i = threadIdx.x; i < count; i += blockDim.x) coef[i] = scale[i]*hpass[i];
+	__syncthreads();
+	double sq = 0.0;
+	for (long long k = (long long)blockIdx.x*blockDim.x+threadIdx.x; k < n; k += (long long)gridDim.x*blockDim.x) {
+		double v = win[k];
+		int i = 0;
+		for (; i+1 < count; i += 2) {
+			v = fma(-coef[i], V[(size_t)i*n+k], v);
+			v = fma(-coef[i+1], V[(size_t)(i+1)*n+k], v);
+		}
+		if (i < count) v = fma(-coef[i], V[(size_t)i*n+k], v);
+		out[k] = v;
+		sq = fma(v, v, sq);
+	}
+	if (norm_partial == nullptr) return;
+	__shared__ double red[kThreads/32];
+	for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double s = 0.0;
+		for (int w = 0; w < kThreads/32; ++w) s += red[w];
+		norm_partial[blockIdx.x] = s;
+	}
+}
+
+// Column j of the Hessenberg matrix: norm, previous rotations, new rotation,
+// residual estimate (Gmres.hpp:272-305).  One warp; lane 0 is sequential.
+__global__ void ArnoldiFinalizeKernel(const double* __restrict__ norm_partial, int blocks, double* __restrict__ H,
+	int restart, int j, double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
+	double* __restrict__ scale, int* __restrict__ state, double* __restrict__ residual, double tolerance)
+{
+	if (state[0]) return;
+	double s = 0.0;
+	for (int b = threadIdx.x; b < blocks; b += 32) s += norm_partial[b];
+	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+	if (threadIdx.x != 0) return;
+	const double next = sqrt(s);
+	H[(size_t)(j+1)*restart+j] = next;
+	scale[j+1] = next > 1e-30 ? 1.0/next : 0.0;
+	for (int i = 0; i < j; ++i) {
+		const double a = H[(size_t)i*restart+j], b = H[(size_t)(i+1)*restart+j];
+		H[(size_t)i*restart+j] = cs[i]*a+sn[i]*b;
+		H[(size_t)(i+1)*restart+j] = -sn[i]*a+cs[i]*b;
+	}
+	const double a = H[(size_t)j*restart+j], b = H[(size_t)(j+1)*restart+j];
+	const double mag = hypot(a, b);
+	cs[j] = mag > 0.0 ? a/mag : 1.0;
+	sn[j] = mag > 0.0 ? b/mag : 0.0;
+	H[(size_t)j*restart+j] = mag;
+	H[(size_t)(j+1)*restart+j] = 0.0;
+	const double old = g[j];
+	g[j] = cs[j]*old;
+	g[j+1] = -sn[j]*old;
+	const double res = fabs(g[j+1]);
+	residual[0] = res;
+	state[1] = j+1;
+	if (res <= tolerance || next <= 1e-30) state[0] = 1;
+}
+
+// Cycle start: g = beta e_0, scale_0 = 1/beta, flags cleared.
+__global__ void CycleInitKernel(const double* __restrict__ beta, double* __restrict__ g, int restart,
+	double* __restrict__ scale, int* __restrict__ state)
+{
+	for (int i = threadIdx.x; i <= restart; i += blockDim.x) g[i] = 0.0;
+	if (threadIdx.x == 0) {
+		g[0] = beta[0];
+		scale[0] = beta[0] > 0.0 ? 1.0/beta[0] : 0.0;
+		state[0] = 0; state[1] = 0; state[2] = 0;
+	}
+}
+
+// Back substitution of the least-squares system (Gmres.hpp:308-315).
+__global__ void BackSolveKernel(const double* __restrict__ H, const double* __restrict__ g, int restart,
+	const int* __restrict__ state, double* __restrict__ y, int* __restrict__ error_flag)
+{
+	const int used = state[1];
+	for (int row = used-1; row >= 0; --row) {
+		double v = g[row];
+		for (int c = row+1; c < used; ++c) v -= H[(size_t)row*restart+c]*y[c];
+		const double d = H[(size_t)row*restart+row];
+		if (fabs(d) < 1e-30) { *error_flag = 1; y[row] = 0.0; continue; }
+		y[row] = v/d;
+	}
+}
+
+// x += sum_i y_i scale_i V_i over the columns of this cycle.
+__global__ void __launch_bounds__(kThreads) SolutionUpdateKernel(const double* __restrict__ V, long long n,
+	const double* __restrict__ scale, const double* __restrict__ y, const int* __restrict__ state,
+	double* __restrict__ x)
+{
+	extern __shared__ double coef[];
+	const int used = state[1];
+	for (int i = threadIdx.x; i < used; i += blockDim.x) coef[i] = y[i]*scale[i];
+	__syncthreads();
+	for (long long k = (long long)blockIdx.x*blockDim.x+threadIdx.x; k < n; k += (long long)gridDim.x*blockDim.x) {
+		double v = x[k];
+		for (int i = 0; i < used; ++i) v = fma(coef[i], V[(size_t)i*n+k], v);
+		x[k] = v;
+	}
+}
+
+__global__ void ResidualKernel(long long n, const double* __restrict__ rhs, const double* __restrict__ ax,
+	double* __restrict__ r)
+{
+	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (i < n) r[i] = rhs[i]-ax[i];
+}
+
+} // namespace
+
+Gmres::Gmres(int nodes, int restart, cudaStream_t stream)
+	: nodes_(nodes), n_(4*nodes), restart_(restart), blocks_(kBlocks), stream_(stream)
+{
+	if (nodes <= 0 || restart <= 0) Fail(-1, "GMRES workspace dimensions must be positive");
+	chunk_ = (int)std::max<long long>(256, ((long long)n_+blocks_-1)/blocks_);
+	V_.Allocate((size_t)(restart+1)*n_);
+	w_.Allocate(n_); r_.Allocate(n_); tmp_.Allocate(n_);
+	inverse_.Allocate((size_t)nodes*16);
+	partial_.Allocate((size_t)(restart+1)*blocks_);
+	hpass_.Allocate(restart+1);
+	H_.Allocate((size_t)(restart+1)*restart);
+	cs_.Allocate(restart); sn_.Allocate(restart); g_.Allocate(restart+1); y_.Allocate(restart);
+	scale_.Allocate(restart+1);
+	norm_partial_.Allocate(PartialSlots());
+	scalar_.Allocate(2);
+	state_.Allocate(4);
+	residual_.Allocate(1);
+	singular_.Allocate(1);
+	CudaCheck(cudaMallocHost(reinterpret_cast<void**>(&host_), sizeof(HostStatus)), "pinned GMRES status");
+	if ((size_t)chunk_*sizeof(double) > 48*1024) {
+		CudaCheck(cudaFuncSetAttribute(MultiDotKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)((size_t)chunk_*sizeof(double))), "multi-dot shared memory");
+	}
+	if ((size_t)(restart+1)*sizeof(double) > 48*1024) {
+		CudaCheck(cudaFuncSetAttribute(UpdateKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)((size_t)(restart+1)*sizeof(double))), "update shared memory");
+		CudaCheck(cudaFuncSetAttribute(SolutionUpdateKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)((size_t)(restart+1)*sizeof(double))), "solution update shared memory");
+	}
+	if ((size_t)chunk_*sizeof(double) > 227*1024) Fail(-7, "GMRES vector too long for the multi-dot chunking");
+}
+
+Gmres::~Gmres()
+{
+	if (host_) cudaFreeHost(host_);
+}
+
+std::size_t Gmres::bytes() const
+{
+	return V_.bytes()+w_.bytes()+r_.bytes()+tmp_.bytes()+inverse_.bytes()+partial_.bytes()+H_.bytes();
+}
+
+void Gmres::Step(const DevicePatternView& pattern, const double* values, int j)
+{
+	const int count = j+1;
+	const int* stop = state_.get();
+	const size_t dot_smem = (size_t)chunk_*sizeof(double);
+	const size_t coef_smem = (size_t)(restart_+1)*sizeof(double);
+	LaunchSpmvBlockJacobi(pattern, values, inverse_.get(), V_.get()+(size_t)j*n_, scale_.get()+j, w_.get(), stop,
+		stream_);
+	for (int pass = 0; pass < 2; ++pass) {
+		MultiDotKernel<<<blocks_, kThreads, dot_smem, stream_>>>(V_.get(), n_, scale_.get(), count, w_.get(),
+			partial_.get(), chunk_, stop);
+		LaunchCheck("MultiDotKernel");
+		DotFinalizeKernel<<<1, kThreads, 0, stream_>>>(partial_.get(), blocks_, count, hpass_.get(), H_.get(),
+			restart_, j, pass, stop);
+		LaunchCheck("DotFinalizeKernel");
+		double* out = pass == 0 ? w_.get() : V_.get()+(size_t)(j+1)*n_;
+		UpdateKernel<<<blocks_, kThreads, coef_smem, stream_>>>(V_.get(), n_, scale_.get(), count, hpass_.get(),
+			w_.get(), out, pass == 0 ? nullptr : norm_partial_.get(), stop);
+		LaunchCheck("UpdateKernel");
+	}
+	launches_ += 8;
+}
+
+double Gmres::TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs,
+	const double* x)
+{
+	LaunchSpmv(pattern, values, x, tmp_.get(), stream_);
+	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), r_.get());
+	LaunchCheck("ResidualKernel");
+	LaunchApplyBlockInverse(nodes_, inverse_.get(), r_.get(), V_.get(), stream_);
+	LaunchNorm(n_, V_.get(), norm_partial_.get(), scalar_.get(), stream_);
+	launches_ += 5;
+	scalar_.Download(host_->beta, 1, stream_);
+	CudaCheck(cudaStreamSynchronize(stream_), "GMRES residual");
+	return host_->beta[0];
+}
+
+GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values, const double* rhs, double* x,
+	double rtol, int max_iterations, long long* launches)
+{
+	launches_ = 0;
+	GmresResult result;
+	singular_.Zero(stream_);
+	LaunchBlockInverse(pattern, values, inverse_.get(), singular_.get(), stream_);
+	launches_ += 1;
+	singular_.Download(&host_->singular, 1, stream_);
+	double beta = TrueResidual(pattern, values, rhs, x);
+	result.singular_blocks = host_->singular;
+	result.residual = beta;
+	if (!std::isfinite(beta)) Fail(-6, "GMRES initial residual is not finite");
+	if (beta == 0.0) {
+		result.converged = true;
+		if (launches) *launches += launches_;
+		return result;
+	}
+	const double tolerance = std::max(1e-30, rtol*beta);
+	const size_t coef_smem = (size_t)(restart_+1)*sizeof(double);
+	while (result.iterations < max_iterations) {
+		CycleInitKernel<<<1, 256, 0, stream_>>>(scalar_.get(), g_.get(), restart_, scale_.get(), state_.get());
+		LaunchCheck("CycleInitKernel");
+		H_.Zero(stream_);
+		launches_ += 1;
+		const int cap = std::min(restart_, max_iterations-result.iterations);
+		for (int j = 0; j < cap;) {
+			const int batch = std::min(kBatch, cap-j);
+			for (int b = 0; b < batch; ++b) {
+				Step(pattern, values, j+b);
+				ArnoldiFinalizeKernel<<<1, 32, 0, stream_>>>(norm_partial_.get(), blocks_, H_.get(), restart_, j+b,
+					cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance);
+				LaunchCheck("ArnoldiFinalizeKernel");
+				launches_ += 1;
+			}
+			j += batch;
+			state_.Download(&host_->stop, 3, stream_);
+			residual_.Download(&host_->residual, 1, stream_);
+			CudaCheck(cudaStreamSynchronize(stream_), "GMRES batch");
+			if (host_->stop) break;
+		}
+		const int used = host_->used;
+		result.iterations += used;
+		result.residual = host_->residual;
+		BackSolveKernel<<<1, 1, 0, stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(),
+			state_.get()+2);
+		LaunchCheck("BackSolveKernel");
+		SolutionUpdateKernel<<<blocks_, kThreads, coef_smem, stream_>>>(V_.get(), n_, scale_.get(), y_.get(),
+			state_.get(), x);
+		LaunchCheck("SolutionUpdateKernel");
+		launches_ += 2;
+		beta = TrueResidual(pattern, values, rhs, x);
+		state_.Download(&host_->stop, 3, stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "GMRES restart");
+		if (host_->error) Fail(-6, "GMRES Hessenberg matrix is singular");
+		result.residual = beta;
+		if (!std::isfinite(beta)) Fail(-6, "GMRES residual is not finite");
+		if (beta <= tolerance) { result.converged = true; break; }
+		if (used == 0) break;
+	}
+	if (launches) *launches += launches_;
+	return result;
+}
+
+} // namespace tfiga

@@ -1,0 +1,55 @@
+// Restarted left-preconditioned GMRES(m) with block-Jacobi preconditioning,
+// the solver of the reference's Newton loop (SolveGmres,
+// solvers/cuda/include/Gmres.hpp:192-336): same preconditioner, restart,
+// tolerance definition (rtol * ||D^{-1} r0||) and true-residual restart check.
+//
+// B200 organisation: the Hessenberg matrix, Givens rotations and residual
+// estimate live on the device; orthogonalisation is classical Gram-Schmidt
+// applied twice (two multi-dot + multi-axpy passes over the basis instead of
+// one dot/axpy pair per basis vector); Krylov vectors are normalised lazily
+// through a per-vector scale; kernels of an iteration batch return early once
+// the device has flagged convergence, so the host waits only once per batch.
+#pragma once
+
+#include "common.hpp"
+#include "kernels.cuh"
+
+namespace tfiga {
+
+struct GmresResult {
+	int iterations = 0;
+	double residual = 0.0;
+	unsigned singular_blocks = 0;
+	bool converged = false;
+};
+
+class Gmres {
+public:
+	Gmres(int nodes, int restart, cudaStream_t stream);
+	~Gmres();
+	Gmres(const Gmres&) = delete;
+	Gmres& operator=(const Gmres&) = delete;
+	// Solves A x = rhs (x holds the initial guess).  Builds the block inverse first.
+	GmresResult Solve(const DevicePatternView& pattern, const double* values, const double* rhs, double* x,
+		double rtol, int max_iterations, long long* launches);
+	int restart() const { return restart_; }
+	std::size_t bytes() const;
+
+private:
+	void Step(const DevicePatternView& pattern, const double* values, int j);
+	double TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs, const double* x);
+
+	int nodes_, n_, restart_, blocks_;
+	int chunk_;
+	cudaStream_t stream_;
+	long long launches_ = 0;
+	DeviceArray<double> V_, w_, r_, tmp_, inverse_, partial_, hpass_, H_, cs_, sn_, g_, y_, scale_, norm_partial_,
+		scalar_;
+	DeviceArray<int> state_;          // [0] stop, [1] used, [2] error
+	DeviceArray<double> residual_;    // [0] residual estimate
+	DeviceArray<unsigned> singular_;
+	struct HostStatus { int stop, used, error, pad; double residual; double beta[2]; unsigned singular; };
+	HostStatus* host_ = nullptr;
+};
+
+} // namespace tfiga

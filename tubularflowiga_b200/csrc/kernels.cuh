@@ -1,0 +1,90 @@
+// Device data layout and kernel entry points of the B200 Navier-Stokes path.
+//
+// Per-element basis tables (built once per mesh, FP64):
+//   phi[((e*5 + t)*64 + q)*NP + a]   t = 0: N, 1..3: dN/dx_t, 4: Laplacian of N
+//   qdata[(e*64 + q)*QD + k]          k = 0 measure (w_q/8 * det), 1..6 metric G =
+//                                     J^-T J^-1 (00,01,02,11,12,22), 7 |sum_j J^-1_j.|^2,
+//                                     8 |G|_F^2, 9 det/8
+// Block-CSR matrix: values[block*16 + 4*i + f] (row field i, column field f),
+// node-major vectors value[4*node + field].
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tfiga {
+
+constexpr int kQuad = 64;       // 4x4x4 Gauss points
+constexpr int kFeatures = 5;    // N, dN/dx, dN/dy, dN/dz, Laplacian
+constexpr int kQData = 10;
+constexpr int kMaxBasis = 64;   // padded basis count NP of the device tables
+
+struct DeviceMeshView {
+	int nodes = 0;
+	int elements = 0;
+	const int32_t* element_offsets = nullptr;
+	const int32_t* connectivity = nullptr;
+	const int32_t* extraction_offsets = nullptr;
+	const uint8_t* extraction_columns = nullptr;
+	const double* extraction_values = nullptr;
+	const double* bezier_points = nullptr;
+};
+
+struct DevicePatternView {
+	int nodes = 0;
+	long long blocks = 0;
+	const int32_t* row_offsets = nullptr;
+	const int32_t* columns = nullptr;
+	const int32_t* diagonal = nullptr;
+};
+
+struct AssemblyParams {
+	double density;
+	double viscosity;
+	double dt;
+};
+
+// ---- basis.cu -----------------------------------------------------------
+void LaunchBuildBasis(const DeviceMeshView& mesh, double* phi, double* qdata, cudaStream_t stream);
+void LaunchElementBlocks(const DeviceMeshView& mesh, const DevicePatternView& pattern, int32_t* element_blocks,
+	cudaStream_t stream);
+void LaunchFaceCoefficients(const DeviceMeshView& mesh, int faces, const int32_t* face_element,
+	const int32_t* face_index, double* face_coef, cudaStream_t stream);
+
+// ---- assemble.cu --------------------------------------------------------
+// Exact-tangent VMS assembly: jacobian values (may be null: residual only) and
+// rhs (= -r) are ADDED to.
+void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double* qdata,
+	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
+	double* values, double* rhs, cudaStream_t stream);
+
+// ---- sparse.cu ----------------------------------------------------------
+void LaunchSpmv(const DevicePatternView& pattern, const double* values, const double* x, double* y,
+	cudaStream_t stream);
+// y = D^{-1} (A (scale * x)) with D^{-1} stored per node as 4x4 (scale read from device, may be null).
+void LaunchSpmvBlockJacobi(const DevicePatternView& pattern, const double* values, const double* inverse,
+	const double* x, const double* scale, double* y, const int* stop, cudaStream_t stream);
+void LaunchBlockInverse(const DevicePatternView& pattern, const double* values, double* inverse,
+	unsigned int* singular, cudaStream_t stream);
+void LaunchApplyBlockInverse(int nodes, const double* inverse, const double* x, double* y, cudaStream_t stream);
+void LaunchDirichletRows(const DevicePatternView& pattern, int count, const int32_t* constrained_nodes,
+	const int32_t* velocity_mask, const int32_t* pressure_mask, const double* velocity, const double* pressure,
+	const double* state, double* values, double* rhs, cudaStream_t stream);
+void LaunchFaceFlows(int faces, const int32_t* face_element, const double* face_coef,
+	const int32_t* element_offsets, const int32_t* connectivity, const double* state, double* face_flow,
+	cudaStream_t stream);
+void LaunchFaceTraction(int faces, const int32_t* face_element, const double* face_coef,
+	const int32_t* element_offsets, const int32_t* connectivity, const double* face_pressure,
+	double* traction, cudaStream_t stream);
+// Deterministic sums: out[0] = sum x[i*stride+offset]^2, out[1] = sum x[i*stride+offset] over count items.
+void LaunchStridedSums(long long count, int stride, int offset, const double* x, double* partial, double* out,
+	cudaStream_t stream);
+// out = sqrt(sum x^2) (deterministic two-stage).
+void LaunchNorm(long long n, const double* x, double* partial, double* out, cudaStream_t stream);
+void LaunchAxpy(long long n, double alpha, const double* x, double* y, cudaStream_t stream);
+void LaunchSegmentSums(int segments, const int32_t* segment_of, int items, const double* values, double* out,
+	cudaStream_t stream);
+
+int PartialSlots();
+
+} // namespace tfiga

@@ -1,0 +1,88 @@
+// Host mesh (FlatMesh layout), .ntiga reader, block pattern, and the
+// device-resident mesh with its per-element basis tables.
+#pragma once
+
+#include "common.hpp"
+#include "kernels.cuh"
+
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace tfiga {
+
+// Flattened mesh: solvers/cuda/include/DeviceMesh.hpp:16-57.
+struct HostMesh {
+	int64_t nodes = 0;
+	std::vector<int32_t> element_offsets{0};
+	std::vector<int32_t> connectivity;
+	std::vector<int32_t> extraction_offsets{0};
+	std::vector<uint8_t> extraction_columns;
+	std::vector<double> extraction_values;
+	std::vector<double> bezier_points;
+	std::vector<int32_t> boundary_labels;      // 6 per element
+	int32_t max_basis = 0;
+	int64_t elements() const { return (int64_t)element_offsets.size()-1; }
+	void Validate() const;
+};
+
+// Reads a v3/v4/v5 .ntiga database (iga::Database, IgaDatabase.hpp:64-161).
+HostMesh ReadNtiga(const std::string& path);
+
+// Node-graph block CSR (BlockPattern, BlockCsr.hpp:15-55).
+struct HostPattern {
+	std::vector<int32_t> row_offsets;
+	std::vector<int32_t> columns;
+	std::vector<int32_t> diagonal;
+	int32_t max_row = 0;
+};
+HostPattern BuildPattern(const HostMesh& mesh);
+
+// A labelled boundary face: element, local face (0..5), label.
+struct BoundaryFace {
+	int32_t element;
+	int32_t face;
+	int32_t label;
+};
+
+class Mesh {
+public:
+	explicit Mesh(HostMesh host);
+	~Mesh();
+	Mesh(const Mesh&) = delete;
+	Mesh& operator=(const Mesh&) = delete;
+
+	const HostMesh& host() const { return host_; }
+	const HostPattern& pattern() const { return pattern_; }
+	DeviceMeshView view() const { return view_; }
+	DevicePatternView pattern_view() const { return pattern_view_; }
+	const double* phi() const { return phi_.get(); }
+	const double* qdata() const { return qdata_.get(); }
+	const int32_t* element_blocks() const { return element_blocks_.get(); }
+	const std::vector<BoundaryFace>& faces() const { return faces_; }
+	const int32_t* face_element() const { return face_element_.get(); }
+	const double* face_coef() const { return face_coef_.get(); }
+	double min_detj() const { return min_detj_; }
+	int64_t bad_samples() const { return bad_samples_; }
+	int64_t device_bytes() const { return device_bytes_; }
+	cudaStream_t stream() const { return stream_; }
+	int64_t nodes() const { return host_.nodes; }
+
+private:
+	HostMesh host_;
+	HostPattern pattern_;
+	cudaStream_t stream_ = nullptr;
+	DeviceArray<int32_t> element_offsets_, connectivity_, extraction_offsets_, row_offsets_, columns_, diagonal_,
+		element_blocks_, face_element_, face_index_;
+	DeviceArray<uint8_t> extraction_columns_;
+	DeviceArray<double> extraction_values_, bezier_points_, phi_, qdata_, face_coef_;
+	DeviceMeshView view_;
+	DevicePatternView pattern_view_;
+	std::vector<BoundaryFace> faces_;
+	double min_detj_ = 0.0;
+	int64_t bad_samples_ = 0;
+	int64_t device_bytes_ = 0;
+};
+
+} // namespace tfiga

@@ -1,0 +1,302 @@
+// Newton iteration and physical step on the device (see ns.hpp).
+#include "ns.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <sstream>
+#include <string>
+
+namespace tfiga {
+
+namespace {
+
+std::string Precise(double v)
+{
+	char buffer[64];
+	std::snprintf(buffer, sizeof(buffer), "%.16e", v);
+	return buffer;
+}
+
+// Scalar slots in scalars_ / pinned_.
+enum : int { kContinuity = 0 /* sq, sum */, kNorm = 2 /* norm, sum */, kUpdateNorm = 4, kSlots = 8 };
+
+} // namespace
+
+NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
+	: mesh_(mesh), params_(params), n4_(4*mesh.nodes()),
+	  gmres_((int)mesh.nodes(), params.gmres_restart > 0 ? params.gmres_restart : 200, mesh.stream())
+{
+	if (!(params.density > 0.0) || !std::isfinite(params.density) || !(params.viscosity > 0.0)
+		|| !std::isfinite(params.viscosity) || !std::isfinite(params.dt) || params.dt < 0.0)
+		Fail(-1, "invalid Navier-Stokes density, dynamic viscosity, or time step");
+	if (params.dt > 0.0) {
+		const double inverse = 1.0/params.dt;
+		if (!std::isfinite(4.0*inverse*inverse) || !std::isfinite(params.density*inverse))
+			Fail(-1, "transient Navier-Stokes time step is not representable");
+	}
+	if (mesh.bad_samples() > 0)
+		Fail(-5, "mesh has "+std::to_string(mesh.bad_samples())+" non-positive quadrature Jacobians; minimum detJ "
+			+std::to_string(mesh.min_detj()));
+	stream_ = mesh.stream();
+	const int64_t n = mesh.nodes();
+	values_.Allocate((size_t)blocks()*16);
+	rhs_.Allocate(n4_); state_.Allocate(n4_); previous_.Allocate(n4_); update_.Allocate(n4_);
+	traction_.Allocate(n4_);
+	velocity_bc_.Allocate(3*n); pressure_bc_.Allocate(n);
+	vmask_.Allocate(n); pmask_.Allocate(n); constrained_.Allocate(n);
+	for (auto* a : {&rhs_, &state_, &previous_, &update_, &traction_, &velocity_bc_, &pressure_bc_}) a->Zero(stream_);
+	vmask_.Zero(stream_); pmask_.Zero(stream_);
+	partial_.Allocate(PartialSlots());
+	scalars_.Allocate(kSlots);
+	// Label slots of the boundary faces.
+	for (const auto& f : mesh.faces())
+		if (!slot_of_label_.count(f.label)) { slot_of_label_[f.label] = 0; }
+	int slot = 0;
+	for (auto& entry : slot_of_label_) { entry.second = slot++; labels_.push_back(entry.first); }
+	for (const auto& f : mesh.faces()) face_slot_host_.push_back(slot_of_label_[f.label]);
+	const size_t faces = mesh.faces().size();
+	if (faces) {
+		face_flow_.Allocate(faces);
+		face_pressure_.Allocate(faces);
+		face_pressure_.Zero(stream_);
+		face_slot_.Allocate(faces);
+		face_slot_.Upload(face_slot_host_.data(), faces, stream_);
+	}
+	label_flow_.Allocate(std::max<size_t>(1, labels_.size()));
+	CudaCheck(cudaMallocHost(reinterpret_cast<void**>(&pinned_), sizeof(double)*(kSlots+labels_.size()+1)),
+		"pinned scalars");
+	for (auto& ev : events_) CudaCheck(cudaEventCreate(&ev), "event");
+	CudaCheck(cudaStreamSynchronize(stream_), "solver setup");
+}
+
+NsSolver::~NsSolver()
+{
+	for (auto& ev : events_) if (ev) cudaEventDestroy(ev);
+	if (pinned_) cudaFreeHost(pinned_);
+}
+
+void NsSolver::SetDirichlet(const int32_t* vmask, const int32_t* pmask, const double* velocity, const double* pressure)
+{
+	const int64_t n = nodes();
+	std::vector<int32_t> vm(vmask, vmask+n), pm(n, 0), list;
+	if (pmask) pm.assign(pmask, pmask+n);
+	for (int64_t i = 0; i < n; ++i) {
+		vm[i] = vm[i] ? 1 : 0; pm[i] = pm[i] ? 1 : 0;
+		if (vm[i] || pm[i]) list.push_back((int32_t)i);
+	}
+	vmask_.Upload(vm.data(), n, stream_);
+	pmask_.Upload(pm.data(), n, stream_);
+	if (!list.empty()) constrained_.Upload(list.data(), list.size(), stream_);
+	constrained_count_ = (int)list.size();
+	SetDirichletValues(velocity, pressure);
+	CudaCheck(cudaStreamSynchronize(stream_), "Dirichlet upload");
+	dirichlet_set_ = true;
+}
+
+void NsSolver::SetDirichletValues(const double* velocity, const double* pressure)
+{
+	const int64_t n = nodes();
+	if (velocity) velocity_bc_.Upload(velocity, 3*n, stream_);
+	if (pressure) pressure_bc_.Upload(pressure, n, stream_);
+}
+
+void NsSolver::SetTractions(const int32_t* labels, const double* pressures, int count)
+{
+	std::map<int32_t, double> traction;
+	for (int i = 0; i < count; ++i) {
+		if (!std::isfinite(pressures[i])) Fail(-1, "pressure traction must be finite");
+		traction[labels[i]] = pressures[i];
+	}
+	for (const auto& t : traction) {
+		bool found = false;
+		for (const auto& f : mesh_.faces()) if (f.label == t.first) { found = true; break; }
+		if (!found)
+			Fail(-4, "pressure traction label "+std::to_string(t.first)
+				+" has no boundary faces in the .ntiga database; repack with iga_pack");
+	}
+	const auto& faces = mesh_.faces();
+	std::vector<double> fp(faces.size(), 0.0);
+	for (size_t i = 0; i < faces.size(); ++i) {
+		const auto it = traction.find(faces[i].label);
+		if (it != traction.end()) fp[i] = it->second;
+	}
+	traction_.Zero(stream_);
+	if (!faces.empty()) {
+		face_pressure_.Upload(fp.data(), fp.size(), stream_);
+		LaunchFaceTraction((int)faces.size(), mesh_.face_element(), mesh_.face_coef(), mesh_.view().element_offsets,
+			mesh_.view().connectivity, face_pressure_.get(), traction_.get(), stream_);
+		launches_ += 1;
+	}
+	CudaCheck(cudaStreamSynchronize(stream_), "traction");
+}
+
+void NsSolver::SetState(const double* state, const double* previous)
+{
+	state_.Upload(state, n4_, stream_);
+	previous_.Upload(previous ? previous : state, n4_, stream_);
+	CudaCheck(cudaStreamSynchronize(stream_), "state upload");
+}
+
+void NsSolver::GetState(double* state)
+{
+	state_.Download(state, n4_, stream_);
+	CudaCheck(cudaStreamSynchronize(stream_), "state download");
+}
+
+void NsSolver::CommitStep()
+{
+	CudaCheck(cudaMemcpyAsync(previous_.get(), state_.get(), n4_*sizeof(double), cudaMemcpyDeviceToDevice, stream_),
+		"previous-state copy");
+}
+
+void NsSolver::Assemble()
+{
+	values_.Zero(stream_);
+	rhs_.Zero(stream_);
+	LaunchAssemble(mesh_.view(), mesh_.phi(), mesh_.qdata(), mesh_.element_blocks(), state_.get(), previous_.get(),
+		{params_.density, params_.viscosity, params_.dt}, values_.get(), rhs_.get(), stream_);
+	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
+	launches_ += 2;
+}
+
+void NsSolver::ApplyDirichlet()
+{
+	if (!dirichlet_set_) Fail(-1, "Dirichlet conditions have not been set");
+	LaunchDirichletRows(mesh_.pattern_view(), constrained_count_, constrained_.get(), vmask_.get(), pmask_.get(),
+		velocity_bc_.get(), pressure_bc_.get(), state_.get(), values_.get(), rhs_.get(), stream_);
+	launches_ += 1;
+}
+
+GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
+{
+	update_.Zero(stream_);
+	return gmres_.Solve(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol, max_iterations,
+		&launches_);
+}
+
+void NsSolver::LaunchDiagnostics()
+{
+	LaunchStridedSums(nodes(), 4, 3, rhs_.get(), partial_.get(), scalars_.get()+kContinuity, stream_);
+	launches_ += 2;
+	const int faces = (int)mesh_.faces().size();
+	if (faces) {
+		LaunchFaceFlows(faces, mesh_.face_element(), mesh_.face_coef(), mesh_.view().element_offsets,
+			mesh_.view().connectivity, state_.get(), face_flow_.get(), stream_);
+		LaunchSegmentSums((int)labels_.size(), face_slot_.get(), faces, face_flow_.get(), label_flow_.get(), stream_);
+		launches_ += 2;
+	}
+}
+
+NsSolver::Diagnostics NsSolver::ReadDiagnostics()
+{
+	// pinned_ already holds the downloaded values (see NewtonIteration).
+	Diagnostics d{};
+	d.continuity_l2 = std::sqrt(pinned_[kContinuity]);
+	d.continuity_sum = pinned_[kContinuity+1];
+	for (size_t i = 0; i < labels_.size(); ++i) {
+		d.net_flow += pinned_[kSlots+i];
+		d.absolute_flow += std::fabs(pinned_[kSlots+i]);
+	}
+	d.imbalance = d.absolute_flow > 0.0 ? 2.0*std::fabs(d.net_flow)/d.absolute_flow : 0.0;
+	return d;
+}
+
+tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
+{
+	tfiga_newton_report report{};
+	CudaCheck(cudaEventRecord(events_[0], stream_), "event");
+	Assemble();
+	LaunchDiagnostics();
+	ApplyDirichlet();
+	LaunchNorm(n4_, rhs_.get(), partial_.get(), scalars_.get()+kNorm, stream_);
+	launches_ += 2;
+	CudaCheck(cudaEventRecord(events_[1], stream_), "event");
+	scalars_.Download(pinned_, kSlots, stream_);
+	if (!labels_.empty()) label_flow_.Download(pinned_+kSlots, labels_.size(), stream_);
+	CudaCheck(cudaStreamSynchronize(stream_), "Navier-Stokes assembly");
+	float ms = 0.0f;
+	CudaCheck(cudaEventElapsedTime(&ms, events_[0], events_[1]), "event time");
+	report.assembly_ms = ms;
+	const Diagnostics d = ReadDiagnostics();
+	report.continuity_l2 = d.continuity_l2;
+	report.continuity_sum = d.continuity_sum;
+	report.net_boundary_flow = d.net_flow;
+	report.absolute_boundary_flow = d.absolute_flow;
+	report.relative_mass_imbalance = d.imbalance;
+	const double norm = pinned_[kNorm];
+	report.residual_l2 = norm;
+	if (!std::isfinite(norm)) Fail(-6, "Navier-Stokes residual is not finite");
+	const double initial = initial_residual < 0.0 ? norm : initial_residual;
+	const double scale = std::sqrt((double)n4_);
+	report.tolerance = std::max(params_.nonlinear_atol*scale, params_.nonlinear_rtol*initial);
+	if (norm <= report.tolerance && d.imbalance <= params_.mass_rtol) {
+		report.converged = 1;
+		return report;
+	}
+	CudaCheck(cudaEventRecord(events_[2], stream_), "event");
+	const GmresResult linear = SolveLinear(params_.gmres_rtol, params_.gmres_max_iterations);
+	CudaCheck(cudaEventRecord(events_[3], stream_), "event");
+	report.linear_iterations = linear.iterations;
+	report.linear_residual = linear.residual;
+	report.singular_diagonal_blocks = (int32_t)linear.singular_blocks;
+	if (!linear.converged)
+		Fail(-6, "Navier-Stokes GMRES failed (residual="+Precise(linear.residual)+", nonlinear_residual="
+			+Precise(norm)+", continuity_l2="+Precise(d.continuity_l2)+", net_boundary_flow="+Precise(d.net_flow)
+			+", relative_mass_imbalance="+Precise(d.imbalance)+")");
+	LaunchNorm(n4_, update_.get(), partial_.get(), scalars_.get()+kUpdateNorm, stream_);
+	LaunchAxpy(n4_, 1.0, update_.get(), state_.get(), stream_);
+	launches_ += 3;
+	scalars_.Download(pinned_+kUpdateNorm, 1, stream_);
+	CudaCheck(cudaStreamSynchronize(stream_), "Navier-Stokes update");
+	CudaCheck(cudaEventElapsedTime(&ms, events_[2], events_[3]), "event time");
+	report.linear_ms = ms;
+	report.update_l2 = pinned_[kUpdateNorm];
+	return report;
+}
+
+tfiga_step_report NsSolver::Step()
+{
+	tfiga_step_report step{};
+	double initial = -1.0;
+	const int max_newton = params_.max_newton > 0 ? params_.max_newton : 12;
+	tfiga_newton_report last{};
+	for (int k = 0; k < max_newton; ++k) {
+		last = NewtonIteration(initial);
+		if (initial < 0.0) { initial = last.residual_l2; step.initial_residual_l2 = initial; }
+		step.assembly_ms += last.assembly_ms;
+		step.linear_ms += last.linear_ms;
+		step.linear_iterations += last.linear_iterations;
+		step.residual_l2 = last.residual_l2;
+		step.relative_mass_imbalance = last.relative_mass_imbalance;
+		step.newton_iterations = k;
+		if (last.converged) { step.converged = 1; return step; }
+	}
+	Fail(-6, "Navier-Stokes nonlinear solve reached MAX_NEWTON (nonlinear_residual="+Precise(last.residual_l2)
+		+", continuity_l2="+Precise(last.continuity_l2)+", net_boundary_flow="+Precise(last.net_boundary_flow)
+		+", relative_mass_imbalance="+Precise(last.relative_mass_imbalance)+")");
+}
+
+void NsSolver::BoundaryFlows(const int32_t* labels, int count, double* flows)
+{
+	const int faces = (int)mesh_.faces().size();
+	std::vector<double> per_label(labels_.size(), 0.0);
+	if (faces) {
+		LaunchFaceFlows(faces, mesh_.face_element(), mesh_.face_coef(), mesh_.view().element_offsets,
+			mesh_.view().connectivity, state_.get(), face_flow_.get(), stream_);
+		LaunchSegmentSums((int)labels_.size(), face_slot_.get(), faces, face_flow_.get(), label_flow_.get(), stream_);
+		launches_ += 2;
+		label_flow_.Download(per_label.data(), labels_.size(), stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "boundary flows");
+	}
+	for (int i = 0; i < count; ++i) {
+		const auto it = slot_of_label_.find(labels[i]);
+		flows[i] = it == slot_of_label_.end() ? 0.0 : per_label[it->second];
+	}
+}
+
+void NsSolver::Synchronize()
+{
+	CudaCheck(cudaStreamSynchronize(stream_), "synchronize");
+}
+
+} // namespace tfiga

@@ -1,0 +1,75 @@
+// Device-resident Navier-Stokes solver: one Newton iteration and one physical
+// step of the reference loop (solvers/cuda/src/iga_cuda.cu:952-1054).
+#pragma once
+
+#include "gmres.hpp"
+#include "mesh.hpp"
+
+#include "../../include/tfiga.h"
+
+#include <map>
+#include <vector>
+
+namespace tfiga {
+
+class NsSolver {
+public:
+	NsSolver(Mesh& mesh, const tfiga_ns_params& params);
+	~NsSolver();
+	NsSolver(const NsSolver&) = delete;
+	NsSolver& operator=(const NsSolver&) = delete;
+
+	void SetDirichlet(const int32_t* vmask, const int32_t* pmask, const double* velocity, const double* pressure);
+	void SetDirichletValues(const double* velocity, const double* pressure);
+	void SetTractions(const int32_t* labels, const double* pressures, int count);
+	void SetState(const double* state, const double* previous);
+	void GetState(double* state);
+	void CommitStep();
+
+	// values/rhs on the device: rhs = -r + traction.
+	void Assemble();
+	void ApplyDirichlet();
+	GmresResult SolveLinear(double rtol, int max_iterations);
+	tfiga_newton_report NewtonIteration(double initial_residual);
+	tfiga_step_report Step();
+	void BoundaryFlows(const int32_t* labels, int count, double* flows);
+	void Synchronize();
+
+	int64_t nodes() const { return mesh_.nodes(); }
+	long long blocks() const { return (long long)mesh_.pattern().columns.size(); }
+	double* values() { return values_.get(); }
+	double* state() { return state_.get(); }
+	double* rhs() { return rhs_.get(); }
+	double* update() { return update_.get(); }
+	const DevicePatternView pattern() const { return mesh_.pattern_view(); }
+	cudaStream_t stream() const { return stream_; }
+	long long launches() const { return launches_; }
+	void AddLaunches(long long n) { launches_ += n; }
+	const tfiga_ns_params& params() const { return params_; }
+
+private:
+	struct Diagnostics {
+		double continuity_l2, continuity_sum, net_flow, absolute_flow, imbalance;
+	};
+	void LaunchDiagnostics();     // continuity sums of rhs + per-label flows of state
+	Diagnostics ReadDiagnostics();
+
+	Mesh& mesh_;
+	tfiga_ns_params params_;
+	cudaStream_t stream_ = nullptr;
+	cudaEvent_t events_[4] = {};
+	long long launches_ = 0;
+	int64_t n4_;
+	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
+	DeviceArray<double> face_flow_, face_pressure_, label_flow_, partial_, scalars_;
+	DeviceArray<int32_t> vmask_, pmask_, constrained_, face_slot_;
+	std::vector<int32_t> labels_;            // distinct face labels (slot order)
+	std::map<int32_t, int> slot_of_label_;
+	std::vector<int32_t> face_slot_host_;
+	int constrained_count_ = 0;
+	bool dirichlet_set_ = false;
+	Gmres gmres_;
+	double* pinned_ = nullptr;               // host mirror of scalars + label flows
+};
+
+} // namespace tfiga

@@ -1,0 +1,344 @@
+// Block-CSR (4x4) kernels: SpMV (optionally fused with the block-Jacobi
+// apply), diagonal-block inverse, Dirichlet rows, boundary-face flows and
+// tractions, and deterministic two-stage reductions.
+//
+// SpMV layout: one warp per block row; lane = 4*slot + r processes row r of
+// blocks slot, slot+8, ... so each warp load covers 8 consecutive 128-byte
+// blocks (coalesced), then the 8 slots are reduced with shuffles.  This
+// replaces the reference's thread-per-row BlockSpmvKernel
+// (solvers/cuda/include/SparseKernels.cuh:25-40), whose loads are strided.
+#include "common.hpp"
+#include "kernels.cuh"
+
+namespace tfiga {
+namespace {
+
+constexpr int kReduceBlocks = 296;   // 2 CTAs per SM for the partial-sum stage
+
+__device__ __forceinline__ double RowBlockDot(const DevicePatternView& p, const double* __restrict__ values,
+	const double* __restrict__ x, int row, int lane)
+{
+	const int r = lane & 3, slot = lane >> 2;
+	double sum = 0.0;
+	const int lo = p.row_offsets[row], hi = p.row_offsets[row+1];
+	for (int b = lo+slot; b < hi; b += 8) {
+		const int col = p.columns[b];
+		const double2* a = reinterpret_cast<const double2*>(values+(size_t)b*16+r*4);
+		const double2 a01 = __ldg(a), a23 = __ldg(a+1);
+		const double2* xv = reinterpret_cast<const double2*>(x+4*(size_t)col);
+		const double2 x01 = __ldg(xv), x23 = __ldg(xv+1);
+		sum = fma(a01.x, x01.x, sum); sum = fma(a01.y, x01.y, sum);
+		sum = fma(a23.x, x23.x, sum); sum = fma(a23.y, x23.y, sum);
+	}
+	sum += __shfl_xor_sync(0xffffffffu, sum, 4);
+	sum += __shfl_xor_sync(0xffffffffu, sum, 8);
+	sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+	return sum;   // lanes 0..3 hold rows 0..3
+}
+
+__global__ void __launch_bounds__(256) SpmvKernel(DevicePatternView p, const double* __restrict__ values,
+	const double* __restrict__ x, double* __restrict__ y)
+{
+	const int row = blockIdx.x*8+(threadIdx.x >> 5);
+	const int lane = threadIdx.x & 31;
+	if (row >= p.nodes) return;
+	const double sum = RowBlockDot(p, values, x, row, lane);
+	if (lane < 4) y[4*(size_t)row+lane] = sum;
+}
+
+__global__ void __launch_bounds__(256) SpmvBlockJacobiKernel(DevicePatternView p, const double* __restrict__ values,
+	const double* __restrict__ inverse, const double* __restrict__ x, const double* __restrict__ scale,
+	double* __restrict__ y, const int* __restrict__ stop)
+{
+	if (stop != nullptr && *stop) return;
+	const int row = blockIdx.x*8+(threadIdx.x >> 5);
+	const int lane = threadIdx.x & 31;
+	if (row >= p.nodes) return;
+	double sum = RowBlockDot(p, values, x, row, lane);
+	if (scale != nullptr) sum *= *scale;
+	const double y0 = __shfl_sync(0xffffffffu, sum, 0), y1 = __shfl_sync(0xffffffffu, sum, 1);
+	const double y2 = __shfl_sync(0xffffffffu, sum, 2), y3 = __shfl_sync(0xffffffffu, sum, 3);
+	if (lane < 4) {
+		const double* d = inverse+(size_t)row*16+lane*4;
+		y[4*(size_t)row+lane] = d[0]*y0+d[1]*y1+d[2]*y2+d[3]*y3;
+	}
+}
+
+// Gauss-Jordan with partial pivoting and the singular fallback of
+// BuildBlockInverseKernel (SparseKernels.cuh:42-89).
+__global__ void BlockInverseKernel(DevicePatternView p, const double* __restrict__ values,
+	double* __restrict__ inverse, unsigned int* __restrict__ singular)
+{
+	const int node = blockIdx.x*blockDim.x+threadIdx.x;
+	if (node >= p.nodes) return;
+	const double* s = values+(size_t)p.diagonal[node]*16;
+	double m[4][8];
+	for (int i = 0; i < 4; ++i)
+		for (int j = 0; j < 8; ++j) m[i][j] = j < 4 ? s[i*4+j] : (j-4 == i ? 1.0 : 0.0);
+	bool failed = false;
+	for (int pivot = 0; pivot < 4; ++pivot) {
+		int best = pivot;
+		for (int r = pivot+1; r < 4; ++r)
+			if (fabs(m[r][pivot]) > fabs(m[best][pivot])) best = r;
+		if (!isfinite(m[best][pivot]) || fabs(m[best][pivot]) < 1e-14) { failed = true; break; }
+		if (best != pivot)
+			for (int c = 0; c < 8; ++c) { const double t = m[pivot][c]; m[pivot][c] = m[best][c]; m[best][c] = t; }
+		const double sc = 1.0/m[pivot][pivot];
+		for (int c = 0; c < 8; ++c) m[pivot][c] *= sc;
+		for (int r = 0; r < 4; ++r) {
+			if (r == pivot) continue;
+			const double factor = m[r][pivot];
+			for (int c = 0; c < 8; ++c) m[r][c] -= factor*m[pivot][c];
+		}
+	}
+	double* d = inverse+(size_t)node*16;
+	if (!failed) {
+		for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) d[i*4+j] = m[i][4+j];
+	} else {
+		atomicAdd(singular, 1u);
+		for (int i = 0; i < 4; ++i)
+			for (int j = 0; j < 4; ++j)
+				d[i*4+j] = i == j && fabs(s[i*4+i]) > 1e-14 ? 1.0/s[i*4+i] : (i == j ? 1.0 : 0.0);
+	}
+}
+
+__global__ void ApplyBlockInverseKernel(int nodes, const double* __restrict__ inverse, const double* __restrict__ x,
+	double* __restrict__ y)
+{
+	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (i >= 4LL*nodes) return;
+	const long long node = i >> 2;
+	const int r = (int)(i & 3);
+	const double* d = inverse+node*16+r*4;
+	const double* v = x+4*node;
+	y[i] = d[0]*v[0]+d[1]*v[1]+d[2]*v[2]+d[3]*v[3];
+}
+
+// Dirichlet rows (IgaCudaKernels.cuh:436-463): a warp per constrained node.
+__global__ void DirichletRowsKernel(DevicePatternView p, int count, const int32_t* __restrict__ nodes,
+	const int32_t* __restrict__ vmask, const int32_t* __restrict__ pmask, const double* __restrict__ velocity,
+	const double* __restrict__ pressure, const double* __restrict__ state, double* __restrict__ values,
+	double* __restrict__ rhs)
+{
+	const int item = blockIdx.x*(blockDim.x >> 5)+(threadIdx.x >> 5);
+	const int lane = threadIdx.x & 31;
+	if (item >= count) return;
+	const int node = nodes[item];
+	const bool cv = vmask[node] != 0, cp = pmask[node] != 0;
+	if (values != nullptr) {
+		const int lo = p.row_offsets[node], hi = p.row_offsets[node+1];
+		for (int b = lo+lane; b < hi; b += 32) {
+			double* blk = values+(size_t)b*16;
+			if (cv) for (int k = 0; k < 12; ++k) blk[k] = 0.0;
+			if (cp) for (int k = 12; k < 16; ++k) blk[k] = 0.0;
+		}
+		__syncwarp();
+		if (lane == 0) {
+			double* diag = values+(size_t)p.diagonal[node]*16;
+			if (cv) { diag[0] = 1.0; diag[5] = 1.0; diag[10] = 1.0; }
+			if (cp) diag[15] = 1.0;
+		}
+	}
+	if (rhs != nullptr && lane < 4) {
+		const bool c = lane < 3 ? cv : cp;
+		if (c) {
+			const double target = lane < 3 ? velocity[3*(size_t)node+lane] : pressure[node];
+			rhs[4*(size_t)node+lane] = target-state[4*(size_t)node+lane];
+		}
+	}
+}
+
+// Outward flow of each boundary face: sum_a F[a].u_a (BoundaryFlow.hpp:165-200).
+__global__ void __launch_bounds__(64) FaceFlowKernel(int faces, const int32_t* __restrict__ face_element,
+	const double* __restrict__ coef, const int32_t* __restrict__ eo, const int32_t* __restrict__ conn,
+	const double* __restrict__ state, double* __restrict__ out)
+{
+	const int face = blockIdx.x;
+	const int e = face_element[face];
+	const int begin = eo[e], nen = eo[e+1]-begin;
+	double v = 0.0;
+	const int a = threadIdx.x;
+	if (a < nen) {
+		const size_t node = (size_t)conn[begin+a];
+		const double* F = coef+((size_t)face*kMaxBasis+a)*3;
+		v = F[0]*state[4*node]+F[1]*state[4*node+1]+F[2]*state[4*node+2];
+	}
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	__shared__ double part[2];
+	if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+	__syncthreads();
+	if (threadIdx.x == 0) out[face] = part[0]+part[1];
+}
+
+// traction[4 node + c] -= p_face F[a][c] (IntegratePressureTractionForces, PressureTractionFlow.hpp:41-64).
+__global__ void __launch_bounds__(64) FaceTractionKernel(int faces, const int32_t* __restrict__ face_element,
+	const double* __restrict__ coef, const int32_t* __restrict__ eo, const int32_t* __restrict__ conn,
+	const double* __restrict__ face_pressure, double* __restrict__ traction)
+{
+	const int face = blockIdx.x;
+	const double pressure = face_pressure[face];
+	if (pressure == 0.0) return;
+	const int e = face_element[face];
+	const int begin = eo[e], nen = eo[e+1]-begin;
+	const int a = threadIdx.x;
+	if (a >= nen) return;
+	const size_t node = (size_t)conn[begin+a];
+	const double* F = coef+((size_t)face*kMaxBasis+a)*3;
+	for (int c = 0; c < 3; ++c) atomicAdd(traction+4*node+c, -pressure*F[c]);
+}
+
+__device__ __forceinline__ double BlockSum(double v, double* shared)
+{
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	if (lane == 0) shared[warp] = v;
+	__syncthreads();
+	v = 0.0;
+	if (warp == 0) {
+		const int warps = blockDim.x >> 5;
+		v = lane < warps ? shared[lane] : 0.0;
+		for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	}
+	__syncthreads();
+	return v;
+}
+
+__global__ void __launch_bounds__(256) StridedPartialKernel(long long count, int stride, int offset,
+	const double* __restrict__ x, double* __restrict__ partial)
+{
+	__shared__ double shared[8];
+	double sq = 0.0, sum = 0.0;
+	for (long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x; i < count; i += (long long)gridDim.x*blockDim.x) {
+		const double v = x[i*stride+offset];
+		sq = fma(v, v, sq);
+		sum += v;
+	}
+	sq = BlockSum(sq, shared);
+	sum = BlockSum(sum, shared);
+	if (threadIdx.x == 0) { partial[2*blockIdx.x] = sq; partial[2*blockIdx.x+1] = sum; }
+}
+
+__global__ void __launch_bounds__(256) FinalizeSumsKernel(int blocks, const double* __restrict__ partial,
+	double* __restrict__ out, int take_sqrt)
+{
+	__shared__ double shared[8];
+	double sq = 0.0, sum = 0.0;
+	for (int i = threadIdx.x; i < blocks; i += blockDim.x) { sq += partial[2*i]; sum += partial[2*i+1]; }
+	sq = BlockSum(sq, shared);
+	sum = BlockSum(sum, shared);
+	if (threadIdx.x == 0) { out[0] = take_sqrt ? sqrt(sq) : sq; out[1] = sum; }
+}
+
+__global__ void AxpyKernel(long long n, double alpha, const double* __restrict__ x, double* __restrict__ y)
+{
+	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (i < n) y[i] = fma(alpha, x[i], y[i]);
+}
+
+__global__ void __launch_bounds__(256) SegmentSumKernel(const int32_t* __restrict__ segment_of, int items,
+	const double* __restrict__ values, double* __restrict__ out)
+{
+	__shared__ double shared[8];
+	const int seg = blockIdx.x;
+	double v = 0.0;
+	for (int i = threadIdx.x; i < items; i += blockDim.x)
+		if (segment_of[i] == seg) v += values[i];
+	v = BlockSum(v, shared);
+	if (threadIdx.x == 0) out[seg] = v;
+}
+
+unsigned Blocks(long long n, int threads) { return (unsigned)((n+threads-1)/threads); }
+
+} // namespace
+
+int PartialSlots() { return 2*kReduceBlocks; }
+
+void LaunchSpmv(const DevicePatternView& p, const double* values, const double* x, double* y, cudaStream_t stream)
+{
+	if (p.nodes == 0) return;
+	SpmvKernel<<<Blocks(p.nodes, 8), 256, 0, stream>>>(p, values, x, y);
+	LaunchCheck("SpmvKernel");
+}
+
+void LaunchSpmvBlockJacobi(const DevicePatternView& p, const double* values, const double* inverse,
+	const double* x, const double* scale, double* y, const int* stop, cudaStream_t stream)
+{
+	if (p.nodes == 0) return;
+	SpmvBlockJacobiKernel<<<Blocks(p.nodes, 8), 256, 0, stream>>>(p, values, inverse, x, scale, y, stop);
+	LaunchCheck("SpmvBlockJacobiKernel");
+}
+
+void LaunchBlockInverse(const DevicePatternView& p, const double* values, double* inverse, unsigned int* singular,
+	cudaStream_t stream)
+{
+	if (p.nodes == 0) return;
+	BlockInverseKernel<<<Blocks(p.nodes, 128), 128, 0, stream>>>(p, values, inverse, singular);
+	LaunchCheck("BlockInverseKernel");
+}
+
+void LaunchApplyBlockInverse(int nodes, const double* inverse, const double* x, double* y, cudaStream_t stream)
+{
+	if (nodes == 0) return;
+	ApplyBlockInverseKernel<<<Blocks(4LL*nodes, 256), 256, 0, stream>>>(nodes, inverse, x, y);
+	LaunchCheck("ApplyBlockInverseKernel");
+}
+
+void LaunchDirichletRows(const DevicePatternView& p, int count, const int32_t* nodes, const int32_t* vmask,
+	const int32_t* pmask, const double* velocity, const double* pressure, const double* state, double* values,
+	double* rhs, cudaStream_t stream)
+{
+	if (count == 0) return;
+	DirichletRowsKernel<<<Blocks(count, 8), 256, 0, stream>>>(p, count, nodes, vmask, pmask, velocity, pressure,
+		state, values, rhs);
+	LaunchCheck("DirichletRowsKernel");
+}
+
+void LaunchFaceFlows(int faces, const int32_t* face_element, const double* face_coef, const int32_t* eo,
+	const int32_t* conn, const double* state, double* face_flow, cudaStream_t stream)
+{
+	if (faces == 0) return;
+	FaceFlowKernel<<<faces, 64, 0, stream>>>(faces, face_element, face_coef, eo, conn, state, face_flow);
+	LaunchCheck("FaceFlowKernel");
+}
+
+void LaunchFaceTraction(int faces, const int32_t* face_element, const double* face_coef, const int32_t* eo,
+	const int32_t* conn, const double* face_pressure, double* traction, cudaStream_t stream)
+{
+	if (faces == 0) return;
+	FaceTractionKernel<<<faces, 64, 0, stream>>>(faces, face_element, face_coef, eo, conn, face_pressure, traction);
+	LaunchCheck("FaceTractionKernel");
+}
+
+void LaunchStridedSums(long long count, int stride, int offset, const double* x, double* partial, double* out,
+	cudaStream_t stream)
+{
+	StridedPartialKernel<<<kReduceBlocks, 256, 0, stream>>>(count, stride, offset, x, partial);
+	LaunchCheck("StridedPartialKernel");
+	FinalizeSumsKernel<<<1, 256, 0, stream>>>(kReduceBlocks, partial, out, 0);
+	LaunchCheck("FinalizeSumsKernel");
+}
+
+void LaunchNorm(long long n, const double* x, double* partial, double* out, cudaStream_t stream)
+{
+	StridedPartialKernel<<<kReduceBlocks, 256, 0, stream>>>(n, 1, 0, x, partial);
+	LaunchCheck("StridedPartialKernel");
+	FinalizeSumsKernel<<<1, 256, 0, stream>>>(kReduceBlocks, partial, out, 1);
+	LaunchCheck("FinalizeSumsKernel");
+}
+
+void LaunchAxpy(long long n, double alpha, const double* x, double* y, cudaStream_t stream)
+{
+	if (n == 0) return;
+	AxpyKernel<<<Blocks(n, 256), 256, 0, stream>>>(n, alpha, x, y);
+	LaunchCheck("AxpyKernel");
+}
+
+void LaunchSegmentSums(int segments, const int32_t* segment_of, int items, const double* values, double* out,
+	cudaStream_t stream)
+{
+	if (segments == 0) return;
+	SegmentSumKernel<<<segments, 256, 0, stream>>>(segment_of, items, values, out);
+	LaunchCheck("SegmentSumKernel");
+}
+
+} // namespace tfiga
