@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Time steps/s of the body-fitted IGA Navier-Stokes solve on one B200.
+
+Workload (the BASELINE metric's mixed-precision config, run here by the plain
+FP64 solver): the 51,200-element pulsatile tube -- an 8x8-core + two 32-cell
+ring-layer O-grid cross-section (128 cells, 145 control points per plane) x
+400 axial layers, R = 1.5 mm, L = 30 mm, tricubic, rho = 1060 kg/m^3,
+mu = 3.5e-3 Pa s, backward Euler dt = 2e-3 s, parabolic inflow scaled by a
+seeded Fourier waveform (mean 0.15 m/s + 4 harmonics, amplitudes U(0, 0.05),
+seed 0, 1 Hz), zero-traction outlet, no-slip wall.  Inputs are synthetic
+(seeded generator), stated in `data`.
+
+A "step" is one physical time step: Newton to ||r|| <= 1e-8 ||r_0|| with the
+exact tangent, each linear solve block-Jacobi GMRES(200) to rtol 1e-8.
+
+Legs of one run (rank 0 prints one JSON line):
+  value     device-timed (CUDA events on the solver stream) with every input
+            resident in HBM; the matrix (> 1.8 GB) exceeds L2, so no flush.
+  e2e       the same steps through the C ABI with pinned host inputs (inlet
+            Dirichlet values) and the state read back every step.
+  roofline  per-kernel CUDA-event timing of the timed region: SpMV + block-
+            Jacobi (HBM-bound) and the FP64 assembly GEMM.
+  cpu_baseline  the reference's own element code (oracle/_ref) and the CPU
+            restatement of block-Jacobi GMRES on a bounded sample, all host
+            cores, scaled to time steps/s.
+  --impl reference  only the CPU reference arm, as its own line.
+
+Multi-GPU: the single-mesh path does not shard ("replicas only"): under
+torchrun every rank runs an independent replica; value = total steps / max
+time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "NS time steps/s at rel.res 1e-8: learned+mixed vs plain FP64 GPU; SpMV GB/s"
+RHO, MU, DT = 1060.0, 3.5e-3, 2e-3
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def workload(name):
+    from tubularflowiga_b200 import meshgen
+    if name == "c1":
+        tube = meshgen.straight_cylinder_1280()
+        desc = ("straight cylinder 1,280 tricubic elements (4x4 core + 16-cell ring) x 40 layers, "
+                "R 1.5 mm, L 30 mm, steady inflow peak 0.2 m/s")
+        wave = None
+    else:
+        tube = meshgen.pulsatile_tube_51200()
+        desc = ("pulsatile tube 51,200 tricubic elements (8x8 core + 2x32-cell ring) x 400 layers, "
+                "R 1.5 mm, L 30 mm, Fourier inflow mean 0.15 m/s + 4 harmonics U(0,0.05) seed 0")
+        wave = meshgen.fourier_waveform(0)
+    return tube, desc, wave
+
+
+def inlet_factor(wave, t):
+    if wave is None:
+        return 0.2
+    th = 2 * np.pi * (t % wave["period"]) / wave["period"] + wave["phase"]
+    return wave["mean"] + sum(c * np.cos((k + 1) * th) + s * np.sin((k + 1) * th)
+                              for k, (c, s) in enumerate(zip(wave["cosine"], wave["sine"])))
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[1])); mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_counts(tube, blocks):
+    """Per-launch algorithmic bytes / flops (SpMV: 8 B values + 4 B column index per block entry set)."""
+    n = tube.mesh.nodes
+    N = 4 * n
+    b_spmv = blocks * (16 * 8 + 4) + 4 * (n + 1) + N * 8 + N * 8
+    b_bjac = n * 16 * 8                      # fused block-Jacobi apply: the 4x4 inverse per node
+    nen = np.diff(tube.mesh.element_offsets).astype(np.float64)
+    f_asm = float((8192.0 * nen * nen).sum())
+    return b_spmv, b_bjac, f_asm
+
+
+def cpu_reference(tube, state, prev, steps_newton, lin_per_newton, budget_s=25.0):
+    """Reference CPU path on a bounded sample: reference element code + CPU block-Jacobi GMRES."""
+    from oracle import oracle as O
+    m = tube.mesh
+    P = O.Pattern(m.nodes, m.element_offsets, m.connectivity)
+    kind = "reference" if O.ref_available() else "port"
+    threads = O.ref().ref_max_threads() if kind == "reference" else O.max_threads()
+    # assembly sample: the first `count` elements, doubled until it takes ~40% of the budget
+    count = max(threads, 64)
+    while True:
+        count = min(count, m.elements)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            O.ref_assemble(m, P, state, prev, RHO, MU, DT, 0, count)
+        else:
+            O.assemble(m, P, state, prev, RHO, MU, DT)
+            count = m.elements
+        dt_s = time.perf_counter() - t0
+        t_el = dt_s / count
+        if dt_s > 0.4 * budget_s or count >= m.elements:
+            break
+        count *= 2
+    asm_elements = min(count, m.elements)
+    t_assembly = t_el * m.elements
+    # GMRES sample on the full-size system pattern (iterations are data-independent in cost)
+    rng = np.random.default_rng(0)
+    vals = np.zeros(P.blocks * 16)
+    vals.reshape(-1, 4, 4)[P.diagonal] = np.eye(4) * 4.0
+    vals += rng.standard_normal(vals.size) * 1e-3
+    rhs = rng.standard_normal(4 * m.nodes)
+    iters = 10
+    while True:
+        t0 = time.perf_counter()
+        O.gmres_bjacobi(P, vals, rhs, restart=200, maxit=iters, rtol=1e-300)
+        dt_s = time.perf_counter() - t0
+        if dt_s > 0.4 * budget_s or iters >= 400:
+            break
+        iters *= 2
+    t_iter = dt_s / iters
+    t_step = steps_newton * (t_assembly + lin_per_newton * t_iter)
+    return {
+        "value": 1.0 / t_step, "unit": "time steps/s", "cores": int(threads), "kind": kind,
+        "sample": (f"reference element assembly of {asm_elements} of {m.elements} elements "
+                   f"({t_el * 1e3:.2f} ms/element wall on {threads} threads) and {iters} block-Jacobi GMRES(200) "
+                   f"iterations of the CPU restatement on the full {4 * m.nodes}-DOF pattern "
+                   f"({t_iter * 1e3:.1f} ms/iteration); step = {steps_newton:.2f} Newton x (assembly + "
+                   f"{lin_per_newton:.0f} GMRES iterations), counts from the GPU run of the same algorithm"),
+        "assembly_s": t_assembly, "gmres_iteration_s": t_iter,
+    }
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    tube, desc, wave = workload(args.workload)
+    from tubularflowiga_b200 import api
+    n = tube.mesh.nodes
+    vmask, pmask, vel = api.tube_boundary_conditions(tube, inlet_factor(wave, 0.0))
+    s0 = api.initial_state(vmask, vel)
+    # Newton and GMRES counts per step of this algorithm on this workload, as measured by the GPU arm.
+    newton, lin = args.ref_newton, args.ref_linear
+    budget = max(4.0, min(args.ref_budget, 120.0 / max(1, args.steps + 1)))
+    cpu_reference(tube, s0, s0, newton, lin, budget_s=2.0)           # warm-up sample
+    samples = [cpu_reference(tube, s0, s0, newton, lin, budget_s=budget) for _ in range(args.steps)]
+    res = dict(samples[-1])
+    res["value"] = float(np.mean([r["value"] for r in samples]))
+    line = {"metric": METRIC, "value": res["value"], "unit": "time steps/s", "impl": "reference",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 / res["value"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": desc, "elements": tube.mesh.elements, "nodes": n,
+                       "solver": "reference CPU element code + CPU block-Jacobi GMRES(200)",
+                       "parallelism": "replicas only"},
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": "time steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget", type=float, default=25.0)
+    ap.add_argument("--ref-newton", type=float, default=3.0)
+    ap.add_argument("--ref-linear", type=float, default=300.0)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, world, rank)
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    from tubularflowiga_b200 import api
+
+    tube, desc, wave = workload(args.workload)
+    n = tube.mesh.nodes
+    mesh = api.Mesh(tube.mesh)
+    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT if args.workload == "c2" else 1e-3,
+                          nonlinear_rtol=1e-8, nonlinear_atol=1e-300, mass_rtol=1e-3,
+                          gmres_restart=200, gmres_max_iterations=5000, gmres_rtol=1e-8)
+    dt = ns.params.dt
+    vmask, pmask, vel0 = api.tube_boundary_conditions(tube, 1.0)
+    profile = vel0.copy()
+
+    def bc(step):
+        return (inlet_factor(wave, (step + 1) * dt) * profile).ravel()
+
+    ns.set_dirichlet(vmask, pmask, inlet_factor(wave, 0.0) * profile)
+    ns.set_tractions({2: 0.0})
+    s0 = api.initial_state(vmask, inlet_factor(wave, 0.0) * profile)
+    ns.set_state(s0, s0)
+    stream = torch.cuda.ExternalStream(ns.stream())
+    total = args.warmup + 2 * args.steps
+    # every step's Dirichlet values resident in HBM before timing (value leg)
+    bc_dev = torch.tensor(np.stack([bc(k) for k in range(total)]), dtype=torch.float64, device="cuda")
+    bc_host = torch.tensor(np.stack([bc(k) for k in range(total)]), dtype=torch.float64).pin_memory()
+    out_host = torch.empty(4 * n, dtype=torch.float64).pin_memory()
+
+    reports = []
+
+    def do_step(k, host=False):
+        if host:
+            api.check(api.lib().tfiga_ns_set_dirichlet_values(ns._h, api.C.c_void_p(bc_host[k].data_ptr()), None))
+        else:
+            api.check(api.lib().tfiga_ns_set_dirichlet_values(ns._h, api.C.c_void_p(bc_dev[k].data_ptr()), None))
+        ns.commit_step()
+        r = ns.step()
+        reports.append(r)
+        if host:
+            api.check(api.lib().tfiga_ns_get_state(ns._h, api.C.c_void_p(out_host.data_ptr())))
+
+    for k in range(args.warmup):
+        do_step(k)
+    reports.clear()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ns.set_profiling(True)
+    ns.profile(reset=True)
+    launches0 = ns.launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for k in range(args.warmup, args.warmup + args.steps):
+            do_step(k)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = ns.launches() - launches0
+    prof = ns.profile(reset=True)
+    ns.set_profiling(False)
+    timed_reports = list(reports)
+    reports.clear()
+    # e2e leg: pinned host inputs, state read back each step
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for k in range(args.warmup + args.steps, total):
+        do_step(k, host=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+
+    if dist:
+        t = torch.tensor([ms, e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
+    hbm, bf16, peak_kind = peaks()
+    b_spmv, b_bjac, f_asm = algorithmic_counts(tube, mesh.blocks)
+    spmv_ms, spmv_n = prof["spmv_block_jacobi"]
+    asm_ms, asm_n = prof["assembly"]
+    orth_ms, orth_n = prof["krylov_orthogonalisation"]
+    kernels = {}
+    if spmv_n:
+        a = (b_spmv + b_bjac) / (spmv_ms / spmv_n * 1e-3) / 1e9
+        kernels["spmv_block_jacobi"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
+                                        "frac": a / hbm, "traffic": None, "launches": spmv_n,
+                                        "avg_ms": spmv_ms / spmv_n, "share": spmv_ms / ms,
+                                        "algorithmic_bytes": b_spmv + b_bjac}
+    if asm_n:
+        a = f_asm / (asm_ms / asm_n * 1e-3) / 1e12
+        kernels["assembly_fp64"] = {"bound": "fp64", "achieved": a, "peak": 37.0, "unit": "TFLOP/s",
+                                    "frac": a / 37.0, "traffic": None, "launches": asm_n,
+                                    "avg_ms": asm_ms / asm_n, "share": asm_ms / ms,
+                                    "peak_note": "nominal B200 FP64 (no measured FP64 peak on this pool)"}
+    kernels["krylov_orthogonalisation"] = {"avg_ms": orth_ms / max(orth_n, 1), "launches": orth_n,
+                                           "share": orth_ms / ms}
+    dominant = max(("spmv_block_jacobi", "assembly_fp64"), key=lambda k: kernels.get(k, {}).get("share", 0))
+    roof = dict(kernels[dominant])
+    roof["kernel"] = dominant
+    if roof["bound"] == "hbm":
+        roof["peak_kind"] = f"{peak_kind} hbm_gbs"
+    steps_per_s = world * args.steps / (ms / 1e3)
+    newton = np.mean([r["newton_iterations"] for r in timed_reports])
+    linear = np.sum([r["linear_iterations"] for r in timed_reports]) / max(1, np.sum(
+        [r["newton_iterations"] for r in timed_reports]))
+    line = {
+        "metric": METRIC, "value": steps_per_s, "unit": "time steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator; BASELINE publishes no dataset)",
+        "config": {"workload": desc, "elements": tube.mesh.elements, "nodes": n, "block_nonzeros": mesh.blocks,
+                   "solver": "plain FP64: exact-tangent Newton to rel.res 1e-8, block-Jacobi GMRES(200) rtol 1e-8",
+                   "l2": "inputs larger than L2 (matrix %.2f GB)" % (mesh.blocks * 128 / 1e9),
+                   "parallelism": "replicas only" if world > 1 else "single GPU"},
+        "newton_per_step": float(newton), "linear_iterations_per_newton": float(linear),
+        "roofline": roof, "kernels": kernels,
+        "spmv_gbs": kernels.get("spmv_block_jacobi", {}).get("achieved"),
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": "time steps/s",
+                "h2d_bytes_per_step": 3 * n * 8, "d2h_bytes_per_step": 4 * n * 8},
+    }
+    if not args.no_cpu_baseline and world == 1:
+        st = ns.get_state()
+        try:
+            cb = cpu_reference(tube, st, st, max(newton, 1.0), max(linear, 1.0), budget_s=args.ref_budget)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as exc:  # noqa: BLE001 -- reported, not hidden
+            line["cpu_baseline"] = {"value": None, "error": str(exc)}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -187,6 +187,17 @@ int tfiga_ns_device_buffers(tfiga_ns* ns, double** values, double** state, doubl
 int64_t tfiga_ns_launch_count(const tfiga_ns* ns);
 /* Waits for the handle's stream (bounded by the driver). */
 int tfiga_ns_synchronize(tfiga_ns* ns);
+/* The handle's CUDA stream (a cudaStream_t), for callers that time with
+ * CUDA events on the launching stream. */
+int tfiga_ns_stream(tfiga_ns* ns, void** stream);
+/* Per-kernel-family device timing with CUDA events recorded around each
+ * launch on the handle's stream (the reference's PhaseProfile,
+ * include/PhaseProfile.hpp:14-138, at kernel granularity).  Families:
+ * 0 assembly, 1 SpMV + block-Jacobi, 2 Krylov orthogonalisation, 3 other. */
+#define TFIGA_PROFILE_FAMILIES 4
+int tfiga_ns_set_profiling(tfiga_ns* ns, int enable);
+/* Totals since the last reset: milliseconds and launch counts per family. */
+int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int32_t reset);
 
 /* ---- drop-in command ------------------------------------------------- */
 /* `navier-stokes DATABASE CASE_DIR [MAX_NEWTON] [OUTPUT] [options]`, the argv of

@@ -91,6 +91,9 @@ def ref():
         R.ref_ntiga_element.argtypes = [C.c_char_p, C.c_uint64, C.POINTER(C.c_int), _ip, _ip, _dp, _dp]
         R.ref_wall_trace.argtypes = [C.c_char_p, C.c_char_p, _ip, C.c_longlong]
         R.ref_wall_trace.restype = C.c_longlong
+        R.ref_assemble.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip, _up, _dp, _dp, _ip, _ip, _dp, _dp,
+                                   C.c_double, C.c_double, C.c_double, C.c_void_p, _dp]
+        R.ref_max_threads.restype = C.c_int
     return _ref
 
 
@@ -237,6 +240,23 @@ def assemble(mesh, pattern, state, previous, density, viscosity, dt, jacobian=Tr
                         density, viscosity, dt, _ptr(values), rhs, C.byref(failed))
     if st:
         raise RuntimeError(f"oracle assembly failed at element {failed.value} ({st})")
+    return values, rhs
+
+
+def ref_assemble(mesh, pattern, state, previous, density, viscosity, dt, first=0, last=None,
+                 jacobian=True):
+    """Assembly of elements [first, last) with the reference's own compiled element code."""
+    R = ref()
+    last = mesh.elements if last is None else last
+    values = np.zeros(pattern.blocks * 16) if jacobian else None
+    rhs = np.zeros(4 * mesh.nodes)
+    prev = np.ascontiguousarray(previous if previous is not None else np.zeros(4 * mesh.nodes), np.float64)
+    st = R.ref_assemble(first, last, mesh.element_offsets, mesh.connectivity, mesh.extraction_offsets,
+                        mesh.extraction_columns, mesh.extraction_values, mesh.bezier_points,
+                        pattern.row_offsets, pattern.columns, np.ascontiguousarray(state, np.float64).ravel(),
+                        prev.ravel(), density, viscosity, dt, _ptr(values), rhs)
+    if st:
+        raise RuntimeError(R.ref_last_error().decode())
     return values, rhs
 
 

@@ -17,6 +17,9 @@
 #include "NavierStokesElement.hpp"
 #include "OutletModel.hpp"
 
+#include <omp.h>
+
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <exception>
@@ -221,5 +224,77 @@ long long ref_wall_trace(const char* database_path, const char* vtk_path, int* o
 		return -1;
 	}
 }
+
+// Global assembly with the reference's own element code: an OpenMP loop over
+// elements [first, last) of a flattened mesh, each element built by
+// iga::BuildNavierStokesElement (exact tangent, 4x4x4 rule) and added into
+// 4x4 block CSR as OwnedRowAssembler::AddElementMatrix does
+// (solvers/cpu/include/OwnedRowAssembler.hpp:210-236).  values may be null
+// (residual only).  Returns 0 or -1.
+int ref_assemble(int first, int last, const int* element_offsets, const int* connectivity,
+	const int* extraction_offsets, const std::uint8_t* extraction_columns, const double* extraction_values,
+	const double* bezier_points, const int* row_offsets, const int* columns, const double* state,
+	const double* previous, double density, double viscosity, double dt, double* values, double* rhs)
+{
+	std::atomic<int> failed{0};
+#pragma omp parallel for schedule(dynamic, 2)
+	for (int e = first; e < last; ++e) {
+		if (failed.load()) continue;
+		try {
+			const int begin = element_offsets[e];
+			const int nen = element_offsets[e+1]-begin;
+			iga::Element element;
+			element.connectivity.resize(static_cast<std::size_t>(nen));
+			element.extraction.assign(static_cast<std::size_t>(nen), std::array<double, 64>{});
+			std::vector<std::array<double, 4>> nodal(static_cast<std::size_t>(nen)), prev(static_cast<std::size_t>(nen));
+			for (int a = 0; a < nen; ++a) {
+				const int node = connectivity[begin+a];
+				element.connectivity[static_cast<std::size_t>(a)] = node;
+				for (int k = extraction_offsets[begin+a]; k < extraction_offsets[begin+a+1]; ++k)
+					element.extraction[static_cast<std::size_t>(a)][extraction_columns[k]] = extraction_values[k];
+				for (int f = 0; f < 4; ++f) {
+					nodal[static_cast<std::size_t>(a)][static_cast<std::size_t>(f)] = state[4*static_cast<std::size_t>(node)+f];
+					prev[static_cast<std::size_t>(a)][static_cast<std::size_t>(f)] = previous[4*static_cast<std::size_t>(node)+f];
+				}
+			}
+			for (int p = 0; p < 64; ++p)
+				for (int d = 0; d < 3; ++d)
+					element.bezier_points[static_cast<std::size_t>(p)][static_cast<std::size_t>(d)] = bezier_points[static_cast<std::size_t>(e)*192+p*3+d];
+			iga::FullCell4x4x4VolumeQuadratureProvider quadrature(element);
+			const auto system = iga::BuildNavierStokesElement(element, nodal,
+				dt > 0.0 ? prev : std::vector<std::array<double, 4>>{}, {density, viscosity, dt}, quadrature.Rule(),
+				values ? iga::NavierStokesAssemblyRequest::ResidualAndJacobian
+					: iga::NavierStokesAssemblyRequest::ResidualOnly);
+			const int ndof = 4*nen;
+			for (int a = 0; a < nen; ++a) {
+				const int row = element.connectivity[static_cast<std::size_t>(a)];
+				for (int f = 0; f < 4; ++f) {
+#pragma omp atomic
+					rhs[4*static_cast<std::size_t>(row)+f] += system.negative_residual[static_cast<std::size_t>(4*a+f)];
+				}
+				if (!values) continue;
+				for (int b = 0; b < nen; ++b) {
+					const int column = element.connectivity[static_cast<std::size_t>(b)];
+					const int* lo = columns+row_offsets[row];
+					const int* hi = columns+row_offsets[row+1];
+					const int* it = std::lower_bound(lo, hi, column);
+					double* block = values+static_cast<std::size_t>(it-columns)*16;
+					for (int i = 0; i < 4; ++i)
+						for (int f = 0; f < 4; ++f) {
+#pragma omp atomic
+							block[i*4+f] += system.jacobian[static_cast<std::size_t>((4*a+i)*ndof+4*b+f)];
+						}
+				}
+			}
+		} catch (const std::exception& error) {
+#pragma omp critical
+			last_error = error.what();
+			failed.store(1);
+		}
+	}
+	return failed.load() ? -1 : 0;
+}
+
+int ref_max_threads() { return omp_get_max_threads(); }
 
 } // extern "C"

@@ -147,8 +147,9 @@ def test_newton_steps_match_oracle_cylinder_1280(api, cylinder_1280):
     vmask, pmask, vel = api.tube_boundary_conditions(tube, 0.2)
     state0 = api.initial_state(vmask, vel)
     mesh = api.Mesh(flat)
-    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, gmres_rtol=1e-14,
-                          gmres_max_iterations=50000, gmres_restart=200)
+    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, gmres_rtol=1e-12,
+                          gmres_max_iterations=50000, gmres_restart=200, nonlinear_rtol=1e-30,
+                          nonlinear_atol=1e-300, mass_rtol=1e300)
     ns.set_dirichlet(vmask, pmask, vel)
     ns.set_tractions({2: 0.0})
     ns.set_state(state0, state0)

@@ -94,6 +94,9 @@ SIGNATURES = {
                                           C.POINTER(C.c_void_p)]),
     "tfiga_ns_launch_count": (C.c_int64, [C.c_void_p]),
     "tfiga_ns_synchronize": (C.c_int, [C.c_void_p]),
+    "tfiga_ns_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "tfiga_ns_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "tfiga_ns_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
     "tfiga_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
 }
 
@@ -265,6 +268,22 @@ class NavierStokes:
 
     def synchronize(self):
         check(lib().tfiga_ns_synchronize(self._h))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib().tfiga_ns_stream(self._h, C.byref(s)))
+        return int(s.value or 0)
+
+    def set_profiling(self, enable: bool):
+        check(lib().tfiga_ns_set_profiling(self._h, int(enable)))
+
+    FAMILIES = ("assembly", "spmv_block_jacobi", "krylov_orthogonalisation", "other")
+
+    def profile(self, reset=False) -> dict:
+        ms = np.zeros(4)
+        counts = np.zeros(4, np.int64)
+        check(lib().tfiga_ns_profile(self._h, _p(ms), _p(counts), int(reset)))
+        return {f: (float(ms[i]), int(counts[i])) for i, f in enumerate(self.FAMILIES)}
 
     def close(self):
         if self._h:

@@ -334,4 +334,30 @@ int tfiga_ns_synchronize(tfiga_ns* ns)
 	});
 }
 
+int tfiga_ns_stream(tfiga_ns* ns, void** stream)
+{
+	return Guard([&] {
+		Require(ns && stream, "null argument");
+		*stream = (void*)ns->solver->stream();
+	});
+}
+
+int tfiga_ns_set_profiling(tfiga_ns* ns, int enable)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		ns->solver->profiler().Enable(enable != 0);
+	});
+}
+
+int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int32_t reset)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		long long counts[tfiga::Profiler::kFamilies];
+		ns->solver->profiler().Totals(milliseconds, counts, reset != 0);
+		if (launches) for (int f = 0; f < tfiga::Profiler::kFamilies; ++f) launches[f] = counts[f];
+	});
+}
+
 } // extern "C"

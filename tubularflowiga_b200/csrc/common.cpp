@@ -67,4 +67,53 @@ void RequireDevice()
 			+std::to_string(prop.major)+std::to_string(prop.minor));
 }
 
+Profiler::~Profiler()
+{
+	for (auto& m : pool_) { cudaEventDestroy(m.start); cudaEventDestroy(m.stop); }
+}
+
+void Profiler::Begin(Family family, cudaStream_t stream)
+{
+	if (!enabled_) return;
+	if (used_ == pool_.size()) {
+		Mark m{};
+		CudaCheck(cudaEventCreate(&m.start), "profile event");
+		CudaCheck(cudaEventCreate(&m.stop), "profile event");
+		pool_.push_back(m);
+	}
+	pool_[used_].family = family;
+	CudaCheck(cudaEventRecord(pool_[used_].start, stream), "profile record");
+	open_ = (int)used_;
+}
+
+void Profiler::End(cudaStream_t stream)
+{
+	if (!enabled_ || open_ < 0) return;
+	CudaCheck(cudaEventRecord(pool_[open_].stop, stream), "profile record");
+	open_ = -1;
+	++used_;
+}
+
+void Profiler::Collect()
+{
+	for (size_t i = 0; i < used_; ++i) {
+		CudaCheck(cudaEventSynchronize(pool_[i].stop), "profile sync");
+		float ms = 0.0f;
+		CudaCheck(cudaEventElapsedTime(&ms, pool_[i].start, pool_[i].stop), "profile elapsed");
+		ms_[pool_[i].family] += ms;
+		count_[pool_[i].family] += 1;
+	}
+	used_ = 0;
+}
+
+void Profiler::Totals(double* ms, long long* counts, bool reset)
+{
+	Collect();
+	for (int f = 0; f < kFamilies; ++f) {
+		if (ms) ms[f] = ms_[f];
+		if (counts) counts[f] = count_[f];
+		if (reset) { ms_[f] = 0.0; count_[f] = 0; }
+	}
+}
+
 } // namespace tfiga

@@ -8,6 +8,7 @@
 #include <stdexcept>
 #include <string>
 #include <utility>
+#include <vector>
 
 namespace tfiga {
 
@@ -65,15 +66,16 @@ public:
 		data_ = nullptr;
 		count_ = 0;
 	}
+	// Source/destination may be host (pageable or pinned) or device memory (unified addressing).
 	void Upload(const T* host, std::size_t count, cudaStream_t stream)
 	{
 		if (count > count_) Fail(-1, "upload exceeds device array size");
-		if (count) CudaCheck(cudaMemcpyAsync(data_, host, count*sizeof(T), cudaMemcpyHostToDevice, stream), "upload");
+		if (count) CudaCheck(cudaMemcpyAsync(data_, host, count*sizeof(T), cudaMemcpyDefault, stream), "upload");
 	}
 	void Download(T* host, std::size_t count, cudaStream_t stream) const
 	{
 		if (count > count_) Fail(-1, "download exceeds device array size");
-		if (count) CudaCheck(cudaMemcpyAsync(host, data_, count*sizeof(T), cudaMemcpyDeviceToHost, stream), "download");
+		if (count) CudaCheck(cudaMemcpyAsync(host, data_, count*sizeof(T), cudaMemcpyDefault, stream), "download");
 	}
 	void Zero(cudaStream_t stream)
 	{
@@ -94,5 +96,28 @@ long long DeviceBytesPeak();
 
 // Requires a device that can run sm_100a code.
 void RequireDevice();
+
+// Device time per kernel family from CUDA events recorded around launches on
+// the launching stream.  Disabled by default; Collect() waits for the stream.
+class Profiler {
+public:
+	enum Family { kAssembly = 0, kSpmv = 1, kOrtho = 2, kOther = 3, kFamilies = 4 };
+	~Profiler();
+	void Enable(bool on) { enabled_ = on; }
+	bool enabled() const { return enabled_; }
+	void Begin(Family family, cudaStream_t stream);
+	void End(cudaStream_t stream);
+	void Collect();
+	void Totals(double* ms, long long* counts, bool reset);
+
+private:
+	struct Mark { cudaEvent_t start, stop; int family; };
+	bool enabled_ = false;
+	std::vector<Mark> pool_;
+	size_t used_ = 0;
+	int open_ = -1;
+	double ms_[kFamilies] = {0, 0, 0, 0};
+	long long count_[kFamilies] = {0, 0, 0, 0};
+};
 
 } // namespace tfiga

@@ -221,8 +221,10 @@ void Gmres::Step(const DevicePatternView& pattern, const double* values, int j)
 	const int* stop = state_.get();
 	const size_t dot_smem = (size_t)chunk_*sizeof(double);
 	const size_t coef_smem = (size_t)(restart_+1)*sizeof(double);
+	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
 	LaunchSpmvBlockJacobi(pattern, values, inverse_.get(), V_.get()+(size_t)j*n_, scale_.get()+j, w_.get(), stop,
 		stream_);
+	if (profiler_) { profiler_->End(stream_); profiler_->Begin(Profiler::kOrtho, stream_); }
 	for (int pass = 0; pass < 2; ++pass) {
 		MultiDotKernel<<<blocks_, kThreads, dot_smem, stream_>>>(V_.get(), n_, scale_.get(), count, w_.get(),
 			partial_.get(), chunk_, stop);
@@ -235,6 +237,7 @@ void Gmres::Step(const DevicePatternView& pattern, const double* values, int j)
 			w_.get(), out, pass == 0 ? nullptr : norm_partial_.get(), stop);
 		LaunchCheck("UpdateKernel");
 	}
+	if (profiler_) profiler_->End(stream_);
 	launches_ += 8;
 }
 

@@ -33,6 +33,7 @@ public:
 	GmresResult Solve(const DevicePatternView& pattern, const double* values, const double* rhs, double* x,
 		double rtol, int max_iterations, long long* launches);
 	int restart() const { return restart_; }
+	void set_profiler(Profiler* profiler) { profiler_ = profiler; }
 	std::size_t bytes() const;
 
 private:
@@ -50,6 +51,7 @@ private:
 	DeviceArray<unsigned> singular_;
 	struct HostStatus { int stop, used, error, pad; double residual; double beta[2]; unsigned singular; };
 	HostStatus* host_ = nullptr;
+	Profiler* profiler_ = nullptr;
 };
 
 } // namespace tfiga

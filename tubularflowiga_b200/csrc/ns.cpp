@@ -66,6 +66,7 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 	CudaCheck(cudaMallocHost(reinterpret_cast<void**>(&pinned_), sizeof(double)*(kSlots+labels_.size()+1)),
 		"pinned scalars");
 	for (auto& ev : events_) CudaCheck(cudaEventCreate(&ev), "event");
+	gmres_.set_profiler(&profiler_);
 	CudaCheck(cudaStreamSynchronize(stream_), "solver setup");
 }
 
@@ -153,8 +154,10 @@ void NsSolver::Assemble()
 {
 	values_.Zero(stream_);
 	rhs_.Zero(stream_);
+	profiler_.Begin(Profiler::kAssembly, stream_);
 	LaunchAssemble(mesh_.view(), mesh_.phi(), mesh_.qdata(), mesh_.element_blocks(), state_.get(), previous_.get(),
 		{params_.density, params_.viscosity, params_.dt}, values_.get(), rhs_.get(), stream_);
+	profiler_.End(stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
 	launches_ += 2;
 }

@@ -46,6 +46,7 @@ public:
 	long long launches() const { return launches_; }
 	void AddLaunches(long long n) { launches_ += n; }
 	const tfiga_ns_params& params() const { return params_; }
+	Profiler& profiler() { return profiler_; }
 
 private:
 	struct Diagnostics {
@@ -69,6 +70,7 @@ private:
 	int constrained_count_ = 0;
 	bool dirichlet_set_ = false;
 	Gmres gmres_;
+	Profiler profiler_;
 	double* pinned_ = nullptr;               // host mirror of scalars + label flows
 };
 
