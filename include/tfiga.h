@@ -82,8 +82,16 @@ typedef struct tfiga_ns_params {
 	double mass_rtol;              /* default 1e-3 */
 	int32_t gmres_restart;         /* default 200 */
 	int32_t gmres_max_iterations;  /* default 5000 */
-	double gmres_rtol;             /* default 1e-8 (preconditioned residual) */
+	double gmres_rtol;             /* default 1e-8 */
+	/* TFIGA_PRECONDITIONER_BLOCK_JACOBI: left-preconditioned GMRES with the
+	 * reference's tolerance on the preconditioned residual (Gmres.hpp:192-336);
+	 * TFIGA_PRECONDITIONER_AMG: flexible GMRES right-preconditioned by one
+	 * point-block aggregation AMG V-cycle, tolerance on the true residual. */
+	int32_t preconditioner;        /* default TFIGA_PRECONDITIONER_BLOCK_JACOBI */
 } tfiga_ns_params;
+
+#define TFIGA_PRECONDITIONER_BLOCK_JACOBI 0
+#define TFIGA_PRECONDITIONER_AMG 1
 
 /* One Newton iteration's log record (iga_cuda.cu:1000-1009, 1034-1045). */
 typedef struct tfiga_newton_report {
@@ -102,6 +110,13 @@ typedef struct tfiga_newton_report {
 	double assembly_ms;
 	double linear_ms;
 } tfiga_newton_report;
+
+/* Multigrid hierarchy of the AMG preconditioner (after the first solve). */
+typedef struct tfiga_amg_info {
+	int32_t levels;
+	int32_t nodes[8];
+	int64_t blocks[8];
+} tfiga_amg_info;
 
 /* One physical step (the Newton loop of iga_cuda.cu:956-1054). */
 typedef struct tfiga_step_report {
@@ -174,6 +189,8 @@ int tfiga_ns_solve_linear(tfiga_ns* ns, double rtol, int32_t max_iterations, dou
 int tfiga_ns_newton_iteration(tfiga_ns* ns, double initial_residual, tfiga_newton_report* report);
 /* One physical step: the Newton loop to convergence (iga_cuda.cu:952-1054). */
 int tfiga_ns_step(tfiga_ns* ns, tfiga_step_report* report);
+/* AMG hierarchy sizes (levels = 0 before the hierarchy is built). */
+int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info);
 /* Outward flow through each labelled boundary (IntegrateBoundaryFlow,
  * BoundaryFlow.hpp:165-200; MeasureFlowConvergence iga_cuda.cu:520-557). */
 int tfiga_ns_boundary_flows(tfiga_ns* ns, const int32_t* labels, int32_t count, double* flows);
@@ -193,7 +210,8 @@ int tfiga_ns_stream(tfiga_ns* ns, void** stream);
 /* Per-kernel-family device timing with CUDA events recorded around each
  * launch on the handle's stream (the reference's PhaseProfile,
  * include/PhaseProfile.hpp:14-138, at kernel granularity).  Families:
- * 0 assembly, 1 SpMV + block-Jacobi, 2 Krylov orthogonalisation, 3 other. */
+ * 0 assembly, 1 SpMV (fused with the block-Jacobi apply in that mode),
+ * 2 Krylov orthogonalisation, 3 AMG V-cycle. */
 #define TFIGA_PROFILE_FAMILIES 4
 int tfiga_ns_set_profiling(tfiga_ns* ns, int enable);
 /* Totals since the last reset: milliseconds and launch counts per family. */

@@ -147,7 +147,7 @@ def test_newton_steps_match_oracle_cylinder_1280(api, cylinder_1280):
     vmask, pmask, vel = api.tube_boundary_conditions(tube, 0.2)
     state0 = api.initial_state(vmask, vel)
     mesh = api.Mesh(flat)
-    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, gmres_rtol=1e-12,
+    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, gmres_rtol=1e-13,
                           gmres_max_iterations=50000, gmres_restart=200, nonlinear_rtol=1e-30,
                           nonlinear_atol=1e-300, mass_rtol=1e300)
     ns.set_dirichlet(vmask, pmask, vel)
@@ -163,6 +163,59 @@ def test_newton_steps_match_oracle_cylinder_1280(api, cylinder_1280):
         assert abs(report["residual_l2"] - norm) <= 1e-9 * max(norm, 1e-30)
         if initial < 0:
             initial = report["residual_l2"]
+        gpu = ns.get_state().reshape(-1, 4)
+        ref = oracle_state.reshape(-1, 4)
+        assert rel(gpu[:, :3], ref[:, :3]) < 1e-10, it
+        assert rel(gpu[:, 3], ref[:, 3]) < 1e-10, it
+
+
+def test_amg_fgmres_solve(api, cylinder_1280):
+    """AMG-preconditioned FGMRES on the C1 Newton system: true residual and direct-solve agreement."""
+    import scipy.sparse.linalg as spla
+    tube = cylinder_1280
+    flat = tube.mesh
+    vmask, pmask, vel = api.tube_boundary_conditions(tube, 0.2)
+    s0 = api.initial_state(vmask, vel)
+    mesh = api.Mesh(flat)
+    iterations = {}
+    for name, pc in (("bj", api.BLOCK_JACOBI), ("amg", api.AMG)):
+        ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, preconditioner=pc)
+        ns.set_dirichlet(vmask, pmask, vel)
+        ns.set_state(s0, s0)
+        ns.assemble(values=False, rhs=False)
+        values, rhs = ns.apply_dirichlet()
+        u, it, _ = ns.solve_linear(rtol=1e-10, max_iterations=5000)
+        iterations[name] = it
+        P = O.Pattern(flat.nodes, flat.element_offsets, flat.connectivity)
+        A = P.to_scipy(values)
+        assert np.linalg.norm(A @ u - rhs) <= 2e-10 * np.linalg.norm(rhs)
+        direct = spla.spsolve(A.tocsc(), rhs)
+        assert rel(u, direct) < 1e-6
+        if pc == api.AMG:
+            info = ns.amg_info()
+            assert info["levels"] >= 2 and info["nodes"][0] == flat.nodes
+            assert all(a > b for a, b in zip(info["nodes"], info["nodes"][1:]))
+    assert iterations["amg"] < iterations["bj"]
+
+
+def test_newton_steps_amg_match_oracle(api, cylinder_1280):
+    """Same 1e-10 Newton-step parity with the AMG-FGMRES linear solver."""
+    tube = cylinder_1280
+    flat = tube.mesh
+    vmask, pmask, vel = api.tube_boundary_conditions(tube, 0.2)
+    state0 = api.initial_state(vmask, vel)
+    mesh = api.Mesh(flat)
+    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, gmres_rtol=1e-13, gmres_max_iterations=5000,
+                          nonlinear_rtol=1e-30, nonlinear_atol=1e-300, mass_rtol=1e300, preconditioner=api.AMG)
+    ns.set_dirichlet(vmask, pmask, vel)
+    ns.set_tractions({2: 0.0})
+    ns.set_state(state0, state0)
+    P = O.Pattern(flat.nodes, flat.element_offsets, flat.connectivity)
+    oracle_state = state0.copy()
+    for it in range(2):
+        ns.newton_iteration(-1.0)
+        oracle_state, _, _ = O.newton_step(flat, P, oracle_state, state0, RHO, MU, DT, vmask, pmask,
+                                           vel.ravel(), np.zeros(flat.nodes))
         gpu = ns.get_state().reshape(-1, 4)
         ref = oracle_state.reshape(-1, 4)
         assert rel(gpu[:, :3], ref[:, :3]) < 1e-10, it

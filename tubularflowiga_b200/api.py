@@ -40,7 +40,15 @@ class NsParams(C.Structure):
     _fields_ = [("density", C.c_double), ("viscosity", C.c_double), ("dt", C.c_double),
                 ("max_newton", C.c_int32), ("nonlinear_rtol", C.c_double), ("nonlinear_atol", C.c_double),
                 ("mass_rtol", C.c_double), ("gmres_restart", C.c_int32), ("gmres_max_iterations", C.c_int32),
-                ("gmres_rtol", C.c_double)]
+                ("gmres_rtol", C.c_double), ("preconditioner", C.c_int32)]
+
+
+BLOCK_JACOBI = 0
+AMG = 1
+
+
+class AmgInfo(C.Structure):
+    _fields_ = [("levels", C.c_int32), ("nodes", C.c_int32 * 8), ("blocks", C.c_int64 * 8)]
 
 
 class NewtonReport(C.Structure):
@@ -88,6 +96,7 @@ SIGNATURES = {
                                         C.POINTER(C.c_double)]),
     "tfiga_ns_newton_iteration": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(NewtonReport)]),
     "tfiga_ns_step": (C.c_int, [C.c_void_p, C.POINTER(StepReport)]),
+    "tfiga_ns_amg_info": (C.c_int, [C.c_void_p, C.POINTER(AmgInfo)]),
     "tfiga_ns_boundary_flows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "tfiga_ns_spmv_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "tfiga_ns_device_buffers": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
@@ -277,7 +286,13 @@ class NavierStokes:
     def set_profiling(self, enable: bool):
         check(lib().tfiga_ns_set_profiling(self._h, int(enable)))
 
-    FAMILIES = ("assembly", "spmv_block_jacobi", "krylov_orthogonalisation", "other")
+    FAMILIES = ("assembly", "spmv", "krylov_orthogonalisation", "amg_vcycle")
+
+    def amg_info(self) -> dict:
+        info = AmgInfo()
+        check(lib().tfiga_ns_amg_info(self._h, C.byref(info)))
+        return {"levels": info.levels, "nodes": list(info.nodes[:info.levels]),
+                "blocks": list(info.blocks[:info.levels])}
 
     def profile(self, reset=False) -> dict:
         ms = np.zeros(4)

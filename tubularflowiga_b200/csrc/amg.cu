@@ -1,0 +1,527 @@
+// Point-block aggregation AMG: host setup, device refresh and V-cycle (see amg.hpp).
+#include "amg.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+namespace tfiga {
+
+struct Amg::Level {
+	int nodes = 0;
+	long long blocks = 0;
+	std::vector<int32_t> h_rows, h_cols, h_diag;     // pattern of this level's operator
+	std::vector<double> h_mask;                      // [4*nodes] 1 = free DOF
+	DeviceArray<int32_t> rows, cols, diag;
+	DeviceArray<double> values, inverse, mask, x, b, r;
+	DeviceArray<unsigned> singular;
+	// transfer to the next level
+	std::vector<int32_t> h_agg;
+	DeviceArray<int32_t> agg, agg_order, agg_offsets, gal_order, gal_offsets, block_row;
+	// coarsest level
+	int dense_n = 0;
+	DeviceArray<double> dense;
+	DeviceArray<int> dense_flag;
+	DevicePatternView view() const { return {nodes, blocks, rows.get(), cols.get(), diag.get()}; }
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+
+unsigned Grid(long long n, int per) { return (unsigned)((n+per-1)/per); }
+
+__global__ void StrengthKernel(long long blocks, const double* __restrict__ values, double* __restrict__ s)
+{
+	const long long b = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (b >= blocks) return;
+	const double* v = values+b*16;
+	s[b] = fabs(v[0])+fabs(v[5])+fabs(v[10]);
+}
+
+// Coarse block = masked sum of its fine blocks, one thread per (coarse block, entry).
+__global__ void GalerkinKernel(long long coarse_blocks, const int32_t* __restrict__ order,
+	const int32_t* __restrict__ offsets, const int32_t* __restrict__ block_row, const int32_t* __restrict__ fine_cols,
+	const double* __restrict__ fine_mask, const double* __restrict__ fine_values, double* __restrict__ coarse_values)
+{
+	const long long t = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (t >= coarse_blocks*16) return;
+	const long long B = t >> 4;
+	const int e = (int)(t & 15), r = e >> 2, c = e & 3;
+	double sum = 0.0;
+	for (int k = offsets[B]; k < offsets[B+1]; ++k) {
+		const int fb = order[k];
+		const double m = fine_mask[4*(size_t)block_row[fb]+r]*fine_mask[4*(size_t)fine_cols[fb]+c];
+		sum += m*fine_values[(size_t)fb*16+e];
+	}
+	coarse_values[t] = sum;
+}
+
+// Masked-out coarse DOFs are decoupled: unit diagonal.
+__global__ void UnitDiagonalKernel(int nodes, const int32_t* __restrict__ diag, const double* __restrict__ mask,
+	double* __restrict__ values)
+{
+	const int i = blockIdx.x*blockDim.x+threadIdx.x;
+	if (i >= 4*nodes) return;
+	const int node = i >> 2, c = i & 3;
+	if (mask[i] == 0.0) values[(size_t)diag[node]*16+c*4+c] = 1.0;
+}
+
+// r = b - A x (warp per block row); x may be null (r = b).
+__global__ void __launch_bounds__(256) ResidualKernel(DevicePatternView p, const double* __restrict__ values,
+	const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ r, const int* __restrict__ stop)
+{
+	if (*stop) return;
+	const int row = blockIdx.x*8+(threadIdx.x >> 5);
+	const int lane = threadIdx.x & 31;
+	if (row >= p.nodes) return;
+	const int rr = lane & 3, slot = lane >> 2;
+	double sum = 0.0;
+	for (int k = p.row_offsets[row]+slot; k < p.row_offsets[row+1]; k += 8) {
+		const double2* a = reinterpret_cast<const double2*>(values+(size_t)k*16+rr*4);
+		const double2 a01 = __ldg(a), a23 = __ldg(a+1);
+		const double2* xv = reinterpret_cast<const double2*>(x+4*(size_t)p.columns[k]);
+		const double2 x01 = __ldg(xv), x23 = __ldg(xv+1);
+		sum = fma(a01.x, x01.x, sum); sum = fma(a01.y, x01.y, sum);
+		sum = fma(a23.x, x23.x, sum); sum = fma(a23.y, x23.y, sum);
+	}
+	sum += __shfl_xor_sync(0xffffffffu, sum, 4);
+	sum += __shfl_xor_sync(0xffffffffu, sum, 8);
+	sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+	if (lane < 4) r[4*(size_t)row+lane] = b[4*(size_t)row+lane]-sum;
+}
+
+// x = omega D^{-1} r (zero initial guess) or x += omega D^{-1} r; thread per DOF.
+__global__ void JacobiKernel(int nodes, const double* __restrict__ inverse, const double* __restrict__ r,
+	double* __restrict__ x, double omega, int accumulate, const int* __restrict__ stop)
+{
+	if (*stop) return;
+	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (i >= 4LL*nodes) return;
+	const long long node = i >> 2;
+	const int c = (int)(i & 3);
+	const double* d = inverse+node*16+c*4;
+	const double* v = r+4*node;
+	const double z = omega*(d[0]*v[0]+d[1]*v[1]+d[2]*v[2]+d[3]*v[3]);
+	x[i] = accumulate ? x[i]+z : z;
+}
+
+// b_c[I,c] = sum_{i in I} mask_i[c] r[i,c] (fine nodes grouped by aggregate).
+__global__ void RestrictKernel(int coarse_nodes, const int32_t* __restrict__ order, const int32_t* __restrict__ offsets,
+	const double* __restrict__ mask, const double* __restrict__ r, double* __restrict__ bc, const int* __restrict__ stop)
+{
+	if (*stop) return;
+	const int t = blockIdx.x*blockDim.x+threadIdx.x;
+	if (t >= 4*coarse_nodes) return;
+	const int I = t >> 2, c = t & 3;
+	double sum = 0.0;
+	for (int k = offsets[I]; k < offsets[I+1]; ++k) {
+		const size_t i = (size_t)order[k];
+		sum += mask[4*i+c]*r[4*i+c];
+	}
+	bc[t] = sum;
+}
+
+// x[i,c] += mask_i[c] x_c[agg(i), c].
+__global__ void ProlongKernel(int nodes, const int32_t* __restrict__ agg, const double* __restrict__ mask,
+	const double* __restrict__ xc, double* __restrict__ x, const int* __restrict__ stop)
+{
+	if (*stop) return;
+	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (i >= 4LL*nodes) return;
+	x[i] += mask[i]*xc[4*(size_t)agg[i >> 2]+(i & 3)];
+}
+
+__global__ void DenseScatterKernel(DevicePatternView p, const double* __restrict__ values, int n, double* __restrict__ dense)
+{
+	const long long t = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (t >= p.blocks*16) return;
+	const long long k = t >> 4;
+	const int e = (int)(t & 15), r = e >> 2, c = e & 3;
+	// row of block k: binary search in row offsets
+	int lo = 0, hi = p.nodes;
+	while (hi-lo > 1) {
+		const int mid = (lo+hi)/2;
+		if (p.row_offsets[mid] <= k) lo = mid; else hi = mid;
+	}
+	const size_t row = 4*(size_t)lo+r, col = 4*(size_t)p.columns[k]+c;
+	dense[row*(size_t)(2*n)+col] = values[t];
+}
+
+// In-place Gauss-Jordan inverse with partial pivoting on [A | I] (n x 2n), one CTA.
+__global__ void __launch_bounds__(1024) DenseInverseKernel(int n, double* __restrict__ a, int* __restrict__ flag)
+{
+	const int ld = 2*n;
+	__shared__ double best_val[32];
+	__shared__ int best_idx[32];
+	__shared__ int pivot_row;
+	for (int i = threadIdx.x; i < n; i += blockDim.x)
+		for (int j = 0; j < n; ++j) a[(size_t)i*ld+n+j] = i == j ? 1.0 : 0.0;
+	__syncthreads();
+	for (int k = 0; k < n; ++k) {
+		double bv = -1.0; int bi = k;
+		for (int i = k+threadIdx.x; i < n; i += blockDim.x) {
+			const double v = fabs(a[(size_t)i*ld+k]);
+			if (v > bv) { bv = v; bi = i; }
+		}
+		for (int o = 16; o > 0; o >>= 1) {
+			const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+			const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+			if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+		}
+		if ((threadIdx.x & 31) == 0) { best_val[threadIdx.x >> 5] = bv; best_idx[threadIdx.x >> 5] = bi; }
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double v = -1.0; int idx = k;
+			for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+				if (best_val[w] > v) { v = best_val[w]; idx = best_idx[w]; }
+			pivot_row = idx;
+			if (!(v > 1e-300)) { *flag = 1; pivot_row = -1; }
+		}
+		__syncthreads();
+		const int pr = pivot_row;
+		if (pr < 0) {
+			// singular column: decouple it (unit pivot) and continue
+			for (int j = threadIdx.x; j < ld; j += blockDim.x) a[(size_t)k*ld+j] = j == k || j == n+k ? 1.0 : 0.0;
+			__syncthreads();
+		} else if (pr != k) {
+			for (int j = threadIdx.x; j < ld; j += blockDim.x) {
+				const double t = a[(size_t)k*ld+j];
+				a[(size_t)k*ld+j] = a[(size_t)pr*ld+j];
+				a[(size_t)pr*ld+j] = t;
+			}
+			__syncthreads();
+		}
+		const double inv = 1.0/a[(size_t)k*ld+k];
+		__syncthreads();
+		for (int j = threadIdx.x; j < ld; j += blockDim.x) a[(size_t)k*ld+j] *= inv;
+		__syncthreads();
+		for (int idx = threadIdx.x; idx < n*ld; idx += blockDim.x) {
+			const int i = idx/ld, j = idx%ld;
+			if (i == k) continue;
+			const double f = a[(size_t)i*ld+k];
+			if (j != k && f != 0.0) a[(size_t)i*ld+j] -= f*a[(size_t)k*ld+j];
+		}
+		__syncthreads();
+		for (int i = threadIdx.x; i < n; i += blockDim.x)
+			if (i != k) a[(size_t)i*ld+k] = 0.0;
+		__syncthreads();
+	}
+}
+
+// x = A^{-1} b with the inverse in the right half of the augmented matrix; warp per row.
+__global__ void DenseApplyKernel(int n, const double* __restrict__ a, const double* __restrict__ b,
+	double* __restrict__ x, const int* __restrict__ stop)
+{
+	if (*stop) return;
+	const int row = blockIdx.x*(blockDim.x >> 5)+(threadIdx.x >> 5);
+	const int lane = threadIdx.x & 31;
+	if (row >= n) return;
+	const double* ar = a+(size_t)row*(2*n)+n;
+	double s = 0.0;
+	for (int j = lane; j < n; j += 32) s = fma(ar[j], b[j], s);
+	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+	if (lane == 0) x[row] = s;
+}
+
+} // namespace
+
+Amg::Amg(const DevicePatternView& fine, const std::vector<int32_t>& row_offsets, const std::vector<int32_t>& columns,
+	cudaStream_t stream, AmgOptions options)
+	: fine_(fine), fine_rows_(row_offsets), fine_columns_(columns), stream_(stream), options_(options)
+{
+}
+
+Amg::~Amg() = default;
+
+std::vector<int> Amg::level_nodes() const
+{
+	std::vector<int> out;
+	for (const auto& l : levels_) out.push_back(l->nodes);
+	return out;
+}
+
+std::vector<long long> Amg::level_blocks() const
+{
+	std::vector<long long> out;
+	for (const auto& l : levels_) out.push_back(l->blocks);
+	return out;
+}
+
+void Amg::SetMasks(const std::vector<int32_t>& velocity_mask, const std::vector<int32_t>& pressure_mask)
+{
+	vmask_ = velocity_mask;
+	pmask_ = pressure_mask;
+	masks_dirty_ = true;
+}
+
+namespace {
+
+// Vanek-style greedy aggregation on the symmetrised strength graph.
+std::vector<int32_t> Aggregate(int nodes, const std::vector<int32_t>& rows, const std::vector<int32_t>& cols,
+	const std::vector<int32_t>& diag, const std::vector<double>& s, double theta, int& coarse)
+{
+	// symmetrised strength: s_ij^sym = (s_ij + s_ji)/2
+	std::vector<std::vector<int32_t>> strong(nodes);
+	for (int i = 0; i < nodes; ++i) {
+		const double sii = s[diag[i]];
+		for (int k = rows[i]; k < rows[i+1]; ++k) {
+			const int j = cols[k];
+			if (j == i) continue;
+			const auto it = std::lower_bound(cols.begin()+rows[j], cols.begin()+rows[j+1], i);
+			const double sji = (it != cols.begin()+rows[j+1] && *it == i) ? s[it-cols.begin()] : 0.0;
+			const double sij = 0.5*(s[k]+sji);
+			const double sjj = s[diag[j]];
+			if (sij >= theta*std::sqrt(sii*sjj) && sij > 0.0) strong[i].push_back(j);
+		}
+	}
+	std::vector<int32_t> agg(nodes, -1);
+	int count = 0;
+	for (int i = 0; i < nodes; ++i) {           // phase 1: whole free neighbourhoods
+		if (agg[i] >= 0 || strong[i].empty()) continue;
+		bool free_nbhd = true;
+		for (int j : strong[i]) if (agg[j] >= 0) { free_nbhd = false; break; }
+		if (!free_nbhd) continue;
+		agg[i] = count;
+		for (int j : strong[i]) agg[j] = count;
+		++count;
+	}
+	std::vector<int32_t> phase1 = agg;
+	for (int i = 0; i < nodes; ++i) {           // phase 2: join a neighbouring phase-1 aggregate
+		if (agg[i] >= 0) continue;
+		for (int j : strong[i]) if (phase1[j] >= 0) { agg[i] = phase1[j]; break; }
+	}
+	for (int i = 0; i < nodes; ++i) {           // phase 3: the rest
+		if (agg[i] >= 0) continue;
+		agg[i] = count;
+		for (int j : strong[i]) if (agg[j] < 0) agg[j] = count;
+		++count;
+	}
+	coarse = count;
+	return agg;
+}
+
+} // namespace
+
+void Amg::Build(const double* values)
+{
+	levels_.clear();
+	auto fine = std::make_unique<Level>();
+	fine->nodes = fine_.nodes;
+	fine->blocks = fine_.blocks;
+	fine->h_rows = fine_rows_;
+	fine->h_cols = fine_columns_;
+	fine->h_diag.resize(fine_.nodes);
+	for (int i = 0; i < fine_.nodes; ++i) {
+		const auto it = std::lower_bound(fine_columns_.begin()+fine_rows_[i], fine_columns_.begin()+fine_rows_[i+1], i);
+		fine->h_diag[i] = (int32_t)(it-fine_columns_.begin());
+	}
+	// strength of the fine operator
+	std::vector<double> s(fine_.blocks);
+	{
+		DeviceArray<double> ds(fine_.blocks);
+		StrengthKernel<<<Grid(fine_.blocks, 256), 256, 0, stream_>>>(fine_.blocks, values, ds.get());
+		LaunchCheck("StrengthKernel");
+		ds.Download(s.data(), s.size(), stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "AMG strength");
+	}
+	levels_.push_back(std::move(fine));
+	while ((int)levels_.size() < options_.max_levels) {
+		Level& L = *levels_.back();
+		if (L.nodes <= options_.coarsest_nodes) break;
+		int nc = 0;
+		L.h_agg = Aggregate(L.nodes, L.h_rows, L.h_cols, L.h_diag, s, options_.strength, nc);
+		if (nc >= (int)(0.9*L.nodes)) break;     // no useful coarsening
+		auto C = std::make_unique<Level>();
+		C->nodes = nc;
+		// coarse pattern and fine-block -> coarse-block map
+		std::vector<std::vector<int32_t>> crow(nc);
+		for (int i = 0; i < L.nodes; ++i)
+			for (int k = L.h_rows[i]; k < L.h_rows[i+1]; ++k) crow[L.h_agg[i]].push_back(L.h_agg[L.h_cols[k]]);
+		C->h_rows.assign(nc+1, 0);
+		for (int I = 0; I < nc; ++I) {
+			auto& r = crow[I];
+			std::sort(r.begin(), r.end());
+			r.erase(std::unique(r.begin(), r.end()), r.end());
+			C->h_rows[I+1] = C->h_rows[I]+(int32_t)r.size();
+		}
+		C->h_cols.reserve(C->h_rows[nc]);
+		C->h_diag.resize(nc);
+		for (int I = 0; I < nc; ++I) {
+			const auto it = std::lower_bound(crow[I].begin(), crow[I].end(), I);
+			C->h_diag[I] = C->h_rows[I]+(int32_t)(it-crow[I].begin());
+			C->h_cols.insert(C->h_cols.end(), crow[I].begin(), crow[I].end());
+		}
+		C->blocks = C->h_rows[nc];
+		std::vector<int32_t> target(L.blocks), block_row(L.blocks);
+		std::vector<double> cs(C->blocks, 0.0);
+		for (int i = 0; i < L.nodes; ++i) {
+			const int I = L.h_agg[i];
+			for (int k = L.h_rows[i]; k < L.h_rows[i+1]; ++k) {
+				const int J = L.h_agg[L.h_cols[k]];
+				const auto it = std::lower_bound(C->h_cols.begin()+C->h_rows[I], C->h_cols.begin()+C->h_rows[I+1], J);
+				target[k] = (int32_t)(it-C->h_cols.begin());
+				block_row[k] = i;
+				cs[target[k]] += s[k];
+			}
+		}
+		// counting sort of fine blocks by coarse block; fine nodes by aggregate
+		std::vector<int32_t> goff(C->blocks+1, 0), gorder(L.blocks);
+		for (long long k = 0; k < L.blocks; ++k) ++goff[target[k]+1];
+		for (long long B = 0; B < C->blocks; ++B) goff[B+1] += goff[B];
+		{
+			std::vector<int32_t> fill(goff.begin(), goff.end()-1);
+			for (long long k = 0; k < L.blocks; ++k) gorder[fill[target[k]]++] = (int32_t)k;
+		}
+		std::vector<int32_t> aoff(nc+1, 0), aorder(L.nodes);
+		for (int i = 0; i < L.nodes; ++i) ++aoff[L.h_agg[i]+1];
+		for (int I = 0; I < nc; ++I) aoff[I+1] += aoff[I];
+		{
+			std::vector<int32_t> fill(aoff.begin(), aoff.end()-1);
+			for (int i = 0; i < L.nodes; ++i) aorder[fill[L.h_agg[i]]++] = i;
+		}
+		auto up = [&](DeviceArray<int32_t>& d, const std::vector<int32_t>& h) { d.Allocate(h.size()); d.Upload(h.data(), h.size(), stream_); };
+		up(L.agg, L.h_agg); up(L.agg_order, aorder); up(L.agg_offsets, aoff);
+		up(L.gal_order, gorder); up(L.gal_offsets, goff); up(L.block_row, block_row);
+		s.swap(cs);
+		levels_.push_back(std::move(C));
+	}
+	// device storage per level
+	for (size_t l = 0; l < levels_.size(); ++l) {
+		Level& L = *levels_[l];
+		auto up = [&](DeviceArray<int32_t>& d, const std::vector<int32_t>& h) { d.Allocate(h.size()); d.Upload(h.data(), h.size(), stream_); };
+		up(L.rows, L.h_rows); up(L.cols, L.h_cols); up(L.diag, L.h_diag);
+		if (l > 0) L.values.Allocate((size_t)L.blocks*16);
+		L.inverse.Allocate((size_t)L.nodes*16);
+		L.singular.Allocate(1);
+		L.mask.Allocate((size_t)4*L.nodes);
+		L.x.Allocate((size_t)4*L.nodes); L.b.Allocate((size_t)4*L.nodes); L.r.Allocate((size_t)4*L.nodes);
+		if (l+1 == levels_.size() && L.nodes <= 512) {
+			L.dense_n = 4*L.nodes;
+			L.dense.Allocate((size_t)L.dense_n*2*L.dense_n);
+			L.dense_flag.Allocate(1);
+		}
+	}
+	CudaCheck(cudaStreamSynchronize(stream_), "AMG setup");
+	built_ = true;
+	masks_dirty_ = true;
+}
+
+void Amg::Refresh(const double* values)
+{
+	if (!built_) Fail(-1, "AMG hierarchy has not been built");
+	fine_values_ = values;
+	if (masks_dirty_) {
+		std::vector<double> m(4*(size_t)levels_[0]->nodes, 1.0);
+		if (!vmask_.empty())
+			for (int i = 0; i < levels_[0]->nodes; ++i) {
+				if (vmask_[i]) m[4*i] = m[4*i+1] = m[4*i+2] = 0.0;
+				if (!pmask_.empty() && pmask_[i]) m[4*i+3] = 0.0;
+			}
+		for (size_t l = 0; l < levels_.size(); ++l) {
+			Level& L = *levels_[l];
+			L.h_mask = m;
+			L.mask.Upload(m.data(), m.size(), stream_);
+			if (l+1 < levels_.size()) {
+				std::vector<double> mc(4*(size_t)levels_[l+1]->nodes, 0.0);
+				for (int i = 0; i < L.nodes; ++i)
+					for (int c = 0; c < 4; ++c)
+						if (m[4*i+c] != 0.0) mc[4*(size_t)L.h_agg[i]+c] = 1.0;
+				m.swap(mc);
+			}
+		}
+		CudaCheck(cudaStreamSynchronize(stream_), "AMG masks");
+		masks_dirty_ = false;
+	}
+	for (size_t l = 0; l+1 < levels_.size(); ++l) {
+		Level& L = *levels_[l];
+		Level& C = *levels_[l+1];
+		const double* fv = l == 0 ? values : L.values.get();
+		GalerkinKernel<<<Grid(C.blocks*16, 256), 256, 0, stream_>>>(C.blocks, L.gal_order.get(), L.gal_offsets.get(),
+			L.block_row.get(), L.cols.get(), L.mask.get(), fv, C.values.get());
+		LaunchCheck("GalerkinKernel");
+		UnitDiagonalKernel<<<Grid(4LL*C.nodes, 256), 256, 0, stream_>>>(C.nodes, C.diag.get(), C.mask.get(),
+			C.values.get());
+		LaunchCheck("UnitDiagonalKernel");
+		launches_ += 2;
+	}
+	for (size_t l = 0; l < levels_.size(); ++l) {
+		Level& L = *levels_[l];
+		if (L.dense_n > 0) continue;
+		L.singular.Zero(stream_);
+		LaunchBlockInverse(L.view(), l == 0 ? values : L.values.get(), L.inverse.get(), L.singular.get(), stream_);
+		launches_ += 1;
+	}
+	Level& Z = *levels_.back();
+	if (Z.dense_n == 0) return;
+	const double* zv = levels_.size() == 1 ? values : Z.values.get();
+	Z.dense.Zero(stream_);
+	Z.dense_flag.Zero(stream_);
+	DenseScatterKernel<<<Grid(Z.blocks*16, 256), 256, 0, stream_>>>(Z.view(), zv, Z.dense_n, Z.dense.get());
+	LaunchCheck("DenseScatterKernel");
+	DenseInverseKernel<<<1, 1024, 0, stream_>>>(Z.dense_n, Z.dense.get(), Z.dense_flag.get());
+	LaunchCheck("DenseInverseKernel");
+	launches_ += 2;
+}
+
+void Amg::Cycle(int l, const double* b, double* x, const int* stop)
+{
+	Level& L = *levels_[l];
+	if (l+1 == (int)levels_.size() && L.dense_n == 0) {
+		// coarsening stalled above the dense limit: damped block-Jacobi sweeps
+		const double* A = l == 0 ? fine_values_ : L.values.get();
+		const long long n4 = 4LL*L.nodes;
+		JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), b, x, options_.omega, 0, stop);
+		for (int s = 1; s < 4; ++s) {
+			ResidualKernel<<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
+			JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), L.r.get(), x, options_.omega, 1, stop);
+		}
+		LaunchCheck("coarsest JacobiKernel");
+		launches_ += 7;
+		return;
+	}
+	if (l+1 == (int)levels_.size()) {
+		DenseApplyKernel<<<Grid(L.dense_n, 8), 256, 0, stream_>>>(L.dense_n, L.dense.get(), b, x, stop);
+		LaunchCheck("DenseApplyKernel");
+		launches_ += 1;
+		return;
+	}
+	Level& C = *levels_[l+1];
+	const double* A = l == 0 ? fine_values_ : L.values.get();
+	const long long n4 = 4LL*L.nodes;
+	const double omega = options_.omega;
+	JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), b, x, omega, 0, stop);
+	LaunchCheck("JacobiKernel");
+	launches_ += 1;
+	for (int s = 1; s < options_.pre_sweeps; ++s) {
+		ResidualKernel<<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
+		JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), L.r.get(), x, omega, 1, stop);
+		launches_ += 2;
+	}
+	ResidualKernel<<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
+	LaunchCheck("ResidualKernel");
+	RestrictKernel<<<Grid(4LL*C.nodes, 256), 256, 0, stream_>>>(C.nodes, L.agg_order.get(), L.agg_offsets.get(),
+		L.mask.get(), L.r.get(), C.b.get(), stop);
+	LaunchCheck("RestrictKernel");
+	launches_ += 2;
+	Cycle(l+1, C.b.get(), C.x.get(), stop);
+	ProlongKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(), C.x.get(), x, stop);
+	LaunchCheck("ProlongKernel");
+	launches_ += 1;
+	for (int s = 0; s < options_.post_sweeps; ++s) {
+		ResidualKernel<<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
+		JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), L.r.get(), x, omega, 1, stop);
+		LaunchCheck("JacobiKernel");
+		launches_ += 2;
+	}
+}
+
+void Amg::Apply(const double* fine_values, const double* v, double* z, const int* stop)
+{
+	fine_values_ = fine_values;
+	if (profiler_) profiler_->Begin(Profiler::kOther, stream_);
+	Cycle(0, v, z, stop);
+	if (profiler_) profiler_->End(stream_);
+}
+
+} // namespace tfiga

@@ -162,6 +162,7 @@ void tfiga_ns_default_params(tfiga_ns_params* p)
 	p->gmres_restart = 200;
 	p->gmres_max_iterations = 5000;
 	p->gmres_rtol = 1e-8;
+	p->preconditioner = TFIGA_PRECONDITIONER_BLOCK_JACOBI;
 }
 
 int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out)
@@ -291,6 +292,20 @@ int tfiga_ns_step(tfiga_ns* ns, tfiga_step_report* report)
 	return Guard([&] {
 		Require(ns && report, "null argument");
 		*report = ns->solver->Step();
+	});
+}
+
+int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info)
+{
+	return Guard([&] {
+		Require(ns && info, "null argument");
+		*info = tfiga_amg_info{};
+		const auto* amg = ns->solver->amg();
+		if (!amg || !amg->built()) return;
+		const auto nodes = amg->level_nodes();
+		const auto blocks = amg->level_blocks();
+		info->levels = (int32_t)std::min<size_t>(8, nodes.size());
+		for (int l = 0; l < info->levels; ++l) { info->nodes[l] = nodes[l]; info->blocks[l] = blocks[l]; }
 	});
 }
 

@@ -1,0 +1,389 @@
+// Case input and host boundary physics (see case_input.hpp).
+#include "case_input.hpp"
+#include "json.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+
+namespace tfiga {
+
+namespace {
+
+std::string ReadText(const std::string& path)
+{
+	std::ifstream in(path);
+	if (!in) Fail(-3, "cannot open "+path);
+	std::stringstream ss;
+	ss << in.rdbuf();
+	return ss.str();
+}
+
+double OptionalNumber(const json::Value& object, const char* key, double fallback, const std::string& context)
+{
+	const auto* v = object.Find(key);
+	return v ? v->Number(context+"."+key) : fallback;
+}
+
+std::vector<double> Numbers(const json::Value& v, const std::string& context)
+{
+	if (v.kind == json::Value::Kind::Number) return {v.number};
+	std::vector<double> out;
+	for (const auto& item : v.Array(context)) out.push_back(item.Number(context));
+	return out;
+}
+
+} // namespace
+
+SimulationConfig ReadSimulationConfig(const std::string& path)
+{
+	const json::Value root = json::Parse(ReadText(path));
+	if (!root.IsObject()) Fail(-4, "simulation_config.json root must be an object");
+	SimulationConfig config;
+	const auto& time = root.At("time", "root");
+	config.dt = time.At("dt", "time").Number("time.dt");
+	config.steps = time.At("steps", "time").Integer("time.steps");
+	if (const auto* temporal = root.Find("temporal_functions")) {
+		for (const auto& item : temporal->Array("temporal_functions")) {
+			TemporalFunction f;
+			f.name = item.At("name", "temporal function").String("temporal function.name");
+			f.kind = item.At("kind", "temporal function").String("temporal function.kind");
+			f.value = OptionalNumber(item, "value", 0.0, "temporal function");
+			f.mean = OptionalNumber(item, "mean", 0.0, "temporal function");
+			f.amplitude = OptionalNumber(item, "amplitude", 0.0, "temporal function");
+			f.period = OptionalNumber(item, "period", 0.0, "temporal function");
+			f.phase = OptionalNumber(item, "phase", 0.0, "temporal function");
+			if (const auto* c = item.Find("cosine")) f.cosine = Numbers(*c, "temporal function.cosine");
+			if (const auto* s = item.Find("sine")) f.sine = Numbers(*s, "temporal function.sine");
+			if (const auto* file = item.Find("file")) f.file = file->String("temporal function.file");
+			if (f.kind != "constant" && f.kind != "sinusoid" && f.kind != "fourier" && f.kind != "periodic_table")
+				Fail(-4, "unknown temporal function kind '"+f.kind+"'");
+			if (f.kind != "constant" && !(f.period > 0.0))
+				Fail(-4, "temporal function '"+f.name+"' needs a positive period");
+			if (f.cosine.size() != f.sine.size())
+				Fail(-4, "fourier cosine and sine arrays must have the same length");
+			config.temporal.push_back(f);
+		}
+	}
+	for (const auto& item : root.At("equation_systems", "root").Array("equation_systems")) {
+		FlowSystem s;
+		s.name = item.At("name", "equation system").String("equation system.name");
+		s.kind = item.At("kind", "equation system").String("equation system.kind");
+		if (const auto* unknowns = item.Find("unknowns"))
+			for (const auto& u : unknowns->Array("unknowns")) s.unknowns.push_back(u.String("unknown"));
+		s.viscosity = OptionalNumber(item, "viscosity", 0.0, "equation system");
+		s.density = OptionalNumber(item, "density", 1.0, "equation system");
+		if (const auto* ti = item.Find("time_integration")) s.time_integration = ti->String("time_integration");
+		if (s.kind == "navier_stokes" && s.time_integration != "steady" && s.time_integration != "backward_euler")
+			Fail(-4, "navier_stokes time_integration must be steady or backward_euler");
+		config.systems.push_back(s);
+	}
+	for (const auto& item : root.At("boundaries", "root").Array("boundaries")) {
+		Boundary b;
+		b.label = item.At("label", "boundary").Integer("boundary.label");
+		if (const auto* name = item.Find("name")) b.name = name->String("boundary.name");
+		for (const auto& c : item.At("conditions", "boundary").Array("boundary.conditions")) {
+			Condition k;
+			const std::string ctx = "boundary "+std::to_string(b.label)+" condition";
+			k.field = c.At("field", ctx).String(ctx+".field");
+			k.type = c.At("type", ctx).String(ctx+".type");
+			if (const auto* v = c.Find("value")) k.value = Numbers(*v, ctx+".value");
+			if (const auto* p = c.Find("profile")) k.profile = p->String(ctx+".profile");
+			k.scale = OptionalNumber(c, "scale", 1.0, ctx);
+			if (const auto* w = c.Find("waveform")) k.waveform = w->String(ctx+".waveform");
+			k.resistance = OptionalNumber(c, "resistance", 0.0, ctx);
+			k.proximal_resistance = OptionalNumber(c, "proximal_resistance", 0.0, ctx);
+			k.distal_resistance = OptionalNumber(c, "distal_resistance", 0.0, ctx);
+			k.capacitance = OptionalNumber(c, "capacitance", 0.0, ctx);
+			k.reference_pressure = OptionalNumber(c, "reference_pressure", 0.0, ctx);
+			k.initial_pressure = OptionalNumber(c, "initial_pressure", 0.0, ctx);
+			if (const auto* g = c.Find("pressure_gauge")) k.pressure_gauge = g->kind == json::Value::Kind::Bool && g->boolean;
+			b.conditions.push_back(k);
+		}
+		config.boundaries.push_back(b);
+	}
+	return config;
+}
+
+const FlowSystem& FindNavierStokesSystem(const SimulationConfig& config, const std::string& name)
+{
+	for (const auto& s : config.systems) {
+		if (name.empty() && s.kind == "navier_stokes") return s;
+		if (!name.empty() && s.name == name) {
+			if (s.kind != "navier_stokes") Fail(-4, "equation system '"+name+"' is not navier_stokes");
+			return s;
+		}
+	}
+	if (name.empty()) Fail(-4, "simulation configuration has no navier_stokes equation system");
+	Fail(-4, "simulation configuration has no navier_stokes system named '"+name+"'");
+}
+
+double EvaluateTemporal(const TemporalFunction& f, double time)
+{
+	const double pi = 3.141592653589793238462643383279502884;
+	if (f.kind == "constant") return f.value;
+	double wrapped = std::fmod(time, f.period);
+	if (wrapped < 0.0) wrapped += f.period;
+	const double theta = 2.0*pi*wrapped/f.period+f.phase;
+	if (f.kind == "sinusoid") return f.mean+f.amplitude*std::sin(theta);
+	if (f.kind == "fourier") {
+		double v = f.mean;
+		for (size_t h = 0; h < f.cosine.size(); ++h) {
+			const double angle = (double)(h+1)*theta;
+			v += f.cosine[h]*std::cos(angle)+f.sine[h]*std::sin(angle);
+		}
+		return v;
+	}
+	Fail(-7, "periodic_table waveforms are not supported by this build");
+}
+
+SimulationConfig MaterializeWaveforms(const SimulationConfig& config, double time)
+{
+	SimulationConfig out = config;
+	for (auto& b : out.boundaries)
+		for (auto& c : b.conditions) {
+			if (c.waveform.empty()) continue;
+			const auto it = std::find_if(config.temporal.begin(), config.temporal.end(),
+				[&](const TemporalFunction& f) { return f.name == c.waveform; });
+			if (it == config.temporal.end()) Fail(-4, "unknown temporal function '"+c.waveform+"'");
+			const double factor = EvaluateTemporal(*it, time);
+			if (c.profile.empty()) for (double& v : c.value) v *= factor;
+			else c.scale *= factor;
+			c.waveform.clear();
+		}
+	return out;
+}
+
+LabeledHexMesh ReadLabeledHexMesh(const std::string& path, int64_t nodes, int64_t elements)
+{
+	std::ifstream in(path);
+	if (!in) Fail(-3, "cannot open mesh: "+path);
+	std::string token;
+	int64_t points = 0;
+	while (in >> token) if (token == "POINTS") {
+		std::string type;
+		if (!(in >> points >> type)) Fail(-4, "invalid POINTS record");
+		break;
+	}
+	if (points != nodes) Fail(-4, "VTK point count does not match database nodes");
+	for (int64_t k = 0; k < 3*points; ++k) {
+		double ignored;
+		if (!(in >> ignored)) Fail(-4, "VTK POINTS record is truncated");
+	}
+	int64_t cells = 0, values = 0;
+	while (in >> token) if (token == "CELLS") {
+		if (!(in >> cells >> values)) Fail(-4, "invalid CELLS record");
+		break;
+	}
+	if (cells != elements) Fail(-4, "VTK cell count does not match database elements");
+	LabeledHexMesh mesh;
+	mesh.cells.resize(cells);
+	for (auto& cell : mesh.cells) {
+		int count = 0;
+		if (!(in >> count) || count != 8) Fail(-4, "only eight-node VTK hexahedra are supported");
+		for (auto& node : cell)
+			if (!(in >> node) || node < 0 || node >= points) Fail(-4, "invalid hexahedron connectivity");
+	}
+	int64_t point_data = 0;
+	while (in >> token) if (token == "POINT_DATA") {
+		if (!(in >> point_data)) Fail(-4, "invalid POINT_DATA record");
+		break;
+	}
+	if (point_data != points) Fail(-4, "VTK POINT_DATA count does not match database nodes");
+	while (in >> token) if (token == "LOOKUP_TABLE") { in >> token; break; }
+	if (!in) Fail(-4, "VTK point labels were not found");
+	mesh.labels.resize(points);
+	for (auto& label : mesh.labels) {
+		double v = 0.0;
+		if (!(in >> v)) Fail(-4, "VTK point-label array is truncated");
+		label = (int)v;
+		if (v != (double)label) Fail(-4, "VTK point label is not integral");
+	}
+	return mesh;
+}
+
+std::vector<std::array<double, 3>> ReadVelocity(const std::string& path, int64_t nodes)
+{
+	std::ifstream in(path);
+	if (!in) Fail(-3, "cannot open velocity field: "+path);
+	std::vector<std::array<double, 3>> v(nodes);
+	for (auto& x : v)
+		if (!(in >> x[0] >> x[1] >> x[2])) Fail(-4, "velocity field is truncated");
+	std::string extra;
+	if (in >> extra) Fail(-4, "velocity field contains extra records");
+	return v;
+}
+
+std::set<int32_t> WallTraceBasis(const HostMesh& mesh, const LabeledHexMesh& labeled)
+{
+	// External faces of the control hex mesh (faces used once), with the local
+	// face numbering of the element faces (BoundarySupport.hpp:84-87).
+	static const int corners[6][4] = {{0, 3, 2, 1}, {0, 1, 5, 4}, {1, 2, 6, 5},
+		{2, 3, 7, 6}, {0, 4, 7, 3}, {4, 5, 6, 7}};
+	std::map<std::array<int32_t, 4>, std::array<int64_t, 3>> faces;   // key -> {element, face, uses}
+	for (int64_t e = 0; e < (int64_t)labeled.cells.size(); ++e)
+		for (int f = 0; f < 6; ++f) {
+			std::array<int32_t, 4> key;
+			for (int c = 0; c < 4; ++c) key[c] = labeled.cells[e][corners[f][c]];
+			std::sort(key.begin(), key.end());
+			auto& entry = faces[key];
+			if (entry[2] == 0) { entry[0] = e; entry[1] = f; }
+			if (++entry[2] > 2) Fail(-4, "non-manifold control-mesh face");
+		}
+	std::set<int32_t> result;
+	for (const auto& item : faces) {
+		if (item.second[2] != 1) continue;
+		const int64_t e = item.second[0];
+		const int f = (int)item.second[1];
+		bool wall = true;
+		for (int c = 0; c < 4 && wall; ++c) wall = labeled.labels.at(labeled.cells[e][corners[f][c]]) == 0;
+		if (!wall) continue;
+		// Bezier columns on the face (FaceBezierColumns, :117-132).
+		std::vector<int> columns;
+		for (int k = 0; k < 4; ++k)
+			for (int j = 0; j < 4; ++j)
+				for (int i = 0; i < 4; ++i)
+					if ((f == 0 && k == 0) || (f == 1 && j == 0) || (f == 2 && i == 3) || (f == 3 && j == 3)
+						|| (f == 4 && i == 0) || (f == 5 && k == 3))
+						columns.push_back(i+4*j+16*k);
+		for (int32_t a = mesh.element_offsets[e]; a < mesh.element_offsets[e+1]; ++a)
+			for (int32_t k = mesh.extraction_offsets[a]; k < mesh.extraction_offsets[a+1]; ++k)
+				if (mesh.extraction_values[k] != 0.0
+					&& std::find(columns.begin(), columns.end(), (int)mesh.extraction_columns[k]) != columns.end()) {
+					result.insert(mesh.connectivity[a]);
+					break;
+				}
+	}
+	return result;
+}
+
+ResolvedBoundaries ResolveFlowBoundaries(const SimulationConfig& config, const FlowSystem& system,
+	const std::vector<int>& labels, const std::vector<std::array<double, 3>>& reference_velocity)
+{
+	if (system.unknowns.size() != 2) Fail(-4, "navier_stokes requires [velocity, pressure] unknowns");
+	const auto& vname = system.unknowns[0];
+	const auto& pname = system.unknowns[1];
+	const size_t n = labels.size();
+	if (reference_velocity.size() != n) Fail(-4, "velocity profile and boundary labels have different node counts");
+	ResolvedBoundaries r;
+	r.velocity_mask.assign(n, 0);
+	r.pressure_mask.assign(n, 0);
+	r.velocity.assign(3*n, 0.0);
+	r.pressure.assign(n, 0.0);
+	std::set<int> mesh_labels, configured;
+	for (int l : labels) if (l >= 0) mesh_labels.insert(l);
+	bool traction = false;
+	for (const auto& b : config.boundaries) {
+		if (!mesh_labels.count(b.label))
+			Fail(-4, "simulation_config.json boundary label "+std::to_string(b.label)
+				+" is not present in controlmesh.vtk");
+		configured.insert(b.label);
+		for (const auto& c : b.conditions) {
+			if (c.field != vname && c.field != pname) continue;
+			if (!c.waveform.empty()) Fail(-7, "time-dependent Navier-Stokes boundary execution is not implemented");
+			if (c.type == "pressure_traction") {
+				if (c.field != pname || c.value.size() != 1)
+					Fail(-4, "pressure_traction requires the Navier-Stokes pressure field");
+				if (c.pressure_gauge)
+					Fail(-4, "pressure_traction already fixes the pressure reference; remove pressure_gauge "
+						"to preserve every continuity equation");
+				traction = true;
+				continue;
+			}
+			if (c.type != "dirichlet")
+				Fail(-4, "navier_stokes boundary field '"+c.field+"' currently supports only dirichlet conditions");
+			if (c.field == vname) {
+				if (c.profile.empty() && c.value.size() != 3)
+					Fail(-4, "velocity Dirichlet condition requires three values or a profile");
+				if (!c.profile.empty() && c.profile != "initial_velocityfield.txt")
+					Fail(-4, "unsupported velocity profile '"+c.profile+"'");
+				for (size_t i = 0; i < n; ++i)
+					if (labels[i] == b.label) {
+						r.velocity_mask[i] = 1;
+						for (int d = 0; d < 3; ++d)
+							r.velocity[3*i+d] = c.profile.empty() ? c.value[d] : c.scale*reference_velocity[i][d];
+					}
+			} else {
+				if (c.value.size() != 1) Fail(-4, "pressure Dirichlet condition requires one value");
+				for (size_t i = 0; i < n; ++i)
+					if (labels[i] == b.label) { r.pressure_mask[i] = 1; r.pressure[i] = c.value[0]; }
+			}
+		}
+	}
+	for (int l : mesh_labels)
+		if (!configured.count(l))
+			Fail(-4, "mesh boundary label "+std::to_string(l)+" has no simulation_config.json boundary definition");
+	r.velocity_nodes = (size_t)std::count(r.velocity_mask.begin(), r.velocity_mask.end(), 1);
+	r.pressure_nodes = (size_t)std::count(r.pressure_mask.begin(), r.pressure_mask.end(), 1);
+	if (r.velocity_nodes == 0 || (r.pressure_nodes == 0 && !traction))
+		Fail(-4, "navier_stokes requires velocity Dirichlet and pressure gauge/traction boundaries");
+	return r;
+}
+
+std::map<int, double> ExtractPressureTractions(const SimulationConfig& config, const FlowSystem& system)
+{
+	const auto& pname = system.unknowns.at(1);
+	std::map<int, double> out;
+	for (const auto& b : config.boundaries)
+		for (const auto& c : b.conditions) {
+			if (c.type != "pressure_traction") continue;
+			if (c.field != pname || c.value.size() != 1)
+				Fail(-4, "pressure_traction must provide one value for the pressure field");
+			if (!out.emplace(b.label, c.value[0]).second) Fail(-4, "duplicate pressure traction boundary label");
+		}
+	return out;
+}
+
+std::vector<OutletModel> InitializeOutletModels(const SimulationConfig& config, const FlowSystem& system)
+{
+	const auto& pname = system.unknowns.at(1);
+	std::vector<OutletModel> models;
+	for (const auto& b : config.boundaries)
+		for (const auto& c : b.conditions) {
+			if (c.field != pname || (c.type != "resistance" && c.type != "windkessel_rc" && c.type != "windkessel_rcr"))
+				continue;
+			OutletModel m;
+			m.label = b.label;
+			m.kind = c.type;
+			m.resistance = c.resistance;
+			m.proximal = c.proximal_resistance;
+			m.distal = c.distal_resistance;
+			m.capacitance = c.capacitance;
+			m.reference_pressure = c.reference_pressure;
+			m.capacitor_pressure = c.initial_pressure;
+			m.pressure = c.type == "resistance" ? c.reference_pressure : c.initial_pressure;
+			models.push_back(m);
+		}
+	return models;
+}
+
+std::array<double, 2> EvaluateOutletModel(const OutletModel& m, double flow, double dt)
+{
+	if (!std::isfinite(flow)) Fail(-6, "outlet flow must be finite");
+	if (m.kind == "resistance") return {m.reference_pressure+m.resistance*flow, m.capacitor_pressure};
+	if (!(dt > 0.0)) Fail(-4, "RC/RCR outlets require positive transient dt");
+	const double r = m.kind == "windkessel_rc" ? m.resistance : m.distal;
+	const double pc = (m.capacitance*m.capacitor_pressure/dt+flow+m.reference_pressure/r)/(m.capacitance/dt+1.0/r);
+	return {pc+(m.kind == "windkessel_rcr" ? m.proximal*flow : 0.0), pc};
+}
+
+SimulationConfig MaterializeOutletPressures(const SimulationConfig& config, const std::vector<OutletModel>& models)
+{
+	SimulationConfig out = config;
+	std::map<int, double> pressures;
+	for (const auto& m : models) pressures.emplace(m.label, m.pressure);
+	for (auto& b : out.boundaries) {
+		const auto it = pressures.find(b.label);
+		if (it == pressures.end()) continue;
+		for (auto& c : b.conditions)
+			if (c.type == "resistance" || c.type == "windkessel_rc" || c.type == "windkessel_rcr") {
+				c.type = "pressure_traction";
+				c.value = {it->second};
+			}
+	}
+	return out;
+}
+
+} // namespace tfiga

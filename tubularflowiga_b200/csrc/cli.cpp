@@ -1,25 +1,39 @@
-// The drop-in command (tfiga_main): device-info and mesh-check
-// (solvers/cuda/src/iga_cuda.cu:278-303, 604-617, 1157-1195).
+// The drop-in command (tfiga_main): device-info, mesh-check and navier-stokes
+// with the reference's arguments, log lines, outputs and exit codes
+// (solvers/cuda/src/iga_cuda.cu:278-303, 389-498, 566-617, 734-1195).
+#include "case_input.hpp"
+#include "json.hpp"
 #include "mesh.hpp"
+#include "ns.hpp"
 
 #include "../../include/tfiga.h"
 
+#include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <exception>
+#include <filesystem>
+#include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <sstream>
 #include <string>
 
+namespace fs = std::filesystem;
+
+namespace tfiga {
 namespace {
+
+using Clock = std::chrono::steady_clock;
 
 void PrintDevice()
 {
 	int device = 0;
-	tfiga::CudaCheck(cudaGetDevice(&device), "cudaGetDevice");
+	CudaCheck(cudaGetDevice(&device), "cudaGetDevice");
 	cudaDeviceProp prop{};
-	tfiga::CudaCheck(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+	CudaCheck(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
 	size_t free_bytes = 0, total = 0;
-	tfiga::CudaCheck(cudaMemGetInfo(&free_bytes, &total), "cudaMemGetInfo");
+	CudaCheck(cudaMemGetInfo(&free_bytes, &total), "cudaMemGetInfo");
 	int runtime = 0, driver = 0;
 	cudaRuntimeGetVersion(&runtime);
 	cudaDriverGetVersion(&driver);
@@ -27,39 +41,447 @@ void PrintDevice()
 		<< prop.minor << " sms=" << prop.multiProcessorCount
 		<< " memory_free_gib=" << free_bytes/1073741824.0 << " memory_total_gib=" << total/1073741824.0 << '\n';
 	std::cout << "cuda_capabilities runtime_build=" << CUDART_VERSION << " runtime_linked=" << runtime
-		<< " driver=" << driver << " arch=sm_100a\n";
+		<< " driver=" << driver << " arch=sm_100a precision=fp64\n";
 }
 
-int MeshCheck(const std::string& path)
+void PrintMesh(const Mesh& mesh)
 {
-	tfiga::Mesh mesh(tfiga::ReadNtiga(path));
 	const auto& h = mesh.host();
 	std::cout << "mesh nodes=" << h.nodes << " elements=" << h.elements() << " basis_entries=" << h.connectivity.size()
 		<< " extraction_nonzeros=" << h.extraction_values.size() << " max_basis=" << h.max_basis
 		<< " block_nonzeros=" << mesh.pattern().columns.size()
 		<< " mean_block_row=" << (double)mesh.pattern().columns.size()/h.nodes << '\n';
+}
+
+int MeshCheck(const std::string& path)
+{
+	Mesh mesh(ReadNtiga(path));
+	PrintMesh(mesh);
 	std::cout << "geometry min_detJ=" << std::setprecision(17) << mesh.min_detj() << " bad_samples="
 		<< mesh.bad_samples() << " device_mesh_gib=" << mesh.device_bytes()/1073741824.0 << '\n';
 	return mesh.bad_samples() ? 1 : 0;
 }
 
+struct Options {
+	std::string database, case_dir, system;
+	int max_newton = 12;
+	double rtol = 1e-5, atol = 1e-10, mass_rtol = 1e-3;
+	std::string output, checkpoint, restart;
+	int output_every = 0, checkpoint_every = 0, stop_after_step = 0;
+	std::string visualization = "auto";
+};
+
+int PositiveInt(const std::string& text, const std::string& option)
+{
+	size_t used = 0;
+	int v = 0;
+	try { v = std::stoi(text, &used); } catch (const std::exception&) { Fail(-1, option+" requires a positive integer"); }
+	if (used != text.size() || v <= 0) Fail(-1, option+" requires a positive integer");
+	return v;
+}
+
+double PositiveDouble(const std::string& text, const std::string& option)
+{
+	size_t used = 0;
+	double v = 0.0;
+	try { v = std::stod(text, &used); } catch (const std::exception&) { Fail(-1, option+" requires a finite positive value"); }
+	if (used != text.size() || !std::isfinite(v) || v <= 0.0) Fail(-1, option+" requires a finite positive value");
+	return v;
+}
+
+// ParseCudaFlowOptions (iga_cuda.cu:447-498).
+Options ParseOptions(int argc, char** argv)
+{
+	if (argc < 4) Fail(-1, "usage: iga_cuda navier-stokes DATABASE.ntiga CASE_DIR [MAX_NEWTON] [OUTPUT] "
+		"[--system NAME] [--max-newton N] [--output PATH] [--output-every N] [--checkpoint PREFIX] "
+		"[--checkpoint-every N] [--restart PREFIX] [--stop-after-step N] [--nonlinear-rtol R] "
+		"[--nonlinear-atol A] [--mass-rtol R] [--visualization-format auto|vtu|vtkhdf]");
+	Options o;
+	o.database = argv[2];
+	o.case_dir = argv[3];
+	int positional = 0;
+	for (int i = 4; i < argc; ++i) {
+		const std::string arg(argv[i]);
+		if (arg.rfind("--", 0) != 0) {
+			if (positional == 0) o.max_newton = PositiveInt(arg, "MAX_NEWTON");
+			else if (positional == 1) o.output = arg;
+			else Fail(-1, "too many positional arguments");
+			++positional;
+			continue;
+		}
+		if (i+1 >= argc) Fail(-1, arg+" requires a value");
+		const std::string v(argv[++i]);
+		if (arg == "--system") o.system = v;
+		else if (arg == "--max-newton") o.max_newton = PositiveInt(v, arg);
+		else if (arg == "--output") o.output = v;
+		else if (arg == "--output-every") o.output_every = PositiveInt(v, arg);
+		else if (arg == "--checkpoint") o.checkpoint = v;
+		else if (arg == "--checkpoint-every") o.checkpoint_every = PositiveInt(v, arg);
+		else if (arg == "--restart") o.restart = v;
+		else if (arg == "--stop-after-step") o.stop_after_step = PositiveInt(v, arg);
+		else if (arg == "--nonlinear-rtol") o.rtol = PositiveDouble(v, arg);
+		else if (arg == "--nonlinear-atol") o.atol = PositiveDouble(v, arg);
+		else if (arg == "--mass-rtol") o.mass_rtol = PositiveDouble(v, arg);
+		else if (arg == "--visualization-format") {
+			if (v != "auto" && v != "vtu" && v != "vtkhdf") Fail(-1, "unknown visualization format: "+v);
+			o.visualization = v;
+		} else Fail(-1, "unknown option: "+arg);
+	}
+	if (o.output_every > 0 && o.output.empty()) Fail(-1, "--output-every requires --output or legacy OUTPUT");
+	if (o.checkpoint_every > 0 && o.checkpoint.empty()) Fail(-1, "--checkpoint-every requires --checkpoint");
+	return o;
+}
+
+std::string Precise(double v)
+{
+	std::ostringstream s;
+	s << std::scientific << std::setprecision(16) << v;
+	return s.str();
+}
+
+// TimeIndexedPath (include/FlowCheckpoint.hpp).
+fs::path TimeIndexed(const fs::path& base, int step)
+{
+	std::ostringstream suffix;
+	suffix << ".step" << std::setw(6) << std::setfill('0') << step;
+	const auto ext = base.extension().string();
+	if (ext.empty()) return base.string()+suffix.str();
+	return base.parent_path()/(base.stem().string()+suffix.str()+ext);
+}
+
+// WriteNavierStokes (iga_cuda.cu:389-400): "u v w" rows and <out>.pressure rows.
+void WriteText(const fs::path& path, const std::vector<double>& state)
+{
+	std::ofstream velocity(path), pressure(path.string()+".pressure");
+	if (!velocity || !pressure) Fail(-3, "cannot create Navier-Stokes output");
+	velocity << std::setprecision(17);
+	pressure << std::setprecision(17);
+	for (size_t node = 0; node < state.size()/4; ++node) {
+		velocity << state[4*node] << ' ' << state[4*node+1] << ' ' << state[4*node+2] << '\n';
+		pressure << state[4*node+3] << '\n';
+	}
+}
+
+// WriteNavierStokesVtk (iga_cuda.cu:351-364): control mesh + velocity/pressure point data.
+void WriteVtk(const fs::path& mesh_path, const fs::path& path, const std::vector<double>& state)
+{
+	std::ifstream mesh(mesh_path);
+	std::ofstream out(path);
+	if (!mesh) Fail(-3, "cannot open VTK mesh "+mesh_path.string());
+	if (!out) Fail(-3, "cannot create "+path.string());
+	out << mesh.rdbuf() << "\nVECTORS Velocity double\n" << std::setprecision(17);
+	for (size_t node = 0; node < state.size()/4; ++node)
+		out << state[4*node] << ' ' << state[4*node+1] << ' ' << state[4*node+2] << '\n';
+	out << "SCALARS Pressure double 1\nLOOKUP_TABLE default\n";
+	for (size_t node = 0; node < state.size()/4; ++node) out << state[4*node+3] << '\n';
+}
+
+// Flow checkpoint: raw float64 state + JSON metadata (FlowCheckpoint.hpp, iga_cuda.cu:566-602).
+void WriteCheckpoint(const fs::path& prefix, int64_t nodes, int completed, double time, double dt, double density,
+	double viscosity, const std::vector<OutletModel>& outlets, const std::vector<double>& state)
+{
+	const fs::path state_path = prefix.string()+".state";
+	{
+		std::ofstream out(state_path, std::ios::binary);
+		if (!out) Fail(-3, "cannot create CUDA flow checkpoint state: "+state_path.string());
+		out.write(reinterpret_cast<const char*>(state.data()), (std::streamsize)(state.size()*sizeof(double)));
+		if (!out) Fail(-3, "cannot write CUDA flow checkpoint state: "+state_path.string());
+	}
+	std::ofstream meta(prefix.string()+".json");
+	if (!meta) Fail(-3, "cannot create checkpoint metadata");
+	meta << std::setprecision(17) << "{\n  \"schema_version\": 1,\n  \"nodes\": " << nodes << ",\n  \"fields\": 4,\n"
+		<< "  \"completed_step\": " << completed << ",\n  \"physical_time\": " << time << ",\n  \"dt\": " << dt
+		<< ",\n  \"density\": " << density << ",\n  \"viscosity\": " << viscosity << ",\n  \"state_file\": \""
+		<< state_path.filename().string() << "\",\n  \"state_format\": \"raw_float64\",\n  \"outlets\": [";
+	for (size_t i = 0; i < outlets.size(); ++i)
+		meta << (i == 0 ? "\n" : ",\n") << "    {\"label\": " << outlets[i].label << ", \"kind\": \"" << outlets[i].kind
+			<< "\", \"flow\": " << outlets[i].flow << ", \"pressure\": " << outlets[i].pressure
+			<< ", \"capacitor_pressure\": " << outlets[i].capacitor_pressure << "}";
+	if (!outlets.empty()) meta << '\n';
+	meta << "  ]\n}\n";
+}
+
+struct Restart {
+	int completed = 0;
+	double time = 0.0;
+	std::vector<double> state;
+};
+
+Restart ReadCheckpoint(const fs::path& prefix, int64_t nodes, double dt, double density, double viscosity,
+	std::vector<OutletModel>& outlets)
+{
+	std::ifstream in(prefix.string()+".json");
+	if (!in) Fail(-3, "cannot open flow checkpoint metadata: "+prefix.string()+".json");
+	std::stringstream ss;
+	ss << in.rdbuf();
+	const auto root = json::Parse(ss.str());
+	if (root.At("state_format", "flow checkpoint").String("state_format") != "raw_float64")
+		Fail(-4, "CUDA flow restart requires raw_float64 checkpoint state");
+	if ((int64_t)root.At("nodes", "flow checkpoint").Number("nodes") != nodes)
+		Fail(-4, "flow checkpoint node count does not match the database");
+	if (root.At("fields", "flow checkpoint").Integer("fields") != 4) Fail(-4, "flow checkpoint must have 4 fields");
+	auto same = [](double a, double b) { return std::fabs(a-b) <= 1e-12*std::max(1.0, std::max(std::fabs(a), std::fabs(b))); };
+	if (!same(root.At("dt", "flow checkpoint").Number("dt"), dt)
+		|| !same(root.At("density", "flow checkpoint").Number("density"), density)
+		|| !same(root.At("viscosity", "flow checkpoint").Number("viscosity"), viscosity))
+		Fail(-4, "flow checkpoint dt, density or viscosity does not match the case");
+	Restart r;
+	r.completed = root.At("completed_step", "flow checkpoint").Integer("completed_step");
+	r.time = root.At("physical_time", "flow checkpoint").Number("physical_time");
+	if (const auto* list = root.Find("outlets"))
+		for (const auto& item : list->Array("outlets")) {
+			const int label = item.At("label", "outlet").Integer("outlet.label");
+			for (auto& m : outlets)
+				if (m.label == label) {
+					m.flow = item.At("flow", "outlet").Number("outlet.flow");
+					m.pressure = item.At("pressure", "outlet").Number("outlet.pressure");
+					m.capacitor_pressure = item.At("capacitor_pressure", "outlet").Number("outlet.capacitor_pressure");
+				}
+		}
+	fs::path state_path(root.At("state_file", "flow checkpoint").String("state_file"));
+	if (state_path.is_relative()) state_path = fs::path(prefix.string()+".json").parent_path()/state_path;
+	std::ifstream sin(state_path, std::ios::binary);
+	if (!sin) Fail(-3, "cannot open CUDA flow checkpoint state: "+state_path.string());
+	r.state.resize((size_t)nodes*4);
+	sin.read(reinterpret_cast<char*>(r.state.data()), (std::streamsize)(r.state.size()*sizeof(double)));
+	char extra = 0;
+	if (!sin || sin.read(&extra, 1)) Fail(-4, "CUDA flow checkpoint state is truncated or has trailing data");
+	return r;
+}
+
+int NavierStokes(int argc, char** argv)
+{
+	const Options options = ParseOptions(argc, argv);
+	const auto total_start = Clock::now();
+	const fs::path case_dir(options.case_dir);
+	HostMesh host = ReadNtiga(options.database);
+	const auto labeled = ReadLabeledHexMesh((case_dir/"controlmesh.vtk").string(), host.nodes, host.elements());
+	const auto wall = WallTraceBasis(host, labeled);
+	const auto reference_velocity = ReadVelocity((case_dir/"initial_velocityfield.txt").string(), host.nodes);
+	if (!fs::exists(case_dir/"simulation_config.json"))
+		Fail(-7, "legacy simulation_parameter.txt / case_config.json cases are not supported; "
+			"provide simulation_config.json");
+	const SimulationConfig config = ReadSimulationConfig((case_dir/"simulation_config.json").string());
+	const FlowSystem& flow = FindNavierStokesSystem(config, options.system);
+	const bool transient = flow.time_integration == "backward_euler";
+	const double viscosity = flow.viscosity, density = flow.density;
+	const double dt = transient ? config.dt : 0.0;
+	const int physical_steps = transient ? config.steps : 1;
+	std::vector<OutletModel> outlets = InitializeOutletModels(config, flow);
+	auto resolve = [&](const SimulationConfig& step_config, std::map<int, double>& tractions) {
+		const auto boundary_config = MaterializeOutletPressures(step_config, outlets);
+		const auto& system = FindNavierStokesSystem(boundary_config, options.system);
+		tractions = ExtractPressureTractions(boundary_config, system);
+		auto r = ResolveFlowBoundaries(boundary_config, system, labeled.labels, reference_velocity);
+		for (const int32_t node : wall) {
+			if (!r.velocity_mask.at(node)) ++r.velocity_nodes;
+			r.velocity_mask[node] = 1;
+			for (int d = 0; d < 3; ++d) r.velocity[3*node+d] = 0.0;
+		}
+		return r;
+	};
+	std::map<int, double> tractions;
+	auto boundaries = resolve(transient ? MaterializeWaveforms(config, 0.0) : config, tractions);
+	if (!transient)
+		for (const auto& m : outlets)
+			if (m.kind != "resistance") Fail(-4, "RC/RCR outlets require backward_euler flow");
+	if (options.stop_after_step > physical_steps) Fail(-1, "--stop-after-step exceeds configured physical steps");
+	const int run_end = options.stop_after_step > 0 ? options.stop_after_step : physical_steps;
+	std::cout << "boundary_config=simulation_config.json viscosity=" << viscosity << " density=" << density
+		<< " time_integration=" << (transient ? "backward_euler" : "steady") << " dt=" << dt
+		<< " steps=" << physical_steps << " run_end_step=" << run_end
+		<< " velocity_nodes=" << boundaries.velocity_nodes << " pressure_nodes=" << boundaries.pressure_nodes << '\n';
+	if (!transient && (!options.restart.empty() || !options.checkpoint.empty() || options.output_every > 0
+		|| options.checkpoint_every > 0))
+		Fail(-1, "restart, checkpoint, and time-indexed output require transient flow");
+	const int64_t nodes = host.nodes;
+	Mesh mesh(std::move(host));
+	PrintMesh(mesh);
+	if (mesh.bad_samples())
+		Fail(-5, "mesh has "+std::to_string(mesh.bad_samples())+" non-positive quadrature Jacobians; minimum detJ "
+			+std::to_string(mesh.min_detj()));
+	const auto preprocess_end = Clock::now();
+	tfiga_ns_params params;
+	tfiga_ns_default_params(&params);
+	params.density = density;
+	params.viscosity = viscosity;
+	params.dt = dt;
+	params.max_newton = options.max_newton;
+	params.nonlinear_rtol = options.rtol;
+	params.nonlinear_atol = options.atol;
+	params.mass_rtol = options.mass_rtol;
+	NsSolver solver(mesh, params);
+	std::vector<int32_t> traction_labels;
+	std::vector<double> traction_values;
+	auto upload_boundaries = [&]() {
+		solver.SetDirichlet(boundaries.velocity_mask.data(), boundaries.pressure_mask.data(),
+			boundaries.velocity.data(), boundaries.pressure.data());
+		traction_labels.clear(); traction_values.clear();
+		for (const auto& t : tractions) { traction_labels.push_back(t.first); traction_values.push_back(t.second); }
+		solver.SetTractions(traction_labels.data(), traction_values.data(), (int)traction_labels.size());
+	};
+	upload_boundaries();
+	int start_step = 0;
+	std::vector<double> state((size_t)nodes*4, 0.0);
+	if (transient && !options.restart.empty()) {
+		auto r = ReadCheckpoint(options.restart, nodes, dt, density, viscosity, outlets);
+		state = r.state;
+		start_step = r.completed;
+		std::cout << "restart=" << options.restart << " completed_step=" << start_step << " physical_time=" << r.time << '\n';
+	} else if (transient) {
+		for (int64_t node = 0; node < nodes; ++node) {
+			if (boundaries.velocity_mask[node]) for (int d = 0; d < 3; ++d) state[4*node+d] = boundaries.velocity[3*node+d];
+			if (boundaries.pressure_mask[node]) state[4*node+3] = boundaries.pressure[node];
+		}
+	}
+	solver.SetState(state.data(), state.data());
+	long long total_iterations = 0;
+	double total_assembly = 0.0, total_linear = 0.0;
+	if (transient && options.output_every > 0) {
+		WriteText(TimeIndexed(options.output, start_step), state);
+	}
+	for (int step = start_step; step < run_end; ++step) {
+		if (step > start_step) solver.CommitStep();
+		const double physical_time = transient ? (step+1)*dt : 0.0;
+		const SimulationConfig step_config = transient ? MaterializeWaveforms(config, physical_time) : config;
+		std::vector<double> previous_capacitor(outlets.size());
+		for (size_t i = 0; i < outlets.size(); ++i) previous_capacitor[i] = outlets[i].capacitor_pressure;
+		const int max_outlet = outlets.empty() ? 1 : 12;
+		bool outlet_converged = false;
+		for (int coupling = 0; coupling < max_outlet; ++coupling) {
+			boundaries = resolve(step_config, tractions);
+			upload_boundaries();
+			double initial = -1.0;
+			bool converged = false;
+			tfiga_newton_report last{};
+			for (int k = 0; k < options.max_newton; ++k) {
+				last = solver.NewtonIteration(initial);
+				if (initial < 0.0) initial = last.residual_l2;
+				total_assembly += last.assembly_ms/1e3;
+				const double rms = last.residual_l2/std::sqrt(4.0*nodes);
+				if (last.converged) {
+					std::cout << "step=" << step+1 << " time=" << physical_time << " converged newton=" << k
+						<< " residual_l2=" << last.residual_l2 << " residual_rms=" << rms << " tolerance=" << last.tolerance
+						<< " absolute_rms_tolerance=" << options.atol << " continuity_l2=" << last.continuity_l2
+						<< " continuity_sum=" << last.continuity_sum << " net_boundary_flow=" << last.net_boundary_flow
+						<< " relative_mass_imbalance=" << last.relative_mass_imbalance
+						<< " mass_tolerance=" << options.mass_rtol << '\n';
+					converged = true;
+					break;
+				}
+				total_linear += last.linear_ms/1e3;
+				total_iterations += last.linear_iterations;
+				std::cout << "step=" << step+1 << " time=" << physical_time << " newton=" << k
+					<< " residual_l2=" << last.residual_l2 << " residual_rms=" << rms
+					<< " continuity_l2=" << last.continuity_l2 << " continuity_sum=" << last.continuity_sum
+					<< " net_boundary_flow=" << last.net_boundary_flow
+					<< " relative_mass_imbalance=" << last.relative_mass_imbalance << " update_l2=" << last.update_l2
+					<< " linear_iterations=" << last.linear_iterations << " linear_residual=" << last.linear_residual
+					<< " singular_diagonal_blocks=" << last.singular_diagonal_blocks
+					<< " assembly_s=" << last.assembly_ms/1e3 << " linear_s=" << last.linear_ms/1e3 << '\n';
+			}
+			if (!converged)
+				Fail(-6, "Navier-Stokes nonlinear solve reached MAX_NEWTON at physical step "+std::to_string(step+1)
+					+" (nonlinear_residual="+Precise(last.residual_l2)+", continuity_l2="+Precise(last.continuity_l2)
+					+", net_boundary_flow="+Precise(last.net_boundary_flow)+", relative_mass_imbalance="
+					+Precise(last.relative_mass_imbalance)+")");
+			if (outlets.empty()) { outlet_converged = true; break; }
+			// Outlet fixed point (iga_cuda.cu:1059-1082, OutletModel.hpp:92-150).
+			std::vector<int32_t> labels;
+			for (const auto& m : outlets) labels.push_back(m.label);
+			std::vector<double> flows(outlets.size());
+			solver.BoundaryFlows(labels.data(), (int)labels.size(), flows.data());
+			double change = 0.0, scale = 1.0;
+			std::vector<std::array<double, 2>> evaluated(outlets.size());
+			for (size_t i = 0; i < outlets.size(); ++i) {
+				auto m = outlets[i];
+				m.capacitor_pressure = previous_capacitor[i];
+				evaluated[i] = EvaluateOutletModel(m, flows[i], dt);
+				change = std::max(change, std::fabs(evaluated[i][0]-outlets[i].pressure));
+				scale = std::max(scale, std::fabs(evaluated[i][0]));
+			}
+			const double tolerance = 1e-8+1e-6*scale;
+			std::cout << "step=" << step+1 << " time=" << physical_time << " outlet_iteration=" << coupling
+				<< " pressure_change=" << change << " tolerance=" << tolerance << '\n';
+			if (change <= tolerance) {
+				for (size_t i = 0; i < outlets.size(); ++i) {
+					outlets[i].flow = flows[i];
+					outlets[i].pressure = evaluated[i][0];
+					outlets[i].capacitor_pressure = evaluated[i][1];
+					std::cout << "outlet label=" << outlets[i].label << " flow=" << outlets[i].flow
+						<< " pressure=" << outlets[i].pressure << " capacitor_pressure="
+						<< outlets[i].capacitor_pressure << '\n';
+				}
+				outlet_converged = true;
+				break;
+			}
+			for (size_t i = 0; i < outlets.size(); ++i) {
+				outlets[i].flow = flows[i];
+				outlets[i].pressure = 0.5*outlets[i].pressure+0.5*evaluated[i][0];
+			}
+		}
+		if (!outlet_converged)
+			Fail(-6, "outlet fixed-point iteration did not converge at physical step "+std::to_string(step+1));
+		const int completed = step+1;
+		if (options.output_every > 0 && completed%options.output_every == 0) {
+			solver.GetState(state.data());
+			WriteText(TimeIndexed(options.output, completed), state);
+		}
+		if (!options.checkpoint.empty()
+			&& (completed == run_end || (options.checkpoint_every > 0 && completed%options.checkpoint_every == 0))) {
+			solver.GetState(state.data());
+			WriteCheckpoint(options.checkpoint, nodes, completed, completed*dt, dt, density, viscosity, outlets, state);
+			std::cout << "checkpoint=" << options.checkpoint << " completed_step=" << completed << '\n';
+		}
+	}
+	solver.GetState(state.data());
+	double vsq = 0.0, psq = 0.0;
+	for (int64_t node = 0; node < nodes; ++node) {
+		for (int d = 0; d < 3; ++d) vsq += state[4*node+d]*state[4*node+d];
+		psq += state[4*node+3]*state[4*node+3];
+	}
+	if (!options.output.empty()) {
+		WriteText(options.output, state);
+		WriteVtk(case_dir/"controlmesh.vtk", options.output+".vtk", state);
+	}
+	std::cout << "navier_stokes_cuda nodes=" << nodes << " elements=" << mesh.host().elements()
+		<< " steps=" << physical_steps << " run_end_step=" << run_end
+		<< " preprocess_s=" << std::chrono::duration<double>(preprocess_end-total_start).count()
+		<< " assembly_s=" << total_assembly << " linear_s=" << total_linear
+		<< " total_linear_iterations=" << total_iterations << " state_l2=" << std::sqrt(vsq+psq)
+		<< " velocity_l2=" << std::sqrt(vsq) << " pressure_l2=" << std::sqrt(psq)
+		<< " gpu_used_gib=" << DeviceBytesPeak()/1073741824.0 << '\n';
+	return 0;
+}
+
 } // namespace
+} // namespace tfiga
 
 extern "C" int tfiga_main(int argc, char** argv)
 {
 	try {
-		if (argc < 2) throw std::runtime_error("usage: iga_cuda_b200 device-info|mesh-check|navier-stokes ...");
+		if (argc < 2) throw std::runtime_error("usage: iga_cuda device-info|mesh-check|navier-stokes ...");
 		tfiga::RequireDevice();
 		const std::string command(argv[1]);
-		PrintDevice();
+		tfiga::PrintDevice();
+		int status = 0;
 		if (command == "device-info") return 0;
 		if (command == "mesh-check") {
-			if (argc != 3) throw std::runtime_error("usage: iga_cuda_b200 mesh-check DATABASE.ntiga");
-			return MeshCheck(argv[2]);
+			if (argc != 3) throw std::runtime_error("usage: iga_cuda mesh-check DATABASE.ntiga");
+			status = tfiga::MeshCheck(argv[2]);
+		} else if (command == "navier-stokes") {
+			status = tfiga::NavierStokes(argc, argv);
+		} else {
+			throw std::runtime_error("unknown command: "+command);
 		}
-		throw std::runtime_error("unknown command: "+command);
+		std::cout << "cuda_allocations scope=project_device_buffers requested_peak_bytes=" << tfiga::DeviceBytesPeak()
+			<< " requested_live_bytes=" << tfiga::DeviceBytesLive() << '\n';
+		std::cout.flush();
+		return status;
 	} catch (const std::exception& error) {
 		std::cerr << "iga_cuda: " << error.what() << '\n';
+		std::cerr << "cuda_allocations scope=project_device_buffers requested_peak_bytes=" << tfiga::DeviceBytesPeak()
+			<< " requested_live_bytes=" << tfiga::DeviceBytesLive() << '\n';
 		return 1;
 	}
 }

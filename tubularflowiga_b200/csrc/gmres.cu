@@ -155,13 +155,23 @@ __global__ void __launch_bounds__(kThreads) SolutionUpdateKernel(const double* _
 {
 	extern __shared__ double coef[];
 	const int used = state[1];
-	for (int i = threadIdx.x; i < used; i += blockDim.x) coef[i] = y[i]*scale[i];
+	for (int i = threadIdx.x; i < used; i += blockDim.x) coef[i] = scale != nullptr ? y[i]*scale[i] : y[i];
 	__syncthreads();
 	for (long long k = (long long)blockIdx.x*blockDim.x+threadIdx.x; k < n; k += (long long)gridDim.x*blockDim.x) {
 		double v = x[k];
 		for (int i = 0; i < used; ++i) v = fma(coef[i], V[(size_t)i*n+k], v);
 		x[k] = v;
 	}
+}
+
+// out = scale[j] * in (materialise a lazily normalised Krylov vector).
+__global__ void ScaleCopyKernel(long long n, const double* __restrict__ in, const double* __restrict__ scale,
+	double* __restrict__ out, const int* __restrict__ stop)
+{
+	if (*stop) return;
+	const double s = *scale;
+	for (long long k = (long long)blockIdx.x*blockDim.x+threadIdx.x; k < n; k += (long long)gridDim.x*blockDim.x)
+		out[k] = s*in[k];
 }
 
 __global__ void ResidualKernel(long long n, const double* __restrict__ rhs, const double* __restrict__ ax,
@@ -217,14 +227,22 @@ std::size_t Gmres::bytes() const
 
 void Gmres::Step(const DevicePatternView& pattern, const double* values, int j)
 {
+	const int* stop = state_.get();
+	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
+	LaunchSpmvBlockJacobi(pattern, values, inverse_.get(), V_.get()+(size_t)j*n_, scale_.get()+j, w_.get(), stop,
+		stream_);
+	if (profiler_) profiler_->End(stream_);
+	launches_ += 1;
+	Orthogonalize(j);
+}
+
+void Gmres::Orthogonalize(int j)
+{
 	const int count = j+1;
 	const int* stop = state_.get();
 	const size_t dot_smem = (size_t)chunk_*sizeof(double);
 	const size_t coef_smem = (size_t)(restart_+1)*sizeof(double);
-	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
-	LaunchSpmvBlockJacobi(pattern, values, inverse_.get(), V_.get()+(size_t)j*n_, scale_.get()+j, w_.get(), stop,
-		stream_);
-	if (profiler_) { profiler_->End(stream_); profiler_->Begin(Profiler::kOrtho, stream_); }
+	if (profiler_) profiler_->Begin(Profiler::kOrtho, stream_);
 	for (int pass = 0; pass < 2; ++pass) {
 		MultiDotKernel<<<blocks_, kThreads, dot_smem, stream_>>>(V_.get(), n_, scale_.get(), count, w_.get(),
 			partial_.get(), chunk_, stop);
@@ -238,7 +256,93 @@ void Gmres::Step(const DevicePatternView& pattern, const double* values, int j)
 		LaunchCheck("UpdateKernel");
 	}
 	if (profiler_) profiler_->End(stream_);
-	launches_ += 8;
+	launches_ += 7;
+}
+
+void Gmres::FlexibleStep(const DevicePatternView& pattern, const double* values, int j, Amg& M)
+{
+	const int* stop = state_.get();
+	ScaleCopyKernel<<<blocks_, kThreads, 0, stream_>>>(n_, V_.get()+(size_t)j*n_, scale_.get()+j, r_.get(), stop);
+	LaunchCheck("ScaleCopyKernel");
+	launches_ += 1;
+	double* z = Z_.get()+(size_t)j*n_;
+	M.Apply(values, r_.get(), z, stop);
+	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
+	LaunchSpmvBlockJacobi(pattern, values, nullptr, z, nullptr, w_.get(), stop, stream_);
+	if (profiler_) profiler_->End(stream_);
+	launches_ += 1;
+	Orthogonalize(j);
+}
+
+double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const double* values, const double* rhs,
+	const double* x)
+{
+	LaunchSpmv(pattern, values, x, tmp_.get(), stream_);
+	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), V_.get());
+	LaunchCheck("ResidualKernel");
+	LaunchNorm(n_, V_.get(), norm_partial_.get(), scalar_.get(), stream_);
+	launches_ += 4;
+	scalar_.Download(host_->beta, 1, stream_);
+	CudaCheck(cudaStreamSynchronize(stream_), "FGMRES residual");
+	return host_->beta[0];
+}
+
+GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const double* values, const double* rhs,
+	double* x, double rtol, int max_iterations, Amg& M, long long* launches)
+{
+	launches_ = 0;
+	const long long amg0 = M.launches();
+	if (Z_.size() == 0) Z_.Allocate((size_t)(restart_+1)*n_);
+	GmresResult result;
+	double beta = TrueResidualPlain(pattern, values, rhs, x);
+	result.residual = beta;
+	if (!std::isfinite(beta)) Fail(-6, "FGMRES initial residual is not finite");
+	if (beta == 0.0) {
+		result.converged = true;
+		if (launches) *launches += launches_;
+		return result;
+	}
+	const double tolerance = std::max(1e-30, rtol*beta);
+	while (result.iterations < max_iterations) {
+		CycleInitKernel<<<1, 256, 0, stream_>>>(scalar_.get(), g_.get(), restart_, scale_.get(), state_.get());
+		LaunchCheck("CycleInitKernel");
+		H_.Zero(stream_);
+		launches_ += 1;
+		const int cap = std::min(restart_, max_iterations-result.iterations);
+		for (int j = 0; j < cap;) {
+			const int batch = std::min(kBatch, cap-j);
+			for (int b = 0; b < batch; ++b) {
+				FlexibleStep(pattern, values, j+b, M);
+				ArnoldiFinalizeKernel<<<1, 32, 0, stream_>>>(norm_partial_.get(), blocks_, H_.get(), restart_, j+b,
+					cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance);
+				LaunchCheck("ArnoldiFinalizeKernel");
+				launches_ += 1;
+			}
+			j += batch;
+			state_.Download(&host_->stop, 3, stream_);
+			residual_.Download(&host_->residual, 1, stream_);
+			CudaCheck(cudaStreamSynchronize(stream_), "FGMRES batch");
+			if (host_->stop) break;
+		}
+		const int used = host_->used;
+		result.iterations += used;
+		BackSolveKernel<<<1, 1, 0, stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(), state_.get()+2);
+		LaunchCheck("BackSolveKernel");
+		SolutionUpdateKernel<<<blocks_, kThreads, (size_t)(restart_+1)*sizeof(double), stream_>>>(Z_.get(), n_,
+			nullptr, y_.get(), state_.get(), x);
+		LaunchCheck("SolutionUpdateKernel");
+		launches_ += 2;
+		beta = TrueResidualPlain(pattern, values, rhs, x);
+		state_.Download(&host_->stop, 3, stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "FGMRES restart");
+		if (host_->error) Fail(-6, "FGMRES Hessenberg matrix is singular");
+		result.residual = beta;
+		if (!std::isfinite(beta)) Fail(-6, "FGMRES residual is not finite");
+		if (beta <= tolerance) { result.converged = true; break; }
+		if (used == 0) break;
+	}
+	if (launches) *launches += launches_+(M.launches()-amg0);
+	return result;
 }
 
 double Gmres::TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs,

@@ -11,6 +11,7 @@
 // the device has flagged convergence, so the host waits only once per batch.
 #pragma once
 
+#include "amg.hpp"
 #include "common.hpp"
 #include "kernels.cuh"
 
@@ -32,18 +33,26 @@ public:
 	// Solves A x = rhs (x holds the initial guess).  Builds the block inverse first.
 	GmresResult Solve(const DevicePatternView& pattern, const double* values, const double* rhs, double* x,
 		double rtol, int max_iterations, long long* launches);
+	// Right-preconditioned flexible GMRES (FGMRES): z_j = M^{-1} v_j stored, tolerance
+	// rtol * ||b - A x0|| on the true residual.
+	GmresResult SolveFlexible(const DevicePatternView& pattern, const double* values, const double* rhs, double* x,
+		double rtol, int max_iterations, Amg& preconditioner, long long* launches);
 	int restart() const { return restart_; }
 	void set_profiler(Profiler* profiler) { profiler_ = profiler; }
 	std::size_t bytes() const;
 
 private:
 	void Step(const DevicePatternView& pattern, const double* values, int j);
+	void Orthogonalize(int j);
+	void FlexibleStep(const DevicePatternView& pattern, const double* values, int j, Amg& preconditioner);
+	double TrueResidualPlain(const DevicePatternView& pattern, const double* values, const double* rhs, const double* x);
 	double TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs, const double* x);
 
 	int nodes_, n_, restart_, blocks_;
 	int chunk_;
 	cudaStream_t stream_;
 	long long launches_ = 0;
+	DeviceArray<double> Z_;
 	DeviceArray<double> V_, w_, r_, tmp_, inverse_, partial_, hpass_, H_, cs_, sn_, g_, y_, scale_, norm_partial_,
 		scalar_;
 	DeviceArray<int> state_;          // [0] stop, [1] used, [2] error

@@ -61,7 +61,8 @@ void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double*
 // ---- sparse.cu ----------------------------------------------------------
 void LaunchSpmv(const DevicePatternView& pattern, const double* values, const double* x, double* y,
 	cudaStream_t stream);
-// y = D^{-1} (A (scale * x)) with D^{-1} stored per node as 4x4 (scale read from device, may be null).
+// y = D^{-1} (A (scale * x)) with D^{-1} stored per node as 4x4 (scale read from device, may be null);
+// inverse == null gives y = scale * A x.  Returns early when *stop is set (stop may be null).
 void LaunchSpmvBlockJacobi(const DevicePatternView& pattern, const double* values, const double* inverse,
 	const double* x, const double* scale, double* y, const int* stop, cudaStream_t stream);
 void LaunchBlockInverse(const DevicePatternView& pattern, const double* values, double* inverse,

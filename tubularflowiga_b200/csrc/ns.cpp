@@ -67,6 +67,12 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 		"pinned scalars");
 	for (auto& ev : events_) CudaCheck(cudaEventCreate(&ev), "event");
 	gmres_.set_profiler(&profiler_);
+	if (params.preconditioner == TFIGA_PRECONDITIONER_AMG) {
+		amg_ = std::make_unique<Amg>(mesh.pattern_view(), mesh.pattern().row_offsets, mesh.pattern().columns, stream_);
+		amg_->set_profiler(&profiler_);
+	} else if (params.preconditioner != TFIGA_PRECONDITIONER_BLOCK_JACOBI) {
+		Fail(-1, "unknown preconditioner "+std::to_string(params.preconditioner));
+	}
 	CudaCheck(cudaStreamSynchronize(stream_), "solver setup");
 }
 
@@ -87,6 +93,7 @@ void NsSolver::SetDirichlet(const int32_t* vmask, const int32_t* pmask, const do
 	}
 	vmask_.Upload(vm.data(), n, stream_);
 	pmask_.Upload(pm.data(), n, stream_);
+	if (amg_) amg_->SetMasks(vm, pm);
 	if (!list.empty()) constrained_.Upload(list.data(), list.size(), stream_);
 	constrained_count_ = (int)list.size();
 	SetDirichletValues(velocity, pressure);
@@ -160,6 +167,8 @@ void NsSolver::Assemble()
 	profiler_.End(stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
 	launches_ += 2;
+	// The AMG hierarchy is built once, from the strength of the first raw (pre-Dirichlet) Jacobian.
+	if (amg_ && !amg_->built()) amg_->Build(values_.get());
 }
 
 void NsSolver::ApplyDirichlet()
@@ -173,6 +182,14 @@ void NsSolver::ApplyDirichlet()
 GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 {
 	update_.Zero(stream_);
+	if (amg_) {
+		if (!amg_->built()) amg_->Build(values_.get());
+		const long long before = amg_->launches();
+		amg_->Refresh(values_.get());
+		launches_ += amg_->launches()-before;
+		return gmres_.SolveFlexible(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol,
+			max_iterations, *amg_, &launches_);
+	}
 	return gmres_.Solve(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol, max_iterations,
 		&launches_);
 }

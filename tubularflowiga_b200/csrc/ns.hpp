@@ -2,12 +2,14 @@
 // step of the reference loop (solvers/cuda/src/iga_cuda.cu:952-1054).
 #pragma once
 
+#include "amg.hpp"
 #include "gmres.hpp"
 #include "mesh.hpp"
 
 #include "../../include/tfiga.h"
 
 #include <map>
+#include <memory>
 #include <vector>
 
 namespace tfiga {
@@ -47,6 +49,7 @@ public:
 	void AddLaunches(long long n) { launches_ += n; }
 	const tfiga_ns_params& params() const { return params_; }
 	Profiler& profiler() { return profiler_; }
+	const Amg* amg() const { return amg_.get(); }
 
 private:
 	struct Diagnostics {
@@ -71,6 +74,7 @@ private:
 	bool dirichlet_set_ = false;
 	Gmres gmres_;
 	Profiler profiler_;
+	std::unique_ptr<Amg> amg_;
 	double* pinned_ = nullptr;               // host mirror of scalars + label flows
 };
 

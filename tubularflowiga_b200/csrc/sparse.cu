@@ -56,6 +56,10 @@ __global__ void __launch_bounds__(256) SpmvBlockJacobiKernel(DevicePatternView p
 	if (row >= p.nodes) return;
 	double sum = RowBlockDot(p, values, x, row, lane);
 	if (scale != nullptr) sum *= *scale;
+	if (inverse == nullptr) {
+		if (lane < 4) y[4*(size_t)row+lane] = sum;
+		return;
+	}
 	const double y0 = __shfl_sync(0xffffffffu, sum, 0), y1 = __shfl_sync(0xffffffffu, sum, 1);
 	const double y2 = __shfl_sync(0xffffffffu, sum, 2), y3 = __shfl_sync(0xffffffffu, sum, 3);
 	if (lane < 4) {
