@@ -1,0 +1,102 @@
+"""The drop-in `navier-stokes` command on a generated case directory.
+
+Checks the reference command's observable contract
+(solvers/cuda/src/iga_cuda.cu:734-1195): exit codes, the key=value log lines,
+the velocity/pressure text outputs (one row per node), and that a run
+restarted from a checkpoint reproduces the uninterrupted run (the reference's
+restart gate is 1e-12, solvers/cuda/VALIDATION.md:60-62).
+"""
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests.conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+COMMAND = ROOT / "tubularflowiga_b200" / "lib" / "iga_cuda_b200"
+
+
+def run(*args):
+    return subprocess.run([str(COMMAND), *map(str, args)], capture_output=True, text=True, timeout=600)
+
+
+@pytest.fixture(scope="module")
+def case(tmp_path_factory):
+    from tubularflowiga_b200 import meshgen
+    d = tmp_path_factory.mktemp("case")
+    tube = meshgen.straight_tube(1.5e-3, 6e-3, core=4, ring=1, layers=4)
+    wave = meshgen.fourier_waveform(0)
+    cfg = meshgen.simulation_config(1060.0, 3.5e-3, 2e-3, 3, 1.0, transient=True, waveform=wave)
+    db = meshgen.write_case(d, tube, cfg)
+    return d, db, tube
+
+
+def test_mesh_check_and_errors(case):
+    d, db, tube = case
+    r = run("mesh-check", db)
+    assert r.returncode == 0, r.stderr
+    assert f"mesh nodes={tube.mesh.nodes} elements={tube.mesh.elements}" in r.stdout
+    assert "bad_samples=0" in r.stdout
+    bad = run("navier-stokes", db)
+    assert bad.returncode == 1 and bad.stderr.startswith("iga_cuda: usage")
+    r = run("navier-stokes", db, d, "--bogus", "1")
+    assert r.returncode == 1 and "unknown option" in r.stderr
+
+
+def test_navier_stokes_run_outputs_and_restart(case, tmp_path):
+    d, db, tube = case
+    out = tmp_path / "flow.txt"
+    r = run("navier-stokes", db, d, "--output", out, "--checkpoint", tmp_path / "ck", "--nonlinear-rtol", "1e-10",
+            "--nonlinear-atol", "1e-30")
+    assert r.returncode == 0, r.stderr
+    assert "boundary_config=simulation_config.json" in r.stdout and "time_integration=backward_euler" in r.stdout
+    assert r.stdout.count(" converged newton=") == 3
+    assert "navier_stokes_cuda nodes=" in r.stdout
+    vel = np.loadtxt(out)
+    prs = np.loadtxt(str(out) + ".pressure")
+    assert vel.shape == (tube.mesh.nodes, 3) and prs.shape == (tube.mesh.nodes,)
+    assert np.isfinite(vel).all() and np.abs(vel[:, 2]).max() > 0.0
+    # stop after step 2 with a checkpoint, then restart for step 3
+    r1 = run("navier-stokes", db, d, "--stop-after-step", "2", "--checkpoint", tmp_path / "half",
+             "--nonlinear-rtol", "1e-10", "--nonlinear-atol", "1e-30")
+    assert r1.returncode == 0, r1.stderr
+    assert (tmp_path / "half.json").exists() and (tmp_path / "half.state").exists()
+    out2 = tmp_path / "restarted.txt"
+    r2 = run("navier-stokes", db, d, "--restart", tmp_path / "half", "--output", out2, "--nonlinear-rtol", "1e-10",
+             "--nonlinear-atol", "1e-30")
+    assert r2.returncode == 0, r2.stderr
+    assert "restart=" in r2.stdout and "completed_step=2" in r2.stdout
+    vel2 = np.loadtxt(out2)
+    assert np.linalg.norm(vel2 - vel) <= 1e-9 * np.linalg.norm(vel)
+    final = np.fromfile(tmp_path / "ck.state", dtype=np.float64).reshape(-1, 4)
+    assert np.allclose(final[:, :3], vel, rtol=0, atol=1e-15 * np.abs(vel).max() + 1e-300)
+
+
+def test_command_matches_api(case, tmp_path):
+    """The command and the Python binding drive the same device path: same state after one step."""
+    from tubularflowiga_b200 import api, meshgen
+    d, db, tube = case
+    out = tmp_path / "one.txt"
+    r = run("navier-stokes", db, d, "--stop-after-step", "1", "--output", out, "--nonlinear-rtol", "1e-10",
+            "--nonlinear-atol", "1e-30")
+    assert r.returncode == 0, r.stderr
+    wave = meshgen.fourier_waveform(0)
+    th = 2 * np.pi * 2e-3
+    factor = wave["mean"] + sum(c * np.cos((k + 1) * th) + s * np.sin((k + 1) * th)
+                                for k, (c, s) in enumerate(zip(wave["cosine"], wave["sine"])))
+    factor0 = wave["mean"] + sum(wave["cosine"])
+    mesh = api.Mesh(db)
+    ns = api.NavierStokes(mesh, density=1060.0, viscosity=3.5e-3, dt=2e-3, nonlinear_rtol=1e-10,
+                          nonlinear_atol=1e-30)
+    vmask, pmask, vel0 = api.tube_boundary_conditions(tube, factor0)
+    s0 = api.initial_state(vmask, vel0)
+    _, _, vel1 = api.tube_boundary_conditions(tube, factor)
+    ns.set_dirichlet(vmask, pmask, vel1)
+    ns.set_tractions({2: 0.0})
+    ns.set_state(s0, s0)
+    ns.step()
+    st = ns.get_state().reshape(-1, 4)
+    cmd = np.loadtxt(out)
+    assert np.linalg.norm(st[:, :3] - cmd) <= 1e-8 * np.linalg.norm(cmd)

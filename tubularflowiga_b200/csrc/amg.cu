@@ -122,14 +122,14 @@ __global__ void RestrictKernel(int coarse_nodes, const int32_t* __restrict__ ord
 	bc[t] = sum;
 }
 
-// x[i,c] += mask_i[c] x_c[agg(i), c].
+// x[i,c] = mask_i[c] x_c[agg(i), c] (piecewise-constant prolongation).
 __global__ void ProlongKernel(int nodes, const int32_t* __restrict__ agg, const double* __restrict__ mask,
 	const double* __restrict__ xc, double* __restrict__ x, const int* __restrict__ stop)
 {
 	if (*stop) return;
 	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
 	if (i >= 4LL*nodes) return;
-	x[i] += mask[i]*xc[4*(size_t)agg[i >> 2]+(i & 3)];
+	x[i] = mask[i]*xc[4*(size_t)agg[i >> 2]+(i & 3)];
 }
 
 __global__ void DenseScatterKernel(DevicePatternView p, const double* __restrict__ values, int n, double* __restrict__ dense)
@@ -325,81 +325,103 @@ void Amg::Build(const double* values)
 		ds.Download(s.data(), s.size(), stream_);
 		CudaCheck(cudaStreamSynchronize(stream_), "AMG strength");
 	}
-	levels_.push_back(std::move(fine));
-	while ((int)levels_.size() < options_.max_levels) {
-		Level& L = *levels_.back();
-		if (L.nodes <= options_.coarsest_nodes) break;
+	// Aggregate the strength graph repeatedly (aggregates of aggregates) until the
+	// coarse space is small enough for a dense solve; compose the maps.
+	std::vector<int32_t> compose(fine_.nodes);
+	std::iota(compose.begin(), compose.end(), 0);
+	std::vector<int32_t> rows = fine_rows_, cols = fine_columns_, diag = fine->h_diag;
+	int nodes = fine_.nodes;
+	for (int round = 0; round < options_.max_levels && nodes > options_.coarsest_nodes; ++round) {
 		int nc = 0;
-		L.h_agg = Aggregate(L.nodes, L.h_rows, L.h_cols, L.h_diag, s, options_.strength, nc);
-		if (nc >= (int)(0.9*L.nodes)) break;     // no useful coarsening
-		auto C = std::make_unique<Level>();
-		C->nodes = nc;
-		// coarse pattern and fine-block -> coarse-block map
-		std::vector<std::vector<int32_t>> crow(nc);
-		for (int i = 0; i < L.nodes; ++i)
-			for (int k = L.h_rows[i]; k < L.h_rows[i+1]; ++k) crow[L.h_agg[i]].push_back(L.h_agg[L.h_cols[k]]);
-		C->h_rows.assign(nc+1, 0);
+		const auto agg = Aggregate(nodes, rows, cols, diag, s, options_.strength, nc);
+		if (nc >= (int)(0.9*nodes)) break;
+		for (auto& c : compose) c = agg[c];
+		// coarse strength graph = summed strengths
+		std::vector<std::vector<std::pair<int32_t, double>>> crow(nc);
+		for (int i = 0; i < nodes; ++i)
+			for (int k = rows[i]; k < rows[i+1]; ++k) crow[agg[i]].push_back({agg[cols[k]], s[k]});
+		std::vector<int32_t> nrows(nc+1, 0), ncols, ndiag(nc);
+		std::vector<double> ns;
 		for (int I = 0; I < nc; ++I) {
 			auto& r = crow[I];
-			std::sort(r.begin(), r.end());
-			r.erase(std::unique(r.begin(), r.end()), r.end());
-			C->h_rows[I+1] = C->h_rows[I]+(int32_t)r.size();
-		}
-		C->h_cols.reserve(C->h_rows[nc]);
-		C->h_diag.resize(nc);
-		for (int I = 0; I < nc; ++I) {
-			const auto it = std::lower_bound(crow[I].begin(), crow[I].end(), I);
-			C->h_diag[I] = C->h_rows[I]+(int32_t)(it-crow[I].begin());
-			C->h_cols.insert(C->h_cols.end(), crow[I].begin(), crow[I].end());
-		}
-		C->blocks = C->h_rows[nc];
-		std::vector<int32_t> target(L.blocks), block_row(L.blocks);
-		std::vector<double> cs(C->blocks, 0.0);
-		for (int i = 0; i < L.nodes; ++i) {
-			const int I = L.h_agg[i];
-			for (int k = L.h_rows[i]; k < L.h_rows[i+1]; ++k) {
-				const int J = L.h_agg[L.h_cols[k]];
-				const auto it = std::lower_bound(C->h_cols.begin()+C->h_rows[I], C->h_cols.begin()+C->h_rows[I+1], J);
-				target[k] = (int32_t)(it-C->h_cols.begin());
-				block_row[k] = i;
-				cs[target[k]] += s[k];
+			std::sort(r.begin(), r.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+			for (size_t k = 0; k < r.size(); ++k) {
+				if (!ncols.empty() && (int)ncols.size() > nrows[I] && ncols.back() == r[k].first) { ns.back() += r[k].second; continue; }
+				if (r[k].first == I) ndiag[I] = (int32_t)ncols.size();
+				ncols.push_back(r[k].first);
+				ns.push_back(r[k].second);
 			}
+			nrows[I+1] = (int32_t)ncols.size();
 		}
-		// counting sort of fine blocks by coarse block; fine nodes by aggregate
-		std::vector<int32_t> goff(C->blocks+1, 0), gorder(L.blocks);
-		for (long long k = 0; k < L.blocks; ++k) ++goff[target[k]+1];
-		for (long long B = 0; B < C->blocks; ++B) goff[B+1] += goff[B];
-		{
-			std::vector<int32_t> fill(goff.begin(), goff.end()-1);
-			for (long long k = 0; k < L.blocks; ++k) gorder[fill[target[k]]++] = (int32_t)k;
-		}
-		std::vector<int32_t> aoff(nc+1, 0), aorder(L.nodes);
-		for (int i = 0; i < L.nodes; ++i) ++aoff[L.h_agg[i]+1];
-		for (int I = 0; I < nc; ++I) aoff[I+1] += aoff[I];
-		{
-			std::vector<int32_t> fill(aoff.begin(), aoff.end()-1);
-			for (int i = 0; i < L.nodes; ++i) aorder[fill[L.h_agg[i]]++] = i;
-		}
-		auto up = [&](DeviceArray<int32_t>& d, const std::vector<int32_t>& h) { d.Allocate(h.size()); d.Upload(h.data(), h.size(), stream_); };
-		up(L.agg, L.h_agg); up(L.agg_order, aorder); up(L.agg_offsets, aoff);
-		up(L.gal_order, gorder); up(L.gal_offsets, goff); up(L.block_row, block_row);
-		s.swap(cs);
-		levels_.push_back(std::move(C));
+		rows.swap(nrows); cols.swap(ncols); diag.swap(ndiag); s.swap(ns);
+		nodes = nc;
+		coarse_history_.push_back(nc);
 	}
-	// device storage per level
+	Level& L = *fine;
+	L.h_agg = compose;
+	const int nc = nodes;
+	auto C = std::make_unique<Level>();
+	C->nodes = nc;
+	// coarse block pattern over the composite map and the fine-block -> coarse-block map
+	std::vector<std::vector<int32_t>> crow(nc);
+	for (int i = 0; i < L.nodes; ++i)
+		for (int k = L.h_rows[i]; k < L.h_rows[i+1]; ++k) crow[compose[i]].push_back(compose[L.h_cols[k]]);
+	C->h_rows.assign(nc+1, 0);
+	for (int I = 0; I < nc; ++I) {
+		auto& r = crow[I];
+		std::sort(r.begin(), r.end());
+		r.erase(std::unique(r.begin(), r.end()), r.end());
+		C->h_rows[I+1] = C->h_rows[I]+(int32_t)r.size();
+	}
+	C->h_diag.resize(nc);
+	for (int I = 0; I < nc; ++I) {
+		const auto it = std::lower_bound(crow[I].begin(), crow[I].end(), I);
+		C->h_diag[I] = C->h_rows[I]+(int32_t)(it-crow[I].begin());
+		C->h_cols.insert(C->h_cols.end(), crow[I].begin(), crow[I].end());
+	}
+	C->blocks = C->h_rows[nc];
+	std::vector<int32_t> target(L.blocks), block_row(L.blocks);
+	for (int i = 0; i < L.nodes; ++i) {
+		const int I = compose[i];
+		for (int k = L.h_rows[i]; k < L.h_rows[i+1]; ++k) {
+			const int J = compose[L.h_cols[k]];
+			const auto it = std::lower_bound(C->h_cols.begin()+C->h_rows[I], C->h_cols.begin()+C->h_rows[I+1], J);
+			target[k] = (int32_t)(it-C->h_cols.begin());
+			block_row[k] = i;
+		}
+	}
+	std::vector<int32_t> goff(C->blocks+1, 0), gorder(L.blocks);
+	for (long long k = 0; k < L.blocks; ++k) ++goff[target[k]+1];
+	for (long long B = 0; B < C->blocks; ++B) goff[B+1] += goff[B];
+	{
+		std::vector<int32_t> fill(goff.begin(), goff.end()-1);
+		for (long long k = 0; k < L.blocks; ++k) gorder[fill[target[k]]++] = (int32_t)k;
+	}
+	std::vector<int32_t> aoff(nc+1, 0), aorder(L.nodes);
+	for (int i = 0; i < L.nodes; ++i) ++aoff[compose[i]+1];
+	for (int I = 0; I < nc; ++I) aoff[I+1] += aoff[I];
+	{
+		std::vector<int32_t> fill(aoff.begin(), aoff.end()-1);
+		for (int i = 0; i < L.nodes; ++i) aorder[fill[compose[i]]++] = i;
+	}
+	auto up = [&](DeviceArray<int32_t>& d, const std::vector<int32_t>& h) { d.Allocate(h.size()); d.Upload(h.data(), h.size(), stream_); };
+	up(L.agg, L.h_agg); up(L.agg_order, aorder); up(L.agg_offsets, aoff);
+	up(L.gal_order, gorder); up(L.gal_offsets, goff); up(L.block_row, block_row);
+	levels_.push_back(std::move(fine));
+	levels_.push_back(std::move(C));
+	if (nc > 2048) Fail(-7, "aggregation stalled: coarse space of "+std::to_string(nc)+" nodes is too large for the dense coarse solve");
 	for (size_t l = 0; l < levels_.size(); ++l) {
-		Level& L = *levels_[l];
-		auto up = [&](DeviceArray<int32_t>& d, const std::vector<int32_t>& h) { d.Allocate(h.size()); d.Upload(h.data(), h.size(), stream_); };
-		up(L.rows, L.h_rows); up(L.cols, L.h_cols); up(L.diag, L.h_diag);
-		if (l > 0) L.values.Allocate((size_t)L.blocks*16);
-		L.inverse.Allocate((size_t)L.nodes*16);
-		L.singular.Allocate(1);
-		L.mask.Allocate((size_t)4*L.nodes);
-		L.x.Allocate((size_t)4*L.nodes); L.b.Allocate((size_t)4*L.nodes); L.r.Allocate((size_t)4*L.nodes);
-		if (l+1 == levels_.size() && L.nodes <= 512) {
-			L.dense_n = 4*L.nodes;
-			L.dense.Allocate((size_t)L.dense_n*2*L.dense_n);
-			L.dense_flag.Allocate(1);
+		Level& V = *levels_[l];
+		up(V.rows, V.h_rows); up(V.cols, V.h_cols); up(V.diag, V.h_diag);
+		if (l > 0) V.values.Allocate((size_t)V.blocks*16);
+		V.inverse.Allocate((size_t)V.nodes*16);
+		V.singular.Allocate(1);
+		V.mask.Allocate((size_t)4*V.nodes);
+		V.x.Allocate((size_t)4*V.nodes); V.b.Allocate((size_t)4*V.nodes); V.r.Allocate((size_t)4*V.nodes);
+		if (l+1 == levels_.size()) {
+			V.dense_n = 4*V.nodes;
+			V.dense.Allocate((size_t)V.dense_n*2*V.dense_n);
+			V.dense_flag.Allocate(1);
 		}
 	}
 	CudaCheck(cudaStreamSynchronize(stream_), "AMG setup");
@@ -445,9 +467,8 @@ void Amg::Refresh(const double* values)
 		LaunchCheck("UnitDiagonalKernel");
 		launches_ += 2;
 	}
-	for (size_t l = 0; l < levels_.size(); ++l) {
+	for (size_t l = 0; l+1 < levels_.size(); ++l) {
 		Level& L = *levels_[l];
-		if (L.dense_n > 0) continue;
 		L.singular.Zero(stream_);
 		LaunchBlockInverse(L.view(), l == 0 ? values : L.values.get(), L.inverse.get(), L.singular.get(), stream_);
 		launches_ += 1;
@@ -466,54 +487,23 @@ void Amg::Refresh(const double* values)
 
 void Amg::Cycle(int l, const double* b, double* x, const int* stop)
 {
+	// Two-level: x = P Ac^{-1} P^T b, then x += D^{-1} (b - A x).
 	Level& L = *levels_[l];
-	if (l+1 == (int)levels_.size() && L.dense_n == 0) {
-		// coarsening stalled above the dense limit: damped block-Jacobi sweeps
-		const double* A = l == 0 ? fine_values_ : L.values.get();
-		const long long n4 = 4LL*L.nodes;
-		JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), b, x, options_.omega, 0, stop);
-		for (int s = 1; s < 4; ++s) {
-			ResidualKernel<<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
-			JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), L.r.get(), x, options_.omega, 1, stop);
-		}
-		LaunchCheck("coarsest JacobiKernel");
-		launches_ += 7;
-		return;
-	}
-	if (l+1 == (int)levels_.size()) {
-		DenseApplyKernel<<<Grid(L.dense_n, 8), 256, 0, stream_>>>(L.dense_n, L.dense.get(), b, x, stop);
-		LaunchCheck("DenseApplyKernel");
-		launches_ += 1;
-		return;
-	}
 	Level& C = *levels_[l+1];
-	const double* A = l == 0 ? fine_values_ : L.values.get();
+	const double* A = fine_values_;
 	const long long n4 = 4LL*L.nodes;
-	const double omega = options_.omega;
-	JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), b, x, omega, 0, stop);
-	LaunchCheck("JacobiKernel");
-	launches_ += 1;
-	for (int s = 1; s < options_.pre_sweeps; ++s) {
-		ResidualKernel<<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
-		JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), L.r.get(), x, omega, 1, stop);
-		launches_ += 2;
-	}
-	ResidualKernel<<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
-	LaunchCheck("ResidualKernel");
 	RestrictKernel<<<Grid(4LL*C.nodes, 256), 256, 0, stream_>>>(C.nodes, L.agg_order.get(), L.agg_offsets.get(),
-		L.mask.get(), L.r.get(), C.b.get(), stop);
+		L.mask.get(), b, C.b.get(), stop);
 	LaunchCheck("RestrictKernel");
-	launches_ += 2;
-	Cycle(l+1, C.b.get(), C.x.get(), stop);
+	DenseApplyKernel<<<Grid(C.dense_n, 8), 256, 0, stream_>>>(C.dense_n, C.dense.get(), C.b.get(), C.x.get(), stop);
+	LaunchCheck("DenseApplyKernel");
 	ProlongKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(), C.x.get(), x, stop);
 	LaunchCheck("ProlongKernel");
-	launches_ += 1;
-	for (int s = 0; s < options_.post_sweeps; ++s) {
-		ResidualKernel<<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
-		JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), L.r.get(), x, omega, 1, stop);
-		LaunchCheck("JacobiKernel");
-		launches_ += 2;
-	}
+	ResidualKernel<<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
+	LaunchCheck("ResidualKernel");
+	JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), L.r.get(), x, options_.omega, 1, stop);
+	LaunchCheck("JacobiKernel");
+	launches_ += 5;
 }
 
 void Amg::Apply(const double* fine_values, const double* v, double* z, const int* stop)

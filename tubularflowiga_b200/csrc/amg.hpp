@@ -1,17 +1,22 @@
-// Point-block (4x4) plain-aggregation algebraic multigrid, used as the right
-// preconditioner of the flexible GMRES.
+// Point-block (4x4) aggregation multigrid, used as the right preconditioner of
+// the flexible GMRES.
 //
-// Algorithm: the reference's scalar AggregationAmg
-// (solvers/cuda/include/AggregationAmg.hpp:32-436): a hierarchy built once on
+// Ingredients follow the reference's scalar AggregationAmg
+// (solvers/cuda/include/AggregationAmg.hpp:32-436): aggregates built once on
 // the host from a strength graph, piecewise-constant prolongation, a Galerkin
-// refresh on the device that sums fine entries into coarse entries, damped
-// Jacobi smoothing and a dense inverse at the coarsest level.  Here it works
-// on the 4x4 node blocks of the Navier-Stokes system (velocity and pressure
-// aggregated together): strength from the trace of the velocity block,
-// Vanek-style greedy aggregation, block-Jacobi smoothing, and Dirichlet
-// degrees of freedom masked out of prolongation and of every coarse operator.
-// Every reduction (Galerkin sums, restriction) runs in a fixed order, so a
-// V-cycle is deterministic.
+// refresh on the device that sums fine entries into coarse entries, and a dense
+// inverse at the coarsest level.  Here it works on the 4x4 node blocks of the
+// Navier-Stokes system (velocity and pressure aggregated together; strength
+// from the trace of the velocity block; Vanek-style greedy aggregation applied
+// repeatedly to the aggregated strength graph until a few hundred aggregates
+// remain).  Damped Jacobi is not a convergent smoother for these IGA operators
+// (cubic B-spline mass matrices have diag/row-sum near 0.1 in 3D), so the
+// preconditioner is two-level: the coarse correction x = P Ac^{-1} P^T v
+// followed by one block-Jacobi step on the remaining residual.  The coarse
+// space carries the long-range (axial) pressure/velocity modes that make
+// block-Jacobi GMRES iterations grow with tube length.  Dirichlet degrees of
+// freedom are masked out of the prolongation and the coarse operator.  Every
+// reduction runs in a fixed order, so an application is deterministic.
 #pragma once
 
 #include "common.hpp"
@@ -24,10 +29,9 @@ namespace tfiga {
 
 struct AmgOptions {
 	double strength = 0.08;        // |s_ij| >= theta sqrt(|s_ii s_jj|) is a strong connection
-	int coarsest_nodes = 160;      // dense inverse at or below this many nodes
-	int max_levels = 8;
-	int pre_sweeps = 1, post_sweeps = 1;
-	double omega = 0.7;            // block-Jacobi damping
+	int coarsest_nodes = 300;      // aggregate until at most this many coarse nodes (dense solve)
+	int max_levels = 8;            // aggregation rounds
+	double omega = 1.0;            // weight of the block-Jacobi step after the coarse correction
 };
 
 class Amg {
@@ -49,6 +53,7 @@ public:
 	void Apply(const double* fine_values, const double* v, double* z, const int* stop);
 	int levels() const { return (int)levels_.size(); }
 	std::vector<int> level_nodes() const;
+	const std::vector<int>& aggregation_rounds() const { return coarse_history_; }
 	std::vector<long long> level_blocks() const;
 	long long launches() const { return launches_; }
 	void set_profiler(Profiler* p) { profiler_ = p; }
@@ -60,6 +65,7 @@ private:
 	DevicePatternView fine_;
 	std::vector<int32_t> fine_rows_, fine_columns_;
 	std::vector<int32_t> vmask_, pmask_;
+	std::vector<int> coarse_history_;
 	cudaStream_t stream_;
 	AmgOptions options_;
 	bool built_ = false;
