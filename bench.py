@@ -59,6 +59,11 @@ def peaks():
 
 def workload(name):
     from tubularflowiga_b200 import meshgen
+    if name == "c2-100":
+        tube = meshgen.straight_tube(1.5e-3, 7.5e-3, core=8, ring=2, layers=100)
+        desc = ("pulsatile tube cross-section of the 51,200-element case, 100 layers (12,800 elements), "
+                "R 1.5 mm, L 7.5 mm, same inflow (profiling case)")
+        return tube, desc, meshgen.fourier_waveform(0)
     if name == "c1":
         tube = meshgen.straight_cylinder_1280()
         desc = ("straight cylinder 1,280 tricubic elements (4x4 core + 16-cell ring) x 40 layers, "
@@ -230,7 +235,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2-100"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
     ap.add_argument("--ref-budget", type=float, default=25.0)
@@ -259,7 +264,7 @@ def main():
     n = tube.mesh.nodes
     mesh = api.Mesh(tube.mesh)
     amg = args.preconditioner == "amg"
-    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT if args.workload == "c2" else 1e-3,
+    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=1e-3 if args.workload == "c1" else DT,
                           nonlinear_rtol=1e-8, nonlinear_atol=1e-300, mass_rtol=1e-3,
                           gmres_restart=200, gmres_max_iterations=5000, gmres_rtol=1e-8,
                           preconditioner=api.AMG if amg else api.BLOCK_JACOBI)
