@@ -88,7 +88,16 @@ typedef struct tfiga_ns_params {
 	 * TFIGA_PRECONDITIONER_AMG: flexible GMRES right-preconditioned by one
 	 * point-block aggregation AMG V-cycle, tolerance on the true residual. */
 	int32_t preconditioner;        /* default TFIGA_PRECONDITIONER_BLOCK_JACOBI */
+	/* TFIGA_PRECISION_FP64: every array and operation in FP64 (the reference's precision).
+	 * TFIGA_PRECISION_MIXED: FP64 nonlinear residual, Newton update and Krylov vectors;
+	 * the Jacobian is contracted in reduced precision and stored in FP32 for SpMV and the
+	 * preconditioner, with FGMRES true-residual restarts acting as FP64 iterative refinement
+	 * (requires TFIGA_PRECONDITIONER_AMG). */
+	int32_t precision;             /* default TFIGA_PRECISION_FP64 */
 } tfiga_ns_params;
+
+#define TFIGA_PRECISION_FP64 0
+#define TFIGA_PRECISION_MIXED 1
 
 #define TFIGA_PRECONDITIONER_BLOCK_JACOBI 0
 #define TFIGA_PRECONDITIONER_AMG 1

@@ -20,7 +20,7 @@ struct Amg::Level {
 	DeviceArray<int32_t> agg, agg_order, agg_offsets, gal_order, gal_offsets, block_row;
 	// coarsest level
 	int dense_n = 0;
-	DeviceArray<double> dense;
+	DeviceArray<double> dense, column;
 	DeviceArray<int> dense_flag;
 	DevicePatternView view() const { return {nodes, blocks, rows.get(), cols.get(), diag.get()}; }
 };
@@ -31,30 +31,46 @@ constexpr int kThreads = 256;
 
 unsigned Grid(long long n, int per) { return (unsigned)((n+per-1)/per); }
 
-__global__ void StrengthKernel(long long blocks, const double* __restrict__ values, double* __restrict__ s)
+template <class T>
+__global__ void StrengthKernel(long long blocks, const T* __restrict__ values, double* __restrict__ s)
 {
 	const long long b = (long long)blockIdx.x*blockDim.x+threadIdx.x;
 	if (b >= blocks) return;
-	const double* v = values+b*16;
-	s[b] = fabs(v[0])+fabs(v[5])+fabs(v[10]);
+	const T* v = values+b*16;
+	s[b] = fabs((double)v[0])+fabs((double)v[5])+fabs((double)v[10]);
 }
 
-// Coarse block = masked sum of its fine blocks, one thread per (coarse block, entry).
-__global__ void GalerkinKernel(long long coarse_blocks, const int32_t* __restrict__ order,
+// Coarse block = masked sum of its fine blocks: one CTA per coarse block, each
+// thread accumulating a strided subset of the fine blocks, then a fixed-order
+// reduction in shared memory (deterministic).
+template <class T>
+__global__ void __launch_bounds__(128) GalerkinKernel(long long coarse_blocks, const int32_t* __restrict__ order,
 	const int32_t* __restrict__ offsets, const int32_t* __restrict__ block_row, const int32_t* __restrict__ fine_cols,
-	const double* __restrict__ fine_mask, const double* __restrict__ fine_values, double* __restrict__ coarse_values)
+	const double* __restrict__ fine_mask, const T* __restrict__ fine_values, double* __restrict__ coarse_values)
 {
-	const long long t = (long long)blockIdx.x*blockDim.x+threadIdx.x;
-	if (t >= coarse_blocks*16) return;
-	const long long B = t >> 4;
-	const int e = (int)(t & 15), r = e >> 2, c = e & 3;
-	double sum = 0.0;
-	for (int k = offsets[B]; k < offsets[B+1]; ++k) {
+	const long long B = blockIdx.x;
+	double acc[16];
+	#pragma unroll
+	for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+	for (int k = offsets[B]+threadIdx.x; k < offsets[B+1]; k += blockDim.x) {
 		const int fb = order[k];
-		const double m = fine_mask[4*(size_t)block_row[fb]+r]*fine_mask[4*(size_t)fine_cols[fb]+c];
-		sum += m*fine_values[(size_t)fb*16+e];
+		const double* mr = fine_mask+4*(size_t)block_row[fb];
+		const double* mc = fine_mask+4*(size_t)fine_cols[fb];
+		const T* v = fine_values+(size_t)fb*16;
+		#pragma unroll
+		for (int e = 0; e < 16; ++e) acc[e] += mr[e >> 2]*mc[e & 3]*(double)v[e];
 	}
-	coarse_values[t] = sum;
+	__shared__ double red[16][129];
+	#pragma unroll
+	for (int e = 0; e < 16; ++e) red[e][threadIdx.x] = acc[e];
+	__syncthreads();
+	for (int stride = 64; stride > 0; stride >>= 1) {
+		if ((int)threadIdx.x < stride)
+			#pragma unroll
+			for (int e = 0; e < 16; ++e) red[e][threadIdx.x] += red[e][threadIdx.x+stride];
+		__syncthreads();
+	}
+	if (threadIdx.x < 16) coarse_values[B*16+threadIdx.x] = red[threadIdx.x][0];
 }
 
 // Masked-out coarse DOFs are decoupled: unit diagonal.
@@ -68,7 +84,25 @@ __global__ void UnitDiagonalKernel(int nodes, const int32_t* __restrict__ diag, 
 }
 
 // r = b - A x (warp per block row); x may be null (r = b).
-__global__ void __launch_bounds__(256) ResidualKernel(DevicePatternView p, const double* __restrict__ values,
+template <class T> struct RowLoad;
+template <> struct RowLoad<double> {
+	static __device__ __forceinline__ void Get(const double* v, long long k, int r, double a[4])
+	{
+		const double2* p = reinterpret_cast<const double2*>(v+(size_t)k*16+r*4);
+		const double2 a01 = __ldg(p), a23 = __ldg(p+1);
+		a[0] = a01.x; a[1] = a01.y; a[2] = a23.x; a[3] = a23.y;
+	}
+};
+template <> struct RowLoad<float> {
+	static __device__ __forceinline__ void Get(const float* v, long long k, int r, double a[4])
+	{
+		const float4 q = __ldg(reinterpret_cast<const float4*>(v+(size_t)k*16+r*4));
+		a[0] = q.x; a[1] = q.y; a[2] = q.z; a[3] = q.w;
+	}
+};
+
+template <class T>
+__global__ void __launch_bounds__(256) ResidualKernel(DevicePatternView p, const T* __restrict__ values,
 	const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ r, const int* __restrict__ stop)
 {
 	if (*stop) return;
@@ -78,12 +112,12 @@ __global__ void __launch_bounds__(256) ResidualKernel(DevicePatternView p, const
 	const int rr = lane & 3, slot = lane >> 2;
 	double sum = 0.0;
 	for (int k = p.row_offsets[row]+slot; k < p.row_offsets[row+1]; k += 8) {
-		const double2* a = reinterpret_cast<const double2*>(values+(size_t)k*16+rr*4);
-		const double2 a01 = __ldg(a), a23 = __ldg(a+1);
+		double a[4];
+		RowLoad<T>::Get(values, k, rr, a);
 		const double2* xv = reinterpret_cast<const double2*>(x+4*(size_t)p.columns[k]);
 		const double2 x01 = __ldg(xv), x23 = __ldg(xv+1);
-		sum = fma(a01.x, x01.x, sum); sum = fma(a01.y, x01.y, sum);
-		sum = fma(a23.x, x23.x, sum); sum = fma(a23.y, x23.y, sum);
+		sum = fma(a[0], x01.x, sum); sum = fma(a[1], x01.y, sum);
+		sum = fma(a[2], x23.x, sum); sum = fma(a[3], x23.y, sum);
 	}
 	sum += __shfl_xor_sync(0xffffffffu, sum, 4);
 	sum += __shfl_xor_sync(0xffffffffu, sum, 8);
@@ -106,20 +140,30 @@ __global__ void JacobiKernel(int nodes, const double* __restrict__ inverse, cons
 	x[i] = accumulate ? x[i]+z : z;
 }
 
-// b_c[I,c] = sum_{i in I} mask_i[c] r[i,c] (fine nodes grouped by aggregate).
-__global__ void RestrictKernel(int coarse_nodes, const int32_t* __restrict__ order, const int32_t* __restrict__ offsets,
-	const double* __restrict__ mask, const double* __restrict__ r, double* __restrict__ bc, const int* __restrict__ stop)
+// b_c[I,c] = sum_{i in I} mask_i[c] r[i,c]: one CTA per aggregate, fixed-order reduction.
+__global__ void __launch_bounds__(128) RestrictKernel(int coarse_nodes, const int32_t* __restrict__ order,
+	const int32_t* __restrict__ offsets, const double* __restrict__ mask, const double* __restrict__ r,
+	double* __restrict__ bc, const int* __restrict__ stop)
 {
 	if (*stop) return;
-	const int t = blockIdx.x*blockDim.x+threadIdx.x;
-	if (t >= 4*coarse_nodes) return;
-	const int I = t >> 2, c = t & 3;
-	double sum = 0.0;
-	for (int k = offsets[I]; k < offsets[I+1]; ++k) {
+	const int I = blockIdx.x;
+	double acc[4] = {0.0, 0.0, 0.0, 0.0};
+	for (int k = offsets[I]+threadIdx.x; k < offsets[I+1]; k += blockDim.x) {
 		const size_t i = (size_t)order[k];
-		sum += mask[4*i+c]*r[4*i+c];
+		const double2* m = reinterpret_cast<const double2*>(mask+4*i);
+		const double2* v = reinterpret_cast<const double2*>(r+4*i);
+		const double2 m01 = m[0], m23 = m[1], v01 = v[0], v23 = v[1];
+		acc[0] += m01.x*v01.x; acc[1] += m01.y*v01.y; acc[2] += m23.x*v23.x; acc[3] += m23.y*v23.y;
 	}
-	bc[t] = sum;
+	__shared__ double red[4][129];
+	for (int c = 0; c < 4; ++c) red[c][threadIdx.x] = acc[c];
+	__syncthreads();
+	for (int stride = 64; stride > 0; stride >>= 1) {
+		if ((int)threadIdx.x < stride)
+			for (int c = 0; c < 4; ++c) red[c][threadIdx.x] += red[c][threadIdx.x+stride];
+		__syncthreads();
+	}
+	if (threadIdx.x < 4) bc[4*I+threadIdx.x] = red[threadIdx.x][0];
 }
 
 // x[i,c] = mask_i[c] x_c[agg(i), c] (piecewise-constant prolongation).
@@ -148,65 +192,74 @@ __global__ void DenseScatterKernel(DevicePatternView p, const double* __restrict
 	dense[row*(size_t)(2*n)+col] = values[t];
 }
 
-// In-place Gauss-Jordan inverse with partial pivoting on [A | I] (n x 2n), one CTA.
-__global__ void __launch_bounds__(1024) DenseInverseKernel(int n, double* __restrict__ a, int* __restrict__ flag)
+// Gauss-Jordan inverse with partial pivoting on the augmented [A | I] (n x 2n,
+// row-major), one pivot per pair of launches so every step uses the whole GPU:
+// GaussJordanPivotKernel (one CTA) selects and swaps the pivot row, scales it
+// and saves column k; GaussJordanEliminateKernel (grid) removes column k from
+// every other row.  A vanishing pivot decouples its unknown (unit row) and
+// raises *flag.
+__global__ void AugmentIdentityKernel(int n, double* __restrict__ a)
+{
+	const long long t = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (t >= (long long)n*n) return;
+	const int i = (int)(t/n), j = (int)(t%n);
+	a[(size_t)i*(2*n)+n+j] = i == j ? 1.0 : 0.0;
+}
+
+__global__ void __launch_bounds__(1024) GaussJordanPivotKernel(int n, int k, double* __restrict__ a,
+	double* __restrict__ column, int* __restrict__ flag)
 {
 	const int ld = 2*n;
 	__shared__ double best_val[32];
 	__shared__ int best_idx[32];
 	__shared__ int pivot_row;
-	for (int i = threadIdx.x; i < n; i += blockDim.x)
-		for (int j = 0; j < n; ++j) a[(size_t)i*ld+n+j] = i == j ? 1.0 : 0.0;
-	__syncthreads();
-	for (int k = 0; k < n; ++k) {
-		double bv = -1.0; int bi = k;
-		for (int i = k+threadIdx.x; i < n; i += blockDim.x) {
-			const double v = fabs(a[(size_t)i*ld+k]);
-			if (v > bv) { bv = v; bi = i; }
-		}
-		for (int o = 16; o > 0; o >>= 1) {
-			const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-			const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-			if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-		}
-		if ((threadIdx.x & 31) == 0) { best_val[threadIdx.x >> 5] = bv; best_idx[threadIdx.x >> 5] = bi; }
-		__syncthreads();
-		if (threadIdx.x == 0) {
-			double v = -1.0; int idx = k;
-			for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
-				if (best_val[w] > v) { v = best_val[w]; idx = best_idx[w]; }
-			pivot_row = idx;
-			if (!(v > 1e-300)) { *flag = 1; pivot_row = -1; }
-		}
-		__syncthreads();
-		const int pr = pivot_row;
-		if (pr < 0) {
-			// singular column: decouple it (unit pivot) and continue
-			for (int j = threadIdx.x; j < ld; j += blockDim.x) a[(size_t)k*ld+j] = j == k || j == n+k ? 1.0 : 0.0;
-			__syncthreads();
-		} else if (pr != k) {
-			for (int j = threadIdx.x; j < ld; j += blockDim.x) {
-				const double t = a[(size_t)k*ld+j];
-				a[(size_t)k*ld+j] = a[(size_t)pr*ld+j];
-				a[(size_t)pr*ld+j] = t;
-			}
-			__syncthreads();
-		}
-		const double inv = 1.0/a[(size_t)k*ld+k];
-		__syncthreads();
-		for (int j = threadIdx.x; j < ld; j += blockDim.x) a[(size_t)k*ld+j] *= inv;
-		__syncthreads();
-		for (int idx = threadIdx.x; idx < n*ld; idx += blockDim.x) {
-			const int i = idx/ld, j = idx%ld;
-			if (i == k) continue;
-			const double f = a[(size_t)i*ld+k];
-			if (j != k && f != 0.0) a[(size_t)i*ld+j] -= f*a[(size_t)k*ld+j];
-		}
-		__syncthreads();
-		for (int i = threadIdx.x; i < n; i += blockDim.x)
-			if (i != k) a[(size_t)i*ld+k] = 0.0;
-		__syncthreads();
+	__shared__ double pivot_inv;
+	double bv = -1.0; int bi = k;
+	for (int i = k+threadIdx.x; i < n; i += blockDim.x) {
+		const double v = fabs(a[(size_t)i*ld+k]);
+		if (v > bv) { bv = v; bi = i; }
 	}
+	for (int o = 16; o > 0; o >>= 1) {
+		const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+		const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+		if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+	}
+	if ((threadIdx.x & 31) == 0) { best_val[threadIdx.x >> 5] = bv; best_idx[threadIdx.x >> 5] = bi; }
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double v = -1.0; int idx = k;
+		for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+			if (best_val[w] > v) { v = best_val[w]; idx = best_idx[w]; }
+		pivot_row = (v > 1e-300) ? idx : -1;
+		if (pivot_row < 0) *flag = 1;
+	}
+	__syncthreads();
+	const int pr = pivot_row;
+	if (pr < 0) {
+		for (int j = threadIdx.x; j < ld; j += blockDim.x) a[(size_t)k*ld+j] = (j == k || j == n+k) ? 1.0 : 0.0;
+	} else if (pr != k) {
+		for (int j = threadIdx.x; j < ld; j += blockDim.x) {
+			const double t = a[(size_t)k*ld+j];
+			a[(size_t)k*ld+j] = a[(size_t)pr*ld+j];
+			a[(size_t)pr*ld+j] = t;
+		}
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) pivot_inv = 1.0/a[(size_t)k*ld+k];
+	__syncthreads();
+	for (int j = threadIdx.x; j < ld; j += blockDim.x) a[(size_t)k*ld+j] *= pivot_inv;
+	for (int i = threadIdx.x; i < n; i += blockDim.x) column[i] = i == k ? 0.0 : a[(size_t)i*ld+k];
+}
+
+__global__ void GaussJordanEliminateKernel(int n, int k, double* __restrict__ a, const double* __restrict__ column)
+{
+	const int ld = 2*n;
+	const long long t = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (t >= (long long)n*ld) return;
+	const int i = (int)(t/ld), j = (int)(t%ld);
+	const double f = column[i];
+	if (f == 0.0) return;
+	a[(size_t)i*ld+j] = j == k ? 0.0 : a[(size_t)i*ld+j]-f*a[(size_t)k*ld+j];
 }
 
 // x = A^{-1} b with the inverse in the right half of the augmented matrix; warp per row.
@@ -303,7 +356,24 @@ std::vector<int32_t> Aggregate(int nodes, const std::vector<int32_t>& rows, cons
 
 } // namespace
 
-void Amg::Build(const double* values)
+template <class T>
+void Amg::Build(const T* values)
+{
+	std::vector<double> s(fine_.blocks);
+	{
+		DeviceArray<double> ds(fine_.blocks);
+		StrengthKernel<T><<<Grid(fine_.blocks, 256), 256, 0, stream_>>>(fine_.blocks, values, ds.get());
+		LaunchCheck("StrengthKernel");
+		ds.Download(s.data(), s.size(), stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "AMG strength");
+	}
+	BuildFromStrength(std::move(s));
+}
+
+template void Amg::Build<double>(const double*);
+template void Amg::Build<float>(const float*);
+
+void Amg::BuildFromStrength(std::vector<double> s)
 {
 	levels_.clear();
 	auto fine = std::make_unique<Level>();
@@ -315,15 +385,6 @@ void Amg::Build(const double* values)
 	for (int i = 0; i < fine_.nodes; ++i) {
 		const auto it = std::lower_bound(fine_columns_.begin()+fine_rows_[i], fine_columns_.begin()+fine_rows_[i+1], i);
 		fine->h_diag[i] = (int32_t)(it-fine_columns_.begin());
-	}
-	// strength of the fine operator
-	std::vector<double> s(fine_.blocks);
-	{
-		DeviceArray<double> ds(fine_.blocks);
-		StrengthKernel<<<Grid(fine_.blocks, 256), 256, 0, stream_>>>(fine_.blocks, values, ds.get());
-		LaunchCheck("StrengthKernel");
-		ds.Download(s.data(), s.size(), stream_);
-		CudaCheck(cudaStreamSynchronize(stream_), "AMG strength");
 	}
 	// Aggregate the strength graph repeatedly (aggregates of aggregates) until the
 	// coarse space is small enough for a dense solve; compose the maps.
@@ -421,6 +482,7 @@ void Amg::Build(const double* values)
 		if (l+1 == levels_.size()) {
 			V.dense_n = 4*V.nodes;
 			V.dense.Allocate((size_t)V.dense_n*2*V.dense_n);
+			V.column.Allocate((size_t)V.dense_n);
 			V.dense_flag.Allocate(1);
 		}
 	}
@@ -429,10 +491,10 @@ void Amg::Build(const double* values)
 	masks_dirty_ = true;
 }
 
-void Amg::Refresh(const double* values)
+template <class T>
+void Amg::Refresh(const T* values)
 {
 	if (!built_) Fail(-1, "AMG hierarchy has not been built");
-	fine_values_ = values;
 	if (masks_dirty_) {
 		std::vector<double> m(4*(size_t)levels_[0]->nodes, 1.0);
 		if (!vmask_.empty())
@@ -458,9 +520,12 @@ void Amg::Refresh(const double* values)
 	for (size_t l = 0; l+1 < levels_.size(); ++l) {
 		Level& L = *levels_[l];
 		Level& C = *levels_[l+1];
-		const double* fv = l == 0 ? values : L.values.get();
-		GalerkinKernel<<<Grid(C.blocks*16, 256), 256, 0, stream_>>>(C.blocks, L.gal_order.get(), L.gal_offsets.get(),
-			L.block_row.get(), L.cols.get(), L.mask.get(), fv, C.values.get());
+		if (l == 0)
+			GalerkinKernel<T><<<(unsigned)C.blocks, 128, 0, stream_>>>(C.blocks, L.gal_order.get(),
+				L.gal_offsets.get(), L.block_row.get(), L.cols.get(), L.mask.get(), values, C.values.get());
+		else
+			GalerkinKernel<double><<<(unsigned)C.blocks, 128, 0, stream_>>>(C.blocks, L.gal_order.get(),
+				L.gal_offsets.get(), L.block_row.get(), L.cols.get(), L.mask.get(), L.values.get(), C.values.get());
 		LaunchCheck("GalerkinKernel");
 		UnitDiagonalKernel<<<Grid(4LL*C.nodes, 256), 256, 0, stream_>>>(C.nodes, C.diag.get(), C.mask.get(),
 			C.values.get());
@@ -470,48 +535,61 @@ void Amg::Refresh(const double* values)
 	for (size_t l = 0; l+1 < levels_.size(); ++l) {
 		Level& L = *levels_[l];
 		L.singular.Zero(stream_);
-		LaunchBlockInverse(L.view(), l == 0 ? values : L.values.get(), L.inverse.get(), L.singular.get(), stream_);
+		if (l == 0) LaunchBlockInverse<T>(L.view(), values, L.inverse.get(), L.singular.get(), stream_);
+		else LaunchBlockInverse<double>(L.view(), L.values.get(), L.inverse.get(), L.singular.get(), stream_);
 		launches_ += 1;
 	}
 	Level& Z = *levels_.back();
 	if (Z.dense_n == 0) return;
-	const double* zv = levels_.size() == 1 ? values : Z.values.get();
 	Z.dense.Zero(stream_);
 	Z.dense_flag.Zero(stream_);
-	DenseScatterKernel<<<Grid(Z.blocks*16, 256), 256, 0, stream_>>>(Z.view(), zv, Z.dense_n, Z.dense.get());
+	DenseScatterKernel<<<Grid(Z.blocks*16, 256), 256, 0, stream_>>>(Z.view(), Z.values.get(), Z.dense_n, Z.dense.get());
 	LaunchCheck("DenseScatterKernel");
-	DenseInverseKernel<<<1, 1024, 0, stream_>>>(Z.dense_n, Z.dense.get(), Z.dense_flag.get());
-	LaunchCheck("DenseInverseKernel");
-	launches_ += 2;
+	const int dn = Z.dense_n;
+	AugmentIdentityKernel<<<Grid((long long)dn*dn, 256), 256, 0, stream_>>>(dn, Z.dense.get());
+	LaunchCheck("AugmentIdentityKernel");
+	for (int k = 0; k < dn; ++k) {
+		GaussJordanPivotKernel<<<1, 1024, 0, stream_>>>(dn, k, Z.dense.get(), Z.column.get(), Z.dense_flag.get());
+		GaussJordanEliminateKernel<<<Grid((long long)dn*2*dn, 256), 256, 0, stream_>>>(dn, k, Z.dense.get(),
+			Z.column.get());
+	}
+	LaunchCheck("GaussJordanEliminateKernel");
+	launches_ += 2+2LL*dn;
 }
 
-void Amg::Cycle(int l, const double* b, double* x, const int* stop)
+template void Amg::Refresh<double>(const double*);
+template void Amg::Refresh<float>(const float*);
+
+template <class T>
+void Amg::Cycle(int l, const T* A, const double* b, double* x, const int* stop)
 {
 	// Two-level: x = P Ac^{-1} P^T b, then x += D^{-1} (b - A x).
 	Level& L = *levels_[l];
 	Level& C = *levels_[l+1];
-	const double* A = fine_values_;
 	const long long n4 = 4LL*L.nodes;
-	RestrictKernel<<<Grid(4LL*C.nodes, 256), 256, 0, stream_>>>(C.nodes, L.agg_order.get(), L.agg_offsets.get(),
+	RestrictKernel<<<C.nodes, 128, 0, stream_>>>(C.nodes, L.agg_order.get(), L.agg_offsets.get(),
 		L.mask.get(), b, C.b.get(), stop);
 	LaunchCheck("RestrictKernel");
 	DenseApplyKernel<<<Grid(C.dense_n, 8), 256, 0, stream_>>>(C.dense_n, C.dense.get(), C.b.get(), C.x.get(), stop);
 	LaunchCheck("DenseApplyKernel");
 	ProlongKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(), C.x.get(), x, stop);
 	LaunchCheck("ProlongKernel");
-	ResidualKernel<<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
+	ResidualKernel<T><<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
 	LaunchCheck("ResidualKernel");
 	JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), L.r.get(), x, options_.omega, 1, stop);
 	LaunchCheck("JacobiKernel");
 	launches_ += 5;
 }
 
-void Amg::Apply(const double* fine_values, const double* v, double* z, const int* stop)
+template <class T>
+void Amg::Apply(const T* fine_values, const double* v, double* z, const int* stop)
 {
-	fine_values_ = fine_values;
 	if (profiler_) profiler_->Begin(Profiler::kOther, stream_);
-	Cycle(0, v, z, stop);
+	Cycle<T>(0, fine_values, v, z, stop);
 	if (profiler_) profiler_->End(stream_);
 }
+
+template void Amg::Apply<double>(const double*, const double*, double*, const int*);
+template void Amg::Apply<float>(const float*, const double*, double*, const int*);
 
 } // namespace tfiga

@@ -42,15 +42,15 @@ public:
 	Amg(const Amg&) = delete;
 	Amg& operator=(const Amg&) = delete;
 
-	// Builds the hierarchy from the strength of `values` (device, fine level); masks: 1 = free DOF.
-	void Build(const double* values);
+	// Builds the hierarchy from the strength of `values` (device, fine level, FP64 or FP32).
+	template <class T> void Build(const T* values);
 	bool built() const { return built_; }
 	// Dirichlet masks of the fine level (velocity / pressure constrained per node).
 	void SetMasks(const std::vector<int32_t>& velocity_mask, const std::vector<int32_t>& pressure_mask);
-	// Galerkin refresh of every coarse operator + smoother inverses from the fine values.
-	void Refresh(const double* values);
-	// z = M^{-1} v (one V-cycle); kernels skip when *stop is set.
-	void Apply(const double* fine_values, const double* v, double* z, const int* stop);
+	// Galerkin refresh of the coarse operator and the fine block-Jacobi inverses from the fine values.
+	template <class T> void Refresh(const T* values);
+	// z = M^{-1} v; kernels skip when *stop is set.
+	template <class T> void Apply(const T* fine_values, const double* v, double* z, const int* stop);
 	int levels() const { return (int)levels_.size(); }
 	std::vector<int> level_nodes() const;
 	const std::vector<int>& aggregation_rounds() const { return coarse_history_; }
@@ -60,7 +60,8 @@ public:
 
 private:
 	struct Level;
-	void Cycle(int level, const double* b, double* x, const int* stop);
+	template <class T> void Cycle(int level, const T* fine, const double* b, double* x, const int* stop);
+	void BuildFromStrength(std::vector<double> s);
 	std::vector<std::unique_ptr<Level>> levels_;
 	DevicePatternView fine_;
 	std::vector<int32_t> fine_rows_, fine_columns_;
@@ -72,7 +73,7 @@ private:
 	bool masks_dirty_ = true;
 	long long launches_ = 0;
 	Profiler* profiler_ = nullptr;
-	const double* fine_values_ = nullptr;
+
 };
 
 } // namespace tfiga

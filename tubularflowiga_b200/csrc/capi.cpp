@@ -163,6 +163,7 @@ void tfiga_ns_default_params(tfiga_ns_params* p)
 	p->gmres_max_iterations = 5000;
 	p->gmres_rtol = 1e-8;
 	p->preconditioner = TFIGA_PRECONDITIONER_BLOCK_JACOBI;
+	p->precision = TFIGA_PRECISION_FP64;
 }
 
 int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out)
@@ -239,8 +240,7 @@ int tfiga_ns_assemble(tfiga_ns* ns, double* values, double* rhs)
 		Require(ns != nullptr, "null handle");
 		auto& s = *ns->solver;
 		s.Assemble();
-		if (values) tfiga::CudaCheck(cudaMemcpyAsync(values, s.values(), (size_t)s.blocks()*16*sizeof(double),
-			cudaMemcpyDeviceToHost, s.stream()), "download values");
+		if (values) s.DownloadValues(values);
 		if (rhs) tfiga::CudaCheck(cudaMemcpyAsync(rhs, s.rhs(), (size_t)s.nodes()*4*sizeof(double),
 			cudaMemcpyDeviceToHost, s.stream()), "download rhs");
 		s.Synchronize();
@@ -253,8 +253,7 @@ int tfiga_ns_apply_dirichlet(tfiga_ns* ns, double* values, double* rhs)
 		Require(ns != nullptr, "null handle");
 		auto& s = *ns->solver;
 		s.ApplyDirichlet();
-		if (values) tfiga::CudaCheck(cudaMemcpyAsync(values, s.values(), (size_t)s.blocks()*16*sizeof(double),
-			cudaMemcpyDeviceToHost, s.stream()), "download values");
+		if (values) s.DownloadValues(values);
 		if (rhs) tfiga::CudaCheck(cudaMemcpyAsync(rhs, s.rhs(), (size_t)s.nodes()*4*sizeof(double),
 			cudaMemcpyDeviceToHost, s.stream()), "download rhs");
 		s.Synchronize();

@@ -43,7 +43,8 @@ __global__ void __launch_bounds__(kThreads) DotFinalizeKernel(const double* __re
 {
 	if (*stop) return;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	for (int i = warp; i < count; i += kThreads/32) {
+	const int i = blockIdx.x*(kThreads/32)+warp;   // a warp per basis vector, spread over CTAs
+	if (i < count) {
 		double s = 0.0;
 		for (int b = lane; b < blocks; b += 32) s += partial[(size_t)i*blocks+b];
 		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -89,37 +90,47 @@ __global__ void __launch_bounds__(kThreads) UpdateKernel(const double* __restric
 }
 
 // Column j of the Hessenberg matrix: norm, previous rotations, new rotation,
-// residual estimate (Gmres.hpp:272-305).  One warp; lane 0 is sequential.
+// residual estimate (Gmres.hpp:272-305).  One warp stages the column and the
+// rotations in shared memory; lane 0 then applies the rotations sequentially.
 __global__ void ArnoldiFinalizeKernel(const double* __restrict__ norm_partial, int blocks, double* __restrict__ H,
 	int restart, int j, double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
 	double* __restrict__ scale, int* __restrict__ state, double* __restrict__ residual, double tolerance)
 {
+	extern __shared__ double sh[];
+	double* col = sh;                 // [restart+1]
+	double* c = col+restart+1;        // [restart]
+	double* s_ = c+restart;           // [restart]
 	if (state[0]) return;
 	double s = 0.0;
 	for (int b = threadIdx.x; b < blocks; b += 32) s += norm_partial[b];
 	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-	if (threadIdx.x != 0) return;
 	const double next = sqrt(s);
-	H[(size_t)(j+1)*restart+j] = next;
-	scale[j+1] = next > 1e-30 ? 1.0/next : 0.0;
-	for (int i = 0; i < j; ++i) {
-		const double a = H[(size_t)i*restart+j], b = H[(size_t)(i+1)*restart+j];
-		H[(size_t)i*restart+j] = cs[i]*a+sn[i]*b;
-		H[(size_t)(i+1)*restart+j] = -sn[i]*a+cs[i]*b;
+	for (int i = threadIdx.x; i <= j; i += 32) col[i] = H[(size_t)i*restart+j];
+	for (int i = threadIdx.x; i < j; i += 32) { c[i] = cs[i]; s_[i] = sn[i]; }
+	__syncwarp();
+	if (threadIdx.x == 0) {
+		col[j+1] = next;
+		for (int i = 0; i < j; ++i) {
+			const double a = col[i], b = col[i+1];
+			col[i] = c[i]*a+s_[i]*b;
+			col[i+1] = -s_[i]*a+c[i]*b;
+		}
+		const double a = col[j], b = col[j+1];
+		const double mag = hypot(a, b);
+		const double cj = mag > 0.0 ? a/mag : 1.0, sj = mag > 0.0 ? b/mag : 0.0;
+		cs[j] = cj; sn[j] = sj;
+		col[j] = mag; col[j+1] = 0.0;
+		const double old = g[j];
+		g[j] = cj*old;
+		g[j+1] = -sj*old;
+		const double res = fabs(g[j+1]);
+		residual[0] = res;
+		scale[j+1] = next > 1e-30 ? 1.0/next : 0.0;
+		state[1] = j+1;
+		if (res <= tolerance || next <= 1e-30) state[0] = 1;
 	}
-	const double a = H[(size_t)j*restart+j], b = H[(size_t)(j+1)*restart+j];
-	const double mag = hypot(a, b);
-	cs[j] = mag > 0.0 ? a/mag : 1.0;
-	sn[j] = mag > 0.0 ? b/mag : 0.0;
-	H[(size_t)j*restart+j] = mag;
-	H[(size_t)(j+1)*restart+j] = 0.0;
-	const double old = g[j];
-	g[j] = cs[j]*old;
-	g[j+1] = -sn[j]*old;
-	const double res = fabs(g[j+1]);
-	residual[0] = res;
-	state[1] = j+1;
-	if (res <= tolerance || next <= 1e-30) state[0] = 1;
+	__syncwarp();
+	for (int i = threadIdx.x; i <= j+1; i += 32) H[(size_t)i*restart+j] = col[i];
 }
 
 // Cycle start: g = beta e_0, scale_0 = 1/beta, flags cleared.
@@ -213,6 +224,10 @@ Gmres::Gmres(int nodes, int restart, cudaStream_t stream)
 			(int)((size_t)(restart+1)*sizeof(double))), "solution update shared memory");
 	}
 	if ((size_t)chunk_*sizeof(double) > 227*1024) Fail(-7, "GMRES vector too long for the multi-dot chunking");
+	finalize_smem_ = (size_t)(3*restart+1)*sizeof(double);
+	if (finalize_smem_ > 48*1024)
+		CudaCheck(cudaFuncSetAttribute(ArnoldiFinalizeKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)finalize_smem_), "Arnoldi finalize shared memory");
 }
 
 Gmres::~Gmres()
@@ -247,8 +262,8 @@ void Gmres::Orthogonalize(int j)
 		MultiDotKernel<<<blocks_, kThreads, dot_smem, stream_>>>(V_.get(), n_, scale_.get(), count, w_.get(),
 			partial_.get(), chunk_, stop);
 		LaunchCheck("MultiDotKernel");
-		DotFinalizeKernel<<<1, kThreads, 0, stream_>>>(partial_.get(), blocks_, count, hpass_.get(), H_.get(),
-			restart_, j, pass, stop);
+		DotFinalizeKernel<<<(count+kThreads/32-1)/(kThreads/32), kThreads, 0, stream_>>>(partial_.get(), blocks_,
+			count, hpass_.get(), H_.get(), restart_, j, pass, stop);
 		LaunchCheck("DotFinalizeKernel");
 		double* out = pass == 0 ? w_.get() : V_.get()+(size_t)(j+1)*n_;
 		UpdateKernel<<<blocks_, kThreads, coef_smem, stream_>>>(V_.get(), n_, scale_.get(), count, hpass_.get(),
@@ -259,7 +274,8 @@ void Gmres::Orthogonalize(int j)
 	launches_ += 7;
 }
 
-void Gmres::FlexibleStep(const DevicePatternView& pattern, const double* values, int j, Amg& M)
+template <class T>
+void Gmres::FlexibleStep(const DevicePatternView& pattern, const T* values, int j, Amg& M)
 {
 	const int* stop = state_.get();
 	ScaleCopyKernel<<<blocks_, kThreads, 0, stream_>>>(n_, V_.get()+(size_t)j*n_, scale_.get()+j, r_.get(), stop);
@@ -268,16 +284,17 @@ void Gmres::FlexibleStep(const DevicePatternView& pattern, const double* values,
 	double* z = Z_.get()+(size_t)j*n_;
 	M.Apply(values, r_.get(), z, stop);
 	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
-	LaunchSpmvBlockJacobi(pattern, values, nullptr, z, nullptr, w_.get(), stop, stream_);
+	LaunchSpmvBlockJacobi<T>(pattern, values, nullptr, z, nullptr, w_.get(), stop, stream_);
 	if (profiler_) profiler_->End(stream_);
 	launches_ += 1;
 	Orthogonalize(j);
 }
 
-double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const double* values, const double* rhs,
+template <class T>
+double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const T* values, const double* rhs,
 	const double* x)
 {
-	LaunchSpmv(pattern, values, x, tmp_.get(), stream_);
+	LaunchSpmv<T>(pattern, values, x, tmp_.get(), stream_);
 	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), V_.get());
 	LaunchCheck("ResidualKernel");
 	LaunchNorm(n_, V_.get(), norm_partial_.get(), scalar_.get(), stream_);
@@ -287,14 +304,15 @@ double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const double* 
 	return host_->beta[0];
 }
 
-GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const double* values, const double* rhs,
+template <class T>
+GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const T* values, const double* rhs,
 	double* x, double rtol, int max_iterations, Amg& M, long long* launches)
 {
 	launches_ = 0;
 	const long long amg0 = M.launches();
 	if (Z_.size() == 0) Z_.Allocate((size_t)(restart_+1)*n_);
 	GmresResult result;
-	double beta = TrueResidualPlain(pattern, values, rhs, x);
+	double beta = TrueResidualPlain<T>(pattern, values, rhs, x);
 	result.residual = beta;
 	if (!std::isfinite(beta)) Fail(-6, "FGMRES initial residual is not finite");
 	if (beta == 0.0) {
@@ -312,8 +330,8 @@ GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const double*
 		for (int j = 0; j < cap;) {
 			const int batch = std::min(kBatch, cap-j);
 			for (int b = 0; b < batch; ++b) {
-				FlexibleStep(pattern, values, j+b, M);
-				ArnoldiFinalizeKernel<<<1, 32, 0, stream_>>>(norm_partial_.get(), blocks_, H_.get(), restart_, j+b,
+				FlexibleStep<T>(pattern, values, j+b, M);
+				ArnoldiFinalizeKernel<<<1, 32, finalize_smem_, stream_>>>(norm_partial_.get(), blocks_, H_.get(), restart_, j+b,
 					cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance);
 				LaunchCheck("ArnoldiFinalizeKernel");
 				launches_ += 1;
@@ -332,7 +350,7 @@ GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const double*
 			nullptr, y_.get(), state_.get(), x);
 		LaunchCheck("SolutionUpdateKernel");
 		launches_ += 2;
-		beta = TrueResidualPlain(pattern, values, rhs, x);
+		beta = TrueResidualPlain<T>(pattern, values, rhs, x);
 		state_.Download(&host_->stop, 3, stream_);
 		CudaCheck(cudaStreamSynchronize(stream_), "FGMRES restart");
 		if (host_->error) Fail(-6, "FGMRES Hessenberg matrix is singular");
@@ -389,7 +407,7 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 			const int batch = std::min(kBatch, cap-j);
 			for (int b = 0; b < batch; ++b) {
 				Step(pattern, values, j+b);
-				ArnoldiFinalizeKernel<<<1, 32, 0, stream_>>>(norm_partial_.get(), blocks_, H_.get(), restart_, j+b,
+				ArnoldiFinalizeKernel<<<1, 32, finalize_smem_, stream_>>>(norm_partial_.get(), blocks_, H_.get(), restart_, j+b,
 					cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance);
 				LaunchCheck("ArnoldiFinalizeKernel");
 				launches_ += 1;
@@ -422,5 +440,10 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 	if (launches) *launches += launches_;
 	return result;
 }
+
+template GmresResult Gmres::SolveFlexible<double>(const DevicePatternView&, const double*, const double*, double*,
+	double, int, Amg&, long long*);
+template GmresResult Gmres::SolveFlexible<float>(const DevicePatternView&, const float*, const double*, double*,
+	double, int, Amg&, long long*);
 
 } // namespace tfiga

@@ -35,7 +35,9 @@ public:
 		double rtol, int max_iterations, long long* launches);
 	// Right-preconditioned flexible GMRES (FGMRES): z_j = M^{-1} v_j stored, tolerance
 	// rtol * ||b - A x0|| on the true residual.
-	GmresResult SolveFlexible(const DevicePatternView& pattern, const double* values, const double* rhs, double* x,
+	// The matrix may be stored in FP64 or FP32 (T); vectors, Hessenberg and Givens stay FP64.
+	template <class T>
+	GmresResult SolveFlexible(const DevicePatternView& pattern, const T* values, const double* rhs, double* x,
 		double rtol, int max_iterations, Amg& preconditioner, long long* launches);
 	int restart() const { return restart_; }
 	void set_profiler(Profiler* profiler) { profiler_ = profiler; }
@@ -44,12 +46,15 @@ public:
 private:
 	void Step(const DevicePatternView& pattern, const double* values, int j);
 	void Orthogonalize(int j);
-	void FlexibleStep(const DevicePatternView& pattern, const double* values, int j, Amg& preconditioner);
-	double TrueResidualPlain(const DevicePatternView& pattern, const double* values, const double* rhs, const double* x);
+	template <class T>
+	void FlexibleStep(const DevicePatternView& pattern, const T* values, int j, Amg& preconditioner);
+	template <class T>
+	double TrueResidualPlain(const DevicePatternView& pattern, const T* values, const double* rhs, const double* x);
 	double TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs, const double* x);
 
 	int nodes_, n_, restart_, blocks_;
 	int chunk_;
+	size_t finalize_smem_ = 0;
 	cudaStream_t stream_;
 	long long launches_ = 0;
 	DeviceArray<double> Z_;

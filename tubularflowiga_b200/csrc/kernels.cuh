@@ -59,18 +59,23 @@ void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double*
 	double* values, double* rhs, cudaStream_t stream);
 
 // ---- sparse.cu ----------------------------------------------------------
-void LaunchSpmv(const DevicePatternView& pattern, const double* values, const double* x, double* y,
-	cudaStream_t stream);
+// Matrix values are FP64 or FP32 (T = double / float); vectors are FP64.
+template <class T>
+void LaunchSpmv(const DevicePatternView& pattern, const T* values, const double* x, double* y, cudaStream_t stream);
 // y = D^{-1} (A (scale * x)) with D^{-1} stored per node as 4x4 (scale read from device, may be null);
 // inverse == null gives y = scale * A x.  Returns early when *stop is set (stop may be null).
-void LaunchSpmvBlockJacobi(const DevicePatternView& pattern, const double* values, const double* inverse,
+template <class T>
+void LaunchSpmvBlockJacobi(const DevicePatternView& pattern, const T* values, const double* inverse,
 	const double* x, const double* scale, double* y, const int* stop, cudaStream_t stream);
-void LaunchBlockInverse(const DevicePatternView& pattern, const double* values, double* inverse,
+template <class T>
+void LaunchBlockInverse(const DevicePatternView& pattern, const T* values, double* inverse,
 	unsigned int* singular, cudaStream_t stream);
+void LaunchToFloat(long long n, const double* in, float* out, cudaStream_t stream);
 void LaunchApplyBlockInverse(int nodes, const double* inverse, const double* x, double* y, cudaStream_t stream);
+template <class T>
 void LaunchDirichletRows(const DevicePatternView& pattern, int count, const int32_t* constrained_nodes,
 	const int32_t* velocity_mask, const int32_t* pressure_mask, const double* velocity, const double* pressure,
-	const double* state, double* values, double* rhs, cudaStream_t stream);
+	const double* state, T* values, double* rhs, cudaStream_t stream);
 void LaunchFaceFlows(int faces, const int32_t* face_element, const double* face_coef,
 	const int32_t* element_offsets, const int32_t* connectivity, const double* state, double* face_flow,
 	cudaStream_t stream);

@@ -67,6 +67,11 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 		"pinned scalars");
 	for (auto& ev : events_) CudaCheck(cudaEventCreate(&ev), "event");
 	gmres_.set_profiler(&profiler_);
+	if (params.precision != TFIGA_PRECISION_FP64 && params.precision != TFIGA_PRECISION_MIXED)
+		Fail(-1, "unknown precision "+std::to_string(params.precision));
+	if (mixed() && params.preconditioner != TFIGA_PRECONDITIONER_AMG)
+		Fail(-7, "mixed precision requires the AMG-preconditioned flexible GMRES");
+	if (mixed()) values32_.Allocate((size_t)blocks()*16);
 	if (params.preconditioner == TFIGA_PRECONDITIONER_AMG) {
 		amg_ = std::make_unique<Amg>(mesh.pattern_view(), mesh.pattern().row_offsets, mesh.pattern().columns, stream_);
 		amg_->set_profiler(&profiler_);
@@ -167,15 +172,26 @@ void NsSolver::Assemble()
 	profiler_.End(stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
 	launches_ += 2;
+	if (mixed()) {
+		LaunchToFloat((long long)blocks()*16, values_.get(), values32_.get(), stream_);
+		launches_ += 1;
+	}
 	// The AMG hierarchy is built once, from the strength of the first raw (pre-Dirichlet) Jacobian.
-	if (amg_ && !amg_->built()) amg_->Build(values_.get());
+	if (amg_ && !amg_->built()) {
+		if (mixed()) amg_->Build(values32_.get());
+		else amg_->Build(values_.get());
+	}
 }
 
 void NsSolver::ApplyDirichlet()
 {
 	if (!dirichlet_set_) Fail(-1, "Dirichlet conditions have not been set");
-	LaunchDirichletRows(mesh_.pattern_view(), constrained_count_, constrained_.get(), vmask_.get(), pmask_.get(),
-		velocity_bc_.get(), pressure_bc_.get(), state_.get(), values_.get(), rhs_.get(), stream_);
+	if (mixed())
+		LaunchDirichletRows<float>(mesh_.pattern_view(), constrained_count_, constrained_.get(), vmask_.get(),
+			pmask_.get(), velocity_bc_.get(), pressure_bc_.get(), state_.get(), values32_.get(), rhs_.get(), stream_);
+	else
+		LaunchDirichletRows<double>(mesh_.pattern_view(), constrained_count_, constrained_.get(), vmask_.get(),
+			pmask_.get(), velocity_bc_.get(), pressure_bc_.get(), state_.get(), values_.get(), rhs_.get(), stream_);
 	launches_ += 1;
 }
 
@@ -183,12 +199,22 @@ GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 {
 	update_.Zero(stream_);
 	if (amg_) {
-		if (!amg_->built()) amg_->Build(values_.get());
 		const long long before = amg_->launches();
-		amg_->Refresh(values_.get());
-		launches_ += amg_->launches()-before;
-		return gmres_.SolveFlexible(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol,
-			max_iterations, *amg_, &launches_);
+		GmresResult result;
+		if (mixed()) {
+			if (!amg_->built()) amg_->Build(values32_.get());
+			amg_->Refresh(values32_.get());
+			launches_ += amg_->launches()-before;
+			result = gmres_.SolveFlexible<float>(mesh_.pattern_view(), values32_.get(), rhs_.get(), update_.get(), rtol,
+				max_iterations, *amg_, &launches_);
+		} else {
+			if (!amg_->built()) amg_->Build(values_.get());
+			amg_->Refresh(values_.get());
+			launches_ += amg_->launches()-before;
+			result = gmres_.SolveFlexible<double>(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol,
+				max_iterations, *amg_, &launches_);
+		}
+		return result;
 	}
 	return gmres_.Solve(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol, max_iterations,
 		&launches_);
@@ -311,6 +337,20 @@ void NsSolver::BoundaryFlows(const int32_t* labels, int count, double* flows)
 	for (int i = 0; i < count; ++i) {
 		const auto it = slot_of_label_.find(labels[i]);
 		flows[i] = it == slot_of_label_.end() ? 0.0 : per_label[it->second];
+	}
+}
+
+void NsSolver::DownloadValues(double* out)
+{
+	const size_t count = (size_t)blocks()*16;
+	if (mixed()) {
+		std::vector<float> tmp(count);
+		values32_.Download(tmp.data(), count, stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "download values");
+		for (size_t i = 0; i < count; ++i) out[i] = tmp[i];
+	} else {
+		values_.Download(out, count, stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "download values");
 	}
 }
 

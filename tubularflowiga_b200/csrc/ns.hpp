@@ -40,6 +40,9 @@ public:
 	int64_t nodes() const { return mesh_.nodes(); }
 	long long blocks() const { return (long long)mesh_.pattern().columns.size(); }
 	double* values() { return values_.get(); }
+	bool mixed() const { return params_.precision == TFIGA_PRECISION_MIXED; }
+	// Active Jacobian values as FP64 on the host (FP32 storage is widened).
+	void DownloadValues(double* out);
 	double* state() { return state_.get(); }
 	double* rhs() { return rhs_.get(); }
 	double* update() { return update_.get(); }
@@ -65,6 +68,7 @@ private:
 	long long launches_ = 0;
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
+	DeviceArray<float> values32_;
 	DeviceArray<double> face_flow_, face_pressure_, label_flow_, partial_, scalars_;
 	DeviceArray<int32_t> vmask_, pmask_, constrained_, face_slot_;
 	std::vector<int32_t> labels_;            // distinct face labels (slot order)

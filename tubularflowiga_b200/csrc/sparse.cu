@@ -15,7 +15,27 @@ namespace {
 
 constexpr int kReduceBlocks = 296;   // 2 CTAs per SM for the partial-sum stage
 
-__device__ __forceinline__ double RowBlockDot(const DevicePatternView& p, const double* __restrict__ values,
+template <class T> struct BlockRow;
+template <> struct BlockRow<double> {
+	// row r of block b: 4 doubles (two 128-bit loads)
+	static __device__ __forceinline__ void Load(const double* values, long long b, int r, double a[4])
+	{
+		const double2* p = reinterpret_cast<const double2*>(values+(size_t)b*16+r*4);
+		const double2 a01 = __ldg(p), a23 = __ldg(p+1);
+		a[0] = a01.x; a[1] = a01.y; a[2] = a23.x; a[3] = a23.y;
+	}
+};
+template <> struct BlockRow<float> {
+	// row r of block b: 4 floats (one 128-bit load)
+	static __device__ __forceinline__ void Load(const float* values, long long b, int r, double a[4])
+	{
+		const float4 v = __ldg(reinterpret_cast<const float4*>(values+(size_t)b*16+r*4));
+		a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+	}
+};
+
+template <class T>
+__device__ __forceinline__ double RowBlockDot(const DevicePatternView& p, const T* __restrict__ values,
 	const double* __restrict__ x, int row, int lane)
 {
 	const int r = lane & 3, slot = lane >> 2;
@@ -23,12 +43,12 @@ __device__ __forceinline__ double RowBlockDot(const DevicePatternView& p, const 
 	const int lo = p.row_offsets[row], hi = p.row_offsets[row+1];
 	for (int b = lo+slot; b < hi; b += 8) {
 		const int col = p.columns[b];
-		const double2* a = reinterpret_cast<const double2*>(values+(size_t)b*16+r*4);
-		const double2 a01 = __ldg(a), a23 = __ldg(a+1);
+		double a[4];
+		BlockRow<T>::Load(values, b, r, a);
 		const double2* xv = reinterpret_cast<const double2*>(x+4*(size_t)col);
 		const double2 x01 = __ldg(xv), x23 = __ldg(xv+1);
-		sum = fma(a01.x, x01.x, sum); sum = fma(a01.y, x01.y, sum);
-		sum = fma(a23.x, x23.x, sum); sum = fma(a23.y, x23.y, sum);
+		sum = fma(a[0], x01.x, sum); sum = fma(a[1], x01.y, sum);
+		sum = fma(a[2], x23.x, sum); sum = fma(a[3], x23.y, sum);
 	}
 	sum += __shfl_xor_sync(0xffffffffu, sum, 4);
 	sum += __shfl_xor_sync(0xffffffffu, sum, 8);
@@ -36,7 +56,8 @@ __device__ __forceinline__ double RowBlockDot(const DevicePatternView& p, const 
 	return sum;   // lanes 0..3 hold rows 0..3
 }
 
-__global__ void __launch_bounds__(256) SpmvKernel(DevicePatternView p, const double* __restrict__ values,
+template <class T>
+__global__ void __launch_bounds__(256) SpmvKernel(DevicePatternView p, const T* __restrict__ values,
 	const double* __restrict__ x, double* __restrict__ y)
 {
 	const int row = blockIdx.x*8+(threadIdx.x >> 5);
@@ -46,7 +67,8 @@ __global__ void __launch_bounds__(256) SpmvKernel(DevicePatternView p, const dou
 	if (lane < 4) y[4*(size_t)row+lane] = sum;
 }
 
-__global__ void __launch_bounds__(256) SpmvBlockJacobiKernel(DevicePatternView p, const double* __restrict__ values,
+template <class T>
+__global__ void __launch_bounds__(256) SpmvBlockJacobiKernel(DevicePatternView p, const T* __restrict__ values,
 	const double* __restrict__ inverse, const double* __restrict__ x, const double* __restrict__ scale,
 	double* __restrict__ y, const int* __restrict__ stop)
 {
@@ -70,12 +92,13 @@ __global__ void __launch_bounds__(256) SpmvBlockJacobiKernel(DevicePatternView p
 
 // Gauss-Jordan with partial pivoting and the singular fallback of
 // BuildBlockInverseKernel (SparseKernels.cuh:42-89).
-__global__ void BlockInverseKernel(DevicePatternView p, const double* __restrict__ values,
+template <class T>
+__global__ void BlockInverseKernel(DevicePatternView p, const T* __restrict__ values,
 	double* __restrict__ inverse, unsigned int* __restrict__ singular)
 {
 	const int node = blockIdx.x*blockDim.x+threadIdx.x;
 	if (node >= p.nodes) return;
-	const double* s = values+(size_t)p.diagonal[node]*16;
+	const T* s = values+(size_t)p.diagonal[node]*16;
 	double m[4][8];
 	for (int i = 0; i < 4; ++i)
 		for (int j = 0; j < 8; ++j) m[i][j] = j < 4 ? s[i*4+j] : (j-4 == i ? 1.0 : 0.0);
@@ -119,9 +142,10 @@ __global__ void ApplyBlockInverseKernel(int nodes, const double* __restrict__ in
 }
 
 // Dirichlet rows (IgaCudaKernels.cuh:436-463): a warp per constrained node.
+template <class T>
 __global__ void DirichletRowsKernel(DevicePatternView p, int count, const int32_t* __restrict__ nodes,
 	const int32_t* __restrict__ vmask, const int32_t* __restrict__ pmask, const double* __restrict__ velocity,
-	const double* __restrict__ pressure, const double* __restrict__ state, double* __restrict__ values,
+	const double* __restrict__ pressure, const double* __restrict__ state, T* __restrict__ values,
 	double* __restrict__ rhs)
 {
 	const int item = blockIdx.x*(blockDim.x >> 5)+(threadIdx.x >> 5);
@@ -132,15 +156,15 @@ __global__ void DirichletRowsKernel(DevicePatternView p, int count, const int32_
 	if (values != nullptr) {
 		const int lo = p.row_offsets[node], hi = p.row_offsets[node+1];
 		for (int b = lo+lane; b < hi; b += 32) {
-			double* blk = values+(size_t)b*16;
-			if (cv) for (int k = 0; k < 12; ++k) blk[k] = 0.0;
-			if (cp) for (int k = 12; k < 16; ++k) blk[k] = 0.0;
+			T* blk = values+(size_t)b*16;
+			if (cv) for (int k = 0; k < 12; ++k) blk[k] = T(0);
+			if (cp) for (int k = 12; k < 16; ++k) blk[k] = T(0);
 		}
 		__syncwarp();
 		if (lane == 0) {
-			double* diag = values+(size_t)p.diagonal[node]*16;
-			if (cv) { diag[0] = 1.0; diag[5] = 1.0; diag[10] = 1.0; }
-			if (cp) diag[15] = 1.0;
+			T* diag = values+(size_t)p.diagonal[node]*16;
+			if (cv) { diag[0] = T(1); diag[5] = T(1); diag[10] = T(1); }
+			if (cp) diag[15] = T(1);
 		}
 	}
 	if (rhs != nullptr && lane < 4) {
@@ -253,31 +277,56 @@ __global__ void __launch_bounds__(256) SegmentSumKernel(const int32_t* __restric
 
 unsigned Blocks(long long n, int threads) { return (unsigned)((n+threads-1)/threads); }
 
+__global__ void ToFloatKernel(long long n, const double* __restrict__ in, float* __restrict__ out)
+{
+	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (i < n) out[i] = (float)in[i];
+}
+
 } // namespace
 
 int PartialSlots() { return 2*kReduceBlocks; }
 
-void LaunchSpmv(const DevicePatternView& p, const double* values, const double* x, double* y, cudaStream_t stream)
+template <class T>
+void LaunchSpmv(const DevicePatternView& p, const T* values, const double* x, double* y, cudaStream_t stream)
 {
 	if (p.nodes == 0) return;
-	SpmvKernel<<<Blocks(p.nodes, 8), 256, 0, stream>>>(p, values, x, y);
+	SpmvKernel<T><<<Blocks(p.nodes, 8), 256, 0, stream>>>(p, values, x, y);
 	LaunchCheck("SpmvKernel");
 }
 
-void LaunchSpmvBlockJacobi(const DevicePatternView& p, const double* values, const double* inverse,
+template <class T>
+void LaunchSpmvBlockJacobi(const DevicePatternView& p, const T* values, const double* inverse,
 	const double* x, const double* scale, double* y, const int* stop, cudaStream_t stream)
 {
 	if (p.nodes == 0) return;
-	SpmvBlockJacobiKernel<<<Blocks(p.nodes, 8), 256, 0, stream>>>(p, values, inverse, x, scale, y, stop);
+	SpmvBlockJacobiKernel<T><<<Blocks(p.nodes, 8), 256, 0, stream>>>(p, values, inverse, x, scale, y, stop);
 	LaunchCheck("SpmvBlockJacobiKernel");
 }
 
-void LaunchBlockInverse(const DevicePatternView& p, const double* values, double* inverse, unsigned int* singular,
+template <class T>
+void LaunchBlockInverse(const DevicePatternView& p, const T* values, double* inverse, unsigned int* singular,
 	cudaStream_t stream)
 {
 	if (p.nodes == 0) return;
-	BlockInverseKernel<<<Blocks(p.nodes, 128), 128, 0, stream>>>(p, values, inverse, singular);
+	BlockInverseKernel<T><<<Blocks(p.nodes, 128), 128, 0, stream>>>(p, values, inverse, singular);
 	LaunchCheck("BlockInverseKernel");
+}
+
+template void LaunchSpmv<double>(const DevicePatternView&, const double*, const double*, double*, cudaStream_t);
+template void LaunchSpmv<float>(const DevicePatternView&, const float*, const double*, double*, cudaStream_t);
+template void LaunchSpmvBlockJacobi<double>(const DevicePatternView&, const double*, const double*, const double*,
+	const double*, double*, const int*, cudaStream_t);
+template void LaunchSpmvBlockJacobi<float>(const DevicePatternView&, const float*, const double*, const double*,
+	const double*, double*, const int*, cudaStream_t);
+template void LaunchBlockInverse<double>(const DevicePatternView&, const double*, double*, unsigned int*, cudaStream_t);
+template void LaunchBlockInverse<float>(const DevicePatternView&, const float*, double*, unsigned int*, cudaStream_t);
+
+void LaunchToFloat(long long n, const double* in, float* out, cudaStream_t stream)
+{
+	if (n == 0) return;
+	ToFloatKernel<<<Blocks(n, 256), 256, 0, stream>>>(n, in, out);
+	LaunchCheck("ToFloatKernel");
 }
 
 void LaunchApplyBlockInverse(int nodes, const double* inverse, const double* x, double* y, cudaStream_t stream)
@@ -287,15 +336,21 @@ void LaunchApplyBlockInverse(int nodes, const double* inverse, const double* x, 
 	LaunchCheck("ApplyBlockInverseKernel");
 }
 
+template <class T>
 void LaunchDirichletRows(const DevicePatternView& p, int count, const int32_t* nodes, const int32_t* vmask,
-	const int32_t* pmask, const double* velocity, const double* pressure, const double* state, double* values,
+	const int32_t* pmask, const double* velocity, const double* pressure, const double* state, T* values,
 	double* rhs, cudaStream_t stream)
 {
 	if (count == 0) return;
-	DirichletRowsKernel<<<Blocks(count, 8), 256, 0, stream>>>(p, count, nodes, vmask, pmask, velocity, pressure,
+	DirichletRowsKernel<T><<<Blocks(count, 8), 256, 0, stream>>>(p, count, nodes, vmask, pmask, velocity, pressure,
 		state, values, rhs);
 	LaunchCheck("DirichletRowsKernel");
 }
+
+template void LaunchDirichletRows<double>(const DevicePatternView&, int, const int32_t*, const int32_t*,
+	const int32_t*, const double*, const double*, const double*, double*, double*, cudaStream_t);
+template void LaunchDirichletRows<float>(const DevicePatternView&, int, const int32_t*, const int32_t*,
+	const int32_t*, const double*, const double*, const double*, float*, double*, cudaStream_t);
 
 void LaunchFaceFlows(int faces, const int32_t* face_element, const double* face_coef, const int32_t* eo,
 	const int32_t* conn, const double* state, double* face_flow, cudaStream_t stream)
