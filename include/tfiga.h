@@ -226,6 +226,21 @@ int tfiga_ns_set_profiling(tfiga_ns* ns, int enable);
 /* Totals since the last reset: milliseconds and launch counts per family. */
 int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int32_t reset);
 
+/* ---- allocation-free kernel ------------------------------------------- */
+/* *norm_device = ||b - A x||_2 for a 4x4 block-CSR matrix given entirely by
+ * device pointers (row_offsets [nodes+1], columns and values [blocks*16]
+ * FP64, x and b [4*nodes]), enqueued on `stream` (a cudaStream_t; NULL is
+ * the legacy default stream).  No counterpart in the reference: it exists for
+ * callers that may not allocate device memory at call time.  It allocates
+ * nothing: its scratch is a static device array of 32768 partial sums, so
+ * nodes <= 262144 (larger -> TFIGA_E_UNSUPPORTED, nothing launched).  No
+ * scratch has to start at zero.  Calls share that scratch, so calls whose
+ * kernels could overlap must be serialized.  The first call on a device looks
+ * up the scratch address; make it before any stream capture begins. */
+int tfiga_block_residual_norm_static(int64_t nodes, const int32_t* row_offsets_device,
+	const int32_t* columns_device, const double* values_device, const double* x_device, const double* b_device,
+	double* norm_device, void* stream);
+
 /* ---- drop-in command ------------------------------------------------- */
 /* `navier-stokes DATABASE CASE_DIR [MAX_NEWTON] [OUTPUT] [options]`, the argv of
  * iga_cuda's navier-stokes command (ParseCudaFlowOptions iga_cuda.cu:447-498,

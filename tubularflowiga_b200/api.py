@@ -110,6 +110,8 @@ SIGNATURES = {
     "tfiga_ns_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "tfiga_ns_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "tfiga_ns_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "tfiga_block_residual_norm_static": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                   C.c_void_p, C.c_void_p, C.c_void_p]),
     "tfiga_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
 }
 
@@ -314,6 +316,14 @@ class NavierStokes:
             self.close()
         except Exception:
             pass
+
+
+def block_residual_norm_static(nodes: int, row_offsets_ptr: int, columns_ptr: int, values_ptr: int, x_ptr: int,
+                               b_ptr: int, norm_ptr: int, stream: int = 0):
+    """Enqueue ||b - A x||_2 (4x4 block CSR, all device pointers) without allocating; see tfiga.h."""
+    check(lib().tfiga_block_residual_norm_static(nodes, C.c_void_p(row_offsets_ptr), C.c_void_p(columns_ptr),
+                                                  C.c_void_p(values_ptr), C.c_void_p(x_ptr), C.c_void_p(b_ptr),
+                                                  C.c_void_p(norm_ptr), C.c_void_p(stream or None)))
 
 
 def tube_boundary_conditions(tube, inlet_scale: float):

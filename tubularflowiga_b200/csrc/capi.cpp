@@ -76,6 +76,11 @@ tfiga::HostMesh FromDesc(const tfiga_mesh_desc* d)
 
 } // namespace
 
+namespace tfiga {
+// Lets entry points outside this file (which do not go through Guard) set the message.
+void RecordLastError(const char* message) { g_error = message; }
+}
+
 extern "C" {
 
 size_t tfiga_last_error(char* buffer, size_t capacity)
