@@ -90,14 +90,18 @@ typedef struct tfiga_ns_params {
 	int32_t preconditioner;        /* default TFIGA_PRECONDITIONER_BLOCK_JACOBI */
 	/* TFIGA_PRECISION_FP64: every array and operation in FP64 (the reference's precision).
 	 * TFIGA_PRECISION_MIXED: FP64 nonlinear residual, Newton update and Krylov vectors;
-	 * the Jacobian is contracted in reduced precision and stored in FP32 for SpMV and the
-	 * preconditioner, with FGMRES true-residual restarts acting as FP64 iterative refinement
-	 * (requires TFIGA_PRECONDITIONER_AMG). */
+	 * the element tangent is contracted on the tensor cores (BF16 operands, FP32
+	 * accumulation) and the Jacobian is stored in FP32 for SpMV and the preconditioner,
+	 * with FGMRES true-residual restarts acting as FP64 iterative refinement.
+	 * TFIGA_PRECISION_FP32_JACOBIAN: as MIXED, but the tangent is assembled in FP64 and
+	 * rounded once to FP32 for storage.
+	 * Both reduced modes require TFIGA_PRECONDITIONER_AMG. */
 	int32_t precision;             /* default TFIGA_PRECISION_FP64 */
 } tfiga_ns_params;
 
 #define TFIGA_PRECISION_FP64 0
 #define TFIGA_PRECISION_MIXED 1
+#define TFIGA_PRECISION_FP32_JACOBIAN 2
 
 #define TFIGA_PRECONDITIONER_BLOCK_JACOBI 0
 #define TFIGA_PRECONDITIONER_AMG 1
@@ -205,9 +209,11 @@ int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info);
 int tfiga_ns_boundary_flows(tfiga_ns* ns, const int32_t* labels, int32_t count, double* flows);
 
 /* ---- raw kernels on device pointers (measurement and integration) ------ */
-/* y = A x over the mesh pattern (BlockSpmvKernel<4>, SparseKernels.cuh:25-40). */
+/* y = A x over the mesh pattern with the active Jacobian (FP32 storage in the
+ * reduced-precision modes) (BlockSpmvKernel<4>, SparseKernels.cuh:25-40). */
 int tfiga_ns_spmv_device(tfiga_ns* ns, const double* x_device, double* y_device);
-/* Device pointers of the handle's matrix values and state (for in-HBM timing). */
+/* Device pointers of the handle's FP64 matrix values (NULL in
+ * TFIGA_PRECISION_MIXED, which keeps no FP64 Jacobian), state and rhs. */
 int tfiga_ns_device_buffers(tfiga_ns* ns, double** values, double** state, double** rhs);
 /* Counters of kernel launches issued by this handle (for launch accounting). */
 int64_t tfiga_ns_launch_count(const tfiga_ns* ns);

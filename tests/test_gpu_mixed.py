@@ -1,0 +1,105 @@
+"""Mixed-precision Newton path (TFIGA_PRECISION_MIXED): tensor-core tangent.
+
+The tangent is contracted on the tcgen05 tensor cores with BF16 operands and
+FP32 accumulation and stored in FP32; the residual stays FP64.  Tolerances:
+* residual (rhs): 1e-12 relative per field, as the FP64 assembly;
+* Jacobian: 2e-2 relative (Frobenius) per field pair (i, f) against the FP64
+  oracle -- BF16 keeps 8 significant bits (unit roundoff 2^-9 ~ 2e-3 per
+  operand), and the blocks whose terms cancel lose a few bits more;
+* Newton: the mixed Newton iteration converges to the FP64 solution; after
+  convergence to 1e-10 of the initial residual the velocity agrees to 1e-8
+  and the pressure to 1e-6 relative L2 with the FP64 path.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RHO, MU, DT = 1060.0, 3.5e-3, 1e-3
+TANGENT_TOL = 2e-2
+
+
+@pytest.fixture(scope="module")
+def api():
+    from tubularflowiga_b200 import api as a
+    return a
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+def random_state(nodes, seed, speed=0.2, pressure=20.0):
+    rng = np.random.default_rng(seed)
+    s = rng.normal(size=(nodes, 4))
+    s[:, :3] *= speed
+    s[:, 3] *= pressure
+    return s.ravel()
+
+
+def check_tensor_tangent(api, flat, rho, mu, dt, seed):
+    mesh = api.Mesh(flat)
+    ns = api.NavierStokes(mesh, density=rho, viscosity=mu, dt=dt, preconditioner=api.AMG, precision=api.MIXED)
+    st = random_state(flat.nodes, seed)
+    pv = random_state(flat.nodes, seed + 1)
+    ns.set_state(st, pv)
+    values, rhs = ns.assemble()
+    P = O.Pattern(flat.nodes, flat.element_offsets, flat.connectivity)
+    ov, orhs = O.assemble(flat, P, st, pv, rho, mu, dt)
+    for f in range(4):
+        assert rel(rhs[f::4], orhs[f::4]) < 1e-12
+    v, r = values.reshape(-1, 4, 4), ov.reshape(-1, 4, 4)
+    errors = np.array([[rel(v[:, i, f], r[:, i, f]) for f in range(4)] for i in range(4)])
+    assert errors.max() < TANGENT_TOL, errors
+    return errors
+
+
+def test_tensor_tangent_small_tube(api, small_tube):
+    check_tensor_tangent(api, small_tube.mesh, RHO, MU, DT, 0)
+
+
+def test_tensor_tangent_steady(api, small_tube):
+    check_tensor_tangent(api, small_tube.mesh, RHO, MU, 0.0, 3)
+
+
+def test_tensor_tangent_reference_tube_ragged(api, reference_tube):
+    """Elements with 36..64 basis functions: padded rows and columns must not leak into the matrix."""
+    from tubularflowiga_b200 import ntiga
+    flat = ntiga.read(reference_tube / "tube-1.ntiga")
+    check_tensor_tangent(api, flat, 1.0, 1.0, 0.1, 5)
+
+
+def test_tensor_tangent_is_repeatable_in_norm(api, small_tube):
+    """Two assemblies of the same state agree to FP32 summation-order noise (atomic scatter order varies)."""
+    flat = small_tube.mesh
+    mesh = api.Mesh(flat)
+    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, preconditioner=api.AMG, precision=api.MIXED)
+    st = random_state(flat.nodes, 9)
+    ns.set_state(st, st)
+    v1, r1 = ns.assemble()
+    v2, r2 = ns.assemble()
+    assert rel(v1, v2) < 1e-6
+    assert rel(r1, r2) < 1e-13
+
+
+def test_mixed_newton_converges_to_fp64_solution(api, cylinder_1280):
+    tube = cylinder_1280
+    flat = tube.mesh
+    vmask, pmask, vel = api.tube_boundary_conditions(tube, 0.2)
+    s0 = api.initial_state(vmask, vel)
+    mesh = api.Mesh(flat)
+    states, reports = {}, {}
+    for name, precision in (("fp64", api.FP64), ("mixed", api.MIXED)):
+        ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, preconditioner=api.AMG, precision=precision,
+                              nonlinear_rtol=1e-10, nonlinear_atol=1e-30, gmres_rtol=1e-10, max_newton=20)
+        ns.set_dirichlet(vmask, pmask, vel)
+        ns.set_tractions({2: 0.0})
+        ns.set_state(s0, s0)
+        reports[name] = ns.step()
+        states[name] = ns.get_state().reshape(-1, 4)
+    assert reports["mixed"]["converged"] and reports["fp64"]["converged"]
+    assert reports["mixed"]["newton_iterations"] <= reports["fp64"]["newton_iterations"] + 4
+    assert rel(states["mixed"][:, :3], states["fp64"][:, :3]) < 1e-8
+    assert rel(states["mixed"][:, 3], states["fp64"][:, 3]) < 1e-6

@@ -45,6 +45,7 @@ class NsParams(C.Structure):
 
 FP64 = 0
 MIXED = 1
+FP32_JACOBIAN = 2
 
 
 BLOCK_JACOBI = 0

@@ -325,7 +325,10 @@ int tfiga_ns_spmv_device(tfiga_ns* ns, const double* x, double* y)
 {
 	return Guard([&] {
 		Require(ns && x && y, "null argument");
-		tfiga::LaunchSpmv(ns->solver->pattern(), ns->solver->values(), x, y, ns->solver->stream());
+		if (ns->solver->mixed())
+			tfiga::LaunchSpmv(ns->solver->pattern(), ns->solver->values32(), x, y, ns->solver->stream());
+		else
+			tfiga::LaunchSpmv(ns->solver->pattern(), ns->solver->values(), x, y, ns->solver->stream());
 		ns->solver->AddLaunches(1);
 	});
 }

@@ -58,6 +58,14 @@ void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double*
 	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
 	double* values, double* rhs, cudaStream_t stream);
 
+// ---- tangent_tc.cu -----------------------------------------------------
+// Tensor-core tangent (BF16 operands, FP32 accumulation) ADDED into FP32
+// values, FP64 residual ADDED into rhs (= -r); status bit 1 set if an MMA
+// completion wait expired.
+void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const double* qdata,
+	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
+	float* values, double* rhs, int* status, cudaStream_t stream);
+
 // ---- sparse.cu ----------------------------------------------------------
 // Matrix values are FP64 or FP32 (T = double / float); vectors are FP64.
 template <class T>

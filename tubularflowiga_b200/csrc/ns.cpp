@@ -39,7 +39,10 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 			+std::to_string(mesh.min_detj()));
 	stream_ = mesh.stream();
 	const int64_t n = mesh.nodes();
-	values_.Allocate((size_t)blocks()*16);
+	if (params.precision != TFIGA_PRECISION_FP64 && params.precision != TFIGA_PRECISION_MIXED
+		&& params.precision != TFIGA_PRECISION_FP32_JACOBIAN)
+		Fail(-1, "unknown precision "+std::to_string(params.precision));
+	if (!tensor_tangent()) values_.Allocate((size_t)blocks()*16);
 	rhs_.Allocate(n4_); state_.Allocate(n4_); previous_.Allocate(n4_); update_.Allocate(n4_);
 	traction_.Allocate(n4_);
 	velocity_bc_.Allocate(3*n); pressure_bc_.Allocate(n);
@@ -67,11 +70,15 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 		"pinned scalars");
 	for (auto& ev : events_) CudaCheck(cudaEventCreate(&ev), "event");
 	gmres_.set_profiler(&profiler_);
-	if (params.precision != TFIGA_PRECISION_FP64 && params.precision != TFIGA_PRECISION_MIXED)
-		Fail(-1, "unknown precision "+std::to_string(params.precision));
 	if (mixed() && params.preconditioner != TFIGA_PRECONDITIONER_AMG)
 		Fail(-7, "mixed precision requires the AMG-preconditioned flexible GMRES");
 	if (mixed()) values32_.Allocate((size_t)blocks()*16);
+	if (tensor_tangent()) {
+		status_.Allocate(1);
+		status_.Zero(stream_);
+		CudaCheck(cudaMallocHost(reinterpret_cast<void**>(&pinned_status_), sizeof(int32_t)), "pinned status");
+		*pinned_status_ = 0;
+	}
 	if (params.preconditioner == TFIGA_PRECONDITIONER_AMG) {
 		amg_ = std::make_unique<Amg>(mesh.pattern_view(), mesh.pattern().row_offsets, mesh.pattern().columns, stream_);
 		amg_->set_profiler(&profiler_);
@@ -85,6 +92,7 @@ NsSolver::~NsSolver()
 {
 	for (auto& ev : events_) if (ev) cudaEventDestroy(ev);
 	if (pinned_) cudaFreeHost(pinned_);
+	if (pinned_status_) cudaFreeHost(pinned_status_);
 }
 
 void NsSolver::SetDirichlet(const int32_t* vmask, const int32_t* pmask, const double* velocity, const double* pressure)
@@ -164,6 +172,19 @@ void NsSolver::CommitStep()
 
 void NsSolver::Assemble()
 {
+	if (tensor_tangent()) {
+		values32_.Zero(stream_);
+		rhs_.Zero(stream_);
+		profiler_.Begin(Profiler::kAssembly, stream_);
+		LaunchTangentTc(mesh_.view(), mesh_.phi(), mesh_.qdata(), mesh_.element_blocks(), state_.get(),
+			previous_.get(), {params_.density, params_.viscosity, params_.dt}, values32_.get(), rhs_.get(),
+			status_.get(), stream_);
+		profiler_.End(stream_);
+		LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
+		launches_ += 2;
+		if (amg_ && !amg_->built()) amg_->Build(values32_.get());
+		return;
+	}
 	values_.Zero(stream_);
 	rhs_.Zero(stream_);
 	profiler_.Begin(Profiler::kAssembly, stream_);
@@ -259,7 +280,10 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	CudaCheck(cudaEventRecord(events_[1], stream_), "event");
 	scalars_.Download(pinned_, kSlots, stream_);
 	if (!labels_.empty()) label_flow_.Download(pinned_+kSlots, labels_.size(), stream_);
+	if (tensor_tangent()) status_.Download(pinned_status_, 1, stream_);
 	CudaCheck(cudaStreamSynchronize(stream_), "Navier-Stokes assembly");
+	if (tensor_tangent() && *pinned_status_ != 0)
+		Fail(-2, "tensor-core tangent: an MMA completion wait expired (status "+std::to_string(*pinned_status_)+")");
 	float ms = 0.0f;
 	CudaCheck(cudaEventElapsedTime(&ms, events_[0], events_[1]), "event time");
 	report.assembly_ms = ms;

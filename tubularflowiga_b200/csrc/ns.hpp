@@ -39,8 +39,12 @@ public:
 
 	int64_t nodes() const { return mesh_.nodes(); }
 	long long blocks() const { return (long long)mesh_.pattern().columns.size(); }
-	double* values() { return values_.get(); }
-	bool mixed() const { return params_.precision == TFIGA_PRECISION_MIXED; }
+	double* values() { return values_.get(); }       // null in TFIGA_PRECISION_MIXED
+	float* values32() { return values32_.get(); }    // null in TFIGA_PRECISION_FP64
+	// FP32 Jacobian storage (both reduced-precision modes).
+	bool mixed() const { return params_.precision != TFIGA_PRECISION_FP64; }
+	// Tangent contracted on the tensor cores (BF16 x BF16 -> FP32); no FP64 Jacobian is kept.
+	bool tensor_tangent() const { return params_.precision == TFIGA_PRECISION_MIXED; }
 	// Active Jacobian values as FP64 on the host (FP32 storage is widened).
 	void DownloadValues(double* out);
 	double* state() { return state_.get(); }
@@ -70,7 +74,7 @@ private:
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
 	DeviceArray<float> values32_;
 	DeviceArray<double> face_flow_, face_pressure_, label_flow_, partial_, scalars_;
-	DeviceArray<int32_t> vmask_, pmask_, constrained_, face_slot_;
+	DeviceArray<int32_t> vmask_, pmask_, constrained_, face_slot_, status_;
 	std::vector<int32_t> labels_;            // distinct face labels (slot order)
 	std::map<int32_t, int> slot_of_label_;
 	std::vector<int32_t> face_slot_host_;
@@ -80,6 +84,7 @@ private:
 	Profiler profiler_;
 	std::unique_ptr<Amg> amg_;
 	double* pinned_ = nullptr;               // host mirror of scalars + label flows
+	int32_t* pinned_status_ = nullptr;       // host mirror of the tensor-core kernel status
 };
 
 } // namespace tfiga

@@ -1,0 +1,413 @@
+// Tensor-core (tcgen05) element tangent for the mixed-precision Newton path:
+// the exact VMS tangent contracted in BF16 with FP32 accumulation in tensor
+// memory and added into an FP32 block-CSR Jacobian, plus the FP64 residual of
+// the same element (the residual drives the Newton refinement and stays FP64).
+//
+// Formulation: identical to the FP64 assembly (vms_point.cuh, the reference's
+// NavierStokesElement.hpp:149-317 with the exact tangent :244-312).  The
+// tangent of element e, row field i, column field f is
+//   K^{if}_{ab} = sum_k Psi(a, k) G^{if}(b, k),   k = (q, s): 64 points x 4 test features,
+//   G^{if}(b, (q, s)) = sum_t M_q^{if}[s][t] Phi_t(b, q),
+// i.e. D[m = (b, f)][n = a] = A[m][k] B[n][k]^T with A = G (K-major) and
+// B = Psi (K-major), one GEMM of M = 512 x N = 64 x K = 256 per row-field
+// pair.
+//
+// Work split.  One CTA per (element, pair of row fields h: i in {2h, 2h+1}),
+// 256 threads, about 107 KiB of shared memory so that two CTAs share an SM
+// and one CTA's scatter overlaps the other's operand build.  Four M = 128
+// accumulator tiles (tile T: row field 2h + T/2, basis b in [32 (T&1), +32),
+// tile row m = 4 (b mod 32) + f) live in 4 x 64 = 256 TMEM columns.
+//   prologue  FP64 state at the 64 points, FP64 coefficients M_q, rc_q of the
+//             two row fields (stored FP32 / FP64), FP64 residual -> rhs;
+//   8 chunks  of 8 points (K = 32): stage Phi (FP32), build Psi and G as BF16
+//             in the 64-byte-swizzled K-major layout, one thread issues
+//             4 tiles x 2 tcgen05.mma (128 x 64 x 16) and commits to an mbarrier;
+//             the next chunk waits on it before overwriting the operands;
+//   epilogue  tcgen05.ld rows (b, f) x 32 columns a, a 4x4 transpose inside
+//             each lane quad gives the four f of one (a, b), which go to the
+//             FP32 matrix as one red.global.add.v4.f32.
+// Every mbarrier wait is bounded (one second of globaltimer); on expiry the
+// CTA records TFIGA status bit 1, waits once more (bounded) for its own MMAs,
+// frees its tensor memory and returns without writing the tangent.
+#include "common.hpp"
+#include "kernels.cuh"
+#include "vms_point.cuh"
+
+#include <cuda_bf16.h>
+
+namespace tfiga {
+namespace {
+
+constexpr int kTcThreads = 256;
+constexpr int kPts = 8;                          // quadrature points per K chunk
+constexpr int kChunks = kQuad/kPts;              // 8
+constexpr int kTiles = 4;                        // M = 128 tiles per CTA
+constexpr int kTileBytes = 128*64;               // 128 rows x 32 BF16 (64 B, one swizzle row)
+constexpr int kTmemCols = 256;                   // 4 tiles x N = 64 FP32 columns
+constexpr unsigned long long kWaitNs = 1000000000ull;
+
+// Shared-memory layout (bytes from a 1024-aligned base).
+constexpr int kOffA = 0;                                         // 4 tiles x 8 KiB
+constexpr int kOffB = kOffA+kTiles*kTileBytes;                   // Psi: 64 rows x 64 B
+constexpr int kOffPhi = kOffB+64*64;                             // float [5][kPts][64]
+constexpr int kOffCoef = kOffPhi+kFeatures*kPts*64*4;            // float [2][64][kCoef]
+constexpr int kOffRC = kOffCoef+2*kQuad*kCoef*4;                 // double [2][64][4]
+constexpr int kOffQS = kOffRC+2*kQuad*4*8;                       // double [64][kQS]; reused as [256] partials
+constexpr int kOffU = kOffQS+kQuad*kQS*8;                        // double [64][4]
+constexpr int kOffUp = kOffU+64*4*8;                             // double [64][4]
+constexpr int kOffBar = kOffUp+64*4*8;                           // mbarrier, TMEM slot
+constexpr int kSmemBytes = kOffBar+16+1024;                      // + alignment slack
+static_assert(kSmemBytes <= 113*1024, "two CTAs per SM");
+
+// Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B BF16, both
+// K-major, M = 128, N = 64.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ uint32_t SmemAddress(const void* p)
+{
+	return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor, K-major, 64-byte swizzle: 8-row atoms of
+// 512 B (stride byte offset 512), leading byte offset unused (1), version 1.
+__device__ __forceinline__ uint64_t DescSw64(uint32_t address)
+{
+	return (uint64_t)((address >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46)
+		| (4ull << 61);
+}
+
+// Byte offset of 16-byte chunk j (0..3) of row r in a 64-byte-swizzled K-major tile.
+__device__ __forceinline__ int Sw64(int r, int j)
+{
+	return r*64+((j ^ ((r >> 1) & 3)) << 4);
+}
+
+__device__ __forceinline__ unsigned long long GlobalTimer()
+{
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+__device__ __forceinline__ void MbarInit(uint64_t* bar)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(SmemAddress(bar)) : "memory");
+	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool MbarTryWait(uint64_t* bar, uint32_t parity)
+{
+	uint32_t done;
+	asm volatile("{\n\t.reg .pred p;\n\t"
+		"mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		"selp.u32 %0, 1, 0, p;\n\t}"
+		: "=r"(done) : "r"(SmemAddress(bar)), "r"(parity) : "memory");
+	return done != 0;
+}
+
+// Waits for completion of the mbarrier phase with the given parity, for at most kWaitNs.
+__device__ bool MbarWaitBounded(uint64_t* bar, uint32_t parity)
+{
+	const unsigned long long start = GlobalTimer();
+	while (!MbarTryWait(bar, parity))
+		if (GlobalTimer()-start > kWaitNs) return false;
+	return true;
+}
+
+__device__ __forceinline__ void MmaBf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+	asm volatile("{\n\t.reg .pred p;\n\t"
+		"setp.ne.b32 p, %4, 0;\n\t"
+		"tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+		:: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0u) : "memory");
+}
+
+__device__ __forceinline__ void MmaCommit(uint64_t* bar)
+{
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+		:: "r"(SmemAddress(bar)) : "memory");
+}
+
+__device__ __forceinline__ void FenceBeforeSync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void FenceAfterSync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void FenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 lanes x 32 consecutive FP32 columns: thread l gets row (lane base + l), columns c..c+31.
+__device__ __forceinline__ void TmemLoad32(uint32_t taddr, float v[32])
+{
+	uint32_t r[32];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+		"{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+		"%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+		: "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+		  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+		  "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+		  "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+		: "r"(taddr));
+	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+	#pragma unroll
+	for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ float Pick4(float x0, float x1, float x2, float x3, int k)
+{
+	return k == 0 ? x0 : k == 1 ? x1 : k == 2 ? x2 : x3;
+}
+
+__device__ __forceinline__ uint32_t PackBf16(float lo, float hi)
+{
+	const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+	return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void StoreShared16(uint32_t address, uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+	asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" :: "r"(address), "r"(a), "r"(b), "r"(c), "r"(d)
+		: "memory");
+}
+
+__device__ __forceinline__ void RedAdd4(float* p, float a, float b, float c, float d)
+{
+	asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" :: "l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
+		: "memory");
+}
+
+__global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView mesh,
+	const double* __restrict__ phi, const double* __restrict__ qdata, const int32_t* __restrict__ element_blocks,
+	const double* __restrict__ state, const double* __restrict__ previous, AssemblyParams prm,
+	float* __restrict__ values, double* __restrict__ rhs, int* __restrict__ status)
+{
+	extern __shared__ uint8_t smem_raw[];
+	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+1023) & ~uintptr_t(1023));
+	const uint32_t sA = SmemAddress(sm+kOffA), sB = SmemAddress(sm+kOffB);
+	float* PhiS = reinterpret_cast<float*>(sm+kOffPhi);
+	float* Coef = reinterpret_cast<float*>(sm+kOffCoef);
+	double* RC = reinterpret_cast<double*>(sm+kOffRC);
+	double* QS = reinterpret_cast<double*>(sm+kOffQS);
+	double* U = reinterpret_cast<double*>(sm+kOffU);
+	double* Up = reinterpret_cast<double*>(sm+kOffUp);
+	uint64_t* bar = reinterpret_cast<uint64_t*>(sm+kOffBar);
+	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm+kOffBar+8);
+
+	const int e = blockIdx.x >> 1;
+	const int h = blockIdx.x & 1;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const int begin = mesh.element_offsets[e];
+	const int nen = mesh.element_offsets[e+1]-begin;
+	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
+
+	// Tensor memory for the four accumulator tiles; the mbarrier.
+	if (warp == 0) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+			:: "r"(SmemAddress(tmem_slot)), "r"(kTmemCols) : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	if (tid == 32) MbarInit(bar);
+
+	// 1. Nodal state.
+	if (tid < kMaxBasis) {
+		const int a = tid;
+		double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, p0 = 0.0, p1 = 0.0, p2 = 0.0;
+		if (a < nen) {
+			const size_t node = (size_t)mesh.connectivity[begin+a];
+			s0 = state[4*node]; s1 = state[4*node+1]; s2 = state[4*node+2]; s3 = state[4*node+3];
+			if (prm.dt > 0.0) { p0 = previous[4*node]; p1 = previous[4*node+1]; p2 = previous[4*node+2]; }
+		}
+		U[a*4] = s0; U[a*4+1] = s1; U[a*4+2] = s2; U[a*4+3] = s3;
+		Up[a*4] = p0; Up[a*4+1] = p1; Up[a*4+2] = p2; Up[a*4+3] = 0.0;
+	}
+	FenceBeforeSync();
+	__syncthreads();
+	FenceAfterSync();
+	const uint32_t tmem = *tmem_slot;
+
+	// 2. State at every point (FP64): a warp per point, lanes over basis functions.
+	for (int q = warp; q < kQuad; q += kTcThreads/32) {
+		double v[22];
+		#pragma unroll
+		for (int k = 0; k < 22; ++k) v[k] = 0.0;
+		for (int a = lane; a < kMaxBasis; a += 32) {
+			const double n = P[(0*kQuad+q)*kMaxBasis+a];
+			const double g0 = P[(1*kQuad+q)*kMaxBasis+a], g1 = P[(2*kQuad+q)*kMaxBasis+a];
+			const double g2 = P[(3*kQuad+q)*kMaxBasis+a], l = P[(4*kQuad+q)*kMaxBasis+a];
+			const double uf[4] = {U[a*4], U[a*4+1], U[a*4+2], U[a*4+3]};
+			v[0] += n*uf[0]; v[1] += n*uf[1]; v[2] += n*uf[2]; v[3] += n*uf[3];
+			v[4] += n*Up[a*4]; v[5] += n*Up[a*4+1]; v[6] += n*Up[a*4+2];
+			#pragma unroll
+			for (int f = 0; f < 4; ++f) { v[7+3*f] += g0*uf[f]; v[8+3*f] += g1*uf[f]; v[9+3*f] += g2*uf[f]; }
+			v[19] += l*uf[0]; v[20] += l*uf[1]; v[21] += l*uf[2];
+		}
+		#pragma unroll
+		for (int k = 0; k < 22; ++k)
+			#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+		if (lane == 0)
+			#pragma unroll
+			for (int k = 0; k < 22; ++k) QS[q*kQS+k] = v[k];
+	}
+	__syncthreads();
+
+	// 3. Coefficients of the two row fields at every point.
+	if (tid < 2*kQuad) {
+		const int il = tid >> 6, q = tid & 63;
+		PointState S;
+		const double* s = QS+q*kQS;
+		for (int c = 0; c < 3; ++c) {
+			S.u[c] = s[kU+c]; S.up[c] = s[kUp+c]; S.lap[c] = s[kLap+c]; S.gp[c] = s[kGrad+9+c];
+			for (int d = 0; d < 3; ++d) S.gv[c][d] = s[kGrad+3*c+d];
+		}
+		S.p = s[kP];
+		RowCoefficients<float>(2*h+il, S, qdata+((size_t)e*kQuad+q)*kQData, prm, Coef+(il*kQuad+q)*kCoef,
+			RC+(il*kQuad+q)*4);
+	}
+	__syncthreads();
+
+	// 4. FP64 residual of the two row fields (rhs holds -r): thread (il, half, a).
+	{
+		const int il = tid >> 7, half = (tid >> 6) & 1, a = tid & 63;
+		double r = 0.0;
+		for (int q = half*32; q < half*32+32; ++q)
+			#pragma unroll
+			for (int s = 0; s < 4; ++s) r += P[(s*kQuad+q)*kMaxBasis+a]*RC[(il*kQuad+q)*4+s];
+		__syncthreads();                       // QS is dead: reuse it for the partial sums
+		QS[tid] = r;
+		__syncthreads();
+		if (half == 0 && a < nen)
+			atomicAdd(rhs+4*(size_t)mesh.connectivity[begin+a]+2*h+il, QS[tid]+QS[tid+64]);
+	}
+
+	// 5. Tangent chunks.
+	const int gil = warp >> 2, gqp = warp & 3;     // G builder: row field, point pair
+	const int gf = lane & 3, gbs = lane >> 2;       //            column field, basis sub-index
+	bool failed = false;
+	uint32_t pending = 0;                            // parity of the last committed chunk
+	for (int c = 0; c < kChunks; ++c) {
+		const int q0 = c*kPts;
+		// Stage Phi of the chunk as FP32, layout [t][point][b].
+		for (int idx = tid; idx < kFeatures*kPts*64; idx += kTcThreads) {
+			const int t = idx >> 9, ql = (idx >> 6) & 7, b = idx & 63;
+			PhiS[idx] = (float)P[(t*kQuad+q0+ql)*kMaxBasis+b];
+		}
+		bool ok = true;
+		if (c > 0) ok = MbarWaitBounded(bar, pending);
+		if (__syncthreads_or(!ok)) { failed = true; break; }
+
+		// B = Psi: row a, K = (point, s); thread (a, point pair).
+		{
+			const int a = tid >> 2, qp = tid & 3;
+			float x[8];
+			#pragma unroll
+			for (int k = 0; k < 8; ++k) x[k] = PhiS[((k & 3)*kPts+2*qp+(k >> 2))*64+a];
+			StoreShared16(sB+Sw64(a, qp), PackBf16(x[0], x[1]), PackBf16(x[2], x[3]), PackBf16(x[4], x[5]),
+				PackBf16(x[6], x[7]));
+		}
+		// A = G: row (b, f) of tile (il, b / 32), K = (point, s).
+		{
+			const int ql0 = 2*gqp;
+			float m0[20], m1[20];
+			const float* c0 = Coef+(gil*kQuad+q0+ql0)*kCoef+gf*20;
+			#pragma unroll
+			for (int k = 0; k < 20; ++k) { m0[k] = c0[k]; m1[k] = c0[kCoef+k]; }
+			#pragma unroll 2
+			for (int bg = 0; bg < 8; ++bg) {
+				const int b = bg*8+gbs;
+				float p0[5], p1[5];
+				#pragma unroll
+				for (int t = 0; t < 5; ++t) {
+					p0[t] = PhiS[(t*kPts+ql0)*64+b];
+					p1[t] = PhiS[(t*kPts+ql0+1)*64+b];
+				}
+				float g[8];
+				#pragma unroll
+				for (int s = 0; s < 4; ++s) {
+					g[s] = m0[s*5]*p0[0]+m0[s*5+1]*p0[1]+m0[s*5+2]*p0[2]+m0[s*5+3]*p0[3]+m0[s*5+4]*p0[4];
+					g[4+s] = m1[s*5]*p1[0]+m1[s*5+1]*p1[1]+m1[s*5+2]*p1[2]+m1[s*5+3]*p1[3]+m1[s*5+4]*p1[4];
+				}
+				const int tile = gil*2+(b >> 5), row = (b & 31)*4+gf;
+				StoreShared16(sA+tile*kTileBytes+Sw64(row, gqp), PackBf16(g[0], g[1]), PackBf16(g[2], g[3]),
+					PackBf16(g[4], g[5]), PackBf16(g[6], g[7]));
+			}
+		}
+		FenceProxyAsync();
+		__syncthreads();
+		if (tid == 0) {
+			FenceAfterSync();
+			#pragma unroll
+			for (int tile = 0; tile < kTiles; ++tile)
+				#pragma unroll
+				for (int ks = 0; ks < 2; ++ks)
+					MmaBf16(tmem+tile*64, DescSw64(sA+tile*kTileBytes+ks*32), DescSw64(sB+ks*32),
+						(c > 0 || ks > 0) ? 1u : 0u);
+			MmaCommit(bar);
+		}
+		pending = (uint32_t)(c & 1);
+	}
+	if (!failed) failed = __syncthreads_or(!MbarWaitBounded(bar, pending)) != 0;
+
+	if (!failed) {
+		// 6. Epilogue: warp -> (row field il = warp/4, TMEM lane quarter warp%4), two tiles, two column halves.
+		FenceAfterSync();
+		const int il = warp >> 2, quarter = warp & 3;
+		const int i = 2*h+il;
+		const int32_t* EB = element_blocks+(size_t)e*kMaxBasis*kMaxBasis;
+		const int f = lane & 3;
+		for (int th = 0; th < 2; ++th) {
+			const int tile = il*2+th;
+			const int b = th*32+quarter*8+(lane >> 2);
+			for (int ah = 0; ah < 2; ++ah) {
+				float v[32];
+				TmemLoad32(tmem+((uint32_t)(quarter*32) << 16)+tile*64+ah*32, v);
+				#pragma unroll
+				for (int g = 0; g < 8; ++g) {
+					const float x0 = v[4*g], x1 = v[4*g+1], x2 = v[4*g+2], x3 = v[4*g+3];
+					float o0 = 0.f, o1 = 0.f, o2 = 0.f, o3 = 0.f;
+					#pragma unroll
+					for (int r = 0; r < 4; ++r) {
+						const int src = f ^ r;    // field of the partner lane = column offset it needs from us
+						const float send = Pick4(x0, x1, x2, x3, src);
+						const float got = r ? __shfl_xor_sync(0xffffffffu, send, r) : send;
+						o0 = src == 0 ? got : o0; o1 = src == 1 ? got : o1;
+						o2 = src == 2 ? got : o2; o3 = src == 3 ? got : o3;
+					}
+					const int a = ah*32+4*g+f;
+					if (a < nen && b < nen) {
+						const int block = EB[a*kMaxBasis+b];
+						if (block >= 0) RedAdd4(values+(size_t)block*16+i*4, o0, o1, o2, o3);
+					}
+				}
+			}
+		}
+	} else {
+		if (tid == 0) atomicOr(status, 1);
+		MbarWaitBounded(bar, pending);          // let this CTA's own MMAs drain before freeing TMEM
+	}
+	FenceBeforeSync();
+	__syncthreads();
+	if (warp == 0) {
+		FenceAfterSync();
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTmemCols)
+			: "memory");
+	}
+}
+
+} // namespace
+
+void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const double* qdata,
+	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
+	float* values, double* rhs, int* status, cudaStream_t stream)
+{
+	if (mesh.elements == 0) return;
+	static bool configured = false;
+	if (!configured) {
+		CudaCheck(cudaFuncSetAttribute(TangentTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes),
+			"tensor-core tangent shared-memory attribute");
+		configured = true;
+	}
+	const long long ctas = 2LL*mesh.elements;
+	if (ctas > 0x7fffffffLL) Fail(-7, "too many elements for one tangent launch");
+	TangentTcKernel<<<(unsigned)ctas, kTcThreads, kSmemBytes, stream>>>(mesh, phi, qdata, element_blocks, state,
+		previous, params, values, rhs, status);
+	LaunchCheck("TangentTcKernel");
+}
+
+} // namespace tfiga
