@@ -1,25 +1,31 @@
 #!/usr/bin/env python
 """Time steps/s of the body-fitted IGA Navier-Stokes solve on one B200.
 
-Workload (the BASELINE metric's mixed-precision config, run here by the plain
-FP64 solver): the 51,200-element pulsatile tube -- an 8x8-core + two 32-cell
-ring-layer O-grid cross-section (128 cells, 145 control points per plane) x
-400 axial layers, R = 1.5 mm, L = 30 mm, tricubic, rho = 1060 kg/m^3,
-mu = 3.5e-3 Pa s, backward Euler dt = 2e-3 s, parabolic inflow scaled by a
-seeded Fourier waveform (mean 0.15 m/s + 4 harmonics, amplitudes U(0, 0.05),
-seed 0, 1 Hz), zero-traction outlet, no-slip wall.  Inputs are synthetic
-(seeded generator), stated in `data`.
+Workload (the metric's mixed-precision config): the 51,200-element pulsatile
+tube -- an 8x8-core + two 32-cell ring-layer O-grid cross-section (128 cells,
+145 control points per plane) x 400 axial layers, R = 1.5 mm, L = 30 mm,
+tricubic, rho = 1060 kg/m^3, mu = 3.5e-3 Pa s, backward Euler dt = 2e-3 s,
+parabolic inflow scaled by a seeded Fourier waveform (mean 0.15 m/s + 4
+harmonics, amplitudes U(0, 0.05), seed 0, 1 Hz), zero-traction outlet,
+no-slip wall.  Inputs are synthetic (seeded generator), stated in `data`.
 
-A "step" is one physical time step: Newton to ||r|| <= 1e-8 ||r_0|| with the
-exact tangent, each linear solve block-Jacobi GMRES(200) to rtol 1e-8.
+A "step" is one physical time step: Newton to ||r|| <= 1e-8 ||r_0|| (FP64
+residual) with the exact tangent, each linear solve AMG-preconditioned
+FGMRES(200) to a true-residual rtol of 1e-8.  --precision mixed (default, the
+config's own precision): tangent contracted on the tcgen05 tensor cores (BF16
+operands, FP32 accumulation), FP32 Jacobian for SpMV and the preconditioner,
+FP64 residual, vectors and refinement.  --precision fp64: every array FP64.
 
 Legs of one run (rank 0 prints one JSON line):
   value     device-timed (CUDA events on the solver stream) with every input
             resident in HBM; the matrix (> 1.8 GB) exceeds L2, so no flush.
   e2e       the same steps through the C ABI with pinned host inputs (inlet
             Dirichlet values) and the state read back every step.
-  roofline  per-kernel CUDA-event timing of the timed region: SpMV + block-
-            Jacobi (HBM-bound) and the FP64 assembly GEMM.
+  roofline  per-kernel CUDA-event timing of the timed region: the tensor-core
+            (or FP64) assembly, SpMV and the AMG V-cycle (HBM-bound).
+  fp64_gpu  (mixed only) the plain FP64 GPU solver on the same steps from the
+            same initial state: its time steps/s, and the relative L2 error
+            of the mixed solution against it after every step.
   cpu_baseline  the reference's own element code (oracle/_ref) and the CPU
             restatement of block-Jacobi GMRES on a bounded sample, all host
             cores, scaled to time steps/s.
@@ -55,6 +61,14 @@ def peaks():
         d = json.loads(p.read_text())
         return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
     return 6650.0, 1590.0, "fallback"
+
+
+def sustained_bf16():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("bf16_tflops_sustained", d["bf16_tflops"]))
+    return 1400.0
 
 
 def workload(name):
@@ -238,6 +252,8 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2-100"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-fp64-leg", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=25.0)
     ap.add_argument("--ref-newton", type=float, default=3.0)
     ap.add_argument("--ref-linear", type=float, default=300.0)
@@ -264,10 +280,14 @@ def main():
     n = tube.mesh.nodes
     mesh = api.Mesh(tube.mesh)
     amg = args.preconditioner == "amg"
-    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=1e-3 if args.workload == "c1" else DT,
-                          nonlinear_rtol=1e-8, nonlinear_atol=1e-300, mass_rtol=1e-3,
-                          gmres_restart=200, gmres_max_iterations=5000, gmres_rtol=1e-8,
-                          preconditioner=api.AMG if amg else api.BLOCK_JACOBI)
+    mixed = args.precision == "mixed"
+    if mixed and not amg:
+        raise SystemExit("--precision mixed needs --preconditioner amg")
+    solver_kw = dict(density=RHO, viscosity=MU, dt=1e-3 if args.workload == "c1" else DT,
+                     nonlinear_rtol=1e-8, nonlinear_atol=1e-300, mass_rtol=1e-3,
+                     gmres_restart=200, gmres_max_iterations=5000, gmres_rtol=1e-8,
+                     preconditioner=api.AMG if amg else api.BLOCK_JACOBI)
+    ns = api.NavierStokes(mesh, precision=api.MIXED if mixed else api.FP64, **solver_kw)
     dt = ns.params.dt
     vmask, pmask, vel0 = api.tube_boundary_conditions(tube, 1.0)
     profile = vel0.copy()
@@ -299,8 +319,10 @@ def main():
         if host:
             api.check(api.lib().tfiga_ns_get_state(ns._h, api.C.c_void_p(out_host.data_ptr())))
 
+    warm_states = []
     for k in range(args.warmup):
         do_step(k)
+        warm_states.append(ns.get_state())
     reports.clear()
     torch.cuda.synchronize()
     if dist:
@@ -334,6 +356,39 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
 
+    # plain FP64 GPU solver on the warm-up steps from the same initial state: per-step error of the
+    # mixed solution against it, and its own time steps/s (steps after the first, CUDA events)
+    fp64_leg = None
+    if mixed and not args.no_fp64_leg:
+        ref = api.NavierStokes(mesh, precision=api.FP64, **solver_kw)
+        ref.set_dirichlet(vmask, pmask, inlet_factor(wave, 0.0) * profile)
+        ref.set_tractions({2: 0.0})
+        ref.set_state(s0, s0)
+        rstream = torch.cuda.ExternalStream(ref.stream())
+        errors, fp64_ms, fp64_steps = [], 0.0, 0
+        for k in range(args.warmup):
+            api.check(api.lib().tfiga_ns_set_dirichlet_values(ref._h, api.C.c_void_p(bc_dev[k].data_ptr()), None))
+            ref.commit_step()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a0.record(rstream)
+            ref.step()
+            a1.record(rstream)
+            torch.cuda.synchronize()
+            if k > 0:
+                fp64_ms += a0.elapsed_time(a1)
+                fp64_steps += 1
+            r64 = ref.get_state().reshape(-1, 4)
+            mx = warm_states[k].reshape(-1, 4)
+            errors.append({"step": k,
+                           "velocity": float(np.linalg.norm(mx[:, :3] - r64[:, :3]) / np.linalg.norm(r64[:, :3])),
+                           "pressure": float(np.linalg.norm(mx[:, 3] - r64[:, 3]) / np.linalg.norm(r64[:, 3]))})
+        fp64_leg = {"value": fp64_steps / (fp64_ms / 1e3) if fp64_steps else None, "unit": "time steps/s",
+                    "steps": fp64_steps, "ms_per_step": fp64_ms / max(fp64_steps, 1),
+                    "error_vs_fp64_per_step": errors}
+        ref.close()
+        del ref
+
     if dist:
         t = torch.tensor([ms, e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -344,12 +399,16 @@ def main():
         return 0
 
     hbm, bf16, peak_kind = peaks()
+    bf16_sustained = sustained_bf16()
     b_spmv, b_bjac, f_asm = algorithmic_counts(tube, mesh.blocks)
     spmv_ms, spmv_n = prof["spmv"]
     asm_ms, asm_n = prof["assembly"]
     orth_ms, orth_n = prof["krylov_orthogonalisation"]
     amg_ms, amg_n = prof["amg_vcycle"]
     kernels = {}
+    if mixed:
+        # FP32 Jacobian: 4-byte values in every pass over the matrix
+        b_spmv -= mesh.blocks * 16 * 4
     spmv_bytes = b_spmv if amg else b_spmv + b_bjac
     spmv_name = "spmv" if amg else "spmv_block_jacobi"
     if spmv_n:
@@ -367,15 +426,24 @@ def main():
                                  "traffic": None, "launches": amg_n, "avg_ms": amg_ms / amg_n,
                                  "share": amg_ms / ms, "algorithmic_bytes": vbytes,
                                  "levels": ns.amg_info()}
-    if asm_n:
+    asm_name = "assembly_tc" if mixed else "assembly_fp64"
+    if asm_n and mixed:
+        # tensor-core element contraction: F_e = 8192 nen^2 MMA flops per element, timed inside the long
+        # Newton step, so against the sustained bf16 peak
         a = f_asm / (asm_ms / asm_n * 1e-3) / 1e12
-        kernels["assembly_fp64"] = {"bound": "fp64", "achieved": a, "peak": 37.0, "unit": "TFLOP/s",
-                                    "frac": a / 37.0, "traffic": None, "launches": asm_n,
-                                    "avg_ms": asm_ms / asm_n, "share": asm_ms / ms,
-                                    "peak_note": "nominal B200 FP64 (no measured FP64 peak on this pool)"}
+        kernels[asm_name] = {"bound": "tensor", "achieved": a, "peak": bf16_sustained, "unit": "TFLOP/s",
+                             "frac": a / bf16_sustained, "traffic": None, "launches": asm_n,
+                             "avg_ms": asm_ms / asm_n, "share": asm_ms / ms,
+                             "peak_kind": f"{peak_kind} bf16_tflops_sustained"}
+    elif asm_n:
+        a = f_asm / (asm_ms / asm_n * 1e-3) / 1e12
+        kernels[asm_name] = {"bound": "fp64", "achieved": a, "peak": 37.0, "unit": "TFLOP/s",
+                             "frac": a / 37.0, "traffic": None, "launches": asm_n,
+                             "avg_ms": asm_ms / asm_n, "share": asm_ms / ms,
+                             "peak_note": "nominal B200 FP64 (no measured FP64 peak on this pool)"}
     kernels["krylov_orthogonalisation"] = {"avg_ms": orth_ms / max(orth_n, 1), "launches": orth_n,
                                            "share": orth_ms / ms}
-    dominant = max((spmv_name, "assembly_fp64", "amg_vcycle"), key=lambda k: kernels.get(k, {}).get("share", 0))
+    dominant = max((spmv_name, asm_name, "amg_vcycle"), key=lambda k: kernels.get(k, {}).get("share", 0))
     roof = dict(kernels[dominant])
     roof["kernel"] = dominant
     if roof["bound"] == "hbm":
@@ -387,15 +455,19 @@ def main():
     line = {
         "metric": METRIC, "value": steps_per_s, "unit": "time steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator; BASELINE publishes no dataset)",
+        "vs_baseline": None, "dtype": "bf16-tc/f32/f64" if mixed else "f64",
+        "data": "synthetic (seeded generator; BASELINE publishes no dataset)",
         "config": {"workload": desc, "elements": tube.mesh.elements, "nodes": n, "block_nonzeros": mesh.blocks,
-                   "solver": ("plain FP64: exact-tangent Newton to rel.res 1e-8, " +
+                   "solver": (("mixed: tcgen05 BF16 tangent (FP32 accumulate), FP32 Jacobian, FP64 residual and "
+                               "refinement; " if mixed else "plain FP64: ") +
+                              "exact-tangent Newton to rel.res 1e-8, " +
                               ("point-block AMG V(1,1)-preconditioned FGMRES(200) rtol 1e-8" if amg else
                                "block-Jacobi GMRES(200) rtol 1e-8")),
                    "l2": "inputs larger than L2 (matrix %.2f GB)" % (mesh.blocks * 128 / 1e9),
                    "parallelism": "replicas only" if world > 1 else "single GPU"},
         "newton_per_step": float(newton), "linear_iterations_per_newton": float(linear),
         "roofline": roof, "kernels": kernels,
+        "fp64_gpu": fp64_leg,
         "spmv_gbs": kernels.get(spmv_name, {}).get("achieved"),
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
