@@ -231,6 +231,10 @@ int tfiga_ns_stream(tfiga_ns* ns, void** stream);
 int tfiga_ns_set_profiling(tfiga_ns* ns, int enable);
 /* Totals since the last reset: milliseconds and launch counts per family. */
 int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int32_t reset);
+/* Algorithmic bytes per family since the last reset, as the solver accounts
+ * them while profiling is on (family 2, Krylov orthogonalisation: 8 n (4 (j+1)
+ * + 6) per Arnoldi step j; the other families report 0). */
+int tfiga_ns_profile_bytes(tfiga_ns* ns, double* bytes);
 
 /* ---- allocation-free kernel ------------------------------------------- */
 /* *norm_device = ||b - A x||_2 for a 4x4 block-CSR matrix given entirely by

@@ -111,6 +111,7 @@ SIGNATURES = {
     "tfiga_ns_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "tfiga_ns_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "tfiga_ns_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "tfiga_ns_profile_bytes": (C.c_int, [C.c_void_p, C.c_void_p]),
     "tfiga_block_residual_norm_static": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                    C.c_void_p, C.c_void_p, C.c_void_p]),
     "tfiga_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
@@ -300,6 +301,11 @@ class NavierStokes:
         check(lib().tfiga_ns_amg_info(self._h, C.byref(info)))
         return {"levels": info.levels, "nodes": list(info.nodes[:info.levels]),
                 "blocks": list(info.blocks[:info.levels])}
+
+    def profile_bytes(self) -> dict:
+        b = np.zeros(4)
+        check(lib().tfiga_ns_profile_bytes(self._h, _p(b)))
+        return {f: float(b[i]) for i, f in enumerate(self.FAMILIES)}
 
     def profile(self, reset=False) -> dict:
         ms = np.zeros(4)

@@ -1,5 +1,6 @@
 // Point-block aggregation AMG: host setup, device refresh and V-cycle (see amg.hpp).
 #include "amg.hpp"
+#include "block_row.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -83,61 +84,27 @@ __global__ void UnitDiagonalKernel(int nodes, const int32_t* __restrict__ diag, 
 	if (mask[i] == 0.0) values[(size_t)diag[node]*16+c*4+c] = 1.0;
 }
 
-// r = b - A x (warp per block row); x may be null (r = b).
-template <class T> struct RowLoad;
-template <> struct RowLoad<double> {
-	static __device__ __forceinline__ void Get(const double* v, long long k, int r, double a[4])
-	{
-		const double2* p = reinterpret_cast<const double2*>(v+(size_t)k*16+r*4);
-		const double2 a01 = __ldg(p), a23 = __ldg(p+1);
-		a[0] = a01.x; a[1] = a01.y; a[2] = a23.x; a[3] = a23.y;
-	}
-};
-template <> struct RowLoad<float> {
-	static __device__ __forceinline__ void Get(const float* v, long long k, int r, double a[4])
-	{
-		const float4 q = __ldg(reinterpret_cast<const float4*>(v+(size_t)k*16+r*4));
-		a[0] = q.x; a[1] = q.y; a[2] = q.z; a[3] = q.w;
-	}
-};
-
+// z = t + omega D^{-1} (b - A t): the residual of the coarse correction t and
+// the block-Jacobi step on it, fused (warp per block row; lanes 0..3 hold the
+// row's residual, lane c applies row c of the node's 4x4 inverse).
 template <class T>
-__global__ void __launch_bounds__(256) ResidualKernel(DevicePatternView p, const T* __restrict__ values,
-	const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ r, const int* __restrict__ stop)
+__global__ void __launch_bounds__(256) ResidualJacobiKernel(DevicePatternView p, const T* __restrict__ values,
+	const double* __restrict__ t, const double* __restrict__ b, const double* __restrict__ inverse, double omega,
+	double* __restrict__ z, const int* __restrict__ stop)
 {
 	if (*stop) return;
 	const int row = blockIdx.x*8+(threadIdx.x >> 5);
 	const int lane = threadIdx.x & 31;
 	if (row >= p.nodes) return;
-	const int rr = lane & 3, slot = lane >> 2;
-	double sum = 0.0;
-	for (int k = p.row_offsets[row]+slot; k < p.row_offsets[row+1]; k += 8) {
-		double a[4];
-		RowLoad<T>::Get(values, k, rr, a);
-		const double2* xv = reinterpret_cast<const double2*>(x+4*(size_t)p.columns[k]);
-		const double2 x01 = __ldg(xv), x23 = __ldg(xv+1);
-		sum = fma(a[0], x01.x, sum); sum = fma(a[1], x01.y, sum);
-		sum = fma(a[2], x23.x, sum); sum = fma(a[3], x23.y, sum);
+	const double ax = RowBlockDot(p, values, t, row, lane);
+	const size_t i = 4*(size_t)row+(lane & 3);
+	const double r = lane < 4 ? b[i]-ax : 0.0;
+	const double r0 = __shfl_sync(0xffffffffu, r, 0), r1 = __shfl_sync(0xffffffffu, r, 1);
+	const double r2 = __shfl_sync(0xffffffffu, r, 2), r3 = __shfl_sync(0xffffffffu, r, 3);
+	if (lane < 4) {
+		const double* d = inverse+(size_t)row*16+lane*4;
+		z[i] = t[i]+omega*(d[0]*r0+d[1]*r1+d[2]*r2+d[3]*r3);
 	}
-	sum += __shfl_xor_sync(0xffffffffu, sum, 4);
-	sum += __shfl_xor_sync(0xffffffffu, sum, 8);
-	sum += __shfl_xor_sync(0xffffffffu, sum, 16);
-	if (lane < 4) r[4*(size_t)row+lane] = b[4*(size_t)row+lane]-sum;
-}
-
-// x = omega D^{-1} r (zero initial guess) or x += omega D^{-1} r; thread per DOF.
-__global__ void JacobiKernel(int nodes, const double* __restrict__ inverse, const double* __restrict__ r,
-	double* __restrict__ x, double omega, int accumulate, const int* __restrict__ stop)
-{
-	if (*stop) return;
-	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
-	if (i >= 4LL*nodes) return;
-	const long long node = i >> 2;
-	const int c = (int)(i & 3);
-	const double* d = inverse+node*16+c*4;
-	const double* v = r+4*node;
-	const double z = omega*(d[0]*v[0]+d[1]*v[1]+d[2]*v[2]+d[3]*v[3]);
-	x[i] = accumulate ? x[i]+z : z;
 }
 
 // b_c[I,c] = sum_{i in I} mask_i[c] r[i,c]: one CTA per aggregate, fixed-order reduction.
@@ -572,13 +539,13 @@ void Amg::Cycle(int l, const T* A, const double* b, double* x, const int* stop)
 	LaunchCheck("RestrictKernel");
 	DenseApplyKernel<<<Grid(C.dense_n, 8), 256, 0, stream_>>>(C.dense_n, C.dense.get(), C.b.get(), C.x.get(), stop);
 	LaunchCheck("DenseApplyKernel");
-	ProlongKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(), C.x.get(), x, stop);
+	ProlongKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(), C.x.get(), L.x.get(),
+		stop);
 	LaunchCheck("ProlongKernel");
-	ResidualKernel<T><<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, x, b, L.r.get(), stop);
-	LaunchCheck("ResidualKernel");
-	JacobiKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.inverse.get(), L.r.get(), x, options_.omega, 1, stop);
-	LaunchCheck("JacobiKernel");
-	launches_ += 5;
+	ResidualJacobiKernel<T><<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, L.x.get(), b, L.inverse.get(),
+		options_.omega, x, stop);
+	LaunchCheck("ResidualJacobiKernel");
+	launches_ += 4;
 }
 
 template <class T>

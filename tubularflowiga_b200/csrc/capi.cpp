@@ -382,4 +382,12 @@ int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int3
 	});
 }
 
+int tfiga_ns_profile_bytes(tfiga_ns* ns, double* bytes)
+{
+	return Guard([&] {
+		Require(ns && bytes, "null argument");
+		ns->solver->profiler().Totals(nullptr, nullptr, false, bytes);
+	});
+}
+
 } // extern "C"

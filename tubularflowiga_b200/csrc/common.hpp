@@ -108,7 +108,9 @@ public:
 	void Begin(Family family, cudaStream_t stream);
 	void End(cudaStream_t stream);
 	void Collect();
-	void Totals(double* ms, long long* counts, bool reset);
+	// Algorithmic bytes a family moved (accounted by the caller, only while enabled).
+	void AddBytes(Family family, double bytes) { if (enabled_) bytes_[family] += bytes; }
+	void Totals(double* ms, long long* counts, bool reset, double* bytes = nullptr);
 
 private:
 	struct Mark { cudaEvent_t start, stop; int family; };
@@ -118,6 +120,7 @@ private:
 	int open_ = -1;
 	double ms_[kFamilies] = {0, 0, 0, 0};
 	long long count_[kFamilies] = {0, 0, 0, 0};
+	double bytes_[kFamilies] = {0, 0, 0, 0};
 };
 
 } // namespace tfiga

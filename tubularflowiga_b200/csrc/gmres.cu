@@ -7,32 +7,55 @@
 namespace tfiga {
 namespace {
 
-constexpr int kBlocks = 296;          // 2 CTAs per SM for the streaming passes
+constexpr int kBlocks = 592;          // 4 CTAs per SM for the streaming passes
 constexpr int kThreads = 256;
+constexpr int kWarps = kThreads/32;
 constexpr int kBatch = 8;             // Arnoldi steps launched per host wait
 
-// partial[i*blocks + cta] = scale[i] * <V_i, w> over this CTA's chunk.
+// partial[i*blocks + cta] = scale[i] * <V_i, w> over this CTA's chunk.  The
+// chunk is a multiple of 128 doubles and n is even, so every row slice is
+// 16-byte aligned: a warp streams two basis vectors at once with 16-byte
+// loads, two steps per iteration, to keep enough bytes in flight for HBM.
 __global__ void __launch_bounds__(kThreads) MultiDotKernel(const double* __restrict__ V, long long n,
 	const double* __restrict__ scale, int count, const double* __restrict__ w, double* __restrict__ partial,
 	int chunk, const int* __restrict__ stop)
 {
 	if (*stop) return;
 	extern __shared__ double wchunk[];
+	double2* w2 = reinterpret_cast<double2*>(wchunk);
 	const long long lo = (long long)blockIdx.x*chunk;
 	const long long rest = n-lo;
-	const int len = rest <= 0 ? 0 : (rest < chunk ? (int)rest : chunk);
-	for (int k = threadIdx.x; k < len; k += blockDim.x) wchunk[k] = w[lo+k];
+	const int len2 = (rest <= 0 ? 0 : (rest < chunk ? (int)rest : chunk)) >> 1;
+	const double2* win = reinterpret_cast<const double2*>(w+lo);
+	for (int k = threadIdx.x; k < len2; k += blockDim.x) w2[k] = win[k];
 	__syncthreads();
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	for (int i = warp; i < count; i += kThreads/32) {
-		const double* vi = V+(size_t)i*n+lo;
-		double s0 = 0.0, s1 = 0.0;
-		int k = lane;
-		for (; k+32 < len; k += 64) { s0 = fma(vi[k], wchunk[k], s0); s1 = fma(vi[k+32], wchunk[k+32], s1); }
-		if (k < len) s0 = fma(vi[k], wchunk[k], s0);
-		double s = s0+s1;
-		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-		if (lane == 0) partial[(size_t)i*gridDim.x+blockIdx.x] = s*scale[i];
+	const double2 zero = make_double2(0.0, 0.0);
+	for (int i0 = warp; i0 < count; i0 += 2*kWarps) {
+		const int i1 = i0+kWarps;
+		const bool two = i1 < count;
+		const double2* a = reinterpret_cast<const double2*>(V+(size_t)i0*n+lo);
+		const double2* b = reinterpret_cast<const double2*>(V+(size_t)(two ? i1 : i0)*n+lo);
+		double sa = 0.0, sb = 0.0, ta = 0.0, tb = 0.0;
+		for (int k = lane; k < len2; k += 64) {
+			const bool more = k+32 < len2;
+			const double2 x0 = a[k], y0 = b[k];
+			const double2 x1 = more ? a[k+32] : zero, y1 = more ? b[k+32] : zero;
+			const double2 w0 = w2[k], w1 = more ? w2[k+32] : zero;
+			sa = fma(x0.x, w0.x, sa); sa = fma(x0.y, w0.y, sa);
+			sb = fma(y0.x, w0.x, sb); sb = fma(y0.y, w0.y, sb);
+			ta = fma(x1.x, w1.x, ta); ta = fma(x1.y, w1.y, ta);
+			tb = fma(y1.x, w1.x, tb); tb = fma(y1.y, w1.y, tb);
+		}
+		double u = sa+ta, v = sb+tb;
+		for (int o = 16; o > 0; o >>= 1) {
+			u += __shfl_xor_sync(0xffffffffu, u, o);
+			v += __shfl_xor_sync(0xffffffffu, v, o);
+		}
+		if (lane == 0) {
+			partial[(size_t)i0*gridDim.x+blockIdx.x] = u*scale[i0];
+			if (two) partial[(size_t)i1*gridDim.x+blockIdx.x] = v*scale[i1];
+		}
 	}
 }
 
@@ -57,6 +80,8 @@ __global__ void __launch_bounds__(kThreads) DotFinalizeKernel(const double* __re
 }
 
 // out = w - sum_i scale_i hpass_i V_i; norm_partial[cta] = sum out^2 (if non-null).
+// out may alias w.  Each thread owns 16-byte pairs of entries and walks the
+// basis four vectors at a time (the FMA order per entry is the basis order).
 __global__ void __launch_bounds__(kThreads) UpdateKernel(const double* __restrict__ V, long long n,
 	const double* __restrict__ scale, int count, const double* __restrict__ hpass, const double* win, double* out,
 	double* __restrict__ norm_partial, const int* __restrict__ stop)
@@ -65,26 +90,38 @@ __global__ void __launch_bounds__(kThreads) UpdateKernel(const double* __restric
 	extern __shared__ double coef[];
 	for (int i = threadIdx.x; i < count; i += blockDim.x) coef[i] = scale[i]*hpass[i];
 	__syncthreads();
+	const long long n2 = n >> 1;
+	const double2* V2 = reinterpret_cast<const double2*>(V);
+	const double2* w2 = reinterpret_cast<const double2*>(win);
+	double2* o2 = reinterpret_cast<double2*>(out);
 	double sq = 0.0;
-	for (long long k = (long long)blockIdx.x*blockDim.x+threadIdx.x; k < n; k += (long long)gridDim.x*blockDim.x) {
-		double v = win[k];
+	for (long long k = (long long)blockIdx.x*blockDim.x+threadIdx.x; k < n2; k += (long long)gridDim.x*blockDim.x) {
+		double2 v = w2[k];
 		int i = 0;
-		for (; i+1 < count; i += 2) {
-			v = fma(-coef[i], V[(size_t)i*n+k], v);
-			v = fma(-coef[i+1], V[(size_t)(i+1)*n+k], v);
+		for (; i+3 < count; i += 4) {
+			const double2 a0 = V2[(size_t)i*n2+k], a1 = V2[(size_t)(i+1)*n2+k];
+			const double2 a2 = V2[(size_t)(i+2)*n2+k], a3 = V2[(size_t)(i+3)*n2+k];
+			v.x = fma(-coef[i], a0.x, v.x); v.y = fma(-coef[i], a0.y, v.y);
+			v.x = fma(-coef[i+1], a1.x, v.x); v.y = fma(-coef[i+1], a1.y, v.y);
+			v.x = fma(-coef[i+2], a2.x, v.x); v.y = fma(-coef[i+2], a2.y, v.y);
+			v.x = fma(-coef[i+3], a3.x, v.x); v.y = fma(-coef[i+3], a3.y, v.y);
 		}
-		if (i < count) v = fma(-coef[i], V[(size_t)i*n+k], v);
-		out[k] = v;
-		sq = fma(v, v, sq);
+		for (; i < count; ++i) {
+			const double2 a0 = V2[(size_t)i*n2+k];
+			v.x = fma(-coef[i], a0.x, v.x); v.y = fma(-coef[i], a0.y, v.y);
+		}
+		o2[k] = v;
+		sq = fma(v.x, v.x, sq);
+		sq = fma(v.y, v.y, sq);
 	}
 	if (norm_partial == nullptr) return;
-	__shared__ double red[kThreads/32];
+	__shared__ double red[kWarps];
 	for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
 	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
 	__syncthreads();
 	if (threadIdx.x == 0) {
 		double s = 0.0;
-		for (int w = 0; w < kThreads/32; ++w) s += red[w];
+		for (int w = 0; w < kWarps; ++w) s += red[w];
 		norm_partial[blockIdx.x] = s;
 	}
 }
@@ -192,13 +229,22 @@ __global__ void ResidualKernel(long long n, const double* __restrict__ rhs, cons
 	if (i < n) r[i] = rhs[i]-ax[i];
 }
 
+// Bytes classical Gram-Schmidt twice moves over one cycle of `used` Arnoldi
+// steps: step j reads the j+1 basis vectors and w in each multi-dot, reads
+// them again and writes w in each update, two passes: 8 n (4 (j+1) + 6).
+double OrthoBytes(long long n, int used)
+{
+	return 8.0*(double)n*(2.0*used*(used+1.0)+6.0*used);
+}
+
 } // namespace
 
 Gmres::Gmres(int nodes, int restart, cudaStream_t stream)
 	: nodes_(nodes), n_(4*nodes), restart_(restart), blocks_(kBlocks), stream_(stream)
 {
 	if (nodes <= 0 || restart <= 0) Fail(-1, "GMRES workspace dimensions must be positive");
-	chunk_ = (int)std::max<long long>(256, ((long long)n_+blocks_-1)/blocks_);
+	// multi-dot chunk per CTA: a multiple of 128 doubles (16-byte aligned row slices, two-step unroll)
+	chunk_ = (int)((((long long)n_+blocks_-1)/blocks_+127)/128*128);
 	V_.Allocate((size_t)(restart+1)*n_);
 	w_.Allocate(n_); r_.Allocate(n_); tmp_.Allocate(n_);
 	inverse_.Allocate((size_t)nodes*16);
@@ -207,7 +253,7 @@ Gmres::Gmres(int nodes, int restart, cudaStream_t stream)
 	H_.Allocate((size_t)(restart+1)*restart);
 	cs_.Allocate(restart); sn_.Allocate(restart); g_.Allocate(restart+1); y_.Allocate(restart);
 	scale_.Allocate(restart+1);
-	norm_partial_.Allocate(PartialSlots());
+	norm_partial_.Allocate(std::max(PartialSlots(), blocks_));
 	scalar_.Allocate(2);
 	state_.Allocate(4);
 	residual_.Allocate(1);
@@ -344,6 +390,7 @@ GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const T* valu
 		}
 		const int used = host_->used;
 		result.iterations += used;
+		if (profiler_) profiler_->AddBytes(Profiler::kOrtho, OrthoBytes(n_, used));
 		BackSolveKernel<<<1, 1, 0, stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(), state_.get()+2);
 		LaunchCheck("BackSolveKernel");
 		SolutionUpdateKernel<<<blocks_, kThreads, (size_t)(restart_+1)*sizeof(double), stream_>>>(Z_.get(), n_,
@@ -420,6 +467,7 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 		}
 		const int used = host_->used;
 		result.iterations += used;
+		if (profiler_) profiler_->AddBytes(Profiler::kOrtho, OrthoBytes(n_, used));
 		result.residual = host_->residual;
 		BackSolveKernel<<<1, 1, 0, stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(),
 			state_.get()+2);

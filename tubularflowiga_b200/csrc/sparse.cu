@@ -2,11 +2,8 @@
 // apply), diagonal-block inverse, Dirichlet rows, boundary-face flows and
 // tractions, and deterministic two-stage reductions.
 //
-// SpMV layout: one warp per block row; lane = 4*slot + r processes row r of
-// blocks slot, slot+8, ... so each warp load covers 8 consecutive 128-byte
-// blocks (coalesced), then the 8 slots are reduced with shuffles.  This
-// replaces the reference's thread-per-row BlockSpmvKernel
-// (solvers/cuda/include/SparseKernels.cuh:25-40), whose loads are strided.
+// SpMV layout: one warp per block row (block_row.cuh).
+#include "block_row.cuh"
 #include "common.hpp"
 #include "kernels.cuh"
 
@@ -14,47 +11,6 @@ namespace tfiga {
 namespace {
 
 constexpr int kReduceBlocks = 296;   // 2 CTAs per SM for the partial-sum stage
-
-template <class T> struct BlockRow;
-template <> struct BlockRow<double> {
-	// row r of block b: 4 doubles (two 128-bit loads)
-	static __device__ __forceinline__ void Load(const double* values, long long b, int r, double a[4])
-	{
-		const double2* p = reinterpret_cast<const double2*>(values+(size_t)b*16+r*4);
-		const double2 a01 = __ldg(p), a23 = __ldg(p+1);
-		a[0] = a01.x; a[1] = a01.y; a[2] = a23.x; a[3] = a23.y;
-	}
-};
-template <> struct BlockRow<float> {
-	// row r of block b: 4 floats (one 128-bit load)
-	static __device__ __forceinline__ void Load(const float* values, long long b, int r, double a[4])
-	{
-		const float4 v = __ldg(reinterpret_cast<const float4*>(values+(size_t)b*16+r*4));
-		a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
-	}
-};
-
-template <class T>
-__device__ __forceinline__ double RowBlockDot(const DevicePatternView& p, const T* __restrict__ values,
-	const double* __restrict__ x, int row, int lane)
-{
-	const int r = lane & 3, slot = lane >> 2;
-	double sum = 0.0;
-	const int lo = p.row_offsets[row], hi = p.row_offsets[row+1];
-	for (int b = lo+slot; b < hi; b += 8) {
-		const int col = p.columns[b];
-		double a[4];
-		BlockRow<T>::Load(values, b, r, a);
-		const double2* xv = reinterpret_cast<const double2*>(x+4*(size_t)col);
-		const double2 x01 = __ldg(xv), x23 = __ldg(xv+1);
-		sum = fma(a[0], x01.x, sum); sum = fma(a[1], x01.y, sum);
-		sum = fma(a[2], x23.x, sum); sum = fma(a[3], x23.y, sum);
-	}
-	sum += __shfl_xor_sync(0xffffffffu, sum, 4);
-	sum += __shfl_xor_sync(0xffffffffu, sum, 8);
-	sum += __shfl_xor_sync(0xffffffffu, sum, 16);
-	return sum;   // lanes 0..3 hold rows 0..3
-}
 
 template <class T>
 __global__ void __launch_bounds__(256) SpmvKernel(DevicePatternView p, const T* __restrict__ values,

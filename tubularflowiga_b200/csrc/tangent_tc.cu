@@ -13,7 +13,7 @@
 // pair.
 //
 // Work split.  One CTA per (element, pair of row fields h: i in {2h, 2h+1}),
-// 256 threads, about 107 KiB of shared memory so that two CTAs share an SM
+// 256 threads, about 109 KiB of shared memory so that two CTAs share an SM
 // and one CTA's scatter overlaps the other's operand build.  Four M = 128
 // accumulator tiles (tile T: row field 2h + T/2, basis b in [32 (T&1), +32),
 // tile row m = 4 (b mod 32) + f) live in 4 x 64 = 256 TMEM columns.
@@ -45,16 +45,18 @@ constexpr int kTiles = 4;                        // M = 128 tiles per CTA
 constexpr int kTileBytes = 128*64;               // 128 rows x 32 BF16 (64 B, one swizzle row)
 constexpr int kTmemCols = 256;                   // 4 tiles x N = 64 FP32 columns
 constexpr unsigned long long kWaitNs = 1000000000ull;
+constexpr int kCoefStride = kCoef+1;             // odd float stride: point-per-thread writes hit distinct banks
+constexpr int kRcStride = 5;                     // doubles per (field, point) residual coefficient row
 
 // Shared-memory layout (bytes from a 1024-aligned base).
 constexpr int kOffA = 0;                                         // 4 tiles x 8 KiB
 constexpr int kOffB = kOffA+kTiles*kTileBytes;                   // Psi: 64 rows x 64 B
 constexpr int kOffPhi = kOffB+64*64;                             // float [5][kPts][64]
-constexpr int kOffCoef = kOffPhi+kFeatures*kPts*64*4;            // float [2][64][kCoef]
-constexpr int kOffRC = kOffCoef+2*kQuad*kCoef*4;                 // double [2][64][4]
-constexpr int kOffQS = kOffRC+2*kQuad*4*8;                       // double [64][kQS]; reused as [256] partials
-constexpr int kOffU = kOffQS+kQuad*kQS*8;                        // double [64][4]
-constexpr int kOffUp = kOffU+64*4*8;                             // double [64][4]
+constexpr int kOffCoef = kOffPhi+kFeatures*kPts*64*4;            // float [2][64][kCoefStride]
+constexpr int kOffRC = kOffCoef+2*kQuad*kCoefStride*4;           // double [2][64][kRcStride]
+constexpr int kOffQS = kOffRC+2*kQuad*kRcStride*8;               // double [64][kQS]; reused as [256] partials
+constexpr int kOffU = kOffQS+kQuad*kQS*8;                        // double [4 fields][64]
+constexpr int kOffUp = kOffU+64*4*8;                             // double [4 fields][64]
 constexpr int kOffBar = kOffUp+64*4*8;                           // mbarrier, TMEM slot
 constexpr int kSmemBytes = kOffBar+16+1024;                      // + alignment slack
 static_assert(kSmemBytes <= 113*1024, "two CTAs per SM");
@@ -213,8 +215,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 			s0 = state[4*node]; s1 = state[4*node+1]; s2 = state[4*node+2]; s3 = state[4*node+3];
 			if (prm.dt > 0.0) { p0 = previous[4*node]; p1 = previous[4*node+1]; p2 = previous[4*node+2]; }
 		}
-		U[a*4] = s0; U[a*4+1] = s1; U[a*4+2] = s2; U[a*4+3] = s3;
-		Up[a*4] = p0; Up[a*4+1] = p1; Up[a*4+2] = p2; Up[a*4+3] = 0.0;
+		U[a] = s0; U[64+a] = s1; U[128+a] = s2; U[192+a] = s3;
+		Up[a] = p0; Up[64+a] = p1; Up[128+a] = p2; Up[192+a] = 0.0;
 	}
 	FenceBeforeSync();
 	__syncthreads();
@@ -230,9 +232,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 			const double n = P[(0*kQuad+q)*kMaxBasis+a];
 			const double g0 = P[(1*kQuad+q)*kMaxBasis+a], g1 = P[(2*kQuad+q)*kMaxBasis+a];
 			const double g2 = P[(3*kQuad+q)*kMaxBasis+a], l = P[(4*kQuad+q)*kMaxBasis+a];
-			const double uf[4] = {U[a*4], U[a*4+1], U[a*4+2], U[a*4+3]};
+			const double uf[4] = {U[a], U[64+a], U[128+a], U[192+a]};
 			v[0] += n*uf[0]; v[1] += n*uf[1]; v[2] += n*uf[2]; v[3] += n*uf[3];
-			v[4] += n*Up[a*4]; v[5] += n*Up[a*4+1]; v[6] += n*Up[a*4+2];
+			v[4] += n*Up[a]; v[5] += n*Up[64+a]; v[6] += n*Up[128+a];
 			#pragma unroll
 			for (int f = 0; f < 4; ++f) { v[7+3*f] += g0*uf[f]; v[8+3*f] += g1*uf[f]; v[9+3*f] += g2*uf[f]; }
 			v[19] += l*uf[0]; v[20] += l*uf[1]; v[21] += l*uf[2];
@@ -257,8 +259,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 			for (int d = 0; d < 3; ++d) S.gv[c][d] = s[kGrad+3*c+d];
 		}
 		S.p = s[kP];
-		RowCoefficients<float>(2*h+il, S, qdata+((size_t)e*kQuad+q)*kQData, prm, Coef+(il*kQuad+q)*kCoef,
-			RC+(il*kQuad+q)*4);
+		RowCoefficients<float>(2*h+il, S, qdata+((size_t)e*kQuad+q)*kQData, prm, Coef+(il*kQuad+q)*kCoefStride,
+			RC+(il*kQuad+q)*kRcStride);
 	}
 	__syncthreads();
 
@@ -268,7 +270,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		double r = 0.0;
 		for (int q = half*32; q < half*32+32; ++q)
 			#pragma unroll
-			for (int s = 0; s < 4; ++s) r += P[(s*kQuad+q)*kMaxBasis+a]*RC[(il*kQuad+q)*4+s];
+			for (int s = 0; s < 4; ++s) r += P[(s*kQuad+q)*kMaxBasis+a]*RC[(il*kQuad+q)*kRcStride+s];
 		__syncthreads();                       // QS is dead: reuse it for the partial sums
 		QS[tid] = r;
 		__syncthreads();
@@ -305,9 +307,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		{
 			const int ql0 = 2*gqp;
 			float m0[20], m1[20];
-			const float* c0 = Coef+(gil*kQuad+q0+ql0)*kCoef+gf*20;
+			const float* c0 = Coef+(gil*kQuad+q0+ql0)*kCoefStride+gf*20;
 			#pragma unroll
-			for (int k = 0; k < 20; ++k) { m0[k] = c0[k]; m1[k] = c0[kCoef+k]; }
+			for (int k = 0; k < 20; ++k) { m0[k] = c0[k]; m1[k] = c0[kCoefStride+k]; }
 			#pragma unroll 2
 			for (int bg = 0; bg < 8; ++bg) {
 				const int b = bg*8+gbs;
@@ -355,6 +357,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 			const int tile = il*2+th;
 			const int b = th*32+quarter*8+(lane >> 2);
 			for (int ah = 0; ah < 2; ++ah) {
+				int blocks[8];                // block of (a = 32 ah + 4 g + f, b), fetched before the TMEM load
+				#pragma unroll
+				for (int g = 0; g < 8; ++g) {
+					const int a = ah*32+4*g+f;
+					blocks[g] = (a < nen && b < nen) ? EB[a*kMaxBasis+b] : -1;
+				}
 				float v[32];
 				TmemLoad32(tmem+((uint32_t)(quarter*32) << 16)+tile*64+ah*32, v);
 				#pragma unroll
@@ -369,11 +377,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 						o0 = src == 0 ? got : o0; o1 = src == 1 ? got : o1;
 						o2 = src == 2 ? got : o2; o3 = src == 3 ? got : o3;
 					}
-					const int a = ah*32+4*g+f;
-					if (a < nen && b < nen) {
-						const int block = EB[a*kMaxBasis+b];
-						if (block >= 0) RedAdd4(values+(size_t)block*16+i*4, o0, o1, o2, o3);
-					}
+					if (blocks[g] >= 0) RedAdd4(values+(size_t)blocks[g]*16+i*4, o0, o1, o2, o3);
 				}
 			}
 		}
