@@ -425,11 +425,14 @@ def main():
                               "avg_ms": spmv_ms / spmv_n, "share": spmv_ms / ms,
                               "algorithmic_bytes": spmv_bytes}
     if amg_n:
-        # one two-level application on the fine level: one residual pass over A (b_spmv), the
-        # block-Jacobi inverse (128 B per node) and six more vector passes (restriction reads b and
-        # the mask, prolongation reads the mask and writes the correction, the fused residual-Jacobi
-        # step reads b and writes z); the dense coarse solve is a few percent on top.
-        vbytes = b_spmv + n * 128 + 6 * 4 * n * 8
+        # one two-level application: restriction (b, mask, aggregate order), the dense coarse inverse
+        # (dn^2 doubles), and the fused fine-level correction, which reads b, the mask, the aggregate
+        # map, the A P blocks with their column indices and row offsets, the block-Jacobi inverse
+        # (128 B per node), and writes z.  The smoother's residual goes through A P, so no pass over A.
+        info = ns.amg_info()
+        dn = 4 * info["nodes"][-1]
+        ap = info["transfer_blocks"]
+        vbytes = (2 * 4 * n * 8 + 4 * n) + dn * dn * 8 + (3 * 4 * n * 8 + 2 * 4 * n + ap * (128 + 4) + n * 128)
         a = vbytes / (amg_ms / amg_n * 1e-3) / 1e9
         kernels["amg_vcycle"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s", "frac": a / hbm,
                                  "traffic": None, "launches": amg_n, "avg_ms": amg_ms / amg_n,

@@ -129,6 +129,7 @@ typedef struct tfiga_amg_info {
 	int32_t levels;
 	int32_t nodes[8];
 	int64_t blocks[8];
+	int64_t transfer_blocks;      /* 4x4 blocks of A P (fine operator times prolongation) */
 } tfiga_amg_info;
 
 /* One physical step (the Newton loop of iga_cuda.cu:956-1054). */

@@ -53,7 +53,8 @@ AMG = 1
 
 
 class AmgInfo(C.Structure):
-    _fields_ = [("levels", C.c_int32), ("nodes", C.c_int32 * 8), ("blocks", C.c_int64 * 8)]
+    _fields_ = [("levels", C.c_int32), ("nodes", C.c_int32 * 8), ("blocks", C.c_int64 * 8),
+                ("transfer_blocks", C.c_int64)]
 
 
 class NewtonReport(C.Structure):
@@ -300,7 +301,7 @@ class NavierStokes:
         info = AmgInfo()
         check(lib().tfiga_ns_amg_info(self._h, C.byref(info)))
         return {"levels": info.levels, "nodes": list(info.nodes[:info.levels]),
-                "blocks": list(info.blocks[:info.levels])}
+                "blocks": list(info.blocks[:info.levels]), "transfer_blocks": int(info.transfer_blocks)}
 
     def profile_bytes(self) -> dict:
         b = np.zeros(4)

@@ -1,6 +1,5 @@
 // Point-block aggregation AMG: host setup, device refresh and V-cycle (see amg.hpp).
 #include "amg.hpp"
-#include "block_row.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -19,6 +18,11 @@ struct Amg::Level {
 	// transfer to the next level
 	std::vector<int32_t> h_agg;
 	DeviceArray<int32_t> agg, agg_order, agg_offsets, gal_order, gal_offsets, block_row;
+	// A P (this level's operator times the masked prolongation): block rows of the fine
+	// nodes, block columns of the coarse nodes, and the fixed-order fine-block lists
+	long long ap_blocks = 0;
+	DeviceArray<int32_t> ap_rows, ap_cols, ap_order, ap_offsets;
+	DeviceArray<double> ap_values;
 	// coarsest level
 	int dense_n = 0;
 	DeviceArray<double> dense, column;
@@ -84,27 +88,64 @@ __global__ void UnitDiagonalKernel(int nodes, const int32_t* __restrict__ diag, 
 	if (mask[i] == 0.0) values[(size_t)diag[node]*16+c*4+c] = 1.0;
 }
 
-// z = t + omega D^{-1} (b - A t): the residual of the coarse correction t and
-// the block-Jacobi step on it, fused (warp per block row; lanes 0..3 hold the
-// row's residual, lane c applies row c of the node's 4x4 inverse).
+// (A P)[i, I] = sum over the fine blocks (i, j) with j in aggregate I of
+// A[i, j] diag(mask_j): a warp per A P block, lanes = (slot, entry), fixed
+// order (deterministic).
 template <class T>
-__global__ void __launch_bounds__(256) ResidualJacobiKernel(DevicePatternView p, const T* __restrict__ values,
-	const double* __restrict__ t, const double* __restrict__ b, const double* __restrict__ inverse, double omega,
-	double* __restrict__ z, const int* __restrict__ stop)
+__global__ void __launch_bounds__(256) ApKernel(long long ap_blocks, const int32_t* __restrict__ order,
+	const int32_t* __restrict__ offsets, const int32_t* __restrict__ fine_cols, const double* __restrict__ mask,
+	const T* __restrict__ values, double* __restrict__ ap)
+{
+	const long long B = ((long long)blockIdx.x*blockDim.x+threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (B >= ap_blocks) return;
+	const int e = lane & 15, slot = lane >> 4;
+	double acc = 0.0;
+	for (int k = offsets[B]+slot; k < offsets[B+1]; k += 2) {
+		const int fb = order[k];
+		acc += mask[4*(size_t)fine_cols[fb]+(e & 3)]*(double)values[(size_t)fb*16+e];
+	}
+	acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+	if (lane < 16) ap[B*16+lane] = acc;
+}
+
+// The fine-level half of the two-level application, one thread per fine node:
+// t = P x_c (masked), r = b - (A P) x_c, z = t + omega D^{-1} r.  Equal to
+// prolongation, residual and block-Jacobi step on the full operator, but it
+// reads the few A P blocks of the row instead of the row of A.
+__global__ void __launch_bounds__(256) CoarseCorrectionKernel(int nodes, const int32_t* __restrict__ agg,
+	const double* __restrict__ mask, const double* __restrict__ xc, const int32_t* __restrict__ ap_rows,
+	const int32_t* __restrict__ ap_cols, const double* __restrict__ ap, const double* __restrict__ b,
+	const double* __restrict__ inverse, double omega, double* __restrict__ z, const int* __restrict__ stop)
 {
 	if (*stop) return;
-	const int row = blockIdx.x*8+(threadIdx.x >> 5);
-	const int lane = threadIdx.x & 31;
-	if (row >= p.nodes) return;
-	const double ax = RowBlockDot(p, values, t, row, lane);
-	const size_t i = 4*(size_t)row+(lane & 3);
-	const double r = lane < 4 ? b[i]-ax : 0.0;
-	const double r0 = __shfl_sync(0xffffffffu, r, 0), r1 = __shfl_sync(0xffffffffu, r, 1);
-	const double r2 = __shfl_sync(0xffffffffu, r, 2), r3 = __shfl_sync(0xffffffffu, r, 3);
-	if (lane < 4) {
-		const double* d = inverse+(size_t)row*16+lane*4;
-		z[i] = t[i]+omega*(d[0]*r0+d[1]*r1+d[2]*r2+d[3]*r3);
+	const int i = blockIdx.x*blockDim.x+threadIdx.x;
+	if (i >= nodes) return;
+	const double2* bv = reinterpret_cast<const double2*>(b+4*(size_t)i);
+	const double2 b01 = bv[0], b23 = bv[1];
+	double r[4] = {b01.x, b01.y, b23.x, b23.y};
+	for (int k = ap_rows[i]; k < ap_rows[i+1]; ++k) {
+		const double2* blk = reinterpret_cast<const double2*>(ap+(size_t)k*16);
+		const double2* xv = reinterpret_cast<const double2*>(xc+4*(size_t)ap_cols[k]);
+		const double2 x01 = xv[0], x23 = xv[1];
+		#pragma unroll
+		for (int row = 0; row < 4; ++row) {
+			const double2 a01 = blk[2*row], a23 = blk[2*row+1];
+			r[row] -= a01.x*x01.x+a01.y*x01.y+a23.x*x23.x+a23.y*x23.y;
+		}
 	}
+	const double* ci = xc+4*(size_t)agg[i];
+	const double* mi = mask+4*(size_t)i;
+	const double2* dinv = reinterpret_cast<const double2*>(inverse+(size_t)i*16);
+	double out[4];
+	#pragma unroll
+	for (int row = 0; row < 4; ++row) {
+		const double2 d01 = dinv[2*row], d23 = dinv[2*row+1];
+		out[row] = mi[row]*ci[row]+omega*(d01.x*r[0]+d01.y*r[1]+d23.x*r[2]+d23.y*r[3]);
+	}
+	double2* zv = reinterpret_cast<double2*>(z+4*(size_t)i);
+	zv[0] = make_double2(out[0], out[1]);
+	zv[1] = make_double2(out[2], out[3]);
 }
 
 // b_c[I,c] = sum_{i in I} mask_i[c] r[i,c]: one CTA per aggregate, fixed-order reduction.
@@ -133,15 +174,6 @@ __global__ void __launch_bounds__(128) RestrictKernel(int coarse_nodes, const in
 	if (threadIdx.x < 4) bc[4*I+threadIdx.x] = red[threadIdx.x][0];
 }
 
-// x[i,c] = mask_i[c] x_c[agg(i), c] (piecewise-constant prolongation).
-__global__ void ProlongKernel(int nodes, const int32_t* __restrict__ agg, const double* __restrict__ mask,
-	const double* __restrict__ xc, double* __restrict__ x, const int* __restrict__ stop)
-{
-	if (*stop) return;
-	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
-	if (i >= 4LL*nodes) return;
-	x[i] = mask[i]*xc[4*(size_t)agg[i >> 2]+(i & 3)];
-}
 
 __global__ void DenseScatterKernel(DevicePatternView p, const double* __restrict__ values, int n, double* __restrict__ dense)
 {
@@ -259,6 +291,11 @@ std::vector<int> Amg::level_nodes() const
 	std::vector<int> out;
 	for (const auto& l : levels_) out.push_back(l->nodes);
 	return out;
+}
+
+long long Amg::transfer_blocks() const
+{
+	return levels_.empty() ? 0 : levels_[0]->ap_blocks;
 }
 
 std::vector<long long> Amg::level_blocks() const
@@ -425,6 +462,31 @@ void Amg::BuildFromStrength(std::vector<double> s)
 		std::vector<int32_t> fill(goff.begin(), goff.end()-1);
 		for (long long k = 0; k < L.blocks; ++k) gorder[fill[target[k]]++] = (int32_t)k;
 	}
+	// A P: per fine row, the distinct aggregates of its column nodes (sorted); every fine block
+	// feeds exactly one A P block
+	std::vector<int32_t> ap_rows(L.nodes+1, 0), ap_cols, ap_target(L.blocks);
+	{
+		std::vector<int32_t> row;
+		for (int i = 0; i < L.nodes; ++i) {
+			row.clear();
+			for (int k = L.h_rows[i]; k < L.h_rows[i+1]; ++k) row.push_back(compose[L.h_cols[k]]);
+			std::sort(row.begin(), row.end());
+			row.erase(std::unique(row.begin(), row.end()), row.end());
+			const int32_t base = (int32_t)ap_cols.size();
+			ap_cols.insert(ap_cols.end(), row.begin(), row.end());
+			ap_rows[i+1] = (int32_t)ap_cols.size();
+			for (int k = L.h_rows[i]; k < L.h_rows[i+1]; ++k)
+				ap_target[k] = base+(int32_t)(std::lower_bound(row.begin(), row.end(), compose[L.h_cols[k]])-row.begin());
+		}
+	}
+	L.ap_blocks = (long long)ap_cols.size();
+	std::vector<int32_t> apoff(L.ap_blocks+1, 0), aporder(L.blocks);
+	for (long long k = 0; k < L.blocks; ++k) ++apoff[ap_target[k]+1];
+	for (long long B = 0; B < L.ap_blocks; ++B) apoff[B+1] += apoff[B];
+	{
+		std::vector<int32_t> fill(apoff.begin(), apoff.end()-1);
+		for (long long k = 0; k < L.blocks; ++k) aporder[fill[ap_target[k]]++] = (int32_t)k;
+	}
 	std::vector<int32_t> aoff(nc+1, 0), aorder(L.nodes);
 	for (int i = 0; i < L.nodes; ++i) ++aoff[compose[i]+1];
 	for (int I = 0; I < nc; ++I) aoff[I+1] += aoff[I];
@@ -435,6 +497,8 @@ void Amg::BuildFromStrength(std::vector<double> s)
 	auto up = [&](DeviceArray<int32_t>& d, const std::vector<int32_t>& h) { d.Allocate(h.size()); d.Upload(h.data(), h.size(), stream_); };
 	up(L.agg, L.h_agg); up(L.agg_order, aorder); up(L.agg_offsets, aoff);
 	up(L.gal_order, gorder); up(L.gal_offsets, goff); up(L.block_row, block_row);
+	up(L.ap_rows, ap_rows); up(L.ap_cols, ap_cols); up(L.ap_order, aporder); up(L.ap_offsets, apoff);
+	L.ap_values.Allocate((size_t)L.ap_blocks*16);
 	levels_.push_back(std::move(fine));
 	levels_.push_back(std::move(C));
 	if (nc > 2048) Fail(-7, "aggregation stalled: coarse space of "+std::to_string(nc)+" nodes is too large for the dense coarse solve");
@@ -494,6 +558,12 @@ void Amg::Refresh(const T* values)
 			GalerkinKernel<double><<<(unsigned)C.blocks, 128, 0, stream_>>>(C.blocks, L.gal_order.get(),
 				L.gal_offsets.get(), L.block_row.get(), L.cols.get(), L.mask.get(), L.values.get(), C.values.get());
 		LaunchCheck("GalerkinKernel");
+		if (l == 0) {
+			ApKernel<T><<<Grid(L.ap_blocks, 8), 256, 0, stream_>>>(L.ap_blocks, L.ap_order.get(), L.ap_offsets.get(),
+				L.cols.get(), L.mask.get(), values, L.ap_values.get());
+			LaunchCheck("ApKernel");
+			launches_ += 1;
+		}
 		UnitDiagonalKernel<<<Grid(4LL*C.nodes, 256), 256, 0, stream_>>>(C.nodes, C.diag.get(), C.mask.get(),
 			C.values.get());
 		LaunchCheck("UnitDiagonalKernel");
@@ -530,22 +600,19 @@ template void Amg::Refresh<float>(const float*);
 template <class T>
 void Amg::Cycle(int l, const T* A, const double* b, double* x, const int* stop)
 {
-	// Two-level: x = P Ac^{-1} P^T b, then x += D^{-1} (b - A x).
+	// Two-level: x_c = Ac^{-1} P^T b, then x = P x_c + omega D^{-1} (b - (A P) x_c).
 	Level& L = *levels_[l];
 	Level& C = *levels_[l+1];
-	const long long n4 = 4LL*L.nodes;
 	RestrictKernel<<<C.nodes, 128, 0, stream_>>>(C.nodes, L.agg_order.get(), L.agg_offsets.get(),
 		L.mask.get(), b, C.b.get(), stop);
 	LaunchCheck("RestrictKernel");
 	DenseApplyKernel<<<Grid(C.dense_n, 8), 256, 0, stream_>>>(C.dense_n, C.dense.get(), C.b.get(), C.x.get(), stop);
 	LaunchCheck("DenseApplyKernel");
-	ProlongKernel<<<Grid(n4, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(), C.x.get(), L.x.get(),
-		stop);
-	LaunchCheck("ProlongKernel");
-	ResidualJacobiKernel<T><<<Grid(L.nodes, 8), 256, 0, stream_>>>(L.view(), A, L.x.get(), b, L.inverse.get(),
-		options_.omega, x, stop);
-	LaunchCheck("ResidualJacobiKernel");
-	launches_ += 4;
+	(void)A;      // the fine operator enters through A P, refreshed with it
+	CoarseCorrectionKernel<<<Grid(L.nodes, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(), C.x.get(),
+		L.ap_rows.get(), L.ap_cols.get(), L.ap_values.get(), b, L.inverse.get(), options_.omega, x, stop);
+	LaunchCheck("CoarseCorrectionKernel");
+	launches_ += 3;
 }
 
 template <class T>

@@ -12,7 +12,9 @@
 // remain).  Damped Jacobi is not a convergent smoother for these IGA operators
 // (cubic B-spline mass matrices have diag/row-sum near 0.1 in 3D), so the
 // preconditioner is two-level: the coarse correction x = P Ac^{-1} P^T v
-// followed by one block-Jacobi step on the remaining residual.  The coarse
+// followed by one block-Jacobi step on the remaining residual, whose residual
+// b - A P x_c is evaluated through the product A P (a few 4x4 blocks per fine
+// row, formed with the Galerkin refresh) instead of a pass over A.  The coarse
 // space carries the long-range (axial) pressure/velocity modes that make
 // block-Jacobi GMRES iterations grow with tube length.  Dirichlet degrees of
 // freedom are masked out of the prolongation and the coarse operator.  Every
@@ -55,6 +57,7 @@ public:
 	std::vector<int> level_nodes() const;
 	const std::vector<int>& aggregation_rounds() const { return coarse_history_; }
 	std::vector<long long> level_blocks() const;
+	long long transfer_blocks() const;
 	long long launches() const { return launches_; }
 	void set_profiler(Profiler* p) { profiler_ = p; }
 

@@ -310,6 +310,7 @@ int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info)
 		const auto blocks = amg->level_blocks();
 		info->levels = (int32_t)std::min<size_t>(8, nodes.size());
 		for (int l = 0; l < info->levels; ++l) { info->nodes[l] = nodes[l]; info->blocks[l] = blocks[l]; }
+		info->transfer_blocks = amg->transfer_blocks();
 	});
 }
 

@@ -61,8 +61,8 @@ void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double*
 // ---- tangent_tc.cu -----------------------------------------------------
 // Tensor-core tangent (BF16 operands, FP32 accumulation) ADDED into FP32
 // values, FP64 residual ADDED into rhs (= -r); status bit 1 set if an MMA
-// completion wait expired.
-void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const double* qdata,
+// completion wait expired.  phi32 is the FP32 copy of phi (Mesh::phi32).
+void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const float* phi32, const double* qdata,
 	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
 	float* values, double* rhs, int* status, cudaStream_t stream);
 

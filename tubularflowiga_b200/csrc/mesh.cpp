@@ -207,6 +207,18 @@ Mesh::Mesh(HostMesh host) : host_(std::move(host))
 		+face_element_.bytes()+face_index_.bytes()+face_coef_.bytes());
 }
 
+const float* Mesh::phi32()
+{
+	if (phi32_.get() == nullptr) {
+		const size_t count = (size_t)host_.elements()*kFeatures*kQuad*kMaxBasis;
+		phi32_.Allocate(count);
+		LaunchToFloat((long long)count, phi_.get(), phi32_.get(), stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "FP32 basis tables");
+		device_bytes_ += (int64_t)phi32_.bytes();
+	}
+	return phi32_.get();
+}
+
 Mesh::~Mesh()
 {
 	if (stream_) cudaStreamDestroy(stream_);

@@ -58,6 +58,8 @@ public:
 	DeviceMeshView view() const { return view_; }
 	DevicePatternView pattern_view() const { return pattern_view_; }
 	const double* phi() const { return phi_.get(); }
+	// FP32 copy of the basis tables (operand staging of the tensor-core tangent), made on first use.
+	const float* phi32();
 	const double* qdata() const { return qdata_.get(); }
 	const int32_t* element_blocks() const { return element_blocks_.get(); }
 	const std::vector<BoundaryFace>& faces() const { return faces_; }
@@ -77,6 +79,7 @@ private:
 		element_blocks_, face_element_, face_index_;
 	DeviceArray<uint8_t> extraction_columns_;
 	DeviceArray<double> extraction_values_, bezier_points_, phi_, qdata_, face_coef_;
+	DeviceArray<float> phi32_;
 	DeviceMeshView view_;
 	DevicePatternView pattern_view_;
 	std::vector<BoundaryFace> faces_;

@@ -176,7 +176,7 @@ void NsSolver::Assemble()
 		values32_.Zero(stream_);
 		rhs_.Zero(stream_);
 		profiler_.Begin(Profiler::kAssembly, stream_);
-		LaunchTangentTc(mesh_.view(), mesh_.phi(), mesh_.qdata(), mesh_.element_blocks(), state_.get(),
+		LaunchTangentTc(mesh_.view(), mesh_.phi(), mesh_.phi32(), mesh_.qdata(), mesh_.element_blocks(), state_.get(),
 			previous_.get(), {params_.density, params_.viscosity, params_.dt}, values32_.get(), rhs_.get(),
 			status_.get(), stream_);
 		profiler_.End(stream_);

@@ -17,10 +17,13 @@
 // and one CTA's scatter overlaps the other's operand build.  Four M = 128
 // accumulator tiles (tile T: row field 2h + T/2, basis b in [32 (T&1), +32),
 // tile row m = 4 (b mod 32) + f) live in 4 x 64 = 256 TMEM columns.
-//   prologue  FP64 state at the 64 points, FP64 coefficients M_q, rc_q of the
-//             two row fields (stored FP32 / FP64), FP64 residual -> rhs;
-//   8 chunks  of 8 points (K = 32): stage Phi (FP32), build Psi and G as BF16
-//             in the 64-byte-swizzled K-major layout, one thread issues
+//   prologue  FP64 state at the 64 points (thread per point and quarter of
+//             the basis, quarters summed in shared memory), FP64 coefficients
+//             M_q, rc_q of the two row fields (thread per field, point and
+//             pair of column fields; stored FP32 / FP64), FP64 residual -> rhs;
+//   8 chunks  of 8 points (K = 32): the FP32 basis of chunk c+1 is copied
+//             (cp.async) into the other buffer while chunk c builds Psi and G
+//             as BF16 in the 64-byte-swizzled K-major layout; one thread issues
 //             4 tiles x 2 tcgen05.mma (128 x 64 x 16) and commits to an mbarrier;
 //             the next chunk waits on it before overwriting the operands;
 //   epilogue  tcgen05.ld rows (b, f) x 32 columns a, a 4x4 transpose inside
@@ -48,18 +51,26 @@ constexpr unsigned long long kWaitNs = 1000000000ull;
 constexpr int kCoefStride = kCoef+1;             // odd float stride: point-per-thread writes hit distinct banks
 constexpr int kRcStride = 5;                     // doubles per (field, point) residual coefficient row
 
-// Shared-memory layout (bytes from a 1024-aligned base).
+// Shared-memory layout (bytes from a 1024-aligned base).  The prologue's
+// point-state partial sums alias the operand tiles and the first basis
+// buffer; the second basis buffer aliases the point state once the
+// coefficients are built.
+constexpr int kPhiBytes = kFeatures*kPts*64*4;                   // float [5][kPts][64] per chunk
+constexpr int kPartStride = 23;                                  // odd double stride of the partial sums
 constexpr int kOffA = 0;                                         // 4 tiles x 8 KiB
 constexpr int kOffB = kOffA+kTiles*kTileBytes;                   // Psi: 64 rows x 64 B
-constexpr int kOffPhi = kOffB+64*64;                             // float [5][kPts][64]
-constexpr int kOffCoef = kOffPhi+kFeatures*kPts*64*4;            // float [2][64][kCoefStride]
+constexpr int kOffPhi0 = kOffB+64*64;                            // basis chunk buffer 0
+constexpr int kOffPart = 0;                                      // double [4][64][kPartStride] (prologue)
+constexpr int kOffQS = kOffPhi0+kPhiBytes;                       // double [64][kQS]; later basis buffer 1
+constexpr int kOffCoef = kOffQS+kQuad*kQS*8;                     // float [2][64][kCoefStride]
 constexpr int kOffRC = kOffCoef+2*kQuad*kCoefStride*4;           // double [2][64][kRcStride]
-constexpr int kOffQS = kOffRC+2*kQuad*kRcStride*8;               // double [64][kQS]; reused as [256] partials
-constexpr int kOffU = kOffQS+kQuad*kQS*8;                        // double [4 fields][64]
+constexpr int kOffU = kOffRC+2*kQuad*kRcStride*8;                // double [4 fields][64]
 constexpr int kOffUp = kOffU+64*4*8;                             // double [4 fields][64]
 constexpr int kOffBar = kOffUp+64*4*8;                           // mbarrier, TMEM slot
 constexpr int kSmemBytes = kOffBar+16+1024;                      // + alignment slack
 static_assert(kSmemBytes <= 113*1024, "two CTAs per SM");
+static_assert(4*64*kPartStride*8 <= kOffQS, "partial sums fit below the point state");
+static_assert(kPhiBytes <= kQuad*kQS*8, "basis buffer 1 fits in the point-state region");
 
 // Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B BF16, both
 // K-major, M = 128, N = 64.
@@ -134,6 +145,28 @@ __device__ __forceinline__ void FenceBeforeSync() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void FenceAfterSync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void FenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// 16-byte global -> shared copy, cached in L2 only.
+__device__ __forceinline__ void CopyAsync16(uint32_t dst, const void* src)
+{
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void CopyAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void CopyAsyncWait()
+{
+	asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
+}
+
+// Basis chunk c (points 8c .. 8c+7, five features, 64 functions) of one
+// element, FP32, into a [5][8][64] buffer: 640 16-byte copies.
+__device__ __forceinline__ void PrefetchPhi(const float* P32, int c, uint32_t dst, int tid)
+{
+	for (int idx = tid; idx < kFeatures*kPts*16; idx += kTcThreads) {
+		const int t = idx/(kPts*16), rem = idx%(kPts*16);
+		CopyAsync16(dst+16*idx, P32+(size_t)(t*kQuad+c*kPts)*kMaxBasis+4*rem);
+	}
+	CopyAsyncCommit();
+}
+
 // 32 lanes x 32 consecutive FP32 columns: thread l gets row (lane base + l), columns c..c+31.
 __device__ __forceinline__ void TmemLoad32(uint32_t taddr, float v[32])
 {
@@ -175,14 +208,16 @@ __device__ __forceinline__ void RedAdd4(float* p, float a, float b, float c, flo
 }
 
 __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView mesh,
-	const double* __restrict__ phi, const double* __restrict__ qdata, const int32_t* __restrict__ element_blocks,
-	const double* __restrict__ state, const double* __restrict__ previous, AssemblyParams prm,
-	float* __restrict__ values, double* __restrict__ rhs, int* __restrict__ status)
+	const double* __restrict__ phi, const float* __restrict__ phi32, const double* __restrict__ qdata,
+	const int32_t* __restrict__ element_blocks, const double* __restrict__ state,
+	const double* __restrict__ previous, AssemblyParams prm, float* __restrict__ values, double* __restrict__ rhs,
+	int* __restrict__ status)
 {
 	extern __shared__ uint8_t smem_raw[];
 	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+1023) & ~uintptr_t(1023));
 	const uint32_t sA = SmemAddress(sm+kOffA), sB = SmemAddress(sm+kOffB);
-	float* PhiS = reinterpret_cast<float*>(sm+kOffPhi);
+	const uint32_t sPhi[2] = {SmemAddress(sm+kOffPhi0), SmemAddress(sm+kOffQS)};
+	double* Part = reinterpret_cast<double*>(sm+kOffPart);
 	float* Coef = reinterpret_cast<float*>(sm+kOffCoef);
 	double* RC = reinterpret_cast<double*>(sm+kOffRC);
 	double* QS = reinterpret_cast<double*>(sm+kOffQS);
@@ -197,6 +232,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
+	const float* P32 = phi32+(size_t)e*kFeatures*kQuad*kMaxBasis;
 
 	// Tensor memory for the four accumulator tiles; the mbarrier.
 	if (warp == 0) {
@@ -223,35 +259,50 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 	FenceAfterSync();
 	const uint32_t tmem = *tmem_slot;
 
-	// 2. State at every point (FP64): a warp per point, lanes over basis functions.
-	for (int q = warp; q < kQuad; q += kTcThreads/32) {
+	// 2. State at every point (FP64): thread (point q, quarter aq of the basis)
+	//    sums 16 functions; the four quarters meet in shared memory.
+	{
+		const int q = tid & 63, aq = tid >> 6;
 		double v[22];
 		#pragma unroll
 		for (int k = 0; k < 22; ++k) v[k] = 0.0;
-		for (int a = lane; a < kMaxBasis; a += 32) {
-			const double n = P[(0*kQuad+q)*kMaxBasis+a];
-			const double g0 = P[(1*kQuad+q)*kMaxBasis+a], g1 = P[(2*kQuad+q)*kMaxBasis+a];
-			const double g2 = P[(3*kQuad+q)*kMaxBasis+a], l = P[(4*kQuad+q)*kMaxBasis+a];
-			const double uf[4] = {U[a], U[64+a], U[128+a], U[192+a]};
-			v[0] += n*uf[0]; v[1] += n*uf[1]; v[2] += n*uf[2]; v[3] += n*uf[3];
-			v[4] += n*Up[a]; v[5] += n*Up[64+a]; v[6] += n*Up[128+a];
+		#pragma unroll 2
+		for (int j = 0; j < 16; j += 2) {
+			const int a = aq*16+j;
+			double2 ph[5];
 			#pragma unroll
-			for (int f = 0; f < 4; ++f) { v[7+3*f] += g0*uf[f]; v[8+3*f] += g1*uf[f]; v[9+3*f] += g2*uf[f]; }
-			v[19] += l*uf[0]; v[20] += l*uf[1]; v[21] += l*uf[2];
+			for (int t = 0; t < 5; ++t) ph[t] = *reinterpret_cast<const double2*>(P+(t*kQuad+q)*kMaxBasis+a);
+			#pragma unroll
+			for (int h2 = 0; h2 < 2; ++h2) {
+				const double n = h2 ? ph[0].y : ph[0].x, g0 = h2 ? ph[1].y : ph[1].x;
+				const double g1 = h2 ? ph[2].y : ph[2].x, g2 = h2 ? ph[3].y : ph[3].x;
+				const double l = h2 ? ph[4].y : ph[4].x;
+				const int b = a+h2;
+				const double uf[4] = {U[b], U[64+b], U[128+b], U[192+b]};
+				v[0] += n*uf[0]; v[1] += n*uf[1]; v[2] += n*uf[2]; v[3] += n*uf[3];
+				v[4] += n*Up[b]; v[5] += n*Up[64+b]; v[6] += n*Up[128+b];
+				#pragma unroll
+				for (int f = 0; f < 4; ++f) { v[7+3*f] += g0*uf[f]; v[8+3*f] += g1*uf[f]; v[9+3*f] += g2*uf[f]; }
+				v[19] += l*uf[0]; v[20] += l*uf[1]; v[21] += l*uf[2];
+			}
 		}
+		double* part = Part+(aq*kQuad+q)*kPartStride;
 		#pragma unroll
-		for (int k = 0; k < 22; ++k)
-			#pragma unroll
-			for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-		if (lane == 0)
-			#pragma unroll
-			for (int k = 0; k < 22; ++k) QS[q*kQS+k] = v[k];
+		for (int k = 0; k < 22; ++k) part[k] = v[k];
 	}
 	__syncthreads();
+	for (int idx = tid; idx < kQuad*22; idx += kTcThreads) {
+		const int q = idx/22, k = idx%22;
+		const double* part = Part+q*kPartStride+k;
+		QS[q*kQS+k] = ((part[0]+part[kQuad*kPartStride])+part[2*kQuad*kPartStride])+part[3*kQuad*kPartStride];
+	}
+	__syncthreads();
+	PrefetchPhi(P32, 0, sPhi[0], tid);           // chunk 0: the partial sums are dead
 
-	// 3. Coefficients of the two row fields at every point.
-	if (tid < 2*kQuad) {
-		const int il = tid >> 6, q = tid & 63;
+	// 3. Coefficients: thread (row field il, point q, column-field pair fp); fp = 0 also
+	//    gives the residual coefficients.
+	{
+		const int q = tid & 63, fp = (tid >> 6) & 1, il = tid >> 7;
 		PointState S;
 		const double* s = QS+q*kQS;
 		for (int c = 0; c < 3; ++c) {
@@ -260,7 +311,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		}
 		S.p = s[kP];
 		RowCoefficients<float>(2*h+il, S, qdata+((size_t)e*kQuad+q)*kQData, prm, Coef+(il*kQuad+q)*kCoefStride,
-			RC+(il*kQuad+q)*kRcStride);
+			fp == 0 ? RC+(il*kQuad+q)*kRcStride : nullptr, 2*fp, 2*fp+2);
 	}
 	__syncthreads();
 
@@ -271,24 +322,26 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		for (int q = half*32; q < half*32+32; ++q)
 			#pragma unroll
 			for (int s = 0; s < 4; ++s) r += P[(s*kQuad+q)*kMaxBasis+a]*RC[(il*kQuad+q)*kRcStride+s];
-		__syncthreads();                       // QS is dead: reuse it for the partial sums
-		QS[tid] = r;
+		QS[tid] = r;                           // the point state is dead: reuse it for the halves
 		__syncthreads();
 		if (half == 0 && a < nen)
 			atomicAdd(rhs+4*(size_t)mesh.connectivity[begin+a]+2*h+il, QS[tid]+QS[tid+64]);
+		__syncthreads();
 	}
 
-	// 5. Tangent chunks.
+	// 5. Tangent chunks.  Basis chunk c+1 is copied into the other buffer while chunk c is built.
 	const int gil = warp >> 2, gqp = warp & 3;     // G builder: row field, point pair
 	const int gf = lane & 3, gbs = lane >> 2;       //            column field, basis sub-index
 	bool failed = false;
 	uint32_t pending = 0;                            // parity of the last committed chunk
 	for (int c = 0; c < kChunks; ++c) {
 		const int q0 = c*kPts;
-		// Stage Phi of the chunk as FP32, layout [t][point][b].
-		for (int idx = tid; idx < kFeatures*kPts*64; idx += kTcThreads) {
-			const int t = idx >> 9, ql = (idx >> 6) & 7, b = idx & 63;
-			PhiS[idx] = (float)P[(t*kQuad+q0+ql)*kMaxBasis+b];
+		const float* PhiS = reinterpret_cast<const float*>(sm+(c & 1 ? kOffQS : kOffPhi0));
+		if (c+1 < kChunks) {
+			PrefetchPhi(P32, c+1, sPhi[(c+1) & 1], tid);
+			CopyAsyncWait<1>();
+		} else {
+			CopyAsyncWait<0>();
 		}
 		bool ok = true;
 		if (c > 0) ok = MbarWaitBounded(bar, pending);
@@ -383,6 +436,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		}
 	} else {
 		if (tid == 0) atomicOr(status, 1);
+		CopyAsyncWait<0>();                     // this thread's basis copies in flight
 		MbarWaitBounded(bar, pending);          // let this CTA's own MMAs drain before freeing TMEM
 	}
 	FenceBeforeSync();
@@ -396,7 +450,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 
 } // namespace
 
-void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const double* qdata,
+void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const float* phi32, const double* qdata,
 	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
 	float* values, double* rhs, int* status, cudaStream_t stream)
 {
@@ -409,8 +463,8 @@ void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const double
 	}
 	const long long ctas = 2LL*mesh.elements;
 	if (ctas > 0x7fffffffLL) Fail(-7, "too many elements for one tangent launch");
-	TangentTcKernel<<<(unsigned)ctas, kTcThreads, kSmemBytes, stream>>>(mesh, phi, qdata, element_blocks, state,
-		previous, params, values, rhs, status);
+	TangentTcKernel<<<(unsigned)ctas, kTcThreads, kSmemBytes, stream>>>(mesh, phi, phi32, qdata, element_blocks,
+		state, previous, params, values, rhs, status);
 	LaunchCheck("TangentTcKernel");
 }
 

@@ -28,10 +28,11 @@ struct PointState {
 // measure: M[f*20 + s*5 + t] multiplies (test feature s of N_a) x (trial
 // feature t of N_b) in K^{if}_{ab}; rc[s] = -measure * c_s gives the
 // residual.  Computed in FP64; C is the storage type of M (double for the
-// FP64 tangent, float for the tensor-core tangent).
+// FP64 tangent, float for the tensor-core tangent).  Only the column fields
+// f in [f_lo, f_hi) are written (M[f_lo*20 .. f_hi*20)); rc may be null.
 template <class C>
 __device__ void RowCoefficients(int i, const PointState& S, const double* qd, const AssemblyParams& prm,
-	C* M, double* rc)
+	C* M, double* rc, int f_lo = 0, int f_hi = 4)
 {
 	const double rho = prm.density, mu = prm.viscosity, nu = mu/rho;
 	const double dt = prm.dt;
@@ -62,7 +63,8 @@ __device__ void RowCoefficients(int i, const PointState& S, const double* qd, co
 	const double divu = S.gv[0][0]+S.gv[1][1]+S.gv[2][2];
 	const double fine_p = -rho*tau_c*divu;
 	// Residual (:218-239).
-	if (i < 3) {
+	if (rc == nullptr) {
+	} else if (i < 3) {
 		double cN = rho*dudt[i];
 		for (int d = 0; d < 3; ++d) cN += rho*a[d]*S.gv[i][d];
 		rc[0] = -meas*cN;
@@ -84,10 +86,12 @@ __device__ void RowCoefficients(int i, const PointState& S, const double* qd, co
 		for (int c = 0; c < 3; ++c)
 			A[c][f] = -dtau_m*R[c]-tau_m*((c == f ? idt : 0.0)+S.gv[c][f]);
 	}
-	for (int k = 0; k < kCoef; ++k) M[k] = C(0);
+	for (int k = f_lo*20; k < f_hi*20; ++k) M[k] = C(0);
 	auto at = [&](int f, int s, int t) -> C& { return M[f*20+s*5+t]; };
+	const int f_vel = f_hi < 3 ? f_hi : 3;     // end of the velocity columns in range
+	const bool p_col = f_hi > 3;               // pressure column in range
 	if (i < 3) {
-		for (int f = 0; f < 3; ++f) {
+		for (int f = f_lo; f < f_vel; ++f) {
 			double nn = rho*S.gv[i][f]+(f == i ? rho*idt : 0.0);
 			for (int d = 0; d < 3; ++d) nn += rho*A[d][f]*S.gv[i][d];
 			at(f, 0, 0) = nn;
@@ -108,21 +112,24 @@ __device__ void RowCoefficients(int i, const PointState& S, const double* qd, co
 				at(f, 1+d, 4) = -rho*tau_m*nu*((f == i ? a[d] : 0.0)+(d == f ? fine[i] : 0.0));
 			}
 		}
-		at(3, 1+i, 0) = -1.0;
-		for (int e = 0; e < 3; ++e) at(3, 0, 1+e) = -tau_m*S.gv[i][e];
-		for (int d = 0; d < 3; ++d)
-			for (int e = 0; e < 3; ++e)
-				at(3, 1+d, 1+e) = tau_m*((e == i ? a[d] : 0.0)+(d == e ? fine[i] : 0.0));
+		if (p_col) {
+			at(3, 1+i, 0) = -1.0;
+			for (int e = 0; e < 3; ++e) at(3, 0, 1+e) = -tau_m*S.gv[i][e];
+			for (int d = 0; d < 3; ++d)
+				for (int e = 0; e < 3; ++e)
+					at(3, 1+d, 1+e) = tau_m*((e == i ? a[d] : 0.0)+(d == e ? fine[i] : 0.0));
+		}
 	} else {
-		for (int f = 0; f < 3; ++f) {
+		for (int f = f_lo; f < f_vel; ++f) {
 			at(f, 0, 1+f) = 1.0;
 			for (int d = 0; d < 3; ++d) at(f, 1+d, 0) = -A[d][f];
 			for (int e = 0; e < 3; ++e) at(f, 1+f, 1+e) = tau_m*S.u[e];
 			at(f, 1+f, 4) = -tau_m*nu;
 		}
-		for (int d = 0; d < 3; ++d) at(3, 1+d, 1+d) = tau_m/rho;
+		if (p_col)
+			for (int d = 0; d < 3; ++d) at(3, 1+d, 1+d) = tau_m/rho;
 	}
-	for (int k = 0; k < kCoef; ++k) M[k] = C(M[k]*meas);
+	for (int k = f_lo*20; k < f_hi*20; ++k) M[k] = C(M[k]*meas);
 }
 
 } // namespace tfiga
