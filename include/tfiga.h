@@ -232,9 +232,12 @@ int tfiga_ns_stream(tfiga_ns* ns, void** stream);
 int tfiga_ns_set_profiling(tfiga_ns* ns, int enable);
 /* Totals since the last reset: milliseconds and launch counts per family. */
 int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int32_t reset);
-/* Algorithmic bytes per family since the last reset, as the solver accounts
- * them while profiling is on (family 2, Krylov orthogonalisation: 8 n (4 (j+1)
- * + 6) per Arnoldi step j; the other families report 0). */
+/* Bytes per family since the last reset, as the solver accounts them while
+ * profiling is on: bytes[0..3] algorithmic, bytes[4..7] actually moved
+ * (2 * TFIGA_PROFILE_FAMILIES entries).  Family 2, Krylov orthogonalisation:
+ * algorithmic s_v n (2j + 7) per Arnoldi step j (+ 8 n for the stored
+ * FGMRES vector), s_v the basis entry size; moved: both classical
+ * Gram-Schmidt passes.  The other families report 0. */
 int tfiga_ns_profile_bytes(tfiga_ns* ns, double* bytes);
 
 /* ---- allocation-free kernel ------------------------------------------- */

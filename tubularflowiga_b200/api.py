@@ -304,9 +304,10 @@ class NavierStokes:
                 "blocks": list(info.blocks[:info.levels]), "transfer_blocks": int(info.transfer_blocks)}
 
     def profile_bytes(self) -> dict:
-        b = np.zeros(4)
+        """{family: (algorithmic bytes, moved bytes)} since the last profile reset."""
+        b = np.zeros(8)
         check(lib().tfiga_ns_profile_bytes(self._h, _p(b)))
-        return {f: float(b[i]) for i, f in enumerate(self.FAMILIES)}
+        return {f: (float(b[i]), float(b[4 + i])) for i, f in enumerate(self.FAMILIES)}
 
     def profile(self, reset=False) -> dict:
         ms = np.zeros(4)

@@ -387,7 +387,7 @@ int tfiga_ns_profile_bytes(tfiga_ns* ns, double* bytes)
 {
 	return Guard([&] {
 		Require(ns && bytes, "null argument");
-		ns->solver->profiler().Totals(nullptr, nullptr, false, bytes);
+		ns->solver->profiler().Totals(nullptr, nullptr, false, bytes, bytes+tfiga::Profiler::kFamilies);
 	});
 }
 

@@ -106,14 +106,15 @@ void Profiler::Collect()
 	used_ = 0;
 }
 
-void Profiler::Totals(double* ms, long long* counts, bool reset, double* bytes)
+void Profiler::Totals(double* ms, long long* counts, bool reset, double* bytes, double* moved)
 {
 	Collect();
 	for (int f = 0; f < kFamilies; ++f) {
 		if (ms) ms[f] = ms_[f];
 		if (counts) counts[f] = count_[f];
 		if (bytes) bytes[f] = bytes_[f];
-		if (reset) { ms_[f] = 0.0; count_[f] = 0; bytes_[f] = 0.0; }
+		if (moved) moved[f] = moved_[f];
+		if (reset) { ms_[f] = 0.0; count_[f] = 0; bytes_[f] = 0.0; moved_[f] = 0.0; }
 	}
 }
 

@@ -110,7 +110,9 @@ public:
 	void Collect();
 	// Algorithmic bytes a family moved (accounted by the caller, only while enabled).
 	void AddBytes(Family family, double bytes) { if (enabled_) bytes_[family] += bytes; }
-	void Totals(double* ms, long long* counts, bool reset, double* bytes = nullptr);
+	// Bytes the kernels actually move for the same work (when it differs from the algorithmic count).
+	void AddMovedBytes(Family family, double bytes) { if (enabled_) moved_[family] += bytes; }
+	void Totals(double* ms, long long* counts, bool reset, double* bytes = nullptr, double* moved = nullptr);
 
 private:
 	struct Mark { cudaEvent_t start, stop; int family; };
@@ -121,6 +123,7 @@ private:
 	double ms_[kFamilies] = {0, 0, 0, 0};
 	long long count_[kFamilies] = {0, 0, 0, 0};
 	double bytes_[kFamilies] = {0, 0, 0, 0};
+	double moved_[kFamilies] = {0, 0, 0, 0};
 };
 
 } // namespace tfiga

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 namespace tfiga {
 namespace {
@@ -12,11 +13,37 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads/32;
 constexpr int kBatch = 8;             // Arnoldi steps launched per host wait
 
+// Two consecutive basis entries as doubles (the basis is FP64, or FP32 in the
+// reduced-precision modes).
+template <class B> struct BasisPair;
+template <> struct BasisPair<double> {
+	static __device__ __forceinline__ double2 Load(const double* p, long long k2)
+	{
+		return reinterpret_cast<const double2*>(p)[k2];
+	}
+	static __device__ __forceinline__ void Store(double* p, long long k2, double2 v)
+	{
+		reinterpret_cast<double2*>(p)[k2] = v;
+	}
+};
+template <> struct BasisPair<float> {
+	static __device__ __forceinline__ double2 Load(const float* p, long long k2)
+	{
+		const float2 v = reinterpret_cast<const float2*>(p)[k2];
+		return make_double2(v.x, v.y);
+	}
+	static __device__ __forceinline__ void Store(float* p, long long k2, double2 v)
+	{
+		reinterpret_cast<float2*>(p)[k2] = make_float2((float)v.x, (float)v.y);
+	}
+};
+
 // partial[i*blocks + cta] = scale[i] * <V_i, w> over this CTA's chunk.  The
 // chunk is a multiple of 128 doubles and n is even, so every row slice is
 // 16-byte aligned: a warp streams two basis vectors at once with 16-byte
 // loads, two steps per iteration, to keep enough bytes in flight for HBM.
-__global__ void __launch_bounds__(kThreads) MultiDotKernel(const double* __restrict__ V, long long n,
+template <class B>
+__global__ void __launch_bounds__(kThreads) MultiDotKernel(const B* __restrict__ V, long long n,
 	const double* __restrict__ scale, int count, const double* __restrict__ w, double* __restrict__ partial,
 	int chunk, const int* __restrict__ stop)
 {
@@ -34,13 +61,14 @@ __global__ void __launch_bounds__(kThreads) MultiDotKernel(const double* __restr
 	for (int i0 = warp; i0 < count; i0 += 2*kWarps) {
 		const int i1 = i0+kWarps;
 		const bool two = i1 < count;
-		const double2* a = reinterpret_cast<const double2*>(V+(size_t)i0*n+lo);
-		const double2* b = reinterpret_cast<const double2*>(V+(size_t)(two ? i1 : i0)*n+lo);
+		const B* a = V+(size_t)i0*n+lo;
+		const B* b = V+(size_t)(two ? i1 : i0)*n+lo;
 		double sa = 0.0, sb = 0.0, ta = 0.0, tb = 0.0;
 		for (int k = lane; k < len2; k += 64) {
 			const bool more = k+32 < len2;
-			const double2 x0 = a[k], y0 = b[k];
-			const double2 x1 = more ? a[k+32] : zero, y1 = more ? b[k+32] : zero;
+			const double2 x0 = BasisPair<B>::Load(a, k), y0 = BasisPair<B>::Load(b, k);
+			const double2 x1 = more ? BasisPair<B>::Load(a, k+32) : zero;
+			const double2 y1 = more ? BasisPair<B>::Load(b, k+32) : zero;
 			const double2 w0 = w2[k], w1 = more ? w2[k+32] : zero;
 			sa = fma(x0.x, w0.x, sa); sa = fma(x0.y, w0.y, sa);
 			sb = fma(y0.x, w0.x, sb); sb = fma(y0.y, w0.y, sb);
@@ -82,8 +110,9 @@ __global__ void __launch_bounds__(kThreads) DotFinalizeKernel(const double* __re
 // out = w - sum_i scale_i hpass_i V_i; norm_partial[cta] = sum out^2 (if non-null).
 // out may alias w.  Each thread owns 16-byte pairs of entries and walks the
 // basis four vectors at a time (the FMA order per entry is the basis order).
-__global__ void __launch_bounds__(kThreads) UpdateKernel(const double* __restrict__ V, long long n,
-	const double* __restrict__ scale, int count, const double* __restrict__ hpass, const double* win, double* out,
+template <class B, class O>
+__global__ void __launch_bounds__(kThreads) UpdateKernel(const B* __restrict__ V, long long n,
+	const double* __restrict__ scale, int count, const double* __restrict__ hpass, const double* win, O* out,
 	double* __restrict__ norm_partial, const int* __restrict__ stop)
 {
 	if (*stop) return;
@@ -91,26 +120,24 @@ __global__ void __launch_bounds__(kThreads) UpdateKernel(const double* __restric
 	for (int i = threadIdx.x; i < count; i += blockDim.x) coef[i] = scale[i]*hpass[i];
 	__syncthreads();
 	const long long n2 = n >> 1;
-	const double2* V2 = reinterpret_cast<const double2*>(V);
 	const double2* w2 = reinterpret_cast<const double2*>(win);
-	double2* o2 = reinterpret_cast<double2*>(out);
 	double sq = 0.0;
 	for (long long k = (long long)blockIdx.x*blockDim.x+threadIdx.x; k < n2; k += (long long)gridDim.x*blockDim.x) {
 		double2 v = w2[k];
 		int i = 0;
 		for (; i+3 < count; i += 4) {
-			const double2 a0 = V2[(size_t)i*n2+k], a1 = V2[(size_t)(i+1)*n2+k];
-			const double2 a2 = V2[(size_t)(i+2)*n2+k], a3 = V2[(size_t)(i+3)*n2+k];
+			const double2 a0 = BasisPair<B>::Load(V+(size_t)i*n, k), a1 = BasisPair<B>::Load(V+(size_t)(i+1)*n, k);
+			const double2 a2 = BasisPair<B>::Load(V+(size_t)(i+2)*n, k), a3 = BasisPair<B>::Load(V+(size_t)(i+3)*n, k);
 			v.x = fma(-coef[i], a0.x, v.x); v.y = fma(-coef[i], a0.y, v.y);
 			v.x = fma(-coef[i+1], a1.x, v.x); v.y = fma(-coef[i+1], a1.y, v.y);
 			v.x = fma(-coef[i+2], a2.x, v.x); v.y = fma(-coef[i+2], a2.y, v.y);
 			v.x = fma(-coef[i+3], a3.x, v.x); v.y = fma(-coef[i+3], a3.y, v.y);
 		}
 		for (; i < count; ++i) {
-			const double2 a0 = V2[(size_t)i*n2+k];
+			const double2 a0 = BasisPair<B>::Load(V+(size_t)i*n, k);
 			v.x = fma(-coef[i], a0.x, v.x); v.y = fma(-coef[i], a0.y, v.y);
 		}
-		o2[k] = v;
+		BasisPair<O>::Store(out, k, v);
 		sq = fma(v.x, v.x, sq);
 		sq = fma(v.y, v.y, sq);
 	}
@@ -213,7 +240,8 @@ __global__ void __launch_bounds__(kThreads) SolutionUpdateKernel(const double* _
 }
 
 // out = scale[j] * in (materialise a lazily normalised Krylov vector).
-__global__ void ScaleCopyKernel(long long n, const double* __restrict__ in, const double* __restrict__ scale,
+template <class B>
+__global__ void ScaleCopyKernel(long long n, const B* __restrict__ in, const double* __restrict__ scale,
 	double* __restrict__ out, const int* __restrict__ stop)
 {
 	if (*stop) return;
@@ -232,9 +260,18 @@ __global__ void ResidualKernel(long long n, const double* __restrict__ rhs, cons
 // Bytes classical Gram-Schmidt twice moves over one cycle of `used` Arnoldi
 // steps: step j reads the j+1 basis vectors and w in each multi-dot, reads
 // them again and writes w in each update, two passes: 8 n (4 (j+1) + 6).
-double OrthoBytes(long long n, int used)
+double OrthoBytes(long long n, int used, int basis_bytes)
 {
-	return 8.0*(double)n*(2.0*used*(used+1.0)+6.0*used);
+	// step j: both passes read the j+1 basis vectors twice (dot, update): 4 (j+1) sB n; the FP64 work
+	// vector is read five times and written once, and the new basis vector is written: (48 + sB) n - 8 n
+	return (double)n*(4.0*basis_bytes*0.5*used*(used+1.0)+(40.0+basis_bytes)*used);
+}
+
+// The survey's algorithmic bytes of the same steps: s_v n (2j + 7) per step with s_v the basis
+// entry size, plus 8 n for the stored FP64 preconditioned vector of FGMRES.
+double ArnoldiBytes(long long n, int used, int basis_bytes, bool flexible)
+{
+	return (double)n*(basis_bytes*(used*(used-1.0)+7.0*used)+(flexible ? 8.0*used : 0.0));
 }
 
 } // namespace
@@ -260,12 +297,19 @@ Gmres::Gmres(int nodes, int restart, cudaStream_t stream)
 	singular_.Allocate(1);
 	CudaCheck(cudaMallocHost(reinterpret_cast<void**>(&host_), sizeof(HostStatus)), "pinned GMRES status");
 	if ((size_t)chunk_*sizeof(double) > 48*1024) {
-		CudaCheck(cudaFuncSetAttribute(MultiDotKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		CudaCheck(cudaFuncSetAttribute(MultiDotKernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)((size_t)chunk_*sizeof(double))), "multi-dot shared memory");
+		CudaCheck(cudaFuncSetAttribute(MultiDotKernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			(int)((size_t)chunk_*sizeof(double))), "multi-dot shared memory");
 	}
 	if ((size_t)(restart+1)*sizeof(double) > 48*1024) {
-		CudaCheck(cudaFuncSetAttribute(UpdateKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			(int)((size_t)(restart+1)*sizeof(double))), "update shared memory");
+		const int coef = (int)((size_t)(restart+1)*sizeof(double));
+		CudaCheck(cudaFuncSetAttribute(UpdateKernel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			coef), "update shared memory");
+		CudaCheck(cudaFuncSetAttribute(UpdateKernel<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			coef), "update shared memory");
+		CudaCheck(cudaFuncSetAttribute(UpdateKernel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			coef), "update shared memory");
 		CudaCheck(cudaFuncSetAttribute(SolutionUpdateKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			(int)((size_t)(restart+1)*sizeof(double))), "solution update shared memory");
 	}
@@ -294,10 +338,11 @@ void Gmres::Step(const DevicePatternView& pattern, const double* values, int j)
 		stream_);
 	if (profiler_) profiler_->End(stream_);
 	launches_ += 1;
-	Orthogonalize(j);
+	Orthogonalize<double>(j, V_.get());
 }
 
-void Gmres::Orthogonalize(int j)
+template <class B>
+void Gmres::Orthogonalize(int j, B* basis)
 {
 	const int count = j+1;
 	const int* stop = state_.get();
@@ -305,26 +350,37 @@ void Gmres::Orthogonalize(int j)
 	const size_t coef_smem = (size_t)(restart_+1)*sizeof(double);
 	if (profiler_) profiler_->Begin(Profiler::kOrtho, stream_);
 	for (int pass = 0; pass < 2; ++pass) {
-		MultiDotKernel<<<blocks_, kThreads, dot_smem, stream_>>>(V_.get(), n_, scale_.get(), count, w_.get(),
+		MultiDotKernel<B><<<blocks_, kThreads, dot_smem, stream_>>>(basis, n_, scale_.get(), count, w_.get(),
 			partial_.get(), chunk_, stop);
 		LaunchCheck("MultiDotKernel");
 		DotFinalizeKernel<<<(count+kThreads/32-1)/(kThreads/32), kThreads, 0, stream_>>>(partial_.get(), blocks_,
 			count, hpass_.get(), H_.get(), restart_, j, pass, stop);
 		LaunchCheck("DotFinalizeKernel");
-		double* out = pass == 0 ? w_.get() : V_.get()+(size_t)(j+1)*n_;
-		UpdateKernel<<<blocks_, kThreads, coef_smem, stream_>>>(V_.get(), n_, scale_.get(), count, hpass_.get(),
-			w_.get(), out, pass == 0 ? nullptr : norm_partial_.get(), stop);
+		if (pass == 0)
+			UpdateKernel<B, double><<<blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
+				hpass_.get(), w_.get(), w_.get(), nullptr, stop);
+		else
+			UpdateKernel<B, B><<<blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
+				hpass_.get(), w_.get(), basis+(size_t)(j+1)*n_, norm_partial_.get(), stop);
 		LaunchCheck("UpdateKernel");
 	}
 	if (profiler_) profiler_->End(stream_);
 	launches_ += 7;
 }
 
+template <> double* Gmres::Basis<double>() { return V_.get(); }
+template <> float* Gmres::Basis<float>()
+{
+	if (V32_.size() == 0) V32_.Allocate((size_t)(restart_+1)*n_);
+	return V32_.get();
+}
+
 template <class T>
 void Gmres::FlexibleStep(const DevicePatternView& pattern, const T* values, int j, Amg& M)
 {
 	const int* stop = state_.get();
-	ScaleCopyKernel<<<blocks_, kThreads, 0, stream_>>>(n_, V_.get()+(size_t)j*n_, scale_.get()+j, r_.get(), stop);
+	T* basis = Basis<T>();
+	ScaleCopyKernel<T><<<blocks_, kThreads, 0, stream_>>>(n_, basis+(size_t)j*n_, scale_.get()+j, r_.get(), stop);
 	LaunchCheck("ScaleCopyKernel");
 	launches_ += 1;
 	double* z = Z_.get()+(size_t)j*n_;
@@ -333,18 +389,24 @@ void Gmres::FlexibleStep(const DevicePatternView& pattern, const T* values, int 
 	LaunchSpmvBlockJacobi<T>(pattern, values, nullptr, z, nullptr, w_.get(), stop, stream_);
 	if (profiler_) profiler_->End(stream_);
 	launches_ += 1;
-	Orthogonalize(j);
+	Orthogonalize<T>(j, basis);
 }
 
 template <class T>
 double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const T* values, const double* rhs,
 	const double* x)
 {
+	// v_0 = b - A x (FP64), stored in the basis precision; beta from the FP64 vector
 	LaunchSpmv<T>(pattern, values, x, tmp_.get(), stream_);
-	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), V_.get());
+	double* r = std::is_same<T, double>::value ? V_.get() : r_.get();
+	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), r);
 	LaunchCheck("ResidualKernel");
-	LaunchNorm(n_, V_.get(), norm_partial_.get(), scalar_.get(), stream_);
+	LaunchNorm(n_, r, norm_partial_.get(), scalar_.get(), stream_);
 	launches_ += 4;
+	if (!std::is_same<T, double>::value) {
+		LaunchToFloat(n_, r, reinterpret_cast<float*>(Basis<T>()), stream_);
+		launches_ += 1;
+	}
 	scalar_.Download(host_->beta, 1, stream_);
 	CudaCheck(cudaStreamSynchronize(stream_), "FGMRES residual");
 	return host_->beta[0];
@@ -390,7 +452,10 @@ GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const T* valu
 		}
 		const int used = host_->used;
 		result.iterations += used;
-		if (profiler_) profiler_->AddBytes(Profiler::kOrtho, OrthoBytes(n_, used));
+		if (profiler_) {
+			profiler_->AddBytes(Profiler::kOrtho, ArnoldiBytes(n_, used, (int)sizeof(T), true));
+			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, (int)sizeof(T)));
+		}
 		BackSolveKernel<<<1, 1, 0, stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(), state_.get()+2);
 		LaunchCheck("BackSolveKernel");
 		SolutionUpdateKernel<<<blocks_, kThreads, (size_t)(restart_+1)*sizeof(double), stream_>>>(Z_.get(), n_,
@@ -467,7 +532,10 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 		}
 		const int used = host_->used;
 		result.iterations += used;
-		if (profiler_) profiler_->AddBytes(Profiler::kOrtho, OrthoBytes(n_, used));
+		if (profiler_) {
+			profiler_->AddBytes(Profiler::kOrtho, ArnoldiBytes(n_, used, 8, false));
+			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, 8));
+		}
 		result.residual = host_->residual;
 		BackSolveKernel<<<1, 1, 0, stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(),
 			state_.get()+2);

@@ -35,7 +35,9 @@ public:
 		double rtol, int max_iterations, long long* launches);
 	// Right-preconditioned flexible GMRES (FGMRES): z_j = M^{-1} v_j stored, tolerance
 	// rtol * ||b - A x0|| on the true residual.
-	// The matrix may be stored in FP64 or FP32 (T); vectors, Hessenberg and Givens stay FP64.
+	// The matrix may be stored in FP64 or FP32 (T); with FP32 the Krylov basis is stored in FP32
+	// too (dots, updates and the work vector in FP64 arithmetic); preconditioned vectors, Hessenberg,
+	// Givens and the solution stay FP64, and each restart's true residual is the FP64 refinement.
 	template <class T>
 	GmresResult SolveFlexible(const DevicePatternView& pattern, const T* values, const double* rhs, double* x,
 		double rtol, int max_iterations, Amg& preconditioner, long long* launches);
@@ -45,7 +47,9 @@ public:
 
 private:
 	void Step(const DevicePatternView& pattern, const double* values, int j);
-	void Orthogonalize(int j);
+	template <class B> void Orthogonalize(int j, B* basis);
+	// Krylov basis storage: FP64, or FP32 when the matrix is stored in FP32 (T = float).
+	template <class B> B* Basis();
 	template <class T>
 	void FlexibleStep(const DevicePatternView& pattern, const T* values, int j, Amg& preconditioner);
 	template <class T>
@@ -58,6 +62,7 @@ private:
 	cudaStream_t stream_;
 	long long launches_ = 0;
 	DeviceArray<double> Z_;
+	DeviceArray<float> V32_;
 	DeviceArray<double> V_, w_, r_, tmp_, inverse_, partial_, hpass_, H_, cs_, sn_, g_, y_, scale_, norm_partial_,
 		scalar_;
 	DeviceArray<int> state_;          // [0] stop, [1] used, [2] error
