@@ -11,7 +11,9 @@ no-slip wall.  Inputs are synthetic (seeded generator), stated in `data`.
 
 A "step" is one physical time step: Newton to ||r|| <= 1e-8 ||r_0|| (FP64
 residual) with the exact tangent, each linear solve AMG-preconditioned
-FGMRES(200) to a true-residual rtol of 1e-8.  --precision mixed (default, the
+FGMRES(200) to a true-residual rtol of 1e-8 (the AMG's dense coarse inverse
+rebuilt every third linear solve, its fine-level data on every solve; both
+precisions).  --precision mixed (default, the
 config's own precision): tangent contracted on the tcgen05 tensor cores (BF16
 operands, FP32 accumulation), FP32 Jacobian for SpMV and the preconditioner,
 FP64 residual, vectors and refinement.  --precision fp64: every array FP64.
@@ -289,7 +291,8 @@ def main():
     solver_kw = dict(density=RHO, viscosity=MU, dt=1e-3 if args.workload == "c1" else DT,
                      nonlinear_rtol=1e-8, nonlinear_atol=1e-300, mass_rtol=1e-3,
                      gmres_restart=200, gmres_max_iterations=5000, gmres_rtol=1e-8,
-                     preconditioner=api.AMG if amg else api.BLOCK_JACOBI)
+                     preconditioner=api.AMG if amg else api.BLOCK_JACOBI,
+                     amg_coarse_period=3)
     ns = api.NavierStokes(mesh, precision=api.MIXED if mixed else api.FP64, **solver_kw)
     dt = ns.params.dt
     vmask, pmask, vel0 = api.tube_boundary_conditions(tube, 1.0)

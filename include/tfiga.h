@@ -97,6 +97,13 @@ typedef struct tfiga_ns_params {
 	 * rounded once to FP32 for storage.
 	 * Both reduced modes require TFIGA_PRECONDITIONER_AMG. */
 	int32_t precision;             /* default TFIGA_PRECISION_FP64 */
+	/* AMG: aggregate until at most this many coarse nodes remain (dense
+	 * coarse solve of 4x that order; at most 2048). */
+	int32_t amg_coarse_nodes;      /* default 300 */
+	/* AMG: rebuild the Galerkin coarse operator and its dense inverse on every
+	 * amg_coarse_period-th linear solve only (the fine-level data, A P and the
+	 * block-Jacobi inverses, are refreshed on every solve). */
+	int32_t amg_coarse_period;     /* default 1 */
 } tfiga_ns_params;
 
 #define TFIGA_PRECISION_FP64 0

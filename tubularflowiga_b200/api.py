@@ -40,7 +40,8 @@ class NsParams(C.Structure):
     _fields_ = [("density", C.c_double), ("viscosity", C.c_double), ("dt", C.c_double),
                 ("max_newton", C.c_int32), ("nonlinear_rtol", C.c_double), ("nonlinear_atol", C.c_double),
                 ("mass_rtol", C.c_double), ("gmres_restart", C.c_int32), ("gmres_max_iterations", C.c_int32),
-                ("gmres_rtol", C.c_double), ("preconditioner", C.c_int32), ("precision", C.c_int32)]
+                ("gmres_rtol", C.c_double), ("preconditioner", C.c_int32), ("precision", C.c_int32),
+                ("amg_coarse_nodes", C.c_int32), ("amg_coarse_period", C.c_int32)]
 
 
 FP64 = 0

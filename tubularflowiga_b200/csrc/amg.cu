@@ -523,9 +523,10 @@ void Amg::BuildFromStrength(std::vector<double> s)
 }
 
 template <class T>
-void Amg::Refresh(const T* values)
+void Amg::Refresh(const T* values, bool coarse)
 {
 	if (!built_) Fail(-1, "AMG hierarchy has not been built");
+	if (masks_dirty_ || !coarse_ready_) coarse = true;
 	if (masks_dirty_) {
 		std::vector<double> m(4*(size_t)levels_[0]->nodes, 1.0);
 		if (!vmask_.empty())
@@ -551,23 +552,29 @@ void Amg::Refresh(const T* values)
 	for (size_t l = 0; l+1 < levels_.size(); ++l) {
 		Level& L = *levels_[l];
 		Level& C = *levels_[l+1];
-		if (l == 0)
-			GalerkinKernel<T><<<(unsigned)C.blocks, 128, 0, stream_>>>(C.blocks, L.gal_order.get(),
-				L.gal_offsets.get(), L.block_row.get(), L.cols.get(), L.mask.get(), values, C.values.get());
-		else
-			GalerkinKernel<double><<<(unsigned)C.blocks, 128, 0, stream_>>>(C.blocks, L.gal_order.get(),
-				L.gal_offsets.get(), L.block_row.get(), L.cols.get(), L.mask.get(), L.values.get(), C.values.get());
-		LaunchCheck("GalerkinKernel");
+		if (coarse) {
+			if (l == 0)
+				GalerkinKernel<T><<<(unsigned)C.blocks, 128, 0, stream_>>>(C.blocks, L.gal_order.get(),
+					L.gal_offsets.get(), L.block_row.get(), L.cols.get(), L.mask.get(), values, C.values.get());
+			else
+				GalerkinKernel<double><<<(unsigned)C.blocks, 128, 0, stream_>>>(C.blocks, L.gal_order.get(),
+					L.gal_offsets.get(), L.block_row.get(), L.cols.get(), L.mask.get(), L.values.get(),
+					C.values.get());
+			LaunchCheck("GalerkinKernel");
+			launches_ += 1;
+		}
 		if (l == 0) {
 			ApKernel<T><<<Grid(L.ap_blocks, 8), 256, 0, stream_>>>(L.ap_blocks, L.ap_order.get(), L.ap_offsets.get(),
 				L.cols.get(), L.mask.get(), values, L.ap_values.get());
 			LaunchCheck("ApKernel");
 			launches_ += 1;
 		}
-		UnitDiagonalKernel<<<Grid(4LL*C.nodes, 256), 256, 0, stream_>>>(C.nodes, C.diag.get(), C.mask.get(),
-			C.values.get());
-		LaunchCheck("UnitDiagonalKernel");
-		launches_ += 2;
+		if (coarse) {
+			UnitDiagonalKernel<<<Grid(4LL*C.nodes, 256), 256, 0, stream_>>>(C.nodes, C.diag.get(), C.mask.get(),
+				C.values.get());
+			LaunchCheck("UnitDiagonalKernel");
+			launches_ += 1;
+		}
 	}
 	for (size_t l = 0; l+1 < levels_.size(); ++l) {
 		Level& L = *levels_[l];
@@ -577,7 +584,8 @@ void Amg::Refresh(const T* values)
 		launches_ += 1;
 	}
 	Level& Z = *levels_.back();
-	if (Z.dense_n == 0) return;
+	if (Z.dense_n == 0 || !coarse) return;
+	coarse_ready_ = true;
 	Z.dense.Zero(stream_);
 	Z.dense_flag.Zero(stream_);
 	DenseScatterKernel<<<Grid(Z.blocks*16, 256), 256, 0, stream_>>>(Z.view(), Z.values.get(), Z.dense_n, Z.dense.get());
@@ -594,8 +602,8 @@ void Amg::Refresh(const T* values)
 	launches_ += 2+2LL*dn;
 }
 
-template void Amg::Refresh<double>(const double*);
-template void Amg::Refresh<float>(const float*);
+template void Amg::Refresh<double>(const double*, bool);
+template void Amg::Refresh<float>(const float*, bool);
 
 template <class T>
 void Amg::Cycle(int l, const T* A, const double* b, double* x, const int* stop)

@@ -49,8 +49,9 @@ public:
 	bool built() const { return built_; }
 	// Dirichlet masks of the fine level (velocity / pressure constrained per node).
 	void SetMasks(const std::vector<int32_t>& velocity_mask, const std::vector<int32_t>& pressure_mask);
-	// Galerkin refresh of the coarse operator and the fine block-Jacobi inverses from the fine values.
-	template <class T> void Refresh(const T* values);
+	// Refresh from the fine values: A P and the fine block-Jacobi inverses always; the Galerkin
+	// coarse operator and its dense inverse when `coarse` (always on the first refresh).
+	template <class T> void Refresh(const T* values, bool coarse = true);
 	// z = M^{-1} v; kernels skip when *stop is set.
 	template <class T> void Apply(const T* fine_values, const double* v, double* z, const int* stop);
 	int levels() const { return (int)levels_.size(); }
@@ -74,6 +75,7 @@ private:
 	AmgOptions options_;
 	bool built_ = false;
 	bool masks_dirty_ = true;
+	bool coarse_ready_ = false;
 	long long launches_ = 0;
 	Profiler* profiler_ = nullptr;
 

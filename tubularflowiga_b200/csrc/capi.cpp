@@ -169,6 +169,8 @@ void tfiga_ns_default_params(tfiga_ns_params* p)
 	p->gmres_rtol = 1e-8;
 	p->preconditioner = TFIGA_PRECONDITIONER_BLOCK_JACOBI;
 	p->precision = TFIGA_PRECISION_FP64;
+	p->amg_coarse_nodes = 300;
+	p->amg_coarse_period = 1;
 }
 
 int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out)

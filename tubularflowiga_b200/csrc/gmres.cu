@@ -209,17 +209,31 @@ __global__ void CycleInitKernel(const double* __restrict__ beta, double* __restr
 	}
 }
 
-// Back substitution of the least-squares system (Gmres.hpp:308-315).
-__global__ void BackSolveKernel(const double* __restrict__ H, const double* __restrict__ g, int restart,
-	const int* __restrict__ state, double* __restrict__ y, int* __restrict__ error_flag)
+// Back substitution of the least-squares system (Gmres.hpp:308-315), column
+// oriented: y_row = b_row / H_row,row, then every earlier right-hand side
+// entry drops its H_t,row y_row term in parallel (one CTA, right-hand side in
+// shared memory).
+__global__ void __launch_bounds__(256) BackSolveKernel(const double* __restrict__ H, const double* __restrict__ g,
+	int restart, const int* __restrict__ state, double* __restrict__ y, int* __restrict__ error_flag)
 {
+	extern __shared__ double rhs[];
+	__shared__ double current;
 	const int used = state[1];
+	for (int i = threadIdx.x; i < used; i += blockDim.x) rhs[i] = g[i];
+	__syncthreads();
 	for (int row = used-1; row >= 0; --row) {
-		double v = g[row];
-		for (int c = row+1; c < used; ++c) v -= H[(size_t)row*restart+c]*y[c];
-		const double d = H[(size_t)row*restart+row];
-		if (fabs(d) < 1e-30) { *error_flag = 1; y[row] = 0.0; continue; }
-		y[row] = v/d;
+		if (threadIdx.x == 0) {
+			const double d = H[(size_t)row*restart+row];
+			double v = 0.0;
+			if (fabs(d) < 1e-30) *error_flag = 1;
+			else v = rhs[row]/d;
+			y[row] = v;
+			current = v;
+		}
+		__syncthreads();
+		const double v = current;
+		for (int t = threadIdx.x; t < row; t += blockDim.x) rhs[t] -= H[(size_t)t*restart+row]*v;
+		__syncthreads();
 	}
 }
 
@@ -314,6 +328,9 @@ Gmres::Gmres(int nodes, int restart, cudaStream_t stream)
 			(int)((size_t)(restart+1)*sizeof(double))), "solution update shared memory");
 	}
 	if ((size_t)chunk_*sizeof(double) > 227*1024) Fail(-7, "GMRES vector too long for the multi-dot chunking");
+	if ((size_t)(restart+1)*sizeof(double) > 48*1024)
+		CudaCheck(cudaFuncSetAttribute(BackSolveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)((size_t)(restart+1)*sizeof(double))), "back substitution shared memory");
 	finalize_smem_ = (size_t)(3*restart+1)*sizeof(double);
 	if (finalize_smem_ > 48*1024)
 		CudaCheck(cudaFuncSetAttribute(ArnoldiFinalizeKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -456,7 +473,7 @@ GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const T* valu
 			profiler_->AddBytes(Profiler::kOrtho, ArnoldiBytes(n_, used, (int)sizeof(T), true));
 			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, (int)sizeof(T)));
 		}
-		BackSolveKernel<<<1, 1, 0, stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(), state_.get()+2);
+		BackSolveKernel<<<1, 256, (size_t)(restart_+1)*sizeof(double), stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(), state_.get()+2);
 		LaunchCheck("BackSolveKernel");
 		SolutionUpdateKernel<<<blocks_, kThreads, (size_t)(restart_+1)*sizeof(double), stream_>>>(Z_.get(), n_,
 			nullptr, y_.get(), state_.get(), x);
@@ -537,7 +554,7 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, 8));
 		}
 		result.residual = host_->residual;
-		BackSolveKernel<<<1, 1, 0, stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(),
+		BackSolveKernel<<<1, 256, (size_t)(restart_+1)*sizeof(double), stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(),
 			state_.get()+2);
 		LaunchCheck("BackSolveKernel");
 		SolutionUpdateKernel<<<blocks_, kThreads, coef_smem, stream_>>>(V_.get(), n_, scale_.get(), y_.get(),

@@ -80,7 +80,13 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 		*pinned_status_ = 0;
 	}
 	if (params.preconditioner == TFIGA_PRECONDITIONER_AMG) {
-		amg_ = std::make_unique<Amg>(mesh.pattern_view(), mesh.pattern().row_offsets, mesh.pattern().columns, stream_);
+		if (params.amg_coarse_nodes < 1 || params.amg_coarse_nodes > 2048)
+			Fail(-1, "amg_coarse_nodes must be in [1, 2048]");
+		if (params.amg_coarse_period < 1) Fail(-1, "amg_coarse_period must be positive");
+		AmgOptions options;
+		options.coarsest_nodes = params.amg_coarse_nodes;
+		amg_ = std::make_unique<Amg>(mesh.pattern_view(), mesh.pattern().row_offsets, mesh.pattern().columns, stream_,
+			options);
 		amg_->set_profiler(&profiler_);
 	} else if (params.preconditioner != TFIGA_PRECONDITIONER_BLOCK_JACOBI) {
 		Fail(-1, "unknown preconditioner "+std::to_string(params.preconditioner));
@@ -219,18 +225,19 @@ void NsSolver::ApplyDirichlet()
 GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 {
 	update_.Zero(stream_);
+	struct Count { long long& n; ~Count() { ++n; } } count{solves_};
 	if (amg_) {
 		const long long before = amg_->launches();
 		GmresResult result;
 		if (mixed()) {
 			if (!amg_->built()) amg_->Build(values32_.get());
-			amg_->Refresh(values32_.get());
+			amg_->Refresh(values32_.get(), solves_ % params_.amg_coarse_period == 0);
 			launches_ += amg_->launches()-before;
 			result = gmres_.SolveFlexible<float>(mesh_.pattern_view(), values32_.get(), rhs_.get(), update_.get(), rtol,
 				max_iterations, *amg_, &launches_);
 		} else {
 			if (!amg_->built()) amg_->Build(values_.get());
-			amg_->Refresh(values_.get());
+			amg_->Refresh(values_.get(), solves_ % params_.amg_coarse_period == 0);
 			launches_ += amg_->launches()-before;
 			result = gmres_.SolveFlexible<double>(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol,
 				max_iterations, *amg_, &launches_);

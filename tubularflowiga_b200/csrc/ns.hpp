@@ -70,6 +70,7 @@ private:
 	cudaStream_t stream_ = nullptr;
 	cudaEvent_t events_[4] = {};
 	long long launches_ = 0;
+	long long solves_ = 0;                   // linear solves so far (coarse refresh period)
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
 	DeviceArray<float> values32_;
