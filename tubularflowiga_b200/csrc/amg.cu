@@ -109,43 +109,38 @@ __global__ void __launch_bounds__(256) ApKernel(long long ap_blocks, const int32
 	if (lane < 16) ap[B*16+lane] = acc;
 }
 
-// The fine-level half of the two-level application, one thread per fine node:
-// t = P x_c (masked), r = b - (A P) x_c, z = t + omega D^{-1} r.  Equal to
-// prolongation, residual and block-Jacobi step on the full operator, but it
-// reads the few A P blocks of the row instead of the row of A.
+// The fine-level half of the two-level application, four threads per fine
+// node (one per field row): t = P x_c (masked), r = b - (A P) x_c,
+// z = t + omega D^{-1} r, the node's four residual entries exchanged within
+// the lane quad.  Equal to prolongation, residual and block-Jacobi step on the
+// full operator, but it reads the few A P blocks of the row instead of the
+// row of A.
 __global__ void __launch_bounds__(256) CoarseCorrectionKernel(int nodes, const int32_t* __restrict__ agg,
 	const double* __restrict__ mask, const double* __restrict__ xc, const int32_t* __restrict__ ap_rows,
 	const int32_t* __restrict__ ap_cols, const double* __restrict__ ap, const double* __restrict__ b,
 	const double* __restrict__ inverse, double omega, double* __restrict__ z, const int* __restrict__ stop)
 {
 	if (*stop) return;
-	const int i = blockIdx.x*blockDim.x+threadIdx.x;
-	if (i >= nodes) return;
-	const double2* bv = reinterpret_cast<const double2*>(b+4*(size_t)i);
-	const double2 b01 = bv[0], b23 = bv[1];
-	double r[4] = {b01.x, b01.y, b23.x, b23.y};
-	for (int k = ap_rows[i]; k < ap_rows[i+1]; ++k) {
-		const double2* blk = reinterpret_cast<const double2*>(ap+(size_t)k*16);
-		const double2* xv = reinterpret_cast<const double2*>(xc+4*(size_t)ap_cols[k]);
-		const double2 x01 = xv[0], x23 = xv[1];
-		#pragma unroll
-		for (int row = 0; row < 4; ++row) {
-			const double2 a01 = blk[2*row], a23 = blk[2*row+1];
-			r[row] -= a01.x*x01.x+a01.y*x01.y+a23.x*x23.x+a23.y*x23.y;
+	const long long t = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	const int i = (int)(t >> 2), row = (int)(t & 3);
+	const bool active = i < nodes;
+	double r = 0.0;
+	if (active) {
+		r = b[t];
+		for (int k = ap_rows[i]; k < ap_rows[i+1]; ++k) {
+			const double2* blk = reinterpret_cast<const double2*>(ap+(size_t)k*16+row*4);
+			const double2* xv = reinterpret_cast<const double2*>(xc+4*(size_t)ap_cols[k]);
+			const double2 a01 = blk[0], a23 = blk[1], x01 = xv[0], x23 = xv[1];
+			r -= a01.x*x01.x+a01.y*x01.y+a23.x*x23.x+a23.y*x23.y;
 		}
 	}
-	const double* ci = xc+4*(size_t)agg[i];
-	const double* mi = mask+4*(size_t)i;
-	const double2* dinv = reinterpret_cast<const double2*>(inverse+(size_t)i*16);
-	double out[4];
-	#pragma unroll
-	for (int row = 0; row < 4; ++row) {
-		const double2 d01 = dinv[2*row], d23 = dinv[2*row+1];
-		out[row] = mi[row]*ci[row]+omega*(d01.x*r[0]+d01.y*r[1]+d23.x*r[2]+d23.y*r[3]);
-	}
-	double2* zv = reinterpret_cast<double2*>(z+4*(size_t)i);
-	zv[0] = make_double2(out[0], out[1]);
-	zv[1] = make_double2(out[2], out[3]);
+	const int base = threadIdx.x & ~3;
+	const double r0 = __shfl_sync(0xffffffffu, r, base & 31), r1 = __shfl_sync(0xffffffffu, r, (base+1) & 31);
+	const double r2 = __shfl_sync(0xffffffffu, r, (base+2) & 31), r3 = __shfl_sync(0xffffffffu, r, (base+3) & 31);
+	if (!active) return;
+	const double2* dinv = reinterpret_cast<const double2*>(inverse+(size_t)i*16+row*4);
+	const double2 d01 = dinv[0], d23 = dinv[1];
+	z[t] = mask[t]*xc[4*(size_t)agg[i]+row]+omega*(d01.x*r0+d01.y*r1+d23.x*r2+d23.y*r3);
 }
 
 // b_c[I,c] = sum_{i in I} mask_i[c] r[i,c]: one CTA per aggregate, fixed-order reduction.
@@ -617,7 +612,7 @@ void Amg::Cycle(int l, const T* A, const double* b, double* x, const int* stop)
 	DenseApplyKernel<<<Grid(C.dense_n, 8), 256, 0, stream_>>>(C.dense_n, C.dense.get(), C.b.get(), C.x.get(), stop);
 	LaunchCheck("DenseApplyKernel");
 	(void)A;      // the fine operator enters through A P, refreshed with it
-	CoarseCorrectionKernel<<<Grid(L.nodes, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(), C.x.get(),
+	CoarseCorrectionKernel<<<Grid(4LL*L.nodes, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(), C.x.get(),
 		L.ap_rows.get(), L.ap_cols.get(), L.ap_values.get(), b, L.inverse.get(), options_.omega, x, stop);
 	LaunchCheck("CoarseCorrectionKernel");
 	launches_ += 3;

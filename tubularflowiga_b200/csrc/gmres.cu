@@ -108,8 +108,10 @@ __global__ void __launch_bounds__(kThreads) DotFinalizeKernel(const double* __re
 }
 
 // out = w - sum_i scale_i hpass_i V_i; norm_partial[cta] = sum out^2 (if non-null).
-// out may alias w.  Each thread owns 16-byte pairs of entries and walks the
-// basis four vectors at a time (the FMA order per entry is the basis order).
+// out may alias w.  One CTA per tile of 32 entry pairs: its 8 warps split the
+// basis (a contiguous slice each, four vectors per step) so that many
+// independent loads are in flight, and warp 0 adds the 8 slice sums to w in
+// a fixed order.
 template <class B, class O>
 __global__ void __launch_bounds__(kThreads) UpdateKernel(const B* __restrict__ V, long long n,
 	const double* __restrict__ scale, int count, const double* __restrict__ hpass, const double* win, O* out,
@@ -117,40 +119,44 @@ __global__ void __launch_bounds__(kThreads) UpdateKernel(const B* __restrict__ V
 {
 	if (*stop) return;
 	extern __shared__ double coef[];
+	__shared__ double2 part[kWarps][32];
 	for (int i = threadIdx.x; i < count; i += blockDim.x) coef[i] = scale[i]*hpass[i];
 	__syncthreads();
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const long long n2 = n >> 1;
-	const double2* w2 = reinterpret_cast<const double2*>(win);
-	double sq = 0.0;
-	for (long long k = (long long)blockIdx.x*blockDim.x+threadIdx.x; k < n2; k += (long long)gridDim.x*blockDim.x) {
-		double2 v = w2[k];
-		int i = 0;
-		for (; i+3 < count; i += 4) {
+	const long long k = (long long)blockIdx.x*32+lane;
+	const int per = (count+kWarps-1)/kWarps;
+	const int lo = warp*per, hi = min(count, lo+per);
+	double2 acc = make_double2(0.0, 0.0);
+	if (k < n2) {
+		int i = lo;
+		for (; i+3 < hi; i += 4) {
 			const double2 a0 = BasisPair<B>::Load(V+(size_t)i*n, k), a1 = BasisPair<B>::Load(V+(size_t)(i+1)*n, k);
 			const double2 a2 = BasisPair<B>::Load(V+(size_t)(i+2)*n, k), a3 = BasisPair<B>::Load(V+(size_t)(i+3)*n, k);
-			v.x = fma(-coef[i], a0.x, v.x); v.y = fma(-coef[i], a0.y, v.y);
-			v.x = fma(-coef[i+1], a1.x, v.x); v.y = fma(-coef[i+1], a1.y, v.y);
-			v.x = fma(-coef[i+2], a2.x, v.x); v.y = fma(-coef[i+2], a2.y, v.y);
-			v.x = fma(-coef[i+3], a3.x, v.x); v.y = fma(-coef[i+3], a3.y, v.y);
+			acc.x = fma(-coef[i], a0.x, acc.x); acc.y = fma(-coef[i], a0.y, acc.y);
+			acc.x = fma(-coef[i+1], a1.x, acc.x); acc.y = fma(-coef[i+1], a1.y, acc.y);
+			acc.x = fma(-coef[i+2], a2.x, acc.x); acc.y = fma(-coef[i+2], a2.y, acc.y);
+			acc.x = fma(-coef[i+3], a3.x, acc.x); acc.y = fma(-coef[i+3], a3.y, acc.y);
 		}
-		for (; i < count; ++i) {
+		for (; i < hi; ++i) {
 			const double2 a0 = BasisPair<B>::Load(V+(size_t)i*n, k);
-			v.x = fma(-coef[i], a0.x, v.x); v.y = fma(-coef[i], a0.y, v.y);
+			acc.x = fma(-coef[i], a0.x, acc.x); acc.y = fma(-coef[i], a0.y, acc.y);
 		}
+	}
+	part[warp][lane] = acc;
+	__syncthreads();
+	if (warp != 0) return;
+	double sq = 0.0;
+	if (k < n2) {
+		double2 v = reinterpret_cast<const double2*>(win)[k];
+		#pragma unroll
+		for (int w = 0; w < kWarps; ++w) { v.x += part[w][lane].x; v.y += part[w][lane].y; }
 		BasisPair<O>::Store(out, k, v);
-		sq = fma(v.x, v.x, sq);
-		sq = fma(v.y, v.y, sq);
+		sq = fma(v.x, v.x, v.y*v.y);
 	}
 	if (norm_partial == nullptr) return;
-	__shared__ double red[kWarps];
 	for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
-	__syncthreads();
-	if (threadIdx.x == 0) {
-		double s = 0.0;
-		for (int w = 0; w < kWarps; ++w) s += red[w];
-		norm_partial[blockIdx.x] = s;
-	}
+	if (lane == 0) norm_partial[blockIdx.x] = sq;
 }
 
 // Column j of the Hessenberg matrix: norm, previous rotations, new rotation,
@@ -164,9 +170,15 @@ __global__ void ArnoldiFinalizeKernel(const double* __restrict__ norm_partial, i
 	double* col = sh;                 // [restart+1]
 	double* c = col+restart+1;        // [restart]
 	double* s_ = c+restart;           // [restart]
+	__shared__ double red[kWarps];
 	if (state[0]) return;
 	double s = 0.0;
-	for (int b = threadIdx.x; b < blocks; b += 32) s += norm_partial[b];
+	for (int b = threadIdx.x; b < blocks; b += blockDim.x) s += norm_partial[b];
+	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+	__syncthreads();
+	if (threadIdx.x >= 32) return;
+	s = threadIdx.x < kWarps ? red[threadIdx.x] : 0.0;
 	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
 	const double next = sqrt(s);
 	for (int i = threadIdx.x; i <= j; i += 32) col[i] = H[(size_t)i*restart+j];
@@ -304,7 +316,8 @@ Gmres::Gmres(int nodes, int restart, cudaStream_t stream)
 	H_.Allocate((size_t)(restart+1)*restart);
 	cs_.Allocate(restart); sn_.Allocate(restart); g_.Allocate(restart+1); y_.Allocate(restart);
 	scale_.Allocate(restart+1);
-	norm_partial_.Allocate(std::max(PartialSlots(), blocks_));
+	update_blocks_ = (int)(((long long)n_/2+31)/32);
+	norm_partial_.Allocate(std::max(std::max(PartialSlots(), blocks_), update_blocks_));
 	scalar_.Allocate(2);
 	state_.Allocate(4);
 	residual_.Allocate(1);
@@ -374,10 +387,10 @@ void Gmres::Orthogonalize(int j, B* basis)
 			count, hpass_.get(), H_.get(), restart_, j, pass, stop);
 		LaunchCheck("DotFinalizeKernel");
 		if (pass == 0)
-			UpdateKernel<B, double><<<blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
+			UpdateKernel<B, double><<<update_blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
 				hpass_.get(), w_.get(), w_.get(), nullptr, stop);
 		else
-			UpdateKernel<B, B><<<blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
+			UpdateKernel<B, B><<<update_blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
 				hpass_.get(), w_.get(), basis+(size_t)(j+1)*n_, norm_partial_.get(), stop);
 		LaunchCheck("UpdateKernel");
 	}
@@ -456,7 +469,7 @@ GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const T* valu
 			const int batch = std::min(kBatch, cap-j);
 			for (int b = 0; b < batch; ++b) {
 				FlexibleStep<T>(pattern, values, j+b, M);
-				ArnoldiFinalizeKernel<<<1, 32, finalize_smem_, stream_>>>(norm_partial_.get(), blocks_, H_.get(), restart_, j+b,
+				ArnoldiFinalizeKernel<<<1, kThreads, finalize_smem_, stream_>>>(norm_partial_.get(), update_blocks_, H_.get(), restart_, j+b,
 					cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance);
 				LaunchCheck("ArnoldiFinalizeKernel");
 				launches_ += 1;
@@ -536,7 +549,7 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 			const int batch = std::min(kBatch, cap-j);
 			for (int b = 0; b < batch; ++b) {
 				Step(pattern, values, j+b);
-				ArnoldiFinalizeKernel<<<1, 32, finalize_smem_, stream_>>>(norm_partial_.get(), blocks_, H_.get(), restart_, j+b,
+				ArnoldiFinalizeKernel<<<1, kThreads, finalize_smem_, stream_>>>(norm_partial_.get(), update_blocks_, H_.get(), restart_, j+b,
 					cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance);
 				LaunchCheck("ArnoldiFinalizeKernel");
 				launches_ += 1;

@@ -57,6 +57,7 @@ private:
 	double TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs, const double* x);
 
 	int nodes_, n_, restart_, blocks_;
+	int update_blocks_ = 0;           // CTAs of the basis update (one per 32 entry pairs)
 	int chunk_;
 	size_t finalize_smem_ = 0;
 	cudaStream_t stream_;
