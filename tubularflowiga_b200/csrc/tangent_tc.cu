@@ -26,9 +26,11 @@
 //             as BF16 in the 64-byte-swizzled K-major layout; one thread issues
 //             4 tiles x 2 tcgen05.mma (128 x 64 x 16) and commits to an mbarrier;
 //             the next chunk waits on it before overwriting the operands;
-//   epilogue  tcgen05.ld rows (b, f) x 32 columns a, a 4x4 transpose inside
-//             each lane quad gives the four f of one (a, b), which go to the
-//             FP32 matrix as one red.global.add.v4.f32.
+//   epilogue  tcgen05.ld rows (b, f) x 32 columns a of both row fields; shuffles
+//             inside each lane quad give every lane the four f of one (a, b,
+//             row field), and the two row fields of one (a, b) -- the two
+//             halves of a 32-byte sector -- go out from adjacent lanes of the
+//             same red.global.add.v4.f32 instruction.
 // Every mbarrier wait is bounded (one second of globaltimer); on expiry the
 // CTA records TFIGA status bit 1, waits once more (bounded) for its own MMAs,
 // frees its tensor memory and returns without writing the tangent.
@@ -400,39 +402,46 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 	if (!failed) failed = __syncthreads_or(!MbarWaitBounded(bar, pending)) != 0;
 
 	if (!failed) {
-		// 6. Epilogue: warp -> (row field il = warp/4, TMEM lane quarter warp%4), two tiles, two column halves.
+		// 6. Epilogue: warp -> (basis half bh = warp/4 of b, TMEM lane quarter warp%4); both row fields.
+		//    Lane f of a quad holds column field f of node b for every a.  In pass p the quad's lanes
+		//    write (a = 4g + (f & 2) + p, row field 2h + (f & 1), all four column fields), so lanes
+		//    f, f^1 fill the two 16-byte halves of one 32-byte sector in the same instruction.  Each
+		//    round r of a pass sends to lane f^r the value it needs from this lane's column field.
 		FenceAfterSync();
-		const int il = warp >> 2, quarter = warp & 3;
-		const int i = 2*h+il;
+		const int bh = warp >> 2, quarter = warp & 3;
 		const int32_t* EB = element_blocks+(size_t)e*kMaxBasis*kMaxBasis;
 		const int f = lane & 3;
-		for (int th = 0; th < 2; ++th) {
-			const int tile = il*2+th;
-			const int b = th*32+quarter*8+(lane >> 2);
-			for (int ah = 0; ah < 2; ++ah) {
-				int blocks[8];                // block of (a = 32 ah + 4 g + f, b), fetched before the TMEM load
+		const int b = bh*32+quarter*8+(lane >> 2);
+		float* row_base = values+(size_t)(2*h+(f & 1))*4;
+		for (int ah = 0; ah < 2; ++ah) {
+			int blocks[2][8];                 // fetched before the TMEM loads
+			#pragma unroll
+			for (int g = 0; g < 8; ++g)
 				#pragma unroll
-				for (int g = 0; g < 8; ++g) {
-					const int a = ah*32+4*g+f;
-					blocks[g] = (a < nen && b < nen) ? EB[a*kMaxBasis+b] : -1;
+				for (int p = 0; p < 2; ++p) {
+					const int a = ah*32+4*g+(f & 2)+p;
+					blocks[p][g] = (a < nen && b < nen) ? EB[a*kMaxBasis+b] : -1;
 				}
-				float v[32];
-				TmemLoad32(tmem+((uint32_t)(quarter*32) << 16)+tile*64+ah*32, v);
+			float v0[32], v1[32];
+			const uint32_t lanes = (uint32_t)(quarter*32) << 16;
+			TmemLoad32(tmem+lanes+bh*64+ah*32, v0);          // row field 2h
+			TmemLoad32(tmem+lanes+(2+bh)*64+ah*32, v1);      // row field 2h+1
+			#pragma unroll
+			for (int g = 0; g < 8; ++g)
 				#pragma unroll
-				for (int g = 0; g < 8; ++g) {
-					const float x0 = v[4*g], x1 = v[4*g+1], x2 = v[4*g+2], x3 = v[4*g+3];
+				for (int p = 0; p < 2; ++p) {
+					const float c00 = v0[4*g+p], c02 = v0[4*g+2+p], c10 = v1[4*g+p], c12 = v1[4*g+2+p];
 					float o0 = 0.f, o1 = 0.f, o2 = 0.f, o3 = 0.f;
 					#pragma unroll
 					for (int r = 0; r < 4; ++r) {
-						const int src = f ^ r;    // field of the partner lane = column offset it needs from us
-						const float send = Pick4(x0, x1, x2, x3, src);
+						const int d = f ^ r;          // the lane served this round (and the source heard from)
+						const float send = (d & 1) ? ((d & 2) ? c12 : c10) : ((d & 2) ? c02 : c00);
 						const float got = r ? __shfl_xor_sync(0xffffffffu, send, r) : send;
-						o0 = src == 0 ? got : o0; o1 = src == 1 ? got : o1;
-						o2 = src == 2 ? got : o2; o3 = src == 3 ? got : o3;
+						o0 = d == 0 ? got : o0; o1 = d == 1 ? got : o1;
+						o2 = d == 2 ? got : o2; o3 = d == 3 ? got : o3;
 					}
-					if (blocks[g] >= 0) RedAdd4(values+(size_t)blocks[g]*16+i*4, o0, o1, o2, o3);
+					if (blocks[p][g] >= 0) RedAdd4(row_base+(size_t)blocks[p][g]*16, o0, o1, o2, o3);
 				}
-			}
 		}
 	} else {
 		if (tid == 0) atomicOr(status, 1);
