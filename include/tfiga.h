@@ -42,6 +42,7 @@ extern "C" {
 
 typedef struct tfiga_mesh tfiga_mesh;
 typedef struct tfiga_ns tfiga_ns;
+typedef struct tfiga_learned tfiga_learned;
 
 /* Flattened mesh, the layout of iga::cuda::FlatMesh
  * (solvers/cuda/include/DeviceMesh.hpp:16-57). */
@@ -246,6 +247,51 @@ int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int3
  * FGMRES vector), s_v the basis entry size; moved: both classical
  * Gram-Schmidt passes.  The other families report 0. */
 int tfiga_ns_profile_bytes(tfiga_ns* ns, double* bytes);
+
+/* ---- learned FGMRES preconditioner stage ------------------------------ */
+/* A message-passing network over the element face-adjacency graph (hidden
+ * width 64, `layers` message-passing layers) that adds N(D^{-1} r) to the AMG
+ * application inside the flexible GMRES: z = M_AMG(r) + N(D^{-1} r).  FGMRES
+ * still drives the FP64 true residual to the same tolerance, so the network
+ * changes only the iteration count.  Training pairs come from the solver
+ * itself: with `collect` on, every solved Newton system J delta = b adds
+ * (D^{-1} b / |b|, (delta - M_AMG(b)) / |b|).  Inference reads BF16 weights
+ * with FP32 accumulation; training (hand-written backward kernels, Adam)
+ * keeps FP32 master weights.  The parameter vector layout and the network
+ * definition are those of the CPU oracle (oracle/learned_oracle.py).  No
+ * counterpart in the reference.  Needs TFIGA_PRECONDITIONER_AMG.  Destroying
+ * the ns handle detaches it. */
+/* linear != 0: identity activation and zero biases (the stage is then a fixed linear operator). */
+int tfiga_learned_create(tfiga_ns* ns, int32_t layers, uint64_t seed, int32_t linear, tfiga_learned** out);
+int tfiga_learned_destroy(tfiga_learned* learned);
+int tfiga_learned_info(const tfiga_learned* learned, int64_t* parameters, int64_t* elements, int32_t* pairs);
+/* learned = NULL detaches; use: apply in the FGMRES; collect: store a pair per Newton solve. */
+int tfiga_ns_set_learned(tfiga_ns* ns, tfiga_learned* learned, int32_t use, int32_t collect);
+/* Linear solves that did not converge with the learned stage and were redone with the AMG alone. */
+int tfiga_ns_learned_fallbacks(const tfiga_ns* ns, int64_t* count);
+/* Per-field input/output scales and loss weights from the stored pairs. */
+int tfiga_learned_fit_scales(tfiga_learned* learned);
+/* `steps` Adam steps over the stored pairs; *loss = mean loss of the last pass. */
+int tfiga_learned_train(tfiga_learned* learned, int32_t steps, double learning_rate, double* loss);
+int tfiga_learned_evaluate(tfiga_learned* learned, double* loss);
+/* Least-squares output gain over the stored pairs, folded into the output scales (clamped at 0, so
+ * a stage that learned nothing adds nothing); *gain receives it. */
+int tfiga_learned_fit_gain(tfiga_learned* learned, double* gain);
+int tfiga_learned_get_parameters(const tfiga_learned* learned, float* parameters);
+int tfiga_learned_set_parameters(tfiga_learned* learned, const float* parameters);
+/* scales[0..3] input, [4..7] output, [8..11] loss weights. */
+int tfiga_learned_get_scales(const tfiga_learned* learned, double* scales);
+int tfiga_learned_set_scales(tfiga_learned* learned, const double* scales);
+/* Face neighbours [6 * elements], -1 = none. */
+int tfiga_learned_neighbours(const tfiga_learned* learned, int32_t* neighbours);
+/* FP32 forward o = N(x) and loss/gradient against a target (device vectors of 4n doubles). */
+int tfiga_learned_forward_device(tfiga_learned* learned, const double* x_device, double* o_device);
+/* The inference path used inside the FGMRES (BF16 weights): z_device += N(x_device). */
+int tfiga_learned_apply_device(tfiga_learned* learned, const double* x_device, double* z_device);
+int tfiga_learned_loss_gradient_device(tfiga_learned* learned, const double* x_device, const double* target_device,
+	double* loss, float* gradient);
+int tfiga_learned_save(const tfiga_learned* learned, const char* path);
+int tfiga_learned_load(tfiga_learned* learned, const char* path);
 
 /* ---- allocation-free kernel ------------------------------------------- */
 /* *norm_device = ||b - A x||_2 for a 4x4 block-CSR matrix given entirely by

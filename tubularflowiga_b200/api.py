@@ -116,6 +116,27 @@ SIGNATURES = {
     "tfiga_ns_profile_bytes": (C.c_int, [C.c_void_p, C.c_void_p]),
     "tfiga_block_residual_norm_static": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                    C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_learned_create": (C.c_int, [C.c_void_p, C.c_int32, C.c_uint64, C.c_int32, C.POINTER(C.c_void_p)]),
+    "tfiga_learned_destroy": (C.c_int, [C.c_void_p]),
+    "tfiga_learned_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                     C.POINTER(C.c_int32)]),
+    "tfiga_ns_set_learned": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
+    "tfiga_learned_fit_scales": (C.c_int, [C.c_void_p]),
+    "tfiga_ns_learned_fallbacks": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "tfiga_learned_train": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.POINTER(C.c_double)]),
+    "tfiga_learned_evaluate": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "tfiga_learned_fit_gain": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "tfiga_learned_get_parameters": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tfiga_learned_set_parameters": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tfiga_learned_get_scales": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tfiga_learned_set_scales": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tfiga_learned_neighbours": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tfiga_learned_forward_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_learned_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_learned_loss_gradient_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                                                     C.c_void_p]),
+    "tfiga_learned_save": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "tfiga_learned_load": (C.c_int, [C.c_void_p, C.c_char_p]),
     "tfiga_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
 }
 
@@ -325,6 +346,108 @@ class NavierStokes:
         try:
             self.close()
         except Exception:
+            pass
+
+
+class Learned:
+    """Learned FGMRES preconditioner stage of a NavierStokes handle (AMG preconditioner); see tfiga.h."""
+
+    def __init__(self, ns: "NavierStokes", layers: int = 3, seed: int = 0, linear: bool = False):
+        self.ns = ns
+        self.layers = layers
+        self.linear = linear
+        self._h = C.c_void_p()
+        check(lib().tfiga_learned_create(ns._h, layers, seed, int(linear), C.byref(self._h)))
+        p, e, q = C.c_int64(), C.c_int64(), C.c_int32()
+        check(lib().tfiga_learned_info(self._h, C.byref(p), C.byref(e), C.byref(q)))
+        self.parameter_count, self.elements = int(p.value), int(e.value)
+
+    def pairs(self) -> int:
+        p, e, q = C.c_int64(), C.c_int64(), C.c_int32()
+        check(lib().tfiga_learned_info(self._h, C.byref(p), C.byref(e), C.byref(q)))
+        return int(q.value)
+
+    def attach(self, use=True, collect=False):
+        check(lib().tfiga_ns_set_learned(self.ns._h, self._h, int(use), int(collect)))
+
+    def detach(self):
+        check(lib().tfiga_ns_set_learned(self.ns._h, None, 0, 0))
+
+    def fit_scales(self):
+        check(lib().tfiga_learned_fit_scales(self._h))
+
+    def fallbacks(self) -> int:
+        c = C.c_int64()
+        check(lib().tfiga_ns_learned_fallbacks(self.ns._h, C.byref(c)))
+        return int(c.value)
+
+    def train(self, steps: int, learning_rate: float = 1e-3) -> float:
+        loss = C.c_double()
+        check(lib().tfiga_learned_train(self._h, steps, learning_rate, C.byref(loss)))
+        return loss.value
+
+    def evaluate(self) -> float:
+        loss = C.c_double()
+        check(lib().tfiga_learned_evaluate(self._h, C.byref(loss)))
+        return loss.value
+
+    def fit_gain(self) -> float:
+        g = C.c_double()
+        check(lib().tfiga_learned_fit_gain(self._h, C.byref(g)))
+        return g.value
+
+    def parameters(self) -> np.ndarray:
+        out = np.zeros(self.parameter_count, np.float32)
+        check(lib().tfiga_learned_get_parameters(self._h, _p(out)))
+        return out
+
+    def set_parameters(self, theta):
+        t = np.ascontiguousarray(theta, np.float32)
+        assert t.size == self.parameter_count
+        check(lib().tfiga_learned_set_parameters(self._h, _p(t)))
+
+    def scales(self) -> np.ndarray:
+        out = np.zeros(12)
+        check(lib().tfiga_learned_get_scales(self._h, _p(out)))
+        return out
+
+    def set_scales(self, scales):
+        s = np.ascontiguousarray(scales, np.float64)
+        check(lib().tfiga_learned_set_scales(self._h, _p(s)))
+
+    def neighbours(self) -> np.ndarray:
+        out = np.zeros((self.elements, 6), np.int32)
+        check(lib().tfiga_learned_neighbours(self._h, _p(out)))
+        return out
+
+    def forward_device(self, x_ptr: int, o_ptr: int):
+        check(lib().tfiga_learned_forward_device(self._h, C.c_void_p(x_ptr), C.c_void_p(o_ptr)))
+
+    def apply_device(self, x_ptr: int, z_ptr: int):
+        check(lib().tfiga_learned_apply_device(self._h, C.c_void_p(x_ptr), C.c_void_p(z_ptr)))
+
+    def loss_gradient_device(self, x_ptr: int, t_ptr: int):
+        loss = C.c_double()
+        grad = np.zeros(self.parameter_count, np.float32)
+        check(lib().tfiga_learned_loss_gradient_device(self._h, C.c_void_p(x_ptr), C.c_void_p(t_ptr), C.byref(loss),
+                                                        _p(grad)))
+        return loss.value, grad
+
+    def save(self, path):
+        check(lib().tfiga_learned_save(self._h, str(path).encode()))
+
+    def load(self, path):
+        check(lib().tfiga_learned_load(self._h, str(path).encode()))
+
+    def close(self):
+        if self._h:
+            lib().tfiga_learned_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 -- interpreter shutdown
             pass
 
 

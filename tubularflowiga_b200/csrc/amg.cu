@@ -288,6 +288,11 @@ std::vector<int> Amg::level_nodes() const
 	return out;
 }
 
+const double* Amg::fine_inverse() const
+{
+	return levels_.empty() ? nullptr : levels_[0]->inverse.get();
+}
+
 long long Amg::transfer_blocks() const
 {
 	return levels_.empty() ? 0 : levels_[0]->ap_blocks;

@@ -59,6 +59,8 @@ public:
 	const std::vector<int>& aggregation_rounds() const { return coarse_history_; }
 	std::vector<long long> level_blocks() const;
 	long long transfer_blocks() const;
+	// Block-Jacobi inverses (4x4 per node, FP64) of the fine level, current after Refresh.
+	const double* fine_inverse() const;
 	long long launches() const { return launches_; }
 	void set_profiler(Profiler* p) { profiler_ = p; }
 

@@ -1,11 +1,14 @@
 // extern "C" boundary: every entry point converts exceptions into a status
 // code plus a thread-local message (tfiga_last_error).
+#include "learned.hpp"
 #include "mesh.hpp"
 #include "ns.hpp"
 
 #include "../../include/tfiga.h"
 
+#include <cmath>
 #include <cstring>
+#include <fstream>
 #include <exception>
 #include <memory>
 #include <new>
@@ -15,9 +18,18 @@ struct tfiga_mesh {
 	std::unique_ptr<tfiga::Mesh> mesh;
 };
 
+struct tfiga_learned;
+
 struct tfiga_ns {
 	tfiga_mesh* mesh = nullptr;
 	std::unique_ptr<tfiga::NsSolver> solver;
+	tfiga_learned* learned = nullptr;       // attached learned stage (not owned)
+};
+
+struct tfiga_learned {
+	std::unique_ptr<tfiga::LearnedPreconditioner> net;
+	tfiga_ns* owner = nullptr;              // the ns handle it was created on (its mesh and stream)
+	tfiga_ns* attached = nullptr;
 };
 
 namespace {
@@ -187,7 +199,13 @@ int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** 
 
 int tfiga_ns_destroy(tfiga_ns* ns)
 {
-	return Guard([&] { delete ns; });
+	return Guard([&] {
+		if (ns && ns->learned) {
+			if (ns->learned->attached == ns) ns->learned->attached = nullptr;
+			if (ns->learned->owner == ns) ns->learned->owner = nullptr;
+		}
+		delete ns;
+	});
 }
 
 int tfiga_ns_set_dirichlet(tfiga_ns* ns, const int32_t* vmask, const int32_t* pmask, const double* velocity,
@@ -382,6 +400,220 @@ int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int3
 		long long counts[tfiga::Profiler::kFamilies];
 		ns->solver->profiler().Totals(milliseconds, counts, reset != 0);
 		if (launches) for (int f = 0; f < tfiga::Profiler::kFamilies; ++f) launches[f] = counts[f];
+	});
+}
+
+int tfiga_learned_create(tfiga_ns* ns, int32_t layers, uint64_t seed, int32_t linear, tfiga_learned** out)
+{
+	return Guard([&] {
+		Require(ns && out, "null argument");
+		*out = nullptr;
+		if (!ns->solver->amg()) tfiga::Fail(TFIGA_E_UNSUPPORTED, "the learned stage needs TFIGA_PRECONDITIONER_AMG");
+		auto handle = std::make_unique<tfiga_learned>();
+		handle->net = std::make_unique<tfiga::LearnedPreconditioner>(*ns->mesh->mesh, layers, seed,
+			ns->solver->stream(), linear != 0);
+		handle->owner = ns;
+		*out = handle.release();
+	});
+}
+
+int tfiga_learned_destroy(tfiga_learned* learned)
+{
+	return Guard([&] {
+		if (!learned) return;
+		if (learned->attached) {
+			learned->attached->solver->SetLearned(nullptr, false, false);
+			learned->attached->learned = nullptr;
+		}
+		delete learned;
+	});
+}
+
+int tfiga_learned_info(const tfiga_learned* learned, int64_t* parameters, int64_t* elements, int32_t* pairs)
+{
+	return Guard([&] {
+		Require(learned != nullptr, "null handle");
+		if (parameters) *parameters = learned->net->parameter_count();
+		if (elements) *elements = learned->net->elements();
+		if (pairs) *pairs = learned->net->pair_count();
+	});
+}
+
+int tfiga_ns_set_learned(tfiga_ns* ns, tfiga_learned* learned, int32_t use, int32_t collect)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		if (learned && learned->owner != ns)
+			tfiga::Fail(TFIGA_E_INVALID, "the learned stage belongs to another solver handle");
+		ns->solver->SetLearned(learned ? learned->net.get() : nullptr, use != 0, collect != 0);
+		if (ns->learned && ns->learned != learned) ns->learned->attached = nullptr;
+		ns->learned = learned;
+		if (learned) learned->attached = ns;
+	});
+}
+
+int tfiga_ns_learned_fallbacks(const tfiga_ns* ns, int64_t* count)
+{
+	return Guard([&] {
+		Require(ns && count, "null argument");
+		*count = ns->solver->learned_fallbacks();
+	});
+}
+
+int tfiga_learned_fit_scales(tfiga_learned* learned)
+{
+	return Guard([&] { Require(learned != nullptr, "null handle"); if (learned->owner) learned->owner->solver->BindLearnedOperator(*learned->net);
+		learned->net->FitScales(); });
+}
+
+int tfiga_learned_train(tfiga_learned* learned, int32_t steps, double learning_rate, double* loss)
+{
+	return Guard([&] {
+		Require(learned != nullptr && steps >= 0, "invalid argument");
+		Require(learning_rate > 0.0 && std::isfinite(learning_rate), "learning rate must be positive");
+		if (learned->owner) learned->owner->solver->BindLearnedOperator(*learned->net);
+		const double l = learned->net->Train(steps, learning_rate);
+		if (loss) *loss = l;
+	});
+}
+
+int tfiga_learned_evaluate(tfiga_learned* learned, double* loss)
+{
+	return Guard([&] {
+		Require(learned && loss, "null argument");
+		if (learned->owner) learned->owner->solver->BindLearnedOperator(*learned->net);
+		*loss = learned->net->EvaluatePairs();
+	});
+}
+
+int tfiga_learned_fit_gain(tfiga_learned* learned, double* gain)
+{
+	return Guard([&] {
+		Require(learned != nullptr, "null handle");
+		if (learned->owner) learned->owner->solver->BindLearnedOperator(*learned->net);
+		const double g = learned->net->FitGain();
+		if (gain) *gain = g;
+	});
+}
+
+int tfiga_learned_get_parameters(const tfiga_learned* learned, float* parameters)
+{
+	return Guard([&] { Require(learned && parameters, "null argument"); learned->net->GetParameters(parameters); });
+}
+
+int tfiga_learned_set_parameters(tfiga_learned* learned, const float* parameters)
+{
+	return Guard([&] { Require(learned && parameters, "null argument"); learned->net->SetParameters(parameters); });
+}
+
+int tfiga_learned_get_scales(const tfiga_learned* learned, double* scales)
+{
+	return Guard([&] {
+		Require(learned && scales, "null argument");
+		learned->net->GetScales(scales, scales+4, scales+8);
+	});
+}
+
+int tfiga_learned_set_scales(tfiga_learned* learned, const double* scales)
+{
+	return Guard([&] {
+		Require(learned && scales, "null argument");
+		learned->net->SetScales(scales, scales+4, scales+8);
+	});
+}
+
+int tfiga_learned_neighbours(const tfiga_learned* learned, int32_t* neighbours)
+{
+	return Guard([&] {
+		Require(learned && neighbours, "null argument");
+		const auto& nb = learned->net->neighbours();
+		std::memcpy(neighbours, nb.data(), nb.size()*sizeof(int32_t));
+	});
+}
+
+int tfiga_learned_forward_device(tfiga_learned* learned, const double* x_device, double* o_device)
+{
+	return Guard([&] {
+		Require(learned && x_device && o_device, "null argument");
+		learned->net->Forward(x_device, o_device);
+		tfiga::CudaCheck(cudaStreamSynchronize(learned->net->stream()), "learned forward");
+	});
+}
+
+int tfiga_learned_apply_device(tfiga_learned* learned, const double* x_device, double* z_device)
+{
+	return Guard([&] {
+		Require(learned && x_device && z_device, "null argument");
+		learned->net->Apply(x_device, z_device, nullptr);
+		tfiga::CudaCheck(cudaStreamSynchronize(learned->net->stream()), "learned apply");
+	});
+}
+
+int tfiga_learned_loss_gradient_device(tfiga_learned* learned, const double* x_device, const double* target_device,
+	double* loss, float* gradient)
+{
+	return Guard([&] {
+		Require(learned && x_device && target_device, "null argument");
+		const double l = learned->net->LossAndGradient(x_device, target_device);
+		if (loss) *loss = l;
+		if (gradient) {
+			tfiga::CudaCheck(cudaMemcpyAsync(gradient, learned->net->gradient(),
+				sizeof(float)*(size_t)learned->net->parameter_count(), cudaMemcpyDeviceToHost, learned->net->stream()),
+				"learned gradient");
+			tfiga::CudaCheck(cudaStreamSynchronize(learned->net->stream()), "learned gradient");
+		}
+	});
+}
+
+namespace {
+const char kLearnedMagic[8] = {'T', 'F', 'L', 'R', 'N', '0', '0', '1'};
+}
+
+int tfiga_learned_save(const tfiga_learned* learned, const char* path)
+{
+	return Guard([&] {
+		Require(learned && path, "null argument");
+		const auto& net = *learned->net;
+		std::vector<float> theta(net.parameter_count());
+		net.GetParameters(theta.data());
+		double scales[12];
+		net.GetScales(scales, scales+4, scales+8);
+		std::ofstream f(path, std::ios::binary);
+		if (!f) tfiga::Fail(TFIGA_E_IO, std::string("cannot write ")+path);
+		const int32_t layers = net.layers();
+		const int64_t count = net.parameter_count();
+		f.write(kLearnedMagic, 8);
+		f.write(reinterpret_cast<const char*>(&layers), sizeof(layers));
+		f.write(reinterpret_cast<const char*>(&count), sizeof(count));
+		f.write(reinterpret_cast<const char*>(theta.data()), sizeof(float)*theta.size());
+		f.write(reinterpret_cast<const char*>(scales), sizeof(scales));
+		if (!f) tfiga::Fail(TFIGA_E_IO, std::string("write failed: ")+path);
+	});
+}
+
+int tfiga_learned_load(tfiga_learned* learned, const char* path)
+{
+	return Guard([&] {
+		Require(learned && path, "null argument");
+		auto& net = *learned->net;
+		std::ifstream f(path, std::ios::binary);
+		if (!f) tfiga::Fail(TFIGA_E_IO, std::string("cannot read ")+path);
+		char magic[8];
+		int32_t layers = 0;
+		int64_t count = 0;
+		f.read(magic, 8);
+		f.read(reinterpret_cast<char*>(&layers), sizeof(layers));
+		f.read(reinterpret_cast<char*>(&count), sizeof(count));
+		if (!f || std::memcmp(magic, kLearnedMagic, 8) != 0) tfiga::Fail(TFIGA_E_FORMAT, "not a learned-stage file");
+		if (layers != net.layers() || count != net.parameter_count())
+			tfiga::Fail(TFIGA_E_FORMAT, "learned-stage file has a different architecture");
+		std::vector<float> theta(count);
+		double scales[12];
+		f.read(reinterpret_cast<char*>(theta.data()), sizeof(float)*theta.size());
+		f.read(reinterpret_cast<char*>(scales), sizeof(scales));
+		if (!f) tfiga::Fail(TFIGA_E_FORMAT, "truncated learned-stage file");
+		net.SetParameters(theta.data());
+		net.SetScales(scales, scales+4, scales+8);
 	});
 }
 

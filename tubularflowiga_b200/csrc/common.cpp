@@ -1,6 +1,8 @@
 // Errors, CUDA checks, device requirement and allocation accounting.
 #include "common.hpp"
 
+#include <cuda_bf16.h>
+
 #include <atomic>
 #include <string>
 
@@ -45,6 +47,7 @@ template class DeviceArray<unsigned>;
 template class DeviceArray<float>;
 template class DeviceArray<int64_t>;
 template class DeviceArray<uint16_t>;
+template class DeviceArray<__nv_bfloat16>;
 
 long long DeviceBytesLive() { return g_live.load(); }
 long long DeviceBytesPeak() { return g_peak.load(); }

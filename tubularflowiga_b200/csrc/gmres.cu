@@ -415,10 +415,24 @@ void Gmres::FlexibleStep(const DevicePatternView& pattern, const T* values, int 
 	launches_ += 1;
 	double* z = Z_.get()+(size_t)j*n_;
 	M.Apply(values, r_.get(), z, stop);
+	if (learned_ != nullptr) {
+		// z += N(D^{-1} r) on the unit residual r
+		LaunchApplyBlockInverse(nodes_, M.fine_inverse(), r_.get(), tmp_.get(), stream_);
+		learned_->Apply(tmp_.get(), z, stop);
+		launches_ += 1+3+learned_->layers();
+	}
 	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
 	LaunchSpmvBlockJacobi<T>(pattern, values, nullptr, z, nullptr, w_.get(), stop, stream_);
 	if (profiler_) profiler_->End(stream_);
 	launches_ += 1;
+	if (collector_ != nullptr && j%kBatch == 0) {
+		if (pair_dinv_.size() == 0) { pair_dinv_.Allocate(n_); pair_amg_.Allocate(n_); pair_aamg_.Allocate(n_); }
+		LaunchApplyBlockInverse(nodes_, M.fine_inverse(), w_.get(), pair_dinv_.get(), stream_);
+		M.Apply(values, w_.get(), pair_amg_.get(), stop);
+		LaunchSpmv<T>(pattern, values, pair_amg_.get(), pair_aamg_.get(), stream_);
+		collector_->AddKrylovPair(pair_dinv_.get(), z, pair_amg_.get(), w_.get(), pair_aamg_.get(), stop);
+		launches_ += 6;
+	}
 	Orthogonalize<T>(j, basis);
 }
 

@@ -14,6 +14,7 @@
 #include "amg.hpp"
 #include "common.hpp"
 #include "kernels.cuh"
+#include "learned.hpp"
 
 namespace tfiga {
 
@@ -42,6 +43,11 @@ public:
 	GmresResult SolveFlexible(const DevicePatternView& pattern, const T* values, const double* rhs, double* x,
 		double rtol, int max_iterations, Amg& preconditioner, long long* launches);
 	int restart() const { return restart_; }
+	// Learned stage added to the AMG application in SolveFlexible (null: AMG only).
+	void set_learned(LearnedPreconditioner* learned) { learned_ = learned; }
+	LearnedPreconditioner* learned() const { return learned_; }
+	// Stores a training pair (w_j = A z_j) into `collector` on every eighth iteration (null: off).
+	void set_collector(LearnedPreconditioner* collector) { collector_ = collector; }
 	void set_profiler(Profiler* profiler) { profiler_ = profiler; }
 	std::size_t bytes() const;
 
@@ -72,6 +78,9 @@ private:
 	struct HostStatus { int stop, used, error, pad; double residual; double beta[2]; unsigned singular; };
 	HostStatus* host_ = nullptr;
 	Profiler* profiler_ = nullptr;
+	LearnedPreconditioner* learned_ = nullptr;
+	LearnedPreconditioner* collector_ = nullptr;
+	DeviceArray<double> pair_dinv_, pair_amg_, pair_aamg_;
 };
 
 } // namespace tfiga

@@ -229,18 +229,37 @@ GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 	if (amg_) {
 		const long long before = amg_->launches();
 		GmresResult result;
+		auto solve = [&]() {
+			if (mixed())
+				return gmres_.SolveFlexible<float>(mesh_.pattern_view(), values32_.get(), rhs_.get(), update_.get(),
+					rtol, max_iterations, *amg_, &launches_);
+			return gmres_.SolveFlexible<double>(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol,
+				max_iterations, *amg_, &launches_);
+		};
 		if (mixed()) {
 			if (!amg_->built()) amg_->Build(values32_.get());
 			amg_->Refresh(values32_.get(), solves_ % params_.amg_coarse_period == 0);
-			launches_ += amg_->launches()-before;
-			result = gmres_.SolveFlexible<float>(mesh_.pattern_view(), values32_.get(), rhs_.get(), update_.get(), rtol,
-				max_iterations, *amg_, &launches_);
 		} else {
 			if (!amg_->built()) amg_->Build(values_.get());
 			amg_->Refresh(values_.get(), solves_ % params_.amg_coarse_period == 0);
-			launches_ += amg_->launches()-before;
-			result = gmres_.SolveFlexible<double>(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol,
-				max_iterations, *amg_, &launches_);
+		}
+		launches_ += amg_->launches()-before;
+		result = solve();
+		if (!result.converged && gmres_.learned() != nullptr) {
+			// the learned stage is only an accelerator: the AMG-only solve is its fallback
+			LearnedPreconditioner* learned = gmres_.learned();
+			gmres_.set_learned(nullptr);
+			update_.Zero(stream_);
+			const int spent = result.iterations;
+			try {
+				result = solve();
+			} catch (...) {
+				gmres_.set_learned(learned);
+				throw;
+			}
+			gmres_.set_learned(learned);
+			result.iterations += spent;
+			++learned_fallbacks_;
 		}
 		return result;
 	}
@@ -320,6 +339,19 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 		Fail(-6, "Navier-Stokes GMRES failed (residual="+Precise(linear.residual)+", nonlinear_residual="
 			+Precise(norm)+", continuity_l2="+Precise(d.continuity_l2)+", net_boundary_flow="+Precise(d.net_flow)
 			+", relative_mass_imbalance="+Precise(d.imbalance)+")");
+	if (collect_pairs_) {
+		// training pair of this solved system, with the AMG data of this Jacobian
+		LaunchApplyBlockInverse((int)nodes(), amg_->fine_inverse(), rhs_.get(), pair_dinv_.get(), stream_);
+		if (mixed()) {
+			amg_->Apply(values32_.get(), rhs_.get(), pair_amg_.get(), zero_flag_.get());
+			LaunchSpmv<float>(mesh_.pattern_view(), values32_.get(), pair_amg_.get(), pair_aamg_.get(), stream_);
+		} else {
+			amg_->Apply(values_.get(), rhs_.get(), pair_amg_.get(), zero_flag_.get());
+			LaunchSpmv<double>(mesh_.pattern_view(), values_.get(), pair_amg_.get(), pair_aamg_.get(), stream_);
+		}
+		learned_->AddSolvedPair(pair_dinv_.get(), update_.get(), pair_amg_.get(), rhs_.get(), pair_aamg_.get(), norm);
+		launches_ += 6;
+	}
 	LaunchNorm(n4_, update_.get(), partial_.get(), scalars_.get()+kUpdateNorm, stream_);
 	LaunchAxpy(n4_, 1.0, update_.get(), state_.get(), stream_);
 	launches_ += 3;
@@ -383,6 +415,28 @@ void NsSolver::DownloadValues(double* out)
 		values_.Download(out, count, stream_);
 		CudaCheck(cudaStreamSynchronize(stream_), "download values");
 	}
+}
+
+void NsSolver::SetLearned(LearnedPreconditioner* learned, bool use, bool collect)
+{
+	if (learned != nullptr && !amg_) Fail(-7, "the learned preconditioner stage needs the AMG-preconditioned FGMRES");
+	learned_ = learned;
+	collect_pairs_ = learned != nullptr && collect;
+	gmres_.set_learned(learned != nullptr && use ? learned : nullptr);
+	gmres_.set_collector(collect_pairs_ ? learned : nullptr);
+	if (collect_pairs_ && pair_dinv_.size() == 0) {
+		pair_dinv_.Allocate(n4_);
+		pair_amg_.Allocate(n4_);
+		pair_aamg_.Allocate(n4_);
+		zero_flag_.Allocate(1);
+		zero_flag_.Zero(stream_);
+	}
+}
+
+void NsSolver::BindLearnedOperator(LearnedPreconditioner& learned)
+{
+	if (mixed()) learned.SetOperator(mesh_.pattern_view(), values32_.get(), nullptr);
+	else learned.SetOperator(mesh_.pattern_view(), nullptr, values_.get());
 }
 
 void NsSolver::Synchronize()

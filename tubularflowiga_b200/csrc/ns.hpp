@@ -57,6 +57,12 @@ public:
 	const tfiga_ns_params& params() const { return params_; }
 	Profiler& profiler() { return profiler_; }
 	const Amg* amg() const { return amg_.get(); }
+	// Learned preconditioner stage (not owned): used in the AMG-FGMRES solves when `use`, and a
+	// training pair stored after every Newton solve when `collect`.
+	void SetLearned(LearnedPreconditioner* learned, bool use, bool collect);
+	long long learned_fallbacks() const { return learned_fallbacks_; }
+	// Binds the current (Dirichlet-row) Jacobian as the operator of the learned stage's residual loss.
+	void BindLearnedOperator(LearnedPreconditioner& learned);
 
 private:
 	struct Diagnostics {
@@ -85,6 +91,11 @@ private:
 	Profiler profiler_;
 	std::unique_ptr<Amg> amg_;
 	double* pinned_ = nullptr;               // host mirror of scalars + label flows
+	LearnedPreconditioner* learned_ = nullptr;
+	bool collect_pairs_ = false;
+	long long learned_fallbacks_ = 0;        // solves redone without the learned stage
+	DeviceArray<double> pair_dinv_, pair_amg_, pair_aamg_;
+	DeviceArray<int> zero_flag_;
 	int32_t* pinned_status_ = nullptr;       // host mirror of the tensor-core kernel status
 };
 
