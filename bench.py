@@ -83,6 +83,12 @@ def workload(name):
         desc = ("pulsatile tube cross-section of the 51,200-element case, 100 layers (12,800 elements), "
                 "R 1.5 mm, L 7.5 mm, same inflow (profiling case)")
         return tube, desc, meshgen.fourier_waveform(0)
+    if name == "c5":
+        batch = meshgen.tube_batch(16, seed=0, min_elements=1000, max_elements=8000)
+        desc = ("batch of 16 independent straight tubes (seed 0): R U(0.5, 3) mm, L U(10, 40) R, "
+                "4x4-core O-grid, 1k-8k tricubic elements each (%d in all), Re U(50, 800), a seeded Fourier "
+                "inflow per tube; one disjoint-union mesh" % batch.mesh.elements)
+        return batch, desc, [meshgen.fourier_waveform(k) for k in range(16)]
     if name == "c1":
         tube = meshgen.straight_cylinder_1280()
         desc = ("straight cylinder 1,280 tricubic elements (4x4 core + 16-cell ring) x 40 layers, "
@@ -94,6 +100,20 @@ def workload(name):
                 "R 1.5 mm, L 30 mm, Fourier inflow mean 0.15 m/s + 4 harmonics U(0,0.05) seed 0")
         wave = meshgen.fourier_waveform(0)
     return tube, desc, wave
+
+
+def boundary(obj, wave):
+    """(vmask, pmask, velocity_at(t)) of a workload: one tube with one waveform, or a tube batch whose
+    tubes each scale their own peak velocity by their own seeded waveform (normalised to mean 1)."""
+    from tubularflowiga_b200 import api
+    if isinstance(wave, list):
+        def velocity_at(t):
+            factors = [inlet_factor(w, t) / w["mean"] for w in wave]
+            return api.batch_boundary_conditions(obj, factors)[2]
+        vmask, pmask, _ = api.batch_boundary_conditions(obj)
+        return vmask, pmask, velocity_at
+    vmask, pmask, profile = api.tube_boundary_conditions(obj, 1.0)
+    return vmask, pmask, lambda t: inlet_factor(wave, t) * profile
 
 
 def inlet_factor(wave, t):
@@ -225,8 +245,8 @@ def run_reference_arm(args, world, rank):
     tube, desc, wave = workload(args.workload)
     from tubularflowiga_b200 import api
     n = tube.mesh.nodes
-    vmask, pmask, vel = api.tube_boundary_conditions(tube, inlet_factor(wave, 0.0))
-    s0 = api.initial_state(vmask, vel)
+    vmask, pmask, velocity_at = boundary(tube, wave)
+    s0 = api.initial_state(vmask, velocity_at(0.0))
     # Newton and GMRES counts per step of this algorithm on this workload, as measured by the GPU arm.
     newton, lin = args.ref_newton, args.ref_linear
     budget = max(4.0, min(args.ref_budget, 120.0 / max(1, args.steps + 1)))
@@ -254,7 +274,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2-100"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2-100", "c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -295,15 +315,14 @@ def main():
                      amg_coarse_period=3)
     ns = api.NavierStokes(mesh, precision=api.MIXED if mixed else api.FP64, **solver_kw)
     dt = ns.params.dt
-    vmask, pmask, vel0 = api.tube_boundary_conditions(tube, 1.0)
-    profile = vel0.copy()
+    vmask, pmask, velocity_at = boundary(tube, wave)
 
     def bc(step):
-        return (inlet_factor(wave, (step + 1) * dt) * profile).ravel()
+        return velocity_at((step + 1) * dt).ravel()
 
-    ns.set_dirichlet(vmask, pmask, inlet_factor(wave, 0.0) * profile)
+    ns.set_dirichlet(vmask, pmask, velocity_at(0.0))
     ns.set_tractions({2: 0.0})
-    s0 = api.initial_state(vmask, inlet_factor(wave, 0.0) * profile)
+    s0 = api.initial_state(vmask, velocity_at(0.0))
     ns.set_state(s0, s0)
     stream = torch.cuda.ExternalStream(ns.stream())
     total = args.warmup + args.steps
@@ -371,7 +390,7 @@ def main():
     fp64_leg = None
     if mixed and not args.no_fp64_leg:
         ref = api.NavierStokes(mesh, precision=api.FP64, **solver_kw)
-        ref.set_dirichlet(vmask, pmask, inlet_factor(wave, 0.0) * profile)
+        ref.set_dirichlet(vmask, pmask, velocity_at(0.0))
         ref.set_tractions({2: 0.0})
         ref.set_state(s0, s0)
         rstream = torch.cuda.ExternalStream(ref.stream())

@@ -473,6 +473,19 @@ def tube_boundary_conditions(tube, inlet_scale: float):
     return vmask, np.zeros(len(labels), np.int32), vel
 
 
+def batch_boundary_conditions(batch, factors=None):
+    """Dirichlet masks/values of a meshgen.TubeBatch: every tube's wall no-slip and its inlet profile
+    scaled by its own peak velocity (times factors[k] when given, e.g. a per-tube waveform value)."""
+    labels = batch.labels
+    vmask = ((labels == 0) | (labels == 1)).astype(np.int32)
+    per_tube = batch.inlet_scale if factors is None else batch.inlet_scale * np.asarray(factors, np.float64)
+    scale = np.repeat(per_tube, np.diff(batch.node_offset))
+    vel = np.zeros((len(labels), 3))
+    inlet = labels == 1
+    vel[inlet] = scale[inlet, None] * batch.profile[inlet]
+    return vmask, np.zeros(len(labels), np.int32), vel
+
+
 def initial_state(vmask, velocity, pmask=None, pressure=None):
     """Initial state of a transient run (iga_cuda.cu:879-889): constrained values, zero elsewhere."""
     n = len(vmask)

@@ -297,3 +297,75 @@ def straight_cylinder_1280() -> Tube:
 def pulsatile_tube_51200() -> Tube:
     """51,200 elements: 8x8 core + two 32-cell ring layers (128 cells/layer) x 400 layers, R 1.5 mm."""
     return straight_tube(1.5e-3, 30e-3, core=8, ring=2, layers=400)
+
+
+@dataclass
+class TubeBatch:
+    """Many independent tubes as one mesh with disjoint node sets (a block-diagonal system).
+
+    Every tube keeps its own labels (wall 0, inlet 1, outlet 2) and peak-1 inlet profile; the
+    union is solved by one Newton/FGMRES loop whose kernels cover all tubes in each launch."""
+    mesh: FlatMesh
+    tubes: list
+    node_offset: np.ndarray        # [T+1] first node of each tube
+    element_offset: np.ndarray     # [T+1] first element of each tube
+    inlet_scale: np.ndarray        # [T] inlet peak velocity of each tube (m/s)
+    labels: np.ndarray             # [n] point labels of the union
+    profile: np.ndarray            # [n, 3] peak-1 inlet profiles of the union
+
+
+def combine_tubes(tubes, inlet_scale, gap: float = 1e-3) -> TubeBatch:
+    """Disjoint union of tubes; tube k is shifted along x so that no two tubes touch."""
+    node_offset = np.zeros(len(tubes) + 1, np.int64)
+    element_offset = np.zeros(len(tubes) + 1, np.int64)
+    eo, conn, xo, xc, xv, bez, lab = [np.zeros(1, np.int64)], [], [np.zeros(1, np.int64)], [], [], [], []
+    labels, profile = [], []
+    x = 0.0
+    for k, t in enumerate(tubes):
+        m = t.mesh
+        node_offset[k + 1] = node_offset[k] + m.nodes
+        element_offset[k + 1] = element_offset[k] + m.elements
+        eo.append(eo[-1][-1] + m.element_offsets[1:].astype(np.int64))
+        conn.append(m.connectivity.astype(np.int64) + node_offset[k])
+        xo.append(xo[-1][-1] + m.extraction_offsets[1:].astype(np.int64))
+        xc.append(m.extraction_columns)
+        xv.append(m.extraction_values)
+        b = m.bezier_points.reshape(-1, 3).copy()
+        b[:, 0] += x + t.radius
+        bez.append(b.ravel())
+        x += 2 * t.radius + gap
+        lab.append(m.boundary_labels)
+        labels.append(t.labels)
+        profile.append(t.profile)
+    mesh = FlatMesh(
+        nodes=int(node_offset[-1]),
+        element_offsets=np.concatenate(eo).astype(np.int32),
+        connectivity=np.concatenate(conn).astype(np.int32),
+        extraction_offsets=np.concatenate(xo).astype(np.int32),
+        extraction_columns=np.concatenate(xc).astype(np.uint8),
+        extraction_values=np.concatenate(xv).astype(np.float64),
+        bezier_points=np.concatenate(bez),
+        boundary_labels=np.concatenate(lab).astype(np.int32),
+    ).contiguous()
+    return TubeBatch(mesh=mesh, tubes=list(tubes), node_offset=node_offset, element_offset=element_offset,
+                     inlet_scale=np.asarray(inlet_scale, np.float64), labels=np.concatenate(labels),
+                     profile=np.concatenate(profile))
+
+
+def tube_batch(count: int, seed: int = 0, min_elements: int = 1000, max_elements: int = 8000,
+               density: float = 1060.0, viscosity: float = 3.5e-3) -> TubeBatch:
+    """Seeded batch of straight tubes of uneven sizes: radius U(0.5, 3) mm, length U(10, 40) radii,
+    4x4-core O-grid (32 cells per layer) with layers chosen so that each tube has an element count
+    drawn U(min_elements, max_elements), Reynolds number U(50, 800) giving the inlet peak velocity
+    Re mu / (rho 2R)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    tubes, scales = [], []
+    for _ in range(count):
+        radius = rng.uniform(0.5e-3, 3e-3)
+        length = rng.uniform(10.0, 40.0) * radius
+        elements = int(rng.uniform(min_elements, max_elements))
+        layers = max(4, elements // 32)
+        tubes.append(straight_tube(radius, length, core=4, ring=1, layers=layers))
+        reynolds = rng.uniform(50.0, 800.0)
+        scales.append(reynolds * viscosity / (density * 2.0 * radius))
+    return combine_tubes(tubes, scales)
