@@ -89,6 +89,12 @@ def workload(name):
                 "4x4-core O-grid, 1k-8k tricubic elements each (%d in all), Re U(50, 800), a seeded Fourier "
                 "inflow per tube; one disjoint-union mesh" % batch.mesh.elements)
         return batch, desc, [meshgen.fourier_waveform(k) for k in range(16)]
+    if name == "c3":
+        y = meshgen.y_bifurcation()
+        desc = ("Y-bifurcation %d tricubic elements: parent R 2.0 mm L 20 mm, daughters R 1.59 mm L 16 mm at "
+                "half-angle 35 deg, swept half-disc O-grids (6x12 core + 3-cell ring per half) x 308 + 247 "
+                "layers; RCR outlets R1 1e8, C 1e-10, R2 1e9 (SI); C2's Fourier inflow" % y.mesh.elements)
+        return y, desc, meshgen.fourier_waveform(0)
     if name == "c1":
         tube = meshgen.straight_cylinder_1280()
         desc = ("straight cylinder 1,280 tricubic elements (4x4 core + 16-cell ring) x 40 layers, "
@@ -100,6 +106,27 @@ def workload(name):
                 "R 1.5 mm, L 30 mm, Fourier inflow mean 0.15 m/s + 4 harmonics U(0,0.05) seed 0")
         wave = meshgen.fourier_waveform(0)
     return tube, desc, wave
+
+
+def step_dt(name):
+    """Time step of a workload: the 1,280-element cylinder 1e-3 s; the tube batch 1e-4 s, because its
+    smallest fast tubes (R 0.5 mm at Re 800, about 1.5 m/s) reach an axial CFL of 70 at 2e-3 s;
+    otherwise 2e-3 s."""
+    return {"c1": 1e-3, "c5": 1e-4}.get(name, DT)
+
+
+def outlet_models(name):
+    """RCR outlets of the Y-bifurcation (labels 2 and 3, zero initial pressure), else None."""
+    if name != "c3":
+        return None
+    from tubularflowiga_b200 import api
+    return [api.Outlet.rcr(label, 1e8, 1e-10, 1e9) for label in (2, 3)]
+
+
+# Outlet coupling of the bench: the relaxed fixed point with relaxation 1 (rigid walls and a Dirichlet
+# inflow fix the total outlet flow, so it reaches the reference's tolerance in two Newton loops; the
+# reference's 0.5 would need about 20 here, more than its cap of 12).
+OUTLET_RELAXATION = 1.0
 
 
 def boundary(obj, wave):
@@ -274,7 +301,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2-100", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2-100", "c3", "c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -308,7 +335,7 @@ def main():
     mixed = args.precision == "mixed"
     if mixed and not amg:
         raise SystemExit("--precision mixed needs --preconditioner amg")
-    solver_kw = dict(density=RHO, viscosity=MU, dt=1e-3 if args.workload == "c1" else DT,
+    solver_kw = dict(density=RHO, viscosity=MU, dt=step_dt(args.workload),
                      nonlinear_rtol=1e-8, nonlinear_atol=1e-300, mass_rtol=1e-3,
                      gmres_restart=200, gmres_max_iterations=5000, gmres_rtol=1e-8,
                      preconditioner=api.AMG if amg else api.BLOCK_JACOBI,
@@ -321,9 +348,12 @@ def main():
         return velocity_at((step + 1) * dt).ravel()
 
     ns.set_dirichlet(vmask, pmask, velocity_at(0.0))
-    ns.set_tractions({2: 0.0})
+    models = outlet_models(args.workload)
+    fixed_tractions = {} if models else {2: 0.0}
+    ns.set_tractions(fixed_tractions)
     s0 = api.initial_state(vmask, velocity_at(0.0))
     ns.set_state(s0, s0)
+    outlets = [api.Outlet(**m.as_dict()) for m in models] if models else None
     stream = torch.cuda.ExternalStream(ns.stream())
     total = args.warmup + args.steps
     # every step's Dirichlet values resident in HBM before timing (value leg)
@@ -339,7 +369,7 @@ def main():
         else:
             api.check(api.lib().tfiga_ns_set_dirichlet_values(ns._h, api.C.c_void_p(bc_dev[k].data_ptr()), None))
         ns.commit_step()
-        r = ns.step()
+        r = ns.step_outlets(outlets, OUTLET_RELAXATION) if outlets else ns.step()
         reports.append(r)
         if host:
             api.check(api.lib().tfiga_ns_get_state(ns._h, api.C.c_void_p(out_host.data_ptr())))
@@ -353,6 +383,7 @@ def main():
     if dist:
         dist.barrier()
     timed_start = ns.get_state()
+    timed_outlets = [o.as_dict() for o in outlets] if outlets else None
     ns.set_profiling(True)
     ns.profile(reset=True)
     launches0 = ns.launches()
@@ -376,6 +407,10 @@ def main():
         dist.barrier()
     # same steps from the same state as the timed leg, inputs from pinned host memory
     ns.set_state(timed_start, timed_start)
+    if outlets:
+        for o, d in zip(outlets, timed_outlets):
+            for k, v in d.items():
+                setattr(o, k, v)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
@@ -391,8 +426,9 @@ def main():
     if mixed and not args.no_fp64_leg:
         ref = api.NavierStokes(mesh, precision=api.FP64, **solver_kw)
         ref.set_dirichlet(vmask, pmask, velocity_at(0.0))
-        ref.set_tractions({2: 0.0})
+        ref.set_tractions(fixed_tractions)
         ref.set_state(s0, s0)
+        ref_outlets = [api.Outlet(**m.as_dict()) for m in models] if models else None
         rstream = torch.cuda.ExternalStream(ref.stream())
         errors, fp64_ms, fp64_steps = [], 0.0, 0
         for k in range(args.warmup):
@@ -401,7 +437,10 @@ def main():
             a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
             a0.record(rstream)
-            ref.step()
+            if ref_outlets:
+                ref.step_outlets(ref_outlets, OUTLET_RELAXATION)
+            else:
+                ref.step()
             a1.record(rstream)
             torch.cuda.synchronize()
             if k > 0:
@@ -507,11 +546,17 @@ def main():
                    "solver": (("mixed: tcgen05 BF16 tangent (FP32 accumulate), FP32 Jacobian, FP64 residual and "
                                "refinement; " if mixed else "plain FP64: ") +
                               "exact-tangent Newton to rel.res 1e-8, " +
+                              ("RCR outlets coupled by the relaxed fixed point (relaxation %g, tolerance "
+                               "1e-8 + 1e-6 |P|), " % OUTLET_RELAXATION if models else "") +
                               ("point-block AMG V(1,1)-preconditioned FGMRES(200) rtol 1e-8" if amg else
                                "block-Jacobi GMRES(200) rtol 1e-8")),
                    "l2": "inputs larger than L2 (matrix %.2f GB)" % (mesh.blocks * 128 / 1e9),
                    "parallelism": "replicas only" if world > 1 else "single GPU"},
         "newton_per_step": float(newton), "linear_iterations_per_newton": float(linear),
+        "outlets": ([{k: o.as_dict()[k] for k in ("label", "flow", "pressure", "capacitor_pressure")}
+                     for o in outlets] if outlets else None),
+        "outlet_iterations_per_step": (float(np.mean([r["outlet_iterations"] for r in timed_reports]))
+                                       if outlets else None),
         "roofline": roof, "kernels": kernels,
         "fp64_gpu": fp64_leg,
         "spmv_gbs": kernels.get(spmv_name, {}).get("achieved"),

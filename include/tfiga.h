@@ -152,6 +152,23 @@ typedef struct tfiga_step_report {
 	double linear_ms;
 } tfiga_step_report;
 
+/* Outlet model of one labelled outlet (OutletModelState, include/OutletModel.hpp:15-26;
+ * EvaluateOutletModel :70-90): resistance P = Pref + R Q; RC / RCR capacitor
+ * Pc = (C Pc_prev / dt + Q + Pref / R_d) / (C / dt + 1 / R_d), P = Pc (+ R_p Q for RCR). */
+enum { TFIGA_OUTLET_RESISTANCE = 0, TFIGA_OUTLET_RC = 1, TFIGA_OUTLET_RCR = 2 };
+typedef struct tfiga_outlet {
+	int32_t label;
+	int32_t kind;                 /* TFIGA_OUTLET_* */
+	double resistance;            /* resistance and RC models */
+	double proximal_resistance;   /* RCR R_p */
+	double distal_resistance;     /* RCR R_d */
+	double capacitance;
+	double reference_pressure;
+	double capacitor_pressure;    /* in: committed value of the previous step; out: this step's */
+	double flow;                  /* out: outward flow of the accepted iterate */
+	double pressure;              /* in: first traction; out: accepted pressure */
+} tfiga_outlet;
+
 /* ---- errors ------------------------------------------------------------ */
 /* Copies the calling thread's last error message; returns its full length. */
 size_t tfiga_last_error(char* buffer, size_t capacity);
@@ -211,6 +228,20 @@ int tfiga_ns_solve_linear(tfiga_ns* ns, double rtol, int32_t max_iterations, dou
 int tfiga_ns_newton_iteration(tfiga_ns* ns, double initial_residual, tfiga_newton_report* report);
 /* One physical step: the Newton loop to convergence (iga_cuda.cu:952-1054). */
 int tfiga_ns_step(tfiga_ns* ns, tfiga_step_report* report);
+/* One physical step coupled to outlet models by the relaxed fixed point of
+ * iga_cuda.cu:927-1086 (EvaluateOutletCoupling / OutletCouplingTolerance /
+ * RelaxOutletCoupling / CommitOutletCoupling, OutletModel.hpp:92-150): the Newton
+ * loop runs with each outlet's pressure as its traction (other labels keep the
+ * tractions of tfiga_ns_set_tractions), the outward flows are evaluated, and the
+ * iteration stops when max |P_eval - P| <= 1e-8 + 1e-6 max(1, |P_eval|); otherwise
+ * P <- (1 - relaxation) P + relaxation P_eval.  The reference uses relaxation 0.5
+ * and 12 iterations; with rigid walls and a Dirichlet inflow the total outlet flow
+ * does not depend on the outlet pressures, so relaxation 1 reaches the same fixed
+ * point in two iterations.  report sums the Newton and linear counts over all
+ * outlet iterations; *outlet_iterations (may be NULL) is the number of Newton
+ * loops.  TFIGA_E_NOT_CONVERGED after max_iterations. */
+int tfiga_ns_step_outlets(tfiga_ns* ns, tfiga_outlet* outlets, int32_t count, double relaxation,
+	int32_t max_iterations, tfiga_step_report* report, int32_t* outlet_iterations);
 /* AMG hierarchy sizes (levels = 0 before the hierarchy is built). */
 int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info);
 /* Outward flow through each labelled boundary (IntegrateBoundaryFlow,

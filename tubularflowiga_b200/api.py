@@ -79,6 +79,34 @@ class StepReport(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+OUTLET_RESISTANCE, OUTLET_RC, OUTLET_RCR = 0, 1, 2
+_OUTLET_KINDS = {"resistance": OUTLET_RESISTANCE, "windkessel_rc": OUTLET_RC, "windkessel_rcr": OUTLET_RCR}
+
+
+class Outlet(C.Structure):
+    """tfiga_outlet: one labelled outlet model (OutletModelState, include/OutletModel.hpp:15-26)."""
+    _fields_ = [("label", C.c_int32), ("kind", C.c_int32), ("resistance", C.c_double),
+                ("proximal_resistance", C.c_double), ("distal_resistance", C.c_double),
+                ("capacitance", C.c_double), ("reference_pressure", C.c_double),
+                ("capacitor_pressure", C.c_double), ("flow", C.c_double), ("pressure", C.c_double)]
+
+    @classmethod
+    def rcr(cls, label, proximal, capacitance, distal, reference_pressure=0.0, initial_pressure=0.0):
+        """RCR outlet starting at capacitor and outlet pressure = initial_pressure (InitializeOutletModels,
+        OutletModel.hpp:41-68)."""
+        return cls(label=label, kind=OUTLET_RCR, proximal_resistance=proximal, capacitance=capacitance,
+                   distal_resistance=distal, reference_pressure=reference_pressure,
+                   capacitor_pressure=initial_pressure, pressure=initial_pressure)
+
+    @classmethod
+    def resistance_model(cls, label, resistance, reference_pressure=0.0):
+        return cls(label=label, kind=OUTLET_RESISTANCE, resistance=resistance,
+                   reference_pressure=reference_pressure, pressure=reference_pressure)
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 # Every exported symbol of include/tfiga.h with its signature.
 SIGNATURES = {
     "tfiga_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
@@ -103,6 +131,8 @@ SIGNATURES = {
                                         C.POINTER(C.c_double)]),
     "tfiga_ns_newton_iteration": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(NewtonReport)]),
     "tfiga_ns_step": (C.c_int, [C.c_void_p, C.POINTER(StepReport)]),
+    "tfiga_ns_step_outlets": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_double, C.c_int32,
+                                        C.POINTER(StepReport), C.POINTER(C.c_int32)]),
     "tfiga_ns_amg_info": (C.c_int, [C.c_void_p, C.POINTER(AmgInfo)]),
     "tfiga_ns_boundary_flows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "tfiga_ns_spmv_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -288,6 +318,22 @@ class NavierStokes:
         r = StepReport()
         check(lib().tfiga_ns_step(self._h, C.byref(r)))
         return r.as_dict()
+
+    def step_outlets(self, outlets, relaxation=0.5, max_iterations=12):
+        """One physical step coupled to outlet models (a list or ctypes array of Outlet, updated in place:
+        accepted flow, pressure and capacitor pressure).  Returns the step report with the number of
+        Newton loops as ``outlet_iterations``."""
+        arr = outlets if isinstance(outlets, C.Array) else (Outlet * len(outlets))(*outlets)
+        r = StepReport()
+        it = C.c_int32()
+        check(lib().tfiga_ns_step_outlets(self._h, C.cast(arr, C.c_void_p) if len(arr) else None, len(arr),
+                                          relaxation, max_iterations, C.byref(r), C.byref(it)))
+        if not isinstance(outlets, C.Array):
+            for k in range(len(outlets)):
+                outlets[k] = arr[k]
+        d = r.as_dict()
+        d["outlet_iterations"] = it.value
+        return d
 
     def boundary_flows(self, labels):
         lab = np.ascontiguousarray(labels, np.int32)

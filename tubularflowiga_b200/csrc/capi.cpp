@@ -319,6 +319,17 @@ int tfiga_ns_step(tfiga_ns* ns, tfiga_step_report* report)
 	});
 }
 
+int tfiga_ns_step_outlets(tfiga_ns* ns, tfiga_outlet* outlets, int32_t count, double relaxation,
+	int32_t max_iterations, tfiga_step_report* report, int32_t* outlet_iterations)
+{
+	return Guard([&] {
+		Require(ns && report && count >= 0 && (count == 0 || outlets), "null argument");
+		int iterations = 0;
+		*report = ns->solver->StepOutlets(outlets, count, relaxation, max_iterations, &iterations);
+		if (outlet_iterations) *outlet_iterations = iterations;
+	});
+}
+
 int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info)
 {
 	return Guard([&] {

@@ -1,6 +1,10 @@
 // Newton iteration and physical step on the device (see ns.hpp).
 #include "ns.hpp"
 
+#include "case_input.hpp"
+
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <sstream>
@@ -134,6 +138,12 @@ void NsSolver::SetTractions(const int32_t* labels, const double* pressures, int 
 		if (!std::isfinite(pressures[i])) Fail(-1, "pressure traction must be finite");
 		traction[labels[i]] = pressures[i];
 	}
+	ApplyTractions(traction);
+	tractions_ = traction;
+}
+
+void NsSolver::ApplyTractions(const std::map<int32_t, double>& traction)
+{
 	for (const auto& t : traction) {
 		bool found = false;
 		for (const auto& f : mesh_.faces()) if (f.label == t.first) { found = true; break; }
@@ -383,6 +393,79 @@ tfiga_step_report NsSolver::Step()
 	Fail(-6, "Navier-Stokes nonlinear solve reached MAX_NEWTON (nonlinear_residual="+Precise(last.residual_l2)
 		+", continuity_l2="+Precise(last.continuity_l2)+", net_boundary_flow="+Precise(last.net_boundary_flow)
 		+", relative_mass_imbalance="+Precise(last.relative_mass_imbalance)+")");
+}
+
+tfiga_step_report NsSolver::StepOutlets(tfiga_outlet* outlets, int count, double relaxation, int max_iterations,
+	int* iterations)
+{
+	if (!(relaxation > 0.0 && relaxation <= 1.0)) Fail(-1, "invalid outlet coupling relaxation");
+	if (max_iterations < 1) Fail(-1, "outlet coupling needs at least one iteration");
+	std::vector<OutletModel> models(count);
+	std::vector<int32_t> labels(count);
+	std::vector<double> previous_capacitor(count), flows(count);
+	for (int i = 0; i < count; ++i) {
+		const tfiga_outlet& o = outlets[i];
+		OutletModel& m = models[i];
+		m.label = o.label;
+		if (o.kind == TFIGA_OUTLET_RESISTANCE) m.kind = "resistance";
+		else if (o.kind == TFIGA_OUTLET_RC) m.kind = "windkessel_rc";
+		else if (o.kind == TFIGA_OUTLET_RCR) m.kind = "windkessel_rcr";
+		else Fail(-1, "unknown outlet model kind "+std::to_string(o.kind));
+		m.resistance = o.resistance;
+		m.proximal = o.proximal_resistance;
+		m.distal = o.distal_resistance;
+		m.capacitance = o.capacitance;
+		m.reference_pressure = o.reference_pressure;
+		m.capacitor_pressure = o.capacitor_pressure;
+		m.flow = o.flow;
+		m.pressure = o.pressure;
+		if (!std::isfinite(m.pressure)) Fail(-1, "outlet pressure must be finite");
+		labels[i] = o.label;
+		previous_capacitor[i] = o.capacitor_pressure;
+	}
+	tfiga_step_report total{};
+	for (int coupling = 0; coupling < max_iterations; ++coupling) {
+		auto traction = tractions_;
+		for (const auto& m : models) traction[m.label] = m.pressure;
+		ApplyTractions(traction);
+		const tfiga_step_report r = Step();
+		if (coupling == 0) total.initial_residual_l2 = r.initial_residual_l2;
+		total.converged = r.converged;
+		total.newton_iterations += r.newton_iterations;
+		total.linear_iterations += r.linear_iterations;
+		total.residual_l2 = r.residual_l2;
+		total.relative_mass_imbalance = r.relative_mass_imbalance;
+		total.assembly_ms += r.assembly_ms;
+		total.linear_ms += r.linear_ms;
+		if (count == 0) { if (iterations) *iterations = 1; return total; }
+		BoundaryFlows(labels.data(), count, flows.data());
+		double change = 0.0, scale = 1.0;
+		std::vector<std::array<double, 2>> evaluated(count);
+		for (int i = 0; i < count; ++i) {
+			OutletModel m = models[i];
+			m.capacitor_pressure = previous_capacitor[i];
+			evaluated[i] = EvaluateOutletModel(m, flows[i], params_.dt);
+			change = std::max(change, std::fabs(evaluated[i][0]-models[i].pressure));
+			scale = std::max(scale, std::fabs(evaluated[i][0]));
+		}
+		if (change <= 1e-8+1e-6*scale) {
+			for (int i = 0; i < count; ++i) {
+				outlets[i].flow = flows[i];
+				outlets[i].pressure = evaluated[i][0];
+				outlets[i].capacitor_pressure = evaluated[i][1];
+			}
+			if (iterations) *iterations = coupling+1;
+			return total;
+		}
+		for (int i = 0; i < count; ++i) {
+			models[i].flow = flows[i];
+			models[i].pressure = (1.0-relaxation)*models[i].pressure+relaxation*evaluated[i][0];
+			outlets[i].flow = flows[i];
+			outlets[i].pressure = models[i].pressure;
+		}
+	}
+	if (iterations) *iterations = max_iterations;
+	Fail(-6, "outlet fixed-point iteration did not converge");
 }
 
 void NsSolver::BoundaryFlows(const int32_t* labels, int count, double* flows)

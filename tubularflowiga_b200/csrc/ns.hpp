@@ -34,6 +34,9 @@ public:
 	GmresResult SolveLinear(double rtol, int max_iterations);
 	tfiga_newton_report NewtonIteration(double initial_residual);
 	tfiga_step_report Step();
+	// Step coupled to outlet models (relaxed fixed point of iga_cuda.cu:927-1086); *iterations = Newton loops.
+	tfiga_step_report StepOutlets(tfiga_outlet* outlets, int count, double relaxation, int max_iterations,
+		int* iterations);
 	void BoundaryFlows(const int32_t* labels, int count, double* flows);
 	void Synchronize();
 
@@ -68,6 +71,7 @@ private:
 	struct Diagnostics {
 		double continuity_l2, continuity_sum, net_flow, absolute_flow, imbalance;
 	};
+	void ApplyTractions(const std::map<int32_t, double>& traction);
 	void LaunchDiagnostics();     // continuity sums of rhs + per-label flows of state
 	Diagnostics ReadDiagnostics();
 
@@ -77,6 +81,7 @@ private:
 	cudaEvent_t events_[4] = {};
 	long long launches_ = 0;
 	long long solves_ = 0;                   // linear solves so far (coarse refresh period)
+	std::map<int32_t, double> tractions_;    // label -> pressure set by SetTractions
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
 	DeviceArray<float> values32_;

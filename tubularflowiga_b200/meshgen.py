@@ -116,6 +116,101 @@ def ogrid_cross_section(radius: float, core: int, ring: int, core_half: float = 
     return pos, patches, rim
 
 
+@dataclass
+class SweptBlock:
+    """A cross-section of 2D patches swept through ``planes`` vertex planes.
+
+    ``patches[p]`` is a [nu+1, nv+1] grid of plane-local vertex ids (u radial for ring patches, rim at
+    u = nu); ``ids[k, v]`` is the global vertex id of plane-local vertex v in plane k, so blocks that
+    share a plane share its vertices (a C0 interface). ``wall[p]`` marks ring patches whose rim faces
+    are no-slip walls (face label 0); ``bottom`` / ``top`` label the faces of the first / last layer."""
+    patches: list
+    ids: np.ndarray
+    wall: list
+    bottom: int | None = None
+    top: int | None = None
+
+
+def swept_mesh(points, blocks):
+    """FlatMesh + VTK hex cells of swept blocks: one element per cell, natural-end cubic B-splines per
+    patch and per block axis.  Elements are enumerated block by block, then layer, patch, v, u."""
+    ext_cache: dict = {}
+
+    def ext(nc_, c_):
+        key = (nc_, c_)
+        if key not in ext_cache:
+            ext_cache[key] = natural_extraction_1d(nc_, c_)
+        return ext_cache[key]
+
+    conn_list, rows_list, labels_list, cells, groups = [], [], [], [], {}
+    for blk in blocks:
+        layers = blk.ids.shape[0] - 1
+        for layer in range(layers):
+            wv, wc = ext(layers, layer)
+            plane_ids = blk.ids[wv]                                   # [nw_l, n_local]
+            for p, grid in enumerate(blk.patches):
+                nu, nv = grid.shape[0] - 1, grid.shape[1] - 1
+                for jv in range(nv):
+                    vv, vc = ext(nv, jv)
+                    for iu in range(nu):
+                        uv, uc = ext(nu, iu)
+                        # local basis ordering: w outer, v, u inner
+                        ids2 = grid[np.ix_(uv, vv)]                   # [nu_l, nv_l]
+                        conn = plane_ids[:, ids2.T].reshape(-1)
+                        key = (layers, layer, nu, iu, nv, jv)
+                        if key not in groups:
+                            # row (w,v,u) x Bernstein index c*16 + b*4 + a (u fastest)
+                            rows = np.einsum("wc,vb,ua->wvucba", wc, vc, uc)
+                            groups[key] = rows.reshape(len(wv) * len(vv) * len(uv), 64)
+                        conn_list.append(conn.astype(np.int32))
+                        rows_list.append(key)
+                        lab = [-1] * 6
+                        if layer == 0 and blk.bottom is not None:
+                            lab[0] = blk.bottom
+                        if layer == layers - 1 and blk.top is not None:
+                            lab[5] = blk.top
+                        if p > 0 and blk.wall[p] and iu == nu - 1:
+                            lab[2] = 0
+                        labels_list.append(lab)
+                        c = [grid[iu, jv], grid[iu + 1, jv], grid[iu + 1, jv + 1], grid[iu, jv + 1]]
+                        cells.append([blk.ids[layer, v] for v in c] + [blk.ids[layer + 1, v] for v in c])
+    E = len(conn_list)
+    nen = np.array([len(c) for c in conn_list], np.int64)
+    element_offsets = np.zeros(E + 1, np.int64)
+    element_offsets[1:] = np.cumsum(nen)
+    connectivity = np.concatenate(conn_list)
+    # Sparse extraction rows and Bezier points, grouped by extraction type.
+    sparse = {}
+    for key, rows in groups.items():
+        cols = [np.nonzero(np.abs(r) > 0.0)[0].astype(np.uint8) for r in rows]
+        sparse[key] = (np.concatenate(cols), np.concatenate([rows[i][cols[i]] for i in range(len(rows))]),
+                       np.array([len(c) for c in cols], np.int64))
+    xc = np.concatenate([sparse[k][0] for k in rows_list])
+    xv = np.concatenate([sparse[k][1] for k in rows_list])
+    xo = np.zeros(int(element_offsets[-1]) + 1, np.int64)
+    xo[1:] = np.cumsum(np.concatenate([sparse[k][2] for k in rows_list]))
+    bezier = np.zeros((E, 64, 3))
+    by_key: dict = {}
+    for e, key in enumerate(rows_list):
+        by_key.setdefault(key, []).append(e)
+    for key, es in by_key.items():
+        es = np.array(es)
+        Cm = groups[key]                                          # [nen, 64]
+        conn = np.stack([conn_list[e] for e in es])               # [g, nen]
+        bezier[es] = np.einsum("ap,gad->gpd", Cm, points[conn])
+    mesh = FlatMesh(
+        nodes=len(points),
+        element_offsets=element_offsets.astype(np.int32),
+        connectivity=connectivity.astype(np.int32),
+        extraction_offsets=xo.astype(np.int32),
+        extraction_columns=xc.astype(np.uint8),
+        extraction_values=xv.astype(np.float64),
+        bezier_points=bezier.ravel(),
+        boundary_labels=np.array(labels_list, np.int32).ravel(),
+    ).contiguous()
+    return mesh, np.array(cells, np.int64)
+
+
 def straight_tube(radius: float, length: float, core: int, ring: int, layers: int,
                   core_half: float = 0.5, bulge: float = 0.2) -> Tube:
     """Straight tube along +z: inlet face label 1 at z=0, outlet label 2 at z=length, wall label 0."""
@@ -141,85 +236,236 @@ def straight_tube(radius: float, length: float, core: int, ring: int, layers: in
     profile = np.zeros((n, 3))
     profile[:, 2] = np.maximum(0.0, 1.0 - r2)
 
-    ext_cache: dict = {}
-
-    def ext(nc_, c_):
-        key = (nc_, c_)
-        if key not in ext_cache:
-            ext_cache[key] = natural_extraction_1d(nc_, c_)
-        return ext_cache[key]
-
-    # Element enumeration: axial layer outermost, then patch, then v, then u.
-    conn_list, rows_list, labels_list, cells, groups = [], [], [], [], {}
-    for layer in range(layers):
-        wv, wc = ext(layers, layer)
-        for p, grid in enumerate(patches):
-            nu, nv = grid.shape[0] - 1, grid.shape[1] - 1
-            for jv in range(nv):
-                vv, vc = ext(nv, jv)
-                for iu in range(nu):
-                    uv, uc = ext(nu, iu)
-                    # local basis ordering: w outer, v, u inner
-                    ids2 = grid[np.ix_(uv, vv)]                       # [nu_l, nv_l]
-                    ids = (wv[:, None, None] * n2d + ids2.T[None, :, :]).reshape(-1)
-                    key = (layers, layer, nu, iu, nv, jv)
-                    if key not in groups:
-                        # row (w,v,u) x Bernstein index c*16 + b*4 + a (u fastest)
-                        rows = np.einsum("wc,vb,ua->wvucba", wc, vc, uc)
-                        groups[key] = rows.reshape(len(wv) * len(vv) * len(uv), 64)
-                    conn_list.append(ids.astype(np.int32))
-                    rows_list.append(key)
-                    lab = [-1] * 6
-                    if layer == 0:
-                        lab[0] = 1
-                    if layer == layers - 1:
-                        lab[5] = 2
-                    if p > 0 and iu == nu - 1:
-                        lab[2] = 0
-                    labels_list.append(lab)
-                    c = [grid[iu, jv], grid[iu + 1, jv], grid[iu + 1, jv + 1], grid[iu, jv + 1]]
-                    cells.append([layer * n2d + v for v in c] + [(layer + 1) * n2d + v for v in c])
-    E = len(conn_list)
-    nen = np.array([len(c) for c in conn_list], np.int64)
-    element_offsets = np.zeros(E + 1, np.int64)
-    element_offsets[1:] = np.cumsum(nen)
-    connectivity = np.concatenate(conn_list)
-    # Sparse extraction rows and Bezier points, grouped by extraction type.
-    xo = [0]
-    xc_parts, xv_parts = [], []
-    sparse_cache = {}
-    for key in groups:
-        rows = groups[key]
-        cols = [np.nonzero(np.abs(r) > 0.0)[0].astype(np.uint8) for r in rows]
-        vals = [rows[i][cols[i]] for i in range(len(rows))]
-        sparse_cache[key] = (cols, vals)
-    bezier = np.zeros((E, 64, 3))
-    for e in range(E):
-        cols, vals = sparse_cache[rows_list[e]]
-        for c, v in zip(cols, vals):
-            xc_parts.append(c); xv_parts.append(v)
-            xo.append(xo[-1] + len(c))
-    by_key: dict = {}
-    for e, key in enumerate(rows_list):
-        by_key.setdefault(key, []).append(e)
-    for key, es in by_key.items():
-        es = np.array(es)
-        Cm = groups[key]                                          # [nen, 64]
-        conn = np.stack([conn_list[e] for e in es])               # [g, nen]
-        bezier[es] = np.einsum("ap,gad->gpd", Cm, points[conn])
-    mesh = FlatMesh(
-        nodes=n,
-        element_offsets=element_offsets.astype(np.int32),
-        connectivity=connectivity.astype(np.int32),
-        extraction_offsets=np.array(xo, np.int32),
-        extraction_columns=np.concatenate(xc_parts).astype(np.uint8),
-        extraction_values=np.concatenate(xv_parts).astype(np.float64),
-        bezier_points=bezier.ravel(),
-        boundary_labels=np.array(labels_list, np.int32).ravel(),
-    ).contiguous()
-    return Tube(mesh=mesh, points=points, labels=labels, cells=np.array(cells, np.int64), profile=profile,
+    ids = np.arange(n, dtype=np.int64).reshape(planes, n2d)
+    block = SweptBlock(patches=patches, ids=ids, wall=[False] + [True] * 4, bottom=1, top=2)
+    mesh, cells = swept_mesh(points, [block])
+    return Tube(mesh=mesh, points=points, labels=labels, cells=cells, profile=profile,
                 radius=radius, length=length, planes=planes, per_plane=n2d)
 
+
+
+def quad_ogrid(sides, center, ax: int, ay: int, ring: int, core_scale: float = 0.5, bulge: float = 0.2):
+    """2D O-grid of a region bounded by four curves: an ``ax x ay`` core and four ring patches.
+
+    ``sides[k](t)`` (t in [0, 1], arrays of t accepted) traces boundary side k counter-clockwise:
+    k = 0 and 2 carry ``ay`` cells, k = 1 and 3 carry ``ax``; side k ends where side k+1 starts.
+    The core corners are the boundary corners pulled toward ``center`` by ``core_scale``; each core
+    side is the chord between its corners bent by ``bulge`` toward the pulled boundary side, and the
+    core interior is their transfinite (Coons) interpolation.  Ring vertex r of a radial line lies
+    at r / ring between the core side and the boundary.
+    Returns (positions [n2d, 2], patches, rim) with ``rim[k]`` the plane-local ids of side k's
+    boundary vertices in side order."""
+    center = np.asarray(center, np.float64)
+    counts = [ay, ax, ay, ax]
+    corners = [np.asarray(sides[k](0.0), np.float64) for k in range(4)]
+
+    def core_side(k, t):
+        t = np.atleast_1d(np.asarray(t, np.float64))
+        c0 = center + core_scale * (corners[k] - center)
+        c1 = center + core_scale * (corners[(k + 1) % 4] - center)
+        chord = (1.0 - t)[:, None] * c0 + t[:, None] * c1
+        pulled = center + core_scale * (np.asarray(sides[k](t), np.float64).reshape(-1, 2) - center)
+        return (1.0 - bulge) * chord + bulge * pulled
+
+    n_core = (ax + 1) * (ay + 1)
+    per_ring = 2 * (ax + ay)
+    pos = np.zeros((n_core + ring * per_ring, 2))
+    # core: Coons patch; i along sides 3 (bottom, i increasing) and 1 (top, i decreasing), j along 0 / 2
+    s_ = np.linspace(0.0, 1.0, ax + 1)
+    t_ = np.linspace(0.0, 1.0, ay + 1)
+    bottom = core_side(3, s_)                 # (i, 0)
+    right = core_side(0, t_)                  # (ax, j)
+    top = core_side(1, 1.0 - s_)              # (i, ay): side 1 runs from i = ax to i = 0
+    left = core_side(2, 1.0 - t_)             # (0, j): side 2 runs from j = ay to j = 0
+    P00, P10, P11, P01 = bottom[0], bottom[-1], top[-1], top[0]
+    for j in range(ay + 1):
+        for i in range(ax + 1):
+            u, v = s_[i], t_[j]
+            pos[i + (ax + 1) * j] = ((1 - v) * bottom[i] + v * top[i] + (1 - u) * left[j] + u * right[j]
+                                     - ((1 - u) * (1 - v) * P00 + u * (1 - v) * P10 + u * v * P11
+                                        + (1 - u) * v * P01))
+
+    def core_boundary(k, m):
+        if k == 0:
+            i, j = ax, m
+        elif k == 1:
+            i, j = ax - m, ay
+        elif k == 2:
+            i, j = 0, ay - m
+        else:
+            i, j = m, 0
+        return i + (ax + 1) * j
+
+    patches = [np.array([[i + (ax + 1) * j for j in range(ay + 1)] for i in range(ax + 1)], np.int64)]
+    offsets = [0, ay, ay + ax, 2 * ay + ax]
+    rim = []
+    for k in range(4):
+        nk = counts[k]
+        grid = np.zeros((ring + 1, nk + 1), np.int64)       # [radial u][tangential v]
+        outer = np.asarray(sides[k](np.linspace(0.0, 1.0, nk + 1)), np.float64).reshape(-1, 2)
+        for m in range(nk + 1):
+            inner = core_boundary(k, m)
+            grid[0, m] = inner
+            for r in range(1, ring + 1):
+                vid = n_core + (r - 1) * per_ring + (offsets[k] + m) % per_ring
+                grid[r, m] = vid
+                rho = r / ring
+                pos[vid] = (1.0 - rho) * pos[inner] + rho * outer[m]
+        patches.append(grid)
+        rim.append(grid[ring].copy())
+    return pos, patches, rim
+
+
+def _arc(cx, cy, radius, a0, a1):
+    return lambda t: np.stack([cx + radius * np.cos(a0 + (a1 - a0) * np.asarray(t, np.float64)),
+                               cy + radius * np.sin(a0 + (a1 - a0) * np.asarray(t, np.float64))], axis=-1)
+
+
+def _segment(p0, p1):
+    p0, p1 = np.asarray(p0, np.float64), np.asarray(p1, np.float64)
+    return lambda t: p0 + np.asarray(t, np.float64)[..., None] * (p1 - p0)
+
+
+def half_disc_section(radius: float, ax: int, ay: int, ring: int):
+    """O-grid of the half disc {s >= 0, s^2 + y^2 <= R^2} in local (s, y): side 0 the arc from -45 to
+    45 degrees, sides 1 / 3 the arcs up to +-90 degrees, side 2 the straight septum s = 0 (y from R to
+    -R).  With ax = ay / 2 every arc cell spans the same angle."""
+    q = 0.25 * math.pi
+    sides = [_arc(0.0, 0.0, radius, -q, q), _arc(0.0, 0.0, radius, q, 2 * q),
+             _segment((0.0, radius), (0.0, -radius)), _arc(0.0, 0.0, radius, -2 * q, -q)]
+    return quad_ogrid(sides, (4.0 * radius / (3.0 * math.pi), 0.0), ax, ay, ring)
+
+
+def disc_section_like_half(radius: float, ax: int, ay: int, ring: int):
+    """O-grid of the disc of radius r centred at (r, 0) (touching s = 0 at the origin) with the
+    topology of ``half_disc_section``: the boundary split in proportion to the cell counts."""
+    per = 2.0 * math.pi / (2 * (ax + ay))
+    a0 = -0.5 * ay * per
+    a1 = a0 + ay * per
+    a2 = a1 + ax * per
+    a3 = a2 + ay * per
+    sides = [_arc(radius, 0.0, radius, a0, a1), _arc(radius, 0.0, radius, a1, a2),
+             _arc(radius, 0.0, radius, a2, a3), _arc(radius, 0.0, radius, a3, a0 + 2.0 * math.pi)]
+    return quad_ogrid(sides, (radius, 0.0), ax, ay, ring)
+
+
+def _smoothstep(x):
+    x = np.clip(x, 0.0, 1.0)
+    return x * x * (3.0 - 2.0 * x)
+
+
+@dataclass
+class Bifurcation:
+    """Y-bifurcation: parent along +z from z = 0 (inlet, label 1), two daughters (outlets labels 2 and
+    3) leaving the junction plane z = parent_length symmetrically about x = 0."""
+    mesh: FlatMesh
+    points: np.ndarray
+    labels: np.ndarray
+    cells: np.ndarray
+    profile: np.ndarray
+    radius: float             # parent radius
+    daughter_radius: float
+    parent_layers: int
+    daughter_layers: int
+    outlet_labels: tuple = (2, 3)
+
+
+def y_bifurcation(parent_radius: float = 2.0e-3, parent_length: float = 20e-3,
+                  daughter_radius: float = 1.59e-3, daughter_length: float = 16e-3,
+                  half_angle_deg: float = 35.0, ax: int = 6, ay: int = 12, ring: int = 3,
+                  parent_layers: int = 308, daughter_layers: int = 247,
+                  bend_length: float | None = None, morph_length: float | None = None) -> Bifurcation:
+    """Swept O-grid Y-bifurcation (all hexahedra, one element per cell, C2 inside each block, C0
+    across block and patch interfaces).
+
+    Each half of the parent is a half-disc O-grid (``half_disc_section``); the two halves share the
+    septum vertices on the diameter x = 0, so the parent cross-section has 2 (ax ay + 2 (ax + ay)
+    ring) cells.  At the junction plane each daughter starts from its half of the parent section;
+    along the daughter (arc length t) the section blends into a disc of the daughter radius
+    (``disc_section_like_half``) over ``morph_length`` and turns about the septum line by the
+    half-angle over ``bend_length`` (smoothstep profiles).  The left daughter's control points all
+    have x <= 0 and the right daughter is its mirror image, so the daughters never overlap (convex
+    hull of the spline); the septum line in the junction plane is the carina edge, a wall.
+    The defaults give 360 (parent_layers + daughter_layers) = 199,800 elements."""
+    R, r = parent_radius, daughter_radius
+    bend = bend_length if bend_length is not None else 0.5 * daughter_length
+    morph = morph_length if morph_length is not None else 0.375 * daughter_length
+    hpos, patches, rim = half_disc_section(R, ax, ay, ring)
+    dpos, dpatches, drim = disc_section_like_half(r, ax, ay, ring)
+    for a, b in zip(patches, dpatches):
+        assert np.array_equal(a, b)
+    nd = len(hpos)
+    septum = rim[2]                                     # local ids, y from +R to -R (local)
+    # Parent plane ids: left half = local ids; right half = new ids except its septum, which is the
+    # left half's septum vertex at the same global y (the left half is rotated by 180 degrees).
+    right_map = np.full(nd, -1, np.int64)
+    right_map[septum] = septum[::-1]
+    others = np.setdiff1d(np.arange(nd), septum)
+    right_map[others] = nd + np.arange(len(others))
+    n_parent = nd + len(others)
+    # parent plane positions
+    ppos = np.zeros((n_parent, 2))
+    ppos[:nd] = -hpos                                   # left half: (s, y) -> (-s, -y)
+    ppos[right_map[others]] = hpos[others]              # right half: (s, y) -> (s, y)
+    planes_p = parent_layers + 1
+    base_left = planes_p * n_parent
+    base_right = base_left + daughter_layers * nd
+    n = base_right + daughter_layers * nd
+    points = np.zeros((n, 3))
+    zp = np.linspace(0.0, parent_length, planes_p)
+    for k in range(planes_p):
+        points[k * n_parent:(k + 1) * n_parent, :2] = ppos
+        points[k * n_parent:(k + 1) * n_parent, 2] = zp[k]
+    # left daughter: pivot path P(t) on the septum line, frame e_s = (-cos th, 0, -sin th), e_y = -y
+    theta_max = math.radians(half_angle_deg)
+    t = np.linspace(0.0, daughter_length, daughter_layers + 1)
+    fine = np.linspace(0.0, daughter_length, 64 * daughter_layers + 1)
+    th_f = theta_max * _smoothstep(fine / bend)
+    dx = np.concatenate([[0.0], np.cumsum(0.5 * (np.sin(th_f[1:]) + np.sin(th_f[:-1])) * np.diff(fine))])
+    dz = np.concatenate([[0.0], np.cumsum(0.5 * (np.cos(th_f[1:]) + np.cos(th_f[:-1])) * np.diff(fine))])
+    px = -np.interp(t, fine, dx)
+    pz = parent_length + np.interp(t, fine, dz)
+    th = theta_max * _smoothstep(t / bend)
+    w = _smoothstep(t / morph)
+    left_ids = np.zeros((daughter_layers + 1, nd), np.int64)
+    right_ids = np.zeros((daughter_layers + 1, nd), np.int64)
+    left_ids[0] = (planes_p - 1) * n_parent + np.arange(nd)
+    right_ids[0] = (planes_p - 1) * n_parent + right_map
+    for j in range(1, daughter_layers + 1):
+        loc = (1.0 - w[j]) * hpos + w[j] * dpos          # [nd, 2] local (s, y)
+        sl, yl = loc[:, 0], loc[:, 1]
+        left = np.stack([px[j] - sl * math.cos(th[j]), -yl, pz[j] - sl * math.sin(th[j])], axis=1)
+        # right daughter = mirror x of the left daughter evaluated at local (s, -y)
+        right = np.stack([-(px[j] - sl * math.cos(th[j])), yl, pz[j] - sl * math.sin(th[j])], axis=1)
+        left_ids[j] = base_left + (j - 1) * nd + np.arange(nd)
+        right_ids[j] = base_right + (j - 1) * nd + np.arange(nd)
+        points[left_ids[j]] = left
+        points[right_ids[j]] = right
+    parent_patches = [p.copy() for p in patches] + [right_map[p] for p in patches]
+    arc_wall = [False, True, True, False, True]          # core, then ring sides 0..3 (2 = septum)
+    blocks = [
+        SweptBlock(patches=parent_patches, ids=np.arange(planes_p * n_parent).reshape(planes_p, n_parent),
+                   wall=arc_wall + arc_wall, bottom=1, top=None),
+        SweptBlock(patches=patches, ids=left_ids, wall=[False] + [True] * 4, bottom=None, top=2),
+        SweptBlock(patches=patches, ids=right_ids, wall=[False] + [True] * 4, bottom=None, top=3),
+    ]
+    mesh, cells = swept_mesh(points, blocks)
+    labels = np.full(n, -1, np.int32)
+    labels[:n_parent] = 1                                        # inlet plane
+    labels[left_ids[-1]] = 2
+    labels[right_ids[-1]] = 3
+    arc = np.unique(np.concatenate([rim[0], rim[1], rim[3]]))
+    for k in range(planes_p):
+        labels[k * n_parent + arc] = 0
+        labels[k * n_parent + right_map[arc]] = 0
+    all_rim = np.unique(np.concatenate(rim))
+    labels[left_ids[:, all_rim].ravel()] = 0
+    labels[right_ids[:, all_rim].ravel()] = 0
+    profile = np.zeros((n, 3))
+    r2 = (points[:n_parent, 0] ** 2 + points[:n_parent, 1] ** 2) / R ** 2
+    profile[:n_parent, 2] = np.maximum(0.0, 1.0 - r2)
+    return Bifurcation(mesh=mesh, points=points, labels=labels, cells=cells, profile=profile, radius=R,
+                       daughter_radius=r, parent_layers=parent_layers, daughter_layers=daughter_layers)
 
 def write_vtk(path, tube: Tube) -> None:
     n, E = len(tube.points), len(tube.cells)
