@@ -129,6 +129,14 @@ def outlet_models(name):
 OUTLET_RELAXATION = 1.0
 
 
+def outlet_step(ns, outlets, coupling):
+    """One step with outlet models: the reference's outer loop (a Newton loop per outlet iteration) or the
+    pressures updated inside one Newton loop; both accept at the same tolerances."""
+    if coupling == "outer":
+        return ns.step_outlets(outlets, OUTLET_RELAXATION)
+    return ns.step_outlets_coupled(outlets, OUTLET_RELAXATION)
+
+
 def boundary(obj, wave):
     """(vmask, pmask, velocity_at(t)) of a workload: one tube with one waveform, or a tube batch whose
     tubes each scale their own peak velocity by their own seeded waveform (normalised to mean 1)."""
@@ -304,8 +312,10 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2-100", "c3", "c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "bf16x3", "fp64"])
     ap.add_argument("--no-fp64-leg", action="store_true")
+    ap.add_argument("--outlet-coupling", default="newton", choices=["newton", "outer"])
+    ap.add_argument("--krylov-fp64-basis", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=25.0)
     ap.add_argument("--ref-newton", type=float, default=3.0)
     ap.add_argument("--ref-linear", type=float, default=300.0)
@@ -332,15 +342,16 @@ def main():
     n = tube.mesh.nodes
     mesh = api.Mesh(tube.mesh)
     amg = args.preconditioner == "amg"
-    mixed = args.precision == "mixed"
+    mixed = args.precision in ("mixed", "bf16x3")
     if mixed and not amg:
         raise SystemExit("--precision mixed needs --preconditioner amg")
     solver_kw = dict(density=RHO, viscosity=MU, dt=step_dt(args.workload),
                      nonlinear_rtol=1e-8, nonlinear_atol=1e-300, mass_rtol=1e-3,
                      gmres_restart=200, gmres_max_iterations=5000, gmres_rtol=1e-8,
                      preconditioner=api.AMG if amg else api.BLOCK_JACOBI,
-                     amg_coarse_period=3)
-    ns = api.NavierStokes(mesh, precision=api.MIXED if mixed else api.FP64, **solver_kw)
+                     amg_coarse_period=3, krylov_fp64_basis=int(args.krylov_fp64_basis))
+    precision = {"mixed": api.MIXED, "bf16x3": api.MIXED_BF16X3, "fp64": api.FP64}[args.precision]
+    ns = api.NavierStokes(mesh, precision=precision, **solver_kw)
     dt = ns.params.dt
     vmask, pmask, velocity_at = boundary(tube, wave)
 
@@ -369,7 +380,7 @@ def main():
         else:
             api.check(api.lib().tfiga_ns_set_dirichlet_values(ns._h, api.C.c_void_p(bc_dev[k].data_ptr()), None))
         ns.commit_step()
-        r = ns.step_outlets(outlets, OUTLET_RELAXATION) if outlets else ns.step()
+        r = outlet_step(ns, outlets, args.outlet_coupling) if outlets else ns.step()
         reports.append(r)
         if host:
             api.check(api.lib().tfiga_ns_get_state(ns._h, api.C.c_void_p(out_host.data_ptr())))
@@ -430,7 +441,7 @@ def main():
         ref.set_state(s0, s0)
         ref_outlets = [api.Outlet(**m.as_dict()) for m in models] if models else None
         rstream = torch.cuda.ExternalStream(ref.stream())
-        errors, fp64_ms, fp64_steps = [], 0.0, 0
+        errors, fp64_ms, fp64_steps, fp64_reports = [], 0.0, 0, []
         for k in range(args.warmup):
             api.check(api.lib().tfiga_ns_set_dirichlet_values(ref._h, api.C.c_void_p(bc_dev[k].data_ptr()), None))
             ref.commit_step()
@@ -438,10 +449,11 @@ def main():
             torch.cuda.synchronize()
             a0.record(rstream)
             if ref_outlets:
-                ref.step_outlets(ref_outlets, OUTLET_RELAXATION)
+                rep = outlet_step(ref, ref_outlets, args.outlet_coupling)
             else:
-                ref.step()
+                rep = ref.step()
             a1.record(rstream)
+            fp64_reports.append(rep)
             torch.cuda.synchronize()
             if k > 0:
                 fp64_ms += a0.elapsed_time(a1)
@@ -453,6 +465,10 @@ def main():
                            "pressure": float(np.linalg.norm(mx[:, 3] - r64[:, 3]) / np.linalg.norm(r64[:, 3]))})
         fp64_leg = {"value": fp64_steps / (fp64_ms / 1e3) if fp64_steps else None, "unit": "time steps/s",
                     "steps": fp64_steps, "ms_per_step": fp64_ms / max(fp64_steps, 1),
+                    "newton_per_step": float(np.mean([r["newton_iterations"] for r in fp64_reports])),
+                    "linear_iterations_per_newton": float(np.sum([r["linear_iterations"] for r in fp64_reports])
+                                                          / max(1, np.sum([r["newton_iterations"]
+                                                                           for r in fp64_reports]))),
                     "error_vs_fp64_per_step": errors}
         ref.close()
         del ref
@@ -543,11 +559,15 @@ def main():
         "vs_baseline": None, "dtype": "bf16-tc/f32/f64" if mixed else "f64",
         "data": "synthetic (seeded generator; BASELINE publishes no dataset)",
         "config": {"workload": desc, "elements": tube.mesh.elements, "nodes": n, "block_nonzeros": mesh.blocks,
-                   "solver": (("mixed: tcgen05 BF16 tangent (FP32 accumulate), FP32 Jacobian, FP64 residual and "
-                               "refinement; " if mixed else "plain FP64: ") +
+                   "solver": (("mixed: tcgen05 %s tangent (FP32 accumulate), FP32 Jacobian, FP64 residual and "
+                               "refinement; " % ("split-BF16 (hi + lo, 3 products)" if args.precision == "bf16x3"
+                                                 else "BF16") if mixed else "plain FP64: ") +
                               "exact-tangent Newton to rel.res 1e-8, " +
                               ("RCR outlets coupled by the relaxed fixed point (relaxation %g, tolerance "
-                               "1e-8 + 1e-6 |P|), " % OUTLET_RELAXATION if models else "") +
+                               "1e-8 + 1e-6 |P|; %s), " % (OUTLET_RELAXATION,
+                                                          "pressures updated inside the Newton loop"
+                                                          if args.outlet_coupling == "newton" else
+                                                          "the reference's outer loop") if models else "") +
                               ("point-block AMG V(1,1)-preconditioned FGMRES(200) rtol 1e-8" if amg else
                                "block-Jacobi GMRES(200) rtol 1e-8")),
                    "l2": "inputs larger than L2 (matrix %.2f GB)" % (mesh.blocks * 128 / 1e9),
@@ -555,8 +575,8 @@ def main():
         "newton_per_step": float(newton), "linear_iterations_per_newton": float(linear),
         "outlets": ([{k: o.as_dict()[k] for k in ("label", "flow", "pressure", "capacitor_pressure")}
                      for o in outlets] if outlets else None),
-        "outlet_iterations_per_step": (float(np.mean([r["outlet_iterations"] for r in timed_reports]))
-                                       if outlets else None),
+        "outlet_iterations_per_step": (float(np.mean([r.get("outlet_iterations", r.get("pressure_updates", 0))
+                                                      for r in timed_reports])) if outlets else None),
         "roofline": roof, "kernels": kernels,
         "fp64_gpu": fp64_leg,
         "spmv_gbs": kernels.get(spmv_name, {}).get("achieved"),

@@ -96,6 +96,10 @@ typedef struct tfiga_ns_params {
 	 * with FGMRES true-residual restarts acting as FP64 iterative refinement.
 	 * TFIGA_PRECISION_FP32_JACOBIAN: as MIXED, but the tangent is assembled in FP64 and
 	 * rounded once to FP32 for storage.
+	 * TFIGA_PRECISION_MIXED_BF16X3: as MIXED, with every tensor-core operand split into
+	 * two BF16 terms (x = hi + lo) and three products per tile (hi hi + hi lo + lo hi):
+	 * a tangent accurate to about 1e-5 instead of 2e-3, so that Newton converges as with
+	 * the FP64 tangent.
 	 * Both reduced modes require TFIGA_PRECONDITIONER_AMG. */
 	int32_t precision;             /* default TFIGA_PRECISION_FP64 */
 	/* AMG: aggregate until at most this many coarse nodes remain (dense
@@ -105,11 +109,16 @@ typedef struct tfiga_ns_params {
 	 * amg_coarse_period-th linear solve only (the fine-level data, A P and the
 	 * block-Jacobi inverses, are refreshed on every solve). */
 	int32_t amg_coarse_period;     /* default 1 */
+	/* Reduced-precision modes: keep the flexible GMRES Krylov basis in FP64 instead
+	 * of FP32 (twice the basis traffic; no loss of orthogonality from FP32 storage
+	 * over long Arnoldi cycles).  Ignored in TFIGA_PRECISION_FP64. */
+	int32_t krylov_fp64_basis;     /* default 0 */
 } tfiga_ns_params;
 
 #define TFIGA_PRECISION_FP64 0
 #define TFIGA_PRECISION_MIXED 1
 #define TFIGA_PRECISION_FP32_JACOBIAN 2
+#define TFIGA_PRECISION_MIXED_BF16X3 3
 
 #define TFIGA_PRECONDITIONER_BLOCK_JACOBI 0
 #define TFIGA_PRECONDITIONER_AMG 1
@@ -242,6 +251,19 @@ int tfiga_ns_step(tfiga_ns* ns, tfiga_step_report* report);
  * loops.  TFIGA_E_NOT_CONVERGED after max_iterations. */
 int tfiga_ns_step_outlets(tfiga_ns* ns, tfiga_outlet* outlets, int32_t count, double relaxation,
 	int32_t max_iterations, tfiga_step_report* report, int32_t* outlet_iterations);
+/* One physical step with the outlet models coupled inside a single Newton loop
+ * (no reference counterpart; same fixed point and acceptance tests as
+ * tfiga_ns_step_outlets): after every Newton update the outward flows are
+ * evaluated and each outlet pressure P moves to (1 - relaxation) P + relaxation
+ * P_eval; the step is accepted when the Newton residual test holds (relative to
+ * the step's first residual) and max |P_eval - P| <= 1e-8 + 1e-6 max(1, |P_eval|).
+ * The reference's outer loop restarts Newton for every outlet iteration and
+ * tightens the residual test to the new, small initial residual; this form
+ * needs about as many Newton solves as a step without outlets.  report counts
+ * the solves; *pressure_updates (may be NULL) the pressure changes.
+ * TFIGA_E_NOT_CONVERGED after max_newton Newton iterations. */
+int tfiga_ns_step_outlets_coupled(tfiga_ns* ns, tfiga_outlet* outlets, int32_t count, double relaxation,
+	int32_t max_newton, tfiga_step_report* report, int32_t* pressure_updates);
 /* AMG hierarchy sizes (levels = 0 before the hierarchy is built). */
 int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info);
 /* Outward flow through each labelled boundary (IntegrateBoundaryFlow,

@@ -9,6 +9,10 @@ FP32 accumulation and stored in FP32; the residual stays FP64.  Tolerances:
 * Newton: the mixed Newton iteration converges to the FP64 solution; after
   convergence to 1e-10 of the initial residual the velocity agrees to 1e-8
   and the pressure to 1e-6 relative L2 with the FP64 path.
+Split-BF16 mode (TFIGA_PRECISION_MIXED_BF16X3, operands hi + lo, three
+products): Jacobian within 1e-4 relative per field pair -- about 2^-16 per
+product plus FP32 accumulation and the FP32 coefficients -- and Newton takes
+no more iterations than with the FP64 tangent.
 """
 import numpy as np
 import pytest
@@ -19,6 +23,7 @@ pytestmark = pytest.mark.gpu
 
 RHO, MU, DT = 1060.0, 3.5e-3, 1e-3
 TANGENT_TOL = 2e-2
+SPLIT_TOL = 1e-4
 
 
 @pytest.fixture(scope="module")
@@ -39,9 +44,10 @@ def random_state(nodes, seed, speed=0.2, pressure=20.0):
     return s.ravel()
 
 
-def check_tensor_tangent(api, flat, rho, mu, dt, seed):
+def check_tensor_tangent(api, flat, rho, mu, dt, seed, precision=None, tol=TANGENT_TOL):
     mesh = api.Mesh(flat)
-    ns = api.NavierStokes(mesh, density=rho, viscosity=mu, dt=dt, preconditioner=api.AMG, precision=api.MIXED)
+    ns = api.NavierStokes(mesh, density=rho, viscosity=mu, dt=dt, preconditioner=api.AMG,
+                          precision=api.MIXED if precision is None else precision)
     st = random_state(flat.nodes, seed)
     pv = random_state(flat.nodes, seed + 1)
     ns.set_state(st, pv)
@@ -52,7 +58,7 @@ def check_tensor_tangent(api, flat, rho, mu, dt, seed):
         assert rel(rhs[f::4], orhs[f::4]) < 1e-12
     v, r = values.reshape(-1, 4, 4), ov.reshape(-1, 4, 4)
     errors = np.array([[rel(v[:, i, f], r[:, i, f]) for f in range(4)] for i in range(4)])
-    assert errors.max() < TANGENT_TOL, errors
+    assert errors.max() < tol, errors
     return errors
 
 
@@ -69,6 +75,40 @@ def test_tensor_tangent_reference_tube_ragged(api, reference_tube):
     from tubularflowiga_b200 import ntiga
     flat = ntiga.read(reference_tube / "tube-1.ntiga")
     check_tensor_tangent(api, flat, 1.0, 1.0, 0.1, 5)
+
+
+def test_split_tangent_small_tube(api, small_tube):
+    errors = check_tensor_tangent(api, small_tube.mesh, RHO, MU, DT, 0, api.MIXED_BF16X3, SPLIT_TOL)
+    plain = check_tensor_tangent(api, small_tube.mesh, RHO, MU, DT, 0)
+    assert errors.max() < 0.05 * plain.max()
+
+
+def test_split_tangent_steady_and_ragged(api, small_tube, reference_tube):
+    from tubularflowiga_b200 import ntiga
+    check_tensor_tangent(api, small_tube.mesh, RHO, MU, 0.0, 3, api.MIXED_BF16X3, SPLIT_TOL)
+    flat = ntiga.read(reference_tube / "tube-1.ntiga")
+    check_tensor_tangent(api, flat, 1.0, 1.0, 0.1, 5, api.MIXED_BF16X3, SPLIT_TOL)
+
+
+def test_split_newton_matches_fp64_iterations(api, cylinder_1280):
+    tube = cylinder_1280
+    flat = tube.mesh
+    vmask, pmask, vel = api.tube_boundary_conditions(tube, 0.2)
+    s0 = api.initial_state(vmask, vel)
+    mesh = api.Mesh(flat)
+    states, reports = {}, {}
+    for name, precision in (("fp64", api.FP64), ("split", api.MIXED_BF16X3)):
+        ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, preconditioner=api.AMG, precision=precision,
+                              nonlinear_rtol=1e-10, nonlinear_atol=1e-30, gmres_rtol=1e-10, max_newton=20)
+        ns.set_dirichlet(vmask, pmask, vel)
+        ns.set_tractions({2: 0.0})
+        ns.set_state(s0, s0)
+        reports[name] = ns.step()
+        states[name] = ns.get_state().reshape(-1, 4)
+    assert reports["split"]["converged"]
+    assert reports["split"]["newton_iterations"] <= reports["fp64"]["newton_iterations"]
+    assert rel(states["split"][:, :3], states["fp64"][:, :3]) < 1e-8
+    assert rel(states["split"][:, 3], states["fp64"][:, 3]) < 1e-6
 
 
 def test_tensor_tangent_is_repeatable_in_norm(api, small_tube):

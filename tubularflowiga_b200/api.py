@@ -41,12 +41,14 @@ class NsParams(C.Structure):
                 ("max_newton", C.c_int32), ("nonlinear_rtol", C.c_double), ("nonlinear_atol", C.c_double),
                 ("mass_rtol", C.c_double), ("gmres_restart", C.c_int32), ("gmres_max_iterations", C.c_int32),
                 ("gmres_rtol", C.c_double), ("preconditioner", C.c_int32), ("precision", C.c_int32),
-                ("amg_coarse_nodes", C.c_int32), ("amg_coarse_period", C.c_int32)]
+                ("amg_coarse_nodes", C.c_int32), ("amg_coarse_period", C.c_int32),
+                ("krylov_fp64_basis", C.c_int32)]
 
 
 FP64 = 0
 MIXED = 1
 FP32_JACOBIAN = 2
+MIXED_BF16X3 = 3
 
 
 BLOCK_JACOBI = 0
@@ -133,6 +135,8 @@ SIGNATURES = {
     "tfiga_ns_step": (C.c_int, [C.c_void_p, C.POINTER(StepReport)]),
     "tfiga_ns_step_outlets": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_double, C.c_int32,
                                         C.POINTER(StepReport), C.POINTER(C.c_int32)]),
+    "tfiga_ns_step_outlets_coupled": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_double, C.c_int32,
+                                                C.POINTER(StepReport), C.POINTER(C.c_int32)]),
     "tfiga_ns_amg_info": (C.c_int, [C.c_void_p, C.POINTER(AmgInfo)]),
     "tfiga_ns_boundary_flows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "tfiga_ns_spmv_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -333,6 +337,21 @@ class NavierStokes:
                 outlets[k] = arr[k]
         d = r.as_dict()
         d["outlet_iterations"] = it.value
+        return d
+
+    def step_outlets_coupled(self, outlets, relaxation=1.0, max_newton=20):
+        """One physical step with the outlet pressures updated inside the Newton loop (same fixed point and
+        tolerances as step_outlets).  Returns the step report with ``pressure_updates``."""
+        arr = outlets if isinstance(outlets, C.Array) else (Outlet * len(outlets))(*outlets)
+        r = StepReport()
+        it = C.c_int32()
+        check(lib().tfiga_ns_step_outlets_coupled(self._h, C.cast(arr, C.c_void_p) if len(arr) else None, len(arr),
+                                                  relaxation, max_newton, C.byref(r), C.byref(it)))
+        if not isinstance(outlets, C.Array):
+            for k in range(len(outlets)):
+                outlets[k] = arr[k]
+        d = r.as_dict()
+        d["pressure_updates"] = it.value
         return d
 
     def boundary_flows(self, labels):

@@ -183,6 +183,7 @@ void tfiga_ns_default_params(tfiga_ns_params* p)
 	p->precision = TFIGA_PRECISION_FP64;
 	p->amg_coarse_nodes = 300;
 	p->amg_coarse_period = 1;
+	p->krylov_fp64_basis = 0;
 }
 
 int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out)
@@ -327,6 +328,17 @@ int tfiga_ns_step_outlets(tfiga_ns* ns, tfiga_outlet* outlets, int32_t count, do
 		int iterations = 0;
 		*report = ns->solver->StepOutlets(outlets, count, relaxation, max_iterations, &iterations);
 		if (outlet_iterations) *outlet_iterations = iterations;
+	});
+}
+
+int tfiga_ns_step_outlets_coupled(tfiga_ns* ns, tfiga_outlet* outlets, int32_t count, double relaxation,
+	int32_t max_newton, tfiga_step_report* report, int32_t* pressure_updates)
+{
+	return Guard([&] {
+		Require(ns && report && count >= 0 && (count == 0 || outlets), "null argument");
+		int updates = 0;
+		*report = ns->solver->StepOutletsCoupled(outlets, count, relaxation, max_newton, &updates);
+		if (pressure_updates) *pressure_updates = updates;
 	});
 }
 

@@ -405,12 +405,12 @@ template <> float* Gmres::Basis<float>()
 	return V32_.get();
 }
 
-template <class T>
+template <class T, class B>
 void Gmres::FlexibleStep(const DevicePatternView& pattern, const T* values, int j, Amg& M)
 {
 	const int* stop = state_.get();
-	T* basis = Basis<T>();
-	ScaleCopyKernel<T><<<blocks_, kThreads, 0, stream_>>>(n_, basis+(size_t)j*n_, scale_.get()+j, r_.get(), stop);
+	B* basis = Basis<B>();
+	ScaleCopyKernel<B><<<blocks_, kThreads, 0, stream_>>>(n_, basis+(size_t)j*n_, scale_.get()+j, r_.get(), stop);
 	LaunchCheck("ScaleCopyKernel");
 	launches_ += 1;
 	double* z = Z_.get()+(size_t)j*n_;
@@ -433,22 +433,22 @@ void Gmres::FlexibleStep(const DevicePatternView& pattern, const T* values, int 
 		collector_->AddKrylovPair(pair_dinv_.get(), z, pair_amg_.get(), w_.get(), pair_aamg_.get(), stop);
 		launches_ += 6;
 	}
-	Orthogonalize<T>(j, basis);
+	Orthogonalize<B>(j, basis);
 }
 
-template <class T>
+template <class T, class B>
 double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const T* values, const double* rhs,
 	const double* x)
 {
 	// v_0 = b - A x (FP64), stored in the basis precision; beta from the FP64 vector
 	LaunchSpmv<T>(pattern, values, x, tmp_.get(), stream_);
-	double* r = std::is_same<T, double>::value ? V_.get() : r_.get();
+	double* r = std::is_same<B, double>::value ? V_.get() : r_.get();
 	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), r);
 	LaunchCheck("ResidualKernel");
 	LaunchNorm(n_, r, norm_partial_.get(), scalar_.get(), stream_);
 	launches_ += 4;
-	if (!std::is_same<T, double>::value) {
-		LaunchToFloat(n_, r, reinterpret_cast<float*>(Basis<T>()), stream_);
+	if (!std::is_same<B, double>::value) {
+		LaunchToFloat(n_, r, reinterpret_cast<float*>(Basis<B>()), stream_);
 		launches_ += 1;
 	}
 	scalar_.Download(host_->beta, 1, stream_);
@@ -458,13 +458,22 @@ double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const T* value
 
 template <class T>
 GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const T* values, const double* rhs,
+	double* x, double rtol, int max_iterations, Amg& M, long long* launches, bool fp64_basis)
+{
+	if (fp64_basis || std::is_same<T, double>::value)
+		return SolveFlexibleImpl<T, double>(pattern, values, rhs, x, rtol, max_iterations, M, launches);
+	return SolveFlexibleImpl<T, float>(pattern, values, rhs, x, rtol, max_iterations, M, launches);
+}
+
+template <class T, class B>
+GmresResult Gmres::SolveFlexibleImpl(const DevicePatternView& pattern, const T* values, const double* rhs,
 	double* x, double rtol, int max_iterations, Amg& M, long long* launches)
 {
 	launches_ = 0;
 	const long long amg0 = M.launches();
 	if (Z_.size() == 0) Z_.Allocate((size_t)(restart_+1)*n_);
 	GmresResult result;
-	double beta = TrueResidualPlain<T>(pattern, values, rhs, x);
+	double beta = TrueResidualPlain<T, B>(pattern, values, rhs, x);
 	result.residual = beta;
 	if (!std::isfinite(beta)) Fail(-6, "FGMRES initial residual is not finite");
 	if (beta == 0.0) {
@@ -482,7 +491,7 @@ GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const T* valu
 		for (int j = 0; j < cap;) {
 			const int batch = std::min(kBatch, cap-j);
 			for (int b = 0; b < batch; ++b) {
-				FlexibleStep<T>(pattern, values, j+b, M);
+				FlexibleStep<T, B>(pattern, values, j+b, M);
 				ArnoldiFinalizeKernel<<<1, kThreads, finalize_smem_, stream_>>>(norm_partial_.get(), update_blocks_, H_.get(), restart_, j+b,
 					cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance);
 				LaunchCheck("ArnoldiFinalizeKernel");
@@ -497,8 +506,8 @@ GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const T* valu
 		const int used = host_->used;
 		result.iterations += used;
 		if (profiler_) {
-			profiler_->AddBytes(Profiler::kOrtho, ArnoldiBytes(n_, used, (int)sizeof(T), true));
-			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, (int)sizeof(T)));
+			profiler_->AddBytes(Profiler::kOrtho, ArnoldiBytes(n_, used, (int)sizeof(B), true));
+			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, (int)sizeof(B)));
 		}
 		BackSolveKernel<<<1, 256, (size_t)(restart_+1)*sizeof(double), stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(), state_.get()+2);
 		LaunchCheck("BackSolveKernel");
@@ -506,7 +515,7 @@ GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const T* valu
 			nullptr, y_.get(), state_.get(), x);
 		LaunchCheck("SolutionUpdateKernel");
 		launches_ += 2;
-		beta = TrueResidualPlain<T>(pattern, values, rhs, x);
+		beta = TrueResidualPlain<T, B>(pattern, values, rhs, x);
 		state_.Download(&host_->stop, 3, stream_);
 		CudaCheck(cudaStreamSynchronize(stream_), "FGMRES restart");
 		if (host_->error) Fail(-6, "FGMRES Hessenberg matrix is singular");
@@ -602,8 +611,8 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 }
 
 template GmresResult Gmres::SolveFlexible<double>(const DevicePatternView&, const double*, const double*, double*,
-	double, int, Amg&, long long*);
+	double, int, Amg&, long long*, bool);
 template GmresResult Gmres::SolveFlexible<float>(const DevicePatternView&, const float*, const double*, double*,
-	double, int, Amg&, long long*);
+	double, int, Amg&, long long*, bool);
 
 } // namespace tfiga

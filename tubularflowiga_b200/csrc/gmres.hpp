@@ -37,11 +37,12 @@ public:
 	// Right-preconditioned flexible GMRES (FGMRES): z_j = M^{-1} v_j stored, tolerance
 	// rtol * ||b - A x0|| on the true residual.
 	// The matrix may be stored in FP64 or FP32 (T); with FP32 the Krylov basis is stored in FP32
-	// too (dots, updates and the work vector in FP64 arithmetic); preconditioned vectors, Hessenberg,
-	// Givens and the solution stay FP64, and each restart's true residual is the FP64 refinement.
+	// too unless fp64_basis (dots, updates and the work vector in FP64 arithmetic); preconditioned
+	// vectors, Hessenberg, Givens and the solution stay FP64, and each restart's true residual is the
+	// FP64 refinement.
 	template <class T>
 	GmresResult SolveFlexible(const DevicePatternView& pattern, const T* values, const double* rhs, double* x,
-		double rtol, int max_iterations, Amg& preconditioner, long long* launches);
+		double rtol, int max_iterations, Amg& preconditioner, long long* launches, bool fp64_basis = false);
 	int restart() const { return restart_; }
 	// Learned stage added to the AMG application in SolveFlexible (null: AMG only).
 	void set_learned(LearnedPreconditioner* learned) { learned_ = learned; }
@@ -54,11 +55,14 @@ public:
 private:
 	void Step(const DevicePatternView& pattern, const double* values, int j);
 	template <class B> void Orthogonalize(int j, B* basis);
-	// Krylov basis storage: FP64, or FP32 when the matrix is stored in FP32 (T = float).
+	// Krylov basis storage: FP64 (V_) or FP32 (V32_, allocated on first use).
 	template <class B> B* Basis();
-	template <class T>
+	template <class T, class B>
+	GmresResult SolveFlexibleImpl(const DevicePatternView& pattern, const T* values, const double* rhs, double* x,
+		double rtol, int max_iterations, Amg& preconditioner, long long* launches);
+	template <class T, class B>
 	void FlexibleStep(const DevicePatternView& pattern, const T* values, int j, Amg& preconditioner);
-	template <class T>
+	template <class T, class B>
 	double TrueResidualPlain(const DevicePatternView& pattern, const T* values, const double* rhs, const double* x);
 	double TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs, const double* x);
 

@@ -64,7 +64,7 @@ void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double*
 // completion wait expired.  phi32 is the FP32 copy of phi (Mesh::phi32).
 void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const float* phi32, const double* qdata,
 	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
-	float* values, double* rhs, int* status, cudaStream_t stream);
+	float* values, double* rhs, int* status, bool split, cudaStream_t stream);
 
 // ---- sparse.cu ----------------------------------------------------------
 // Matrix values are FP64 or FP32 (T = double / float); vectors are FP64.

@@ -44,7 +44,7 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 	stream_ = mesh.stream();
 	const int64_t n = mesh.nodes();
 	if (params.precision != TFIGA_PRECISION_FP64 && params.precision != TFIGA_PRECISION_MIXED
-		&& params.precision != TFIGA_PRECISION_FP32_JACOBIAN)
+		&& params.precision != TFIGA_PRECISION_FP32_JACOBIAN && params.precision != TFIGA_PRECISION_MIXED_BF16X3)
 		Fail(-1, "unknown precision "+std::to_string(params.precision));
 	if (!tensor_tangent()) values_.Allocate((size_t)blocks()*16);
 	rhs_.Allocate(n4_); state_.Allocate(n4_); previous_.Allocate(n4_); update_.Allocate(n4_);
@@ -194,7 +194,7 @@ void NsSolver::Assemble()
 		profiler_.Begin(Profiler::kAssembly, stream_);
 		LaunchTangentTc(mesh_.view(), mesh_.phi(), mesh_.phi32(), mesh_.qdata(), mesh_.element_blocks(), state_.get(),
 			previous_.get(), {params_.density, params_.viscosity, params_.dt}, values32_.get(), rhs_.get(),
-			status_.get(), stream_);
+			status_.get(), params_.precision == TFIGA_PRECISION_MIXED_BF16X3, stream_);
 		profiler_.End(stream_);
 		LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
 		launches_ += 2;
@@ -242,7 +242,7 @@ GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 		auto solve = [&]() {
 			if (mixed())
 				return gmres_.SolveFlexible<float>(mesh_.pattern_view(), values32_.get(), rhs_.get(), update_.get(),
-					rtol, max_iterations, *amg_, &launches_);
+					rtol, max_iterations, *amg_, &launches_, params_.krylov_fp64_basis != 0);
 			return gmres_.SolveFlexible<double>(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol,
 				max_iterations, *amg_, &launches_);
 		};
@@ -400,28 +400,12 @@ tfiga_step_report NsSolver::StepOutlets(tfiga_outlet* outlets, int count, double
 {
 	if (!(relaxation > 0.0 && relaxation <= 1.0)) Fail(-1, "invalid outlet coupling relaxation");
 	if (max_iterations < 1) Fail(-1, "outlet coupling needs at least one iteration");
-	std::vector<OutletModel> models(count);
+	std::vector<OutletModel> models = OutletModels(outlets, count);
 	std::vector<int32_t> labels(count);
 	std::vector<double> previous_capacitor(count), flows(count);
 	for (int i = 0; i < count; ++i) {
-		const tfiga_outlet& o = outlets[i];
-		OutletModel& m = models[i];
-		m.label = o.label;
-		if (o.kind == TFIGA_OUTLET_RESISTANCE) m.kind = "resistance";
-		else if (o.kind == TFIGA_OUTLET_RC) m.kind = "windkessel_rc";
-		else if (o.kind == TFIGA_OUTLET_RCR) m.kind = "windkessel_rcr";
-		else Fail(-1, "unknown outlet model kind "+std::to_string(o.kind));
-		m.resistance = o.resistance;
-		m.proximal = o.proximal_resistance;
-		m.distal = o.distal_resistance;
-		m.capacitance = o.capacitance;
-		m.reference_pressure = o.reference_pressure;
-		m.capacitor_pressure = o.capacitor_pressure;
-		m.flow = o.flow;
-		m.pressure = o.pressure;
-		if (!std::isfinite(m.pressure)) Fail(-1, "outlet pressure must be finite");
-		labels[i] = o.label;
-		previous_capacitor[i] = o.capacitor_pressure;
+		labels[i] = outlets[i].label;
+		previous_capacitor[i] = outlets[i].capacitor_pressure;
 	}
 	tfiga_step_report total{};
 	for (int coupling = 0; coupling < max_iterations; ++coupling) {
@@ -466,6 +450,94 @@ tfiga_step_report NsSolver::StepOutlets(tfiga_outlet* outlets, int count, double
 	}
 	if (iterations) *iterations = max_iterations;
 	Fail(-6, "outlet fixed-point iteration did not converge");
+}
+
+std::vector<OutletModel> NsSolver::OutletModels(const tfiga_outlet* outlets, int count) const
+{
+	std::vector<OutletModel> models(count);
+	for (int i = 0; i < count; ++i) {
+		const tfiga_outlet& o = outlets[i];
+		OutletModel& m = models[i];
+		m.label = o.label;
+		if (o.kind == TFIGA_OUTLET_RESISTANCE) m.kind = "resistance";
+		else if (o.kind == TFIGA_OUTLET_RC) m.kind = "windkessel_rc";
+		else if (o.kind == TFIGA_OUTLET_RCR) m.kind = "windkessel_rcr";
+		else Fail(-1, "unknown outlet model kind "+std::to_string(o.kind));
+		m.resistance = o.resistance;
+		m.proximal = o.proximal_resistance;
+		m.distal = o.distal_resistance;
+		m.capacitance = o.capacitance;
+		m.reference_pressure = o.reference_pressure;
+		m.capacitor_pressure = o.capacitor_pressure;
+		m.flow = o.flow;
+		m.pressure = o.pressure;
+		if (!std::isfinite(m.pressure)) Fail(-1, "outlet pressure must be finite");
+	}
+	return models;
+}
+
+tfiga_step_report NsSolver::StepOutletsCoupled(tfiga_outlet* outlets, int count, double relaxation, int max_newton,
+	int* updates)
+{
+	if (!(relaxation > 0.0 && relaxation <= 1.0)) Fail(-1, "invalid outlet coupling relaxation");
+	if (max_newton < 1) Fail(-1, "outlet coupling needs at least one Newton iteration");
+	std::vector<OutletModel> models = OutletModels(outlets, count);
+	std::vector<int32_t> labels(count);
+	std::vector<double> previous_capacitor(count), flows(count);
+	for (int i = 0; i < count; ++i) {
+		labels[i] = outlets[i].label;
+		previous_capacitor[i] = outlets[i].capacitor_pressure;
+	}
+	tfiga_step_report step{};
+	double initial = -1.0;
+	int changes = 0;
+	tfiga_newton_report last{};
+	for (int k = 0; k < max_newton; ++k) {
+		auto traction = tractions_;
+		for (const auto& m : models) traction[m.label] = m.pressure;
+		ApplyTractions(traction);
+		last = NewtonIteration(initial);
+		if (initial < 0.0) { initial = last.residual_l2; step.initial_residual_l2 = initial; }
+		step.assembly_ms += last.assembly_ms;
+		step.linear_ms += last.linear_ms;
+		step.linear_iterations += last.linear_iterations;
+		step.residual_l2 = last.residual_l2;
+		step.relative_mass_imbalance = last.relative_mass_imbalance;
+		if (!last.converged) ++step.newton_iterations;
+		// flows of the current state (after this iteration's update, if it solved)
+		BoundaryFlows(labels.data(), count, flows.data());
+		double change = 0.0, scale = 1.0;
+		std::vector<std::array<double, 2>> evaluated(count);
+		for (int i = 0; i < count; ++i) {
+			OutletModel m = models[i];
+			m.capacitor_pressure = previous_capacitor[i];
+			evaluated[i] = EvaluateOutletModel(m, flows[i], params_.dt);
+			change = std::max(change, std::fabs(evaluated[i][0]-models[i].pressure));
+			scale = std::max(scale, std::fabs(evaluated[i][0]));
+		}
+		if (last.converged && change <= 1e-8+1e-6*scale) {
+			for (int i = 0; i < count; ++i) {
+				outlets[i].flow = flows[i];
+				outlets[i].pressure = evaluated[i][0];
+				outlets[i].capacitor_pressure = evaluated[i][1];
+			}
+			step.converged = 1;
+			if (updates) *updates = changes;
+			return step;
+		}
+		if (change > 1e-8+1e-6*scale) {
+			++changes;
+			for (int i = 0; i < count; ++i) {
+				models[i].flow = flows[i];
+				models[i].pressure = (1.0-relaxation)*models[i].pressure+relaxation*evaluated[i][0];
+				outlets[i].flow = flows[i];
+				outlets[i].pressure = models[i].pressure;
+			}
+		}
+	}
+	if (updates) *updates = changes;
+	Fail(-6, "Navier-Stokes nonlinear solve with coupled outlets reached MAX_NEWTON (nonlinear_residual="
+		+Precise(last.residual_l2)+", relative_mass_imbalance="+Precise(last.relative_mass_imbalance)+")");
 }
 
 void NsSolver::BoundaryFlows(const int32_t* labels, int count, double* flows)

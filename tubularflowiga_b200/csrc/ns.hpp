@@ -4,6 +4,7 @@
 
 #include "amg.hpp"
 #include "gmres.hpp"
+#include "case_input.hpp"
 #include "mesh.hpp"
 
 #include "../../include/tfiga.h"
@@ -37,6 +38,10 @@ public:
 	// Step coupled to outlet models (relaxed fixed point of iga_cuda.cu:927-1086); *iterations = Newton loops.
 	tfiga_step_report StepOutlets(tfiga_outlet* outlets, int count, double relaxation, int max_iterations,
 		int* iterations);
+	// Step with the outlet pressures updated after every Newton update (one Newton loop); *updates =
+	// pressure updates.  Same acceptance tests as StepOutlets.
+	tfiga_step_report StepOutletsCoupled(tfiga_outlet* outlets, int count, double relaxation, int max_newton,
+		int* updates);
 	void BoundaryFlows(const int32_t* labels, int count, double* flows);
 	void Synchronize();
 
@@ -47,7 +52,10 @@ public:
 	// FP32 Jacobian storage (both reduced-precision modes).
 	bool mixed() const { return params_.precision != TFIGA_PRECISION_FP64; }
 	// Tangent contracted on the tensor cores (BF16 x BF16 -> FP32); no FP64 Jacobian is kept.
-	bool tensor_tangent() const { return params_.precision == TFIGA_PRECISION_MIXED; }
+	bool tensor_tangent() const
+	{
+		return params_.precision == TFIGA_PRECISION_MIXED || params_.precision == TFIGA_PRECISION_MIXED_BF16X3;
+	}
 	// Active Jacobian values as FP64 on the host (FP32 storage is widened).
 	void DownloadValues(double* out);
 	double* state() { return state_.get(); }
@@ -72,6 +80,7 @@ private:
 		double continuity_l2, continuity_sum, net_flow, absolute_flow, imbalance;
 	};
 	void ApplyTractions(const std::map<int32_t, double>& traction);
+	std::vector<OutletModel> OutletModels(const tfiga_outlet* outlets, int count) const;
 	void LaunchDiagnostics();     // continuity sums of rhs + per-label flows of state
 	Diagnostics ReadDiagnostics();
 

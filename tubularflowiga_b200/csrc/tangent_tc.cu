@@ -31,6 +31,14 @@
 //             row field), and the two row fields of one (a, b) -- the two
 //             halves of a 32-byte sector -- go out from adjacent lanes of the
 //             same red.global.add.v4.f32 instruction.
+// Split mode (TFIGA_PRECISION_MIXED_BF16X3): every operand x is carried as
+// hi = bf16(x) and lo = bf16(x - hi), and the contraction takes the three
+// products hi.hi + hi.lo + lo.hi (the dropped lo.lo term is 2^-16 relative),
+// so the tangent is accurate to about 1e-5 instead of BF16's 2e-3.  The
+// shared-memory layout is unchanged: chunks hold 4 points (K = 16), and each
+// 64-byte swizzled row carries the hi values in its first 32 bytes and the lo
+// values in its last 32; the three MMAs of a tile start their A / B
+// descriptors at byte 0 or 32 of the row.
 // Every mbarrier wait is bounded (one second of globaltimer); on expiry the
 // CTA records TFIGA status bit 1, waits once more (bounded) for its own MMAs,
 // frees its tensor memory and returns without writing the tangent.
@@ -44,8 +52,7 @@ namespace tfiga {
 namespace {
 
 constexpr int kTcThreads = 256;
-constexpr int kPts = 8;                          // quadrature points per K chunk
-constexpr int kChunks = kQuad/kPts;              // 8
+constexpr int kPts = 8;                          // quadrature points per K chunk (buffers sized for 8)
 constexpr int kTiles = 4;                        // M = 128 tiles per CTA
 constexpr int kTileBytes = 128*64;               // 128 rows x 32 BF16 (64 B, one swizzle row)
 constexpr int kTmemCols = 256;                   // 4 tiles x N = 64 FP32 columns
@@ -158,13 +165,14 @@ template <int N> __device__ __forceinline__ void CopyAsyncWait()
 	asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
 }
 
-// Basis chunk c (points 8c .. 8c+7, five features, 64 functions) of one
-// element, FP32, into a [5][8][64] buffer: 640 16-byte copies.
+// Basis chunk c (points NP c .. NP c + NP - 1, five features, 64 functions) of
+// one element, FP32, into a [5][NP][64] buffer: 5 NP 16 16-byte copies.
+template <int NP>
 __device__ __forceinline__ void PrefetchPhi(const float* P32, int c, uint32_t dst, int tid)
 {
-	for (int idx = tid; idx < kFeatures*kPts*16; idx += kTcThreads) {
-		const int t = idx/(kPts*16), rem = idx%(kPts*16);
-		CopyAsync16(dst+16*idx, P32+(size_t)(t*kQuad+c*kPts)*kMaxBasis+4*rem);
+	for (int idx = tid; idx < kFeatures*NP*16; idx += kTcThreads) {
+		const int t = idx/(NP*16), rem = idx%(NP*16);
+		CopyAsync16(dst+16*idx, P32+(size_t)(t*kQuad+c*NP)*kMaxBasis+4*rem);
 	}
 	CopyAsyncCommit();
 }
@@ -197,6 +205,12 @@ __device__ __forceinline__ uint32_t PackBf16(float lo, float hi)
 	return *reinterpret_cast<const uint32_t*>(&v);
 }
 
+// x - bf16(x): the part of x that its BF16 rounding drops (exact in FP32).
+__device__ __forceinline__ float Bf16Residual(float x)
+{
+	return x-__bfloat162float(__float2bfloat16_rn(x));
+}
+
 __device__ __forceinline__ void StoreShared16(uint32_t address, uint32_t a, uint32_t b, uint32_t c, uint32_t d)
 {
 	asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" :: "r"(address), "r"(a), "r"(b), "r"(c), "r"(d)
@@ -209,6 +223,7 @@ __device__ __forceinline__ void RedAdd4(float* p, float a, float b, float c, flo
 		: "memory");
 }
 
+template <bool kSplit>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const float* __restrict__ phi32, const double* __restrict__ qdata,
 	const int32_t* __restrict__ element_blocks, const double* __restrict__ state,
@@ -299,7 +314,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		QS[q*kQS+k] = ((part[0]+part[kQuad*kPartStride])+part[2*kQuad*kPartStride])+part[3*kQuad*kPartStride];
 	}
 	__syncthreads();
-	PrefetchPhi(P32, 0, sPhi[0], tid);           // chunk 0: the partial sums are dead
+	constexpr int NP = kSplit ? 4 : kPts;        // points per K chunk
+	constexpr int kChunks = kQuad/NP;
+	PrefetchPhi<NP>(P32, 0, sPhi[0], tid);       // chunk 0: the partial sums are dead
 
 	// 3. Coefficients: thread (row field il, point q, column-field pair fp); fp = 0 also
 	//    gives the residual coefficients.
@@ -337,10 +354,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 	bool failed = false;
 	uint32_t pending = 0;                            // parity of the last committed chunk
 	for (int c = 0; c < kChunks; ++c) {
-		const int q0 = c*kPts;
+		const int q0 = c*NP;
 		const float* PhiS = reinterpret_cast<const float*>(sm+(c & 1 ? kOffQS : kOffPhi0));
 		if (c+1 < kChunks) {
-			PrefetchPhi(P32, c+1, sPhi[(c+1) & 1], tid);
+			PrefetchPhi<NP>(P32, c+1, sPhi[(c+1) & 1], tid);
 			CopyAsyncWait<1>();
 		} else {
 			CopyAsyncWait<0>();
@@ -349,30 +366,40 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		if (c > 0) ok = MbarWaitBounded(bar, pending);
 		if (__syncthreads_or(!ok)) { failed = true; break; }
 
-		// B = Psi: row a, K = (point, s); thread (a, point pair).
+		// B = Psi: row a, K = (point, s); thread (a, 16-byte unit u of the row).  Plain: unit u is
+		// point pair u.  Split: units 0, 1 hold hi of point pairs 0, 1 and units 2, 3 their lo.
 		{
-			const int a = tid >> 2, qp = tid & 3;
+			const int a = tid >> 2, u = tid & 3;
+			const int qp = kSplit ? (u & 1) : u;
 			float x[8];
 			#pragma unroll
-			for (int k = 0; k < 8; ++k) x[k] = PhiS[((k & 3)*kPts+2*qp+(k >> 2))*64+a];
-			StoreShared16(sB+Sw64(a, qp), PackBf16(x[0], x[1]), PackBf16(x[2], x[3]), PackBf16(x[4], x[5]),
+			for (int k = 0; k < 8; ++k) x[k] = PhiS[((k & 3)*NP+2*qp+(k >> 2))*64+a];
+			if (kSplit && u >= 2) {
+				#pragma unroll
+				for (int k = 0; k < 8; ++k) x[k] = Bf16Residual(x[k]);
+			}
+			StoreShared16(sB+Sw64(a, u), PackBf16(x[0], x[1]), PackBf16(x[2], x[3]), PackBf16(x[4], x[5]),
 				PackBf16(x[6], x[7]));
 		}
-		// A = G: row (b, f) of tile (il, b / 32), K = (point, s).
+		// A = G: row (b, f) of tile (il, b / 32), K = (point, s).  Plain: warp (il, point pair) over all
+		// b.  Split: warp (il, point pair, half of the b groups), writing hi and lo units.
 		{
-			const int ql0 = 2*gqp;
+			const int qpair = kSplit ? (gqp & 1) : gqp;
+			const int ql0 = 2*qpair;
+			constexpr int kGroups = kSplit ? 4 : 8;
+			const int g0 = kSplit ? (gqp >> 1)*4 : 0;
 			float m0[20], m1[20];
 			const float* c0 = Coef+(gil*kQuad+q0+ql0)*kCoefStride+gf*20;
 			#pragma unroll
 			for (int k = 0; k < 20; ++k) { m0[k] = c0[k]; m1[k] = c0[kCoefStride+k]; }
 			#pragma unroll 2
-			for (int bg = 0; bg < 8; ++bg) {
-				const int b = bg*8+gbs;
+			for (int j = 0; j < kGroups; ++j) {
+				const int b = (g0+j)*8+gbs;
 				float p0[5], p1[5];
 				#pragma unroll
 				for (int t = 0; t < 5; ++t) {
-					p0[t] = PhiS[(t*kPts+ql0)*64+b];
-					p1[t] = PhiS[(t*kPts+ql0+1)*64+b];
+					p0[t] = PhiS[(t*NP+ql0)*64+b];
+					p1[t] = PhiS[(t*NP+ql0+1)*64+b];
 				}
 				float g[8];
 				#pragma unroll
@@ -381,8 +408,15 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 					g[4+s] = m1[s*5]*p1[0]+m1[s*5+1]*p1[1]+m1[s*5+2]*p1[2]+m1[s*5+3]*p1[3]+m1[s*5+4]*p1[4];
 				}
 				const int tile = gil*2+(b >> 5), row = (b & 31)*4+gf;
-				StoreShared16(sA+tile*kTileBytes+Sw64(row, gqp), PackBf16(g[0], g[1]), PackBf16(g[2], g[3]),
+				const uint32_t dst = sA+tile*kTileBytes;
+				StoreShared16(dst+Sw64(row, qpair), PackBf16(g[0], g[1]), PackBf16(g[2], g[3]),
 					PackBf16(g[4], g[5]), PackBf16(g[6], g[7]));
+				if (kSplit) {
+					#pragma unroll
+					for (int k = 0; k < 8; ++k) g[k] = Bf16Residual(g[k]);
+					StoreShared16(dst+Sw64(row, 2+qpair), PackBf16(g[0], g[1]), PackBf16(g[2], g[3]),
+						PackBf16(g[4], g[5]), PackBf16(g[6], g[7]));
+				}
 			}
 		}
 		FenceProxyAsync();
@@ -390,11 +424,18 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		if (tid == 0) {
 			FenceAfterSync();
 			#pragma unroll
-			for (int tile = 0; tile < kTiles; ++tile)
-				#pragma unroll
-				for (int ks = 0; ks < 2; ++ks)
-					MmaBf16(tmem+tile*64, DescSw64(sA+tile*kTileBytes+ks*32), DescSw64(sB+ks*32),
-						(c > 0 || ks > 0) ? 1u : 0u);
+			for (int tile = 0; tile < kTiles; ++tile) {
+				const uint32_t a = sA+tile*kTileBytes;
+				if (kSplit) {
+					MmaBf16(tmem+tile*64, DescSw64(a), DescSw64(sB), c > 0 ? 1u : 0u);       // hi hi
+					MmaBf16(tmem+tile*64, DescSw64(a), DescSw64(sB+32), 1u);                 // hi lo
+					MmaBf16(tmem+tile*64, DescSw64(a+32), DescSw64(sB), 1u);                 // lo hi
+				} else {
+					#pragma unroll
+					for (int ks = 0; ks < 2; ++ks)
+						MmaBf16(tmem+tile*64, DescSw64(a+ks*32), DescSw64(sB+ks*32), (c > 0 || ks > 0) ? 1u : 0u);
+				}
+			}
 			MmaCommit(bar);
 		}
 		pending = (uint32_t)(c & 1);
@@ -461,19 +502,25 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 
 void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const float* phi32, const double* qdata,
 	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
-	float* values, double* rhs, int* status, cudaStream_t stream)
+	float* values, double* rhs, int* status, bool split, cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
 	static bool configured = false;
 	if (!configured) {
-		CudaCheck(cudaFuncSetAttribute(TangentTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes),
-			"tensor-core tangent shared-memory attribute");
+		CudaCheck(cudaFuncSetAttribute(TangentTcKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			kSmemBytes), "tensor-core tangent shared-memory attribute");
+		CudaCheck(cudaFuncSetAttribute(TangentTcKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			kSmemBytes), "tensor-core tangent shared-memory attribute");
 		configured = true;
 	}
 	const long long ctas = 2LL*mesh.elements;
 	if (ctas > 0x7fffffffLL) Fail(-7, "too many elements for one tangent launch");
-	TangentTcKernel<<<(unsigned)ctas, kTcThreads, kSmemBytes, stream>>>(mesh, phi, phi32, qdata, element_blocks,
-		state, previous, params, values, rhs, status);
+	if (split)
+		TangentTcKernel<true><<<(unsigned)ctas, kTcThreads, kSmemBytes, stream>>>(mesh, phi, phi32, qdata,
+			element_blocks, state, previous, params, values, rhs, status);
+	else
+		TangentTcKernel<false><<<(unsigned)ctas, kTcThreads, kSmemBytes, stream>>>(mesh, phi, phi32, qdata,
+			element_blocks, state, previous, params, values, rhs, status);
 	LaunchCheck("TangentTcKernel");
 }
 
