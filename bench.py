@@ -1,36 +1,45 @@
 #!/usr/bin/env python
 """Time steps/s of the body-fitted IGA Navier-Stokes solve on one B200.
 
-Workload (the metric's mixed-precision config): the 51,200-element pulsatile
-tube -- an 8x8-core + two 32-cell ring-layer O-grid cross-section (128 cells,
-145 control points per plane) x 400 axial layers, R = 1.5 mm, L = 30 mm,
-tricubic, rho = 1060 kg/m^3, mu = 3.5e-3 Pa s, backward Euler dt = 2e-3 s,
-parabolic inflow scaled by a seeded Fourier waveform (mean 0.15 m/s + 4
-harmonics, amplitudes U(0, 0.05), seed 0, 1 Hz), zero-traction outlet,
-no-slip wall.  Inputs are synthetic (seeded generator), stated in `data`.
+Workload (default --workload c3, the config the metric's mixed-vs-FP64
+comparison is quoted on): the Y-bifurcation -- parent R 2.0 mm, L 20 mm;
+daughters R 1.59 mm (Murray), L 16 mm, half-angle 35 deg; swept half-disc
+O-grids, 199,800 tricubic elements, 217,271 control points; rho = 1060 kg/m^3,
+mu = 3.5e-3 Pa s, backward Euler dt = 2e-3 s; parabolic inflow scaled by a
+seeded Fourier waveform (mean 0.15 m/s + 4 harmonics, amplitudes U(0, 0.05),
+seed 0, 1 Hz); each daughter outlet a 0D RCR model (R1 1e8, C 1e-10, R2 1e9
+SI, zero initial pressure); no-slip walls.  Other workloads: c2 (the
+51,200-element pulsatile tube), c1 (the 1,280-element cylinder), c2-100 (a
+12,800-element section, profiling), c5 (16 independent tubes as one mesh).
+Inputs are synthetic (seeded generator), stated in `data`.
 
 A "step" is one physical time step: Newton to ||r|| <= 1e-8 ||r_0|| (FP64
 residual) with the exact tangent, each linear solve AMG-preconditioned
 FGMRES(200) to a true-residual rtol of 1e-8 (the AMG's dense coarse inverse
 rebuilt every third linear solve, its fine-level data on every solve; both
-precisions).  --precision mixed (default, the
-config's own precision): tangent contracted on the tcgen05 tensor cores (BF16
-operands, FP32 accumulation), FP32 Jacobian for SpMV and the preconditioner,
-FP64 residual, vectors and refinement.  --precision fp64: every array FP64.
+precisions).  Outlet pressures follow the RCR models by the relaxed fixed
+point (relaxation 1, tolerance 1e-8 + 1e-6 |P|), updated inside the Newton
+loop (--outlet-coupling newton; "outer" runs the reference's loop of Newton
+solves).  --precision bf16x3 (default): tangent contracted on the tcgen05
+tensor cores with split-BF16 operands (hi + lo, three products, FP32
+accumulation), FP32 Jacobian for SpMV and the preconditioner, FP32 Krylov
+basis, FP64 residual, vectors and refinement; --precision mixed: plain BF16
+operands; --precision fp64: every array FP64.
 
 Legs of one run (rank 0 prints one JSON line):
   value     device-timed (CUDA events on the solver stream) with every input
-            resident in HBM; the matrix (1.5 GB FP32, 1.9 GB FP64) exceeds L2,
-            so no flush.
+            resident in HBM; the matrix (3.1 GB FP32 at C3) exceeds L2, so no
+            flush.
   e2e       the same steps again, from the same starting state, through the
             C ABI with pinned host inputs (inlet Dirichlet values) and the
             state read back every step.
   roofline  per-kernel CUDA-event timing of the timed region: the tensor-core
             (or FP64) assembly, SpMV, the AMG V-cycle and the Krylov
             orthogonalisation (HBM-bound); the dominant one by share.
-  fp64_gpu  (mixed only) the plain FP64 GPU solver on the same steps from the
-            same initial state: its time steps/s, and the relative L2 error
-            of the mixed solution against it after every step.
+  fp64_gpu  (mixed only) the plain FP64 GPU solver on the warm-up steps from
+            the same initial state (same outlet coupling): its time steps/s,
+            Newton and FGMRES counts, and the relative L2 error of the mixed
+            solution against it after every step.
   cpu_baseline  the reference's own element code (oracle/_ref) and the CPU
             restatement of block-Jacobi GMRES on a bounded sample, all host
             cores, scaled to time steps/s.
@@ -309,16 +318,16 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2-100", "c3", "c5"])
+    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c1", "c2-100", "c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "bf16x3", "fp64"])
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "mixed", "fp64"])
     ap.add_argument("--no-fp64-leg", action="store_true")
     ap.add_argument("--outlet-coupling", default="newton", choices=["newton", "outer"])
     ap.add_argument("--krylov-fp64-basis", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=25.0)
-    ap.add_argument("--ref-newton", type=float, default=3.0)
-    ap.add_argument("--ref-linear", type=float, default=300.0)
+    ap.add_argument("--ref-newton", type=float, default=4.0)
+    ap.add_argument("--ref-linear", type=float, default=223.0)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

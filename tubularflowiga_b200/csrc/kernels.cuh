@@ -61,10 +61,12 @@ void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double*
 // ---- tangent_tc.cu -----------------------------------------------------
 // Tensor-core tangent (BF16 operands, FP32 accumulation) ADDED into FP32
 // values, FP64 residual ADDED into rhs (= -r); status bit 1 set if an MMA
-// completion wait expired.  phi32 is the FP32 copy of phi (Mesh::phi32).
+// completion wait expired.  phi32 is the FP32 copy of phi (Mesh::phi32);
+// coef is workspace of elements x 4 x 80 x 64 floats (the point coefficients
+// passed from the FP64 point kernel to the tensor-core kernel).
 void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const float* phi32, const double* qdata,
 	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
-	float* values, double* rhs, int* status, bool split, cudaStream_t stream);
+	float* coef, float* values, double* rhs, int* status, bool split, cudaStream_t stream);
 
 // ---- sparse.cu ----------------------------------------------------------
 // Matrix values are FP64 or FP32 (T = double / float); vectors are FP64.

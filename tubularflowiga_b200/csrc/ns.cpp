@@ -77,6 +77,7 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 	if (mixed() && params.preconditioner != TFIGA_PRECONDITIONER_AMG)
 		Fail(-7, "mixed precision requires the AMG-preconditioned flexible GMRES");
 	if (mixed()) values32_.Allocate((size_t)blocks()*16);
+	if (tensor_tangent()) coef32_.Allocate((size_t)mesh.host().elements()*4*80*64);
 	if (tensor_tangent()) {
 		status_.Allocate(1);
 		status_.Zero(stream_);
@@ -193,8 +194,8 @@ void NsSolver::Assemble()
 		rhs_.Zero(stream_);
 		profiler_.Begin(Profiler::kAssembly, stream_);
 		LaunchTangentTc(mesh_.view(), mesh_.phi(), mesh_.phi32(), mesh_.qdata(), mesh_.element_blocks(), state_.get(),
-			previous_.get(), {params_.density, params_.viscosity, params_.dt}, values32_.get(), rhs_.get(),
-			status_.get(), params_.precision == TFIGA_PRECISION_MIXED_BF16X3, stream_);
+			previous_.get(), {params_.density, params_.viscosity, params_.dt}, coef32_.get(), values32_.get(),
+			rhs_.get(), status_.get(), params_.precision == TFIGA_PRECISION_MIXED_BF16X3, stream_);
 		profiler_.End(stream_);
 		LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
 		launches_ += 2;

@@ -94,6 +94,7 @@ private:
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
 	DeviceArray<float> values32_;
+	DeviceArray<float> coef32_;              // tensor-core tangent: point coefficients [e][4][80][64]
 	DeviceArray<double> face_flow_, face_pressure_, label_flow_, partial_, scalars_;
 	DeviceArray<int32_t> vmask_, pmask_, constrained_, face_slot_, status_;
 	std::vector<int32_t> labels_;            // distinct face labels (slot order)

@@ -9,36 +9,42 @@
 //   K^{if}_{ab} = sum_k Psi(a, k) G^{if}(b, k),   k = (q, s): 64 points x 4 test features,
 //   G^{if}(b, (q, s)) = sum_t M_q^{if}[s][t] Phi_t(b, q),
 // i.e. D[m = (b, f)][n = a] = A[m][k] B[n][k]^T with A = G (K-major) and
-// B = Psi (K-major), one GEMM of M = 512 x N = 64 x K = 256 per row-field
-// pair.
+// B = Psi (K-major), one GEMM of M = 512 x N = 64 x K = 256 per row field.
 //
-// Work split.  One CTA per (element, pair of row fields h: i in {2h, 2h+1}),
-// 256 threads, about 109 KiB of shared memory so that two CTAs share an SM
-// and one CTA's scatter overlaps the other's operand build.  Four M = 128
-// accumulator tiles (tile T: row field 2h + T/2, basis b in [32 (T&1), +32),
-// tile row m = 4 (b mod 32) + f) live in 4 x 64 = 256 TMEM columns.
-//   prologue  FP64 state at the 64 points (thread per point and quarter of
-//             the basis, quarters summed in shared memory), FP64 coefficients
-//             M_q, rc_q of the two row fields (thread per field, point and
-//             pair of column fields; stored FP32 / FP64), FP64 residual -> rhs;
-//   8 chunks  of 8 points (K = 32): the FP32 basis of chunk c+1 is copied
-//             (cp.async) into the other buffer while chunk c builds Psi and G
-//             as BF16 in the 64-byte-swizzled K-major layout; one thread issues
-//             4 tiles x 2 tcgen05.mma (128 x 64 x 16) and commits to an mbarrier;
-//             the next chunk waits on it before overwriting the operands;
-//   epilogue  tcgen05.ld rows (b, f) x 32 columns a of both row fields; shuffles
-//             inside each lane quad give every lane the four f of one (a, b,
-//             row field), and the two row fields of one (a, b) -- the two
-//             halves of a 32-byte sector -- go out from adjacent lanes of the
-//             same red.global.add.v4.f32 instruction.
+// Two kernels.
+//   TangentPointKernel (FP64, CTA per element, 256 threads): nodal state, the
+//     state at the 64 points (thread per point and quarter of the basis, the
+//     quarters summed in shared memory), the coefficients M_q of all four row
+//     fields (thread per row field and point, two column-field halves through
+//     a shared-memory scratch) written to a coefficient array laid out
+//     [element][row field][80 coefficients][64 points] (coalesced over the
+//     points), and the FP64 residual (thread per row field and basis
+//     function) added into rhs.
+//   TangentTcKernel (CTA per element and row-field pair h: i in {2h, 2h+1},
+//     256 threads, 4 M = 128 accumulator tiles in 256 TMEM columns; tile T:
+//     row field 2h + T/2, basis b in [32 (T&1), +32), tile row m = 4 (b mod
+//     32) + f): K chunks of NP points; the FP32 basis and the two row fields'
+//     coefficients of chunk c+2 are copied (cp.async) into the buffers chunk
+//     c has just consumed, and the operand tiles are double-buffered, so chunk
+//     c+1 is built while the MMAs of chunk c run.  Psi and G are written as
+//     BF16 in the 64-byte-swizzled K-major layout with K ordered (s, point)
+//     inside each point pair; the two points of a pair ride in one FP32
+//     register pair (fma.rn.f32x2), and a pair's two coefficients are one
+//     8-byte shared-memory load.  One thread issues the tile MMAs
+//     (tcgen05.mma.cta_group::1.kind::f16, M = 128, N = 64, K = 16) and
+//     commits them to the mbarrier of the operand buffer.  Epilogue:
+//     tcgen05.ld rows (b, f) x 32 columns a of both row fields; shuffles inside
+//     each lane quad give every lane the four f of one (a, b, row field), and
+//     the two row fields of one (a, b) -- the two halves of a 32-byte sector --
+//     go out from adjacent lanes of the same red.global.add.v4.f32.
 // Split mode (TFIGA_PRECISION_MIXED_BF16X3): every operand x is carried as
 // hi = bf16(x) and lo = bf16(x - hi), and the contraction takes the three
 // products hi.hi + hi.lo + lo.hi (the dropped lo.lo term is 2^-16 relative),
-// so the tangent is accurate to about 1e-5 instead of BF16's 2e-3.  The
-// shared-memory layout is unchanged: chunks hold 4 points (K = 16), and each
-// 64-byte swizzled row carries the hi values in its first 32 bytes and the lo
-// values in its last 32; the three MMAs of a tile start their A / B
-// descriptors at byte 0 or 32 of the row.
+// so the tangent is accurate to about 1e-5 instead of BF16's 2e-3.  Chunks
+// hold 4 points (K = 16) and each 64-byte swizzled row carries the hi values
+// in its first 32 bytes and the lo values in its last 32; the three MMAs of a
+// tile start their A / B descriptors at byte 0 or 32 of the row.  Plain mode:
+// chunks of 8 points, K = 32 per row, two K = 16 MMAs per tile.
 // Every mbarrier wait is bounded (one second of globaltimer); on expiry the
 // CTA records TFIGA status bit 1, waits once more (bounded) for its own MMAs,
 // frees its tensor memory and returns without writing the tangent.
@@ -52,34 +58,39 @@ namespace tfiga {
 namespace {
 
 constexpr int kTcThreads = 256;
-constexpr int kPts = 8;                          // quadrature points per K chunk (buffers sized for 8)
+constexpr int kMaxPts = 8;                       // points per K chunk (plain); split uses 4
 constexpr int kTiles = 4;                        // M = 128 tiles per CTA
 constexpr int kTileBytes = 128*64;               // 128 rows x 32 BF16 (64 B, one swizzle row)
 constexpr int kTmemCols = 256;                   // 4 tiles x N = 64 FP32 columns
 constexpr unsigned long long kWaitNs = 1000000000ull;
-constexpr int kCoefStride = kCoef+1;             // odd float stride: point-per-thread writes hit distinct banks
 constexpr int kRcStride = 5;                     // doubles per (field, point) residual coefficient row
+constexpr int kPartStride = 23;                  // odd double stride of the point-state partial sums
+constexpr int kScratchStride = 41;               // odd float stride of the per-thread coefficient scratch
 
-// Shared-memory layout (bytes from a 1024-aligned base).  The prologue's
-// point-state partial sums alias the operand tiles and the first basis
-// buffer; the second basis buffer aliases the point state once the
-// coefficients are built.
-constexpr int kPhiBytes = kFeatures*kPts*64*4;                   // float [5][kPts][64] per chunk
-constexpr int kPartStride = 23;                                  // odd double stride of the partial sums
-constexpr int kOffA = 0;                                         // 4 tiles x 8 KiB
-constexpr int kOffB = kOffA+kTiles*kTileBytes;                   // Psi: 64 rows x 64 B
-constexpr int kOffPhi0 = kOffB+64*64;                            // basis chunk buffer 0
-constexpr int kOffPart = 0;                                      // double [4][64][kPartStride] (prologue)
-constexpr int kOffQS = kOffPhi0+kPhiBytes;                       // double [64][kQS]; later basis buffer 1
-constexpr int kOffCoef = kOffQS+kQuad*kQS*8;                     // float [2][64][kCoefStride]
-constexpr int kOffRC = kOffCoef+2*kQuad*kCoefStride*4;           // double [2][64][kRcStride]
-constexpr int kOffU = kOffRC+2*kQuad*kRcStride*8;                // double [4 fields][64]
-constexpr int kOffUp = kOffU+64*4*8;                             // double [4 fields][64]
-constexpr int kOffBar = kOffUp+64*4*8;                           // mbarrier, TMEM slot
-constexpr int kSmemBytes = kOffBar+16+1024;                      // + alignment slack
-static_assert(kSmemBytes <= 113*1024, "two CTAs per SM");
-static_assert(4*64*kPartStride*8 <= kOffQS, "partial sums fit below the point state");
-static_assert(kPhiBytes <= kQuad*kQS*8, "basis buffer 1 fits in the point-state region");
+// TangentTcKernel shared memory (bytes from a 1024-aligned base).
+constexpr int kOperandBytes = kTiles*kTileBytes+64*64;            // A tiles + B (Psi: 64 rows x 64 B)
+constexpr int kOffOp0 = 0;                                        // operand buffer 0
+constexpr int kOffOp1 = kOperandBytes;                            // operand buffer 1 (36 KiB, 1024-aligned)
+constexpr int kPhiBytes = kFeatures*kMaxPts*64*4;                 // float [5][NP][64] per chunk
+constexpr int kOffPhi0 = 2*kOperandBytes;
+constexpr int kOffPhi1 = kOffPhi0+kPhiBytes;
+constexpr int kCfBytes = 2*kCoef*kMaxPts*4;                       // float [2 rows][80][NP] per chunk
+constexpr int kOffCf0 = kOffPhi1+kPhiBytes;
+constexpr int kOffCf1 = kOffCf0+kCfBytes;
+constexpr int kOffBar = kOffCf1+kCfBytes;                         // 2 mbarriers, TMEM slot
+constexpr int kTcSmemBytes = kOffBar+32+1024;                     // + alignment slack
+static_assert(kTcSmemBytes <= 113*1024, "two CTAs per SM");
+static_assert(kOffOp1 % 1024 == 0, "operand buffers 1024-aligned");
+
+// TangentPointKernel shared memory (bytes).
+constexpr int kPtOffU = 0;                                        // double [4 fields][64]
+constexpr int kPtOffUp = kPtOffU+64*4*8;                          // double [4 fields][64]
+constexpr int kPtOffPart = kPtOffUp+64*4*8;                       // double [4][64][kPartStride]
+constexpr int kPtPartBytes = 4*64*kPartStride*8;                  // (later: float [256][kScratchStride])
+constexpr int kPtOffQS = kPtOffPart+kPtPartBytes;                 // double [64][kQS]
+constexpr int kPtOffRC = kPtOffQS+kQuad*kQS*8;                    // double [4][64][kRcStride]
+constexpr int kPtSmemBytes = kPtOffRC+4*kQuad*kRcStride*8;
+static_assert(kTcThreads*kScratchStride*4 <= kPtPartBytes, "coefficient scratch fits in the partial sums");
 
 // Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B BF16, both
 // K-major, M = 128, N = 64.
@@ -165,18 +176,6 @@ template <int N> __device__ __forceinline__ void CopyAsyncWait()
 	asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
 }
 
-// Basis chunk c (points NP c .. NP c + NP - 1, five features, 64 functions) of
-// one element, FP32, into a [5][NP][64] buffer: 5 NP 16 16-byte copies.
-template <int NP>
-__device__ __forceinline__ void PrefetchPhi(const float* P32, int c, uint32_t dst, int tid)
-{
-	for (int idx = tid; idx < kFeatures*NP*16; idx += kTcThreads) {
-		const int t = idx/(NP*16), rem = idx%(NP*16);
-		CopyAsync16(dst+16*idx, P32+(size_t)(t*kQuad+c*NP)*kMaxBasis+4*rem);
-	}
-	CopyAsyncCommit();
-}
-
 // 32 lanes x 32 consecutive FP32 columns: thread l gets row (lane base + l), columns c..c+31.
 __device__ __forceinline__ void TmemLoad32(uint32_t taddr, float v[32])
 {
@@ -211,6 +210,47 @@ __device__ __forceinline__ float Bf16Residual(float x)
 	return x-__bfloat162float(__float2bfloat16_rn(x));
 }
 
+// Two FP32 values in one 64-bit register pair (first value in the low half), for the packed
+// FP32 pipe of sm_100 (fma / sub .f32x2: one instruction for both halves).
+__device__ __forceinline__ unsigned long long Pack2(float lo, float hi)
+{
+	unsigned long long d;
+	asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+	return d;
+}
+__device__ __forceinline__ float Low(unsigned long long v) { return __uint_as_float((uint32_t)v); }
+__device__ __forceinline__ float High(unsigned long long v) { return __uint_as_float((uint32_t)(v >> 32)); }
+__device__ __forceinline__ unsigned long long Fma2(unsigned long long a, unsigned long long b, unsigned long long c)
+{
+	unsigned long long d;
+	asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+	return d;
+}
+__device__ __forceinline__ unsigned long long Mul2(unsigned long long a, unsigned long long b)
+{
+	unsigned long long d;
+	asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+	return d;
+}
+__device__ __forceinline__ unsigned long long Sub2(unsigned long long a, unsigned long long b)
+{
+	unsigned long long d;
+	asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+	return d;
+}
+
+// BF16 pair of a packed FP32 pair (low half -> low 16 bits).
+__device__ __forceinline__ uint32_t Bf16Pair(unsigned long long v)
+{
+	return PackBf16(Low(v), High(v));
+}
+
+// The FP32 pair a BF16 pair stands for (exact).
+__device__ __forceinline__ unsigned long long WidenBf16Pair(uint32_t h)
+{
+	return Pack2(__uint_as_float(h << 16), __uint_as_float(h & 0xffff0000u));
+}
+
 __device__ __forceinline__ void StoreShared16(uint32_t address, uint32_t a, uint32_t b, uint32_t c, uint32_t d)
 {
 	asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" :: "r"(address), "r"(a), "r"(b), "r"(c), "r"(d)
@@ -223,41 +263,43 @@ __device__ __forceinline__ void RedAdd4(float* p, float a, float b, float c, flo
 		: "memory");
 }
 
-template <bool kSplit>
-__global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView mesh,
-	const double* __restrict__ phi, const float* __restrict__ phi32, const double* __restrict__ qdata,
-	const int32_t* __restrict__ element_blocks, const double* __restrict__ state,
-	const double* __restrict__ previous, AssemblyParams prm, float* __restrict__ values, double* __restrict__ rhs,
-	int* __restrict__ status)
+
+// Basis chunk c (points NP c .. NP c + NP - 1, five features, 64 functions) of
+// one element, FP32, into a [5][NP][64] buffer; the coefficients of the two row
+// fields 2h, 2h+1 at those points into a [2][80][NP] buffer.  One commit group.
+template <int NP>
+__device__ __forceinline__ void PrefetchChunk(const float* P32, const float* CF, int c, uint32_t phi_dst,
+	uint32_t cf_dst, int tid)
+{
+	for (int idx = tid; idx < kFeatures*NP*16; idx += kTcThreads) {
+		const int t = idx/(NP*16), rem = idx%(NP*16);
+		CopyAsync16(phi_dst+16*idx, P32+(size_t)(t*kQuad+c*NP)*kMaxBasis+4*rem);
+	}
+	for (int idx = tid; idx < 2*kCoef*NP/4; idx += kTcThreads) {
+		const int rk = idx/(NP/4), part = idx%(NP/4);           // rk = row field * 80 + k
+		CopyAsync16(cf_dst+16*idx, CF+(size_t)rk*kQuad+c*NP+4*part);
+	}
+	CopyAsyncCommit();
+}
+
+__global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshView mesh,
+	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ state,
+	const double* __restrict__ previous, AssemblyParams prm, float* __restrict__ coef, double* __restrict__ rhs)
 {
 	extern __shared__ uint8_t smem_raw[];
-	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+1023) & ~uintptr_t(1023));
-	const uint32_t sA = SmemAddress(sm+kOffA), sB = SmemAddress(sm+kOffB);
-	const uint32_t sPhi[2] = {SmemAddress(sm+kOffPhi0), SmemAddress(sm+kOffQS)};
-	double* Part = reinterpret_cast<double*>(sm+kOffPart);
-	float* Coef = reinterpret_cast<float*>(sm+kOffCoef);
-	double* RC = reinterpret_cast<double*>(sm+kOffRC);
-	double* QS = reinterpret_cast<double*>(sm+kOffQS);
-	double* U = reinterpret_cast<double*>(sm+kOffU);
-	double* Up = reinterpret_cast<double*>(sm+kOffUp);
-	uint64_t* bar = reinterpret_cast<uint64_t*>(sm+kOffBar);
-	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm+kOffBar+8);
+	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+15) & ~uintptr_t(15));
+	double* U = reinterpret_cast<double*>(sm+kPtOffU);
+	double* Up = reinterpret_cast<double*>(sm+kPtOffUp);
+	double* Part = reinterpret_cast<double*>(sm+kPtOffPart);
+	float* Scratch = reinterpret_cast<float*>(sm+kPtOffPart);
+	double* QS = reinterpret_cast<double*>(sm+kPtOffQS);
+	double* RC = reinterpret_cast<double*>(sm+kPtOffRC);
 
-	const int e = blockIdx.x >> 1;
-	const int h = blockIdx.x & 1;
-	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const int e = blockIdx.x;
+	const int tid = threadIdx.x;
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
-	const float* P32 = phi32+(size_t)e*kFeatures*kQuad*kMaxBasis;
-
-	// Tensor memory for the four accumulator tiles; the mbarrier.
-	if (warp == 0) {
-		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-			:: "r"(SmemAddress(tmem_slot)), "r"(kTmemCols) : "memory");
-		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-	}
-	if (tid == 32) MbarInit(bar);
 
 	// 1. Nodal state.
 	if (tid < kMaxBasis) {
@@ -271,10 +313,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		U[a] = s0; U[64+a] = s1; U[128+a] = s2; U[192+a] = s3;
 		Up[a] = p0; Up[64+a] = p1; Up[128+a] = p2; Up[192+a] = 0.0;
 	}
-	FenceBeforeSync();
 	__syncthreads();
-	FenceAfterSync();
-	const uint32_t tmem = *tmem_slot;
 
 	// 2. State at every point (FP64): thread (point q, quarter aq of the basis)
 	//    sums 16 functions; the four quarters meet in shared memory.
@@ -314,14 +353,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		QS[q*kQS+k] = ((part[0]+part[kQuad*kPartStride])+part[2*kQuad*kPartStride])+part[3*kQuad*kPartStride];
 	}
 	__syncthreads();
-	constexpr int NP = kSplit ? 4 : kPts;        // points per K chunk
-	constexpr int kChunks = kQuad/NP;
-	PrefetchPhi<NP>(P32, 0, sPhi[0], tid);       // chunk 0: the partial sums are dead
 
-	// 3. Coefficients: thread (row field il, point q, column-field pair fp); fp = 0 also
-	//    gives the residual coefficients.
+	// 3. Coefficients: thread (row field il, point q), two column-field halves through the
+	//    scratch (the partial sums are dead), stored coalesced over the points.
 	{
-		const int q = tid & 63, fp = (tid >> 6) & 1, il = tid >> 7;
+		const int q = tid & 63, il = tid >> 6;
 		PointState S;
 		const double* s = QS+q*kQS;
 		for (int c = 0; c < 3; ++c) {
@@ -329,51 +365,93 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 			for (int d = 0; d < 3; ++d) S.gv[c][d] = s[kGrad+3*c+d];
 		}
 		S.p = s[kP];
-		RowCoefficients<float>(2*h+il, S, qdata+((size_t)e*kQuad+q)*kQData, prm, Coef+(il*kQuad+q)*kCoefStride,
-			fp == 0 ? RC+(il*kQuad+q)*kRcStride : nullptr, 2*fp, 2*fp+2);
+		const double* qd = qdata+((size_t)e*kQuad+q)*kQData;
+		float* scratch = Scratch+tid*kScratchStride;
+		float* out = coef+((size_t)e*4+il)*kCoef*kQuad+q;
+		for (int half = 0; half < 2; ++half) {
+			RowCoefficients<float>(il, S, qd, prm, scratch, half == 0 ? RC+(il*kQuad+q)*kRcStride : nullptr,
+				2*half, 2*half+2);
+			#pragma unroll 8
+			for (int k = 0; k < 40; ++k) out[(size_t)(half*40+k)*kQuad] = scratch[k];
+		}
 	}
 	__syncthreads();
 
-	// 4. FP64 residual of the two row fields (rhs holds -r): thread (il, half, a).
+	// 4. FP64 residual of the four row fields (rhs holds -r): thread (il, a).
 	{
-		const int il = tid >> 7, half = (tid >> 6) & 1, a = tid & 63;
+		const int il = tid >> 6, a = tid & 63;
 		double r = 0.0;
-		for (int q = half*32; q < half*32+32; ++q)
+		for (int q = 0; q < kQuad; ++q) {
+			const double* rc = RC+(il*kQuad+q)*kRcStride;
 			#pragma unroll
-			for (int s = 0; s < 4; ++s) r += P[(s*kQuad+q)*kMaxBasis+a]*RC[(il*kQuad+q)*kRcStride+s];
-		QS[tid] = r;                           // the point state is dead: reuse it for the halves
-		__syncthreads();
-		if (half == 0 && a < nen)
-			atomicAdd(rhs+4*(size_t)mesh.connectivity[begin+a]+2*h+il, QS[tid]+QS[tid+64]);
-		__syncthreads();
+			for (int s = 0; s < 4; ++s) r += P[(s*kQuad+q)*kMaxBasis+a]*rc[s];
+		}
+		if (a < nen) atomicAdd(rhs+4*(size_t)mesh.connectivity[begin+a]+il, r);
 	}
+}
 
-	// 5. Tangent chunks.  Basis chunk c+1 is copied into the other buffer while chunk c is built.
-	const int gil = warp >> 2, gqp = warp & 3;     // G builder: row field, point pair
+template <bool kSplit>
+__global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView mesh,
+	const float* __restrict__ phi32, const float* __restrict__ coef, const int32_t* __restrict__ element_blocks,
+	float* __restrict__ values, int* __restrict__ status)
+{
+	constexpr int NP = kSplit ? 4 : kMaxPts;     // points per K chunk
+	constexpr int kChunks = kQuad/NP;
+	extern __shared__ uint8_t smem_raw[];
+	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+1023) & ~uintptr_t(1023));
+	const uint32_t sOp[2] = {SmemAddress(sm+kOffOp0), SmemAddress(sm+kOffOp1)};
+	const uint32_t sPhi[2] = {SmemAddress(sm+kOffPhi0), SmemAddress(sm+kOffPhi1)};
+	const uint32_t sCf[2] = {SmemAddress(sm+kOffCf0), SmemAddress(sm+kOffCf1)};
+	uint64_t* bars = reinterpret_cast<uint64_t*>(sm+kOffBar);
+	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm+kOffBar+16);
+
+	const int e = blockIdx.x >> 1;
+	const int h = blockIdx.x & 1;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const int begin = mesh.element_offsets[e];
+	const int nen = mesh.element_offsets[e+1]-begin;
+	const float* P32 = phi32+(size_t)e*kFeatures*kQuad*kMaxBasis;
+	const float* CF = coef+((size_t)e*4+2*h)*kCoef*kQuad;
+
+	PrefetchChunk<NP>(P32, CF, 0, sPhi[0], sCf[0], tid);
+	PrefetchChunk<NP>(P32, CF, 1, sPhi[1], sCf[1], tid);
+	// Tensor memory for the four accumulator tiles; one mbarrier per operand buffer.
+	if (warp == 0) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+			:: "r"(SmemAddress(tmem_slot)), "r"(kTmemCols) : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	if (tid == 32) { MbarInit(bars); MbarInit(bars+1); }
+	FenceBeforeSync();
+	__syncthreads();
+	FenceAfterSync();
+	const uint32_t tmem = *tmem_slot;
+
+	// Chunks.  Chunk c builds operand buffer c & 1 once the MMAs of chunk c - 2 (the last users
+	// of that buffer) have completed; chunk c's basis and coefficients came in two chunks ago.
+	const int gil = warp >> 2, gqp = warp & 3;     // G builder: row field, point pair / b quarter
 	const int gf = lane & 3, gbs = lane >> 2;       //            column field, basis sub-index
 	bool failed = false;
-	uint32_t pending = 0;                            // parity of the last committed chunk
+	int issued = 0;                                  // chunks whose MMAs were committed
 	for (int c = 0; c < kChunks; ++c) {
-		const int q0 = c*NP;
-		const float* PhiS = reinterpret_cast<const float*>(sm+(c & 1 ? kOffQS : kOffPhi0));
-		if (c+1 < kChunks) {
-			PrefetchPhi<NP>(P32, c+1, sPhi[(c+1) & 1], tid);
-			CopyAsyncWait<1>();
-		} else {
-			CopyAsyncWait<0>();
-		}
+		const int buf = c & 1;
+		const float* PhiS = reinterpret_cast<const float*>(sm+(buf ? kOffPhi1 : kOffPhi0));
+		const float* CfS = reinterpret_cast<const float*>(sm+(buf ? kOffCf1 : kOffCf0));
+		CopyAsyncWait<1>();                      // all groups but the newest: chunk c is here
 		bool ok = true;
-		if (c > 0) ok = MbarWaitBounded(bar, pending);
+		if (c >= 2) ok = MbarWaitBounded(bars+buf, (uint32_t)(((c-2) >> 1) & 1));
 		if (__syncthreads_or(!ok)) { failed = true; break; }
+		const uint32_t sA = sOp[buf], sB = sOp[buf]+kTiles*kTileBytes;
 
-		// B = Psi: row a, K = (point, s); thread (a, 16-byte unit u of the row).  Plain: unit u is
-		// point pair u.  Split: units 0, 1 hold hi of point pairs 0, 1 and units 2, 3 their lo.
+		// B = Psi: row a, K = (s, point) inside each 16-byte unit (k = 2 s + point of the pair);
+		// thread (a, 16-byte unit u of the row).  Plain: unit u is point pair u.  Split: units 0, 1
+		// hold hi of point pairs 0, 1 and units 2, 3 their lo.
 		{
 			const int a = tid >> 2, u = tid & 3;
 			const int qp = kSplit ? (u & 1) : u;
 			float x[8];
 			#pragma unroll
-			for (int k = 0; k < 8; ++k) x[k] = PhiS[((k & 3)*NP+2*qp+(k >> 2))*64+a];
+			for (int k = 0; k < 8; ++k) x[k] = PhiS[((k >> 1)*NP+2*qp+(k & 1))*64+a];
 			if (kSplit && u >= 2) {
 				#pragma unroll
 				for (int k = 0; k < 8; ++k) x[k] = Bf16Residual(x[k]);
@@ -381,41 +459,43 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 			StoreShared16(sB+Sw64(a, u), PackBf16(x[0], x[1]), PackBf16(x[2], x[3]), PackBf16(x[4], x[5]),
 				PackBf16(x[6], x[7]));
 		}
-		// A = G: row (b, f) of tile (il, b / 32), K = (point, s).  Plain: warp (il, point pair) over all
-		// b.  Split: warp (il, point pair, half of the b groups), writing hi and lo units.
+		// A = G: row (b, f) of tile (il, b / 32).  Plain: warp (il, point pair) over all b.  Split:
+		// warp (il, point pair, half of the b groups), writing hi and lo units.  Both points of
+		// the pair ride in one register pair: coefficients mm[k] = (M_q0, M_q1)[k] (one 8-byte
+		// load from the [2][80][NP] chunk), basis pb[t] = (Phi_t(q0, b), Phi_t(q1, b)).
 		{
 			const int qpair = kSplit ? (gqp & 1) : gqp;
 			const int ql0 = 2*qpair;
 			constexpr int kGroups = kSplit ? 4 : 8;
 			const int g0 = kSplit ? (gqp >> 1)*4 : 0;
-			float m0[20], m1[20];
-			const float* c0 = Coef+(gil*kQuad+q0+ql0)*kCoefStride+gf*20;
+			unsigned long long mm[20];
+			const float* c0 = CfS+(gil*kCoef+gf*20)*NP+ql0;
 			#pragma unroll
-			for (int k = 0; k < 20; ++k) { m0[k] = c0[k]; m1[k] = c0[kCoefStride+k]; }
+			for (int k = 0; k < 20; ++k) mm[k] = *reinterpret_cast<const unsigned long long*>(c0+k*NP);
 			#pragma unroll 2
 			for (int j = 0; j < kGroups; ++j) {
 				const int b = (g0+j)*8+gbs;
-				float p0[5], p1[5];
+				unsigned long long pb[5];
 				#pragma unroll
-				for (int t = 0; t < 5; ++t) {
-					p0[t] = PhiS[(t*NP+ql0)*64+b];
-					p1[t] = PhiS[(t*NP+ql0+1)*64+b];
-				}
-				float g[8];
+				for (int t = 0; t < 5; ++t) pb[t] = Pack2(PhiS[(t*NP+ql0)*64+b], PhiS[(t*NP+ql0+1)*64+b]);
+				unsigned long long gg[4];
 				#pragma unroll
 				for (int s = 0; s < 4; ++s) {
-					g[s] = m0[s*5]*p0[0]+m0[s*5+1]*p0[1]+m0[s*5+2]*p0[2]+m0[s*5+3]*p0[3]+m0[s*5+4]*p0[4];
-					g[4+s] = m1[s*5]*p1[0]+m1[s*5+1]*p1[1]+m1[s*5+2]*p1[2]+m1[s*5+3]*p1[3]+m1[s*5+4]*p1[4];
+					gg[s] = Mul2(mm[s*5], pb[0]);
+					#pragma unroll
+					for (int t = 1; t < 5; ++t) gg[s] = Fma2(mm[s*5+t], pb[t], gg[s]);
 				}
 				const int tile = gil*2+(b >> 5), row = (b & 31)*4+gf;
 				const uint32_t dst = sA+tile*kTileBytes;
-				StoreShared16(dst+Sw64(row, qpair), PackBf16(g[0], g[1]), PackBf16(g[2], g[3]),
-					PackBf16(g[4], g[5]), PackBf16(g[6], g[7]));
+				uint32_t hi[4];
+				#pragma unroll
+				for (int s = 0; s < 4; ++s) hi[s] = Bf16Pair(gg[s]);
+				StoreShared16(dst+Sw64(row, qpair), hi[0], hi[1], hi[2], hi[3]);
 				if (kSplit) {
+					uint32_t lo[4];
 					#pragma unroll
-					for (int k = 0; k < 8; ++k) g[k] = Bf16Residual(g[k]);
-					StoreShared16(dst+Sw64(row, 2+qpair), PackBf16(g[0], g[1]), PackBf16(g[2], g[3]),
-						PackBf16(g[4], g[5]), PackBf16(g[6], g[7]));
+					for (int s = 0; s < 4; ++s) lo[s] = Bf16Pair(Sub2(gg[s], WidenBf16Pair(hi[s])));
+					StoreShared16(dst+Sw64(row, 2+qpair), lo[0], lo[1], lo[2], lo[3]);
 				}
 			}
 		}
@@ -436,18 +516,22 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 						MmaBf16(tmem+tile*64, DescSw64(a+ks*32), DescSw64(sB+ks*32), (c > 0 || ks > 0) ? 1u : 0u);
 				}
 			}
-			MmaCommit(bar);
+			MmaCommit(bars+buf);
 		}
-		pending = (uint32_t)(c & 1);
+		issued = c+1;
+		// the staging buffers of chunk c are free: fetch chunk c + 2 into them (an empty group at the end)
+		if (c+2 < kChunks) PrefetchChunk<NP>(P32, CF, c+2, sPhi[buf], sCf[buf], tid);
+		else CopyAsyncCommit();
 	}
-	if (!failed) failed = __syncthreads_or(!MbarWaitBounded(bar, pending)) != 0;
+	if (!failed)
+		failed = __syncthreads_or(!MbarWaitBounded(bars+((kChunks-1) & 1), (uint32_t)(((kChunks-1) >> 1) & 1))) != 0;
 
 	if (!failed) {
-		// 6. Epilogue: warp -> (basis half bh = warp/4 of b, TMEM lane quarter warp%4); both row fields.
-		//    Lane f of a quad holds column field f of node b for every a.  In pass p the quad's lanes
-		//    write (a = 4g + (f & 2) + p, row field 2h + (f & 1), all four column fields), so lanes
-		//    f, f^1 fill the two 16-byte halves of one 32-byte sector in the same instruction.  Each
-		//    round r of a pass sends to lane f^r the value it needs from this lane's column field.
+		// Epilogue: warp -> (basis half bh = warp/4 of b, TMEM lane quarter warp%4); both row fields.
+		// Lane f of a quad holds column field f of node b for every a.  In pass p the quad's lanes
+		// write (a = 4g + (f & 2) + p, row field 2h + (f & 1), all four column fields), so lanes
+		// f, f^1 fill the two 16-byte halves of one 32-byte sector in the same instruction.  Each
+		// round r of a pass sends to lane f^r the value it needs from this lane's column field.
 		FenceAfterSync();
 		const int bh = warp >> 2, quarter = warp & 3;
 		const int32_t* EB = element_blocks+(size_t)e*kMaxBasis*kMaxBasis;
@@ -486,8 +570,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		}
 	} else {
 		if (tid == 0) atomicOr(status, 1);
-		CopyAsyncWait<0>();                     // this thread's basis copies in flight
-		MbarWaitBounded(bar, pending);          // let this CTA's own MMAs drain before freeing TMEM
+		CopyAsyncWait<0>();                     // this thread's copies in flight
+		// let this CTA's own MMAs drain before freeing TMEM: the newest commit covers all earlier ones
+		if (issued > 0) MbarWaitBounded(bars+((issued-1) & 1), (uint32_t)(((issued-1) >> 1) & 1));
 	}
 	FenceBeforeSync();
 	__syncthreads();
@@ -502,25 +587,30 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 
 void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const float* phi32, const double* qdata,
 	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
-	float* values, double* rhs, int* status, bool split, cudaStream_t stream)
+	float* coef, float* values, double* rhs, int* status, bool split, cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
 	static bool configured = false;
 	if (!configured) {
+		CudaCheck(cudaFuncSetAttribute(TangentPointKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
 		CudaCheck(cudaFuncSetAttribute(TangentTcKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			kSmemBytes), "tensor-core tangent shared-memory attribute");
+			kTcSmemBytes), "tensor-core tangent shared-memory attribute");
 		CudaCheck(cudaFuncSetAttribute(TangentTcKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			kSmemBytes), "tensor-core tangent shared-memory attribute");
+			kTcSmemBytes), "tensor-core tangent shared-memory attribute");
 		configured = true;
 	}
 	const long long ctas = 2LL*mesh.elements;
 	if (ctas > 0x7fffffffLL) Fail(-7, "too many elements for one tangent launch");
+	TangentPointKernel<<<(unsigned)mesh.elements, kTcThreads, kPtSmemBytes+16, stream>>>(mesh, phi, qdata, state,
+		previous, params, coef, rhs);
+	LaunchCheck("TangentPointKernel");
 	if (split)
-		TangentTcKernel<true><<<(unsigned)ctas, kTcThreads, kSmemBytes, stream>>>(mesh, phi, phi32, qdata,
-			element_blocks, state, previous, params, values, rhs, status);
+		TangentTcKernel<true><<<(unsigned)ctas, kTcThreads, kTcSmemBytes, stream>>>(mesh, phi32, coef,
+			element_blocks, values, status);
 	else
-		TangentTcKernel<false><<<(unsigned)ctas, kTcThreads, kSmemBytes, stream>>>(mesh, phi, phi32, qdata,
-			element_blocks, state, previous, params, values, rhs, status);
+		TangentTcKernel<false><<<(unsigned)ctas, kTcThreads, kTcSmemBytes, stream>>>(mesh, phi32, coef,
+			element_blocks, values, status);
 	LaunchCheck("TangentTcKernel");
 }
 

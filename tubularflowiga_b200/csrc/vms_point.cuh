@@ -25,12 +25,12 @@ struct PointState {
 };
 
 // Coefficients of row field i at one point, all scaled by the point
-// measure: M[f*20 + s*5 + t] multiplies (test feature s of N_a) x (trial
-// feature t of N_b) in K^{if}_{ab}; rc[s] = -measure * c_s gives the
-// residual.  Computed in FP64; C is the storage type of M (double for the
-// FP64 tangent, float for the tensor-core tangent).  Only the column fields
-// f in [f_lo, f_hi) are written (M[f_lo*20 .. f_hi*20)); rc may be null.
-template <class C>
+// measure: M[((f - f_lo)*20 + s*5 + t)*kStride] multiplies (test feature s
+// of N_a) x (trial feature t of N_b) in K^{if}_{ab}; rc[s] = -measure * c_s
+// gives the residual.  Computed in FP64; C is the storage type of M (double
+// for the FP64 tangent, float for the tensor-core tangent).  Only the column
+// fields f in [f_lo, f_hi) are written; rc may be null.
+template <class C, int kStride = 1>
 __device__ void RowCoefficients(int i, const PointState& S, const double* qd, const AssemblyParams& prm,
 	C* M, double* rc, int f_lo = 0, int f_hi = 4)
 {
@@ -86,8 +86,8 @@ __device__ void RowCoefficients(int i, const PointState& S, const double* qd, co
 		for (int c = 0; c < 3; ++c)
 			A[c][f] = -dtau_m*R[c]-tau_m*((c == f ? idt : 0.0)+S.gv[c][f]);
 	}
-	for (int k = f_lo*20; k < f_hi*20; ++k) M[k] = C(0);
-	auto at = [&](int f, int s, int t) -> C& { return M[f*20+s*5+t]; };
+	for (int k = 0; k < (f_hi-f_lo)*20; ++k) M[k*kStride] = C(0);
+	auto at = [&](int f, int s, int t) -> C& { return M[((f-f_lo)*20+s*5+t)*kStride]; };
 	const int f_vel = f_hi < 3 ? f_hi : 3;     // end of the velocity columns in range
 	const bool p_col = f_hi > 3;               // pressure column in range
 	if (i < 3) {
@@ -129,7 +129,7 @@ __device__ void RowCoefficients(int i, const PointState& S, const double* qd, co
 		if (p_col)
 			for (int d = 0; d < 3; ++d) at(3, 1+d, 1+d) = tau_m/rho;
 	}
-	for (int k = f_lo*20; k < f_hi*20; ++k) M[k] = C(M[k]*meas);
+	for (int k = 0; k < (f_hi-f_lo)*20; ++k) M[k*kStride] = C(M[k*kStride]*meas);
 }
 
 } // namespace tfiga
