@@ -498,6 +498,7 @@ def main():
     asm_ms, asm_n = prof["assembly"]
     orth_ms, orth_n = prof["krylov_orthogonalisation"]
     amg_ms, amg_n = prof["amg_vcycle"]
+    res_ms, res_n = prof.get("residual", (0.0, 0))
     kernels = {}
     if mixed:
         # FP32 Jacobian: 4-byte values in every pass over the matrix
@@ -539,6 +540,15 @@ def main():
                              "frac": a / 37.0, "traffic": None, "launches": asm_n,
                              "avg_ms": asm_ms / asm_n, "share": asm_ms / ms,
                              "peak_note": "nominal B200 FP64 (no measured FP64 peak on this pool)"}
+    if res_n:
+        # FP64 residual + point coefficients of the tensor-core modes: per element it reads the FP64
+        # basis tables (5 x 64 x 64 doubles) and the point data (64 x 11 doubles) and writes the
+        # coefficients of four row fields (4 x 80 x 64 floats)
+        rbytes = tube.mesh.elements * (5 * 64 * 64 * 8 + 64 * 11 * 8 + 4 * 80 * 64 * 4)
+        a = rbytes / (res_ms / res_n * 1e-3) / 1e9
+        kernels["residual_point"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s", "frac": a / hbm,
+                                     "traffic": None, "launches": res_n, "avg_ms": res_ms / res_n,
+                                     "share": res_ms / ms, "algorithmic_bytes": rbytes}
     if orth_n:
         # algorithmic bytes of Arnoldi step j as the solver accounts them: s_v N (2j + 7) (one dot
         # pass, one update pass, the normalisation; s_v = 4 for the FP32 basis of the mixed solver)
@@ -552,7 +562,7 @@ def main():
                                                "algorithmic_bytes_per_launch": algo / orth_n,
                                                "moved_bytes_per_launch": orth_moved / orth_n,
                                                "moved_gbs": orth_moved / (orth_ms * 1e-3) / 1e9}
-    dominant = max((spmv_name, asm_name, "amg_vcycle", "krylov_orthogonalisation"),
+    dominant = max((spmv_name, asm_name, "amg_vcycle", "krylov_orthogonalisation", "residual_point"),
                    key=lambda k: kernels.get(k, {}).get("share", 0))
     roof = dict(kernels[dominant])
     roof["kernel"] = dominant

@@ -287,14 +287,17 @@ int tfiga_ns_stream(tfiga_ns* ns, void** stream);
 /* Per-kernel-family device timing with CUDA events recorded around each
  * launch on the handle's stream (the reference's PhaseProfile,
  * include/PhaseProfile.hpp:14-138, at kernel granularity).  Families:
- * 0 assembly, 1 SpMV (fused with the block-Jacobi apply in that mode),
- * 2 Krylov orthogonalisation, 3 AMG V-cycle. */
-#define TFIGA_PROFILE_FAMILIES 4
+ * 0 assembly (the tangent; in the tensor-core modes the tcgen05 kernel),
+ * 1 SpMV (fused with the block-Jacobi apply in that mode), 2 Krylov
+ * orthogonalisation, 3 AMG V-cycle, 4 the FP64 residual and point
+ * coefficients of the tensor-core modes (0 elsewhere: the FP64 kernel does
+ * both in family 0). */
+#define TFIGA_PROFILE_FAMILIES 5
 int tfiga_ns_set_profiling(tfiga_ns* ns, int enable);
 /* Totals since the last reset: milliseconds and launch counts per family. */
 int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int32_t reset);
 /* Bytes per family since the last reset, as the solver accounts them while
- * profiling is on: bytes[0..3] algorithmic, bytes[4..7] actually moved
+ * profiling is on: bytes[0..4] algorithmic, bytes[5..9] actually moved
  * (2 * TFIGA_PROFILE_FAMILIES entries).  Family 2, Krylov orthogonalisation:
  * algorithmic s_v n (2j + 7) per Arnoldi step j (+ 8 n for the stored
  * FGMRES vector), s_v the basis entry size; moved: both classical

@@ -382,7 +382,7 @@ class NavierStokes:
     def set_profiling(self, enable: bool):
         check(lib().tfiga_ns_set_profiling(self._h, int(enable)))
 
-    FAMILIES = ("assembly", "spmv", "krylov_orthogonalisation", "amg_vcycle")
+    FAMILIES = ("assembly", "spmv", "krylov_orthogonalisation", "amg_vcycle", "residual")
 
     def amg_info(self) -> dict:
         info = AmgInfo()
@@ -392,13 +392,14 @@ class NavierStokes:
 
     def profile_bytes(self) -> dict:
         """{family: (algorithmic bytes, moved bytes)} since the last profile reset."""
-        b = np.zeros(8)
+        n = len(self.FAMILIES)
+        b = np.zeros(2 * n)
         check(lib().tfiga_ns_profile_bytes(self._h, _p(b)))
-        return {f: (float(b[i]), float(b[4 + i])) for i, f in enumerate(self.FAMILIES)}
+        return {f: (float(b[i]), float(b[n + i])) for i, f in enumerate(self.FAMILIES)}
 
     def profile(self, reset=False) -> dict:
-        ms = np.zeros(4)
-        counts = np.zeros(4, np.int64)
+        ms = np.zeros(len(self.FAMILIES))
+        counts = np.zeros(len(self.FAMILIES), np.int64)
         check(lib().tfiga_ns_profile(self._h, _p(ms), _p(counts), int(reset)))
         return {f: (float(ms[i]), int(counts[i])) for i, f in enumerate(self.FAMILIES)}
 

@@ -101,7 +101,7 @@ void RequireDevice();
 // the launching stream.  Disabled by default; Collect() waits for the stream.
 class Profiler {
 public:
-	enum Family { kAssembly = 0, kSpmv = 1, kOrtho = 2, kOther = 3, kFamilies = 4 };
+	enum Family { kAssembly = 0, kSpmv = 1, kOrtho = 2, kOther = 3, kResidual = 4, kFamilies = 5 };
 	~Profiler();
 	void Enable(bool on) { enabled_ = on; }
 	bool enabled() const { return enabled_; }
@@ -120,10 +120,10 @@ private:
 	std::vector<Mark> pool_;
 	size_t used_ = 0;
 	int open_ = -1;
-	double ms_[kFamilies] = {0, 0, 0, 0};
-	long long count_[kFamilies] = {0, 0, 0, 0};
-	double bytes_[kFamilies] = {0, 0, 0, 0};
-	double moved_[kFamilies] = {0, 0, 0, 0};
+	double ms_[kFamilies] = {};
+	long long count_[kFamilies] = {};
+	double bytes_[kFamilies] = {};
+	double moved_[kFamilies] = {};
 };
 
 } // namespace tfiga

@@ -59,14 +59,17 @@ void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double*
 	double* values, double* rhs, cudaStream_t stream);
 
 // ---- tangent_tc.cu -----------------------------------------------------
-// Tensor-core tangent (BF16 operands, FP32 accumulation) ADDED into FP32
-// values, FP64 residual ADDED into rhs (= -r); status bit 1 set if an MMA
-// completion wait expired.  phi32 is the FP32 copy of phi (Mesh::phi32);
-// coef is workspace of elements x 4 x 80 x 64 floats (the point coefficients
-// passed from the FP64 point kernel to the tensor-core kernel).
-void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const float* phi32, const double* qdata,
-	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
-	float* coef, float* values, double* rhs, int* status, bool split, cudaStream_t stream);
+// Tensor-core tangent in two launches.  LaunchTangentPoint: FP64 point state,
+// the coefficients of all four row fields into coef (workspace of elements x 4
+// x 80 x 64 floats) and the FP64 residual ADDED into rhs (= -r).
+// LaunchTangentTc: the tangent contracted on the tcgen05 tensor cores from
+// coef and phi32 (the FP32 copy of phi, Mesh::phi32), BF16 or split-BF16
+// operands, FP32 accumulation, ADDED into the FP32 values; status bit 1 set if
+// an MMA completion wait expired.
+void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const double* qdata, const double* state,
+	const double* previous, AssemblyParams params, float* coef, double* rhs, cudaStream_t stream);
+void LaunchTangentTc(const DeviceMeshView& mesh, const float* phi32, const float* coef,
+	const int32_t* element_blocks, float* values, int* status, bool split, cudaStream_t stream);
 
 // ---- sparse.cu ----------------------------------------------------------
 // Matrix values are FP64 or FP32 (T = double / float); vectors are FP64.

@@ -32,6 +32,8 @@ public:
 	// values/rhs on the device: rhs = -r + traction.
 	void Assemble();
 	void ApplyDirichlet();
+	void ApplyDirichletRhs();       // rhs rows only (g - u on constrained entries)
+	void ApplyDirichletMatrix();    // Jacobian rows only (zero rows, unit diagonal)
 	GmresResult SolveLinear(double rtol, int max_iterations);
 	tfiga_newton_report NewtonIteration(double initial_residual);
 	tfiga_step_report Step();
@@ -80,6 +82,11 @@ private:
 		double continuity_l2, continuity_sum, net_flow, absolute_flow, imbalance;
 	};
 	void ApplyTractions(const std::map<int32_t, double>& traction);
+	// Tensor-core modes: the FP64 residual and point coefficients (rhs = -r + traction), then the
+	// tangent from those coefficients into the FP32 Jacobian (builds the AMG on first use).
+	void AssembleResidualTc();
+	void ApplyDirichletParts(bool matrix, bool rhs);
+	void AssembleTangentTc();
 	std::vector<OutletModel> OutletModels(const tfiga_outlet* outlets, int count) const;
 	void LaunchDiagnostics();     // continuity sums of rhs + per-label flows of state
 	Diagnostics ReadDiagnostics();
@@ -87,7 +94,7 @@ private:
 	Mesh& mesh_;
 	tfiga_ns_params params_;
 	cudaStream_t stream_ = nullptr;
-	cudaEvent_t events_[4] = {};
+	cudaEvent_t events_[6] = {};
 	long long launches_ = 0;
 	long long solves_ = 0;                   // linear solves so far (coarse refresh period)
 	std::map<int32_t, double> tractions_;    // label -> pressure set by SetTractions

@@ -18,8 +18,9 @@
 //     fields (thread per row field and point, two column-field halves through
 //     a shared-memory scratch) written to a coefficient array laid out
 //     [element][row field][80 coefficients][64 points] (coalesced over the
-//     points), and the FP64 residual (thread per row field and basis
-//     function) added into rhs.
+//     points), and the FP64 residual (thread per basis function and quarter
+//     of the points, one read of each basis value for the four row fields)
+//     added into rhs.
 //   TangentTcKernel (CTA per element and row-field pair h: i in {2h, 2h+1},
 //     256 threads, 4 M = 128 accumulator tiles in 256 TMEM columns; tile T:
 //     row field 2h + T/2, basis b in [32 (T&1), +32), tile row m = 4 (b mod
@@ -377,15 +378,27 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 	}
 	__syncthreads();
 
-	// 4. FP64 residual of the four row fields (rhs holds -r): thread (il, a).
+	// 4. FP64 residual of the four row fields (rhs holds -r): thread (basis function a, quarter
+	//    qq of the points) reads each basis value once for all four row fields; the quarters meet
+	//    in shared memory (the coefficient scratch is dead).
 	{
-		const int il = tid >> 6, a = tid & 63;
-		double r = 0.0;
-		for (int q = 0; q < kQuad; ++q) {
-			const double* rc = RC+(il*kQuad+q)*kRcStride;
+		const int a = tid & 63, qq = tid >> 6;
+		double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
+		for (int q = qq*16; q < qq*16+16; ++q) {
 			#pragma unroll
-			for (int s = 0; s < 4; ++s) r += P[(s*kQuad+q)*kMaxBasis+a]*rc[s];
+			for (int s = 0; s < 4; ++s) {
+				const double v = P[(s*kQuad+q)*kMaxBasis+a];
+				r0 += v*RC[(0*kQuad+q)*kRcStride+s];
+				r1 += v*RC[(1*kQuad+q)*kRcStride+s];
+				r2 += v*RC[(2*kQuad+q)*kRcStride+s];
+				r3 += v*RC[(3*kQuad+q)*kRcStride+s];
+			}
 		}
+		double* red = Part;                     // [4 quarters][4 row fields][64]
+		red[(qq*4+0)*64+a] = r0; red[(qq*4+1)*64+a] = r1; red[(qq*4+2)*64+a] = r2; red[(qq*4+3)*64+a] = r3;
+		__syncthreads();
+		const int il = tid >> 6;
+		const double r = ((red[(0*4+il)*64+a]+red[(1*4+il)*64+a])+red[(2*4+il)*64+a])+red[(3*4+il)*64+a];
 		if (a < nen) atomicAdd(rhs+4*(size_t)mesh.connectivity[begin+a]+il, r);
 	}
 }
@@ -585,15 +598,27 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 
 } // namespace
 
-void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const float* phi32, const double* qdata,
-	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
-	float* coef, float* values, double* rhs, int* status, bool split, cudaStream_t stream)
+void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const double* qdata, const double* state,
+	const double* previous, AssemblyParams params, float* coef, double* rhs, cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
 	static bool configured = false;
 	if (!configured) {
 		CudaCheck(cudaFuncSetAttribute(TangentPointKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
+		configured = true;
+	}
+	TangentPointKernel<<<(unsigned)mesh.elements, kTcThreads, kPtSmemBytes+16, stream>>>(mesh, phi, qdata, state,
+		previous, params, coef, rhs);
+	LaunchCheck("TangentPointKernel");
+}
+
+void LaunchTangentTc(const DeviceMeshView& mesh, const float* phi32, const float* coef,
+	const int32_t* element_blocks, float* values, int* status, bool split, cudaStream_t stream)
+{
+	if (mesh.elements == 0) return;
+	static bool configured = false;
+	if (!configured) {
 		CudaCheck(cudaFuncSetAttribute(TangentTcKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			kTcSmemBytes), "tensor-core tangent shared-memory attribute");
 		CudaCheck(cudaFuncSetAttribute(TangentTcKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -602,9 +627,6 @@ void LaunchTangentTc(const DeviceMeshView& mesh, const double* phi, const float*
 	}
 	const long long ctas = 2LL*mesh.elements;
 	if (ctas > 0x7fffffffLL) Fail(-7, "too many elements for one tangent launch");
-	TangentPointKernel<<<(unsigned)mesh.elements, kTcThreads, kPtSmemBytes+16, stream>>>(mesh, phi, qdata, state,
-		previous, params, coef, rhs);
-	LaunchCheck("TangentPointKernel");
 	if (split)
 		TangentTcKernel<true><<<(unsigned)ctas, kTcThreads, kTcSmemBytes, stream>>>(mesh, phi32, coef,
 			element_blocks, values, status);
