@@ -283,6 +283,20 @@ __device__ __forceinline__ void PrefetchChunk(const float* P32, const float* CF,
 	CopyAsyncCommit();
 }
 
+// Coefficients of row field kRow at one point: both column-field halves through the thread's
+// scratch, stored at out[k * 64] (coalesced over the points of a warp).
+template <int kRow>
+__device__ __forceinline__ void PointCoefficients(const PointState& S, const double* qd, const AssemblyParams& prm,
+	float* scratch, double* rc, float* out)
+{
+	RowCoefficients<float>(kRow, S, qd, prm, scratch, rc, 0, 2);
+	#pragma unroll 8
+	for (int k = 0; k < 40; ++k) out[(size_t)k*kQuad] = scratch[k];
+	RowCoefficients<float>(kRow, S, qd, prm, scratch, nullptr, 2, 4);
+	#pragma unroll 8
+	for (int k = 0; k < 40; ++k) out[(size_t)(40+k)*kQuad] = scratch[k];
+}
+
 __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ state,
 	const double* __restrict__ previous, AssemblyParams prm, float* __restrict__ coef, double* __restrict__ rhs)
@@ -356,24 +370,29 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 	__syncthreads();
 
 	// 3. Coefficients: thread (row field il, point q), two column-field halves through the
-	//    scratch (the partial sums are dead), stored coalesced over the points.
+	//    scratch (the partial sums are dead), stored coalesced over the points.  The row field is
+	//    uniform over a warp and a compile-time constant of each branch, so the point state and the
+	//    coefficient temporaries stay in registers.
 	{
 		const int q = tid & 63, il = tid >> 6;
 		PointState S;
 		const double* s = QS+q*kQS;
+		#pragma unroll
 		for (int c = 0; c < 3; ++c) {
 			S.u[c] = s[kU+c]; S.up[c] = s[kUp+c]; S.lap[c] = s[kLap+c]; S.gp[c] = s[kGrad+9+c];
+			#pragma unroll
 			for (int d = 0; d < 3; ++d) S.gv[c][d] = s[kGrad+3*c+d];
 		}
 		S.p = s[kP];
 		const double* qd = qdata+((size_t)e*kQuad+q)*kQData;
 		float* scratch = Scratch+tid*kScratchStride;
 		float* out = coef+((size_t)e*4+il)*kCoef*kQuad+q;
-		for (int half = 0; half < 2; ++half) {
-			RowCoefficients<float>(il, S, qd, prm, scratch, half == 0 ? RC+(il*kQuad+q)*kRcStride : nullptr,
-				2*half, 2*half+2);
-			#pragma unroll 8
-			for (int k = 0; k < 40; ++k) out[(size_t)(half*40+k)*kQuad] = scratch[k];
+		double* rc = RC+(il*kQuad+q)*kRcStride;
+		switch (il) {
+		case 0: PointCoefficients<0>(S, qd, prm, scratch, rc, out); break;
+		case 1: PointCoefficients<1>(S, qd, prm, scratch, rc, out); break;
+		case 2: PointCoefficients<2>(S, qd, prm, scratch, rc, out); break;
+		default: PointCoefficients<3>(S, qd, prm, scratch, rc, out); break;
 		}
 	}
 	__syncthreads();

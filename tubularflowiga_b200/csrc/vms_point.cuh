@@ -31,8 +31,8 @@ struct PointState {
 // for the FP64 tangent, float for the tensor-core tangent).  Only the column
 // fields f in [f_lo, f_hi) are written; rc may be null.
 template <class C, int kStride = 1>
-__device__ void RowCoefficients(int i, const PointState& S, const double* qd, const AssemblyParams& prm,
-	C* M, double* rc, int f_lo = 0, int f_hi = 4)
+__device__ __forceinline__ void RowCoefficients(int i, const PointState& S, const double* qd,
+	const AssemblyParams& prm, C* M, double* rc, int f_lo = 0, int f_hi = 4)
 {
 	const double rho = prm.density, mu = prm.viscosity, nu = mu/rho;
 	const double dt = prm.dt;
