@@ -525,7 +525,9 @@ def main():
         info = ns.amg_info()
         dn = 4 * info["nodes"][-1]
         ap = info["transfer_blocks"]
-        vbytes = (2 * 4 * n * 8 + 4 * n) + dn * dn * 8 + (3 * 4 * n * 8 + 2 * 4 * n + ap * (128 + 4) + n * 128)
+        ap_entry = 4 if mixed else 8        # A P is stored in the fine matrix's precision
+        vbytes = (2 * 4 * n * 8 + 4 * n) + dn * dn * 8 + (3 * 4 * n * 8 + 2 * 4 * n + ap * (16 * ap_entry + 4)
+                                                          + n * 128)
         a = vbytes / (amg_ms / amg_n * 1e-3) / 1e9
         kernels["amg_vcycle"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s", "frac": a / hbm,
                                  "traffic": None, "launches": amg_n, "avg_ms": amg_ms / amg_n,

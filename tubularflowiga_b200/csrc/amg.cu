@@ -22,7 +22,8 @@ struct Amg::Level {
 	// nodes, block columns of the coarse nodes, and the fixed-order fine-block lists
 	long long ap_blocks = 0;
 	DeviceArray<int32_t> ap_rows, ap_cols, ap_order, ap_offsets;
-	DeviceArray<double> ap_values;
+	DeviceArray<double> ap_values;      // A P with an FP64 fine matrix
+	DeviceArray<float> ap_values32;     // A P with an FP32 fine matrix (stored in its precision)
 	// coarsest level
 	int dense_n = 0;
 	DeviceArray<double> dense, column;
@@ -90,11 +91,11 @@ __global__ void UnitDiagonalKernel(int nodes, const int32_t* __restrict__ diag, 
 
 // (A P)[i, I] = sum over the fine blocks (i, j) with j in aggregate I of
 // A[i, j] diag(mask_j): a warp per A P block, lanes = (slot, entry), fixed
-// order (deterministic).
+// order (deterministic); summed in FP64, stored in the fine matrix's precision.
 template <class T>
 __global__ void __launch_bounds__(256) ApKernel(long long ap_blocks, const int32_t* __restrict__ order,
 	const int32_t* __restrict__ offsets, const int32_t* __restrict__ fine_cols, const double* __restrict__ mask,
-	const T* __restrict__ values, double* __restrict__ ap)
+	const T* __restrict__ values, T* __restrict__ ap)
 {
 	const long long B = ((long long)blockIdx.x*blockDim.x+threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
@@ -106,8 +107,24 @@ __global__ void __launch_bounds__(256) ApKernel(long long ap_blocks, const int32
 		acc += mask[4*(size_t)fine_cols[fb]+(e & 3)]*(double)values[(size_t)fb*16+e];
 	}
 	acc += __shfl_xor_sync(0xffffffffu, acc, 16);
-	if (lane < 16) ap[B*16+lane] = acc;
+	if (lane < 16) ap[B*16+lane] = T(acc);
 }
+
+template <class A> struct ApRow;
+template <> struct ApRow<double> {
+	static __device__ __forceinline__ void Load(const double* p, double v[4])
+	{
+		const double2 a01 = reinterpret_cast<const double2*>(p)[0], a23 = reinterpret_cast<const double2*>(p)[1];
+		v[0] = a01.x; v[1] = a01.y; v[2] = a23.x; v[3] = a23.y;
+	}
+};
+template <> struct ApRow<float> {
+	static __device__ __forceinline__ void Load(const float* p, double v[4])
+	{
+		const float4 a = *reinterpret_cast<const float4*>(p);
+		v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+	}
+};
 
 // The fine-level half of the two-level application, four threads per fine
 // node (one per field row): t = P x_c (masked), r = b - (A P) x_c,
@@ -115,9 +132,10 @@ __global__ void __launch_bounds__(256) ApKernel(long long ap_blocks, const int32
 // the lane quad.  Equal to prolongation, residual and block-Jacobi step on the
 // full operator, but it reads the few A P blocks of the row instead of the
 // row of A.
+template <class A>
 __global__ void __launch_bounds__(256) CoarseCorrectionKernel(int nodes, const int32_t* __restrict__ agg,
 	const double* __restrict__ mask, const double* __restrict__ xc, const int32_t* __restrict__ ap_rows,
-	const int32_t* __restrict__ ap_cols, const double* __restrict__ ap, const double* __restrict__ b,
+	const int32_t* __restrict__ ap_cols, const A* __restrict__ ap, const double* __restrict__ b,
 	const double* __restrict__ inverse, double omega, double* __restrict__ z, const int* __restrict__ stop)
 {
 	if (*stop) return;
@@ -128,10 +146,11 @@ __global__ void __launch_bounds__(256) CoarseCorrectionKernel(int nodes, const i
 	if (active) {
 		r = b[t];
 		for (int k = ap_rows[i]; k < ap_rows[i+1]; ++k) {
-			const double2* blk = reinterpret_cast<const double2*>(ap+(size_t)k*16+row*4);
+			double a[4];
+			ApRow<A>::Load(ap+(size_t)k*16+row*4, a);
 			const double2* xv = reinterpret_cast<const double2*>(xc+4*(size_t)ap_cols[k]);
-			const double2 a01 = blk[0], a23 = blk[1], x01 = xv[0], x23 = xv[1];
-			r -= a01.x*x01.x+a01.y*x01.y+a23.x*x23.x+a23.y*x23.y;
+			const double2 x01 = xv[0], x23 = xv[1];
+			r -= a[0]*x01.x+a[1]*x01.y+a[2]*x23.x+a[3]*x23.y;
 		}
 	}
 	const int base = threadIdx.x & ~3;
@@ -498,7 +517,7 @@ void Amg::BuildFromStrength(std::vector<double> s)
 	up(L.agg, L.h_agg); up(L.agg_order, aorder); up(L.agg_offsets, aoff);
 	up(L.gal_order, gorder); up(L.gal_offsets, goff); up(L.block_row, block_row);
 	up(L.ap_rows, ap_rows); up(L.ap_cols, ap_cols); up(L.ap_order, aporder); up(L.ap_offsets, apoff);
-	L.ap_values.Allocate((size_t)L.ap_blocks*16);
+	// A P storage follows the fine matrix's precision; allocated on the first refresh
 	levels_.push_back(std::move(fine));
 	levels_.push_back(std::move(C));
 	if (nc > 2048) Fail(-7, "aggregation stalled: coarse space of "+std::to_string(nc)+" nodes is too large for the dense coarse solve");
@@ -520,6 +539,18 @@ void Amg::BuildFromStrength(std::vector<double> s)
 	CudaCheck(cudaStreamSynchronize(stream_), "AMG setup");
 	built_ = true;
 	masks_dirty_ = true;
+}
+
+template <> double* Amg::ApValues<double>(Level& L)
+{
+	if (L.ap_values.size() == 0) L.ap_values.Allocate((size_t)L.ap_blocks*16);
+	return L.ap_values.get();
+}
+
+template <> float* Amg::ApValues<float>(Level& L)
+{
+	if (L.ap_values32.size() == 0) L.ap_values32.Allocate((size_t)L.ap_blocks*16);
+	return L.ap_values32.get();
 }
 
 template <class T>
@@ -564,8 +595,9 @@ void Amg::Refresh(const T* values, bool coarse)
 			launches_ += 1;
 		}
 		if (l == 0) {
+			T* ap = ApValues<T>(L);
 			ApKernel<T><<<Grid(L.ap_blocks, 8), 256, 0, stream_>>>(L.ap_blocks, L.ap_order.get(), L.ap_offsets.get(),
-				L.cols.get(), L.mask.get(), values, L.ap_values.get());
+				L.cols.get(), L.mask.get(), values, ap);
 			LaunchCheck("ApKernel");
 			launches_ += 1;
 		}
@@ -617,8 +649,8 @@ void Amg::Cycle(int l, const T* A, const double* b, double* x, const int* stop)
 	DenseApplyKernel<<<Grid(C.dense_n, 8), 256, 0, stream_>>>(C.dense_n, C.dense.get(), C.b.get(), C.x.get(), stop);
 	LaunchCheck("DenseApplyKernel");
 	(void)A;      // the fine operator enters through A P, refreshed with it
-	CoarseCorrectionKernel<<<Grid(4LL*L.nodes, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(), C.x.get(),
-		L.ap_rows.get(), L.ap_cols.get(), L.ap_values.get(), b, L.inverse.get(), options_.omega, x, stop);
+	CoarseCorrectionKernel<T><<<Grid(4LL*L.nodes, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(),
+		C.x.get(), L.ap_rows.get(), L.ap_cols.get(), ApValues<T>(L), b, L.inverse.get(), options_.omega, x, stop);
 	LaunchCheck("CoarseCorrectionKernel");
 	launches_ += 3;
 }

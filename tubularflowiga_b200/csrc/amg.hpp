@@ -67,6 +67,7 @@ public:
 private:
 	struct Level;
 	template <class T> void Cycle(int level, const T* fine, const double* b, double* x, const int* stop);
+	template <class T> T* ApValues(Level& level);   // A P blocks in the fine matrix's precision
 	void BuildFromStrength(std::vector<double> s);
 	std::vector<std::unique_ptr<Level>> levels_;
 	DevicePatternView fine_;

@@ -172,8 +172,15 @@ __global__ void ArnoldiFinalizeKernel(const double* __restrict__ norm_partial, i
 	double* s_ = c+restart;           // [restart]
 	__shared__ double red[kWarps];
 	if (state[0]) return;
-	double s = 0.0;
-	for (int b = threadIdx.x; b < blocks; b += blockDim.x) s += norm_partial[b];
+	// eight independent running sums per thread (loads in flight, fixed order: deterministic)
+	double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+	int b = threadIdx.x;
+	for (; b+7*(int)blockDim.x < blocks; b += 8*blockDim.x) {
+		#pragma unroll
+		for (int u = 0; u < 8; ++u) acc[u] += norm_partial[b+u*blockDim.x];
+	}
+	for (int u = 0; b < blocks; b += blockDim.x, ++u) acc[u & 7] += norm_partial[b];
+	double s = ((acc[0]+acc[1])+(acc[2]+acc[3]))+((acc[4]+acc[5])+(acc[6]+acc[7]));
 	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
 	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
 	__syncthreads();
