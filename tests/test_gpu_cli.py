@@ -100,3 +100,44 @@ def test_command_matches_api(case, tmp_path):
     st = ns.get_state().reshape(-1, 4)
     cmd = np.loadtxt(out)
     assert np.linalg.norm(st[:, :3] - cmd) <= 1e-8 * np.linalg.norm(cmd)
+
+
+def test_vtu_pvd_and_velocity_manifest(case, tmp_path):
+    """VTU snapshots, the final VTU, the PVD collection and the velocity manifest
+    (WriteVtu / WritePvd, include/VtkOutput.hpp:107-191; WriteVelocityManifest,
+    include/VelocitySeries.hpp:92-103): each VTU holds the control mesh of controlmesh.vtk
+    with the state of the matching text snapshot, and the collection lists them by time."""
+    import xml.etree.ElementTree as ET
+    d, db, tube = case
+    out = tmp_path / "flow.txt"
+    r = run("navier-stokes", db, d, "--output", out, "--output-every", "1", "--visualization-format", "vtu")
+    assert r.returncode == 0, r.stderr
+    n, E = tube.mesh.nodes, tube.mesh.elements
+    for step in range(4):
+        vtu = tmp_path / f"flow.step{step:06d}.vtu"
+        text = tmp_path / f"flow.step{step:06d}.txt"
+        assert vtu.exists() and text.exists()
+        root = ET.parse(vtu).getroot()
+        piece = root.find("UnstructuredGrid/Piece")
+        assert int(piece.get("NumberOfPoints")) == n and int(piece.get("NumberOfCells")) == E
+        time = float(root.find("UnstructuredGrid/FieldData/DataArray").text)
+        assert time == pytest.approx(2e-3 * step, rel=1e-15, abs=1e-300)
+        arrays = {a.get("Name"): np.array(a.text.split(), float) for a in piece.find("PointData")}
+        assert np.array_equal(arrays["velocity"].reshape(n, 3), np.loadtxt(text))
+        assert np.array_equal(arrays["pressure"], np.loadtxt(str(text) + ".pressure"))
+        pts = np.array(piece.find("Points/DataArray").text.split(), float).reshape(n, 3)
+        assert np.allclose(pts, tube.points, rtol=0, atol=1e-15)
+        cells = {a.get("Name"): np.array(a.text.split(), np.int64) for a in piece.find("Cells")}
+        assert np.array_equal(cells["connectivity"].reshape(E, 8), tube.cells)
+        assert np.array_equal(cells["offsets"], 8 * np.arange(1, E + 1)) and (cells["types"] == 12).all()
+    final = ET.parse(tmp_path / "flow.vtu").getroot().find("UnstructuredGrid/Piece/PointData")
+    assert np.array_equal(np.array(final[0].text.split(), float).reshape(n, 3), np.loadtxt(out))
+    sets = ET.parse(tmp_path / "flow.pvd").getroot().findall("Collection/DataSet")
+    assert [s.get("file") for s in sets] == [f"flow.step{k:06d}.vtu" for k in range(4)]
+    assert [float(s.get("timestep")) for s in sets] == pytest.approx([2e-3 * k for k in range(4)])
+    rows = (tmp_path / "flow.series.csv").read_text().splitlines()
+    assert rows[0] == "time,file" and len(rows) == 5
+    assert [r.split(",")[1] for r in rows[1:]] == [f"flow.step{k:06d}.txt" for k in range(4)]
+    assert [float(r.split(",")[0]) for r in rows[1:]] == pytest.approx([2e-3 * k for k in range(4)])
+    bad = run("navier-stokes", db, d, "--output", tmp_path / "x.txt", "--visualization-format", "vtkhdf")
+    assert bad.returncode == 1 and "HDF5" in bad.stderr

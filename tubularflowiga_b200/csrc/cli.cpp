@@ -123,7 +123,11 @@ Options ParseOptions(int argc, char** argv)
 		else if (arg == "--nonlinear-atol") o.atol = PositiveDouble(v, arg);
 		else if (arg == "--mass-rtol") o.mass_rtol = PositiveDouble(v, arg);
 		else if (arg == "--visualization-format") {
-			if (v != "auto" && v != "vtu" && v != "vtkhdf") Fail(-1, "unknown visualization format: "+v);
+			// ParseVisualizationFormat (include/VtkOutput.hpp:17-25)
+			if (v != "auto" && v != "vtu" && v != "vtkhdf" && v != "bezier-vtkhdf")
+				Fail(-1, "--visualization-format must be auto, vtu, or vtkhdf");
+			if (v == "vtkhdf" || v == "bezier-vtkhdf")
+				Fail(-4, "--visualization-format vtkhdf needs HDF5, which this build does not include; use vtu");
 			o.visualization = v;
 		} else Fail(-1, "unknown option: "+arg);
 	}
@@ -174,6 +178,148 @@ void WriteVtk(const fs::path& mesh_path, const fs::path& path, const std::vector
 		out << state[4*node] << ' ' << state[4*node+1] << ' ' << state[4*node+2] << '\n';
 	out << "SCALARS Pressure double 1\nLOOKUP_TABLE default\n";
 	for (size_t node = 0; node < state.size()/4; ++node) out << state[4*node+3] << '\n';
+}
+
+// ASCII legacy unstructured grid of controlmesh.vtk (ReadLegacyUnstructuredGrid,
+// include/VtkOutput.hpp:61-105): points, cell connectivity, offsets and types.
+struct VtkGrid {
+	std::vector<double> points;
+	std::vector<int64_t> connectivity, offsets;
+	std::vector<unsigned> types;
+};
+
+VtkGrid ReadVtkGrid(const fs::path& path)
+{
+	std::ifstream in(path);
+	if (!in) Fail(-3, "cannot open VTK mesh: "+path.string());
+	VtkGrid g;
+	std::string token;
+	size_t points = 0, cells = 0;
+	while (in >> token) {
+		if (token == "POINTS") {
+			std::string type;
+			in >> points >> type;
+			g.points.resize(3*points);
+			for (auto& v : g.points)
+				if (!(in >> v)) Fail(-4, "truncated VTK points: "+path.string());
+		} else if (token == "CELLS") {
+			size_t entries = 0;
+			in >> cells >> entries;
+			for (size_t c = 0; c < cells; ++c) {
+				size_t count = 0;
+				if (!(in >> count)) Fail(-4, "truncated VTK cells: "+path.string());
+				for (size_t k = 0; k < count; ++k) {
+					int64_t index = -1;
+					if (!(in >> index) || index < 0 || (size_t)index >= points)
+						Fail(-4, "invalid VTK cell connectivity: "+path.string());
+					g.connectivity.push_back(index);
+				}
+				g.offsets.push_back((int64_t)g.connectivity.size());
+			}
+		} else if (token == "CELL_TYPES") {
+			size_t count = 0;
+			in >> count;
+			g.types.resize(count);
+			for (auto& t : g.types)
+				if (!(in >> t)) Fail(-4, "truncated VTK cell types: "+path.string());
+			break;
+		}
+	}
+	if (points == 0 || cells == 0 || g.offsets.size() != cells || g.types.size() != cells)
+		Fail(-4, "VTK mesh is not a complete ASCII unstructured grid: "+path.string());
+	return g;
+}
+
+// VTK XML unstructured grid with velocity (3) and pressure (1) point arrays and the
+// physical time as TimeValue field data (WriteVtu, include/VtkOutput.hpp:107-155).
+void WriteVtuFile(const VtkGrid& g, const fs::path& path, const std::vector<double>& state, double time)
+{
+	const size_t points = g.points.size()/3;
+	if (state.size() != 4*points) Fail(-4, "VTU point-array size mismatch for 'velocity'");
+	if (!path.parent_path().empty()) fs::create_directories(path.parent_path());
+	std::ofstream out(path);
+	if (!out) Fail(-3, "cannot create VTU output: "+path.string());
+	out << std::setprecision(17) << "<?xml version=\"1.0\"?>\n"
+		<< "<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n"
+		<< "  <UnstructuredGrid>\n"
+		<< "    <FieldData><DataArray type=\"Float64\" Name=\"TimeValue\" NumberOfTuples=\"1\" format=\"ascii\">"
+		<< time << "</DataArray></FieldData>\n"
+		<< "    <Piece NumberOfPoints=\"" << points << "\" NumberOfCells=\"" << g.offsets.size() << "\">\n"
+		<< "      <PointData>\n"
+		<< "        <DataArray type=\"Float64\" Name=\"velocity\" NumberOfComponents=\"3\" format=\"ascii\">\n          ";
+	for (size_t node = 0; node < points; ++node)
+		out << state[4*node] << ' ' << state[4*node+1] << ' ' << state[4*node+2] << ' ';
+	out << "\n        </DataArray>\n"
+		<< "        <DataArray type=\"Float64\" Name=\"pressure\" NumberOfComponents=\"1\" format=\"ascii\">\n          ";
+	for (size_t node = 0; node < points; ++node) out << state[4*node+3] << ' ';
+	out << "\n        </DataArray>\n      </PointData>\n"
+		<< "      <Points><DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n        ";
+	for (double v : g.points) out << v << ' ';
+	out << "\n      </DataArray></Points>\n      <Cells>\n"
+		<< "        <DataArray type=\"Int64\" Name=\"connectivity\" format=\"ascii\">\n          ";
+	for (auto v : g.connectivity) out << v << ' ';
+	out << "\n        </DataArray>\n        <DataArray type=\"Int64\" Name=\"offsets\" format=\"ascii\">\n          ";
+	for (auto v : g.offsets) out << v << ' ';
+	out << "\n        </DataArray>\n        <DataArray type=\"UInt8\" Name=\"types\" format=\"ascii\">\n          ";
+	for (auto v : g.types) out << v << ' ';
+	out << "\n        </DataArray>\n      </Cells>\n    </Piece>\n  </UnstructuredGrid>\n</VTKFile>\n";
+	out.close();
+	if (!out) Fail(-3, "cannot write VTU output: "+path.string());
+}
+
+// <stem>.stepNNNNNN.vtu, <stem>.vtu, <stem>.pvd, <stem>.series.csv next to the output
+// (VtuStepPath / VtuFinalPath / PvdPath, VtkOutput.hpp:157-174; VelocityManifestPath,
+// VelocitySeries.hpp:87-90).
+fs::path SiblingPath(const fs::path& base, const std::string& suffix)
+{
+	return base.parent_path()/(base.stem().string()+suffix);
+}
+
+fs::path VtuStep(const fs::path& base, int step)
+{
+	std::ostringstream name;
+	name << ".step" << std::setw(6) << std::setfill('0') << step << ".vtu";
+	return SiblingPath(base, name.str());
+}
+
+// XML attribute text (EscapeVtkXml, VtkOutput.hpp:48-59).
+std::string XmlEscape(const std::string& value)
+{
+	std::string out;
+	for (char c : value) {
+		if (c == '&') out += "&amp;";
+		else if (c == '<') out += "&lt;";
+		else if (c == '>') out += "&gt;";
+		else if (c == '"') out += "&quot;";
+		else out.push_back(c);
+	}
+	return out;
+}
+
+// ParaView collection of the VTU snapshots (WritePvd, VtkOutput.hpp:176-191).
+void WritePvdFile(const fs::path& path, const std::vector<std::pair<double, fs::path>>& snapshots)
+{
+	std::ofstream out(path);
+	if (!out) Fail(-3, "cannot create PVD output: "+path.string());
+	out << "<?xml version=\"1.0\"?>\n<VTKFile type=\"Collection\" version=\"0.1\" byte_order=\"LittleEndian\">\n"
+		<< "  <Collection>\n";
+	for (const auto& s : snapshots)
+		out << "    <DataSet timestep=\"" << std::setprecision(17) << s.first << "\" group=\"\" part=\"0\" file=\""
+			<< XmlEscape(s.second.filename().string()) << "\"/>\n";
+	out << "  </Collection>\n</VTKFile>\n";
+	out.close();
+	if (!out) Fail(-3, "cannot write PVD output: "+path.string());
+}
+
+// time,file rows of the text velocity snapshots (WriteVelocityManifest, VelocitySeries.hpp:92-103).
+void WriteManifest(const fs::path& path, const std::vector<std::pair<double, fs::path>>& snapshots)
+{
+	std::ofstream out(path);
+	if (!out) Fail(-3, "cannot create velocity manifest: "+path.string());
+	out << "time,file\n";
+	for (const auto& s : snapshots) out << std::setprecision(17) << s.first << ',' << s.second.filename().string() << '\n';
+	out.close();
+	if (!out) Fail(-3, "cannot write velocity manifest: "+path.string());
 }
 
 // Flow checkpoint: raw float64 state + JSON metadata (FlowCheckpoint.hpp, iga_cuda.cu:566-602).
@@ -337,8 +483,17 @@ int NavierStokes(int argc, char** argv)
 	solver.SetState(state.data(), state.data());
 	long long total_iterations = 0;
 	double total_assembly = 0.0, total_linear = 0.0;
+	// VTU snapshots and the PVD collection (iga_cuda.cu:902-916, 1086-1100, 1126-1141); "auto"
+	// resolves to VTU in this build (the Bezier VTKHDF format needs HDF5).
+	const VtkGrid grid = options.output.empty() ? VtkGrid{} : ReadVtkGrid(case_dir/"controlmesh.vtk");
+	std::vector<std::pair<double, fs::path>> vtu_snapshots, velocity_snapshots;
 	if (transient && options.output_every > 0) {
-		WriteText(TimeIndexed(options.output, start_step), state);
+		const fs::path text = TimeIndexed(options.output, start_step);
+		WriteText(text, state);
+		const fs::path vtu = VtuStep(options.output, start_step);
+		WriteVtuFile(grid, vtu, state, start_step*dt);
+		vtu_snapshots.push_back({start_step*dt, vtu});
+		velocity_snapshots.push_back({start_step*dt, text});
 	}
 	for (int step = start_step; step < run_end; ++step) {
 		if (step > start_step) solver.CommitStep();
@@ -425,7 +580,12 @@ int NavierStokes(int argc, char** argv)
 		const int completed = step+1;
 		if (options.output_every > 0 && completed%options.output_every == 0) {
 			solver.GetState(state.data());
-			WriteText(TimeIndexed(options.output, completed), state);
+			const fs::path text = TimeIndexed(options.output, completed);
+			WriteText(text, state);
+			const fs::path vtu = VtuStep(options.output, completed);
+			WriteVtuFile(grid, vtu, state, completed*dt);
+			vtu_snapshots.push_back({completed*dt, vtu});
+			velocity_snapshots.push_back({completed*dt, text});
 		}
 		if (!options.checkpoint.empty()
 			&& (completed == run_end || (options.checkpoint_every > 0 && completed%options.checkpoint_every == 0))) {
@@ -443,6 +603,13 @@ int NavierStokes(int argc, char** argv)
 	if (!options.output.empty()) {
 		WriteText(options.output, state);
 		WriteVtk(case_dir/"controlmesh.vtk", options.output+".vtk", state);
+		const double final_time = transient ? run_end*dt : 0.0;
+		const fs::path vtu = SiblingPath(options.output, ".vtu");
+		WriteVtuFile(grid, vtu, state, final_time);
+		if (vtu_snapshots.empty()) vtu_snapshots.push_back({final_time, vtu});
+		WritePvdFile(SiblingPath(options.output, ".pvd"), vtu_snapshots);
+		if (!velocity_snapshots.empty())
+			WriteManifest(SiblingPath(options.output, ".series.csv"), velocity_snapshots);
 	}
 	std::cout << "navier_stokes_cuda nodes=" << nodes << " elements=" << mesh.host().elements()
 		<< " steps=" << physical_steps << " run_end_step=" << run_end
