@@ -121,6 +121,23 @@ def workload(name):
     return tube, desc, wave
 
 
+def max_over_ranks(dist, values, device):
+    """Each rank's device-timed milliseconds -> their maximum over all ranks (one all-reduce that every
+    rank takes; identity without a process group)."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def replica_throughput(world, steps, ms):
+    """Whole-job time steps/s of `world` independent replicas that each took `steps` steps, timed by the
+    slowest rank (`ms`, milliseconds)."""
+    return world * steps / (ms / 1e3)
+
+
 def step_dt(name):
     """Time step of a workload: the 1,280-element cylinder 1e-3 s; the tube batch 1e-4 s, because its
     smallest fast tubes (R 0.5 mm at Re 800, about 1.5 m/s) reach an axial CFL of 70 at 2e-3 s;
@@ -487,10 +504,7 @@ def main():
         ref.close()
         del ref
 
-    if dist:
-        t = torch.tensor([ms, e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms], "cuda")
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -576,7 +590,7 @@ def main():
     roof["kernel"] = dominant
     if roof["bound"] == "hbm":
         roof["peak_kind"] = f"{peak_kind} hbm_gbs"
-    steps_per_s = world * args.steps / (ms / 1e3)
+    steps_per_s = replica_throughput(world, args.steps, ms)
     newton = np.mean([r["newton_iterations"] for r in timed_reports])
     linear = np.sum([r["linear_iterations"] for r in timed_reports]) / max(1, np.sum(
         [r["newton_iterations"] for r in timed_reports]))
@@ -609,7 +623,7 @@ def main():
         "spmv_gbs": kernels.get(spmv_name, {}).get("achieved"),
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
-        "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": "time steps/s",
+        "e2e": {"value": replica_throughput(world, args.steps, e2e_ms), "unit": "time steps/s",
                 "h2d_bytes_per_step": 3 * n * 8, "d2h_bytes_per_step": 4 * n * 8},
     }
     if not args.no_cpu_baseline and world == 1:
