@@ -15,7 +15,10 @@ Inputs are synthetic (seeded generator), stated in `data`.
 
 A "step" is one physical time step: Newton to ||r|| <= 1e-8 ||r_0|| (FP64
 residual) with the exact tangent, each linear solve AMG-preconditioned
-FGMRES(64) to a true-residual rtol of 1e-8 (the AMG's dense coarse inverse
+FGMRES(64) -- by default (--forcing ew) to an Eisenstat-Walker forcing
+tolerance, with the step's Dirichlet values lifted into the state first so
+that r_0 is the PDE residual; --forcing fixed solves every system to a
+true-residual rtol of 1e-8 as the reference (the AMG's dense coarse inverse
 rebuilt every third linear solve, its fine-level data on every solve; both
 precisions).  Outlet pressures follow the RCR models by the relaxed fixed
 point (relaxation 1, tolerance 1e-8 + 1e-6 |P|), updated inside the Newton
@@ -37,9 +40,11 @@ Legs of one run (rank 0 prints one JSON line):
             (or FP64) assembly, SpMV, the AMG V-cycle and the Krylov
             orthogonalisation (HBM-bound); the dominant one by share.
   fp64_gpu  (mixed only) the plain FP64 GPU solver on the warm-up steps from
-            the same initial state (same outlet coupling): its time steps/s,
-            Newton and FGMRES counts, and the relative L2 error of the mixed
-            solution against it after every step.
+            the same initial state (same outlet coupling), run with the fixed
+            1e-8 tolerance and in the mixed arm's forcing mode; the faster of
+            the two is reported (both values under "variants") with its Newton
+            and FGMRES counts and the relative L2 error of the mixed solution
+            against it after every step.
   cpu_baseline  the reference's own element code (oracle/_ref) and the CPU
             restatement of block-Jacobi GMRES on a bounded sample, all host
             cores, scaled to time steps/s.
@@ -347,6 +352,8 @@ def main():
     ap.add_argument("--outlet-coupling", default="newton", choices=["newton", "outer"])
     ap.add_argument("--krylov-fp64-basis", action="store_true")
     ap.add_argument("--restart", type=int, default=64, help="FGMRES restart length")
+    ap.add_argument("--forcing", default="ew", choices=["fixed", "ew"],
+                    help="linear tolerance per Newton solve: fixed 1e-8, or Eisenstat-Walker forcing")
     ap.add_argument("--ref-budget", type=float, default=25.0)
     ap.add_argument("--ref-newton", type=float, default=4.0)
     ap.add_argument("--ref-linear", type=float, default=228.0)
@@ -380,7 +387,8 @@ def main():
                      nonlinear_rtol=1e-8, nonlinear_atol=1e-300, mass_rtol=1e-3,
                      gmres_restart=args.restart, gmres_max_iterations=5000, gmres_rtol=1e-8,
                      preconditioner=api.AMG if amg else api.BLOCK_JACOBI,
-                     amg_coarse_period=3, krylov_fp64_basis=int(args.krylov_fp64_basis))
+                     amg_coarse_period=3, krylov_fp64_basis=int(args.krylov_fp64_basis),
+                     newton_forcing=int(args.forcing == "ew"))
     precision = {"mixed": api.MIXED, "bf16x3": api.MIXED_BF16X3, "fp64": api.FP64}[args.precision]
     ns = api.NavierStokes(mesh, precision=precision, **solver_kw)
     dt = ns.params.dt
@@ -466,43 +474,51 @@ def main():
     # mixed solution against it, and its own time steps/s (steps after the first, CUDA events)
     fp64_leg = None
     if mixed and not args.no_fp64_leg:
-        ref = api.NavierStokes(mesh, precision=api.FP64, **solver_kw)
-        ref.set_dirichlet(vmask, pmask, velocity_at(0.0))
-        ref.set_tractions(fixed_tractions)
-        ref.set_state(s0, s0)
-        ref_outlets = [api.Outlet(**m.as_dict()) for m in models] if models else None
-        rstream = torch.cuda.ExternalStream(ref.stream())
-        errors, fp64_ms, fp64_steps, fp64_reports = [], 0.0, 0, []
-        for k in range(args.warmup):
-            api.check(api.lib().tfiga_ns_set_dirichlet_values(ref._h, api.C.c_void_p(bc_dev[k].data_ptr()), None))
-            ref.commit_step()
-            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            a0.record(rstream)
-            if ref_outlets:
-                rep = outlet_step(ref, ref_outlets, args.outlet_coupling)
-            else:
-                rep = ref.step()
-            a1.record(rstream)
-            fp64_reports.append(rep)
-            torch.cuda.synchronize()
-            if k > 0:
-                fp64_ms += a0.elapsed_time(a1)
-                fp64_steps += 1
-            r64 = ref.get_state().reshape(-1, 4)
-            mx = warm_states[k].reshape(-1, 4)
-            errors.append({"step": k,
-                           "velocity": float(np.linalg.norm(mx[:, :3] - r64[:, :3]) / np.linalg.norm(r64[:, :3])),
-                           "pressure": float(np.linalg.norm(mx[:, 3] - r64[:, 3]) / np.linalg.norm(r64[:, 3]))})
-        fp64_leg = {"value": fp64_steps / (fp64_ms / 1e3) if fp64_steps else None, "unit": "time steps/s",
-                    "steps": fp64_steps, "ms_per_step": fp64_ms / max(fp64_steps, 1),
+        # the plain FP64 solver in each linear-tolerance mode (fixed 1e-8 as the reference, and the
+        # forcing mode when the mixed arm uses it); the faster one is the baseline reported
+        def fp64_run(forcing):
+            kw = dict(solver_kw, newton_forcing=int(forcing == "ew"))
+            ref = api.NavierStokes(mesh, precision=api.FP64, **kw)
+            ref.set_dirichlet(vmask, pmask, velocity_at(0.0))
+            ref.set_tractions(fixed_tractions)
+            ref.set_state(s0, s0)
+            ref_outlets = [api.Outlet(**m.as_dict()) for m in models] if models else None
+            rstream = torch.cuda.ExternalStream(ref.stream())
+            errors, fp64_ms, fp64_steps, fp64_reports = [], 0.0, 0, []
+            for k in range(args.warmup):
+                api.check(api.lib().tfiga_ns_set_dirichlet_values(ref._h, api.C.c_void_p(bc_dev[k].data_ptr()),
+                                                                  None))
+                ref.commit_step()
+                a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                a0.record(rstream)
+                if ref_outlets:
+                    rep = outlet_step(ref, ref_outlets, args.outlet_coupling)
+                else:
+                    rep = ref.step()
+                a1.record(rstream)
+                fp64_reports.append(rep)
+                torch.cuda.synchronize()
+                if k > 0:
+                    fp64_ms += a0.elapsed_time(a1)
+                    fp64_steps += 1
+                r64 = ref.get_state().reshape(-1, 4)
+                mx = warm_states[k].reshape(-1, 4)
+                errors.append({"step": k,
+                               "velocity": float(np.linalg.norm(mx[:, :3] - r64[:, :3]) / np.linalg.norm(r64[:, :3])),
+                               "pressure": float(np.linalg.norm(mx[:, 3] - r64[:, 3]) / np.linalg.norm(r64[:, 3]))})
+            ref.close()
+            return {"value": fp64_steps / (fp64_ms / 1e3) if fp64_steps else None, "unit": "time steps/s",
+                    "forcing": forcing, "steps": fp64_steps, "ms_per_step": fp64_ms / max(fp64_steps, 1),
                     "newton_per_step": float(np.mean([r["newton_iterations"] for r in fp64_reports])),
                     "linear_iterations_per_newton": float(np.sum([r["linear_iterations"] for r in fp64_reports])
                                                           / max(1, np.sum([r["newton_iterations"]
                                                                            for r in fp64_reports]))),
                     "error_vs_fp64_per_step": errors}
-        ref.close()
-        del ref
+
+        runs = [fp64_run(mode) for mode in dict.fromkeys(["fixed", args.forcing])]
+        fp64_leg = dict(max(runs, key=lambda r: r["value"] or 0.0))
+        fp64_leg["variants"] = {r["forcing"]: r["value"] for r in runs}
 
     ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms], "cuda")
     if rank != 0:
@@ -604,12 +620,15 @@ def main():
                                "refinement; " % ("split-BF16 (hi + lo, 3 products)" if args.precision == "bf16x3"
                                                  else "BF16") if mixed else "plain FP64: ") +
                               "exact-tangent Newton to rel.res 1e-8, " +
+                              ("inexact Newton (Eisenstat-Walker forcing tolerances, Dirichlet values lifted "
+                               "into the state at step start), " if args.forcing == "ew" else "") +
                               ("RCR outlets coupled by the relaxed fixed point (relaxation %g, tolerance "
                                "1e-8 + 1e-6 |P|; %s), " % (OUTLET_RELAXATION,
                                                           "pressures updated inside the Newton loop"
                                                           if args.outlet_coupling == "newton" else
                                                           "the reference's outer loop") if models else "") +
-                              ("point-block two-level AMG-preconditioned FGMRES(%d) rtol 1e-8" % args.restart if amg else
+                              ("point-block two-level AMG-preconditioned FGMRES(%d)%s" % (args.restart, " rtol 1e-8" if args.forcing == "fixed"
+                                                                                   else "") if amg else
                                "block-Jacobi GMRES(200) rtol 1e-8")),
                    "l2": "inputs larger than L2 (matrix %.2f GB)" % (mesh.blocks * 128 / 1e9),
                    "parallelism": "replicas only" if world > 1 else "single GPU"},

@@ -113,6 +113,15 @@ typedef struct tfiga_ns_params {
 	 * of FP32 (twice the basis traffic; no loss of orthogonality from FP32 storage
 	 * over long Arnoldi cycles).  Ignored in TFIGA_PRECISION_FP64. */
 	int32_t krylov_fp64_basis;     /* default 0 */
+	/* Inexact Newton: 1 solves each Newton system to an Eisenstat-Walker forcing
+	 * tolerance eta_k = 0.9 (|r_k| / |r_{k-1}|)^2 (safeguarded, at most 1e-3, at least
+	 * gmres_rtol and at least half of what the Newton tolerance still asks for)
+	 * instead of gmres_rtol.  The step (tfiga_ns_step and the outlet steps) first sets
+	 * the constrained entries of the state to their prescribed values, so the residual
+	 * of the first Newton iteration -- the reference of the relative Newton test -- is
+	 * that of the PDE rows at the lifted state.  0 (default): every system to
+	 * gmres_rtol and no lifting, as the reference. */
+	int32_t newton_forcing;        /* default 0 */
 } tfiga_ns_params;
 
 #define TFIGA_PRECISION_FP64 0

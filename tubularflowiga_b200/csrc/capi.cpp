@@ -184,6 +184,7 @@ void tfiga_ns_default_params(tfiga_ns_params* p)
 	p->amg_coarse_nodes = 300;
 	p->amg_coarse_period = 1;
 	p->krylov_fp64_basis = 0;
+	p->newton_forcing = 0;
 }
 
 int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out)

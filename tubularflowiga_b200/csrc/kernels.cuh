@@ -85,6 +85,9 @@ void LaunchBlockInverse(const DevicePatternView& pattern, const T* values, doubl
 	unsigned int* singular, cudaStream_t stream);
 void LaunchToFloat(long long n, const double* in, float* out, cudaStream_t stream);
 void LaunchApplyBlockInverse(int nodes, const double* inverse, const double* x, double* y, cudaStream_t stream);
+// state = prescribed value on the constrained entries (the Dirichlet values lifted into the state).
+void LaunchLiftDirichlet(int count, const int32_t* nodes, const int32_t* vmask, const int32_t* pmask,
+	const double* velocity, const double* pressure, double* state, cudaStream_t stream);
 template <class T>
 void LaunchDirichletRows(const DevicePatternView& pattern, int count, const int32_t* constrained_nodes,
 	const int32_t* velocity_mask, const int32_t* pressure_mask, const double* velocity, const double* pressure,

@@ -240,6 +240,14 @@ void NsSolver::ApplyDirichlet()
 	ApplyDirichletParts(true, true);
 }
 
+void NsSolver::LiftDirichletForForcing()
+{
+	if (!params_.newton_forcing || !dirichlet_set_) return;
+	LaunchLiftDirichlet(constrained_count_, constrained_.get(), vmask_.get(), pmask_.get(), velocity_bc_.get(),
+		pressure_bc_.get(), state_.get(), stream_);
+	launches_ += 1;
+}
+
 void NsSolver::ApplyDirichletRhs()
 {
 	ApplyDirichletParts(false, true);
@@ -387,7 +395,26 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 		report.assembly_ms += ms;
 	}
 	CudaCheck(cudaEventRecord(events_[2], stream_), "event");
-	const GmresResult linear = SolveLinear(params_.gmres_rtol, params_.gmres_max_iterations);
+	// Linear tolerance: gmres_rtol, or the Eisenstat-Walker forcing term (choice 2, gamma 0.9,
+	// alpha 2) with its safeguard, capped at 1e-3, floored at gmres_rtol and at half of what the
+	// Newton test still asks for, so the last solve does not oversolve.
+	double eta = params_.gmres_rtol;
+	if (params_.newton_forcing) {
+		constexpr double kEtaMax = 1e-3;
+		if (initial_residual < 0.0) eta = kEtaMax;
+		else {
+			const double ratio = norm/forcing_norm_;
+			eta = 0.9*ratio*ratio;
+			const double safeguard = 0.9*forcing_eta_*forcing_eta_;
+			if (safeguard > 0.1) eta = std::max(eta, safeguard);
+			eta = std::min(eta, kEtaMax);
+		}
+		eta = std::max(eta, params_.gmres_rtol);
+		eta = std::max(eta, std::min(0.1, 0.5*report.tolerance/norm));
+		forcing_norm_ = norm;
+		forcing_eta_ = eta;
+	}
+	const GmresResult linear = SolveLinear(eta, params_.gmres_max_iterations);
 	CudaCheck(cudaEventRecord(events_[3], stream_), "event");
 	report.linear_iterations = linear.iterations;
 	report.linear_residual = linear.residual;
@@ -424,6 +451,7 @@ tfiga_step_report NsSolver::Step()
 {
 	tfiga_step_report step{};
 	double initial = -1.0;
+	LiftDirichletForForcing();
 	const int max_newton = params_.max_newton > 0 ? params_.max_newton : 12;
 	tfiga_newton_report last{};
 	for (int k = 0; k < max_newton; ++k) {
@@ -538,6 +566,7 @@ tfiga_step_report NsSolver::StepOutletsCoupled(tfiga_outlet* outlets, int count,
 	tfiga_step_report step{};
 	double initial = -1.0;
 	int changes = 0;
+	LiftDirichletForForcing();
 	tfiga_newton_report last{};
 	for (int k = 0; k < max_newton; ++k) {
 		auto traction = tractions_;

@@ -33,6 +33,9 @@ public:
 	void Assemble();
 	void ApplyDirichlet();
 	void ApplyDirichletRhs();       // rhs rows only (g - u on constrained entries)
+	// Inexact-Newton mode: the prescribed values into the state before a step's first Newton
+	// iteration, so that its residual (and the forcing tolerances) measure the PDE rows only.
+	void LiftDirichletForForcing();
 	void ApplyDirichletMatrix();    // Jacobian rows only (zero rows, unit diagonal)
 	GmresResult SolveLinear(double rtol, int max_iterations);
 	tfiga_newton_report NewtonIteration(double initial_residual);
@@ -97,6 +100,7 @@ private:
 	cudaEvent_t events_[6] = {};
 	long long launches_ = 0;
 	long long solves_ = 0;                   // linear solves so far (coarse refresh period)
+	double forcing_norm_ = 0.0, forcing_eta_ = 0.0;   // previous residual and forcing term (inexact Newton)
 	std::map<int32_t, double> tractions_;    // label -> pressure set by SetTractions
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;

@@ -97,6 +97,18 @@ __global__ void ApplyBlockInverseKernel(int nodes, const double* __restrict__ in
 	y[i] = d[0]*v[0]+d[1]*v[1]+d[2]*v[2]+d[3]*v[3];
 }
 
+// state = prescribed value on every constrained entry (thread per constrained node).
+__global__ void LiftDirichletKernel(int count, const int32_t* __restrict__ nodes, const int32_t* __restrict__ vmask,
+	const int32_t* __restrict__ pmask, const double* __restrict__ velocity, const double* __restrict__ pressure,
+	double* __restrict__ state)
+{
+	const int item = blockIdx.x*blockDim.x+threadIdx.x;
+	if (item >= count) return;
+	const size_t node = (size_t)nodes[item];
+	if (vmask[node]) for (int d = 0; d < 3; ++d) state[4*node+d] = velocity[3*node+d];
+	if (pmask[node]) state[4*node+3] = pressure[node];
+}
+
 // Dirichlet rows (IgaCudaKernels.cuh:436-463): a warp per constrained node.
 template <class T>
 __global__ void DirichletRowsKernel(DevicePatternView p, int count, const int32_t* __restrict__ nodes,
@@ -307,6 +319,15 @@ template void LaunchDirichletRows<double>(const DevicePatternView&, int, const i
 	const int32_t*, const double*, const double*, const double*, double*, double*, cudaStream_t);
 template void LaunchDirichletRows<float>(const DevicePatternView&, int, const int32_t*, const int32_t*,
 	const int32_t*, const double*, const double*, const double*, float*, double*, cudaStream_t);
+
+void LaunchLiftDirichlet(int count, const int32_t* nodes, const int32_t* vmask, const int32_t* pmask,
+	const double* velocity, const double* pressure, double* state, cudaStream_t stream)
+{
+	if (count == 0) return;
+	LiftDirichletKernel<<<(unsigned)((count+255)/256), 256, 0, stream>>>(count, nodes, vmask, pmask, velocity,
+		pressure, state);
+	LaunchCheck("LiftDirichletKernel");
+}
 
 void LaunchFaceFlows(int faces, const int32_t* face_element, const double* face_coef, const int32_t* eo,
 	const int32_t* conn, const double* state, double* face_flow, cudaStream_t stream)
