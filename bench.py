@@ -17,7 +17,9 @@ A "step" is one physical time step: Newton to ||r|| <= 1e-8 ||r_0|| (FP64
 residual) with the exact tangent, each linear solve AMG-preconditioned
 FGMRES(64) -- by default (--forcing ew) to an Eisenstat-Walker forcing
 tolerance, with the step's Dirichlet values lifted into the state first so
-that r_0 is the PDE residual; --forcing fixed solves every system to a
+that r_0 is the PDE residual, and in the tensor-core modes the previous
+iteration's tangent kept while Newton contracts within 100x the linear
+tolerance (--tangent-reuse 0 turns that off); --forcing fixed solves every system to a
 true-residual rtol of 1e-8 as the reference (the AMG's dense coarse inverse
 rebuilt every third linear solve, its fine-level data on every solve; both
 precisions).  Outlet pressures follow the RCR models by the relaxed fixed
@@ -352,6 +354,9 @@ def main():
     ap.add_argument("--outlet-coupling", default="newton", choices=["newton", "outer"])
     ap.add_argument("--krylov-fp64-basis", action="store_true")
     ap.add_argument("--restart", type=int, default=64, help="FGMRES restart length")
+    ap.add_argument("--tangent-reuse", type=float, default=100.0,
+                    help="tensor-core modes: keep the previous Newton iteration's tangent while its contraction "
+                         "is within this factor of its linear tolerance (0: off)")
     ap.add_argument("--forcing", default="ew", choices=["fixed", "ew"],
                     help="linear tolerance per Newton solve: fixed 1e-8, or Eisenstat-Walker forcing")
     ap.add_argument("--ref-budget", type=float, default=25.0)
@@ -388,7 +393,7 @@ def main():
                      gmres_restart=args.restart, gmres_max_iterations=5000, gmres_rtol=1e-8,
                      preconditioner=api.AMG if amg else api.BLOCK_JACOBI,
                      amg_coarse_period=3, krylov_fp64_basis=int(args.krylov_fp64_basis),
-                     newton_forcing=int(args.forcing == "ew"))
+                     newton_forcing=int(args.forcing == "ew"), tangent_reuse_factor=args.tangent_reuse)
     precision = {"mixed": api.MIXED, "bf16x3": api.MIXED_BF16X3, "fp64": api.FP64}[args.precision]
     ns = api.NavierStokes(mesh, precision=precision, **solver_kw)
     dt = ns.params.dt
@@ -622,6 +627,8 @@ def main():
                               "exact-tangent Newton to rel.res 1e-8, " +
                               ("inexact Newton (Eisenstat-Walker forcing tolerances, Dirichlet values lifted "
                                "into the state at step start), " if args.forcing == "ew" else "") +
+                              ("tangent reused while Newton contracts within %g x the linear tolerance, "
+                               % args.tangent_reuse if (args.tangent_reuse > 0 and mixed) else "") +
                               ("RCR outlets coupled by the relaxed fixed point (relaxation %g, tolerance "
                                "1e-8 + 1e-6 |P|; %s), " % (OUTLET_RELAXATION,
                                                           "pressures updated inside the Newton loop"

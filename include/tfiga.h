@@ -122,6 +122,16 @@ typedef struct tfiga_ns_params {
 	 * that of the PDE rows at the lifted state.  0 (default): every system to
 	 * gmres_rtol and no lifting, as the reference. */
 	int32_t newton_forcing;        /* default 0 */
+	/* Tensor-core modes: a factor c > 0 keeps the previous Newton iteration's
+	 * tangent (and its Dirichlet rows) while that iteration reached what its linear
+	 * tolerance allowed, |r_k| <= c eta_{k-1} |r_{k-1}| (eta the relative tolerance
+	 * of the previous linear solve): a tangent that still gives the contraction the
+	 * linear solve asked for is good enough.  The tangent is contracted afresh at the
+	 * first iteration of every step and whenever the contraction falls short.  The
+	 * residual is always evaluated in FP64 at the current state, so only the Newton
+	 * convergence rate can change.  Ignored in TFIGA_PRECISION_FP64 (its assembly
+	 * computes residual and tangent together).  Default 0 (off). */
+	double tangent_reuse_factor;   /* default 0 */
 } tfiga_ns_params;
 
 #define TFIGA_PRECISION_FP64 0

@@ -42,3 +42,34 @@ def test_forcing_step_matches_fixed_tolerance_step(cylinder_1280, precision_name
     assert rel(states[1][:, :3], states[0][:, :3]) < 1e-8
     assert rel(states[1][:, 3], states[0][:, 3]) < 1e-6
     assert reports[1]["linear_iterations"] < reports[0]["linear_iterations"]
+
+
+def test_tangent_reuse_step_matches_fixed_tolerance_step(cylinder_1280):
+    """Split-BF16 step with forcing and tangent reuse (factor 100): the same solution as the
+    fixed-tolerance step within the same tolerances, and no more tensor-core tangent launches than
+    the forcing step without reuse."""
+    from tubularflowiga_b200 import api
+    tube = cylinder_1280
+    vmask, pmask, vel = api.tube_boundary_conditions(tube, 0.2)
+    s0 = api.initial_state(vmask, vel * 0.9)
+    mesh = api.Mesh(tube.mesh)
+    states, tangents = {}, {}
+    for name, kw in (("fixed", {}), ("forcing", dict(newton_forcing=1)),
+                     ("reuse", dict(newton_forcing=1, tangent_reuse_factor=100.0))):
+        ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, preconditioner=api.AMG,
+                              precision=api.MIXED_BF16X3, nonlinear_rtol=1e-10, nonlinear_atol=1e-30,
+                              gmres_rtol=1e-10, max_newton=30, gmres_restart=64, **kw)
+        ns.set_dirichlet(vmask, pmask, vel)
+        ns.set_tractions({2: 0.0})
+        ns.set_state(s0, s0)
+        ns.set_profiling(True)
+        ns.profile(reset=True)
+        report = ns.step()
+        assert report["converged"]
+        tangents[name] = ns.profile()["assembly"][1]
+        states[name] = ns.get_state().reshape(-1, 4)
+        ns.close()
+    for name in ("forcing", "reuse"):
+        assert rel(states[name][:, :3], states["fixed"][:, :3]) < 1e-8
+        assert rel(states[name][:, 3], states["fixed"][:, 3]) < 1e-6
+    assert 1 <= tangents["reuse"] <= tangents["forcing"]

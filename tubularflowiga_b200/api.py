@@ -42,7 +42,8 @@ class NsParams(C.Structure):
                 ("mass_rtol", C.c_double), ("gmres_restart", C.c_int32), ("gmres_max_iterations", C.c_int32),
                 ("gmres_rtol", C.c_double), ("preconditioner", C.c_int32), ("precision", C.c_int32),
                 ("amg_coarse_nodes", C.c_int32), ("amg_coarse_period", C.c_int32),
-                ("krylov_fp64_basis", C.c_int32), ("newton_forcing", C.c_int32)]
+                ("krylov_fp64_basis", C.c_int32), ("newton_forcing", C.c_int32),
+                ("tangent_reuse_factor", C.c_double)]
 
 
 FP64 = 0

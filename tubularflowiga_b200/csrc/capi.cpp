@@ -185,6 +185,7 @@ void tfiga_ns_default_params(tfiga_ns_params* p)
 	p->amg_coarse_period = 1;
 	p->krylov_fp64_basis = 0;
 	p->newton_forcing = 0;
+	p->tangent_reuse_factor = 0.0;
 }
 
 int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out)

@@ -46,6 +46,8 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 	if (params.precision != TFIGA_PRECISION_FP64 && params.precision != TFIGA_PRECISION_MIXED
 		&& params.precision != TFIGA_PRECISION_FP32_JACOBIAN && params.precision != TFIGA_PRECISION_MIXED_BF16X3)
 		Fail(-1, "unknown precision "+std::to_string(params.precision));
+	if (!(params.tangent_reuse_factor >= 0.0 && std::isfinite(params.tangent_reuse_factor)))
+		Fail(-1, "tangent_reuse_factor must be finite and non-negative");
 	if (!tensor_tangent()) values_.Allocate((size_t)blocks()*16);
 	rhs_.Allocate(n4_); state_.Allocate(n4_); previous_.Allocate(n4_); update_.Allocate(n4_);
 	traction_.Allocate(n4_);
@@ -123,6 +125,7 @@ void NsSolver::SetDirichlet(const int32_t* vmask, const int32_t* pmask, const do
 	SetDirichletValues(velocity, pressure);
 	CudaCheck(cudaStreamSynchronize(stream_), "Dirichlet upload");
 	dirichlet_set_ = true;
+	tangent_valid_ = false;
 }
 
 void NsSolver::SetDirichletValues(const double* velocity, const double* pressure)
@@ -170,6 +173,7 @@ void NsSolver::ApplyTractions(const std::map<int32_t, double>& traction)
 
 void NsSolver::SetState(const double* state, const double* previous)
 {
+	tangent_valid_ = false;
 	state_.Upload(state, n4_, stream_);
 	previous_.Upload(previous ? previous : state, n4_, stream_);
 	CudaCheck(cudaStreamSynchronize(stream_), "state upload");
@@ -183,6 +187,7 @@ void NsSolver::GetState(double* state)
 
 void NsSolver::CommitStep()
 {
+	tangent_valid_ = false;
 	CudaCheck(cudaMemcpyAsync(previous_.get(), state_.get(), n4_*sizeof(double), cudaMemcpyDeviceToDevice, stream_),
 		"previous-state copy");
 }
@@ -382,10 +387,17 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 		report.converged = 1;
 		return report;
 	}
-	if (tc) {
+	// Tangent reuse: keep the previous iteration's tangent while that iteration contracted the
+	// residual about as far as its linear tolerance allowed.
+	const bool reuse = tc && params_.tangent_reuse_factor > 0.0 && tangent_valid_ && initial_residual >= 0.0
+		&& norm <= params_.tangent_reuse_factor*reuse_eta_*reuse_norm_;
+	reuse_norm_ = norm;
+	if (tc && !reuse) {
 		CudaCheck(cudaEventRecord(events_[4], stream_), "event");
 		AssembleTangentTc();
 		ApplyDirichletMatrix();
+		tangent_valid_ = true;
+		++tangent_contractions_;
 		CudaCheck(cudaEventRecord(events_[5], stream_), "event");
 		status_.Download(pinned_status_, 1, stream_);
 		CudaCheck(cudaStreamSynchronize(stream_), "tensor-core tangent");
@@ -414,6 +426,7 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 		forcing_norm_ = norm;
 		forcing_eta_ = eta;
 	}
+	reuse_eta_ = eta;
 	const GmresResult linear = SolveLinear(eta, params_.gmres_max_iterations);
 	CudaCheck(cudaEventRecord(events_[3], stream_), "event");
 	report.linear_iterations = linear.iterations;

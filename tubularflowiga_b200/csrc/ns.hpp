@@ -77,6 +77,7 @@ public:
 	// training pair stored after every Newton solve when `collect`.
 	void SetLearned(LearnedPreconditioner* learned, bool use, bool collect);
 	long long learned_fallbacks() const { return learned_fallbacks_; }
+	long long tangent_contractions() const { return tangent_contractions_; }
 	// Binds the current (Dirichlet-row) Jacobian as the operator of the learned stage's residual loss.
 	void BindLearnedOperator(LearnedPreconditioner& learned);
 
@@ -101,6 +102,9 @@ private:
 	long long launches_ = 0;
 	long long solves_ = 0;                   // linear solves so far (coarse refresh period)
 	double forcing_norm_ = 0.0, forcing_eta_ = 0.0;   // previous residual and forcing term (inexact Newton)
+	bool tangent_valid_ = false;             // values32_ holds the tangent of this step's last iteration
+	double reuse_norm_ = 0.0, reuse_eta_ = 0.0;   // previous Newton residual and linear tolerance (tangent reuse)
+	long long tangent_contractions_ = 0;     // tensor-core tangent launches
 	std::map<int32_t, double> tractions_;    // label -> pressure set by SetTractions
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
