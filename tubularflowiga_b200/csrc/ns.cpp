@@ -126,6 +126,7 @@ void NsSolver::SetDirichlet(const int32_t* vmask, const int32_t* pmask, const do
 	CudaCheck(cudaStreamSynchronize(stream_), "Dirichlet upload");
 	dirichlet_set_ = true;
 	tangent_valid_ = false;
+	amg_current_ = false;
 }
 
 void NsSolver::SetDirichletValues(const double* velocity, const double* pressure)
@@ -205,6 +206,7 @@ void NsSolver::AssembleResidualTc()
 
 void NsSolver::AssembleTangentTc()
 {
+	amg_current_ = false;
 	values32_.Zero(stream_);
 	profiler_.Begin(Profiler::kAssembly, stream_);
 	LaunchTangentTc(mesh_.view(), mesh_.phi32(), coef32_.get(), mesh_.element_blocks(), values32_.get(), status_.get(),
@@ -221,6 +223,7 @@ void NsSolver::Assemble()
 		AssembleTangentTc();
 		return;
 	}
+	amg_current_ = false;
 	values_.Zero(stream_);
 	rhs_.Zero(stream_);
 	profiler_.Begin(Profiler::kAssembly, stream_);
@@ -265,6 +268,7 @@ void NsSolver::ApplyDirichletMatrix()
 
 void NsSolver::ApplyDirichletParts(bool matrix, bool rhs)
 {
+	if (matrix) amg_current_ = false;
 	if (!dirichlet_set_) Fail(-1, "Dirichlet conditions have not been set");
 	double* r = rhs ? rhs_.get() : nullptr;
 	if (mixed())
@@ -292,12 +296,19 @@ GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 			return gmres_.SolveFlexible<double>(mesh_.pattern_view(), values_.get(), rhs_.get(), update_.get(), rtol,
 				max_iterations, *amg_, &launches_);
 		};
-		if (mixed()) {
-			if (!amg_->built()) amg_->Build(values32_.get());
-			amg_->Refresh(values32_.get(), solves_ % params_.amg_coarse_period == 0);
-		} else {
-			if (!amg_->built()) amg_->Build(values_.get());
-			amg_->Refresh(values_.get(), solves_ % params_.amg_coarse_period == 0);
+		// refresh the AMG data only when the Jacobian changed since the last refresh (a reused
+		// tangent keeps them); the dense coarse inverse every amg_coarse_period-th refresh
+		if (!amg_current_) {
+			const bool coarse = refreshes_ % params_.amg_coarse_period == 0;
+			if (mixed()) {
+				if (!amg_->built()) amg_->Build(values32_.get());
+				amg_->Refresh(values32_.get(), coarse);
+			} else {
+				if (!amg_->built()) amg_->Build(values_.get());
+				amg_->Refresh(values_.get(), coarse);
+			}
+			++refreshes_;
+			amg_current_ = true;
 		}
 		launches_ += amg_->launches()-before;
 		result = solve();

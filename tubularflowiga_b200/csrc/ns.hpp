@@ -105,6 +105,8 @@ private:
 	bool tangent_valid_ = false;             // values32_ holds the tangent of this step's last iteration
 	double reuse_norm_ = 0.0, reuse_eta_ = 0.0;   // previous Newton residual and linear tolerance (tangent reuse)
 	long long tangent_contractions_ = 0;     // tensor-core tangent launches
+	bool amg_current_ = false;               // the AMG data were refreshed from the current Jacobian
+	long long refreshes_ = 0;                // AMG refreshes so far (coarse refresh period)
 	std::map<int32_t, double> tractions_;    // label -> pressure set by SetTractions
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
