@@ -52,6 +52,18 @@ Legs of one run (rank 0 prints one JSON line):
             cores, scaled to time steps/s.
   --impl reference  only the CPU reference arm, as its own line.
 
+--workload transport: the two-species transport of the reference's `transport`
+command on the C3 Y-bifurcation, its own JSON line.  The velocity is that of
+one mixed Navier-Stokes step of C3 from rest (the flow the reference's
+`solve` chain hands to transport); a step is rhs = P c, the inlet values set,
+and L c' = rhs by block-Jacobi GMRES(50) to rtol 1e-8, warm-started.  value:
+device-timed steps with L and P resident in HBM (L alone 1.6 GB, beyond L2);
+e2e: the whole job through the C ABI from host buffers (velocity, mask and
+inlet values uploaded, assembly, the steps, the final state read back),
+steps / wall time; cpu_baseline: the CPU restatement of the step (2x2
+SpMV + block-Jacobi GMRES) on all host cores for a bounded number of
+iterations, scaled by the GPU's iterations per step.
+
 Multi-GPU: the single-mesh path does not shard ("replicas only"): under
 torchrun every rank runs an independent replica; value = total steps / max
 time over ranks.
@@ -340,13 +352,205 @@ def run_reference_arm(args, world, rank):
     return 0
 
 
+TRANSPORT_METRIC = "two-species transport time steps/s (backward Euler, block-Jacobi GMRES(50) rtol 1e-8)"
+# Transport coefficients of the transport workload (SI): a small solute (D 1e-9 m^2/s) exchanging with an
+# advected species (k+ 1/s, k- 0.1/s, k'+ 0.5/s), inlet values N0 1, N+ 0.5, artificial diffusion 1e-6 m^2/s,
+# dt 2e-3 s as the flow.
+TRANSPORT = dict(diffusion=1e-9, vplus=1.0, kplus=1.0, kminus=0.1, detach_plus=0.5, dt=2e-3, n0_bc=1.0,
+                 nplus_bc=0.5, artificial_diffusion=1e-6)
+
+
+def flow_velocity(api, mesh, tube, wave):
+    """Nodal velocity [n, 3] after one mixed Navier-Stokes step of C3 from rest."""
+    ns = api.NavierStokes(mesh, precision=api.MIXED_BF16X3, density=RHO, viscosity=MU, dt=DT,
+                          nonlinear_rtol=1e-8, nonlinear_atol=1e-300, gmres_restart=64, gmres_max_iterations=5000,
+                          gmres_rtol=1e-8, preconditioner=api.AMG, amg_coarse_period=3, newton_forcing=1,
+                          tangent_reuse_factor=100.0)
+    vmask, pmask, velocity_at = boundary(tube, wave)
+    ns.set_dirichlet(vmask, pmask, velocity_at(0.0))
+    s0 = api.initial_state(vmask, velocity_at(0.0))
+    ns.set_state(s0, s0)
+    outlets = [api.Outlet(**m.as_dict()) for m in outlet_models("c3")]
+    api.check(api.lib().tfiga_ns_set_dirichlet_values(ns._h, _host_ptr(velocity_at(DT).ravel()), None))
+    ns.commit_step()
+    outlet_step(ns, outlets, "newton")
+    v = ns.get_state().reshape(-1, 4)[:, :3].copy()
+    ns.close()
+    return v
+
+
+def _host_ptr(a):
+    from tubularflowiga_b200 import api
+    a = np.ascontiguousarray(a, np.float64)
+    _host_ptr.keep = a
+    return api.C.c_void_p(a.ctypes.data)
+
+
+def transport_cpu_reference(mesh, left, previous, state, iterations_per_step, budget_iterations=30):
+    """CPU restatement of one transport step on all host cores: 2x2 SpMV P c and block-Jacobi GMRES(50) run
+    for a bounded number of iterations, scaled to the GPU's iterations per step."""
+    from oracle import oracle as O
+    ro, cols, diag = mesh.pattern()
+    t0 = time.perf_counter()
+    rhs = O.transport_spmv(ro, cols, previous, state)
+    t_spmv = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    _, its, _ = O.transport_gmres(ro, cols, diag, left, rhs, state, restart=50, maxit=budget_iterations,
+                                  rtol=1e-300)
+    t_gmres = time.perf_counter() - t0
+    its = max(its if its > 0 else budget_iterations, 1)
+    step_s = t_spmv + t_gmres * iterations_per_step / its
+    return {"value": 1.0 / step_s, "unit": "time steps/s", "cores": O.max_threads(), "kind": "port",
+            "sample": "one 2x2 SpMV (P c) and %d block-Jacobi GMRES(50) iterations (CPU restatement, including "
+                      "its block-inverse build) on the full C3 transport system, scaled to %.1f iterations "
+                      "per step" % (budget_iterations, iterations_per_step)}
+
+
+def run_transport(args, world, rank, local):
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    from tubularflowiga_b200 import api
+    tube, desc, wave = workload("c3")
+    n = tube.mesh.nodes
+    mesh = api.Mesh(tube.mesh)
+    velocity = flow_velocity(api, mesh, tube, wave)
+    params = api.transport_params(steps=args.warmup + args.steps, **TRANSPORT)
+    mask, n0, nplus = api.resolve_transport_boundaries(tube.labels, velocity, params)
+    velocity_pinned = torch.tensor(velocity.ravel()).pin_memory()
+    mask_pinned = torch.tensor(mask).pin_memory()
+    n0_pinned = torch.tensor(n0).pin_memory()
+    nplus_pinned = torch.tensor(nplus).pin_memory()
+    out_pinned = torch.empty(2 * n, dtype=torch.float64).pin_memory()
+
+    def create():
+        h = api.C.c_void_p()
+        api.check(api.lib().tfiga_transport_create(mesh._h, api.C.byref(params),
+                                                   api.C.c_void_p(velocity_pinned.data_ptr()),
+                                                   api.C.c_void_p(mask_pinned.data_ptr()),
+                                                   api.C.c_void_p(n0_pinned.data_ptr()),
+                                                   api.C.c_void_p(nplus_pinned.data_ptr()), api.C.byref(h)))
+        return h
+
+    lib = api.lib()
+    h = create()
+    report = api.TransportReport()
+    assembly_ms = api.C.c_double()
+    api.check(lib.tfiga_transport_info(h, api.C.byref(assembly_ms), None, None))
+    stream_ptr = api.C.c_void_p()
+    api.check(lib.tfiga_transport_stream(h, api.C.byref(stream_ptr)))
+    stream = torch.cuda.ExternalStream(stream_ptr.value)
+    api.check(lib.tfiga_transport_step(h, args.warmup, api.C.byref(report)))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = api.C.c_int64()
+    api.check(lib.tfiga_transport_info(h, None, None, api.C.byref(launches0)))
+    api.check(lib.tfiga_transport_set_profiling(h, 1))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        api.check(lib.tfiga_transport_step(h, args.steps, api.C.byref(report)))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches1 = api.C.c_int64()
+    api.check(lib.tfiga_transport_info(h, None, None, api.C.byref(launches1)))
+    fam_ms = np.zeros(5)
+    fam_n = np.zeros(5, np.int64)
+    api.check(lib.tfiga_transport_profile(h, api.C.c_void_p(fam_ms.ctypes.data), api.C.c_void_p(fam_n.ctypes.data), 1))
+    api.check(lib.tfiga_transport_set_profiling(h, 0))
+    timed = report.as_dict()
+    left = previous = state = None
+    if not args.no_cpu_baseline and world == 1 and rank == 0:
+        left = np.zeros(4 * mesh.blocks)
+        previous = np.zeros(4 * mesh.blocks)
+        api.check(lib.tfiga_transport_matrices(h, api.C.c_void_p(left.ctypes.data),
+                                               api.C.c_void_p(previous.ctypes.data)))
+        state = np.zeros(2 * n)
+        api.check(lib.tfiga_transport_get_state(h, api.C.c_void_p(state.ctypes.data)))
+    api.check(lib.tfiga_transport_destroy(h))
+    # e2e: the whole job through the C ABI from pinned host buffers, final state read back
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h = create()
+    api.check(lib.tfiga_transport_step(h, args.warmup + args.steps, None))
+    api.check(lib.tfiga_transport_get_state(h, api.C.c_void_p(out_pinned.data_ptr())))
+    e2e_s = time.perf_counter() - t0
+    api.check(lib.tfiga_transport_destroy(h))
+    total_steps = args.warmup + args.steps
+    ms, e2e_ms = max_over_ranks(dist, [ms, e2e_s * 1e3], "cuda")
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+    hbm, _, peak_kind = peaks()
+    its_per_step = timed["total_iterations"] / max(args.steps, 1)
+    spmv_ms, spmv_n = float(fam_ms[1]), int(fam_n[1])
+    orth_ms, orth_n = float(fam_ms[2]), int(fam_n[2])
+    # one block-Jacobi SpMV launch: 2x2 values (32 B) + column index (4 B) per block, row offsets, the
+    # input vector and the output once (16 B per node each), the 2x2 inverse (32 B per node)
+    spmv_bytes = mesh.blocks * 36 + 4 * (n + 1) + 16 * n * 2 + 32 * n
+    kernels = {}
+    if spmv_n:
+        a = spmv_bytes / (spmv_ms / spmv_n * 1e-3) / 1e9
+        kernels["spmv_block_jacobi_2x2"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
+                                            "frac": a / hbm, "traffic": None, "launches": spmv_n,
+                                            "avg_ms": spmv_ms / spmv_n, "share": spmv_ms / ms,
+                                            "algorithmic_bytes": spmv_bytes}
+    if orth_n:
+        kernels["krylov_orthogonalisation"] = {"launches": orth_n, "avg_ms": orth_ms / orth_n,
+                                               "share": orth_ms / ms}
+    roof = dict(kernels.get("spmv_block_jacobi_2x2", {}))
+    roof["kernel"] = "spmv_block_jacobi_2x2"
+    roof["peak_kind"] = f"{peak_kind} hbm_gbs"
+    line = {
+        "metric": TRANSPORT_METRIC, "value": replica_throughput(world, args.steps, ms), "unit": "time steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator; velocity from one Navier-Stokes step of the same mesh)",
+        "config": {"workload": "two-species transport on the " + desc, "elements": tube.mesh.elements, "nodes": n,
+                   "block_nonzeros": mesh.blocks, "coefficients": TRANSPORT,
+                   "solver": "backward Euler, constant L and P assembled once; block-Jacobi GMRES(50) rtol 1e-8 "
+                             "warm-started; FP64",
+                   "l2": "inputs larger than L2 (L %.2f GB)" % (mesh.blocks * 32 / 1e9),
+                   "parallelism": "replicas only" if world > 1 else "single GPU"},
+        "gmres_iterations_per_step": its_per_step, "final_l2": timed["final_l2"],
+        "assembly_ms": assembly_ms.value, "roofline": roof, "kernels": kernels,
+        "gpu_launches": int(launches1.value - launches0.value), "clocks": clocks.summary(),
+        "e2e": {"value": replica_throughput(world, total_steps, e2e_ms), "unit": "time steps/s",
+                "h2d_bytes_per_step": (velocity.nbytes + mask.nbytes + n0.nbytes + nplus.nbytes) / total_steps,
+                "d2h_bytes_per_step": 16 * n / total_steps,
+                "includes": "create (uploads and assembly) + %d steps + final state read back" % total_steps},
+    }
+    if left is not None:
+        try:
+            cb = transport_cpu_reference(mesh, left, previous, state, its_per_step)
+            line["cpu_baseline"] = cb
+        except Exception as exc:  # noqa: BLE001 -- reported, not hidden
+            line["cpu_baseline"] = {"value": None, "error": str(exc)}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c1", "c2-100", "c5"])
+    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c1", "c2-100", "c5", "transport"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "mixed", "fp64"])
@@ -369,6 +573,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, world, rank)
+    if args.workload == "transport":
+        return run_transport(args, world, rank, local)
 
     import torch
     dist = None

@@ -43,6 +43,7 @@ extern "C" {
 typedef struct tfiga_mesh tfiga_mesh;
 typedef struct tfiga_ns tfiga_ns;
 typedef struct tfiga_learned tfiga_learned;
+typedef struct tfiga_transport tfiga_transport;
 
 /* Flattened mesh, the layout of iga::cuda::FlatMesh
  * (solvers/cuda/include/DeviceMesh.hpp:16-57). */
@@ -368,6 +369,97 @@ int tfiga_learned_loss_gradient_device(tfiga_learned* learned, const double* x_d
 int tfiga_learned_save(const tfiga_learned* learned, const char* path);
 int tfiga_learned_load(tfiga_learned* learned, const char* path);
 
+/* ---- two-species transport ------------------------------------------ */
+/* The `iga_cuda transport` path (Transport, solvers/cuda/src/iga_cuda.cu:621-732):
+ * N0 (attached: diffusion and exchange) and N+ (advected by a prescribed nodal
+ * velocity, SUPG-stabilised) on the mesh of a tfiga_mesh, 2 unknowns per node
+ * stored value[2*node + field] (field 0 = N0, 1 = N+), 2x2 blocks
+ * values[block*4 + 2*i + j] on the mesh's block pattern.  Backward Euler with
+ * a constant left matrix L and previous-state matrix P assembled once
+ * (AssembleTransportKernel, IgaCudaKernels.cuh:155-237; the CPU element is
+ * BuildTransportElement, solvers/cpu/include/TransportElement.hpp:213-253);
+ * constrained rows zeroed with an identity diagonal block in L
+ * (ApplyTransportBoundaryKernel, IgaCudaKernels.cuh:411-424).  A step is
+ * rhs = P c, the boundary values written into rhs
+ * (SetTransportBoundaryVectorKernel :426-434), then L c' = rhs by block-Jacobi
+ * GMRES(restart) to gmres_rtol of the preconditioned residual, started from 0
+ * on the first step and from c afterwards, the block inverse built once. */
+
+/* iga::TransportParameters (solvers/cpu/include/CaseInput.hpp:19-33) plus the
+ * solver settings the reference fixes in Transport (restart 50, rtol 1e-8,
+ * at most 10000 iterations: iga_cuda.cu:660, 691). */
+typedef struct tfiga_transport_params {
+	double diffusion;            /* D: N0 diffusion */
+	double vplus;                /* inlet velocity scale; weights the artificial diffusion */
+	double vminus;               /* read, unused by the two-species model */
+	double kplus;                /* N0 -> N+ exchange rate */
+	double kminus;               /* N0 loss rate */
+	double detach_plus;          /* k'plus: N+ -> N0 detachment rate */
+	double detach_minus;         /* k'minus: read, unused */
+	double dt;
+	int32_t steps;               /* nstep */
+	int32_t restart;             /* GMRES restart */
+	double n0_bc;                /* N0bc: legacy inlet value of N0 */
+	double nplus_bc;             /* Nplusbc: legacy inlet value of N+ */
+	double nminus_bc;            /* Nminusbc: read, unused */
+	double artificial_diffusion; /* SUPG-weighted artificial diffusion coefficient */
+	double gmres_rtol;
+	int32_t gmres_max_iterations;
+	int32_t reserved;
+} tfiga_transport_params;
+
+/* Totals of one tfiga_transport_step call (the `transport step=` and
+ * `transport_cuda` log lines, iga_cuda.cu:702-731). */
+typedef struct tfiga_transport_report {
+	int32_t steps;               /* steps taken by the call */
+	int32_t last_iterations;     /* GMRES iterations of the last step */
+	int64_t total_iterations;    /* over the call's steps */
+	double last_residual;        /* final preconditioned residual of the last step */
+	double final_l2;             /* ||c||_2 after the last step (cublasDnrm2, iga_cuda.cu:711-713) */
+	uint32_t singular_blocks;    /* singular diagonal blocks of the block-Jacobi build */
+	uint32_t reserved;
+} tfiga_transport_report;
+
+/* Zeros, restart 50, gmres_rtol 1e-8, gmres_max_iterations 10000. */
+void tfiga_transport_default_params(tfiga_transport_params* params);
+/* simulation_parameter.txt (ReadTransportParameters, CaseInput.hpp:85-118) into
+ * the physical fields of *params (solver fields untouched).  Errors:
+ * TFIGA_E_IO (unreadable), TFIGA_E_FORMAT (missing key, dt <= 0, nstep < 0). */
+int tfiga_transport_read_params(const char* path, tfiga_transport_params* params);
+/* Boundary resolution of a legacy case (ResolveBoundaryConditions,
+ * CaseInput.hpp:162-258): labels[nodes] of controlmesh.vtk, the reference
+ * velocity [3*nodes] and, when case_config_path names an existing file, its
+ * schema-1 rules (ReadCaseConfiguration, include/CaseConfig.hpp:280-387).
+ * Writes the transport mask and values [nodes] (any may be NULL) and returns
+ * the constrained count in *transport_nodes. */
+int tfiga_transport_resolve_boundaries(int64_t nodes, const int32_t* labels, const double* reference_velocity,
+	const tfiga_transport_params* params, const char* case_config_path, int32_t* constrained, double* n0,
+	double* nplus, int64_t* transport_nodes);
+/* Assembles L and P from the nodal velocity [3*nodes], applies the boundary
+ * rows of the constrained[nodes] mask and sets the boundary values n0/nplus
+ * [nodes] into the zero initial state (iga_cuda.cu:664-679).  Host or device
+ * pointers.  The handle keeps a reference to the mesh. */
+int tfiga_transport_create(tfiga_mesh* mesh, const tfiga_transport_params* params, const double* velocity,
+	const int32_t* constrained, const double* n0, const double* nplus, tfiga_transport** out);
+int tfiga_transport_destroy(tfiga_transport* transport);
+/* `steps` backward-Euler steps (the loop of iga_cuda.cu:683-707); report may
+ * be NULL.  TFIGA_E_NOT_CONVERGED when a step's GMRES stops above tolerance. */
+int tfiga_transport_step(tfiga_transport* transport, int32_t steps, tfiga_transport_report* report);
+/* State c [2*nodes], host or device. */
+int tfiga_transport_set_state(tfiga_transport* transport, const double* state);
+int tfiga_transport_get_state(tfiga_transport* transport, double* state);
+/* L and P after the boundary rows, [4*blocks] each (either may be NULL). */
+int tfiga_transport_matrices(tfiga_transport* transport, double* left, double* previous);
+/* Device time of the assembly launch sequence (ms), steps taken, kernel launches issued. */
+int tfiga_transport_info(const tfiga_transport* transport, double* assembly_ms, int32_t* steps, int64_t* launches);
+/* The handle's CUDA stream (a cudaStream_t). */
+int tfiga_transport_stream(tfiga_transport* transport, void** stream);
+/* Per-family device timing as tfiga_ns_set_profiling / tfiga_ns_profile:
+ * family 1 SpMV (P c and the block-Jacobi SpMV of GMRES), 2 Krylov
+ * orthogonalisation; the others stay 0. */
+int tfiga_transport_set_profiling(tfiga_transport* transport, int enable);
+int tfiga_transport_profile(tfiga_transport* transport, double* milliseconds, int64_t* launches, int32_t reset);
+
 /* ---- allocation-free kernel ------------------------------------------- */
 /* *norm_device = ||b - A x||_2 for a 4x4 block-CSR matrix given entirely by
  * device pointers (row_offsets [nodes+1], columns and values [blocks*16]
@@ -386,8 +478,9 @@ int tfiga_block_residual_norm_static(int64_t nodes, const int32_t* row_offsets_d
 /* ---- drop-in command ------------------------------------------------- */
 /* `navier-stokes DATABASE CASE_DIR [MAX_NEWTON] [OUTPUT] [options]`, the argv of
  * iga_cuda's navier-stokes command (ParseCudaFlowOptions iga_cuda.cu:447-498,
- * NavierStokes :734-1153).  argv[0] is the program name, argv[1] the command
- * ("navier-stokes", "mesh-check" or "device-info").  Prints the reference's
+ * NavierStokes :734-1153), or `transport DATABASE CASE_DIR [STEPS] [OUTPUT]
+ * [VELOCITY]` (Transport :621-732).  argv[0] is the program name, argv[1] the
+ * command ("navier-stokes", "transport", "mesh-check" or "device-info").  Prints the reference's
  * key=value lines to stdout; returns the process exit code (0 or 1). */
 int tfiga_main(int argc, char** argv);
 

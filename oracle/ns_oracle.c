@@ -618,71 +618,82 @@ void tfo_apply_dirichlet(int nodes, const int* row_offsets, const int* diagonal,
 		}
 }
 
-/* y = A x over 4x4 blocks (BlockSpmvKernel, SparseKernels.cuh:25-40). */
-void tfo_spmv(int nodes, const int* row_offsets, const int* columns, const double* values,
+/* y = A x over F x F blocks (BlockSpmvKernel<F>, SparseKernels.cuh:25-40), F <= 4. */
+static void spmv_f(int F, int nodes, const int* row_offsets, const int* columns, const double* values,
 	const double* x, double* y)
 {
 #pragma omp parallel for schedule(static)
 	for (int row = 0; row < nodes; ++row) {
 		double r[4] = {0, 0, 0, 0};
 		for (int b = row_offsets[row]; b < row_offsets[row+1]; ++b) {
-			const double* blk = values+(size_t)b*16;
-			const double* xc = x+4*(size_t)columns[b];
-			for (int i = 0; i < 4; ++i)
-				r[i] += blk[i*4]*xc[0]+blk[i*4+1]*xc[1]+blk[i*4+2]*xc[2]+blk[i*4+3]*xc[3];
+			const double* blk = values+(size_t)b*F*F;
+			const double* xc = x+(size_t)F*columns[b];
+			for (int i = 0; i < F; ++i)
+				for (int j = 0; j < F; ++j) r[i] += blk[i*F+j]*xc[j];
 		}
-		for (int i = 0; i < 4; ++i) y[4*(size_t)row+i] = r[i];
+		for (int i = 0; i < F; ++i) y[(size_t)F*row+i] = r[i];
 	}
 }
 
+void tfo_spmv(int nodes, const int* row_offsets, const int* columns, const double* values,
+	const double* x, double* y)
+{
+	spmv_f(4, nodes, row_offsets, columns, values, x, y);
+}
+
 /* Diagonal-block Gauss-Jordan inverse with partial pivoting and the
- * singular fallback (BuildBlockInverseKernel, SparseKernels.cuh:42-89). */
-int tfo_block_inverse(int nodes, const int* diagonal, const double* values, double* inverse)
+ * singular fallback (BuildBlockInverseKernel<F>, SparseKernels.cuh:42-89), F <= 4. */
+static int block_inverse_f(int F, int nodes, const int* diagonal, const double* values, double* inverse)
 {
 	int singular = 0;
 #pragma omp parallel for schedule(static) reduction(+:singular)
 	for (int node = 0; node < nodes; ++node) {
-		const double* s = values+(size_t)diagonal[node]*16;
+		const double* s = values+(size_t)diagonal[node]*F*F;
 		double m[4][8];
-		for (int i = 0; i < 4; ++i)
-			for (int j = 0; j < 8; ++j) m[i][j] = j < 4 ? s[i*4+j] : (j-4 == i ? 1.0 : 0.0);
+		for (int i = 0; i < F; ++i)
+			for (int j = 0; j < 2*F; ++j) m[i][j] = j < F ? s[i*F+j] : (j-F == i ? 1.0 : 0.0);
 		int failed = 0;
-		for (int pivot = 0; pivot < 4; ++pivot) {
+		for (int pivot = 0; pivot < F; ++pivot) {
 			int best = pivot;
-			for (int row = pivot+1; row < 4; ++row)
+			for (int row = pivot+1; row < F; ++row)
 				if (fabs(m[row][pivot]) > fabs(m[best][pivot])) best = row;
 			if (!isfinite(m[best][pivot]) || fabs(m[best][pivot]) < 1e-14) { failed = 1; break; }
 			if (best != pivot)
-				for (int c = 0; c < 8; ++c) { const double t = m[pivot][c]; m[pivot][c] = m[best][c]; m[best][c] = t; }
+				for (int c = 0; c < 2*F; ++c) { const double t = m[pivot][c]; m[pivot][c] = m[best][c]; m[best][c] = t; }
 			const double scale = 1.0/m[pivot][pivot];
-			for (int c = 0; c < 8; ++c) m[pivot][c] *= scale;
-			for (int row = 0; row < 4; ++row) {
+			for (int c = 0; c < 2*F; ++c) m[pivot][c] *= scale;
+			for (int row = 0; row < F; ++row) {
 				if (row == pivot) continue;
 				const double factor = m[row][pivot];
-				for (int c = 0; c < 8; ++c) m[row][c] -= factor*m[pivot][c];
+				for (int c = 0; c < 2*F; ++c) m[row][c] -= factor*m[pivot][c];
 			}
 		}
-		double* d = inverse+(size_t)node*16;
+		double* d = inverse+(size_t)node*F*F;
 		if (!failed) {
-			for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) d[i*4+j] = m[i][4+j];
+			for (int i = 0; i < F; ++i) for (int j = 0; j < F; ++j) d[i*F+j] = m[i][F+j];
 		} else {
 			++singular;
-			for (int i = 0; i < 4; ++i)
-				for (int j = 0; j < 4; ++j)
-					d[i*4+j] = i == j && fabs(s[i*4+i]) > 1e-14 ? 1.0/s[i*4+i] : (i == j ? 1.0 : 0.0);
+			for (int i = 0; i < F; ++i)
+				for (int j = 0; j < F; ++j)
+					d[i*F+j] = i == j && fabs(s[i*F+i]) > 1e-14 ? 1.0/s[i*F+i] : (i == j ? 1.0 : 0.0);
 		}
 	}
 	return singular;
 }
 
-static void apply_block_inverse(int nodes, const double* inverse, const double* x, double* y)
+int tfo_block_inverse(int nodes, const int* diagonal, const double* values, double* inverse)
+{
+	return block_inverse_f(4, nodes, diagonal, values, inverse);
+}
+
+static void apply_block_inverse_f(int F, int nodes, const double* inverse, const double* x, double* y)
 {
 #pragma omp parallel for schedule(static)
 	for (int node = 0; node < nodes; ++node)
-		for (int i = 0; i < 4; ++i) {
+		for (int i = 0; i < F; ++i) {
 			double r = 0.0;
-			for (int j = 0; j < 4; ++j) r += inverse[((size_t)node*4+i)*4+j]*x[4*(size_t)node+j];
-			y[4*(size_t)node+i] = r;
+			for (int j = 0; j < F; ++j) r += inverse[((size_t)node*F+i)*F+j]*x[(size_t)F*node+j];
+			y[(size_t)F*node+i] = r;
 		}
 }
 
@@ -708,12 +719,12 @@ static void axpy(long long n, double alpha, const double* x, double* y)
  * iteration count (>= 0) or TFO_NOT_CONVERGED; *residual gets the final
  * preconditioned residual norm.
  */
-int tfo_gmres_bjacobi(int nodes, const int* row_offsets, const int* columns, const int* diagonal,
+static int gmres_bjacobi_f(int F, int nodes, const int* row_offsets, const int* columns, const int* diagonal,
 	const double* values, const double* rhs, double* x, int restart, int maximum_iterations,
 	double rtol, double* residual_out, int* singular_out)
 {
-	const long long n = 4LL*nodes;
-	double* inverse = (double*)malloc(sizeof(double)*(size_t)n*4);
+	const long long n = (long long)F*nodes;
+	double* inverse = (double*)malloc(sizeof(double)*(size_t)n*F);
 	double* raw = (double*)malloc(sizeof(double)*(size_t)n);
 	double* res = (double*)malloc(sizeof(double)*(size_t)n);
 	double* work = (double*)malloc(sizeof(double)*(size_t)n);
@@ -724,11 +735,11 @@ int tfo_gmres_bjacobi(int nodes, const int* row_offsets, const int* columns, con
 	double* g = (double*)calloc((size_t)restart+1, sizeof(double));
 	double* y = (double*)calloc((size_t)restart, sizeof(double));
 	if (!inverse || !raw || !res || !work || !V || !h || !cs || !sn || !g || !y) return TFO_NO_MEMORY;
-	const int singular = tfo_block_inverse(nodes, diagonal, values, inverse);
+	const int singular = block_inverse_f(F, nodes, diagonal, values, inverse);
 	if (singular_out) *singular_out = singular;
-	tfo_spmv(nodes, row_offsets, columns, values, x, raw);
+	spmv_f(F, nodes, row_offsets, columns, values, x, raw);
 	for (long long i = 0; i < n; ++i) res[i] = rhs[i]-raw[i];
-	apply_block_inverse(nodes, inverse, res, work);
+	apply_block_inverse_f(F, nodes, inverse, res, work);
 	const double initial = sqrt(dot(n, work, work));
 	int iterations = 0, converged = 0;
 	double residual = initial;
@@ -742,8 +753,8 @@ int tfo_gmres_bjacobi(int nodes, const int* row_offsets, const int* columns, con
 		g[0] = beta;
 		int used = 0;
 		for (int j = 0; j < restart && iterations < maximum_iterations; ++j) {
-			tfo_spmv(nodes, row_offsets, columns, values, V+(size_t)j*n, raw);
-			apply_block_inverse(nodes, inverse, raw, work);
+			spmv_f(F, nodes, row_offsets, columns, values, V+(size_t)j*n, raw);
+			apply_block_inverse_f(F, nodes, inverse, raw, work);
 			for (int i = 0; i <= j; ++i) {
 				const double value = dot(n, V+(size_t)i*n, work);
 				h[(size_t)i*restart+j] = value;
@@ -778,9 +789,9 @@ int tfo_gmres_bjacobi(int nodes, const int* row_offsets, const int* columns, con
 			y[row] = value/h[(size_t)row*restart+row];
 		}
 		for (int i = 0; i < used; ++i) axpy(n, y[i], V+(size_t)i*n, x);
-		tfo_spmv(nodes, row_offsets, columns, values, x, raw);
+		spmv_f(F, nodes, row_offsets, columns, values, x, raw);
 		for (long long i = 0; i < n; ++i) res[i] = rhs[i]-raw[i];
-		apply_block_inverse(nodes, inverse, res, work);
+		apply_block_inverse_f(F, nodes, inverse, res, work);
 		beta = sqrt(dot(n, work, work));
 		residual = beta;
 		if (beta <= tolerance) converged = 1;
@@ -790,6 +801,30 @@ int tfo_gmres_bjacobi(int nodes, const int* row_offsets, const int* columns, con
 	return converged ? iterations : TFO_NOT_CONVERGED;
 }
 
+int tfo_gmres_bjacobi(int nodes, const int* row_offsets, const int* columns, const int* diagonal,
+	const double* values, const double* rhs, double* x, int restart, int maximum_iterations,
+	double rtol, double* residual_out, int* singular_out)
+{
+	return gmres_bjacobi_f(4, nodes, row_offsets, columns, diagonal, values, rhs, x, restart, maximum_iterations,
+		rtol, residual_out, singular_out);
+}
+
+/* The same GMRES on the 2x2 transport system (SolveGmres<2>, iga_cuda.cu:691). */
+int tfo_transport_gmres(int nodes, const int* row_offsets, const int* columns, const int* diagonal,
+	const double* values, const double* rhs, double* x, int restart, int maximum_iterations,
+	double rtol, double* residual_out, int* singular_out)
+{
+	return gmres_bjacobi_f(2, nodes, row_offsets, columns, diagonal, values, rhs, x, restart, maximum_iterations,
+		rtol, residual_out, singular_out);
+}
+
+/* y = A x over 2x2 blocks (BlockSpmvKernel<2>). */
+void tfo_transport_spmv(int nodes, const int* row_offsets, const int* columns, const double* values,
+	const double* x, double* y)
+{
+	spmv_f(2, nodes, row_offsets, columns, values, x, y);
+}
+
 int tfo_max_threads(void)
 {
 #ifdef _OPENMP
@@ -797,4 +832,145 @@ int tfo_max_threads(void)
 #else
 	return 1;
 #endif
+}
+
+/* ---------------------------------------------------------------------------
+ * Two-species transport (N0 attached, N+ advected): the reference's
+ * `iga_cuda transport` path.
+ * ------------------------------------------------------------------------- */
+
+/*
+ * Transport parameters, in the order of iga::TransportParameters
+ * (solvers/cpu/include/CaseInput.hpp:19-33): D, vplus, vminus, kplus,
+ * kminus, k'plus, k'minus, dt, (steps), N0bc, Nplusbc, Nminusbc,
+ * artificial_diffusion.  Only the ones the element reads are passed here:
+ * p[0] D, p[1] vplus, p[2] kplus, p[3] kminus, p[4] k'plus, p[5] dt,
+ * p[6] artificial_diffusion.
+ */
+
+/*
+ * BuildTransportElement (TransportElement.hpp:213-253; the device form is
+ * AssembleTransportKernel, IgaCudaKernels.cuh:155-237): the backward-Euler
+ * left matrix and the previous-state matrix of one element, dense
+ * (2 nen)^2 with dof 2a = N0 and 2a+1 = N+ of basis a.  velocity[a*3+d] is
+ * the nodal velocity of basis a.  Per Gauss point:
+ *   u = sum_a N_a u_a,  tau = (|u.grad N|_1^-2 + (dt/2)^-2)^-1/2 (0 if u.grad N = 0),
+ *   T_a = N_a + tau u.grad N_a (SUPG test function of N+),
+ *   L00 += ((1 + dt (k+ + k-)) N_a N_b + dt D grad N_a.grad N_b) w
+ *   L0+ += -k'+ dt N_a N_b w
+ *   L+0 += -k+ dt T_a N_b w
+ *   L++ += ((1 + dt k'+) T_a N_b + dt T_a u.grad N_b + dt v+ ad T_a grad N_a.grad N_b) w
+ *   P00 += N_a N_b w,  P++ += T_a N_b w,
+ * with w the Gauss weight times det(dx/dxi).
+ */
+int tfo_transport_element(const double* C, const double* X, int nen, const double* velocity,
+	const double* p, double* left, double* previous)
+{
+	if (nen <= 0 || nen > 80) return TFO_BAD_INPUT;
+	const double D = p[0], vplus = p[1], kplus = p[2], kminus = p[3], detach = p[4], dt = p[5],
+		artificial = p[6];
+	const int ndof = 2*nen;
+	memset(left, 0, sizeof(double)*(size_t)ndof*ndof);
+	memset(previous, 0, sizeof(double)*(size_t)ndof*ndof);
+	double qp[64*3], qw[64], N[80], dN[240], T[80], inv[9], det;
+	tfo_gauss_rule(qp, qw);
+	for (int q = 0; q < 64; ++q) {
+		const int st = tfo_basis(C, X, nen, qp[3*q], qp[3*q+1], qp[3*q+2], 0, N, dN, NULL, inv, &det);
+		if (st != TFO_OK) return st;
+		const double w = qw[q]*det;
+		double u[3] = {0.0, 0.0, 0.0};
+		for (int a = 0; a < nen; ++a)
+			for (int d = 0; d < 3; ++d) u[d] += N[a]*velocity[a*3+d];
+		double inverse_length = 0.0;
+		for (int a = 0; a < nen; ++a)
+			inverse_length += fabs(u[0]*dN[3*a]+u[1]*dN[3*a+1]+u[2]*dN[3*a+2]);
+		const double tau_space = inverse_length > 0.0 ? 1.0/inverse_length : 0.0;
+		const double tau_time = dt/2.0;
+		const double tau = tau_space > 0.0
+			? 1.0/sqrt(1.0/(tau_space*tau_space)+1.0/(tau_time*tau_time)) : 0.0;
+		for (int a = 0; a < nen; ++a)
+			T[a] = N[a]+tau*(u[0]*dN[3*a]+u[1]*dN[3*a+1]+u[2]*dN[3*a+2]);
+		for (int a = 0; a < nen; ++a)
+			for (int b = 0; b < nen; ++b) {
+				const double gg = dN[3*a]*dN[3*b]+dN[3*a+1]*dN[3*b+1]+dN[3*a+2]*dN[3*b+2];
+				const double adv = u[0]*dN[3*b]+u[1]*dN[3*b+1]+u[2]*dN[3*b+2];
+				const double mass = N[a]*N[b];
+				double* l0 = left+(size_t)(2*a)*ndof+2*b;
+				double* lp = left+(size_t)(2*a+1)*ndof+2*b;
+				l0[0] += ((1.0+dt*(kplus+kminus))*mass+dt*D*gg)*w;
+				l0[1] += -detach*dt*mass*w;
+				lp[0] += -kplus*dt*T[a]*N[b]*w;
+				lp[1] += ((1.0+dt*detach)*T[a]*N[b]+dt*T[a]*adv+dt*vplus*artificial*T[a]*gg)*w;
+				previous[(size_t)(2*a)*ndof+2*b] += mass*w;
+				previous[(size_t)(2*a+1)*ndof+2*b+1] += T[a]*N[b]*w;
+			}
+	}
+	return TFO_OK;
+}
+
+/*
+ * Global transport assembly into 2x2 block CSR (values[block*4 + 2i + j]) over
+ * the node-graph pattern, then the boundary rows of ApplyTransportBoundaryKernel
+ * (IgaCudaKernels.cuh:411-424): a constrained node's row blocks are zeroed in
+ * both matrices and its diagonal block of `left` becomes the identity.
+ * velocity[node*3+d]; constrained[node] != 0 marks a Dirichlet node (may be NULL).
+ */
+int tfo_transport_assemble(int nodes, int elements, const int* element_offsets, const int* connectivity,
+	const int* extraction_offsets, const uint8_t* extraction_columns, const double* extraction_values,
+	const double* bezier_points, const int* row_offsets, const int* columns, const int* diagonal,
+	const double* velocity, const double* p, const int* constrained, double* left, double* previous,
+	int* failed_element)
+{
+	int failure = -1, status_out = TFO_OK;
+#pragma omp parallel
+	{
+		double* C = (double*)malloc(sizeof(double)*80*64);
+		double* el = (double*)malloc(sizeof(double)*160*160);
+		double* ep = (double*)malloc(sizeof(double)*160*160);
+		double vel[240];
+		long long blocks[80];
+#pragma omp for schedule(dynamic, 4)
+		for (int e = 0; e < elements; ++e) {
+			const int begin = element_offsets[e];
+			const int nen = element_offsets[e+1]-begin;
+			memset(C, 0, sizeof(double)*(size_t)nen*64);
+			for (int a = 0; a < nen; ++a) {
+				for (int k = extraction_offsets[begin+a]; k < extraction_offsets[begin+a+1]; ++k)
+					C[a*64+extraction_columns[k]] = extraction_values[k];
+				for (int d = 0; d < 3; ++d) vel[a*3+d] = velocity[3*(size_t)connectivity[begin+a]+d];
+			}
+			const int status = tfo_transport_element(C, bezier_points+(size_t)e*192, nen, vel, p, el, ep);
+			if (status != TFO_OK) {
+#pragma omp critical
+				{ failure = e; status_out = status; }
+				continue;
+			}
+			const int ndof = 2*nen;
+			for (int a = 0; a < nen; ++a) {
+				const int row = connectivity[begin+a];
+				for (int b = 0; b < nen; ++b)
+					blocks[b] = find_block(row_offsets, columns, row, connectivity[begin+b]);
+				for (int b = 0; b < nen; ++b)
+					for (int i = 0; i < 2; ++i)
+						for (int j = 0; j < 2; ++j) {
+							const size_t at = (size_t)(2*a+i)*ndof+2*b+j;
+#pragma omp atomic
+							left[blocks[b]*4+2*i+j] += el[at];
+#pragma omp atomic
+							previous[blocks[b]*4+2*i+j] += ep[at];
+						}
+			}
+		}
+		free(C); free(el); free(ep);
+	}
+	if (failed_element) *failed_element = failure;
+	if (status_out != TFO_OK || !constrained) return status_out;
+	for (int node = 0; node < nodes; ++node) {
+		if (!constrained[node]) continue;
+		for (int b = row_offsets[node]; b < row_offsets[node+1]; ++b)
+			for (int k = 0; k < 4; ++k) { left[(size_t)b*4+k] = 0.0; previous[(size_t)b*4+k] = 0.0; }
+		left[(size_t)diagonal[node]*4] = 1.0;
+		left[(size_t)diagonal[node]*4+3] = 1.0;
+	}
+	return TFO_OK;
 }

@@ -64,6 +64,12 @@ def lib():
         L.tfo_gmres_bjacobi.argtypes = [C.c_int, _ip, _ip, _ip, _dp, _dp, _dp, C.c_int, C.c_int, C.c_double,
                                         C.POINTER(C.c_double), C.POINTER(C.c_int)]
         L.tfo_max_threads.restype = C.c_int
+        L.tfo_transport_element.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
+        L.tfo_transport_spmv.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp]
+        L.tfo_transport_gmres.argtypes = [C.c_int, _ip, _ip, _ip, _dp, _dp, _dp, C.c_int, C.c_int, C.c_double,
+                                          C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.tfo_transport_assemble.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip, _up, _dp, _dp, _ip, _ip, _ip,
+                                             _dp, _dp, C.c_void_p, _dp, _dp, C.POINTER(C.c_int)]
     return _lib
 
 
@@ -94,6 +100,7 @@ def ref():
         R.ref_assemble.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip, _up, _dp, _dp, _ip, _ip, _dp, _dp,
                                    C.c_double, C.c_double, C.c_double, C.c_void_p, _dp]
         R.ref_max_threads.restype = C.c_int
+        R.ref_transport_element.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
     return _ref
 
 
@@ -299,6 +306,101 @@ def newton_step(mesh, pattern, state, previous, density, viscosity, dt, vmask, p
     A = pattern.to_scipy(values)
     update = spla.spsolve(A.tocsc(), rhs)
     return np.asarray(state, np.float64).ravel() + update, norm, raw
+
+
+# --------------------------------------------------------------------------
+# Two-species transport (iga_cuda transport, iga_cuda.cu:621-732)
+# --------------------------------------------------------------------------
+
+# Element parameter vector of tfo_transport_element / ref_transport_element.
+TRANSPORT_KEYS = ("diffusion", "vplus", "kplus", "kminus", "detach_plus", "dt", "artificial_diffusion")
+
+
+def transport_vector(params):
+    """params: a mapping with TRANSPORT_KEYS (missing ones are 0)."""
+    return np.array([float(params.get(k, 0.0)) for k in TRANSPORT_KEYS], np.float64)
+
+
+def transport_element(Cx, X, velocity, params, use_ref=False):
+    """(left, previous), each (2 nen)^2 with dof 2a = N0, 2a + 1 = N+."""
+    nen = Cx.shape[0]
+    left = np.zeros((2 * nen) ** 2)
+    previous = np.zeros((2 * nen) ** 2)
+    f = ref().ref_transport_element if use_ref else lib().tfo_transport_element
+    st = f(np.ascontiguousarray(Cx, np.float64).ravel(), np.ascontiguousarray(X, np.float64).ravel(), nen,
+           np.ascontiguousarray(velocity, np.float64).ravel(), transport_vector(params), left, previous)
+    if st:
+        raise RuntimeError(f"transport element failed ({st})")
+    return left.reshape(2 * nen, 2 * nen), previous.reshape(2 * nen, 2 * nen)
+
+
+def transport_assemble(mesh, pattern, velocity, params, constrained=None):
+    """Global 2x2 block-CSR (left, previous) with the boundary rows applied."""
+    left = np.zeros(pattern.blocks * 4)
+    previous = np.zeros(pattern.blocks * 4)
+    failed = C.c_int(-1)
+    mask = None if constrained is None else np.ascontiguousarray(constrained, np.int32)
+    st = lib().tfo_transport_assemble(mesh.nodes, mesh.elements, mesh.element_offsets, mesh.connectivity,
+                                      mesh.extraction_offsets, mesh.extraction_columns, mesh.extraction_values,
+                                      mesh.bezier_points, pattern.row_offsets, pattern.columns, pattern.diagonal,
+                                      np.ascontiguousarray(velocity, np.float64).ravel(), transport_vector(params),
+                                      _ptr(mask), left, previous, C.byref(failed))
+    if st:
+        raise RuntimeError(f"oracle transport assembly failed at element {failed.value} ({st})")
+    return left, previous
+
+
+def transport_scipy(pattern, values):
+    import scipy.sparse as sp
+    v = np.asarray(values).reshape(-1, 2, 2)
+    return sp.bsr_matrix((v, pattern.columns, pattern.row_offsets),
+                         shape=(2 * pattern.nodes, 2 * pattern.nodes)).tocsr()
+
+
+def transport_initial(nodes, constrained, n0, nplus):
+    """Zero state with the boundary values set (SetTransportBoundaryVectorKernel, IgaCudaKernels.cuh:426-434)."""
+    c = np.zeros(2 * nodes)
+    m = np.asarray(constrained) != 0
+    c[0::2][m] = np.asarray(n0)[m]
+    c[1::2][m] = np.asarray(nplus)[m]
+    return c
+
+
+def transport_steps(pattern, left, previous, current, constrained, n0, nplus, steps):
+    """`steps` backward-Euler steps solved directly: rhs = P c, boundary values set in rhs, L c' = rhs
+    (the loop of iga_cuda.cu:683-707 with an exact linear solve)."""
+    import scipy.sparse.linalg as spla
+    L = transport_scipy(pattern, left).tocsc()
+    P = transport_scipy(pattern, previous)
+    lu = spla.splu(L)
+    m = np.asarray(constrained) != 0
+    c = np.array(current, np.float64)
+    for _ in range(steps):
+        rhs = P @ c
+        rhs[0::2][m] = np.asarray(n0)[m]
+        rhs[1::2][m] = np.asarray(nplus)[m]
+        c = lu.solve(rhs)
+    return c
+
+
+def transport_spmv(row_offsets, columns, values, x):
+    nodes = len(row_offsets) - 1
+    y = np.zeros(2 * nodes)
+    lib().tfo_transport_spmv(nodes, np.ascontiguousarray(row_offsets, np.int32),
+                             np.ascontiguousarray(columns, np.int32), values, np.ascontiguousarray(x, np.float64), y)
+    return y
+
+
+def transport_gmres(row_offsets, columns, diagonal, values, rhs, x0, restart=50, maxit=10000, rtol=1e-8):
+    """Block-Jacobi GMRES(restart) on the 2x2 system (the CPU restatement); returns (x, iterations, residual)."""
+    nodes = len(row_offsets) - 1
+    x = np.array(x0, np.float64)
+    res = C.c_double(); singular = C.c_int()
+    it = lib().tfo_transport_gmres(nodes, np.ascontiguousarray(row_offsets, np.int32),
+                                   np.ascontiguousarray(columns, np.int32), np.ascontiguousarray(diagonal, np.int32),
+                                   values, np.ascontiguousarray(rhs, np.float64), x, restart, maxit, rtol,
+                                   C.byref(res), C.byref(singular))
+    return x, it, res.value
 
 
 def max_threads() -> int:

@@ -12,6 +12,7 @@
 //   iga::EvaluateOutletModel           include/OutletModel.hpp:70-90
 //   iga::Database::Load                solvers/cpu/include/IgaDatabase.hpp:124-161
 //   iga::WallTraceBasis                solvers/cpu/include/BoundarySupport.hpp:134-150
+//   iga::BuildTransportElement         solvers/cpu/include/TransportElement.hpp:213-260
 #include "BoundaryFlow.hpp"
 #include "BoundarySupport.hpp"
 #include "NavierStokesElement.hpp"
@@ -296,5 +297,33 @@ int ref_assemble(int first, int last, const int* element_offsets, const int* con
 }
 
 int ref_max_threads() { return omp_get_max_threads(); }
+
+// Two-species transport element (left and previous matrices, dense (2 nen)^2).
+// p: D, vplus, kplus, kminus, k'plus, dt, artificial_diffusion.
+int ref_transport_element(const double* C, const double* X, int nen, const double* velocity,
+	const double* p, double* left, double* previous)
+{
+	try {
+		const auto element = MakeElement(C, X, nen);
+		std::vector<std::array<double, 3>> nodal(static_cast<std::size_t>(nen));
+		for (int a = 0; a < nen; ++a)
+			for (int d = 0; d < 3; ++d) nodal[static_cast<std::size_t>(a)][static_cast<std::size_t>(d)] = velocity[a*3+d];
+		iga::TransportParameters parameters;
+		parameters.diffusion = p[0];
+		parameters.vplus = p[1];
+		parameters.kplus = p[2];
+		parameters.kminus = p[3];
+		parameters.detach_plus = p[4];
+		parameters.dt = p[5];
+		parameters.artificial_diffusion = p[6];
+		const auto matrices = iga::BuildTransportElement(element, nodal, parameters);
+		std::memcpy(left, matrices.left.data(), sizeof(double)*matrices.left.size());
+		std::memcpy(previous, matrices.previous.data(), sizeof(double)*matrices.previous.size());
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
 
 } // extern "C"

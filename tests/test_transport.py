@@ -1,0 +1,203 @@
+"""Two-species transport on the CPU: the oracle's transport element against the
+reference's own element (golden vectors and, where the reference build exists,
+element by element), closed-form identities of the element, and the host-side
+case inputs of the `transport` command through the C ABI (no GPU needed).
+
+Reference: BuildTransportElement (solvers/cpu/include/TransportElement.hpp:213-253),
+ReadTransportParameters and ResolveBoundaryConditions
+(solvers/cpu/include/CaseInput.hpp:85-118, 162-258), ParseCaseConfiguration
+(include/CaseConfig.hpp:280-387).
+"""
+import ctypes
+import json
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests.conftest import GOLDEN, ROOT, requires_ref
+from oracle import oracle as O
+from tests.golden.make_element_golden import curved, unit_element
+from tests.golden.make_transport_golden import PARAMS, cases
+
+
+def rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_transport_golden_element_vectors():
+    g = np.load(GOLDEN / "transport_golden.npz")
+    for key, C, X, vel, p in cases():
+        left, previous = O.transport_element(C, X, vel, p)
+        assert rel(left, g[f"{key}_left"]) < 1e-13, key
+        assert rel(previous, g[f"{key}_previous"]) < 1e-13, key
+
+
+@requires_ref
+def test_transport_restatement_matches_reference_build(reference_tube):
+    """Element by element against the reference's compiled element (ragged nen, random velocity)."""
+    from tubularflowiga_b200 import ntiga
+    mesh = ntiga.read(reference_tube / "tube-1.ntiga")
+    rng = np.random.default_rng(3)
+    nens = set()
+    for e in rng.choice(mesh.elements, 16, replace=False):
+        conn, C, X, _ = mesh.element(int(e))
+        nens.add(len(conn))
+        vel = rng.normal(size=(len(conn), 3))
+        for p in PARAMS.values():
+            a = O.transport_element(C, X, vel, p)
+            b = O.transport_element(C, X, vel, p, use_ref=True)
+            assert rel(a[0], b[0]) < 1e-12 and rel(a[1], b[1]) < 1e-12
+    assert len(nens) >= 3, nens
+
+
+def test_transport_element_identities():
+    """Partition of unity and the zero-velocity form of the blocks."""
+    C, X = unit_element()
+    X = curved(X)
+    p = dict(PARAMS["reaction"])
+    left, previous = O.transport_element(C, X, np.zeros((64, 3)), p)
+    M = previous[0::2, 0::2]
+    # sum_b M_ab = int N_a, sum_ab M_ab = volume (= sum of w over the rule)
+    volume = M.sum()
+    qp, qw = O.gauss_rule()
+    dets = [O.basis(C, X, *qp[q], hessian=False)[4] for q in range(64)]
+    assert abs(volume - float(np.dot(qw, dets))) < 1e-15
+    assert np.allclose(previous[1::2, 1::2], M, rtol=0, atol=1e-18)     # T = N without velocity
+    assert np.all(previous[0::2, 1::2] == 0) and np.all(previous[1::2, 0::2] == 0)
+    dt, kp, km, det = p["dt"], p["kplus"], p["kminus"], p["detach_plus"]
+    assert np.allclose(left[0::2, 1::2], -det * dt * M, rtol=1e-13, atol=1e-20)
+    assert np.allclose(left[1::2, 0::2], -kp * dt * M, rtol=1e-13, atol=1e-20)
+    K = (left[0::2, 0::2] - (1 + dt * (kp + km)) * M) / (dt * p["diffusion"])
+    assert np.allclose(K.sum(axis=1), 0.0, atol=1e-12 * np.abs(K).max())   # stiffness annihilates constants
+    assert np.allclose(K, K.T, atol=1e-12 * np.abs(K).max())
+
+
+# ---- host-side case inputs through the C ABI ------------------------------------------------
+
+@pytest.fixture(scope="module")
+def api():
+    from tubularflowiga_b200 import api, build
+    build.build()
+    return api
+
+
+def test_read_transport_params(api, tmp_path):
+    from tubularflowiga_b200 import meshgen
+    want = {"diffusion": 1e-5, "vplus": 0.8, "vminus": 0.3, "kplus": 0.5, "kminus": 0.1, "detach_plus": 0.2,
+            "detach_minus": 0.05, "dt": 1e-3, "steps": 7, "n0_bc": 1.0, "nplus_bc": 0.25, "nminus_bc": 0.5,
+            "artificial_diffusion": 1e-4}
+    path = tmp_path / "simulation_parameter.txt"
+    path.write_text(meshgen.transport_parameter_text(want))
+    got = api.read_transport_params(path).as_dict()
+    for k, v in want.items():
+        assert got[k] == v, k
+    assert (got["restart"], got["gmres_rtol"], got["gmres_max_iterations"]) == (50, 1e-8, 10000)
+    # artificial_diffusion is optional and may be spelled artificial_diffusion_weight
+    path.write_text(path.read_text().replace("artificial_diffusion", "artificial_diffusion_weight"))
+    assert api.read_transport_params(path).artificial_diffusion == 1e-4
+    path.write_text("\n".join(l for l in path.read_text().splitlines() if not l.startswith("artificial")))
+    assert api.read_transport_params(path).artificial_diffusion == 0.0
+    path.write_text(path.read_text().replace("D 1", "X 1"))
+    with pytest.raises(api.TfigaError) as err:
+        api.read_transport_params(path)
+    assert err.value.status == -4 and "missing transport parameter: D" in str(err.value)
+    path.write_text(meshgen.transport_parameter_text(dict(want, dt=0.0)))
+    with pytest.raises(api.TfigaError, match="dt and nstep must be positive"):
+        api.read_transport_params(path)
+    with pytest.raises(api.TfigaError) as err:
+        api.read_transport_params(tmp_path / "missing.txt")
+    assert err.value.status == -3
+
+
+def test_resolve_transport_boundaries(api, tmp_path, small_tube):
+    """Legacy labels, then case_config.json rules (inlet transport values, inherit_legacy false)."""
+    t = small_tube
+    p = api.transport_params(vplus=0.8, n0_bc=1.5, nplus_bc=0.25)
+    mask, n0, nplus = api.resolve_transport_boundaries(t.labels, t.profile, p)
+    inlet = t.labels == 1
+    assert np.array_equal(mask, inlet.astype(np.int32))
+    assert np.all(n0[inlet] == 1.5) and np.all(nplus[inlet] == 0.25)
+    assert np.all(n0[~inlet] == 0) and np.all(nplus[~inlet] == 0)
+    # an absent case_config.json is the legacy default
+    same = api.resolve_transport_boundaries(t.labels, t.profile, p, tmp_path / "case_config.json")
+    assert all(np.array_equal(a, b) for a, b in zip(same, (mask, n0, nplus)))
+
+    cfg = tmp_path / "case_config.json"
+    cfg.write_text(json.dumps({"schema_version": 1, "boundaries": {"conditions": [
+        {"label": 1, "type": "inlet", "transport": {"N0": 2.0, "Nplus": 0.75}}]}}))
+    mask2, n02, nplus2 = api.resolve_transport_boundaries(t.labels, t.profile, p, cfg)
+    assert np.array_equal(mask2, mask) and np.all(n02[inlet] == 2.0) and np.all(nplus2[inlet] == 0.75)
+    # the outlet label as an inlet adds its nodes to the constrained set
+    cfg.write_text(json.dumps({"boundaries": {"inherit_legacy": True, "conditions": [
+        {"label": 2, "type": "inlet"}]}}))
+    with pytest.raises(api.TfigaError, match="no pressure boundary nodes"):
+        api.resolve_transport_boundaries(t.labels, t.profile, p, cfg)
+    cfg.write_text(json.dumps({"boundaries": {"inherit_legacy": False, "conditions": [
+        {"label": 1, "type": "inlet"}, {"label": 2, "type": "outlet"}]}}))
+    with pytest.raises(api.TfigaError, match="mesh boundary label 0 has no case_config.json rule"):
+        api.resolve_transport_boundaries(t.labels, t.profile, p, cfg)
+    for bad, message in (
+            ({"boundaries": {"conditions": [{"label": 7, "type": "wall"}]}}, "label 7 is not present"),
+            ({"boundaries": {"conditions": [{"label": 1, "type": "inlet", "colour": 1}]}}, "unknown"),
+            ({"boundaries": {"conditions": [{"label": 1, "type": "inlet"}, {"label": 1, "type": "inlet"}]}},
+             "duplicate boundary label 1"),
+            ({"schema_version": 2, "boundaries": {"conditions": []}}, "only schema_version 1"),
+            ({"boundaries": {"conditions": [{"label": 2, "type": "outlet", "transport": {"N0": 1, "Nplus": 1}}]}},
+             "outlet rules only support an optional pressure"),
+            ({"boundaries": {"conditions": [{"label": 1, "type": "inlet", "transport": {"N0": 1}}]}},
+             "requires N0 and Nplus")):
+        cfg.write_text(json.dumps(bad))
+        with pytest.raises(api.TfigaError, match=message) as err:
+            api.resolve_transport_boundaries(t.labels, t.profile, p, cfg)
+        assert err.value.status == -4
+
+
+STRUCTS = {"tfiga_mesh_desc": "MeshDesc", "tfiga_mesh_info": "MeshInfo", "tfiga_ns_params": "NsParams",
+           "tfiga_amg_info": "AmgInfo", "tfiga_newton_report": "NewtonReport", "tfiga_step_report": "StepReport",
+           "tfiga_outlet": "Outlet", "tfiga_transport_params": "TransportParams",
+           "tfiga_transport_report": "TransportReport"}
+
+
+def test_struct_layouts_match_the_header(api, tmp_path):
+    """sizeof and every field offset of the header's structs, compiled with gcc, equal the ctypes mirror."""
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "tfiga.h"', 'int main(void) {']
+    for c_name, py_name in STRUCTS.items():
+        lines.append(f'printf("{c_name} %zu\\n", sizeof({c_name}));')
+        for field, _ in getattr(api, py_name)._fields_:
+            lines.append(f'printf("{c_name}.{field} %zu\\n", offsetof({c_name}, {field}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    for c_name, py_name in STRUCTS.items():
+        cls = getattr(api, py_name)
+        assert int(got[c_name]) == ctypes.sizeof(cls), c_name
+        for field, _ in cls._fields_:
+            assert int(got[f"{c_name}.{field}"]) == getattr(cls, field).offset, (c_name, field)
+
+
+def test_transport_oracle_gmres_matches_direct_solve(small_tube):
+    """The CPU restatement of the transport step's block-Jacobi GMRES(50) (the bench's CPU baseline)
+    reaches the sparse-LU solution of the oracle's assembled system."""
+    t = small_tube
+    params = {"diffusion": 1e-5, "vplus": 0.8, "kplus": 0.5, "kminus": 0.1, "detach_plus": 0.2, "dt": 1e-3,
+              "artificial_diffusion": 1e-4}
+    velocity = t.profile + 0.05
+    pattern = O.Pattern(t.mesh.nodes, t.mesh.element_offsets, t.mesh.connectivity)
+    mask = (t.labels == 1).astype(np.int32)
+    n0, nplus = mask * 1.0, mask * 0.25
+    left, previous = O.transport_assemble(t.mesh, pattern, velocity, params, mask)
+    c0 = O.transport_initial(t.mesh.nodes, mask, n0, nplus)
+    want = O.transport_steps(pattern, left, previous, c0, mask, n0, nplus, 1)
+    rhs = O.transport_spmv(pattern.row_offsets, pattern.columns, previous, c0)
+    rhs[0::2][mask != 0] = n0[mask != 0]
+    rhs[1::2][mask != 0] = nplus[mask != 0]
+    x, iterations, residual = O.transport_gmres(pattern.row_offsets, pattern.columns, pattern.diagonal, left, rhs,
+                                                np.zeros_like(rhs))
+    assert iterations > 0
+    for f in (0, 1):
+        assert np.linalg.norm(x[f::2] - want[f::2]) <= 1e-6 * np.linalg.norm(want[f::2])

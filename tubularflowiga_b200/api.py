@@ -110,6 +110,27 @@ class Outlet(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TransportParams(C.Structure):
+    _fields_ = [("diffusion", C.c_double), ("vplus", C.c_double), ("vminus", C.c_double),
+                ("kplus", C.c_double), ("kminus", C.c_double), ("detach_plus", C.c_double),
+                ("detach_minus", C.c_double), ("dt", C.c_double), ("steps", C.c_int32), ("restart", C.c_int32),
+                ("n0_bc", C.c_double), ("nplus_bc", C.c_double), ("nminus_bc", C.c_double),
+                ("artificial_diffusion", C.c_double), ("gmres_rtol", C.c_double),
+                ("gmres_max_iterations", C.c_int32), ("reserved", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class TransportReport(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("last_iterations", C.c_int32), ("total_iterations", C.c_int64),
+                ("last_residual", C.c_double), ("final_l2", C.c_double), ("singular_blocks", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 # Every exported symbol of include/tfiga.h with its signature.
 SIGNATURES = {
     "tfiga_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
@@ -172,6 +193,23 @@ SIGNATURES = {
                                                      C.c_void_p]),
     "tfiga_learned_save": (C.c_int, [C.c_void_p, C.c_char_p]),
     "tfiga_learned_load": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "tfiga_transport_default_params": (None, [C.POINTER(TransportParams)]),
+    "tfiga_transport_read_params": (C.c_int, [C.c_char_p, C.POINTER(TransportParams)]),
+    "tfiga_transport_resolve_boundaries": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(TransportParams),
+                                                     C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                     C.POINTER(C.c_int64)]),
+    "tfiga_transport_create": (C.c_int, [C.c_void_p, C.POINTER(TransportParams), C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "tfiga_transport_destroy": (C.c_int, [C.c_void_p]),
+    "tfiga_transport_step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(TransportReport)]),
+    "tfiga_transport_set_state": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tfiga_transport_get_state": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tfiga_transport_matrices": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_transport_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_int64)]),
+    "tfiga_transport_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "tfiga_transport_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "tfiga_transport_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
     "tfiga_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
 }
 
@@ -515,6 +553,110 @@ class Learned:
         try:
             self.close()
         except Exception:  # noqa: BLE001 -- interpreter shutdown
+            pass
+
+
+def transport_params(**overrides) -> TransportParams:
+    p = TransportParams()
+    lib().tfiga_transport_default_params(C.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def read_transport_params(path, **overrides) -> TransportParams:
+    """simulation_parameter.txt of a legacy transport case (ReadTransportParameters)."""
+    p = transport_params()
+    check(lib().tfiga_transport_read_params(str(path).encode(), C.byref(p)))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def resolve_transport_boundaries(labels, reference_velocity, params: TransportParams, case_config=None):
+    """(constrained, n0, nplus) of a legacy case: controlmesh.vtk labels, the reference velocity and an
+    optional case_config.json (ResolveBoundaryConditions)."""
+    labels = np.ascontiguousarray(labels, np.int32)
+    vel = np.ascontiguousarray(reference_velocity, np.float64).reshape(-1)
+    n = labels.size
+    mask = np.zeros(n, np.int32)
+    n0 = np.zeros(n)
+    nplus = np.zeros(n)
+    count = C.c_int64()
+    path = None if case_config is None else str(case_config).encode()
+    check(lib().tfiga_transport_resolve_boundaries(n, _p(labels), _p(vel), C.byref(params), path, _p(mask),
+                                                   _p(n0), _p(nplus), C.byref(count)))
+    return mask, n0, nplus
+
+
+class Transport:
+    """Two-species transport solver (tfiga_transport): the `iga_cuda transport` path."""
+
+    def __init__(self, mesh: Mesh, params: TransportParams, velocity, constrained, n0, nplus):
+        self.mesh = mesh
+        self.params = params
+        n = mesh.nodes
+        self._velocity = np.ascontiguousarray(velocity, np.float64).reshape(-1)
+        self._mask = np.ascontiguousarray(constrained, np.int32).reshape(-1)
+        self._n0 = np.ascontiguousarray(n0, np.float64).reshape(-1)
+        self._nplus = np.ascontiguousarray(nplus, np.float64).reshape(-1)
+        if (self._velocity.size != 3 * n or self._mask.size != n or self._n0.size != n
+                or self._nplus.size != n):
+            raise ValueError("transport inputs must have 3*nodes velocities and nodes mask/values")
+        self._h = C.c_void_p()
+        check(lib().tfiga_transport_create(mesh._h, C.byref(params), _p(self._velocity), _p(self._mask),
+                                           _p(self._n0), _p(self._nplus), C.byref(self._h)))
+
+    def step(self, steps: int = 1) -> dict:
+        r = TransportReport()
+        check(lib().tfiga_transport_step(self._h, steps, C.byref(r)))
+        return r.as_dict()
+
+    def set_state(self, state):
+        s = np.ascontiguousarray(state, np.float64).reshape(-1)
+        if s.size != 2 * self.mesh.nodes:
+            raise ValueError("state must have 2*nodes entries")
+        check(lib().tfiga_transport_set_state(self._h, _p(s)))
+
+    def get_state(self, out=None):
+        out = np.zeros(2 * self.mesh.nodes) if out is None else out
+        check(lib().tfiga_transport_get_state(self._h, _p(out)))
+        return out
+
+    def matrices(self):
+        left = np.zeros(4 * self.mesh.blocks)
+        previous = np.zeros(4 * self.mesh.blocks)
+        check(lib().tfiga_transport_matrices(self._h, _p(left), _p(previous)))
+        return left, previous
+
+    def info(self) -> dict:
+        ms = C.c_double(); steps = C.c_int32(); launches = C.c_int64()
+        check(lib().tfiga_transport_info(self._h, C.byref(ms), C.byref(steps), C.byref(launches)))
+        return {"assembly_ms": ms.value, "steps": steps.value, "launches": launches.value}
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib().tfiga_transport_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def set_profiling(self, enable: bool):
+        check(lib().tfiga_transport_set_profiling(self._h, 1 if enable else 0))
+
+    def profile(self, reset=False) -> dict:
+        families = NavierStokes.FAMILIES
+        ms = np.zeros(len(families)); counts = np.zeros(len(families), np.int64)
+        check(lib().tfiga_transport_profile(self._h, _p(ms), _p(counts), 1 if reset else 0))
+        return {f: (float(ms[i]), int(counts[i])) for i, f in enumerate(families)}
+
+    def close(self):
+        if self._h:
+            lib().tfiga_transport_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
             pass
 
 

@@ -1,11 +1,15 @@
 // extern "C" boundary: every entry point converts exceptions into a status
 // code plus a thread-local message (tfiga_last_error).
+#include "case_input.hpp"
 #include "learned.hpp"
 #include "mesh.hpp"
 #include "ns.hpp"
+#include "transport.hpp"
 
 #include "../../include/tfiga.h"
 
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <fstream>
@@ -13,6 +17,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <vector>
 
 struct tfiga_mesh {
 	std::unique_ptr<tfiga::Mesh> mesh;
@@ -24,6 +29,12 @@ struct tfiga_ns {
 	tfiga_mesh* mesh = nullptr;
 	std::unique_ptr<tfiga::NsSolver> solver;
 	tfiga_learned* learned = nullptr;       // attached learned stage (not owned)
+};
+
+struct tfiga_transport {
+	tfiga_mesh* mesh = nullptr;
+	std::unique_ptr<tfiga::TransportSolver> solver;
+	tfiga_transport_params params;
 };
 
 struct tfiga_learned {
@@ -424,6 +435,168 @@ int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int3
 		Require(ns != nullptr, "null handle");
 		long long counts[tfiga::Profiler::kFamilies];
 		ns->solver->profiler().Totals(milliseconds, counts, reset != 0);
+		if (launches) for (int f = 0; f < tfiga::Profiler::kFamilies; ++f) launches[f] = counts[f];
+	});
+}
+
+void tfiga_transport_default_params(tfiga_transport_params* params)
+{
+	if (!params) return;
+	std::memset(params, 0, sizeof(*params));
+	params->restart = 50;
+	params->gmres_rtol = 1e-8;
+	params->gmres_max_iterations = 10000;
+}
+
+int tfiga_transport_read_params(const char* path, tfiga_transport_params* params)
+{
+	return Guard([&] {
+		Require(path && params, "null argument");
+		const tfiga::TransportParameters p = tfiga::ReadTransportParameters(path);
+		params->diffusion = p.diffusion;
+		params->vplus = p.vplus;
+		params->vminus = p.vminus;
+		params->kplus = p.kplus;
+		params->kminus = p.kminus;
+		params->detach_plus = p.detach_plus;
+		params->detach_minus = p.detach_minus;
+		params->dt = p.dt;
+		params->steps = p.steps;
+		params->n0_bc = p.n0_bc;
+		params->nplus_bc = p.nplus_bc;
+		params->nminus_bc = p.nminus_bc;
+		params->artificial_diffusion = p.artificial_diffusion;
+	});
+}
+
+int tfiga_transport_resolve_boundaries(int64_t nodes, const int32_t* labels, const double* reference_velocity,
+	const tfiga_transport_params* params, const char* case_config_path, int32_t* constrained, double* n0,
+	double* nplus, int64_t* transport_nodes)
+{
+	return Guard([&] {
+		Require(nodes > 0 && labels && reference_velocity && params, "null argument");
+		tfiga::TransportParameters p;
+		p.vplus = params->vplus;
+		p.n0_bc = params->n0_bc;
+		p.nplus_bc = params->nplus_bc;
+		std::vector<int> label(labels, labels+nodes);
+		std::vector<std::array<double, 3>> velocity((size_t)nodes);
+		for (int64_t i = 0; i < nodes; ++i)
+			for (int d = 0; d < 3; ++d) velocity[(size_t)i][d] = reference_velocity[3*i+d];
+		const tfiga::CaseConfiguration configuration = case_config_path
+			? tfiga::ReadCaseConfiguration(case_config_path) : tfiga::CaseConfiguration{};
+		const auto r = tfiga::ResolveLegacyBoundaries(configuration, label, velocity, p);
+		if (constrained) std::copy(r.transport_mask.begin(), r.transport_mask.end(), constrained);
+		if (n0) std::copy(r.n0.begin(), r.n0.end(), n0);
+		if (nplus) std::copy(r.nplus.begin(), r.nplus.end(), nplus);
+		if (transport_nodes) *transport_nodes = (int64_t)r.transport_nodes;
+	});
+}
+
+int tfiga_transport_create(tfiga_mesh* mesh, const tfiga_transport_params* params, const double* velocity,
+	const int32_t* constrained, const double* n0, const double* nplus, tfiga_transport** out)
+{
+	return Guard([&] {
+		Require(mesh && params && out, "null argument");
+		*out = nullptr;
+		Require(params->restart > 0, "restart must be positive");
+		Require(params->gmres_rtol > 0.0 && params->gmres_max_iterations > 0, "GMRES tolerance and limit must be positive");
+		tfiga::RequireDevice();
+		const tfiga::TransportCoefficients c{params->diffusion, params->vplus, params->kplus, params->kminus,
+			params->detach_plus, params->dt, params->artificial_diffusion};
+		auto handle = std::make_unique<tfiga_transport>();
+		handle->mesh = mesh;
+		handle->params = *params;
+		handle->solver = std::make_unique<tfiga::TransportSolver>(*mesh->mesh, c, velocity, constrained, n0, nplus,
+			params->restart);
+		*out = handle.release();
+	});
+}
+
+int tfiga_transport_destroy(tfiga_transport* transport)
+{
+	return Guard([&] { delete transport; });
+}
+
+int tfiga_transport_step(tfiga_transport* transport, int32_t steps, tfiga_transport_report* report)
+{
+	return Guard([&] {
+		Require(transport != nullptr, "null handle");
+		Require(steps >= 0, "steps must be non-negative");
+		tfiga_transport_report r;
+		std::memset(&r, 0, sizeof(r));
+		for (int32_t k = 0; k < steps; ++k) {
+			const auto step = transport->solver->Step(transport->params.gmres_rtol,
+				transport->params.gmres_max_iterations);
+			r.steps += 1;
+			r.last_iterations = step.iterations;
+			r.total_iterations += step.iterations;
+			r.last_residual = step.residual;
+			r.singular_blocks = std::max(r.singular_blocks, step.singular_blocks);
+		}
+		if (report) {
+			r.final_l2 = transport->solver->StateNorm();
+			*report = r;
+		}
+	});
+}
+
+int tfiga_transport_set_state(tfiga_transport* transport, const double* state)
+{
+	return Guard([&] {
+		Require(transport && state, "null argument");
+		transport->solver->SetState(state);
+	});
+}
+
+int tfiga_transport_get_state(tfiga_transport* transport, double* state)
+{
+	return Guard([&] {
+		Require(transport && state, "null argument");
+		transport->solver->GetState(state);
+	});
+}
+
+int tfiga_transport_matrices(tfiga_transport* transport, double* left, double* previous)
+{
+	return Guard([&] {
+		Require(transport != nullptr, "null handle");
+		transport->solver->Matrices(left, previous);
+	});
+}
+
+int tfiga_transport_info(const tfiga_transport* transport, double* assembly_ms, int32_t* steps, int64_t* launches)
+{
+	return Guard([&] {
+		Require(transport != nullptr, "null handle");
+		if (assembly_ms) *assembly_ms = transport->solver->assembly_ms();
+		if (steps) *steps = transport->solver->steps();
+		if (launches) *launches = transport->solver->launches();
+	});
+}
+
+int tfiga_transport_stream(tfiga_transport* transport, void** stream)
+{
+	return Guard([&] {
+		Require(transport && stream, "null argument");
+		*stream = (void*)transport->solver->stream();
+	});
+}
+
+int tfiga_transport_set_profiling(tfiga_transport* transport, int enable)
+{
+	return Guard([&] {
+		Require(transport != nullptr, "null handle");
+		transport->solver->profiler().Enable(enable != 0);
+	});
+}
+
+int tfiga_transport_profile(tfiga_transport* transport, double* milliseconds, int64_t* launches, int32_t reset)
+{
+	return Guard([&] {
+		Require(transport != nullptr, "null handle");
+		long long counts[tfiga::Profiler::kFamilies];
+		transport->solver->profiler().Totals(milliseconds, counts, reset != 0);
 		if (launches) for (int f = 0; f < tfiga::Profiler::kFamilies; ++f) launches[f] = counts[f];
 	});
 }

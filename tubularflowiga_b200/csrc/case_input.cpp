@@ -386,4 +386,256 @@ SimulationConfig MaterializeOutletPressures(const SimulationConfig& config, cons
 	return out;
 }
 
+// ---- legacy two-species transport case ------------------------------------
+
+TransportParameters ReadTransportParameters(const std::string& path)
+{
+	std::ifstream in(path);
+	if (!in) Fail(-3, "cannot open simulation parameters: "+path);
+	std::map<std::string, double> values;
+	std::string key;
+	double value = 0.0;
+	while (in >> key >> value) values[key] = value;
+	auto required = [&](const char* name) {
+		const auto it = values.find(name);
+		if (it == values.end()) Fail(-4, std::string("missing transport parameter: ")+name);
+		return it->second;
+	};
+	TransportParameters p;
+	p.diffusion = required("D");
+	p.vplus = required("vplus");
+	p.vminus = required("vminus");
+	p.kplus = required("kplus");
+	p.kminus = required("kminus");
+	p.detach_plus = required("k'plus");
+	p.detach_minus = required("k'minus");
+	p.dt = required("dt");
+	p.steps = (int)required("nstep");
+	p.n0_bc = required("N0bc");
+	p.nplus_bc = required("Nplusbc");
+	p.nminus_bc = required("Nminusbc");
+	auto artificial = values.find("artificial_diffusion");
+	if (artificial == values.end()) artificial = values.find("artificial_diffusion_weight");
+	if (artificial != values.end()) p.artificial_diffusion = artificial->second;
+	if (p.dt <= 0.0 || p.steps < 0) Fail(-4, "dt and nstep must be positive");
+	return p;
+}
+
+namespace {
+
+[[noreturn]] void CaseFail(const std::string& message) { Fail(-4, "case_config.json: "+message); }
+
+void KnownKeys(const json::Value& object, std::initializer_list<const char*> allowed, const std::string& context)
+{
+	for (const auto& m : object.members) {
+		bool ok = false;
+		for (const char* a : allowed) ok = ok || m.first == a;
+		if (!ok) CaseFail("unknown "+context+" key '"+m.first+"'");
+	}
+}
+
+const json::Value& CaseObject(const json::Value& v, const std::string& context)
+{
+	if (!v.IsObject()) CaseFail(context+" must be an object");
+	return v;
+}
+
+double CaseNumber(const json::Value& v, const std::string& context)
+{
+	if (v.kind != json::Value::Kind::Number || !std::isfinite(v.number)) CaseFail(context+" must be a finite number");
+	return v.number;
+}
+
+int CaseInteger(const json::Value& v, const std::string& context)
+{
+	const double n = CaseNumber(v, context);
+	if (std::floor(n) != n || n < 0.0 || n > 2147483647.0) CaseFail(context+" must be a non-negative integer");
+	return (int)n;
+}
+
+const std::string& CaseString(const json::Value& v, const std::string& context)
+{
+	if (v.kind != json::Value::Kind::String) CaseFail(context+" must be a string");
+	return v.text;
+}
+
+CaseBoundaryRule ParseRule(const json::Value& value, size_t index)
+{
+	const std::string context = "boundaries.conditions["+std::to_string(index)+"]";
+	const auto& object = CaseObject(value, context);
+	KnownKeys(object, {"label", "name", "type", "velocity", "velocity_scale", "pressure", "transport"}, context);
+	const auto* label = object.Find("label");
+	const auto* type = object.Find("type");
+	if (!label || !type) CaseFail(context+" requires label and type");
+	CaseBoundaryRule rule;
+	rule.label = CaseInteger(*label, context+".label");
+	rule.type = CaseString(*type, context+".type");
+	if (rule.type != "interior" && rule.type != "wall" && rule.type != "inlet" && rule.type != "outlet")
+		CaseFail("unsupported boundary type '"+rule.type+"'");
+	if (const auto* name = object.Find("name")) rule.name = CaseString(*name, context+".name");
+	if (const auto* scale = object.Find("velocity_scale")) {
+		rule.has_velocity_scale = true;
+		rule.velocity_scale = CaseNumber(*scale, context+".velocity_scale");
+	}
+	if (const auto* velocity = object.Find("velocity")) {
+		if (velocity->kind != json::Value::Kind::Array) CaseFail(context+".velocity must be an array");
+		if (velocity->items.size() != 3) CaseFail(context+".velocity must have three entries");
+		rule.has_velocity = true;
+		for (int i = 0; i < 3; ++i)
+			rule.velocity[i] = CaseNumber(velocity->items[i], context+".velocity["+std::to_string(i)+"]");
+	}
+	if (const auto* pressure = object.Find("pressure")) {
+		rule.has_pressure = true;
+		rule.pressure = CaseNumber(*pressure, context+".pressure");
+	}
+	if (const auto* transport = object.Find("transport")) {
+		CaseObject(*transport, context+".transport");
+		KnownKeys(*transport, {"N0", "Nplus"}, context+".transport");
+		const auto* n0 = transport->Find("N0");
+		const auto* nplus = transport->Find("Nplus");
+		if (!n0 || !nplus) CaseFail(context+".transport requires N0 and Nplus");
+		rule.has_transport = true;
+		rule.n0 = CaseNumber(*n0, context+".transport.N0");
+		rule.nplus = CaseNumber(*nplus, context+".transport.Nplus");
+	}
+	if (rule.has_velocity && rule.has_velocity_scale) CaseFail(context+" cannot set both velocity and velocity_scale");
+	if (rule.type == "interior") {
+		if (rule.has_velocity || rule.has_velocity_scale || rule.has_pressure || rule.has_transport)
+			CaseFail("interior boundary rules cannot set values");
+	} else if (rule.type == "wall") {
+		if (rule.has_velocity_scale || rule.has_pressure || rule.has_transport)
+			CaseFail("wall rules only support an optional velocity");
+	} else if (rule.type == "inlet") {
+		if (rule.has_pressure) CaseFail("inlet rules cannot set pressure");
+	} else if (rule.has_velocity || rule.has_velocity_scale || rule.has_transport) {
+		CaseFail("outlet rules only support an optional pressure");
+	}
+	return rule;
+}
+
+} // namespace
+
+CaseConfiguration ParseCaseConfiguration(const std::string& text)
+{
+	json::Value root;
+	try {
+		root = json::Parse(text);
+	} catch (const Error&) {
+		throw;
+	} catch (const std::exception& error) {
+		CaseFail(error.what());
+	}
+	CaseObject(root, "root");
+	KnownKeys(root, {"schema_version", "boundaries"}, "root");
+	if (const auto* version = root.Find("schema_version"))
+		if (CaseInteger(*version, "schema_version") != 1) CaseFail("only schema_version 1 is supported");
+	const auto* boundaries = root.Find("boundaries");
+	if (!boundaries) CaseFail("missing boundaries object");
+	CaseObject(*boundaries, "boundaries");
+	KnownKeys(*boundaries, {"inherit_legacy", "conditions"}, "boundaries");
+	CaseConfiguration configuration;
+	configuration.present = true;
+	if (const auto* inherit = boundaries->Find("inherit_legacy")) {
+		if (inherit->kind != json::Value::Kind::Bool) CaseFail("boundaries.inherit_legacy must be a boolean");
+		configuration.inherit_legacy = inherit->boolean;
+	}
+	const auto* conditions = boundaries->Find("conditions");
+	if (!conditions) CaseFail("boundaries.conditions is required");
+	if (conditions->kind != json::Value::Kind::Array) CaseFail("boundaries.conditions must be an array");
+	std::set<int> labels;
+	for (size_t i = 0; i < conditions->items.size(); ++i) {
+		CaseBoundaryRule rule = ParseRule(conditions->items[i], i);
+		if (!labels.insert(rule.label).second) CaseFail("duplicate boundary label "+std::to_string(rule.label));
+		configuration.boundaries.push_back(std::move(rule));
+	}
+	return configuration;
+}
+
+CaseConfiguration ReadCaseConfiguration(const std::string& path)
+{
+	std::ifstream in(path);
+	if (!in) return {};
+	std::stringstream ss;
+	ss << in.rdbuf();
+	return ParseCaseConfiguration(ss.str());
+}
+
+LegacyBoundaries ResolveLegacyBoundaries(const CaseConfiguration& configuration, const std::vector<int>& labels,
+	const std::vector<std::array<double, 3>>& reference_velocity, const TransportParameters& parameters)
+{
+	if (labels.size() != reference_velocity.size())
+		Fail(-4, "boundary labels and velocity field have different node counts");
+	const size_t nodes = labels.size();
+	LegacyBoundaries r;
+	r.velocity_mask.assign(nodes, 0);
+	r.pressure_mask.assign(nodes, 0);
+	r.transport_mask.assign(nodes, 0);
+	r.velocity.assign(3*nodes, 0.0);
+	r.pressure.assign(nodes, 0.0);
+	r.n0.assign(nodes, 0.0);
+	r.nplus.assign(nodes, 0.0);
+	auto clear = [&](size_t node) {
+		r.velocity_mask[node] = r.pressure_mask[node] = r.transport_mask[node] = 0;
+		for (int d = 0; d < 3; ++d) r.velocity[3*node+d] = 0.0;
+		r.pressure[node] = r.n0[node] = r.nplus[node] = 0.0;
+	};
+	if (!configuration.present || configuration.inherit_legacy)
+		for (size_t node = 0; node < nodes; ++node) {
+			if (labels[node] == 0) {
+				r.velocity_mask[node] = 1;
+			} else if (labels[node] == 1) {
+				r.velocity_mask[node] = 1;
+				for (int d = 0; d < 3; ++d) r.velocity[3*node+d] = parameters.vplus*reference_velocity[node][d];
+				r.transport_mask[node] = 1;
+				r.n0[node] = parameters.n0_bc;
+				r.nplus[node] = parameters.nplus_bc;
+			} else if (labels[node] >= 2) {
+				r.pressure_mask[node] = 1;
+			}
+		}
+	std::set<int> configured;
+	for (const auto& rule : configuration.boundaries) {
+		configured.insert(rule.label);
+		bool found = false;
+		for (size_t node = 0; node < nodes; ++node) {
+			if (labels[node] != rule.label) continue;
+			found = true;
+			clear(node);
+			if (rule.type == "wall") {
+				r.velocity_mask[node] = 1;
+				if (rule.has_velocity) for (int d = 0; d < 3; ++d) r.velocity[3*node+d] = rule.velocity[d];
+			} else if (rule.type == "inlet") {
+				r.velocity_mask[node] = 1;
+				if (rule.has_velocity) {
+					for (int d = 0; d < 3; ++d) r.velocity[3*node+d] = rule.velocity[d];
+				} else {
+					const double scale = rule.has_velocity_scale ? rule.velocity_scale : parameters.vplus;
+					for (int d = 0; d < 3; ++d) r.velocity[3*node+d] = scale*reference_velocity[node][d];
+				}
+				r.transport_mask[node] = 1;
+				r.n0[node] = rule.has_transport ? rule.n0 : parameters.n0_bc;
+				r.nplus[node] = rule.has_transport ? rule.nplus : parameters.nplus_bc;
+			} else if (rule.type == "outlet") {
+				r.pressure_mask[node] = 1;
+				r.pressure[node] = rule.has_pressure ? rule.pressure : 0.0;
+			}
+		}
+		if (!found)
+			Fail(-4, "case_config.json boundary label "+std::to_string(rule.label)+" is not present in controlmesh.vtk");
+	}
+	if (configuration.present && !configuration.inherit_legacy)
+		for (int label : labels)
+			if (label >= 0 && !configured.count(label))
+				Fail(-4, "mesh boundary label "+std::to_string(label)
+					+" has no case_config.json rule while inherit_legacy is false");
+	for (size_t node = 0; node < nodes; ++node) {
+		r.velocity_nodes += r.velocity_mask[node] == 1;
+		r.pressure_nodes += r.pressure_mask[node] == 1;
+		r.transport_nodes += r.transport_mask[node] == 1;
+	}
+	if (r.velocity_nodes == 0) Fail(-4, "case has no velocity boundary nodes");
+	if (r.pressure_nodes == 0) Fail(-4, "case has no pressure boundary nodes");
+	return r;
+}
+
 } // namespace tfiga

@@ -98,4 +98,45 @@ std::array<double, 2> EvaluateOutletModel(const OutletModel& model, double flow,
 // MaterializeOutletPressures (OutletModel.hpp:152-170).
 SimulationConfig MaterializeOutletPressures(const SimulationConfig& config, const std::vector<OutletModel>& models);
 
+// ---- legacy two-species transport case (the `transport` command) ----------
+
+// iga::TransportParameters (solvers/cpu/include/CaseInput.hpp:19-33).
+struct TransportParameters {
+	double diffusion = 0.0, vplus = 0.0, vminus = 0.0, kplus = 0.0, kminus = 0.0;
+	double detach_plus = 0.0, detach_minus = 0.0, dt = 0.0;
+	int steps = 0;
+	double n0_bc = 0.0, nplus_bc = 0.0, nminus_bc = 0.0, artificial_diffusion = 0.0;
+};
+// ReadTransportParameters (CaseInput.hpp:85-118): whitespace-separated `key value` pairs of
+// simulation_parameter.txt; D vplus vminus kplus kminus k'plus k'minus dt nstep N0bc Nplusbc
+// Nminusbc required, artificial_diffusion (or artificial_diffusion_weight) optional.
+TransportParameters ReadTransportParameters(const std::string& path);
+
+// case_config.json schema 1 (include/CaseConfig.hpp:29-48, 280-387).
+struct CaseBoundaryRule {
+	int label = -1;
+	std::string name, type = "interior";   // interior | wall | inlet | outlet
+	bool has_velocity = false, has_velocity_scale = false, has_pressure = false, has_transport = false;
+	std::array<double, 3> velocity{{0.0, 0.0, 0.0}};
+	double velocity_scale = 1.0, pressure = 0.0, n0 = 0.0, nplus = 0.0;
+};
+struct CaseConfiguration {
+	bool present = false;
+	bool inherit_legacy = true;
+	std::vector<CaseBoundaryRule> boundaries;
+};
+// ReadCaseConfiguration (CaseConfig.hpp:373-387): an absent file is an empty configuration.
+CaseConfiguration ReadCaseConfiguration(const std::string& path);
+CaseConfiguration ParseCaseConfiguration(const std::string& text);
+
+// ResolveBoundaryConditions (CaseInput.hpp:162-258): legacy labels (0 wall, 1 inlet, >= 2 outlet)
+// unless the configuration replaces them, then the configured rules label by label.
+struct LegacyBoundaries {
+	std::vector<int32_t> velocity_mask, pressure_mask, transport_mask;
+	std::vector<double> velocity, pressure, n0, nplus;   // velocity 3 per node
+	size_t velocity_nodes = 0, pressure_nodes = 0, transport_nodes = 0;
+};
+LegacyBoundaries ResolveLegacyBoundaries(const CaseConfiguration& configuration, const std::vector<int>& labels,
+	const std::vector<std::array<double, 3>>& reference_velocity, const TransportParameters& parameters);
+
 } // namespace tfiga

@@ -1,10 +1,11 @@
-// The drop-in command (tfiga_main): device-info, mesh-check and navier-stokes
-// with the reference's arguments, log lines, outputs and exit codes
-// (solvers/cuda/src/iga_cuda.cu:278-303, 389-498, 566-617, 734-1195).
+// The drop-in command (tfiga_main): device-info, mesh-check, navier-stokes and
+// transport with the reference's arguments, log lines, outputs and exit codes
+// (solvers/cuda/src/iga_cuda.cu:278-303, 327-400, 389-498, 566-1195).
 #include "case_input.hpp"
 #include "json.hpp"
 #include "mesh.hpp"
 #include "ns.hpp"
+#include "transport.hpp"
 
 #include "../../include/tfiga.h"
 
@@ -621,13 +622,97 @@ int NavierStokes(int argc, char** argv)
 	return 0;
 }
 
+// WriteTransport (iga_cuda.cu:327-335): "node N0 N+" rows.
+void WriteTransportText(const fs::path& path, const std::vector<double>& values)
+{
+	std::ofstream out(path);
+	if (!out) Fail(-3, "cannot create "+path.string());
+	out << std::setprecision(17);
+	for (size_t node = 0; node < values.size()/2; ++node)
+		out << node << ' ' << values[2*node] << ' ' << values[2*node+1] << '\n';
+}
+
+// WriteTransportVtk (iga_cuda.cu:337-349): control mesh + N0 / Nplus point scalars.
+void WriteTransportVtk(const fs::path& mesh_path, const fs::path& path, const std::vector<double>& values)
+{
+	std::ifstream mesh(mesh_path);
+	std::ofstream out(path);
+	if (!mesh) Fail(-3, "cannot open VTK mesh "+mesh_path.string());
+	if (!out) Fail(-3, "cannot create "+path.string());
+	out << mesh.rdbuf() << "\nSCALARS N0 double 1\nLOOKUP_TABLE default\n" << std::setprecision(17);
+	for (size_t node = 0; node < values.size()/2; ++node) out << values[2*node] << '\n';
+	out << "SCALARS Nplus double 1\nLOOKUP_TABLE default\n";
+	for (size_t node = 0; node < values.size()/2; ++node) out << values[2*node+1] << '\n';
+}
+
+// `transport DATABASE CASE_DIR [STEPS] [OUTPUT] [VELOCITY]` (Transport, iga_cuda.cu:621-732).
+int Transport(int argc, char** argv)
+{
+	if (argc < 4) Fail(-1, "usage: iga_cuda transport DATABASE.ntiga CASE_DIR [STEPS] [OUTPUT] [VELOCITY]");
+	const auto total_start = Clock::now();
+	const fs::path case_dir(argv[3]);
+	HostMesh host = ReadNtiga(argv[2]);
+	TransportParameters parameters = ReadTransportParameters((case_dir/"simulation_parameter.txt").string());
+	if (argc >= 5) parameters.steps = std::stoi(argv[4]);
+	const auto labeled = ReadLabeledHexMesh((case_dir/"controlmesh.vtk").string(), host.nodes, host.elements());
+	const fs::path velocity_path = argc >= 7 ? fs::path(argv[6]) : case_dir/"initial_velocityfield.txt";
+	const auto velocity_host = ReadVelocity(velocity_path.string(), host.nodes);
+	const auto configuration = ReadCaseConfiguration((case_dir/"case_config.json").string());
+	const auto boundaries = ResolveLegacyBoundaries(configuration, labeled.labels, velocity_host, parameters);
+	std::cout << "boundary_config=" << (configuration.present ? "case_config.json" : "legacy-defaults")
+		<< " transport_nodes=" << boundaries.transport_nodes << '\n';
+	Mesh mesh(std::move(host));
+	PrintMesh(mesh);
+	const auto preprocess_end = Clock::now();
+	if (mesh.bad_samples())
+		Fail(-5, "geometry has "+std::to_string(mesh.bad_samples())+" non-positive Jacobian samples");
+	std::vector<double> velocity(3*(size_t)mesh.nodes());
+	for (size_t node = 0; node < velocity_host.size(); ++node)
+		for (int d = 0; d < 3; ++d) velocity[3*node+d] = velocity_host[node][d];
+	const TransportCoefficients coefficients{parameters.diffusion, parameters.vplus, parameters.kplus,
+		parameters.kminus, parameters.detach_plus, parameters.dt, parameters.artificial_diffusion};
+	constexpr int kRestart = 50;
+	const auto assembly_start = Clock::now();
+	TransportSolver solver(mesh, coefficients, velocity.data(), boundaries.transport_mask.data(),
+		boundaries.n0.data(), boundaries.nplus.data(), kRestart);
+	const auto assembly_end = Clock::now();
+	long long total_iterations = 0;
+	unsigned singular = 0;
+	const auto solve_start = Clock::now();
+	for (int step = 0; step < parameters.steps; ++step) {
+		const TransportStepResult r = solver.Step(1e-8, 10000);
+		total_iterations += r.iterations;
+		singular = std::max(singular, r.singular_blocks);
+		if ((step+1)%25 == 0 || step+1 == parameters.steps)
+			std::cout << "transport step=" << step+1 << '/' << parameters.steps << " iterations=" << r.iterations
+				<< " residual=" << r.residual << '\n';
+	}
+	CudaCheck(cudaStreamSynchronize(solver.stream()), "transport solve");
+	const auto solve_end = Clock::now();
+	const double norm = solver.StateNorm();
+	if (argc >= 6) {
+		std::vector<double> output(2*(size_t)mesh.nodes());
+		solver.GetState(output.data());
+		WriteTransportText(argv[5], output);
+		WriteTransportVtk(case_dir/"controlmesh.vtk", std::string(argv[5])+".vtk", output);
+	}
+	std::cout << "transport_cuda nodes=" << mesh.nodes() << " elements=" << mesh.host().elements()
+		<< " steps=" << parameters.steps
+		<< " preprocess_s=" << std::chrono::duration<double>(preprocess_end-total_start).count()
+		<< " assembly_s=" << std::chrono::duration<double>(assembly_end-assembly_start).count()
+		<< " solve_s=" << std::chrono::duration<double>(solve_end-solve_start).count()
+		<< " total_iterations=" << total_iterations << " final_l2=" << norm
+		<< " singular_diagonal_blocks=" << singular << " gpu_used_gib=" << DeviceBytesPeak()/1073741824.0 << '\n';
+	return 0;
+}
+
 } // namespace
 } // namespace tfiga
 
 extern "C" int tfiga_main(int argc, char** argv)
 {
 	try {
-		if (argc < 2) throw std::runtime_error("usage: iga_cuda device-info|mesh-check|navier-stokes ...");
+		if (argc < 2) throw std::runtime_error("usage: iga_cuda device-info|mesh-check|navier-stokes|transport ...");
 		tfiga::RequireDevice();
 		const std::string command(argv[1]);
 		tfiga::PrintDevice();
@@ -638,6 +723,8 @@ extern "C" int tfiga_main(int argc, char** argv)
 			status = tfiga::MeshCheck(argv[2]);
 		} else if (command == "navier-stokes") {
 			status = tfiga::NavierStokes(argc, argv);
+		} else if (command == "transport") {
+			status = tfiga::Transport(argc, argv);
 		} else {
 			throw std::runtime_error("unknown command: "+command);
 		}

@@ -309,15 +309,16 @@ double ArnoldiBytes(long long n, int used, int basis_bytes, bool flexible)
 
 } // namespace
 
-Gmres::Gmres(int nodes, int restart, cudaStream_t stream)
-	: nodes_(nodes), n_(4*nodes), restart_(restart), blocks_(kBlocks), stream_(stream)
+Gmres::Gmres(int nodes, int restart, cudaStream_t stream, int fields)
+	: nodes_(nodes), fields_(fields), n_(fields*nodes), restart_(restart), blocks_(kBlocks), stream_(stream)
 {
 	if (nodes <= 0 || restart <= 0) Fail(-1, "GMRES workspace dimensions must be positive");
+	if (fields != 2 && fields != 4) Fail(-7, "GMRES supports 2x2 and 4x4 blocks");
 	// multi-dot chunk per CTA: a multiple of 128 doubles (16-byte aligned row slices, two-step unroll)
 	chunk_ = (int)((((long long)n_+blocks_-1)/blocks_+127)/128*128);
 	V_.Allocate((size_t)(restart+1)*n_);
 	w_.Allocate(n_); r_.Allocate(n_); tmp_.Allocate(n_);
-	inverse_.Allocate((size_t)nodes*16);
+	inverse_.Allocate((size_t)nodes*fields*fields);
 	partial_.Allocate((size_t)(restart+1)*blocks_);
 	hpass_.Allocate(restart+1);
 	H_.Allocate((size_t)(restart+1)*restart);
@@ -371,8 +372,12 @@ void Gmres::Step(const DevicePatternView& pattern, const double* values, int j)
 {
 	const int* stop = state_.get();
 	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
-	LaunchSpmvBlockJacobi(pattern, values, inverse_.get(), V_.get()+(size_t)j*n_, scale_.get()+j, w_.get(), stop,
-		stream_);
+	if (fields_ == 2)
+		LaunchSpmvBlockJacobi2(pattern, values, inverse_.get(), V_.get()+(size_t)j*n_, scale_.get()+j, w_.get(),
+			stop, stream_);
+	else
+		LaunchSpmvBlockJacobi(pattern, values, inverse_.get(), V_.get()+(size_t)j*n_, scale_.get()+j, w_.get(), stop,
+			stream_);
 	if (profiler_) profiler_->End(stream_);
 	launches_ += 1;
 	Orthogonalize<double>(j, V_.get());
@@ -467,6 +472,7 @@ template <class T>
 GmresResult Gmres::SolveFlexible(const DevicePatternView& pattern, const T* values, const double* rhs,
 	double* x, double rtol, int max_iterations, Amg& M, long long* launches, bool fp64_basis)
 {
+	if (fields_ != 4) Fail(-7, "the flexible GMRES with AMG needs 4x4 blocks");
 	if (fp64_basis || std::is_same<T, double>::value)
 		return SolveFlexibleImpl<T, double>(pattern, values, rhs, x, rtol, max_iterations, M, launches);
 	return SolveFlexibleImpl<T, float>(pattern, values, rhs, x, rtol, max_iterations, M, launches);
@@ -538,10 +544,12 @@ GmresResult Gmres::SolveFlexibleImpl(const DevicePatternView& pattern, const T* 
 double Gmres::TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs,
 	const double* x)
 {
-	LaunchSpmv(pattern, values, x, tmp_.get(), stream_);
+	if (fields_ == 2) LaunchSpmv2(pattern, values, x, tmp_.get(), stream_);
+	else LaunchSpmv(pattern, values, x, tmp_.get(), stream_);
 	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), r_.get());
 	LaunchCheck("ResidualKernel");
-	LaunchApplyBlockInverse(nodes_, inverse_.get(), r_.get(), V_.get(), stream_);
+	if (fields_ == 2) LaunchApplyBlockInverse2(nodes_, inverse_.get(), r_.get(), V_.get(), stream_);
+	else LaunchApplyBlockInverse(nodes_, inverse_.get(), r_.get(), V_.get(), stream_);
 	LaunchNorm(n_, V_.get(), norm_partial_.get(), scalar_.get(), stream_);
 	launches_ += 5;
 	scalar_.Download(host_->beta, 1, stream_);
@@ -550,16 +558,20 @@ double Gmres::TrueResidual(const DevicePatternView& pattern, const double* value
 }
 
 GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values, const double* rhs, double* x,
-	double rtol, int max_iterations, long long* launches)
+	double rtol, int max_iterations, long long* launches, bool rebuild_preconditioner)
 {
 	launches_ = 0;
 	GmresResult result;
-	singular_.Zero(stream_);
-	LaunchBlockInverse(pattern, values, inverse_.get(), singular_.get(), stream_);
-	launches_ += 1;
-	singular_.Download(&host_->singular, 1, stream_);
+	if (rebuild_preconditioner) {
+		singular_.Zero(stream_);
+		if (fields_ == 2) LaunchBlockInverse2(pattern, values, inverse_.get(), singular_.get(), stream_);
+		else LaunchBlockInverse(pattern, values, inverse_.get(), singular_.get(), stream_);
+		launches_ += 1;
+		singular_.Download(&host_->singular, 1, stream_);
+	}
 	double beta = TrueResidual(pattern, values, rhs, x);
-	result.singular_blocks = host_->singular;
+	if (rebuild_preconditioner) singular_count_ = host_->singular;
+	result.singular_blocks = singular_count_;
 	result.residual = beta;
 	if (!std::isfinite(beta)) Fail(-6, "GMRES initial residual is not finite");
 	if (beta == 0.0) {

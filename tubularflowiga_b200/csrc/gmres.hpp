@@ -27,23 +27,26 @@ struct GmresResult {
 
 class Gmres {
 public:
-	Gmres(int nodes, int restart, cudaStream_t stream);
+	// fields: unknowns per node, the block size of the matrix (4: Navier-Stokes, 2: transport).
+	Gmres(int nodes, int restart, cudaStream_t stream, int fields = 4);
 	~Gmres();
 	Gmres(const Gmres&) = delete;
 	Gmres& operator=(const Gmres&) = delete;
-	// Solves A x = rhs (x holds the initial guess).  Builds the block inverse first.
+	// Solves A x = rhs (x holds the initial guess).  Builds the block inverse first unless
+	// rebuild_preconditioner is false (the matrix is the one of the previous Solve).
 	GmresResult Solve(const DevicePatternView& pattern, const double* values, const double* rhs, double* x,
-		double rtol, int max_iterations, long long* launches);
+		double rtol, int max_iterations, long long* launches, bool rebuild_preconditioner = true);
 	// Right-preconditioned flexible GMRES (FGMRES): z_j = M^{-1} v_j stored, tolerance
 	// rtol * ||b - A x0|| on the true residual.
 	// The matrix may be stored in FP64 or FP32 (T); with FP32 the Krylov basis is stored in FP32
 	// too unless fp64_basis (dots, updates and the work vector in FP64 arithmetic); preconditioned
 	// vectors, Hessenberg, Givens and the solution stay FP64, and each restart's true residual is the
-	// FP64 refinement.
+	// FP64 refinement.  Needs fields == 4.
 	template <class T>
 	GmresResult SolveFlexible(const DevicePatternView& pattern, const T* values, const double* rhs, double* x,
 		double rtol, int max_iterations, Amg& preconditioner, long long* launches, bool fp64_basis = false);
 	int restart() const { return restart_; }
+	int fields() const { return fields_; }
 	// Learned stage added to the AMG application in SolveFlexible (null: AMG only).
 	void set_learned(LearnedPreconditioner* learned) { learned_ = learned; }
 	LearnedPreconditioner* learned() const { return learned_; }
@@ -66,7 +69,8 @@ private:
 	double TrueResidualPlain(const DevicePatternView& pattern, const T* values, const double* rhs, const double* x);
 	double TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs, const double* x);
 
-	int nodes_, n_, restart_, blocks_;
+	int nodes_, fields_, n_, restart_, blocks_;
+	unsigned singular_count_ = 0;     // singular diagonal blocks of the last block-inverse build
 	int update_blocks_ = 0;           // CTAs of the basis update (one per 32 entry pairs)
 	int chunk_;
 	size_t finalize_smem_ = 0;

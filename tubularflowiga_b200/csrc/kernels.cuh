@@ -86,6 +86,17 @@ void LaunchBlockInverse(const DevicePatternView& pattern, const T* values, doubl
 void LaunchToFloat(long long n, const double* in, float* out, cudaStream_t stream);
 void LaunchApplyBlockInverse(int nodes, const double* inverse, const double* x, double* y, cudaStream_t stream);
 // state = prescribed value on the constrained entries (the Dirichlet values lifted into the state).
+// ---- transport.cu (2x2 block CSR: values[block*4 + 2i + j], vectors value[2*node + field]) ----
+void LaunchSpmv2(const DevicePatternView& pattern, const double* values, const double* x, double* y,
+	cudaStream_t stream);
+// y = D^{-1} (A x) * (*scale) with D^{-1} the 2x2 block-Jacobi inverse (scale may be null; stop: the
+// GMRES early-out flag, may be null).
+void LaunchSpmvBlockJacobi2(const DevicePatternView& pattern, const double* values, const double* inverse,
+	const double* x, const double* scale, double* y, const int* stop, cudaStream_t stream);
+void LaunchBlockInverse2(const DevicePatternView& pattern, const double* values, double* inverse,
+	unsigned int* singular, cudaStream_t stream);
+void LaunchApplyBlockInverse2(int nodes, const double* inverse, const double* x, double* y, cudaStream_t stream);
+
 void LaunchLiftDirichlet(int count, const int32_t* nodes, const int32_t* vmask, const int32_t* pmask,
 	const double* velocity, const double* pressure, double* state, cudaStream_t stream);
 template <class T>

@@ -47,54 +47,58 @@ __global__ void __launch_bounds__(256) SpmvBlockJacobiKernel(DevicePatternView p
 }
 
 // Gauss-Jordan with partial pivoting and the singular fallback of
-// BuildBlockInverseKernel (SparseKernels.cuh:42-89).
-template <class T>
+// BuildBlockInverseKernel (SparseKernels.cuh:42-89), for F x F diagonal blocks.
+template <int F, class T>
 __global__ void BlockInverseKernel(DevicePatternView p, const T* __restrict__ values,
 	double* __restrict__ inverse, unsigned int* __restrict__ singular)
 {
 	const int node = blockIdx.x*blockDim.x+threadIdx.x;
 	if (node >= p.nodes) return;
-	const T* s = values+(size_t)p.diagonal[node]*16;
-	double m[4][8];
-	for (int i = 0; i < 4; ++i)
-		for (int j = 0; j < 8; ++j) m[i][j] = j < 4 ? s[i*4+j] : (j-4 == i ? 1.0 : 0.0);
+	const T* s = values+(size_t)p.diagonal[node]*F*F;
+	double m[F][2*F];
+	for (int i = 0; i < F; ++i)
+		for (int j = 0; j < 2*F; ++j) m[i][j] = j < F ? s[i*F+j] : (j-F == i ? 1.0 : 0.0);
 	bool failed = false;
-	for (int pivot = 0; pivot < 4; ++pivot) {
+	for (int pivot = 0; pivot < F; ++pivot) {
 		int best = pivot;
-		for (int r = pivot+1; r < 4; ++r)
+		for (int r = pivot+1; r < F; ++r)
 			if (fabs(m[r][pivot]) > fabs(m[best][pivot])) best = r;
 		if (!isfinite(m[best][pivot]) || fabs(m[best][pivot]) < 1e-14) { failed = true; break; }
 		if (best != pivot)
-			for (int c = 0; c < 8; ++c) { const double t = m[pivot][c]; m[pivot][c] = m[best][c]; m[best][c] = t; }
+			for (int c = 0; c < 2*F; ++c) { const double t = m[pivot][c]; m[pivot][c] = m[best][c]; m[best][c] = t; }
 		const double sc = 1.0/m[pivot][pivot];
-		for (int c = 0; c < 8; ++c) m[pivot][c] *= sc;
-		for (int r = 0; r < 4; ++r) {
+		for (int c = 0; c < 2*F; ++c) m[pivot][c] *= sc;
+		for (int r = 0; r < F; ++r) {
 			if (r == pivot) continue;
 			const double factor = m[r][pivot];
-			for (int c = 0; c < 8; ++c) m[r][c] -= factor*m[pivot][c];
+			for (int c = 0; c < 2*F; ++c) m[r][c] -= factor*m[pivot][c];
 		}
 	}
-	double* d = inverse+(size_t)node*16;
+	double* d = inverse+(size_t)node*F*F;
 	if (!failed) {
-		for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) d[i*4+j] = m[i][4+j];
+		for (int i = 0; i < F; ++i) for (int j = 0; j < F; ++j) d[i*F+j] = m[i][F+j];
 	} else {
 		atomicAdd(singular, 1u);
-		for (int i = 0; i < 4; ++i)
-			for (int j = 0; j < 4; ++j)
-				d[i*4+j] = i == j && fabs(s[i*4+i]) > 1e-14 ? 1.0/s[i*4+i] : (i == j ? 1.0 : 0.0);
+		for (int i = 0; i < F; ++i)
+			for (int j = 0; j < F; ++j)
+				d[i*F+j] = i == j && fabs(s[i*F+i]) > 1e-14 ? 1.0/s[i*F+i] : (i == j ? 1.0 : 0.0);
 	}
 }
 
+template <int F>
 __global__ void ApplyBlockInverseKernel(int nodes, const double* __restrict__ inverse, const double* __restrict__ x,
 	double* __restrict__ y)
 {
 	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
-	if (i >= 4LL*nodes) return;
-	const long long node = i >> 2;
-	const int r = (int)(i & 3);
-	const double* d = inverse+node*16+r*4;
-	const double* v = x+4*node;
-	y[i] = d[0]*v[0]+d[1]*v[1]+d[2]*v[2]+d[3]*v[3];
+	if (i >= (long long)F*nodes) return;
+	const long long node = i/F;
+	const int r = (int)(i-node*F);
+	const double* d = inverse+node*F*F+r*F;
+	const double* v = x+F*node;
+	double s = d[0]*v[0];
+	#pragma unroll
+	for (int c = 1; c < F; ++c) s += d[c]*v[c];
+	y[i] = s;
 }
 
 // state = prescribed value on every constrained entry (thread per constrained node).
@@ -277,7 +281,7 @@ void LaunchBlockInverse(const DevicePatternView& p, const T* values, double* inv
 	cudaStream_t stream)
 {
 	if (p.nodes == 0) return;
-	BlockInverseKernel<T><<<Blocks(p.nodes, 128), 128, 0, stream>>>(p, values, inverse, singular);
+	BlockInverseKernel<4, T><<<Blocks(p.nodes, 128), 128, 0, stream>>>(p, values, inverse, singular);
 	LaunchCheck("BlockInverseKernel");
 }
 
@@ -300,8 +304,23 @@ void LaunchToFloat(long long n, const double* in, float* out, cudaStream_t strea
 void LaunchApplyBlockInverse(int nodes, const double* inverse, const double* x, double* y, cudaStream_t stream)
 {
 	if (nodes == 0) return;
-	ApplyBlockInverseKernel<<<Blocks(4LL*nodes, 256), 256, 0, stream>>>(nodes, inverse, x, y);
+	ApplyBlockInverseKernel<4><<<Blocks(4LL*nodes, 256), 256, 0, stream>>>(nodes, inverse, x, y);
 	LaunchCheck("ApplyBlockInverseKernel");
+}
+
+void LaunchBlockInverse2(const DevicePatternView& p, const double* values, double* inverse, unsigned int* singular,
+	cudaStream_t stream)
+{
+	if (p.nodes == 0) return;
+	BlockInverseKernel<2, double><<<Blocks(p.nodes, 128), 128, 0, stream>>>(p, values, inverse, singular);
+	LaunchCheck("BlockInverseKernel<2>");
+}
+
+void LaunchApplyBlockInverse2(int nodes, const double* inverse, const double* x, double* y, cudaStream_t stream)
+{
+	if (nodes == 0) return;
+	ApplyBlockInverseKernel<2><<<Blocks(2LL*nodes, 256), 256, 0, stream>>>(nodes, inverse, x, y);
+	LaunchCheck("ApplyBlockInverseKernel<2>");
 }
 
 template <class T>

@@ -534,6 +534,38 @@ def write_case(directory, tube: Tube, config: dict, database_name: str = "tube-1
     return db
 
 
+# Keys of a legacy transport case's simulation_parameter.txt (iga::ReadTransportParameters).
+TRANSPORT_PARAMETER_KEYS = {"diffusion": "D", "vplus": "vplus", "vminus": "vminus", "kplus": "kplus",
+                            "kminus": "kminus", "detach_plus": "k'plus", "detach_minus": "k'minus", "dt": "dt",
+                            "steps": "nstep", "n0_bc": "N0bc", "nplus_bc": "Nplusbc", "nminus_bc": "Nminusbc",
+                            "artificial_diffusion": "artificial_diffusion"}
+
+
+def transport_parameter_text(params: dict) -> str:
+    """simulation_parameter.txt: one `key value` line per parameter (missing ones are 0)."""
+    lines = []
+    for name, key in TRANSPORT_PARAMETER_KEYS.items():
+        v = params.get(name, 0)
+        lines.append(f"{key} {int(v)}" if name == "steps" else f"{key} {float(v):.17g}")
+    return "\n".join(lines) + "\n"
+
+
+def write_transport_case(directory, tube: Tube, params: dict, velocity=None, case_config: dict | None = None,
+                         database_name: str = "tube-1.ntiga") -> Path:
+    """Legacy transport case (controlmesh.vtk, initial_velocityfield.txt, simulation_parameter.txt and an
+    optional case_config.json) plus the database; returns the database path."""
+    d = Path(directory)
+    d.mkdir(parents=True, exist_ok=True)
+    write_vtk(d / "controlmesh.vtk", tube)
+    np.savetxt(d / "initial_velocityfield.txt", tube.profile if velocity is None else velocity, fmt="%.17g")
+    (d / "simulation_parameter.txt").write_text(transport_parameter_text(params))
+    if case_config is not None:
+        (d / "case_config.json").write_text(json.dumps(case_config, indent=1))
+    db = d / database_name
+    write_ntiga(db, tube.mesh)
+    return db
+
+
 # Benchmark configurations (SI units: m, kg/m^3, Pa s).
 def straight_cylinder_1280() -> Tube:
     """1,280 elements: 4x4 core + one 16-cell ring layer (32 cells/layer) x 40 layers, R 1.5 mm, L 30 mm."""
