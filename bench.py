@@ -421,7 +421,9 @@ def run_transport(args, world, rank, local):
     n = tube.mesh.nodes
     mesh = api.Mesh(tube.mesh)
     velocity = flow_velocity(api, mesh, tube, wave)
-    params = api.transport_params(steps=args.warmup + args.steps, **TRANSPORT)
+    fp32 = args.transport_precision == "fp32"
+    params = api.transport_params(steps=args.warmup + args.steps, restart=args.transport_restart,
+                                  precision=api.MIXED if fp32 else api.FP64, **TRANSPORT)
     mask, n0, nplus = api.resolve_transport_boundaries(tube.labels, velocity, params)
     velocity_pinned = torch.tensor(velocity.ravel()).pin_memory()
     mask_pinned = torch.tensor(mask).pin_memory()
@@ -497,9 +499,9 @@ def run_transport(args, world, rank, local):
     its_per_step = timed["total_iterations"] / max(args.steps, 1)
     spmv_ms, spmv_n = float(fam_ms[1]), int(fam_n[1])
     orth_ms, orth_n = float(fam_ms[2]), int(fam_n[2])
-    # one block-Jacobi SpMV launch: 2x2 values (32 B) + column index (4 B) per block, row offsets, the
-    # input vector and the output once (16 B per node each), the 2x2 inverse (32 B per node)
-    spmv_bytes = mesh.blocks * 36 + 4 * (n + 1) + 16 * n * 2 + 32 * n
+    # one block-Jacobi SpMV launch: 2x2 values (32 B FP64, 16 B FP32) + column index (4 B) per block, row
+    # offsets, the input vector and the output once (16 B per node each), the 2x2 inverse (32 B per node)
+    spmv_bytes = mesh.blocks * (20 if fp32 else 36) + 4 * (n + 1) + 16 * n * 2 + 32 * n
     kernels = {}
     if spmv_n:
         a = spmv_bytes / (spmv_ms / spmv_n * 1e-3) / 1e9
@@ -516,12 +518,14 @@ def run_transport(args, world, rank, local):
     line = {
         "metric": TRANSPORT_METRIC, "value": replica_throughput(world, args.steps, ms), "unit": "time steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64" if fp32 else "f64",
         "data": "synthetic (seeded generator; velocity from one Navier-Stokes step of the same mesh)",
         "config": {"workload": "two-species transport on the " + desc, "elements": tube.mesh.elements, "nodes": n,
                    "block_nonzeros": mesh.blocks, "coefficients": TRANSPORT,
-                   "solver": "backward Euler, constant L and P assembled once; block-Jacobi GMRES(50) rtol 1e-8 "
-                             "warm-started; FP64",
+                   "solver": ("backward Euler, constant L and P assembled once; block-Jacobi GMRES(%d) rtol 1e-8 "
+                              "warm-started; %s" % (args.transport_restart,
+                                                    "FP32 copy of L in the Arnoldi SpMV, FP64 vectors, block "
+                                                    "inverse and true residual" if fp32 else "FP64")),
                    "l2": "inputs larger than L2 (L %.2f GB)" % (mesh.blocks * 32 / 1e9),
                    "parallelism": "replicas only" if world > 1 else "single GPU"},
         "gmres_iterations_per_step": its_per_step, "final_l2": timed["final_l2"],
@@ -563,6 +567,9 @@ def main():
                          "is within this factor of its linear tolerance (0: off)")
     ap.add_argument("--forcing", default="ew", choices=["fixed", "ew"],
                     help="linear tolerance per Newton solve: fixed 1e-8, or Eisenstat-Walker forcing")
+    ap.add_argument("--transport-precision", default="fp64", choices=["fp64", "fp32"],
+                    help="transport workload: FP32 copy of L for the Arnoldi SpMV (FP64 true residual)")
+    ap.add_argument("--transport-restart", type=int, default=50, help="transport workload: GMRES restart")
     ap.add_argument("--ref-budget", type=float, default=25.0)
     ap.add_argument("--ref-newton", type=float, default=4.0)
     ap.add_argument("--ref-linear", type=float, default=228.0)

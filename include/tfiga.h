@@ -405,7 +405,11 @@ typedef struct tfiga_transport_params {
 	double artificial_diffusion; /* SUPG-weighted artificial diffusion coefficient */
 	double gmres_rtol;
 	int32_t gmres_max_iterations;
-	int32_t reserved;
+	/* TFIGA_PRECISION_FP64 (the reference's arithmetic) or TFIGA_PRECISION_MIXED:
+	 * L also kept in FP32 for the SpMV inside the Arnoldi process, while the
+	 * block inverse, the vectors and the true residual of every restart (the
+	 * stopping test) stay FP64. */
+	int32_t precision;
 } tfiga_transport_params;
 
 /* Totals of one tfiga_transport_step call (the `transport step=` and
@@ -420,7 +424,7 @@ typedef struct tfiga_transport_report {
 	uint32_t reserved;
 } tfiga_transport_report;
 
-/* Zeros, restart 50, gmres_rtol 1e-8, gmres_max_iterations 10000. */
+/* Zeros, restart 50, gmres_rtol 1e-8, gmres_max_iterations 10000, FP64. */
 void tfiga_transport_default_params(tfiga_transport_params* params);
 /* simulation_parameter.txt (ReadTransportParameters, CaseInput.hpp:85-118) into
  * the physical fields of *params (solver fields untouched).  Errors:

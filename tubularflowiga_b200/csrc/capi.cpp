@@ -501,6 +501,8 @@ int tfiga_transport_create(tfiga_mesh* mesh, const tfiga_transport_params* param
 		*out = nullptr;
 		Require(params->restart > 0, "restart must be positive");
 		Require(params->gmres_rtol > 0.0 && params->gmres_max_iterations > 0, "GMRES tolerance and limit must be positive");
+		Require(params->precision == TFIGA_PRECISION_FP64 || params->precision == TFIGA_PRECISION_MIXED,
+			"transport precision must be TFIGA_PRECISION_FP64 or TFIGA_PRECISION_MIXED");
 		tfiga::RequireDevice();
 		const tfiga::TransportCoefficients c{params->diffusion, params->vplus, params->kplus, params->kminus,
 			params->detach_plus, params->dt, params->artificial_diffusion};
@@ -508,7 +510,7 @@ int tfiga_transport_create(tfiga_mesh* mesh, const tfiga_transport_params* param
 		handle->mesh = mesh;
 		handle->params = *params;
 		handle->solver = std::make_unique<tfiga::TransportSolver>(*mesh->mesh, c, velocity, constrained, n0, nplus,
-			params->restart);
+			params->restart, params->precision == TFIGA_PRECISION_MIXED);
 		*out = handle.release();
 	});
 }

@@ -368,7 +368,8 @@ std::size_t Gmres::bytes() const
 	return V_.bytes()+w_.bytes()+r_.bytes()+tmp_.bytes()+inverse_.bytes()+partial_.bytes()+H_.bytes();
 }
 
-void Gmres::Step(const DevicePatternView& pattern, const double* values, int j)
+template <class T>
+void Gmres::Step(const DevicePatternView& pattern, const T* values, int j)
 {
 	const int* stop = state_.get();
 	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
@@ -558,7 +559,7 @@ double Gmres::TrueResidual(const DevicePatternView& pattern, const double* value
 }
 
 GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values, const double* rhs, double* x,
-	double rtol, int max_iterations, long long* launches, bool rebuild_preconditioner)
+	double rtol, int max_iterations, long long* launches, bool rebuild_preconditioner, const float* krylov_values)
 {
 	launches_ = 0;
 	GmresResult result;
@@ -590,7 +591,8 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 		for (int j = 0; j < cap;) {
 			const int batch = std::min(kBatch, cap-j);
 			for (int b = 0; b < batch; ++b) {
-				Step(pattern, values, j+b);
+				if (krylov_values) Step(pattern, krylov_values, j+b);
+				else Step(pattern, values, j+b);
 				ArnoldiFinalizeKernel<<<1, kThreads, finalize_smem_, stream_>>>(norm_partial_.get(), update_blocks_, H_.get(), restart_, j+b,
 					cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance);
 				LaunchCheck("ArnoldiFinalizeKernel");

@@ -33,9 +33,12 @@ public:
 	Gmres(const Gmres&) = delete;
 	Gmres& operator=(const Gmres&) = delete;
 	// Solves A x = rhs (x holds the initial guess).  Builds the block inverse first unless
-	// rebuild_preconditioner is false (the matrix is the one of the previous Solve).
+	// rebuild_preconditioner is false (the matrix is the one of the previous Solve).  With
+	// krylov_values (an FP32 copy of A) the Arnoldi SpMV reads it; the block inverse and each
+	// restart's true residual use the FP64 values.
 	GmresResult Solve(const DevicePatternView& pattern, const double* values, const double* rhs, double* x,
-		double rtol, int max_iterations, long long* launches, bool rebuild_preconditioner = true);
+		double rtol, int max_iterations, long long* launches, bool rebuild_preconditioner = true,
+		const float* krylov_values = nullptr);
 	// Right-preconditioned flexible GMRES (FGMRES): z_j = M^{-1} v_j stored, tolerance
 	// rtol * ||b - A x0|| on the true residual.
 	// The matrix may be stored in FP64 or FP32 (T); with FP32 the Krylov basis is stored in FP32
@@ -56,7 +59,8 @@ public:
 	std::size_t bytes() const;
 
 private:
-	void Step(const DevicePatternView& pattern, const double* values, int j);
+	template <class T>
+	void Step(const DevicePatternView& pattern, const T* values, int j);
 	template <class B> void Orthogonalize(int j, B* basis);
 	// Krylov basis storage: FP64 (V_) or FP32 (V32_, allocated on first use).
 	template <class B> B* Basis();

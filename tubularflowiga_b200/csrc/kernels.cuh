@@ -90,8 +90,9 @@ void LaunchApplyBlockInverse(int nodes, const double* inverse, const double* x, 
 void LaunchSpmv2(const DevicePatternView& pattern, const double* values, const double* x, double* y,
 	cudaStream_t stream);
 // y = D^{-1} (A x) * (*scale) with D^{-1} the 2x2 block-Jacobi inverse (scale may be null; stop: the
-// GMRES early-out flag, may be null).
-void LaunchSpmvBlockJacobi2(const DevicePatternView& pattern, const double* values, const double* inverse,
+// GMRES early-out flag, may be null).  Values FP64 or FP32.
+template <class T>
+void LaunchSpmvBlockJacobi2(const DevicePatternView& pattern, const T* values, const double* inverse,
 	const double* x, const double* scale, double* y, const int* stop, cudaStream_t stream);
 void LaunchBlockInverse2(const DevicePatternView& pattern, const double* values, double* inverse,
 	unsigned int* singular, cudaStream_t stream);

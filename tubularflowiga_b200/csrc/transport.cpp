@@ -7,7 +7,7 @@
 namespace tfiga {
 
 TransportSolver::TransportSolver(Mesh& mesh, const TransportCoefficients& coefficients, const double* velocity,
-	const int32_t* constrained, const double* n0, const double* nplus, int restart)
+	const int32_t* constrained, const double* n0, const double* nplus, int restart, bool fp32_krylov)
 	: mesh_(mesh), nodes_((int)mesh.nodes()), gmres_((int)mesh.nodes(), restart, mesh.stream(), 2)
 {
 	if (!(coefficients.dt > 0.0) || !std::isfinite(coefficients.dt)) Fail(-1, "transport dt must be positive");
@@ -48,6 +48,11 @@ TransportSolver::TransportSolver(Mesh& mesh, const TransportCoefficients& coeffi
 		coefficients, left_.get(), previous_.get(), s);
 	LaunchTransportBoundaryRows(pattern, constrained_count_, constrained_.get(), left_.get(), previous_.get(), s);
 	LaunchTransportBoundaryValues(constrained_count_, constrained_.get(), n0_.get(), nplus_.get(), current_.get(), s);
+	if (fp32_krylov) {
+		left32_.Allocate((size_t)pattern.blocks*4);
+		LaunchToFloat((long long)pattern.blocks*4, left_.get(), left32_.get(), s);
+		launches_ += 1;
+	}
 	CudaCheck(cudaEventRecord(stop, s), "event");
 	CudaCheck(cudaStreamSynchronize(s), "transport assembly");
 	float ms = 0.0f;
@@ -74,7 +79,7 @@ TransportStepResult TransportSolver::Step(double rtol, int max_iterations)
 		"transport warm start");
 	long long launches = 0;
 	const GmresResult r = gmres_.Solve(pattern, left_.get(), rhs_.get(), next_.get(), rtol, max_iterations,
-		&launches, steps_ == 0);
+		&launches, steps_ == 0, left32_.size() ? left32_.get() : nullptr);
 	launches_ += launches;
 	if (!r.converged)
 		Fail(-6, "transport GMRES did not converge at step "+std::to_string(steps_)+"; residual "

@@ -19,8 +19,9 @@
 // The pair -> block map is the per-mesh element_blocks table (no search).
 //
 // SpMV (BlockSpmvKernel<2>, SparseKernels.cuh:25-40): one warp per block row,
-// lane l multiplies blocks l, l + 32, ... (32 bytes of values each, two
-// 16-byte loads), so a warp streams 1 KB of the matrix per step.
+// lane l multiplies blocks l, l + 32, ... (32 bytes of FP64 values each, two
+// 16-byte loads; or 16 bytes of FP32 values, one load), so a warp streams up
+// to 1 KB of the matrix per step.
 #include "common.hpp"
 #include "kernels.cuh"
 #include "transport.hpp"
@@ -164,8 +165,27 @@ __global__ void TransportBoundaryValuesKernel(int count, const int32_t* __restri
 	vector[2*node+1] = nplus[node];
 }
 
+// One 2x2 block (row-major) as doubles: two 16-byte loads (FP64) or one (FP32).
+template <class T> struct Block2;
+template <> struct Block2<double> {
+	static __device__ __forceinline__ void Get(const double* values, int b, double a[4])
+	{
+		const double2* v = reinterpret_cast<const double2*>(values+4*(size_t)b);
+		const double2 r0 = __ldg(v), r1 = __ldg(v+1);
+		a[0] = r0.x; a[1] = r0.y; a[2] = r1.x; a[3] = r1.y;
+	}
+};
+template <> struct Block2<float> {
+	static __device__ __forceinline__ void Get(const float* values, int b, double a[4])
+	{
+		const float4 v = __ldg(reinterpret_cast<const float4*>(values+4*(size_t)b));
+		a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+	}
+};
+
 // Returns (A x)[2 row + (lane & 1)] in every lane.
-__device__ __forceinline__ double RowBlockDot2(const DevicePatternView& p, const double* __restrict__ values,
+template <class T>
+__device__ __forceinline__ double RowBlockDot2(const DevicePatternView& p, const T* __restrict__ values,
 	const double* __restrict__ x, int row, int lane)
 {
 	double s0 = 0.0, s1 = 0.0;
@@ -175,11 +195,11 @@ __device__ __forceinline__ double RowBlockDot2(const DevicePatternView& p, const
 	while (b < hi) {
 		const int next = b+32;
 		const int next_col = next < hi ? p.columns[next] : 0;
-		const double2* v = reinterpret_cast<const double2*>(values+4*(size_t)b);
-		const double2 r0 = __ldg(v), r1 = __ldg(v+1);
+		double a[4];
+		Block2<T>::Get(values, b, a);
 		const double2 xv = __ldg(reinterpret_cast<const double2*>(x+2*(size_t)col));
-		s0 = fma(r0.x, xv.x, s0); s0 = fma(r0.y, xv.y, s0);
-		s1 = fma(r1.x, xv.x, s1); s1 = fma(r1.y, xv.y, s1);
+		s0 = fma(a[0], xv.x, s0); s0 = fma(a[1], xv.y, s0);
+		s1 = fma(a[2], xv.x, s1); s1 = fma(a[3], xv.y, s1);
 		b = next;
 		col = next_col;
 	}
@@ -205,7 +225,8 @@ __global__ void __launch_bounds__(256) Spmv2Kernel(DevicePatternView p, const do
 	if (lane < 2) y[2*(size_t)row+lane] = sum;
 }
 
-__global__ void __launch_bounds__(256) SpmvBlockJacobi2Kernel(DevicePatternView p, const double* __restrict__ values,
+template <class T>
+__global__ void __launch_bounds__(256) SpmvBlockJacobi2Kernel(DevicePatternView p, const T* __restrict__ values,
 	const double* __restrict__ inverse, const double* __restrict__ x, const double* __restrict__ scale,
 	double* __restrict__ y, const int* __restrict__ stop)
 {
@@ -263,12 +284,18 @@ void LaunchSpmv2(const DevicePatternView& p, const double* values, const double*
 	LaunchCheck("Spmv2Kernel");
 }
 
-void LaunchSpmvBlockJacobi2(const DevicePatternView& p, const double* values, const double* inverse,
+template <class T>
+void LaunchSpmvBlockJacobi2(const DevicePatternView& p, const T* values, const double* inverse,
 	const double* x, const double* scale, double* y, const int* stop, cudaStream_t stream)
 {
 	if (p.nodes == 0) return;
-	SpmvBlockJacobi2Kernel<<<Grid(p.nodes, 8), 256, 0, stream>>>(p, values, inverse, x, scale, y, stop);
+	SpmvBlockJacobi2Kernel<T><<<Grid(p.nodes, 8), 256, 0, stream>>>(p, values, inverse, x, scale, y, stop);
 	LaunchCheck("SpmvBlockJacobi2Kernel");
 }
+
+template void LaunchSpmvBlockJacobi2<double>(const DevicePatternView&, const double*, const double*, const double*,
+	const double*, double*, const int*, cudaStream_t);
+template void LaunchSpmvBlockJacobi2<float>(const DevicePatternView&, const float*, const double*, const double*,
+	const double*, double*, const int*, cudaStream_t);
 
 } // namespace tfiga

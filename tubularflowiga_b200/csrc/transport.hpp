@@ -51,9 +51,10 @@ class TransportSolver {
 public:
 	// velocity [3 nodes], constrained [nodes] (nonzero: Dirichlet node), n0 / nplus [nodes]:
 	// host or device pointers.  Assembles both matrices, applies the boundary rows and sets the
-	// boundary values into the zero initial state.
+	// boundary values into the zero initial state.  fp32_krylov: an FP32 copy of L serves the SpMV
+	// of the Arnoldi process (the true residual of every restart stays FP64).
 	TransportSolver(Mesh& mesh, const TransportCoefficients& coefficients, const double* velocity,
-		const int32_t* constrained, const double* n0, const double* nplus, int restart);
+		const int32_t* constrained, const double* n0, const double* nplus, int restart, bool fp32_krylov = false);
 	TransportSolver(const TransportSolver&) = delete;
 	TransportSolver& operator=(const TransportSolver&) = delete;
 
@@ -80,6 +81,7 @@ private:
 	long long launches_ = 0;
 	double assembly_ms_ = 0.0;
 	DeviceArray<double> left_, previous_, current_, next_, rhs_, n0_, nplus_, scratch_;
+	DeviceArray<float> left32_;        // FP32 copy of L (fp32_krylov)
 	DeviceArray<int32_t> constrained_;
 	int constrained_count_ = 0;
 	Gmres gmres_;
