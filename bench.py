@@ -417,10 +417,15 @@ def run_transport(args, world, rank, local):
     else:
         torch.cuda.set_device(0)
     from tubularflowiga_b200 import api
-    tube, desc, wave = workload("c3")
+    tube, desc, wave = workload(args.transport_mesh)
     n = tube.mesh.nodes
     mesh = api.Mesh(tube.mesh)
-    velocity = flow_velocity(api, mesh, tube, wave)
+    if args.transport_mesh == "c3":
+        velocity = flow_velocity(api, mesh, tube, wave)
+    else:
+        # Poiseuille flow of the straight tube: peak 2 x mean along the axis
+        velocity = 0.3 * tube.profile
+        desc += "; Poiseuille velocity, mean 0.15 m/s"
     fp32 = args.transport_precision == "fp32"
     params = api.transport_params(steps=args.warmup + args.steps, restart=args.transport_restart,
                                   precision=api.MIXED if fp32 else api.FP64, **TRANSPORT)
@@ -570,6 +575,9 @@ def main():
     ap.add_argument("--transport-precision", default="fp64", choices=["fp64", "fp32"],
                     help="transport workload: FP32 copy of L for the Arnoldi SpMV (FP64 true residual)")
     ap.add_argument("--transport-restart", type=int, default=50, help="transport workload: GMRES restart")
+    ap.add_argument("--transport-mesh", default="c3", choices=["c3", "c2-100"],
+                    help="transport workload mesh: c3 with the velocity of one Navier-Stokes step, or the "
+                         "12,800-element tube section with its Poiseuille profile at 0.15 m/s mean (profiling case)")
     ap.add_argument("--ref-budget", type=float, default=25.0)
     ap.add_argument("--ref-newton", type=float, default=4.0)
     ap.add_argument("--ref-linear", type=float, default=228.0)
