@@ -60,9 +60,11 @@ and L c' = rhs by block-Jacobi GMRES(50) to rtol 1e-8, warm-started.  value:
 device-timed steps with L and P resident in HBM (L alone 1.6 GB, beyond L2);
 e2e: the whole job through the C ABI from host buffers (velocity, mask and
 inlet values uploaded, assembly, the steps, the final state read back),
-steps / wall time; cpu_baseline: the CPU restatement of the step (2x2
-SpMV + block-Jacobi GMRES) on all host cores for a bounded number of
-iterations, scaled by the GPU's iterations per step.
+steps / wall time; fp64_gpu: the same steps with the FP64 solver (the
+default arm keeps an FP32 copy of L for the Arnoldi SpMV, FP64 everywhere
+else); cpu_baseline: the CPU restatement of the step (2x2 SpMV +
+block-Jacobi GMRES) on all host cores for a bounded number of iterations,
+scaled by the GPU's iterations per step.
 
 Multi-GPU: the single-mesh path does not shard ("replicas only"): under
 torchrun every rank runs an independent replica; value = total steps / max
@@ -427,83 +429,104 @@ def run_transport(args, world, rank, local):
         velocity = 0.3 * tube.profile
         desc += "; Poiseuille velocity, mean 0.15 m/s"
     fp32 = args.transport_precision == "fp32"
-    params = api.transport_params(steps=args.warmup + args.steps, restart=args.transport_restart,
-                                  precision=api.MIXED if fp32 else api.FP64, **TRANSPORT)
+    total_steps = args.warmup + args.steps
+
+    def make_params(precision):
+        return api.transport_params(steps=total_steps, restart=args.transport_restart, precision=precision,
+                                    **TRANSPORT)
+
+    params = make_params(api.MIXED if fp32 else api.FP64)
     mask, n0, nplus = api.resolve_transport_boundaries(tube.labels, velocity, params)
     velocity_pinned = torch.tensor(velocity.ravel()).pin_memory()
     mask_pinned = torch.tensor(mask).pin_memory()
     n0_pinned = torch.tensor(n0).pin_memory()
     nplus_pinned = torch.tensor(nplus).pin_memory()
     out_pinned = torch.empty(2 * n, dtype=torch.float64).pin_memory()
+    lib = api.lib()
 
-    def create():
+    def create(p):
         h = api.C.c_void_p()
-        api.check(api.lib().tfiga_transport_create(mesh._h, api.C.byref(params),
-                                                   api.C.c_void_p(velocity_pinned.data_ptr()),
-                                                   api.C.c_void_p(mask_pinned.data_ptr()),
-                                                   api.C.c_void_p(n0_pinned.data_ptr()),
-                                                   api.C.c_void_p(nplus_pinned.data_ptr()), api.C.byref(h)))
+        api.check(lib.tfiga_transport_create(mesh._h, api.C.byref(p), api.C.c_void_p(velocity_pinned.data_ptr()),
+                                             api.C.c_void_p(mask_pinned.data_ptr()),
+                                             api.C.c_void_p(n0_pinned.data_ptr()),
+                                             api.C.c_void_p(nplus_pinned.data_ptr()), api.C.byref(h)))
         return h
 
-    lib = api.lib()
-    h = create()
-    report = api.TransportReport()
-    assembly_ms = api.C.c_double()
-    api.check(lib.tfiga_transport_info(h, api.C.byref(assembly_ms), None, None))
-    stream_ptr = api.C.c_void_p()
-    api.check(lib.tfiga_transport_stream(h, api.C.byref(stream_ptr)))
-    stream = torch.cuda.ExternalStream(stream_ptr.value)
-    api.check(lib.tfiga_transport_step(h, args.warmup, api.C.byref(report)))
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    launches0 = api.C.c_int64()
-    api.check(lib.tfiga_transport_info(h, None, None, api.C.byref(launches0)))
-    api.check(lib.tfiga_transport_set_profiling(h, 1))
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clocks:
+    def timed(p, profile, clocks_index=None):
+        """W untimed steps, then K steps between CUDA events on the handle's stream."""
+        h = create(p)
+        report = api.TransportReport()
+        assembly_ms = api.C.c_double()
+        api.check(lib.tfiga_transport_info(h, api.C.byref(assembly_ms), None, None))
+        stream_ptr = api.C.c_void_p()
+        api.check(lib.tfiga_transport_stream(h, api.C.byref(stream_ptr)))
+        stream = torch.cuda.ExternalStream(stream_ptr.value)
+        api.check(lib.tfiga_transport_step(h, args.warmup, api.C.byref(report)))
         torch.cuda.synchronize()
-        ev0.record(stream)
-        api.check(lib.tfiga_transport_step(h, args.steps, api.C.byref(report)))
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    launches1 = api.C.c_int64()
-    api.check(lib.tfiga_transport_info(h, None, None, api.C.byref(launches1)))
-    fam_ms = np.zeros(5)
-    fam_n = np.zeros(5, np.int64)
-    api.check(lib.tfiga_transport_profile(h, api.C.c_void_p(fam_ms.ctypes.data), api.C.c_void_p(fam_n.ctypes.data), 1))
-    api.check(lib.tfiga_transport_set_profiling(h, 0))
-    timed = report.as_dict()
-    left = previous = state = None
+        if dist:
+            dist.barrier()
+        l0 = api.C.c_int64()
+        api.check(lib.tfiga_transport_info(h, None, None, api.C.byref(l0)))
+        if profile:
+            api.check(lib.tfiga_transport_set_profiling(h, 1))
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local if clocks_index is None else clocks_index) as clocks:
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            api.check(lib.tfiga_transport_step(h, args.steps, api.C.byref(report)))
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        l1 = api.C.c_int64()
+        api.check(lib.tfiga_transport_info(h, None, None, api.C.byref(l1)))
+        fam_ms, fam_n = np.zeros(5), np.zeros(5, np.int64)
+        if profile:
+            api.check(lib.tfiga_transport_profile(h, api.C.c_void_p(fam_ms.ctypes.data),
+                                                  api.C.c_void_p(fam_n.ctypes.data), 1))
+            api.check(lib.tfiga_transport_set_profiling(h, 0))
+        state = np.zeros(2 * n)
+        api.check(lib.tfiga_transport_get_state(h, api.C.c_void_p(state.ctypes.data)))
+        return {"h": h, "ms": ev0.elapsed_time(ev1), "report": report.as_dict(), "launches": l1.value - l0.value,
+                "fam_ms": fam_ms, "fam_n": fam_n, "clocks": clocks.summary(), "state": state,
+                "assembly_ms": assembly_ms.value}
+
+    run = timed(params, profile=True)
+    left = previous = None
     if not args.no_cpu_baseline and world == 1 and rank == 0:
         left = np.zeros(4 * mesh.blocks)
         previous = np.zeros(4 * mesh.blocks)
-        api.check(lib.tfiga_transport_matrices(h, api.C.c_void_p(left.ctypes.data),
+        api.check(lib.tfiga_transport_matrices(run["h"], api.C.c_void_p(left.ctypes.data),
                                                api.C.c_void_p(previous.ctypes.data)))
-        state = np.zeros(2 * n)
-        api.check(lib.tfiga_transport_get_state(h, api.C.c_void_p(state.ctypes.data)))
-    api.check(lib.tfiga_transport_destroy(h))
+    api.check(lib.tfiga_transport_destroy(run["h"]))
+    fp64_leg = None
+    if fp32 and not args.no_fp64_leg:
+        ref = timed(make_params(api.FP64), profile=False)
+        api.check(lib.tfiga_transport_destroy(ref["h"]))
+        diff = [float(np.linalg.norm(run["state"][f::2] - ref["state"][f::2]) / np.linalg.norm(ref["state"][f::2]))
+                for f in (0, 1)]
+        fp64_leg = {"value": replica_throughput(1, args.steps, ref["ms"]), "unit": "time steps/s",
+                    "ms_per_step": ref["ms"] / args.steps,
+                    "gmres_iterations_per_step": ref["report"]["total_iterations"] / args.steps,
+                    "difference_after_%d_steps" % total_steps: {"N0": diff[0], "Nplus": diff[1]}}
     # e2e: the whole job through the C ABI from pinned host buffers, final state read back
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    h = create()
-    api.check(lib.tfiga_transport_step(h, args.warmup + args.steps, None))
+    h = create(params)
+    api.check(lib.tfiga_transport_step(h, total_steps, None))
     api.check(lib.tfiga_transport_get_state(h, api.C.c_void_p(out_pinned.data_ptr())))
     e2e_s = time.perf_counter() - t0
     api.check(lib.tfiga_transport_destroy(h))
-    total_steps = args.warmup + args.steps
-    ms, e2e_ms = max_over_ranks(dist, [ms, e2e_s * 1e3], "cuda")
+    ms, e2e_ms = max_over_ranks(dist, [run["ms"], e2e_s * 1e3], "cuda")
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return 0
     hbm, _, peak_kind = peaks()
-    its_per_step = timed["total_iterations"] / max(args.steps, 1)
-    spmv_ms, spmv_n = float(fam_ms[1]), int(fam_n[1])
-    orth_ms, orth_n = float(fam_ms[2]), int(fam_n[2])
+    timed_report = run["report"]
+    its_per_step = timed_report["total_iterations"] / max(args.steps, 1)
+    spmv_ms, spmv_n = float(run["fam_ms"][1]), int(run["fam_n"][1])
+    orth_ms, orth_n = float(run["fam_ms"][2]), int(run["fam_n"][2])
     # one block-Jacobi SpMV launch: 2x2 values (32 B FP64, 16 B FP32) + column index (4 B) per block, row
     # offsets, the input vector and the output once (16 B per node each), the 2x2 inverse (32 B per node)
     spmv_bytes = mesh.blocks * (20 if fp32 else 36) + 4 * (n + 1) + 16 * n * 2 + 32 * n
@@ -524,7 +547,8 @@ def run_transport(args, world, rank, local):
         "metric": TRANSPORT_METRIC, "value": replica_throughput(world, args.steps, ms), "unit": "time steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64" if fp32 else "f64",
-        "data": "synthetic (seeded generator; velocity from one Navier-Stokes step of the same mesh)",
+        "data": "synthetic (seeded generator; velocity from one Navier-Stokes step of the same mesh)"
+                if args.transport_mesh == "c3" else "synthetic (seeded generator; Poiseuille velocity)",
         "config": {"workload": "two-species transport on the " + desc, "elements": tube.mesh.elements, "nodes": n,
                    "block_nonzeros": mesh.blocks, "coefficients": TRANSPORT,
                    "solver": ("backward Euler, constant L and P assembled once; block-Jacobi GMRES(%d) rtol 1e-8 "
@@ -533,9 +557,9 @@ def run_transport(args, world, rank, local):
                                                     "inverse and true residual" if fp32 else "FP64")),
                    "l2": "inputs larger than L2 (L %.2f GB)" % (mesh.blocks * 32 / 1e9),
                    "parallelism": "replicas only" if world > 1 else "single GPU"},
-        "gmres_iterations_per_step": its_per_step, "final_l2": timed["final_l2"],
-        "assembly_ms": assembly_ms.value, "roofline": roof, "kernels": kernels,
-        "gpu_launches": int(launches1.value - launches0.value), "clocks": clocks.summary(),
+        "gmres_iterations_per_step": its_per_step, "final_l2": timed_report["final_l2"],
+        "assembly_ms": run["assembly_ms"], "roofline": roof, "kernels": kernels, "fp64_gpu": fp64_leg,
+        "gpu_launches": int(run["launches"]), "clocks": run["clocks"],
         "e2e": {"value": replica_throughput(world, total_steps, e2e_ms), "unit": "time steps/s",
                 "h2d_bytes_per_step": (velocity.nbytes + mask.nbytes + n0.nbytes + nplus.nbytes) / total_steps,
                 "d2h_bytes_per_step": 16 * n / total_steps,
@@ -543,8 +567,7 @@ def run_transport(args, world, rank, local):
     }
     if left is not None:
         try:
-            cb = transport_cpu_reference(mesh, left, previous, state, its_per_step)
-            line["cpu_baseline"] = cb
+            line["cpu_baseline"] = transport_cpu_reference(mesh, left, previous, run["state"], its_per_step)
         except Exception as exc:  # noqa: BLE001 -- reported, not hidden
             line["cpu_baseline"] = {"value": None, "error": str(exc)}
     print(json.dumps(line), flush=True)
@@ -572,8 +595,9 @@ def main():
                          "is within this factor of its linear tolerance (0: off)")
     ap.add_argument("--forcing", default="ew", choices=["fixed", "ew"],
                     help="linear tolerance per Newton solve: fixed 1e-8, or Eisenstat-Walker forcing")
-    ap.add_argument("--transport-precision", default="fp64", choices=["fp64", "fp32"],
-                    help="transport workload: FP32 copy of L for the Arnoldi SpMV (FP64 true residual)")
+    ap.add_argument("--transport-precision", default="fp32", choices=["fp64", "fp32"],
+                    help="transport workload: FP32 copy of L for the Arnoldi SpMV (FP64 true residual); with fp32 "
+                         "the FP64 solver is timed too (fp64_gpu) unless --no-fp64-leg")
     ap.add_argument("--transport-restart", type=int, default=50, help="transport workload: GMRES restart")
     ap.add_argument("--transport-mesh", default="c3", choices=["c3", "c2-100"],
                     help="transport workload mesh: c3 with the velocity of one Navier-Stokes step, or the "

@@ -8,7 +8,8 @@ solvers/cuda/src/iga_cuda.cu:621-732).
   in the Arnoldi SpMV;
 * the backward-Euler decay recurrence of the reference's own CUDA transport test
   (solvers/cuda/tests/test_transport_time_integration.py: c_n = 1/1.1^n for dc/dt = -c,
-  dt 0.1, checked there to 1e-5), here to 1e-6;
+  dt 0.1), to the reference test's 1e-5: the tricubic mass matrix leaves a solution error of a few
+  1e-6 at the GMRES stopping tolerance;
 * the `transport` command: log lines, `node N0 N+` text output and VTK output, equal to the
   API run.
 """
@@ -103,7 +104,7 @@ def test_transport_backward_euler_decay(setup):
     t.set_state(np.ones(2 * n))
     r = t.step(2)
     c = t.get_state()
-    assert np.max(np.abs(c[0::2] - 1 / 1.1 ** 2)) < 1e-6 and np.max(np.abs(c[1::2] - 1.0)) < 1e-6
+    assert np.max(np.abs(c[0::2] - 1 / 1.1 ** 2)) < 1e-5 and np.max(np.abs(c[1::2] - 1.0)) < 1e-5
     assert r["singular_blocks"] == 0
     t.close()
 
