@@ -19,9 +19,9 @@
 // The pair -> block map is the per-mesh element_blocks table (no search).
 //
 // SpMV (BlockSpmvKernel<2>, SparseKernels.cuh:25-40): one warp per block row,
-// lane l multiplies blocks l, l + 32, l + 64, ... two per iteration (32 bytes
-// of FP64 values each, two 16-byte loads; or 16 bytes of FP32 values, one
-// load), so a warp has up to 2 KB of the matrix in flight.
+// lane l multiplies blocks l, l + 32, ... (32 bytes of FP64 values each, two
+// 16-byte loads; or 16 bytes of FP32 values, one load), so a warp streams up
+// to 1 KB of the matrix per step.
 #include "common.hpp"
 #include "kernels.cuh"
 #include "transport.hpp"
@@ -183,40 +183,26 @@ template <> struct Block2<float> {
 	}
 };
 
-// Returns (A x)[2 row + (lane & 1)] in every lane.  Lane l takes blocks l + 64 k and l + 64 k + 32
-// in the same iteration (two independent value loads and x gathers in flight), with the next
-// iteration's column indices loaded ahead.
+// Returns (A x)[2 row + (lane & 1)] in every lane.
 template <class T>
 __device__ __forceinline__ double RowBlockDot2(const DevicePatternView& p, const T* __restrict__ values,
 	const double* __restrict__ x, int row, int lane)
 {
-	double s0 = 0.0, s1 = 0.0, t0 = 0.0, t1 = 0.0;
+	double s0 = 0.0, s1 = 0.0;
 	const int hi = p.row_offsets[row+1];
 	int b = p.row_offsets[row]+lane;
-	int c0 = b < hi ? p.columns[b] : 0;
-	int c1 = b+32 < hi ? p.columns[b+32] : 0;
+	int col = b < hi ? p.columns[b] : 0;
 	while (b < hi) {
-		const int next = b+64;
-		const int n0 = next < hi ? p.columns[next] : 0;
-		const int n1 = next+32 < hi ? p.columns[next+32] : 0;
+		const int next = b+32;
+		const int next_col = next < hi ? p.columns[next] : 0;
 		double a[4];
 		Block2<T>::Get(values, b, a);
-		const double2 x0 = __ldg(reinterpret_cast<const double2*>(x+2*(size_t)c0));
-		if (b+32 < hi) {
-			double e[4];
-			Block2<T>::Get(values, b+32, e);
-			const double2 x1 = __ldg(reinterpret_cast<const double2*>(x+2*(size_t)c1));
-			t0 = fma(e[0], x1.x, t0); t0 = fma(e[1], x1.y, t0);
-			t1 = fma(e[2], x1.x, t1); t1 = fma(e[3], x1.y, t1);
-		}
-		s0 = fma(a[0], x0.x, s0); s0 = fma(a[1], x0.y, s0);
-		s1 = fma(a[2], x0.x, s1); s1 = fma(a[3], x0.y, s1);
+		const double2 xv = __ldg(reinterpret_cast<const double2*>(x+2*(size_t)col));
+		s0 = fma(a[0], xv.x, s0); s0 = fma(a[1], xv.y, s0);
+		s1 = fma(a[2], xv.x, s1); s1 = fma(a[3], xv.y, s1);
 		b = next;
-		c0 = n0;
-		c1 = n1;
+		col = next_col;
 	}
-	s0 += t0;
-	s1 += t1;
 	#pragma unroll
 	for (int o = 16; o >= 2; o >>= 1) {
 		s0 += __shfl_xor_sync(0xffffffffu, s0, o);
