@@ -92,6 +92,9 @@ RHO, MU, DT = 1060.0, 3.5e-3, 2e-3
 # (dram__bytes_read.sum + dram__bytes_write.sum = 202,687,488 B on the 12,800-element section,
 # 2,919,695 blocks); the launch streams the matrix once, so traffic scales with the block count.
 SPMV_FP32_DRAM_BYTES_PER_BLOCK = 202687488 / 2919695
+# The same for the transport's 2x2 block-Jacobi SpMV with the FP32 copy of L (59,472,384 B on the same
+# section's 2,919,695 blocks).
+TRANSPORT_SPMV_FP32_DRAM_BYTES_PER_BLOCK = 59472384 / 2919695
 
 
 def peaks():
@@ -533,8 +536,9 @@ def run_transport(args, world, rank, local):
     kernels = {}
     if spmv_n:
         a = spmv_bytes / (spmv_ms / spmv_n * 1e-3) / 1e9
+        traffic = TRANSPORT_SPMV_FP32_DRAM_BYTES_PER_BLOCK * mesh.blocks if fp32 else None
         kernels["spmv_block_jacobi_2x2"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
-                                            "frac": a / hbm, "traffic": None, "launches": spmv_n,
+                                            "frac": a / hbm, "traffic": traffic, "launches": spmv_n,
                                             "avg_ms": spmv_ms / spmv_n, "share": spmv_ms / ms,
                                             "algorithmic_bytes": spmv_bytes}
     if orth_n:
