@@ -193,15 +193,25 @@ void NsSolver::CommitStep()
 		"previous-state copy");
 }
 
-void NsSolver::AssembleResidualTc()
+void NsSolver::AssembleResidualTc(bool coefficients)
 {
 	rhs_.Zero(stream_);
 	profiler_.Begin(Profiler::kResidual, stream_);
 	LaunchTangentPoint(mesh_.view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
-		{params_.density, params_.viscosity, params_.dt}, coef32_.get(), rhs_.get(), stream_);
+		{params_.density, params_.viscosity, params_.dt}, coefficients ? coef32_.get() : nullptr, rhs_.get(),
+		stream_);
 	profiler_.End(stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
 	launches_ += 2;
+}
+
+void NsSolver::AssembleCoefficientsTc()
+{
+	profiler_.Begin(Profiler::kResidual, stream_);
+	LaunchTangentPoint(mesh_.view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
+		{params_.density, params_.viscosity, params_.dt}, coef32_.get(), nullptr, stream_);
+	profiler_.End(stream_);
+	launches_ += 1;
 }
 
 void NsSolver::AssembleTangentTc()
@@ -219,7 +229,7 @@ void NsSolver::AssembleTangentTc()
 void NsSolver::Assemble()
 {
 	if (tensor_tangent()) {
-		AssembleResidualTc();
+		AssembleResidualTc(true);
 		AssembleTangentTc();
 		return;
 	}
@@ -368,7 +378,9 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	// before the tangent, and an iteration that passes it contracts no tangent at all.
 	const bool tc = tensor_tangent();
 	CudaCheck(cudaEventRecord(events_[0], stream_), "event");
-	if (tc) AssembleResidualTc();
+	// the residual-only point kernel: the coefficients are computed only for an iteration that
+	// contracts a new tangent
+	if (tc) AssembleResidualTc(false);
 	else Assemble();
 	LaunchDiagnostics();
 	if (tc) ApplyDirichletRhs();
@@ -405,6 +417,7 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	reuse_norm_ = norm;
 	if (tc && !reuse) {
 		CudaCheck(cudaEventRecord(events_[4], stream_), "event");
+		AssembleCoefficientsTc();
 		AssembleTangentTc();
 		ApplyDirichletMatrix();
 		tangent_valid_ = true;
