@@ -833,11 +833,10 @@ def main():
                              "avg_ms": asm_ms / asm_n, "share": asm_ms / ms,
                              "peak_note": "nominal B200 FP64 (no measured FP64 peak on this pool)"}
     if res_n:
-        # FP64 point kernels of the tensor-core modes: every launch reads the FP64 basis tables
-        # (5 x 64 x 64 doubles per element) and the point data (64 x 11 doubles); the launches that
-        # precede a tangent (one per tensor-core launch) also write the coefficients of four row
-        # fields (4 x 80 x 64 floats per element).  Bytes per launch: the mean over the family.
-        rbytes = tube.mesh.elements * ((5 * 64 * 64 * 8 + 64 * 11 * 8) + 4 * 80 * 64 * 4 * asm_n / res_n)
+        # FP64 residual + point coefficients of the tensor-core modes: per element it reads the FP64
+        # basis tables (5 x 64 x 64 doubles) and the point data (64 x 11 doubles) and writes the
+        # coefficients of four row fields (4 x 80 x 64 floats)
+        rbytes = tube.mesh.elements * (5 * 64 * 64 * 8 + 64 * 11 * 8 + 4 * 80 * 64 * 4)
         a = rbytes / (res_ms / res_n * 1e-3) / 1e9
         kernels["residual_point"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s", "frac": a / hbm,
                                      "traffic": None, "launches": res_n, "avg_ms": res_ms / res_n,

@@ -193,25 +193,15 @@ void NsSolver::CommitStep()
 		"previous-state copy");
 }
 
-void NsSolver::AssembleResidualTc(bool coefficients)
+void NsSolver::AssembleResidualTc()
 {
 	rhs_.Zero(stream_);
 	profiler_.Begin(Profiler::kResidual, stream_);
 	LaunchTangentPoint(mesh_.view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
-		{params_.density, params_.viscosity, params_.dt}, coefficients ? coef32_.get() : nullptr, rhs_.get(),
-		stream_);
+		{params_.density, params_.viscosity, params_.dt}, coef32_.get(), rhs_.get(), stream_);
 	profiler_.End(stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
 	launches_ += 2;
-}
-
-void NsSolver::AssembleCoefficientsTc()
-{
-	profiler_.Begin(Profiler::kResidual, stream_);
-	LaunchTangentPoint(mesh_.view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
-		{params_.density, params_.viscosity, params_.dt}, coef32_.get(), nullptr, stream_);
-	profiler_.End(stream_);
-	launches_ += 1;
 }
 
 void NsSolver::AssembleTangentTc()
@@ -229,7 +219,7 @@ void NsSolver::AssembleTangentTc()
 void NsSolver::Assemble()
 {
 	if (tensor_tangent()) {
-		AssembleResidualTc(true);
+		AssembleResidualTc();
 		AssembleTangentTc();
 		return;
 	}
@@ -378,9 +368,7 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	// before the tangent, and an iteration that passes it contracts no tangent at all.
 	const bool tc = tensor_tangent();
 	CudaCheck(cudaEventRecord(events_[0], stream_), "event");
-	// the residual-only point kernel: the coefficients are computed only for an iteration that
-	// contracts a new tangent
-	if (tc) AssembleResidualTc(false);
+	if (tc) AssembleResidualTc();
 	else Assemble();
 	LaunchDiagnostics();
 	if (tc) ApplyDirichletRhs();
@@ -417,7 +405,6 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	reuse_norm_ = norm;
 	if (tc && !reuse) {
 		CudaCheck(cudaEventRecord(events_[4], stream_), "event");
-		AssembleCoefficientsTc();
 		AssembleTangentTc();
 		ApplyDirichletMatrix();
 		tangent_valid_ = true;

@@ -86,12 +86,9 @@ private:
 		double continuity_l2, continuity_sum, net_flow, absolute_flow, imbalance;
 	};
 	void ApplyTractions(const std::map<int32_t, double>& traction);
-	// Tensor-core modes: the FP64 residual (rhs = -r + traction), with the point coefficients of the
-	// same state when `coefficients`; AssembleCoefficientsTc: the point coefficients alone (for a
-	// tangent after a residual-only pass); AssembleTangentTc: the tangent from those coefficients into
-	// the FP32 Jacobian (builds the AMG on first use).
-	void AssembleResidualTc(bool coefficients);
-	void AssembleCoefficientsTc();
+	// Tensor-core modes: the FP64 residual and point coefficients (rhs = -r + traction), then the
+	// tangent from those coefficients into the FP32 Jacobian (builds the AMG on first use).
+	void AssembleResidualTc();
 	void ApplyDirichletParts(bool matrix, bool rhs);
 	void AssembleTangentTc();
 	std::vector<OutletModel> OutletModels(const tfiga_outlet* outlets, int count) const;

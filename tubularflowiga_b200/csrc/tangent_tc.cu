@@ -297,8 +297,6 @@ __device__ __forceinline__ void PointCoefficients(const PointState& S, const dou
 	for (int k = 0; k < 40; ++k) out[(size_t)(40+k)*kQuad] = scratch[k];
 }
 
-// kWriteCoef: write the tangent coefficients; kResidual: add the residual into rhs (at least one).
-template <bool kWriteCoef, bool kResidual>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ state,
 	const double* __restrict__ previous, AssemblyParams prm, float* __restrict__ coef, double* __restrict__ rhs)
@@ -387,26 +385,16 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 		}
 		S.p = s[kP];
 		const double* qd = qdata+((size_t)e*kQuad+q)*kQData;
+		float* scratch = Scratch+tid*kScratchStride;
+		float* out = coef+((size_t)e*4+il)*kCoef*kQuad+q;
 		double* rc = RC+(il*kQuad+q)*kRcStride;
-		if constexpr (kWriteCoef) {
-			float* scratch = Scratch+tid*kScratchStride;
-			float* out = coef+((size_t)e*4+il)*kCoef*kQuad+q;
-			switch (il) {
-			case 0: PointCoefficients<0>(S, qd, prm, scratch, rc, out); break;
-			case 1: PointCoefficients<1>(S, qd, prm, scratch, rc, out); break;
-			case 2: PointCoefficients<2>(S, qd, prm, scratch, rc, out); break;
-			default: PointCoefficients<3>(S, qd, prm, scratch, rc, out); break;
-			}
-		} else {
-			switch (il) {
-			case 0: RowCoefficients<float, 1, false>(0, S, qd, prm, nullptr, rc); break;
-			case 1: RowCoefficients<float, 1, false>(1, S, qd, prm, nullptr, rc); break;
-			case 2: RowCoefficients<float, 1, false>(2, S, qd, prm, nullptr, rc); break;
-			default: RowCoefficients<float, 1, false>(3, S, qd, prm, nullptr, rc); break;
-			}
+		switch (il) {
+		case 0: PointCoefficients<0>(S, qd, prm, scratch, rc, out); break;
+		case 1: PointCoefficients<1>(S, qd, prm, scratch, rc, out); break;
+		case 2: PointCoefficients<2>(S, qd, prm, scratch, rc, out); break;
+		default: PointCoefficients<3>(S, qd, prm, scratch, rc, out); break;
 		}
 	}
-	if constexpr (!kResidual) return;
 	__syncthreads();
 
 	// 4. FP64 residual of the four row fields (rhs holds -r): thread (basis function a, quarter
@@ -633,28 +621,14 @@ void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const dou
 	const double* previous, AssemblyParams params, float* coef, double* rhs, cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
-	if (!coef && !rhs) Fail(-1, "tangent point kernel: nothing to compute");
 	static bool configured = false;
 	if (!configured) {
-		CudaCheck(cudaFuncSetAttribute(TangentPointKernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
-		CudaCheck(cudaFuncSetAttribute(TangentPointKernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
-		CudaCheck(cudaFuncSetAttribute(TangentPointKernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		CudaCheck(cudaFuncSetAttribute(TangentPointKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
 		configured = true;
 	}
-	const unsigned grid = (unsigned)mesh.elements;
-	const size_t smem = kPtSmemBytes+16;
-	if (coef && rhs)
-		TangentPointKernel<true, true><<<grid, kTcThreads, smem, stream>>>(mesh, phi, qdata, state, previous, params,
-			coef, rhs);
-	else if (coef)
-		TangentPointKernel<true, false><<<grid, kTcThreads, smem, stream>>>(mesh, phi, qdata, state, previous,
-			params, coef, nullptr);
-	else
-		TangentPointKernel<false, true><<<grid, kTcThreads, smem, stream>>>(mesh, phi, qdata, state, previous,
-			params, nullptr, rhs);
+	TangentPointKernel<<<(unsigned)mesh.elements, kTcThreads, kPtSmemBytes+16, stream>>>(mesh, phi, qdata, state,
+		previous, params, coef, rhs);
 	LaunchCheck("TangentPointKernel");
 }
 
