@@ -92,6 +92,9 @@ constexpr int kPtOffQS = kPtOffPart+kPtPartBytes;                 // double [64]
 constexpr int kPtOffRC = kPtOffQS+kQuad*kQS*8;                    // double [4][64][kRcStride]
 constexpr int kPtSmemBytes = kPtOffRC+4*kQuad*kRcStride*8;
 static_assert(kTcThreads*kScratchStride*4 <= kPtPartBytes, "coefficient scratch fits in the partial sums");
+constexpr int kStageBasis = 16;                  // basis functions per staged chunk of the point-state stage
+constexpr int kStageStride = kStageBasis+1;      // odd double stride of a staged (feature, point) row
+static_assert(kFeatures*kQuad*kStageStride*8 <= kPtPartBytes, "staged basis chunk fits in the partial sums");
 
 // Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B BF16, both
 // K-major, M = 128, N = 64.
@@ -330,25 +333,32 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 	}
 	__syncthreads();
 
-	// 2. State at every point (FP64): thread (point q, quarter aq of the basis)
-	//    sums 16 functions; the four quarters meet in shared memory.
+	// 2. State at every point (FP64): the basis tables are staged 16 functions at a time in shared
+	//    memory with coalesced 16-byte loads (rows of 17 doubles, so that 8-byte reads across the
+	//    points of a warp are conflict-free); thread (point q, quarter aq) takes 4 functions of each
+	//    chunk; the four quarters meet in shared memory.  The staging buffer overlays the partial
+	//    sums, which are written only after the last chunk has been read.
 	{
+		double* Stage = Part;
 		const int q = tid & 63, aq = tid >> 6;
 		double v[22];
 		#pragma unroll
 		for (int k = 0; k < 22; ++k) v[k] = 0.0;
-		#pragma unroll 2
-		for (int j = 0; j < 16; j += 2) {
-			const int a = aq*16+j;
-			double2 ph[5];
+		for (int a0 = 0; a0 < kMaxBasis; a0 += kStageBasis) {
+			if (a0) __syncthreads();                 // the previous chunk has been read
+			for (int idx = tid; idx < kFeatures*kQuad*(kStageBasis/2); idx += kTcThreads) {
+				const int row = idx/(kStageBasis/2), k = idx%(kStageBasis/2);     // row = t*64 + point
+				const double2 w = *reinterpret_cast<const double2*>(P+(size_t)row*kMaxBasis+a0+2*k);
+				Stage[row*kStageStride+2*k] = w.x;
+				Stage[row*kStageStride+2*k+1] = w.y;
+			}
+			__syncthreads();
 			#pragma unroll
-			for (int t = 0; t < 5; ++t) ph[t] = *reinterpret_cast<const double2*>(P+(t*kQuad+q)*kMaxBasis+a);
-			#pragma unroll
-			for (int h2 = 0; h2 < 2; ++h2) {
-				const double n = h2 ? ph[0].y : ph[0].x, g0 = h2 ? ph[1].y : ph[1].x;
-				const double g1 = h2 ? ph[2].y : ph[2].x, g2 = h2 ? ph[3].y : ph[3].x;
-				const double l = h2 ? ph[4].y : ph[4].x;
-				const int b = a+h2;
+			for (int jj = 0; jj < kStageBasis/4; ++jj) {
+				const int j = aq*(kStageBasis/4)+jj, b = a0+j;
+				const double n = Stage[(0*kQuad+q)*kStageStride+j], g0 = Stage[(1*kQuad+q)*kStageStride+j];
+				const double g1 = Stage[(2*kQuad+q)*kStageStride+j], g2 = Stage[(3*kQuad+q)*kStageStride+j];
+				const double l = Stage[(4*kQuad+q)*kStageStride+j];
 				const double uf[4] = {U[b], U[64+b], U[128+b], U[192+b]};
 				v[0] += n*uf[0]; v[1] += n*uf[1]; v[2] += n*uf[2]; v[3] += n*uf[3];
 				v[4] += n*Up[b]; v[5] += n*Up[64+b]; v[6] += n*Up[128+b];
@@ -357,6 +367,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 				v[19] += l*uf[0]; v[20] += l*uf[1]; v[21] += l*uf[2];
 			}
 		}
+		__syncthreads();                             // the last chunk has been read
 		double* part = Part+(aq*kQuad+q)*kPartStride;
 		#pragma unroll
 		for (int k = 0; k < 22; ++k) part[k] = v[k];
