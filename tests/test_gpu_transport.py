@@ -70,6 +70,35 @@ def test_transport_assembly_matches_oracle(setup):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32_krylov"])
+def test_transport_reference_tube_ragged(reference_tube):
+    """The reference-generated mesh (nen in {36, ..., 64}, its own labels and velocity file):
+    assembly against the oracle, one step against the direct solve."""
+    from tubularflowiga_b200 import api, ntiga
+    flat = ntiga.read(reference_tube / "tube-1.ntiga")
+    assert len(set(np.diff(flat.element_offsets))) >= 4
+    words = (reference_tube / "controlmesh.vtk").read_text().split()
+    first = words.index("LOOKUP_TABLE") + 2
+    labels = np.array([int(float(w)) for w in words[first:first + flat.nodes]], np.int32)
+    velocity = np.loadtxt(reference_tube / "initial_velocityfield.txt").reshape(-1, 3)
+    p = dict(PARAMS, dt=0.05, diffusion=1e-3)
+    params = api.transport_params(**p)
+    mask, n0, nplus = api.resolve_transport_boundaries(labels, velocity, params)
+    assert mask.sum() > 0
+    mesh = api.Mesh(flat)
+    t = api.Transport(mesh, params, velocity, mask, n0, nplus)
+    left, previous = t.matrices()
+    pattern = O.Pattern(flat.nodes, flat.element_offsets, flat.connectivity)
+    ol, op = O.transport_assemble(flat, pattern, velocity, p, mask)
+    for got, want in ((left, ol), (previous, op)):
+        assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
+    t.step(1)
+    c = O.transport_steps(pattern, ol, op, O.transport_initial(flat.nodes, mask, n0, nplus), mask, n0, nplus, 1)
+    got = t.get_state()
+    for f in (0, 1):
+        assert np.linalg.norm(got[f::2] - c[f::2]) <= 1e-6 * np.linalg.norm(c[f::2])
+    t.close()
+
+
 def test_transport_steps_match_direct_solve(setup, precision):
     """Both arithmetic modes stop on the FP64 true residual, so both meet the same bound."""
     api, tube, mesh, velocity, params, (mask, n0, nplus), pattern = setup
