@@ -69,7 +69,6 @@ def test_transport_assembly_matches_oracle(setup):
     t.close()
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32_krylov"])
 def test_transport_reference_tube_ragged(reference_tube):
     """The reference-generated mesh (nen in {36, ..., 64}, its own labels and velocity file):
     assembly against the oracle, one step against the direct solve."""
@@ -99,6 +98,7 @@ def test_transport_reference_tube_ragged(reference_tube):
     t.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32_krylov"])
 def test_transport_steps_match_direct_solve(setup, precision):
     """Both arithmetic modes stop on the FP64 true residual, so both meet the same bound."""
     api, tube, mesh, velocity, params, (mask, n0, nplus), pattern = setup
