@@ -210,6 +210,15 @@ const char* tfiga_version(void);
  * iga_cuda.cu:73-220): uploads the mesh, builds the block pattern and the
  * per-element basis tables on the device, and checks the geometry. */
 int tfiga_mesh_create(const tfiga_mesh_desc* desc, tfiga_mesh** out);
+/* Batched tubes: the disjoint union of `count` meshes as one mesh, solved by one
+ * tfiga_ns handle (the tubes' unknowns form independent diagonal blocks of one
+ * system; connectivity of tube k is offset by the nodes of tubes 0..k-1, the
+ * geometry is used as given).  node_offsets / element_offsets [count+1] (either
+ * may be NULL) receive where each tube's nodes and elements start; they are
+ * filled before the device mesh is built.  No counterpart in the reference
+ * (its C5-like runs solve one tube per process). */
+int tfiga_batch_mesh_create(const tfiga_mesh_desc* tubes, int32_t count, tfiga_mesh** out, int64_t* node_offsets,
+	int64_t* element_offsets);
 /* Same from a packed .ntiga file (iga::Database, IgaDatabase.hpp:95-161). */
 int tfiga_mesh_load_ntiga(const char* path, tfiga_mesh** out);
 int tfiga_mesh_destroy(tfiga_mesh* mesh);

@@ -66,3 +66,26 @@ def test_no_cpu_fallback_without_device(library):
         api.Mesh(tube.mesh)
     assert err.value.status == -2 and "no CPU fallback" in str(err.value)
     assert np.all(np.isfinite(tube.mesh.bezier_points))
+
+
+def test_batch_mesh_offsets_before_device(library):
+    """tfiga_batch_mesh_create builds the union (and its offsets) on the host before it needs the
+    device; without one it reports TFIGA_E_CUDA."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    from tubularflowiga_b200 import api, meshgen
+    tubes = [meshgen.straight_tube(1e-3, 2e-3, 4, 1, k) for k in (1, 2, 3)]
+    meshes = [t.mesh.contiguous() for t in tubes]
+    descs = (api.MeshDesc * 3)(*[api.MeshDesc(m.nodes, m.elements, api._p(m.element_offsets),
+                                              api._p(m.connectivity), api._p(m.extraction_offsets),
+                                              api._p(m.extraction_columns), api._p(m.extraction_values),
+                                              api._p(m.bezier_points), api._p(m.boundary_labels)) for m in meshes])
+    nodes = np.full(4, -1, np.int64)
+    elements = np.full(4, -1, np.int64)
+    h = ctypes.c_void_p()
+    status = library.tfiga_batch_mesh_create(descs, 3, ctypes.byref(h), api._p(nodes), api._p(elements))
+    assert status == -2 and "no CPU fallback" in api.last_error()
+    assert list(nodes) == [0] + list(np.cumsum([m.nodes for m in meshes]))
+    assert list(elements) == [0] + list(np.cumsum([m.elements for m in meshes]))
+    assert library.tfiga_batch_mesh_create(descs, 0, ctypes.byref(h), None, None) == -1

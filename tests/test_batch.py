@@ -51,3 +51,20 @@ def test_union_solve_matches_individual_tubes():
         part = union[batch.node_offset[k]:batch.node_offset[k + 1]]
         assert np.linalg.norm(part[:, :3] - ref[:, :3]) <= 1e-8 * np.linalg.norm(ref[:, :3])
         assert np.linalg.norm(part[:, 3] - ref[:, 3]) <= 1e-6 * max(np.linalg.norm(ref[:, 3]), 1e-300)
+
+
+@pytest.mark.gpu
+def test_batch_mesh_through_the_c_abi_matches_the_union():
+    """tfiga_batch_mesh_create gives the same mesh as the generator's disjoint union (pattern, sizes,
+    geometry check) and the tube offsets."""
+    from tubularflowiga_b200 import api, meshgen
+    tubes = [meshgen.straight_tube(1e-3, 3e-3, 4, 1, k) for k in (2, 3)]
+    union = meshgen.combine_tubes(tubes, [1.0, 1.0])
+    a = api.Mesh([t.mesh for t in tubes])
+    b = api.Mesh(union.mesh)
+    assert list(a.node_offsets) == list(union.node_offset) and list(a.element_offsets) == list(union.element_offset)
+    for key in ("nodes", "elements", "basis_entries", "extraction_nonzeros", "block_nonzeros", "bad_samples"):
+        assert a.info[key] == b.info[key], key
+    assert abs(a.info["min_detj"] - b.info["min_detj"]) <= 1e-12 * abs(b.info["min_detj"])
+    for x, y in zip(a.pattern(), b.pattern()):
+        assert np.array_equal(x, y)

@@ -137,6 +137,8 @@ SIGNATURES = {
     "tfiga_version": (C.c_char_p, []),
     "tfiga_mesh_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(C.c_void_p)]),
     "tfiga_mesh_load_ntiga": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "tfiga_batch_mesh_create": (C.c_int, [C.POINTER(MeshDesc), C.c_int32, C.POINTER(C.c_void_p), C.c_void_p,
+                                          C.c_void_p]),
     "tfiga_mesh_destroy": (C.c_int, [C.c_void_p]),
     "tfiga_mesh_info_get": (C.c_int, [C.c_void_p, C.POINTER(MeshInfo)]),
     "tfiga_mesh_pattern": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -258,10 +260,23 @@ class Mesh:
     """Device-resident mesh (tfiga_mesh)."""
 
     def __init__(self, source):
+        """source: a .ntiga path, a FlatMesh, or a list of FlatMesh (batched tubes: their disjoint union,
+        with self.node_offsets / self.element_offsets marking where each tube starts)."""
         L = lib()
         self._h = C.c_void_p()
         if isinstance(source, (str, Path)):
             check(L.tfiga_mesh_load_ntiga(str(source).encode(), C.byref(self._h)))
+        elif isinstance(source, (list, tuple)):
+            meshes = [m.contiguous() for m in source]
+            self._keep = meshes
+            descs = (MeshDesc * len(meshes))(*[
+                MeshDesc(m.nodes, m.elements, _p(m.element_offsets), _p(m.connectivity), _p(m.extraction_offsets),
+                         _p(m.extraction_columns), _p(m.extraction_values), _p(m.bezier_points),
+                         _p(m.boundary_labels)) for m in meshes])
+            self.node_offsets = np.zeros(len(meshes) + 1, np.int64)
+            self.element_offsets = np.zeros(len(meshes) + 1, np.int64)
+            check(L.tfiga_batch_mesh_create(descs, len(meshes), C.byref(self._h), _p(self.node_offsets),
+                                            _p(self.element_offsets)))
         else:
             m: FlatMesh = source.contiguous()
             self._keep = m

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <array>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <fstream>
@@ -128,6 +129,45 @@ int tfiga_mesh_create(const tfiga_mesh_desc* desc, tfiga_mesh** out)
 		*out = nullptr;
 		auto handle = std::make_unique<tfiga_mesh>();
 		handle->mesh = std::make_unique<tfiga::Mesh>(FromDesc(desc));
+		*out = handle.release();
+	});
+}
+
+int tfiga_batch_mesh_create(const tfiga_mesh_desc* tubes, int32_t count, tfiga_mesh** out, int64_t* node_offsets,
+	int64_t* element_offsets)
+{
+	return Guard([&] {
+		Require(out != nullptr && tubes != nullptr && count > 0, "batch needs tubes and an out handle");
+		*out = nullptr;
+		tfiga::HostMesh all;
+		int64_t nodes = 0, elements = 0;
+		if (node_offsets) node_offsets[0] = 0;
+		if (element_offsets) element_offsets[0] = 0;
+		for (int32_t k = 0; k < count; ++k) {
+			const tfiga::HostMesh m = FromDesc(tubes+k);
+			const int32_t entry0 = all.element_offsets.back();
+			const int32_t nnz0 = all.extraction_offsets.back();
+			Require(nodes+m.nodes < INT32_MAX && (int64_t)entry0+(int64_t)m.connectivity.size() < INT32_MAX
+				&& (int64_t)nnz0+(int64_t)m.extraction_values.size() < INT32_MAX, "batch exceeds 32-bit indices");
+			for (int64_t e = 1; e <= m.elements(); ++e) all.element_offsets.push_back(entry0+m.element_offsets[e]);
+			for (const int32_t node : m.connectivity) all.connectivity.push_back((int32_t)(node+nodes));
+			for (size_t i = 1; i < m.extraction_offsets.size(); ++i)
+				all.extraction_offsets.push_back(nnz0+m.extraction_offsets[i]);
+			all.extraction_columns.insert(all.extraction_columns.end(), m.extraction_columns.begin(),
+				m.extraction_columns.end());
+			all.extraction_values.insert(all.extraction_values.end(), m.extraction_values.begin(),
+				m.extraction_values.end());
+			all.bezier_points.insert(all.bezier_points.end(), m.bezier_points.begin(), m.bezier_points.end());
+			all.boundary_labels.insert(all.boundary_labels.end(), m.boundary_labels.begin(), m.boundary_labels.end());
+			all.max_basis = std::max(all.max_basis, m.max_basis);
+			nodes += m.nodes;
+			elements += m.elements();
+			if (node_offsets) node_offsets[k+1] = nodes;
+			if (element_offsets) element_offsets[k+1] = elements;
+		}
+		all.nodes = nodes;
+		auto handle = std::make_unique<tfiga_mesh>();
+		handle->mesh = std::make_unique<tfiga::Mesh>(std::move(all));
 		*out = handle.release();
 	});
 }
