@@ -405,21 +405,50 @@ int NavierStokes(int argc, char** argv)
 	const auto labeled = ReadLabeledHexMesh((case_dir/"controlmesh.vtk").string(), host.nodes, host.elements());
 	const auto wall = WallTraceBasis(host, labeled);
 	const auto reference_velocity = ReadVelocity((case_dir/"initial_velocityfield.txt").string(), host.nodes);
-	if (!fs::exists(case_dir/"simulation_config.json"))
-		Fail(-7, "legacy simulation_parameter.txt / case_config.json cases are not supported; "
-			"provide simulation_config.json");
-	const SimulationConfig config = ReadSimulationConfig((case_dir/"simulation_config.json").string());
-	const FlowSystem& flow = FindNavierStokesSystem(config, options.system);
-	const bool transient = flow.time_integration == "backward_euler";
-	const double viscosity = flow.viscosity, density = flow.density;
-	const double dt = transient ? config.dt : 0.0;
-	const int physical_steps = transient ? config.steps : 1;
-	std::vector<OutletModel> outlets = InitializeOutletModels(config, flow);
+	// simulation_config.json, or a legacy case: simulation_parameter.txt (+ case_config.json) with the
+	// reference's legacy flow defaults, steady, viscosity 0.1, density 1, Dirichlet pressure on the
+	// outlet labels (iga_cuda.cu:761-795).
+	const bool legacy = !fs::exists(case_dir/"simulation_config.json");
+	const SimulationConfig config = legacy ? SimulationConfig{}
+		: ReadSimulationConfig((case_dir/"simulation_config.json").string());
+	bool transient = false;
+	double viscosity = 0.1, density = 1.0, dt = 0.0;
+	int physical_steps = 1;
+	std::vector<OutletModel> outlets;
+	std::string boundary_source = "simulation_config.json";
+	ResolvedBoundaries legacy_boundaries;
+	if (!legacy) {
+		const FlowSystem& flow = FindNavierStokesSystem(config, options.system);
+		transient = flow.time_integration == "backward_euler";
+		viscosity = flow.viscosity;
+		density = flow.density;
+		dt = transient ? config.dt : 0.0;
+		physical_steps = transient ? config.steps : 1;
+		outlets = InitializeOutletModels(config, flow);
+	} else {
+		const TransportParameters parameters = ReadTransportParameters((case_dir/"simulation_parameter.txt").string());
+		const CaseConfiguration case_configuration = ReadCaseConfiguration((case_dir/"case_config.json").string());
+		const LegacyBoundaries lb = ResolveLegacyBoundaries(case_configuration, labeled.labels, reference_velocity,
+			parameters);
+		legacy_boundaries.velocity_mask = lb.velocity_mask;
+		legacy_boundaries.pressure_mask = lb.pressure_mask;
+		legacy_boundaries.velocity = lb.velocity;
+		legacy_boundaries.pressure = lb.pressure;
+		legacy_boundaries.velocity_nodes = lb.velocity_nodes;
+		legacy_boundaries.pressure_nodes = lb.pressure_nodes;
+		boundary_source = case_configuration.present ? "case_config.json" : "legacy-defaults";
+	}
 	auto resolve = [&](const SimulationConfig& step_config, std::map<int, double>& tractions) {
-		const auto boundary_config = MaterializeOutletPressures(step_config, outlets);
-		const auto& system = FindNavierStokesSystem(boundary_config, options.system);
-		tractions = ExtractPressureTractions(boundary_config, system);
-		auto r = ResolveFlowBoundaries(boundary_config, system, labeled.labels, reference_velocity);
+		ResolvedBoundaries r;
+		if (legacy) {
+			tractions.clear();
+			r = legacy_boundaries;
+		} else {
+			const auto boundary_config = MaterializeOutletPressures(step_config, outlets);
+			const auto& system = FindNavierStokesSystem(boundary_config, options.system);
+			tractions = ExtractPressureTractions(boundary_config, system);
+			r = ResolveFlowBoundaries(boundary_config, system, labeled.labels, reference_velocity);
+		}
 		for (const int32_t node : wall) {
 			if (!r.velocity_mask.at(node)) ++r.velocity_nodes;
 			r.velocity_mask[node] = 1;
@@ -434,7 +463,7 @@ int NavierStokes(int argc, char** argv)
 			if (m.kind != "resistance") Fail(-4, "RC/RCR outlets require backward_euler flow");
 	if (options.stop_after_step > physical_steps) Fail(-1, "--stop-after-step exceeds configured physical steps");
 	const int run_end = options.stop_after_step > 0 ? options.stop_after_step : physical_steps;
-	std::cout << "boundary_config=simulation_config.json viscosity=" << viscosity << " density=" << density
+	std::cout << "boundary_config=" << boundary_source << " viscosity=" << viscosity << " density=" << density
 		<< " time_integration=" << (transient ? "backward_euler" : "steady") << " dt=" << dt
 		<< " steps=" << physical_steps << " run_end_step=" << run_end
 		<< " velocity_nodes=" << boundaries.velocity_nodes << " pressure_nodes=" << boundaries.pressure_nodes << '\n';
