@@ -111,9 +111,9 @@ def test_learned_stage_training_and_iterations(cylinder_1280):
 
     The training (residual loss through the bound Jacobian) must lower the loss, the fitted output
     gain must be finite and non-negative, and a step with the stage attached must still converge to
-    the same FP64 Newton tolerance (FGMRES is the judge; a solve that fails with the stage is redone
+    the same FP64 Newton tolerance (FGMRES's true residual decides; a solve that fails with the stage is redone
     with the AMG alone).  The iteration counts of both runs are reported: on these tubes the stage
-    does not lower them (see the measurements beside the learned stage in the design notes)."""
+    does not lower them."""
     from tubularflowiga_b200 import api
     tube = cylinder_1280
     vmask, pmask, vel = api.tube_boundary_conditions(tube, 0.2)

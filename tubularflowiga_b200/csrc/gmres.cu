@@ -300,7 +300,7 @@ double OrthoBytes(long long n, int used, int basis_bytes)
 	return (double)n*(4.0*basis_bytes*0.5*used*(used+1.0)+(40.0+basis_bytes)*used);
 }
 
-// The survey's algorithmic bytes of the same steps: s_v n (2j + 7) per step with s_v the basis
+// The algorithmic bytes of the same steps: s_v n (2j + 7) per step with s_v the basis
 // entry size, plus 8 n for the stored FP64 preconditioned vector of FGMRES.
 double ArnoldiBytes(long long n, int used, int basis_bytes, bool flexible)
 {
