@@ -173,3 +173,14 @@ def test_pattern_and_oracle_gmres(small_tube):
     assert it > 0 and singular == 0
     assert np.linalg.norm(A @ x - rhs) <= 1e-7 * np.linalg.norm(rhs)
     assert np.allclose(O.spmv(P, values, x), A @ x, rtol=1e-13, atol=1e-20)
+
+
+def test_ntiga_writer_reproduces_the_reference_pack_byte_for_byte(reference_tube, tmp_path):
+    """The generator's .ntiga writer, given the content of the database the reference's own
+    iga_pack wrote (tests/golden/reference_tube, solvers/cpu/src/iga_pack.cpp:278-417), writes
+    the same bytes: header, ownership and rank indices, element records and their order."""
+    from tubularflowiga_b200 import ntiga
+    source = (reference_tube / "tube-1.ntiga").read_bytes()
+    mesh = ntiga.read(reference_tube / "tube-1.ntiga")
+    ntiga.write(tmp_path / "copy.ntiga", mesh)
+    assert (tmp_path / "copy.ntiga").read_bytes() == source

@@ -137,7 +137,8 @@ def read(path) -> FlatMesh:
 
 
 def write(path, mesh: FlatMesh) -> None:
-    """Write a single-rank v5 database (all elements owned by rank 0)."""
+    """Write a single-rank v5 database (all elements owned by rank 0); element ids and types are
+    kept when the mesh carries them (a database read by `read`)."""
     E = mesh.elements
     rec_dtype = np.dtype([("c", "u1"), ("v", "<f8")])
     head = bytearray()
@@ -155,7 +156,9 @@ def write(path, mesh: FlatMesh) -> None:
         offsets[e] = pos
         b, t = int(mesh.element_offsets[e]), int(mesh.element_offsets[e + 1])
         nen = t - b
-        parts = [struct.pack("<QiiI", e, 0, 0, nen),
+        eid = int(mesh.ids[e]) if mesh.ids is not None else e
+        typ = int(mesh.types[e]) if mesh.types is not None else 0
+        parts = [struct.pack("<QiiI", eid, typ, 0, nen),
                  np.asarray(mesh.boundary_labels[6 * e:6 * e + 6], "<i4").tobytes(),
                  np.asarray(mesh.connectivity[b:t], "<i4").tobytes()]
         for a in range(nen):
