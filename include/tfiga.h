@@ -448,6 +448,13 @@ int tfiga_transport_read_params(const char* path, tfiga_transport_params* params
 int tfiga_transport_resolve_boundaries(int64_t nodes, const int32_t* labels, const double* reference_velocity,
 	const tfiga_transport_params* params, const char* case_config_path, int32_t* constrained, double* n0,
 	double* nplus, int64_t* transport_nodes);
+/* The whole resolution of a legacy case (ResolveBoundaryConditions, CaseInput.hpp:162-258), as the
+ * navier-stokes command uses it without simulation_config.json: velocity mask and values [nodes],
+ * [3*nodes], pressure mask and values, transport mask and values [nodes] (any output may be NULL);
+ * counts[3] = velocity, pressure and transport nodes (may be NULL).  Host only. */
+int tfiga_resolve_legacy_boundaries(int64_t nodes, const int32_t* labels, const double* reference_velocity,
+	const tfiga_transport_params* params, const char* case_config_path, int32_t* velocity_mask, double* velocity,
+	int32_t* pressure_mask, double* pressure, int32_t* transport_mask, double* n0, double* nplus, int64_t* counts);
 /* Assembles L and P from the nodal velocity [3*nodes], applies the boundary
  * rows of the constrained[nodes] mask and sets the boundary values n0/nplus
  * [nodes] into the zero initial state (iga_cuda.cu:664-679).  Host or device

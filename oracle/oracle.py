@@ -101,6 +101,9 @@ def ref():
                                    C.c_double, C.c_double, C.c_double, C.c_void_p, _dp]
         R.ref_max_threads.restype = C.c_int
         R.ref_transport_element.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
+        R.ref_resolve_boundaries.argtypes = [C.c_longlong, _ip, _dp, C.c_double, C.c_double, C.c_double, C.c_char_p,
+                                             _ip, _ip, _ip, _dp, _dp, _dp, _dp,
+                                             np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
     return _ref
 
 
@@ -348,6 +351,22 @@ def transport_assemble(mesh, pattern, velocity, params, constrained=None):
     if st:
         raise RuntimeError(f"oracle transport assembly failed at element {failed.value} ({st})")
     return left, previous
+
+
+def ref_resolve_boundaries(labels, velocity, vplus, n0_bc, nplus_bc, case_config_text=None):
+    """The reference's own ResolveBoundaryConditions (+ ParseCaseConfiguration) on the given inputs."""
+    labels = np.ascontiguousarray(labels, np.int32)
+    n = labels.size
+    out = {"velocity_mask": np.zeros(n, np.int32), "pressure_mask": np.zeros(n, np.int32),
+           "transport_mask": np.zeros(n, np.int32), "velocity": np.zeros(3 * n), "pressure": np.zeros(n),
+           "n0": np.zeros(n), "nplus": np.zeros(n), "counts": np.zeros(3, np.int64)}
+    st = ref().ref_resolve_boundaries(n, labels, np.ascontiguousarray(velocity, np.float64).ravel(), vplus, n0_bc,
+                                      nplus_bc, None if case_config_text is None else case_config_text.encode(),
+                                      out["velocity_mask"], out["pressure_mask"], out["transport_mask"],
+                                      out["velocity"], out["pressure"], out["n0"], out["nplus"], out["counts"])
+    if st:
+        raise RuntimeError(ref().ref_last_error().decode())
+    return out
 
 
 def transport_scipy(pattern, values):

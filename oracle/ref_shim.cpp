@@ -13,6 +13,8 @@
 //   iga::Database::Load                solvers/cpu/include/IgaDatabase.hpp:124-161
 //   iga::WallTraceBasis                solvers/cpu/include/BoundarySupport.hpp:134-150
 //   iga::BuildTransportElement         solvers/cpu/include/TransportElement.hpp:213-260
+//   iga::ParseCaseConfiguration        include/CaseConfig.hpp:340-371
+//   iga::ResolveBoundaryConditions     solvers/cpu/include/CaseInput.hpp:162-258
 #include "BoundaryFlow.hpp"
 #include "BoundarySupport.hpp"
 #include "NavierStokesElement.hpp"
@@ -297,6 +299,45 @@ int ref_assemble(int first, int last, const int* element_offsets, const int* con
 }
 
 int ref_max_threads() { return omp_get_max_threads(); }
+
+// Boundary resolution of a legacy case: labels[nodes], reference velocity [3 nodes], the transport
+// parameters it reads (vplus, N0bc, Nplusbc) and case_config.json text (NULL: absent).  Outputs
+// [nodes] (velocity [3 nodes]); counts[3] = velocity, pressure, transport nodes.
+int ref_resolve_boundaries(long long nodes, const int* labels, const double* velocity, double vplus, double n0_bc,
+	double nplus_bc, const char* case_config, int* velocity_mask, int* pressure_mask, int* transport_mask,
+	double* velocity_out, double* pressure, double* n0, double* nplus, long long* counts)
+{
+	try {
+		std::vector<int> label(labels, labels+nodes);
+		std::vector<std::array<double, 3>> reference(static_cast<std::size_t>(nodes));
+		for (long long i = 0; i < nodes; ++i)
+			for (int d = 0; d < 3; ++d) reference[static_cast<std::size_t>(i)][static_cast<std::size_t>(d)] = velocity[3*i+d];
+		iga::TransportParameters parameters;
+		parameters.vplus = vplus;
+		parameters.n0_bc = n0_bc;
+		parameters.nplus_bc = nplus_bc;
+		const iga::CaseConfiguration configuration = case_config ? iga::ParseCaseConfiguration(case_config)
+			: iga::CaseConfiguration{};
+		const auto r = iga::ResolveBoundaryConditions(configuration, label, reference, parameters);
+		for (long long i = 0; i < nodes; ++i) {
+			const auto k = static_cast<std::size_t>(i);
+			velocity_mask[i] = r.velocity_constrained[k];
+			pressure_mask[i] = r.pressure_constrained[k];
+			transport_mask[i] = r.transport_constrained[k];
+			for (int d = 0; d < 3; ++d) velocity_out[3*i+d] = r.velocity[k][static_cast<std::size_t>(d)];
+			pressure[i] = r.pressure[k];
+			n0[i] = r.n0[k];
+			nplus[i] = r.nplus[k];
+		}
+		counts[0] = static_cast<long long>(r.velocity_nodes);
+		counts[1] = static_cast<long long>(r.pressure_nodes);
+		counts[2] = static_cast<long long>(r.transport_nodes);
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
 
 // Two-species transport element (left and previous matrices, dense (2 nen)^2).
 // p: D, vplus, kplus, kminus, k'plus, dt, artificial_diffusion.

@@ -201,3 +201,44 @@ def test_transport_oracle_gmres_matches_direct_solve(small_tube):
     assert iterations > 0
     for f in (0, 1):
         assert np.linalg.norm(x[f::2] - want[f::2]) <= 1e-6 * np.linalg.norm(want[f::2])
+
+
+@requires_ref
+def test_legacy_boundaries_match_the_reference_resolver(api, tmp_path, small_tube):
+    """Every mask and value of a legacy case against the reference's own ParseCaseConfiguration +
+    ResolveBoundaryConditions (compiled unmodified into oracle/_ref), for the legacy defaults and a
+    set of case_config.json rule sets, including the ones the reference rejects (same message)."""
+    t = small_tube
+    rng = np.random.default_rng(5)
+    velocity = rng.normal(size=(t.mesh.nodes, 3))
+    p = api.transport_params(vplus=0.7, n0_bc=1.25, nplus_bc=0.375)
+    configs = [None,
+               {"boundaries": {"conditions": [{"label": 1, "type": "inlet", "transport": {"N0": 2.0, "Nplus": 0.5}}]}},
+               {"boundaries": {"conditions": [{"label": 1, "type": "inlet", "velocity_scale": 3.0}]}},
+               {"boundaries": {"conditions": [{"label": 1, "type": "inlet", "velocity": [0.1, 0.2, 0.3]},
+                                              {"label": 0, "type": "wall", "velocity": [0.0, 0.0, 0.05]},
+                                              {"label": 2, "type": "outlet", "pressure": 7.5}]}},
+               {"schema_version": 1, "boundaries": {"inherit_legacy": False, "conditions": [
+                   {"label": 0, "type": "wall"}, {"label": 1, "type": "inlet"}, {"label": 2, "type": "outlet"}]}},
+               {"boundaries": {"conditions": [{"label": 2, "type": "interior"}]}},
+               {"boundaries": {"inherit_legacy": False, "conditions": [{"label": 1, "type": "inlet"}]}},
+               {"boundaries": {"conditions": [{"label": 9, "type": "wall"}]}},
+               {"boundaries": {"conditions": [{"label": 1, "type": "inlet", "velocity": [1, 2, 3],
+                                               "velocity_scale": 2.0}]}}]
+    keys = ("velocity_mask", "velocity", "pressure_mask", "pressure", "transport_mask", "n0", "nplus", "counts")
+    for cfg in configs:
+        path = None
+        if cfg is not None:
+            path = tmp_path / "case_config.json"
+            path.write_text(json.dumps(cfg))
+        try:
+            want = O.ref_resolve_boundaries(t.labels, velocity, 0.7, 1.25, 0.375,
+                                            None if cfg is None else json.dumps(cfg))
+        except RuntimeError as ref_error:
+            with pytest.raises(api.TfigaError) as err:
+                api.resolve_legacy_boundaries(t.labels, velocity, p, path)
+            assert str(ref_error) in str(err.value), (cfg, str(ref_error), str(err.value))
+            continue
+        got = api.resolve_legacy_boundaries(t.labels, velocity, p, path)
+        for k in keys:
+            assert np.array_equal(got[k], want[k]), (cfg, k)

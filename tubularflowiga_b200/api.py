@@ -200,6 +200,8 @@ SIGNATURES = {
     "tfiga_transport_resolve_boundaries": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(TransportParams),
                                                      C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                      C.POINTER(C.c_int64)]),
+    "tfiga_resolve_legacy_boundaries": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(TransportParams),
+                                                  C.c_char_p] + [C.c_void_p] * 8),
     "tfiga_transport_create": (C.c_int, [C.c_void_p, C.POINTER(TransportParams), C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     "tfiga_transport_destroy": (C.c_int, [C.c_void_p]),
@@ -602,6 +604,22 @@ def resolve_transport_boundaries(labels, reference_velocity, params: TransportPa
     check(lib().tfiga_transport_resolve_boundaries(n, _p(labels), _p(vel), C.byref(params), path, _p(mask),
                                                    _p(n0), _p(nplus), C.byref(count)))
     return mask, n0, nplus
+
+
+def resolve_legacy_boundaries(labels, reference_velocity, params: TransportParams, case_config=None) -> dict:
+    """Every mask and value of a legacy case (ResolveBoundaryConditions): velocity, pressure, transport."""
+    labels = np.ascontiguousarray(labels, np.int32)
+    vel = np.ascontiguousarray(reference_velocity, np.float64).reshape(-1)
+    n = labels.size
+    out = {"velocity_mask": np.zeros(n, np.int32), "velocity": np.zeros(3 * n), "pressure_mask": np.zeros(n, np.int32),
+           "pressure": np.zeros(n), "transport_mask": np.zeros(n, np.int32), "n0": np.zeros(n),
+           "nplus": np.zeros(n), "counts": np.zeros(3, np.int64)}
+    path = None if case_config is None else str(case_config).encode()
+    check(lib().tfiga_resolve_legacy_boundaries(n, _p(labels), _p(vel), C.byref(params), path,
+                                                *[_p(out[k]) for k in ("velocity_mask", "velocity", "pressure_mask",
+                                                                       "pressure", "transport_mask", "n0", "nplus",
+                                                                       "counts")]))
+    return out
 
 
 class Transport:

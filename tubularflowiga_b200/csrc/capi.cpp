@@ -509,9 +509,9 @@ int tfiga_transport_read_params(const char* path, tfiga_transport_params* params
 	});
 }
 
-int tfiga_transport_resolve_boundaries(int64_t nodes, const int32_t* labels, const double* reference_velocity,
-	const tfiga_transport_params* params, const char* case_config_path, int32_t* constrained, double* n0,
-	double* nplus, int64_t* transport_nodes)
+int tfiga_resolve_legacy_boundaries(int64_t nodes, const int32_t* labels, const double* reference_velocity,
+	const tfiga_transport_params* params, const char* case_config_path, int32_t* velocity_mask, double* velocity,
+	int32_t* pressure_mask, double* pressure, int32_t* transport_mask, double* n0, double* nplus, int64_t* counts)
 {
 	return Guard([&] {
 		Require(nodes > 0 && labels && reference_velocity && params, "null argument");
@@ -520,17 +520,36 @@ int tfiga_transport_resolve_boundaries(int64_t nodes, const int32_t* labels, con
 		p.n0_bc = params->n0_bc;
 		p.nplus_bc = params->nplus_bc;
 		std::vector<int> label(labels, labels+nodes);
-		std::vector<std::array<double, 3>> velocity((size_t)nodes);
+		std::vector<std::array<double, 3>> reference((size_t)nodes);
 		for (int64_t i = 0; i < nodes; ++i)
-			for (int d = 0; d < 3; ++d) velocity[(size_t)i][d] = reference_velocity[3*i+d];
+			for (int d = 0; d < 3; ++d) reference[(size_t)i][d] = reference_velocity[3*i+d];
 		const tfiga::CaseConfiguration configuration = case_config_path
 			? tfiga::ReadCaseConfiguration(case_config_path) : tfiga::CaseConfiguration{};
-		const auto r = tfiga::ResolveLegacyBoundaries(configuration, label, velocity, p);
-		if (constrained) std::copy(r.transport_mask.begin(), r.transport_mask.end(), constrained);
+		const auto r = tfiga::ResolveLegacyBoundaries(configuration, label, reference, p);
+		if (velocity_mask) std::copy(r.velocity_mask.begin(), r.velocity_mask.end(), velocity_mask);
+		if (velocity) std::copy(r.velocity.begin(), r.velocity.end(), velocity);
+		if (pressure_mask) std::copy(r.pressure_mask.begin(), r.pressure_mask.end(), pressure_mask);
+		if (pressure) std::copy(r.pressure.begin(), r.pressure.end(), pressure);
+		if (transport_mask) std::copy(r.transport_mask.begin(), r.transport_mask.end(), transport_mask);
 		if (n0) std::copy(r.n0.begin(), r.n0.end(), n0);
 		if (nplus) std::copy(r.nplus.begin(), r.nplus.end(), nplus);
-		if (transport_nodes) *transport_nodes = (int64_t)r.transport_nodes;
+		if (counts) {
+			counts[0] = (int64_t)r.velocity_nodes;
+			counts[1] = (int64_t)r.pressure_nodes;
+			counts[2] = (int64_t)r.transport_nodes;
+		}
 	});
+}
+
+int tfiga_transport_resolve_boundaries(int64_t nodes, const int32_t* labels, const double* reference_velocity,
+	const tfiga_transport_params* params, const char* case_config_path, int32_t* constrained, double* n0,
+	double* nplus, int64_t* transport_nodes)
+{
+	int64_t counts[3] = {0, 0, 0};
+	const int status = tfiga_resolve_legacy_boundaries(nodes, labels, reference_velocity, params, case_config_path,
+		nullptr, nullptr, nullptr, nullptr, constrained, n0, nplus, counts);
+	if (status == TFIGA_OK && transport_nodes) *transport_nodes = counts[2];
+	return status;
 }
 
 int tfiga_transport_create(tfiga_mesh* mesh, const tfiga_transport_params* params, const double* velocity,
