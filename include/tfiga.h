@@ -378,6 +378,21 @@ int tfiga_learned_loss_gradient_device(tfiga_learned* learned, const double* x_d
 int tfiga_learned_save(const tfiga_learned* learned, const char* path);
 int tfiga_learned_load(tfiga_learned* learned, const char* path);
 
+/* ---- case inputs (host only) ------------------------------------------ */
+/* The flow boundary set-up of the navier-stokes command for a simulation_config.json case at
+ * physical time `time` with the outlet models at their initial state (iga_cuda.cu:766-790:
+ * ReadSimulationConfiguration, FindNavierStokesSystem, InitializeOutletModels,
+ * MaterializeBoundaryWaveforms, MaterializeOutletPressures, ExtractPressureTractions,
+ * ResolveFlowBoundaries), before the wall trace.  system may be NULL or "" (the first
+ * Navier-Stokes system).  Outputs [nodes] ([3*nodes] for velocity; any may be NULL);
+ * counts[2] = velocity, pressure nodes; traction_labels / traction_values receive up to
+ * *traction_count entries (in: capacity, out: the number of labelled pressure tractions);
+ * physics[5] = viscosity, density, dt, steps, transient (1 or 0). */
+int tfiga_resolve_flow_boundaries(const char* config_path, const char* system, double time, int64_t nodes,
+	const int32_t* labels, const double* reference_velocity, int32_t* velocity_mask, double* velocity,
+	int32_t* pressure_mask, double* pressure, int64_t* counts, int32_t* traction_labels, double* traction_values,
+	int32_t* traction_count, double* physics);
+
 /* ---- two-species transport ------------------------------------------ */
 /* The `iga_cuda transport` path (Transport, solvers/cuda/src/iga_cuda.cu:621-732):
  * N0 (attached: diffusion and exchange) and N+ (advected by a prescribed nodal

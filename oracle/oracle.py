@@ -101,6 +101,9 @@ def ref():
                                    C.c_double, C.c_double, C.c_double, C.c_void_p, _dp]
         R.ref_max_threads.restype = C.c_int
         R.ref_transport_element.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
+        R.ref_flow_boundaries.argtypes = [C.c_char_p, C.c_char_p, C.c_double, C.c_longlong, _ip, _dp, _ip, _dp, _ip,
+                                          _dp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS"), _ip,
+                                          _dp, C.POINTER(C.c_int), _dp]
         R.ref_resolve_boundaries.argtypes = [C.c_longlong, _ip, _dp, C.c_double, C.c_double, C.c_double, C.c_char_p,
                                              _ip, _ip, _ip, _dp, _dp, _dp, _dp,
                                              np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
@@ -351,6 +354,25 @@ def transport_assemble(mesh, pattern, velocity, params, constrained=None):
     if st:
         raise RuntimeError(f"oracle transport assembly failed at element {failed.value} ({st})")
     return left, previous
+
+
+def ref_flow_boundaries(config_path, labels, velocity, time=0.0, system=""):
+    """The reference's own flow boundary set-up (iga_cuda.cu:766-790) of a simulation_config.json case."""
+    labels = np.ascontiguousarray(labels, np.int32)
+    n = labels.size
+    out = {"velocity_mask": np.zeros(n, np.int32), "velocity": np.zeros(3 * n), "pressure_mask": np.zeros(n, np.int32),
+           "pressure": np.zeros(n), "counts": np.zeros(2, np.int64)}
+    tl, tv, count = np.zeros(64, np.int32), np.zeros(64), C.c_int(64)
+    physics = np.zeros(5)
+    st = ref().ref_flow_boundaries(str(config_path).encode(), system.encode(), time, n, labels,
+                                   np.ascontiguousarray(velocity, np.float64).ravel(), out["velocity_mask"],
+                                   out["velocity"], out["pressure_mask"], out["pressure"], out["counts"], tl, tv,
+                                   C.byref(count), physics)
+    if st:
+        raise RuntimeError(ref().ref_last_error().decode())
+    out["tractions"] = {int(tl[i]): float(tv[i]) for i in range(min(count.value, 64))}
+    out["physics"] = physics
+    return out
 
 
 def ref_resolve_boundaries(labels, velocity, vplus, n0_bc, nplus_bc, case_config_text=None):

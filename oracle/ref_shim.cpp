@@ -14,11 +14,18 @@
 //   iga::WallTraceBasis                solvers/cpu/include/BoundarySupport.hpp:134-150
 //   iga::BuildTransportElement         solvers/cpu/include/TransportElement.hpp:213-260
 //   iga::ParseCaseConfiguration        include/CaseConfig.hpp:340-371
+//   the flow boundary set-up of NavierStokes (solvers/cuda/src/iga_cuda.cu:766-790):
+//   ReadSimulationConfiguration, FindNavierStokesSystem, InitializeOutletModels,
+//   MaterializeBoundaryWaveforms, MaterializeOutletPressures, ExtractPressureTractions,
+//   ResolveFlowBoundaries
 //   iga::ResolveBoundaryConditions     solvers/cpu/include/CaseInput.hpp:162-258
 #include "BoundaryFlow.hpp"
 #include "BoundarySupport.hpp"
+#include "GenericCaseInput.hpp"
 #include "NavierStokesElement.hpp"
 #include "OutletModel.hpp"
+#include "PressureTraction.hpp"
+#include "TemporalFunction.hpp"
 
 #include <omp.h>
 
@@ -26,6 +33,7 @@
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <filesystem>
 #include <string>
 #include <vector>
 
@@ -332,6 +340,56 @@ int ref_resolve_boundaries(long long nodes, const int* labels, const double* vel
 		counts[0] = static_cast<long long>(r.velocity_nodes);
 		counts[1] = static_cast<long long>(r.pressure_nodes);
 		counts[2] = static_cast<long long>(r.transport_nodes);
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+// Flow boundary conditions of a simulation_config.json case at physical time t, outlet models at
+// their initial state.  physics[5] = viscosity, density, dt, steps, transient; counts[2] = velocity,
+// pressure nodes; tractions: labels / values up to *traction_count entries (in: capacity, out: count).
+int ref_flow_boundaries(const char* config_path, const char* system, double time, long long nodes, const int* labels,
+	const double* velocity, int* velocity_mask, double* velocity_out, int* pressure_mask, double* pressure,
+	long long* counts, int* traction_labels, double* traction_values, int* traction_count, double* physics)
+{
+	try {
+		const std::filesystem::path path(config_path);
+		const auto configuration = iga::ReadSimulationConfiguration(path.string());
+		const auto& flow = iga::FindNavierStokesSystem(configuration, system);
+		const bool transient = flow.time_integration == "backward_euler";
+		const auto models = iga::InitializeOutletModels(configuration, flow);
+		const auto waveform = transient
+			? iga::MaterializeBoundaryWaveforms(configuration, path.parent_path(), time) : configuration;
+		const auto materialized = iga::MaterializeOutletPressures(waveform, models);
+		const auto& resolved_system = iga::FindNavierStokesSystem(materialized, system);
+		const auto tractions = iga::ExtractPressureTractions(materialized, resolved_system);
+		std::vector<int> label(labels, labels+nodes);
+		std::vector<std::array<double, 3>> reference(static_cast<std::size_t>(nodes));
+		for (long long i = 0; i < nodes; ++i)
+			for (int d = 0; d < 3; ++d) reference[static_cast<std::size_t>(i)][static_cast<std::size_t>(d)] = velocity[3*i+d];
+		const auto r = iga::ResolveFlowBoundaries(materialized, resolved_system, label, reference);
+		for (long long i = 0; i < nodes; ++i) {
+			const auto k = static_cast<std::size_t>(i);
+			velocity_mask[i] = r.velocity_constrained[k];
+			pressure_mask[i] = r.pressure_constrained[k];
+			for (int d = 0; d < 3; ++d) velocity_out[3*i+d] = r.velocity[k][static_cast<std::size_t>(d)];
+			pressure[i] = r.pressure[k];
+		}
+		counts[0] = static_cast<long long>(r.velocity_nodes);
+		counts[1] = static_cast<long long>(r.pressure_nodes);
+		int n = 0;
+		for (const auto& t : tractions) {
+			if (n < *traction_count) { traction_labels[n] = t.first; traction_values[n] = t.second; }
+			++n;
+		}
+		*traction_count = n;
+		physics[0] = flow.viscosity;
+		physics[1] = flow.density;
+		physics[2] = transient ? configuration.time.dt : 0.0;
+		physics[3] = transient ? configuration.time.steps : 1;
+		physics[4] = transient ? 1.0 : 0.0;
 		return 0;
 	} catch (const std::exception& error) {
 		last_error = error.what();

@@ -242,3 +242,51 @@ def test_legacy_boundaries_match_the_reference_resolver(api, tmp_path, small_tub
         got = api.resolve_legacy_boundaries(t.labels, velocity, p, path)
         for k in keys:
             assert np.array_equal(got[k], want[k]), (cfg, k)
+
+
+@requires_ref
+def test_flow_boundaries_match_the_reference_set_up(api, tmp_path, small_tube):
+    """The navier-stokes command's boundary set-up of simulation_config.json cases (schema 4:
+    steady and transient, Fourier and sinusoid waveforms at several times, zero-traction, resistance,
+    RC and RCR outlets, wall velocity) against the reference's own compiled ReadSimulationConfiguration
+    ... ResolveFlowBoundaries chain (iga_cuda.cu:766-790): every mask, value, traction and the physics."""
+    from tubularflowiga_b200 import meshgen
+    t = small_tube
+    rng = np.random.default_rng(9)
+    velocity = t.profile + 0.1 * rng.normal(size=t.profile.shape)
+    wave = meshgen.fourier_waveform(3)
+    sine = {"name": "inflow", "kind": "sinusoid", "units": "m/s", "mean": 0.2, "amplitude": 0.05, "period": 0.8,
+            "phase": 0.3}
+    outlet = lambda cond: [{"label": 2, "name": "outlet", "conditions": [dict(field="pressure", **cond)]}]
+    cases = [
+        meshgen.simulation_config(1060.0, 3.5e-3, 2e-3, 3, 0.7, transient=False),
+        meshgen.simulation_config(1060.0, 3.5e-3, 2e-3, 5, 1.3, transient=True, waveform=wave),
+        meshgen.simulation_config(1.0, 0.01, 1e-2, 4, 2.0, transient=True, waveform=sine),
+        meshgen.simulation_config(1060.0, 3.5e-3, 2e-3, 3, 1.0, transient=True, waveform=wave,
+                                  outlets=outlet({"type": "resistance", "resistance": 2e7,
+                                                  "reference_pressure": 10.0})),
+        meshgen.simulation_config(1060.0, 3.5e-3, 2e-3, 3, 1.0, transient=True, waveform=wave,
+                                  outlets=outlet({"type": "windkessel_rc", "resistance": 3e8, "capacitance": 2e-10,
+                                                  "initial_pressure": 40.0})),
+        meshgen.simulation_config(1060.0, 3.5e-3, 2e-3, 3, 1.0, transient=True, waveform=wave,
+                                  outlets=outlet({"type": "windkessel_rcr", "proximal_resistance": 1e8,
+                                                  "capacitance": 1e-10, "distal_resistance": 1e9,
+                                                  "initial_pressure": 25.0})),
+        meshgen.simulation_config(1060.0, 3.5e-3, 2e-3, 3, 1.0, transient=True,
+                                  outlets=outlet({"type": "pressure_traction", "value": 133.0})),
+    ]
+    cases[1]["boundaries"][0]["conditions"][0]["value"] = [0.0, 0.0, 0.01]
+    keys = ("velocity_mask", "velocity", "pressure_mask", "pressure", "counts")
+    for k, cfg in enumerate(cases):
+        path = tmp_path / f"case{k}" / "simulation_config.json"
+        path.parent.mkdir()
+        path.write_text(json.dumps(cfg))
+        for time in (0.0, 0.37, 1.05):
+            want = O.ref_flow_boundaries(path, t.labels, velocity, time)
+            got = api.resolve_flow_boundaries(path, t.labels, velocity, time)
+            for key in keys:
+                assert np.allclose(got[key], want[key], rtol=1e-15, atol=0), (k, time, key)
+            assert got["tractions"].keys() == want["tractions"].keys(), (k, time)
+            for label, value in want["tractions"].items():
+                assert got["tractions"][label] == pytest.approx(value, rel=1e-15, abs=0), (k, time)
+            assert np.array_equal(got["physics"], want["physics"]), (k, time)

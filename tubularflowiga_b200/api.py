@@ -200,6 +200,9 @@ SIGNATURES = {
     "tfiga_transport_resolve_boundaries": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(TransportParams),
                                                      C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                      C.POINTER(C.c_int64)]),
+    "tfiga_resolve_flow_boundaries": (C.c_int, [C.c_char_p, C.c_char_p, C.c_double, C.c_int64, C.c_void_p,
+                                                C.c_void_p] + [C.c_void_p] * 5 + [C.c_void_p, C.c_void_p,
+                                                                                  C.POINTER(C.c_int32), C.c_void_p]),
     "tfiga_resolve_legacy_boundaries": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(TransportParams),
                                                   C.c_char_p] + [C.c_void_p] * 8),
     "tfiga_transport_create": (C.c_int, [C.c_void_p, C.POINTER(TransportParams), C.c_void_p, C.c_void_p,
@@ -604,6 +607,25 @@ def resolve_transport_boundaries(labels, reference_velocity, params: TransportPa
     check(lib().tfiga_transport_resolve_boundaries(n, _p(labels), _p(vel), C.byref(params), path, _p(mask),
                                                    _p(n0), _p(nplus), C.byref(count)))
     return mask, n0, nplus
+
+
+def resolve_flow_boundaries(config_path, labels, reference_velocity, time=0.0, system=None) -> dict:
+    """The navier-stokes command's boundary set-up of a simulation_config.json case at `time` (before
+    the wall trace): masks, values, labelled pressure tractions and the flow physics."""
+    labels = np.ascontiguousarray(labels, np.int32)
+    vel = np.ascontiguousarray(reference_velocity, np.float64).reshape(-1)
+    n = labels.size
+    out = {"velocity_mask": np.zeros(n, np.int32), "velocity": np.zeros(3 * n), "pressure_mask": np.zeros(n, np.int32),
+           "pressure": np.zeros(n), "counts": np.zeros(2, np.int64)}
+    tl, tv, count = np.zeros(64, np.int32), np.zeros(64), C.c_int32(64)
+    physics = np.zeros(5)
+    check(lib().tfiga_resolve_flow_boundaries(str(config_path).encode(), None if system is None else system.encode(),
+                                              time, n, _p(labels), _p(vel), _p(out["velocity_mask"]),
+                                              _p(out["velocity"]), _p(out["pressure_mask"]), _p(out["pressure"]),
+                                              _p(out["counts"]), _p(tl), _p(tv), C.byref(count), _p(physics)))
+    out["tractions"] = {int(tl[i]): float(tv[i]) for i in range(min(count.value, 64))}
+    out["physics"] = physics
+    return out
 
 
 def resolve_legacy_boundaries(labels, reference_velocity, params: TransportParams, case_config=None) -> dict:

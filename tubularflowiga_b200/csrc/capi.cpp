@@ -509,6 +509,53 @@ int tfiga_transport_read_params(const char* path, tfiga_transport_params* params
 	});
 }
 
+int tfiga_resolve_flow_boundaries(const char* config_path, const char* system, double time, int64_t nodes,
+	const int32_t* labels, const double* reference_velocity, int32_t* velocity_mask, double* velocity,
+	int32_t* pressure_mask, double* pressure, int64_t* counts, int32_t* traction_labels, double* traction_values,
+	int32_t* traction_count, double* physics)
+{
+	return Guard([&] {
+		Require(config_path && nodes > 0 && labels && reference_velocity, "null argument");
+		const std::string name = system ? system : "";
+		const tfiga::SimulationConfig config = tfiga::ReadSimulationConfig(config_path);
+		const tfiga::FlowSystem& flow = tfiga::FindNavierStokesSystem(config, name);
+		const bool transient = flow.time_integration == "backward_euler";
+		const auto models = tfiga::InitializeOutletModels(config, flow);
+		const tfiga::SimulationConfig materialized = tfiga::MaterializeOutletPressures(
+			transient ? tfiga::MaterializeWaveforms(config, time) : config, models);
+		const tfiga::FlowSystem& resolved_system = tfiga::FindNavierStokesSystem(materialized, name);
+		const auto tractions = tfiga::ExtractPressureTractions(materialized, resolved_system);
+		std::vector<int> label(labels, labels+nodes);
+		std::vector<std::array<double, 3>> reference((size_t)nodes);
+		for (int64_t i = 0; i < nodes; ++i)
+			for (int d = 0; d < 3; ++d) reference[(size_t)i][d] = reference_velocity[3*i+d];
+		const auto r = tfiga::ResolveFlowBoundaries(materialized, resolved_system, label, reference);
+		if (velocity_mask) std::copy(r.velocity_mask.begin(), r.velocity_mask.end(), velocity_mask);
+		if (velocity) std::copy(r.velocity.begin(), r.velocity.end(), velocity);
+		if (pressure_mask) std::copy(r.pressure_mask.begin(), r.pressure_mask.end(), pressure_mask);
+		if (pressure) std::copy(r.pressure.begin(), r.pressure.end(), pressure);
+		if (counts) { counts[0] = (int64_t)r.velocity_nodes; counts[1] = (int64_t)r.pressure_nodes; }
+		if (traction_count) {
+			int32_t n = 0;
+			for (const auto& t : tractions) {
+				if (n < *traction_count && traction_labels && traction_values) {
+					traction_labels[n] = t.first;
+					traction_values[n] = t.second;
+				}
+				++n;
+			}
+			*traction_count = n;
+		}
+		if (physics) {
+			physics[0] = flow.viscosity;
+			physics[1] = flow.density;
+			physics[2] = transient ? config.dt : 0.0;
+			physics[3] = transient ? config.steps : 1;
+			physics[4] = transient ? 1.0 : 0.0;
+		}
+	});
+}
+
 int tfiga_resolve_legacy_boundaries(int64_t nodes, const int32_t* labels, const double* reference_velocity,
 	const tfiga_transport_params* params, const char* case_config_path, int32_t* velocity_mask, double* velocity,
 	int32_t* pressure_mask, double* pressure, int32_t* transport_mask, double* n0, double* nplus, int64_t* counts)

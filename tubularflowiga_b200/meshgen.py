@@ -508,7 +508,8 @@ def simulation_config(density: float, viscosity: float, dt: float, steps: int, i
             {"field": "pressure", "type": "pressure_traction", "value": 0.0}]}]
     boundaries += outlets
     cfg = {
-        "schema_version": 4,
+        "schema_version": 3,
+        "dimension": "3d",
         "fields": [{"name": "velocity", "kind": "vector3"}, {"name": "pressure", "kind": "pressure"}],
         "time": {"dt": dt, "steps": steps},
         "equation_systems": [{"name": "blood_flow", "kind": "navier_stokes",
