@@ -101,6 +101,7 @@ def ref():
                                    C.c_double, C.c_double, C.c_double, C.c_void_p, _dp]
         R.ref_max_threads.restype = C.c_int
         R.ref_transport_element.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
+        R.ref_read_transport_parameters.argtypes = [C.c_char_p, _dp]
         R.ref_flow_boundaries.argtypes = [C.c_char_p, C.c_char_p, C.c_double, C.c_longlong, _ip, _dp, _ip, _dp, _ip,
                                           _dp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS"), _ip,
                                           _dp, C.POINTER(C.c_int), _dp]
@@ -354,6 +355,14 @@ def transport_assemble(mesh, pattern, velocity, params, constrained=None):
     if st:
         raise RuntimeError(f"oracle transport assembly failed at element {failed.value} ({st})")
     return left, previous
+
+
+def ref_read_transport_parameters(path):
+    """The reference's ReadTransportParameters: the 13 values in the order of its struct."""
+    out = np.zeros(13)
+    if ref().ref_read_transport_parameters(str(path).encode(), out):
+        raise RuntimeError(ref().ref_last_error().decode())
+    return out
 
 
 def ref_flow_boundaries(config_path, labels, velocity, time=0.0, system=""):

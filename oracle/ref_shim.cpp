@@ -14,6 +14,7 @@
 //   iga::WallTraceBasis                solvers/cpu/include/BoundarySupport.hpp:134-150
 //   iga::BuildTransportElement         solvers/cpu/include/TransportElement.hpp:213-260
 //   iga::ParseCaseConfiguration        include/CaseConfig.hpp:340-371
+//   iga::ReadTransportParameters       solvers/cpu/include/CaseInput.hpp:85-118
 //   the flow boundary set-up of NavierStokes (solvers/cuda/src/iga_cuda.cu:766-790):
 //   ReadSimulationConfiguration, FindNavierStokesSystem, InitializeOutletModels,
 //   MaterializeBoundaryWaveforms, MaterializeOutletPressures, ExtractPressureTractions,
@@ -390,6 +391,22 @@ int ref_flow_boundaries(const char* config_path, const char* system, double time
 		physics[2] = transient ? configuration.time.dt : 0.0;
 		physics[3] = transient ? configuration.time.steps : 1;
 		physics[4] = transient ? 1.0 : 0.0;
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+// simulation_parameter.txt: out[13] = D, vplus, vminus, kplus, kminus, k'plus, k'minus, dt, nstep,
+// N0bc, Nplusbc, Nminusbc, artificial_diffusion.
+int ref_read_transport_parameters(const char* path, double* out)
+{
+	try {
+		const auto p = iga::ReadTransportParameters(path);
+		const double values[13] = {p.diffusion, p.vplus, p.vminus, p.kplus, p.kminus, p.detach_plus, p.detach_minus,
+			p.dt, static_cast<double>(p.steps), p.n0_bc, p.nplus_bc, p.nminus_bc, p.artificial_diffusion};
+		std::memcpy(out, values, sizeof(values));
 		return 0;
 	} catch (const std::exception& error) {
 		last_error = error.what();

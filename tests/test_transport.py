@@ -290,3 +290,32 @@ def test_flow_boundaries_match_the_reference_set_up(api, tmp_path, small_tube):
             for label, value in want["tractions"].items():
                 assert got["tractions"][label] == pytest.approx(value, rel=1e-15, abs=0), (k, time)
             assert np.array_equal(got["physics"], want["physics"]), (k, time)
+
+
+@requires_ref
+def test_transport_params_match_the_reference_reader(api, tmp_path):
+    """simulation_parameter.txt through tfiga_transport_read_params against the reference's own
+    ReadTransportParameters: values, the optional artificial-diffusion spellings, and failures."""
+    order = ("diffusion", "vplus", "vminus", "kplus", "kminus", "detach_plus", "detach_minus", "dt", "steps",
+             "n0_bc", "nplus_bc", "nminus_bc", "artificial_diffusion")
+    texts = ["D 1e-3\nvplus 0.5\nvminus 0.25\nkplus 2\nkminus 0.5\nk'plus 0.125\nk'minus 0.0625\ndt 0.01\n"
+             "nstep 12\nN0bc 1\nNplusbc 0.5\nNminusbc 0.25\n",
+             "nstep 3 dt 0.5 D 0 vplus 1 vminus 1 kplus 0 kminus 0 k'plus 0 k'minus 0 N0bc 0 Nplusbc 0 Nminusbc 0 "
+             "artificial_diffusion_weight 0.75\n",
+             "D 1\nD 2\nvplus 1\nvminus 1\nkplus 1\nkminus 1\nk'plus 1\nk'minus 1\ndt 1\nnstep 1\nN0bc 1\n"
+             "Nplusbc 1\nNminusbc 1\nartificial_diffusion 3\nartificial_diffusion_weight 4\n",
+             "D 1\nvplus 1\n",
+             "D 1\nvplus 1\nvminus 1\nkplus 1\nkminus 1\nk'plus 1\nk'minus 1\ndt 0\nnstep 1\nN0bc 1\nNplusbc 1\n"
+             "Nminusbc 1\n"]
+    for k, text in enumerate(texts):
+        path = tmp_path / f"p{k}.txt"
+        path.write_text(text)
+        try:
+            want = O.ref_read_transport_parameters(path)
+        except RuntimeError as ref_error:
+            with pytest.raises(api.TfigaError) as err:
+                api.read_transport_params(path)
+            assert str(ref_error) in str(err.value), (k, str(ref_error), str(err.value))
+            continue
+        got = api.read_transport_params(path).as_dict()
+        assert [float(got[name]) for name in order] == list(want), k
