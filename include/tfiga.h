@@ -393,6 +393,11 @@ int tfiga_resolve_flow_boundaries(const char* config_path, const char* system, d
 	int32_t* pressure_mask, double* pressure, int64_t* counts, int32_t* traction_labels, double* traction_values,
 	int32_t* traction_count, double* physics);
 
+/* The navier-stokes command's VTU snapshot (WriteNavierStokesVtu, iga_cuda.cu:366-388; WriteVtu,
+ * include/VtkOutput.hpp:107-155): the control mesh of the legacy ASCII mesh_vtk with `velocity` (3)
+ * and `pressure` (1) point arrays from state [4*nodes] and TimeValue = time.  Host only. */
+int tfiga_write_vtu(const char* mesh_vtk, const char* output, const double* state, int64_t nodes, double time);
+
 /* ---- two-species transport ------------------------------------------ */
 /* The `iga_cuda transport` path (Transport, solvers/cuda/src/iga_cuda.cu:621-732):
  * N0 (attached: diffusion and exchange) and N+ (advected by a prescribed nodal

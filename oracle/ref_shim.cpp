@@ -15,6 +15,8 @@
 //   iga::BuildTransportElement         solvers/cpu/include/TransportElement.hpp:213-260
 //   iga::ParseCaseConfiguration        include/CaseConfig.hpp:340-371
 //   iga::ReadTransportParameters       solvers/cpu/include/CaseInput.hpp:85-118
+//   iga::WriteVtu                      include/VtkOutput.hpp:107-155 (the arrays of
+//                                      WriteNavierStokesVtu, solvers/cuda/src/iga_cuda.cu:366-388)
 //   the flow boundary set-up of NavierStokes (solvers/cuda/src/iga_cuda.cu:766-790):
 //   ReadSimulationConfiguration, FindNavierStokesSystem, InitializeOutletModels,
 //   MaterializeBoundaryWaveforms, MaterializeOutletPressures, ExtractPressureTractions,
@@ -27,6 +29,7 @@
 #include "OutletModel.hpp"
 #include "PressureTraction.hpp"
 #include "TemporalFunction.hpp"
+#include "VtkOutput.hpp"
 
 #include <omp.h>
 
@@ -391,6 +394,24 @@ int ref_flow_boundaries(const char* config_path, const char* system, double time
 		physics[2] = transient ? configuration.time.dt : 0.0;
 		physics[3] = transient ? configuration.time.steps : 1;
 		physics[4] = transient ? 1.0 : 0.0;
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+// VTU snapshot of a Navier-Stokes state [4 nodes] on the control mesh of mesh_vtk.
+int ref_write_vtu(const char* mesh_vtk, const char* output, const double* state, long long nodes, double time)
+{
+	try {
+		std::vector<double> velocity(static_cast<std::size_t>(3*nodes)), pressure(static_cast<std::size_t>(nodes));
+		for (long long node = 0; node < nodes; ++node) {
+			for (int c = 0; c < 3; ++c) velocity[static_cast<std::size_t>(3*node+c)] = state[4*node+c];
+			pressure[static_cast<std::size_t>(node)] = state[4*node+3];
+		}
+		std::vector<iga::VtkPointArray> arrays{{"velocity", 3, std::move(velocity)}, {"pressure", 1, std::move(pressure)}};
+		iga::WriteVtu(mesh_vtk, output, arrays, time);
 		return 0;
 	} catch (const std::exception& error) {
 		last_error = error.what();

@@ -184,3 +184,23 @@ def test_ntiga_writer_reproduces_the_reference_pack_byte_for_byte(reference_tube
     mesh = ntiga.read(reference_tube / "tube-1.ntiga")
     ntiga.write(tmp_path / "copy.ntiga", mesh)
     assert (tmp_path / "copy.ntiga").read_bytes() == source
+
+
+@requires_ref
+def test_vtu_snapshot_matches_the_reference_writer_byte_for_byte(tmp_path, small_tube, reference_tube):
+    """tfiga_write_vtu (the navier-stokes command's VTU snapshots) against the reference's own WriteVtu
+    with the arrays of WriteNavierStokesVtu: identical files, on a generated control mesh and on the
+    reference-generated one."""
+    from tubularflowiga_b200 import api, build, meshgen
+    build.build()
+    meshgen.write_vtk(tmp_path / "controlmesh.vtk", small_tube)
+    rng = np.random.default_rng(4)
+    for k, (mesh_vtk, nodes) in enumerate(((tmp_path / "controlmesh.vtk", small_tube.mesh.nodes),
+                                           (reference_tube / "controlmesh.vtk", 725))):
+        state = rng.normal(size=4 * nodes) * np.array([0.3, 0.3, 0.3, 40.0] * nodes)
+        ours, theirs = tmp_path / f"ours{k}.vtu", tmp_path / f"ref{k}.vtu"
+        api.check(api.lib().tfiga_write_vtu(str(mesh_vtk).encode(), str(ours).encode(),
+                                            state.ctypes.data_as(ctypes.c_void_p), nodes, 0.125 * (k + 1)))
+        assert O.ref().ref_write_vtu(str(mesh_vtk).encode(), str(theirs).encode(), state, nodes,
+                                     0.125 * (k + 1)) == 0
+        assert ours.read_bytes() == theirs.read_bytes()

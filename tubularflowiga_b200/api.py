@@ -200,6 +200,7 @@ SIGNATURES = {
     "tfiga_transport_resolve_boundaries": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(TransportParams),
                                                      C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                      C.POINTER(C.c_int64)]),
+    "tfiga_write_vtu": (C.c_int, [C.c_char_p, C.c_char_p, C.c_void_p, C.c_int64, C.c_double]),
     "tfiga_resolve_flow_boundaries": (C.c_int, [C.c_char_p, C.c_char_p, C.c_double, C.c_int64, C.c_void_p,
                                                 C.c_void_p] + [C.c_void_p] * 5 + [C.c_void_p, C.c_void_p,
                                                                                   C.POINTER(C.c_int32), C.c_void_p]),

@@ -738,6 +738,30 @@ int Transport(int argc, char** argv)
 } // namespace
 } // namespace tfiga
 
+namespace tfiga {
+void RecordLastError(const char* message);
+}
+
+// The VTU snapshot writer of the navier-stokes command (WriteNavierStokesVtu, iga_cuda.cu:366-388:
+// the control mesh of mesh_vtk with velocity and pressure point arrays and the physical time).
+extern "C" int tfiga_write_vtu(const char* mesh_vtk, const char* output, const double* state, int64_t nodes,
+	double time)
+{
+	try {
+		if (!mesh_vtk || !output || !state || nodes <= 0) tfiga::Fail(TFIGA_E_INVALID, "null argument");
+		const tfiga::VtkGrid grid = tfiga::ReadVtkGrid(mesh_vtk);
+		const std::vector<double> values(state, state+4*nodes);
+		tfiga::WriteVtuFile(grid, output, values, time);
+		return TFIGA_OK;
+	} catch (const tfiga::Error& error) {
+		tfiga::RecordLastError(error.what());
+		return error.status;
+	} catch (const std::exception& error) {
+		tfiga::RecordLastError(error.what());
+		return TFIGA_E_INVALID;
+	}
+}
+
 extern "C" int tfiga_main(int argc, char** argv)
 {
 	try {
