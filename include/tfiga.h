@@ -398,6 +398,18 @@ int tfiga_resolve_flow_boundaries(const char* config_path, const char* system, d
  * and `pressure` (1) point arrays from state [4*nodes] and TimeValue = time.  Host only. */
 int tfiga_write_vtu(const char* mesh_vtk, const char* output, const double* state, int64_t nodes, double time);
 
+/* The navier-stokes command's checkpoint (WriteCudaFlowCheckpoint, iga_cuda.cu:584-602):
+ * PREFIX.state (raw float64 [4*nodes]) and PREFIX.json (schema 1: nodes, fields, completed step,
+ * time, dt, density, viscosity, state file and format, outlet states).  Host only. */
+int tfiga_write_flow_checkpoint(const char* prefix, int64_t nodes, int32_t completed_step, double physical_time,
+	double dt, double density, double viscosity, const tfiga_outlet* outlets, int32_t count, const double* state);
+/* Restart from it (ReadFlowCheckpointMetadata + ValidateFlowCheckpoint + ReadCudaFlowCheckpoint,
+ * include/FlowCheckpoint.hpp:186-211, iga_cuda.cu:566-582): checks nodes, dt, density, viscosity
+ * and the state size; outlets whose labels appear take the stored flow, pressure and capacitor
+ * pressure.  Host only. */
+int tfiga_read_flow_checkpoint(const char* prefix, int64_t nodes, double dt, double density, double viscosity,
+	tfiga_outlet* outlets, int32_t count, double* state, int32_t* completed_step, double* physical_time);
+
 /* ---- two-species transport ------------------------------------------ */
 /* The `iga_cuda transport` path (Transport, solvers/cuda/src/iga_cuda.cu:621-732):
  * N0 (attached: diffusion and exchange) and N+ (advected by a prescribed nodal

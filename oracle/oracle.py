@@ -102,6 +102,11 @@ def ref():
         R.ref_max_threads.restype = C.c_int
         R.ref_transport_element.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
         R.ref_read_transport_parameters.argtypes = [C.c_char_p, _dp]
+        R.ref_write_flow_checkpoint.argtypes = [C.c_char_p, C.c_longlong, C.c_int, C.c_double, C.c_double, C.c_double,
+                                                C.c_double, _ip, _dp, C.c_int, _dp]
+        R.ref_read_flow_checkpoint.argtypes = [C.c_char_p, C.c_longlong, C.c_int, C.c_double, C.c_double, C.c_double,
+                                               _dp, C.POINTER(C.c_int), C.POINTER(C.c_double), _ip, _dp,
+                                               C.POINTER(C.c_int)]
         R.ref_write_vtu.argtypes = [C.c_char_p, C.c_char_p, _dp, C.c_longlong, C.c_double]
         R.ref_flow_boundaries.argtypes = [C.c_char_p, C.c_char_p, C.c_double, C.c_longlong, _ip, _dp, _ip, _dp, _ip,
                                           _dp, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS"), _ip,

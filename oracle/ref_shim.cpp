@@ -15,6 +15,9 @@
 //   iga::BuildTransportElement         solvers/cpu/include/TransportElement.hpp:213-260
 //   iga::ParseCaseConfiguration        include/CaseConfig.hpp:340-371
 //   iga::ReadTransportParameters       solvers/cpu/include/CaseInput.hpp:85-118
+//   iga::WriteFlowCheckpointMetadata / ReadFlowCheckpointMetadata / ValidateFlowCheckpoint
+//                                      include/FlowCheckpoint.hpp:176-211, with the raw state
+//                                      file of solvers/cuda/src/iga_cuda.cu:566-602
 //   iga::WriteVtu                      include/VtkOutput.hpp:107-155 (the arrays of
 //                                      WriteNavierStokesVtu, solvers/cuda/src/iga_cuda.cu:366-388)
 //   the flow boundary set-up of NavierStokes (solvers/cuda/src/iga_cuda.cu:766-790):
@@ -24,6 +27,7 @@
 //   iga::ResolveBoundaryConditions     solvers/cpu/include/CaseInput.hpp:162-258
 #include "BoundaryFlow.hpp"
 #include "BoundarySupport.hpp"
+#include "FlowCheckpoint.hpp"
 #include "GenericCaseInput.hpp"
 #include "NavierStokesElement.hpp"
 #include "OutletModel.hpp"
@@ -38,6 +42,7 @@
 #include <cstring>
 #include <exception>
 #include <filesystem>
+#include <fstream>
 #include <string>
 #include <vector>
 
@@ -394,6 +399,71 @@ int ref_flow_boundaries(const char* config_path, const char* system, double time
 		physics[2] = transient ? configuration.time.dt : 0.0;
 		physics[3] = transient ? configuration.time.steps : 1;
 		physics[4] = transient ? 1.0 : 0.0;
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+// Flow checkpoint as the CUDA command writes it: raw state + metadata.  outlets: count entries of
+// (label, kind 0/1/2 = resistance / windkessel_rc / windkessel_rcr) and (flow, pressure, capacitor).
+int ref_write_flow_checkpoint(const char* prefix, long long nodes, int completed, double time, double dt,
+	double density, double viscosity, const int* outlet_ints, const double* outlet_values, int count,
+	const double* state)
+{
+	try {
+		static const char* kinds[3] = {"resistance", "windkessel_rc", "windkessel_rcr"};
+		const auto state_path = iga::FlowCheckpointStatePath(prefix);
+		std::ofstream output(state_path, std::ios::binary);
+		output.write(reinterpret_cast<const char*>(state), static_cast<std::streamsize>(4*nodes*sizeof(double)));
+		output.close();
+		iga::FlowCheckpointMetadata metadata;
+		metadata.nodes = static_cast<std::uint64_t>(nodes);
+		metadata.completed_step = completed;
+		metadata.physical_time = time;
+		metadata.dt = dt;
+		metadata.density = density;
+		metadata.viscosity = viscosity;
+		metadata.state_file = state_path.filename().string();
+		metadata.state_format = "raw_float64";
+		for (int i = 0; i < count; ++i)
+			metadata.outlets.push_back({outlet_ints[2*i], kinds[outlet_ints[2*i+1]], outlet_values[3*i],
+				outlet_values[3*i+1], outlet_values[3*i+2]});
+		iga::WriteFlowCheckpointMetadata(prefix, metadata);
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+// The reference's restart path: metadata, validation against (nodes, steps, dt, density, viscosity),
+// and the raw state.  outlet_values[3*i]: flow, pressure, capacitor pressure of metadata outlet i.
+int ref_read_flow_checkpoint(const char* prefix, long long nodes, int steps, double dt, double density,
+	double viscosity, double* state, int* completed, double* time, int* outlet_labels, double* outlet_values,
+	int* count)
+{
+	try {
+		const auto metadata = iga::ReadFlowCheckpointMetadata(prefix);
+		iga::ValidateFlowCheckpoint(metadata, static_cast<std::uint64_t>(nodes), steps, dt, density, viscosity);
+		if (metadata.state_format != "raw_float64") throw std::runtime_error("not raw_float64");
+		std::filesystem::path path(metadata.state_file);
+		if (path.is_relative()) path = iga::FlowCheckpointMetadataPath(prefix).parent_path()/path;
+		std::ifstream input(path, std::ios::binary);
+		input.read(reinterpret_cast<char*>(state), static_cast<std::streamsize>(4*nodes*sizeof(double)));
+		char extra = 0;
+		if (!input || input.read(&extra, 1)) throw std::runtime_error("state is truncated or has trailing data");
+		*completed = metadata.completed_step;
+		*time = metadata.physical_time;
+		const int n = std::min<int>(*count, static_cast<int>(metadata.outlets.size()));
+		for (int i = 0; i < n; ++i) {
+			outlet_labels[i] = metadata.outlets[static_cast<std::size_t>(i)].label;
+			outlet_values[3*i] = metadata.outlets[static_cast<std::size_t>(i)].flow;
+			outlet_values[3*i+1] = metadata.outlets[static_cast<std::size_t>(i)].pressure;
+			outlet_values[3*i+2] = metadata.outlets[static_cast<std::size_t>(i)].capacitor_pressure;
+		}
+		*count = static_cast<int>(metadata.outlets.size());
 		return 0;
 	} catch (const std::exception& error) {
 		last_error = error.what();

@@ -204,3 +204,52 @@ def test_vtu_snapshot_matches_the_reference_writer_byte_for_byte(tmp_path, small
         assert O.ref().ref_write_vtu(str(mesh_vtk).encode(), str(theirs).encode(), state, nodes,
                                      0.125 * (k + 1)) == 0
         assert ours.read_bytes() == theirs.read_bytes()
+
+
+@requires_ref
+def test_flow_checkpoint_matches_the_reference_format(tmp_path):
+    """tfiga_write_flow_checkpoint writes the metadata and state bytes the reference's own
+    WriteFlowCheckpointMetadata + raw state write produce; each side restarts from the other's files
+    (the reference through ReadFlowCheckpointMetadata + ValidateFlowCheckpoint)."""
+    from tubularflowiga_b200 import api, build
+    build.build()
+    rng = np.random.default_rng(8)
+    nodes = 57
+    state = rng.normal(size=4 * nodes)
+    outlets = (api.Outlet * 2)(api.Outlet.rcr(2, 1e8, 1e-10, 1e9), api.Outlet.resistance_model(3, 2e7, 5.0))
+    outlets[0].flow, outlets[0].pressure, outlets[0].capacitor_pressure = 1.25e-6, 143.9, 74.2
+    outlets[1].flow, outlets[1].pressure, outlets[1].capacitor_pressure = -3.5e-7, 12.5, 0.0
+    args = (nodes, 7, 7 * 2e-3, 2e-3, 1060.0, 3.5e-3)
+    ours, theirs = tmp_path / "ours", tmp_path / "theirs"
+    api.check(api.lib().tfiga_write_flow_checkpoint(str(ours).encode(), *args, outlets, 2,
+                                                    state.ctypes.data_as(ctypes.c_void_p)))
+    ints = np.array([2, 2, 3, 0], np.int32)
+    vals = np.array([1.25e-6, 143.9, 74.2, -3.5e-7, 12.5, 0.0])
+    assert O.ref().ref_write_flow_checkpoint(str(theirs).encode(), *args, ints, vals, 2, state) == 0
+    assert (tmp_path / "ours.json").read_text() == (tmp_path / "theirs.json").read_text().replace("theirs.state",
+                                                                                                 "ours.state")
+    assert (tmp_path / "ours.state").read_bytes() == (tmp_path / "theirs.state").read_bytes()
+    # the reference restarts from our files
+    back = np.zeros(4 * nodes)
+    completed, time, count = ctypes.c_int(), ctypes.c_double(), ctypes.c_int(4)
+    labels, values = np.zeros(4, np.int32), np.zeros(12)
+    assert O.ref().ref_read_flow_checkpoint(str(ours).encode(), nodes, 10, 2e-3, 1060.0, 3.5e-3, back,
+                                            ctypes.byref(completed), ctypes.byref(time), labels, values,
+                                            ctypes.byref(count)) == 0
+    assert np.array_equal(back, state) and completed.value == 7 and count.value == 2
+    assert list(labels[:2]) == [2, 3] and np.array_equal(values[:6], vals)
+    # we restart from the reference's files
+    fresh = (api.Outlet * 2)(api.Outlet.rcr(2, 1e8, 1e-10, 1e9), api.Outlet.resistance_model(3, 2e7, 5.0))
+    back2 = np.zeros(4 * nodes)
+    step, t = ctypes.c_int32(), ctypes.c_double()
+    api.check(api.lib().tfiga_read_flow_checkpoint(str(theirs).encode(), nodes, 2e-3, 1060.0, 3.5e-3, fresh, 2,
+                                                   back2.ctypes.data_as(ctypes.c_void_p), ctypes.byref(step),
+                                                   ctypes.byref(t)))
+    assert np.array_equal(back2, state) and step.value == 7 and t.value == 7 * 2e-3
+    assert (fresh[0].flow, fresh[0].pressure, fresh[0].capacitor_pressure) == (1.25e-6, 143.9, 74.2)
+    # a mismatched configuration is refused by both
+    assert api.lib().tfiga_read_flow_checkpoint(str(theirs).encode(), nodes, 1e-3, 1060.0, 3.5e-3, fresh, 2,
+                                                back2.ctypes.data_as(ctypes.c_void_p), None, None) == -4
+    assert O.ref().ref_read_flow_checkpoint(str(ours).encode(), nodes, 10, 1e-3, 1060.0, 3.5e-3, back,
+                                            ctypes.byref(completed), ctypes.byref(time), labels, values,
+                                            ctypes.byref(count)) == -1

@@ -742,6 +742,85 @@ namespace tfiga {
 void RecordLastError(const char* message);
 }
 
+namespace {
+
+const char* OutletKindName(int32_t kind)
+{
+	switch (kind) {
+	case TFIGA_OUTLET_RESISTANCE: return "resistance";
+	case TFIGA_OUTLET_RC: return "windkessel_rc";
+	case TFIGA_OUTLET_RCR: return "windkessel_rcr";
+	default: tfiga::Fail(TFIGA_E_INVALID, "unknown outlet kind");
+	}
+}
+
+template <class F>
+int HostGuard(F&& body)
+{
+	try {
+		body();
+		return TFIGA_OK;
+	} catch (const tfiga::Error& error) {
+		tfiga::RecordLastError(error.what());
+		return error.status;
+	} catch (const std::exception& error) {
+		tfiga::RecordLastError(error.what());
+		return TFIGA_E_INVALID;
+	}
+}
+
+} // namespace
+
+// The navier-stokes command's checkpoint (WriteCudaFlowCheckpoint, iga_cuda.cu:584-602).
+extern "C" int tfiga_write_flow_checkpoint(const char* prefix, int64_t nodes, int32_t completed_step,
+	double physical_time, double dt, double density, double viscosity, const tfiga_outlet* outlets, int32_t count,
+	const double* state)
+{
+	return HostGuard([&] {
+		if (!prefix || !state || nodes <= 0 || count < 0 || (count > 0 && !outlets))
+			tfiga::Fail(TFIGA_E_INVALID, "null argument");
+		std::vector<tfiga::OutletModel> models((size_t)count);
+		for (int32_t i = 0; i < count; ++i) {
+			models[i].label = outlets[i].label;
+			models[i].kind = OutletKindName(outlets[i].kind);
+			models[i].flow = outlets[i].flow;
+			models[i].pressure = outlets[i].pressure;
+			models[i].capacitor_pressure = outlets[i].capacitor_pressure;
+		}
+		tfiga::WriteCheckpoint(prefix, nodes, completed_step, physical_time, dt, density, viscosity, models,
+			std::vector<double>(state, state+4*nodes));
+	});
+}
+
+// Restart from a checkpoint (ReadFlowCheckpointMetadata, ValidateFlowCheckpoint, ReadCudaFlowCheckpoint,
+// include/FlowCheckpoint.hpp:186-211, iga_cuda.cu:566-582): the outlets whose labels appear in the
+// metadata take its flow, pressure and capacitor pressure.
+extern "C" int tfiga_read_flow_checkpoint(const char* prefix, int64_t nodes, double dt, double density,
+	double viscosity, tfiga_outlet* outlets, int32_t count, double* state, int32_t* completed_step,
+	double* physical_time)
+{
+	return HostGuard([&] {
+		if (!prefix || !state || nodes <= 0 || count < 0 || (count > 0 && !outlets))
+			tfiga::Fail(TFIGA_E_INVALID, "null argument");
+		std::vector<tfiga::OutletModel> models((size_t)count);
+		for (int32_t i = 0; i < count; ++i) {
+			models[i].label = outlets[i].label;
+			models[i].flow = outlets[i].flow;
+			models[i].pressure = outlets[i].pressure;
+			models[i].capacitor_pressure = outlets[i].capacitor_pressure;
+		}
+		const auto r = tfiga::ReadCheckpoint(prefix, nodes, dt, density, viscosity, models);
+		std::copy(r.state.begin(), r.state.end(), state);
+		for (int32_t i = 0; i < count; ++i) {
+			outlets[i].flow = models[i].flow;
+			outlets[i].pressure = models[i].pressure;
+			outlets[i].capacitor_pressure = models[i].capacitor_pressure;
+		}
+		if (completed_step) *completed_step = r.completed;
+		if (physical_time) *physical_time = r.time;
+	});
+}
+
 // The VTU snapshot writer of the navier-stokes command (WriteNavierStokesVtu, iga_cuda.cu:366-388:
 // the control mesh of mesh_vtk with velocity and pressure point arrays and the physical time).
 extern "C" int tfiga_write_vtu(const char* mesh_vtk, const char* output, const double* state, int64_t nodes,
