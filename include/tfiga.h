@@ -398,6 +398,13 @@ int tfiga_resolve_flow_boundaries(const char* config_path, const char* system, d
  * and `pressure` (1) point arrays from state [4*nodes] and TimeValue = time.  Host only. */
 int tfiga_write_vtu(const char* mesh_vtk, const char* output, const double* state, int64_t nodes, double time);
 
+/* The bases the navier-stokes command holds at no slip (WallTraceBasis,
+ * solvers/cpu/include/BoundarySupport.hpp:82-150): every basis with a nonzero trace on a face of
+ * controlmesh.vtk's wall (label 0) hexes, from the database read by this library's .ntiga reader.
+ * Sorted node indices, up to `capacity` written; *count = their number.  Host only. */
+int tfiga_wall_trace_basis(const char* database, const char* controlmesh_vtk, int32_t* nodes, int64_t capacity,
+	int64_t* count);
+
 /* The navier-stokes command's checkpoint (WriteCudaFlowCheckpoint, iga_cuda.cu:584-602):
  * PREFIX.state (raw float64 [4*nodes]) and PREFIX.json (schema 1: nodes, fields, completed step,
  * time, dt, density, viscosity, state file and format, outlet states).  Host only. */

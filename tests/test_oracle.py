@@ -253,3 +253,23 @@ def test_flow_checkpoint_matches_the_reference_format(tmp_path):
     assert O.ref().ref_read_flow_checkpoint(str(ours).encode(), nodes, 10, 1e-3, 1060.0, 3.5e-3, back,
                                             ctypes.byref(completed), ctypes.byref(time), labels, values,
                                             ctypes.byref(count)) == -1
+
+
+@requires_ref
+def test_wall_trace_and_ntiga_reader_match_the_reference(tmp_path, small_tube, reference_tube):
+    """The command's no-slip basis set from this library's .ntiga reader (tfiga_wall_trace_basis)
+    equals the reference's own WallTraceBasis over its own Database, on a generated case and on the
+    reference-generated tube."""
+    from tubularflowiga_b200 import api, build, meshgen
+    build.build()
+    db = meshgen.write_case(tmp_path, small_tube, meshgen.simulation_config(1060, 3.5e-3, 1e-3, 2, 0.2))
+    for database, vtk, nodes in ((db, tmp_path / "controlmesh.vtk", small_tube.mesh.nodes),
+                                 (reference_tube / "tube-1.ntiga", reference_tube / "controlmesh.vtk", 725)):
+        want = np.zeros(nodes, np.int32)
+        n_ref = O.ref().ref_wall_trace(str(database).encode(), str(vtk).encode(), want, nodes)
+        got = np.zeros(nodes, np.int32)
+        count = ctypes.c_int64()
+        api.check(api.lib().tfiga_wall_trace_basis(str(database).encode(), str(vtk).encode(),
+                                                   got.ctypes.data_as(ctypes.c_void_p), nodes, ctypes.byref(count)))
+        assert count.value == n_ref > 0
+        assert np.array_equal(got[:count.value], np.sort(want[:n_ref]))

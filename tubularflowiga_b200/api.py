@@ -200,6 +200,7 @@ SIGNATURES = {
     "tfiga_transport_resolve_boundaries": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(TransportParams),
                                                      C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                      C.POINTER(C.c_int64)]),
+    "tfiga_wall_trace_basis": (C.c_int, [C.c_char_p, C.c_char_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
     "tfiga_write_flow_checkpoint": (C.c_int, [C.c_char_p, C.c_int64, C.c_int32, C.c_double, C.c_double, C.c_double,
                                               C.c_double, C.c_void_p, C.c_int32, C.c_void_p]),
     "tfiga_read_flow_checkpoint": (C.c_int, [C.c_char_p, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_void_p,

@@ -771,6 +771,25 @@ int HostGuard(F&& body)
 
 } // namespace
 
+// The no-slip bases of the navier-stokes command (WallTraceBasis, BoundarySupport.hpp:82-150) from
+// the database (this library's .ntiga reader) and controlmesh.vtk: sorted node indices.
+extern "C" int tfiga_wall_trace_basis(const char* database, const char* controlmesh_vtk, int32_t* nodes_out,
+	int64_t capacity, int64_t* count)
+{
+	return HostGuard([&] {
+		if (!database || !controlmesh_vtk || !count) tfiga::Fail(TFIGA_E_INVALID, "null argument");
+		const tfiga::HostMesh host = tfiga::ReadNtiga(database);
+		const auto labeled = tfiga::ReadLabeledHexMesh(controlmesh_vtk, host.nodes, host.elements());
+		const auto wall = tfiga::WallTraceBasis(host, labeled);
+		*count = (int64_t)wall.size();
+		int64_t i = 0;
+		for (const int32_t node : wall) {
+			if (i < capacity && nodes_out) nodes_out[i] = node;
+			++i;
+		}
+	});
+}
+
 // The navier-stokes command's checkpoint (WriteCudaFlowCheckpoint, iga_cuda.cu:584-602).
 extern "C" int tfiga_write_flow_checkpoint(const char* prefix, int64_t nodes, int32_t completed_step,
 	double physical_time, double dt, double density, double viscosity, const tfiga_outlet* outlets, int32_t count,
