@@ -719,9 +719,12 @@ static void axpy(long long n, double alpha, const double* x, double* y)
  * iteration count (>= 0) or TFO_NOT_CONVERGED; *residual gets the final
  * preconditioned residual norm.
  */
-static int gmres_bjacobi_f(int F, int nodes, const int* row_offsets, const int* columns, const int* diagonal,
+typedef void (*precond_fn)(const void* context, const double* in, double* out);
+
+/* apply (may be NULL): the left preconditioner M^{-1}; NULL = the block-Jacobi inverse. */
+static int gmres_precond_f(int F, int nodes, const int* row_offsets, const int* columns, const int* diagonal,
 	const double* values, const double* rhs, double* x, int restart, int maximum_iterations,
-	double rtol, double* residual_out, int* singular_out)
+	double rtol, double* residual_out, int* singular_out, precond_fn apply, const void* context)
 {
 	const long long n = (long long)F*nodes;
 	double* inverse = (double*)malloc(sizeof(double)*(size_t)n*F);
@@ -735,11 +738,12 @@ static int gmres_bjacobi_f(int F, int nodes, const int* row_offsets, const int* 
 	double* g = (double*)calloc((size_t)restart+1, sizeof(double));
 	double* y = (double*)calloc((size_t)restart, sizeof(double));
 	if (!inverse || !raw || !res || !work || !V || !h || !cs || !sn || !g || !y) return TFO_NO_MEMORY;
-	const int singular = block_inverse_f(F, nodes, diagonal, values, inverse);
+	const int singular = apply ? 0 : block_inverse_f(F, nodes, diagonal, values, inverse);
 	if (singular_out) *singular_out = singular;
 	spmv_f(F, nodes, row_offsets, columns, values, x, raw);
 	for (long long i = 0; i < n; ++i) res[i] = rhs[i]-raw[i];
-	apply_block_inverse_f(F, nodes, inverse, res, work);
+	if (apply) apply(context, res, work);
+	else apply_block_inverse_f(F, nodes, inverse, res, work);
 	const double initial = sqrt(dot(n, work, work));
 	int iterations = 0, converged = 0;
 	double residual = initial;
@@ -754,7 +758,8 @@ static int gmres_bjacobi_f(int F, int nodes, const int* row_offsets, const int* 
 		int used = 0;
 		for (int j = 0; j < restart && iterations < maximum_iterations; ++j) {
 			spmv_f(F, nodes, row_offsets, columns, values, V+(size_t)j*n, raw);
-			apply_block_inverse_f(F, nodes, inverse, raw, work);
+			if (apply) apply(context, raw, work);
+			else apply_block_inverse_f(F, nodes, inverse, raw, work);
 			for (int i = 0; i <= j; ++i) {
 				const double value = dot(n, V+(size_t)i*n, work);
 				h[(size_t)i*restart+j] = value;
@@ -791,7 +796,8 @@ static int gmres_bjacobi_f(int F, int nodes, const int* row_offsets, const int* 
 		for (int i = 0; i < used; ++i) axpy(n, y[i], V+(size_t)i*n, x);
 		spmv_f(F, nodes, row_offsets, columns, values, x, raw);
 		for (long long i = 0; i < n; ++i) res[i] = rhs[i]-raw[i];
-		apply_block_inverse_f(F, nodes, inverse, res, work);
+		if (apply) apply(context, res, work);
+		else apply_block_inverse_f(F, nodes, inverse, res, work);
 		beta = sqrt(dot(n, work, work));
 		residual = beta;
 		if (beta <= tolerance) converged = 1;
@@ -805,8 +811,8 @@ int tfo_gmres_bjacobi(int nodes, const int* row_offsets, const int* columns, con
 	const double* values, const double* rhs, double* x, int restart, int maximum_iterations,
 	double rtol, double* residual_out, int* singular_out)
 {
-	return gmres_bjacobi_f(4, nodes, row_offsets, columns, diagonal, values, rhs, x, restart, maximum_iterations,
-		rtol, residual_out, singular_out);
+	return gmres_precond_f(4, nodes, row_offsets, columns, diagonal, values, rhs, x, restart, maximum_iterations,
+		rtol, residual_out, singular_out, NULL, NULL);
 }
 
 /* The same GMRES on the 2x2 transport system (SolveGmres<2>, iga_cuda.cu:691). */
@@ -814,8 +820,8 @@ int tfo_transport_gmres(int nodes, const int* row_offsets, const int* columns, c
 	const double* values, const double* rhs, double* x, int restart, int maximum_iterations,
 	double rtol, double* residual_out, int* singular_out)
 {
-	return gmres_bjacobi_f(2, nodes, row_offsets, columns, diagonal, values, rhs, x, restart, maximum_iterations,
-		rtol, residual_out, singular_out);
+	return gmres_precond_f(2, nodes, row_offsets, columns, diagonal, values, rhs, x, restart, maximum_iterations,
+		rtol, residual_out, singular_out, NULL, NULL);
 }
 
 /* y = A x over 2x2 blocks (BlockSpmvKernel<2>). */
@@ -823,6 +829,196 @@ void tfo_transport_spmv(int nodes, const int* row_offsets, const int* columns, c
 	const double* x, double* y)
 {
 	spmv_f(2, nodes, row_offsets, columns, values, x, y);
+}
+
+/*
+ * Flow-line preconditioner for the 2x2 transport system (no counterpart in the reference, which
+ * uses block-Jacobi): the restatement a device version is checked against.
+ *
+ * Lines: node i links to the pattern neighbour j with the largest a_ij = L++_ji - L++_ij > 0
+ * (the antisymmetric part of the advected species' block, positive towards downstream); a node
+ * keeps only its strongest upstream link; every node without an upstream link starts a chain.
+ * line_offsets[lines+1], line_nodes[nodes] (every node exactly once, in chain order).
+ */
+int tfo_flow_lines(int nodes, const int* row_offsets, const int* columns, const double* values, int* line_offsets,
+	int* line_nodes)
+{
+	int* down = (int*)malloc(sizeof(int)*(size_t)nodes);
+	double* dval = (double*)malloc(sizeof(double)*(size_t)nodes);
+	int* up = (int*)malloc(sizeof(int)*(size_t)nodes);
+	double* uval = (double*)malloc(sizeof(double)*(size_t)nodes);
+	char* seen = (char*)calloc((size_t)nodes, 1);
+	if (!down || !dval || !up || !uval || !seen) return TFO_NO_MEMORY;
+	for (int i = 0; i < nodes; ++i) {
+		down[i] = -1; dval[i] = 0.0; up[i] = -1; uval[i] = 0.0;
+		for (int b = row_offsets[i]; b < row_offsets[i+1]; ++b) {
+			const int j = columns[b];
+			if (j == i) continue;
+			const long long t = find_block(row_offsets, columns, j, i);
+			const double a = (t >= 0 ? values[t*4+3] : 0.0)-values[(size_t)b*4+3];
+			if (a > dval[i]) { dval[i] = a; down[i] = j; }
+		}
+	}
+	for (int i = 0; i < nodes; ++i) {
+		const int j = down[i];
+		if (j >= 0 && (up[j] < 0 || dval[i] > uval[j])) { up[j] = i; uval[j] = dval[i]; }
+	}
+	for (int i = 0; i < nodes; ++i)
+		if (down[i] >= 0 && up[down[i]] != i) down[i] = -1;
+	int lines = 0, at = 0;
+	line_offsets[0] = 0;
+	for (int h = 0; h < nodes; ++h) {
+		if (up[h] >= 0 || seen[h]) continue;
+		for (int i = h; i >= 0 && !seen[i]; i = down[i]) { seen[i] = 1; line_nodes[at++] = i; }
+		line_offsets[++lines] = at;
+	}
+	/* nodes on closed loops (every node has an upstream link): each loop becomes one line */
+	for (int h = 0; h < nodes; ++h) {
+		if (seen[h]) continue;
+		for (int i = h; i >= 0 && !seen[i]; i = down[i]) { seen[i] = 1; line_nodes[at++] = i; }
+		line_offsets[++lines] = at;
+	}
+	free(down); free(dval); free(up); free(uval); free(seen);
+	return lines;
+}
+
+/* 2x2 helpers (row-major). */
+static void inv2(const double* a, double* r)
+{
+	const double det = a[0]*a[3]-a[1]*a[2];
+	r[0] = a[3]/det; r[1] = -a[1]/det; r[2] = -a[2]/det; r[3] = a[0]/det;
+}
+static void mul2(const double* a, const double* b, double* r)
+{
+	r[0] = a[0]*b[0]+a[1]*b[2]; r[1] = a[0]*b[1]+a[1]*b[3];
+	r[2] = a[2]*b[0]+a[3]*b[2]; r[3] = a[2]*b[1]+a[3]*b[3];
+}
+
+/*
+ * Banded block LU (no pivoting) of every line's 2x2-block submatrix.  band_width[line] = the
+ * largest |position difference| of two coupled nodes of the line; band_offsets[line] = start of
+ * its storage in `factors` (4 doubles per block, m rows of 2w+1 blocks, block (p, q) at
+ * row p, slot q - p + w).  Returns the number of doubles `factors` needs when factors == NULL.
+ * After the call the band holds L (unit lower, below the diagonal) and U (on and above it), and
+ * the diagonal slots hold U_pp^{-1}.
+ */
+long long tfo_line_factors(int nodes, const int* row_offsets, const int* columns, const double* values,
+	int lines, const int* line_offsets, const int* line_nodes, int* band_width, long long* band_offsets,
+	double* factors)
+{
+	int* pos = (int*)malloc(sizeof(int)*(size_t)nodes);
+	int* line_of = (int*)malloc(sizeof(int)*(size_t)nodes);
+	if (!pos || !line_of) return TFO_NO_MEMORY;
+	for (int l = 0; l < lines; ++l)
+		for (int k = line_offsets[l]; k < line_offsets[l+1]; ++k) {
+			pos[line_nodes[k]] = k-line_offsets[l];
+			line_of[line_nodes[k]] = l;
+		}
+	long long total = 0;
+	for (int l = 0; l < lines; ++l) {
+		int w = 0;
+		for (int k = line_offsets[l]; k < line_offsets[l+1]; ++k) {
+			const int i = line_nodes[k];
+			for (int b = row_offsets[i]; b < row_offsets[i+1]; ++b)
+				if (line_of[columns[b]] == l) {
+					const int d = abs(pos[columns[b]]-pos[i]);
+					if (d > w) w = d;
+				}
+		}
+		band_width[l] = w;
+		band_offsets[l] = total;
+		total += 4LL*(line_offsets[l+1]-line_offsets[l])*(2*w+1);
+	}
+	if (!factors) { free(pos); free(line_of); return total; }
+	memset(factors, 0, sizeof(double)*(size_t)total);
+	for (int l = 0; l < lines; ++l) {
+		const int m = line_offsets[l+1]-line_offsets[l], w = band_width[l], s = 2*w+1;
+		double* B = factors+band_offsets[l];
+		for (int k = line_offsets[l]; k < line_offsets[l+1]; ++k) {
+			const int i = line_nodes[k], p = pos[i];
+			for (int b = row_offsets[i]; b < row_offsets[i+1]; ++b)
+				if (line_of[columns[b]] == l)
+					memcpy(B+4*((size_t)p*s+(pos[columns[b]]-p+w)), values+(size_t)b*4, 4*sizeof(double));
+		}
+		for (int p = 0; p < m; ++p) {
+			double dinv[4], lrp[4], t[4];
+			inv2(B+4*((size_t)p*s+w), dinv);
+			for (int r = p+1; r <= p+w && r < m; ++r) {
+				double* Arp = B+4*((size_t)r*s+(p-r+w));
+				mul2(Arp, dinv, lrp);
+				memcpy(Arp, lrp, sizeof(lrp));
+				for (int c = p+1; c <= p+w && c < m; ++c) {
+					double* Arc = B+4*((size_t)r*s+(c-r+w));
+					mul2(lrp, B+4*((size_t)p*s+(c-p+w)), t);
+					for (int e = 0; e < 4; ++e) Arc[e] -= t[e];
+				}
+			}
+			memcpy(B+4*((size_t)p*s+w), dinv, sizeof(dinv));
+		}
+	}
+	free(pos); free(line_of);
+	return total;
+}
+
+/* out = M^{-1} in: forward and backward substitution along every line. */
+void tfo_line_apply(int lines, const int* line_offsets, const int* line_nodes, const int* band_width,
+	const long long* band_offsets, const double* factors, const double* in, double* out)
+{
+#pragma omp parallel for schedule(dynamic, 16)
+	for (int l = 0; l < lines; ++l) {
+		const int m = line_offsets[l+1]-line_offsets[l], w = band_width[l], s = 2*w+1;
+		const double* B = factors+band_offsets[l];
+		const int* nodes = line_nodes+line_offsets[l];
+		double* y = (double*)malloc(sizeof(double)*2*(size_t)m);
+		for (int p = 0; p < m; ++p) {
+			double v0 = in[2*(size_t)nodes[p]], v1 = in[2*(size_t)nodes[p]+1];
+			for (int q = p-w > 0 ? p-w : 0; q < p; ++q) {
+				const double* L = B+4*((size_t)p*s+(q-p+w));
+				v0 -= L[0]*y[2*q]+L[1]*y[2*q+1];
+				v1 -= L[2]*y[2*q]+L[3]*y[2*q+1];
+			}
+			y[2*p] = v0; y[2*p+1] = v1;
+		}
+		for (int p = m-1; p >= 0; --p) {
+			double v0 = y[2*p], v1 = y[2*p+1];
+			for (int q = p+1; q <= p+w && q < m; ++q) {
+				const double* U = B+4*((size_t)p*s+(q-p+w));
+				v0 -= U[0]*y[2*q]+U[1]*y[2*q+1];
+				v1 -= U[2]*y[2*q]+U[3]*y[2*q+1];
+			}
+			const double* D = B+4*((size_t)p*s+w);
+			y[2*p] = D[0]*v0+D[1]*v1;
+			y[2*p+1] = D[2]*v0+D[3]*v1;
+		}
+		for (int p = 0; p < m; ++p) { out[2*(size_t)nodes[p]] = y[2*p]; out[2*(size_t)nodes[p]+1] = y[2*p+1]; }
+		free(y);
+	}
+}
+
+typedef struct {
+	int lines;
+	const int* line_offsets;
+	const int* line_nodes;
+	const int* band_width;
+	const long long* band_offsets;
+	const double* factors;
+} line_context;
+
+static void line_precond(const void* context, const double* in, double* out)
+{
+	const line_context* c = (const line_context*)context;
+	tfo_line_apply(c->lines, c->line_offsets, c->line_nodes, c->band_width, c->band_offsets, c->factors, in, out);
+}
+
+/* GMRES(restart) on the 2x2 transport system, left-preconditioned with the flow-line factors. */
+int tfo_transport_gmres_lines(int nodes, const int* row_offsets, const int* columns, const double* values,
+	int lines, const int* line_offsets, const int* line_nodes, const int* band_width, const long long* band_offsets,
+	const double* factors, const double* rhs, double* x, int restart, int maximum_iterations, double rtol,
+	double* residual_out)
+{
+	const line_context c = {lines, line_offsets, line_nodes, band_width, band_offsets, factors};
+	return gmres_precond_f(2, nodes, row_offsets, columns, NULL, values, rhs, x, restart, maximum_iterations, rtol,
+		residual_out, NULL, line_precond, &c);
 }
 
 int tfo_max_threads(void)

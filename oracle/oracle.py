@@ -66,6 +66,13 @@ def lib():
         L.tfo_max_threads.restype = C.c_int
         L.tfo_transport_element.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
         L.tfo_transport_spmv.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp]
+        _lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+        L.tfo_flow_lines.argtypes = [C.c_int, _ip, _ip, _dp, _ip, _ip]
+        L.tfo_line_factors.argtypes = [C.c_int, _ip, _ip, _dp, C.c_int, _ip, _ip, _ip, _lp, C.c_void_p]
+        L.tfo_line_factors.restype = C.c_longlong
+        L.tfo_line_apply.argtypes = [C.c_int, _ip, _ip, _ip, _lp, _dp, _dp, _dp]
+        L.tfo_transport_gmres_lines.argtypes = [C.c_int, _ip, _ip, _dp, C.c_int, _ip, _ip, _ip, _lp, _dp, _dp, _dp,
+                                                C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double)]
         L.tfo_transport_gmres.argtypes = [C.c_int, _ip, _ip, _ip, _dp, _dp, _dp, C.c_int, C.c_int, C.c_double,
                                           C.POINTER(C.c_double), C.POINTER(C.c_int)]
         L.tfo_transport_assemble.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip, _up, _dp, _dp, _ip, _ip, _ip,
@@ -457,6 +464,46 @@ def transport_gmres(row_offsets, columns, diagonal, values, rhs, x0, restart=50,
                                    values, np.ascontiguousarray(rhs, np.float64), x, restart, maxit, rtol,
                                    C.byref(res), C.byref(singular))
     return x, it, res.value
+
+
+class FlowLines:
+    """Flow-line preconditioner of the 2x2 transport matrix (tfo_flow_lines / tfo_line_factors)."""
+
+    def __init__(self, row_offsets, columns, values):
+        self.row_offsets = np.ascontiguousarray(row_offsets, np.int32)
+        self.columns = np.ascontiguousarray(columns, np.int32)
+        self.values = np.ascontiguousarray(values, np.float64)
+        self.nodes = len(self.row_offsets) - 1
+        self.line_offsets = np.zeros(self.nodes + 1, np.int32)
+        self.line_nodes = np.zeros(self.nodes, np.int32)
+        L = lib()
+        self.lines = L.tfo_flow_lines(self.nodes, self.row_offsets, self.columns, self.values, self.line_offsets,
+                                      self.line_nodes)
+        if self.lines < 0:
+            raise RuntimeError("flow lines failed")
+        self.line_offsets = self.line_offsets[:self.lines + 1].copy()
+        self.band_width = np.zeros(self.lines, np.int32)
+        self.band_offsets = np.zeros(self.lines, np.int64)
+        size = L.tfo_line_factors(self.nodes, self.row_offsets, self.columns, self.values, self.lines,
+                                  self.line_offsets, self.line_nodes, self.band_width, self.band_offsets, None)
+        self.factors = np.zeros(size)
+        L.tfo_line_factors(self.nodes, self.row_offsets, self.columns, self.values, self.lines, self.line_offsets,
+                           self.line_nodes, self.band_width, self.band_offsets, _ptr(self.factors))
+
+    def apply(self, r):
+        out = np.zeros(2 * self.nodes)
+        lib().tfo_line_apply(self.lines, self.line_offsets, self.line_nodes, self.band_width, self.band_offsets,
+                             self.factors, np.ascontiguousarray(r, np.float64), out)
+        return out
+
+    def gmres(self, rhs, x0, restart=50, maxit=10000, rtol=1e-8):
+        x = np.array(x0, np.float64)
+        res = C.c_double()
+        it = lib().tfo_transport_gmres_lines(self.nodes, self.row_offsets, self.columns, self.values, self.lines,
+                                             self.line_offsets, self.line_nodes, self.band_width, self.band_offsets,
+                                             self.factors, np.ascontiguousarray(rhs, np.float64), x, restart, maxit,
+                                             rtol, C.byref(res))
+        return x, it, res.value
 
 
 def max_threads() -> int:
