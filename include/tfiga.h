@@ -494,6 +494,16 @@ int tfiga_transport_resolve_boundaries(int64_t nodes, const int32_t* labels, con
 int tfiga_resolve_legacy_boundaries(int64_t nodes, const int32_t* labels, const double* reference_velocity,
 	const tfiga_transport_params* params, const char* case_config_path, int32_t* velocity_mask, double* velocity,
 	int32_t* pressure_mask, double* pressure, int32_t* transport_mask, double* n0, double* nplus, int64_t* counts);
+/* The flow-line preconditioner's host construction for a 2x2 block system given by host arrays
+ * (row_offsets [nodes+1], sorted columns, values [4*blocks]): lines chained along the largest
+ * antisymmetric coupling of the second field (a_ij = L++_ji - L++_ij > 0), then the banded 2x2-block
+ * LU (no pivoting) of every line's system.  Outputs (any may be NULL): line_offsets [lines+1],
+ * line_nodes [nodes], band_width and band_offsets [lines], factors [*factor_count]; *lines and
+ * *factor_count give the sizes (call once with NULL arrays to size them).  No counterpart in the
+ * reference (it preconditions with block-Jacobi).  Host only. */
+int tfiga_transport_flow_lines(int64_t nodes, const int32_t* row_offsets, const int32_t* columns,
+	const double* values, int32_t* line_offsets, int32_t* line_nodes, int32_t* band_width, int64_t* band_offsets,
+	double* factors, int32_t* lines, int64_t* factor_count);
 /* Assembles L and P from the nodal velocity [3*nodes], applies the boundary
  * rows of the constrained[nodes] mask and sets the boundary values n0/nplus
  * [nodes] into the zero initial state (iga_cuda.cu:664-679).  Host or device

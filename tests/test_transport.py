@@ -363,3 +363,21 @@ def test_flow_line_preconditioner_oracle(small_tube):
                                 np.zeros_like(rhs), rtol=1e-12)[0], lines.gmres(rhs, np.zeros_like(rhs), rtol=1e-12)[0]):
         for f in (0, 1):
             assert np.linalg.norm(x[f::2] - want[f::2]) <= 1e-9 * np.linalg.norm(want[f::2])
+
+
+def test_flow_line_host_builder_matches_the_oracle(api, small_tube):
+    """The library's host construction of the flow lines and their banded factors
+    (tfiga_transport_flow_lines) equals the oracle's restatement."""
+    from tubularflowiga_b200 import meshgen
+    tube = meshgen.straight_tube(1.5e-3, 7.5e-3, core=8, ring=2, layers=12)
+    flat = tube.mesh
+    params = {"diffusion": 1e-9, "vplus": 1.0, "kplus": 1.0, "kminus": 0.1, "detach_plus": 0.5, "dt": 2e-3,
+              "artificial_diffusion": 1e-6}
+    pattern = O.Pattern(flat.nodes, flat.element_offsets, flat.connectivity)
+    mask = (tube.labels == 1).astype(np.int32)
+    left, _ = O.transport_assemble(flat, pattern, 0.3 * tube.profile + 0.01, params, mask)
+    want = O.FlowLines(pattern.row_offsets, pattern.columns, left)
+    got = api.transport_flow_lines(pattern.row_offsets, pattern.columns, left)
+    for key in ("line_offsets", "line_nodes", "band_width", "band_offsets"):
+        assert np.array_equal(got[key], getattr(want, key)), key
+    assert np.allclose(got["factors"], want.factors, rtol=1e-14, atol=1e-14 * np.abs(want.factors).max())

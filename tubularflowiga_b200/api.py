@@ -211,6 +211,9 @@ SIGNATURES = {
                                                                                   C.POINTER(C.c_int32), C.c_void_p]),
     "tfiga_resolve_legacy_boundaries": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(TransportParams),
                                                   C.c_char_p] + [C.c_void_p] * 8),
+    "tfiga_transport_flow_lines": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_int64)]),
     "tfiga_transport_create": (C.c_int, [C.c_void_p, C.POINTER(TransportParams), C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     "tfiga_transport_destroy": (C.c_int, [C.c_void_p]),
@@ -647,6 +650,25 @@ def resolve_legacy_boundaries(labels, reference_velocity, params: TransportParam
                                                 *[_p(out[k]) for k in ("velocity_mask", "velocity", "pressure_mask",
                                                                        "pressure", "transport_mask", "n0", "nplus",
                                                                        "counts")]))
+    return out
+
+
+def transport_flow_lines(row_offsets, columns, values) -> dict:
+    """Host construction of the flow-line preconditioner of a 2x2 block system (tfiga_transport_flow_lines)."""
+    ro = np.ascontiguousarray(row_offsets, np.int32)
+    co = np.ascontiguousarray(columns, np.int32)
+    va = np.ascontiguousarray(values, np.float64)
+    n = len(ro) - 1
+    lines, count = C.c_int32(), C.c_int64()
+    L = lib()
+    check(L.tfiga_transport_flow_lines(n, _p(ro), _p(co), _p(va), None, None, None, None, None, C.byref(lines),
+                                       C.byref(count)))
+    out = {"line_offsets": np.zeros(lines.value + 1, np.int32), "line_nodes": np.zeros(n, np.int32),
+           "band_width": np.zeros(lines.value, np.int32), "band_offsets": np.zeros(lines.value, np.int64),
+           "factors": np.zeros(count.value)}
+    check(L.tfiga_transport_flow_lines(n, _p(ro), _p(co), _p(va), _p(out["line_offsets"]), _p(out["line_nodes"]),
+                                       _p(out["band_width"]), _p(out["band_offsets"]), _p(out["factors"]),
+                                       C.byref(lines), C.byref(count)))
     return out
 
 

@@ -1,6 +1,7 @@
 // extern "C" boundary: every entry point converts exceptions into a status
 // code plus a thread-local message (tfiga_last_error).
 #include "case_input.hpp"
+#include "flow_lines.hpp"
 #include "learned.hpp"
 #include "mesh.hpp"
 #include "ns.hpp"
@@ -597,6 +598,23 @@ int tfiga_transport_resolve_boundaries(int64_t nodes, const int32_t* labels, con
 		nullptr, nullptr, nullptr, nullptr, constrained, n0, nplus, counts);
 	if (status == TFIGA_OK && transport_nodes) *transport_nodes = counts[2];
 	return status;
+}
+
+int tfiga_transport_flow_lines(int64_t nodes, const int32_t* row_offsets, const int32_t* columns,
+	const double* values, int32_t* line_offsets, int32_t* line_nodes, int32_t* band_width, int64_t* band_offsets,
+	double* factors, int32_t* lines, int64_t* factor_count)
+{
+	return Guard([&] {
+		Require(nodes > 0 && nodes < INT32_MAX && row_offsets && columns && values, "null argument");
+		const tfiga::FlowLineFactors f = tfiga::BuildFlowLines((int32_t)nodes, row_offsets, columns, values);
+		if (lines) *lines = f.lines();
+		if (factor_count) *factor_count = (int64_t)f.factors.size();
+		if (line_offsets) std::copy(f.line_offsets.begin(), f.line_offsets.end(), line_offsets);
+		if (line_nodes) std::copy(f.line_nodes.begin(), f.line_nodes.end(), line_nodes);
+		if (band_width) std::copy(f.band_width.begin(), f.band_width.end(), band_width);
+		if (band_offsets) std::copy(f.band_offsets.begin(), f.band_offsets.end(), band_offsets);
+		if (factors) std::copy(f.factors.begin(), f.factors.end(), factors);
+	});
 }
 
 int tfiga_transport_create(tfiga_mesh* mesh, const tfiga_transport_params* params, const double* velocity,
