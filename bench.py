@@ -436,6 +436,8 @@ def run_transport(args, world, rank, local):
 
     def make_params(precision):
         return api.transport_params(steps=total_steps, restart=args.transport_restart, precision=precision,
+                                    preconditioner=(api.TRANSPORT_FLOW_LINES if args.transport_preconditioner
+                                                    == "flow-lines" else api.TRANSPORT_BLOCK_JACOBI),
                                     **TRANSPORT)
 
     params = make_params(api.MIXED if fp32 else api.FP64)
@@ -555,8 +557,8 @@ def run_transport(args, world, rank, local):
                 if args.transport_mesh == "c3" else "synthetic (seeded generator; Poiseuille velocity)",
         "config": {"workload": "two-species transport on the " + desc, "elements": tube.mesh.elements, "nodes": n,
                    "block_nonzeros": mesh.blocks, "coefficients": TRANSPORT,
-                   "solver": ("backward Euler, constant L and P assembled once; block-Jacobi GMRES(%d) rtol 1e-8 "
-                              "warm-started; %s" % (args.transport_restart,
+                   "solver": ("backward Euler, constant L and P assembled once; %s GMRES(%d) rtol 1e-8 "
+                              "warm-started; %s" % (args.transport_preconditioner, args.transport_restart,
                                                     "FP32 copy of L in the Arnoldi SpMV, FP64 vectors, block "
                                                     "inverse and true residual" if fp32 else "FP64")),
                    "l2": "inputs larger than L2 (L %.2f GB)" % (mesh.blocks * 32 / 1e9),
@@ -603,6 +605,8 @@ def main():
                     help="transport workload: FP32 copy of L for the Arnoldi SpMV (FP64 true residual); with fp32 "
                          "the FP64 solver is timed too (fp64_gpu) unless --no-fp64-leg")
     ap.add_argument("--transport-restart", type=int, default=50, help="transport workload: GMRES restart")
+    ap.add_argument("--transport-preconditioner", default="block-jacobi", choices=["block-jacobi", "flow-lines"],
+                    help="transport workload: the reference's block-Jacobi or the flow-line factors")
     ap.add_argument("--transport-mesh", default="c3", choices=["c3", "c2-100"],
                     help="transport workload mesh: c3 with the velocity of one Navier-Stokes step, or the "
                          "12,800-element tube section with its Poiseuille profile at 0.15 m/s mean (profiling case)")

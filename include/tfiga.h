@@ -458,7 +458,14 @@ typedef struct tfiga_transport_params {
 	 * block inverse, the vectors and the true residual of every restart (the
 	 * stopping test) stay FP64. */
 	int32_t precision;
+	/* TFIGA_TRANSPORT_BLOCK_JACOBI (the reference's) or TFIGA_TRANSPORT_FLOW_LINES: exact solves
+	 * along flow lines read from L (tfiga_transport_flow_lines), factored once per handle. */
+	int32_t preconditioner;
+	int32_t reserved;
 } tfiga_transport_params;
+
+#define TFIGA_TRANSPORT_BLOCK_JACOBI 0
+#define TFIGA_TRANSPORT_FLOW_LINES 1
 
 /* Totals of one tfiga_transport_step call (the `transport step=` and
  * `transport_cuda` log lines, iga_cuda.cu:702-731). */

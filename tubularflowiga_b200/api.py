@@ -116,10 +116,15 @@ class TransportParams(C.Structure):
                 ("detach_minus", C.c_double), ("dt", C.c_double), ("steps", C.c_int32), ("restart", C.c_int32),
                 ("n0_bc", C.c_double), ("nplus_bc", C.c_double), ("nminus_bc", C.c_double),
                 ("artificial_diffusion", C.c_double), ("gmres_rtol", C.c_double),
-                ("gmres_max_iterations", C.c_int32), ("precision", C.c_int32)]
+                ("gmres_max_iterations", C.c_int32), ("precision", C.c_int32), ("preconditioner", C.c_int32),
+                ("reserved", C.c_int32)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+TRANSPORT_BLOCK_JACOBI = 0
+TRANSPORT_FLOW_LINES = 1
 
 
 class TransportReport(C.Structure):

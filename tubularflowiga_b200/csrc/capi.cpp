@@ -627,6 +627,8 @@ int tfiga_transport_create(tfiga_mesh* mesh, const tfiga_transport_params* param
 		Require(params->gmres_rtol > 0.0 && params->gmres_max_iterations > 0, "GMRES tolerance and limit must be positive");
 		Require(params->precision == TFIGA_PRECISION_FP64 || params->precision == TFIGA_PRECISION_MIXED,
 			"transport precision must be TFIGA_PRECISION_FP64 or TFIGA_PRECISION_MIXED");
+		Require(params->preconditioner == TFIGA_TRANSPORT_BLOCK_JACOBI
+			|| params->preconditioner == TFIGA_TRANSPORT_FLOW_LINES, "unknown transport preconditioner");
 		tfiga::RequireDevice();
 		const tfiga::TransportCoefficients c{params->diffusion, params->vplus, params->kplus, params->kminus,
 			params->detach_plus, params->dt, params->artificial_diffusion};
@@ -634,7 +636,8 @@ int tfiga_transport_create(tfiga_mesh* mesh, const tfiga_transport_params* param
 		handle->mesh = mesh;
 		handle->params = *params;
 		handle->solver = std::make_unique<tfiga::TransportSolver>(*mesh->mesh, c, velocity, constrained, n0, nplus,
-			params->restart, params->precision == TFIGA_PRECISION_MIXED);
+			params->restart, params->precision == TFIGA_PRECISION_MIXED,
+			params->preconditioner == TFIGA_TRANSPORT_FLOW_LINES);
 		*out = handle.release();
 	});
 }

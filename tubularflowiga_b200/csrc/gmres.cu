@@ -373,7 +373,12 @@ void Gmres::Step(const DevicePatternView& pattern, const T* values, int j)
 {
 	const int* stop = state_.get();
 	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
-	if (fields_ == 2)
+	if (fields_ == 2 && line_on_) {
+		LaunchSpmvBlockJacobi2(pattern, values, static_cast<const double*>(nullptr), V_.get()+(size_t)j*n_,
+			scale_.get()+j, tmp_.get(), stop, stream_);
+		LaunchLineApply(line_, tmp_.get(), w_.get(), stop, stream_);
+		launches_ += 1;
+	} else if (fields_ == 2)
 		LaunchSpmvBlockJacobi2(pattern, values, inverse_.get(), V_.get()+(size_t)j*n_, scale_.get()+j, w_.get(),
 			stop, stream_);
 	else
@@ -549,7 +554,8 @@ double Gmres::TrueResidual(const DevicePatternView& pattern, const double* value
 	else LaunchSpmv(pattern, values, x, tmp_.get(), stream_);
 	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), r_.get());
 	LaunchCheck("ResidualKernel");
-	if (fields_ == 2) LaunchApplyBlockInverse2(nodes_, inverse_.get(), r_.get(), V_.get(), stream_);
+	if (fields_ == 2 && line_on_) LaunchLineApply(line_, r_.get(), V_.get(), nullptr, stream_);
+	else if (fields_ == 2) LaunchApplyBlockInverse2(nodes_, inverse_.get(), r_.get(), V_.get(), stream_);
 	else LaunchApplyBlockInverse(nodes_, inverse_.get(), r_.get(), V_.get(), stream_);
 	LaunchNorm(n_, V_.get(), norm_partial_.get(), scalar_.get(), stream_);
 	launches_ += 5;

@@ -50,6 +50,12 @@ public:
 		double rtol, int max_iterations, Amg& preconditioner, long long* launches, bool fp64_basis = false);
 	int restart() const { return restart_; }
 	int fields() const { return fields_; }
+	// 2x2 blocks: precondition Solve with the flow-line factors instead of block-Jacobi (null: off).
+	void set_line_preconditioner(const LinePreconditionerView* view)
+	{
+		line_on_ = view != nullptr;
+		if (view) line_ = *view;
+	}
 	// Learned stage added to the AMG application in SolveFlexible (null: AMG only).
 	void set_learned(LearnedPreconditioner* learned) { learned_ = learned; }
 	LearnedPreconditioner* learned() const { return learned_; }
@@ -75,6 +81,8 @@ private:
 
 	int nodes_, fields_, n_, restart_, blocks_;
 	unsigned singular_count_ = 0;     // singular diagonal blocks of the last block-inverse build
+	bool line_on_ = false;            // flow-line preconditioner (2x2 blocks)
+	LinePreconditionerView line_;
 	int update_blocks_ = 0;           // CTAs of the basis update (one per 32 entry pairs)
 	int chunk_;
 	size_t finalize_smem_ = 0;

@@ -97,6 +97,19 @@ void LaunchSpmvBlockJacobi2(const DevicePatternView& pattern, const T* values, c
 void LaunchBlockInverse2(const DevicePatternView& pattern, const double* values, double* inverse,
 	unsigned int* singular, cudaStream_t stream);
 void LaunchApplyBlockInverse2(int nodes, const double* inverse, const double* x, double* y, cudaStream_t stream);
+// Device view of the flow-line factors (flow_lines.hpp): y = M^{-1} x by a forward and a backward
+// substitution along every line, one thread per line (x and y must not overlap; stop: the GMRES
+// early-out flag, may be null).
+struct LinePreconditionerView {
+	int lines = 0;
+	const int32_t* line_offsets = nullptr;
+	const int32_t* line_nodes = nullptr;
+	const int32_t* band_width = nullptr;
+	const int64_t* band_offsets = nullptr;
+	const double* factors = nullptr;
+};
+void LaunchLineApply(const LinePreconditionerView& view, const double* x, double* y, const int* stop,
+	cudaStream_t stream);
 
 void LaunchLiftDirichlet(int count, const int32_t* nodes, const int32_t* vmask, const int32_t* pmask,
 	const double* velocity, const double* pressure, double* state, cudaStream_t stream);

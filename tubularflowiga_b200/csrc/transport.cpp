@@ -1,13 +1,16 @@
 // Host side of the two-species transport solver (iga_cuda.cu:621-732).
 #include "transport.hpp"
 
+#include "flow_lines.hpp"
+
 #include <cmath>
 #include <string>
 
 namespace tfiga {
 
 TransportSolver::TransportSolver(Mesh& mesh, const TransportCoefficients& coefficients, const double* velocity,
-	const int32_t* constrained, const double* n0, const double* nplus, int restart, bool fp32_krylov)
+	const int32_t* constrained, const double* n0, const double* nplus, int restart, bool fp32_krylov,
+	bool flow_lines)
 	: mesh_(mesh), nodes_((int)mesh.nodes()), gmres_((int)mesh.nodes(), restart, mesh.stream(), 2)
 {
 	if (!(coefficients.dt > 0.0) || !std::isfinite(coefficients.dt)) Fail(-1, "transport dt must be positive");
@@ -62,6 +65,33 @@ TransportSolver::TransportSolver(Mesh& mesh, const TransportCoefficients& coeffi
 	assembly_ms_ = ms;
 	launches_ += 3;
 	gmres_.set_profiler(&profiler_);
+	if (flow_lines) {
+		// Built once on the host from L after the boundary rows (L is constant over the steps).
+		std::vector<double> values((size_t)pattern.blocks*4);
+		left_.Download(values.data(), values.size(), s);
+		CudaCheck(cudaStreamSynchronize(s), "flow-line matrix");
+		const HostPattern& hp = mesh_.pattern();
+		const FlowLineFactors f = BuildFlowLines(nodes_, hp.row_offsets.data(), hp.columns.data(), values.data());
+		line_offsets_.Allocate(f.line_offsets.size());
+		line_offsets_.Upload(f.line_offsets.data(), f.line_offsets.size(), s);
+		line_nodes_.Allocate(f.line_nodes.size());
+		line_nodes_.Upload(f.line_nodes.data(), f.line_nodes.size(), s);
+		band_width_.Allocate(f.band_width.size());
+		band_width_.Upload(f.band_width.data(), f.band_width.size(), s);
+		band_offsets_.Allocate(f.band_offsets.size());
+		band_offsets_.Upload(f.band_offsets.data(), f.band_offsets.size(), s);
+		line_factors_.Allocate(f.factors.size());
+		line_factors_.Upload(f.factors.data(), f.factors.size(), s);
+		CudaCheck(cudaStreamSynchronize(s), "flow-line factors");
+		LinePreconditionerView view;
+		view.lines = f.lines();
+		view.line_offsets = line_offsets_.get();
+		view.line_nodes = line_nodes_.get();
+		view.band_width = band_width_.get();
+		view.band_offsets = band_offsets_.get();
+		view.factors = line_factors_.get();
+		gmres_.set_line_preconditioner(&view);
+	}
 }
 
 TransportStepResult TransportSolver::Step(double rtol, int max_iterations)

@@ -247,6 +247,47 @@ __global__ void __launch_bounds__(256) SpmvBlockJacobi2Kernel(DevicePatternView 
 	}
 }
 
+// Flow-line preconditioner apply: thread per line, forward substitution with the unit lower band,
+// backward substitution with the upper band and the inverted diagonal blocks; the forward result
+// is kept in y at the line's nodes (every node is on exactly one line).
+__global__ void __launch_bounds__(128) LineApplyKernel(LinePreconditionerView v, const double* __restrict__ x,
+	double* __restrict__ y, const int* __restrict__ stop)
+{
+	if (stop != nullptr && *stop) return;
+	const int l = blockIdx.x*blockDim.x+threadIdx.x;
+	if (l >= v.lines) return;
+	const int lo = v.line_offsets[l], m = v.line_offsets[l+1]-lo, w = v.band_width[l], s = 2*w+1;
+	const double* B = v.factors+v.band_offsets[l];
+	const int32_t* nodes = v.line_nodes+lo;
+	for (int p = 0; p < m; ++p) {
+		const size_t i = 2*(size_t)nodes[p];
+		double v0 = x[i], v1 = x[i+1];
+		for (int q = p-w > 0 ? p-w : 0; q < p; ++q) {
+			const double* L = B+4*((size_t)p*s+(q-p+w));
+			const size_t j = 2*(size_t)nodes[q];
+			const double y0 = y[j], y1 = y[j+1];
+			v0 -= L[0]*y0+L[1]*y1;
+			v1 -= L[2]*y0+L[3]*y1;
+		}
+		y[i] = v0;
+		y[i+1] = v1;
+	}
+	for (int p = m-1; p >= 0; --p) {
+		const size_t i = 2*(size_t)nodes[p];
+		double v0 = y[i], v1 = y[i+1];
+		for (int q = p+1; q <= p+w && q < m; ++q) {
+			const double* U = B+4*((size_t)p*s+(q-p+w));
+			const size_t j = 2*(size_t)nodes[q];
+			const double x0 = y[j], x1 = y[j+1];
+			v0 -= U[0]*x0+U[1]*x1;
+			v1 -= U[2]*x0+U[3]*x1;
+		}
+		const double* D = B+4*((size_t)p*s+w);
+		y[i] = D[0]*v0+D[1]*v1;
+		y[i+1] = D[2]*v0+D[3]*v1;
+	}
+}
+
 unsigned Grid(long long n, int per_block) { return (unsigned)((n+per_block-1)/per_block); }
 
 } // namespace
@@ -291,6 +332,14 @@ void LaunchSpmvBlockJacobi2(const DevicePatternView& p, const T* values, const d
 	if (p.nodes == 0) return;
 	SpmvBlockJacobi2Kernel<T><<<Grid(p.nodes, 8), 256, 0, stream>>>(p, values, inverse, x, scale, y, stop);
 	LaunchCheck("SpmvBlockJacobi2Kernel");
+}
+
+void LaunchLineApply(const LinePreconditionerView& view, const double* x, double* y, const int* stop,
+	cudaStream_t stream)
+{
+	if (view.lines == 0) return;
+	LineApplyKernel<<<Grid(view.lines, 128), 128, 0, stream>>>(view, x, y, stop);
+	LaunchCheck("LineApplyKernel");
 }
 
 template void LaunchSpmvBlockJacobi2<double>(const DevicePatternView&, const double*, const double*, const double*,

@@ -52,9 +52,12 @@ public:
 	// velocity [3 nodes], constrained [nodes] (nonzero: Dirichlet node), n0 / nplus [nodes]:
 	// host or device pointers.  Assembles both matrices, applies the boundary rows and sets the
 	// boundary values into the zero initial state.  fp32_krylov: an FP32 copy of L serves the SpMV
-	// of the Arnoldi process (the true residual of every restart stays FP64).
+	// of the Arnoldi process (the true residual of every restart stays FP64).  flow_lines: the
+	// GMRES is preconditioned with the flow-line factors of L (flow_lines.hpp) instead of
+	// block-Jacobi.
 	TransportSolver(Mesh& mesh, const TransportCoefficients& coefficients, const double* velocity,
-		const int32_t* constrained, const double* n0, const double* nplus, int restart, bool fp32_krylov = false);
+		const int32_t* constrained, const double* n0, const double* nplus, int restart, bool fp32_krylov = false,
+		bool flow_lines = false);
 	TransportSolver(const TransportSolver&) = delete;
 	TransportSolver& operator=(const TransportSolver&) = delete;
 
@@ -82,6 +85,9 @@ private:
 	double assembly_ms_ = 0.0;
 	DeviceArray<double> left_, previous_, current_, next_, rhs_, n0_, nplus_, scratch_;
 	DeviceArray<float> left32_;        // FP32 copy of L (fp32_krylov)
+	DeviceArray<int32_t> line_offsets_, line_nodes_, band_width_;   // flow-line factors (flow_lines)
+	DeviceArray<int64_t> band_offsets_;
+	DeviceArray<double> line_factors_;
 	DeviceArray<int32_t> constrained_;
 	int constrained_count_ = 0;
 	Gmres gmres_;
