@@ -120,7 +120,7 @@ size_t tfiga_last_error(char* buffer, size_t capacity)
 
 const char* tfiga_version(void)
 {
-	return "tubularflowiga-b200 0.1 sm_100a fp64";
+	return "tubularflowiga-b200 0.2 sm_100a (FP64; tcgen05 split-BF16 tangent)";
 }
 
 int tfiga_mesh_create(const tfiga_mesh_desc* desc, tfiga_mesh** out)
