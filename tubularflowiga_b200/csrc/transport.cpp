@@ -22,7 +22,7 @@ TransportSolver::TransportSolver(Mesh& mesh, const TransportCoefficients& coeffi
 	previous_.Allocate((size_t)pattern.blocks*4);
 	current_.Allocate(2*n); next_.Allocate(2*n); rhs_.Allocate(2*n);
 	n0_.Allocate(n); nplus_.Allocate(n);
-	scratch_.Allocate(2*296+2);   // LaunchNorm: 296 two-entry partial sums, then (norm, sum)
+	scratch_.Allocate((size_t)PartialSlots()+2);   // LaunchNorm: the partial sums, then (norm, sum)
 	left_.Zero(s); previous_.Zero(s); current_.Zero(s); next_.Zero(s); rhs_.Zero(s);
 	n0_.Upload(n0, n, s);
 	nplus_.Upload(nplus, n, s);
@@ -145,10 +145,11 @@ void TransportSolver::Matrices(double* left, double* previous)
 
 double TransportSolver::StateNorm()
 {
-	LaunchNorm(2LL*nodes_, current_.get(), scratch_.get(), scratch_.get()+2*296, mesh_.stream());
+	LaunchNorm(2LL*nodes_, current_.get(), scratch_.get(), scratch_.get()+PartialSlots(), mesh_.stream());
 	launches_ += 2;
 	double norm[2] = {0.0, 0.0};
-	CudaCheck(cudaMemcpyAsync(norm, scratch_.get()+2*296, 2*sizeof(double), cudaMemcpyDeviceToHost, mesh_.stream()),
+	CudaCheck(cudaMemcpyAsync(norm, scratch_.get()+PartialSlots(), 2*sizeof(double), cudaMemcpyDeviceToHost,
+		mesh_.stream()),
 		"transport norm");
 	CudaCheck(cudaStreamSynchronize(mesh_.stream()), "transport norm");
 	return norm[0];
