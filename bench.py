@@ -376,19 +376,13 @@ def flow_velocity(api, mesh, tube, wave):
     s0 = api.initial_state(vmask, velocity_at(0.0))
     ns.set_state(s0, s0)
     outlets = [api.Outlet(**m.as_dict()) for m in outlet_models("c3")]
-    api.check(api.lib().tfiga_ns_set_dirichlet_values(ns._h, _host_ptr(velocity_at(DT).ravel()), None))
+    inlet = np.ascontiguousarray(velocity_at(DT).ravel(), np.float64)
+    api.check(api.lib().tfiga_ns_set_dirichlet_values(ns._h, api.C.c_void_p(inlet.ctypes.data), None))
     ns.commit_step()
     outlet_step(ns, outlets, "newton")
     v = ns.get_state().reshape(-1, 4)[:, :3].copy()
     ns.close()
     return v
-
-
-def _host_ptr(a):
-    from tubularflowiga_b200 import api
-    a = np.ascontiguousarray(a, np.float64)
-    _host_ptr.keep = a
-    return api.C.c_void_p(a.ctypes.data)
 
 
 def transport_cpu_reference(mesh, left, previous, state, iterations_per_step, budget_iterations=30):
