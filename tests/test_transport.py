@@ -381,3 +381,42 @@ def test_flow_line_host_builder_matches_the_oracle(api, small_tube):
     for key in ("line_offsets", "line_nodes", "band_width", "band_offsets"):
         assert np.array_equal(got[key], getattr(want, key)), key
     assert np.allclose(got["factors"], want.factors, rtol=1e-14, atol=1e-14 * np.abs(want.factors).max())
+
+
+@requires_ref
+def test_simulation_config_root_errors_match_the_reference(api, tmp_path, small_tube):
+    """Root-level validation of simulation_config.json (schema versions, dimension / geometry / mesh,
+    unknown root keys, time step, waveform units): the same files fail in this parser and in the
+    reference's own ReadSimulationConfiguration, with the reference's message."""
+    from tubularflowiga_b200 import meshgen
+    t = small_tube
+    base = meshgen.simulation_config(1060.0, 3.5e-3, 2e-3, 3, 1.0, transient=True,
+                                     waveform=meshgen.fourier_waveform(1))
+
+    def variant(edit):
+        cfg = json.loads(json.dumps(base))
+        edit(cfg)
+        return cfg
+
+    bad = [
+        variant(lambda c: c.pop("dimension")),
+        variant(lambda c: c.update(dimension="2d")),
+        variant(lambda c: c.update(schema_version=5)),
+        variant(lambda c: c.update(schema_version=2)),
+        variant(lambda c: c.update(schema_version=4)),
+        variant(lambda c: c.update(colour="blue")),
+        variant(lambda c: c.update(geometry={"kind": "swc_network"})),
+        variant(lambda c: c["temporal_functions"][0].pop("units")),
+        variant(lambda c: c["temporal_functions"][0].update(units="")),
+        variant(lambda c: c["time"].update(dt=0.0)),
+        variant(lambda c: c.pop("schema_version")),
+    ]
+    for k, cfg in enumerate(bad):
+        path = tmp_path / f"bad{k}" / "simulation_config.json"
+        path.parent.mkdir()
+        path.write_text(json.dumps(cfg))
+        with pytest.raises(RuntimeError) as ref_error:
+            O.ref_flow_boundaries(path, t.labels, t.profile, 0.0)
+        with pytest.raises(api.TfigaError) as err:
+            api.resolve_flow_boundaries(path, t.labels, t.profile, 0.0)
+        assert str(ref_error.value) in str(err.value), (k, str(ref_error.value), str(err.value))

@@ -27,6 +27,58 @@ double OptionalNumber(const json::Value& object, const char* key, double fallbac
 	return v ? v->Number(context+"."+key) : fallback;
 }
 
+// The reference's generic JSON validation helpers (include/CaseConfig.hpp:230-270), defined with
+// the case_config.json reader below; its simulation_config.json parser reuses them, messages included.
+void KnownKeys(const json::Value& object, std::initializer_list<const char*> allowed, const std::string& context);
+int CaseInteger(const json::Value& v, const std::string& context);
+const std::string& CaseString(const json::Value& v, const std::string& context);
+
+[[noreturn]] void SimulationFail(const std::string& message) { Fail(-4, "simulation_config.json: "+message); }
+
+// Root structure checks of ParseSimulationConfiguration (include/SimulationConfig.hpp:263-287,
+// 324-347): known root keys, schema 2/3/4 with its dimension / geometry / mesh rules, a positive
+// time step, named temporal functions with non-empty units.  The contents of geometry and mesh are
+// not read here.
+void ValidateSimulationRoot(const json::Value& root)
+{
+	KnownKeys(root, {"schema_version", "dimension", "geometry", "mesh", "fields", "equation_systems", "boundaries",
+		"time", "temporal_functions", "velocity_sources", "physiology", "simulation_scope", "perfusate",
+		"external_circuit", "coupling"}, "root");
+	const auto* version = root.Find("schema_version");
+	if (!version) SimulationFail("root requires 'schema_version'");
+	const int schema = CaseInteger(*version, "schema_version");
+	const auto* dimension = root.Find("dimension");
+	if (schema == 2) {
+		if (dimension || root.Find("geometry") || root.Find("mesh"))
+			SimulationFail("schema_version 2 does not accept dimension, geometry, or mesh");
+	} else if (schema == 3) {
+		if (!dimension || CaseString(*dimension, "dimension") != "3d")
+			SimulationFail("schema_version 3 3d configuration requires dimension '3d'");
+		if (root.Find("geometry") || root.Find("mesh"))
+			SimulationFail("schema_version 3 3d configuration does not accept geometry or mesh");
+	} else if (schema == 4) {
+		if (!dimension || CaseString(*dimension, "dimension") != "3d")
+			SimulationFail("schema_version 4 requires dimension '3d'");
+		if (!root.Find("geometry")) SimulationFail("root requires 'geometry'");
+		if (!root.Find("mesh")) SimulationFail("root requires 'mesh'");
+	} else {
+		SimulationFail("supported schema versions are 2, 3, and 4");
+	}
+	if (const auto* time = root.Find("time"))
+		if (const auto* dt = time->Find("dt"))
+			if (dt->kind == json::Value::Kind::Number && !(dt->number > 0.0)) SimulationFail("time.dt must be positive");
+	if (const auto* temporal = root.Find("temporal_functions"))
+		if (temporal->kind == json::Value::Kind::Array)
+			for (size_t i = 0; i < temporal->items.size(); ++i) {
+				const auto& item = temporal->items[i];
+				const std::string context = "temporal_functions["+std::to_string(i)+"]";
+				const auto* units = item.Find("units");
+				if (!units) SimulationFail(context+" requires 'units'");
+				if (CaseString(*units, context+".units").empty())
+					SimulationFail("temporal function units cannot be empty");
+			}
+}
+
 std::vector<double> Numbers(const json::Value& v, const std::string& context)
 {
 	if (v.kind == json::Value::Kind::Number) return {v.number};
@@ -41,6 +93,7 @@ SimulationConfig ReadSimulationConfig(const std::string& path)
 {
 	const json::Value root = json::Parse(ReadText(path));
 	if (!root.IsObject()) Fail(-4, "simulation_config.json root must be an object");
+	ValidateSimulationRoot(root);
 	SimulationConfig config;
 	const auto& time = root.At("time", "root");
 	config.dt = time.At("dt", "time").Number("time.dt");
