@@ -384,10 +384,11 @@ def test_flow_line_host_builder_matches_the_oracle(api, small_tube):
 
 
 @requires_ref
-def test_simulation_config_root_errors_match_the_reference(api, tmp_path, small_tube):
-    """Root-level validation of simulation_config.json (schema versions, dimension / geometry / mesh,
-    unknown root keys, time step, waveform units): the same files fail in this parser and in the
-    reference's own ReadSimulationConfiguration, with the reference's message."""
+def test_simulation_config_errors_match_the_reference(api, tmp_path, small_tube):
+    """Validation of simulation_config.json for the flow path (root keys and schema rules, fields, time,
+    temporal functions, equation systems, boundaries and their conditions, outlet models): 39 invalid
+    files fail here and in the reference's own ReadSimulationConfiguration chain with the reference's
+    message, and the valid base file resolves in both."""
     from tubularflowiga_b200 import meshgen
     t = small_tube
     base = meshgen.simulation_config(1060.0, 3.5e-3, 2e-3, 3, 1.0, transient=True,
@@ -398,23 +399,42 @@ def test_simulation_config_root_errors_match_the_reference(api, tmp_path, small_
         edit(cfg)
         return cfg
 
+    rcr = {"label": 2, "name": "outlet", "conditions": [{"field": "pressure", "type": "windkessel_rcr",
+                                                          "proximal_resistance": 1e8, "capacitance": 0.0,
+                                                          "distal_resistance": 1e9}]}
+    cond = lambda c, k: c["boundaries"][k]["conditions"][0]
     bad = [
-        variant(lambda c: c.pop("dimension")),
-        variant(lambda c: c.update(dimension="2d")),
-        variant(lambda c: c.update(schema_version=5)),
-        variant(lambda c: c.update(schema_version=2)),
-        variant(lambda c: c.update(schema_version=4)),
-        variant(lambda c: c.update(colour="blue")),
-        variant(lambda c: c.update(geometry={"kind": "swc_network"})),
-        variant(lambda c: c["temporal_functions"][0].pop("units")),
-        variant(lambda c: c["temporal_functions"][0].update(units="")),
-        variant(lambda c: c["time"].update(dt=0.0)),
-        variant(lambda c: c.pop("schema_version")),
+        lambda c: c.pop("dimension"), lambda c: c.update(dimension="2d"), lambda c: c.update(schema_version=5),
+        lambda c: c.update(schema_version=2), lambda c: c.update(schema_version=4), lambda c: c.update(colour=1),
+        lambda c: c.update(geometry={"kind": "swc_network"}), lambda c: c.pop("schema_version"),
+        lambda c: c.pop("fields"), lambda c: c.update(fields=[]), lambda c: c["fields"][0].update(kind="tensor"),
+        lambda c: c["fields"].append(dict(c["fields"][0])), lambda c: c["fields"][0].update(colour=1),
+        lambda c: c["time"].update(dt=0.0), lambda c: c["time"].update(steps=-1), lambda c: c["time"].update(colour=1),
+        lambda c: c["temporal_functions"][0].pop("units"), lambda c: c["temporal_functions"][0].update(units=""),
+        lambda c: c["temporal_functions"][0].update(kind="spline"),
+        lambda c: c["temporal_functions"].append(dict(c["temporal_functions"][0])),
+        lambda c: c["temporal_functions"][0].update(period=0.0), lambda c: c["temporal_functions"][0].update(colour=1),
+        lambda c: c.pop("equation_systems"), lambda c: c["equation_systems"][0].update(kind="euler"),
+        lambda c: c["equation_systems"][0].update(colour=1),
+        lambda c: c["equation_systems"][0].update(unknowns=["velocity"]),
+        lambda c: c["equation_systems"][0].update(viscosity=-1.0),
+        lambda c: c["equation_systems"][0].update(time_integration="bdf2"),
+        lambda c: c.pop("boundaries"), lambda c: c["boundaries"][0].update(colour=1),
+        lambda c: c["boundaries"][0].pop("label"), lambda c: c["boundaries"].append(dict(c["boundaries"][0])),
+        lambda c: cond(c, 0).update(type="magic"), lambda c: cond(c, 0).update(field="temperature"),
+        lambda c: cond(c, 0).update(colour=1), lambda c: cond(c, 0).update(value=[0, 0]),
+        lambda c: cond(c, 1).update(profile="nofile.txt"), lambda c: cond(c, 1).update(waveform="nothing"),
+        lambda c: c["boundaries"].__setitem__(2, rcr),
     ]
-    for k, cfg in enumerate(bad):
-        path = tmp_path / f"bad{k}" / "simulation_config.json"
+    assert len(bad) == 39
+    for k, edit in enumerate([lambda c: None] + bad):
+        path = tmp_path / f"case{k}" / "simulation_config.json"
         path.parent.mkdir()
-        path.write_text(json.dumps(cfg))
+        path.write_text(json.dumps(variant(edit)))
+        if k == 0:
+            O.ref_flow_boundaries(path, t.labels, t.profile, 0.0)
+            api.resolve_flow_boundaries(path, t.labels, t.profile, 0.0)
+            continue
         with pytest.raises(RuntimeError) as ref_error:
             O.ref_flow_boundaries(path, t.labels, t.profile, 0.0)
         with pytest.raises(api.TfigaError) as err:

@@ -35,18 +35,45 @@ const std::string& CaseString(const json::Value& v, const std::string& context);
 
 [[noreturn]] void SimulationFail(const std::string& message) { Fail(-4, "simulation_config.json: "+message); }
 
-// Root structure checks of ParseSimulationConfiguration (include/SimulationConfig.hpp:263-287,
-// 324-347): known root keys, schema 2/3/4 with its dimension / geometry / mesh rules, a positive
-// time step, named temporal functions with non-empty units.  The contents of geometry and mesh are
-// not read here.
+double CaseNumber(const json::Value& v, const std::string& context);
+const json::Value& CaseObject(const json::Value& v, const std::string& context);
+
+const json::Value& Required(const json::Value& object, const char* key, const std::string& context)
+{
+	const auto* v = object.Find(key);
+	if (!v) SimulationFail(context+" requires '"+key+"'");
+	return *v;
+}
+
+const std::vector<json::Value>& CaseArray(const json::Value& v, const std::string& context)
+{
+	if (v.kind != json::Value::Kind::Array) Fail(-4, "case_config.json: "+context+" must be an array");
+	return v.items;
+}
+
+std::vector<double> ValueVector(const json::Value& v, const std::string& context)
+{
+	if (v.kind == json::Value::Kind::Number) return {CaseNumber(v, context)};
+	std::vector<double> out;
+	const auto& items = CaseArray(v, context);
+	for (size_t i = 0; i < items.size(); ++i) out.push_back(CaseNumber(items[i], context+"["+std::to_string(i)+"]"));
+	return out;
+}
+
+// The checks of ParseSimulationConfiguration (include/SimulationConfig.hpp:263-600) that concern
+// the flow path, in the reference's order and with its messages (its generic helpers name
+// case_config.json): root keys and schema 2/3/4 rules; fields; time; temporal functions; equation
+// systems (names, kinds, unknowns, Navier-Stokes physics and time integration); boundaries and their
+// conditions (known keys, fields, kinds, value / profile, outlet-model parameters, waveforms).  Not
+// repeated: the contents of geometry, mesh, coupling, perfusate, velocity_sources, physiology and
+// the terms and stabilization of transport systems.
 void ValidateSimulationRoot(const json::Value& root)
 {
+	CaseObject(root, "root");
 	KnownKeys(root, {"schema_version", "dimension", "geometry", "mesh", "fields", "equation_systems", "boundaries",
 		"time", "temporal_functions", "velocity_sources", "physiology", "simulation_scope", "perfusate",
 		"external_circuit", "coupling"}, "root");
-	const auto* version = root.Find("schema_version");
-	if (!version) SimulationFail("root requires 'schema_version'");
-	const int schema = CaseInteger(*version, "schema_version");
+	const int schema = CaseInteger(Required(root, "schema_version", "root"), "schema_version");
 	const auto* dimension = root.Find("dimension");
 	if (schema == 2) {
 		if (dimension || root.Find("geometry") || root.Find("mesh"))
@@ -59,24 +86,173 @@ void ValidateSimulationRoot(const json::Value& root)
 	} else if (schema == 4) {
 		if (!dimension || CaseString(*dimension, "dimension") != "3d")
 			SimulationFail("schema_version 4 requires dimension '3d'");
-		if (!root.Find("geometry")) SimulationFail("root requires 'geometry'");
-		if (!root.Find("mesh")) SimulationFail("root requires 'mesh'");
+		Required(root, "geometry", "root");
+		Required(root, "mesh", "root");
 	} else {
 		SimulationFail("supported schema versions are 2, 3, and 4");
 	}
-	if (const auto* time = root.Find("time"))
-		if (const auto* dt = time->Find("dt"))
-			if (dt->kind == json::Value::Kind::Number && !(dt->number > 0.0)) SimulationFail("time.dt must be positive");
-	if (const auto* temporal = root.Find("temporal_functions"))
-		if (temporal->kind == json::Value::Kind::Array)
-			for (size_t i = 0; i < temporal->items.size(); ++i) {
-				const auto& item = temporal->items[i];
-				const std::string context = "temporal_functions["+std::to_string(i)+"]";
-				const auto* units = item.Find("units");
-				if (!units) SimulationFail(context+" requires 'units'");
-				if (CaseString(*units, context+".units").empty())
-					SimulationFail("temporal function units cannot be empty");
+
+	std::set<std::string> fields;
+	const auto& field_list = CaseArray(Required(root, "fields", "root"), "fields");
+	for (size_t i = 0; i < field_list.size(); ++i) {
+		const std::string context = "fields["+std::to_string(i)+"]";
+		const auto& object = CaseObject(field_list[i], context);
+		KnownKeys(object, {"name", "kind", "initial_value"}, context);
+		const std::string name = CaseString(Required(object, "name", context), context+".name");
+		const std::string kind = CaseString(Required(object, "kind", context), context+".kind");
+		if (kind != "scalar" && kind != "vector3" && kind != "pressure")
+			SimulationFail("unsupported field kind '"+kind+"'");
+		if (const auto* v = object.Find("initial_value")) CaseNumber(*v, context+".initial_value");
+		if (name.empty() || !fields.insert(name).second) SimulationFail("field names must be non-empty and unique");
+	}
+	if (fields.empty()) SimulationFail("fields cannot be empty");
+
+	const auto& time = CaseObject(Required(root, "time", "root"), "time");
+	KnownKeys(time, {"dt", "steps"}, "time");
+	const double dt = CaseNumber(Required(time, "dt", "time"), "time.dt");
+	CaseInteger(Required(time, "steps", "time"), "time.steps");
+	if (!(dt > 0.0)) SimulationFail("time.dt must be positive");
+
+	std::set<std::string> temporal;
+	if (const auto* list = root.Find("temporal_functions")) {
+		const auto& functions = CaseArray(*list, "temporal_functions");
+		for (size_t i = 0; i < functions.size(); ++i) {
+			const std::string context = "temporal_functions["+std::to_string(i)+"]";
+			const auto& object = CaseObject(functions[i], context);
+			KnownKeys(object, {"name", "kind", "units", "value", "mean", "amplitude", "period", "phase", "file",
+				"interpolation", "cosine", "sine"}, context);
+			const std::string name = CaseString(Required(object, "name", context), context+".name");
+			const std::string kind = CaseString(Required(object, "kind", context), context+".kind");
+			if (kind != "constant" && kind != "sinusoid" && kind != "periodic_table" && kind != "fourier")
+				SimulationFail("unsupported temporal function kind '"+kind+"'");
+			const std::string units = CaseString(Required(object, "units", context), context+".units");
+			if (name.empty() || !temporal.insert(name).second)
+				SimulationFail("temporal function names must be non-empty and unique");
+			if (units.empty()) SimulationFail("temporal function units cannot be empty");
+			for (const char* key : {"value", "mean", "amplitude", "period", "phase"})
+				if (const auto* v = object.Find(key)) CaseNumber(*v, context+"."+key);
+			const double period = object.Find("period") ? object.Find("period")->number : 0.0;
+			std::string file, interpolation;
+			if (const auto* v = object.Find("file")) file = CaseString(*v, context+".file");
+			if (const auto* v = object.Find("interpolation")) interpolation = CaseString(*v, context+".interpolation");
+			std::vector<double> cosine, sine;
+			if (const auto* v = object.Find("cosine")) cosine = ValueVector(*v, context+".cosine");
+			if (const auto* v = object.Find("sine")) sine = ValueVector(*v, context+".sine");
+			if (kind == "constant" && !object.Find("value")) SimulationFail("constant temporal function requires value");
+			if (kind == "sinusoid" && (!object.Find("mean") || !object.Find("amplitude") || !(period > 0.0)))
+				SimulationFail("sinusoid requires mean, amplitude, and positive period");
+			if (kind == "periodic_table" && (file.empty() || !(period > 0.0) || interpolation != "linear"))
+				SimulationFail("periodic_table requires file, positive period, and linear interpolation");
+			if (kind == "fourier" && (!(period > 0.0) || cosine.size() != sine.size() || cosine.empty()))
+				SimulationFail("fourier requires positive period and equal non-empty cosine/sine arrays");
+		}
+	}
+
+	const auto& systems = CaseArray(Required(root, "equation_systems", "root"), "equation_systems");
+	std::set<std::string> system_names;
+	for (size_t i = 0; i < systems.size(); ++i) {
+		const std::string context = "equation_systems["+std::to_string(i)+"]";
+		const auto& object = CaseObject(systems[i], context);
+		KnownKeys(object, {"name", "kind", "unknowns", "terms", "stabilization", "viscosity", "density",
+			"time_integration"}, context);
+		const std::string name = CaseString(Required(object, "name", context), context+".name");
+		const std::string kind = CaseString(Required(object, "kind", context), context+".kind");
+		if (kind != "linear_transport" && kind != "navier_stokes")
+			SimulationFail("unsupported equation-system kind '"+kind+"'");
+		if (name.empty() || !system_names.insert(name).second)
+			SimulationFail("equation-system names must be non-empty and unique");
+		const auto& unknowns = CaseArray(Required(object, "unknowns", context), context+".unknowns");
+		std::set<std::string> local;
+		for (size_t j = 0; j < unknowns.size(); ++j) {
+			const std::string u = CaseString(unknowns[j], context+".unknowns["+std::to_string(j)+"]");
+			if (!fields.count(u)) SimulationFail("unknown field '"+u+"'");
+			if (!local.insert(u).second) SimulationFail("duplicate system unknown '"+u+"'");
+		}
+		if (local.empty()) SimulationFail("system unknowns cannot be empty");
+		double viscosity = 0.0, density = 1.0;
+		std::string integration = "steady";
+		if (const auto* v = object.Find("viscosity")) viscosity = CaseNumber(*v, context+".viscosity");
+		if (const auto* v = object.Find("density")) density = CaseNumber(*v, context+".density");
+		if (const auto* v = object.Find("time_integration")) integration = CaseString(*v, context+".time_integration");
+		if (kind == "navier_stokes") {
+			if (!(viscosity > 0.0)) SimulationFail("navier_stokes viscosity must be positive");
+			if (!(density > 0.0)) SimulationFail("navier_stokes density must be positive");
+			if (integration != "steady" && integration != "backward_euler")
+				SimulationFail("navier_stokes time_integration must be 'steady' or 'backward_euler'");
+		} else if (object.Find("density")) {
+			SimulationFail("density applies only to navier_stokes");
+		}
+	}
+	if (systems.empty()) SimulationFail("equation_systems cannot be empty");
+
+	const auto& boundaries = CaseArray(Required(root, "boundaries", "root"), "boundaries");
+	std::set<int> labels;
+	for (size_t i = 0; i < boundaries.size(); ++i) {
+		const std::string context = "boundaries["+std::to_string(i)+"]";
+		const auto& object = CaseObject(boundaries[i], context);
+		KnownKeys(object, {"label", "name", "conditions"}, context);
+		const int label = CaseInteger(Required(object, "label", context), context+".label");
+		CaseString(Required(object, "name", context), context+".name");
+		if (!labels.insert(label).second) SimulationFail("duplicate boundary label");
+		const auto& conditions = CaseArray(Required(object, "conditions", context), context+".conditions");
+		std::set<std::string> conditioned;
+		for (size_t j = 0; j < conditions.size(); ++j) {
+			const std::string c = context+".conditions["+std::to_string(j)+"]";
+			const auto& cond = CaseObject(conditions[j], c);
+			KnownKeys(cond, {"field", "type", "value", "coefficient", "exterior_value", "profile", "scale", "waveform",
+				"resistance", "proximal_resistance", "distal_resistance", "capacitance", "reference_pressure",
+				"initial_pressure", "pressure_gauge", "dirichlet_dofs"}, c);
+			const std::string field = CaseString(Required(cond, "field", c), c+".field");
+			const std::string type = CaseString(Required(cond, "type", c), c+".type");
+			if (type != "dirichlet" && type != "no_flux" && type != "flux" && type != "robin"
+				&& type != "advective_outflow" && type != "pressure_traction" && type != "resistance"
+				&& type != "windkessel_rc" && type != "windkessel_rcr")
+				SimulationFail("unsupported boundary condition '"+type+"'");
+			if (!fields.count(field) || !conditioned.insert(field).second)
+				SimulationFail("boundary fields must exist and be unique per boundary");
+			std::vector<double> value;
+			if (const auto* v = cond.Find("value")) value = ValueVector(*v, c+".value");
+			double coefficient = 0.0, resistance = 0.0, proximal = 0.0, distal = 0.0, capacitance = 0.0;
+			if (const auto* v = cond.Find("coefficient")) coefficient = CaseNumber(*v, c+".coefficient");
+			if (const auto* v = cond.Find("exterior_value")) CaseNumber(*v, c+".exterior_value");
+			std::string dofs = "face_support";
+			if (const auto* v = cond.Find("dirichlet_dofs")) dofs = CaseString(*v, c+".dirichlet_dofs");
+			if (dofs != "face_support" && dofs != "node_label")
+				SimulationFail("dirichlet_dofs must be 'face_support' or 'node_label'");
+			std::string profile, waveform;
+			if (const auto* v = cond.Find("profile")) profile = CaseString(*v, c+".profile");
+			if (const auto* v = cond.Find("scale")) CaseNumber(*v, c+".scale");
+			if (const auto* v = cond.Find("waveform")) waveform = CaseString(*v, c+".waveform");
+			if (const auto* v = cond.Find("resistance")) resistance = CaseNumber(*v, c+".resistance");
+			if (const auto* v = cond.Find("proximal_resistance")) proximal = CaseNumber(*v, c+".proximal_resistance");
+			if (const auto* v = cond.Find("distal_resistance")) distal = CaseNumber(*v, c+".distal_resistance");
+			if (const auto* v = cond.Find("capacitance")) capacitance = CaseNumber(*v, c+".capacitance");
+			if (const auto* v = cond.Find("reference_pressure")) CaseNumber(*v, c+".reference_pressure");
+			if (const auto* v = cond.Find("initial_pressure")) CaseNumber(*v, c+".initial_pressure");
+			bool gauge = false;
+			if (const auto* v = cond.Find("pressure_gauge")) {
+				if (v->kind != json::Value::Kind::Bool) Fail(-4, "case_config.json: "+c+".pressure_gauge must be a boolean");
+				gauge = v->boolean;
 			}
+			if (type == "dirichlet" && value.empty() && profile.empty())
+				SimulationFail("dirichlet requires value or profile");
+			if (!value.empty() && !profile.empty()) SimulationFail("boundary condition cannot set both value and profile");
+			if (type == "flux" && value.size() != 1) SimulationFail("flux requires one value");
+			if (type == "pressure_traction" && value.size() != 1) SimulationFail("pressure_traction requires one value");
+			if (gauge && (type != "pressure_traction" || value.size() != 1))
+				SimulationFail("pressure_gauge requires pressure_traction with one value");
+			if (type == "robin" && coefficient == 0.0) SimulationFail("robin requires nonzero coefficient");
+			if (type == "resistance" && !(resistance > 0.0))
+				SimulationFail("resistance outlet requires positive resistance");
+			if (type == "windkessel_rc" && (!(resistance > 0.0) || !(capacitance > 0.0)))
+				SimulationFail("windkessel_rc requires positive resistance and capacitance");
+			if (type == "windkessel_rcr" && (proximal < 0.0 || !(distal > 0.0) || !(capacitance > 0.0)))
+				SimulationFail("windkessel_rcr requires nonnegative proximal resistance and positive distal resistance "
+					"and capacitance");
+			if (!waveform.empty() && ((type != "dirichlet" && type != "pressure_traction") || !temporal.count(waveform)))
+				SimulationFail("waveform must name a temporal function on a Dirichlet or pressure_traction condition");
+		}
+	}
 }
 
 std::vector<double> Numbers(const json::Value& v, const std::string& context)
@@ -377,7 +553,9 @@ ResolvedBoundaries ResolveFlowBoundaries(const SimulationConfig& config, const F
 
 std::map<int, double> ExtractPressureTractions(const SimulationConfig& config, const FlowSystem& system)
 {
-	const auto& pname = system.unknowns.at(1);
+	if (system.kind != "navier_stokes" || system.unknowns.size() != 2)
+		Fail(-4, "pressure traction requires a Navier-Stokes system");
+	const auto& pname = system.unknowns[1];
 	std::map<int, double> out;
 	for (const auto& b : config.boundaries)
 		for (const auto& c : b.conditions) {
@@ -391,7 +569,9 @@ std::map<int, double> ExtractPressureTractions(const SimulationConfig& config, c
 
 std::vector<OutletModel> InitializeOutletModels(const SimulationConfig& config, const FlowSystem& system)
 {
-	const auto& pname = system.unknowns.at(1);
+	if (system.kind != "navier_stokes" || system.unknowns.size() != 2)
+		Fail(-4, "outlet models require a Navier-Stokes velocity-pressure system");
+	const auto& pname = system.unknowns[1];
 	std::vector<OutletModel> models;
 	for (const auto& b : config.boundaries)
 		for (const auto& c : b.conditions) {
