@@ -546,7 +546,10 @@ int tfiga_transport_profile(tfiga_transport* transport, double* milliseconds, in
  * nodes <= 262144 (larger -> TFIGA_E_UNSUPPORTED, nothing launched).  No
  * scratch has to start at zero.  Calls share that scratch, so calls whose
  * kernels could overlap must be serialized.  The first call on a device looks
- * up the scratch address; make it before any stream capture begins. */
+ * up the scratch address; make it before any stream capture begins.  The
+ * address is kept with the id of the context it was looked up in: after
+ * cudaDeviceReset the next call looks it up again (so, again, outside any
+ * capture). */
 int tfiga_block_residual_norm_static(int64_t nodes, const int32_t* row_offsets_device,
 	const int32_t* columns_device, const double* values_device, const double* x_device, const double* b_device,
 	double* norm_device, void* stream);

@@ -18,14 +18,19 @@
 //    kernels overlap (different streams, or different host threads) race on
 //    it; calls must be ordered on one stream or otherwise serialized;
 //  * the first call on each device performs the symbol lookup, so make that
-//    first call before any stream capture on that device begins.
+//    first call before any stream capture on that device begins; the address
+//    is cached with the unique id of the context it was looked up in, so a
+//    call made after cudaDeviceReset (a new primary context) looks it up again
+//    instead of using the stale address.
 // The two kernels sum in a fixed order, so equal inputs give bitwise equal
 // norms.
 #include "common.hpp"
 
 #include "../../include/tfiga.h"
 
-#include <atomic>
+#include <cuda.h>
+
+#include <mutex>
 
 namespace tfiga {
 void RecordLastError(const char* message);
@@ -41,7 +46,13 @@ constexpr int kFinalizeThreads = 1024;
 
 static __device__ __align__(256) double g_partials[kMaxPartials];
 
-std::atomic<double*> g_scratch[kMaxDevices];
+// Per device: the scratch address and the id of the context it belongs to (0: none yet).
+struct ScratchEntry {
+	unsigned long long context_id = 0;
+	double* address = nullptr;
+};
+ScratchEntry g_scratch[kMaxDevices];
+std::mutex g_scratch_mutex;
 
 __global__ void __launch_bounds__(256) ResidualPartialKernel(int nodes, const int32_t* __restrict__ row_offsets,
 	const int32_t* __restrict__ columns, const double* __restrict__ values, const double* __restrict__ x,
@@ -102,22 +113,67 @@ int Reject(int status, const char* message)
 	return status;
 }
 
-// Address of this device's scratch array (looked up once per device).
+// Driver entry points for the current context and its process-unique id, taken through the
+// runtime so the library needs no link against libcuda.
+using CtxGetCurrent = CUresult (*)(CUcontext*);
+using CtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+
+bool DriverEntryPoints(CtxGetCurrent* get_current, CtxGetId* get_id)
+{
+	static CtxGetCurrent current = nullptr;
+	static CtxGetId id = nullptr;
+	static std::once_flag once;
+	std::call_once(once, [] {
+		void* f = nullptr;
+		cudaDriverEntryPointQueryResult found{};
+		if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &found) == cudaSuccess
+			&& found == cudaDriverEntryPointSuccess)
+			current = reinterpret_cast<CtxGetCurrent>(f);
+		f = nullptr;
+		if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &found) == cudaSuccess
+			&& found == cudaDriverEntryPointSuccess)
+			id = reinterpret_cast<CtxGetId>(f);
+	});
+	*get_current = current;
+	*get_id = id;
+	return current != nullptr && id != nullptr;
+}
+
+// Id of the calling thread's current context, or 0 when none is current (or it is gone).
+unsigned long long CurrentContextId(CtxGetCurrent get_current, CtxGetId get_id)
+{
+	CUcontext context = nullptr;
+	unsigned long long id = 0;
+	if (get_current(&context) != CUDA_SUCCESS || context == nullptr || get_id(context, &id) != CUDA_SUCCESS) return 0;
+	return id;
+}
+
+// Address of this device's scratch array, looked up once per device and context: the cached
+// address is reused only while the context it was looked up in is still the current one.
 int Scratch(double** out)
 {
 	int device = 0;
 	if (cudaGetDevice(&device) != cudaSuccess) return Reject(TFIGA_E_CUDA, "cudaGetDevice failed");
 	if (device < 0 || device >= kMaxDevices) return Reject(TFIGA_E_UNSUPPORTED, "device ordinal above 63");
-	double* p = g_scratch[device].load(std::memory_order_acquire);
-	if (p == nullptr) {
+	CtxGetCurrent get_current = nullptr;
+	CtxGetId get_id = nullptr;
+	if (!DriverEntryPoints(&get_current, &get_id))
+		return Reject(TFIGA_E_CUDA, "driver entry points cuCtxGetCurrent / cuCtxGetId unavailable");
+	unsigned long long context_id = CurrentContextId(get_current, get_id);
+	std::lock_guard<std::mutex> lock(g_scratch_mutex);
+	ScratchEntry& entry = g_scratch[device];
+	if (context_id == 0 || entry.context_id != context_id || entry.address == nullptr) {
+		// the lookup also makes the runtime (re)create the device's primary context when none is current
 		void* address = nullptr;
 		const cudaError_t e = cudaGetSymbolAddress(&address, g_partials);
 		if (e != cudaSuccess || address == nullptr)
 			return Reject(TFIGA_E_CUDA, "cudaGetSymbolAddress of the residual-norm scratch failed");
-		p = static_cast<double*>(address);
-		g_scratch[device].store(p, std::memory_order_release);
+		context_id = CurrentContextId(get_current, get_id);
+		if (context_id == 0) return Reject(TFIGA_E_CUDA, "no current CUDA context after the scratch lookup");
+		entry.address = static_cast<double*>(address);
+		entry.context_id = context_id;
 	}
-	*out = p;
+	*out = entry.address;
 	return TFIGA_OK;
 }
 
