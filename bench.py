@@ -277,55 +277,97 @@ def algorithmic_counts(tube, blocks):
     return b_spmv, b_bjac, f_asm
 
 
-def cpu_reference(tube, state, prev, steps_newton, lin_per_newton, budget_s=25.0):
-    """Reference CPU path on a bounded sample: reference element code + CPU block-Jacobi GMRES."""
-    from oracle import oracle as O
-    m = tube.mesh
-    P = O.Pattern(m.nodes, m.element_offsets, m.connectivity)
-    kind = "reference" if O.ref_available() else "port"
-    threads = O.ref().ref_max_threads() if kind == "reference" else O.max_threads()
-    # assembly sample: the first `count` elements, doubled until it takes ~40% of the budget
-    count = max(threads, 64)
-    while True:
-        count = min(count, m.elements)
+# Newton iterations per step and GMRES iterations per Newton iteration of the reference's own solver
+# algorithm on each workload -- exact-tangent Newton to rel.res 1e-8, every linear system to rtol 1e-8 by
+# left block-Jacobi GMRES(200) (iga_cuda.cu:956-1054, Gmres.hpp:69-213), outlets coupled inside the Newton
+# loop -- recorded from a GPU run of this library in that mode:
+#   python bench.py --workload W --precision fp64 --preconditioner block-jacobi --forcing fixed \
+#       --tangent-reuse 0 --restart 200 --newton-rtol 1e-8 --no-fp64-leg --no-cpu-baseline --steps 2 --warmup 1
+# The CPU arm prices those counts at its own measured element and GMRES-iteration costs.
+REFERENCE_COUNTS = {
+    "c3": {"newton_per_step": 4.0, "gmres_per_newton": 228.0, "recorded": "provisional"},
+}
+
+
+class CpuReference:
+    """The reference's CPU path for one workload, set up once: its own element code (oracle/_ref, OpenMP
+    over all host cores; the CPU restatement where the reference build is absent) and the CPU restatement
+    of block-Jacobi GMRES(200) (Gmres.hpp:69-213) on the workload's full block pattern.
+
+    A sample times a bounded part of one time step -- the assembly of the first `elements` elements and
+    `iterations` GMRES iterations -- and extrapolates it to a whole step of `newton` Newton iterations with
+    `gmres` GMRES iterations each: step = newton x (E x t_element + gmres x t_iteration)."""
+
+    def __init__(self, tube, state, prev):
+        from oracle import oracle as O
+        self.O = O
+        self.mesh = tube.mesh
+        self.state, self.prev = state, prev
+        m = tube.mesh
+        self.P = O.Pattern(m.nodes, m.element_offsets, m.connectivity)
+        self.kind = "reference" if O.ref_available() else "port"
+        self.threads = O.ref().ref_max_threads() if self.kind == "reference" else O.max_threads()
+        # GMRES operand: 4 I diagonal blocks plus small off-diagonal entries (the cost of an iteration
+        # does not depend on the values); tiled from a 1 Mi-value random block so that filling the
+        # multi-GB array is a memory copy
+        rng = np.random.default_rng(0)
+        vals = np.resize(rng.standard_normal(1 << 20) * 1e-3, self.P.blocks * 16)
+        vals.reshape(-1, 4, 4)[self.P.diagonal] += np.eye(4) * 4.0
+        self.vals = vals
+        self.rhs = rng.standard_normal(4 * m.nodes)
+        self.elements, self.iterations = max(self.threads, 64), 10
+
+    def _time_assembly(self, count):
+        m = self.mesh
         t0 = time.perf_counter()
-        if kind == "reference":
-            O.ref_assemble(m, P, state, prev, RHO, MU, DT, 0, count)
+        if self.kind == "reference":
+            self.O.ref_assemble(m, self.P, self.state, self.prev, RHO, MU, DT, 0, count)
         else:
-            O.assemble(m, P, state, prev, RHO, MU, DT)
-            count = m.elements
-        dt_s = time.perf_counter() - t0
-        t_el = dt_s / count
-        if dt_s > 0.4 * budget_s or count >= m.elements:
-            break
-        count *= 2
-    asm_elements = min(count, m.elements)
-    t_assembly = t_el * m.elements
-    # GMRES sample on the full-size system pattern (iterations are data-independent in cost)
-    rng = np.random.default_rng(0)
-    vals = np.zeros(P.blocks * 16)
-    vals.reshape(-1, 4, 4)[P.diagonal] = np.eye(4) * 4.0
-    vals += rng.standard_normal(vals.size) * 1e-3
-    rhs = rng.standard_normal(4 * m.nodes)
-    iters = 10
-    while True:
+            self.O.assemble(m, self.P, self.state, self.prev, RHO, MU, DT)
+        return time.perf_counter() - t0
+
+    def _time_gmres(self, iterations):
         t0 = time.perf_counter()
-        O.gmres_bjacobi(P, vals, rhs, restart=200, maxit=iters, rtol=1e-300)
-        dt_s = time.perf_counter() - t0
-        if dt_s > 0.4 * budget_s or iters >= 400:
-            break
-        iters *= 2
-    t_iter = dt_s / iters
-    t_step = steps_newton * (t_assembly + lin_per_newton * t_iter)
-    return {
-        "value": 1.0 / t_step, "unit": "time steps/s", "cores": int(threads), "kind": kind,
-        "sample": (f"reference element assembly of {asm_elements} of {m.elements} elements "
-                   f"({t_el * 1e3:.2f} ms/element wall on {threads} threads) and {iters} block-Jacobi GMRES(200) "
-                   f"iterations of the CPU restatement on the full {4 * m.nodes}-DOF pattern "
-                   f"({t_iter * 1e3:.1f} ms/iteration); step = {steps_newton:.2f} Newton x (assembly + "
-                   f"{lin_per_newton:.0f} GMRES iterations), counts from the GPU run of the same algorithm"),
-        "assembly_s": t_assembly, "gmres_iteration_s": t_iter,
-    }
+        self.O.gmres_bjacobi(self.P, self.vals, self.rhs, restart=200, maxit=iterations, rtol=1e-300)
+        return time.perf_counter() - t0
+
+    def calibrate(self, budget_s):
+        """Sample sizes for which one sample takes about budget_s (doubling from small sizes)."""
+        m = self.mesh
+        count = max(self.threads, 64)
+        while True:
+            count = min(count, m.elements) if self.kind == "reference" else m.elements
+            if self._time_assembly(count) > 0.45 * budget_s or count >= m.elements:
+                break
+            count *= 2
+        iters = 5
+        while True:
+            if self._time_gmres(iters) > 0.45 * budget_s or iters >= 400:
+                break
+            iters *= 2
+        self.elements, self.iterations = count, iters
+
+    def sample(self, newton, gmres):
+        t_el = self._time_assembly(self.elements) / self.elements
+        t_it = self._time_gmres(self.iterations) / self.iterations
+        t_step = newton * (t_el * self.mesh.elements + gmres * t_it)
+        return {
+            "value": 1.0 / t_step, "unit": "time steps/s", "cores": int(self.threads), "kind": self.kind,
+            "sample": (f"reference element assembly of {self.elements} of {self.mesh.elements} elements "
+                       f"({t_el * 1e3:.2f} ms/element wall on {self.threads} threads) and {self.iterations} "
+                       f"block-Jacobi GMRES(200) iterations of the CPU restatement on the full "
+                       f"{4 * self.mesh.nodes}-DOF pattern ({t_it * 1e3:.1f} ms/iteration); extrapolated to "
+                       f"a step of {newton:.2f} Newton x (assembly + {gmres:.0f} GMRES iterations), the counts "
+                       f"of the reference's algorithm recorded on the GPU"),
+            "sample_s": t_el * self.elements + t_it * self.iterations, "step_s": t_step,
+        }
+
+
+def reference_counts(name):
+    c = REFERENCE_COUNTS.get(name)
+    if c is None:
+        raise SystemExit("no recorded reference-algorithm counts for workload " + name)
+    return c["newton_per_step"], c["gmres_per_newton"]
 
 
 def run_reference_arm(args, world, rank):
@@ -336,11 +378,16 @@ def run_reference_arm(args, world, rank):
     n = tube.mesh.nodes
     vmask, pmask, velocity_at = boundary(tube, wave)
     s0 = api.initial_state(vmask, velocity_at(0.0))
-    # Newton and GMRES counts per step of this algorithm on this workload, as measured by the GPU arm.
-    newton, lin = args.ref_newton, args.ref_linear
-    budget = max(4.0, min(args.ref_budget, 120.0 / max(1, args.steps + 1)))
-    cpu_reference(tube, s0, s0, newton, lin, budget_s=2.0)           # warm-up sample
-    samples = [cpu_reference(tube, s0, s0, newton, lin, budget_s=budget) for _ in range(args.steps)]
+    newton, lin = reference_counts(args.workload)
+    cpu = CpuReference(tube, s0, s0)
+    # each timed step is one bounded sample of the step, sized so that the whole run stays within a few
+    # minutes; the warm-up steps calibrate the sample size
+    budget = max(2.0, min(args.ref_budget, 150.0 / max(1, args.steps)))
+    for _ in range(max(1, args.warmup)):
+        cpu.calibrate(budget)
+    t0 = time.perf_counter()
+    samples = [cpu.sample(newton, lin) for _ in range(args.steps)]
+    wall = time.perf_counter() - t0
     res = dict(samples[-1])
     res["value"] = float(np.mean([r["value"] for r in samples]))
     line = {"metric": METRIC, "value": res["value"], "unit": "time steps/s", "impl": "reference",
@@ -348,8 +395,14 @@ def run_reference_arm(args, world, rank):
             "ms_per_step": 1e3 / res["value"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
             "config": {"workload": desc, "elements": tube.mesh.elements, "nodes": n,
-                       "solver": "reference CPU element code + CPU block-Jacobi GMRES(200)",
+                       "solver": "reference CPU element code + CPU block-Jacobi GMRES(200); Newton and GMRES "
+                                 "counts of the reference's algorithm recorded on the GPU",
                        "parallelism": "replicas only"},
+            "extrapolated": {"note": "each timed step runs a bounded sample of the full step and is "
+                                     "extrapolated to it, so ms_per_step x steps exceeds the run's wall time",
+                             "sample_s_per_step": float(np.mean([r["sample_s"] for r in samples])),
+                             "sampled_wall_s": wall, "newton_per_step": newton, "gmres_per_newton": lin,
+                             "counts_recorded": REFERENCE_COUNTS[args.workload]["recorded"]},
             "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": res["value"], "unit": "time steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -604,9 +657,10 @@ def main():
     ap.add_argument("--transport-mesh", default="c3", choices=["c3", "c2-100"],
                     help="transport workload mesh: c3 with the velocity of one Navier-Stokes step, or the "
                          "12,800-element tube section with its Poiseuille profile at 0.15 m/s mean (profiling case)")
-    ap.add_argument("--ref-budget", type=float, default=25.0)
-    ap.add_argument("--ref-newton", type=float, default=4.0)
-    ap.add_argument("--ref-linear", type=float, default=228.0)
+    ap.add_argument("--ref-budget", type=float, default=20.0,
+                    help="seconds of CPU work per sample of the CPU reference path")
+    ap.add_argument("--newton-rtol", type=float, default=1e-10,
+                    help="Newton test ||r|| <= rtol ||r_0|| of every arm (FP64 residual)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -636,7 +690,7 @@ def main():
     if mixed and not amg:
         raise SystemExit("--precision mixed needs --preconditioner amg")
     solver_kw = dict(density=RHO, viscosity=MU, dt=step_dt(args.workload),
-                     nonlinear_rtol=1e-8, nonlinear_atol=1e-300, mass_rtol=1e-3,
+                     nonlinear_rtol=args.newton_rtol, nonlinear_atol=1e-300, mass_rtol=1e-3,
                      gmres_restart=args.restart, gmres_max_iterations=5000, gmres_rtol=1e-8,
                      preconditioner=api.AMG if amg else api.BLOCK_JACOBI,
                      amg_coarse_period=3, krylov_fp64_basis=int(args.krylov_fp64_basis),
@@ -665,69 +719,94 @@ def main():
 
     reports = []
 
-    def do_step(k, host=False):
+    def do_step(solver, solver_outlets, k, host=False, record=None):
         if host:
-            api.check(api.lib().tfiga_ns_set_dirichlet_values(ns._h, api.C.c_void_p(bc_host[k].data_ptr()), None))
+            api.check(api.lib().tfiga_ns_set_dirichlet_values(solver._h, api.C.c_void_p(bc_host[k].data_ptr()),
+                                                              None))
         else:
-            api.check(api.lib().tfiga_ns_set_dirichlet_values(ns._h, api.C.c_void_p(bc_dev[k].data_ptr()), None))
-        ns.commit_step()
-        r = outlet_step(ns, outlets, args.outlet_coupling) if outlets else ns.step()
-        reports.append(r)
+            api.check(api.lib().tfiga_ns_set_dirichlet_values(solver._h, api.C.c_void_p(bc_dev[k].data_ptr()),
+                                                              None))
+        solver.commit_step()
+        r = outlet_step(solver, solver_outlets, args.outlet_coupling) if solver_outlets else solver.step()
+        if record is not None:
+            record.append(r)
         if host:
-            api.check(api.lib().tfiga_ns_get_state(ns._h, api.C.c_void_p(out_host.data_ptr())))
+            api.check(api.lib().tfiga_ns_get_state(solver._h, api.C.c_void_p(out_host.data_ptr())))
 
-    warm_states = []
+    states = []                                   # the arm's state after every step (error legs)
     for k in range(args.warmup):
-        do_step(k)
-        warm_states.append(ns.get_state())
-    reports.clear()
+        do_step(ns, outlets, k)
+        states.append(ns.get_state())
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     timed_start = ns.get_state()
     timed_outlets = [o.as_dict() for o in outlets] if outlets else None
-    ns.set_profiling(True)
-    ns.profile(reset=True)
+
+    def restart():
+        ns.set_state(timed_start, timed_start)
+        if outlets:
+            for o, d in zip(outlets, timed_outlets):
+                for key, v in d.items():
+                    setattr(o, key, v)
+
+    # value leg: CUDA events on the solver stream, every input resident in HBM, no instrumentation
+    ns.set_profiling(False)
     launches0 = ns.launches()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clocks:
         torch.cuda.synchronize()
         ev0.record(stream)
-        for k in range(args.warmup, args.warmup + args.steps):
-            do_step(k)
+        for k in range(args.warmup, total):
+            do_step(ns, outlets, k, record=reports)
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     launches = ns.launches() - launches0
+    timed_reports = list(reports)
+    tangents = None
+
+    # profile leg: the same steps again from the same state with per-family CUDA events on the solver
+    # stream (kernel rooflines and step shares, against this pass's own duration); the state after
+    # every step is kept for the error legs
+    restart()
+    ns.set_profiling(True)
+    ns.profile(reset=True)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    prof_ms = 0.0
+    for k in range(args.warmup, total):
+        torch.cuda.synchronize()
+        p0.record(stream)
+        do_step(ns, outlets, k)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        prof_ms += p0.elapsed_time(p1)
+        states.append(ns.get_state())
     orth_algo, orth_moved = ns.profile_bytes()["krylov_orthogonalisation"]
     prof = ns.profile(reset=True)
     ns.set_profiling(False)
-    timed_reports = list(reports)
-    reports.clear()
-    # e2e leg: pinned host inputs, state read back each step
+
+    # e2e leg: same steps from the same state through the C ABI, inputs from pinned host memory, the
+    # state read back every step
     if dist:
         dist.barrier()
-    # same steps from the same state as the timed leg, inputs from pinned host memory
-    ns.set_state(timed_start, timed_start)
-    if outlets:
-        for o, d in zip(outlets, timed_outlets):
-            for k, v in d.items():
-                setattr(o, k, v)
+    restart()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
-    for k in range(args.warmup, args.warmup + args.steps):
-        do_step(k, host=True)
+    for k in range(args.warmup, total):
+        do_step(ns, outlets, k, host=True)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
 
-    # plain FP64 GPU solver on the warm-up steps from the same initial state: per-step error of the
-    # mixed solution against it, and its own time steps/s (steps after the first, CUDA events)
+    # plain FP64 GPU solver on the same steps: the same Dirichlet sequence and starting state, the same
+    # Newton test, residual-first check, tangent-reuse rule, outlet coupling and restart; the warm-up
+    # steps untimed, the timed steps between CUDA events.  Run with the mixed arm's linear-tolerance mode
+    # and with the fixed tolerance 1e-8 of the reference; the faster is the baseline.  The mixed state
+    # after every step is compared with the FP64 run of the same mode.
     fp64_leg = None
     if mixed and not args.no_fp64_leg:
-        # the plain FP64 solver in each linear-tolerance mode (fixed 1e-8 as the reference, and the
-        # forcing mode when the mixed arm uses it); the faster one is the baseline reported
         def fp64_run(forcing):
             kw = dict(solver_kw, newton_forcing=int(forcing == "ew"))
             ref = api.NavierStokes(mesh, precision=api.FP64, **kw)
@@ -736,41 +815,50 @@ def main():
             ref.set_state(s0, s0)
             ref_outlets = [api.Outlet(**m.as_dict()) for m in models] if models else None
             rstream = torch.cuda.ExternalStream(ref.stream())
-            errors, fp64_ms, fp64_steps, fp64_reports = [], 0.0, 0, []
-            for k in range(args.warmup):
-                api.check(api.lib().tfiga_ns_set_dirichlet_values(ref._h, api.C.c_void_p(bc_dev[k].data_ptr()),
-                                                                  None))
-                ref.commit_step()
-                a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            errors, fp64_reports = [], []
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            fp64_ms = 0.0
+            for k in range(total):
                 torch.cuda.synchronize()
                 a0.record(rstream)
-                if ref_outlets:
-                    rep = outlet_step(ref, ref_outlets, args.outlet_coupling)
-                else:
-                    rep = ref.step()
+                do_step(ref, ref_outlets, k, record=fp64_reports if k >= args.warmup else None)
                 a1.record(rstream)
-                fp64_reports.append(rep)
                 torch.cuda.synchronize()
-                if k > 0:
+                if k >= args.warmup:
                     fp64_ms += a0.elapsed_time(a1)
-                    fp64_steps += 1
                 r64 = ref.get_state().reshape(-1, 4)
-                mx = warm_states[k].reshape(-1, 4)
+                mx = states[k].reshape(-1, 4)
                 errors.append({"step": k,
                                "velocity": float(np.linalg.norm(mx[:, :3] - r64[:, :3]) / np.linalg.norm(r64[:, :3])),
                                "pressure": float(np.linalg.norm(mx[:, 3] - r64[:, 3]) / np.linalg.norm(r64[:, 3]))})
             ref.close()
-            return {"value": fp64_steps / (fp64_ms / 1e3) if fp64_steps else None, "unit": "time steps/s",
-                    "forcing": forcing, "steps": fp64_steps, "ms_per_step": fp64_ms / max(fp64_steps, 1),
-                    "newton_per_step": float(np.mean([r["newton_iterations"] for r in fp64_reports])),
+            newton_n = np.sum([r["newton_iterations"] for r in fp64_reports])
+            return {"value": args.steps / (fp64_ms / 1e3), "unit": "time steps/s", "forcing": forcing,
+                    "steps": args.steps, "timed_steps": [args.warmup, total - 1],
+                    "ms_per_step": fp64_ms / args.steps,
+                    "newton_per_step": float(newton_n / args.steps),
                     "linear_iterations_per_newton": float(np.sum([r["linear_iterations"] for r in fp64_reports])
-                                                          / max(1, np.sum([r["newton_iterations"]
-                                                                           for r in fp64_reports]))),
-                    "error_vs_fp64_per_step": errors}
+                                                          / max(1, newton_n)),
+                    "error_vs_fp64_per_step": errors,
+                    "max_error": {"velocity": max(e["velocity"] for e in errors),
+                                  "pressure": max(e["pressure"] for e in errors)}}
 
-        runs = [fp64_run(mode) for mode in dict.fromkeys(["fixed", args.forcing])]
-        fp64_leg = dict(max(runs, key=lambda r: r["value"] or 0.0))
-        fp64_leg["variants"] = {r["forcing"]: r["value"] for r in runs}
+        runs = {mode: fp64_run(mode) for mode in dict.fromkeys([args.forcing, "fixed"])}
+        best = max(runs.values(), key=lambda r: r["value"] or 0.0)
+        same = runs[args.forcing]
+        fp64_leg = {k: v for k, v in best.items() if k not in ("error_vs_fp64_per_step", "max_error")}
+        fp64_leg["variants"] = {m: {k: r[k] for k in ("value", "ms_per_step", "newton_per_step",
+                                                       "linear_iterations_per_newton", "max_error")}
+                                for m, r in runs.items()}
+        fp64_leg["error_vs_fp64_per_step"] = same["error_vs_fp64_per_step"]
+        fp64_leg["max_error"] = same["max_error"]
+        fp64_leg["error_reference"] = ("the FP64 run with the mixed arm's own settings (%s linear tolerance, "
+                                       "Newton rel.res %g), every step from the same initial state"
+                                       % (args.forcing, args.newton_rtol))
+        fp64_leg["same_as_mixed"] = ("same steps (warm-up %d untimed, %d timed), Dirichlet sequence, outlet "
+                                     "coupling, Newton test, residual-first check, tangent-reuse factor %g and "
+                                     "FGMRES restart; precision FP64 everywhere" % (args.warmup, args.steps,
+                                                                                    args.tangent_reuse))
 
     ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms], "cuda")
     if rank != 0:
@@ -797,7 +885,7 @@ def main():
         traffic = SPMV_FP32_DRAM_BYTES_PER_BLOCK * mesh.blocks if (mixed and amg) else None
         kernels[spmv_name] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
                               "frac": a / hbm, "traffic": traffic, "launches": spmv_n,
-                              "avg_ms": spmv_ms / spmv_n, "share": spmv_ms / ms,
+                              "avg_ms": spmv_ms / spmv_n, "share": spmv_ms / prof_ms,
                               "algorithmic_bytes": spmv_bytes}
     if amg_n:
         # one two-level application: restriction (b, mask, aggregate order), the dense coarse inverse
@@ -813,7 +901,7 @@ def main():
         a = vbytes / (amg_ms / amg_n * 1e-3) / 1e9
         kernels["amg_vcycle"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s", "frac": a / hbm,
                                  "traffic": None, "launches": amg_n, "avg_ms": amg_ms / amg_n,
-                                 "share": amg_ms / ms, "algorithmic_bytes": vbytes,
+                                 "share": amg_ms / prof_ms, "algorithmic_bytes": vbytes,
                                  "levels": ns.amg_info()}
     asm_name = "assembly_tc" if mixed else "assembly_fp64"
     if asm_n and mixed:
@@ -822,23 +910,23 @@ def main():
         a = f_asm / (asm_ms / asm_n * 1e-3) / 1e12
         kernels[asm_name] = {"bound": "tensor", "achieved": a, "peak": bf16_sustained, "unit": "TFLOP/s",
                              "frac": a / bf16_sustained, "traffic": None, "launches": asm_n,
-                             "avg_ms": asm_ms / asm_n, "share": asm_ms / ms,
+                             "avg_ms": asm_ms / asm_n, "share": asm_ms / prof_ms,
                              "peak_kind": f"{peak_kind} bf16_tflops_sustained"}
     elif asm_n:
         a = f_asm / (asm_ms / asm_n * 1e-3) / 1e12
         kernels[asm_name] = {"bound": "fp64", "achieved": a, "peak": 37.0, "unit": "TFLOP/s",
                              "frac": a / 37.0, "traffic": None, "launches": asm_n,
-                             "avg_ms": asm_ms / asm_n, "share": asm_ms / ms,
+                             "avg_ms": asm_ms / asm_n, "share": asm_ms / prof_ms,
                              "peak_note": "nominal B200 FP64 (no measured FP64 peak on this pool)"}
     if res_n:
-        # FP64 residual + point coefficients of the tensor-core modes: per element it reads the FP64
-        # basis tables (5 x 64 x 64 doubles) and the point data (64 x 11 doubles) and writes the
-        # coefficients of four row fields (4 x 80 x 64 floats)
-        rbytes = tube.mesh.elements * (5 * 64 * 64 * 8 + 64 * 11 * 8 + 4 * 80 * 64 * 4)
+        # FP64 residual (+ point coefficients in the tensor-core modes): per element it reads the FP64
+        # basis tables (5 x 64 x 64 doubles) and the point data (64 x 11 doubles) and, in the tensor-core
+        # modes, writes the coefficients of four row fields (4 x 80 x 64 floats)
+        rbytes = tube.mesh.elements * (5 * 64 * 64 * 8 + 64 * 11 * 8 + (4 * 80 * 64 * 4 if mixed else 0))
         a = rbytes / (res_ms / res_n * 1e-3) / 1e9
         kernels["residual_point"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s", "frac": a / hbm,
                                      "traffic": None, "launches": res_n, "avg_ms": res_ms / res_n,
-                                     "share": res_ms / ms, "algorithmic_bytes": rbytes}
+                                     "share": res_ms / prof_ms, "algorithmic_bytes": rbytes}
     if orth_n:
         # algorithmic bytes of Arnoldi step j as the solver accounts them: s_v N (2j + 7) (one dot
         # pass, one update pass, the normalisation; s_v = 4 for the FP32 basis of the mixed solver)
@@ -848,14 +936,16 @@ def main():
         a = algo / (orth_ms * 1e-3) / 1e9
         kernels["krylov_orthogonalisation"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
                                                "frac": a / hbm, "traffic": None, "launches": orth_n,
-                                               "avg_ms": orth_ms / orth_n, "share": orth_ms / ms,
+                                               "avg_ms": orth_ms / orth_n, "share": orth_ms / prof_ms,
                                                "algorithmic_bytes_per_launch": algo / orth_n,
                                                "moved_bytes_per_launch": orth_moved / orth_n,
                                                "moved_gbs": orth_moved / (orth_ms * 1e-3) / 1e9}
+    attributed = sum(k.get("share", 0.0) for k in kernels.values())
     dominant = max((spmv_name, asm_name, "amg_vcycle", "krylov_orthogonalisation", "residual_point"),
                    key=lambda k: kernels.get(k, {}).get("share", 0))
     roof = dict(kernels[dominant])
     roof["kernel"] = dominant
+    roof["timing"] = "per-launch CUDA events of an instrumented repeat of the timed steps"
     if roof["bound"] == "hbm":
         roof["peak_kind"] = f"{peak_kind} hbm_gbs"
     steps_per_s = replica_throughput(world, args.steps, ms)
@@ -871,11 +961,12 @@ def main():
                    "solver": (("mixed: tcgen05 %s tangent (FP32 accumulate), FP32 Jacobian, FP64 residual and "
                                "refinement; " % ("split-BF16 (hi + lo, 3 products)" if args.precision == "bf16x3"
                                                  else "BF16") if mixed else "plain FP64: ") +
-                              "exact-tangent Newton to rel.res 1e-8, " +
+                              "exact-tangent Newton to rel.res %g (FP64 residual, tested before the tangent is "
+                              "assembled), " % args.newton_rtol +
                               ("inexact Newton (Eisenstat-Walker forcing tolerances, Dirichlet values lifted "
                                "into the state at step start), " if args.forcing == "ew" else "") +
                               ("tangent reused while Newton contracts within %g x the linear tolerance, "
-                               % args.tangent_reuse if (args.tangent_reuse > 0 and mixed) else "") +
+                               % args.tangent_reuse if args.tangent_reuse > 0 else "") +
                               ("RCR outlets coupled by the relaxed fixed point (relaxation %g, tolerance "
                                "1e-8 + 1e-6 |P|; %s), " % (OUTLET_RELAXATION,
                                                           "pressures updated inside the Newton loop"
@@ -883,7 +974,8 @@ def main():
                                                           "the reference's outer loop") if models else "") +
                               ("point-block two-level AMG-preconditioned FGMRES(%d)%s" % (args.restart, " rtol 1e-8" if args.forcing == "fixed"
                                                                                    else "") if amg else
-                               "block-Jacobi GMRES(200) rtol 1e-8")),
+                               "block-Jacobi GMRES(%d) rtol 1e-8" % args.restart)),
+                   "newton_rtol": args.newton_rtol,
                    "l2": "inputs larger than L2 (matrix %.2f GB)" % (mesh.blocks * 128 / 1e9),
                    "parallelism": "replicas only" if world > 1 else "single GPU"},
         "newton_per_step": float(newton), "linear_iterations_per_newton": float(linear),
@@ -892,6 +984,9 @@ def main():
         "outlet_iterations_per_step": (float(np.mean([r.get("outlet_iterations", r.get("pressure_updates", 0))
                                                       for r in timed_reports])) if outlets else None),
         "roofline": roof, "kernels": kernels,
+        "profile_pass": {"ms_per_step": prof_ms / args.steps, "attributed_share": attributed,
+                         "note": "kernel families timed in a repeat of the timed steps; shares are of that "
+                                 "pass's duration"},
         "fp64_gpu": fp64_leg,
         "spmv_gbs": kernels.get(spmv_name, {}).get("achieved"),
         "gpu_launches": int(launches),
@@ -899,10 +994,15 @@ def main():
         "e2e": {"value": replica_throughput(world, args.steps, e2e_ms), "unit": "time steps/s",
                 "h2d_bytes_per_step": 3 * n * 8, "d2h_bytes_per_step": 4 * n * 8},
     }
+    if fp64_leg:
+        line["mixed_over_fp64"] = {m: steps_per_s / v["value"] for m, v in fp64_leg["variants"].items()}
     if not args.no_cpu_baseline and world == 1:
         st = ns.get_state()
         try:
-            cb = cpu_reference(tube, st, st, max(newton, 1.0), max(linear, 1.0), budget_s=args.ref_budget)
+            rn, rl = reference_counts(args.workload) if args.workload in REFERENCE_COUNTS else (newton, linear)
+            cpu = CpuReference(tube, st, st)
+            cpu.calibrate(args.ref_budget)
+            cb = cpu.sample(rn, rl)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as exc:  # noqa: BLE001 -- reported, not hidden
             line["cpu_baseline"] = {"value": None, "error": str(exc)}
@@ -910,7 +1010,6 @@ def main():
     if dist:
         dist.destroy_process_group()
     return 0
-
 
 if __name__ == "__main__":
     sys.exit(main())

@@ -123,15 +123,15 @@ typedef struct tfiga_ns_params {
 	 * that of the PDE rows at the lifted state.  0 (default): every system to
 	 * gmres_rtol and no lifting, as the reference. */
 	int32_t newton_forcing;        /* default 0 */
-	/* Tensor-core modes: a factor c > 0 keeps the previous Newton iteration's
+	/* Every precision mode: a factor c > 0 keeps the previous Newton iteration's
 	 * tangent (and its Dirichlet rows) while that iteration reached what its linear
 	 * tolerance allowed, |r_k| <= c eta_{k-1} |r_{k-1}| (eta the relative tolerance
 	 * of the previous linear solve): a tangent that still gives the contraction the
-	 * linear solve asked for is good enough.  The tangent is contracted afresh at the
+	 * linear solve asked for is good enough.  The tangent is assembled afresh at the
 	 * first iteration of every step and whenever the contraction falls short.  The
-	 * residual is always evaluated in FP64 at the current state, so only the Newton
-	 * convergence rate can change.  Ignored in TFIGA_PRECISION_FP64 (its assembly
-	 * computes residual and tangent together).  Default 0 (off). */
+	 * residual is always evaluated in FP64 at the current state (by its own kernel,
+	 * before the tangent, so a converged check assembles no tangent), so only the
+	 * Newton convergence rate can change.  Default 0 (off). */
 	double tangent_reuse_factor;   /* default 0 */
 } tfiga_ns_params;
 
@@ -526,6 +526,11 @@ int tfiga_transport_set_state(tfiga_transport* transport, const double* state);
 int tfiga_transport_get_state(tfiga_transport* transport, double* state);
 /* L and P after the boundary rows, [4*blocks] each (either may be NULL). */
 int tfiga_transport_matrices(tfiga_transport* transport, double* left, double* previous);
+/* y = M^{-1} x [2*nodes] (host or device) with the handle's flow-line factors
+ * (params.preconditioner TFIGA_TRANSPORT_FLOW_LINES; TFIGA_E_INVALID otherwise): the
+ * device application the GMRES uses, exposed to check it.  No counterpart in the
+ * reference (it preconditions with block-Jacobi). */
+int tfiga_transport_apply_preconditioner(tfiga_transport* transport, const double* x, double* y);
 /* Device time of the assembly launch sequence (ms), steps taken, kernel launches issued. */
 int tfiga_transport_info(const tfiga_transport* transport, double* assembly_ms, int32_t* steps, int64_t* launches);
 /* The handle's CUDA stream (a cudaStream_t). */

@@ -121,6 +121,8 @@ def ref():
         R.ref_resolve_boundaries.argtypes = [C.c_longlong, _ip, _dp, C.c_double, C.c_double, C.c_double, C.c_char_p,
                                              _ip, _ip, _ip, _dp, _dp, _dp, _dp,
                                              np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+        R.ref_womersley_axial_velocity.argtypes = [C.c_double] * 5 + [_dp, _dp, C.c_int, C.c_double, C.c_double,
+                                                   C.POINTER(C.c_double)]
     return _ref
 
 
@@ -504,6 +506,117 @@ class FlowLines:
                                              self.factors, np.ascontiguousarray(rhs, np.float64), x, restart, maxit,
                                              rtol, C.byref(res))
         return x, it, res.value
+
+
+# --------------------------------------------------------------------------
+# Convergence diagnostics of the Newton loop and closed-form pipe flows
+# --------------------------------------------------------------------------
+
+def measure_flow_convergence(mesh, state, raw_rhs, use_ref=False):
+    """MeasureFlowConvergence (solvers/cuda/src/iga_cuda.cu:520-557): the continuity L2 norm and sum of
+    the raw rhs (after the traction, before the Dirichlet rows; continuity is field 3 of every node),
+    the boundary flow of the state per face label (IntegrateBoundaryFlow over every labelled face,
+    labels >= 0), their net and absolute sums in label order, and the relative mass imbalance
+    2 |net| / absolute (0 when no flow)."""
+    raw = np.asarray(raw_rhs, np.float64).reshape(-1, 4)
+    st = np.asarray(state, np.float64).reshape(-1, 4)
+    continuity_sq = 0.0
+    continuity_sum = 0.0
+    for c in raw[:, 3]:
+        continuity_sq += c * c
+        continuity_sum += c
+    flows = {}
+    labels_all = np.asarray(mesh.boundary_labels).reshape(-1, 6)
+    for e in np.nonzero((labels_all >= 0).any(axis=1))[0]:
+        conn, Cx, X, labels = mesh.element(int(e))
+        nodal = np.ascontiguousarray(st[conn])
+        for face in range(6):
+            if labels[face] >= 0:
+                lab = int(labels[face])
+                flows[lab] = flows.get(lab, 0.0) + boundary_flow(Cx, X, face, nodal, use_ref=use_ref)
+    net = 0.0
+    absolute = 0.0
+    for lab in sorted(flows):
+        net += flows[lab]
+        absolute += abs(flows[lab])
+    return {"continuity_l2": float(np.sqrt(continuity_sq)), "continuity_sum": float(continuity_sum),
+            "boundary_flow": flows, "net_boundary_flow": net, "absolute_boundary_flow": absolute,
+            "relative_mass_imbalance": 2.0 * abs(net) / absolute if absolute > 0.0 else 0.0}
+
+
+def newton_accepts(residual_l2, initial_residual_l2, dofs, nonlinear_atol, nonlinear_rtol, imbalance, mass_rtol):
+    """The Newton acceptance test of NavierStokes (solvers/cuda/src/iga_cuda.cu:989-996): accept when
+    ||r|| <= max(atol sqrt(dofs), rtol ||r_0||) and the relative mass imbalance <= mass_rtol.
+    Returns (accepted, tolerance)."""
+    tolerance = max(nonlinear_atol * np.sqrt(dofs), nonlinear_rtol * initial_residual_l2)
+    return bool(residual_l2 <= tolerance and imbalance <= mass_rtol), float(tolerance)
+
+
+def complex_bessel_j0(z):
+    """J0 of a complex argument by its power series sum_k (-z^2/4)^k / (k!)^2, summed until the term
+    falls below 8 eps of the sum past k > |z| (the series and stopping rule of ComplexBesselJ0,
+    solvers/cpu/include/WomersleyReference.hpp:131-148, in double precision)."""
+    z = complex(z)
+    factor = -z * z / 4.0
+    term = 1.0 + 0.0j
+    total = term
+    for order in range(1, 10001):
+        term *= factor / float(order * order)
+        total += term
+        if order > abs(z) and abs(term) <= 8.0 * np.finfo(float).eps * max(1.0, abs(total)):
+            return total
+    raise RuntimeError("complex Bessel J0 series did not converge")
+
+
+def womersley_axial_velocity(radius, density, viscosity, period, mean_gradient, cosine, sine, r, t,
+                             use_ref=False):
+    """Axial velocity of fully developed pipe flow driven by the pressure gradient (along the flow)
+    G(t) = mean + sum_k cosine[k] cos(k w t) + sine[k] sin(k w t), w = 2 pi / period
+    (WomersleyAxialVelocity, solvers/cpu/include/WomersleyReference.hpp:150-189): the Poiseuille part
+    mean (R^2 - r^2) / (4 mu) plus, for every harmonic k, Re[(cosine_k - i sine_k) / (i w_k rho)
+    (1 - J0(a_k r/R) / J0(a_k)) e^{i w_k t}] with a_k = alpha_k e^{-i pi/4}, alpha_k = R sqrt(w_k rho / mu)."""
+    cosine = np.asarray(cosine, np.float64)
+    sine = np.asarray(sine, np.float64)
+    h = max(len(cosine), len(sine))
+    cosine = np.pad(cosine, (0, h - len(cosine)))
+    sine = np.pad(sine, (0, h - len(sine)))
+    if use_ref:
+        out = C.c_double()
+        c = np.ascontiguousarray(cosine if h else np.zeros(1))
+        s = np.ascontiguousarray(sine if h else np.zeros(1))
+        if ref().ref_womersley_axial_velocity(radius, density, viscosity, period, mean_gradient, c, s, h, r, t,
+                                              C.byref(out)):
+            raise RuntimeError(ref().ref_last_error().decode())
+        return out.value
+    fraction = min(r / radius, 1.0)
+    velocity = mean_gradient * (radius * radius - r * r) / (4.0 * viscosity)
+    fundamental = 2.0 * np.pi / period
+    for k in range(h):
+        omega = (k + 1) * fundamental
+        alpha = radius * np.sqrt(omega * density / viscosity)
+        wall = complex(alpha / np.sqrt(2.0), -alpha / np.sqrt(2.0))
+        profile = 1.0 - complex_bessel_j0(wall * fraction) / complex_bessel_j0(wall)
+        amplitude = complex(cosine[k], -sine[k]) / (1j * omega * density) * profile
+        velocity += float((amplitude * np.exp(1j * omega * t)).real)
+    return velocity
+
+
+def evaluate_state(mesh, control_points, state, elements, points):
+    """The state sum_a N_a(xi) state_a and the physical point sum_a N_a(xi) P_a (the spline geometry map
+    through the control points P) at the parametric points `points` [m, 3] of every listed element.
+    Returns (x [len(elements) m, 3], state [len(elements) m, 4], det [len(elements) m]) with det the
+    Jacobian determinant of the map from the unit parametric cube (the volume weight of a unit-cube
+    quadrature rule)."""
+    st = np.asarray(state, np.float64).reshape(-1, 4)
+    xs, us, ms = [], [], []
+    for e in elements:
+        conn, Cx, X, _ = mesh.element(int(e))
+        for (u, v, w) in points:
+            N, _, _, _, det = basis(Cx, X, u, v, w, hessian=False)
+            xs.append(N @ control_points[conn])
+            us.append(N @ st[conn])
+            ms.append(det)
+    return np.array(xs), np.array(us), np.array(ms)
 
 
 def max_threads() -> int:

@@ -25,6 +25,7 @@
 //   MaterializeBoundaryWaveforms, MaterializeOutletPressures, ExtractPressureTractions,
 //   ResolveFlowBoundaries
 //   iga::ResolveBoundaryConditions     solvers/cpu/include/CaseInput.hpp:162-258
+//   iga::WomersleyAxialVelocity        solvers/cpu/include/WomersleyReference.hpp:150-189
 #include "BoundaryFlow.hpp"
 #include "BoundarySupport.hpp"
 #include "FlowCheckpoint.hpp"
@@ -34,6 +35,7 @@
 #include "PressureTraction.hpp"
 #include "TemporalFunction.hpp"
 #include "VtkOutput.hpp"
+#include "WomersleyReference.hpp"
 
 #include <omp.h>
 
@@ -526,6 +528,29 @@ int ref_transport_element(const double* C, const double* X, int nen, const doubl
 		const auto matrices = iga::BuildTransportElement(element, nodal, parameters);
 		std::memcpy(left, matrices.left.data(), sizeof(double)*matrices.left.size());
 		std::memcpy(previous, matrices.previous.data(), sizeof(double)*matrices.previous.size());
+		return 0;
+	} catch (const std::exception& error) {
+		last_error = error.what();
+		return -1;
+	}
+}
+
+// Axial Womersley velocity at radial distance r and time t of a pipe of the given radius driven by
+// the pressure gradient mean + sum_k cosine[k] cos((k+1) w t) + sine[k] sin((k+1) w t).
+int ref_womersley_axial_velocity(double radius, double density, double viscosity, double period,
+	double mean_gradient, const double* cosine, const double* sine, int harmonics, double r, double t,
+	double* velocity)
+{
+	try {
+		iga::WomersleyReferenceConfiguration configuration;
+		configuration.radius = radius;
+		configuration.density = density;
+		configuration.dynamic_viscosity = viscosity;
+		configuration.period = period;
+		configuration.mean_pressure_gradient = mean_gradient;
+		configuration.cosine_pressure_gradient.assign(cosine, cosine+harmonics);
+		configuration.sine_pressure_gradient.assign(sine, sine+harmonics);
+		*velocity = iga::WomersleyAxialVelocity(configuration, r, t);
 		return 0;
 	} catch (const std::exception& error) {
 		last_error = error.what();

@@ -1,0 +1,179 @@
+"""Converged flows against closed-form pipe flows (the reference's own validation targets).
+
+* C1 steady: the 1,280-element cylinder (R 1.5 mm, L 30 mm, rho 1060, mu 3.5e-3) with
+  the parabolic inflow of peak U = 0.2 m/s and a traction-free outlet, solved to the
+  steady state (dt = 0) by the plain FP64 solver.  Away from the ends the flow is
+  Poiseuille: u_z = U (1 - r^2/R^2), no transverse velocity, and an axial pressure
+  gradient dp/dz = -4 mu U / R^2 (the pressure drop 4 mu U L / R^2 of the C1
+  check).  The spline wall of this coarse O-grid lies slightly inside the circle of
+  radius R, so the profile is compared with the Poiseuille flow of the discrete
+  pipe -- the same cross-section area and flow rate -- on the middle third of the
+  tube with the oracle's basis functions (volume-weighted relative L2 of the
+  velocity; the fitted pressure gradient against Hagen-Poiseuille).
+* C2 pulsatile: the 8x8-core + 2x32-ring cross-section of the 51,200-element tube,
+  driven by a pressure drop with a mean and four Fourier harmonics at 1 Hz (inlet
+  traction, traction-free outlet, no-slip wall), stepped by the split-BF16 mixed
+  solver from the Womersley field at t = 0.  The axial velocity follows Womersley's
+  solution (the oracle's restatement of WomersleyAxialVelocity,
+  solvers/cpu/include/WomersleyReference.hpp:150-189, pinned to the compiled
+  reference in test_oracle.py), measured as the volume-weighted relative L2 error of
+  the velocity over the middle of the tube as the reference's validator does
+  (solvers/cpu/src/iga_flow_validate.cpp:113-150).
+
+Tolerances are stated beside each assertion; they bound the discretisation error of
+the coarse tricubic O-grid (its spline wall lies slightly inside the circle of
+radius R) and, for the pulsatile case, backward Euler's first-order time error.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RHO, MU = 1060.0, 3.5e-3
+# interior sample points of an element (parametric, unit cube), 3 per direction
+_G = (0.5 - np.sqrt(0.15), 0.5, 0.5 + np.sqrt(0.15))
+POINTS = [(u, v, w) for w in _G for v in _G for u in _G]
+WEIGHTS = np.array([a * b * c for c in (5, 8, 5) for b in (5, 8, 5) for a in (5, 8, 5)], np.float64) / 18.0 ** 3
+
+
+def middle_elements(tube, lo, hi):
+    """Elements whose control cell lies within lo <= z <= hi."""
+    z = tube.points[tube.cells][:, :, 2]
+    return np.nonzero((z.min(axis=1) >= lo) & (z.max(axis=1) <= hi))[0]
+
+
+def sample(tube, state, elements):
+    x, u, m = O.evaluate_state(tube.mesh, tube.points, state, elements, POINTS)
+    w = np.tile(WEIGHTS, len(elements)) * m
+    return x, u, w
+
+
+def fit_cross_section(tube, profile):
+    """Control values of an axial velocity that depends on the cross-section position only: the
+    weighted least-squares fit of profile(r) by the spline of one element layer, repeated on every
+    plane (the axial B-splines sum to one, so every layer then carries the same fit)."""
+    per_plane = tube.per_plane
+    first_layer = np.nonzero(tube.points[tube.cells][:, :, 2].max(axis=1) <= tube.points[per_plane, 2] + 1e-12)[0]
+    rows, target, weight = [], [], []
+    for e in first_layer:
+        conn, Cx, X, _ = tube.mesh.element(int(e))
+        for (u, v, w), wq in zip(POINTS, WEIGHTS):
+            N, _, _, _, det = O.basis(Cx, X, u, v, w, hessian=False)
+            row = np.zeros(per_plane)
+            np.add.at(row, conn % per_plane, N)
+            x = N @ tube.points[conn]
+            rows.append(row)
+            target.append(profile(np.hypot(x[0], x[1])))
+            weight.append(wq * det)
+    sw = np.sqrt(np.array(weight))
+    coef = np.linalg.lstsq(np.array(rows) * sw[:, None], np.array(target) * sw, rcond=None)[0]
+    return np.tile(coef, tube.planes)
+
+
+def test_c1_steady_flow_is_poiseuille(cylinder_1280):
+    from tubularflowiga_b200 import api
+    tube = cylinder_1280
+    R, L, U = tube.radius, tube.length, 0.2
+    vmask, pmask, vel = api.tube_boundary_conditions(tube, U)
+    # initial guess: Poiseuille at the control points
+    s0 = np.zeros((tube.mesh.nodes, 4))
+    s0[:, 2] = U * tube.profile[:, 2]
+    s0[:, 3] = 4.0 * MU * U * (L - tube.points[:, 2]) / R ** 2
+    s0[vmask != 0, :3] = vel[vmask != 0]
+    mesh = api.Mesh(tube.mesh)
+    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=0.0, preconditioner=api.AMG, nonlinear_rtol=1e-10,
+                          nonlinear_atol=1e-300, gmres_rtol=1e-10, max_newton=30)
+    ns.set_dirichlet(vmask, pmask, vel)
+    ns.set_tractions({2: 0.0})
+    ns.set_state(s0.ravel(), s0.ravel())
+    report = ns.step()
+    assert report["converged"]
+    state = ns.get_state()
+    ns.close()
+    z_lo, z_hi = L / 3, 2 * L / 3
+    x, u, w = sample(tube, state, middle_elements(tube, z_lo, z_hi))
+    # the discrete pipe: its spline wall lies inside the circle of radius R, so the profile is compared
+    # with the Poiseuille flow of the same cross-section area (effective radius) and the same flow rate
+    area = np.sum(w) / (z_hi - z_lo)
+    r_eff = np.sqrt(area / np.pi)
+    flow = np.sum(w * u[:, 2]) / (z_hi - z_lo)
+    u_eff = 2.0 * flow / area
+    r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / r_eff ** 2
+    exact = u_eff * (1.0 - r2)
+    err_axial = np.sqrt(np.sum(w * (u[:, 2] - exact) ** 2) / np.sum(w * exact ** 2))
+    err_transverse = np.sqrt(np.sum(w * (u[:, 0] ** 2 + u[:, 1] ** 2)) / np.sum(w * exact ** 2))
+    # pressure gradient: least-squares slope of p(z) over the samples, against Hagen-Poiseuille
+    A = np.stack([x[:, 2], np.ones_like(x[:, 2])], axis=1) * np.sqrt(w)[:, None]
+    slope = np.linalg.lstsq(A, u[:, 3] * np.sqrt(w), rcond=None)[0][0]
+    expect_slope = -4.0 * MU * u_eff / r_eff ** 2
+    err_gradient = abs(slope - expect_slope) / abs(expect_slope)
+    nominal = U * (1.0 - (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2)
+    err_nominal = np.sqrt(np.sum(w * (u[:, 2] - nominal) ** 2) / np.sum(w * nominal ** 2))
+    print(f"poiseuille: r_eff/R {r_eff / R:.5f} u_eff/U {u_eff / U:.5f}; axial {err_axial:.3e} transverse "
+          f"{err_transverse:.3e} dp/dz {slope:.6g} (Hagen-Poiseuille {expect_slope:.6g}, {err_gradient:.3e}; "
+          f"nominal {-4.0 * MU * U / R ** 2:.6g}); against the nominal profile {err_nominal:.3e}; "
+          f"newton {report['newton_iterations']}")
+    assert err_axial < 2e-2          # velocity profile, volume-weighted relative L2
+    assert err_transverse < 2e-3     # no secondary flow
+    assert err_gradient < 3e-2       # pressure gradient of the measured flow rate
+
+
+def womersley_case():
+    """Pressure gradient of the pulsatile case: a mean giving 0.15 m/s mean velocity (G0 = 8 mu Ubar / R^2)
+    and four harmonics at 1 Hz, cosine and sine amplitudes U(0, 1/3) G0 from seed 0."""
+    R = 1.5e-3
+    g0 = 8.0 * MU * 0.15 / R ** 2
+    rng = np.random.default_rng(0)
+    cosine = rng.uniform(0.0, 1.0 / 3.0, 4) * g0
+    sine = rng.uniform(0.0, 1.0 / 3.0, 4) * g0
+    return R, 1.0, g0, cosine, sine
+
+
+def gradient_at(g0, cosine, sine, period, t):
+    th = 2.0 * np.pi * t / period
+    return g0 + sum(c * np.cos((k + 1) * th) + s * np.sin((k + 1) * th)
+                    for k, (c, s) in enumerate(zip(cosine, sine)))
+
+
+def test_c2_pulsatile_flow_is_womersley():
+    from tubularflowiga_b200 import api, meshgen
+    R, period, g0, cosine, sine = womersley_case()
+    L = 12e-3
+    tube = meshgen.straight_tube(R, L, core=8, ring=2, layers=80)
+    dt, steps = 1e-3, 200
+    labels = tube.labels
+    vmask = (labels == 0).astype(np.int32)           # no-slip wall only: inlet and outlet are tractions
+    pmask = np.zeros_like(vmask)
+    vel = np.zeros((tube.mesh.nodes, 3))
+
+    def womersley(r, t):
+        return np.array([O.womersley_axial_velocity(R, RHO, MU, period, g0, cosine, sine, ri, t) for ri in r])
+
+    s0 = np.zeros((tube.mesh.nodes, 4))
+    s0[:, 2] = fit_cross_section(tube, lambda r: womersley([min(r, R)], 0.0)[0])
+    s0[vmask != 0, :3] = 0.0
+    s0[:, 3] = gradient_at(g0, cosine, sine, period, 0.0) * (L - tube.points[:, 2])
+    mesh = api.Mesh(tube.mesh)
+    ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=dt, preconditioner=api.AMG,
+                          precision=api.MIXED_BF16X3, nonlinear_rtol=1e-8, nonlinear_atol=1e-300, gmres_rtol=1e-8,
+                          gmres_restart=64, newton_forcing=1, tangent_reuse_factor=100.0, amg_coarse_period=3)
+    ns.set_dirichlet(vmask, pmask, vel)
+    ns.set_state(s0.ravel(), s0.ravel())
+    elements = middle_elements(tube, L / 4, 3 * L / 4)[::4]
+    errors = []
+    for k in range(1, steps + 1):
+        t = k * dt
+        ns.set_tractions({1: gradient_at(g0, cosine, sine, period, t) * L, 2: 0.0})
+        ns.commit_step()
+        assert ns.step()["converged"]
+        if k % 50 == 0:
+            x, u, w = sample(tube, ns.get_state(), elements)
+            r = np.hypot(x[:, 0], x[:, 1])
+            exact = womersley(np.minimum(r, R), t)
+            diff = (u[:, 0] ** 2 + u[:, 1] ** 2 + (u[:, 2] - exact) ** 2)
+            errors.append(float(np.sqrt(np.sum(w * diff) / np.sum(w * exact ** 2))))
+    ns.close()
+    print("womersley volume relative L2 at t = 0.05, 0.10, 0.15, 0.20 s:", errors)
+    assert max(errors) < 3e-2        # tricubic O-grid + backward Euler (omega_4 dt = 0.025)

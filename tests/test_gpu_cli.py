@@ -141,3 +141,51 @@ def test_vtu_pvd_and_velocity_manifest(case, tmp_path):
     assert [float(r.split(",")[0]) for r in rows[1:]] == pytest.approx([2e-3 * k for k in range(4)])
     bad = run("navier-stokes", db, d, "--output", tmp_path / "x.txt", "--visualization-format", "vtkhdf")
     assert bad.returncode == 1 and "HDF5" in bad.stderr
+
+
+def test_legacy_case_matches_oracle(tmp_path):
+    """A legacy case (simulation_parameter.txt, no simulation_config.json): the command takes the
+    reference's legacy branch (solvers/cuda/src/iga_cuda.cu:761-796: steady, viscosity 0.1, density 1,
+    boundaries from ResolveBoundaryConditions -- inlet velocity vplus x the reference velocity, Dirichlet
+    pressure on the outlet labels -- plus the no-slip wall trace).  Its converged state equals the
+    oracle's: Newton with direct solves of the oracle's FP64 systems, the boundary masks and values from
+    the reference's own compiled resolver, the wall trace added; velocity and pressure within 1e-8."""
+    import scipy.sparse.linalg as spla
+    from oracle import oracle as O
+    if not O.ref_available():
+        pytest.skip("reference element build (oracle/_ref) not present")
+    from tubularflowiga_b200 import meshgen
+    tube = meshgen.straight_tube(1.5e-3, 6e-3, core=4, ring=1, layers=4)
+    params = {"diffusion": 1e-5, "vplus": 0.8, "kplus": 0.5, "kminus": 0.1, "detach_plus": 0.2, "dt": 1e-3,
+              "steps": 1, "n0_bc": 1.0, "nplus_bc": 0.25, "artificial_diffusion": 1e-4}
+    db = meshgen.write_transport_case(tmp_path / "legacy", tube, params, velocity=0.05 * tube.profile)
+    out = tmp_path / "legacy.txt"
+    r = run("navier-stokes", db, tmp_path / "legacy", "--output", out, "--nonlinear-rtol", "1e-13",
+            "--nonlinear-atol", "1e-30")
+    assert r.returncode == 0, r.stderr
+    assert "boundary_config=legacy-defaults" in r.stdout
+    vel = np.loadtxt(out)
+    prs = np.loadtxt(str(out) + ".pressure")
+    # the oracle: legacy boundaries (reference resolver) + wall trace (the label-0 vertices of the
+    # generated tube), steady Newton with direct solves from zero
+    flat = tube.mesh
+    bc = O.ref_resolve_boundaries(tube.labels, 0.05 * tube.profile, params["vplus"], params["n0_bc"],
+                                  params["nplus_bc"])
+    vmask = bc["velocity_mask"].copy()
+    velocity = bc["velocity"].reshape(-1, 3).copy()
+    wall = tube.labels == 0
+    vmask[wall] = 1
+    velocity[wall] = 0.0
+    assert bc["pressure_mask"].sum() > 0
+    P = O.Pattern(flat.nodes, flat.element_offsets, flat.connectivity)
+    state = np.zeros(4 * flat.nodes)
+    for _ in range(20):
+        values, rhs = O.assemble(flat, P, state, None, 1.0, 0.1, 0.0)
+        O.apply_dirichlet(P, vmask, bc["pressure_mask"], velocity.ravel(), bc["pressure"], state, values, rhs)
+        update = spla.spsolve(P.to_scipy(values).tocsc(), rhs)
+        state = state + update
+        if np.linalg.norm(update) <= 1e-14 * np.linalg.norm(state):
+            break
+    ref = state.reshape(-1, 4)
+    assert np.linalg.norm(vel - ref[:, :3]) <= 1e-8 * np.linalg.norm(ref[:, :3])
+    assert np.linalg.norm(prs - ref[:, 3]) <= 1e-8 * np.linalg.norm(ref[:, 3])

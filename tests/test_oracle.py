@@ -273,3 +273,60 @@ def test_wall_trace_and_ntiga_reader_match_the_reference(tmp_path, small_tube, r
                                                    got.ctypes.data_as(ctypes.c_void_p), nodes, ctypes.byref(count)))
         assert count.value == n_ref > 0
         assert np.array_equal(got[:count.value], np.sort(want[:n_ref]))
+
+
+def test_womersley_restatement_known_answers():
+    """The reference's own known answers for its Womersley solution
+    (solvers/cpu/tests/test_womersley_reference.cpp:8-57), on the oracle's restatement."""
+    import scipy.special as sp
+    # the reference sums in long double (1e-14 there); in double the alternating series at |z| = 10
+    # cancels terms of size 1e3, so 1e-13 here
+    for value in (1.0, 5.0, 10.0):
+        assert abs(O.complex_bessel_j0(complex(value, 0.0)).real - sp.j0(value)) < 1e-13
+    moderate = O.complex_bessel_j0(complex(10.0, -10.0))
+    assert abs(moderate - complex(-2314.9753144452134, -411.5628570253805)) / abs(moderate) < 1e-13
+    args = dict(radius=1.0, density=1.0, viscosity=1.0, period=2.0, mean_gradient=4.0, cosine=[2.0], sine=[])
+    assert abs(O.womersley_axial_velocity(r=1.0, t=0.25, **args)) < 1e-14
+    assert abs(O.womersley_axial_velocity(r=0.4, t=0.25, **args) - O.womersley_axial_velocity(r=0.4, t=2.25, **args)) \
+        < 1e-13
+    steady = dict(args, cosine=[], sine=[])
+    assert abs(O.womersley_axial_velocity(r=0.5, t=17.0, **steady) - 0.75) < 1e-15
+    quasi = dict(args, mean_gradient=0.0, period=1e7)
+    assert abs(O.womersley_axial_velocity(r=0.0, t=0.0, **quasi) - 0.5) < 1e-7
+
+
+@requires_ref
+def test_womersley_restatement_matches_reference_build():
+    """The restatement against the reference's compiled WomersleyAxialVelocity on the pulsatile test's
+    pipe (R 1.5 mm, blood, 1 Hz, a mean and four harmonics): 1e-12 relative over radii and times."""
+    rng = np.random.default_rng(1)
+    g0 = 1866.7
+    cosine, sine = rng.uniform(0, 600, 4), rng.uniform(0, 600, 4)
+    for r in np.linspace(0.0, 1.5e-3, 7):
+        for t in (0.0, 0.13, 0.5, 0.77):
+            a = O.womersley_axial_velocity(1.5e-3, 1060.0, 3.5e-3, 1.0, g0, cosine, sine, r, t)
+            b = O.womersley_axial_velocity(1.5e-3, 1060.0, 3.5e-3, 1.0, g0, cosine, sine, r, t, use_ref=True)
+            assert abs(a - b) <= 1e-12 * max(abs(b), 1e-3)
+
+
+@requires_ref
+def test_flow_convergence_restatement_uses_the_reference_flow_integrals(small_tube):
+    """measure_flow_convergence: per-label flows with the restated face integral equal those with the
+    reference's compiled IntegrateBoundaryFlow; the imbalance of a state carrying only the inlet
+    profile is 2; continuity norms are those of field 3 of the raw rhs."""
+    flat = small_tube.mesh
+    rng = np.random.default_rng(5)
+    st = rng.normal(size=4 * flat.nodes)
+    raw = rng.normal(size=4 * flat.nodes)
+    a = O.measure_flow_convergence(flat, st, raw)
+    b = O.measure_flow_convergence(flat, st, raw, use_ref=True)
+    assert a["boundary_flow"].keys() == b["boundary_flow"].keys() == {0, 1, 2}
+    for k in a["boundary_flow"]:
+        assert abs(a["boundary_flow"][k] - b["boundary_flow"][k]) <= 1e-12 * b["absolute_boundary_flow"]
+    assert a["continuity_l2"] == pytest.approx(np.linalg.norm(raw[3::4]), rel=1e-14)
+    inlet_only = np.zeros((flat.nodes, 4))
+    inlet_only[small_tube.labels == 1, :3] = small_tube.profile[small_tube.labels == 1]
+    c = O.measure_flow_convergence(flat, inlet_only.ravel(), raw)
+    assert c["relative_mass_imbalance"] == pytest.approx(2.0, rel=1e-14)
+    assert O.newton_accepts(1.0, 1e9, 4 * flat.nodes, 1e-300, 1e-8, c["relative_mass_imbalance"], 1e-3)[0] is False
+    assert O.newton_accepts(1.0, 1e9, 4 * flat.nodes, 1e-300, 1e-8, c["relative_mass_imbalance"], 2.5)[0] is True

@@ -226,6 +226,7 @@ SIGNATURES = {
     "tfiga_transport_set_state": (C.c_int, [C.c_void_p, C.c_void_p]),
     "tfiga_transport_get_state": (C.c_int, [C.c_void_p, C.c_void_p]),
     "tfiga_transport_matrices": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_transport_apply_preconditioner": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "tfiga_transport_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32),
                                        C.POINTER(C.c_int64)]),
     "tfiga_transport_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
@@ -716,6 +717,15 @@ class Transport:
         previous = np.zeros(4 * self.mesh.blocks)
         check(lib().tfiga_transport_matrices(self._h, _p(left), _p(previous)))
         return left, previous
+
+    def apply_preconditioner(self, x):
+        """y = M^{-1} x with the handle's flow-line factors (TRANSPORT_FLOW_LINES handles only)."""
+        xs = np.ascontiguousarray(x, np.float64).reshape(-1)
+        if xs.size != 2 * self.mesh.nodes:
+            raise ValueError("x must have 2*nodes entries")
+        y = np.zeros_like(xs)
+        check(lib().tfiga_transport_apply_preconditioner(self._h, _p(xs), _p(y)))
+        return y
 
     def info(self) -> dict:
         ms = C.c_double(); steps = C.c_int32(); launches = C.c_int64()

@@ -189,6 +189,141 @@ constexpr size_t SharedBytes(int np)
 	return sizeof(double)*(size_t)(np*4+np*4+kQuad*kQS+kQuad*kCoef+kQuad*4+kChunkK*np+kChunkK*4*np);
 }
 
+// Elements with 65..80 basis functions (rare: the spline extraction's extraordinary vertices), from
+// their 80-wide tables.  CTA per (element, row field), 256 threads: nodal state, point state (warp per
+// point), the row field's coefficients M_q and residual coefficients (thread per point), the residual
+// (thread per basis function), then the tangent K^{if}_{ab} = sum_q sum_s Psi_s(a, q) sum_t
+// M_q^{if}[s][t] Phi_t(b, q) with one task per (a, eight consecutive b): per point the task folds its
+// test function into w[f][t] = sum_s Psi_s(a, q) M_q[f][s][t] and adds w[f][.] Phi_.(b, q) for its b.
+// FP64 throughout; the sums are added into FP64 or FP32 block storage.
+constexpr int kLargeThreads = 256;
+constexpr int kLargeBGroup = 8;
+
+constexpr size_t LargeSharedBytes()
+{
+	return sizeof(double)*(size_t)(kMaxBasisLarge*4*2+kQuad*kQS+kQuad*kCoef+kQuad*4);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kLargeThreads) AssembleLargeKernel(DeviceMeshView mesh, int first,
+	const double* __restrict__ phi, const double* __restrict__ qdata, const int32_t* __restrict__ element_blocks,
+	const double* __restrict__ state, const double* __restrict__ previous, AssemblyParams prm,
+	T* __restrict__ values, double* __restrict__ rhs)
+{
+	constexpr int NP = kMaxBasisLarge;
+	extern __shared__ __align__(16) double lsm[];
+	double* U = lsm;                          // [NP][4]
+	double* Up = U+NP*4;                      // [NP][4]
+	double* QS = Up+NP*4;                     // [64][kQS]
+	double* Msm = QS+kQuad*kQS;               // [64][kCoef]
+	double* RC = Msm+kQuad*kCoef;             // [64][4]
+	const int e = first+(blockIdx.x >> 2);
+	const int row = blockIdx.x & 3;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const int begin = mesh.element_offsets[e];
+	const int nen = mesh.element_offsets[e+1]-begin;
+	const double* P = phi+(size_t)(e-first)*kFeatures*kQuad*NP;
+
+	for (int a = tid; a < NP; a += kLargeThreads) {
+		double s[4] = {0.0, 0.0, 0.0, 0.0}, p[3] = {0.0, 0.0, 0.0};
+		if (a < nen) {
+			const size_t node = (size_t)mesh.connectivity[begin+a];
+			for (int f = 0; f < 4; ++f) s[f] = state[4*node+f];
+			if (prm.dt > 0.0) for (int f = 0; f < 3; ++f) p[f] = previous[4*node+f];
+		}
+		for (int f = 0; f < 4; ++f) U[a*4+f] = s[f];
+		for (int f = 0; f < 3; ++f) Up[a*4+f] = p[f];
+		Up[a*4+3] = 0.0;
+	}
+	__syncthreads();
+	for (int q = warp; q < kQuad; q += kLargeThreads/32) {
+		double v[22];
+		#pragma unroll
+		for (int k = 0; k < 22; ++k) v[k] = 0.0;
+		for (int a = lane; a < NP; a += 32) {
+			const double n = P[(0*kQuad+q)*NP+a];
+			const double g0 = P[(1*kQuad+q)*NP+a], g1 = P[(2*kQuad+q)*NP+a], g2 = P[(3*kQuad+q)*NP+a];
+			const double l = P[(4*kQuad+q)*NP+a];
+			const double uf[4] = {U[a*4], U[a*4+1], U[a*4+2], U[a*4+3]};
+			v[0] += n*uf[0]; v[1] += n*uf[1]; v[2] += n*uf[2]; v[3] += n*uf[3];
+			v[4] += n*Up[a*4]; v[5] += n*Up[a*4+1]; v[6] += n*Up[a*4+2];
+			#pragma unroll
+			for (int f = 0; f < 4; ++f) { v[7+3*f] += g0*uf[f]; v[8+3*f] += g1*uf[f]; v[9+3*f] += g2*uf[f]; }
+			v[19] += l*uf[0]; v[20] += l*uf[1]; v[21] += l*uf[2];
+		}
+		#pragma unroll
+		for (int k = 0; k < 22; ++k)
+			#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+		if (lane == 0)
+			#pragma unroll
+			for (int k = 0; k < 22; ++k) QS[q*kQS+k] = v[k];
+	}
+	__syncthreads();
+	if (tid < kQuad) {
+		PointState S;
+		const double* s = QS+tid*kQS;
+		for (int c = 0; c < 3; ++c) {
+			S.u[c] = s[kU+c]; S.up[c] = s[kUp+c]; S.lap[c] = s[kLap+c]; S.gp[c] = s[kGrad+9+c];
+			for (int d = 0; d < 3; ++d) S.gv[c][d] = s[kGrad+3*c+d];
+		}
+		S.p = s[kP];
+		RowCoefficients(row, S, qdata+((size_t)e*kQuad+tid)*kQData, prm, Msm+tid*kCoef, RC+tid*4);
+	}
+	__syncthreads();
+	if (rhs != nullptr)
+		for (int a = tid; a < nen; a += kLargeThreads) {
+			double r = 0.0;
+			for (int q = 0; q < kQuad; ++q)
+				#pragma unroll
+				for (int s = 0; s < 4; ++s) r += P[(s*kQuad+q)*NP+a]*RC[q*4+s];
+			atomicAdd(rhs+4*(size_t)mesh.connectivity[begin+a]+row, r);
+		}
+	if (values == nullptr) return;
+	const int32_t* EB = element_blocks+(size_t)(e-first)*NP*NP;
+	constexpr int kGroups = NP/kLargeBGroup;
+	for (int task = tid; task < NP*kGroups; task += kLargeThreads) {
+		const int a = task/kGroups, b0 = (task%kGroups)*kLargeBGroup;
+		if (a >= nen || b0 >= nen) continue;
+		double acc[kLargeBGroup][4];
+		#pragma unroll
+		for (int j = 0; j < kLargeBGroup; ++j)
+			#pragma unroll
+			for (int f = 0; f < 4; ++f) acc[j][f] = 0.0;
+		for (int q = 0; q < kQuad; ++q) {
+			double psi[4];
+			#pragma unroll
+			for (int s = 0; s < 4; ++s) psi[s] = P[(s*kQuad+q)*NP+a];
+			const double* Mq = Msm+q*kCoef;
+			double w[4][5];
+			#pragma unroll
+			for (int f = 0; f < 4; ++f)
+				#pragma unroll
+				for (int t = 0; t < 5; ++t)
+					w[f][t] = psi[0]*Mq[f*20+t]+psi[1]*Mq[f*20+5+t]+psi[2]*Mq[f*20+10+t]+psi[3]*Mq[f*20+15+t];
+			#pragma unroll
+			for (int j = 0; j < kLargeBGroup; ++j) {
+				double ph[5];
+				#pragma unroll
+				for (int t = 0; t < 5; ++t) ph[t] = P[(t*kQuad+q)*NP+b0+j];
+				#pragma unroll
+				for (int f = 0; f < 4; ++f)
+					acc[j][f] += w[f][0]*ph[0]+w[f][1]*ph[1]+w[f][2]*ph[2]+w[f][3]*ph[3]+w[f][4]*ph[4];
+			}
+		}
+		#pragma unroll
+		for (int j = 0; j < kLargeBGroup; ++j) {
+			const int b = b0+j;
+			if (b >= nen) break;
+			const int block = EB[a*NP+b];
+			if (block < 0) continue;
+			T* dst = values+(size_t)block*16+row*4;
+			#pragma unroll
+			for (int f = 0; f < 4; ++f) atomicAdd(dst+f, (T)acc[j][f]);
+		}
+	}
+}
+
 } // namespace
 
 void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double* qdata,
@@ -209,5 +344,28 @@ void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double*
 		state, previous, params, values, rhs);
 	LaunchCheck("AssembleKernel");
 }
+
+template <class T>
+void LaunchAssembleLarge(const DeviceMeshView& mesh, int first, int count, const double* phi, const double* qdata,
+	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params, T* values,
+	double* rhs, cudaStream_t stream)
+{
+	if (count == 0 || (values == nullptr && rhs == nullptr)) return;
+	constexpr size_t bytes = LargeSharedBytes();
+	static bool configured = false;
+	if (!configured) {
+		CudaCheck(cudaFuncSetAttribute(AssembleLargeKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)bytes), "large-element assembly shared-memory attribute");
+		configured = true;
+	}
+	AssembleLargeKernel<T><<<4u*(unsigned)count, kLargeThreads, bytes, stream>>>(mesh, first, phi, qdata,
+		element_blocks, state, previous, params, values, rhs);
+	LaunchCheck("AssembleLargeKernel");
+}
+
+template void LaunchAssembleLarge<double>(const DeviceMeshView&, int, int, const double*, const double*,
+	const int32_t*, const double*, const double*, AssemblyParams, double*, double*, cudaStream_t);
+template void LaunchAssembleLarge<float>(const DeviceMeshView&, int, int, const double*, const double*,
+	const int32_t*, const double*, const double*, AssemblyParams, float*, double*, cudaStream_t);
 
 } // namespace tfiga

@@ -53,11 +53,13 @@ __device__ __forceinline__ bool Invert(const double a[3][3], double inv[3][3], d
 
 constexpr int kChunk = 16;   // basis functions staged per shared-memory pass
 
+// Elements first + blockIdx.x; phi is indexed from `first` (table of NP padded functions per
+// element), qdata by the global element id.
 template <int NP>
-__global__ void __launch_bounds__(64) BuildBasisKernel(DeviceMeshView mesh, double* __restrict__ phi,
+__global__ void __launch_bounds__(64) BuildBasisKernel(DeviceMeshView mesh, int first, double* __restrict__ phi,
 	double* __restrict__ qdata)
 {
-	const int e = blockIdx.x;
+	const int e = first+blockIdx.x;
 	const int q = threadIdx.x;
 	__shared__ double X[192];
 	__shared__ double tile[kFeatures][kQuad][kChunk+1];
@@ -144,7 +146,7 @@ __global__ void __launch_bounds__(64) BuildBasisKernel(DeviceMeshView mesh, doub
 		// Coalesced write-out: kChunk consecutive basis entries per (feature, point).
 		for (int idx = q; idx < kFeatures*kQuad*kChunk; idx += 64) {
 			const int l = idx%kChunk, qq = (idx/kChunk)%kQuad, t = idx/(kChunk*kQuad);
-			phi[(((size_t)e*kFeatures+t)*kQuad+qq)*NP+chunk+l] = tile[t][qq][l];
+			phi[(((size_t)(e-first)*kFeatures+t)*kQuad+qq)*NP+chunk+l] = tile[t][qq][l];
 		}
 		__syncthreads();
 	}
@@ -153,9 +155,10 @@ __global__ void __launch_bounds__(64) BuildBasisKernel(DeviceMeshView mesh, doub
 // Block index of every (a, b) basis pair of every element, by binary search
 // of the sorted block row (FindBlock, SparseKernels.cuh:13-23), done once.
 template <int NP>
-__global__ void ElementBlocksKernel(DeviceMeshView mesh, DevicePatternView pattern, int32_t* __restrict__ out)
+__global__ void ElementBlocksKernel(DeviceMeshView mesh, DevicePatternView pattern, int first,
+	int32_t* __restrict__ out)
 {
-	const int e = blockIdx.x;
+	const int e = first+blockIdx.x;
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	for (int pair = threadIdx.x; pair < NP*NP; pair += blockDim.x) {
@@ -172,7 +175,7 @@ __global__ void ElementBlocksKernel(DeviceMeshView mesh, DevicePatternView patte
 			}
 			block = first < end && pattern.columns[first] == column ? first : -1;
 		}
-		out[(size_t)e*NP*NP+pair] = block;
+		out[(size_t)(e-first)*NP*NP+pair] = block;
 	}
 }
 
@@ -222,21 +225,21 @@ __global__ void __launch_bounds__(64) FaceCoefficientsKernel(DeviceMeshView mesh
 	__syncthreads();
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
-	const int a = threadIdx.x;
-	double F[3] = {0.0, 0.0, 0.0};
-	if (a < nen) {
-		const int lo = mesh.extraction_offsets[begin+a], hi = mesh.extraction_offsets[begin+a+1];
-		for (int s = 0; s < 16; ++s) {
-			double N = 0.0;
-			for (int k = lo; k < hi; ++k) {
-				const int p = mesh.extraction_columns[k];
-				N += mesh.extraction_values[k]*B[s][0][p&3]*B[s][1][(p>>2)&3]*B[s][2][p>>4];
+	for (int a = threadIdx.x; a < NP; a += blockDim.x) {
+		double F[3] = {0.0, 0.0, 0.0};
+		if (a < nen) {
+			const int lo = mesh.extraction_offsets[begin+a], hi = mesh.extraction_offsets[begin+a+1];
+			for (int s = 0; s < 16; ++s) {
+				double N = 0.0;
+				for (int k = lo; k < hi; ++k) {
+					const int p = mesh.extraction_columns[k];
+					N += mesh.extraction_values[k]*B[s][0][p&3]*B[s][1][(p>>2)&3]*B[s][2][p>>4];
+				}
+				for (int c = 0; c < 3; ++c) F[c] += scale[s][c]*N;
 			}
-			for (int c = 0; c < 3; ++c) F[c] += scale[s][c]*N;
 		}
-	}
-	if (a < NP)
 		for (int c = 0; c < 3; ++c) face_coef[((size_t)face_id*NP+a)*3+c] = F[c];
+	}
 }
 
 } // namespace
@@ -244,23 +247,44 @@ __global__ void __launch_bounds__(64) FaceCoefficientsKernel(DeviceMeshView mesh
 void LaunchBuildBasis(const DeviceMeshView& mesh, double* phi, double* qdata, cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
-	BuildBasisKernel<kMaxBasis><<<mesh.elements, 64, 0, stream>>>(mesh, phi, qdata);
+	BuildBasisKernel<kMaxBasis><<<mesh.elements, 64, 0, stream>>>(mesh, 0, phi, qdata);
 	LaunchCheck("BuildBasisKernel");
+}
+
+void LaunchBuildBasisLarge(const DeviceMeshView& mesh, int first, int count, double* phi, double* qdata,
+	cudaStream_t stream)
+{
+	if (count == 0) return;
+	BuildBasisKernel<kMaxBasisLarge><<<count, 64, 0, stream>>>(mesh, first, phi, qdata);
+	LaunchCheck("BuildBasisKernel<80>");
 }
 
 void LaunchElementBlocks(const DeviceMeshView& mesh, const DevicePatternView& pattern, int32_t* element_blocks,
 	cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
-	ElementBlocksKernel<kMaxBasis><<<mesh.elements, 256, 0, stream>>>(mesh, pattern, element_blocks);
+	ElementBlocksKernel<kMaxBasis><<<mesh.elements, 256, 0, stream>>>(mesh, pattern, 0, element_blocks);
 	LaunchCheck("ElementBlocksKernel");
 }
 
+void LaunchElementBlocksLarge(const DeviceMeshView& mesh, const DevicePatternView& pattern, int first, int count,
+	int32_t* element_blocks, cudaStream_t stream)
+{
+	if (count == 0) return;
+	ElementBlocksKernel<kMaxBasisLarge><<<count, 256, 0, stream>>>(mesh, pattern, first, element_blocks);
+	LaunchCheck("ElementBlocksKernel<80>");
+}
+
 void LaunchFaceCoefficients(const DeviceMeshView& mesh, int faces, const int32_t* face_element,
-	const int32_t* face_index, double* face_coef, cudaStream_t stream)
+	const int32_t* face_index, double* face_coef, int stride, cudaStream_t stream)
 {
 	if (faces == 0) return;
-	FaceCoefficientsKernel<kMaxBasis><<<faces, 64, 0, stream>>>(mesh, face_element, face_index, face_coef);
+	if (stride == kMaxBasis)
+		FaceCoefficientsKernel<kMaxBasis><<<faces, 64, 0, stream>>>(mesh, face_element, face_index, face_coef);
+	else if (stride == kMaxBasisLarge)
+		FaceCoefficientsKernel<kMaxBasisLarge><<<faces, 64, 0, stream>>>(mesh, face_element, face_index, face_coef);
+	else
+		Fail(-1, "face coefficient stride must be 64 or 80");
 	LaunchCheck("FaceCoefficientsKernel");
 }
 

@@ -694,6 +694,14 @@ int tfiga_transport_matrices(tfiga_transport* transport, double* left, double* p
 	});
 }
 
+int tfiga_transport_apply_preconditioner(tfiga_transport* transport, const double* x, double* y)
+{
+	return Guard([&] {
+		Require(transport && x && y, "null argument");
+		transport->solver->ApplyLinePreconditioner(x, y);
+	});
+}
+
 int tfiga_transport_info(const tfiga_transport* transport, double* assembly_ms, int32_t* steps, int64_t* launches)
 {
 	return Guard([&] {

@@ -18,6 +18,9 @@ constexpr int kQuad = 64;       // 4x4x4 Gauss points
 constexpr int kFeatures = 5;    // N, dN/dx, dN/dy, dN/dz, Laplacian
 constexpr int kQData = 10;
 constexpr int kMaxBasis = 64;   // padded basis count NP of the device tables
+// Elements with 65..80 basis functions (the reference's limit, solvers/cuda/include/DeviceMesh.hpp:55-56)
+// keep their own tables padded to 80 and go through the large-element kernels.
+constexpr int kMaxBasisLarge = 80;
 
 struct DeviceMeshView {
 	int nodes = 0;
@@ -45,11 +48,19 @@ struct AssemblyParams {
 };
 
 // ---- basis.cu -----------------------------------------------------------
+// Tables of the first mesh.elements elements (64 padded functions each).
 void LaunchBuildBasis(const DeviceMeshView& mesh, double* phi, double* qdata, cudaStream_t stream);
 void LaunchElementBlocks(const DeviceMeshView& mesh, const DevicePatternView& pattern, int32_t* element_blocks,
 	cudaStream_t stream);
+// Tables of the elements [first, first + count) with 80 padded functions: phi and element_blocks
+// indexed from `first`, qdata by the global element id.
+void LaunchBuildBasisLarge(const DeviceMeshView& mesh, int first, int count, double* phi, double* qdata,
+	cudaStream_t stream);
+void LaunchElementBlocksLarge(const DeviceMeshView& mesh, const DevicePatternView& pattern, int first, int count,
+	int32_t* element_blocks, cudaStream_t stream);
+// face_coef[face][stride][3] with stride 64 or 80 (the widest element of the mesh).
 void LaunchFaceCoefficients(const DeviceMeshView& mesh, int faces, const int32_t* face_element,
-	const int32_t* face_index, double* face_coef, cudaStream_t stream);
+	const int32_t* face_index, double* face_coef, int stride, cudaStream_t stream);
 
 // ---- assemble.cu --------------------------------------------------------
 // Exact-tangent VMS assembly: jacobian values (may be null: residual only) and
@@ -57,11 +68,19 @@ void LaunchFaceCoefficients(const DeviceMeshView& mesh, int faces, const int32_t
 void LaunchAssemble(const DeviceMeshView& mesh, const double* phi, const double* qdata,
 	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params,
 	double* values, double* rhs, cudaStream_t stream);
+// The same element (FP64 point state, coefficients, residual and exact tangent) for the elements
+// [first, first + count) with up to 80 basis functions, from their 80-wide tables; values (FP64 or
+// FP32 storage, may be null: residual only) and rhs (may be null: tangent only) are ADDED to.
+template <class T>
+void LaunchAssembleLarge(const DeviceMeshView& mesh, int first, int count, const double* phi, const double* qdata,
+	const int32_t* element_blocks, const double* state, const double* previous, AssemblyParams params, T* values,
+	double* rhs, cudaStream_t stream);
 
 // ---- tangent_tc.cu -----------------------------------------------------
 // Tensor-core tangent in two launches.  LaunchTangentPoint: FP64 point state,
 // the coefficients of all four row fields into coef (workspace of elements x 4
-// x 80 x 64 floats) and the FP64 residual ADDED into rhs (= -r).
+// x 80 x 64 floats; null: residual only) and the FP64 residual ADDED into rhs
+// (= -r).
 // LaunchTangentTc: the tangent contracted on the tcgen05 tensor cores from
 // coef and phi32 (the FP32 copy of phi, Mesh::phi32), BF16 or split-BF16
 // operands, FP32 accumulation, ADDED into the FP32 values; status bit 1 set if
@@ -117,10 +136,10 @@ template <class T>
 void LaunchDirichletRows(const DevicePatternView& pattern, int count, const int32_t* constrained_nodes,
 	const int32_t* velocity_mask, const int32_t* pressure_mask, const double* velocity, const double* pressure,
 	const double* state, T* values, double* rhs, cudaStream_t stream);
-void LaunchFaceFlows(int faces, const int32_t* face_element, const double* face_coef,
+void LaunchFaceFlows(int faces, const int32_t* face_element, const double* face_coef, int stride,
 	const int32_t* element_offsets, const int32_t* connectivity, const double* state, double* face_flow,
 	cudaStream_t stream);
-void LaunchFaceTraction(int faces, const int32_t* face_element, const double* face_coef,
+void LaunchFaceTraction(int faces, const int32_t* face_element, const double* face_coef, int stride,
 	const int32_t* element_offsets, const int32_t* connectivity, const double* face_pressure,
 	double* traction, cudaStream_t stream);
 // Deterministic sums: out[0] = sum x[i*stride+offset]^2, out[1] = sum x[i*stride+offset] over count items.

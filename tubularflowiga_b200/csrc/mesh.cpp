@@ -143,13 +143,55 @@ HostPattern BuildPattern(const HostMesh& mesh)
 	return p;
 }
 
+int64_t MoveLargeElementsLast(HostMesh& m)
+{
+	const int64_t E = m.elements();
+	std::vector<int64_t> order;
+	order.reserve((size_t)E);
+	for (int64_t e = 0; e < E; ++e)
+		if (m.element_offsets[e+1]-m.element_offsets[e] <= kMaxBasis) order.push_back(e);
+	const int64_t regular = (int64_t)order.size();
+	if (regular == E) return E;
+	for (int64_t e = 0; e < E; ++e)
+		if (m.element_offsets[e+1]-m.element_offsets[e] > kMaxBasis) order.push_back(e);
+	HostMesh out;
+	out.nodes = m.nodes;
+	out.max_basis = m.max_basis;
+	out.connectivity.reserve(m.connectivity.size());
+	out.extraction_offsets.reserve(m.extraction_offsets.size());
+	out.extraction_columns.reserve(m.extraction_columns.size());
+	out.extraction_values.reserve(m.extraction_values.size());
+	out.bezier_points.reserve(m.bezier_points.size());
+	out.boundary_labels.reserve(m.boundary_labels.size());
+	for (const int64_t e : order) {
+		for (int32_t k = m.element_offsets[e]; k < m.element_offsets[e+1]; ++k) {
+			out.connectivity.push_back(m.connectivity[k]);
+			const int32_t lo = m.extraction_offsets[k], hi = m.extraction_offsets[k+1];
+			out.extraction_columns.insert(out.extraction_columns.end(), m.extraction_columns.begin()+lo,
+				m.extraction_columns.begin()+hi);
+			out.extraction_values.insert(out.extraction_values.end(), m.extraction_values.begin()+lo,
+				m.extraction_values.begin()+hi);
+			out.extraction_offsets.push_back((int32_t)out.extraction_values.size());
+		}
+		out.element_offsets.push_back((int32_t)out.connectivity.size());
+		out.bezier_points.insert(out.bezier_points.end(), m.bezier_points.begin()+192*e,
+			m.bezier_points.begin()+192*(e+1));
+		out.boundary_labels.insert(out.boundary_labels.end(), m.boundary_labels.begin()+6*e,
+			m.boundary_labels.begin()+6*(e+1));
+	}
+	m = std::move(out);
+	return regular;
+}
+
 Mesh::Mesh(HostMesh host) : host_(std::move(host))
 {
 	RequireDevice();
 	host_.Validate();
-	if (host_.max_basis > kMaxBasis)
-		Fail(-7, "elements with more than 64 basis functions are not supported by this build (max_basis="
+	if (host_.max_basis > kMaxBasisLarge)
+		Fail(-7, "CUDA kernels support at most 80 basis functions per element (max_basis="
 			+std::to_string(host_.max_basis)+")");
+	regular_elements_ = MoveLargeElementsLast(host_);
+	face_stride_ = host_.max_basis > kMaxBasis ? kMaxBasisLarge : kMaxBasis;
 	pattern_ = BuildPattern(host_);
 	CudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "mesh stream");
 	const int64_t E = host_.elements();
@@ -170,11 +212,21 @@ Mesh::Mesh(HostMesh host) : host_(std::move(host))
 		extraction_columns_.get(), extraction_values_.get(), bezier_points_.get()};
 	pattern_view_ = {(int)host_.nodes, (long long)pattern_.columns.size(), row_offsets_.get(), columns_.get(),
 		diagonal_.get()};
-	phi_.Allocate((size_t)E*kFeatures*kQuad*kMaxBasis);
+	regular_view_ = view_;
+	regular_view_.elements = (int)regular_elements_;
+	const int64_t large = E-regular_elements_;
+	phi_.Allocate((size_t)regular_elements_*kFeatures*kQuad*kMaxBasis);
 	qdata_.Allocate((size_t)E*kQuad*kQData);
-	LaunchBuildBasis(view_, phi_.get(), qdata_.get(), stream_);
-	element_blocks_.Allocate((size_t)E*kMaxBasis*kMaxBasis);
-	LaunchElementBlocks(view_, pattern_view_, element_blocks_.get(), stream_);
+	LaunchBuildBasis(regular_view_, phi_.get(), qdata_.get(), stream_);
+	element_blocks_.Allocate((size_t)regular_elements_*kMaxBasis*kMaxBasis);
+	LaunchElementBlocks(regular_view_, pattern_view_, element_blocks_.get(), stream_);
+	if (large > 0) {
+		phi_large_.Allocate((size_t)large*kFeatures*kQuad*kMaxBasisLarge);
+		LaunchBuildBasisLarge(view_, (int)regular_elements_, (int)large, phi_large_.get(), qdata_.get(), stream_);
+		element_blocks_large_.Allocate((size_t)large*kMaxBasisLarge*kMaxBasisLarge);
+		LaunchElementBlocksLarge(view_, pattern_view_, (int)regular_elements_, (int)large,
+			element_blocks_large_.get(), stream_);
+	}
 	// Labelled boundary faces in element order.
 	std::vector<int32_t> fe, fi;
 	for (int64_t e = 0; e < E; ++e)
@@ -188,9 +240,9 @@ Mesh::Mesh(HostMesh host) : host_(std::move(host))
 	if (!faces_.empty()) {
 		up(face_element_, fe);
 		up(face_index_, fi);
-		face_coef_.Allocate(faces_.size()*kMaxBasis*3);
+		face_coef_.Allocate(faces_.size()*face_stride_*3);
 		LaunchFaceCoefficients(view_, (int)faces_.size(), face_element_.get(), face_index_.get(), face_coef_.get(),
-			stream_);
+			face_stride_, stream_);
 	}
 	std::vector<double> qd((size_t)E*kQuad*kQData);
 	qdata_.Download(qd.data(), qd.size(), stream_);
@@ -204,13 +256,14 @@ Mesh::Mesh(HostMesh host) : host_(std::move(host))
 	device_bytes_ = (int64_t)(element_offsets_.bytes()+connectivity_.bytes()+extraction_offsets_.bytes()
 		+extraction_columns_.bytes()+extraction_values_.bytes()+bezier_points_.bytes()+row_offsets_.bytes()
 		+columns_.bytes()+diagonal_.bytes()+phi_.bytes()+qdata_.bytes()+element_blocks_.bytes()
-		+face_element_.bytes()+face_index_.bytes()+face_coef_.bytes());
+		+face_element_.bytes()+face_index_.bytes()+face_coef_.bytes()+phi_large_.bytes()
+		+element_blocks_large_.bytes());
 }
 
 const float* Mesh::phi32()
 {
 	if (phi32_.get() == nullptr) {
-		const size_t count = (size_t)host_.elements()*kFeatures*kQuad*kMaxBasis;
+		const size_t count = (size_t)regular_elements_*kFeatures*kQuad*kMaxBasis;
 		phi32_.Allocate(count);
 		LaunchToFloat((long long)count, phi_.get(), phi32_.get(), stream_);
 		CudaCheck(cudaStreamSynchronize(stream_), "FP32 basis tables");

@@ -46,6 +46,15 @@ struct BoundaryFace {
 	int32_t label;
 };
 
+// Stable partition of the elements: those with at most 64 basis functions first, the others (up to
+// 80) last, each group in its original order.  Returns the number of elements in the first group.
+int64_t MoveLargeElementsLast(HostMesh& mesh);
+
+// Device mesh.  Elements with 65..80 basis functions (from the reference spline extraction's
+// extraordinary vertices) are moved behind the others at construction: the fast kernels run over
+// regular_view() (the first regular_elements(), 64-wide tables phi / element_blocks), the
+// large-element kernels over [large_first(), large_first() + large_count()) with 80-wide tables.
+// Meshes without such elements keep their element order.
 class Mesh {
 public:
 	explicit Mesh(HostMesh host);
@@ -56,6 +65,13 @@ public:
 	const HostMesh& host() const { return host_; }
 	const HostPattern& pattern() const { return pattern_; }
 	DeviceMeshView view() const { return view_; }
+	DeviceMeshView regular_view() const { return regular_view_; }
+	int64_t regular_elements() const { return regular_elements_; }
+	int large_first() const { return (int)regular_elements_; }
+	int large_count() const { return (int)(host_.elements()-regular_elements_); }
+	const double* phi_large() const { return phi_large_.get(); }
+	const int32_t* element_blocks_large() const { return element_blocks_large_.get(); }
+	int face_stride() const { return face_stride_; }
 	DevicePatternView pattern_view() const { return pattern_view_; }
 	const double* phi() const { return phi_.get(); }
 	// FP32 copy of the basis tables (operand staging of the tensor-core tangent), made on first use.
@@ -78,9 +94,12 @@ private:
 	DeviceArray<int32_t> element_offsets_, connectivity_, extraction_offsets_, row_offsets_, columns_, diagonal_,
 		element_blocks_, face_element_, face_index_;
 	DeviceArray<uint8_t> extraction_columns_;
-	DeviceArray<double> extraction_values_, bezier_points_, phi_, qdata_, face_coef_;
+	DeviceArray<double> extraction_values_, bezier_points_, phi_, qdata_, face_coef_, phi_large_;
+	DeviceArray<int32_t> element_blocks_large_;
 	DeviceArray<float> phi32_;
-	DeviceMeshView view_;
+	DeviceMeshView view_, regular_view_;
+	int64_t regular_elements_ = 0;
+	int face_stride_ = kMaxBasis;
 	DevicePatternView pattern_view_;
 	std::vector<BoundaryFace> faces_;
 	double min_detj_ = 0.0;

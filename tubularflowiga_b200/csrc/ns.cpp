@@ -165,8 +165,8 @@ void NsSolver::ApplyTractions(const std::map<int32_t, double>& traction)
 	traction_.Zero(stream_);
 	if (!faces.empty()) {
 		face_pressure_.Upload(fp.data(), fp.size(), stream_);
-		LaunchFaceTraction((int)faces.size(), mesh_.face_element(), mesh_.face_coef(), mesh_.view().element_offsets,
-			mesh_.view().connectivity, face_pressure_.get(), traction_.get(), stream_);
+		LaunchFaceTraction((int)faces.size(), mesh_.face_element(), mesh_.face_coef(), mesh_.face_stride(),
+			mesh_.view().element_offsets, mesh_.view().connectivity, face_pressure_.get(), traction_.get(), stream_);
 		launches_ += 1;
 	}
 	CudaCheck(cudaStreamSynchronize(stream_), "traction");
@@ -197,11 +197,22 @@ void NsSolver::AssembleResidualTc()
 {
 	rhs_.Zero(stream_);
 	profiler_.Begin(Profiler::kResidual, stream_);
-	LaunchTangentPoint(mesh_.view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
+	LaunchTangentPoint(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
 		{params_.density, params_.viscosity, params_.dt}, coef32_.get(), rhs_.get(), stream_);
+	LargeElements<float>(nullptr, rhs_.get());
 	profiler_.End(stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
 	launches_ += 2;
+}
+
+template <class T>
+void NsSolver::LargeElements(T* values, double* rhs)
+{
+	if (mesh_.large_count() == 0) return;
+	LaunchAssembleLarge<T>(mesh_.view(), mesh_.large_first(), mesh_.large_count(), mesh_.phi_large(), mesh_.qdata(),
+		mesh_.element_blocks_large(), state_.get(), previous_.get(), {params_.density, params_.viscosity, params_.dt},
+		values, rhs, stream_);
+	launches_ += 1;
 }
 
 void NsSolver::AssembleTangentTc()
@@ -209,11 +220,52 @@ void NsSolver::AssembleTangentTc()
 	amg_current_ = false;
 	values32_.Zero(stream_);
 	profiler_.Begin(Profiler::kAssembly, stream_);
-	LaunchTangentTc(mesh_.view(), mesh_.phi32(), coef32_.get(), mesh_.element_blocks(), values32_.get(), status_.get(),
-		params_.precision == TFIGA_PRECISION_MIXED_BF16X3, stream_);
+	LaunchTangentTc(mesh_.regular_view(), mesh_.phi32(), coef32_.get(), mesh_.element_blocks(), values32_.get(),
+		status_.get(), params_.precision == TFIGA_PRECISION_MIXED_BF16X3, stream_);
+	LargeElements<float>(values32_.get(), nullptr);
 	profiler_.End(stream_);
 	launches_ += 1;
 	if (amg_ && !amg_->built()) amg_->Build(values32_.get());
+}
+
+void NsSolver::AssembleResidual()
+{
+	if (tensor_tangent()) {
+		AssembleResidualTc();
+		return;
+	}
+	rhs_.Zero(stream_);
+	profiler_.Begin(Profiler::kResidual, stream_);
+	LaunchTangentPoint(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
+		{params_.density, params_.viscosity, params_.dt}, nullptr, rhs_.get(), stream_);
+	LargeElements<double>(nullptr, rhs_.get());
+	profiler_.End(stream_);
+	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
+	launches_ += 2;
+}
+
+void NsSolver::AssembleTangent()
+{
+	if (tensor_tangent()) {
+		AssembleTangentTc();
+		return;
+	}
+	amg_current_ = false;
+	values_.Zero(stream_);
+	profiler_.Begin(Profiler::kAssembly, stream_);
+	LaunchAssemble(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), mesh_.element_blocks(), state_.get(),
+		previous_.get(), {params_.density, params_.viscosity, params_.dt}, values_.get(), nullptr, stream_);
+	LargeElements<double>(values_.get(), nullptr);
+	profiler_.End(stream_);
+	launches_ += 1;
+	if (mixed()) {
+		LaunchToFloat((long long)blocks()*16, values_.get(), values32_.get(), stream_);
+		launches_ += 1;
+	}
+	if (amg_ && !amg_->built()) {
+		if (mixed()) amg_->Build(values32_.get());
+		else amg_->Build(values_.get());
+	}
 }
 
 void NsSolver::Assemble()
@@ -227,8 +279,9 @@ void NsSolver::Assemble()
 	values_.Zero(stream_);
 	rhs_.Zero(stream_);
 	profiler_.Begin(Profiler::kAssembly, stream_);
-	LaunchAssemble(mesh_.view(), mesh_.phi(), mesh_.qdata(), mesh_.element_blocks(), state_.get(), previous_.get(),
-		{params_.density, params_.viscosity, params_.dt}, values_.get(), rhs_.get(), stream_);
+	LaunchAssemble(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), mesh_.element_blocks(), state_.get(),
+		previous_.get(), {params_.density, params_.viscosity, params_.dt}, values_.get(), rhs_.get(), stream_);
+	LargeElements<double>(values_.get(), rhs_.get());
 	profiler_.End(stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
 	launches_ += 2;
@@ -340,8 +393,8 @@ void NsSolver::LaunchDiagnostics()
 	launches_ += 2;
 	const int faces = (int)mesh_.faces().size();
 	if (faces) {
-		LaunchFaceFlows(faces, mesh_.face_element(), mesh_.face_coef(), mesh_.view().element_offsets,
-			mesh_.view().connectivity, state_.get(), face_flow_.get(), stream_);
+		LaunchFaceFlows(faces, mesh_.face_element(), mesh_.face_coef(), mesh_.face_stride(),
+			mesh_.view().element_offsets, mesh_.view().connectivity, state_.get(), face_flow_.get(), stream_);
 		LaunchSegmentSums((int)labels_.size(), face_slot_.get(), faces, face_flow_.get(), label_flow_.get(), stream_);
 		launches_ += 2;
 	}
@@ -364,15 +417,15 @@ NsSolver::Diagnostics NsSolver::ReadDiagnostics()
 tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 {
 	tfiga_newton_report report{};
-	// Tensor-core modes: the FP64 residual comes from its own kernel, so the convergence test runs
-	// before the tangent, and an iteration that passes it contracts no tangent at all.
+	// Residual first (every precision mode): the FP64 residual comes from its own kernel, so the
+	// convergence test runs before the tangent, and an iteration that passes it assembles no
+	// tangent at all.  The residual is the one the combined assembly computes (same point
+	// formulas, FP64), so only the order of the floating-point sums differs.
 	const bool tc = tensor_tangent();
 	CudaCheck(cudaEventRecord(events_[0], stream_), "event");
-	if (tc) AssembleResidualTc();
-	else Assemble();
+	AssembleResidual();
 	LaunchDiagnostics();
-	if (tc) ApplyDirichletRhs();
-	else ApplyDirichlet();
+	ApplyDirichletRhs();
 	LaunchNorm(n4_, rhs_.get(), partial_.get(), scalars_.get()+kNorm, stream_);
 	launches_ += 2;
 	CudaCheck(cudaEventRecord(events_[1], stream_), "event");
@@ -400,19 +453,19 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	}
 	// Tangent reuse: keep the previous iteration's tangent while that iteration contracted the
 	// residual about as far as its linear tolerance allowed.
-	const bool reuse = tc && params_.tangent_reuse_factor > 0.0 && tangent_valid_ && initial_residual >= 0.0
+	const bool reuse = params_.tangent_reuse_factor > 0.0 && tangent_valid_ && initial_residual >= 0.0
 		&& norm <= params_.tangent_reuse_factor*reuse_eta_*reuse_norm_;
 	reuse_norm_ = norm;
-	if (tc && !reuse) {
+	if (!reuse) {
 		CudaCheck(cudaEventRecord(events_[4], stream_), "event");
-		AssembleTangentTc();
+		AssembleTangent();
 		ApplyDirichletMatrix();
 		tangent_valid_ = true;
 		++tangent_contractions_;
 		CudaCheck(cudaEventRecord(events_[5], stream_), "event");
-		status_.Download(pinned_status_, 1, stream_);
-		CudaCheck(cudaStreamSynchronize(stream_), "tensor-core tangent");
-		if (*pinned_status_ != 0)
+		if (tc) status_.Download(pinned_status_, 1, stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "tangent assembly");
+		if (tc && *pinned_status_ != 0)
 			Fail(-2, "tensor-core tangent: an MMA completion wait expired (status "+std::to_string(*pinned_status_)+")");
 		CudaCheck(cudaEventElapsedTime(&ms, events_[4], events_[5]), "event time");
 		report.assembly_ms += ms;
@@ -645,8 +698,8 @@ void NsSolver::BoundaryFlows(const int32_t* labels, int count, double* flows)
 	const int faces = (int)mesh_.faces().size();
 	std::vector<double> per_label(labels_.size(), 0.0);
 	if (faces) {
-		LaunchFaceFlows(faces, mesh_.face_element(), mesh_.face_coef(), mesh_.view().element_offsets,
-			mesh_.view().connectivity, state_.get(), face_flow_.get(), stream_);
+		LaunchFaceFlows(faces, mesh_.face_element(), mesh_.face_coef(), mesh_.face_stride(),
+			mesh_.view().element_offsets, mesh_.view().connectivity, state_.get(), face_flow_.get(), stream_);
 		LaunchSegmentSums((int)labels_.size(), face_slot_.get(), faces, face_flow_.get(), label_flow_.get(), stream_);
 		launches_ += 2;
 		label_flow_.Download(per_label.data(), labels_.size(), stream_);

@@ -91,6 +91,15 @@ private:
 	void AssembleResidualTc();
 	void ApplyDirichletParts(bool matrix, bool rhs);
 	void AssembleTangentTc();
+	// Every mode, for the residual-first Newton iteration: the FP64 residual alone (rhs = -r +
+	// traction; in the tensor-core modes with the point coefficients), then -- only for an
+	// iteration that solves with a new tangent -- the Jacobian alone (FP64 assembly, or the
+	// tensor-core contraction; builds the AMG on first use).
+	void AssembleResidual();
+	void AssembleTangent();
+	// The elements with 65..80 basis functions (FP64 large-element kernel): tangent added into values
+	// and residual into rhs, either may be null.  No launch when the mesh has none.
+	template <class T> void LargeElements(T* values, double* rhs);
 	std::vector<OutletModel> OutletModels(const tfiga_outlet* outlets, int count) const;
 	void LaunchDiagnostics();     // continuity sums of rhs + per-label flows of state
 	Diagnostics ReadDiagnostics();
@@ -102,9 +111,9 @@ private:
 	long long launches_ = 0;
 	long long solves_ = 0;                   // linear solves so far (coarse refresh period)
 	double forcing_norm_ = 0.0, forcing_eta_ = 0.0;   // previous residual and forcing term (inexact Newton)
-	bool tangent_valid_ = false;             // values32_ holds the tangent of this step's last iteration
+	bool tangent_valid_ = false;             // the Jacobian holds the tangent of this step's last iteration
 	double reuse_norm_ = 0.0, reuse_eta_ = 0.0;   // previous Newton residual and linear tolerance (tangent reuse)
-	long long tangent_contractions_ = 0;     // tensor-core tangent launches
+	long long tangent_contractions_ = 0;     // tangent assemblies (FP64 or tensor-core) by NewtonIteration
 	bool amg_current_ = false;               // the AMG data were refreshed from the current Jacobian
 	long long refreshes_ = 0;                // AMG refreshes so far (coarse refresh period)
 	std::map<int32_t, double> tractions_;    // label -> pressure set by SetTractions

@@ -150,18 +150,17 @@ __global__ void DirichletRowsKernel(DevicePatternView p, int count, const int32_
 
 // Outward flow of each boundary face: sum_a F[a].u_a (BoundaryFlow.hpp:165-200).
 __global__ void __launch_bounds__(64) FaceFlowKernel(int faces, const int32_t* __restrict__ face_element,
-	const double* __restrict__ coef, const int32_t* __restrict__ eo, const int32_t* __restrict__ conn,
+	const double* __restrict__ coef, int stride, const int32_t* __restrict__ eo, const int32_t* __restrict__ conn,
 	const double* __restrict__ state, double* __restrict__ out)
 {
 	const int face = blockIdx.x;
 	const int e = face_element[face];
 	const int begin = eo[e], nen = eo[e+1]-begin;
 	double v = 0.0;
-	const int a = threadIdx.x;
-	if (a < nen) {
+	for (int a = threadIdx.x; a < nen; a += 64) {
 		const size_t node = (size_t)conn[begin+a];
-		const double* F = coef+((size_t)face*kMaxBasis+a)*3;
-		v = F[0]*state[4*node]+F[1]*state[4*node+1]+F[2]*state[4*node+2];
+		const double* F = coef+((size_t)face*stride+a)*3;
+		v += F[0]*state[4*node]+F[1]*state[4*node+1]+F[2]*state[4*node+2];
 	}
 	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
 	__shared__ double part[2];
@@ -172,7 +171,7 @@ __global__ void __launch_bounds__(64) FaceFlowKernel(int faces, const int32_t* _
 
 // traction[4 node + c] -= p_face F[a][c] (IntegratePressureTractionForces, PressureTractionFlow.hpp:41-64).
 __global__ void __launch_bounds__(64) FaceTractionKernel(int faces, const int32_t* __restrict__ face_element,
-	const double* __restrict__ coef, const int32_t* __restrict__ eo, const int32_t* __restrict__ conn,
+	const double* __restrict__ coef, int stride, const int32_t* __restrict__ eo, const int32_t* __restrict__ conn,
 	const double* __restrict__ face_pressure, double* __restrict__ traction)
 {
 	const int face = blockIdx.x;
@@ -180,11 +179,11 @@ __global__ void __launch_bounds__(64) FaceTractionKernel(int faces, const int32_
 	if (pressure == 0.0) return;
 	const int e = face_element[face];
 	const int begin = eo[e], nen = eo[e+1]-begin;
-	const int a = threadIdx.x;
-	if (a >= nen) return;
-	const size_t node = (size_t)conn[begin+a];
-	const double* F = coef+((size_t)face*kMaxBasis+a)*3;
-	for (int c = 0; c < 3; ++c) atomicAdd(traction+4*node+c, -pressure*F[c]);
+	for (int a = threadIdx.x; a < nen; a += 64) {
+		const size_t node = (size_t)conn[begin+a];
+		const double* F = coef+((size_t)face*stride+a)*3;
+		for (int c = 0; c < 3; ++c) atomicAdd(traction+4*node+c, -pressure*F[c]);
+	}
 }
 
 __device__ __forceinline__ double BlockSum(double v, double* shared)
@@ -348,19 +347,20 @@ void LaunchLiftDirichlet(int count, const int32_t* nodes, const int32_t* vmask, 
 	LaunchCheck("LiftDirichletKernel");
 }
 
-void LaunchFaceFlows(int faces, const int32_t* face_element, const double* face_coef, const int32_t* eo,
+void LaunchFaceFlows(int faces, const int32_t* face_element, const double* face_coef, int stride, const int32_t* eo,
 	const int32_t* conn, const double* state, double* face_flow, cudaStream_t stream)
 {
 	if (faces == 0) return;
-	FaceFlowKernel<<<faces, 64, 0, stream>>>(faces, face_element, face_coef, eo, conn, state, face_flow);
+	FaceFlowKernel<<<faces, 64, 0, stream>>>(faces, face_element, face_coef, stride, eo, conn, state, face_flow);
 	LaunchCheck("FaceFlowKernel");
 }
 
-void LaunchFaceTraction(int faces, const int32_t* face_element, const double* face_coef, const int32_t* eo,
-	const int32_t* conn, const double* face_pressure, double* traction, cudaStream_t stream)
+void LaunchFaceTraction(int faces, const int32_t* face_element, const double* face_coef, int stride,
+	const int32_t* eo, const int32_t* conn, const double* face_pressure, double* traction, cudaStream_t stream)
 {
 	if (faces == 0) return;
-	FaceTractionKernel<<<faces, 64, 0, stream>>>(faces, face_element, face_coef, eo, conn, face_pressure, traction);
+	FaceTractionKernel<<<faces, 64, 0, stream>>>(faces, face_element, face_coef, stride, eo, conn, face_pressure,
+		traction);
 	LaunchCheck("FaceTractionKernel");
 }
 

@@ -300,6 +300,9 @@ __device__ __forceinline__ void PointCoefficients(const PointState& S, const dou
 	for (int k = 0; k < 40; ++k) out[(size_t)(40+k)*kQuad] = scratch[k];
 }
 
+// kWriteCoef: also write the tangent coefficients of the four row fields (false: the FP64
+// residual only, for the residual-first Newton check of the FP64 solver).
+template <bool kWriteCoef>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ state,
 	const double* __restrict__ previous, AssemblyParams prm, float* __restrict__ coef, double* __restrict__ rhs)
@@ -396,14 +399,23 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 		}
 		S.p = s[kP];
 		const double* qd = qdata+((size_t)e*kQuad+q)*kQData;
-		float* scratch = Scratch+tid*kScratchStride;
-		float* out = coef+((size_t)e*4+il)*kCoef*kQuad+q;
 		double* rc = RC+(il*kQuad+q)*kRcStride;
-		switch (il) {
-		case 0: PointCoefficients<0>(S, qd, prm, scratch, rc, out); break;
-		case 1: PointCoefficients<1>(S, qd, prm, scratch, rc, out); break;
-		case 2: PointCoefficients<2>(S, qd, prm, scratch, rc, out); break;
-		default: PointCoefficients<3>(S, qd, prm, scratch, rc, out); break;
+		if constexpr (kWriteCoef) {
+			float* scratch = Scratch+tid*kScratchStride;
+			float* out = coef+((size_t)e*4+il)*kCoef*kQuad+q;
+			switch (il) {
+			case 0: PointCoefficients<0>(S, qd, prm, scratch, rc, out); break;
+			case 1: PointCoefficients<1>(S, qd, prm, scratch, rc, out); break;
+			case 2: PointCoefficients<2>(S, qd, prm, scratch, rc, out); break;
+			default: PointCoefficients<3>(S, qd, prm, scratch, rc, out); break;
+			}
+		} else {
+			switch (il) {
+			case 0: RowCoefficients<float, 1, false>(0, S, qd, prm, nullptr, rc); break;
+			case 1: RowCoefficients<float, 1, false>(1, S, qd, prm, nullptr, rc); break;
+			case 2: RowCoefficients<float, 1, false>(2, S, qd, prm, nullptr, rc); break;
+			default: RowCoefficients<float, 1, false>(3, S, qd, prm, nullptr, rc); break;
+			}
 		}
 	}
 	__syncthreads();
@@ -632,14 +644,21 @@ void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const dou
 	const double* previous, AssemblyParams params, float* coef, double* rhs, cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
+	if (rhs == nullptr) Fail(-1, "tangent point kernel: the residual output is required");
 	static bool configured = false;
 	if (!configured) {
-		CudaCheck(cudaFuncSetAttribute(TangentPointKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		CudaCheck(cudaFuncSetAttribute(TangentPointKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
+		CudaCheck(cudaFuncSetAttribute(TangentPointKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
 		configured = true;
 	}
-	TangentPointKernel<<<(unsigned)mesh.elements, kTcThreads, kPtSmemBytes+16, stream>>>(mesh, phi, qdata, state,
-		previous, params, coef, rhs);
+	if (coef)
+		TangentPointKernel<true><<<(unsigned)mesh.elements, kTcThreads, kPtSmemBytes+16, stream>>>(mesh, phi, qdata,
+			state, previous, params, coef, rhs);
+	else
+		TangentPointKernel<false><<<(unsigned)mesh.elements, kTcThreads, kPtSmemBytes+16, stream>>>(mesh, phi, qdata,
+			state, previous, params, nullptr, rhs);
 	LaunchCheck("TangentPointKernel");
 }
 

@@ -47,8 +47,11 @@ TransportSolver::TransportSolver(Mesh& mesh, const TransportCoefficients& coeffi
 	CudaCheck(cudaEventCreate(&start), "event");
 	CudaCheck(cudaEventCreate(&stop), "event");
 	CudaCheck(cudaEventRecord(start, s), "event");
-	LaunchTransportAssembly(mesh_.view(), mesh_.phi(), mesh_.qdata(), mesh_.element_blocks(), velocity_device.get(),
-		coefficients, left_.get(), previous_.get(), s);
+	LaunchTransportAssembly(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), mesh_.element_blocks(),
+		velocity_device.get(), coefficients, left_.get(), previous_.get(), s);
+	LaunchTransportAssemblyLarge(mesh_.view(), mesh_.large_first(), mesh_.large_count(), mesh_.phi_large(),
+		mesh_.qdata(), mesh_.element_blocks_large(), velocity_device.get(), coefficients, left_.get(), previous_.get(),
+		s);
 	LaunchTransportBoundaryRows(pattern, constrained_count_, constrained_.get(), left_.get(), previous_.get(), s);
 	LaunchTransportBoundaryValues(constrained_count_, constrained_.get(), n0_.get(), nplus_.get(), current_.get(), s);
 	if (fp32_krylov) {
@@ -63,7 +66,7 @@ TransportSolver::TransportSolver(Mesh& mesh, const TransportCoefficients& coeffi
 	cudaEventDestroy(start);
 	cudaEventDestroy(stop);
 	assembly_ms_ = ms;
-	launches_ += 3;
+	launches_ += 3+(mesh_.large_count() > 0 ? 1 : 0);
 	gmres_.set_profiler(&profiler_);
 	if (flow_lines) {
 		// Built once on the host from L after the boundary rows (L is constant over the steps).
@@ -91,6 +94,8 @@ TransportSolver::TransportSolver(Mesh& mesh, const TransportCoefficients& coeffi
 		view.band_offsets = band_offsets_.get();
 		view.factors = line_factors_.get();
 		gmres_.set_line_preconditioner(&view);
+		line_view_ = view;
+		flow_lines_ = true;
 	}
 }
 
@@ -141,6 +146,19 @@ void TransportSolver::Matrices(double* left, double* previous)
 	if (left) left_.Download(left, count, mesh_.stream());
 	if (previous) previous_.Download(previous, count, mesh_.stream());
 	CudaCheck(cudaStreamSynchronize(mesh_.stream()), "transport matrices");
+}
+
+void TransportSolver::ApplyLinePreconditioner(const double* x, double* y)
+{
+	if (!flow_lines_) Fail(-1, "the transport handle has no flow-line preconditioner");
+	cudaStream_t s = mesh_.stream();
+	const size_t n2 = 2*(size_t)nodes_;
+	// rhs_ and next_ are step scratch: Step rewrites both before reading them
+	rhs_.Upload(x, n2, s);
+	LaunchLineApply(line_view_, rhs_.get(), next_.get(), nullptr, s);
+	launches_ += 1;
+	next_.Download(y, n2, s);
+	CudaCheck(cudaStreamSynchronize(s), "flow-line preconditioner");
 }
 
 double TransportSolver::StateNorm()

@@ -134,6 +134,97 @@ __global__ void __launch_bounds__(256, 1) TransportAssemblyKernel(DeviceMeshView
 	}
 }
 
+// Elements with 65..80 basis functions, from their 80-wide tables: CTA per element, 256 threads.  A warp
+// per point forms the interpolated velocity, tau and the point weight; then one task per (a, eight
+// consecutive b) sums M, S, P and X over the 64 points (T_a and u.grad N formed on the fly) and adds
+// the same 2x2 blocks as TransportAssemblyKernel.
+constexpr int kLargeGroup = 8;
+
+__global__ void __launch_bounds__(256) TransportAssemblyLargeKernel(DeviceMeshView mesh, int first,
+	const double* __restrict__ phi, const double* __restrict__ qdata, const int32_t* __restrict__ element_blocks,
+	const double* __restrict__ velocity, TransportCoefficients c, double* __restrict__ left,
+	double* __restrict__ previous)
+{
+	constexpr int NP = kMaxBasisLarge;
+	__shared__ double sVel[NP][3];
+	__shared__ double sU[kQuad][3];
+	__shared__ double sTau[kQuad], sW[kQuad];
+	const int e = first+blockIdx.x;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const int begin = mesh.element_offsets[e];
+	const int nen = mesh.element_offsets[e+1]-begin;
+	const double* P = phi+(size_t)(e-first)*kFeatures*kQuad*NP;
+	for (int i = tid; i < NP*3; i += blockDim.x) {
+		const int a = i/3, d = i-3*a;
+		sVel[a][d] = a < nen ? velocity[3*(size_t)mesh.connectivity[begin+a]+d] : 0.0;
+	}
+	__syncthreads();
+	for (int q = warp; q < kQuad; q += 8) {
+		double u[3] = {0.0, 0.0, 0.0};
+		for (int a = lane; a < NP; a += 32)
+			for (int d = 0; d < 3; ++d) u[d] += P[(0*kQuad+q)*NP+a]*sVel[a][d];
+		for (int d = 0; d < 3; ++d)
+			for (int o = 16; o > 0; o >>= 1) u[d] += __shfl_xor_sync(0xffffffffu, u[d], o);
+		double inverse_length = 0.0;
+		for (int a = lane; a < NP; a += 32)
+			inverse_length += fabs(u[0]*P[(1*kQuad+q)*NP+a]+u[1]*P[(2*kQuad+q)*NP+a]+u[2]*P[(3*kQuad+q)*NP+a]);
+		for (int o = 16; o > 0; o >>= 1) inverse_length += __shfl_xor_sync(0xffffffffu, inverse_length, o);
+		if (lane == 0) {
+			const double tau_space = inverse_length > 0.0 ? 1.0/inverse_length : 0.0;
+			const double tau_time = c.dt/2.0;
+			sTau[q] = tau_space > 0.0 ? 1.0/sqrt(1.0/(tau_space*tau_space)+1.0/(tau_time*tau_time)) : 0.0;
+			sW[q] = qdata[((size_t)e*kQuad+q)*kQData];
+			for (int d = 0; d < 3; ++d) sU[q][d] = u[d];
+		}
+	}
+	__syncthreads();
+	const double cad = c.dt*c.vplus*c.artificial_diffusion;
+	const double l00_mass = 1.0+c.dt*(c.kplus+c.kminus), l0p_mass = -c.detach_plus*c.dt;
+	const double lp0_p = -c.kplus*c.dt, lpp_p = 1.0+c.dt*c.detach_plus, l00_s = c.dt*c.diffusion;
+	const int32_t* EB = element_blocks+(size_t)(e-first)*NP*NP;
+	constexpr int kGroups = NP/kLargeGroup;
+	for (int task = tid; task < NP*kGroups; task += blockDim.x) {
+		const int a = task/kGroups, b0 = (task%kGroups)*kLargeGroup;
+		if (a >= nen || b0 >= nen) continue;
+		double M[kLargeGroup], S[kLargeGroup], Pp[kLargeGroup], X[kLargeGroup];
+		#pragma unroll
+		for (int j = 0; j < kLargeGroup; ++j) { M[j] = 0.0; S[j] = 0.0; Pp[j] = 0.0; X[j] = 0.0; }
+		for (int q = 0; q < kQuad; ++q) {
+			const double w = sW[q], u0 = sU[q][0], u1 = sU[q][1], u2 = sU[q][2];
+			const double na = P[(0*kQuad+q)*NP+a];
+			const double ga0 = P[(1*kQuad+q)*NP+a], ga1 = P[(2*kQuad+q)*NP+a], ga2 = P[(3*kQuad+q)*NP+a];
+			const double ta = na+sTau[q]*(u0*ga0+u1*ga1+u2*ga2);
+			const double wN = w*na, wT = w*ta;
+			#pragma unroll
+			for (int j = 0; j < kLargeGroup; ++j) {
+				const int b = b0+j;
+				const double nb = P[(0*kQuad+q)*NP+b];
+				const double gb0 = P[(1*kQuad+q)*NP+b], gb1 = P[(2*kQuad+q)*NP+b], gb2 = P[(3*kQuad+q)*NP+b];
+				const double gg = ga0*gb0+ga1*gb1+ga2*gb2;
+				M[j] = fma(wN, nb, M[j]);
+				S[j] = fma(w, gg, S[j]);
+				Pp[j] = fma(wT, nb, Pp[j]);
+				X[j] = fma(wT, c.dt*(u0*gb0+u1*gb1+u2*gb2)+cad*gg, X[j]);
+			}
+		}
+		#pragma unroll
+		for (int j = 0; j < kLargeGroup; ++j) {
+			const int b = b0+j;
+			if (b >= nen) break;
+			const int block = EB[a*NP+b];
+			if (block < 0) continue;
+			double* l = left+(size_t)block*4;
+			double* p = previous+(size_t)block*4;
+			atomicAdd(l, l00_mass*M[j]+l00_s*S[j]);
+			atomicAdd(l+1, l0p_mass*M[j]);
+			atomicAdd(l+2, lp0_p*Pp[j]);
+			atomicAdd(l+3, lpp_p*Pp[j]+X[j]);
+			atomicAdd(p, M[j]);
+			atomicAdd(p+3, Pp[j]);
+		}
+	}
+}
+
 // Constrained rows (ApplyTransportBoundaryKernel, IgaCudaKernels.cuh:411-424): zero in both
 // matrices, identity diagonal block in `left`.  A warp per constrained node.
 __global__ void TransportBoundaryRowsKernel(DevicePatternView p, int count, const int32_t* __restrict__ nodes,
@@ -300,6 +391,16 @@ void LaunchTransportAssembly(const DeviceMeshView& mesh, const double* phi, cons
 	TransportAssemblyKernel<<<mesh.elements, 256, 0, stream>>>(mesh, phi, qdata, element_blocks, velocity,
 		coefficients, left, previous);
 	LaunchCheck("TransportAssemblyKernel");
+}
+
+void LaunchTransportAssemblyLarge(const DeviceMeshView& mesh, int first, int count, const double* phi,
+	const double* qdata, const int32_t* element_blocks, const double* velocity,
+	const TransportCoefficients& coefficients, double* left, double* previous, cudaStream_t stream)
+{
+	if (count == 0) return;
+	TransportAssemblyLargeKernel<<<count, 256, 0, stream>>>(mesh, first, phi, qdata, element_blocks, velocity,
+		coefficients, left, previous);
+	LaunchCheck("TransportAssemblyLargeKernel");
 }
 
 void LaunchTransportBoundaryRows(const DevicePatternView& pattern, int count, const int32_t* nodes, double* left,

@@ -36,6 +36,10 @@ struct TransportCoefficients {
 void LaunchTransportAssembly(const DeviceMeshView& mesh, const double* phi, const double* qdata,
 	const int32_t* element_blocks, const double* velocity, const TransportCoefficients& coefficients, double* left,
 	double* previous, cudaStream_t stream);
+// The same for the elements [first, first + count) with up to 80 basis functions (80-wide tables).
+void LaunchTransportAssemblyLarge(const DeviceMeshView& mesh, int first, int count, const double* phi,
+	const double* qdata, const int32_t* element_blocks, const double* velocity,
+	const TransportCoefficients& coefficients, double* left, double* previous, cudaStream_t stream);
 void LaunchTransportBoundaryRows(const DevicePatternView& pattern, int count, const int32_t* nodes, double* left,
 	double* previous, cudaStream_t stream);
 void LaunchTransportBoundaryValues(int count, const int32_t* nodes, const double* n0, const double* nplus,
@@ -67,6 +71,8 @@ public:
 	void SetState(const double* state);   // [2 nodes], host or device
 	void GetState(double* state);         // [2 nodes], host or device
 	void Matrices(double* left, double* previous);   // [4 blocks] each, host or device
+	// y = M^{-1} x with the flow-line factors (flow_lines mode only), x and y [2 nodes], host or device.
+	void ApplyLinePreconditioner(const double* x, double* y);
 	double StateNorm();
 	int steps() const { return steps_; }
 	long long launches() const { return launches_; }
@@ -88,6 +94,8 @@ private:
 	DeviceArray<int32_t> line_offsets_, line_nodes_, band_width_;   // flow-line factors (flow_lines)
 	DeviceArray<int64_t> band_offsets_;
 	DeviceArray<double> line_factors_;
+	LinePreconditionerView line_view_;
+	bool flow_lines_ = false;
 	DeviceArray<int32_t> constrained_;
 	int constrained_count_ = 0;
 	Gmres gmres_;

@@ -29,8 +29,9 @@ struct PointState {
 // of N_a) x (trial feature t of N_b) in K^{if}_{ab}; rc[s] = -measure * c_s
 // gives the residual.  Computed in FP64; C is the storage type of M (double
 // for the FP64 tangent, float for the tensor-core tangent).  Only the column
-// fields f in [f_lo, f_hi) are written; rc may be null.
-template <class C, int kStride = 1>
+// fields f in [f_lo, f_hi) are written; rc may be null.  kTangent false: only
+// rc is computed (M is not touched and may be null).
+template <class C, int kStride = 1, bool kTangent = true>
 __device__ __forceinline__ void RowCoefficients(int i, const PointState& S, const double* qd,
 	const AssemblyParams& prm, C* M, double* rc, int f_lo = 0, int f_hi = 4)
 {
@@ -77,6 +78,7 @@ __device__ __forceinline__ void RowCoefficients(int i, const PointState& S, cons
 		rc[0] = -meas*divu;
 		for (int d = 0; d < 3; ++d) rc[1+d] = meas*fine[d];
 	}
+	if constexpr (!kTangent) return;
 	// Exact tangent (:248-312), collected by (test, trial) feature.
 	const double t3 = tau_m*tau_m*tau_m;
 	double dtau_c[3], A[3][3];
