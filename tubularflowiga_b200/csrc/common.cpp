@@ -1,5 +1,6 @@
 // Errors, CUDA checks, device requirement and allocation accounting.
 #include "common.hpp"
+#include "kernels.cuh"
 
 #include <cuda_bf16.h>
 
@@ -48,6 +49,7 @@ template class DeviceArray<float>;
 template class DeviceArray<int64_t>;
 template class DeviceArray<uint16_t>;
 template class DeviceArray<__nv_bfloat16>;
+template class DeviceArray<DeviceOutlet>;
 
 long long DeviceBytesLive() { return g_live.load(); }
 long long DeviceBytesPeak() { return g_peak.load(); }

@@ -153,4 +153,23 @@ void LaunchSegmentSums(int segments, const int32_t* segment_of, int items, const
 
 int PartialSlots();
 
+// ---- outlets.cu ---------------------------------------------------------
+// One 0D outlet coupled on the device (kind: TFIGA_OUTLET_*; slot: the label slot of its faces, -1 if
+// none).  capacitor_pressure is the value at the start of the step; pressure the one in use; flow,
+// evaluated and evaluated_capacitor the last evaluation.
+struct DeviceOutlet {
+	int32_t kind;
+	int32_t slot;
+	double resistance, proximal, distal, capacitance, reference_pressure, capacitor_pressure;
+	double pressure, flow, evaluated, evaluated_capacitor;
+};
+// Evaluates every outlet at label_flow; when `update` and the largest change exceeds
+// 1e-8 + 1e-6 max(1, max |P_eval|), relaxes all pressures (and adds one to *updates); *accepted = 1
+// when the pressures in use match their evaluation within that tolerance, else 0.
+void LaunchOutletUpdate(int count, DeviceOutlet* outlets, const double* label_flow, double dt, double relaxation,
+	bool update, double* accepted, int* updates, cudaStream_t stream);
+// face_pressure[f] = outlets[slot_outlet[face_slot[f]]].pressure, or base[f] when that is -1.
+void LaunchFacePressures(int faces, const int32_t* face_slot, const int32_t* slot_outlet, const double* base,
+	const DeviceOutlet* outlets, double* face_pressure, cudaStream_t stream);
+
 } // namespace tfiga

@@ -22,7 +22,8 @@ std::string Precise(double v)
 }
 
 // Scalar slots in scalars_ / pinned_.
-enum : int { kContinuity = 0 /* sq, sum */, kNorm = 2 /* norm, sum */, kUpdateNorm = 4, kSlots = 8 };
+enum : int { kContinuity = 0 /* sq, sum */, kNorm = 2 /* norm, sum */, kUpdateNorm = 4, kOutletAccepted = 6,
+	kSlots = 8 };
 
 } // namespace
 
@@ -387,12 +388,12 @@ GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 		&launches_);
 }
 
-void NsSolver::LaunchDiagnostics()
+void NsSolver::LaunchDiagnostics(bool flows)
 {
 	LaunchStridedSums(nodes(), 4, 3, rhs_.get(), partial_.get(), scalars_.get()+kContinuity, stream_);
 	launches_ += 2;
 	const int faces = (int)mesh_.faces().size();
-	if (faces) {
+	if (faces && flows) {
 		LaunchFaceFlows(faces, mesh_.face_element(), mesh_.face_coef(), mesh_.face_stride(),
 			mesh_.view().element_offsets, mesh_.view().connectivity, state_.get(), face_flow_.get(), stream_);
 		LaunchSegmentSums((int)labels_.size(), face_slot_.get(), faces, face_flow_.get(), label_flow_.get(), stream_);
@@ -423,8 +424,10 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	// formulas, FP64), so only the order of the floating-point sums differs.
 	const bool tc = tensor_tangent();
 	CudaCheck(cudaEventRecord(events_[0], stream_), "event");
+	const bool outlets = outlet_count_ >= 0;
+	if (outlets) CoupleOutletsOnDevice();
 	AssembleResidual();
-	LaunchDiagnostics();
+	LaunchDiagnostics(!outlets);
 	ApplyDirichletRhs();
 	LaunchNorm(n4_, rhs_.get(), partial_.get(), scalars_.get()+kNorm, stream_);
 	launches_ += 2;
@@ -435,6 +438,7 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	float ms = 0.0f;
 	CudaCheck(cudaEventElapsedTime(&ms, events_[0], events_[1]), "event time");
 	report.assembly_ms = ms;
+	if (outlets) last_outlet_ok_ = pinned_[kOutletAccepted] != 0.0;
 	const Diagnostics d = ReadDiagnostics();
 	report.continuity_l2 = d.continuity_l2;
 	report.continuity_sum = d.continuity_sum;
@@ -628,27 +632,93 @@ std::vector<OutletModel> NsSolver::OutletModels(const tfiga_outlet* outlets, int
 	return models;
 }
 
+void NsSolver::CoupleOutletsOnDevice()
+{
+	const int faces = (int)mesh_.faces().size();
+	if (faces) {
+		LaunchFaceFlows(faces, mesh_.face_element(), mesh_.face_coef(), mesh_.face_stride(),
+			mesh_.view().element_offsets, mesh_.view().connectivity, state_.get(), face_flow_.get(), stream_);
+		LaunchSegmentSums((int)labels_.size(), face_slot_.get(), faces, face_flow_.get(), label_flow_.get(), stream_);
+		launches_ += 2;
+	}
+	LaunchOutletUpdate(outlet_count_, outlets_dev_.get(), label_flow_.get(), params_.dt, outlet_relaxation_,
+		outlet_iteration_ > 0, scalars_.get()+kOutletAccepted, outlet_updates_.get(), stream_);
+	launches_ += 1;
+	traction_.Zero(stream_);
+	if (faces) {
+		LaunchFacePressures(faces, face_slot_.get(), slot_outlet_.get(), face_base_.get(), outlets_dev_.get(),
+			face_pressure_.get(), stream_);
+		LaunchFaceTraction(faces, mesh_.face_element(), mesh_.face_coef(), mesh_.face_stride(),
+			mesh_.view().element_offsets, mesh_.view().connectivity, face_pressure_.get(), traction_.get(), stream_);
+		launches_ += 2;
+	}
+	++outlet_iteration_;
+}
+
 tfiga_step_report NsSolver::StepOutletsCoupled(tfiga_outlet* outlets, int count, double relaxation, int max_newton,
 	int* updates)
 {
 	if (!(relaxation > 0.0 && relaxation <= 1.0)) Fail(-1, "invalid outlet coupling relaxation");
 	if (max_newton < 1) Fail(-1, "outlet coupling needs at least one Newton iteration");
-	std::vector<OutletModel> models = OutletModels(outlets, count);
-	std::vector<int32_t> labels(count);
-	std::vector<double> previous_capacitor(count), flows(count);
+	const std::vector<OutletModel> models = OutletModels(outlets, count);
+	// The models, the label slot -> outlet map and the fixed per-face tractions go to the device once;
+	// every Newton iteration then updates the outlets there (CoupleOutletsOnDevice).
+	std::vector<DeviceOutlet> host(count);
+	std::vector<int32_t> slot_outlet(std::max<size_t>(1, labels_.size()), -1);
 	for (int i = 0; i < count; ++i) {
-		labels[i] = outlets[i].label;
-		previous_capacitor[i] = outlets[i].capacitor_pressure;
+		const tfiga_outlet& o = outlets[i];
+		if (o.kind != TFIGA_OUTLET_RESISTANCE && !(params_.dt > 0.0))
+			Fail(-4, "RC/RCR outlets require positive transient dt");
+		DeviceOutlet& d = host[i];
+		d.kind = o.kind;
+		const auto it = slot_of_label_.find(o.label);
+		d.slot = it == slot_of_label_.end() ? -1 : it->second;
+		if (d.slot >= 0) slot_outlet[d.slot] = i;
+		d.resistance = o.resistance; d.proximal = o.proximal_resistance; d.distal = o.distal_resistance;
+		d.capacitance = o.capacitance; d.reference_pressure = o.reference_pressure;
+		d.capacitor_pressure = o.capacitor_pressure;
+		d.pressure = models[i].pressure;
+		d.flow = o.flow; d.evaluated = d.pressure; d.evaluated_capacitor = o.capacitor_pressure;
 	}
+	const auto& faces = mesh_.faces();
+	std::vector<double> base(faces.size(), 0.0);
+	for (size_t f = 0; f < faces.size(); ++f) {
+		const auto it = tractions_.find(faces[f].label);
+		if (it != tractions_.end()) base[f] = it->second;
+	}
+	if (outlets_dev_.size() < (size_t)std::max(1, count)) outlets_dev_.Allocate(std::max(1, count));
+	if (slot_outlet_.size() < slot_outlet.size()) slot_outlet_.Allocate(slot_outlet.size());
+	if (outlet_updates_.size() == 0) outlet_updates_.Allocate(1);
+	if (!faces.empty() && face_base_.size() < faces.size()) face_base_.Allocate(faces.size());
+	if (count) outlets_dev_.Upload(host.data(), count, stream_);
+	slot_outlet_.Upload(slot_outlet.data(), slot_outlet.size(), stream_);
+	if (!faces.empty()) face_base_.Upload(base.data(), base.size(), stream_);
+	outlet_updates_.Zero(stream_);
+	CudaCheck(cudaStreamSynchronize(stream_), "outlet upload");
+	struct Deactivate {
+		int& count;
+		~Deactivate() { count = -1; }
+	} deactivate{outlet_count_};
+	outlet_count_ = count;
+	outlet_relaxation_ = relaxation;
+	outlet_iteration_ = 0;
 	tfiga_step_report step{};
 	double initial = -1.0;
-	int changes = 0;
 	LiftDirichletForForcing();
 	tfiga_newton_report last{};
+	auto read_back = [&](bool accepted) {
+		int32_t changes = 0;
+		if (count) outlets_dev_.Download(host.data(), count, stream_);
+		outlet_updates_.Download(&changes, 1, stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "outlet read-back");
+		for (int i = 0; i < count; ++i) {
+			outlets[i].flow = host[i].flow;
+			outlets[i].pressure = accepted ? host[i].evaluated : host[i].pressure;
+			if (accepted) outlets[i].capacitor_pressure = host[i].evaluated_capacitor;
+		}
+		if (updates) *updates = changes;
+	};
 	for (int k = 0; k < max_newton; ++k) {
-		auto traction = tractions_;
-		for (const auto& m : models) traction[m.label] = m.pressure;
-		ApplyTractions(traction);
 		last = NewtonIteration(initial);
 		if (initial < 0.0) { initial = last.residual_l2; step.initial_residual_l2 = initial; }
 		step.assembly_ms += last.assembly_ms;
@@ -657,38 +727,13 @@ tfiga_step_report NsSolver::StepOutletsCoupled(tfiga_outlet* outlets, int count,
 		step.residual_l2 = last.residual_l2;
 		step.relative_mass_imbalance = last.relative_mass_imbalance;
 		if (!last.converged) ++step.newton_iterations;
-		// flows of the current state (after this iteration's update, if it solved)
-		BoundaryFlows(labels.data(), count, flows.data());
-		double change = 0.0, scale = 1.0;
-		std::vector<std::array<double, 2>> evaluated(count);
-		for (int i = 0; i < count; ++i) {
-			OutletModel m = models[i];
-			m.capacitor_pressure = previous_capacitor[i];
-			evaluated[i] = EvaluateOutletModel(m, flows[i], params_.dt);
-			change = std::max(change, std::fabs(evaluated[i][0]-models[i].pressure));
-			scale = std::max(scale, std::fabs(evaluated[i][0]));
-		}
-		if (last.converged && change <= 1e-8+1e-6*scale) {
-			for (int i = 0; i < count; ++i) {
-				outlets[i].flow = flows[i];
-				outlets[i].pressure = evaluated[i][0];
-				outlets[i].capacitor_pressure = evaluated[i][1];
-			}
+		if (last.converged && last_outlet_ok_) {
+			read_back(true);
 			step.converged = 1;
-			if (updates) *updates = changes;
 			return step;
 		}
-		if (change > 1e-8+1e-6*scale) {
-			++changes;
-			for (int i = 0; i < count; ++i) {
-				models[i].flow = flows[i];
-				models[i].pressure = (1.0-relaxation)*models[i].pressure+relaxation*evaluated[i][0];
-				outlets[i].flow = flows[i];
-				outlets[i].pressure = models[i].pressure;
-			}
-		}
 	}
-	if (updates) *updates = changes;
+	read_back(false);
 	Fail(-6, "Navier-Stokes nonlinear solve with coupled outlets reached MAX_NEWTON (nonlinear_residual="
 		+Precise(last.residual_l2)+", relative_mass_imbalance="+Precise(last.relative_mass_imbalance)+")");
 }

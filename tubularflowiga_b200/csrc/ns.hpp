@@ -101,7 +101,10 @@ private:
 	// and residual into rhs, either may be null.  No launch when the mesh has none.
 	template <class T> void LargeElements(T* values, double* rhs);
 	std::vector<OutletModel> OutletModels(const tfiga_outlet* outlets, int count) const;
-	void LaunchDiagnostics();     // continuity sums of rhs + per-label flows of state
+	void LaunchDiagnostics(bool flows);   // continuity sums of rhs (+ per-label flows of state when `flows`)
+	// Device outlet coupling of StepOutletsCoupled, before an iteration's residual: per-label flows of
+	// the state, the outlet update, the per-face pressures and the traction rhs.
+	void CoupleOutletsOnDevice();
 	Diagnostics ReadDiagnostics();
 
 	Mesh& mesh_;
@@ -138,6 +141,14 @@ private:
 	DeviceArray<double> pair_dinv_, pair_amg_, pair_aamg_;
 	DeviceArray<int> zero_flag_;
 	int32_t* pinned_status_ = nullptr;       // host mirror of the tensor-core kernel status
+	// outlets coupled on the device (StepOutletsCoupled): active while outlet_count_ >= 0
+	DeviceArray<DeviceOutlet> outlets_dev_;
+	DeviceArray<int32_t> slot_outlet_, outlet_updates_;
+	DeviceArray<double> face_base_;
+	int outlet_count_ = -1;
+	int outlet_iteration_ = 0;
+	double outlet_relaxation_ = 1.0;
+	bool last_outlet_ok_ = false;
 };
 
 } // namespace tfiga
