@@ -440,3 +440,37 @@ def test_simulation_config_errors_match_the_reference(api, tmp_path, small_tube)
         with pytest.raises(api.TfigaError) as err:
             api.resolve_flow_boundaries(path, t.labels, t.profile, 0.0)
         assert str(ref_error.value) in str(err.value), (k, str(ref_error.value), str(err.value))
+
+
+@requires_ref
+def test_periodic_table_waveforms_match_the_reference_set_up(api, small_tube, tmp_path):
+    """periodic_table inflow waveforms (a CSV of time,value samples, linearly interpolated and wrapped at
+    the period; TemporalFunction.hpp:45-134) through the flow boundary set-up against the reference's own
+    compiled chain: the materialised inlet values at times inside, between and past the samples and
+    across the wrap; and the CSV's validation messages."""
+    from tubularflowiga_b200 import meshgen
+    t = small_tube
+    rng = np.random.default_rng(4)
+    velocity = t.profile + 0.1 * rng.normal(size=t.profile.shape)
+    table = {"name": "inflow", "kind": "periodic_table", "units": "m/s", "period": 0.8, "file": "inflow.csv",
+             "interpolation": "linear"}
+    cfg = meshgen.simulation_config(1060.0, 3.5e-3, 2e-3, 4, 1.0, transient=True, waveform=table)
+    d = tmp_path / "table"
+    d.mkdir()
+    (d / "simulation_config.json").write_text(json.dumps(cfg))
+    (d / "inflow.csv").write_text("# inflow factor\ntime,value\n0.0, 0.4\n0.1,1.3\n 0.25 ,0.9\n0.5,0.2\n0.7,0.55\n")
+    keys = ("velocity_mask", "velocity", "pressure_mask", "pressure", "counts")
+    for time in (0.0, 0.05, 0.1, 0.3, 0.69, 0.75, 0.8, 1.23, 2.4001):
+        want = O.ref_flow_boundaries(d / "simulation_config.json", t.labels, velocity, time)
+        got = api.resolve_flow_boundaries(d / "simulation_config.json", t.labels, velocity, time)
+        for key in keys:
+            assert np.allclose(got[key], want[key], rtol=1e-15, atol=0), (time, key)
+    bad = {"one sample": "0.0,1.0\n", "not at zero": "0.1,1.0\n0.2,2.0\n", "decreasing": "0.0,1\n0.5,2\n0.3,3\n",
+           "past the period": "0.0,1\n0.9,2\n", "three fields": "0.0,1,2\n0.5,2\n", "text": "0.0,a\n0.5,2\n"}
+    for name, text in bad.items():
+        (d / "inflow.csv").write_text(text)
+        with pytest.raises(RuntimeError) as want:
+            O.ref_flow_boundaries(d / "simulation_config.json", t.labels, velocity, 0.3)
+        with pytest.raises(api.TfigaError) as got:
+            api.resolve_flow_boundaries(d / "simulation_config.json", t.labels, velocity, 0.3)
+        assert str(want.value) in str(got.value), (name, str(want.value), str(got.value))

@@ -13,6 +13,7 @@
 #include <array>
 #include <climits>
 #include <cmath>
+#include <filesystem>
 #include <cstring>
 #include <fstream>
 #include <exception>
@@ -523,7 +524,8 @@ int tfiga_resolve_flow_boundaries(const char* config_path, const char* system, d
 		const bool transient = flow.time_integration == "backward_euler";
 		const auto models = tfiga::InitializeOutletModels(config, flow);
 		const tfiga::SimulationConfig materialized = tfiga::MaterializeOutletPressures(
-			transient ? tfiga::MaterializeWaveforms(config, time) : config, models);
+			transient ? tfiga::MaterializeWaveforms(config,
+				std::filesystem::path(config_path).parent_path().string(), time) : config, models);
 		const tfiga::FlowSystem& resolved_system = tfiga::FindNavierStokesSystem(materialized, name);
 		const auto tractions = tfiga::ExtractPressureTractions(materialized, resolved_system);
 		std::vector<int> label(labels, labels+nodes);

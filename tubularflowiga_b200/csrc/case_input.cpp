@@ -1,5 +1,7 @@
 // Case input and host boundary physics (see case_input.hpp).
 #include "case_input.hpp"
+
+#include <filesystem>
 #include "json.hpp"
 
 #include <algorithm>
@@ -349,10 +351,74 @@ const FlowSystem& FindNavierStokesSystem(const SimulationConfig& config, const s
 	Fail(-4, "simulation configuration has no navier_stokes system named '"+name+"'");
 }
 
-double EvaluateTemporal(const TemporalFunction& f, double time)
+namespace {
+
+std::string TrimTemporal(const std::string& text)
+{
+	const auto first = text.find_first_not_of(" \t\r");
+	if (first == std::string::npos) return {};
+	const auto last = text.find_last_not_of(" \t\r");
+	return text.substr(first, last-first+1);
+}
+
+double TemporalNumber(const std::string& text, const std::string& context)
+{
+	const std::string token = TrimTemporal(text);
+	size_t used = 0;
+	double value = 0.0;
+	try {
+		value = std::stod(token, &used);
+	} catch (const std::exception&) {
+		Fail(-4, context+" contains a non-numeric value");
+	}
+	if (used != token.size() || !std::isfinite(value)) Fail(-4, context+" contains a non-finite or malformed value");
+	return value;
+}
+
+} // namespace
+
+std::vector<TemporalSample> ParseTemporalCsv(const std::string& text, double period, const std::string& context)
+{
+	if (!(period > 0.0)) Fail(-4, context+" requires a positive period");
+	std::vector<TemporalSample> samples;
+	std::istringstream input(text);
+	std::string line;
+	size_t number = 0;
+	while (std::getline(input, line)) {
+		++number;
+		line = TrimTemporal(line);
+		if (line.empty() || line.front() == '#') continue;
+		const auto comma = line.find(',');
+		if (comma == std::string::npos || line.find(',', comma+1) != std::string::npos)
+			Fail(-4, context+" line "+std::to_string(number)+" must contain exactly time,value");
+		const std::string first = TrimTemporal(line.substr(0, comma)), second = TrimTemporal(line.substr(comma+1));
+		if (samples.empty() && first == "time" && second == "value") continue;
+		const std::string where = context+" line "+std::to_string(number);
+		const double time = TemporalNumber(first, where), value = TemporalNumber(second, where);
+		if (time < 0.0 || time >= period) Fail(-4, context+" sample times must be in [0, period)");
+		if (!samples.empty() && !(time > samples.back().time))
+			Fail(-4, context+" sample times must be strictly increasing");
+		samples.push_back({time, value});
+	}
+	if (samples.size() < 2 || samples.front().time != 0.0)
+		Fail(-4, context+" requires at least two samples beginning at time zero");
+	return samples;
+}
+
+std::vector<TemporalSample> ReadTemporalCsv(const std::string& path, double period)
+{
+	std::ifstream in(path, std::ios::binary);
+	if (!in) Fail(-3, "cannot open temporal CSV: "+path);
+	std::ostringstream text;
+	text << in.rdbuf();
+	return ParseTemporalCsv(text.str(), period, path);
+}
+
+double EvaluateTemporal(const TemporalFunction& f, double time, const std::vector<TemporalSample>* samples)
 {
 	const double pi = 3.141592653589793238462643383279502884;
 	if (f.kind == "constant") return f.value;
+	if (!(f.period > 0.0)) Fail(-4, "temporal function period must be positive");
 	double wrapped = std::fmod(time, f.period);
 	if (wrapped < 0.0) wrapped += f.period;
 	const double theta = 2.0*pi*wrapped/f.period+f.phase;
@@ -365,10 +431,25 @@ double EvaluateTemporal(const TemporalFunction& f, double time)
 		}
 		return v;
 	}
-	Fail(-7, "periodic_table waveforms are not supported by this build");
+	if (samples == nullptr) Fail(-4, "periodic_table evaluation requires loaded samples");
+	if (samples->size() < 2 || samples->front().time != 0.0) Fail(-4, "periodic_table samples are invalid");
+	// the first sample after `wrapped`; past the last sample the segment closes on the first at t = period
+	const auto upper = std::upper_bound(samples->begin(), samples->end(), wrapped,
+		[](double value, const TemporalSample& sample) { return value < sample.time; });
+	TemporalSample lower, next;
+	if (upper == samples->end()) {
+		lower = samples->back();
+		next = {f.period, samples->front().value};
+	} else {
+		if (upper == samples->begin()) Fail(-4, "periodic_table samples must begin at zero");
+		lower = *(upper-1);
+		next = *upper;
+	}
+	const double fraction = (wrapped-lower.time)/(next.time-lower.time);
+	return lower.value+fraction*(next.value-lower.value);
 }
 
-SimulationConfig MaterializeWaveforms(const SimulationConfig& config, double time)
+SimulationConfig MaterializeWaveforms(const SimulationConfig& config, const std::string& case_directory, double time)
 {
 	SimulationConfig out = config;
 	for (auto& b : out.boundaries)
@@ -377,7 +458,15 @@ SimulationConfig MaterializeWaveforms(const SimulationConfig& config, double tim
 			const auto it = std::find_if(config.temporal.begin(), config.temporal.end(),
 				[&](const TemporalFunction& f) { return f.name == c.waveform; });
 			if (it == config.temporal.end()) Fail(-4, "unknown temporal function '"+c.waveform+"'");
-			const double factor = EvaluateTemporal(*it, time);
+			std::vector<TemporalSample> samples;
+			const std::vector<TemporalSample>* loaded = nullptr;
+			if (it->kind == "periodic_table") {
+				const std::filesystem::path relative(it->file);
+				if (relative.is_absolute()) Fail(-4, "temporal CSV path must be relative to the case directory");
+				samples = ReadTemporalCsv((std::filesystem::path(case_directory)/relative).string(), it->period);
+				loaded = &samples;
+			}
+			const double factor = EvaluateTemporal(*it, time, loaded);
 			if (c.profile.empty()) for (double& v : c.value) v *= factor;
 			else c.scale *= factor;
 			c.waveform.clear();

@@ -57,10 +57,23 @@ struct SimulationConfig {
 SimulationConfig ReadSimulationConfig(const std::string& path);
 // FindNavierStokesSystem (solvers/cpu/include/GenericCaseInput.hpp:153-172).
 const FlowSystem& FindNavierStokesSystem(const SimulationConfig& config, const std::string& name);
-// EvaluateTemporalFunction (include/TemporalFunction.hpp:97-143), analytic kinds.
-double EvaluateTemporal(const TemporalFunction& f, double time);
-// MaterializeBoundaryWaveforms (include/TemporalFunction.hpp:145-171).
-SimulationConfig MaterializeWaveforms(const SimulationConfig& config, double time);
+// One (time, value) sample of a periodic_table waveform.
+struct TemporalSample {
+	double time = 0.0, value = 0.0;
+};
+// ParseTemporalCsv / ReadTemporalCsv (include/TemporalFunction.hpp:45-88): `time,value` lines ('#'
+// comments, blank lines and a leading `time,value` header skipped), times strictly increasing in
+// [0, period), at least two samples starting at 0; the reference's messages.
+std::vector<TemporalSample> ParseTemporalCsv(const std::string& text, double period, const std::string& context);
+std::vector<TemporalSample> ReadTemporalCsv(const std::string& path, double period);
+// EvaluateTemporalFunction (include/TemporalFunction.hpp:97-134): constant, sinusoid, fourier, and
+// periodic_table (linear interpolation of `samples`, wrapping from the last sample to the first at
+// t = period).
+double EvaluateTemporal(const TemporalFunction& f, double time, const std::vector<TemporalSample>* samples = nullptr);
+// MaterializeBoundaryWaveforms (include/TemporalFunction.hpp:145-171): periodic_table files are read
+// relative to case_directory (absolute paths rejected).
+SimulationConfig MaterializeWaveforms(const SimulationConfig& config, const std::string& case_directory,
+	double time);
 
 // ReadLabeledHexMesh (solvers/cpu/include/BoundarySupport.hpp:25-73).
 struct LabeledHexMesh {

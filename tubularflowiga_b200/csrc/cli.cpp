@@ -457,7 +457,7 @@ int NavierStokes(int argc, char** argv)
 		return r;
 	};
 	std::map<int, double> tractions;
-	auto boundaries = resolve(transient ? MaterializeWaveforms(config, 0.0) : config, tractions);
+	auto boundaries = resolve(transient ? MaterializeWaveforms(config, case_dir.string(), 0.0) : config, tractions);
 	if (!transient)
 		for (const auto& m : outlets)
 			if (m.kind != "resistance") Fail(-4, "RC/RCR outlets require backward_euler flow");
@@ -528,7 +528,8 @@ int NavierStokes(int argc, char** argv)
 	for (int step = start_step; step < run_end; ++step) {
 		if (step > start_step) solver.CommitStep();
 		const double physical_time = transient ? (step+1)*dt : 0.0;
-		const SimulationConfig step_config = transient ? MaterializeWaveforms(config, physical_time) : config;
+		const SimulationConfig step_config = transient ? MaterializeWaveforms(config, case_dir.string(), physical_time)
+			: config;
 		std::vector<double> previous_capacitor(outlets.size());
 		for (size_t i = 0; i < outlets.size(); ++i) previous_capacitor[i] = outlets[i].capacitor_pressure;
 		const int max_outlet = outlets.empty() ? 1 : 12;
