@@ -27,13 +27,15 @@ struct Amg::Level {
 	// coarsest level
 	int dense_n = 0;
 	DeviceArray<double> dense, column;
-	DeviceArray<int> dense_flag;
+	DeviceArray<double> panel;          // blocked Gauss-Jordan: two n x 32 panel copies + the 32 x 32 pivot-block inverse
+	DeviceArray<int> dense_flag, pivots;
 	DevicePatternView view() const { return {nodes, blocks, rows.get(), cols.get(), diag.get()}; }
 };
 
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kPanel = 32;          // pivot columns per blocked Gauss-Jordan panel
 
 unsigned Grid(long long n, int per) { return (unsigned)((n+per-1)/per); }
 
@@ -273,6 +275,168 @@ __global__ void GaussJordanEliminateKernel(int n, int k, double* __restrict__ a,
 	const double f = column[i];
 	if (f == 0.0) return;
 	a[(size_t)i*ld+j] = j == k ? 0.0 : a[(size_t)i*ld+j]-f*a[(size_t)k*ld+j];
+}
+
+// Blocked Gauss-Jordan on the augmented [A | I] (n x 2n, row-major): 32 pivot columns per pair of
+// launches instead of one.  For the panel of columns k0 .. k0 + b - 1 (b <= 32):
+//   GaussJordanPanelKernel (one CTA): copies the panel's n x b columns twice (W, O), runs Gauss-Jordan
+//     with partial pivoting on W alone (pivot rows searched below k0 + jj, swaps applied to W and O), so
+//     that O ends up as the row-permuted original panel and the pivot block A_RR = O[k0 .. k0 + b) is
+//     factorable in natural order; inverts A_RR in shared memory (Gauss-Jordan without further
+//     pivoting: its pivots are the panel's) and records the swaps;
+//   GaussJordanUpdateKernel (CTA per 16 columns of all 2n): applies the swaps, then
+//     rows R = k0 .. k0 + b - 1  <-  Z = A_RR^{-1} Y_R,   every other row i  <-  Y_i - O_i Z,
+//   which is what the b single-column eliminations do to those columns.
+// A vanishing pivot (|max| <= 1e-300) raises *flag; the caller then redoes the inverse column by column.
+constexpr int kPanelThreads = 1024;
+constexpr int kUpdateColumns = 16;
+
+__global__ void __launch_bounds__(kPanelThreads) GaussJordanPanelKernel(int n, int k0, int b,
+	const double* __restrict__ a, double* __restrict__ panel, int* __restrict__ pivots, int* __restrict__ flag)
+{
+	const int ld = 2*n;
+	double* W = panel;                      // [n][b]
+	double* O = panel+(size_t)n*kPanel;     // [n][b]
+	double* Ainv = panel+(size_t)2*n*kPanel; // [b][b]
+	__shared__ double best_val[32];
+	__shared__ int best_idx[32];
+	__shared__ int pivot_row;
+	__shared__ double pivot_value;
+	__shared__ double block[kPanel][2*kPanel+1];
+	const int tid = threadIdx.x;
+	for (long long idx = tid; idx < (long long)n*b; idx += kPanelThreads) {
+		const int i = (int)(idx/b), j = (int)(idx%b);
+		const double v = a[(size_t)i*ld+k0+j];
+		W[(size_t)i*b+j] = v;
+		O[(size_t)i*b+j] = v;
+	}
+	__syncthreads();
+	for (int jj = 0; jj < b; ++jj) {
+		const int j = k0+jj;
+		double bv = -1.0; int bi = j;
+		for (int i = j+tid; i < n; i += kPanelThreads) {
+			const double v = fabs(W[(size_t)i*b+jj]);
+			if (v > bv) { bv = v; bi = i; }
+		}
+		for (int o = 16; o > 0; o >>= 1) {
+			const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+			const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+			if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+		}
+		if ((tid & 31) == 0) { best_val[tid >> 5] = bv; best_idx[tid >> 5] = bi; }
+		__syncthreads();
+		if (tid == 0) {
+			double v = -1.0; int idx = j;
+			for (int w = 0; w < kPanelThreads/32; ++w)
+				if (best_val[w] > v || (best_val[w] == v && best_idx[w] < idx)) { v = best_val[w]; idx = best_idx[w]; }
+			if (!(v > 1e-300)) { *flag = 1; idx = j; }
+			pivot_row = idx;
+			pivots[jj] = idx;
+		}
+		__syncthreads();
+		const int pr = pivot_row;
+		if (pr != j)
+			for (int c = tid; c < b; c += kPanelThreads) {
+				double t = W[(size_t)j*b+c]; W[(size_t)j*b+c] = W[(size_t)pr*b+c]; W[(size_t)pr*b+c] = t;
+				t = O[(size_t)j*b+c]; O[(size_t)j*b+c] = O[(size_t)pr*b+c]; O[(size_t)pr*b+c] = t;
+			}
+		__syncthreads();
+		if (tid == 0) {
+			const double v = W[(size_t)j*b+jj];
+			pivot_value = v != 0.0 ? v : 1.0;
+		}
+		__syncthreads();
+		const double inv = 1.0/pivot_value;
+		// eliminate column jj of the panel from every other row (row j scaled in place afterwards)
+		for (long long idx = tid; idx < (long long)n*b; idx += kPanelThreads) {
+			const int i = (int)(idx/b), c = (int)(idx%b);
+			if (i == j || c <= jj) continue;
+			const double f = W[(size_t)i*b+jj]*inv;
+			if (f != 0.0) W[(size_t)i*b+c] -= f*W[(size_t)j*b+c];
+		}
+		__syncthreads();
+		for (long long i = tid; i < n; i += kPanelThreads)
+			if (i != j) W[(size_t)i*b+jj] = 0.0;
+		for (int c = tid; c < b; c += kPanelThreads) W[(size_t)j*b+c] *= inv;
+		__syncthreads();
+	}
+	// inverse of the pivot block A_RR = O[k0 .. k0 + b) by Gauss-Jordan in natural order
+	for (int idx = tid; idx < b*2*b; idx += kPanelThreads) {
+		const int r = idx/(2*b), c = idx%(2*b);
+		block[r][c] = c < b ? O[(size_t)(k0+r)*b+c] : (c-b == r ? 1.0 : 0.0);
+	}
+	__syncthreads();
+	for (int jj = 0; jj < b; ++jj) {
+		if (tid == 0) {
+			const double v = block[jj][jj];
+			pivot_value = v != 0.0 ? v : 1.0;
+		}
+		__syncthreads();
+		const double inv = 1.0/pivot_value;
+		for (int idx = tid; idx < b*2*b; idx += kPanelThreads) {
+			const int r = idx/(2*b), c = idx%(2*b);
+			if (r == jj || c == jj) continue;
+			const double f = block[r][jj]*inv;
+			if (f != 0.0) block[r][c] -= f*block[jj][c];
+		}
+		__syncthreads();
+		for (int r = tid; r < b; r += kPanelThreads) if (r != jj) block[r][jj] = 0.0;
+		for (int c = tid; c < 2*b; c += kPanelThreads) block[jj][c] *= inv;
+		__syncthreads();
+	}
+	for (int idx = tid; idx < b*b; idx += kPanelThreads) Ainv[idx] = block[idx/b][b+idx%b];
+}
+
+__global__ void __launch_bounds__(256) GaussJordanUpdateKernel(int n, int k0, int b, double* __restrict__ a,
+	const double* __restrict__ panel, const int* __restrict__ pivots)
+{
+	const int ld = 2*n;
+	const double* O = panel+(size_t)n*kPanel;
+	const double* Ainv = panel+(size_t)2*n*kPanel;
+	__shared__ double sA[kPanel][kPanel+1];
+	__shared__ double sY[kPanel][kUpdateColumns];
+	__shared__ double sZ[kPanel][kUpdateColumns];
+	__shared__ int sP[kPanel];
+	const int tid = threadIdx.x;
+	const int c0 = blockIdx.x*kUpdateColumns;
+	const int cols = min(kUpdateColumns, ld-c0);
+	for (int idx = tid; idx < b*b; idx += blockDim.x) sA[idx/b][idx%b] = Ainv[idx];
+	if (tid < b) sP[tid] = pivots[tid];
+	__syncthreads();
+	// the panel's row swaps, in order, one thread per column of the tile
+	if (tid < cols)
+		for (int jj = 0; jj < b; ++jj) {
+			const int j = k0+jj, p = sP[jj];
+			if (p != j) {
+				const double t = a[(size_t)j*ld+c0+tid];
+				a[(size_t)j*ld+c0+tid] = a[(size_t)p*ld+c0+tid];
+				a[(size_t)p*ld+c0+tid] = t;
+			}
+		}
+	__syncthreads();
+	for (int idx = tid; idx < b*kUpdateColumns; idx += blockDim.x) {
+		const int r = idx/kUpdateColumns, c = idx%kUpdateColumns;
+		sY[r][c] = c < cols ? a[(size_t)(k0+r)*ld+c0+c] : 0.0;
+	}
+	__syncthreads();
+	for (int idx = tid; idx < b*kUpdateColumns; idx += blockDim.x) {
+		const int r = idx/kUpdateColumns, c = idx%kUpdateColumns;
+		double z = 0.0;
+		for (int k = 0; k < b; ++k) z = fma(sA[r][k], sY[k][c], z);
+		sZ[r][c] = z;
+		if (c < cols) a[(size_t)(k0+r)*ld+c0+c] = z;
+	}
+	__syncthreads();
+	// every other row: Y_i -= O_i Z (threads: 16 columns x 16 row lanes)
+	const int c = tid % kUpdateColumns, lane = tid / kUpdateColumns;
+	if (c < cols)
+		for (int i = lane; i < n; i += blockDim.x/kUpdateColumns) {
+			if (i >= k0 && i < k0+b) continue;
+			const double* o = O+(size_t)i*b;
+			double s = 0.0;
+			for (int k = 0; k < b; ++k) s = fma(o[k], sZ[k][c], s);
+			a[(size_t)i*ld+c0+c] -= s;
+		}
 }
 
 // x = A^{-1} b with the inverse in the right half of the augmented matrix; warp per row.
@@ -534,6 +698,8 @@ void Amg::BuildFromStrength(std::vector<double> s)
 			V.dense.Allocate((size_t)V.dense_n*2*V.dense_n);
 			V.column.Allocate((size_t)V.dense_n);
 			V.dense_flag.Allocate(1);
+			V.panel.Allocate((size_t)2*V.dense_n*kPanel+kPanel*kPanel);
+			V.pivots.Allocate(kPanel);
 		}
 	}
 	CudaCheck(cudaStreamSynchronize(stream_), "AMG setup");
@@ -625,6 +791,25 @@ void Amg::Refresh(const T* values, bool coarse)
 	const int dn = Z.dense_n;
 	AugmentIdentityKernel<<<Grid((long long)dn*dn, 256), 256, 0, stream_>>>(dn, Z.dense.get());
 	LaunchCheck("AugmentIdentityKernel");
+	launches_ += 2;
+	for (int k0 = 0; k0 < dn; k0 += kPanel) {
+		const int b = std::min(kPanel, dn-k0);
+		GaussJordanPanelKernel<<<1, kPanelThreads, 0, stream_>>>(dn, k0, b, Z.dense.get(), Z.panel.get(),
+			Z.pivots.get(), Z.dense_flag.get());
+		GaussJordanUpdateKernel<<<Grid(2LL*dn, kUpdateColumns), 256, 0, stream_>>>(dn, k0, b, Z.dense.get(),
+			Z.panel.get(), Z.pivots.get());
+		launches_ += 2;
+	}
+	LaunchCheck("GaussJordanUpdateKernel");
+	// a vanishing panel pivot: redo the inverse one column at a time (that path decouples the unknown)
+	int flag = 0;
+	Z.dense_flag.Download(&flag, 1, stream_);
+	CudaCheck(cudaStreamSynchronize(stream_), "AMG coarse inverse");
+	if (flag == 0) return;
+	Z.dense.Zero(stream_);
+	Z.dense_flag.Zero(stream_);
+	DenseScatterKernel<<<Grid(Z.blocks*16, 256), 256, 0, stream_>>>(Z.view(), Z.values.get(), Z.dense_n, Z.dense.get());
+	AugmentIdentityKernel<<<Grid((long long)dn*dn, 256), 256, 0, stream_>>>(dn, Z.dense.get());
 	for (int k = 0; k < dn; ++k) {
 		GaussJordanPivotKernel<<<1, 1024, 0, stream_>>>(dn, k, Z.dense.get(), Z.column.get(), Z.dense_flag.get());
 		GaussJordanEliminateKernel<<<Grid((long long)dn*2*dn, 256), 256, 0, stream_>>>(dn, k, Z.dense.get(),
