@@ -133,12 +133,25 @@ typedef struct tfiga_ns_params {
 	 * before the tangent, so a converged check assembles no tangent), so only the
 	 * Newton convergence rate can change.  Default 0 (off). */
 	double tangent_reuse_factor;   /* default 0 */
+	/* Tensor-core modes: how the tangent's operands reach the tensor cores.
+	 * TFIGA_TANGENT_COEFFICIENTS: the point kernel stores every element's point
+	 * coefficients (80 KiB per element) and an FP32 copy of the basis tables is kept;
+	 * TFIGA_TANGENT_FUSED: the point kernel stores the FP64 point state (11 KiB per
+	 * element) and the tensor-core kernel makes the coefficients itself and stages
+	 * the basis from the FP64 tables (about 96 KiB per element less);
+	 * TFIGA_TANGENT_AUTO: the first tangent assembly times both (when the memory for
+	 * the first one is free) and keeps the faster; the fused one otherwise.
+	 * Both give the same tangent up to the order of the FP32 additions. */
+	int32_t tangent_kernel;        /* default TFIGA_TANGENT_AUTO */
 } tfiga_ns_params;
 
 #define TFIGA_PRECISION_FP64 0
 #define TFIGA_PRECISION_MIXED 1
 #define TFIGA_PRECISION_FP32_JACOBIAN 2
 #define TFIGA_PRECISION_MIXED_BF16X3 3
+#define TFIGA_TANGENT_AUTO 0
+#define TFIGA_TANGENT_COEFFICIENTS 1
+#define TFIGA_TANGENT_FUSED 2
 
 #define TFIGA_PRECONDITIONER_BLOCK_JACOBI 0
 #define TFIGA_PRECONDITIONER_AMG 1
@@ -295,6 +308,10 @@ int tfiga_ns_step_outlets_coupled(tfiga_ns* ns, tfiga_outlet* outlets, int32_t c
 	int32_t max_newton, tfiga_step_report* report, int32_t* pressure_updates);
 /* AMG hierarchy sizes (levels = 0 before the hierarchy is built). */
 int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info);
+/* Tensor-core modes: the tangent organisation in use (*kernel: TFIGA_TANGENT_*, AUTO before the
+ * first tangent) and the autotuner's times of the coefficient-array and fused organisations (ms,
+ * 0 when not timed).  No counterpart in the reference.  Any output may be NULL. */
+int tfiga_ns_tangent_kernel(tfiga_ns* ns, int32_t* kernel, double* coefficients_ms, double* fused_ms);
 /* Outward flow through each labelled boundary (IntegrateBoundaryFlow,
  * BoundaryFlow.hpp:165-200; MeasureFlowConvergence iga_cuda.cu:520-557). */
 int tfiga_ns_boundary_flows(tfiga_ns* ns, const int32_t* labels, int32_t count, double* flows);

@@ -44,10 +44,10 @@ def random_state(nodes, seed, speed=0.2, pressure=20.0):
     return s.ravel()
 
 
-def check_tensor_tangent(api, flat, rho, mu, dt, seed, precision=None, tol=TANGENT_TOL):
+def check_tensor_tangent(api, flat, rho, mu, dt, seed, precision=None, tol=TANGENT_TOL, kernel=0):
     mesh = api.Mesh(flat)
     ns = api.NavierStokes(mesh, density=rho, viscosity=mu, dt=dt, preconditioner=api.AMG,
-                          precision=api.MIXED if precision is None else precision)
+                          precision=api.MIXED if precision is None else precision, tangent_kernel=kernel)
     st = random_state(flat.nodes, seed)
     pv = random_state(flat.nodes, seed + 1)
     ns.set_state(st, pv)
@@ -77,17 +77,45 @@ def test_tensor_tangent_reference_tube_ragged(api, reference_tube):
     check_tensor_tangent(api, flat, 1.0, 1.0, 0.1, 5)
 
 
-def test_split_tangent_small_tube(api, small_tube):
-    errors = check_tensor_tangent(api, small_tube.mesh, RHO, MU, DT, 0, api.MIXED_BF16X3, SPLIT_TOL)
-    plain = check_tensor_tangent(api, small_tube.mesh, RHO, MU, DT, 0)
+# both tangent organisations: point coefficients stored by the point kernel (1), coefficients made in the
+# tensor-core kernel from the stored point state with the basis staged from the FP64 tables (2)
+KERNELS = [1, 2]
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_split_tangent_small_tube(api, small_tube, kernel):
+    errors = check_tensor_tangent(api, small_tube.mesh, RHO, MU, DT, 0, api.MIXED_BF16X3, SPLIT_TOL, kernel)
+    plain = check_tensor_tangent(api, small_tube.mesh, RHO, MU, DT, 0, kernel=kernel)
     assert errors.max() < 0.05 * plain.max()
 
 
-def test_split_tangent_steady_and_ragged(api, small_tube, reference_tube):
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_split_tangent_steady_and_ragged(api, small_tube, reference_tube, kernel):
     from tubularflowiga_b200 import ntiga
-    check_tensor_tangent(api, small_tube.mesh, RHO, MU, 0.0, 3, api.MIXED_BF16X3, SPLIT_TOL)
+    check_tensor_tangent(api, small_tube.mesh, RHO, MU, 0.0, 3, api.MIXED_BF16X3, SPLIT_TOL, kernel)
     flat = ntiga.read(reference_tube / "tube-1.ntiga")
-    check_tensor_tangent(api, flat, 1.0, 1.0, 0.1, 5, api.MIXED_BF16X3, SPLIT_TOL)
+    check_tensor_tangent(api, flat, 1.0, 1.0, 0.1, 5, api.MIXED_BF16X3, SPLIT_TOL, kernel)
+
+
+def test_tangent_autotuner_picks_one_and_matches(api, small_tube):
+    """TFIGA_TANGENT_AUTO: the first tangent times both organisations (memory is plentiful here), keeps
+    one, and every tangent it assembles agrees with the fixed organisations' to FP32 addition order."""
+    flat = small_tube.mesh
+    st, pv = random_state(flat.nodes, 21), random_state(flat.nodes, 22)
+    got = {}
+    for kernel in (0, 1, 2):
+        ns = api.NavierStokes(api.Mesh(flat), density=RHO, viscosity=MU, dt=DT, preconditioner=api.AMG,
+                              precision=api.MIXED_BF16X3, tangent_kernel=kernel)
+        ns.set_state(st, pv)
+        got[kernel] = ns.assemble()[0]
+        info = ns.tangent_kernel()
+        if kernel == 0:
+            assert info["kernel"] in ("coefficients", "fused")
+            assert info["coefficients_ms"] > 0 and info["fused_ms"] > 0
+            again = ns.assemble()[0]
+            assert rel(again, got[0]) < 1e-6
+        ns.close()
+    assert rel(got[1], got[2]) < 1e-6 and rel(got[0], got[2]) < 1e-6
 
 
 def test_split_newton_matches_fp64_iterations(api, cylinder_1280):

@@ -239,6 +239,7 @@ void tfiga_ns_default_params(tfiga_ns_params* p)
 	p->krylov_fp64_basis = 0;
 	p->newton_forcing = 0;
 	p->tangent_reuse_factor = 0.0;
+	p->tangent_kernel = TFIGA_TANGENT_AUTO;
 }
 
 int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out)
@@ -394,6 +395,16 @@ int tfiga_ns_step_outlets_coupled(tfiga_ns* ns, tfiga_outlet* outlets, int32_t c
 		int updates = 0;
 		*report = ns->solver->StepOutletsCoupled(outlets, count, relaxation, max_newton, &updates);
 		if (pressure_updates) *pressure_updates = updates;
+	});
+}
+
+int tfiga_ns_tangent_kernel(tfiga_ns* ns, int32_t* kernel, double* coefficients_ms, double* fused_ms)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		if (kernel) *kernel = ns->solver->tangent_kernel();
+		if (coefficients_ms) *coefficients_ms = ns->solver->tune_ms(TFIGA_TANGENT_COEFFICIENTS);
+		if (fused_ms) *fused_ms = ns->solver->tune_ms(TFIGA_TANGENT_FUSED);
 	});
 }
 

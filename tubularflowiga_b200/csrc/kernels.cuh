@@ -85,10 +85,18 @@ void LaunchAssembleLarge(const DeviceMeshView& mesh, int first, int count, const
 // coef and phi32 (the FP32 copy of phi, Mesh::phi32), BF16 or split-BF16
 // operands, FP32 accumulation, ADDED into the FP32 values; status bit 1 set if
 // an MMA completion wait expired.
+// point_state (elements x 64 x 22 doubles, may be null): the point state for LaunchTangentTcFused
+// instead of the coefficients (coef and point_state are not both given).
 void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const double* qdata, const double* state,
-	const double* previous, AssemblyParams params, float* coef, double* rhs, cudaStream_t stream);
+	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs,
+	cudaStream_t stream);
 void LaunchTangentTc(const DeviceMeshView& mesh, const float* phi32, const float* coef,
 	const int32_t* element_blocks, float* values, int* status, bool split, cudaStream_t stream);
+// The same contraction with the coefficients made in the kernel from the stored point state and the
+// basis staged from the FP64 tables (no coefficient array, no FP32 copy of the tables).
+void LaunchTangentTcFused(const DeviceMeshView& mesh, const double* phi, const double* qdata,
+	const double* point_state, AssemblyParams params, const int32_t* element_blocks, float* values, int* status,
+	bool split, cudaStream_t stream);
 
 // ---- sparse.cu ----------------------------------------------------------
 // Matrix values are FP64 or FP32 (T = double / float); vectors are FP64.

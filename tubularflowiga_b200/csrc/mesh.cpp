@@ -272,6 +272,13 @@ const float* Mesh::phi32()
 	return phi32_.get();
 }
 
+void Mesh::ReleasePhi32()
+{
+	if (phi32_.get() == nullptr) return;
+	device_bytes_ -= (int64_t)phi32_.bytes();
+	phi32_.Release();
+}
+
 Mesh::~Mesh()
 {
 	if (stream_) cudaStreamDestroy(stream_);

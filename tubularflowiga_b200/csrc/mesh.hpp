@@ -76,6 +76,7 @@ public:
 	const double* phi() const { return phi_.get(); }
 	// FP32 copy of the basis tables (operand staging of the tensor-core tangent), made on first use.
 	const float* phi32();
+	void ReleasePhi32();
 	const double* qdata() const { return qdata_.get(); }
 	const int32_t* element_blocks() const { return element_blocks_.get(); }
 	const std::vector<BoundaryFace>& faces() const { return faces_; }

@@ -80,7 +80,15 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 	if (mixed() && params.preconditioner != TFIGA_PRECONDITIONER_AMG)
 		Fail(-7, "mixed precision requires the AMG-preconditioned flexible GMRES");
 	if (mixed()) values32_.Allocate((size_t)blocks()*16);
-	if (tensor_tangent()) coef32_.Allocate((size_t)mesh.host().elements()*4*80*64);
+	if (params.tangent_kernel != TFIGA_TANGENT_AUTO && params.tangent_kernel != TFIGA_TANGENT_COEFFICIENTS
+		&& params.tangent_kernel != TFIGA_TANGENT_FUSED)
+		Fail(-1, "unknown tangent_kernel "+std::to_string(params.tangent_kernel));
+	tangent_kernel_ = params.tangent_kernel;
+	if (tensor_tangent()) {
+		const size_t regular = (size_t)mesh.regular_elements();
+		if (tangent_kernel_ == TFIGA_TANGENT_COEFFICIENTS) coef32_.Allocate(regular*4*80*64);
+		else point_state_.Allocate(regular*kQuad*22);
+	}
 	if (tensor_tangent()) {
 		status_.Allocate(1);
 		status_.Zero(stream_);
@@ -198,8 +206,10 @@ void NsSolver::AssembleResidualTc()
 {
 	rhs_.Zero(stream_);
 	profiler_.Begin(Profiler::kResidual, stream_);
+	const bool coefficients = tangent_kernel_ == TFIGA_TANGENT_COEFFICIENTS;
 	LaunchTangentPoint(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
-		{params_.density, params_.viscosity, params_.dt}, coef32_.get(), rhs_.get(), stream_);
+		{params_.density, params_.viscosity, params_.dt}, coefficients ? coef32_.get() : nullptr,
+		coefficients ? nullptr : point_state_.get(), rhs_.get(), stream_);
 	LargeElements<float>(nullptr, rhs_.get());
 	profiler_.End(stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
@@ -219,14 +229,80 @@ void NsSolver::LargeElements(T* values, double* rhs)
 void NsSolver::AssembleTangentTc()
 {
 	amg_current_ = false;
-	values32_.Zero(stream_);
+	const bool split = params_.precision == TFIGA_PRECISION_MIXED_BF16X3;
+	const AssemblyParams prm{params_.density, params_.viscosity, params_.dt};
 	profiler_.Begin(Profiler::kAssembly, stream_);
-	LaunchTangentTc(mesh_.regular_view(), mesh_.phi32(), coef32_.get(), mesh_.element_blocks(), values32_.get(),
-		status_.get(), params_.precision == TFIGA_PRECISION_MIXED_BF16X3, stream_);
+	if (tangent_kernel_ == TFIGA_TANGENT_AUTO) {
+		AutotuneTangent();
+	} else {
+		values32_.Zero(stream_);
+		if (tangent_kernel_ == TFIGA_TANGENT_FUSED)
+			LaunchTangentTcFused(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), point_state_.get(), prm,
+				mesh_.element_blocks(), values32_.get(), status_.get(), split, stream_);
+		else
+			LaunchTangentTc(mesh_.regular_view(), mesh_.phi32(), coef32_.get(), mesh_.element_blocks(),
+				values32_.get(), status_.get(), split, stream_);
+		launches_ += 1;
+	}
 	LargeElements<float>(values32_.get(), nullptr);
 	profiler_.End(stream_);
-	launches_ += 1;
 	if (amg_ && !amg_->built()) amg_->Build(values32_.get());
+}
+
+void NsSolver::AutotuneTangent()
+{
+	const bool split = params_.precision == TFIGA_PRECISION_MIXED_BF16X3;
+	const AssemblyParams prm{params_.density, params_.viscosity, params_.dt};
+	const DeviceMeshView view = mesh_.regular_view();
+	cudaEvent_t ev[4];
+	for (auto& e : ev) CudaCheck(cudaEventCreate(&e), "autotune event");
+	struct Events {
+		cudaEvent_t* e;
+		~Events() { for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]); }
+	} guard{ev};
+	// the fused organisation first: the residual pass has just stored its point state
+	values32_.Zero(stream_);
+	CudaCheck(cudaEventRecord(ev[0], stream_), "event");
+	LaunchTangentTcFused(view, mesh_.phi(), mesh_.qdata(), point_state_.get(), prm, mesh_.element_blocks(),
+		values32_.get(), status_.get(), split, stream_);
+	CudaCheck(cudaEventRecord(ev[1], stream_), "event");
+	launches_ += 1;
+	CudaCheck(cudaStreamSynchronize(stream_), "tangent autotune");
+	float ms = 0.0f;
+	CudaCheck(cudaEventElapsedTime(&ms, ev[0], ev[1]), "event time");
+	tune_ms_[1] = ms;
+	// the coefficient-array organisation, when its arrays fit with 2 GiB to spare
+	const size_t regular = (size_t)mesh_.regular_elements();
+	const size_t need = regular*4*80*64*sizeof(float)+regular*kFeatures*kQuad*kMaxBasis*sizeof(float);
+	size_t free_bytes = 0, total_bytes = 0;
+	CudaCheck(cudaMemGetInfo(&free_bytes, &total_bytes), "device memory");
+	if (free_bytes < need+(size_t(2) << 30)) {
+		tangent_kernel_ = TFIGA_TANGENT_FUSED;
+		return;
+	}
+	coef32_.Allocate(regular*4*80*64);
+	// the same state's coefficients; the residual this pass adds goes to the Newton update vector,
+	// which the linear solve clears before use
+	LaunchTangentPoint(view, mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(), prm, coef32_.get(), nullptr,
+		update_.get(), stream_);
+	const float* phi32 = mesh_.phi32();
+	values32_.Zero(stream_);
+	CudaCheck(cudaEventRecord(ev[2], stream_), "event");
+	LaunchTangentTc(view, phi32, coef32_.get(), mesh_.element_blocks(), values32_.get(), status_.get(), split,
+		stream_);
+	CudaCheck(cudaEventRecord(ev[3], stream_), "event");
+	launches_ += 2;
+	CudaCheck(cudaStreamSynchronize(stream_), "tangent autotune");
+	CudaCheck(cudaEventElapsedTime(&ms, ev[2], ev[3]), "event time");
+	tune_ms_[0] = ms;
+	if (tune_ms_[0] < tune_ms_[1]) {
+		tangent_kernel_ = TFIGA_TANGENT_COEFFICIENTS;
+		point_state_.Release();
+	} else {
+		tangent_kernel_ = TFIGA_TANGENT_FUSED;
+		coef32_.Release();
+		mesh_.ReleasePhi32();
+	}
 }
 
 void NsSolver::AssembleResidual()
@@ -238,7 +314,7 @@ void NsSolver::AssembleResidual()
 	rhs_.Zero(stream_);
 	profiler_.Begin(Profiler::kResidual, stream_);
 	LaunchTangentPoint(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
-		{params_.density, params_.viscosity, params_.dt}, nullptr, rhs_.get(), stream_);
+		{params_.density, params_.viscosity, params_.dt}, nullptr, nullptr, rhs_.get(), stream_);
 	LargeElements<double>(nullptr, rhs_.get());
 	profiler_.End(stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);

@@ -78,6 +78,10 @@ public:
 	void SetLearned(LearnedPreconditioner* learned, bool use, bool collect);
 	long long learned_fallbacks() const { return learned_fallbacks_; }
 	long long tangent_contractions() const { return tangent_contractions_; }
+	// Tensor-core modes: the tangent organisation in use (TFIGA_TANGENT_*; TFIGA_TANGENT_AUTO until the
+	// first tangent has been assembled) and the autotuner's timings of both (ms, 0 if not run).
+	int tangent_kernel() const { return tangent_kernel_; }
+	double tune_ms(int kernel) const { return kernel == TFIGA_TANGENT_FUSED ? tune_ms_[1] : tune_ms_[0]; }
 	// Binds the current (Dirichlet-row) Jacobian as the operator of the learned stage's residual loss.
 	void BindLearnedOperator(LearnedPreconditioner& learned);
 
@@ -91,6 +95,10 @@ private:
 	void AssembleResidualTc();
 	void ApplyDirichletParts(bool matrix, bool rhs);
 	void AssembleTangentTc();
+	// TFIGA_TANGENT_AUTO: times both tangent organisations on the current state (the separate one only
+	// when its arrays fit in free memory), keeps the faster and releases the other's arrays; values32_
+	// then holds the tangent.
+	void AutotuneTangent();
 	// Every mode, for the residual-first Newton iteration: the FP64 residual alone (rhs = -r +
 	// traction; in the tensor-core modes with the point coefficients), then -- only for an
 	// iteration that solves with a new tangent -- the Jacobian alone (FP64 assembly, or the
@@ -124,6 +132,9 @@ private:
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
 	DeviceArray<float> values32_;
 	DeviceArray<float> coef32_;              // tensor-core tangent: point coefficients [e][4][80][64]
+	DeviceArray<double> point_state_;        // fused tensor-core tangent: FP64 point state [e][64][22]
+	int tangent_kernel_ = 0;                 // TFIGA_TANGENT_* in use
+	double tune_ms_[2] = {0.0, 0.0};         // autotuner: coefficient-array and fused tangent times
 	DeviceArray<double> face_flow_, face_pressure_, label_flow_, partial_, scalars_;
 	DeviceArray<int32_t> vmask_, pmask_, constrained_, face_slot_, status_;
 	std::vector<int32_t> labels_;            // distinct face labels (slot order)

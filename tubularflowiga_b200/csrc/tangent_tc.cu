@@ -93,6 +93,7 @@ constexpr int kPtOffRC = kPtOffQS+kQuad*kQS*8;                    // double [4][
 constexpr int kPtSmemBytes = kPtOffRC+4*kQuad*kRcStride*8;
 static_assert(kTcThreads*kScratchStride*4 <= kPtPartBytes, "coefficient scratch fits in the partial sums");
 constexpr int kStageBasis = 16;                  // basis functions per staged chunk of the point-state stage
+constexpr int kPointStride = 22;                 // doubles per point of the stored point state (kU .. kLap+2)
 constexpr int kStageStride = kStageBasis+1;      // odd double stride of a staged (feature, point) row
 static_assert(kFeatures*kQuad*kStageStride*8 <= kPtPartBytes, "staged basis chunk fits in the partial sums");
 
@@ -300,12 +301,17 @@ __device__ __forceinline__ void PointCoefficients(const PointState& S, const dou
 	for (int k = 0; k < 40; ++k) out[(size_t)(40+k)*kQuad] = scratch[k];
 }
 
-// kWriteCoef: also write the tangent coefficients of the four row fields (false: the FP64
-// residual only, for the residual-first Newton check of the FP64 solver).
-template <bool kWriteCoef>
+// kMode: what the kernel stores besides adding the FP64 residual into rhs -- kPointResidual nothing
+// (the residual-first Newton check of the FP64 solver), kPointCoefficients the tangent coefficients of
+// the four row fields (TangentTcKernel), kPointState the FP64 state at the 64 points
+// (TangentTcFusedKernel).
+enum : int { kPointResidual = 0, kPointCoefficients = 1, kPointState = 2 };
+
+template <int kMode>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ state,
-	const double* __restrict__ previous, AssemblyParams prm, float* __restrict__ coef, double* __restrict__ rhs)
+	const double* __restrict__ previous, AssemblyParams prm, float* __restrict__ coef,
+	double* __restrict__ point_state, double* __restrict__ rhs)
 {
 	extern __shared__ uint8_t smem_raw[];
 	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+15) & ~uintptr_t(15));
@@ -379,7 +385,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 	for (int idx = tid; idx < kQuad*22; idx += kTcThreads) {
 		const int q = idx/22, k = idx%22;
 		const double* part = Part+q*kPartStride+k;
-		QS[q*kQS+k] = ((part[0]+part[kQuad*kPartStride])+part[2*kQuad*kPartStride])+part[3*kQuad*kPartStride];
+		const double v = ((part[0]+part[kQuad*kPartStride])+part[2*kQuad*kPartStride])+part[3*kQuad*kPartStride];
+		QS[q*kQS+k] = v;
+		if constexpr (kMode == kPointState) point_state[(size_t)e*kQuad*kPointStride+idx] = v;
 	}
 	__syncthreads();
 
@@ -400,7 +408,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 		S.p = s[kP];
 		const double* qd = qdata+((size_t)e*kQuad+q)*kQData;
 		double* rc = RC+(il*kQuad+q)*kRcStride;
-		if constexpr (kWriteCoef) {
+		if constexpr (kMode == kPointCoefficients) {
 			float* scratch = Scratch+tid*kScratchStride;
 			float* out = coef+((size_t)e*4+il)*kCoef*kQuad+q;
 			switch (il) {
@@ -638,27 +646,285 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 	}
 }
 
+// ---- fused variant: coefficients made in the tensor-core kernel ------------------------------------
+// TangentTcFusedKernel: the same contraction as TangentTcKernel, but its operands come from tables
+// that cost far less memory.  The point kernel stores the FP64 state at the 64 points (11 KiB per
+// element instead of 80 KiB of coefficients); this kernel computes its two row fields' coefficients
+// M_q from it in its prologue (FP64 arithmetic, FP32 storage, bitwise the coefficients the point
+// kernel would have written) into shared memory, and stages the basis chunks from the FP64 tables:
+// the next-but-one chunk is loaded into registers while the current chunk is built and converted to
+// FP32 in shared memory after it, so no FP32 copy of the tables is kept.  One CTA per (element,
+// row-field pair) and SM: 512 threads (16 warps), 256 TMEM columns, 133 KiB of shared memory.
+constexpr int kFusedThreads = 512;
+constexpr int kFOffOp0 = 0;
+constexpr int kFOffOp1 = kOperandBytes;
+constexpr int kFOffPhi0 = 2*kOperandBytes;
+constexpr int kFOffPhi1 = kFOffPhi0+kPhiBytes;
+constexpr int kFCoefBytes = 2*kCoef*kQuad*4;                      // float [2 rows][80][64 points]
+constexpr int kFOffCoef = kFOffPhi1+kPhiBytes;
+constexpr int kFOffBar = kFOffCoef+kFCoefBytes;
+constexpr int kFusedSmemBytes = kFOffBar+32+1024;
+static_assert(kFusedSmemBytes <= 227*1024, "fused tangent shared memory");
+static_assert(kQuad*kPointStride*8 <= kOperandBytes, "point-state staging fits in operand buffer 0");
+
+// One basis chunk (points NP c .. NP c + NP - 1, five features, 64 functions) of one element:
+// FP64 loads into registers, then FP32 stores into a [5][NP][64] buffer.
+template <int NP>
+struct PhiChunk {
+	static constexpr int kPairs = kFeatures*NP*32;                     // double2 per chunk
+	static constexpr int kSlots = (kPairs+kFusedThreads-1)/kFusedThreads;
+	double2 v[kSlots];
+	__device__ __forceinline__ void Load(const double* P, int c, int tid)
+	{
+		#pragma unroll
+		for (int s = 0; s < kSlots; ++s) {
+			const int idx = tid+s*kFusedThreads;
+			if (idx < kPairs) {
+				const int t = idx/(NP*32), rem = idx%(NP*32), q = rem/32, b2 = rem%32;
+				v[s] = __ldg(reinterpret_cast<const double2*>(P+(size_t)(t*kQuad+c*NP+q)*kMaxBasis)+b2);
+			}
+		}
+	}
+	__device__ __forceinline__ void Store(float* dst, int tid) const
+	{
+		#pragma unroll
+		for (int s = 0; s < kSlots; ++s) {
+			const int idx = tid+s*kFusedThreads;
+			if (idx < kPairs) {
+				const int t = idx/(NP*32), rem = idx%(NP*32), q = rem/32, b2 = rem%32;
+				reinterpret_cast<float2*>(dst+(t*NP+q)*64)[b2] = make_float2((float)v[s].x, (float)v[s].y);
+			}
+		}
+	}
+};
+
+template <bool kSplit>
+__global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceMeshView mesh,
+	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ point_state,
+	AssemblyParams prm, const int32_t* __restrict__ element_blocks, float* __restrict__ values,
+	int* __restrict__ status)
+{
+	constexpr int NP = kSplit ? 4 : kMaxPts;     // points per K chunk
+	constexpr int kChunks = kQuad/NP;
+	extern __shared__ uint8_t smem_raw[];
+	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+1023) & ~uintptr_t(1023));
+	const uint32_t sOp[2] = {SmemAddress(sm+kFOffOp0), SmemAddress(sm+kFOffOp1)};
+	float* PhiF[2] = {reinterpret_cast<float*>(sm+kFOffPhi0), reinterpret_cast<float*>(sm+kFOffPhi1)};
+	float* CoefS = reinterpret_cast<float*>(sm+kFOffCoef);
+	uint64_t* bars = reinterpret_cast<uint64_t*>(sm+kFOffBar);
+	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm+kFOffBar+16);
+
+	const int e = blockIdx.x >> 1;
+	const int h = blockIdx.x & 1;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const int begin = mesh.element_offsets[e];
+	const int nen = mesh.element_offsets[e+1]-begin;
+	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
+
+	PhiChunk<NP> stage;
+	stage.Load(P, 0, tid);
+	if (warp == 0) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+			:: "r"(SmemAddress(tmem_slot)), "r"(kTmemCols) : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	if (tid == 32) { MbarInit(bars); MbarInit(bars+1); }
+	// the element's point state, staged in operand buffer 0 (free until the first chunk is built)
+	double* QSs = reinterpret_cast<double*>(sm+kFOffOp0);
+	const double* PS = point_state+(size_t)e*kQuad*kPointStride;
+	for (int idx = tid; idx < kQuad*kPointStride; idx += kFusedThreads) QSs[idx] = PS[idx];
+	stage.Store(PhiF[0], tid);
+	stage.Load(P, 1, tid);
+	FenceBeforeSync();
+	__syncthreads();
+	FenceAfterSync();
+	const uint32_t tmem = *tmem_slot;
+	// coefficients of row fields 2h, 2h + 1 at every point: thread (row rl, point q, column field f)
+	{
+		const int rl = tid >> 8, q = (tid >> 2) & 63, f = tid & 3;
+		const double* s = QSs+q*kPointStride;
+		PointState S;
+		#pragma unroll
+		for (int c = 0; c < 3; ++c) {
+			S.u[c] = s[kU+c]; S.up[c] = s[kUp+c]; S.lap[c] = s[kLap+c]; S.gp[c] = s[kGrad+9+c];
+			#pragma unroll
+			for (int d = 0; d < 3; ++d) S.gv[c][d] = s[kGrad+3*c+d];
+		}
+		S.p = s[kP];
+		RowCoefficients<float, kQuad>(2*h+rl, S, qdata+((size_t)e*kQuad+q)*kQData, prm,
+			CoefS+(rl*kCoef+f*20)*kQuad+q, nullptr, f, f+1);
+	}
+	stage.Store(PhiF[1], tid);
+	__syncthreads();                             // coefficients and chunks 0, 1 in place; QSs free
+
+	// Chunks: as TangentTcKernel, with 16 warps: warp & 7 picks the row field and point pair (and in
+	// split mode the basis half) as there, warp >> 3 half of that warp's basis groups.
+	const int gil = (warp >> 2) & 1, gqp = warp & 3, ghalf = warp >> 3;
+	const int gf = lane & 3, gbs = lane >> 2;
+	bool failed = false;
+	int issued = 0;
+	for (int c = 0; c < kChunks; ++c) {
+		const int buf = c & 1;
+		const float* PhiS = PhiF[buf];
+		if (c+2 < kChunks) stage.Load(P, c+2, tid);
+		bool ok = true;
+		if (c >= 2) ok = MbarWaitBounded(bars+buf, (uint32_t)(((c-2) >> 1) & 1));
+		if (__syncthreads_or(!ok)) { failed = true; break; }
+		const uint32_t sA = sOp[buf], sB = sOp[buf]+kTiles*kTileBytes;
+		if (tid < kTcThreads) {
+			const int a = tid >> 2, u = tid & 3;
+			const int qp = kSplit ? (u & 1) : u;
+			float x[8];
+			#pragma unroll
+			for (int k = 0; k < 8; ++k) x[k] = PhiS[((k >> 1)*NP+2*qp+(k & 1))*64+a];
+			if (kSplit && u >= 2) {
+				#pragma unroll
+				for (int k = 0; k < 8; ++k) x[k] = Bf16Residual(x[k]);
+			}
+			StoreShared16(sB+Sw64(a, u), PackBf16(x[0], x[1]), PackBf16(x[2], x[3]), PackBf16(x[4], x[5]),
+				PackBf16(x[6], x[7]));
+		}
+		{
+			const int qpair = kSplit ? (gqp & 1) : gqp;
+			const int ql0 = 2*qpair;
+			constexpr int kGroups = kSplit ? 2 : 4;
+			const int g0 = kSplit ? (gqp >> 1)*4+ghalf*2 : ghalf*4;
+			unsigned long long mm[20];
+			const float* c0 = CoefS+(gil*kCoef+gf*20)*kQuad+c*NP+ql0;
+			#pragma unroll
+			for (int k = 0; k < 20; ++k) mm[k] = *reinterpret_cast<const unsigned long long*>(c0+k*kQuad);
+			#pragma unroll
+			for (int j = 0; j < kGroups; ++j) {
+				const int b = (g0+j)*8+gbs;
+				unsigned long long pb[5];
+				#pragma unroll
+				for (int t = 0; t < 5; ++t) pb[t] = Pack2(PhiS[(t*NP+ql0)*64+b], PhiS[(t*NP+ql0+1)*64+b]);
+				unsigned long long gg[4];
+				#pragma unroll
+				for (int s = 0; s < 4; ++s) {
+					gg[s] = Mul2(mm[s*5], pb[0]);
+					#pragma unroll
+					for (int t = 1; t < 5; ++t) gg[s] = Fma2(mm[s*5+t], pb[t], gg[s]);
+				}
+				const int tile = gil*2+(b >> 5), row = (b & 31)*4+gf;
+				const uint32_t dst = sA+tile*kTileBytes;
+				uint32_t hi[4];
+				#pragma unroll
+				for (int s = 0; s < 4; ++s) hi[s] = Bf16Pair(gg[s]);
+				StoreShared16(dst+Sw64(row, qpair), hi[0], hi[1], hi[2], hi[3]);
+				if (kSplit) {
+					uint32_t lo[4];
+					#pragma unroll
+					for (int s = 0; s < 4; ++s) lo[s] = Bf16Pair(Sub2(gg[s], WidenBf16Pair(hi[s])));
+					StoreShared16(dst+Sw64(row, 2+qpair), lo[0], lo[1], lo[2], lo[3]);
+				}
+			}
+		}
+		FenceProxyAsync();
+		__syncthreads();
+		if (tid == 0) {
+			FenceAfterSync();
+			#pragma unroll
+			for (int tile = 0; tile < kTiles; ++tile) {
+				const uint32_t a = sA+tile*kTileBytes;
+				if (kSplit) {
+					MmaBf16(tmem+tile*64, DescSw64(a), DescSw64(sB), c > 0 ? 1u : 0u);
+					MmaBf16(tmem+tile*64, DescSw64(a), DescSw64(sB+32), 1u);
+					MmaBf16(tmem+tile*64, DescSw64(a+32), DescSw64(sB), 1u);
+				} else {
+					#pragma unroll
+					for (int ks = 0; ks < 2; ++ks)
+						MmaBf16(tmem+tile*64, DescSw64(a+ks*32), DescSw64(sB+ks*32), (c > 0 || ks > 0) ? 1u : 0u);
+				}
+			}
+			MmaCommit(bars+buf);
+		}
+		issued = c+1;
+		// every thread has passed this chunk's barrier, so the chunk's basis buffer is free for chunk c + 2
+		if (c+2 < kChunks) stage.Store(PhiF[buf], tid);
+	}
+	if (!failed)
+		failed = __syncthreads_or(!MbarWaitBounded(bars+((kChunks-1) & 1), (uint32_t)(((kChunks-1) >> 1) & 1))) != 0;
+
+	if (!failed) {
+		// Epilogue as TangentTcKernel's, each warp taking one of the two a halves: warp -> (a half
+		// warp >> 3, basis half (warp >> 2) & 1, TMEM lane quarter warp & 3).
+		FenceAfterSync();
+		const int bh = (warp >> 2) & 1, quarter = warp & 3, ah = warp >> 3;
+		const int32_t* EB = element_blocks+(size_t)e*kMaxBasis*kMaxBasis;
+		const int f = lane & 3;
+		const int b = bh*32+quarter*8+(lane >> 2);
+		float* row_base = values+(size_t)(2*h+(f & 1))*4;
+		int blocks[2][8];
+		#pragma unroll
+		for (int g = 0; g < 8; ++g)
+			#pragma unroll
+			for (int p = 0; p < 2; ++p) {
+				const int a = ah*32+4*g+(f & 2)+p;
+				blocks[p][g] = (a < nen && b < nen) ? EB[a*kMaxBasis+b] : -1;
+			}
+		float v0[32], v1[32];
+		const uint32_t lanes = (uint32_t)(quarter*32) << 16;
+		TmemLoad32(tmem+lanes+bh*64+ah*32, v0);
+		TmemLoad32(tmem+lanes+(2+bh)*64+ah*32, v1);
+		#pragma unroll
+		for (int g = 0; g < 8; ++g)
+			#pragma unroll
+			for (int p = 0; p < 2; ++p) {
+				const float c00 = v0[4*g+p], c02 = v0[4*g+2+p], c10 = v1[4*g+p], c12 = v1[4*g+2+p];
+				float o0 = 0.f, o1 = 0.f, o2 = 0.f, o3 = 0.f;
+				#pragma unroll
+				for (int r = 0; r < 4; ++r) {
+					const int d = f ^ r;
+					const float send = (d & 1) ? ((d & 2) ? c12 : c10) : ((d & 2) ? c02 : c00);
+					const float got = r ? __shfl_xor_sync(0xffffffffu, send, r) : send;
+					o0 = d == 0 ? got : o0; o1 = d == 1 ? got : o1;
+					o2 = d == 2 ? got : o2; o3 = d == 3 ? got : o3;
+				}
+				if (blocks[p][g] >= 0) RedAdd4(row_base+(size_t)blocks[p][g]*16, o0, o1, o2, o3);
+			}
+	} else {
+		if (tid == 0) atomicOr(status, 1);
+		if (issued > 0) MbarWaitBounded(bars+((issued-1) & 1), (uint32_t)(((issued-1) >> 1) & 1));
+	}
+	FenceBeforeSync();
+	__syncthreads();
+	if (warp == 0) {
+		FenceAfterSync();
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTmemCols)
+			: "memory");
+	}
+}
+
 } // namespace
 
 void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const double* qdata, const double* state,
-	const double* previous, AssemblyParams params, float* coef, double* rhs, cudaStream_t stream)
+	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs, cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
 	if (rhs == nullptr) Fail(-1, "tangent point kernel: the residual output is required");
+	if (coef && point_state) Fail(-1, "tangent point kernel: coefficients or point state, not both");
 	static bool configured = false;
 	if (!configured) {
-		CudaCheck(cudaFuncSetAttribute(TangentPointKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		CudaCheck(cudaFuncSetAttribute(TangentPointKernel<kPointResidual>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
-		CudaCheck(cudaFuncSetAttribute(TangentPointKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		CudaCheck(cudaFuncSetAttribute(TangentPointKernel<kPointCoefficients>,
+			cudaFuncAttributeMaxDynamicSharedMemorySize, kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
+		CudaCheck(cudaFuncSetAttribute(TangentPointKernel<kPointState>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
 		configured = true;
 	}
+	const unsigned grid = (unsigned)mesh.elements;
+	const size_t bytes = kPtSmemBytes+16;
 	if (coef)
-		TangentPointKernel<true><<<(unsigned)mesh.elements, kTcThreads, kPtSmemBytes+16, stream>>>(mesh, phi, qdata,
-			state, previous, params, coef, rhs);
+		TangentPointKernel<kPointCoefficients><<<grid, kTcThreads, bytes, stream>>>(mesh, phi, qdata, state, previous,
+			params, coef, nullptr, rhs);
+	else if (point_state)
+		TangentPointKernel<kPointState><<<grid, kTcThreads, bytes, stream>>>(mesh, phi, qdata, state, previous,
+			params, nullptr, point_state, rhs);
 	else
-		TangentPointKernel<false><<<(unsigned)mesh.elements, kTcThreads, kPtSmemBytes+16, stream>>>(mesh, phi, qdata,
-			state, previous, params, nullptr, rhs);
+		TangentPointKernel<kPointResidual><<<grid, kTcThreads, bytes, stream>>>(mesh, phi, qdata, state, previous,
+			params, nullptr, nullptr, rhs);
 	LaunchCheck("TangentPointKernel");
 }
 
@@ -683,6 +949,30 @@ void LaunchTangentTc(const DeviceMeshView& mesh, const float* phi32, const float
 		TangentTcKernel<false><<<(unsigned)ctas, kTcThreads, kTcSmemBytes, stream>>>(mesh, phi32, coef,
 			element_blocks, values, status);
 	LaunchCheck("TangentTcKernel");
+}
+
+void LaunchTangentTcFused(const DeviceMeshView& mesh, const double* phi, const double* qdata,
+	const double* point_state, AssemblyParams params, const int32_t* element_blocks, float* values, int* status,
+	bool split, cudaStream_t stream)
+{
+	if (mesh.elements == 0) return;
+	static bool configured = false;
+	if (!configured) {
+		CudaCheck(cudaFuncSetAttribute(TangentTcFusedKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			kFusedSmemBytes), "fused tensor-core tangent shared-memory attribute");
+		CudaCheck(cudaFuncSetAttribute(TangentTcFusedKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			kFusedSmemBytes), "fused tensor-core tangent shared-memory attribute");
+		configured = true;
+	}
+	const long long ctas = 2LL*mesh.elements;
+	if (ctas > 0x7fffffffLL) Fail(-7, "too many elements for one tangent launch");
+	if (split)
+		TangentTcFusedKernel<true><<<(unsigned)ctas, kFusedThreads, kFusedSmemBytes, stream>>>(mesh, phi, qdata,
+			point_state, params, element_blocks, values, status);
+	else
+		TangentTcFusedKernel<false><<<(unsigned)ctas, kFusedThreads, kFusedSmemBytes, stream>>>(mesh, phi, qdata,
+			point_state, params, element_blocks, values, status);
+	LaunchCheck("TangentTcFusedKernel");
 }
 
 } // namespace tfiga

@@ -244,6 +244,55 @@ def straight_tube(radius: float, length: float, core: int, ring: int, layers: in
 
 
 
+def helical_tube(radius: float, length: float, curvature_radius: float, core: int, ring: int, layers: int,
+                 handed: float = 1.0, core_half: float = 0.5, bulge: float = 0.2) -> Tube:
+    """Tube of the straight tube's O-grid swept along a helix whose curvature radius is
+    ``curvature_radius``: helix radius a and pitch parameter c equal (a 45 degree helix), so the
+    curvature a / (a^2 + c^2) is 1 / curvature_radius for a = c = curvature_radius / 2.  Each vertex
+    plane sits at arc length s_k = k length / layers and spans the Frenet normal and binormal there;
+    the centreline starts at the origin with tangent (0, c, c) / |.| rotated onto +z, so the inlet
+    face is the plane z = 0 as for the straight tube.  Labels and the peak-1 inlet profile (along the
+    inlet tangent) follow ``straight_tube``.  ``handed`` = +1 or -1 picks the helix's sense."""
+    if not curvature_radius > radius:
+        raise ValueError("the curvature radius must exceed the tube radius")
+    pos2, patches, rim = ogrid_cross_section(radius, core, ring, core_half, bulge)
+    n2d = len(pos2)
+    planes = layers + 1
+    a = c = 0.5 * curvature_radius
+    speed = math.hypot(a, c)
+    s = np.linspace(0.0, length, planes)
+    t = s / speed
+    # helix along +y (local frame), starting at (a, 0, 0): P(t) = (a cos t, c t, handed a sin t)
+    P = np.stack([a * np.cos(t), c * t, handed * a * np.sin(t)], axis=1)
+    T = np.stack([-a * np.sin(t), np.full_like(t, c), handed * a * np.cos(t)], axis=1) / speed
+    N = np.stack([-np.cos(t), np.zeros_like(t), -handed * np.sin(t)], axis=1)
+    B = np.cross(T, N)
+    # rigid motion taking P(0) to the origin and T(0) to +z, N(0) to +x
+    frame0 = np.stack([N[0], B[0], T[0]])                 # rows: images of x, y, z
+    P = (P - P[0]) @ frame0.T
+    T, N, B = T @ frame0.T, N @ frame0.T, B @ frame0.T
+    points = np.zeros((planes * n2d, 3))
+    for k in range(planes):
+        points[k * n2d:(k + 1) * n2d] = P[k] + pos2[:, :1] * N[k] + pos2[:, 1:2] * B[k]
+    n = len(points)
+    labels = np.full(n, -1, np.int32)
+    for k in range(planes):
+        lab = labels[k * n2d:(k + 1) * n2d]
+        if k == 0:
+            lab[:] = 1
+        elif k == planes - 1:
+            lab[:] = 2
+        lab[rim] = 0
+    r2 = (pos2[:, 0] ** 2 + pos2[:, 1] ** 2) / radius ** 2
+    profile = np.zeros((n, 3))
+    profile[:n2d] = np.maximum(0.0, 1.0 - r2)[:, None] * T[0]
+    ids = np.arange(n, dtype=np.int64).reshape(planes, n2d)
+    block = SweptBlock(patches=patches, ids=ids, wall=[False] + [True] * 4, bottom=1, top=2)
+    mesh, cells = swept_mesh(points, [block])
+    return Tube(mesh=mesh, points=points, labels=labels, cells=cells, profile=profile,
+                radius=radius, length=length, planes=planes, per_plane=n2d)
+
+
 def quad_ogrid(sides, center, ax: int, ay: int, ring: int, core_scale: float = 0.5, bulge: float = 0.2):
     """2D O-grid of a region bounded by four curves: an ``ax x ay`` core and four ring patches.
 
@@ -631,20 +680,79 @@ def combine_tubes(tubes, inlet_scale, gap: float = 1e-3) -> TubeBatch:
                      profile=np.concatenate(profile))
 
 
-def tube_batch(count: int, seed: int = 0, min_elements: int = 1000, max_elements: int = 8000,
-               density: float = 1060.0, viscosity: float = 3.5e-3) -> TubeBatch:
-    """Seeded batch of straight tubes of uneven sizes: radius U(0.5, 3) mm, length U(10, 40) radii,
-    4x4-core O-grid (32 cells per layer) with layers chosen so that each tube has an element count
-    drawn U(min_elements, max_elements), Reynolds number U(50, 800) giving the inlet peak velocity
-    Re mu / (rho 2R)."""
+@dataclass
+class TubeSpec:
+    """Parameters of one tube of a batch (enough to build it, or to estimate its cost)."""
+    radius: float
+    length: float
+    layers: int
+    inlet_scale: float
+    curvature_radius: float = 0.0      # 0: straight, else helical with this centreline curvature radius
+    handed: float = 1.0
+
+    @property
+    def elements(self) -> int:
+        return 32 * self.layers
+
+    def build(self) -> Tube:
+        if self.curvature_radius > 0.0:
+            return helical_tube(self.radius, self.length, self.curvature_radius, core=4, ring=1, layers=self.layers,
+                                handed=self.handed)
+        return straight_tube(self.radius, self.length, core=4, ring=1, layers=self.layers)
+
+
+def tube_batch_specs(count: int, seed: int = 0, min_elements: int = 1000, max_elements: int = 8000,
+                     density: float = 1060.0, viscosity: float = 3.5e-3, helical: float = 0.0,
+                     log_sizes: bool = False) -> list:
+    """Seeded tube parameters: radius U(0.5, 3) mm, length U(10, 40) radii, 4x4-core O-grid (32 cells
+    per layer) with layers giving an element count drawn U(min_elements, max_elements) (log-uniform with
+    ``log_sizes``), Reynolds number U(50, 800) giving the inlet peak velocity Re mu / (rho 2R); with
+    probability ``helical`` a tube is helically curved with centreline curvature radius U(10, 40) mm."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    tubes, scales = [], []
+    specs = []
     for _ in range(count):
         radius = rng.uniform(0.5e-3, 3e-3)
         length = rng.uniform(10.0, 40.0) * radius
-        elements = int(rng.uniform(min_elements, max_elements))
+        if log_sizes:
+            elements = int(math.exp(rng.uniform(math.log(min_elements), math.log(max_elements))))
+        else:
+            elements = int(rng.uniform(min_elements, max_elements))
         layers = max(4, elements // 32)
-        tubes.append(straight_tube(radius, length, core=4, ring=1, layers=layers))
         reynolds = rng.uniform(50.0, 800.0)
-        scales.append(reynolds * viscosity / (density * 2.0 * radius))
-    return combine_tubes(tubes, scales)
+        curved = rng.uniform() < helical
+        curvature = rng.uniform(10e-3, 40e-3) if curved else 0.0
+        handed = 1.0 if rng.uniform() < 0.5 else -1.0
+        specs.append(TubeSpec(radius, length, layers, reynolds * viscosity / (density * 2.0 * radius),
+                              curvature, handed))
+    return specs
+
+
+def tube_batch(count: int, seed: int = 0, min_elements: int = 1000, max_elements: int = 8000,
+               density: float = 1060.0, viscosity: float = 3.5e-3, helical: float = 0.0,
+               log_sizes: bool = False, indices=None) -> TubeBatch:
+    """Seeded batch of tubes of uneven sizes (``tube_batch_specs``) as one disjoint-union mesh; with
+    ``indices``, only those tubes of the seeded batch (in that order)."""
+    specs = tube_batch_specs(count, seed, min_elements, max_elements, density, viscosity, helical, log_sizes)
+    chosen = range(count) if indices is None else indices
+    return combine_tubes([specs[k].build() for k in chosen], [specs[k].inlet_scale for k in chosen])
+
+
+def tube_cost(spec: TubeSpec) -> float:
+    """Work estimate of one tube for partitioning a batch: sum_e nen_e^2 (the element contraction)
+    plus the 4x4 block nonzeros (SpMV and Krylov), with nen = 64 and about 216 blocks per node row
+    (a cubic C2 node couples to a 6x6x6 neighbourhood) for 1.03 nodes per element."""
+    return spec.elements * 64.0 * 64.0 + 1.03 * spec.elements * 216.0
+
+
+def pack_tubes(costs, parts: int) -> list:
+    """Greedy longest-processing-time bin packing: tubes in decreasing cost, each into the part with the
+    smallest total so far (ties to the lower part); each part's tubes in increasing index.  The largest
+    part is within 4/3 of the optimum."""
+    order = sorted(range(len(costs)), key=lambda k: (-costs[k], k))
+    totals = [0.0] * parts
+    members = [[] for _ in range(parts)]
+    for k in order:
+        p = min(range(parts), key=lambda j: (totals[j], j))
+        totals[p] += costs[k]
+        members[p].append(k)
+    return [sorted(m) for m in members]
