@@ -113,7 +113,35 @@ def sustained_bf16():
     return 1400.0
 
 
-def workload(name):
+# The batched-tube workload: 64 seeded tubes, straight or helical, 1k-30k elements (log-uniform).
+C5_TUBES = 64
+C5_BATCH = dict(seed=0, min_elements=1000, max_elements=30000, helical=0.5, log_sizes=True)
+
+
+def c5_specs():
+    from tubularflowiga_b200 import meshgen
+    return meshgen.tube_batch_specs(C5_TUBES, **C5_BATCH)
+
+
+def tube_part(specs, world, rank):
+    """The tubes rank `rank` of `world` solves: greedy longest-first packing on the tube cost model, so
+    the GPUs get about equal work; no tube is split, so the ranks exchange nothing while solving."""
+    from tubularflowiga_b200 import meshgen
+    return meshgen.pack_tubes([meshgen.tube_cost(s) for s in specs], world)[rank]
+
+
+def gather_tube_metrics(dist, tube_ids, metrics):
+    """Per-tube metrics of every rank, in tube order, on every rank (one all_gather of Python objects;
+    identity without a process group)."""
+    local = list(zip([int(k) for k in tube_ids], metrics))
+    if dist is None:
+        return [m for _, m in sorted(local)]
+    parts = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, local)
+    return [m for _, m in sorted(item for part in parts for item in part)]
+
+
+def workload(name, world=1, rank=0):
     from tubularflowiga_b200 import meshgen
     if name == "c2-100":
         tube = meshgen.straight_tube(1.5e-3, 7.5e-3, core=8, ring=2, layers=100)
@@ -121,11 +149,16 @@ def workload(name):
                 "R 1.5 mm, L 7.5 mm, same inflow (profiling case)")
         return tube, desc, meshgen.fourier_waveform(0)
     if name == "c5":
-        batch = meshgen.tube_batch(16, seed=0, min_elements=1000, max_elements=8000)
-        desc = ("batch of 16 independent straight tubes (seed 0): R U(0.5, 3) mm, L U(10, 40) R, "
-                "4x4-core O-grid, 1k-8k tricubic elements each (%d in all), Re U(50, 800), a seeded Fourier "
-                "inflow per tube; one disjoint-union mesh" % batch.mesh.elements)
-        return batch, desc, [meshgen.fourier_waveform(k) for k in range(16)]
+        specs = c5_specs()
+        part = tube_part(specs, world, rank)
+        batch = meshgen.tube_batch(C5_TUBES, indices=part, **C5_BATCH)
+        batch.tube_ids = part
+        desc = ("batch of %d independent tubes (seed 0), half of them helical (centreline curvature radius "
+                "U(10, 40) mm): R U(0.5, 3) mm, L U(10, 40) R, 4x4-core O-grid, 1k-30k tricubic elements each "
+                "(log-uniform; %d in all, %d on this rank's GPU), Re U(50, 800), a seeded Fourier inflow per "
+                "tube; each GPU's tubes (greedy cost packing) as one disjoint-union mesh with per-tube Newton "
+                "tests" % (C5_TUBES, sum(s.elements for s in specs), batch.mesh.elements))
+        return batch, desc, [meshgen.fourier_waveform(k) for k in part]
     if name == "c3":
         y = meshgen.y_bifurcation()
         desc = ("Y-bifurcation %d tricubic elements: parent R 2.0 mm L 20 mm, daughters R 1.59 mm L 16 mm at "
@@ -682,7 +715,7 @@ def main():
         torch.cuda.set_device(0)
     from tubularflowiga_b200 import api
 
-    tube, desc, wave = workload(args.workload)
+    tube, desc, wave = workload(args.workload, world, rank)
     n = tube.mesh.nodes
     mesh = api.Mesh(tube.mesh)
     amg = args.preconditioner == "amg"
@@ -697,6 +730,9 @@ def main():
                      newton_forcing=int(args.forcing == "ew"), tangent_reuse_factor=args.tangent_reuse)
     precision = {"mixed": api.MIXED, "bf16x3": api.MIXED_BF16X3, "fp64": api.FP64}[args.precision]
     ns = api.NavierStokes(mesh, precision=precision, **solver_kw)
+    batched = args.workload == "c5"
+    if batched:
+        ns.set_segments(tube.node_offset)
     dt = ns.params.dt
     vmask, pmask, velocity_at = boundary(tube, wave)
 
@@ -800,6 +836,19 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
 
+    tube_metrics = None
+    amg_levels = ns.amg_info() if amg else None
+    tangent_info = ns.tangent_kernel() if mixed else None
+    if batched:
+        done, residuals = ns.segment_status()
+        specs = c5_specs()
+        tube_metrics = [{"tube": int(tube.tube_ids[k]), "rank": rank,
+                         "elements": int(tube.element_offset[k + 1] - tube.element_offset[k]),
+                         "helical": bool(specs[tube.tube_ids[k]].curvature_radius > 0),
+                         "final_residual": float(residuals[k]), "passed": bool(done[k])}
+                        for k in range(len(tube.tubes))]
+        ns.close()              # the FP64 arm below needs the memory; its errors use the saved states
+
     # plain FP64 GPU solver on the same steps: the same Dirichlet sequence and starting state, the same
     # Newton test, residual-first check, tangent-reuse rule, outlet coupling and restart; the warm-up
     # steps untimed, the timed steps between CUDA events.  Run with the mixed arm's linear-tolerance mode
@@ -831,6 +880,17 @@ def main():
                 errors.append({"step": k,
                                "velocity": float(np.linalg.norm(mx[:, :3] - r64[:, :3]) / np.linalg.norm(r64[:, :3])),
                                "pressure": float(np.linalg.norm(mx[:, 3] - r64[:, 3]) / np.linalg.norm(r64[:, 3]))})
+            if batched:
+                # per-tube relative L2 error of the mixed state against this run after the last step
+                r64 = ref.get_state().reshape(-1, 4)
+                mx = states[total - 1].reshape(-1, 4)
+                per_tube = []
+                for k in range(len(tube.tubes)):
+                    lo, hi = tube.node_offset[k], tube.node_offset[k + 1]
+                    per_tube.append({"velocity": float(np.linalg.norm(mx[lo:hi, :3] - r64[lo:hi, :3])
+                                                       / np.linalg.norm(r64[lo:hi, :3])),
+                                     "pressure": float(np.linalg.norm(mx[lo:hi, 3] - r64[lo:hi, 3])
+                                                       / max(np.linalg.norm(r64[lo:hi, 3]), 1e-300))})
             ref.close()
             newton_n = np.sum([r["newton_iterations"] for r in fp64_reports])
             return {"value": args.steps / (fp64_ms / 1e3), "unit": "time steps/s", "forcing": forcing,
@@ -840,13 +900,18 @@ def main():
                     "linear_iterations_per_newton": float(np.sum([r["linear_iterations"] for r in fp64_reports])
                                                           / max(1, newton_n)),
                     "error_vs_fp64_per_step": errors,
+                    "per_tube_error": per_tube if batched else None,
                     "max_error": {"velocity": max(e["velocity"] for e in errors),
                                   "pressure": max(e["pressure"] for e in errors)}}
 
         runs = {mode: fp64_run(mode) for mode in dict.fromkeys([args.forcing, "fixed"])}
         best = max(runs.values(), key=lambda r: r["value"] or 0.0)
         same = runs[args.forcing]
-        fp64_leg = {k: v for k, v in best.items() if k not in ("error_vs_fp64_per_step", "max_error")}
+        fp64_leg = {k: v for k, v in best.items() if k not in ("error_vs_fp64_per_step", "max_error",
+                                                               "per_tube_error")}
+        if batched and tube_metrics is not None:
+            for m, err in zip(tube_metrics, same["per_tube_error"]):
+                m["error_vs_fp64"] = err
         fp64_leg["variants"] = {m: {k: r[k] for k in ("value", "ms_per_step", "newton_per_step",
                                                        "linear_iterations_per_newton", "max_error")}
                                 for m, r in runs.items()}
@@ -861,6 +926,8 @@ def main():
                                                                                     args.tangent_reuse))
 
     ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms], "cuda")
+    if batched:
+        tube_metrics = gather_tube_metrics(dist, tube.tube_ids, tube_metrics)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -892,7 +959,7 @@ def main():
         # (dn^2 doubles), and the fused fine-level correction, which reads b, the mask, the aggregate
         # map, the A P blocks with their column indices and row offsets, the block-Jacobi inverse
         # (128 B per node), and writes z.  The smoother's residual goes through A P, so no pass over A.
-        info = ns.amg_info()
+        info = amg_levels
         dn = 4 * info["nodes"][-1]
         ap = info["transfer_blocks"]
         ap_entry = 4 if mixed else 8        # A P is stored in the fine matrix's precision
@@ -902,7 +969,7 @@ def main():
         kernels["amg_vcycle"] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s", "frac": a / hbm,
                                  "traffic": None, "launches": amg_n, "avg_ms": amg_ms / amg_n,
                                  "share": amg_ms / prof_ms, "algorithmic_bytes": vbytes,
-                                 "levels": ns.amg_info()}
+                                 "levels": amg_levels}
     asm_name = "assembly_tc" if mixed else "assembly_fp64"
     if asm_n and mixed:
         # tensor-core element contraction: F_e = 8192 nen^2 MMA flops per element, timed inside the long
@@ -996,8 +1063,12 @@ def main():
     }
     if fp64_leg:
         line["mixed_over_fp64"] = {m: steps_per_s / v["value"] for m, v in fp64_leg["variants"].items()}
+    if tangent_info is not None:
+        line["tangent_kernel"] = tangent_info
+    if batched:
+        line["tubes"] = tube_metrics
     if not args.no_cpu_baseline and world == 1:
-        st = ns.get_state()
+        st = states[-1]
         try:
             rn, rl = reference_counts(args.workload) if args.workload in REFERENCE_COUNTS else (newton, linear)
             cpu = CpuReference(tube, st, st)

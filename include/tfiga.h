@@ -308,6 +308,16 @@ int tfiga_ns_step_outlets_coupled(tfiga_ns* ns, tfiga_outlet* outlets, int32_t c
 	int32_t max_newton, tfiga_step_report* report, int32_t* pressure_updates);
 /* AMG hierarchy sizes (levels = 0 before the hierarchy is built). */
 int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info);
+/* Batched tubes (north-star form 2; no counterpart in the reference, which solves one mesh): the node
+ * ranges [node_offsets[k], node_offsets[k+1]) of count independent tubes (node_offsets increasing
+ * from 0 to nodes, e.g. tfiga_batch_mesh_create's node offsets); count 0 removes them.  The Newton
+ * test is then taken per tube, relative to the tube's own first residual of the step, and a tube that
+ * passes is frozen for the rest of the step (its rows of the linear system carry a zero rhs); the
+ * step converges when every tube has passed. */
+int tfiga_ns_set_segments(tfiga_ns* ns, const int64_t* node_offsets, int32_t count);
+/* Per tube, after a Newton iteration: done[k] 1 when tube k has passed its test in this step, and its
+ * residual norm (either output may be NULL). */
+int tfiga_ns_segment_status(tfiga_ns* ns, int32_t* done, double* residuals);
 /* Tensor-core modes: the tangent organisation in use (*kernel: TFIGA_TANGENT_*, AUTO before the
  * first tangent) and the autotuner's times of the coefficient-array and fused organisations (ms,
  * 0 when not timed).  No counterpart in the reference.  Any output may be NULL. */

@@ -172,6 +172,8 @@ SIGNATURES = {
                                                 C.POINTER(StepReport), C.POINTER(C.c_int32)]),
     "tfiga_ns_amg_info": (C.c_int, [C.c_void_p, C.POINTER(AmgInfo)]),
     "tfiga_ns_tangent_kernel": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_ns_set_segments": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "tfiga_ns_segment_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "tfiga_ns_boundary_flows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "tfiga_ns_spmv_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "tfiga_ns_device_buffers": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
@@ -462,6 +464,23 @@ class NavierStokes:
         check(lib().tfiga_ns_set_profiling(self._h, int(enable)))
 
     FAMILIES = ("assembly", "spmv", "krylov_orthogonalisation", "amg_vcycle", "residual")
+
+    def set_segments(self, node_offsets):
+        """Per-tube Newton tests over the node ranges of a batch (tfiga_ns_set_segments); None removes them."""
+        if node_offsets is None:
+            self._segments = None
+            check(lib().tfiga_ns_set_segments(self._h, None, 0))
+            return
+        self._segments = np.ascontiguousarray(node_offsets, np.int64)
+        check(lib().tfiga_ns_set_segments(self._h, _p(self._segments), len(self._segments) - 1))
+
+    def segment_status(self):
+        """(done [T], residual norms [T]) after the last Newton iteration."""
+        count = len(self._segments) - 1
+        done = np.zeros(count, np.int32)
+        res = np.zeros(count)
+        check(lib().tfiga_ns_segment_status(self._h, _p(done), _p(res)))
+        return done, res
 
     def tangent_kernel(self) -> dict:
         """The tensor-core tangent organisation in use and the autotuner's timings."""

@@ -398,6 +398,22 @@ int tfiga_ns_step_outlets_coupled(tfiga_ns* ns, tfiga_outlet* outlets, int32_t c
 	});
 }
 
+int tfiga_ns_set_segments(tfiga_ns* ns, const int64_t* node_offsets, int32_t count)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		ns->solver->SetSegments(node_offsets, count);
+	});
+}
+
+int tfiga_ns_segment_status(tfiga_ns* ns, int32_t* done, double* residuals)
+{
+	return Guard([&] {
+		Require(ns != nullptr, "null handle");
+		ns->solver->SegmentStatus(done, residuals);
+	});
+}
+
 int tfiga_ns_tangent_kernel(tfiga_ns* ns, int32_t* kernel, double* coefficients_ms, double* fused_ms)
 {
 	return Guard([&] {

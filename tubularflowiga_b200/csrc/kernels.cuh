@@ -159,6 +159,12 @@ void LaunchAxpy(long long n, double alpha, const double* x, double* y, cudaStrea
 void LaunchSegmentSums(int segments, const int32_t* segment_of, int items, const double* values, double* out,
 	cudaStream_t stream);
 
+// Independent segments of a vector (the tubes of a batched mesh, in entries): out[k] = sum of x^2 over
+// [offsets[k], offsets[k+1]); and x = 0 on every segment whose flag is set.
+void LaunchSegmentSquares(int segments, const int64_t* offsets, const double* x, double* out, cudaStream_t stream);
+void LaunchZeroFlaggedSegments(int segments, const int64_t* offsets, const int32_t* flag, double* x,
+	cudaStream_t stream);
+
 int PartialSlots();
 
 // ---- outlets.cu ---------------------------------------------------------

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <sstream>
 #include <string>
@@ -114,6 +115,7 @@ NsSolver::~NsSolver()
 {
 	for (auto& ev : events_) if (ev) cudaEventDestroy(ev);
 	if (pinned_) cudaFreeHost(pinned_);
+	if (pinned_segments_) cudaFreeHost(pinned_segments_);
 	if (pinned_status_) cudaFreeHost(pinned_status_);
 }
 
@@ -507,6 +509,11 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	ApplyDirichletRhs();
 	LaunchNorm(n4_, rhs_.get(), partial_.get(), scalars_.get()+kNorm, stream_);
 	launches_ += 2;
+	if (segments_) {
+		LaunchSegmentSquares(segments_, segment_entries_.get(), rhs_.get(), segment_sq_.get(), stream_);
+		segment_sq_.Download(pinned_segments_, segments_, stream_);
+		launches_ += 1;
+	}
 	CudaCheck(cudaEventRecord(events_[1], stream_), "event");
 	scalars_.Download(pinned_, kSlots, stream_);
 	if (!labels_.empty()) label_flow_.Download(pinned_+kSlots, labels_.size(), stream_);
@@ -527,9 +534,35 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	const double initial = initial_residual < 0.0 ? norm : initial_residual;
 	const double scale = std::sqrt((double)n4_);
 	report.tolerance = std::max(params_.nonlinear_atol*scale, params_.nonlinear_rtol*initial);
-	if (norm <= report.tolerance && d.imbalance <= params_.mass_rtol) {
+	bool residual_ok = norm <= report.tolerance;
+	double active_tolerance = report.tolerance;      // tightest test still open (forcing floor)
+	if (segments_) {
+		// per-segment Newton tests; a segment that passed stays frozen for the rest of the step
+		if (initial_residual < 0.0) std::fill(segment_done_host_.begin(), segment_done_host_.end(), 0);
+		residual_ok = true;
+		active_tolerance = std::numeric_limits<double>::infinity();
+		for (int k = 0; k < segments_; ++k) {
+			segment_norm_[k] = std::sqrt(pinned_segments_[k]);
+			if (initial_residual < 0.0) segment_initial_[k] = segment_norm_[k];
+			const double tol = std::max(params_.nonlinear_atol*std::sqrt(4.0*(segment_nodes_[k+1]-segment_nodes_[k])),
+				params_.nonlinear_rtol*segment_initial_[k]);
+			if (segment_norm_[k] <= tol) segment_done_host_[k] = 1;
+			if (!segment_done_host_[k]) {
+				residual_ok = false;
+				active_tolerance = std::min(active_tolerance, tol);
+			}
+		}
+		if (!std::isfinite(active_tolerance)) active_tolerance = report.tolerance;
+	}
+	if (residual_ok && d.imbalance <= params_.mass_rtol) {
 		report.converged = 1;
 		return report;
+	}
+	if (segments_) {
+		// frozen segments take no update: their rhs rows vanish before the linear solve
+		segment_done_.Upload(segment_done_host_.data(), segments_, stream_);
+		LaunchZeroFlaggedSegments(segments_, segment_entries_.get(), segment_done_.get(), rhs_.get(), stream_);
+		launches_ += 1;
 	}
 	// Tangent reuse: keep the previous iteration's tangent while that iteration contracted the
 	// residual about as far as its linear tolerance allowed.
@@ -566,7 +599,7 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 			eta = std::min(eta, kEtaMax);
 		}
 		eta = std::max(eta, params_.gmres_rtol);
-		eta = std::max(eta, std::min(0.1, 0.5*report.tolerance/norm));
+		eta = std::max(eta, std::min(0.1, 0.5*active_tolerance/norm));
 		forcing_norm_ = norm;
 		forcing_eta_ = eta;
 	}
@@ -829,6 +862,42 @@ void NsSolver::BoundaryFlows(const int32_t* labels, int count, double* flows)
 	for (int i = 0; i < count; ++i) {
 		const auto it = slot_of_label_.find(labels[i]);
 		flows[i] = it == slot_of_label_.end() ? 0.0 : per_label[it->second];
+	}
+}
+
+void NsSolver::SetSegments(const int64_t* node_offsets, int count)
+{
+	if (count < 0) Fail(-1, "segment count must be non-negative");
+	if (count == 0) {
+		segments_ = 0;
+		return;
+	}
+	if (node_offsets == nullptr) Fail(-1, "null segment offsets");
+	if (node_offsets[0] != 0 || node_offsets[count] != nodes()) Fail(-1, "segments must cover the nodes from 0");
+	for (int k = 0; k < count; ++k)
+		if (!(node_offsets[k+1] > node_offsets[k])) Fail(-1, "segment offsets must increase");
+	segment_nodes_.assign(node_offsets, node_offsets+count+1);
+	std::vector<int64_t> entries(count+1);
+	for (int k = 0; k <= count; ++k) entries[k] = 4*node_offsets[k];
+	segment_entries_.Allocate(count+1);
+	segment_entries_.Upload(entries.data(), count+1, stream_);
+	segment_sq_.Allocate(count);
+	segment_done_.Allocate(count);
+	segment_initial_.assign(count, 0.0);
+	segment_norm_.assign(count, 0.0);
+	segment_done_host_.assign(count, 0);
+	if (pinned_segments_) cudaFreeHost(pinned_segments_);
+	pinned_segments_ = nullptr;
+	CudaCheck(cudaMallocHost(reinterpret_cast<void**>(&pinned_segments_), sizeof(double)*count), "pinned segments");
+	CudaCheck(cudaStreamSynchronize(stream_), "segments");
+	segments_ = count;
+}
+
+void NsSolver::SegmentStatus(int32_t* done, double* residuals) const
+{
+	for (int k = 0; k < segments_; ++k) {
+		if (done) done[k] = segment_done_host_[k];
+		if (residuals) residuals[k] = segment_norm_[k];
 	}
 }
 

@@ -48,6 +48,15 @@ public:
 	tfiga_step_report StepOutletsCoupled(tfiga_outlet* outlets, int count, double relaxation, int max_newton,
 		int* updates);
 	void BoundaryFlows(const int32_t* labels, int count, double* flows);
+	// Independent segments of the node range (the tubes of a batched mesh): node_offsets[count + 1],
+	// increasing from 0 to nodes; count 0 removes them.  With segments the Newton test is taken per
+	// segment -- ||r_k|| <= max(atol sqrt(4 n_k), rtol ||r_k,0||) with r_k,0 the segment's residual at
+	// the step's first iteration -- and a segment that passes is frozen: its rhs rows are zeroed before
+	// each later linear solve, so its update is zero (the system is block diagonal over the segments).
+	// The step converges when every segment passes (and the mass test holds).
+	void SetSegments(const int64_t* node_offsets, int count);
+	// After a Newton iteration: per segment 1 if it has passed its test in this step, and its residual.
+	void SegmentStatus(int32_t* done, double* residuals) const;
 	void Synchronize();
 
 	int64_t nodes() const { return mesh_.nodes(); }
@@ -160,6 +169,15 @@ private:
 	int outlet_iteration_ = 0;
 	double outlet_relaxation_ = 1.0;
 	bool last_outlet_ok_ = false;
+	// segments (SetSegments)
+	int segments_ = 0;
+	std::vector<int64_t> segment_nodes_;
+	std::vector<double> segment_initial_, segment_norm_;
+	std::vector<int32_t> segment_done_host_;
+	DeviceArray<int64_t> segment_entries_;
+	DeviceArray<double> segment_sq_;
+	DeviceArray<int32_t> segment_done_;
+	double* pinned_segments_ = nullptr;
 };
 
 } // namespace tfiga

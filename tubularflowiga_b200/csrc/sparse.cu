@@ -256,6 +256,29 @@ __global__ void ToFloatKernel(long long n, const double* __restrict__ in, float*
 
 } // namespace
 
+// out[k] = sum of x[i]^2 over [offsets[k], offsets[k+1]) -- one CTA per segment, fixed order.
+__global__ void __launch_bounds__(256) SegmentSquaresKernel(const int64_t* __restrict__ offsets,
+	const double* __restrict__ x, double* __restrict__ out)
+{
+	__shared__ double shared[8];
+	const int64_t lo = offsets[blockIdx.x], hi = offsets[blockIdx.x+1];
+	double sq = 0.0;
+	for (long long i = lo+threadIdx.x; i < hi; i += blockDim.x) sq += x[i]*x[i];
+	sq = BlockSum(sq, shared);
+	if (threadIdx.x == 0) out[blockIdx.x] = sq;
+}
+
+// x[i] = 0 on the segments k whose flag[k] is set.
+__global__ void ZeroFlaggedSegmentsKernel(int segments, const int64_t* __restrict__ offsets,
+	const int32_t* __restrict__ flag, double* __restrict__ x)
+{
+	const int k = blockIdx.y;
+	if (k >= segments || !flag[k]) return;
+	const int64_t lo = offsets[k], hi = offsets[k+1];
+	for (long long i = lo+(long long)blockIdx.x*blockDim.x+threadIdx.x; i < hi; i += (long long)gridDim.x*blockDim.x)
+		x[i] = 0.0;
+}
+
 int PartialSlots() { return 2*kReduceBlocks; }
 
 template <class T>
@@ -379,6 +402,21 @@ void LaunchNorm(long long n, const double* x, double* partial, double* out, cuda
 	LaunchCheck("StridedPartialKernel");
 	FinalizeSumsKernel<<<1, 256, 0, stream>>>(kReduceBlocks, partial, out, 1);
 	LaunchCheck("FinalizeSumsKernel");
+}
+
+void LaunchSegmentSquares(int segments, const int64_t* offsets, const double* x, double* out, cudaStream_t stream)
+{
+	if (segments == 0) return;
+	SegmentSquaresKernel<<<segments, 256, 0, stream>>>(offsets, x, out);
+	LaunchCheck("SegmentSquaresKernel");
+}
+
+void LaunchZeroFlaggedSegments(int segments, const int64_t* offsets, const int32_t* flag, double* x,
+	cudaStream_t stream)
+{
+	if (segments == 0) return;
+	ZeroFlaggedSegmentsKernel<<<dim3(16, segments), 256, 0, stream>>>(segments, offsets, flag, x);
+	LaunchCheck("ZeroFlaggedSegmentsKernel");
 }
 
 void LaunchAxpy(long long n, double alpha, const double* x, double* y, cudaStream_t stream)
