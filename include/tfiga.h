@@ -149,6 +149,8 @@ typedef struct tfiga_ns_params {
 #define TFIGA_PRECISION_MIXED 1
 #define TFIGA_PRECISION_FP32_JACOBIAN 2
 #define TFIGA_PRECISION_MIXED_BF16X3 3
+#define TFIGA_LEARNED_RESIDUAL_LOSS 0
+#define TFIGA_LEARNED_ERROR_LOSS 1
 #define TFIGA_TANGENT_AUTO 0
 #define TFIGA_TANGENT_COEFFICIENTS 1
 #define TFIGA_TANGENT_FUSED 2
@@ -381,6 +383,12 @@ int tfiga_learned_info(const tfiga_learned* learned, int64_t* parameters, int64_
 int tfiga_ns_set_learned(tfiga_ns* ns, tfiga_learned* learned, int32_t use, int32_t collect);
 /* Linear solves that did not converge with the learned stage and were redone with the AMG alone. */
 int tfiga_ns_learned_fallbacks(const tfiga_ns* ns, int64_t* count);
+/* Training loss: TFIGA_LEARNED_RESIDUAL_LOSS (default) fits A N(x) to the residual the AMG leaves,
+ * through the current Jacobian; TFIGA_LEARNED_ERROR_LOSS fits N(x) to the FP64 error of the AMG,
+ * delta - M_AMG(b), of the solver's own (residual, FP64 solution) pairs. */
+int tfiga_learned_set_loss(tfiga_learned* learned, int32_t loss);
+/* Pair store size (default 128; before the first pair is stored): 3 vectors of 4n doubles each. */
+int tfiga_learned_set_capacity(tfiga_learned* learned, int32_t capacity);
 /* Per-field input/output scales and loss weights from the stored pairs. */
 int tfiga_learned_fit_scales(tfiga_learned* learned);
 /* `steps` Adam steps over the stored pairs; *loss = mean loss of the last pass. */

@@ -192,6 +192,8 @@ SIGNATURES = {
                                      C.POINTER(C.c_int32)]),
     "tfiga_ns_set_learned": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
     "tfiga_learned_fit_scales": (C.c_int, [C.c_void_p]),
+    "tfiga_learned_set_loss": (C.c_int, [C.c_void_p, C.c_int32]),
+    "tfiga_learned_set_capacity": (C.c_int, [C.c_void_p, C.c_int32]),
     "tfiga_ns_learned_fallbacks": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "tfiga_learned_train": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.POINTER(C.c_double)]),
     "tfiga_learned_evaluate": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
@@ -543,6 +545,13 @@ class Learned:
 
     def detach(self):
         check(lib().tfiga_ns_set_learned(self.ns._h, None, 0, 0))
+
+    def set_loss(self, error: bool):
+        """Train on the FP64 error of the AMG (error=True) or on the residual it leaves (default)."""
+        check(lib().tfiga_learned_set_loss(self._h, 1 if error else 0))
+
+    def set_capacity(self, capacity: int):
+        check(lib().tfiga_learned_set_capacity(self._h, int(capacity)))
 
     def fit_scales(self):
         check(lib().tfiga_learned_fit_scales(self._h))

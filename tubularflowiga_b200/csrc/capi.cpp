@@ -44,6 +44,7 @@ struct tfiga_learned {
 	std::unique_ptr<tfiga::LearnedPreconditioner> net;
 	tfiga_ns* owner = nullptr;              // the ns handle it was created on (its mesh and stream)
 	tfiga_ns* attached = nullptr;
+	int32_t loss = TFIGA_LEARNED_RESIDUAL_LOSS;
 };
 
 namespace {
@@ -824,9 +825,37 @@ int tfiga_ns_learned_fallbacks(const tfiga_ns* ns, int64_t* count)
 	});
 }
 
+namespace {
+
+// The residual loss trains through the owner's current Jacobian; the error loss through none.
+void BindLoss(tfiga_learned* learned)
+{
+	if (learned->loss == TFIGA_LEARNED_ERROR_LOSS) learned->net->SetOperator({}, nullptr, nullptr);
+	else if (learned->owner) learned->owner->solver->BindLearnedOperator(*learned->net);
+}
+
+} // namespace
+
+int tfiga_learned_set_loss(tfiga_learned* learned, int32_t loss)
+{
+	return Guard([&] {
+		Require(learned != nullptr, "null handle");
+		Require(loss == TFIGA_LEARNED_RESIDUAL_LOSS || loss == TFIGA_LEARNED_ERROR_LOSS, "unknown learned loss");
+		learned->loss = loss;
+	});
+}
+
+int tfiga_learned_set_capacity(tfiga_learned* learned, int32_t capacity)
+{
+	return Guard([&] {
+		Require(learned != nullptr && capacity > 0, "invalid argument");
+		learned->net->SetCapacity(capacity);
+	});
+}
+
 int tfiga_learned_fit_scales(tfiga_learned* learned)
 {
-	return Guard([&] { Require(learned != nullptr, "null handle"); if (learned->owner) learned->owner->solver->BindLearnedOperator(*learned->net);
+	return Guard([&] { Require(learned != nullptr, "null handle"); BindLoss(learned);
 		learned->net->FitScales(); });
 }
 
@@ -835,7 +864,7 @@ int tfiga_learned_train(tfiga_learned* learned, int32_t steps, double learning_r
 	return Guard([&] {
 		Require(learned != nullptr && steps >= 0, "invalid argument");
 		Require(learning_rate > 0.0 && std::isfinite(learning_rate), "learning rate must be positive");
-		if (learned->owner) learned->owner->solver->BindLearnedOperator(*learned->net);
+		BindLoss(learned);
 		const double l = learned->net->Train(steps, learning_rate);
 		if (loss) *loss = l;
 	});
@@ -845,7 +874,7 @@ int tfiga_learned_evaluate(tfiga_learned* learned, double* loss)
 {
 	return Guard([&] {
 		Require(learned && loss, "null argument");
-		if (learned->owner) learned->owner->solver->BindLearnedOperator(*learned->net);
+		BindLoss(learned);
 		*loss = learned->net->EvaluatePairs();
 	});
 }
@@ -854,7 +883,7 @@ int tfiga_learned_fit_gain(tfiga_learned* learned, double* gain)
 {
 	return Guard([&] {
 		Require(learned != nullptr, "null handle");
-		if (learned->owner) learned->owner->solver->BindLearnedOperator(*learned->net);
+		BindLoss(learned);
 		const double g = learned->net->FitGain();
 		if (gain) *gain = g;
 	});

@@ -825,10 +825,17 @@ void LearnedPreconditioner::AddPair(const double* x, const double* target)
 	pair_count_ = std::min(pair_count_+1, capacity_);
 }
 
+void LearnedPreconditioner::SetCapacity(int capacity)
+{
+	if (capacity_ != 0) Fail(-1, "the learned stage's pair store is already allocated");
+	if (capacity < 1) Fail(-1, "pair capacity must be positive");
+	requested_capacity_ = capacity;
+}
+
 void LearnedPreconditioner::AllocatePairs()
 {
 	if (capacity_ != 0) return;
-	capacity_ = kPairCapacity;
+	capacity_ = requested_capacity_;
 	for (auto* a : {&pairs_x_, &pairs_t_, &pairs_q_}) {
 		a->Allocate((size_t)capacity_*4*nodes_);
 		a->Zero(stream_);

@@ -85,6 +85,8 @@ public:
 	bool has_operator() const { return op32_ != nullptr || op64_ != nullptr; }
 	double ResidualLossAndGradient(const double* x, const double* q);
 	int pair_count() const { return pair_count_; }
+	// Size of the pair store (before the first pair; default kPairCapacity).
+	void SetCapacity(int capacity);
 	int pair_capacity() const { return capacity_; }
 	// Scales from the stored pairs (RMS per field; loss weights 1/RMS^2 of the target).
 	void FitScales();
@@ -125,7 +127,7 @@ private:
 	const double* op64_ = nullptr;
 	DeviceArray<double> ro_, g_, atg_;
 	double scale_in_[4] = {1, 1, 1, 1}, scale_out_[4] = {1, 1, 1, 1}, weight_[4] = {1, 1, 1, 1};
-	int pair_count_ = 0, capacity_ = 0, next_pair_ = 0;
+	int pair_count_ = 0, capacity_ = 0, next_pair_ = 0, requested_capacity_ = kPairCapacity;
 	long long adam_steps_ = 0;
 	bool bf16_dirty_ = true;
 	bool linear_ = false;
