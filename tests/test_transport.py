@@ -440,6 +440,32 @@ def test_simulation_config_errors_match_the_reference(api, tmp_path, small_tube)
         with pytest.raises(api.TfigaError) as err:
             api.resolve_flow_boundaries(path, t.labels, t.profile, 0.0)
         assert str(ref_error.value) in str(err.value), (k, str(ref_error.value), str(err.value))
+    # a transport system beside the flow: its time integration and its terms
+    transport = {"name": "species", "kind": "linear_transport", "unknowns": ["pressure"]}
+    for k, system in enumerate([dict(transport, time_integration="steady",
+                                     terms=[{"operator": "mass", "equation": "pressure"}]),
+                                transport]):
+        path = tmp_path / f"transport{k}" / "simulation_config.json"
+        path.parent.mkdir()
+        path.write_text(json.dumps(variant(lambda c: c["equation_systems"].append(system))))
+        with pytest.raises(RuntimeError) as ref_error:
+            O.ref_flow_boundaries(path, t.labels, t.profile, 0.0)
+        with pytest.raises(api.TfigaError) as err:
+            api.resolve_flow_boundaries(path, t.labels, t.profile, 0.0)
+        assert str(ref_error.value) in str(err.value), (k, str(ref_error.value), str(err.value))
+    # texts json.dumps cannot write: a repeated key, and two unknown keys in the opposite of sorted order
+    text = json.dumps(base)
+    raw = [text.replace('"time": {', '"time": {"dt": 0.004, ', 1),
+           text.replace('"schema_version"', '"zeta": 1, "alpha": 2, "schema_version"', 1)]
+    for k, body in enumerate(raw):
+        path = tmp_path / f"raw{k}" / "simulation_config.json"
+        path.parent.mkdir()
+        path.write_text(body)
+        with pytest.raises(RuntimeError) as ref_error:
+            O.ref_flow_boundaries(path, t.labels, t.profile, 0.0)
+        with pytest.raises(api.TfigaError) as err:
+            api.resolve_flow_boundaries(path, t.labels, t.profile, 0.0)
+        assert str(ref_error.value) in str(err.value), (k, str(ref_error.value), str(err.value))
 
 
 @requires_ref

@@ -184,6 +184,15 @@ void ValidateSimulationRoot(const json::Value& root)
 		} else if (object.Find("density")) {
 			SimulationFail("density applies only to navier_stokes");
 		}
+		if (kind == "linear_transport") {
+			// the system-level checks of a transport system (its terms' contents are not repeated here)
+			if (!object.Find("time_integration")) integration = "backward_euler";
+			if (integration != "backward_euler" && integration != "bdf2")
+				SimulationFail("linear_transport time_integration must be 'backward_euler' or 'bdf2'");
+			const auto* terms = object.Find("terms");
+			if (terms == nullptr || CaseArray(*terms, context+".terms").empty())
+				SimulationFail("linear_transport requires terms");
+		}
 	}
 	if (systems.empty()) SimulationFail("equation_systems cannot be empty");
 
@@ -749,11 +758,15 @@ namespace {
 
 void KnownKeys(const json::Value& object, std::initializer_list<const char*> allowed, const std::string& context)
 {
+	// the reference walks its keys in sorted order (a std::map), so the first unknown key it reports is
+	// the smallest one
+	const std::string* first = nullptr;
 	for (const auto& m : object.members) {
 		bool ok = false;
 		for (const char* a : allowed) ok = ok || m.first == a;
-		if (!ok) CaseFail("unknown "+context+" key '"+m.first+"'");
+		if (!ok && (first == nullptr || m.first < *first)) first = &m.first;
 	}
+	if (first) CaseFail("unknown "+context+" key '"+*first+"'");
 }
 
 const json::Value& CaseObject(const json::Value& v, const std::string& context)

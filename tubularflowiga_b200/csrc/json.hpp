@@ -93,7 +93,14 @@ private:
 				Skip();
 				std::string key = ParseString();
 				Expect(':');
-				v.members.emplace_back(std::move(key), ParseValue());
+				Value member = ParseValue();
+				// a repeated key is an error, with the message and byte position of the reference's
+				// JSON reader (include/CaseConfig.hpp:124-142), which every case file goes through
+				for (const auto& m : v.members)
+					if (m.first == key)
+						throw std::runtime_error("case_config.json: duplicate object key '"+key+"' at byte "
+							+std::to_string(i_));
+				v.members.emplace_back(std::move(key), std::move(member));
 			} while (Eat(','));
 			Expect('}');
 		} else if (c == '[') {
