@@ -159,6 +159,14 @@ def workload(name, world=1, rank=0):
                 "tube; each GPU's tubes (greedy cost packing) as one disjoint-union mesh with per-tube Newton "
                 "tests" % (C5_TUBES, sum(s.elements for s in specs), batch.mesh.elements))
         return batch, desc, [meshgen.fourier_waveform(k) for k in part]
+    if name == "c4":
+        tree = meshgen.binary_tree()
+        desc = ("binary tree (seed 0) of depth 4 (15 segments, 8 outlets): root R 2.5 mm along +z, daughter "
+                "radii by Murray's law x U(0.9, 1.1), lengths U(8, 12) R, branch angles U(30, 80) deg in "
+                "alternating planes; swept O-grid regions (8x8 core + 3-cell ring, 2^m per segment above 2^m "
+                "outlets), %d tricubic elements; traction-free outlets; C2's Fourier inflow"
+                % tree.mesh.elements)
+        return tree, desc, meshgen.fourier_waveform(0)
     if name == "c3":
         y = meshgen.y_bifurcation()
         desc = ("Y-bifurcation %d tricubic elements: parent R 2.0 mm L 20 mm, daughters R 1.59 mm L 16 mm at "
@@ -668,7 +676,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c1", "c2-100", "c5", "transport"])
+    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c1", "c2-100", "c4", "c5", "transport"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "mixed", "fp64"])
@@ -741,7 +749,7 @@ def main():
 
     ns.set_dirichlet(vmask, pmask, velocity_at(0.0))
     models = outlet_models(args.workload)
-    fixed_tractions = {} if models else {2: 0.0}
+    fixed_tractions = {} if models else {label: 0.0 for label in getattr(tube, "outlet_labels", (2,))}
     ns.set_tractions(fixed_tractions)
     s0 = api.initial_state(vmask, velocity_at(0.0))
     ns.set_state(s0, s0)
@@ -847,6 +855,7 @@ def main():
                          "helical": bool(specs[tube.tube_ids[k]].curvature_radius > 0),
                          "final_residual": float(residuals[k]), "passed": bool(done[k])}
                         for k in range(len(tube.tubes))]
+    if batched or args.workload == "c4":
         ns.close()              # the FP64 arm below needs the memory; its errors use the saved states
 
     # plain FP64 GPU solver on the same steps: the same Dirichlet sequence and starting state, the same

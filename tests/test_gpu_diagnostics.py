@@ -9,7 +9,8 @@ are checked against the oracle's restatement of the reference's
 MeasureFlowConvergence and acceptance test (solvers/cuda/src/iga_cuda.cu:520-557,
 989-996), evaluated on the oracle's own FP64 assembly of the same state:
 * diagnostics: 1e-12 relative (continuity sum and net flow: 1e-12 of the sum of
-  magnitudes, since both are signed sums that can cancel);
+  magnitudes, since both are signed sums that can cancel), with an absolute floor of
+  1e-20 on the continuity norm and sum for converged states, whose rows cancel;
 * the accept / reject decision of every Newton iteration of a step, including
   iterations that the mass test alone rejects (mass_rtol at the default 1e-3 and
   at a value the step-start imbalance exceeds).
@@ -41,10 +42,16 @@ def oracle_diagnostics(flat, pattern, state, previous, traction):
     return O.measure_flow_convergence(flat, state, rhs + traction)
 
 
+# Absolute floor of the continuity diagnostics: near a converged state the continuity rows are sums of
+# element contributions of about 1e-7 that cancel to 1e-12, so the device's and the oracle's summation
+# orders differ by a few roundings of those contributions (measured 3.4e-24 at a 1.75e-12 norm).
+CONTINUITY_FLOOR = 1e-20
+
+
 def check_report(report, expect):
-    assert abs(report["continuity_l2"] - expect["continuity_l2"]) <= 1e-12 * expect["continuity_l2"]
+    assert abs(report["continuity_l2"] - expect["continuity_l2"]) <= 1e-12 * expect["continuity_l2"] + CONTINUITY_FLOOR
     scale_c = expect["continuity_l2"] * 1e3
-    assert abs(report["continuity_sum"] - expect["continuity_sum"]) <= 1e-12 * scale_c
+    assert abs(report["continuity_sum"] - expect["continuity_sum"]) <= 1e-12 * scale_c + CONTINUITY_FLOOR
     absolute = expect["absolute_boundary_flow"]
     assert abs(report["absolute_boundary_flow"] - absolute) <= 1e-12 * absolute
     assert abs(report["net_boundary_flow"] - expect["net_boundary_flow"]) <= 1e-12 * absolute

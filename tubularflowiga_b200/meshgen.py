@@ -516,6 +516,328 @@ def y_bifurcation(parent_radius: float = 2.0e-3, parent_length: float = 20e-3,
     return Bifurcation(mesh=mesh, points=points, labels=labels, cells=cells, profile=profile, radius=R,
                        daughter_radius=r, parent_layers=parent_layers, daughter_layers=daughter_layers)
 
+# --- binary trees ---------------------------------------------------------------------------------
+#
+# A tree segment whose subtree ends in 2^m outlets has a cross-section of 2^m O-grid regions (each a
+# ``quad_ogrid`` with an n x n core).  At its end the section is a disc split by a diameter (the
+# septum) into two halves of 2^(m-1) regions each; each half is the start section of one daughter,
+# which morphs it into its own disc of 2^(m-1) regions.  So no section changes topology along a
+# segment, and every junction is conforming (the daughters share the parent's last vertex plane).
+#
+# Section layouts, in a segment's local frame (s away from the parent's septum, y along it):
+#   half-disc layouts S_m(R), the half disc {s >= 0, s^2 + y^2 <= R^2} (a daughter's start):
+#     S_0: one region (sides: arc -45..45 deg, arc 45..90, flat side, arc -90..-45);
+#     S_1: two quarter discs split by the chord y = 0;
+#     S_2: four regions around a hub H = (0.4 R, 0) with spokes to the flat side's midpoint, the arc's
+#          midpoint and the arc points at +-acos(0.4) (the spokes to them are parallel to y);
+#   disc layouts E_m(r) (a segment's end, centred on the disc's centre):
+#     E_0: one region with corners at -45, 45, 135 and 225 deg;
+#     E_m: S_{m-1}(r) rotated by +90 deg (the half y > 0, daughter 0) and by -90 deg (y < 0,
+#          daughter 1); their flat sides meet on the septum y = 0.
+# S_m and E_m list the same regions with the same side numbering and the same shared sides (checked
+# when the layouts are built), so vertex positions morph linearly from one to the other.
+
+_TREE_HUB = 0.4                     # S_2's hub on the s axis, in units of R
+
+
+def _half_layout_sides(m: int, R: float):
+    """Regions of S_m(R): per region its four side curves (counter-clockwise)."""
+    q = 0.25 * math.pi
+    o = (0.0, 0.0)
+    if m == 0:
+        return [[_arc(0.0, 0.0, R, -q, q), _arc(0.0, 0.0, R, q, 2 * q), _segment((0.0, R), (0.0, -R)),
+                 _arc(0.0, 0.0, R, -2 * q, -q)]]
+    if m == 1:
+        return [[_arc(0.0, 0.0, R, q, 2 * q), _segment((0.0, R), o), _segment(o, (R, 0.0)), _arc(0.0, 0.0, R, 0.0, q)],
+                [_arc(0.0, 0.0, R, -2 * q, -q), _arc(0.0, 0.0, R, -q, 0.0), _segment((R, 0.0), o),
+                 _segment(o, (0.0, -R))]]
+    if m == 2:
+        phi = math.acos(_TREE_HUB)
+        H, E = (_TREE_HUB * R, 0.0), (R, 0.0)
+        N, S = (R * math.cos(phi), R * math.sin(phi)), (R * math.cos(phi), -R * math.sin(phi))
+        return [[_segment((0.0, R), o), _segment(o, H), _segment(H, N), _arc(0.0, 0.0, R, phi, 2 * q)],
+                [_arc(0.0, 0.0, R, 0.0, 0.5 * phi), _arc(0.0, 0.0, R, 0.5 * phi, phi), _segment(N, H), _segment(H, E)],
+                [_arc(0.0, 0.0, R, -0.5 * phi, 0.0), _segment(E, H), _segment(H, S), _arc(0.0, 0.0, R, -phi, -0.5 * phi)],
+                [_segment(o, (0.0, -R)), _arc(0.0, 0.0, R, -2 * q, -phi), _segment(S, H), _segment(H, o)]]
+    raise ValueError("tree sections support at most 4 regions per half (depth <= 4)")
+
+
+# shared sides (region, side) <-> (region, side) of S_m, and its flat-side sides from (0, R) to (0, -R)
+_HALF_PAIRS = {0: [], 1: [((0, 2), (1, 2))],
+               2: [((0, 2), (1, 2)), ((1, 3), (2, 1)), ((2, 2), (3, 2)), ((3, 3), (0, 1))]}
+_HALF_FLAT = {0: [(0, 2)], 1: [(0, 1), (1, 3)], 2: [(0, 0), (3, 0)]}
+
+
+def _disc_pairs(m: int):
+    """Shared sides of E_m: each daughter half's own, plus the septum pairs (daughter 0's k-th flat side
+    with daughter 1's flat side counted from the other end)."""
+    if m == 0:
+        return []
+    k = 2 ** (m - 1)
+    pairs = list(_HALF_PAIRS[m - 1]) + [((a + k, sa), (b + k, sb)) for (a, sa), (b, sb) in _HALF_PAIRS[m - 1]]
+    flat = _HALF_FLAT[m - 1]
+    for i, (a, sa) in enumerate(flat):
+        b, sb = flat[len(flat) - 1 - i]
+        pairs.append(((a, sa), (b + k, sb)))
+    return pairs
+
+
+def _region_centre(sides):
+    """Area centroid of a region bounded by four side curves (polygon of 64 samples per side)."""
+    t = np.linspace(0.0, 1.0, 65)[:-1]
+    p = np.concatenate([np.asarray(s(t), np.float64).reshape(-1, 2) for s in sides])
+    x, y = p[:, 0], p[:, 1]
+    xn, yn = np.roll(x, -1), np.roll(y, -1)
+    c = x * yn - xn * y
+    a = 0.5 * c.sum()
+    return np.array([((x + xn) * c).sum(), ((y + yn) * c).sum()]) / (6.0 * a)
+
+
+def _layout_positions(sides_list, core: int, ring: int):
+    out = []
+    for sides in sides_list:
+        pos, patches, rim = quad_ogrid(sides, _region_centre(sides), core, core, ring)
+        out.append(pos)
+    return out, patches, rim
+
+
+def _rot90(pos, sign):
+    """(s, y) -> (-y, s) for sign +1 (daughter 0's half), (y, -s) for sign -1 (daughter 1's)."""
+    return np.stack([-sign * pos[:, 1], sign * pos[:, 0]], axis=1)
+
+
+@dataclass
+class TreeSection:
+    """Plane layout of 2^m O-grid regions: region-local quad_ogrid vertex v of region i is plane-local
+    vertex ``ids[i, v]``; ``start`` = S_m(1) and ``end`` = E_m(1) (centred) positions per plane-local
+    vertex; ``patches[i]`` region i's patches in plane-local ids; ``wall[i]`` its patches' wall flags
+    (core False, ring patch k True when side k is on the outer boundary); ``boundary`` the plane-local
+    ids on the outer boundary."""
+    m: int
+    ids: np.ndarray
+    start: np.ndarray
+    end: np.ndarray
+    patches: list
+    wall: list
+    boundary: np.ndarray
+
+
+def tree_section(m: int, core: int, ring: int) -> TreeSection:
+    """The layout of a segment with 2^m outlets below it (``start`` is None for m = 3, the root of a
+    depth-4 tree, which starts at the inlet with its end layout)."""
+    regions = 2 ** m
+    if m == 0:
+        disc, patches, rim = _layout_positions(
+            [[_arc(0.0, 0.0, 1.0, a, a + 0.5 * math.pi) for a in
+              (-0.25 * math.pi, 0.25 * math.pi, 0.75 * math.pi, 1.25 * math.pi)]], core, ring)
+    else:
+        sub, patches, rim = _layout_positions(_half_layout_sides(m - 1, 1.0), core, ring)
+        disc = [_rot90(p, 1.0) for p in sub] + [_rot90(p, -1.0) for p in sub]
+    half = _layout_positions(_half_layout_sides(m, 1.0), core, ring)[0] if m in _HALF_PAIRS else None
+    pairs = _disc_pairs(m)
+    if half is not None and sorted(map(sorted, _HALF_PAIRS[m])) != sorted(map(sorted, pairs)):
+        raise AssertionError("half and disc layouts disagree on shared sides")
+    nl = len(disc[0])
+    parent = np.arange(regions * nl)
+
+    def find(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+
+    for (a, sa), (b, sb) in pairs:
+        for u, v in zip(a * nl + rim[sa], b * nl + rim[sb][::-1]):
+            fu, fv = find(int(u)), find(int(v))
+            if fu != fv:
+                parent[max(fu, fv)] = min(fu, fv)
+    roots = np.array([find(x) for x in range(regions * nl)])
+    _, ids = np.unique(roots, return_inverse=True)
+    ids = ids.reshape(regions, nl)
+    count = int(ids.max()) + 1
+    layouts = []
+    for src in (half, disc):
+        if src is None:
+            layouts.append(None)
+            continue
+        dst = np.full((count, 2), np.nan)
+        for i in range(regions):
+            seen = ~np.isnan(dst[ids[i], 0])
+            if np.any(np.abs(dst[ids[i]][seen] - src[i][seen]).max(initial=0.0) > 1e-12):
+                raise AssertionError("shared sides do not coincide")
+            dst[ids[i]] = src[i]
+        layouts.append(dst)
+    shared = {rs for pr in pairs for rs in pr}
+    wall = [[False] + [(i, k) not in shared for k in range(4)] for i in range(regions)]
+    bnd = np.unique(np.concatenate([ids[i][rim[k]] for i in range(regions) for k in range(4)
+                                    if (i, k) not in shared]))
+    return TreeSection(m=m, ids=ids, start=layouts[0], end=layouts[1],
+                       patches=[[ids[i][p] for p in patches] for i in range(regions)], wall=wall, boundary=bnd)
+
+
+@dataclass
+class TreeSegment:
+    """One vessel of a binary tree, in pre-order.  ``side`` 0 / 1: the half of the parent's end
+    section it starts from (+y / -y of the parent's end frame); ``outlet``: the outlet label of a
+    terminal segment (2, 3, ... in pre-order), else -1."""
+    level: int
+    parent: int
+    side: int
+    radius: float
+    length: float
+    half_angle: float          # turn of the centreline away from the parent's septum (rad); 0 for the root
+    layers: int = 0
+    outlet: int = -1
+
+
+def tree_segments(depth: int = 4, seed: int = 0, root_radius: float = 2.5e-3) -> list:
+    """Seeded binary tree of ``depth`` generations (2^depth - 1 segments): each daughter's radius is the
+    parent's over 2^(1/3) (Murray's law for equal daughters) times U(0.9, 1.1); each segment is
+    U(8, 12) of its radii long; each bifurcation's branch angle (between the two daughters) is
+    U(30, 80) degrees, half of it to each daughter."""
+    if not 1 <= depth <= 4:
+        raise ValueError("tree depth must be 1..4")
+    rng = np.random.Generator(np.random.PCG64(seed))
+    segs: list = []
+
+    def grow(level, parent, side, radius, half_angle):
+        index = len(segs)
+        segs.append(TreeSegment(level, parent, side, radius, rng.uniform(8.0, 12.0) * radius, half_angle))
+        if level + 1 == depth:
+            return
+        angle = math.radians(rng.uniform(30.0, 80.0))
+        radii = [radius * 2.0 ** (-1.0 / 3.0) * rng.uniform(0.9, 1.1) for _ in range(2)]
+        for c in range(2):
+            grow(level + 1, index, c, radii[c], 0.5 * angle)
+
+    grow(0, -1, 0, root_radius, 0.0)
+    label = 2
+    for s in segs:
+        if s.level == depth - 1:
+            s.outlet = label
+            label += 1
+    return segs
+
+
+@dataclass
+class Tree:
+    """Binary tree of swept O-grid segments: inlet label 1 at the root's first plane (z = 0, flow along
+    +z), one outlet label per terminal segment, wall 0.  ``element_offset[i]`` / ``plane_ids[i]``:
+    segment i's first element and its vertex planes' global ids; ``frames[i]``: its end centre,
+    axis, e_s, e_y."""
+    mesh: FlatMesh
+    points: np.ndarray
+    labels: np.ndarray
+    cells: np.ndarray
+    profile: np.ndarray
+    radius: float
+    segments: list
+    element_offset: np.ndarray
+    plane_ids: list
+    frames: list
+    outlet_labels: tuple
+
+
+def binary_tree(depth: int = 4, seed: int = 0, root_radius: float = 2.5e-3, elements: int = 600_000,
+                core: int = 8, ring: int = 3, bend_fraction: float = 0.5, morph_fraction: float = 0.375) -> Tree:
+    """Swept O-grid binary tree (all hexahedra, one element per cell, C2 inside each patch and segment,
+    C0 across patch and junction interfaces) on ``tree_segments``' seeded skeleton.
+
+    A segment with 2^m terminal segments below it has 2^m regions of ``core`` x ``core`` cores with
+    ``ring`` ring layers each, so every generation has 2^(depth-1) (core^2 + 4 core ring) cells per
+    plane (1,280 for the defaults); the axial spacing is chosen so that the tree has about ``elements``
+    elements.  The root runs straight along +z with its disc layout.  A daughter starts from its half
+    of the parent's last plane (shared vertices), turns its centreline by its half-angle away from the
+    parent's septum over ``bend_fraction`` of its length (about the septum line, smoothstep profile),
+    and morphs its half-disc layout into its own disc over ``morph_fraction`` of it; its points keep
+    s >= 0 in its turning frame, so the two daughters stay on their own sides of the parent's septum
+    plane.  Daughters' septa are perpendicular to their parent's, so successive bifurcation planes
+    alternate."""
+    segs = tree_segments(depth, seed, root_radius)
+    sections = [tree_section(m, core, ring) for m in range(depth)]
+    per_region = core * core + 4 * core * ring
+    spacing = sum(per_region * 2 ** (depth - 1 - s.level) * s.length for s in segs) / elements
+    for s in segs:
+        s.layers = max(3, int(round(s.length / spacing)))
+    counts = []
+    for s in segs:
+        sec = sections[depth - 1 - s.level]
+        counts.append((s.layers + (1 if s.parent < 0 else 0)) * len(sec.end))
+    n = int(sum(counts))
+    points = np.zeros((n, 3))
+    labels = np.full(n, -1, np.int32)
+    plane_ids: list = []
+    frames: list = []
+    blocks = []
+    base = 0
+    fine_per_layer = 64
+    for i, s in enumerate(segs):
+        sec = sections[depth - 1 - s.level]
+        nl = len(sec.end)
+        ids = np.zeros((s.layers + 1, nl), np.int64)
+        if s.parent < 0:
+            d, es, ey = np.array([0.0, 0.0, 1.0]), np.array([1.0, 0.0, 0.0]), np.array([0.0, 1.0, 0.0])
+            ids[:] = base + np.arange((s.layers + 1) * nl).reshape(s.layers + 1, nl)
+            for k in range(s.layers + 1):
+                z = s.length * k / s.layers
+                points[ids[k]] = (z * d + s.radius * (sec.end[:, :1] * es + sec.end[:, 1:] * ey))
+            base += (s.layers + 1) * nl
+            centre = s.length * d
+            labels[ids[0]] = 1
+        else:
+            p = segs[s.parent]
+            pc, pd, pes, pey = frames[s.parent]
+            psec = sections[depth - 1 - p.level]
+            k_half = len(sec.ids)
+            to_parent = np.full(nl, -1, np.int64)
+            for r in range(k_half):
+                to_parent[sec.ids[r]] = psec.ids[s.side * k_half + r]
+            ids[0] = plane_ids[s.parent][-1][to_parent]
+            ids[1:] = base + np.arange(s.layers * nl).reshape(s.layers, nl)
+            base += s.layers * nl
+            n0 = pey if s.side == 0 else -pey
+            ey = np.cross(pd, n0)
+            t = s.length * np.arange(s.layers + 1) / s.layers
+            fine = np.linspace(0.0, s.length, fine_per_layer * s.layers + 1)
+            bend = bend_fraction * s.length
+            th_f = s.half_angle * _smoothstep(fine / bend)
+            dirs = np.cos(th_f)[:, None] * pd + np.sin(th_f)[:, None] * n0
+            path = np.concatenate([np.zeros((1, 3)), np.cumsum(0.5 * (dirs[1:] + dirs[:-1]) * np.diff(fine)[:, None],
+                                                               axis=0)])
+            pivot = pc + np.stack([np.interp(t, fine, path[:, a]) for a in range(3)], axis=1)
+            th = s.half_angle * _smoothstep(t / bend)
+            w = _smoothstep(t / (morph_fraction * s.length))
+            target = s.radius * sec.end + np.array([s.radius, 0.0])
+            for k in range(1, s.layers + 1):
+                loc = (1.0 - w[k]) * p.radius * sec.start + w[k] * target
+                e_s = math.cos(th[k]) * n0 - math.sin(th[k]) * pd
+                points[ids[k]] = pivot[k] + loc[:, :1] * e_s + loc[:, 1:] * ey
+            d = math.cos(th[-1]) * pd + math.sin(th[-1]) * n0
+            es = math.cos(th[-1]) * n0 - math.sin(th[-1]) * pd
+            centre = pivot[-1] + s.radius * es
+        if s.outlet >= 0:
+            labels[ids[-1]] = s.outlet
+        plane_ids.append(ids)
+        frames.append((centre, d, es, ey))
+        blocks.append(SweptBlock(patches=[g for reg in sec.patches for g in reg], ids=ids,
+                                 wall=[f for reg in sec.wall for f in reg],
+                                 bottom=1 if s.parent < 0 else None, top=s.outlet if s.outlet >= 0 else None))
+    for i, s in enumerate(segs):
+        labels[plane_ids[i][:, sections[depth - 1 - s.level].boundary].ravel()] = 0
+    mesh, cells = swept_mesh(points, blocks)
+    per_plane = [len(sections[depth - 1 - s.level].ids) * per_region for s in segs]
+    element_offset = np.zeros(len(segs) + 1, np.int64)
+    element_offset[1:] = np.cumsum([per_plane[i] * s.layers for i, s in enumerate(segs)])
+    profile = np.zeros((n, 3))
+    inlet = plane_ids[0][0]
+    r2 = (points[inlet, 0] ** 2 + points[inlet, 1] ** 2) / root_radius ** 2
+    profile[inlet, 2] = np.maximum(0.0, 1.0 - r2)
+    profile[labels != 1] = 0.0
+    return Tree(mesh=mesh, points=points, labels=labels, cells=cells, profile=profile, radius=root_radius,
+                segments=segs, element_offset=element_offset, plane_ids=plane_ids, frames=frames,
+                outlet_labels=tuple(s.outlet for s in segs if s.outlet >= 0))
+
+
 def write_vtk(path, tube: Tube) -> None:
     n, E = len(tube.points), len(tube.cells)
     with open(path, "w") as f:
