@@ -1016,6 +1016,13 @@ def main():
                                                "algorithmic_bytes_per_launch": algo / orth_n,
                                                "moved_bytes_per_launch": orth_moved / orth_n,
                                                "moved_gbs": orth_moved / (orth_ms * 1e-3) / 1e9}
+    # the rest of the step: AMG set-up for each new Jacobian and the Newton / FGMRES vector bookkeeping
+    # (zeroing, traction, diagnostics, Dirichlet rows, norms, restarts, state updates, outlet coupling)
+    for name in ("amg_setup", "newton_vectors"):
+        ms_f, n_f = prof.get(name, (0.0, 0))
+        if n_f:
+            kernels[name] = {"bound": None, "launches": n_f, "ms_per_step": ms_f / args.steps,
+                             "share": ms_f / prof_ms}
     attributed = sum(k.get("share", 0.0) for k in kernels.values())
     dominant = max((spmv_name, asm_name, "amg_vcycle", "krylov_orthogonalisation", "residual_point"),
                    key=lambda k: kernels.get(k, {}).get("share", 0))

@@ -349,13 +349,17 @@ int tfiga_ns_stream(tfiga_ns* ns, void** stream);
  * 1 SpMV (fused with the block-Jacobi apply in that mode), 2 Krylov
  * orthogonalisation, 3 AMG V-cycle, 4 the FP64 residual and point
  * coefficients of the tensor-core modes (0 elsewhere: the FP64 kernel does
- * both in family 0). */
-#define TFIGA_PROFILE_FAMILIES 5
+ * both in family 0), 5 AMG set-up for a new Jacobian (point-block inverses,
+ * Galerkin coarse operator, dense coarse inverse), 6 the Newton loop's own
+ * vector work (residual and Jacobian zeroing, traction, convergence
+ * diagnostics, Dirichlet rows, norms, the state update, device outlet
+ * coupling, per-segment tests). */
+#define TFIGA_PROFILE_FAMILIES 7
 int tfiga_ns_set_profiling(tfiga_ns* ns, int enable);
 /* Totals since the last reset: milliseconds and launch counts per family. */
 int tfiga_ns_profile(tfiga_ns* ns, double* milliseconds, int64_t* launches, int32_t reset);
 /* Bytes per family since the last reset, as the solver accounts them while
- * profiling is on: bytes[0..4] algorithmic, bytes[5..9] actually moved
+ * profiling is on: bytes[0..6] algorithmic, bytes[7..13] actually moved
  * (2 * TFIGA_PROFILE_FAMILIES entries).  Family 2, Krylov orthogonalisation:
  * algorithmic s_v n (2j + 7) per Arnoldi step j (+ 8 n for the stored
  * FGMRES vector), s_v the basis entry size; moved: both classical

@@ -465,7 +465,8 @@ class NavierStokes:
     def set_profiling(self, enable: bool):
         check(lib().tfiga_ns_set_profiling(self._h, int(enable)))
 
-    FAMILIES = ("assembly", "spmv", "krylov_orthogonalisation", "amg_vcycle", "residual")
+    FAMILIES = ("assembly", "spmv", "krylov_orthogonalisation", "amg_vcycle", "residual", "amg_setup",
+                "newton_vectors")
 
     def set_segments(self, node_offsets):
         """Per-tube Newton tests over the node ranges of a batch (tfiga_ns_set_segments); None removes them."""

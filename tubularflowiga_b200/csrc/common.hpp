@@ -101,7 +101,8 @@ void RequireDevice();
 // the launching stream.  Disabled by default; Collect() waits for the stream.
 class Profiler {
 public:
-	enum Family { kAssembly = 0, kSpmv = 1, kOrtho = 2, kOther = 3, kResidual = 4, kFamilies = 5 };
+	enum Family { kAssembly = 0, kSpmv = 1, kOrtho = 2, kOther = 3, kResidual = 4, kSetup = 5, kVector = 6,
+		kFamilies = 7 };
 	~Profiler();
 	void Enable(bool on) { enabled_ = on; }
 	bool enabled() const { return enabled_; }

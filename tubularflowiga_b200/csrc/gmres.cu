@@ -412,8 +412,11 @@ void Gmres::Orthogonalize(int j, B* basis)
 				hpass_.get(), w_.get(), basis+(size_t)(j+1)*n_, norm_partial_.get(), stop);
 		LaunchCheck("UpdateKernel");
 	}
+	ArnoldiFinalizeKernel<<<1, kThreads, finalize_smem_, stream_>>>(norm_partial_.get(), update_blocks_, H_.get(),
+		restart_, j, cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance_);
+	LaunchCheck("ArnoldiFinalizeKernel");
 	if (profiler_) profiler_->End(stream_);
-	launches_ += 7;
+	launches_ += 8;
 }
 
 template <> double* Gmres::Basis<double>() { return V_.get(); }
@@ -428,8 +431,10 @@ void Gmres::FlexibleStep(const DevicePatternView& pattern, const T* values, int 
 {
 	const int* stop = state_.get();
 	B* basis = Basis<B>();
+	if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
 	ScaleCopyKernel<B><<<blocks_, kThreads, 0, stream_>>>(n_, basis+(size_t)j*n_, scale_.get()+j, r_.get(), stop);
 	LaunchCheck("ScaleCopyKernel");
+	if (profiler_) profiler_->End(stream_);
 	launches_ += 1;
 	double* z = Z_.get()+(size_t)j*n_;
 	M.Apply(values, r_.get(), z, stop);
@@ -459,6 +464,7 @@ double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const T* value
 	const double* x)
 {
 	// v_0 = b - A x (FP64), stored in the basis precision; beta from the FP64 vector
+	if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
 	LaunchSpmv<T>(pattern, values, x, tmp_.get(), stream_);
 	double* r = std::is_same<B, double>::value ? V_.get() : r_.get();
 	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), r);
@@ -469,6 +475,7 @@ double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const T* value
 		LaunchToFloat(n_, r, reinterpret_cast<float*>(Basis<B>()), stream_);
 		launches_ += 1;
 	}
+	if (profiler_) profiler_->End(stream_);
 	scalar_.Download(host_->beta, 1, stream_);
 	CudaCheck(cudaStreamSynchronize(stream_), "FGMRES residual");
 	return host_->beta[0];
@@ -501,21 +508,18 @@ GmresResult Gmres::SolveFlexibleImpl(const DevicePatternView& pattern, const T* 
 		return result;
 	}
 	const double tolerance = std::max(1e-30, rtol*beta);
+	tolerance_ = tolerance;
 	while (result.iterations < max_iterations) {
+		if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
 		CycleInitKernel<<<1, 256, 0, stream_>>>(scalar_.get(), g_.get(), restart_, scale_.get(), state_.get());
 		LaunchCheck("CycleInitKernel");
 		H_.Zero(stream_);
+		if (profiler_) profiler_->End(stream_);
 		launches_ += 1;
 		const int cap = std::min(restart_, max_iterations-result.iterations);
 		for (int j = 0; j < cap;) {
 			const int batch = std::min(kBatch, cap-j);
-			for (int b = 0; b < batch; ++b) {
-				FlexibleStep<T, B>(pattern, values, j+b, M);
-				ArnoldiFinalizeKernel<<<1, kThreads, finalize_smem_, stream_>>>(norm_partial_.get(), update_blocks_, H_.get(), restart_, j+b,
-					cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance);
-				LaunchCheck("ArnoldiFinalizeKernel");
-				launches_ += 1;
-			}
+			for (int b = 0; b < batch; ++b) FlexibleStep<T, B>(pattern, values, j+b, M);
 			j += batch;
 			state_.Download(&host_->stop, 3, stream_);
 			residual_.Download(&host_->residual, 1, stream_);
@@ -528,11 +532,13 @@ GmresResult Gmres::SolveFlexibleImpl(const DevicePatternView& pattern, const T* 
 			profiler_->AddBytes(Profiler::kOrtho, ArnoldiBytes(n_, used, (int)sizeof(B), true));
 			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, (int)sizeof(B)));
 		}
+		if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
 		BackSolveKernel<<<1, 256, (size_t)(restart_+1)*sizeof(double), stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(), state_.get()+2);
 		LaunchCheck("BackSolveKernel");
 		SolutionUpdateKernel<<<blocks_, kThreads, (size_t)(restart_+1)*sizeof(double), stream_>>>(Z_.get(), n_,
 			nullptr, y_.get(), state_.get(), x);
 		LaunchCheck("SolutionUpdateKernel");
+		if (profiler_) profiler_->End(stream_);
 		launches_ += 2;
 		beta = TrueResidualPlain<T, B>(pattern, values, rhs, x);
 		state_.Download(&host_->stop, 3, stream_);
@@ -550,6 +556,7 @@ GmresResult Gmres::SolveFlexibleImpl(const DevicePatternView& pattern, const T* 
 double Gmres::TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs,
 	const double* x)
 {
+	if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
 	if (fields_ == 2) LaunchSpmv2(pattern, values, x, tmp_.get(), stream_);
 	else LaunchSpmv(pattern, values, x, tmp_.get(), stream_);
 	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), r_.get());
@@ -558,6 +565,7 @@ double Gmres::TrueResidual(const DevicePatternView& pattern, const double* value
 	else if (fields_ == 2) LaunchApplyBlockInverse2(nodes_, inverse_.get(), r_.get(), V_.get(), stream_);
 	else LaunchApplyBlockInverse(nodes_, inverse_.get(), r_.get(), V_.get(), stream_);
 	LaunchNorm(n_, V_.get(), norm_partial_.get(), scalar_.get(), stream_);
+	if (profiler_) profiler_->End(stream_);
 	launches_ += 5;
 	scalar_.Download(host_->beta, 1, stream_);
 	CudaCheck(cudaStreamSynchronize(stream_), "GMRES residual");
@@ -587,11 +595,14 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 		return result;
 	}
 	const double tolerance = std::max(1e-30, rtol*beta);
+	tolerance_ = tolerance;
 	const size_t coef_smem = (size_t)(restart_+1)*sizeof(double);
 	while (result.iterations < max_iterations) {
+		if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
 		CycleInitKernel<<<1, 256, 0, stream_>>>(scalar_.get(), g_.get(), restart_, scale_.get(), state_.get());
 		LaunchCheck("CycleInitKernel");
 		H_.Zero(stream_);
+		if (profiler_) profiler_->End(stream_);
 		launches_ += 1;
 		const int cap = std::min(restart_, max_iterations-result.iterations);
 		for (int j = 0; j < cap;) {
@@ -599,10 +610,6 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 			for (int b = 0; b < batch; ++b) {
 				if (krylov_values) Step(pattern, krylov_values, j+b);
 				else Step(pattern, values, j+b);
-				ArnoldiFinalizeKernel<<<1, kThreads, finalize_smem_, stream_>>>(norm_partial_.get(), update_blocks_, H_.get(), restart_, j+b,
-					cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance);
-				LaunchCheck("ArnoldiFinalizeKernel");
-				launches_ += 1;
 			}
 			j += batch;
 			state_.Download(&host_->stop, 3, stream_);
@@ -617,12 +624,14 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, 8));
 		}
 		result.residual = host_->residual;
+		if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
 		BackSolveKernel<<<1, 256, (size_t)(restart_+1)*sizeof(double), stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(),
 			state_.get()+2);
 		LaunchCheck("BackSolveKernel");
 		SolutionUpdateKernel<<<blocks_, kThreads, coef_smem, stream_>>>(V_.get(), n_, scale_.get(), y_.get(),
 			state_.get(), x);
 		LaunchCheck("SolutionUpdateKernel");
+		if (profiler_) profiler_->End(stream_);
 		launches_ += 2;
 		beta = TrueResidual(pattern, values, rhs, x);
 		state_.Download(&host_->stop, 3, stream_);

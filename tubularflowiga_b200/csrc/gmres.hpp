@@ -67,6 +67,8 @@ public:
 private:
 	template <class T>
 	void Step(const DevicePatternView& pattern, const T* values, int j);
+	// Both classical Gram-Schmidt passes of Arnoldi step j, then its Givens finalisation against
+	// tolerance_ (one profiling interval of family kOrtho).
 	template <class B> void Orthogonalize(int j, B* basis);
 	// Krylov basis storage: FP64 (V_) or FP32 (V32_, allocated on first use).
 	template <class B> B* Basis();
@@ -98,6 +100,7 @@ private:
 	struct HostStatus { int stop, used, error, pad; double residual; double beta[2]; unsigned singular; };
 	HostStatus* host_ = nullptr;
 	Profiler* profiler_ = nullptr;
+	double tolerance_ = 0.0;                 // absolute residual target of the current solve
 	LearnedPreconditioner* learned_ = nullptr;
 	LearnedPreconditioner* collector_ = nullptr;
 	DeviceArray<double> pair_dinv_, pair_amg_, pair_aamg_;

@@ -206,7 +206,9 @@ void NsSolver::CommitStep()
 
 void NsSolver::AssembleResidualTc()
 {
+	profiler_.Begin(Profiler::kVector, stream_);
 	rhs_.Zero(stream_);
+	profiler_.End(stream_);
 	profiler_.Begin(Profiler::kResidual, stream_);
 	const bool coefficients = tangent_kernel_ == TFIGA_TANGENT_COEFFICIENTS;
 	LaunchTangentPoint(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
@@ -214,7 +216,9 @@ void NsSolver::AssembleResidualTc()
 		coefficients ? nullptr : point_state_.get(), rhs_.get(), stream_);
 	LargeElements<float>(nullptr, rhs_.get());
 	profiler_.End(stream_);
+	profiler_.Begin(Profiler::kVector, stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
+	profiler_.End(stream_);
 	launches_ += 2;
 }
 
@@ -313,13 +317,17 @@ void NsSolver::AssembleResidual()
 		AssembleResidualTc();
 		return;
 	}
+	profiler_.Begin(Profiler::kVector, stream_);
 	rhs_.Zero(stream_);
+	profiler_.End(stream_);
 	profiler_.Begin(Profiler::kResidual, stream_);
 	LaunchTangentPoint(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
 		{params_.density, params_.viscosity, params_.dt}, nullptr, nullptr, rhs_.get(), stream_);
 	LargeElements<double>(nullptr, rhs_.get());
 	profiler_.End(stream_);
+	profiler_.Begin(Profiler::kVector, stream_);
 	LaunchAxpy(n4_, 1.0, traction_.get(), rhs_.get(), stream_);
+	profiler_.End(stream_);
 	launches_ += 2;
 }
 
@@ -330,17 +338,17 @@ void NsSolver::AssembleTangent()
 		return;
 	}
 	amg_current_ = false;
-	values_.Zero(stream_);
 	profiler_.Begin(Profiler::kAssembly, stream_);
+	values_.Zero(stream_);
 	LaunchAssemble(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), mesh_.element_blocks(), state_.get(),
 		previous_.get(), {params_.density, params_.viscosity, params_.dt}, values_.get(), nullptr, stream_);
 	LargeElements<double>(values_.get(), nullptr);
-	profiler_.End(stream_);
-	launches_ += 1;
 	if (mixed()) {
 		LaunchToFloat((long long)blocks()*16, values_.get(), values32_.get(), stream_);
 		launches_ += 1;
 	}
+	profiler_.End(stream_);
+	launches_ += 1;
 	if (amg_ && !amg_->built()) {
 		if (mixed()) amg_->Build(values32_.get());
 		else amg_->Build(values_.get());
@@ -416,7 +424,9 @@ void NsSolver::ApplyDirichletParts(bool matrix, bool rhs)
 
 GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 {
+	profiler_.Begin(Profiler::kVector, stream_);
 	update_.Zero(stream_);
+	profiler_.End(stream_);
 	struct Count { long long& n; ~Count() { ++n; } } count{solves_};
 	if (amg_) {
 		const long long before = amg_->launches();
@@ -432,6 +442,7 @@ GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 		// tangent keeps them); the dense coarse inverse every amg_coarse_period-th refresh
 		if (!amg_current_) {
 			const bool coarse = refreshes_ % params_.amg_coarse_period == 0;
+			profiler_.Begin(Profiler::kSetup, stream_);
 			if (mixed()) {
 				if (!amg_->built()) amg_->Build(values32_.get());
 				amg_->Refresh(values32_.get(), coarse);
@@ -439,6 +450,7 @@ GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 				if (!amg_->built()) amg_->Build(values_.get());
 				amg_->Refresh(values_.get(), coarse);
 			}
+			profiler_.End(stream_);
 			++refreshes_;
 			amg_current_ = true;
 		}
@@ -503,8 +515,13 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	const bool tc = tensor_tangent();
 	CudaCheck(cudaEventRecord(events_[0], stream_), "event");
 	const bool outlets = outlet_count_ >= 0;
-	if (outlets) CoupleOutletsOnDevice();
+	if (outlets) {
+		profiler_.Begin(Profiler::kVector, stream_);
+		CoupleOutletsOnDevice();
+		profiler_.End(stream_);
+	}
 	AssembleResidual();
+	profiler_.Begin(Profiler::kVector, stream_);
 	LaunchDiagnostics(!outlets);
 	ApplyDirichletRhs();
 	LaunchNorm(n4_, rhs_.get(), partial_.get(), scalars_.get()+kNorm, stream_);
@@ -514,6 +531,7 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 		segment_sq_.Download(pinned_segments_, segments_, stream_);
 		launches_ += 1;
 	}
+	profiler_.End(stream_);
 	CudaCheck(cudaEventRecord(events_[1], stream_), "event");
 	scalars_.Download(pinned_, kSlots, stream_);
 	if (!labels_.empty()) label_flow_.Download(pinned_+kSlots, labels_.size(), stream_);
@@ -560,8 +578,10 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	}
 	if (segments_) {
 		// frozen segments take no update: their rhs rows vanish before the linear solve
+		profiler_.Begin(Profiler::kVector, stream_);
 		segment_done_.Upload(segment_done_host_.data(), segments_, stream_);
 		LaunchZeroFlaggedSegments(segments_, segment_entries_.get(), segment_done_.get(), rhs_.get(), stream_);
+		profiler_.End(stream_);
 		launches_ += 1;
 	}
 	// Tangent reuse: keep the previous iteration's tangent while that iteration contracted the
@@ -572,7 +592,9 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	if (!reuse) {
 		CudaCheck(cudaEventRecord(events_[4], stream_), "event");
 		AssembleTangent();
+		profiler_.Begin(Profiler::kVector, stream_);
 		ApplyDirichletMatrix();
+		profiler_.End(stream_);
 		tangent_valid_ = true;
 		++tangent_contractions_;
 		CudaCheck(cudaEventRecord(events_[5], stream_), "event");
@@ -626,8 +648,10 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 		learned_->AddSolvedPair(pair_dinv_.get(), update_.get(), pair_amg_.get(), rhs_.get(), pair_aamg_.get(), norm);
 		launches_ += 6;
 	}
+	profiler_.Begin(Profiler::kVector, stream_);
 	LaunchNorm(n4_, update_.get(), partial_.get(), scalars_.get()+kUpdateNorm, stream_);
 	LaunchAxpy(n4_, 1.0, update_.get(), state_.get(), stream_);
+	profiler_.End(stream_);
 	launches_ += 3;
 	scalars_.Download(pinned_+kUpdateNorm, 1, stream_);
 	CudaCheck(cudaStreamSynchronize(stream_), "Navier-Stokes update");
