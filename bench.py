@@ -319,14 +319,20 @@ def algorithmic_counts(tube, blocks):
 
 
 # Newton iterations per step and GMRES iterations per Newton iteration of the reference's own solver
-# algorithm on each workload -- exact-tangent Newton to rel.res 1e-8, every linear system to rtol 1e-8 by
-# left block-Jacobi GMRES(200) (iga_cuda.cu:956-1054, Gmres.hpp:69-213), outlets coupled inside the Newton
-# loop -- recorded from a GPU run of this library in that mode:
-#   python bench.py --workload W --precision fp64 --preconditioner block-jacobi --forcing fixed \
-#       --tangent-reuse 0 --restart 200 --newton-rtol 1e-8 --no-fp64-leg --no-cpu-baseline --steps 2 --warmup 1
+# algorithm on each workload -- exact-tangent Newton to rel.res 1e-8 with a fresh tangent every iteration,
+# every linear system to rtol 1e-8 by left block-Jacobi GMRES(200) with the 5000-iteration cap
+# (iga_cuda.cu:956-1054, Gmres.hpp:69-213) -- recorded on the GPU by this library in that mode:
+#   python bench.py --record-reference-counts --workload W --steps 3
 # The CPU arm prices those counts at its own measured element and GMRES-iteration costs.
 REFERENCE_COUNTS = {
-    "c3": {"newton_per_step": 4.0, "gmres_per_newton": 228.0, "recorded": "provisional"},
+    "c3": {"newton_per_step": 6.0, "gmres_per_newton": 3068.3,
+           "recorded": "B200, outlets held at their initial 0 Pa: step 1 converged in 6 Newton iterations with "
+                       "3526, 3696, 2703, 2657, 2657 and 3171 GMRES iterations; the first linear system of step 2 "
+                       "stopped at the 5000-iteration cap (preconditioned residual 2.7e-2 of its start), where the "
+                       "reference command exits with 'Navier-Stokes GMRES failed'.  The arm prices step 1."},
+    "c2-100": {"newton_per_step": 2.0, "gmres_per_newton": 381.0,
+               "recorded": "B200: steps 1-3 converged in 5, 3 and 2 Newton iterations (GMRES 211-287, 294-389, "
+                           "362-400); the arm prices step 3"},
 }
 
 
@@ -397,9 +403,10 @@ class CpuReference:
             "sample": (f"reference element assembly of {self.elements} of {self.mesh.elements} elements "
                        f"({t_el * 1e3:.2f} ms/element wall on {self.threads} threads) and {self.iterations} "
                        f"block-Jacobi GMRES(200) iterations of the CPU restatement on the full "
-                       f"{4 * self.mesh.nodes}-DOF pattern ({t_it * 1e3:.1f} ms/iteration); extrapolated to "
-                       f"a step of {newton:.2f} Newton x (assembly + {gmres:.0f} GMRES iterations), the counts "
-                       f"of the reference's algorithm recorded on the GPU"),
+                       f"{4 * self.mesh.nodes}-DOF pattern ({t_it * 1e3:.1f} ms/iteration: the first Arnoldi "
+                       f"steps of a cycle, cheaper than the cycle's average, so the step time is a lower bound); "
+                       f"extrapolated to a step of {newton:.2f} Newton x (assembly + {gmres:.0f} GMRES "
+                       f"iterations), the counts of the reference's algorithm recorded on the GPU"),
             "sample_s": t_el * self.elements + t_it * self.iterations, "step_s": t_step,
         }
 
@@ -409,6 +416,52 @@ def reference_counts(name):
     if c is None:
         raise SystemExit("no recorded reference-algorithm counts for workload " + name)
     return c["newton_per_step"], c["gmres_per_newton"]
+
+
+def record_reference_counts(args):
+    """Newton and GMRES counts of the reference's solver algorithm on a workload (FP64, block-Jacobi
+    GMRES(200) to rtol 1e-8 with its 5000-iteration cap, Newton to rel.res 1e-8 with the tangent of every
+    iterate, Dirichlet values lifted by the first update), one JSON line per step; stops at the first
+    failure, as the reference command does."""
+    import torch
+    torch.cuda.set_device(0)
+    from tubularflowiga_b200 import api
+    tube, desc, wave = workload(args.workload)
+    mesh = api.Mesh(tube.mesh)
+    vmask, pmask, velocity_at = boundary(tube, wave)
+    dt = step_dt(args.workload)
+    ns = api.NavierStokes(mesh, precision=api.FP64, preconditioner=api.BLOCK_JACOBI, density=RHO, viscosity=MU,
+                          dt=dt, nonlinear_rtol=1e-8, nonlinear_atol=1e-300, mass_rtol=1e-3, gmres_restart=200,
+                          gmres_max_iterations=5000, gmres_rtol=1e-8, newton_forcing=0, tangent_reuse_factor=0.0)
+    ns.set_dirichlet(vmask, pmask, velocity_at(0.0))
+    ns.set_tractions({label: 0.0 for label in getattr(tube, "outlet_labels", (2, 3) if args.workload == "c3"
+                                                       else (2,))})
+    s0 = api.initial_state(vmask, velocity_at(0.0))
+    ns.set_state(s0, s0)
+    for k in range(args.steps):
+        ns.set_dirichlet_values(velocity_at((k + 1) * dt).ravel())
+        ns.commit_step()
+        initial, gmres, status = -1.0, [], "converged"
+        for _ in range(30):
+            try:
+                r = ns.newton_iteration(initial)
+            except api.TfigaError as e:
+                gmres.append(5000)
+                status = "failed: " + str(e)
+                break
+            if initial < 0:
+                initial = r["residual_l2"]
+            if r["converged"]:
+                break
+            gmres.append(r["linear_iterations"])
+        else:
+            status = "no convergence in 30 Newton iterations"
+        print(json.dumps({"workload": args.workload, "step": k + 1, "newton": len(gmres), "gmres": gmres,
+                          "status": status}), flush=True)
+        if status != "converged":
+            break
+    ns.close()
+    return 0
 
 
 def run_reference_arm(args, world, rank):
@@ -681,6 +734,12 @@ def main():
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "mixed", "fp64"])
     ap.add_argument("--no-fp64-leg", action="store_true")
+    ap.add_argument("--learned", type=int, default=0,
+                    help="time the learned FGMRES stage too, trained on pairs from this many further steps")
+    ap.add_argument("--learned-pairs", type=int, default=256, help="pair store of the learned leg")
+    ap.add_argument("--learned-adam", type=int, default=2000, help="Adam steps of the learned leg")
+    ap.add_argument("--record-reference-counts", action="store_true",
+                    help="print the Newton and GMRES counts of the reference's solver algorithm on the workload")
     ap.add_argument("--outlet-coupling", default="newton", choices=["newton", "outer"])
     ap.add_argument("--krylov-fp64-basis", action="store_true")
     ap.add_argument("--restart", type=int, default=64, help="FGMRES restart length")
@@ -709,6 +768,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, world, rank)
+    if args.record_reference_counts:
+        return record_reference_counts(args)
     if args.workload == "transport":
         return run_transport(args, world, rank, local)
 
@@ -843,6 +904,54 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
+
+    # learned leg (--learned N): the learned FGMRES stage in the timed path.  Training pairs from N further
+    # untimed steps after the timed ones (flexible-GMRES pairs w = A z and Newton pairs), the residual loss
+    # through the bound Jacobian, --learned-adam Adam steps, the fitted output gain; then the timed steps
+    # again from the same starting state with the stage attached, between CUDA events.
+    learned_leg = None
+    if args.learned > 0 and amg and not batched:
+        net = api.Learned(ns, layers=3, seed=0, linear=False)
+        net.set_capacity(args.learned_pairs)
+        net.set_loss(False)
+        net.attach(use=False, collect=True)
+        t_train = time.perf_counter()
+        for k in range(args.learned):
+            ns.set_dirichlet_values(bc(total + k))
+            ns.commit_step()
+            outlet_step(ns, outlets, args.outlet_coupling) if outlets else ns.step()
+        net.fit_scales()
+        loss0 = net.evaluate()
+        net.train(args.learned_adam, 1e-3)
+        loss1 = net.evaluate()
+        gain = net.fit_gain()
+        train_s = time.perf_counter() - t_train
+        restart()
+        net.attach(use=True, collect=False)
+        learned_reports = []
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        l0.record(stream)
+        for k in range(args.warmup, total):
+            do_step(ns, outlets, k, record=learned_reports)
+        l1.record(stream)
+        torch.cuda.synchronize()
+        learned_ms = l0.elapsed_time(l1)
+        fallbacks = net.fallbacks()
+        net.detach()
+        net.close()
+        newton_l = sum(r["newton_iterations"] for r in learned_reports)
+        learned_leg = {"value": replica_throughput(world, args.steps, learned_ms), "unit": "time steps/s",
+                       "ms_per_step": learned_ms / args.steps, "newton_per_step": newton_l / args.steps,
+                       "linear_iterations_per_newton": sum(r["linear_iterations"] for r in learned_reports)
+                       / max(1, newton_l),
+                       "linear_iterations_per_step": [r["linear_iterations"] for r in learned_reports],
+                       "amg_only_linear_iterations_per_step": [r["linear_iterations"] for r in timed_reports],
+                       "fallbacks": fallbacks,
+                       "training": {"steps": args.learned, "pairs": args.learned_pairs, "adam_steps": args.learned_adam,
+                                    "loss": [loss0, loss1], "output_gain": gain, "seconds": train_s},
+                       "note": "same timed steps and starting state as the mixed arm, AMG + learned stage "
+                               "(3-layer message passing, width 64, BF16 weights) in the flexible GMRES"}
 
     tube_metrics = None
     amg_levels = ns.amg_info() if amg else None
@@ -1081,6 +1190,9 @@ def main():
         line["mixed_over_fp64"] = {m: steps_per_s / v["value"] for m, v in fp64_leg["variants"].items()}
     if tangent_info is not None:
         line["tangent_kernel"] = tangent_info
+    if learned_leg is not None:
+        learned_leg["over_mixed"] = learned_leg["value"] / steps_per_s
+        line["learned"] = learned_leg
     if batched:
         line["tubes"] = tube_metrics
     if not args.no_cpu_baseline and world == 1:
