@@ -225,10 +225,10 @@ def womersley_errors(drive, steps=200, dt=1e-3, check_every=50):
 def test_womersley_traction_driven_at_low_reynolds():
     errors = womersley_errors("traction")
     print("womersley (traction, Re 1) volume relative L2 at t = 0.05 .. 0.20 s:", errors)
-    assert max(errors) < 5e-2        # the reference's Womersley gate
+    assert max(errors) < 2e-2        # measured 6.1e-3 .. 9.5e-3; the reference's own gate is 5e-2
 
 
 def test_c2_pulsatile_inflow_is_womersley():
     errors = womersley_errors("inflow")
     print("womersley (C2 inflow, Re 136) volume relative L2 at t = 0.05 .. 0.20 s:", errors)
-    assert max(errors) < 5e-2        # the reference's Womersley gate
+    assert max(errors) < 1e-2        # measured 3.6e-3 .. 3.7e-3; the reference's own gate is 5e-2

@@ -152,14 +152,18 @@ def test_learned_stage_training_and_iterations(cylinder_1280):
 
 
 @pytest.mark.gpu
-def test_learned_stage_lowers_fgmres_iterations_on_held_out_steps():
+def test_learned_stage_on_held_out_steps():
     """The 12,800-element pulsatile section (C2's cross-section and inflow, 100 layers) with the split-BF16
     solver: training pairs from 40 steps (a 1,024-pair store of flexible-GMRES pairs w = A z and Newton
     pairs), the residual loss through the bound Jacobian, 3,000 Adam steps and the fitted output gain; then
     five held-out steps, from the same state and with the same Dirichlet sequence, with and without the
-    stage.  Asserted: the stage takes fewer FGMRES iterations in total than the AMG alone, on every step
-    at most as many, with no solve falling back to the AMG alone.  The gain is small (measured 876 -> 860
-    ... 831 -> 813 iterations per step, about 2%)."""
+    stage.  Asserted: training lowers the loss, the output gain is finite and non-negative, and every
+    held-out step converges with the stage and without a fallback to the AMG alone.  The iteration counts
+    are reported, not asserted: the stage does not give a reliable gain.  Two runs of this protocol on a
+    B200 gave 860, 841, 827, 815, 813 FGMRES iterations per step with the stage against 876, 855, 845,
+    831, 831 without (2% fewer), and 1640, 1986, 2058, 2002, 2063 against 876, 858, 844, 831, 831 (2.3
+    times more); the training is not deterministic (FP32 atomics in the gradient) and the fitted gain
+    (0.068, 0.026) is small either way."""
     import bench
     from tubularflowiga_b200 import api
     tube, _, wave = bench.workload("c2-100")
@@ -203,7 +207,5 @@ def test_learned_stage_lowers_fgmres_iterations_on_held_out_steps():
     print(f"held-out FGMRES iterations per step: AMG {counts[False]}, AMG + learned stage {counts[True]} "
           f"(residual loss {before:.3e} -> {after:.3e}, gain {gain:.3f}, fallbacks {net.fallbacks()})")
     assert net.fallbacks() == 0
-    assert sum(counts[True]) < sum(counts[False])
-    assert all(a <= b for a, b in zip(counts[True], counts[False]))
     net.detach()
     ns.close()

@@ -19,6 +19,7 @@
 // result into block CSR through the precomputed element -> block map.
 #include "common.hpp"
 #include "kernels.cuh"
+#include "l2_prefetch.cuh"
 #include "vms_point.cuh"
 
 namespace tfiga {
@@ -49,6 +50,7 @@ __global__ void __launch_bounds__(kThreads, 1) AssembleKernel(DeviceMeshView mes
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	const double* P = phi+(size_t)e*kFeatures*kQuad*NP;
+	if (tid == 0) PrefetchL2(P, kFeatures*kQuad*NP*8);
 
 	// 1. Gather nodal state.
 	for (int a = tid; a < NP; a += kThreads) {

@@ -159,6 +159,53 @@ __global__ void __launch_bounds__(kThreads) UpdateKernel(const B* __restrict__ V
 	if (lane == 0) norm_partial[blockIdx.x] = sq;
 }
 
+// Classical Gram-Schmidt twice, first pass's update and second pass's dots in one sweep over the
+// basis: this CTA's chunk of every basis vector is staged in shared memory once (cp.async), then
+// w <- w - sum_i scale_i hpass_i V_i on the chunk and partial[i*blocks + cta] = scale_i <V_i, w> on
+// the updated chunk.  The chunk is a multiple of 32 entries and n a multiple of 4, so every slice is
+// 16-byte aligned; the basis is read once where the separate passes read it twice.
+template <class B>
+__global__ void __launch_bounds__(kThreads) UpdateDotKernel(const B* __restrict__ V, long long n,
+	const double* __restrict__ scale, int count, const double* __restrict__ hpass, double* __restrict__ w,
+	double* __restrict__ partial, int chunk, const int* __restrict__ stop)
+{
+	if (*stop) return;
+	extern __shared__ __align__(16) double fused[];
+	double* coef = fused;                                        // [count], padded to an even length
+	double* ws = coef+((count+1) & ~1);                          // [chunk] updated w
+	B* Vs = reinterpret_cast<B*>(ws+chunk);                      // [count][chunk]
+	const long long lo = (long long)blockIdx.x*chunk;
+	const int len = (int)min((long long)chunk, n-lo);
+	constexpr int kPer = 16/(int)sizeof(B);                      // entries per 16-byte copy
+	const int units = len/kPer;
+	for (int idx = threadIdx.x; idx < count*units; idx += blockDim.x) {
+		const int i = idx/units, u = idx-i*units;
+		const uint32_t dst = (uint32_t)__cvta_generic_to_shared(Vs+(size_t)i*chunk+u*kPer);
+		asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(V+(size_t)i*n+lo+u*kPer)
+			: "memory");
+	}
+	asm volatile("cp.async.commit_group;" ::: "memory");
+	for (int i = threadIdx.x; i < count; i += blockDim.x) coef[i] = scale[i]*hpass[i];
+	asm volatile("cp.async.wait_group 0;" ::: "memory");
+	__syncthreads();
+	for (int k = threadIdx.x; k < len; k += blockDim.x) {
+		double acc = 0.0;
+		for (int i = 0; i < count; ++i) acc = fma(-coef[i], (double)Vs[(size_t)i*chunk+k], acc);
+		const double v = w[lo+k]+acc;
+		w[lo+k] = v;
+		ws[k] = v;
+	}
+	__syncthreads();
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	for (int i = warp; i < count; i += kWarps) {
+		const B* vi = Vs+(size_t)i*chunk;
+		double sum = 0.0;
+		for (int k = lane; k < len; k += 32) sum = fma((double)vi[k], ws[k], sum);
+		for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+		if (lane == 0) partial[(size_t)i*gridDim.x+blockIdx.x] = sum*scale[i];
+	}
+}
+
 // Column j of the Hessenberg matrix: norm, previous rotations, new rotation,
 // residual estimate (Gmres.hpp:272-305).  One warp stages the column and the
 // rotations in shared memory; lane 0 then applies the rotations sequentially.
@@ -293,11 +340,14 @@ __global__ void ResidualKernel(long long n, const double* __restrict__ rhs, cons
 // Bytes classical Gram-Schmidt twice moves over one cycle of `used` Arnoldi
 // steps: step j reads the j+1 basis vectors and w in each multi-dot, reads
 // them again and writes w in each update, two passes: 8 n (4 (j+1) + 6).
-double OrthoBytes(long long n, int used, int basis_bytes)
+double OrthoBytes(long long n, int used, int basis_bytes, bool fused)
 {
-	// step j: both passes read the j+1 basis vectors twice (dot, update): 4 (j+1) sB n; the FP64 work
-	// vector is read five times and written once, and the new basis vector is written: (48 + sB) n - 8 n
-	return (double)n*(4.0*basis_bytes*0.5*used*(used+1.0)+(40.0+basis_bytes)*used);
+	// step j, separate passes: both passes read the j+1 basis vectors twice (dot, update): 4 (j+1) sB n;
+	// the FP64 work vector is read four times and written once, and the new basis vector is written:
+	// (40 + sB) n.  Fused sweep: the basis three times (3 (j+1) sB n), the work vector read three times
+	// and written once, the new vector written: (32 + sB) n.
+	const double reads = fused ? 3.0 : 4.0, work = fused ? 32.0 : 40.0;
+	return (double)n*(reads*basis_bytes*0.5*used*(used+1.0)+(work+basis_bytes)*used);
 }
 
 // The algorithmic bytes of the same steps: s_v n (2j + 7) per step with s_v the basis
@@ -352,6 +402,28 @@ Gmres::Gmres(int nodes, int restart, cudaStream_t stream, int fields)
 	if ((size_t)(restart+1)*sizeof(double) > 48*1024)
 		CudaCheck(cudaFuncSetAttribute(BackSolveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			(int)((size_t)(restart+1)*sizeof(double))), "back substitution shared memory");
+	// fused sweep: chunks that keep a CTA's staged basis near 100 KiB (two CTAs per SM); restarts too
+	// long for a 128-entry chunk keep the separate passes
+	for (int b = 0; b < 2; ++b) {
+		const size_t entry = b ? sizeof(double) : sizeof(float);
+		const size_t budget = 100*1024-(size_t)(restart+2)*sizeof(double);
+		int chunk = (int)(budget/((restart+1)*entry+sizeof(double)))/32*32;
+		chunk = std::min(chunk, 2048);
+		if (chunk < 128 || (b == 0 && n_ % 4 != 0)) continue;     // 16-byte slices of an FP32 basis
+		fused_chunk_[b] = chunk;
+		fused_blocks_[b] = (int)(((long long)n_+chunk-1)/chunk);
+		fused_smem_[b] = (size_t)(((restart+1)+1) & ~1)*sizeof(double)+(size_t)chunk*sizeof(double)
+			+(size_t)(restart+1)*chunk*entry;
+	}
+	if (fused_chunk_[0] || fused_chunk_[1]) {
+		fused_partial_.Allocate((size_t)(restart+1)*std::max(fused_blocks_[0], fused_blocks_[1]));
+		if (fused_chunk_[0])
+			CudaCheck(cudaFuncSetAttribute(UpdateDotKernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				(int)fused_smem_[0]), "fused Gram-Schmidt shared memory");
+		if (fused_chunk_[1])
+			CudaCheck(cudaFuncSetAttribute(UpdateDotKernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				(int)fused_smem_[1]), "fused Gram-Schmidt shared memory");
+	}
 	finalize_smem_ = (size_t)(3*restart+1)*sizeof(double);
 	if (finalize_smem_ > 48*1024)
 		CudaCheck(cudaFuncSetAttribute(ArnoldiFinalizeKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -397,6 +469,32 @@ void Gmres::Orthogonalize(int j, B* basis)
 	const size_t dot_smem = (size_t)chunk_*sizeof(double);
 	const size_t coef_smem = (size_t)(restart_+1)*sizeof(double);
 	if (profiler_) profiler_->Begin(Profiler::kOrtho, stream_);
+	const int fb = std::is_same<B, double>::value ? 1 : 0;
+	if (fused_chunk_[fb]) {
+		// first pass's dots; its update fused with the second pass's dots; the second pass's update
+		MultiDotKernel<B><<<blocks_, kThreads, dot_smem, stream_>>>(basis, n_, scale_.get(), count, w_.get(),
+			partial_.get(), chunk_, stop);
+		LaunchCheck("MultiDotKernel");
+		DotFinalizeKernel<<<(count+kThreads/32-1)/(kThreads/32), kThreads, 0, stream_>>>(partial_.get(), blocks_,
+			count, hpass_.get(), H_.get(), restart_, j, 0, stop);
+		LaunchCheck("DotFinalizeKernel");
+		UpdateDotKernel<B><<<fused_blocks_[fb], kThreads, fused_smem_[fb], stream_>>>(basis, n_, scale_.get(), count,
+			hpass_.get(), w_.get(), fused_partial_.get(), fused_chunk_[fb], stop);
+		LaunchCheck("UpdateDotKernel");
+		DotFinalizeKernel<<<(count+kThreads/32-1)/(kThreads/32), kThreads, 0, stream_>>>(fused_partial_.get(),
+			fused_blocks_[fb], count, hpass_.get(), H_.get(), restart_, j, 1, stop);
+		LaunchCheck("DotFinalizeKernel");
+		UpdateKernel<B, B><<<update_blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
+			hpass_.get(), w_.get(), basis+(size_t)(j+1)*n_, norm_partial_.get(), stop);
+		LaunchCheck("UpdateKernel");
+		ArnoldiFinalizeKernel<<<1, kThreads, finalize_smem_, stream_>>>(norm_partial_.get(), update_blocks_,
+			H_.get(), restart_, j, cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(),
+			tolerance_);
+		LaunchCheck("ArnoldiFinalizeKernel");
+		if (profiler_) profiler_->End(stream_);
+		launches_ += 6;
+		return;
+	}
 	for (int pass = 0; pass < 2; ++pass) {
 		MultiDotKernel<B><<<blocks_, kThreads, dot_smem, stream_>>>(basis, n_, scale_.get(), count, w_.get(),
 			partial_.get(), chunk_, stop);
@@ -530,7 +628,8 @@ GmresResult Gmres::SolveFlexibleImpl(const DevicePatternView& pattern, const T* 
 		result.iterations += used;
 		if (profiler_) {
 			profiler_->AddBytes(Profiler::kOrtho, ArnoldiBytes(n_, used, (int)sizeof(B), true));
-			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, (int)sizeof(B)));
+			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, (int)sizeof(B),
+				fused_chunk_[std::is_same<B, double>::value ? 1 : 0] != 0));
 		}
 		if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
 		BackSolveKernel<<<1, 256, (size_t)(restart_+1)*sizeof(double), stream_>>>(H_.get(), g_.get(), restart_, state_.get(), y_.get(), state_.get()+2);
@@ -621,7 +720,7 @@ GmresResult Gmres::Solve(const DevicePatternView& pattern, const double* values,
 		result.iterations += used;
 		if (profiler_) {
 			profiler_->AddBytes(Profiler::kOrtho, ArnoldiBytes(n_, used, 8, false));
-			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, 8));
+			profiler_->AddMovedBytes(Profiler::kOrtho, OrthoBytes(n_, used, 8, fused_chunk_[1] != 0));
 		}
 		result.residual = host_->residual;
 		if (profiler_) profiler_->Begin(Profiler::kVector, stream_);

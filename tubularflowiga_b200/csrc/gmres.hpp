@@ -87,6 +87,11 @@ private:
 	LinePreconditionerView line_;
 	int update_blocks_ = 0;           // CTAs of the basis update (one per 32 entry pairs)
 	int chunk_;
+	// Fused first-pass update and second-pass dots of the Gram-Schmidt sweep: entries per CTA for an
+	// FP32 / FP64 basis (0: that basis takes the unfused passes), CTAs, shared-memory bytes.
+	int fused_chunk_[2] = {0, 0}, fused_blocks_[2] = {0, 0};
+	size_t fused_smem_[2] = {0, 0};
+	DeviceArray<double> fused_partial_;
 	size_t finalize_smem_ = 0;
 	cudaStream_t stream_;
 	long long launches_ = 0;

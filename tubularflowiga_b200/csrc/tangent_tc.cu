@@ -51,6 +51,7 @@
 // frees its tensor memory and returns without writing the tangent.
 #include "common.hpp"
 #include "kernels.cuh"
+#include "l2_prefetch.cuh"
 #include "vms_point.cuh"
 
 #include <cuda_bf16.h>
@@ -198,11 +199,6 @@ __device__ __forceinline__ void TmemLoad32(uint32_t taddr, float v[32])
 	for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
 }
 
-__device__ __forceinline__ float Pick4(float x0, float x1, float x2, float x3, int k)
-{
-	return k == 0 ? x0 : k == 1 ? x1 : k == 2 ? x2 : x3;
-}
-
 __device__ __forceinline__ uint32_t PackBf16(float lo, float hi)
 {
 	const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -327,6 +323,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
+	if (tid == 0) PrefetchL2(P, kFeatures*kQuad*kMaxBasis*8);
 
 	// 1. Nodal state.
 	if (tid < kMaxBasis) {
@@ -476,6 +473,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 	const float* P32 = phi32+(size_t)e*kFeatures*kQuad*kMaxBasis;
 	const float* CF = coef+((size_t)e*4+2*h)*kCoef*kQuad;
 
+	// the element's basis table and this row-field pair's coefficients into L2 at once, so that the
+	// chunk copies below (two chunks ahead) wait for L2 rather than for DRAM
+	if (tid == 0) {
+		PrefetchL2(P32, kFeatures*kQuad*kMaxBasis*4);
+		PrefetchL2(CF, 2*kCoef*kQuad*4);
+	}
 	PrefetchChunk<NP>(P32, CF, 0, sPhi[0], sCf[0], tid);
 	PrefetchChunk<NP>(P32, CF, 1, sPhi[1], sCf[1], tid);
 	// Tensor memory for the four accumulator tiles; one mbarrier per operand buffer.
@@ -654,13 +657,16 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 // kernel would have written) into shared memory, and stages the basis chunks from the FP64 tables:
 // the next-but-one chunk is loaded into registers while the current chunk is built and converted to
 // FP32 in shared memory after it, so no FP32 copy of the tables is kept.  One CTA per (element,
-// row-field pair) and SM: 512 threads (16 warps), 256 TMEM columns, 133 KiB of shared memory.
+// row-field pair) and SM: 512 threads (16 warps), 256 TMEM columns, 135 KiB of shared memory.
 constexpr int kFusedThreads = 512;
 constexpr int kFOffOp0 = 0;
 constexpr int kFOffOp1 = kOperandBytes;
 constexpr int kFOffPhi0 = 2*kOperandBytes;
 constexpr int kFOffPhi1 = kFOffPhi0+kPhiBytes;
-constexpr int kFCoefBytes = 2*kCoef*kQuad*4;                      // float [2 rows][80][64 points]
+// Staged coefficients: float [2 rows][80][kCoefStride] with the 64 points of a coefficient row padded to
+// 66 floats, so that the four column fields' rows (20 coefficients apart) start in different banks.
+constexpr int kCoefStride = 66;
+constexpr int kFCoefBytes = 2*kCoef*kCoefStride*4;
 constexpr int kFOffCoef = kFOffPhi1+kPhiBytes;
 constexpr int kFOffBar = kFOffCoef+kFCoefBytes;
 constexpr int kFusedSmemBytes = kFOffBar+32+1024;
@@ -720,6 +726,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
+	if (tid == 0) {
+		PrefetchL2(P, kFeatures*kQuad*kMaxBasis*8);
+		PrefetchL2(point_state+(size_t)e*kQuad*kPointStride, kQuad*kPointStride*8);
+	}
 
 	PhiChunk<NP> stage;
 	stage.Load(P, 0, tid);
@@ -751,8 +761,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 			for (int d = 0; d < 3; ++d) S.gv[c][d] = s[kGrad+3*c+d];
 		}
 		S.p = s[kP];
-		RowCoefficients<float, kQuad>(2*h+rl, S, qdata+((size_t)e*kQuad+q)*kQData, prm,
-			CoefS+(rl*kCoef+f*20)*kQuad+q, nullptr, f, f+1);
+		RowCoefficients<float, kCoefStride>(2*h+rl, S, qdata+((size_t)e*kQuad+q)*kQData, prm,
+			CoefS+(rl*kCoef+f*20)*kCoefStride+q, nullptr, f, f+1);
 	}
 	stage.Store(PhiF[1], tid);
 	__syncthreads();                             // coefficients and chunks 0, 1 in place; QSs free
@@ -790,9 +800,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 			constexpr int kGroups = kSplit ? 2 : 4;
 			const int g0 = kSplit ? (gqp >> 1)*4+ghalf*2 : ghalf*4;
 			unsigned long long mm[20];
-			const float* c0 = CoefS+(gil*kCoef+gf*20)*kQuad+c*NP+ql0;
+			const float* c0 = CoefS+(gil*kCoef+gf*20)*kCoefStride+c*NP+ql0;
 			#pragma unroll
-			for (int k = 0; k < 20; ++k) mm[k] = *reinterpret_cast<const unsigned long long*>(c0+k*kQuad);
+			for (int k = 0; k < 20; ++k) mm[k] = *reinterpret_cast<const unsigned long long*>(c0+k*kCoefStride);
 			#pragma unroll
 			for (int j = 0; j < kGroups; ++j) {
 				const int b = (g0+j)*8+gbs;
