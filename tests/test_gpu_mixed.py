@@ -7,8 +7,11 @@ FP32 accumulation and stored in FP32; the residual stays FP64.  Tolerances:
   oracle -- BF16 keeps 8 significant bits (unit roundoff 2^-9 ~ 2e-3 per
   operand), and the blocks whose terms cancel lose a few bits more;
 * Newton: the mixed Newton iteration converges to the FP64 solution; after
-  convergence to 1e-10 of the initial residual the velocity agrees to 1e-8
-  and the pressure to 1e-6 relative L2 with the FP64 path.
+  convergence to 1e-10 of the initial residual velocity and pressure agree to
+  1e-8 relative L2 with the FP64 path (the north star's bar; measured about
+  2e-13 on the cylinder), and over several transient steps of the pulsatile
+  section with the bench's solver settings every step stays within 1e-8
+  (measured 3e-11 .. 7e-11).
 Split-BF16 mode (TFIGA_PRECISION_MIXED_BF16X3, operands hi + lo, three
 products): Jacobian within 1e-4 relative per field pair -- about 2^-16 per
 product plus FP32 accumulation and the FP32 coefficients -- and Newton takes
@@ -136,7 +139,7 @@ def test_split_newton_matches_fp64_iterations(api, cylinder_1280):
     assert reports["split"]["converged"]
     assert reports["split"]["newton_iterations"] <= reports["fp64"]["newton_iterations"]
     assert rel(states["split"][:, :3], states["fp64"][:, :3]) < 1e-8
-    assert rel(states["split"][:, 3], states["fp64"][:, 3]) < 1e-6
+    assert rel(states["split"][:, 3], states["fp64"][:, 3]) < 1e-8
 
 
 def test_tensor_tangent_is_repeatable_in_norm(api, small_tube):
@@ -170,4 +173,39 @@ def test_mixed_newton_converges_to_fp64_solution(api, cylinder_1280):
     assert reports["mixed"]["converged"] and reports["fp64"]["converged"]
     assert reports["mixed"]["newton_iterations"] <= reports["fp64"]["newton_iterations"] + 4
     assert rel(states["mixed"][:, :3], states["fp64"][:, :3]) < 1e-8
-    assert rel(states["mixed"][:, 3], states["fp64"][:, 3]) < 1e-6
+    assert rel(states["mixed"][:, 3], states["fp64"][:, 3]) < 1e-8
+
+
+def test_split_transient_steps_match_fp64_on_the_pulsatile_section(api):
+    """The 12,800-element section of the pulsatile tube (C2's cross-section and Fourier inflow, 100 layers),
+    four backward-Euler steps at dt 2e-3 with the bench's solver settings (Newton rel.res 1e-10 on the FP64
+    residual, Eisenstat-Walker linear tolerances, tangent reuse factor 100, AMG-FGMRES(64)): the split-BF16
+    mixed solver and the FP64 solver from the same state with the same Dirichlet sequence agree within
+    1e-8 relative L2 on velocity and on pressure after every step."""
+    import bench
+    tube, _, wave = bench.workload("c2-100")
+    mesh = api.Mesh(tube.mesh)
+    vmask, pmask, velocity_at = bench.boundary(tube, wave)
+    dt = 2e-3
+    s0 = api.initial_state(vmask, velocity_at(0.0))
+    trajectories = {}
+    for name, precision in (("fp64", api.FP64), ("split", api.MIXED_BF16X3)):
+        ns = api.NavierStokes(mesh, precision=precision, density=1060.0, viscosity=3.5e-3, dt=dt,
+                              nonlinear_rtol=1e-10, nonlinear_atol=1e-300, mass_rtol=1e-3, gmres_restart=64,
+                              gmres_max_iterations=5000, gmres_rtol=1e-8, preconditioner=api.AMG,
+                              amg_coarse_period=3, newton_forcing=1, tangent_reuse_factor=100.0)
+        ns.set_dirichlet(vmask, pmask, velocity_at(0.0))
+        ns.set_tractions({2: 0.0})
+        ns.set_state(s0, s0)
+        states = []
+        for k in range(4):
+            ns.set_dirichlet_values(velocity_at((k + 1) * dt).ravel())
+            ns.commit_step()
+            assert ns.step()["converged"]
+            states.append(ns.get_state().reshape(-1, 4))
+        ns.close()
+        trajectories[name] = states
+    for k, (a, b) in enumerate(zip(trajectories["split"], trajectories["fp64"])):
+        ev, ep = rel(a[:, :3], b[:, :3]), rel(a[:, 3], b[:, 3])
+        print(f"step {k + 1}: split vs FP64 velocity {ev:.3e} pressure {ep:.3e}")
+        assert ev < 1e-8 and ep < 1e-8

@@ -86,9 +86,10 @@ void LaunchAssembleLarge(const DeviceMeshView& mesh, int first, int count, const
 // operands, FP32 accumulation, ADDED into the FP32 values; status bit 1 set if
 // an MMA completion wait expired.
 // point_state (elements x 64 x 22 doubles, may be null): the point state for LaunchTangentTcFused
-// instead of the coefficients (coef and point_state are not both given).
+// instead of the coefficients (coef and point_state are not both given).  queue: one device int, the
+// persistent CTAs' element counter (zeroed here on the stream before the launch).
 void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const double* qdata, const double* state,
-	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs,
+	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs, int* queue,
 	cudaStream_t stream);
 void LaunchTangentTc(const DeviceMeshView& mesh, const float* phi32, const float* coef,
 	const int32_t* element_blocks, float* values, int* status, bool split, cudaStream_t stream);

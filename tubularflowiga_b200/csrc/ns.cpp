@@ -90,6 +90,7 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 		if (tangent_kernel_ == TFIGA_TANGENT_COEFFICIENTS) coef32_.Allocate(regular*4*80*64);
 		else point_state_.Allocate(regular*kQuad*22);
 	}
+	queue_.Allocate(1);                       // work counter of the persistent point kernel
 	if (tensor_tangent()) {
 		status_.Allocate(1);
 		status_.Zero(stream_);
@@ -213,7 +214,7 @@ void NsSolver::AssembleResidualTc()
 	const bool coefficients = tangent_kernel_ == TFIGA_TANGENT_COEFFICIENTS;
 	LaunchTangentPoint(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
 		{params_.density, params_.viscosity, params_.dt}, coefficients ? coef32_.get() : nullptr,
-		coefficients ? nullptr : point_state_.get(), rhs_.get(), stream_);
+		coefficients ? nullptr : point_state_.get(), rhs_.get(), queue_.get(), stream_);
 	LargeElements<float>(nullptr, rhs_.get());
 	profiler_.End(stream_);
 	profiler_.Begin(Profiler::kVector, stream_);
@@ -290,7 +291,7 @@ void NsSolver::AutotuneTangent()
 	// the same state's coefficients; the residual this pass adds goes to the Newton update vector,
 	// which the linear solve clears before use
 	LaunchTangentPoint(view, mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(), prm, coef32_.get(), nullptr,
-		update_.get(), stream_);
+		update_.get(), queue_.get(), stream_);
 	const float* phi32 = mesh_.phi32();
 	values32_.Zero(stream_);
 	CudaCheck(cudaEventRecord(ev[2], stream_), "event");
@@ -322,7 +323,7 @@ void NsSolver::AssembleResidual()
 	profiler_.End(stream_);
 	profiler_.Begin(Profiler::kResidual, stream_);
 	LaunchTangentPoint(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
-		{params_.density, params_.viscosity, params_.dt}, nullptr, nullptr, rhs_.get(), stream_);
+		{params_.density, params_.viscosity, params_.dt}, nullptr, nullptr, rhs_.get(), queue_.get(), stream_);
 	LargeElements<double>(nullptr, rhs_.get());
 	profiler_.End(stream_);
 	profiler_.Begin(Profiler::kVector, stream_);

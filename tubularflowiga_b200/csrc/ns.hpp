@@ -145,7 +145,7 @@ private:
 	int tangent_kernel_ = 0;                 // TFIGA_TANGENT_* in use
 	double tune_ms_[2] = {0.0, 0.0};         // autotuner: coefficient-array and fused tangent times
 	DeviceArray<double> face_flow_, face_pressure_, label_flow_, partial_, scalars_;
-	DeviceArray<int32_t> vmask_, pmask_, constrained_, face_slot_, status_;
+	DeviceArray<int32_t> vmask_, pmask_, constrained_, face_slot_, status_, queue_;
 	std::vector<int32_t> labels_;            // distinct face labels (slot order)
 	std::map<int32_t, int> slot_of_label_;
 	std::vector<int32_t> face_slot_host_;

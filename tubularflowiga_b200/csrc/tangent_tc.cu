@@ -303,11 +303,14 @@ __device__ __forceinline__ void PointCoefficients(const PointState& S, const dou
 // (TangentTcFusedKernel).
 enum : int { kPointResidual = 0, kPointCoefficients = 1, kPointState = 2 };
 
+// Persistent: each CTA takes elements from a work queue (*queue, zeroed by the launcher) one at a time and
+// claims its next element while it works on the current one, prefetching that element's basis table into
+// L2, so that every element's table is in L2 when its CTA starts on it.
 template <int kMode>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ state,
 	const double* __restrict__ previous, AssemblyParams prm, float* __restrict__ coef,
-	double* __restrict__ point_state, double* __restrict__ rhs)
+	double* __restrict__ point_state, double* __restrict__ rhs, int* __restrict__ queue)
 {
 	extern __shared__ uint8_t smem_raw[];
 	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+15) & ~uintptr_t(15));
@@ -317,13 +320,24 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 	float* Scratch = reinterpret_cast<float*>(sm+kPtOffPart);
 	double* QS = reinterpret_cast<double*>(sm+kPtOffQS);
 	double* RC = reinterpret_cast<double*>(sm+kPtOffRC);
+	__shared__ int next;
 
-	const int e = blockIdx.x;
 	const int tid = threadIdx.x;
+	constexpr uint32_t kTableBytes = kFeatures*kQuad*kMaxBasis*8;
+	if (tid == 0) {
+		next = atomicAdd(queue, 1);
+		if (next < mesh.elements) PrefetchL2(phi+(size_t)next*kFeatures*kQuad*kMaxBasis, kTableBytes);
+	}
+	__syncthreads();
+	for (int e = next; e < mesh.elements; e = next) {
+	__syncthreads();                                 // every thread has read next
+	if (tid == 0) {
+		next = atomicAdd(queue, 1);
+		if (next < mesh.elements) PrefetchL2(phi+(size_t)next*kFeatures*kQuad*kMaxBasis, kTableBytes);
+	}
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
-	if (tid == 0) PrefetchL2(P, kFeatures*kQuad*kMaxBasis*8);
 
 	// 1. Nodal state.
 	if (tid < kMaxBasis) {
@@ -447,6 +461,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 		const int il = tid >> 6;
 		const double r = ((red[(0*4+il)*64+a]+red[(1*4+il)*64+a])+red[(2*4+il)*64+a])+red[(3*4+il)*64+a];
 		if (a < nen) atomicAdd(rhs+4*(size_t)mesh.connectivity[begin+a]+il, r);
+	}
+	__syncthreads();                                 // the element's shared memory is free; next is set
 	}
 }
 
@@ -909,10 +925,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 } // namespace
 
 void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const double* qdata, const double* state,
-	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs, cudaStream_t stream)
+	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs, int* queue,
+	cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
 	if (rhs == nullptr) Fail(-1, "tangent point kernel: the residual output is required");
+	if (queue == nullptr) Fail(-1, "tangent point kernel: the work-queue counter is required");
 	if (coef && point_state) Fail(-1, "tangent point kernel: coefficients or point state, not both");
 	static bool configured = false;
 	if (!configured) {
@@ -924,17 +942,25 @@ void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const dou
 			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
 		configured = true;
 	}
-	const unsigned grid = (unsigned)mesh.elements;
+	// two persistent CTAs per SM (the kernel's occupancy), no more than there are elements
+	static int sms = 0;
+	if (sms == 0) {
+		int device = 0;
+		CudaCheck(cudaGetDevice(&device), "device");
+		CudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+	}
+	const unsigned grid = (unsigned)std::min<long long>(mesh.elements, 2LL*sms);
 	const size_t bytes = kPtSmemBytes+16;
+	CudaCheck(cudaMemsetAsync(queue, 0, sizeof(int), stream), "point-kernel work queue");
 	if (coef)
 		TangentPointKernel<kPointCoefficients><<<grid, kTcThreads, bytes, stream>>>(mesh, phi, qdata, state, previous,
-			params, coef, nullptr, rhs);
+			params, coef, nullptr, rhs, queue);
 	else if (point_state)
 		TangentPointKernel<kPointState><<<grid, kTcThreads, bytes, stream>>>(mesh, phi, qdata, state, previous,
-			params, nullptr, point_state, rhs);
+			params, nullptr, point_state, rhs, queue);
 	else
 		TangentPointKernel<kPointResidual><<<grid, kTcThreads, bytes, stream>>>(mesh, phi, qdata, state, previous,
-			params, nullptr, nullptr, rhs);
+			params, nullptr, nullptr, rhs, queue);
 	LaunchCheck("TangentPointKernel");
 }
 
