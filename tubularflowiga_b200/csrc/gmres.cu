@@ -402,14 +402,15 @@ Gmres::Gmres(int nodes, int restart, cudaStream_t stream, int fields)
 	if ((size_t)(restart+1)*sizeof(double) > 48*1024)
 		CudaCheck(cudaFuncSetAttribute(BackSolveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			(int)((size_t)(restart+1)*sizeof(double))), "back substitution shared memory");
-	// fused sweep: chunks that keep a CTA's staged basis near 100 KiB (two CTAs per SM); restarts too
-	// long for a 128-entry chunk keep the separate passes
+	// fused sweep: chunks that keep a CTA's staged basis near 36 KiB (six CTAs per SM, so that loads of
+	// some CTAs overlap the arithmetic of others; at 100 KiB, two CTAs per SM, the sweep was slower than
+	// the separate passes); restarts too long for a 64-entry chunk keep the separate passes
 	for (int b = 0; b < 2; ++b) {
 		const size_t entry = b ? sizeof(double) : sizeof(float);
-		const size_t budget = 100*1024-(size_t)(restart+2)*sizeof(double);
+		const size_t budget = 36*1024-(size_t)(restart+2)*sizeof(double);
 		int chunk = (int)(budget/((restart+1)*entry+sizeof(double)))/32*32;
 		chunk = std::min(chunk, 2048);
-		if (chunk < 128 || (b == 0 && n_ % 4 != 0)) continue;     // 16-byte slices of an FP32 basis
+		if (chunk < 64 || (b == 0 && n_ % 4 != 0)) continue;      // 16-byte slices of an FP32 basis
 		fused_chunk_[b] = chunk;
 		fused_blocks_[b] = (int)(((long long)n_+chunk-1)/chunk);
 		fused_smem_[b] = (size_t)(((restart+1)+1) & ~1)*sizeof(double)+(size_t)chunk*sizeof(double)

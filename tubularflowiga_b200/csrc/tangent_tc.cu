@@ -303,9 +303,10 @@ __device__ __forceinline__ void PointCoefficients(const PointState& S, const dou
 // (TangentTcFusedKernel).
 enum : int { kPointResidual = 0, kPointCoefficients = 1, kPointState = 2 };
 
-// Persistent: each CTA takes elements from a work queue (*queue, zeroed by the launcher) one at a time and
-// claims its next element while it works on the current one, prefetching that element's basis table into
-// L2, so that every element's table is in L2 when its CTA starts on it.
+// Persistent: each CTA takes elements from a work queue (*queue, zeroed by the launcher) one at a time,
+// claiming its next element while it works on the current one, and prefetches the element's basis table
+// into L2 as it starts on it.  (Prefetching the next element's table as well doubled the tables live in
+// L2 and made the kernel 1.6 times slower: 31 against 19 ms on the 199,800-element Y-bifurcation.)
 template <int kMode>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ state,
@@ -324,16 +325,13 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 
 	const int tid = threadIdx.x;
 	constexpr uint32_t kTableBytes = kFeatures*kQuad*kMaxBasis*8;
-	if (tid == 0) {
-		next = atomicAdd(queue, 1);
-		if (next < mesh.elements) PrefetchL2(phi+(size_t)next*kFeatures*kQuad*kMaxBasis, kTableBytes);
-	}
+	if (tid == 0) next = atomicAdd(queue, 1);
 	__syncthreads();
 	for (int e = next; e < mesh.elements; e = next) {
 	__syncthreads();                                 // every thread has read next
 	if (tid == 0) {
 		next = atomicAdd(queue, 1);
-		if (next < mesh.elements) PrefetchL2(phi+(size_t)next*kFeatures*kQuad*kMaxBasis, kTableBytes);
+		PrefetchL2(phi+(size_t)e*kFeatures*kQuad*kMaxBasis, kTableBytes);
 	}
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
@@ -466,10 +464,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 	}
 }
 
+// lookahead: the number of CTAs resident at once (two per SM); CTA k also prefetches the tables of
+// CTA k + lookahead, which starts about when CTA k finishes.
 template <bool kSplit>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView mesh,
 	const float* __restrict__ phi32, const float* __restrict__ coef, const int32_t* __restrict__ element_blocks,
-	float* __restrict__ values, int* __restrict__ status)
+	float* __restrict__ values, int* __restrict__ status, int lookahead)
 {
 	constexpr int NP = kSplit ? 4 : kMaxPts;     // points per K chunk
 	constexpr int kChunks = kQuad/NP;
@@ -490,10 +490,17 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 	const float* CF = coef+((size_t)e*4+2*h)*kCoef*kQuad;
 
 	// the element's basis table and this row-field pair's coefficients into L2 at once, so that the
-	// chunk copies below (two chunks ahead) wait for L2 rather than for DRAM
+	// chunk copies below (one chunk ahead) wait for L2 rather than for DRAM; and those of the CTA one
+	// resident wave later
 	if (tid == 0) {
 		PrefetchL2(P32, kFeatures*kQuad*kMaxBasis*4);
 		PrefetchL2(CF, 2*kCoef*kQuad*4);
+		const long long ahead = (long long)blockIdx.x+lookahead;
+		if (ahead < 2LL*mesh.elements) {
+			const long long ea = ahead >> 1;
+			if ((ahead & 1) == 0) PrefetchL2(phi32+(size_t)ea*kFeatures*kQuad*kMaxBasis, kFeatures*kQuad*kMaxBasis*4);
+			PrefetchL2(coef+((size_t)ea*4+2*(ahead & 1))*kCoef*kQuad, 2*kCoef*kQuad*4);
+		}
 	}
 	PrefetchChunk<NP>(P32, CF, 0, sPhi[0], sCf[0], tid);
 	PrefetchChunk<NP>(P32, CF, 1, sPhi[1], sCf[1], tid);
@@ -509,20 +516,22 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 	FenceAfterSync();
 	const uint32_t tmem = *tmem_slot;
 
-	// Chunks.  Chunk c builds operand buffer c & 1 once the MMAs of chunk c - 2 (the last users
-	// of that buffer) have completed; chunk c's basis and coefficients came in two chunks ago.
+	// Chunks, one barrier each.  On entry to chunk c its basis and coefficients are in staging buffer
+	// c & 1 and visible to every thread, and operand buffer c & 1 is free.  The chunk builds its operands,
+	// each thread waits for its own copies of chunk c + 1 (issued one chunk earlier), and thread 0 waits
+	// for the MMAs of chunk c - 1, the last users of operand buffer (c + 1) & 1; the barrier then makes
+	// all of that hold for chunk c + 1, thread 0 issues chunk c's MMAs, and chunk c + 2's data is fetched
+	// into the staging buffer chunk c has just consumed.  Only thread 0 polls an mbarrier.
 	const int gil = warp >> 2, gqp = warp & 3;     // G builder: row field, point pair / b quarter
 	const int gf = lane & 3, gbs = lane >> 2;       //            column field, basis sub-index
 	bool failed = false;
 	int issued = 0;                                  // chunks whose MMAs were committed
+	CopyAsyncWait<1>();                              // chunk 0 (this thread's copies)
+	__syncthreads();                                 // ... and every thread's
 	for (int c = 0; c < kChunks; ++c) {
 		const int buf = c & 1;
 		const float* PhiS = reinterpret_cast<const float*>(sm+(buf ? kOffPhi1 : kOffPhi0));
 		const float* CfS = reinterpret_cast<const float*>(sm+(buf ? kOffCf1 : kOffCf0));
-		CopyAsyncWait<1>();                      // all groups but the newest: chunk c is here
-		bool ok = true;
-		if (c >= 2) ok = MbarWaitBounded(bars+buf, (uint32_t)(((c-2) >> 1) & 1));
-		if (__syncthreads_or(!ok)) { failed = true; break; }
 		const uint32_t sA = sOp[buf], sB = sOp[buf]+kTiles*kTileBytes;
 
 		// B = Psi: row a, K = (s, point) inside each 16-byte unit (k = 2 s + point of the pair);
@@ -582,7 +591,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 			}
 		}
 		FenceProxyAsync();
-		__syncthreads();
+		CopyAsyncWait<0>();                      // chunk c + 1 (the only group in flight)
+		bool ok = true;
+		if (tid == 0 && c >= 1) ok = MbarWaitBounded(bars+((c-1) & 1), (uint32_t)(((c-1) >> 1) & 1));
+		if (__syncthreads_or(!ok)) { failed = true; break; }
 		if (tid == 0) {
 			FenceAfterSync();
 			#pragma unroll
@@ -605,6 +617,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		if (c+2 < kChunks) PrefetchChunk<NP>(P32, CF, c+2, sPhi[buf], sCf[buf], tid);
 		else CopyAsyncCommit();
 	}
+	// every thread observes the last commit itself before it reads the accumulators
 	if (!failed)
 		failed = __syncthreads_or(!MbarWaitBounded(bars+((kChunks-1) & 1), (uint32_t)(((kChunks-1) >> 1) & 1))) != 0;
 
@@ -724,7 +737,7 @@ template <bool kSplit>
 __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ point_state,
 	AssemblyParams prm, const int32_t* __restrict__ element_blocks, float* __restrict__ values,
-	int* __restrict__ status)
+	int* __restrict__ status, int lookahead)
 {
 	constexpr int NP = kSplit ? 4 : kMaxPts;     // points per K chunk
 	constexpr int kChunks = kQuad/NP;
@@ -745,6 +758,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 	if (tid == 0) {
 		PrefetchL2(P, kFeatures*kQuad*kMaxBasis*8);
 		PrefetchL2(point_state+(size_t)e*kQuad*kPointStride, kQuad*kPointStride*8);
+		// the element of the CTA one resident wave later (the pair of CTAs of an element shares it)
+		const long long ahead = (long long)blockIdx.x+lookahead;
+		if (ahead < 2LL*mesh.elements && (ahead & 1) == 0) {
+			const long long ea = ahead >> 1;
+			PrefetchL2(phi+(size_t)ea*kFeatures*kQuad*kMaxBasis, kFeatures*kQuad*kMaxBasis*8);
+			PrefetchL2(point_state+(size_t)ea*kQuad*kPointStride, kQuad*kPointStride*8);
+		}
 	}
 
 	PhiChunk<NP> stage;
@@ -789,13 +809,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 	const int gf = lane & 3, gbs = lane >> 2;
 	bool failed = false;
 	int issued = 0;
+	// One barrier per chunk, as TangentTcKernel: after building chunk c, thread 0 waits for the MMAs of
+	// chunk c - 1 (the last users of operand buffer (c + 1) & 1) before the barrier.
 	for (int c = 0; c < kChunks; ++c) {
 		const int buf = c & 1;
 		const float* PhiS = PhiF[buf];
 		if (c+2 < kChunks) stage.Load(P, c+2, tid);
-		bool ok = true;
-		if (c >= 2) ok = MbarWaitBounded(bars+buf, (uint32_t)(((c-2) >> 1) & 1));
-		if (__syncthreads_or(!ok)) { failed = true; break; }
 		const uint32_t sA = sOp[buf], sB = sOp[buf]+kTiles*kTileBytes;
 		if (tid < kTcThreads) {
 			const int a = tid >> 2, u = tid & 3;
@@ -847,7 +866,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 			}
 		}
 		FenceProxyAsync();
-		__syncthreads();
+		bool ok = true;
+		if (tid == 0 && c >= 1) ok = MbarWaitBounded(bars+((c-1) & 1), (uint32_t)(((c-1) >> 1) & 1));
+		if (__syncthreads_or(!ok)) { failed = true; break; }
 		if (tid == 0) {
 			FenceAfterSync();
 			#pragma unroll
@@ -924,6 +945,22 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 
 } // namespace
 
+namespace {
+
+// SMs of the current device (queried once per process).
+int MultiprocessorCount()
+{
+	static int sms = 0;
+	if (sms == 0) {
+		int device = 0;
+		CudaCheck(cudaGetDevice(&device), "device");
+		CudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+	}
+	return sms;
+}
+
+} // namespace
+
 void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const double* qdata, const double* state,
 	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs, int* queue,
 	cudaStream_t stream)
@@ -943,13 +980,7 @@ void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const dou
 		configured = true;
 	}
 	// two persistent CTAs per SM (the kernel's occupancy), no more than there are elements
-	static int sms = 0;
-	if (sms == 0) {
-		int device = 0;
-		CudaCheck(cudaGetDevice(&device), "device");
-		CudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
-	}
-	const unsigned grid = (unsigned)std::min<long long>(mesh.elements, 2LL*sms);
+	const unsigned grid = (unsigned)std::min<long long>(mesh.elements, 2LL*MultiprocessorCount());
 	const size_t bytes = kPtSmemBytes+16;
 	CudaCheck(cudaMemsetAsync(queue, 0, sizeof(int), stream), "point-kernel work queue");
 	if (coef)
@@ -978,12 +1009,13 @@ void LaunchTangentTc(const DeviceMeshView& mesh, const float* phi32, const float
 	}
 	const long long ctas = 2LL*mesh.elements;
 	if (ctas > 0x7fffffffLL) Fail(-7, "too many elements for one tangent launch");
+	const int lookahead = 2*MultiprocessorCount();            // two CTAs per SM
 	if (split)
 		TangentTcKernel<true><<<(unsigned)ctas, kTcThreads, kTcSmemBytes, stream>>>(mesh, phi32, coef,
-			element_blocks, values, status);
+			element_blocks, values, status, lookahead);
 	else
 		TangentTcKernel<false><<<(unsigned)ctas, kTcThreads, kTcSmemBytes, stream>>>(mesh, phi32, coef,
-			element_blocks, values, status);
+			element_blocks, values, status, lookahead);
 	LaunchCheck("TangentTcKernel");
 }
 
@@ -1002,12 +1034,13 @@ void LaunchTangentTcFused(const DeviceMeshView& mesh, const double* phi, const d
 	}
 	const long long ctas = 2LL*mesh.elements;
 	if (ctas > 0x7fffffffLL) Fail(-7, "too many elements for one tangent launch");
+	const int lookahead = MultiprocessorCount();              // one CTA per SM
 	if (split)
 		TangentTcFusedKernel<true><<<(unsigned)ctas, kFusedThreads, kFusedSmemBytes, stream>>>(mesh, phi, qdata,
-			point_state, params, element_blocks, values, status);
+			point_state, params, element_blocks, values, status, lookahead);
 	else
 		TangentTcFusedKernel<false><<<(unsigned)ctas, kFusedThreads, kFusedSmemBytes, stream>>>(mesh, phi, qdata,
-			point_state, params, element_blocks, values, status);
+			point_state, params, element_blocks, values, status, lookahead);
 	LaunchCheck("TangentTcFusedKernel");
 }
 
