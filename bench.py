@@ -213,9 +213,9 @@ def step_dt(name):
 # Per-workload solver settings of both arms.  The binary tree's Newton test is one decade tighter: at
 # rel.res 1e-10 its mixed and FP64 arms accepted states up to 2.3e-8 apart in pressure (traction-free
 # outlets, 600k elements).  Its coarse level has 1,762 point blocks (7,048 unknowns), whose dense inverse
-# dominated the AMG set-up when rebuilt every third refresh.
+# took 19% of the step when rebuilt every third refresh (0.3% every ninth); the tube batch is as large.
 NEWTON_RTOL = {"c4": 1e-11}
-COARSE_PERIOD = {"c4": 9}
+COARSE_PERIOD = {"c4": 9, "c5": 9}
 
 
 def outlet_models(name):
@@ -740,7 +740,7 @@ def main():
     ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c1", "c2-100", "c4", "c5", "transport"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
-    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "mixed", "fp64"])
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32", "mixed", "fp64"])
     ap.add_argument("--no-fp64-leg", action="store_true")
     ap.add_argument("--tangent-kernel", default="auto", choices=["auto", "coefficients", "fused"],
                     help="tensor-core tangent organisation (auto: the autotuner times both on the first tangent)")
@@ -806,7 +806,7 @@ def main():
     n = tube.mesh.nodes
     mesh = api.Mesh(tube.mesh)
     amg = args.preconditioner == "amg"
-    mixed = args.precision in ("mixed", "bf16x3")
+    mixed = args.precision in ("mixed", "bf16x3", "tf32")
     if mixed and not amg:
         raise SystemExit("--precision mixed needs --preconditioner amg")
     solver_kw = dict(density=RHO, viscosity=MU, dt=step_dt(args.workload),
@@ -817,7 +817,8 @@ def main():
                      newton_forcing=int(args.forcing == "ew"), tangent_reuse_factor=args.tangent_reuse,
                      tangent_kernel={"auto": api.TANGENT_AUTO, "coefficients": api.TANGENT_COEFFICIENTS,
                                      "fused": api.TANGENT_FUSED}[args.tangent_kernel])
-    precision = {"mixed": api.MIXED, "bf16x3": api.MIXED_BF16X3, "fp64": api.FP64}[args.precision]
+    precision = {"mixed": api.MIXED, "bf16x3": api.MIXED_BF16X3, "tf32": api.MIXED_TF32,
+                 "fp64": api.FP64}[args.precision]
     ns = api.NavierStokes(mesh, precision=precision, **solver_kw)
     batched = args.workload == "c5"
     if batched:
@@ -1167,12 +1168,13 @@ def main():
     line = {
         "metric": METRIC, "value": steps_per_s, "unit": "time steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16-tc/f32/f64" if mixed else "f64",
+        "vs_baseline": None, "dtype": ("tf32-tc/f32/f64" if args.precision == "tf32" else "bf16-tc/f32/f64") if mixed else "f64",
         "data": "synthetic (seeded generator; BASELINE publishes no dataset)",
         "config": {"workload": desc, "elements": tube.mesh.elements, "nodes": n, "block_nonzeros": mesh.blocks,
                    "solver": (("mixed: tcgen05 %s tangent (FP32 accumulate), FP32 Jacobian, FP64 residual and "
-                               "refinement; " % ("split-BF16 (hi + lo, 3 products)" if args.precision == "bf16x3"
-                                                 else "BF16") if mixed else "plain FP64: ") +
+                               "refinement; " % {"bf16x3": "split-BF16 (hi + lo, 3 products)", "tf32": "TF32",
+                                                 "mixed": "BF16"}.get(args.precision, "") if mixed
+                               else "plain FP64: ") +
                               "exact-tangent Newton to rel.res %g (FP64 residual, tested before the tangent is "
                               "assembled), " % args.newton_rtol +
                               ("inexact Newton (Eisenstat-Walker forcing tolerances, Dirichlet values lifted "

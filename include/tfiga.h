@@ -101,7 +101,10 @@ typedef struct tfiga_ns_params {
 	 * two BF16 terms (x = hi + lo) and three products per tile (hi hi + hi lo + lo hi):
 	 * a tangent accurate to about 1e-5 instead of 2e-3, so that Newton converges as with
 	 * the FP64 tangent.
-	 * Both reduced modes require TFIGA_PRECONDITIONER_AMG. */
+	 * TFIGA_PRECISION_MIXED_TF32: as MIXED, with TF32 tensor-core operands (FP32 values
+	 * rounded to 10 fraction bits, one product per tile): a tangent accurate to about
+	 * 5e-4 with no splitting of the operands.
+	 * The reduced modes require TFIGA_PRECONDITIONER_AMG. */
 	int32_t precision;             /* default TFIGA_PRECISION_FP64 */
 	/* AMG: aggregate until at most this many coarse nodes remain (dense
 	 * coarse solve of 4x that order; at most 2048). */
@@ -149,6 +152,7 @@ typedef struct tfiga_ns_params {
 #define TFIGA_PRECISION_MIXED 1
 #define TFIGA_PRECISION_FP32_JACOBIAN 2
 #define TFIGA_PRECISION_MIXED_BF16X3 3
+#define TFIGA_PRECISION_MIXED_TF32 4
 #define TFIGA_LEARNED_RESIDUAL_LOSS 0
 #define TFIGA_LEARNED_ERROR_LOSS 1
 #define TFIGA_TANGENT_AUTO 0

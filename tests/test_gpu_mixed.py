@@ -16,6 +16,9 @@ Split-BF16 mode (TFIGA_PRECISION_MIXED_BF16X3, operands hi + lo, three
 products): Jacobian within 1e-4 relative per field pair -- about 2^-16 per
 product plus FP32 accumulation and the FP32 coefficients -- and Newton takes
 no more iterations than with the FP64 tangent.
+TF32 mode (TFIGA_PRECISION_MIXED_TF32, FP32 operands rounded to TF32, one
+product): Jacobian within 5e-3 relative per field pair (2^-11 per operand,
+eight times finer than BF16), and Newton converges to the FP64 solution.
 """
 import numpy as np
 import pytest
@@ -27,6 +30,7 @@ pytestmark = pytest.mark.gpu
 RHO, MU, DT = 1060.0, 3.5e-3, 1e-3
 TANGENT_TOL = 2e-2
 SPLIT_TOL = 1e-4
+TF32_TOL = 5e-3
 
 
 @pytest.fixture(scope="module")
@@ -98,6 +102,39 @@ def test_split_tangent_steady_and_ragged(api, small_tube, reference_tube, kernel
     check_tensor_tangent(api, small_tube.mesh, RHO, MU, 0.0, 3, api.MIXED_BF16X3, SPLIT_TOL, kernel)
     flat = ntiga.read(reference_tube / "tube-1.ntiga")
     check_tensor_tangent(api, flat, 1.0, 1.0, 0.1, 5, api.MIXED_BF16X3, SPLIT_TOL, kernel)
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_tf32_tangent(api, small_tube, reference_tube, kernel):
+    from tubularflowiga_b200 import ntiga
+    errors = check_tensor_tangent(api, small_tube.mesh, RHO, MU, DT, 0, api.MIXED_TF32, TF32_TOL, kernel)
+    plain = check_tensor_tangent(api, small_tube.mesh, RHO, MU, DT, 0, kernel=kernel)
+    print(f"TF32 tangent error per field pair: max {errors.max():.2e} (BF16 {plain.max():.2e})")
+    assert errors.max() < 0.5 * plain.max()
+    check_tensor_tangent(api, small_tube.mesh, RHO, MU, 0.0, 3, api.MIXED_TF32, TF32_TOL, kernel)
+    flat = ntiga.read(reference_tube / "tube-1.ntiga")
+    check_tensor_tangent(api, flat, 1.0, 1.0, 0.1, 5, api.MIXED_TF32, TF32_TOL, kernel)
+
+
+def test_tf32_newton_converges_to_fp64_solution(api, cylinder_1280):
+    tube = cylinder_1280
+    flat = tube.mesh
+    vmask, pmask, vel = api.tube_boundary_conditions(tube, 0.2)
+    s0 = api.initial_state(vmask, vel)
+    mesh = api.Mesh(flat)
+    states, reports = {}, {}
+    for name, precision in (("fp64", api.FP64), ("tf32", api.MIXED_TF32)):
+        ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, preconditioner=api.AMG, precision=precision,
+                              nonlinear_rtol=1e-10, nonlinear_atol=1e-30, gmres_rtol=1e-10, max_newton=20)
+        ns.set_dirichlet(vmask, pmask, vel)
+        ns.set_tractions({2: 0.0})
+        ns.set_state(s0, s0)
+        reports[name] = ns.step()
+        states[name] = ns.get_state().reshape(-1, 4)
+    print("Newton iterations: FP64", reports["fp64"]["newton_iterations"], "TF32", reports["tf32"]["newton_iterations"])
+    assert reports["tf32"]["converged"]
+    assert rel(states["tf32"][:, :3], states["fp64"][:, :3]) < 1e-8
+    assert rel(states["tf32"][:, 3], states["fp64"][:, 3]) < 1e-8
 
 
 def test_tangent_autotuner_picks_one_and_matches(api, small_tube):

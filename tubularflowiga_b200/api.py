@@ -54,6 +54,7 @@ FP64 = 0
 MIXED = 1
 FP32_JACOBIAN = 2
 MIXED_BF16X3 = 3
+MIXED_TF32 = 4
 
 
 BLOCK_JACOBI = 0

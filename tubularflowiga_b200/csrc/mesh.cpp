@@ -265,7 +265,7 @@ const float* Mesh::phi32()
 	if (phi32_.get() == nullptr) {
 		const size_t count = (size_t)regular_elements_*kFeatures*kQuad*kMaxBasis;
 		phi32_.Allocate(count);
-		LaunchToFloat((long long)count, phi_.get(), phi32_.get(), stream_);
+		LaunchToFloatPointPairs((long long)regular_elements_*kFeatures, phi_.get(), phi32_.get(), stream_);
 		CudaCheck(cudaStreamSynchronize(stream_), "FP32 basis tables");
 		device_bytes_ += (int64_t)phi32_.bytes();
 	}

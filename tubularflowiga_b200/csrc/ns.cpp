@@ -46,7 +46,8 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 	stream_ = mesh.stream();
 	const int64_t n = mesh.nodes();
 	if (params.precision != TFIGA_PRECISION_FP64 && params.precision != TFIGA_PRECISION_MIXED
-		&& params.precision != TFIGA_PRECISION_FP32_JACOBIAN && params.precision != TFIGA_PRECISION_MIXED_BF16X3)
+		&& params.precision != TFIGA_PRECISION_FP32_JACOBIAN && params.precision != TFIGA_PRECISION_MIXED_BF16X3
+		&& params.precision != TFIGA_PRECISION_MIXED_TF32)
 		Fail(-1, "unknown precision "+std::to_string(params.precision));
 	if (!(params.tangent_reuse_factor >= 0.0 && std::isfinite(params.tangent_reuse_factor)))
 		Fail(-1, "tangent_reuse_factor must be finite and non-negative");
@@ -236,7 +237,7 @@ void NsSolver::LargeElements(T* values, double* rhs)
 void NsSolver::AssembleTangentTc()
 {
 	amg_current_ = false;
-	const bool split = params_.precision == TFIGA_PRECISION_MIXED_BF16X3;
+	const int operands = tc_operands();
 	const AssemblyParams prm{params_.density, params_.viscosity, params_.dt};
 	profiler_.Begin(Profiler::kAssembly, stream_);
 	if (tangent_kernel_ == TFIGA_TANGENT_AUTO) {
@@ -245,10 +246,10 @@ void NsSolver::AssembleTangentTc()
 		values32_.Zero(stream_);
 		if (tangent_kernel_ == TFIGA_TANGENT_FUSED)
 			LaunchTangentTcFused(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), point_state_.get(), prm,
-				mesh_.element_blocks(), values32_.get(), status_.get(), split, stream_);
+				mesh_.element_blocks(), values32_.get(), status_.get(), operands, stream_);
 		else
 			LaunchTangentTc(mesh_.regular_view(), mesh_.phi32(), coef32_.get(), mesh_.element_blocks(),
-				values32_.get(), status_.get(), split, stream_);
+				values32_.get(), status_.get(), operands, stream_);
 		launches_ += 1;
 	}
 	LargeElements<float>(values32_.get(), nullptr);
@@ -258,7 +259,7 @@ void NsSolver::AssembleTangentTc()
 
 void NsSolver::AutotuneTangent()
 {
-	const bool split = params_.precision == TFIGA_PRECISION_MIXED_BF16X3;
+	const int operands = tc_operands();
 	const AssemblyParams prm{params_.density, params_.viscosity, params_.dt};
 	const DeviceMeshView view = mesh_.regular_view();
 	cudaEvent_t ev[4];
@@ -271,7 +272,7 @@ void NsSolver::AutotuneTangent()
 	values32_.Zero(stream_);
 	CudaCheck(cudaEventRecord(ev[0], stream_), "event");
 	LaunchTangentTcFused(view, mesh_.phi(), mesh_.qdata(), point_state_.get(), prm, mesh_.element_blocks(),
-		values32_.get(), status_.get(), split, stream_);
+		values32_.get(), status_.get(), operands, stream_);
 	CudaCheck(cudaEventRecord(ev[1], stream_), "event");
 	launches_ += 1;
 	CudaCheck(cudaStreamSynchronize(stream_), "tangent autotune");
@@ -295,7 +296,7 @@ void NsSolver::AutotuneTangent()
 	const float* phi32 = mesh_.phi32();
 	values32_.Zero(stream_);
 	CudaCheck(cudaEventRecord(ev[2], stream_), "event");
-	LaunchTangentTc(view, phi32, coef32_.get(), mesh_.element_blocks(), values32_.get(), status_.get(), split,
+	LaunchTangentTc(view, phi32, coef32_.get(), mesh_.element_blocks(), values32_.get(), status_.get(), operands,
 		stream_);
 	CudaCheck(cudaEventRecord(ev[3], stream_), "event");
 	launches_ += 2;

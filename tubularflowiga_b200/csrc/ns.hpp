@@ -65,10 +65,17 @@ public:
 	float* values32() { return values32_.get(); }    // null in TFIGA_PRECISION_FP64
 	// FP32 Jacobian storage (both reduced-precision modes).
 	bool mixed() const { return params_.precision != TFIGA_PRECISION_FP64; }
-	// Tangent contracted on the tensor cores (BF16 x BF16 -> FP32); no FP64 Jacobian is kept.
+	// Tangent contracted on the tensor cores (FP32 accumulation); no FP64 Jacobian is kept.
 	bool tensor_tangent() const
 	{
-		return params_.precision == TFIGA_PRECISION_MIXED || params_.precision == TFIGA_PRECISION_MIXED_BF16X3;
+		return params_.precision == TFIGA_PRECISION_MIXED || params_.precision == TFIGA_PRECISION_MIXED_BF16X3
+			|| params_.precision == TFIGA_PRECISION_MIXED_TF32;
+	}
+	// The tensor-core operand organisation of the precision mode (TC_OPERANDS_*).
+	int tc_operands() const
+	{
+		return params_.precision == TFIGA_PRECISION_MIXED_BF16X3 ? TC_OPERANDS_SPLIT
+			: params_.precision == TFIGA_PRECISION_MIXED_TF32 ? TC_OPERANDS_TF32 : TC_OPERANDS_BF16;
 	}
 	// Active Jacobian values as FP64 on the host (FP32 storage is widened).
 	void DownloadValues(double* out);

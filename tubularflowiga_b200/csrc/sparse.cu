@@ -316,6 +316,29 @@ template void LaunchSpmvBlockJacobi<float>(const DevicePatternView&, const float
 template void LaunchBlockInverse<double>(const DevicePatternView&, const double*, double*, unsigned int*, cudaStream_t);
 template void LaunchBlockInverse<float>(const DevicePatternView&, const float*, double*, unsigned int*, cudaStream_t);
 
+namespace {
+
+// One thread per (table, point pair, function): two FP64 reads 64 apart, one 8-byte store.
+__global__ void ToFloatPointPairsKernel(long long pairs, const double* __restrict__ in, float* __restrict__ out)
+{
+	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
+	if (i >= pairs) return;
+	const long long table = i >> 11, rest = i & 2047;          // 32 pairs x 64 functions per table
+	const int pair = (int)(rest >> 6), b = (int)(rest & 63);
+	const double* t = in+table*4096;
+	reinterpret_cast<float2*>(out)[i] = make_float2((float)t[(2*pair)*64+b], (float)t[(2*pair+1)*64+b]);
+}
+
+} // namespace
+
+void LaunchToFloatPointPairs(long long tables, const double* in, float* out, cudaStream_t stream)
+{
+	if (tables == 0) return;
+	const long long pairs = tables*2048;
+	ToFloatPointPairsKernel<<<Blocks(pairs, 256), 256, 0, stream>>>(pairs, in, out);
+	LaunchCheck("ToFloatPointPairsKernel");
+}
+
 void LaunchToFloat(long long n, const double* in, float* out, cudaStream_t stream)
 {
 	if (n == 0) return;

@@ -73,10 +73,13 @@ constexpr int kScratchStride = 41;               // odd float stride of the per-
 constexpr int kOperandBytes = kTiles*kTileBytes+64*64;            // A tiles + B (Psi: 64 rows x 64 B)
 constexpr int kOffOp0 = 0;                                        // operand buffer 0
 constexpr int kOffOp1 = kOperandBytes;                            // operand buffer 1 (36 KiB, 1024-aligned)
-constexpr int kPhiBytes = kFeatures*kMaxPts*64*4;                 // float [5][NP][64] per chunk
+constexpr int kPhiBytes = kFeatures*kMaxPts*64*4;                 // float [5][NP/2][64][2] per chunk
 constexpr int kOffPhi0 = 2*kOperandBytes;
 constexpr int kOffPhi1 = kOffPhi0+kPhiBytes;
-constexpr int kCfBytes = 2*kCoef*kMaxPts*4;                       // float [2 rows][80][NP] per chunk
+// float [2 rows][80][NP] per chunk, each row field's 4 column-field groups of 20 rows followed by
+// kCfPad floats, so that the four column fields' coefficients (read together) start in different banks
+constexpr int kCfPad = 8;
+constexpr int kCfBytes = (2*kCoef*kMaxPts+8*kCfPad)*4;
 constexpr int kOffCf0 = kOffPhi1+kPhiBytes;
 constexpr int kOffCf1 = kOffCf0+kCfBytes;
 constexpr int kOffBar = kOffCf1+kCfBytes;                         // 2 mbarriers, TMEM slot
@@ -101,6 +104,14 @@ static_assert(kFeatures*kQuad*kStageStride*8 <= kPtPartBytes, "staged basis chun
 // Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B BF16, both
 // K-major, M = 128, N = 64.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// kind::tf32: D FP32, A and B TF32 (format 2), both K-major, M = 128, N = 64.
+constexpr uint32_t kIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+// Operand organisations of the tensor-core tangent (template parameter kMode):
+constexpr int kModeBf16 = 0;      // BF16 operands, K = 32 (8 points) per chunk, two K = 16 MMAs per tile
+constexpr int kModeSplit = 1;     // split BF16 (hi + lo), K = 16 (4 points), three products per tile
+constexpr int kModeTf32 = 2;      // TF32 operands (FP32 in shared memory, rounded to TF32), K = 16 (4
+                                  // points), two K = 8 MMAs per tile; no conversion into two terms
 
 __device__ __forceinline__ uint32_t SmemAddress(const void* p)
 {
@@ -161,6 +172,14 @@ __device__ __forceinline__ void MmaBf16(uint32_t tmem_d, uint64_t adesc, uint64_
 		:: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0u) : "memory");
 }
 
+__device__ __forceinline__ void MmaTf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+	asm volatile("{\n\t.reg .pred p;\n\t"
+		"setp.ne.b32 p, %4, 0;\n\t"
+		"tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+		:: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdescTf32), "r"(accumulate), "r"(0u) : "memory");
+}
+
 __device__ __forceinline__ void MmaCommit(uint64_t* bar)
 {
 	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
@@ -203,6 +222,14 @@ __device__ __forceinline__ uint32_t PackBf16(float lo, float hi)
 {
 	const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
 	return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// x rounded to TF32 (10 fraction bits, nearest with ties away), as the 32-bit pattern the MMA reads.
+__device__ __forceinline__ uint32_t Tf32(float x)
+{
+	uint32_t r;
+	asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+	return r;
 }
 
 // x - bf16(x): the part of x that its BF16 rounding drops (exact in FP32).
@@ -266,8 +293,10 @@ __device__ __forceinline__ void RedAdd4(float* p, float a, float b, float c, flo
 
 
 // Basis chunk c (points NP c .. NP c + NP - 1, five features, 64 functions) of
-// one element, FP32, into a [5][NP][64] buffer; the coefficients of the two row
-// fields 2h, 2h+1 at those points into a [2][80][NP] buffer.  One commit group.
+// one element, FP32 with the points of each pair interleaved (the layout of
+// Mesh::phi32), into a [5][NP/2][64][2] buffer; the coefficients of the two row
+// fields 2h, 2h+1 at those points into a [2][80][NP] buffer (padded per group of
+// 20 rows).  One commit group.
 template <int NP>
 __device__ __forceinline__ void PrefetchChunk(const float* P32, const float* CF, int c, uint32_t phi_dst,
 	uint32_t cf_dst, int tid)
@@ -278,7 +307,7 @@ __device__ __forceinline__ void PrefetchChunk(const float* P32, const float* CF,
 	}
 	for (int idx = tid; idx < 2*kCoef*NP/4; idx += kTcThreads) {
 		const int rk = idx/(NP/4), part = idx%(NP/4);           // rk = row field * 80 + k
-		CopyAsync16(cf_dst+16*idx, CF+(size_t)rk*kQuad+c*NP+4*part);
+		CopyAsync16(cf_dst+16*idx+(rk/20)*kCfPad*4, CF+(size_t)rk*kQuad+c*NP+4*part);
 	}
 	CopyAsyncCommit();
 }
@@ -466,12 +495,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 
 // lookahead: the number of CTAs resident at once (two per SM); CTA k also prefetches the tables of
 // CTA k + lookahead, which starts about when CTA k finishes.
-template <bool kSplit>
+template <int kMode>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView mesh,
 	const float* __restrict__ phi32, const float* __restrict__ coef, const int32_t* __restrict__ element_blocks,
 	float* __restrict__ values, int* __restrict__ status, int lookahead)
 {
-	constexpr int NP = kSplit ? 4 : kMaxPts;     // points per K chunk
+	constexpr bool kSplit = kMode == kModeSplit, kTf32 = kMode == kModeTf32;
+	constexpr bool kFour = kMode != kModeBf16;   // four points (K = 16) per chunk
+	constexpr int NP = kFour ? 4 : kMaxPts;      // points per K chunk
 	constexpr int kChunks = kQuad/NP;
 	extern __shared__ uint8_t smem_raw[];
 	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+1023) & ~uintptr_t(1023));
@@ -538,29 +569,42 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 		// thread (a, 16-byte unit u of the row).  Plain: unit u is point pair u.  Split: units 0, 1
 		// hold hi of point pairs 0, 1 and units 2, 3 their lo.
 		{
-			const int a = tid >> 2, u = tid & 3;
-			const int qp = kSplit ? (u & 1) : u;
-			float x[8];
-			#pragma unroll
-			for (int k = 0; k < 8; ++k) x[k] = PhiS[((k >> 1)*NP+2*qp+(k & 1))*64+a];
-			if (kSplit && u >= 2) {
+			// thread (unit u, row a): a warp reads 32 consecutive functions of one point pair
+			const int u = tid >> 6, a = tid & 63;
+			const float2* pairs = reinterpret_cast<const float2*>(PhiS);     // [5][NP/2][64] point pairs
+			if constexpr (kTf32) {
+				// unit u: point pair u >> 1, test features 2 (u & 1) and 2 (u & 1) + 1, both points each
+				const int qp = u >> 1, s0 = 2*(u & 1);
+				const float2 x0 = pairs[(s0*(NP/2)+qp)*64+a], x1 = pairs[((s0+1)*(NP/2)+qp)*64+a];
+				StoreShared16(sB+Sw64(a, u), Tf32(x0.x), Tf32(x0.y), Tf32(x1.x), Tf32(x1.y));
+			} else {
+				const int qp = kSplit ? (u & 1) : u;
+				float x[8];
 				#pragma unroll
-				for (int k = 0; k < 8; ++k) x[k] = Bf16Residual(x[k]);
+				for (int s = 0; s < 4; ++s) {
+					const float2 v = pairs[(s*(NP/2)+qp)*64+a];
+					x[2*s] = v.x;
+					x[2*s+1] = v.y;
+				}
+				if (kSplit && u >= 2) {
+					#pragma unroll
+					for (int k = 0; k < 8; ++k) x[k] = Bf16Residual(x[k]);
+				}
+				StoreShared16(sB+Sw64(a, u), PackBf16(x[0], x[1]), PackBf16(x[2], x[3]), PackBf16(x[4], x[5]),
+					PackBf16(x[6], x[7]));
 			}
-			StoreShared16(sB+Sw64(a, u), PackBf16(x[0], x[1]), PackBf16(x[2], x[3]), PackBf16(x[4], x[5]),
-				PackBf16(x[6], x[7]));
 		}
 		// A = G: row (b, f) of tile (il, b / 32).  Plain: warp (il, point pair) over all b.  Split:
 		// warp (il, point pair, half of the b groups), writing hi and lo units.  Both points of
 		// the pair ride in one register pair: coefficients mm[k] = (M_q0, M_q1)[k] (one 8-byte
 		// load from the [2][80][NP] chunk), basis pb[t] = (Phi_t(q0, b), Phi_t(q1, b)).
 		{
-			const int qpair = kSplit ? (gqp & 1) : gqp;
+			const int qpair = kFour ? (gqp & 1) : gqp;
 			const int ql0 = 2*qpair;
-			constexpr int kGroups = kSplit ? 4 : 8;
-			const int g0 = kSplit ? (gqp >> 1)*4 : 0;
+			constexpr int kGroups = kFour ? 4 : 8;
+			const int g0 = kFour ? (gqp >> 1)*4 : 0;
 			unsigned long long mm[20];
-			const float* c0 = CfS+(gil*kCoef+gf*20)*NP+ql0;
+			const float* c0 = CfS+(gil*kCoef+gf*20)*NP+(gil*4+gf)*kCfPad+ql0;
 			#pragma unroll
 			for (int k = 0; k < 20; ++k) mm[k] = *reinterpret_cast<const unsigned long long*>(c0+k*NP);
 			#pragma unroll 2
@@ -568,7 +612,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 				const int b = (g0+j)*8+gbs;
 				unsigned long long pb[5];
 				#pragma unroll
-				for (int t = 0; t < 5; ++t) pb[t] = Pack2(PhiS[(t*NP+ql0)*64+b], PhiS[(t*NP+ql0+1)*64+b]);
+				for (int t = 0; t < 5; ++t)
+					pb[t] = *reinterpret_cast<const unsigned long long*>(PhiS+((t*(NP/2)+qpair)*64+b)*2);
 				unsigned long long gg[4];
 				#pragma unroll
 				for (int s = 0; s < 4; ++s) {
@@ -578,15 +623,23 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 				}
 				const int tile = gil*2+(b >> 5), row = (b & 31)*4+gf;
 				const uint32_t dst = sA+tile*kTileBytes;
-				uint32_t hi[4];
-				#pragma unroll
-				for (int s = 0; s < 4; ++s) hi[s] = Bf16Pair(gg[s]);
-				StoreShared16(dst+Sw64(row, qpair), hi[0], hi[1], hi[2], hi[3]);
-				if (kSplit) {
-					uint32_t lo[4];
+				if constexpr (kTf32) {
+					// units 2 qpair (features 0, 1) and 2 qpair + 1 (features 2, 3), both points each
+					StoreShared16(dst+Sw64(row, 2*qpair), Tf32(Low(gg[0])), Tf32(High(gg[0])), Tf32(Low(gg[1])),
+						Tf32(High(gg[1])));
+					StoreShared16(dst+Sw64(row, 2*qpair+1), Tf32(Low(gg[2])), Tf32(High(gg[2])), Tf32(Low(gg[3])),
+						Tf32(High(gg[3])));
+				} else {
+					uint32_t hi[4];
 					#pragma unroll
-					for (int s = 0; s < 4; ++s) lo[s] = Bf16Pair(Sub2(gg[s], WidenBf16Pair(hi[s])));
-					StoreShared16(dst+Sw64(row, 2+qpair), lo[0], lo[1], lo[2], lo[3]);
+					for (int s = 0; s < 4; ++s) hi[s] = Bf16Pair(gg[s]);
+					StoreShared16(dst+Sw64(row, qpair), hi[0], hi[1], hi[2], hi[3]);
+					if (kSplit) {
+						uint32_t lo[4];
+						#pragma unroll
+						for (int s = 0; s < 4; ++s) lo[s] = Bf16Pair(Sub2(gg[s], WidenBf16Pair(hi[s])));
+						StoreShared16(dst+Sw64(row, 2+qpair), lo[0], lo[1], lo[2], lo[3]);
+					}
 				}
 			}
 		}
@@ -600,7 +653,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 			#pragma unroll
 			for (int tile = 0; tile < kTiles; ++tile) {
 				const uint32_t a = sA+tile*kTileBytes;
-				if (kSplit) {
+				if constexpr (kTf32) {
+					#pragma unroll
+					for (int ks = 0; ks < 2; ++ks)
+						MmaTf32(tmem+tile*64, DescSw64(a+ks*32), DescSw64(sB+ks*32), (c > 0 || ks > 0) ? 1u : 0u);
+				} else if (kSplit) {
 					MmaBf16(tmem+tile*64, DescSw64(a), DescSw64(sB), c > 0 ? 1u : 0u);       // hi hi
 					MmaBf16(tmem+tile*64, DescSw64(a), DescSw64(sB+32), 1u);                 // hi lo
 					MmaBf16(tmem+tile*64, DescSw64(a+32), DescSw64(sB), 1u);                 // lo hi
@@ -704,9 +761,11 @@ static_assert(kQuad*kPointStride*8 <= kOperandBytes, "point-state staging fits i
 
 // One basis chunk (points NP c .. NP c + NP - 1, five features, 64 functions) of one element:
 // FP64 loads into registers, then FP32 stores into a [5][NP][64] buffer.
+// One (feature, point pair, function) per slot: the two points' FP64 values (64 apart in the table)
+// into registers, then one float2 into the [5][NP/2][64][2] staging layout of the coefficient kernel.
 template <int NP>
 struct PhiChunk {
-	static constexpr int kPairs = kFeatures*NP*32;                     // double2 per chunk
+	static constexpr int kPairs = kFeatures*(NP/2)*64;                 // point pairs per chunk
 	static constexpr int kSlots = (kPairs+kFusedThreads-1)/kFusedThreads;
 	double2 v[kSlots];
 	__device__ __forceinline__ void Load(const double* P, int c, int tid)
@@ -715,8 +774,9 @@ struct PhiChunk {
 		for (int s = 0; s < kSlots; ++s) {
 			const int idx = tid+s*kFusedThreads;
 			if (idx < kPairs) {
-				const int t = idx/(NP*32), rem = idx%(NP*32), q = rem/32, b2 = rem%32;
-				v[s] = __ldg(reinterpret_cast<const double2*>(P+(size_t)(t*kQuad+c*NP+q)*kMaxBasis)+b2);
+				const int t = idx/((NP/2)*64), rem = idx%((NP/2)*64), qp = rem/64, b = rem%64;
+				const double* row = P+(size_t)(t*kQuad+c*NP+2*qp)*kMaxBasis+b;
+				v[s] = make_double2(__ldg(row), __ldg(row+kMaxBasis));
 			}
 		}
 	}
@@ -725,21 +785,20 @@ struct PhiChunk {
 		#pragma unroll
 		for (int s = 0; s < kSlots; ++s) {
 			const int idx = tid+s*kFusedThreads;
-			if (idx < kPairs) {
-				const int t = idx/(NP*32), rem = idx%(NP*32), q = rem/32, b2 = rem%32;
-				reinterpret_cast<float2*>(dst+(t*NP+q)*64)[b2] = make_float2((float)v[s].x, (float)v[s].y);
-			}
+			if (idx < kPairs) reinterpret_cast<float2*>(dst)[idx] = make_float2((float)v[s].x, (float)v[s].y);
 		}
 	}
 };
 
-template <bool kSplit>
+template <int kMode>
 __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ point_state,
 	AssemblyParams prm, const int32_t* __restrict__ element_blocks, float* __restrict__ values,
 	int* __restrict__ status, int lookahead)
 {
-	constexpr int NP = kSplit ? 4 : kMaxPts;     // points per K chunk
+	constexpr bool kSplit = kMode == kModeSplit, kTf32 = kMode == kModeTf32;
+	constexpr bool kFour = kMode != kModeBf16;   // four points (K = 16) per chunk
+	constexpr int NP = kFour ? 4 : kMaxPts;      // points per K chunk
 	constexpr int kChunks = kQuad/NP;
 	extern __shared__ uint8_t smem_raw[];
 	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+1023) & ~uintptr_t(1023));
@@ -817,23 +876,36 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 		if (c+2 < kChunks) stage.Load(P, c+2, tid);
 		const uint32_t sA = sOp[buf], sB = sOp[buf]+kTiles*kTileBytes;
 		if (tid < kTcThreads) {
-			const int a = tid >> 2, u = tid & 3;
-			const int qp = kSplit ? (u & 1) : u;
-			float x[8];
-			#pragma unroll
-			for (int k = 0; k < 8; ++k) x[k] = PhiS[((k >> 1)*NP+2*qp+(k & 1))*64+a];
-			if (kSplit && u >= 2) {
+			// thread (unit u, row a): a warp reads 32 consecutive functions of one point pair
+			const int u = tid >> 6, a = tid & 63;
+			const float2* pairs = reinterpret_cast<const float2*>(PhiS);     // [5][NP/2][64] point pairs
+			if constexpr (kTf32) {
+				// unit u: point pair u >> 1, test features 2 (u & 1) and 2 (u & 1) + 1, both points each
+				const int qp = u >> 1, s0 = 2*(u & 1);
+				const float2 x0 = pairs[(s0*(NP/2)+qp)*64+a], x1 = pairs[((s0+1)*(NP/2)+qp)*64+a];
+				StoreShared16(sB+Sw64(a, u), Tf32(x0.x), Tf32(x0.y), Tf32(x1.x), Tf32(x1.y));
+			} else {
+				const int qp = kSplit ? (u & 1) : u;
+				float x[8];
 				#pragma unroll
-				for (int k = 0; k < 8; ++k) x[k] = Bf16Residual(x[k]);
+				for (int s = 0; s < 4; ++s) {
+					const float2 v = pairs[(s*(NP/2)+qp)*64+a];
+					x[2*s] = v.x;
+					x[2*s+1] = v.y;
+				}
+				if (kSplit && u >= 2) {
+					#pragma unroll
+					for (int k = 0; k < 8; ++k) x[k] = Bf16Residual(x[k]);
+				}
+				StoreShared16(sB+Sw64(a, u), PackBf16(x[0], x[1]), PackBf16(x[2], x[3]), PackBf16(x[4], x[5]),
+					PackBf16(x[6], x[7]));
 			}
-			StoreShared16(sB+Sw64(a, u), PackBf16(x[0], x[1]), PackBf16(x[2], x[3]), PackBf16(x[4], x[5]),
-				PackBf16(x[6], x[7]));
 		}
 		{
-			const int qpair = kSplit ? (gqp & 1) : gqp;
+			const int qpair = kFour ? (gqp & 1) : gqp;
 			const int ql0 = 2*qpair;
-			constexpr int kGroups = kSplit ? 2 : 4;
-			const int g0 = kSplit ? (gqp >> 1)*4+ghalf*2 : ghalf*4;
+			constexpr int kGroups = kFour ? 2 : 4;
+			const int g0 = kFour ? (gqp >> 1)*4+ghalf*2 : ghalf*4;
 			unsigned long long mm[20];
 			const float* c0 = CoefS+(gil*kCoef+gf*20)*kCoefStride+c*NP+ql0;
 			#pragma unroll
@@ -843,7 +915,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 				const int b = (g0+j)*8+gbs;
 				unsigned long long pb[5];
 				#pragma unroll
-				for (int t = 0; t < 5; ++t) pb[t] = Pack2(PhiS[(t*NP+ql0)*64+b], PhiS[(t*NP+ql0+1)*64+b]);
+				for (int t = 0; t < 5; ++t)
+					pb[t] = *reinterpret_cast<const unsigned long long*>(PhiS+((t*(NP/2)+qpair)*64+b)*2);
 				unsigned long long gg[4];
 				#pragma unroll
 				for (int s = 0; s < 4; ++s) {
@@ -853,15 +926,23 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 				}
 				const int tile = gil*2+(b >> 5), row = (b & 31)*4+gf;
 				const uint32_t dst = sA+tile*kTileBytes;
-				uint32_t hi[4];
-				#pragma unroll
-				for (int s = 0; s < 4; ++s) hi[s] = Bf16Pair(gg[s]);
-				StoreShared16(dst+Sw64(row, qpair), hi[0], hi[1], hi[2], hi[3]);
-				if (kSplit) {
-					uint32_t lo[4];
+				if constexpr (kTf32) {
+					// units 2 qpair (features 0, 1) and 2 qpair + 1 (features 2, 3), both points each
+					StoreShared16(dst+Sw64(row, 2*qpair), Tf32(Low(gg[0])), Tf32(High(gg[0])), Tf32(Low(gg[1])),
+						Tf32(High(gg[1])));
+					StoreShared16(dst+Sw64(row, 2*qpair+1), Tf32(Low(gg[2])), Tf32(High(gg[2])), Tf32(Low(gg[3])),
+						Tf32(High(gg[3])));
+				} else {
+					uint32_t hi[4];
 					#pragma unroll
-					for (int s = 0; s < 4; ++s) lo[s] = Bf16Pair(Sub2(gg[s], WidenBf16Pair(hi[s])));
-					StoreShared16(dst+Sw64(row, 2+qpair), lo[0], lo[1], lo[2], lo[3]);
+					for (int s = 0; s < 4; ++s) hi[s] = Bf16Pair(gg[s]);
+					StoreShared16(dst+Sw64(row, qpair), hi[0], hi[1], hi[2], hi[3]);
+					if (kSplit) {
+						uint32_t lo[4];
+						#pragma unroll
+						for (int s = 0; s < 4; ++s) lo[s] = Bf16Pair(Sub2(gg[s], WidenBf16Pair(hi[s])));
+						StoreShared16(dst+Sw64(row, 2+qpair), lo[0], lo[1], lo[2], lo[3]);
+					}
 				}
 			}
 		}
@@ -874,7 +955,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1) TangentTcFusedKernel(DeviceM
 			#pragma unroll
 			for (int tile = 0; tile < kTiles; ++tile) {
 				const uint32_t a = sA+tile*kTileBytes;
-				if (kSplit) {
+				if constexpr (kTf32) {
+					#pragma unroll
+					for (int ks = 0; ks < 2; ++ks)
+						MmaTf32(tmem+tile*64, DescSw64(a+ks*32), DescSw64(sB+ks*32), (c > 0 || ks > 0) ? 1u : 0u);
+				} else if (kSplit) {
 					MmaBf16(tmem+tile*64, DescSw64(a), DescSw64(sB), c > 0 ? 1u : 0u);
 					MmaBf16(tmem+tile*64, DescSw64(a), DescSw64(sB+32), 1u);
 					MmaBf16(tmem+tile*64, DescSw64(a+32), DescSw64(sB), 1u);
@@ -995,52 +1080,76 @@ void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const dou
 	LaunchCheck("TangentPointKernel");
 }
 
-void LaunchTangentTc(const DeviceMeshView& mesh, const float* phi32, const float* coef,
-	const int32_t* element_blocks, float* values, int* status, bool split, cudaStream_t stream)
+namespace {
+
+template <int kMode>
+void StartTangentTc(unsigned ctas, const DeviceMeshView& mesh, const float* phi32, const float* coef,
+	const int32_t* element_blocks, float* values, int* status, int lookahead, cudaStream_t stream)
 {
-	if (mesh.elements == 0) return;
 	static bool configured = false;
 	if (!configured) {
-		CudaCheck(cudaFuncSetAttribute(TangentTcKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			kTcSmemBytes), "tensor-core tangent shared-memory attribute");
-		CudaCheck(cudaFuncSetAttribute(TangentTcKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		CudaCheck(cudaFuncSetAttribute(TangentTcKernel<kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			kTcSmemBytes), "tensor-core tangent shared-memory attribute");
 		configured = true;
 	}
+	TangentTcKernel<kMode><<<ctas, kTcThreads, kTcSmemBytes, stream>>>(mesh, phi32, coef, element_blocks, values,
+		status, lookahead);
+}
+
+template <int kMode>
+void StartTangentTcFused(unsigned ctas, const DeviceMeshView& mesh, const double* phi, const double* qdata,
+	const double* point_state, AssemblyParams params, const int32_t* element_blocks, float* values, int* status,
+	int lookahead, cudaStream_t stream)
+{
+	static bool configured = false;
+	if (!configured) {
+		CudaCheck(cudaFuncSetAttribute(TangentTcFusedKernel<kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			kFusedSmemBytes), "fused tensor-core tangent shared-memory attribute");
+		configured = true;
+	}
+	TangentTcFusedKernel<kMode><<<ctas, kFusedThreads, kFusedSmemBytes, stream>>>(mesh, phi, qdata, point_state,
+		params, element_blocks, values, status, lookahead);
+}
+
+} // namespace
+
+void LaunchTangentTc(const DeviceMeshView& mesh, const float* phi32, const float* coef,
+	const int32_t* element_blocks, float* values, int* status, int operands, cudaStream_t stream)
+{
+	if (mesh.elements == 0) return;
 	const long long ctas = 2LL*mesh.elements;
 	if (ctas > 0x7fffffffLL) Fail(-7, "too many elements for one tangent launch");
 	const int lookahead = 2*MultiprocessorCount();            // two CTAs per SM
-	if (split)
-		TangentTcKernel<true><<<(unsigned)ctas, kTcThreads, kTcSmemBytes, stream>>>(mesh, phi32, coef,
-			element_blocks, values, status, lookahead);
+	if (operands == TC_OPERANDS_SPLIT)
+		StartTangentTc<kModeSplit>((unsigned)ctas, mesh, phi32, coef, element_blocks, values, status, lookahead, stream);
+	else if (operands == TC_OPERANDS_TF32)
+		StartTangentTc<kModeTf32>((unsigned)ctas, mesh, phi32, coef, element_blocks, values, status, lookahead, stream);
+	else if (operands == TC_OPERANDS_BF16)
+		StartTangentTc<kModeBf16>((unsigned)ctas, mesh, phi32, coef, element_blocks, values, status, lookahead, stream);
 	else
-		TangentTcKernel<false><<<(unsigned)ctas, kTcThreads, kTcSmemBytes, stream>>>(mesh, phi32, coef,
-			element_blocks, values, status, lookahead);
+		Fail(-1, "tensor-core tangent: unknown operand organisation");
 	LaunchCheck("TangentTcKernel");
 }
 
 void LaunchTangentTcFused(const DeviceMeshView& mesh, const double* phi, const double* qdata,
 	const double* point_state, AssemblyParams params, const int32_t* element_blocks, float* values, int* status,
-	bool split, cudaStream_t stream)
+	int operands, cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
-	static bool configured = false;
-	if (!configured) {
-		CudaCheck(cudaFuncSetAttribute(TangentTcFusedKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			kFusedSmemBytes), "fused tensor-core tangent shared-memory attribute");
-		CudaCheck(cudaFuncSetAttribute(TangentTcFusedKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			kFusedSmemBytes), "fused tensor-core tangent shared-memory attribute");
-		configured = true;
-	}
 	const long long ctas = 2LL*mesh.elements;
 	if (ctas > 0x7fffffffLL) Fail(-7, "too many elements for one tangent launch");
 	const int lookahead = MultiprocessorCount();              // one CTA per SM
-	if (split)
-		TangentTcFusedKernel<true><<<(unsigned)ctas, kFusedThreads, kFusedSmemBytes, stream>>>(mesh, phi, qdata,
-			point_state, params, element_blocks, values, status, lookahead);
+	if (operands == TC_OPERANDS_SPLIT)
+		StartTangentTcFused<kModeSplit>((unsigned)ctas, mesh, phi, qdata, point_state, params, element_blocks, values,
+			status, lookahead, stream);
+	else if (operands == TC_OPERANDS_TF32)
+		StartTangentTcFused<kModeTf32>((unsigned)ctas, mesh, phi, qdata, point_state, params, element_blocks, values,
+			status, lookahead, stream);
+	else if (operands == TC_OPERANDS_BF16)
+		StartTangentTcFused<kModeBf16>((unsigned)ctas, mesh, phi, qdata, point_state, params, element_blocks, values,
+			status, lookahead, stream);
 	else
-		TangentTcFusedKernel<false><<<(unsigned)ctas, kFusedThreads, kFusedSmemBytes, stream>>>(mesh, phi, qdata,
-			point_state, params, element_blocks, values, status, lookahead);
+		Fail(-1, "fused tensor-core tangent: unknown operand organisation");
 	LaunchCheck("TangentTcFusedKernel");
 }
 
