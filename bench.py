@@ -214,7 +214,10 @@ def step_dt(name):
 # rel.res 1e-10 its mixed and FP64 arms accepted states up to 2.3e-8 apart in pressure (traction-free
 # outlets, 600k elements).  Its coarse level has 1,762 point blocks (7,048 unknowns), whose dense inverse
 # took 19% of the step when rebuilt every third refresh (0.3% every ninth); the tube batch is as large.
-NEWTON_RTOL = {"c4": 1e-11}
+# The tube batch tests every tube against its own first residual (per-tube Newton tests); at 1e-10 the
+# smallest tubes' targets fell below what the union's FGMRES (FP32 Jacobian) can still resolve, and a
+# linear solve stagnated at 3e-10, so the batch runs at the metric's rel.res 1e-8.
+NEWTON_RTOL = {"c4": 1e-11, "c5": 1e-8}
 COARSE_PERIOD = {"c4": 9, "c5": 9}
 
 
