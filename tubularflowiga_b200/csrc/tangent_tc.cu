@@ -333,9 +333,10 @@ __device__ __forceinline__ void PointCoefficients(const PointState& S, const dou
 enum : int { kPointResidual = 0, kPointCoefficients = 1, kPointState = 2 };
 
 // Persistent: each CTA takes elements from a work queue (*queue, zeroed by the launcher) one at a time,
-// claiming its next element while it works on the current one, and prefetches the element's basis table
-// into L2 as it starts on it.  (Prefetching the next element's table as well doubled the tables live in
-// L2 and made the kernel 1.6 times slower: 31 against 19 ms on the 199,800-element Y-bifurcation.)
+// claiming its next element while it works on the current one.  No L2 prefetch: prefetching the next
+// element's table doubled the tables live in L2 (31 against 19 ms per launch on the 199,800-element
+// Y-bifurcation), and prefetching the current one as the CTA starts on it only raced the CTA's own
+// loads (22 ms).
 template <int kMode>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ state,
@@ -353,15 +354,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 	__shared__ int next;
 
 	const int tid = threadIdx.x;
-	constexpr uint32_t kTableBytes = kFeatures*kQuad*kMaxBasis*8;
 	if (tid == 0) next = atomicAdd(queue, 1);
 	__syncthreads();
 	for (int e = next; e < mesh.elements; e = next) {
 	__syncthreads();                                 // every thread has read next
-	if (tid == 0) {
-		next = atomicAdd(queue, 1);
-		PrefetchL2(phi+(size_t)e*kFeatures*kQuad*kMaxBasis, kTableBytes);
-	}
+	if (tid == 0) next = atomicAdd(queue, 1);
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
