@@ -206,6 +206,31 @@ __global__ void __launch_bounds__(kThreads) UpdateDotKernel(const B* __restrict_
 	}
 }
 
+// y += sum_k coef_k (g_k . x) g_k over sparse g_k; one CTA, outlets in turn (indices are distinct
+// within an outlet, so the scatter needs no atomics).
+__global__ void __launch_bounds__(kThreads) LowRankKernel(int count, const int* __restrict__ ptr,
+	const int* __restrict__ idx, const double* __restrict__ val, const double* __restrict__ coef,
+	const double* __restrict__ x, double* __restrict__ y, const int* __restrict__ stop)
+{
+	if (stop && *stop) return;
+	__shared__ double part[kWarps];
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	for (int k = 0; k < count; ++k) {
+		const int lo = ptr[k], hi = ptr[k+1];
+		double s = 0.0;
+		for (int j = lo+threadIdx.x; j < hi; j += blockDim.x) s = fma(val[j], x[idx[j]], s);
+		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+		if (lane == 0) part[warp] = s;
+		__syncthreads();
+		double dot = 0.0;
+		#pragma unroll
+		for (int w = 0; w < kWarps; ++w) dot += part[w];
+		const double scale = coef[k]*dot;
+		for (int j = lo+threadIdx.x; j < hi; j += blockDim.x) y[idx[j]] += scale*val[j];
+		__syncthreads();
+	}
+}
+
 // Column j of the Hessenberg matrix: norm, previous rotations, new rotation,
 // residual estimate (Gmres.hpp:272-305).  One warp stages the column and the
 // rotations in shared memory; lane 0 then applies the rotations sequentially.
@@ -358,6 +383,13 @@ double ArnoldiBytes(long long n, int used, int basis_bytes, bool flexible)
 }
 
 } // namespace
+
+void Gmres::AddLowRank(const double* x, double* y, const int* stop)
+{
+	LowRankKernel<<<1, kThreads, 0, stream_>>>(low_.count, low_.ptr, low_.idx, low_.val, low_.coef, x, y, stop);
+	LaunchCheck("LowRankKernel");
+	launches_ += 1;
+}
 
 Gmres::Gmres(int nodes, int restart, cudaStream_t stream, int fields)
 	: nodes_(nodes), fields_(fields), n_(fields*nodes), restart_(restart), blocks_(kBlocks), stream_(stream)
@@ -545,6 +577,7 @@ void Gmres::FlexibleStep(const DevicePatternView& pattern, const T* values, int 
 	}
 	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
 	LaunchSpmvBlockJacobi<T>(pattern, values, nullptr, z, nullptr, w_.get(), stop, stream_);
+	if (low_on_) AddLowRank(z, w_.get(), stop);
 	if (profiler_) profiler_->End(stream_);
 	launches_ += 1;
 	if (collector_ != nullptr && j%kBatch == 0) {
@@ -565,6 +598,7 @@ double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const T* value
 	// v_0 = b - A x (FP64), stored in the basis precision; beta from the FP64 vector
 	if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
 	LaunchSpmv<T>(pattern, values, x, tmp_.get(), stream_);
+	if (low_on_) AddLowRank(x, tmp_.get(), nullptr);
 	double* r = std::is_same<B, double>::value ? V_.get() : r_.get();
 	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), r);
 	LaunchCheck("ResidualKernel");

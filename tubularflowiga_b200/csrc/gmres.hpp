@@ -62,6 +62,15 @@ public:
 	// Stores a training pair (w_j = A z_j) into `collector` on every eighth iteration (null: off).
 	void set_collector(LearnedPreconditioner* collector) { collector_ = collector; }
 	void set_profiler(Profiler* profiler) { profiler_ = profiler; }
+	// Low-rank term of the flexible solve's operator, A + sum_k c_k g_k g_k^T with each g_k a sparse
+	// vector (entries ptr[k] .. ptr[k+1] of idx / val, distinct indices per k): the outlet coupling's
+	// share of the Newton Jacobian.  Null: off.
+	struct LowRank { int count; const int* ptr; const int* idx; const double* val; const double* coef; };
+	void set_low_rank(const LowRank* term)
+	{
+		low_on_ = term != nullptr && term->count > 0;
+		if (low_on_) low_ = *term;
+	}
 	std::size_t bytes() const;
 
 private:
@@ -106,6 +115,10 @@ private:
 	HostStatus* host_ = nullptr;
 	Profiler* profiler_ = nullptr;
 	double tolerance_ = 0.0;                 // absolute residual target of the current solve
+	bool low_on_ = false;
+	LowRank low_{};
+	// y += sum_k c_k (g_k . x) g_k (skipped when *stop; stop may be null).
+	void AddLowRank(const double* x, double* y, const int* stop);
 	LearnedPreconditioner* learned_ = nullptr;
 	LearnedPreconditioner* collector_ = nullptr;
 	DeviceArray<double> pair_dinv_, pair_amg_, pair_aamg_;

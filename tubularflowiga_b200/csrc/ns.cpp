@@ -140,6 +140,7 @@ void NsSolver::SetDirichlet(const int32_t* vmask, const int32_t* pmask, const do
 	dirichlet_set_ = true;
 	tangent_valid_ = false;
 	amg_current_ = false;
+	lr_dirty_ = true;
 }
 
 void NsSolver::SetDirichletValues(const double* velocity, const double* pressure)
@@ -830,10 +831,35 @@ tfiga_step_report NsSolver::StepOutletsCoupled(tfiga_outlet* outlets, int count,
 	if (!faces.empty()) face_base_.Upload(base.data(), base.size(), stream_);
 	outlet_updates_.Zero(stream_);
 	CudaCheck(cudaStreamSynchronize(stream_), "outlet upload");
+	// The coupling's share of the Newton Jacobian: the residual carries P_k(Q_k(u)) g_k with
+	// Q_k = g_k . u the outward flow of outlet k (g_k the face coefficients of its label on the free
+	// velocity unknowns), so its derivative is sum_k dP_k/dQ_k g_k g_k^T, with dP/dQ = relaxation x
+	// (R | 1 / (C/dt + 1/R) | R1 + 1 / (C/dt + 1/R2)) for the resistance / RC / RCR models.  The flexible
+	// GMRES applies it next to the SpMV, so Newton converges on the coupled system instead of lagging
+	// the pressures one iteration behind.
+	std::vector<int32_t> lr_labels;
+	std::vector<double> lr_coef;
+	for (int i = 0; i < count; ++i) {
+		if (host[i].slot < 0) continue;
+		const DeviceOutlet& d = host[i];
+		double dpdq = 0.0;
+		if (d.kind == TFIGA_OUTLET_RESISTANCE) dpdq = d.resistance;
+		else if (d.kind == TFIGA_OUTLET_RC) dpdq = 1.0/(d.capacitance/params_.dt+1.0/d.resistance);
+		else dpdq = d.proximal+1.0/(d.capacitance/params_.dt+1.0/d.distal);
+		lr_labels.push_back(outlets[i].label);
+		lr_coef.push_back(relaxation*dpdq);
+	}
+	if (amg_ && !lr_labels.empty()) {
+		if (lr_dirty_ || lr_labels != lr_labels_) BuildOutletFlowVectors(lr_labels);
+		lr_coef_.Upload(lr_coef.data(), lr_coef.size(), stream_);
+		const Gmres::LowRank term{(int)lr_labels.size(), lr_ptr_.get(), lr_idx_.get(), lr_val_.get(), lr_coef_.get()};
+		gmres_.set_low_rank(&term);
+	}
 	struct Deactivate {
 		int& count;
-		~Deactivate() { count = -1; }
-	} deactivate{outlet_count_};
+		Gmres& gmres;
+		~Deactivate() { count = -1; gmres.set_low_rank(nullptr); }
+	} deactivate{outlet_count_, gmres_};
 	outlet_count_ = count;
 	outlet_relaxation_ = relaxation;
 	outlet_iteration_ = 0;
@@ -871,6 +897,47 @@ tfiga_step_report NsSolver::StepOutletsCoupled(tfiga_outlet* outlets, int count,
 	read_back(false);
 	Fail(-6, "Navier-Stokes nonlinear solve with coupled outlets reached MAX_NEWTON (nonlinear_residual="
 		+Precise(last.residual_l2)+", relative_mass_imbalance="+Precise(last.relative_mass_imbalance)+")");
+}
+
+void NsSolver::BuildOutletFlowVectors(const std::vector<int32_t>& labels)
+{
+	const auto& faces = mesh_.faces();
+	const int64_t n = nodes();
+	std::vector<int32_t> vm(n);
+	vmask_.Download(vm.data(), n, stream_);
+	std::vector<int32_t> ptr{0}, idx;
+	std::vector<double> val, g(n4_);
+	std::vector<double> fp(faces.size());
+	for (const int32_t label : labels) {
+		// -F per unknown for a unit pressure on the label's faces (the traction kernel), i.e. -g
+		for (size_t f = 0; f < faces.size(); ++f) fp[f] = faces[f].label == label ? 1.0 : 0.0;
+		face_pressure_.Upload(fp.data(), fp.size(), stream_);
+		update_.Zero(stream_);
+		LaunchFaceTraction((int)faces.size(), mesh_.face_element(), mesh_.face_coef(), mesh_.face_stride(),
+			mesh_.view().element_offsets, mesh_.view().connectivity, face_pressure_.get(), update_.get(), stream_);
+		launches_ += 1;
+		update_.Download(g.data(), n4_, stream_);
+		CudaCheck(cudaStreamSynchronize(stream_), "outlet flow vector");
+		for (int64_t i = 0; i < n; ++i) {
+			if (vm[i]) continue;                              // Dirichlet velocity: no update, no flow change
+			for (int c = 0; c < 3; ++c)
+				if (g[4*i+c] != 0.0) { idx.push_back((int32_t)(4*i+c)); val.push_back(-g[4*i+c]); }
+		}
+		ptr.push_back((int32_t)idx.size());
+	}
+	lr_ptr_.Allocate(ptr.size());
+	lr_ptr_.Upload(ptr.data(), ptr.size(), stream_);
+	lr_idx_.Allocate(std::max<size_t>(1, idx.size()));
+	lr_val_.Allocate(std::max<size_t>(1, val.size()));
+	if (!idx.empty()) {
+		lr_idx_.Upload(idx.data(), idx.size(), stream_);
+		lr_val_.Upload(val.data(), val.size(), stream_);
+	}
+	lr_coef_.Allocate(labels.size());
+	// (the face pressures are rebuilt from the outlet pressures before every coupled residual)
+	CudaCheck(cudaStreamSynchronize(stream_), "outlet flow vectors");
+	lr_labels_ = labels;
+	lr_dirty_ = false;
 }
 
 void NsSolver::BoundaryFlows(const int32_t* labels, int count, double* flows)

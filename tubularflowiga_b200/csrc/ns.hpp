@@ -173,6 +173,13 @@ private:
 	DeviceArray<int32_t> slot_outlet_, outlet_updates_;
 	DeviceArray<double> face_base_;
 	int outlet_count_ = -1;
+	// outward-flow vectors of the coupled outlets (sparse, on the free velocity unknowns) and their
+	// Jacobian coefficients dP/dQ, for the flexible GMRES's low-rank term
+	DeviceArray<int32_t> lr_ptr_, lr_idx_;
+	DeviceArray<double> lr_val_, lr_coef_;
+	std::vector<int32_t> lr_labels_;
+	bool lr_dirty_ = true;
+	void BuildOutletFlowVectors(const std::vector<int32_t>& labels);
 	int outlet_iteration_ = 0;
 	double outlet_relaxation_ = 1.0;
 	bool last_outlet_ok_ = false;
