@@ -213,12 +213,12 @@ def test_mixed_newton_converges_to_fp64_solution(api, cylinder_1280):
     assert rel(states["mixed"][:, 3], states["fp64"][:, 3]) < 1e-8
 
 
-def test_split_transient_steps_match_fp64_on_the_pulsatile_section(api):
+def test_mixed_transient_steps_match_fp64_on_the_pulsatile_section(api):
     """The 12,800-element section of the pulsatile tube (C2's cross-section and Fourier inflow, 100 layers),
     four backward-Euler steps at dt 2e-3 with the bench's solver settings (Newton rel.res 1e-10 on the FP64
     residual, Eisenstat-Walker linear tolerances, tangent reuse factor 100, AMG-FGMRES(64)): the split-BF16
-    mixed solver and the FP64 solver from the same state with the same Dirichlet sequence agree within
-    1e-8 relative L2 on velocity and on pressure after every step."""
+    and the plain-BF16 mixed solvers and the FP64 solver from the same state with the same Dirichlet
+    sequence agree within 1e-8 relative L2 on velocity and on pressure after every step."""
     import bench
     tube, _, wave = bench.workload("c2-100")
     mesh = api.Mesh(tube.mesh)
@@ -226,7 +226,7 @@ def test_split_transient_steps_match_fp64_on_the_pulsatile_section(api):
     dt = 2e-3
     s0 = api.initial_state(vmask, velocity_at(0.0))
     trajectories = {}
-    for name, precision in (("fp64", api.FP64), ("split", api.MIXED_BF16X3)):
+    for name, precision in (("fp64", api.FP64), ("split", api.MIXED_BF16X3), ("bf16", api.MIXED)):
         ns = api.NavierStokes(mesh, precision=precision, density=1060.0, viscosity=3.5e-3, dt=dt,
                               nonlinear_rtol=1e-10, nonlinear_atol=1e-300, mass_rtol=1e-3, gmres_restart=64,
                               gmres_max_iterations=5000, gmres_rtol=1e-8, preconditioner=api.AMG,
@@ -242,7 +242,8 @@ def test_split_transient_steps_match_fp64_on_the_pulsatile_section(api):
             states.append(ns.get_state().reshape(-1, 4))
         ns.close()
         trajectories[name] = states
-    for k, (a, b) in enumerate(zip(trajectories["split"], trajectories["fp64"])):
-        ev, ep = rel(a[:, :3], b[:, :3]), rel(a[:, 3], b[:, 3])
-        print(f"step {k + 1}: split vs FP64 velocity {ev:.3e} pressure {ep:.3e}")
-        assert ev < 1e-8 and ep < 1e-8
+    for name in ("split", "bf16"):
+        for k, (a, b) in enumerate(zip(trajectories[name], trajectories["fp64"])):
+            ev, ep = rel(a[:, :3], b[:, :3]), rel(a[:, 3], b[:, 3])
+            print(f"step {k + 1}: {name} vs FP64 velocity {ev:.3e} pressure {ep:.3e}")
+            assert ev < 1e-8 and ep < 1e-8

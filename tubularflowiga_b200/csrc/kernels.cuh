@@ -165,10 +165,10 @@ void LaunchSegmentSums(int segments, const int32_t* segment_of, int items, const
 	cudaStream_t stream);
 
 // Independent segments of a vector (the tubes of a batched mesh, in entries): out[k] = sum of x^2 over
-// [offsets[k], offsets[k+1]); and x = 0 on every segment whose flag is set.
+// [offsets[k], offsets[k+1]).
 void LaunchSegmentSquares(int segments, const int64_t* offsets, const double* x, double* out, cudaStream_t stream);
-void LaunchZeroFlaggedSegments(int segments, const int64_t* offsets, const int32_t* flag, double* x,
-	cudaStream_t stream);
+// x *= scale[k] over each segment k (0 clears it).
+void LaunchScaleSegments(int segments, const int64_t* offsets, const double* scale, double* x, cudaStream_t stream);
 
 int PartialSlots();
 

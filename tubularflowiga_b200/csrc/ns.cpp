@@ -556,12 +556,12 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 	const double scale = std::sqrt((double)n4_);
 	report.tolerance = std::max(params_.nonlinear_atol*scale, params_.nonlinear_rtol*initial);
 	bool residual_ok = norm <= report.tolerance;
-	double active_tolerance = report.tolerance;      // tightest test still open (forcing floor)
+	double floor_ratio = report.tolerance/norm;       // reduction the open Newton tests still ask for
 	if (segments_) {
 		// per-segment Newton tests; a segment that passed stays frozen for the rest of the step
 		if (initial_residual < 0.0) std::fill(segment_done_host_.begin(), segment_done_host_.end(), 0);
 		residual_ok = true;
-		active_tolerance = std::numeric_limits<double>::infinity();
+		floor_ratio = std::numeric_limits<double>::infinity();
 		for (int k = 0; k < segments_; ++k) {
 			segment_norm_[k] = std::sqrt(pinned_segments_[k]);
 			if (initial_residual < 0.0) segment_initial_[k] = segment_norm_[k];
@@ -570,20 +570,29 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 			if (segment_norm_[k] <= tol) segment_done_host_[k] = 1;
 			if (!segment_done_host_[k]) {
 				residual_ok = false;
-				active_tolerance = std::min(active_tolerance, tol);
+				floor_ratio = std::min(floor_ratio, tol/segment_norm_[k]);
 			}
 		}
-		if (!std::isfinite(active_tolerance)) active_tolerance = report.tolerance;
+		if (!std::isfinite(floor_ratio)) floor_ratio = report.tolerance/norm;
 	}
 	if (residual_ok && d.imbalance <= params_.mass_rtol) {
 		report.converged = 1;
 		return report;
 	}
 	if (segments_) {
-		// frozen segments take no update: their rhs rows vanish before the linear solve
+		// Frozen segments take no update: their rhs rows vanish before the linear solve.  Each open
+		// segment's rhs is scaled to unit norm, so that the union's Krylov solve weighs every segment
+		// alike instead of resolving the small ones only to the large ones' absolute accuracy; the
+		// Jacobian is block diagonal over the segments, so a segment's solution scales by the same
+		// factor and is scaled back after the solve.
+		for (int k = 0; k < segments_; ++k) {
+			const bool open = !segment_done_host_[k] && segment_norm_[k] > 0.0;
+			segment_scale_host_[k] = open ? 1.0/segment_norm_[k] : 0.0;
+			segment_scale_host_[segments_+k] = open ? segment_norm_[k] : 0.0;
+		}
 		profiler_.Begin(Profiler::kVector, stream_);
-		segment_done_.Upload(segment_done_host_.data(), segments_, stream_);
-		LaunchZeroFlaggedSegments(segments_, segment_entries_.get(), segment_done_.get(), rhs_.get(), stream_);
+		segment_scale_.Upload(segment_scale_host_.data(), 2*segments_, stream_);
+		LaunchScaleSegments(segments_, segment_entries_.get(), segment_scale_.get(), rhs_.get(), stream_);
 		profiler_.End(stream_);
 		launches_ += 1;
 	}
@@ -617,16 +626,24 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 		constexpr double kEtaMax = 1e-3;
 		if (initial_residual < 0.0) eta = kEtaMax;
 		else {
-			const double ratio = norm/forcing_norm_;
+			// with segments, the slowest-contracting open segment's ratio (each is solved at unit scale)
+			double ratio = norm/forcing_norm_;
+			if (segments_) {
+				ratio = 0.0;
+				for (int k = 0; k < segments_; ++k)
+					if (!segment_done_host_[k] && segment_forcing_[k] > 0.0)
+						ratio = std::max(ratio, segment_norm_[k]/segment_forcing_[k]);
+			}
 			eta = 0.9*ratio*ratio;
 			const double safeguard = 0.9*forcing_eta_*forcing_eta_;
 			if (safeguard > 0.1) eta = std::max(eta, safeguard);
 			eta = std::min(eta, kEtaMax);
 		}
 		eta = std::max(eta, params_.gmres_rtol);
-		eta = std::max(eta, std::min(0.1, 0.5*active_tolerance/norm));
+		eta = std::max(eta, std::min(0.1, 0.5*floor_ratio));
 		forcing_norm_ = norm;
 		forcing_eta_ = eta;
+		if (segments_) segment_forcing_ = segment_norm_;
 	}
 	reuse_eta_ = eta;
 	const GmresResult linear = SolveLinear(eta, params_.gmres_max_iterations);
@@ -652,6 +669,10 @@ tfiga_newton_report NsSolver::NewtonIteration(double initial_residual)
 		launches_ += 6;
 	}
 	profiler_.Begin(Profiler::kVector, stream_);
+	if (segments_) {
+		LaunchScaleSegments(segments_, segment_entries_.get(), segment_scale_.get()+segments_, update_.get(), stream_);
+		launches_ += 1;
+	}
 	LaunchNorm(n4_, update_.get(), partial_.get(), scalars_.get()+kUpdateNorm, stream_);
 	LaunchAxpy(n4_, 1.0, update_.get(), state_.get(), stream_);
 	profiler_.End(stream_);
@@ -975,8 +996,10 @@ void NsSolver::SetSegments(const int64_t* node_offsets, int count)
 	segment_entries_.Allocate(count+1);
 	segment_entries_.Upload(entries.data(), count+1, stream_);
 	segment_sq_.Allocate(count);
-	segment_done_.Allocate(count);
+	segment_scale_.Allocate(2*(size_t)count);
+	segment_scale_host_.assign(2*(size_t)count, 0.0);
 	segment_initial_.assign(count, 0.0);
+	segment_forcing_.assign(count, 0.0);
 	segment_norm_.assign(count, 0.0);
 	segment_done_host_.assign(count, 0);
 	if (pinned_segments_) cudaFreeHost(pinned_segments_);

@@ -52,7 +52,8 @@ public:
 	// increasing from 0 to nodes; count 0 removes them.  With segments the Newton test is taken per
 	// segment -- ||r_k|| <= max(atol sqrt(4 n_k), rtol ||r_k,0||) with r_k,0 the segment's residual at
 	// the step's first iteration -- and a segment that passes is frozen: its rhs rows are zeroed before
-	// each later linear solve, so its update is zero (the system is block diagonal over the segments).
+	// each later linear solve, so its update is zero (the system is block diagonal over the segments),
+	// and each open segment's rhs is scaled to unit norm for the solve (its update scaled back after).
 	// The step converges when every segment passes (and the mass test holds).
 	void SetSegments(const int64_t* node_offsets, int count);
 	// After a Newton iteration: per segment 1 if it has passed its test in this step, and its residual.
@@ -147,7 +148,7 @@ private:
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
 	DeviceArray<float> values32_;
-	DeviceArray<float> coef32_;              // tensor-core tangent: point coefficients [e][4][80][64]
+	DeviceArray<float> coef32_;              // tensor-core tangent: point coefficients [e][4][16][80][4]
 	DeviceArray<double> point_state_;        // fused tensor-core tangent: FP64 point state [e][64][22]
 	int tangent_kernel_ = 0;                 // TFIGA_TANGENT_* in use
 	double tune_ms_[2] = {0.0, 0.0};         // autotuner: coefficient-array and fused tangent times
@@ -186,11 +187,12 @@ private:
 	// segments (SetSegments)
 	int segments_ = 0;
 	std::vector<int64_t> segment_nodes_;
-	std::vector<double> segment_initial_, segment_norm_;
+	std::vector<double> segment_initial_, segment_norm_, segment_forcing_;
 	std::vector<int32_t> segment_done_host_;
 	DeviceArray<int64_t> segment_entries_;
 	DeviceArray<double> segment_sq_;
-	DeviceArray<int32_t> segment_done_;
+	DeviceArray<double> segment_scale_;      // [rhs scale of each segment][update scale of each segment]
+	std::vector<double> segment_scale_host_;
 	double* pinned_segments_ = nullptr;
 };
 

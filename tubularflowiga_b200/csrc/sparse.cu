@@ -268,15 +268,17 @@ __global__ void __launch_bounds__(256) SegmentSquaresKernel(const int64_t* __res
 	if (threadIdx.x == 0) out[blockIdx.x] = sq;
 }
 
-// x[i] = 0 on the segments k whose flag[k] is set.
-__global__ void ZeroFlaggedSegmentsKernel(int segments, const int64_t* __restrict__ offsets,
-	const int32_t* __restrict__ flag, double* __restrict__ x)
+// x[i] *= scale[k] over segment k's entries (scale 0 clears the segment).
+__global__ void ScaleSegmentsKernel(int segments, const int64_t* __restrict__ offsets,
+	const double* __restrict__ scale, double* __restrict__ x)
 {
 	const int k = blockIdx.y;
-	if (k >= segments || !flag[k]) return;
+	if (k >= segments) return;
+	const double s = scale[k];
+	if (s == 1.0) return;
 	const int64_t lo = offsets[k], hi = offsets[k+1];
 	for (long long i = lo+(long long)blockIdx.x*blockDim.x+threadIdx.x; i < hi; i += (long long)gridDim.x*blockDim.x)
-		x[i] = 0.0;
+		x[i] = s == 0.0 ? 0.0 : s*x[i];
 }
 
 int PartialSlots() { return 2*kReduceBlocks; }
@@ -434,12 +436,11 @@ void LaunchSegmentSquares(int segments, const int64_t* offsets, const double* x,
 	LaunchCheck("SegmentSquaresKernel");
 }
 
-void LaunchZeroFlaggedSegments(int segments, const int64_t* offsets, const int32_t* flag, double* x,
-	cudaStream_t stream)
+void LaunchScaleSegments(int segments, const int64_t* offsets, const double* scale, double* x, cudaStream_t stream)
 {
 	if (segments == 0) return;
-	ZeroFlaggedSegmentsKernel<<<dim3(16, segments), 256, 0, stream>>>(segments, offsets, flag, x);
-	LaunchCheck("ZeroFlaggedSegmentsKernel");
+	ScaleSegmentsKernel<<<dim3(16, segments), 256, 0, stream>>>(segments, offsets, scale, x);
+	LaunchCheck("ScaleSegmentsKernel");
 }
 
 void LaunchAxpy(long long n, double alpha, const double* x, double* y, cudaStream_t stream)
