@@ -748,6 +748,9 @@ def main():
                     help="mixed: BF16 tensor-core tangent; bf16x3: split BF16 (hi + lo, three products); "
                          "tf32: TF32 operands; fp64: the FP64 solver alone")
     ap.add_argument("--no-fp64-leg", action="store_true")
+    ap.add_argument("--krylov-operator", default="fp32", choices=["fp32", "bf16"],
+                    help="storage of the Jacobian the flexible GMRES applies (reduced-precision modes): the FP32 "
+                         "assembly, or a BF16 copy of it (half the SpMV's matrix traffic)")
     ap.add_argument("--tangent-kernel", default="auto", choices=["auto", "coefficients", "fused"],
                     help="tensor-core tangent organisation (auto: the autotuner times both on the first tangent)")
     ap.add_argument("--learned", type=int, default=0,
@@ -823,7 +826,8 @@ def main():
                      amg_coarse_period=args.amg_coarse_period, krylov_fp64_basis=int(args.krylov_fp64_basis),
                      newton_forcing=int(args.forcing == "ew"), tangent_reuse_factor=args.tangent_reuse,
                      tangent_kernel={"auto": api.TANGENT_AUTO, "coefficients": api.TANGENT_COEFFICIENTS,
-                                     "fused": api.TANGENT_FUSED}[args.tangent_kernel])
+                                     "fused": api.TANGENT_FUSED}[args.tangent_kernel],
+                     krylov_bf16_operator=int(args.krylov_operator == "bf16"))
     precision = {"mixed": api.MIXED, "bf16x3": api.MIXED_BF16X3, "tf32": api.MIXED_TF32,
                  "fp64": api.FP64}[args.precision]
     ns = api.NavierStokes(mesh, precision=precision, **solver_kw)
@@ -1089,8 +1093,8 @@ def main():
     res_ms, res_n = prof.get("residual", (0.0, 0))
     kernels = {}
     if mixed:
-        # FP32 Jacobian: 4-byte values in every pass over the matrix
-        b_spmv -= mesh.blocks * 16 * 4
+        # FP32 Jacobian: 4-byte values in every pass over the matrix (2-byte with the BF16 copy)
+        b_spmv -= mesh.blocks * 16 * (6 if args.krylov_operator == "bf16" else 4)
     spmv_bytes = b_spmv if amg else b_spmv + b_bjac
     spmv_name = "spmv" if amg else "spmv_block_jacobi"
     if spmv_n:
@@ -1197,6 +1201,7 @@ def main():
                                                                                    else "") if amg else
                                "block-Jacobi GMRES(%d) rtol 1e-8" % args.restart)),
                    "newton_rtol": args.newton_rtol, "amg_coarse_period": args.amg_coarse_period,
+                   "krylov_operator": args.krylov_operator if mixed else "fp64",
                    "l2": "inputs larger than L2 (matrix %.2f GB)" % (mesh.blocks * 128 / 1e9),
                    "parallelism": "replicas only" if world > 1 else "single GPU"},
         "newton_per_step": float(newton), "linear_iterations_per_newton": float(linear),

@@ -146,6 +146,12 @@ typedef struct tfiga_ns_params {
 	 * the first one is free) and keeps the faster; the fused one otherwise.
 	 * Both give the same tangent up to the order of the FP32 additions. */
 	int32_t tangent_kernel;        /* default TFIGA_TANGENT_AUTO */
+	/* Reduced-precision modes: 1 keeps a BF16 copy of the FP32 Jacobian (rounded to
+	 * nearest even after each assembly) and applies it in the flexible GMRES's
+	 * products and true residuals, halving the SpMV's matrix traffic; the AMG keeps the
+	 * FP32 values.  The Newton residual stays FP64, so only the Newton convergence
+	 * rate can change.  Ignored in TFIGA_PRECISION_FP64. */
+	int32_t krylov_bf16_operator;  /* default 0 */
 } tfiga_ns_params;
 
 #define TFIGA_PRECISION_FP64 0

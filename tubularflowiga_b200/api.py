@@ -43,7 +43,8 @@ class NsParams(C.Structure):
                 ("gmres_rtol", C.c_double), ("preconditioner", C.c_int32), ("precision", C.c_int32),
                 ("amg_coarse_nodes", C.c_int32), ("amg_coarse_period", C.c_int32),
                 ("krylov_fp64_basis", C.c_int32), ("newton_forcing", C.c_int32),
-                ("tangent_reuse_factor", C.c_double), ("tangent_kernel", C.c_int32)]
+                ("tangent_reuse_factor", C.c_double), ("tangent_kernel", C.c_int32),
+                ("krylov_bf16_operator", C.c_int32)]
 
 
 TANGENT_AUTO = 0

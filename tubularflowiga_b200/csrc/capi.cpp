@@ -241,6 +241,7 @@ void tfiga_ns_default_params(tfiga_ns_params* p)
 	p->newton_forcing = 0;
 	p->tangent_reuse_factor = 0.0;
 	p->tangent_kernel = TFIGA_TANGENT_AUTO;
+	p->krylov_bf16_operator = 0;
 }
 
 int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out)

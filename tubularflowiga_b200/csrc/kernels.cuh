@@ -113,6 +113,8 @@ template <class T>
 void LaunchBlockInverse(const DevicePatternView& pattern, const T* values, double* inverse,
 	unsigned int* singular, cudaStream_t stream);
 void LaunchToFloat(long long n, const double* in, float* out, cudaStream_t stream);
+// out = BF16(in) (round to nearest even), stored as raw 16-bit patterns.
+void LaunchToBf16(long long n, const float* in, uint16_t* out, cudaStream_t stream);
 // FP32 copy of basis tables [table][64 points][64 functions] (FP64) with the points of each pair
 // interleaved: out[table][point pair][function][2] (the tensor-core tangent's staging layout).
 void LaunchToFloatPointPairs(long long tables, const double* in, float* out, cudaStream_t stream);

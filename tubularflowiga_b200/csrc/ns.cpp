@@ -82,6 +82,12 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 	if (mixed() && params.preconditioner != TFIGA_PRECONDITIONER_AMG)
 		Fail(-7, "mixed precision requires the AMG-preconditioned flexible GMRES");
 	if (mixed()) values32_.Allocate((size_t)blocks()*16);
+	if (params.krylov_bf16_operator != 0 && params.krylov_bf16_operator != 1)
+		Fail(-1, "krylov_bf16_operator must be 0 or 1");
+	if (mixed() && params.krylov_bf16_operator) {
+		values16_.Allocate((size_t)blocks()*16);
+		gmres_.set_operator16(values16_.get());
+	}
 	if (params.tangent_kernel != TFIGA_TANGENT_AUTO && params.tangent_kernel != TFIGA_TANGENT_COEFFICIENTS
 		&& params.tangent_kernel != TFIGA_TANGENT_FUSED)
 		Fail(-1, "unknown tangent_kernel "+std::to_string(params.tangent_kernel));
@@ -449,6 +455,10 @@ GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 			if (mixed()) {
 				if (!amg_->built()) amg_->Build(values32_.get());
 				amg_->Refresh(values32_.get(), coarse);
+				if (values16_.size()) {
+					LaunchToBf16((long long)blocks()*16, values32_.get(), values16_.get(), stream_);
+					launches_ += 1;
+				}
 			} else {
 				if (!amg_->built()) amg_->Build(values_.get());
 				amg_->Refresh(values_.get(), coarse);

@@ -148,6 +148,7 @@ private:
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
 	DeviceArray<float> values32_;
+	DeviceArray<uint16_t> values16_;         // BF16 copy of values32_ for the Krylov products (optional)
 	DeviceArray<float> coef32_;              // tensor-core tangent: point coefficients [e][4][16][80][4]
 	DeviceArray<double> point_state_;        // fused tensor-core tangent: FP64 point state [e][64][22]
 	int tangent_kernel_ = 0;                 // TFIGA_TANGENT_* in use

@@ -12,16 +12,17 @@
 // B = Psi (K-major), one GEMM of M = 512 x N = 64 x K = 256 per row field.
 //
 // Two kernels.
-//   TangentPointKernel (FP64, CTA per element, 256 threads): nodal state, the
-//     state at the 64 points (thread per point and quarter of the basis, the
-//     quarters summed in shared memory), the coefficients M_q of all four row
-//     fields (thread per row field and point, two column-field halves through
-//     a shared-memory scratch) written to a coefficient array laid out
-//     [element][row field][16 point quads][80 coefficients][4 points] (a K
-//     chunk's coefficients of one row field are one contiguous run), and the
-//     FP64 residual (thread per basis function and quarter
-//     of the points, one read of each basis value for the four row fields)
-//     added into rhs.
+//   TangentPointKernel (FP64, persistent, two 256-thread CTAs per SM, one
+//     element at a time; the FP64 tables stream through shared memory with
+//     cp.async one chunk ahead): nodal state, the state at the 64 points
+//     (thread per point and quarter of the basis, the quarters summed by
+//     shuffles), the coefficients M_q of all four row fields (thread per row
+//     field and point, two column-field halves through a shared-memory
+//     scratch) written to a coefficient array laid out [element][row field]
+//     [16 point quads][80 coefficients][4 points] (a K chunk's coefficients of
+//     one row field are one contiguous run), and the FP64 residual (thread per
+//     basis function and pair of points of each chunk, one read of each basis
+//     value for the four row fields) added into rhs.
 //   TangentTcKernel (CTA per element and row-field pair h: i in {2h, 2h+1},
 //     256 threads, 4 M = 128 accumulator tiles in 256 TMEM columns; tile T:
 //     row field 2h + T/2, basis b in [32 (T&1), +32), tile row m = 4 (b mod
@@ -67,7 +68,6 @@ constexpr int kTileBytes = 128*64;               // 128 rows x 32 BF16 (64 B, on
 constexpr int kTmemCols = 256;                   // 4 tiles x N = 64 FP32 columns
 constexpr unsigned long long kWaitNs = 1000000000ull;
 constexpr int kRcStride = 5;                     // doubles per (field, point) residual coefficient row
-constexpr int kPartStride = 23;                  // odd double stride of the point-state partial sums
 constexpr int kScratchStride = 41;               // odd float stride of the per-thread coefficient scratch
 
 // TangentTcKernel shared memory (bytes from a 1024-aligned base).
@@ -88,19 +88,26 @@ constexpr int kTcSmemBytes = kOffBar+32+1024;                     // + alignment
 static_assert(kTcSmemBytes <= 113*1024, "two CTAs per SM");
 static_assert(kOffOp1 % 1024 == 0, "operand buffers 1024-aligned");
 
-// TangentPointKernel shared memory (bytes).
-constexpr int kPtOffU = 0;                                        // double [4 fields][64]
+// TangentPointKernel shared memory (bytes from a 16-aligned base).  Two staging buffers, each either
+// a point-state chunk -- 8 basis functions of the five tables at the 64 points, rows of kPtRow
+// doubles (8 values, 4 pad: 96 B, 16-byte aligned for cp.async, and 8-byte reads across the points
+// of a warp conflict-free) -- or a residual chunk -- the four tables N, dN/dx at 8 points, rows of the
+// 64 functions.  The coefficient scratch (float [256][kScratchStride]) overlays both buffers.
+constexpr int kPtChunkB = 8;                                      // functions per point-state chunk
+constexpr int kPtRow = 12;                                        // doubles per staged (table, point) row
+constexpr int kPtChunkQ = 8;                                      // points per residual chunk
+constexpr int kPtBufBytes = kFeatures*kQuad*kPtRow*8;             // 30,720
+constexpr int kPtOffBuf = 0;                                      // two staging buffers
+constexpr int kPtOffU = 2*kPtBufBytes;                            // double [4 fields][64]
 constexpr int kPtOffUp = kPtOffU+64*4*8;                          // double [4 fields][64]
-constexpr int kPtOffPart = kPtOffUp+64*4*8;                       // double [4][64][kPartStride]
-constexpr int kPtPartBytes = 4*64*kPartStride*8;                  // (later: float [256][kScratchStride])
-constexpr int kPtOffQS = kPtOffPart+kPtPartBytes;                 // double [64][kQS]
+constexpr int kPtOffQS = kPtOffUp+64*4*8;                         // double [64][kQS] (later: residual partials)
 constexpr int kPtOffRC = kPtOffQS+kQuad*kQS*8;                    // double [4][64][kRcStride]
 constexpr int kPtSmemBytes = kPtOffRC+4*kQuad*kRcStride*8;
-static_assert(kTcThreads*kScratchStride*4 <= kPtPartBytes, "coefficient scratch fits in the partial sums");
-constexpr int kStageBasis = 16;                  // basis functions per staged chunk of the point-state stage
+static_assert(kTcThreads*kScratchStride*4 <= 2*kPtBufBytes, "coefficient scratch fits in the staging buffers");
+static_assert(4*kPtChunkQ*kMaxBasis*8 <= kPtBufBytes, "residual chunk fits in a staging buffer");
+static_assert(4*4*64*8 <= kQuad*kQS*8, "residual partial sums fit in the point-state slots");
+static_assert(2*kPtSmemBytes+32 <= 228*1024, "two CTAs per SM");
 constexpr int kPointStride = 22;                 // doubles per point of the stored point state (kU .. kLap+2)
-constexpr int kStageStride = kStageBasis+1;      // odd double stride of a staged (feature, point) row
-static_assert(kFeatures*kQuad*kStageStride*8 <= kPtPartBytes, "staged basis chunk fits in the partial sums");
 
 // Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B BF16, both
 // K-major, M = 128, N = 64.
@@ -335,11 +342,36 @@ __device__ __forceinline__ void PointCoefficients(const PointState& S, const dou
 // (TangentTcFusedKernel).
 enum : int { kPointResidual = 0, kPointCoefficients = 1, kPointState = 2 };
 
-// Persistent: each CTA takes elements from a work queue (*queue, zeroed by the launcher) one at a time,
-// claiming its next element while it works on the current one.  No L2 prefetch: prefetching the next
-// element's table doubled the tables live in L2 (31 against 19 ms per launch on the 199,800-element
-// Y-bifurcation), and prefetching the current one as the CTA starts on it only raced the CTA's own
-// loads (22 ms).
+// Point-state chunk c of an element's FP64 tables (functions 8c .. 8c + 7 of the five tables at the 64
+// points) into a staging buffer of kPtRow-double rows: four 16-byte copies per row.  One commit group.
+__device__ __forceinline__ void StagePointChunk(const double* P, int c, uint32_t dst, int tid)
+{
+	#pragma unroll
+	for (int i = tid; i < kFeatures*kQuad*4; i += kTcThreads) {
+		const int row = i >> 2, piece = i & 3;                       // row = table * 64 + point
+		CopyAsync16(dst+(row*kPtRow+2*piece)*8, P+(size_t)row*kMaxBasis+kPtChunkB*c+2*piece);
+	}
+	CopyAsyncCommit();
+}
+
+// Residual chunk c (points 8c .. 8c + 7 of the tables N, dN/dx_d) into [4][8][64]: each table's eight
+// rows are one contiguous 4 KiB run.  One commit group.
+__device__ __forceinline__ void StageResidualChunk(const double* P, int c, uint32_t dst, int tid)
+{
+	#pragma unroll
+	for (int i = tid; i < 4*kPtChunkQ*kMaxBasis/2; i += kTcThreads) {
+		const int t = i >> 8, rem = i & 255;                         // 256 copies per table
+		CopyAsync16(dst+(t*kPtChunkQ*kMaxBasis+2*rem)*8, P+(size_t)(t*kQuad+kPtChunkQ*c)*kMaxBasis+2*rem);
+	}
+	CopyAsyncCommit();
+}
+
+// Persistent: each CTA takes elements from a work queue (*queue, zeroed by the launcher), claiming the
+// next element as it starts on the current one.  The FP64 tables stream through two shared-memory
+// staging buffers with cp.async, one chunk ahead of the arithmetic: eight point-state chunks, then
+// eight residual chunks (read again, from L2), and during the last two residual chunks the next
+// element's first two point-state chunks.  Exactly two copy groups are in flight at the top of every
+// chunk (empty groups where there is nothing to fetch), so each chunk waits for the older one.
 template <int kMode>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ state,
@@ -348,25 +380,31 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 {
 	extern __shared__ uint8_t smem_raw[];
 	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+15) & ~uintptr_t(15));
+	const uint32_t sBuf[2] = {SmemAddress(sm+kPtOffBuf), SmemAddress(sm+kPtOffBuf+kPtBufBytes)};
 	double* U = reinterpret_cast<double*>(sm+kPtOffU);
 	double* Up = reinterpret_cast<double*>(sm+kPtOffUp);
-	double* Part = reinterpret_cast<double*>(sm+kPtOffPart);
-	float* Scratch = reinterpret_cast<float*>(sm+kPtOffPart);
+	float* Scratch = reinterpret_cast<float*>(sm+kPtOffBuf);
 	double* QS = reinterpret_cast<double*>(sm+kPtOffQS);
 	double* RC = reinterpret_cast<double*>(sm+kPtOffRC);
 	__shared__ int next;
 
-	const int tid = threadIdx.x;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 	if (tid == 0) next = atomicAdd(queue, 1);
 	__syncthreads();
-	for (int e = next; e < mesh.elements; e = next) {
+	int e = next;
+	if (e < mesh.elements) {
+		const double* P0 = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
+		StagePointChunk(P0, 0, sBuf[0], tid);
+		StagePointChunk(P0, 1, sBuf[1], tid);
+	}
+	while (e < mesh.elements) {
 	__syncthreads();                                 // every thread has read next
 	if (tid == 0) next = atomicAdd(queue, 1);
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
 
-	// 1. Nodal state.
+	// 1. Nodal state (the element's first two point-state chunks are in flight).
 	if (tid < kMaxBasis) {
 		const int a = tid;
 		double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, p0 = 0.0, p1 = 0.0, p2 = 0.0;
@@ -378,34 +416,24 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 		U[a] = s0; U[64+a] = s1; U[128+a] = s2; U[192+a] = s3;
 		Up[a] = p0; Up[64+a] = p1; Up[128+a] = p2; Up[192+a] = 0.0;
 	}
-	__syncthreads();
 
-	// 2. State at every point (FP64): the basis tables are staged 16 functions at a time in shared
-	//    memory with coalesced 16-byte loads (rows of 17 doubles, so that 8-byte reads across the
-	//    points of a warp are conflict-free); thread (point q, quarter aq) takes 4 functions of each
-	//    chunk; the four quarters meet in shared memory.  The staging buffer overlays the partial
-	//    sums, which are written only after the last chunk has been read.
+	// 2. State at every point (FP64): thread (point q = 8 warp + lane / 4, function quarter aq = lane % 4)
+	//    takes functions aq and aq + 4 of every chunk, so the 32 lanes' reads of a row fall in distinct
+	//    bank pairs two by two; the four quarters of a point are adjacent lanes and meet by shuffles.
 	{
-		double* Stage = Part;
-		const int q = tid & 63, aq = tid >> 6;
+		const int q = 8*warp+(lane >> 2), aq = lane & 3;
 		double v[22];
 		#pragma unroll
 		for (int k = 0; k < 22; ++k) v[k] = 0.0;
-		for (int a0 = 0; a0 < kMaxBasis; a0 += kStageBasis) {
-			if (a0) __syncthreads();                 // the previous chunk has been read
-			for (int idx = tid; idx < kFeatures*kQuad*(kStageBasis/2); idx += kTcThreads) {
-				const int row = idx/(kStageBasis/2), k = idx%(kStageBasis/2);     // row = t*64 + point
-				const double2 w = *reinterpret_cast<const double2*>(P+(size_t)row*kMaxBasis+a0+2*k);
-				Stage[row*kStageStride+2*k] = w.x;
-				Stage[row*kStageStride+2*k+1] = w.y;
-			}
-			__syncthreads();
+		for (int c = 0; c < kMaxBasis/kPtChunkB; ++c) {
+			CopyAsyncWait<1>();                          // chunk c (this thread's copies)
+			__syncthreads();                             // ... and every thread's (and U, Up at c = 0)
+			const double* row = reinterpret_cast<const double*>(sm+kPtOffBuf+(c & 1)*kPtBufBytes)+q*kPtRow;
 			#pragma unroll
-			for (int jj = 0; jj < kStageBasis/4; ++jj) {
-				const int j = aq*(kStageBasis/4)+jj, b = a0+j;
-				const double n = Stage[(0*kQuad+q)*kStageStride+j], g0 = Stage[(1*kQuad+q)*kStageStride+j];
-				const double g1 = Stage[(2*kQuad+q)*kStageStride+j], g2 = Stage[(3*kQuad+q)*kStageStride+j];
-				const double l = Stage[(4*kQuad+q)*kStageStride+j];
+			for (int jj = 0; jj < 2; ++jj) {
+				const int j = aq+4*jj, b = kPtChunkB*c+j;
+				const double n = row[j], g0 = row[kQuad*kPtRow+j], g1 = row[2*kQuad*kPtRow+j];
+				const double g2 = row[3*kQuad*kPtRow+j], l = row[4*kQuad*kPtRow+j];
 				const double uf[4] = {U[b], U[64+b], U[128+b], U[192+b]};
 				v[0] += n*uf[0]; v[1] += n*uf[1]; v[2] += n*uf[2]; v[3] += n*uf[3];
 				v[4] += n*Up[b]; v[5] += n*Up[64+b]; v[6] += n*Up[128+b];
@@ -413,26 +441,29 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 				for (int f = 0; f < 4; ++f) { v[7+3*f] += g0*uf[f]; v[8+3*f] += g1*uf[f]; v[9+3*f] += g2*uf[f]; }
 				v[19] += l*uf[0]; v[20] += l*uf[1]; v[21] += l*uf[2];
 			}
+			__syncthreads();                             // buffer c & 1 has been read
+			if (c+2 < kMaxBasis/kPtChunkB) StagePointChunk(P, c+2, sBuf[c & 1], tid);
+			else if constexpr (kMode != kPointCoefficients) StageResidualChunk(P, c+2-kMaxBasis/kPtChunkB, sBuf[c & 1], tid);
+			else CopyAsyncCommit();                      // (the coefficient scratch takes the buffers next)
 		}
-		__syncthreads();                             // the last chunk has been read
-		double* part = Part+(aq*kQuad+q)*kPartStride;
 		#pragma unroll
-		for (int k = 0; k < 22; ++k) part[k] = v[k];
-	}
-	__syncthreads();
-	for (int idx = tid; idx < kQuad*22; idx += kTcThreads) {
-		const int q = idx/22, k = idx%22;
-		const double* part = Part+q*kPartStride+k;
-		const double v = ((part[0]+part[kQuad*kPartStride])+part[2*kQuad*kPartStride])+part[3*kQuad*kPartStride];
-		QS[q*kQS+k] = v;
-		if constexpr (kMode == kPointState) point_state[(size_t)e*kQuad*kPointStride+idx] = v;
+		for (int k = 0; k < 22; ++k) {
+			v[k] += __shfl_xor_sync(0xffffffffu, v[k], 1);
+			v[k] += __shfl_xor_sync(0xffffffffu, v[k], 2);
+		}
+		#pragma unroll
+		for (int k = 0; k < 22; ++k)
+			if ((k & 3) == aq) {
+				QS[q*kQS+k] = v[k];
+				if constexpr (kMode == kPointState) point_state[((size_t)e*kQuad+q)*kPointStride+k] = v[k];
+			}
 	}
 	__syncthreads();
 
 	// 3. Coefficients: thread (row field il, point q), two column-field halves through the
-	//    scratch (the partial sums are dead), stored coalesced over the points.  The row field is
-	//    uniform over a warp and a compile-time constant of each branch, so the point state and the
-	//    coefficient temporaries stay in registers.
+	//    scratch, stored coalesced over the points of a quad.  The row field is uniform over a warp
+	//    and a compile-time constant of each branch, so the point state and the coefficient
+	//    temporaries stay in registers.
 	{
 		const int q = tid & 63, il = tid >> 6;
 		PointState S;
@@ -464,32 +495,51 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 			}
 		}
 	}
-	__syncthreads();
+	__syncthreads();                                 // RC complete; the scratch is dead
+	const int en = next;                             // the next element (claimed at the top)
+	if constexpr (kMode == kPointCoefficients) {
+		// the two residual chunks the other modes fetched during the point-state stage (the two empty
+		// groups committed there are complete once these are waited for)
+		StageResidualChunk(P, 0, sBuf[0], tid);
+		StageResidualChunk(P, 1, sBuf[1], tid);
+	}
 
-	// 4. FP64 residual of the four row fields (rhs holds -r): thread (basis function a, quarter
-	//    qq of the points) reads each basis value once for all four row fields; the quarters meet
-	//    in shared memory (the coefficient scratch is dead).
+	// 4. FP64 residual of the four row fields (rhs holds -r): thread (basis function a, point pair qq
+	//    of each chunk) reads each table value once for all four row fields; the four pairs meet in
+	//    shared memory (the point-state slots are dead).
 	{
 		const int a = tid & 63, qq = tid >> 6;
 		double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
-		for (int q = qq*16; q < qq*16+16; ++q) {
+		for (int c = 0; c < kQuad/kPtChunkQ; ++c) {
+			CopyAsyncWait<1>();
+			__syncthreads();
+			const double* B4 = reinterpret_cast<const double*>(sm+kPtOffBuf+(c & 1)*kPtBufBytes);
 			#pragma unroll
-			for (int s = 0; s < 4; ++s) {
-				const double v = P[(s*kQuad+q)*kMaxBasis+a];
-				r0 += v*RC[(0*kQuad+q)*kRcStride+s];
-				r1 += v*RC[(1*kQuad+q)*kRcStride+s];
-				r2 += v*RC[(2*kQuad+q)*kRcStride+s];
-				r3 += v*RC[(3*kQuad+q)*kRcStride+s];
+			for (int p = 0; p < 2; ++p) {
+				const int ql = 2*qq+p, q = kPtChunkQ*c+ql;
+				#pragma unroll
+				for (int s = 0; s < 4; ++s) {
+					const double v = B4[(s*kPtChunkQ+ql)*kMaxBasis+a];
+					r0 += v*RC[(0*kQuad+q)*kRcStride+s];
+					r1 += v*RC[(1*kQuad+q)*kRcStride+s];
+					r2 += v*RC[(2*kQuad+q)*kRcStride+s];
+					r3 += v*RC[(3*kQuad+q)*kRcStride+s];
+				}
 			}
+			__syncthreads();                             // buffer c & 1 has been read
+			if (c+2 < kQuad/kPtChunkQ) StageResidualChunk(P, c+2, sBuf[c & 1], tid);
+			else if (en < mesh.elements)
+				StagePointChunk(phi+(size_t)en*kFeatures*kQuad*kMaxBasis, c+2-kQuad/kPtChunkQ, sBuf[c & 1], tid);
+			else CopyAsyncCommit();
 		}
-		double* red = Part;                     // [4 quarters][4 row fields][64]
+		double* red = QS;                            // [4 pairs][4 row fields][64]
 		red[(qq*4+0)*64+a] = r0; red[(qq*4+1)*64+a] = r1; red[(qq*4+2)*64+a] = r2; red[(qq*4+3)*64+a] = r3;
 		__syncthreads();
 		const int il = tid >> 6;
 		const double r = ((red[(0*4+il)*64+a]+red[(1*4+il)*64+a])+red[(2*4+il)*64+a])+red[(3*4+il)*64+a];
 		if (a < nen) atomicAdd(rhs+4*(size_t)mesh.connectivity[begin+a]+il, r);
 	}
-	__syncthreads();                                 // the element's shared memory is free; next is set
+	e = en;
 	}
 }
 
