@@ -26,11 +26,12 @@ precisions).  Outlet pressures follow the RCR models by the relaxed fixed
 point (relaxation 1, tolerance 1e-8 + 1e-6 |P|), updated inside the Newton
 loop (--outlet-coupling newton; "outer" runs the reference's loop of Newton
 solves), with the models' dP/dQ terms in the Newton Jacobian.  --precision
-mixed (default): tangent contracted on the tcgen05 tensor cores with BF16
-operands (FP32 accumulation), FP32 Jacobian for SpMV and the preconditioner,
-FP32 Krylov basis, FP64 residual, vectors and refinement; --precision bf16x3:
-split-BF16 operands (hi + lo, three products); --precision tf32: TF32
-operands; --precision fp64: every array FP64.
+bf16x3 (default): tangent contracted on the tcgen05 tensor cores with
+split-BF16 operands (hi + lo, three products, FP32 accumulation), FP32
+Jacobian for SpMV and the preconditioner, FP32 Krylov basis, FP64 residual,
+vectors and refinement; --precision mixed: plain BF16 operands (a tangent
+accurate to about 1e-2, so Newton contracts more slowly on the coupled
+system); --precision tf32: TF32 operands; --precision fp64: every array FP64.
 
 Legs of one run (rank 0 prints one JSON line):
   value     device-timed (CUDA events on the solver stream) with every input
@@ -744,14 +745,11 @@ def main():
     ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c1", "c2-100", "c4", "c5", "transport"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "block-jacobi"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "bf16x3", "tf32", "fp64"],
-                    help="mixed: BF16 tensor-core tangent; bf16x3: split BF16 (hi + lo, three products); "
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "mixed", "tf32", "fp64"],
+                    help="bf16x3: split-BF16 tensor-core tangent (hi + lo, three products); mixed: plain BF16; "
                          "tf32: TF32 operands; fp64: the FP64 solver alone")
     ap.add_argument("--no-fp64-leg", action="store_true")
-    ap.add_argument("--krylov-operator", default="fp32", choices=["fp32", "bf16"],
-                    help="storage of the Jacobian the flexible GMRES applies (reduced-precision modes): the FP32 "
-                         "assembly, or a BF16 copy of it (half the SpMV's matrix traffic)")
-    ap.add_argument("--tangent-kernel", default="auto", choices=["auto", "coefficients", "fused"],
+    ap.add_argument("--tangent-kernel", default="auto", choices=["auto", "coefficients", "fused", "element"],
                     help="tensor-core tangent organisation (auto: the autotuner times both on the first tangent)")
     ap.add_argument("--learned", type=int, default=0,
                     help="time the learned FGMRES stage too, trained on pairs from this many further steps")
@@ -826,8 +824,7 @@ def main():
                      amg_coarse_period=args.amg_coarse_period, krylov_fp64_basis=int(args.krylov_fp64_basis),
                      newton_forcing=int(args.forcing == "ew"), tangent_reuse_factor=args.tangent_reuse,
                      tangent_kernel={"auto": api.TANGENT_AUTO, "coefficients": api.TANGENT_COEFFICIENTS,
-                                     "fused": api.TANGENT_FUSED}[args.tangent_kernel],
-                     krylov_bf16_operator=int(args.krylov_operator == "bf16"))
+                                     "fused": api.TANGENT_FUSED, "element": api.TANGENT_ELEMENT}[args.tangent_kernel])
     precision = {"mixed": api.MIXED, "bf16x3": api.MIXED_BF16X3, "tf32": api.MIXED_TF32,
                  "fp64": api.FP64}[args.precision]
     ns = api.NavierStokes(mesh, precision=precision, **solver_kw)
@@ -1093,8 +1090,8 @@ def main():
     res_ms, res_n = prof.get("residual", (0.0, 0))
     kernels = {}
     if mixed:
-        # FP32 Jacobian: 4-byte values in every pass over the matrix (2-byte with the BF16 copy)
-        b_spmv -= mesh.blocks * 16 * (6 if args.krylov_operator == "bf16" else 4)
+        # FP32 Jacobian: 4-byte values in every pass over the matrix
+        b_spmv -= mesh.blocks * 16 * 4
     spmv_bytes = b_spmv if amg else b_spmv + b_bjac
     spmv_name = "spmv" if amg else "spmv_block_jacobi"
     if spmv_n:
@@ -1201,7 +1198,6 @@ def main():
                                                                                    else "") if amg else
                                "block-Jacobi GMRES(%d) rtol 1e-8" % args.restart)),
                    "newton_rtol": args.newton_rtol, "amg_coarse_period": args.amg_coarse_period,
-                   "krylov_operator": args.krylov_operator if mixed else "fp64",
                    "l2": "inputs larger than L2 (matrix %.2f GB)" % (mesh.blocks * 128 / 1e9),
                    "parallelism": "replicas only" if world > 1 else "single GPU"},
         "newton_per_step": float(newton), "linear_iterations_per_newton": float(linear),

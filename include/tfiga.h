@@ -142,16 +142,14 @@ typedef struct tfiga_ns_params {
 	 * TFIGA_TANGENT_FUSED: the point kernel stores the FP64 point state (11 KiB per
 	 * element) and the tensor-core kernel makes the coefficients itself and stages
 	 * the basis from the FP64 tables (about 96 KiB per element less);
-	 * TFIGA_TANGENT_AUTO: the first tangent assembly times both (when the memory for
-	 * the first one is free) and keeps the faster; the fused one otherwise.
-	 * Both give the same tangent up to the order of the FP32 additions. */
+	 * TFIGA_TANGENT_ELEMENT: the arrays of TFIGA_TANGENT_COEFFICIENTS contracted by one
+	 * persistent CTA per SM that takes whole elements (all four row fields at once, the
+	 * basis staged once per element);
+	 * TFIGA_TANGENT_AUTO: the first tangent assembly times the three (the two
+	 * coefficient-array ones when their memory is free) and keeps the fastest; the
+	 * fused one otherwise.
+	 * All give the same tangent up to the order of the FP32 additions. */
 	int32_t tangent_kernel;        /* default TFIGA_TANGENT_AUTO */
-	/* Reduced-precision modes: 1 keeps a BF16 copy of the FP32 Jacobian (rounded to
-	 * nearest even after each assembly) and applies it in the flexible GMRES's
-	 * products and true residuals, halving the SpMV's matrix traffic; the AMG keeps the
-	 * FP32 values.  The Newton residual stays FP64, so only the Newton convergence
-	 * rate can change.  Ignored in TFIGA_PRECISION_FP64. */
-	int32_t krylov_bf16_operator;  /* default 0 */
 } tfiga_ns_params;
 
 #define TFIGA_PRECISION_FP64 0
@@ -164,6 +162,7 @@ typedef struct tfiga_ns_params {
 #define TFIGA_TANGENT_AUTO 0
 #define TFIGA_TANGENT_COEFFICIENTS 1
 #define TFIGA_TANGENT_FUSED 2
+#define TFIGA_TANGENT_ELEMENT 3
 
 #define TFIGA_PRECONDITIONER_BLOCK_JACOBI 0
 #define TFIGA_PRECONDITIONER_AMG 1
@@ -320,20 +319,25 @@ int tfiga_ns_step_outlets_coupled(tfiga_ns* ns, tfiga_outlet* outlets, int32_t c
 	int32_t max_newton, tfiga_step_report* report, int32_t* pressure_updates);
 /* AMG hierarchy sizes (levels = 0 before the hierarchy is built). */
 int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info);
-/* Batched tubes (north-star form 2; no counterpart in the reference, which solves one mesh): the node
- * ranges [node_offsets[k], node_offsets[k+1]) of count independent tubes (node_offsets increasing
+/* Batched tubes (a batching form with no counterpart in the reference, which solves one mesh): the
+ * node ranges [node_offsets[k], node_offsets[k+1]) of count independent tubes (node_offsets increasing
  * from 0 to nodes, e.g. tfiga_batch_mesh_create's node offsets); count 0 removes them.  The Newton
  * test is then taken per tube, relative to the tube's own first residual of the step, and a tube that
- * passes is frozen for the rest of the step (its rows of the linear system carry a zero rhs); the
- * step converges when every tube has passed. */
+ * passes is frozen for the rest of the step (its rows of the linear system carry a zero rhs); each
+ * open tube's rhs is scaled to unit norm for the linear solve and its update scaled back, so the
+ * union's Krylov solve resolves every tube relative to itself; the step converges when every tube
+ * has passed. */
 int tfiga_ns_set_segments(tfiga_ns* ns, const int64_t* node_offsets, int32_t count);
 /* Per tube, after a Newton iteration: done[k] 1 when tube k has passed its test in this step, and its
  * residual norm (either output may be NULL). */
 int tfiga_ns_segment_status(tfiga_ns* ns, int32_t* done, double* residuals);
 /* Tensor-core modes: the tangent organisation in use (*kernel: TFIGA_TANGENT_*, AUTO before the
- * first tangent) and the autotuner's times of the coefficient-array and fused organisations (ms,
- * 0 when not timed).  No counterpart in the reference.  Any output may be NULL. */
+ * first tangent) and the autotuner's times of the coefficient-array (row-field-pair kernel) and fused
+ * organisations (ms, 0 when not timed).  No counterpart in the reference.  Any output may be NULL. */
 int tfiga_ns_tangent_kernel(tfiga_ns* ns, int32_t* kernel, double* coefficients_ms, double* fused_ms);
+/* The autotuner's time of the element kernel (TFIGA_TANGENT_ELEMENT) on the coefficient arrays (ms, 0
+ * when not timed). */
+int tfiga_ns_tangent_element_ms(tfiga_ns* ns, double* element_ms);
 /* Outward flow through each labelled boundary (IntegrateBoundaryFlow,
  * BoundaryFlow.hpp:165-200; MeasureFlowConvergence iga_cuda.cu:520-557). */
 int tfiga_ns_boundary_flows(tfiga_ns* ns, const int32_t* labels, int32_t count, double* flows);

@@ -84,9 +84,10 @@ def test_tensor_tangent_reference_tube_ragged(api, reference_tube):
     check_tensor_tangent(api, flat, 1.0, 1.0, 0.1, 5)
 
 
-# both tangent organisations: point coefficients stored by the point kernel (1), coefficients made in the
-# tensor-core kernel from the stored point state with the basis staged from the FP64 tables (2)
-KERNELS = [1, 2]
+# the tangent organisations: point coefficients stored by the point kernel and contracted per row-field
+# pair (1) or per element (3), coefficients made in the tensor-core kernel from the stored point state
+# with the basis staged from the FP64 tables (2)
+KERNELS = [1, 2, 3]
 
 
 @pytest.mark.parametrize("kernel", KERNELS)
@@ -138,24 +139,25 @@ def test_tf32_newton_converges_to_fp64_solution(api, cylinder_1280):
 
 
 def test_tangent_autotuner_picks_one_and_matches(api, small_tube):
-    """TFIGA_TANGENT_AUTO: the first tangent times both organisations (memory is plentiful here), keeps
-    one, and every tangent it assembles agrees with the fixed organisations' to FP32 addition order."""
+    """TFIGA_TANGENT_AUTO: the first tangent times the three organisations (memory is plentiful here),
+    keeps one, and every tangent it assembles agrees with the fixed organisations' to FP32 addition
+    order."""
     flat = small_tube.mesh
     st, pv = random_state(flat.nodes, 21), random_state(flat.nodes, 22)
     got = {}
-    for kernel in (0, 1, 2):
+    for kernel in (0, 1, 2, 3):
         ns = api.NavierStokes(api.Mesh(flat), density=RHO, viscosity=MU, dt=DT, preconditioner=api.AMG,
                               precision=api.MIXED_BF16X3, tangent_kernel=kernel)
         ns.set_state(st, pv)
         got[kernel] = ns.assemble()[0]
         info = ns.tangent_kernel()
         if kernel == 0:
-            assert info["kernel"] in ("coefficients", "fused")
-            assert info["coefficients_ms"] > 0 and info["fused_ms"] > 0
+            assert info["kernel"] in ("coefficients", "fused", "element")
+            assert info["coefficients_ms"] > 0 and info["fused_ms"] > 0 and info["element_ms"] > 0
             again = ns.assemble()[0]
             assert rel(again, got[0]) < 1e-6
         ns.close()
-    assert rel(got[1], got[2]) < 1e-6 and rel(got[0], got[2]) < 1e-6
+    assert rel(got[1], got[2]) < 1e-6 and rel(got[0], got[2]) < 1e-6 and rel(got[3], got[1]) < 1e-6
 
 
 def test_split_newton_matches_fp64_iterations(api, cylinder_1280):
@@ -199,18 +201,16 @@ def test_mixed_newton_converges_to_fp64_solution(api, cylinder_1280):
     s0 = api.initial_state(vmask, vel)
     mesh = api.Mesh(flat)
     states, reports = {}, {}
-    for name, precision, bf16_operator in (("fp64", api.FP64, 0), ("mixed", api.MIXED, 0),
-                                           ("bf16_operator", api.MIXED, 1)):
+    for name, precision in (("fp64", api.FP64), ("mixed", api.MIXED)):
         ns = api.NavierStokes(mesh, density=RHO, viscosity=MU, dt=DT, preconditioner=api.AMG, precision=precision,
-                              nonlinear_rtol=1e-10, nonlinear_atol=1e-30, gmres_rtol=1e-10, max_newton=20,
-                              krylov_bf16_operator=bf16_operator)
+                              nonlinear_rtol=1e-10, nonlinear_atol=1e-30, gmres_rtol=1e-10, max_newton=20)
         ns.set_dirichlet(vmask, pmask, vel)
         ns.set_tractions({2: 0.0})
         ns.set_state(s0, s0)
         reports[name] = ns.step()
         states[name] = ns.get_state().reshape(-1, 4)
         ns.close()
-    for name in ("mixed", "bf16_operator"):
+    for name in ("mixed",):
         print(name, reports[name]["newton_iterations"], "Newton iterations; FP64", reports["fp64"]["newton_iterations"])
         assert reports[name]["converged"] and reports["fp64"]["converged"]
         assert reports[name]["newton_iterations"] <= reports["fp64"]["newton_iterations"] + 4
@@ -222,9 +222,8 @@ def test_mixed_transient_steps_match_fp64_on_the_pulsatile_section(api):
     """The 12,800-element section of the pulsatile tube (C2's cross-section and Fourier inflow, 100 layers),
     four backward-Euler steps at dt 2e-3 with the bench's solver settings (Newton rel.res 1e-10 on the FP64
     residual, Eisenstat-Walker linear tolerances, tangent reuse factor 100, AMG-FGMRES(64)): the split-BF16
-    and the plain-BF16 mixed solvers (the latter also with the BF16 copy of the Jacobian in the Krylov
-    products) and the FP64 solver from the same state with the same Dirichlet sequence agree within 1e-8
-    relative L2 on velocity and on pressure after every step."""
+    and the plain-BF16 mixed solvers and the FP64 solver from the same state with the same Dirichlet
+    sequence agree within 1e-8 relative L2 on velocity and on pressure after every step."""
     import bench
     tube, _, wave = bench.workload("c2-100")
     mesh = api.Mesh(tube.mesh)
@@ -232,13 +231,11 @@ def test_mixed_transient_steps_match_fp64_on_the_pulsatile_section(api):
     dt = 2e-3
     s0 = api.initial_state(vmask, velocity_at(0.0))
     trajectories = {}
-    for name, precision, bf16_operator in (("fp64", api.FP64, 0), ("split", api.MIXED_BF16X3, 0),
-                                           ("bf16", api.MIXED, 0), ("bf16_operator", api.MIXED, 1)):
+    for name, precision in (("fp64", api.FP64), ("split", api.MIXED_BF16X3), ("bf16", api.MIXED)):
         ns = api.NavierStokes(mesh, precision=precision, density=1060.0, viscosity=3.5e-3, dt=dt,
                               nonlinear_rtol=1e-10, nonlinear_atol=1e-300, mass_rtol=1e-3, gmres_restart=64,
                               gmres_max_iterations=5000, gmres_rtol=1e-8, preconditioner=api.AMG,
-                              amg_coarse_period=3, newton_forcing=1, tangent_reuse_factor=100.0,
-                              krylov_bf16_operator=bf16_operator)
+                              amg_coarse_period=3, newton_forcing=1, tangent_reuse_factor=100.0)
         ns.set_dirichlet(vmask, pmask, velocity_at(0.0))
         ns.set_tractions({2: 0.0})
         ns.set_state(s0, s0)
@@ -250,7 +247,7 @@ def test_mixed_transient_steps_match_fp64_on_the_pulsatile_section(api):
             states.append(ns.get_state().reshape(-1, 4))
         ns.close()
         trajectories[name] = states
-    for name in ("split", "bf16", "bf16_operator"):
+    for name in ("split", "bf16"):
         for k, (a, b) in enumerate(zip(trajectories[name], trajectories["fp64"])):
             ev, ep = rel(a[:, :3], b[:, :3]), rel(a[:, 3], b[:, 3])
             print(f"step {k + 1}: {name} vs FP64 velocity {ev:.3e} pressure {ep:.3e}")

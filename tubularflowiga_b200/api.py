@@ -43,13 +43,13 @@ class NsParams(C.Structure):
                 ("gmres_rtol", C.c_double), ("preconditioner", C.c_int32), ("precision", C.c_int32),
                 ("amg_coarse_nodes", C.c_int32), ("amg_coarse_period", C.c_int32),
                 ("krylov_fp64_basis", C.c_int32), ("newton_forcing", C.c_int32),
-                ("tangent_reuse_factor", C.c_double), ("tangent_kernel", C.c_int32),
-                ("krylov_bf16_operator", C.c_int32)]
+                ("tangent_reuse_factor", C.c_double), ("tangent_kernel", C.c_int32)]
 
 
 TANGENT_AUTO = 0
 TANGENT_COEFFICIENTS = 1
 TANGENT_FUSED = 2
+TANGENT_ELEMENT = 3
 
 FP64 = 0
 MIXED = 1
@@ -174,6 +174,7 @@ SIGNATURES = {
                                                 C.POINTER(StepReport), C.POINTER(C.c_int32)]),
     "tfiga_ns_amg_info": (C.c_int, [C.c_void_p, C.POINTER(AmgInfo)]),
     "tfiga_ns_tangent_kernel": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tfiga_ns_tangent_element_ms": (C.c_int, [C.c_void_p, C.c_void_p]),
     "tfiga_ns_set_segments": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "tfiga_ns_segment_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "tfiga_ns_boundary_flows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
@@ -491,8 +492,12 @@ class NavierStokes:
         """The tensor-core tangent organisation in use and the autotuner's timings."""
         k = C.c_int32(); a = C.c_double(); b = C.c_double()
         check(lib().tfiga_ns_tangent_kernel(self._h, C.byref(k), C.byref(a), C.byref(b)))
-        names = {TANGENT_AUTO: "auto", TANGENT_COEFFICIENTS: "coefficients", TANGENT_FUSED: "fused"}
-        return {"kernel": names.get(k.value, str(k.value)), "coefficients_ms": a.value, "fused_ms": b.value}
+        names = {TANGENT_AUTO: "auto", TANGENT_COEFFICIENTS: "coefficients", TANGENT_FUSED: "fused",
+                 TANGENT_ELEMENT: "element"}
+        el = C.c_double()
+        check(lib().tfiga_ns_tangent_element_ms(self._h, C.byref(el)))
+        return {"kernel": names.get(k.value, str(k.value)), "coefficients_ms": a.value, "fused_ms": b.value,
+                "element_ms": el.value}
 
     def amg_info(self) -> dict:
         info = AmgInfo()

@@ -1,8 +1,7 @@
 // One 4x4 block row of A x, shared by the SpMV kernels and the AMG residual.
 //
 // A warp owns one block row; lane l multiplies whole blocks l, l+32, ...
-// (16 FP32 values in four 128-bit loads, 16 FP64 values in eight, or 16 BF16
-// values in two), so a
+// (16 FP32 values in four 128-bit loads, or 16 FP64 values in eight), so a
 // warp keeps 32 blocks of values in flight, and the column index of a lane's
 // next block is loaded one step ahead so that the x gather does not wait on
 // it.  The four row sums are then reduced across the warp (three butterfly
@@ -32,25 +31,6 @@ template <> struct BlockLoad<float> {
 		for (int k = 0; k < 4; ++k) {
 			const float4 v = __ldg(p+k);
 			a[4*k] = v.x; a[4*k+1] = v.y; a[4*k+2] = v.z; a[4*k+3] = v.w;
-		}
-	}
-};
-
-// BF16 values stored as raw 16-bit patterns (the upper half of the FP32 pattern): 16 values in two
-// 128-bit loads, widened exactly.
-template <> struct BlockLoad<uint16_t> {
-	static __device__ __forceinline__ void Get(const uint16_t* values, long long b, double a[16])
-	{
-		const uint4* p = reinterpret_cast<const uint4*>(values+(size_t)b*16);
-		#pragma unroll
-		for (int k = 0; k < 2; ++k) {
-			const uint4 v = __ldg(p+k);
-			const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-			#pragma unroll
-			for (int i = 0; i < 4; ++i) {
-				a[8*k+2*i] = (double)__uint_as_float(w[i] << 16);
-				a[8*k+2*i+1] = (double)__uint_as_float(w[i] & 0xffff0000u);
-			}
 		}
 	}
 };

@@ -241,7 +241,6 @@ void tfiga_ns_default_params(tfiga_ns_params* p)
 	p->newton_forcing = 0;
 	p->tangent_reuse_factor = 0.0;
 	p->tangent_kernel = TFIGA_TANGENT_AUTO;
-	p->krylov_bf16_operator = 0;
 }
 
 int tfiga_ns_create(tfiga_mesh* mesh, const tfiga_ns_params* params, tfiga_ns** out)
@@ -423,6 +422,14 @@ int tfiga_ns_tangent_kernel(tfiga_ns* ns, int32_t* kernel, double* coefficients_
 		if (kernel) *kernel = ns->solver->tangent_kernel();
 		if (coefficients_ms) *coefficients_ms = ns->solver->tune_ms(TFIGA_TANGENT_COEFFICIENTS);
 		if (fused_ms) *fused_ms = ns->solver->tune_ms(TFIGA_TANGENT_FUSED);
+	});
+}
+
+int tfiga_ns_tangent_element_ms(tfiga_ns* ns, double* element_ms)
+{
+	return Guard([&] {
+		Require(ns && element_ms, "null argument");
+		*element_ms = ns->solver->tune_ms(TFIGA_TANGENT_ELEMENT);
 	});
 }
 

@@ -576,8 +576,7 @@ void Gmres::FlexibleStep(const DevicePatternView& pattern, const T* values, int 
 		launches_ += 1+3+learned_->layers();
 	}
 	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
-	if (operator16_) LaunchSpmvBlockJacobi<uint16_t>(pattern, operator16_, nullptr, z, nullptr, w_.get(), stop, stream_);
-	else LaunchSpmvBlockJacobi<T>(pattern, values, nullptr, z, nullptr, w_.get(), stop, stream_);
+	LaunchSpmvBlockJacobi<T>(pattern, values, nullptr, z, nullptr, w_.get(), stop, stream_);
 	if (low_on_) AddLowRank(z, w_.get(), stop);
 	if (profiler_) profiler_->End(stream_);
 	launches_ += 1;
@@ -598,8 +597,7 @@ double Gmres::TrueResidualPlain(const DevicePatternView& pattern, const T* value
 {
 	// v_0 = b - A x (FP64), stored in the basis precision; beta from the FP64 vector
 	if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
-	if (operator16_) LaunchSpmv<uint16_t>(pattern, operator16_, x, tmp_.get(), stream_);
-	else LaunchSpmv<T>(pattern, values, x, tmp_.get(), stream_);
+	LaunchSpmv<T>(pattern, values, x, tmp_.get(), stream_);
 	if (low_on_) AddLowRank(x, tmp_.get(), nullptr);
 	double* r = std::is_same<B, double>::value ? V_.get() : r_.get();
 	ResidualKernel<<<(unsigned)((n_+255)/256), 256, 0, stream_>>>(n_, rhs, tmp_.get(), r);

@@ -71,10 +71,6 @@ public:
 		low_on_ = term != nullptr && term->count > 0;
 		if (low_on_) low_ = *term;
 	}
-	// BF16 copy of the operator (raw 16-bit patterns, the block-CSR layout of `values`) used by the
-	// flexible solve's products A z and its true residuals instead of `values`; the preconditioner still
-	// takes `values`.  Null: off.
-	void set_operator16(const uint16_t* values) { operator16_ = values; }
 	std::size_t bytes() const;
 
 private:
@@ -119,7 +115,6 @@ private:
 	HostStatus* host_ = nullptr;
 	Profiler* profiler_ = nullptr;
 	double tolerance_ = 0.0;                 // absolute residual target of the current solve
-	const uint16_t* operator16_ = nullptr;
 	bool low_on_ = false;
 	LowRank low_{};
 	// y += sum_k c_k (g_k . x) g_k (skipped when *stop; stop may be null).

@@ -79,20 +79,23 @@ void LaunchAssembleLarge(const DeviceMeshView& mesh, int first, int count, const
 // ---- tangent_tc.cu -----------------------------------------------------
 // Tensor-core tangent in two launches.  LaunchTangentPoint: FP64 point state,
 // the coefficients of all four row fields into coef (workspace of elements x 4
-// x 80 x 64 floats; null: residual only) and the FP64 residual ADDED into rhs
+// x 16 x 80 x 4 floats, point-quad major; null: residual only) and the FP64 residual ADDED into rhs
 // (= -r).
 // LaunchTangentTc: the tangent contracted on the tcgen05 tensor cores from
 // coef and phi32 (the FP32 copy of phi, Mesh::phi32), FP32 accumulation, ADDED
 // into the FP32 values; status bit 1 set if an MMA completion wait expired.
 // operands: TC_OPERANDS_BF16, TC_OPERANDS_SPLIT (hi + lo BF16) or TC_OPERANDS_TF32.
 // point_state (elements x 64 x 22 doubles, may be null): the point state for LaunchTangentTcFused
-// instead of the coefficients (coef and point_state are not both given).  queue: one device int, the
-// persistent CTAs' element counter (zeroed here on the stream before the launch).
+// instead of the coefficients (coef and point_state are not both given).
 void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const double* qdata, const double* state,
-	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs, int* queue,
+	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs,
 	cudaStream_t stream);
 enum : int { TC_OPERANDS_BF16 = 0, TC_OPERANDS_SPLIT = 1, TC_OPERANDS_TF32 = 2 };
 void LaunchTangentTc(const DeviceMeshView& mesh, const float* phi32, const float* coef,
+	const int32_t* element_blocks, float* values, int* status, int operands, cudaStream_t stream);
+// The same contraction with one persistent CTA per SM taking whole elements (all four row fields, the
+// basis chunk staged once per element; 512 TMEM columns, so one CTA per SM).
+void LaunchTangentTcElement(const DeviceMeshView& mesh, const float* phi32, const float* coef,
 	const int32_t* element_blocks, float* values, int* status, int operands, cudaStream_t stream);
 // The same contraction with the coefficients made in the kernel from the stored point state and the
 // basis staged from the FP64 tables (no coefficient array, no FP32 copy of the tables).
@@ -113,8 +116,6 @@ template <class T>
 void LaunchBlockInverse(const DevicePatternView& pattern, const T* values, double* inverse,
 	unsigned int* singular, cudaStream_t stream);
 void LaunchToFloat(long long n, const double* in, float* out, cudaStream_t stream);
-// out = BF16(in) (round to nearest even), stored as raw 16-bit patterns.
-void LaunchToBf16(long long n, const float* in, uint16_t* out, cudaStream_t stream);
 // FP32 copy of basis tables [table][64 points][64 functions] (FP64) with the points of each pair
 // interleaved: out[table][point pair][function][2] (the tensor-core tangent's staging layout).
 void LaunchToFloatPointPairs(long long tables, const double* in, float* out, cudaStream_t stream);

@@ -82,22 +82,15 @@ NsSolver::NsSolver(Mesh& mesh, const tfiga_ns_params& params)
 	if (mixed() && params.preconditioner != TFIGA_PRECONDITIONER_AMG)
 		Fail(-7, "mixed precision requires the AMG-preconditioned flexible GMRES");
 	if (mixed()) values32_.Allocate((size_t)blocks()*16);
-	if (params.krylov_bf16_operator != 0 && params.krylov_bf16_operator != 1)
-		Fail(-1, "krylov_bf16_operator must be 0 or 1");
-	if (mixed() && params.krylov_bf16_operator) {
-		values16_.Allocate((size_t)blocks()*16);
-		gmres_.set_operator16(values16_.get());
-	}
 	if (params.tangent_kernel != TFIGA_TANGENT_AUTO && params.tangent_kernel != TFIGA_TANGENT_COEFFICIENTS
-		&& params.tangent_kernel != TFIGA_TANGENT_FUSED)
+		&& params.tangent_kernel != TFIGA_TANGENT_FUSED && params.tangent_kernel != TFIGA_TANGENT_ELEMENT)
 		Fail(-1, "unknown tangent_kernel "+std::to_string(params.tangent_kernel));
 	tangent_kernel_ = params.tangent_kernel;
 	if (tensor_tangent()) {
 		const size_t regular = (size_t)mesh.regular_elements();
-		if (tangent_kernel_ == TFIGA_TANGENT_COEFFICIENTS) coef32_.Allocate(regular*4*80*64);
+		if (coefficient_arrays()) coef32_.Allocate(regular*4*80*64);
 		else point_state_.Allocate(regular*kQuad*22);
 	}
-	queue_.Allocate(1);                       // work counter of the persistent point kernel
 	if (tensor_tangent()) {
 		status_.Allocate(1);
 		status_.Zero(stream_);
@@ -219,10 +212,10 @@ void NsSolver::AssembleResidualTc()
 	rhs_.Zero(stream_);
 	profiler_.End(stream_);
 	profiler_.Begin(Profiler::kResidual, stream_);
-	const bool coefficients = tangent_kernel_ == TFIGA_TANGENT_COEFFICIENTS;
+	const bool coefficients = coefficient_arrays();
 	LaunchTangentPoint(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
 		{params_.density, params_.viscosity, params_.dt}, coefficients ? coef32_.get() : nullptr,
-		coefficients ? nullptr : point_state_.get(), rhs_.get(), queue_.get(), stream_);
+		coefficients ? nullptr : point_state_.get(), rhs_.get(), stream_);
 	LargeElements<float>(nullptr, rhs_.get());
 	profiler_.End(stream_);
 	profiler_.Begin(Profiler::kVector, stream_);
@@ -254,6 +247,9 @@ void NsSolver::AssembleTangentTc()
 		if (tangent_kernel_ == TFIGA_TANGENT_FUSED)
 			LaunchTangentTcFused(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), point_state_.get(), prm,
 				mesh_.element_blocks(), values32_.get(), status_.get(), operands, stream_);
+		else if (tangent_kernel_ == TFIGA_TANGENT_ELEMENT)
+			LaunchTangentTcElement(mesh_.regular_view(), mesh_.phi32(), coef32_.get(), mesh_.element_blocks(),
+				values32_.get(), status_.get(), operands, stream_);
 		else
 			LaunchTangentTc(mesh_.regular_view(), mesh_.phi32(), coef32_.get(), mesh_.element_blocks(),
 				values32_.get(), status_.get(), operands, stream_);
@@ -299,7 +295,7 @@ void NsSolver::AutotuneTangent()
 	// the same state's coefficients; the residual this pass adds goes to the Newton update vector,
 	// which the linear solve clears before use
 	LaunchTangentPoint(view, mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(), prm, coef32_.get(), nullptr,
-		update_.get(), queue_.get(), stream_);
+		update_.get(), stream_);
 	const float* phi32 = mesh_.phi32();
 	values32_.Zero(stream_);
 	CudaCheck(cudaEventRecord(ev[2], stream_), "event");
@@ -310,8 +306,20 @@ void NsSolver::AutotuneTangent()
 	CudaCheck(cudaStreamSynchronize(stream_), "tangent autotune");
 	CudaCheck(cudaEventElapsedTime(&ms, ev[2], ev[3]), "event time");
 	tune_ms_[0] = ms;
-	if (tune_ms_[0] < tune_ms_[1]) {
-		tangent_kernel_ = TFIGA_TANGENT_COEFFICIENTS;
+	// the same arrays contracted element by element (its tangent, equal to the others' up to the order
+	// of the FP32 additions, is the one kept)
+	values32_.Zero(stream_);
+	CudaCheck(cudaEventRecord(ev[2], stream_), "event");
+	LaunchTangentTcElement(view, phi32, coef32_.get(), mesh_.element_blocks(), values32_.get(), status_.get(),
+		operands, stream_);
+	CudaCheck(cudaEventRecord(ev[3], stream_), "event");
+	launches_ += 1;
+	CudaCheck(cudaStreamSynchronize(stream_), "tangent autotune");
+	CudaCheck(cudaEventElapsedTime(&ms, ev[2], ev[3]), "event time");
+	tune_ms_[2] = ms;
+	const double arrays_ms = std::min(tune_ms_[0], tune_ms_[2]);
+	if (arrays_ms < tune_ms_[1]) {
+		tangent_kernel_ = tune_ms_[2] <= tune_ms_[0] ? TFIGA_TANGENT_ELEMENT : TFIGA_TANGENT_COEFFICIENTS;
 		point_state_.Release();
 	} else {
 		tangent_kernel_ = TFIGA_TANGENT_FUSED;
@@ -331,7 +339,7 @@ void NsSolver::AssembleResidual()
 	profiler_.End(stream_);
 	profiler_.Begin(Profiler::kResidual, stream_);
 	LaunchTangentPoint(mesh_.regular_view(), mesh_.phi(), mesh_.qdata(), state_.get(), previous_.get(),
-		{params_.density, params_.viscosity, params_.dt}, nullptr, nullptr, rhs_.get(), queue_.get(), stream_);
+		{params_.density, params_.viscosity, params_.dt}, nullptr, nullptr, rhs_.get(), stream_);
 	LargeElements<double>(nullptr, rhs_.get());
 	profiler_.End(stream_);
 	profiler_.Begin(Profiler::kVector, stream_);
@@ -455,10 +463,6 @@ GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 			if (mixed()) {
 				if (!amg_->built()) amg_->Build(values32_.get());
 				amg_->Refresh(values32_.get(), coarse);
-				if (values16_.size()) {
-					LaunchToBf16((long long)blocks()*16, values32_.get(), values16_.get(), stream_);
-					launches_ += 1;
-				}
 			} else {
 				if (!amg_->built()) amg_->Build(values_.get());
 				amg_->Refresh(values_.get(), coarse);

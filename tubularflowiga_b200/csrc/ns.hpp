@@ -98,7 +98,10 @@ public:
 	// Tensor-core modes: the tangent organisation in use (TFIGA_TANGENT_*; TFIGA_TANGENT_AUTO until the
 	// first tangent has been assembled) and the autotuner's timings of both (ms, 0 if not run).
 	int tangent_kernel() const { return tangent_kernel_; }
-	double tune_ms(int kernel) const { return kernel == TFIGA_TANGENT_FUSED ? tune_ms_[1] : tune_ms_[0]; }
+	double tune_ms(int kernel) const
+	{
+		return kernel == TFIGA_TANGENT_FUSED ? tune_ms_[1] : kernel == TFIGA_TANGENT_ELEMENT ? tune_ms_[2] : tune_ms_[0];
+	}
 	// Binds the current (Dirichlet-row) Jacobian as the operator of the learned stage's residual loss.
 	void BindLearnedOperator(LearnedPreconditioner& learned);
 
@@ -148,13 +151,16 @@ private:
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
 	DeviceArray<float> values32_;
-	DeviceArray<uint16_t> values16_;         // BF16 copy of values32_ for the Krylov products (optional)
 	DeviceArray<float> coef32_;              // tensor-core tangent: point coefficients [e][4][16][80][4]
 	DeviceArray<double> point_state_;        // fused tensor-core tangent: FP64 point state [e][64][22]
 	int tangent_kernel_ = 0;                 // TFIGA_TANGENT_* in use
-	double tune_ms_[2] = {0.0, 0.0};         // autotuner: coefficient-array and fused tangent times
+	double tune_ms_[3] = {0.0, 0.0, 0.0};    // autotuner: coefficient-array (pair), fused, element times
+	bool coefficient_arrays() const
+	{
+		return tangent_kernel_ == TFIGA_TANGENT_COEFFICIENTS || tangent_kernel_ == TFIGA_TANGENT_ELEMENT;
+	}
 	DeviceArray<double> face_flow_, face_pressure_, label_flow_, partial_, scalars_;
-	DeviceArray<int32_t> vmask_, pmask_, constrained_, face_slot_, status_, queue_;
+	DeviceArray<int32_t> vmask_, pmask_, constrained_, face_slot_, status_;
 	std::vector<int32_t> labels_;            // distinct face labels (slot order)
 	std::map<int32_t, int> slot_of_label_;
 	std::vector<int32_t> face_slot_host_;

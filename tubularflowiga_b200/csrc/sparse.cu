@@ -3,8 +3,6 @@
 // tractions, and deterministic two-stage reductions.
 //
 // SpMV layout: one warp per block row (block_row.cuh).
-#include <cuda_bf16.h>
-
 #include "block_row.cuh"
 #include "common.hpp"
 #include "kernels.cuh"
@@ -250,16 +248,6 @@ __global__ void __launch_bounds__(256) SegmentSumKernel(const int32_t* __restric
 
 unsigned Blocks(long long n, int threads) { return (unsigned)((n+threads-1)/threads); }
 
-// out = BF16(in), round to nearest even, two values per thread (raw 16-bit patterns).
-__global__ void ToBf16Kernel(long long n, const float* __restrict__ in, uint16_t* __restrict__ out)
-{
-	const long long i = 2*((long long)blockIdx.x*blockDim.x+threadIdx.x);
-	if (i >= n) return;
-	const __nv_bfloat16 lo = __float2bfloat16_rn(in[i]);
-	out[i] = __bfloat16_as_ushort(lo);
-	if (i+1 < n) out[i+1] = __bfloat16_as_ushort(__float2bfloat16_rn(in[i+1]));
-}
-
 __global__ void ToFloatKernel(long long n, const double* __restrict__ in, float* __restrict__ out)
 {
 	const long long i = (long long)blockIdx.x*blockDim.x+threadIdx.x;
@@ -327,9 +315,6 @@ template void LaunchSpmvBlockJacobi<double>(const DevicePatternView&, const doub
 	const double*, double*, const int*, cudaStream_t);
 template void LaunchSpmvBlockJacobi<float>(const DevicePatternView&, const float*, const double*, const double*,
 	const double*, double*, const int*, cudaStream_t);
-template void LaunchSpmv<uint16_t>(const DevicePatternView&, const uint16_t*, const double*, double*, cudaStream_t);
-template void LaunchSpmvBlockJacobi<uint16_t>(const DevicePatternView&, const uint16_t*, const double*, const double*,
-	const double*, double*, const int*, cudaStream_t);
 template void LaunchBlockInverse<double>(const DevicePatternView&, const double*, double*, unsigned int*, cudaStream_t);
 template void LaunchBlockInverse<float>(const DevicePatternView&, const float*, double*, unsigned int*, cudaStream_t);
 
@@ -354,13 +339,6 @@ void LaunchToFloatPointPairs(long long tables, const double* in, float* out, cud
 	const long long pairs = tables*2048;
 	ToFloatPointPairsKernel<<<Blocks(pairs, 256), 256, 0, stream>>>(pairs, in, out);
 	LaunchCheck("ToFloatPointPairsKernel");
-}
-
-void LaunchToBf16(long long n, const float* in, uint16_t* out, cudaStream_t stream)
-{
-	if (n == 0) return;
-	ToBf16Kernel<<<Blocks(n/2+1, 256), 256, 0, stream>>>(n, in, out);
-	LaunchCheck("ToBf16Kernel");
 }
 
 void LaunchToFloat(long long n, const double* in, float* out, cudaStream_t stream)

@@ -12,17 +12,15 @@
 // B = Psi (K-major), one GEMM of M = 512 x N = 64 x K = 256 per row field.
 //
 // Two kernels.
-//   TangentPointKernel (FP64, persistent, two 256-thread CTAs per SM, one
-//     element at a time; the FP64 tables stream through shared memory with
-//     cp.async one chunk ahead): nodal state, the state at the 64 points
-//     (thread per point and quarter of the basis, the quarters summed by
-//     shuffles), the coefficients M_q of all four row fields (thread per row
-//     field and point, two column-field halves through a shared-memory
-//     scratch) written to a coefficient array laid out [element][row field]
-//     [16 point quads][80 coefficients][4 points] (a K chunk's coefficients of
-//     one row field are one contiguous run), and the FP64 residual (thread per
-//     basis function and pair of points of each chunk, one read of each basis
-//     value for the four row fields) added into rhs.
+//   TangentPointKernel (FP64, CTA per element, 256 threads): nodal state, the
+//     state at the 64 points (thread per point and quarter of the basis, the
+//     quarters summed in shared memory), the coefficients M_q of all four row
+//     fields (thread per row field and point, two column-field halves through
+//     a shared-memory scratch) written to a coefficient array laid out
+//     [element][row field][16 point quads][80 coefficients][4 points] (a K
+//     chunk's coefficients of one row field are one contiguous run), and the
+//     FP64 residual (thread per basis function and quarter of the points, one
+//     read of each basis value for the four row fields) added into rhs.
 //   TangentTcKernel (CTA per element and row-field pair h: i in {2h, 2h+1},
 //     256 threads, 4 M = 128 accumulator tiles in 256 TMEM columns; tile T:
 //     row field 2h + T/2, basis b in [32 (T&1), +32), tile row m = 4 (b mod
@@ -68,6 +66,7 @@ constexpr int kTileBytes = 128*64;               // 128 rows x 32 BF16 (64 B, on
 constexpr int kTmemCols = 256;                   // 4 tiles x N = 64 FP32 columns
 constexpr unsigned long long kWaitNs = 1000000000ull;
 constexpr int kRcStride = 5;                     // doubles per (field, point) residual coefficient row
+constexpr int kPartStride = 23;                  // odd double stride of the point-state partial sums
 constexpr int kScratchStride = 41;               // odd float stride of the per-thread coefficient scratch
 
 // TangentTcKernel shared memory (bytes from a 1024-aligned base).
@@ -88,26 +87,19 @@ constexpr int kTcSmemBytes = kOffBar+32+1024;                     // + alignment
 static_assert(kTcSmemBytes <= 113*1024, "two CTAs per SM");
 static_assert(kOffOp1 % 1024 == 0, "operand buffers 1024-aligned");
 
-// TangentPointKernel shared memory (bytes from a 16-aligned base).  Two staging buffers, each either
-// a point-state chunk -- 8 basis functions of the five tables at the 64 points, rows of kPtRow
-// doubles (8 values, 4 pad: 96 B, 16-byte aligned for cp.async, and 8-byte reads across the points
-// of a warp conflict-free) -- or a residual chunk -- the four tables N, dN/dx at 8 points, rows of the
-// 64 functions.  The coefficient scratch (float [256][kScratchStride]) overlays both buffers.
-constexpr int kPtChunkB = 8;                                      // functions per point-state chunk
-constexpr int kPtRow = 12;                                        // doubles per staged (table, point) row
-constexpr int kPtChunkQ = 8;                                      // points per residual chunk
-constexpr int kPtBufBytes = kFeatures*kQuad*kPtRow*8;             // 30,720
-constexpr int kPtOffBuf = 0;                                      // two staging buffers
-constexpr int kPtOffU = 2*kPtBufBytes;                            // double [4 fields][64]
+// TangentPointKernel shared memory (bytes).
+constexpr int kPtOffU = 0;                                        // double [4 fields][64]
 constexpr int kPtOffUp = kPtOffU+64*4*8;                          // double [4 fields][64]
-constexpr int kPtOffQS = kPtOffUp+64*4*8;                         // double [64][kQS] (later: residual partials)
+constexpr int kPtOffPart = kPtOffUp+64*4*8;                       // double [4][64][kPartStride]
+constexpr int kPtPartBytes = 4*64*kPartStride*8;                  // (later: float [256][kScratchStride])
+constexpr int kPtOffQS = kPtOffPart+kPtPartBytes;                 // double [64][kQS]
 constexpr int kPtOffRC = kPtOffQS+kQuad*kQS*8;                    // double [4][64][kRcStride]
 constexpr int kPtSmemBytes = kPtOffRC+4*kQuad*kRcStride*8;
-static_assert(kTcThreads*kScratchStride*4 <= 2*kPtBufBytes, "coefficient scratch fits in the staging buffers");
-static_assert(4*kPtChunkQ*kMaxBasis*8 <= kPtBufBytes, "residual chunk fits in a staging buffer");
-static_assert(4*4*64*8 <= kQuad*kQS*8, "residual partial sums fit in the point-state slots");
-static_assert(2*kPtSmemBytes+32 <= 228*1024, "two CTAs per SM");
+static_assert(kTcThreads*kScratchStride*4 <= kPtPartBytes, "coefficient scratch fits in the partial sums");
+constexpr int kStageBasis = 16;                  // basis functions per staged chunk of the point-state stage
 constexpr int kPointStride = 22;                 // doubles per point of the stored point state (kU .. kLap+2)
+constexpr int kStageStride = kStageBasis+1;      // odd double stride of a staged (feature, point) row
+static_assert(kFeatures*kQuad*kStageStride*8 <= kPtPartBytes, "staged basis chunk fits in the partial sums");
 
 // Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B BF16, both
 // K-major, M = 128, N = 64.
@@ -302,10 +294,10 @@ __device__ __forceinline__ void RedAdd4(float* p, float a, float b, float c, flo
 
 // Basis chunk c (points NP c .. NP c + NP - 1, five features, 64 functions) of
 // one element, FP32 with the points of each pair interleaved (the layout of
-// Mesh::phi32), into a [5][NP/2][64][2] buffer; the coefficients of the two row
-// fields 2h, 2h+1 at those points into a [2][80][NP] buffer (padded per group of
-// 20 rows).  One commit group.
-template <int NP>
+// Mesh::phi32), into a [5][NP/2][64][2] buffer; the coefficients of kRows row
+// fields (from CF on) at those points into a [kRows][80][NP] buffer (padded per
+// group of 20 rows).  One commit group.
+template <int NP, int kRows = 2>
 __device__ __forceinline__ void PrefetchChunk(const float* P32, const float* CF, int c, uint32_t phi_dst,
 	uint32_t cf_dst, int tid)
 {
@@ -313,7 +305,7 @@ __device__ __forceinline__ void PrefetchChunk(const float* P32, const float* CF,
 		const int t = idx/(NP*16), rem = idx%(NP*16);
 		CopyAsync16(phi_dst+16*idx, P32+(size_t)(t*kQuad+c*NP)*kMaxBasis+4*rem);
 	}
-	for (int idx = tid; idx < 2*kCoef*NP/4; idx += kTcThreads) {
+	for (int idx = tid; idx < kRows*kCoef*NP/4; idx += kTcThreads) {
 		const int rk = idx/(NP/4), part = idx%(NP/4);           // rk = row field * 80 + k
 		const int row = rk/kCoef, k = rk%kCoef;
 		CopyAsync16(cf_dst+16*idx+(rk/20)*kCfPad*4, CF+(size_t)row*kCoef*kQuad+((c*(NP/4)+part)*kCoef+k)*4);
@@ -342,69 +334,29 @@ __device__ __forceinline__ void PointCoefficients(const PointState& S, const dou
 // (TangentTcFusedKernel).
 enum : int { kPointResidual = 0, kPointCoefficients = 1, kPointState = 2 };
 
-// Point-state chunk c of an element's FP64 tables (functions 8c .. 8c + 7 of the five tables at the 64
-// points) into a staging buffer of kPtRow-double rows: four 16-byte copies per row.  One commit group.
-__device__ __forceinline__ void StagePointChunk(const double* P, int c, uint32_t dst, int tid)
-{
-	#pragma unroll
-	for (int i = tid; i < kFeatures*kQuad*4; i += kTcThreads) {
-		const int row = i >> 2, piece = i & 3;                       // row = table * 64 + point
-		CopyAsync16(dst+(row*kPtRow+2*piece)*8, P+(size_t)row*kMaxBasis+kPtChunkB*c+2*piece);
-	}
-	CopyAsyncCommit();
-}
-
-// Residual chunk c (points 8c .. 8c + 7 of the tables N, dN/dx_d) into [4][8][64]: each table's eight
-// rows are one contiguous 4 KiB run.  One commit group.
-__device__ __forceinline__ void StageResidualChunk(const double* P, int c, uint32_t dst, int tid)
-{
-	#pragma unroll
-	for (int i = tid; i < 4*kPtChunkQ*kMaxBasis/2; i += kTcThreads) {
-		const int t = i >> 8, rem = i & 255;                         // 256 copies per table
-		CopyAsync16(dst+(t*kPtChunkQ*kMaxBasis+2*rem)*8, P+(size_t)(t*kQuad+kPtChunkQ*c)*kMaxBasis+2*rem);
-	}
-	CopyAsyncCommit();
-}
-
-// Persistent: each CTA takes elements from a work queue (*queue, zeroed by the launcher), claiming the
-// next element as it starts on the current one.  The FP64 tables stream through two shared-memory
-// staging buffers with cp.async, one chunk ahead of the arithmetic: eight point-state chunks, then
-// eight residual chunks (read again, from L2), and during the last two residual chunks the next
-// element's first two point-state chunks.  Exactly two copy groups are in flight at the top of every
-// chunk (empty groups where there is nothing to fetch), so each chunk waits for the older one.
 template <int kMode>
 __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshView mesh,
 	const double* __restrict__ phi, const double* __restrict__ qdata, const double* __restrict__ state,
 	const double* __restrict__ previous, AssemblyParams prm, float* __restrict__ coef,
-	double* __restrict__ point_state, double* __restrict__ rhs, int* __restrict__ queue)
+	double* __restrict__ point_state, double* __restrict__ rhs)
 {
 	extern __shared__ uint8_t smem_raw[];
 	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+15) & ~uintptr_t(15));
-	const uint32_t sBuf[2] = {SmemAddress(sm+kPtOffBuf), SmemAddress(sm+kPtOffBuf+kPtBufBytes)};
 	double* U = reinterpret_cast<double*>(sm+kPtOffU);
 	double* Up = reinterpret_cast<double*>(sm+kPtOffUp);
-	float* Scratch = reinterpret_cast<float*>(sm+kPtOffBuf);
+	double* Part = reinterpret_cast<double*>(sm+kPtOffPart);
+	float* Scratch = reinterpret_cast<float*>(sm+kPtOffPart);
 	double* QS = reinterpret_cast<double*>(sm+kPtOffQS);
 	double* RC = reinterpret_cast<double*>(sm+kPtOffRC);
-	__shared__ int next;
 
-	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-	if (tid == 0) next = atomicAdd(queue, 1);
-	__syncthreads();
-	int e = next;
-	if (e < mesh.elements) {
-		const double* P0 = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
-		StagePointChunk(P0, 0, sBuf[0], tid);
-		StagePointChunk(P0, 1, sBuf[1], tid);
-	}
-	while (e < mesh.elements) {
-	__syncthreads();                                 // every thread has read next
-	if (tid == 0) next = atomicAdd(queue, 1);
+	const int e = blockIdx.x;
+	const int tid = threadIdx.x;
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
+	if (tid == 0) PrefetchL2(P, kFeatures*kQuad*kMaxBasis*8);
 
-	// 1. Nodal state (the element's first two point-state chunks are in flight).
+	// 1. Nodal state.
 	if (tid < kMaxBasis) {
 		const int a = tid;
 		double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, p0 = 0.0, p1 = 0.0, p2 = 0.0;
@@ -416,24 +368,34 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 		U[a] = s0; U[64+a] = s1; U[128+a] = s2; U[192+a] = s3;
 		Up[a] = p0; Up[64+a] = p1; Up[128+a] = p2; Up[192+a] = 0.0;
 	}
+	__syncthreads();
 
-	// 2. State at every point (FP64): thread (point q = 8 warp + lane / 4, function quarter aq = lane % 4)
-	//    takes functions aq and aq + 4 of every chunk, so the 32 lanes' reads of a row fall in distinct
-	//    bank pairs two by two; the four quarters of a point are adjacent lanes and meet by shuffles.
+	// 2. State at every point (FP64): the basis tables are staged 16 functions at a time in shared
+	//    memory with coalesced 16-byte loads (rows of 17 doubles, so that 8-byte reads across the
+	//    points of a warp are conflict-free); thread (point q, quarter aq) takes 4 functions of each
+	//    chunk; the four quarters meet in shared memory.  The staging buffer overlays the partial
+	//    sums, which are written only after the last chunk has been read.
 	{
-		const int q = 8*warp+(lane >> 2), aq = lane & 3;
+		double* Stage = Part;
+		const int q = tid & 63, aq = tid >> 6;
 		double v[22];
 		#pragma unroll
 		for (int k = 0; k < 22; ++k) v[k] = 0.0;
-		for (int c = 0; c < kMaxBasis/kPtChunkB; ++c) {
-			CopyAsyncWait<1>();                          // chunk c (this thread's copies)
-			__syncthreads();                             // ... and every thread's (and U, Up at c = 0)
-			const double* row = reinterpret_cast<const double*>(sm+kPtOffBuf+(c & 1)*kPtBufBytes)+q*kPtRow;
+		for (int a0 = 0; a0 < kMaxBasis; a0 += kStageBasis) {
+			if (a0) __syncthreads();                 // the previous chunk has been read
+			for (int idx = tid; idx < kFeatures*kQuad*(kStageBasis/2); idx += kTcThreads) {
+				const int row = idx/(kStageBasis/2), k = idx%(kStageBasis/2);     // row = t*64 + point
+				const double2 w = *reinterpret_cast<const double2*>(P+(size_t)row*kMaxBasis+a0+2*k);
+				Stage[row*kStageStride+2*k] = w.x;
+				Stage[row*kStageStride+2*k+1] = w.y;
+			}
+			__syncthreads();
 			#pragma unroll
-			for (int jj = 0; jj < 2; ++jj) {
-				const int j = aq+4*jj, b = kPtChunkB*c+j;
-				const double n = row[j], g0 = row[kQuad*kPtRow+j], g1 = row[2*kQuad*kPtRow+j];
-				const double g2 = row[3*kQuad*kPtRow+j], l = row[4*kQuad*kPtRow+j];
+			for (int jj = 0; jj < kStageBasis/4; ++jj) {
+				const int j = aq*(kStageBasis/4)+jj, b = a0+j;
+				const double n = Stage[(0*kQuad+q)*kStageStride+j], g0 = Stage[(1*kQuad+q)*kStageStride+j];
+				const double g1 = Stage[(2*kQuad+q)*kStageStride+j], g2 = Stage[(3*kQuad+q)*kStageStride+j];
+				const double l = Stage[(4*kQuad+q)*kStageStride+j];
 				const double uf[4] = {U[b], U[64+b], U[128+b], U[192+b]};
 				v[0] += n*uf[0]; v[1] += n*uf[1]; v[2] += n*uf[2]; v[3] += n*uf[3];
 				v[4] += n*Up[b]; v[5] += n*Up[64+b]; v[6] += n*Up[128+b];
@@ -441,29 +403,26 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 				for (int f = 0; f < 4; ++f) { v[7+3*f] += g0*uf[f]; v[8+3*f] += g1*uf[f]; v[9+3*f] += g2*uf[f]; }
 				v[19] += l*uf[0]; v[20] += l*uf[1]; v[21] += l*uf[2];
 			}
-			__syncthreads();                             // buffer c & 1 has been read
-			if (c+2 < kMaxBasis/kPtChunkB) StagePointChunk(P, c+2, sBuf[c & 1], tid);
-			else if constexpr (kMode != kPointCoefficients) StageResidualChunk(P, c+2-kMaxBasis/kPtChunkB, sBuf[c & 1], tid);
-			else CopyAsyncCommit();                      // (the coefficient scratch takes the buffers next)
 		}
+		__syncthreads();                             // the last chunk has been read
+		double* part = Part+(aq*kQuad+q)*kPartStride;
 		#pragma unroll
-		for (int k = 0; k < 22; ++k) {
-			v[k] += __shfl_xor_sync(0xffffffffu, v[k], 1);
-			v[k] += __shfl_xor_sync(0xffffffffu, v[k], 2);
-		}
-		#pragma unroll
-		for (int k = 0; k < 22; ++k)
-			if ((k & 3) == aq) {
-				QS[q*kQS+k] = v[k];
-				if constexpr (kMode == kPointState) point_state[((size_t)e*kQuad+q)*kPointStride+k] = v[k];
-			}
+		for (int k = 0; k < 22; ++k) part[k] = v[k];
+	}
+	__syncthreads();
+	for (int idx = tid; idx < kQuad*22; idx += kTcThreads) {
+		const int q = idx/22, k = idx%22;
+		const double* part = Part+q*kPartStride+k;
+		const double v = ((part[0]+part[kQuad*kPartStride])+part[2*kQuad*kPartStride])+part[3*kQuad*kPartStride];
+		QS[q*kQS+k] = v;
+		if constexpr (kMode == kPointState) point_state[(size_t)e*kQuad*kPointStride+idx] = v;
 	}
 	__syncthreads();
 
 	// 3. Coefficients: thread (row field il, point q), two column-field halves through the
-	//    scratch, stored coalesced over the points of a quad.  The row field is uniform over a warp
-	//    and a compile-time constant of each branch, so the point state and the coefficient
-	//    temporaries stay in registers.
+	//    scratch (the partial sums are dead), stored coalesced over the points.  The row field is
+	//    uniform over a warp and a compile-time constant of each branch, so the point state and the
+	//    coefficient temporaries stay in registers.
 	{
 		const int q = tid & 63, il = tid >> 6;
 		PointState S;
@@ -495,51 +454,30 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 			}
 		}
 	}
-	__syncthreads();                                 // RC complete; the scratch is dead
-	const int en = next;                             // the next element (claimed at the top)
-	if constexpr (kMode == kPointCoefficients) {
-		// the two residual chunks the other modes fetched during the point-state stage (the two empty
-		// groups committed there are complete once these are waited for)
-		StageResidualChunk(P, 0, sBuf[0], tid);
-		StageResidualChunk(P, 1, sBuf[1], tid);
-	}
+	__syncthreads();
 
-	// 4. FP64 residual of the four row fields (rhs holds -r): thread (basis function a, point pair qq
-	//    of each chunk) reads each table value once for all four row fields; the four pairs meet in
-	//    shared memory (the point-state slots are dead).
+	// 4. FP64 residual of the four row fields (rhs holds -r): thread (basis function a, quarter
+	//    qq of the points) reads each basis value once for all four row fields; the quarters meet
+	//    in shared memory (the coefficient scratch is dead).
 	{
 		const int a = tid & 63, qq = tid >> 6;
 		double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
-		for (int c = 0; c < kQuad/kPtChunkQ; ++c) {
-			CopyAsyncWait<1>();
-			__syncthreads();
-			const double* B4 = reinterpret_cast<const double*>(sm+kPtOffBuf+(c & 1)*kPtBufBytes);
+		for (int q = qq*16; q < qq*16+16; ++q) {
 			#pragma unroll
-			for (int p = 0; p < 2; ++p) {
-				const int ql = 2*qq+p, q = kPtChunkQ*c+ql;
-				#pragma unroll
-				for (int s = 0; s < 4; ++s) {
-					const double v = B4[(s*kPtChunkQ+ql)*kMaxBasis+a];
-					r0 += v*RC[(0*kQuad+q)*kRcStride+s];
-					r1 += v*RC[(1*kQuad+q)*kRcStride+s];
-					r2 += v*RC[(2*kQuad+q)*kRcStride+s];
-					r3 += v*RC[(3*kQuad+q)*kRcStride+s];
-				}
+			for (int s = 0; s < 4; ++s) {
+				const double v = P[(s*kQuad+q)*kMaxBasis+a];
+				r0 += v*RC[(0*kQuad+q)*kRcStride+s];
+				r1 += v*RC[(1*kQuad+q)*kRcStride+s];
+				r2 += v*RC[(2*kQuad+q)*kRcStride+s];
+				r3 += v*RC[(3*kQuad+q)*kRcStride+s];
 			}
-			__syncthreads();                             // buffer c & 1 has been read
-			if (c+2 < kQuad/kPtChunkQ) StageResidualChunk(P, c+2, sBuf[c & 1], tid);
-			else if (en < mesh.elements)
-				StagePointChunk(phi+(size_t)en*kFeatures*kQuad*kMaxBasis, c+2-kQuad/kPtChunkQ, sBuf[c & 1], tid);
-			else CopyAsyncCommit();
 		}
-		double* red = QS;                            // [4 pairs][4 row fields][64]
+		double* red = Part;                     // [4 quarters][4 row fields][64]
 		red[(qq*4+0)*64+a] = r0; red[(qq*4+1)*64+a] = r1; red[(qq*4+2)*64+a] = r2; red[(qq*4+3)*64+a] = r3;
 		__syncthreads();
 		const int il = tid >> 6;
 		const double r = ((red[(0*4+il)*64+a]+red[(1*4+il)*64+a])+red[(2*4+il)*64+a])+red[(3*4+il)*64+a];
 		if (a < nen) atomicAdd(rhs+4*(size_t)mesh.connectivity[begin+a]+il, r);
-	}
-	e = en;
 	}
 }
 
@@ -781,6 +719,273 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentTcKernel(DeviceMeshView 
 	if (warp == 0) {
 		FenceAfterSync();
 		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTmemCols)
+			: "memory");
+	}
+}
+
+// ---- element variant: one persistent CTA per SM, all four row fields ---------------------------------
+// TangentTcQuadKernel: the contraction of TangentTcKernel for all four row fields of an element in one
+// CTA, so that the basis chunk is staged and Psi built once per element instead of once per row-field
+// pair, and each G-building thread keeps the coefficients of two row fields in registers and reuses
+// every basis value it loads for both (half the basis loads per G entry).  Eight M = 128 accumulator
+// tiles (row field il, basis half) fill the 512 TMEM columns, so one CTA runs per SM; it is persistent
+// (elements blockIdx.x, + gridDim.x, ...), keeps its tensor memory and mbarriers across elements, and
+// fetches the next element's first two chunks before the epilogue of the current one.
+constexpr int kQTiles = 8;
+constexpr int kQTmemCols = 512;
+constexpr int kQOperandBytes = kQTiles*kTileBytes+64*64;          // A tiles + B, 68 KiB
+constexpr int kQOffOp0 = 0;
+constexpr int kQOffOp1 = kQOperandBytes;
+constexpr int kQOffPhi0 = 2*kQOperandBytes;
+constexpr int kQOffPhi1 = kQOffPhi0+kPhiBytes;
+constexpr int kQCfBytes = (4*kCoef*kMaxPts+16*kCfPad)*4;           // float [4 rows][80][NP], padded
+constexpr int kQOffCf0 = kQOffPhi1+kPhiBytes;
+constexpr int kQOffCf1 = kQOffCf0+kQCfBytes;
+constexpr int kQOffBar = kQOffCf1+kQCfBytes;                       // 2 mbarriers, TMEM slot
+constexpr int kQSmemBytes = kQOffBar+32+1024;
+static_assert(kQSmemBytes <= 227*1024, "element tangent shared memory");
+static_assert(kQOffOp1 % 1024 == 0, "operand buffers 1024-aligned");
+
+template <int kMode>
+__global__ void __launch_bounds__(kTcThreads, 1) TangentTcQuadKernel(DeviceMeshView mesh,
+	const float* __restrict__ phi32, const float* __restrict__ coef, const int32_t* __restrict__ element_blocks,
+	float* __restrict__ values, int* __restrict__ status)
+{
+	constexpr bool kSplit = kMode == kModeSplit, kTf32 = kMode == kModeTf32;
+	constexpr bool kFour = kMode != kModeBf16;   // four points (K = 16) per chunk
+	constexpr int NP = kFour ? 4 : kMaxPts;      // points per K chunk
+	constexpr int kChunks = kQuad/NP;            // even: chunk c of every element uses buffer c & 1
+	static_assert(kChunks % 2 == 0, "chunks per element");
+	extern __shared__ uint8_t smem_raw[];
+	uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw)+1023) & ~uintptr_t(1023));
+	const uint32_t sOp[2] = {SmemAddress(sm+kQOffOp0), SmemAddress(sm+kQOffOp1)};
+	const uint32_t sPhi[2] = {SmemAddress(sm+kQOffPhi0), SmemAddress(sm+kQOffPhi1)};
+	const uint32_t sCf[2] = {SmemAddress(sm+kQOffCf0), SmemAddress(sm+kQOffCf1)};
+	uint64_t* bars = reinterpret_cast<uint64_t*>(sm+kQOffBar);
+	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm+kQOffBar+16);
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const size_t kPhiPer = (size_t)kFeatures*kQuad*kMaxBasis, kCfPer = (size_t)4*kCoef*kQuad;
+
+	int e = blockIdx.x;
+	if (e >= mesh.elements) return;
+	PrefetchChunk<NP, 4>(phi32+e*kPhiPer, coef+e*kCfPer, 0, sPhi[0], sCf[0], tid);
+	PrefetchChunk<NP, 4>(phi32+e*kPhiPer, coef+e*kCfPer, 1, sPhi[1], sCf[1], tid);
+	if (warp == 0) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+			:: "r"(SmemAddress(tmem_slot)), "r"(kQTmemCols) : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	if (tid == 32) { MbarInit(bars); MbarInit(bars+1); }
+	FenceBeforeSync();
+	__syncthreads();
+	FenceAfterSync();
+	const uint32_t tmem = *tmem_slot;
+
+	// G builder: warp -> (row-field pair ip: rows 2 ip, 2 ip + 1; point pair / basis quarter gqp);
+	// lane -> (column field gf, basis sub-index gbs).
+	const int ip = warp >> 2, gqp = warp & 3;
+	const int gf = lane & 3, gbs = lane >> 2;
+	bool failed = false;
+	long long done = 0;                              // chunks of the elements before this one
+	long long committed = 0;                         // chunks whose MMAs were committed
+	for (; e < mesh.elements; e += gridDim.x) {
+		const int begin = mesh.element_offsets[e];
+		const int nen = mesh.element_offsets[e+1]-begin;
+		const float* P32 = phi32+e*kPhiPer;
+		const float* CF = coef+e*kCfPer;
+		const int en = e+(int)gridDim.x;
+		// the next element's tables into L2 while this one is contracted
+		if (tid == 0 && en < mesh.elements) {
+			PrefetchL2(phi32+en*kPhiPer, (int)(kPhiPer*4));
+			PrefetchL2(coef+en*kCfPer, (int)(kCfPer*4));
+		}
+		CopyAsyncWait<1>();                          // chunk 0 (this thread's copies)
+		__syncthreads();                             // ... and every thread's
+		for (int c = 0; c < kChunks; ++c) {
+			const long long gc = done+c;             // chunk index over the CTA's lifetime
+			const int buf = c & 1;
+			const float* PhiS = reinterpret_cast<const float*>(sm+(buf ? kQOffPhi1 : kQOffPhi0));
+			const float* CfS = reinterpret_cast<const float*>(sm+(buf ? kQOffCf1 : kQOffCf0));
+			const uint32_t sA = sOp[buf], sB = sOp[buf]+kQTiles*kTileBytes;
+			// B = Psi (as in TangentTcKernel), built once for all four row fields.
+			{
+				const int u = tid >> 6, a = tid & 63;
+				const float2* pairs = reinterpret_cast<const float2*>(PhiS);
+				if constexpr (kTf32) {
+					const int qp = u >> 1, s0 = 2*(u & 1);
+					const float2 x0 = pairs[(s0*(NP/2)+qp)*64+a], x1 = pairs[((s0+1)*(NP/2)+qp)*64+a];
+					StoreShared16(sB+Sw64(a, u), Tf32(x0.x), Tf32(x0.y), Tf32(x1.x), Tf32(x1.y));
+				} else {
+					const int qp = kSplit ? (u & 1) : u;
+					float x[8];
+					#pragma unroll
+					for (int s = 0; s < 4; ++s) {
+						const float2 v = pairs[(s*(NP/2)+qp)*64+a];
+						x[2*s] = v.x;
+						x[2*s+1] = v.y;
+					}
+					if (kSplit && u >= 2) {
+						#pragma unroll
+						for (int k = 0; k < 8; ++k) x[k] = Bf16Residual(x[k]);
+					}
+					StoreShared16(sB+Sw64(a, u), PackBf16(x[0], x[1]), PackBf16(x[2], x[3]), PackBf16(x[4], x[5]),
+						PackBf16(x[6], x[7]));
+				}
+			}
+			// A = G for row fields 2 ip and 2 ip + 1: each basis pair pb feeds both rows' products.
+			{
+				const int qpair = kFour ? (gqp & 1) : gqp;
+				const int ql0 = 2*qpair;
+				constexpr int kGroups = kFour ? 4 : 8;
+				const int g0 = kFour ? (gqp >> 1)*4 : 0;
+				unsigned long long mm[2][20];
+				#pragma unroll
+				for (int r = 0; r < 2; ++r) {
+					const int il = 2*ip+r;
+					const float* c0 = CfS+(il*kCoef+gf*20)*NP+(il*4+gf)*kCfPad+ql0;
+					#pragma unroll
+					for (int k = 0; k < 20; ++k) mm[r][k] = *reinterpret_cast<const unsigned long long*>(c0+k*NP);
+				}
+				#pragma unroll 1
+				for (int j = 0; j < kGroups; ++j) {
+					const int b = (g0+j)*8+gbs;
+					unsigned long long pb[5];
+					#pragma unroll
+					for (int t = 0; t < 5; ++t)
+						pb[t] = *reinterpret_cast<const unsigned long long*>(PhiS+((t*(NP/2)+qpair)*64+b)*2);
+					#pragma unroll
+					for (int r = 0; r < 2; ++r) {
+						unsigned long long gg[4];
+						#pragma unroll
+						for (int s = 0; s < 4; ++s) {
+							gg[s] = Mul2(mm[r][s*5], pb[0]);
+							#pragma unroll
+							for (int t = 1; t < 5; ++t) gg[s] = Fma2(mm[r][s*5+t], pb[t], gg[s]);
+						}
+						const int tile = (2*ip+r)*2+(b >> 5), row = (b & 31)*4+gf;
+						const uint32_t dst = sA+tile*kTileBytes;
+						if constexpr (kTf32) {
+							StoreShared16(dst+Sw64(row, 2*qpair), Tf32(Low(gg[0])), Tf32(High(gg[0])), Tf32(Low(gg[1])),
+								Tf32(High(gg[1])));
+							StoreShared16(dst+Sw64(row, 2*qpair+1), Tf32(Low(gg[2])), Tf32(High(gg[2])), Tf32(Low(gg[3])),
+								Tf32(High(gg[3])));
+						} else {
+							uint32_t hi[4];
+							#pragma unroll
+							for (int s = 0; s < 4; ++s) hi[s] = Bf16Pair(gg[s]);
+							StoreShared16(dst+Sw64(row, qpair), hi[0], hi[1], hi[2], hi[3]);
+							if (kSplit) {
+								uint32_t lo[4];
+								#pragma unroll
+								for (int s = 0; s < 4; ++s) lo[s] = Bf16Pair(Sub2(gg[s], WidenBf16Pair(hi[s])));
+								StoreShared16(dst+Sw64(row, 2+qpair), lo[0], lo[1], lo[2], lo[3]);
+							}
+						}
+					}
+				}
+			}
+			FenceProxyAsync();
+			CopyAsyncWait<0>();                      // chunk c + 1 (the only group in flight)
+			bool ok = true;
+			// the MMAs of chunk gc - 1 (this element's previous chunk, or the previous element's last)
+			// were the last users of operand buffer (c + 1) & 1
+			if (tid == 0 && gc >= 1) ok = MbarWaitBounded(bars+((gc-1) & 1), (uint32_t)(((gc-1) >> 1) & 1));
+			if (__syncthreads_or(!ok)) { failed = true; break; }
+			if (tid == 0) {
+				FenceAfterSync();
+				#pragma unroll
+				for (int tile = 0; tile < kQTiles; ++tile) {
+					const uint32_t a = sA+tile*kTileBytes;
+					if constexpr (kTf32) {
+						#pragma unroll
+						for (int ks = 0; ks < 2; ++ks)
+							MmaTf32(tmem+tile*64, DescSw64(a+ks*32), DescSw64(sB+ks*32), (c > 0 || ks > 0) ? 1u : 0u);
+					} else if (kSplit) {
+						MmaBf16(tmem+tile*64, DescSw64(a), DescSw64(sB), c > 0 ? 1u : 0u);
+						MmaBf16(tmem+tile*64, DescSw64(a), DescSw64(sB+32), 1u);
+						MmaBf16(tmem+tile*64, DescSw64(a+32), DescSw64(sB), 1u);
+					} else {
+						#pragma unroll
+						for (int ks = 0; ks < 2; ++ks)
+							MmaBf16(tmem+tile*64, DescSw64(a+ks*32), DescSw64(sB+ks*32), (c > 0 || ks > 0) ? 1u : 0u);
+					}
+				}
+				MmaCommit(bars+buf);
+			}
+			committed = gc+1;
+			// the staging buffers of chunk c are free: fetch chunk c + 2, or the next element's chunk
+			// c + 2 - kChunks (an empty group after the last element)
+			if (c+2 < kChunks) PrefetchChunk<NP, 4>(P32, CF, c+2, sPhi[buf], sCf[buf], tid);
+			else if (en < mesh.elements)
+				PrefetchChunk<NP, 4>(phi32+en*kPhiPer, coef+en*kCfPer, c+2-kChunks, sPhi[buf], sCf[buf], tid);
+			else CopyAsyncCommit();
+		}
+		if (failed) break;
+		done += kChunks;
+		// every thread observes the element's last commit itself before it reads the accumulators
+		if (__syncthreads_or(!MbarWaitBounded(bars+((done-1) & 1), (uint32_t)(((done-1) >> 1) & 1)))) {
+			failed = true;
+			break;
+		}
+		// Epilogue (as in TangentTcKernel) for row-field pairs p = 0, 1: warp -> (basis half bh, TMEM lane
+		// quarter); tile (row field il, half bh) sits in columns (2 il + bh) 64.
+		FenceAfterSync();
+		{
+			const int bh = warp >> 2, quarter = warp & 3;
+			const int32_t* EB = element_blocks+(size_t)e*kMaxBasis*kMaxBasis;
+			const int f = lane & 3;
+			const int b = bh*32+quarter*8+(lane >> 2);
+			for (int p = 0; p < 2; ++p) {
+				float* row_base = values+(size_t)(2*p+(f & 1))*4;
+				for (int ah = 0; ah < 2; ++ah) {
+					int blocks[2][8];
+					#pragma unroll
+					for (int g = 0; g < 8; ++g)
+						#pragma unroll
+						for (int q = 0; q < 2; ++q) {
+							const int a = ah*32+4*g+(f & 2)+q;
+							blocks[q][g] = (a < nen && b < nen) ? EB[a*kMaxBasis+b] : -1;
+						}
+					float v0[32], v1[32];
+					const uint32_t lanes = (uint32_t)(quarter*32) << 16;
+					TmemLoad32(tmem+lanes+(4*p+bh)*64+ah*32, v0);          // row field 2p
+					TmemLoad32(tmem+lanes+(4*p+2+bh)*64+ah*32, v1);        // row field 2p + 1
+					#pragma unroll
+					for (int g = 0; g < 8; ++g)
+						#pragma unroll
+						for (int q = 0; q < 2; ++q) {
+							const float c00 = v0[4*g+q], c02 = v0[4*g+2+q], c10 = v1[4*g+q], c12 = v1[4*g+2+q];
+							float o0 = 0.f, o1 = 0.f, o2 = 0.f, o3 = 0.f;
+							#pragma unroll
+							for (int r = 0; r < 4; ++r) {
+								const int d = f ^ r;
+								const float send = (d & 1) ? ((d & 2) ? c12 : c10) : ((d & 2) ? c02 : c00);
+								const float got = r ? __shfl_xor_sync(0xffffffffu, send, r) : send;
+								o0 = d == 0 ? got : o0; o1 = d == 1 ? got : o1;
+								o2 = d == 2 ? got : o2; o3 = d == 3 ? got : o3;
+							}
+							if (blocks[q][g] >= 0) RedAdd4(row_base+(size_t)blocks[q][g]*16, o0, o1, o2, o3);
+						}
+				}
+			}
+		}
+		// the accumulators have been read before the next element's first MMAs overwrite them
+		FenceBeforeSync();
+		__syncthreads();
+		FenceAfterSync();
+	}
+	if (failed) {
+		if (tid == 0) atomicOr(status, 1);
+		CopyAsyncWait<0>();
+		// let this CTA's own MMAs drain before freeing TMEM: the newest commit covers all earlier ones
+		if (tid == 0 && committed > 0)
+			MbarWaitBounded(bars+((committed-1) & 1), (uint32_t)(((committed-1) >> 1) & 1));
+	}
+	FenceBeforeSync();
+	__syncthreads();
+	if (warp == 0) {
+		FenceAfterSync();
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kQTmemCols)
 			: "memory");
 	}
 }
@@ -1097,12 +1302,10 @@ int MultiprocessorCount()
 } // namespace
 
 void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const double* qdata, const double* state,
-	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs, int* queue,
-	cudaStream_t stream)
+	const double* previous, AssemblyParams params, float* coef, double* point_state, double* rhs, cudaStream_t stream)
 {
 	if (mesh.elements == 0) return;
 	if (rhs == nullptr) Fail(-1, "tangent point kernel: the residual output is required");
-	if (queue == nullptr) Fail(-1, "tangent point kernel: the work-queue counter is required");
 	if (coef && point_state) Fail(-1, "tangent point kernel: coefficients or point state, not both");
 	static bool configured = false;
 	if (!configured) {
@@ -1114,19 +1317,17 @@ void LaunchTangentPoint(const DeviceMeshView& mesh, const double* phi, const dou
 			kPtSmemBytes+16), "tangent point-kernel shared-memory attribute");
 		configured = true;
 	}
-	// two persistent CTAs per SM (the kernel's occupancy), no more than there are elements
-	const unsigned grid = (unsigned)std::min<long long>(mesh.elements, 2LL*MultiprocessorCount());
+	const unsigned grid = (unsigned)mesh.elements;
 	const size_t bytes = kPtSmemBytes+16;
-	CudaCheck(cudaMemsetAsync(queue, 0, sizeof(int), stream), "point-kernel work queue");
 	if (coef)
 		TangentPointKernel<kPointCoefficients><<<grid, kTcThreads, bytes, stream>>>(mesh, phi, qdata, state, previous,
-			params, coef, nullptr, rhs, queue);
+			params, coef, nullptr, rhs);
 	else if (point_state)
 		TangentPointKernel<kPointState><<<grid, kTcThreads, bytes, stream>>>(mesh, phi, qdata, state, previous,
-			params, nullptr, point_state, rhs, queue);
+			params, nullptr, point_state, rhs);
 	else
 		TangentPointKernel<kPointResidual><<<grid, kTcThreads, bytes, stream>>>(mesh, phi, qdata, state, previous,
-			params, nullptr, nullptr, rhs, queue);
+			params, nullptr, nullptr, rhs);
 	LaunchCheck("TangentPointKernel");
 }
 
@@ -1147,6 +1348,20 @@ void StartTangentTc(unsigned ctas, const DeviceMeshView& mesh, const float* phi3
 }
 
 template <int kMode>
+void StartTangentTcQuad(unsigned ctas, const DeviceMeshView& mesh, const float* phi32, const float* coef,
+	const int32_t* element_blocks, float* values, int* status, cudaStream_t stream)
+{
+	static bool configured = false;
+	if (!configured) {
+		CudaCheck(cudaFuncSetAttribute(TangentTcQuadKernel<kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			kQSmemBytes), "element tensor-core tangent shared-memory attribute");
+		configured = true;
+	}
+	TangentTcQuadKernel<kMode><<<ctas, kTcThreads, kQSmemBytes, stream>>>(mesh, phi32, coef, element_blocks, values,
+		status);
+}
+
+template <int kMode>
 void StartTangentTcFused(unsigned ctas, const DeviceMeshView& mesh, const double* phi, const double* qdata,
 	const double* point_state, AssemblyParams params, const int32_t* element_blocks, float* values, int* status,
 	int lookahead, cudaStream_t stream)
@@ -1162,6 +1377,22 @@ void StartTangentTcFused(unsigned ctas, const DeviceMeshView& mesh, const double
 }
 
 } // namespace
+
+void LaunchTangentTcElement(const DeviceMeshView& mesh, const float* phi32, const float* coef,
+	const int32_t* element_blocks, float* values, int* status, int operands, cudaStream_t stream)
+{
+	if (mesh.elements == 0) return;
+	const unsigned ctas = (unsigned)std::min<long long>(mesh.elements, MultiprocessorCount());
+	if (operands == TC_OPERANDS_SPLIT)
+		StartTangentTcQuad<kModeSplit>(ctas, mesh, phi32, coef, element_blocks, values, status, stream);
+	else if (operands == TC_OPERANDS_TF32)
+		StartTangentTcQuad<kModeTf32>(ctas, mesh, phi32, coef, element_blocks, values, status, stream);
+	else if (operands == TC_OPERANDS_BF16)
+		StartTangentTcQuad<kModeBf16>(ctas, mesh, phi32, coef, element_blocks, values, status, stream);
+	else
+		Fail(-1, "tensor-core tangent: unknown operand organisation");
+	LaunchCheck("TangentTcQuadKernel");
+}
 
 void LaunchTangentTc(const DeviceMeshView& mesh, const float* phi32, const float* coef,
 	const int32_t* element_blocks, float* values, int* status, int operands, cudaStream_t stream)
