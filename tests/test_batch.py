@@ -94,15 +94,19 @@ def test_helical_tube_geometry():
 
 
 @pytest.mark.gpu
-def test_per_tube_newton_tests_match_individual_tubes():
-    """Per-tube Newton tests on a batch of straight and helical tubes (tfiga_ns_set_segments): every tube
-    passes its own relative test, and its part of the union equals the tube solved alone with the same
-    test (1e-8 velocity, 1e-6 pressure relative L2)."""
+@pytest.mark.parametrize("precision", ["bf16x3", "fp64"])
+def test_per_tube_newton_tests_match_individual_tubes(precision):
+    """Per-tube Newton tests and per-tube FGMRES on a batch of straight and helical tubes
+    (tfiga_ns_set_segments: each tube its own Newton test, and its own Arnoldi process, Hessenberg
+    matrix and tolerance inside the union's linear solve): every tube passes its own relative test, and
+    its part of the union equals the tube solved alone with the same test (1e-8 velocity, 1e-6 pressure
+    relative L2); FP32 Krylov basis with the split-BF16 tangent, FP64 basis with the FP64 solver."""
     from tubularflowiga_b200 import api, meshgen
     batch = meshgen.tube_batch(4, seed=5, min_elements=150, max_elements=400, helical=0.5)
     specs = meshgen.tube_batch_specs(4, seed=5, min_elements=150, max_elements=400, helical=0.5)
     assert any(s.curvature_radius > 0 for s in specs) and any(s.curvature_radius == 0 for s in specs)
-    kw = dict(density=1060.0, viscosity=3.5e-3, dt=1e-3, preconditioner=api.AMG, precision=api.MIXED_BF16X3,
+    mode = api.MIXED_BF16X3 if precision == "bf16x3" else api.FP64
+    kw = dict(density=1060.0, viscosity=3.5e-3, dt=1e-3, preconditioner=api.AMG, precision=mode,
               nonlinear_rtol=1e-10, nonlinear_atol=1e-300, gmres_rtol=1e-10, gmres_max_iterations=20000,
               max_newton=25, gmres_restart=64)
     vmask, pmask, vel = api.batch_boundary_conditions(batch)

@@ -71,6 +71,17 @@ public:
 		low_on_ = term != nullptr && term->count > 0;
 		if (low_on_) low_ = *term;
 	}
+	// Independent segments of the unknowns (entry offsets, count + 1 values increasing from 0 to the
+	// system size; fewer than 2 values: none) for SolveFlexibleSegments.
+	void SetSegments(const std::vector<int64_t>& entry_offsets);
+	int segments() const { return segments_; }
+	// SolveFlexible with one Arnoldi process per segment sharing the SpMV and preconditioner launches:
+	// each segment its own Hessenberg matrix, rotations and tolerance rtol * ||b_k - A x0_k|| (the matrix
+	// and the preconditioner must not couple segments).  Converged when every segment meets its own;
+	// iterations count the union's steps.  No learned stage.
+	template <class T>
+	GmresResult SolveFlexibleSegments(const DevicePatternView& pattern, const T* values, const double* rhs, double* x,
+		double rtol, int max_iterations, Amg& preconditioner, long long* launches, bool fp64_basis = false);
 	std::size_t bytes() const;
 
 private:
@@ -89,6 +100,21 @@ private:
 	template <class T, class B>
 	double TrueResidualPlain(const DevicePatternView& pattern, const T* values, const double* rhs, const double* x);
 	double TrueResidual(const DevicePatternView& pattern, const double* values, const double* rhs, const double* x);
+	template <class T, class B>
+	GmresResult SolveFlexibleSegmentsImpl(const DevicePatternView& pattern, const T* values, const double* rhs,
+		double* x, double rtol, int max_iterations, Amg& preconditioner, long long* launches);
+	template <class T, class B>
+	void SegFlexibleStep(const DevicePatternView& pattern, const T* values, int j, Amg& preconditioner);
+	// r = b - A x, segment norms into seg_host_beta_ / seg_beta_, r stored as basis vector 0
+	template <class T, class B>
+	void SegTrueResidual(const DevicePatternView& pattern, const T* values, const double* rhs, const double* x);
+	int segments_ = 0, seg_dot_cx_ = 0, seg_vec_cx_ = 0;
+	DeviceArray<int64_t> seg_off_;
+	DeviceArray<double> seg_H_, seg_cs_, seg_sn_, seg_g_, seg_y_, seg_scale_, seg_hpass_, seg_partial_,
+		seg_norm_partial_, seg_tol_, seg_beta_, seg_sq_, seg_residual_;
+	DeviceArray<int> seg_stop_, seg_used_, seg_all_;
+	std::vector<double> seg_host_beta_, seg_host_tol_;
+	std::vector<int> seg_host_flags_;
 
 	int nodes_, fields_, n_, restart_, blocks_;
 	unsigned singular_count_ = 0;     // singular diagonal blocks of the last block-inverse build
@@ -123,5 +149,8 @@ private:
 	LearnedPreconditioner* collector_ = nullptr;
 	DeviceArray<double> pair_dinv_, pair_amg_, pair_aamg_;
 };
+
+template <> double* Gmres::Basis<double>();
+template <> float* Gmres::Basis<float>();
 
 } // namespace tfiga

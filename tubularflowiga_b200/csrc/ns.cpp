@@ -449,6 +449,13 @@ GmresResult NsSolver::SolveLinear(double rtol, int max_iterations)
 		const long long before = amg_->launches();
 		GmresResult result;
 		auto solve = [&]() {
+			// batched tubes: one Arnoldi process per tube over the shared launches
+			if (segments_ && mixed())
+				return gmres_.SolveFlexibleSegments<float>(mesh_.pattern_view(), values32_.get(), rhs_.get(),
+					update_.get(), rtol, max_iterations, *amg_, &launches_, params_.krylov_fp64_basis != 0);
+			if (segments_)
+				return gmres_.SolveFlexibleSegments<double>(mesh_.pattern_view(), values_.get(), rhs_.get(),
+					update_.get(), rtol, max_iterations, *amg_, &launches_);
 			if (mixed())
 				return gmres_.SolveFlexible<float>(mesh_.pattern_view(), values32_.get(), rhs_.get(), update_.get(),
 					rtol, max_iterations, *amg_, &launches_, params_.krylov_fp64_basis != 0);
@@ -998,6 +1005,7 @@ void NsSolver::SetSegments(const int64_t* node_offsets, int count)
 	if (count < 0) Fail(-1, "segment count must be non-negative");
 	if (count == 0) {
 		segments_ = 0;
+		gmres_.SetSegments({});
 		return;
 	}
 	if (node_offsets == nullptr) Fail(-1, "null segment offsets");
@@ -1007,6 +1015,7 @@ void NsSolver::SetSegments(const int64_t* node_offsets, int count)
 	segment_nodes_.assign(node_offsets, node_offsets+count+1);
 	std::vector<int64_t> entries(count+1);
 	for (int k = 0; k <= count; ++k) entries[k] = 4*node_offsets[k];
+	gmres_.SetSegments(entries);
 	segment_entries_.Allocate(count+1);
 	segment_entries_.Upload(entries.data(), count+1, stream_);
 	segment_sq_.Allocate(count);
