@@ -846,7 +846,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) TangentTcQuadKernel(DeviceMeshV
 					#pragma unroll
 					for (int k = 0; k < 20; ++k) mm[r][k] = *reinterpret_cast<const unsigned long long*>(c0+k*NP);
 				}
-				#pragma unroll 1
+				// two basis groups per iteration: twice the independent FMA chains between the basis loads
+				#pragma unroll 2
 				for (int j = 0; j < kGroups; ++j) {
 					const int b = (g0+j)*8+gbs;
 					unsigned long long pb[5];
