@@ -206,29 +206,27 @@ __global__ void __launch_bounds__(kThreads) UpdateDotKernel(const B* __restrict_
 	}
 }
 
-// y += sum_k coef_k (g_k . x) g_k over sparse g_k; one CTA, outlets in turn (indices are distinct
-// within an outlet, so the scatter needs no atomics).
-__global__ void __launch_bounds__(kThreads) LowRankKernel(int count, const int* __restrict__ ptr,
+// y += sum_k coef_k (g_k . x) g_k over sparse g_k; one CTA per outlet k (the dot in a fixed order;
+// the scatter by atomic adds, as two outlets' vectors may share unknowns).
+__global__ void __launch_bounds__(kThreads) LowRankKernel(const int* __restrict__ ptr,
 	const int* __restrict__ idx, const double* __restrict__ val, const double* __restrict__ coef,
 	const double* __restrict__ x, double* __restrict__ y, const int* __restrict__ stop)
 {
 	if (stop && *stop) return;
 	__shared__ double part[kWarps];
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	for (int k = 0; k < count; ++k) {
-		const int lo = ptr[k], hi = ptr[k+1];
-		double s = 0.0;
-		for (int j = lo+threadIdx.x; j < hi; j += blockDim.x) s = fma(val[j], x[idx[j]], s);
-		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-		if (lane == 0) part[warp] = s;
-		__syncthreads();
-		double dot = 0.0;
-		#pragma unroll
-		for (int w = 0; w < kWarps; ++w) dot += part[w];
-		const double scale = coef[k]*dot;
-		for (int j = lo+threadIdx.x; j < hi; j += blockDim.x) y[idx[j]] += scale*val[j];
-		__syncthreads();
-	}
+	const int k = blockIdx.x;
+	const int lo = ptr[k], hi = ptr[k+1];
+	double s = 0.0;
+	for (int j = lo+threadIdx.x; j < hi; j += blockDim.x) s = fma(val[j], x[idx[j]], s);
+	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+	if (lane == 0) part[warp] = s;
+	__syncthreads();
+	double dot = 0.0;
+	#pragma unroll
+	for (int w = 0; w < kWarps; ++w) dot += part[w];
+	const double scale = coef[k]*dot;
+	for (int j = lo+threadIdx.x; j < hi; j += blockDim.x) atomicAdd(y+idx[j], scale*val[j]);
 }
 
 // Column j of the Hessenberg matrix: norm, previous rotations, new rotation,
@@ -386,7 +384,7 @@ double ArnoldiBytes(long long n, int used, int basis_bytes, bool flexible)
 
 void Gmres::AddLowRank(const double* x, double* y, const int* stop)
 {
-	LowRankKernel<<<1, kThreads, 0, stream_>>>(low_.count, low_.ptr, low_.idx, low_.val, low_.coef, x, y, stop);
+	LowRankKernel<<<low_.count, kThreads, 0, stream_>>>(low_.ptr, low_.idx, low_.val, low_.coef, x, y, stop);
 	LaunchCheck("LowRankKernel");
 	launches_ += 1;
 }
