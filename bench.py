@@ -1006,6 +1006,8 @@ def main():
         def fp64_run(forcing):
             kw = dict(solver_kw, newton_forcing=int(forcing == "ew"))
             ref = api.NavierStokes(mesh, precision=api.FP64, **kw)
+            if batched:
+                ref.set_segments(tube.node_offset)          # per-tube Newton tests and FGMRES, as the mixed arm
             ref.set_dirichlet(vmask, pmask, velocity_at(0.0))
             ref.set_tractions(fixed_tractions)
             ref.set_state(s0, s0)
@@ -1068,9 +1070,10 @@ def main():
                                        "Newton rel.res %g), every step from the same initial state"
                                        % (args.forcing, args.newton_rtol))
         fp64_leg["same_as_mixed"] = ("same steps (warm-up %d untimed, %d timed), Dirichlet sequence, outlet "
-                                     "coupling, Newton test, residual-first check, tangent-reuse factor %g and "
+                                     "coupling, Newton test%s, residual-first check, tangent-reuse factor %g and "
                                      "FGMRES restart; precision FP64 everywhere" % (args.warmup, args.steps,
-                                                                                    args.tangent_reuse))
+                                                                                    " and FGMRES per tube" if batched
+                                                                                    else "", args.tangent_reuse))
 
     ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms], "cuda")
     if batched:
