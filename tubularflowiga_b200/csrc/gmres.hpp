@@ -110,6 +110,7 @@ private:
 	void SegTrueResidual(const DevicePatternView& pattern, const T* values, const double* rhs, const double* x);
 	int segments_ = 0, seg_dot_cx_ = 0, seg_vec_cx_ = 0;
 	DeviceArray<int64_t> seg_off_;
+	DeviceArray<int32_t> seg_node_;      // segment of every node (block row)
 	DeviceArray<double> seg_H_, seg_cs_, seg_sn_, seg_g_, seg_y_, seg_scale_, seg_hpass_, seg_partial_,
 		seg_norm_partial_, seg_tol_, seg_beta_, seg_sq_, seg_residual_;
 	DeviceArray<int> seg_stop_, seg_used_, seg_all_;

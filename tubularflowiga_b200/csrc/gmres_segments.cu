@@ -3,8 +3,9 @@
 // operator (SpMV) run over the union -- the matrix is block diagonal over the segments and the AMG's
 // aggregates never cross them -- while every segment keeps its own Gram-Schmidt coefficients,
 // normalisation, Hessenberg matrix, Givens rotations, residual estimate and tolerance
-// rtol * ||b_k - A_k x_k||, and stops on its own.  A stopped segment's next vector is zero, so the
-// shared launches do no work for it, and the union's iteration ends when every segment has stopped.
+// rtol * ||b_k - A_k x_k||, and stops on its own.  A stopped segment's next vector is zero, the SpMV
+// skips its block rows and the Gram-Schmidt kernels its chunks, and the union's iteration ends when
+// every segment has stopped.
 // The single-system solver's tolerance definition (true residual at every restart) is kept per segment.
 //
 // Grids are two-dimensional: blockIdx.y is the segment, blockIdx.x a chunk of it (CTAs past the end of
@@ -306,6 +307,8 @@ void Gmres::SetSegments(const std::vector<int64_t>& entry_offsets)
 	if (count <= 0) { segments_ = 0; return; }
 	if (count > 1024) Fail(-7, "at most 1024 segments per flexible solve");
 	if (entry_offsets[0] != 0 || entry_offsets[count] != n_) Fail(-1, "segments must cover the unknowns");
+	for (int k = 0; k <= count; ++k)
+		if (entry_offsets[k] % fields_) Fail(-1, "segments must hold whole nodes");
 	int64_t longest = 0;
 	for (int k = 0; k < count; ++k) {
 		if (entry_offsets[k+1] <= entry_offsets[k] || (entry_offsets[k] & 1)) Fail(-1, "bad segment offsets");
@@ -318,6 +321,11 @@ void Gmres::SetSegments(const std::vector<int64_t>& entry_offsets)
 	const int stride = restart_+1;
 	seg_off_.Allocate(count+1);
 	seg_off_.Upload(entry_offsets.data(), count+1, stream_);
+	std::vector<int32_t> node_seg(n_/fields_);
+	for (int k = 0; k < count; ++k)
+		for (int64_t e = entry_offsets[k]/fields_; e < entry_offsets[k+1]/fields_; ++e) node_seg[e] = k;
+	seg_node_.Allocate(node_seg.size());
+	seg_node_.Upload(node_seg.data(), node_seg.size(), stream_);
 	seg_H_.Allocate((size_t)count*(restart_+1)*restart_);
 	seg_cs_.Allocate((size_t)count*restart_);
 	seg_sn_.Allocate((size_t)count*restart_);
@@ -374,7 +382,8 @@ void Gmres::SegFlexibleStep(const DevicePatternView& pattern, const T* values, i
 	double* z = Z_.get()+(size_t)j*n_;
 	M.Apply(values, r_.get(), z, all);
 	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
-	LaunchSpmvBlockJacobi<T>(pattern, values, nullptr, z, nullptr, w_.get(), all, stream_);
+	// the rows of stopped segments are skipped: nothing reads their w again in this cycle
+	LaunchSpmvMasked<T>(pattern, values, z, w_.get(), all, seg_node_.get(), seg_stop_.get(), stream_);
 	if (low_on_) AddLowRank(z, w_.get(), all);
 	if (profiler_) profiler_->End(stream_);
 	launches_ += 2;

@@ -112,6 +112,12 @@ void LaunchSpmv(const DevicePatternView& pattern, const T* values, const double*
 template <class T>
 void LaunchSpmvBlockJacobi(const DevicePatternView& pattern, const T* values, const double* inverse,
 	const double* x, const double* scale, double* y, const int* stop, cudaStream_t stream);
+// y = A x on the block rows whose segment is still open (node_seg[row] its segment, seg_stop[s] set once
+// segment s has stopped; the rows of stopped segments are skipped and keep their old y).  Returns
+// early when *stop is set.
+template <class T>
+void LaunchSpmvMasked(const DevicePatternView& pattern, const T* values, const double* x, double* y,
+	const int* stop, const int32_t* node_seg, const int* seg_stop, cudaStream_t stream);
 template <class T>
 void LaunchBlockInverse(const DevicePatternView& pattern, const T* values, double* inverse,
 	unsigned int* singular, cudaStream_t stream);

@@ -291,6 +291,30 @@ void LaunchSpmv(const DevicePatternView& p, const T* values, const double* x, do
 	LaunchCheck("SpmvKernel");
 }
 
+// y = A x on the block rows of segments still open (node_seg[row] the row's segment, seg_stop[s] set
+// once segment s has stopped: its rows are skipped and y there is left as it was).
+template <class T>
+__global__ void __launch_bounds__(256) SpmvMaskedKernel(DevicePatternView p, const T* __restrict__ values,
+	const double* __restrict__ x, double* __restrict__ y, const int* __restrict__ stop,
+	const int32_t* __restrict__ node_seg, const int* __restrict__ seg_stop)
+{
+	if (*stop) return;
+	const int row = blockIdx.x*8+(threadIdx.x >> 5);
+	const int lane = threadIdx.x & 31;
+	if (row >= p.nodes || seg_stop[node_seg[row]]) return;
+	const double sum = RowBlockDot(p, values, x, row, lane);
+	if (lane < 4) y[4*(size_t)row+lane] = sum;
+}
+
+template <class T>
+void LaunchSpmvMasked(const DevicePatternView& p, const T* values, const double* x, double* y, const int* stop,
+	const int32_t* node_seg, const int* seg_stop, cudaStream_t stream)
+{
+	if (p.nodes == 0) return;
+	SpmvMaskedKernel<T><<<Blocks(p.nodes, 8), 256, 0, stream>>>(p, values, x, y, stop, node_seg, seg_stop);
+	LaunchCheck("SpmvMaskedKernel");
+}
+
 template <class T>
 void LaunchSpmvBlockJacobi(const DevicePatternView& p, const T* values, const double* inverse,
 	const double* x, const double* scale, double* y, const int* stop, cudaStream_t stream)
@@ -313,6 +337,10 @@ template void LaunchSpmv<double>(const DevicePatternView&, const double*, const 
 template void LaunchSpmv<float>(const DevicePatternView&, const float*, const double*, double*, cudaStream_t);
 template void LaunchSpmvBlockJacobi<double>(const DevicePatternView&, const double*, const double*, const double*,
 	const double*, double*, const int*, cudaStream_t);
+template void LaunchSpmvMasked<double>(const DevicePatternView&, const double*, const double*, double*, const int*,
+	const int32_t*, const int*, cudaStream_t);
+template void LaunchSpmvMasked<float>(const DevicePatternView&, const float*, const double*, double*, const int*,
+	const int32_t*, const int*, cudaStream_t);
 template void LaunchSpmvBlockJacobi<float>(const DevicePatternView&, const float*, const double*, const double*,
 	const double*, double*, const int*, cudaStream_t);
 template void LaunchBlockInverse<double>(const DevicePatternView&, const double*, double*, unsigned int*, cudaStream_t);
