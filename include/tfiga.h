@@ -323,10 +323,11 @@ int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info);
  * node ranges [node_offsets[k], node_offsets[k+1]) of count independent tubes (node_offsets increasing
  * from 0 to nodes, e.g. tfiga_batch_mesh_create's node offsets); count 0 removes them.  The Newton
  * test is then taken per tube, relative to the tube's own first residual of the step, and a tube that
- * passes is frozen for the rest of the step (its rows of the linear system carry a zero rhs); each
- * open tube's rhs is scaled to unit norm for the linear solve and its update scaled back, so the
- * union's Krylov solve resolves every tube relative to itself; the step converges when every tube
- * has passed. */
+ * passes is frozen for the rest of the step (its rows of the linear system carry a zero rhs); the
+ * linear solves run one FGMRES per tube over shared launches (each tube its own Arnoldi process,
+ * Hessenberg matrix and tolerance, stopping on its own; the AMG preconditioner only), each open
+ * tube's rhs scaled to unit norm and its update scaled back; the step converges when every tube has
+ * passed. */
 int tfiga_ns_set_segments(tfiga_ns* ns, const int64_t* node_offsets, int32_t count);
 /* Per tube, after a Newton iteration: done[k] 1 when tube k has passed its test in this step, and its
  * residual norm (either output may be NULL). */
