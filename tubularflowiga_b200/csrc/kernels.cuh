@@ -79,7 +79,7 @@ void LaunchAssembleLarge(const DeviceMeshView& mesh, int first, int count, const
 // ---- tangent_tc.cu -----------------------------------------------------
 // Tensor-core tangent in two launches.  LaunchTangentPoint: FP64 point state,
 // the coefficients of all four row fields into coef (workspace of elements x 4
-// x 16 x 80 x 4 floats, point-quad major; null: residual only) and the FP64 residual ADDED into rhs
+// x 80 x 64 floats; null: residual only) and the FP64 residual ADDED into rhs
 // (= -r).
 // LaunchTangentTc: the tangent contracted on the tcgen05 tensor cores from
 // coef and phi32 (the FP32 copy of phi, Mesh::phi32), FP32 accumulation, ADDED

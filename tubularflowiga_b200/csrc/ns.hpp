@@ -151,7 +151,7 @@ private:
 	int64_t n4_;
 	DeviceArray<double> values_, rhs_, state_, previous_, update_, traction_, velocity_bc_, pressure_bc_;
 	DeviceArray<float> values32_;
-	DeviceArray<float> coef32_;              // tensor-core tangent: point coefficients [e][4][16][80][4]
+	DeviceArray<float> coef32_;              // tensor-core tangent: point coefficients [e][4][80][64]
 	DeviceArray<double> point_state_;        // fused tensor-core tangent: FP64 point state [e][64][22]
 	int tangent_kernel_ = 0;                 // TFIGA_TANGENT_* in use
 	double tune_ms_[3] = {0.0, 0.0, 0.0};    // autotuner: coefficient-array (pair), fused, element times

@@ -17,10 +17,10 @@
 //     quarters summed in shared memory), the coefficients M_q of all four row
 //     fields (thread per row field and point, two column-field halves through
 //     a shared-memory scratch) written to a coefficient array laid out
-//     [element][row field][16 point quads][80 coefficients][4 points] (a K
-//     chunk's coefficients of one row field are one contiguous run), and the
-//     FP64 residual (thread per basis function and quarter of the points, one
-//     read of each basis value for the four row fields) added into rhs.
+//     [element][row field][80 coefficients][64 points] (coalesced over the
+//     points), and the FP64 residual (thread per basis function and quarter
+//     of the points, one read of each basis value for the four row fields)
+//     added into rhs.
 //   TangentTcKernel (CTA per element and row-field pair h: i in {2h, 2h+1},
 //     256 threads, 4 M = 128 accumulator tiles in 256 TMEM columns; tile T:
 //     row field 2h + T/2, basis b in [32 (T&1), +32), tile row m = 4 (b mod
@@ -307,25 +307,23 @@ __device__ __forceinline__ void PrefetchChunk(const float* P32, const float* CF,
 	}
 	for (int idx = tid; idx < kRows*kCoef*NP/4; idx += kTcThreads) {
 		const int rk = idx/(NP/4), part = idx%(NP/4);           // rk = row field * 80 + k
-		const int row = rk/kCoef, k = rk%kCoef;
-		CopyAsync16(cf_dst+16*idx+(rk/20)*kCfPad*4, CF+(size_t)row*kCoef*kQuad+((c*(NP/4)+part)*kCoef+k)*4);
+		CopyAsync16(cf_dst+16*idx+(rk/20)*kCfPad*4, CF+(size_t)rk*kQuad+c*NP+4*part);
 	}
 	CopyAsyncCommit();
 }
 
 // Coefficients of row field kRow at one point: both column-field halves through the thread's
-// scratch, stored at out[4 k] (the point's slot in its quad's [80][4] block; the four points of a
-// quad fill each 16-byte group).
+// scratch, stored at out[k * 64] (coalesced over the points of a warp).
 template <int kRow>
 __device__ __forceinline__ void PointCoefficients(const PointState& S, const double* qd, const AssemblyParams& prm,
 	float* scratch, double* rc, float* out)
 {
 	RowCoefficients<float>(kRow, S, qd, prm, scratch, rc, 0, 2);
 	#pragma unroll 8
-	for (int k = 0; k < 40; ++k) out[k*4] = scratch[k];
+	for (int k = 0; k < 40; ++k) out[(size_t)k*kQuad] = scratch[k];
 	RowCoefficients<float>(kRow, S, qd, prm, scratch, nullptr, 2, 4);
 	#pragma unroll 8
-	for (int k = 0; k < 40; ++k) out[(40+k)*4] = scratch[k];
+	for (int k = 0; k < 40; ++k) out[(size_t)(40+k)*kQuad] = scratch[k];
 }
 
 // kMode: what the kernel stores besides adding the FP64 residual into rhs -- kPointResidual nothing
@@ -438,7 +436,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 		double* rc = RC+(il*kQuad+q)*kRcStride;
 		if constexpr (kMode == kPointCoefficients) {
 			float* scratch = Scratch+tid*kScratchStride;
-			float* out = coef+((size_t)e*4+il)*kCoef*kQuad+(q >> 2)*kCoef*4+(q & 3);
+			float* out = coef+((size_t)e*4+il)*kCoef*kQuad+q;
 			switch (il) {
 			case 0: PointCoefficients<0>(S, qd, prm, scratch, rc, out); break;
 			case 1: PointCoefficients<1>(S, qd, prm, scratch, rc, out); break;
