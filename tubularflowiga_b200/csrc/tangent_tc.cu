@@ -352,7 +352,6 @@ __global__ void __launch_bounds__(kTcThreads, 2) TangentPointKernel(DeviceMeshVi
 	const int begin = mesh.element_offsets[e];
 	const int nen = mesh.element_offsets[e+1]-begin;
 	const double* P = phi+(size_t)e*kFeatures*kQuad*kMaxBasis;
-	if (tid == 0) PrefetchL2(P, kFeatures*kQuad*kMaxBasis*8);
 
 	// 1. Nodal state.
 	if (tid < kMaxBasis) {
