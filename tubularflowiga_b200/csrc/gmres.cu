@@ -38,41 +38,25 @@ template <> struct BasisPair<float> {
 	}
 };
 
-// partial[i*blocks + cta] = scale[i] * <V_i, w> over this CTA's chunk, and w_norm[cta] = |w|^2 over
-// it (if non-null); nothing when project is given and *project is 0.  The chunk is a multiple of 128
-// doubles and n is even, so every row slice is 16-byte aligned: a warp streams two basis vectors at
-// once with 16-byte loads, two steps per iteration, to keep enough bytes in flight for HBM.
+// partial[i*blocks + cta] = scale[i] * <V_i, w> over this CTA's chunk.  The
+// chunk is a multiple of 128 doubles and n is even, so every row slice is
+// 16-byte aligned: a warp streams two basis vectors at once with 16-byte
+// loads, two steps per iteration, to keep enough bytes in flight for HBM.
 template <class B>
 __global__ void __launch_bounds__(kThreads) MultiDotKernel(const B* __restrict__ V, long long n,
 	const double* __restrict__ scale, int count, const double* __restrict__ w, double* __restrict__ partial,
-	int chunk, const int* __restrict__ stop, double* __restrict__ w_norm, const int* __restrict__ project)
+	int chunk, const int* __restrict__ stop)
 {
-	if (*stop || (project != nullptr && *project == 0)) return;
+	if (*stop) return;
 	extern __shared__ double wchunk[];
-	__shared__ double red[kWarps];
 	double2* w2 = reinterpret_cast<double2*>(wchunk);
 	const long long lo = (long long)blockIdx.x*chunk;
 	const long long rest = n-lo;
 	const int len2 = (rest <= 0 ? 0 : (rest < chunk ? (int)rest : chunk)) >> 1;
 	const double2* win = reinterpret_cast<const double2*>(w+lo);
-	double sq = 0.0;
-	for (int k = threadIdx.x; k < len2; k += blockDim.x) {
-		const double2 v = win[k];
-		w2[k] = v;
-		sq = fma(v.x, v.x, fma(v.y, v.y, sq));
-	}
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	if (w_norm != nullptr) {
-		for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-		if (lane == 0) red[warp] = sq;
-	}
+	for (int k = threadIdx.x; k < len2; k += blockDim.x) w2[k] = win[k];
 	__syncthreads();
-	if (w_norm != nullptr && threadIdx.x == 0) {
-		double t = 0.0;
-		#pragma unroll
-		for (int k = 0; k < kWarps; ++k) t += red[k];
-		w_norm[blockIdx.x] = t;
-	}
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const double2 zero = make_double2(0.0, 0.0);
 	for (int i0 = warp; i0 < count; i0 += 2*kWarps) {
 		const int i1 = i0+kWarps;
@@ -103,19 +87,14 @@ __global__ void __launch_bounds__(kThreads) MultiDotKernel(const B* __restrict__
 	}
 }
 
-// hpass[i] = sum over CTAs; H[i][j] = (pass == 0 ? hpass : H + hpass).  With project given and *project
-// 0 (the second pass is not needed): hpass = 0 and H unchanged.
+// hpass[i] = sum over CTAs; H[i][j] = (pass == 0 ? hpass : H + hpass).
 __global__ void __launch_bounds__(kThreads) DotFinalizeKernel(const double* __restrict__ partial, int blocks,
 	int count, double* __restrict__ hpass, double* __restrict__ H, int restart, int j, int pass,
-	const int* __restrict__ stop, const int* __restrict__ project)
+	const int* __restrict__ stop)
 {
 	if (*stop) return;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int i = blockIdx.x*(kThreads/32)+warp;   // a warp per basis vector, spread over CTAs
-	if (project != nullptr && *project == 0) {
-		if (i < count && lane == 0) hpass[i] = 0.0;
-		return;
-	}
 	if (i < count) {
 		double s = 0.0;
 		for (int b = lane; b < blocks; b += 32) s += partial[(size_t)i*blocks+b];
@@ -136,13 +115,11 @@ __global__ void __launch_bounds__(kThreads) DotFinalizeKernel(const double* __re
 template <class B, class O>
 __global__ void __launch_bounds__(kThreads) UpdateKernel(const B* __restrict__ V, long long n,
 	const double* __restrict__ scale, int count, const double* __restrict__ hpass, const double* win, O* out,
-	double* __restrict__ norm_partial, const int* __restrict__ stop, const int* __restrict__ project)
+	double* __restrict__ norm_partial, const int* __restrict__ stop)
 {
 	if (*stop) return;
 	extern __shared__ double coef[];
 	__shared__ double2 part[kWarps][32];
-	// no projection (the second pass not needed): out = w, the basis is not read
-	if (project != nullptr && *project == 0) count = 0;
 	for (int i = threadIdx.x; i < count; i += blockDim.x) coef[i] = scale[i]*hpass[i];
 	__syncthreads();
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -190,10 +167,9 @@ __global__ void __launch_bounds__(kThreads) UpdateKernel(const B* __restrict__ V
 template <class B>
 __global__ void __launch_bounds__(kThreads) UpdateDotKernel(const B* __restrict__ V, long long n,
 	const double* __restrict__ scale, int count, const double* __restrict__ hpass, double* __restrict__ w,
-	double* __restrict__ partial, int chunk, const int* __restrict__ stop, double* __restrict__ w_norm)
+	double* __restrict__ partial, int chunk, const int* __restrict__ stop)
 {
 	if (*stop) return;
-	__shared__ double red[kWarps];
 	extern __shared__ __align__(16) double fused[];
 	double* coef = fused;                                        // [count], padded to an even length
 	double* ws = coef+((count+1) & ~1);                          // [chunk] updated w
@@ -212,25 +188,15 @@ __global__ void __launch_bounds__(kThreads) UpdateDotKernel(const B* __restrict_
 	for (int i = threadIdx.x; i < count; i += blockDim.x) coef[i] = scale[i]*hpass[i];
 	asm volatile("cp.async.wait_group 0;" ::: "memory");
 	__syncthreads();
-	double sq = 0.0;
 	for (int k = threadIdx.x; k < len; k += blockDim.x) {
 		double acc = 0.0;
 		for (int i = 0; i < count; ++i) acc = fma(-coef[i], (double)Vs[(size_t)i*chunk+k], acc);
 		const double v = w[lo+k]+acc;
 		w[lo+k] = v;
 		ws[k] = v;
-		sq = fma(v, v, sq);
 	}
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-	if (lane == 0) red[warp] = sq;
 	__syncthreads();
-	if (threadIdx.x == 0) {
-		double t = 0.0;
-		#pragma unroll
-		for (int k = 0; k < kWarps; ++k) t += red[k];
-		w_norm[blockIdx.x] = t;
-	}
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	for (int i = warp; i < count; i += kWarps) {
 		const B* vi = Vs+(size_t)i*chunk;
 		double sum = 0.0;
@@ -261,31 +227,6 @@ __global__ void __launch_bounds__(kThreads) LowRankKernel(const int* __restrict_
 	for (int w = 0; w < kWarps; ++w) dot += part[w];
 	const double scale = coef[k]*dot;
 	for (int j = lo+threadIdx.x; j < hi; j += blockDim.x) atomicAdd(y+idx[j], scale*val[j]);
-}
-
-// Selective reorthogonalisation (the Daniel-Gragg-Kaufman-Stewart test): the second Gram-Schmidt
-// pass runs only when the first removed more than half of w's squared norm, |w1|^2 < |w0|^2 / 2
-// (w0 before, w1 after the first pass; partial sums over CTAs, fixed order).
-__global__ void ReorthDecideKernel(const double* __restrict__ before, int nb, const double* __restrict__ after,
-	int na, int* __restrict__ project, const int* __restrict__ stop)
-{
-	if (*stop) return;
-	__shared__ double red[2][kWarps];
-	double b = 0.0, a = 0.0;
-	for (int k = threadIdx.x; k < nb; k += blockDim.x) b += before[k];
-	for (int k = threadIdx.x; k < na; k += blockDim.x) a += after[k];
-	for (int o = 16; o > 0; o >>= 1) {
-		b += __shfl_xor_sync(0xffffffffu, b, o);
-		a += __shfl_xor_sync(0xffffffffu, a, o);
-	}
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	if (lane == 0) { red[0][warp] = b; red[1][warp] = a; }
-	__syncthreads();
-	if (threadIdx.x == 0) {
-		double tb = 0.0, ta = 0.0;
-		for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tb += red[0][w]; ta += red[1][w]; }
-		*project = ta < 0.5*tb ? 1 : 0;
-	}
 }
 
 // Column j of the Hessenberg matrix: norm, previous rotations, new rotation,
@@ -465,8 +406,6 @@ Gmres::Gmres(int nodes, int restart, cudaStream_t stream, int fields)
 	scale_.Allocate(restart+1);
 	update_blocks_ = (int)(((long long)n_/2+31)/32);
 	norm_partial_.Allocate(std::max(std::max(PartialSlots(), blocks_), update_blocks_));
-	reorth_before_.Allocate(blocks_);
-	reorth_flag_.Allocate(1);
 	scalar_.Allocate(2);
 	state_.Allocate(4);
 	residual_.Allocate(1);
@@ -507,7 +446,6 @@ Gmres::Gmres(int nodes, int restart, cudaStream_t stream, int fields)
 		fused_smem_[b] = (size_t)(((restart+1)+1) & ~1)*sizeof(double)+(size_t)chunk*sizeof(double)
 			+(size_t)(restart+1)*chunk*entry;
 	}
-	reorth_after_.Allocate(std::max(update_blocks_, std::max(fused_blocks_[0], fused_blocks_[1])));
 	if (fused_chunk_[0] || fused_chunk_[1]) {
 		fused_partial_.Allocate((size_t)(restart+1)*std::max(fused_blocks_[0], fused_blocks_[1]));
 		if (fused_chunk_[0])
@@ -557,71 +495,57 @@ void Gmres::Step(const DevicePatternView& pattern, const T* values, int j)
 template <class B>
 void Gmres::Orthogonalize(int j, B* basis)
 {
-	// classical Gram-Schmidt, the second pass only where the first lost more than half of |w|^2
 	const int count = j+1;
 	const int* stop = state_.get();
-	int* project = reorth_flag_.get();
 	const size_t dot_smem = (size_t)chunk_*sizeof(double);
 	const size_t coef_smem = (size_t)(restart_+1)*sizeof(double);
-	const unsigned fin_blocks = (unsigned)((count+kThreads/32-1)/(kThreads/32));
 	if (profiler_) profiler_->Begin(Profiler::kOrtho, stream_);
 	const int fb = std::is_same<B, double>::value ? 1 : 0;
 	if (fused_chunk_[fb]) {
-		// first pass's dots (and |w0|^2); its update fused with the second pass's dots (and |w1|^2); the
-		// second pass's update, or a copy of w1 when the test finds the first pass enough
+		// first pass's dots; its update fused with the second pass's dots; the second pass's update
 		MultiDotKernel<B><<<blocks_, kThreads, dot_smem, stream_>>>(basis, n_, scale_.get(), count, w_.get(),
-			partial_.get(), chunk_, stop, reorth_before_.get(), nullptr);
+			partial_.get(), chunk_, stop);
 		LaunchCheck("MultiDotKernel");
-		DotFinalizeKernel<<<fin_blocks, kThreads, 0, stream_>>>(partial_.get(), blocks_, count, hpass_.get(), H_.get(),
-			restart_, j, 0, stop, nullptr);
+		DotFinalizeKernel<<<(count+kThreads/32-1)/(kThreads/32), kThreads, 0, stream_>>>(partial_.get(), blocks_,
+			count, hpass_.get(), H_.get(), restart_, j, 0, stop);
 		LaunchCheck("DotFinalizeKernel");
 		UpdateDotKernel<B><<<fused_blocks_[fb], kThreads, fused_smem_[fb], stream_>>>(basis, n_, scale_.get(), count,
-			hpass_.get(), w_.get(), fused_partial_.get(), fused_chunk_[fb], stop, reorth_after_.get());
+			hpass_.get(), w_.get(), fused_partial_.get(), fused_chunk_[fb], stop);
 		LaunchCheck("UpdateDotKernel");
-		ReorthDecideKernel<<<1, kThreads, 0, stream_>>>(reorth_before_.get(), blocks_, reorth_after_.get(),
-			fused_blocks_[fb], project, stop);
-		LaunchCheck("ReorthDecideKernel");
-		DotFinalizeKernel<<<fin_blocks, kThreads, 0, stream_>>>(fused_partial_.get(), fused_blocks_[fb], count,
-			hpass_.get(), H_.get(), restart_, j, 1, stop, project);
+		DotFinalizeKernel<<<(count+kThreads/32-1)/(kThreads/32), kThreads, 0, stream_>>>(fused_partial_.get(),
+			fused_blocks_[fb], count, hpass_.get(), H_.get(), restart_, j, 1, stop);
 		LaunchCheck("DotFinalizeKernel");
 		UpdateKernel<B, B><<<update_blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
-			hpass_.get(), w_.get(), basis+(size_t)(j+1)*n_, norm_partial_.get(), stop, project);
+			hpass_.get(), w_.get(), basis+(size_t)(j+1)*n_, norm_partial_.get(), stop);
 		LaunchCheck("UpdateKernel");
 		ArnoldiFinalizeKernel<<<1, kThreads, finalize_smem_, stream_>>>(norm_partial_.get(), update_blocks_,
 			H_.get(), restart_, j, cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(),
 			tolerance_);
 		LaunchCheck("ArnoldiFinalizeKernel");
 		if (profiler_) profiler_->End(stream_);
-		launches_ += 7;
+		launches_ += 6;
 		return;
 	}
-	// first pass (|w0|^2 with its dots, |w1|^2 with its update), the test, the second pass if needed
-	MultiDotKernel<B><<<blocks_, kThreads, dot_smem, stream_>>>(basis, n_, scale_.get(), count, w_.get(),
-		partial_.get(), chunk_, stop, reorth_before_.get(), nullptr);
-	LaunchCheck("MultiDotKernel");
-	DotFinalizeKernel<<<fin_blocks, kThreads, 0, stream_>>>(partial_.get(), blocks_, count, hpass_.get(), H_.get(),
-		restart_, j, 0, stop, nullptr);
-	LaunchCheck("DotFinalizeKernel");
-	UpdateKernel<B, double><<<update_blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
-		hpass_.get(), w_.get(), w_.get(), reorth_after_.get(), stop, nullptr);
-	LaunchCheck("UpdateKernel");
-	ReorthDecideKernel<<<1, kThreads, 0, stream_>>>(reorth_before_.get(), blocks_, reorth_after_.get(), update_blocks_,
-		project, stop);
-	LaunchCheck("ReorthDecideKernel");
-	MultiDotKernel<B><<<blocks_, kThreads, dot_smem, stream_>>>(basis, n_, scale_.get(), count, w_.get(),
-		partial_.get(), chunk_, stop, nullptr, project);
-	LaunchCheck("MultiDotKernel");
-	DotFinalizeKernel<<<fin_blocks, kThreads, 0, stream_>>>(partial_.get(), blocks_, count, hpass_.get(), H_.get(),
-		restart_, j, 1, stop, project);
-	LaunchCheck("DotFinalizeKernel");
-	UpdateKernel<B, B><<<update_blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
-		hpass_.get(), w_.get(), basis+(size_t)(j+1)*n_, norm_partial_.get(), stop, project);
-	LaunchCheck("UpdateKernel");
+	for (int pass = 0; pass < 2; ++pass) {
+		MultiDotKernel<B><<<blocks_, kThreads, dot_smem, stream_>>>(basis, n_, scale_.get(), count, w_.get(),
+			partial_.get(), chunk_, stop);
+		LaunchCheck("MultiDotKernel");
+		DotFinalizeKernel<<<(count+kThreads/32-1)/(kThreads/32), kThreads, 0, stream_>>>(partial_.get(), blocks_,
+			count, hpass_.get(), H_.get(), restart_, j, pass, stop);
+		LaunchCheck("DotFinalizeKernel");
+		if (pass == 0)
+			UpdateKernel<B, double><<<update_blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
+				hpass_.get(), w_.get(), w_.get(), nullptr, stop);
+		else
+			UpdateKernel<B, B><<<update_blocks_, kThreads, coef_smem, stream_>>>(basis, n_, scale_.get(), count,
+				hpass_.get(), w_.get(), basis+(size_t)(j+1)*n_, norm_partial_.get(), stop);
+		LaunchCheck("UpdateKernel");
+	}
 	ArnoldiFinalizeKernel<<<1, kThreads, finalize_smem_, stream_>>>(norm_partial_.get(), update_blocks_, H_.get(),
 		restart_, j, cs_.get(), sn_.get(), g_.get(), scale_.get(), state_.get(), residual_.get(), tolerance_);
 	LaunchCheck("ArnoldiFinalizeKernel");
 	if (profiler_) profiler_->End(stream_);
-	launches_ += 9;
+	launches_ += 8;
 }
 
 template <> double* Gmres::Basis<double>() { return V_.get(); }

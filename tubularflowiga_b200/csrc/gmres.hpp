@@ -5,9 +5,8 @@
 //
 // B200 organisation: the Hessenberg matrix, Givens rotations and residual
 // estimate live on the device; orthogonalisation is classical Gram-Schmidt
-// (multi-dot + multi-axpy passes over the basis instead of one dot/axpy pair
-// per basis vector) with a second pass only where the first removed more than
-// half of the vector's squared norm; Krylov vectors are normalised lazily
+// applied twice (two multi-dot + multi-axpy passes over the basis instead of
+// one dot/axpy pair per basis vector); Krylov vectors are normalised lazily
 // through a per-vector scale; kernels of an iteration batch return early once
 // the device has flagged convergence, so the host waits only once per batch.
 #pragma once
@@ -129,10 +128,6 @@ private:
 	int fused_chunk_[2] = {0, 0}, fused_blocks_[2] = {0, 0};
 	size_t fused_smem_[2] = {0, 0};
 	DeviceArray<double> fused_partial_;
-	// selective reorthogonalisation: |w|^2 partial sums before / after the first Gram-Schmidt pass and
-	// the device flag that the second pass is needed
-	DeviceArray<double> reorth_before_, reorth_after_;
-	DeviceArray<int> reorth_flag_;
 	size_t finalize_smem_ = 0;
 	cudaStream_t stream_;
 	long long launches_ = 0;
