@@ -916,7 +916,9 @@ def main():
         torch.cuda.synchronize()
         prof_ms += p0.elapsed_time(p1)
         states.append(ns.get_state())
-    orth_algo, orth_moved = ns.profile_bytes()["krylov_orthogonalisation"]
+    prof_bytes = ns.profile_bytes()
+    orth_algo, orth_moved = prof_bytes["krylov_orthogonalisation"]
+    spmv_counted = prof_bytes["spmv"][0]     # the per-tube solver counts the rows of open tubes only
     prof = ns.profile(reset=True)
     ns.set_profiling(False)
 
@@ -1097,9 +1099,14 @@ def main():
         b_spmv -= mesh.blocks * 16 * 4
     spmv_bytes = b_spmv if amg else b_spmv + b_bjac
     spmv_name = "spmv" if amg else "spmv_block_jacobi"
+    masked = spmv_counted > 0 and spmv_n > 0
+    if masked:
+        # tube batch: each Arnoldi SpMV skips the block rows of tubes that have stopped, so its bytes are
+        # those of the open tubes' rows (counted by the solver at its host waits, a lower bound)
+        spmv_bytes = spmv_counted / spmv_n
     if spmv_n:
         a = spmv_bytes / (spmv_ms / spmv_n * 1e-3) / 1e9
-        traffic = SPMV_FP32_DRAM_BYTES_PER_BLOCK * mesh.blocks if (mixed and amg) else None
+        traffic = (SPMV_FP32_DRAM_BYTES_PER_BLOCK * mesh.blocks if (mixed and amg) else None) if not masked else None
         kernels[spmv_name] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
                               "frac": a / hbm, "traffic": traffic, "launches": spmv_n,
                               "avg_ms": spmv_ms / spmv_n, "share": spmv_ms / prof_ms,

@@ -72,8 +72,9 @@ public:
 		if (low_on_) low_ = *term;
 	}
 	// Independent segments of the unknowns (entry offsets, count + 1 values increasing from 0 to the
-	// system size; fewer than 2 values: none) for SolveFlexibleSegments.
-	void SetSegments(const std::vector<int64_t>& entry_offsets);
+	// system size; fewer than 2 values: none) for SolveFlexibleSegments; blocks[k] the matrix blocks of
+	// segment k's rows (for the profiler's byte counts of the masked SpMV).
+	void SetSegments(const std::vector<int64_t>& entry_offsets, const std::vector<int64_t>& blocks = {});
 	int segments() const { return segments_; }
 	// SolveFlexible with one Arnoldi process per segment sharing the SpMV and preconditioner launches:
 	// each segment its own Hessenberg matrix, rotations and tolerance rtol * ||b_k - A x0_k|| (the matrix
@@ -115,7 +116,9 @@ private:
 		seg_norm_partial_, seg_tol_, seg_beta_, seg_sq_, seg_residual_;
 	DeviceArray<int> seg_stop_, seg_used_, seg_all_;
 	std::vector<double> seg_host_beta_, seg_host_tol_;
-	std::vector<int> seg_host_flags_;
+	std::vector<int> seg_host_flags_, seg_host_stop_;
+	std::vector<int64_t> seg_blocks_;    // matrix blocks per segment (byte accounting)
+	std::vector<int64_t> seg_len_;       // entries per segment
 
 	int nodes_, fields_, n_, restart_, blocks_;
 	unsigned singular_count_ = 0;     // singular diagonal blocks of the last block-inverse build

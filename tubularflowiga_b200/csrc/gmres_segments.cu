@@ -301,7 +301,7 @@ __global__ void SegStoreBasisKernel(long long n, const double* __restrict__ r, B
 
 } // namespace
 
-void Gmres::SetSegments(const std::vector<int64_t>& entry_offsets)
+void Gmres::SetSegments(const std::vector<int64_t>& entry_offsets, const std::vector<int64_t>& blocks)
 {
 	const int count = (int)entry_offsets.size()-1;
 	if (count <= 0) { segments_ = 0; return; }
@@ -317,6 +317,8 @@ void Gmres::SetSegments(const std::vector<int64_t>& entry_offsets)
 	if (restart_+1 > 129) Fail(-7, "segmented flexible GMRES supports restarts up to 128");
 	segments_ = count;
 	seg_dot_cx_ = (int)((longest+kDotChunk-1)/kDotChunk);
+	seg_len_.resize(count);
+	for (int k = 0; k < count; ++k) seg_len_[k] = entry_offsets[k+1]-entry_offsets[k];
 	seg_vec_cx_ = (int)((longest+kVecChunk-1)/kVecChunk);
 	const int stride = restart_+1;
 	seg_off_.Allocate(count+1);
@@ -345,6 +347,8 @@ void Gmres::SetSegments(const std::vector<int64_t>& entry_offsets)
 	seg_host_beta_.assign(count, 0.0);
 	seg_host_tol_.assign(count, 0.0);
 	seg_host_flags_.assign(4, 0);
+	seg_host_stop_.assign(count, 0);
+	seg_blocks_ = blocks;
 	CudaCheck(cudaStreamSynchronize(stream_), "segments");
 }
 
@@ -468,19 +472,35 @@ GmresResult Gmres::SolveFlexibleSegmentsImpl(const DevicePatternView& pattern, c
 		for (int j = 0; j < cap;) {
 			const int batch = std::min(kSegBatch, cap-j);
 			for (int b = 0; b < batch; ++b) SegFlexibleStep<T, B>(pattern, values, j+b, M);
-			j += batch;
 			seg_all_.Download(seg_host_flags_.data(), 3, stream_);
+			if (profiler_) seg_stop_.Download(seg_host_stop_.data(), segments_, stream_);
 			CudaCheck(cudaStreamSynchronize(stream_), "segmented FGMRES batch");
+			if (profiler_) {
+				// the work of the segments still open at the end of the batch (a lower bound: a segment
+				// that stopped inside the batch did part of it): SpMV blocks and vectors, and the
+				// Gram-Schmidt traffic of steps j .. j + batch - 1 over their entries
+				double entries = 0.0, blocks = 0.0;
+				for (int k = 0; k < segments_; ++k)
+					if (!seg_host_stop_[k]) {
+						const double len = (double)(seg_len_[k]);
+						entries += len;
+						if ((size_t)k < seg_blocks_.size()) blocks += (double)seg_blocks_[k];
+					}
+				const double basis = (double)sizeof(B), vb = sizeof(T) == 4 ? 68.0 : 132.0;
+				profiler_->AddBytes(Profiler::kSpmv, batch*(blocks*vb+entries*(8.0+8.0)));
+				double algo = 0.0, moved = 0.0;
+				for (int s = j; s < j+batch; ++s) {
+					algo += entries*(basis*(2.0*s+7.0)+8.0);
+					moved += entries*(4.0*basis*(s+1.0)+40.0+basis);
+				}
+				profiler_->AddBytes(Profiler::kOrtho, algo);
+				profiler_->AddMovedBytes(Profiler::kOrtho, moved);
+			}
+			j += batch;
 			used = seg_host_flags_[1];
 			if (seg_host_flags_[0]) break;
 		}
 		result.iterations += used;
-		if (profiler_) {
-			// the union's vectors, as the single-system count (stopped segments move less)
-			const double basis = (double)sizeof(B);
-			profiler_->AddBytes(Profiler::kOrtho, (double)n_*(basis*(used*(used-1.0)+7.0*used)+8.0*used));
-			profiler_->AddMovedBytes(Profiler::kOrtho, (double)n_*(4.0*basis*0.5*used*(used+1.0)+(40.0+basis)*used));
-		}
 		if (profiler_) profiler_->Begin(Profiler::kVector, stream_);
 		SegBackSolveKernel<<<segments_, 256, (size_t)(restart_+1)*sizeof(double), stream_>>>(seg_H_.get(), seg_g_.get(),
 			restart_, stride, seg_used_.get(), seg_y_.get(), seg_all_.get());

@@ -1013,9 +1013,11 @@ void NsSolver::SetSegments(const int64_t* node_offsets, int count)
 	for (int k = 0; k < count; ++k)
 		if (!(node_offsets[k+1] > node_offsets[k])) Fail(-1, "segment offsets must increase");
 	segment_nodes_.assign(node_offsets, node_offsets+count+1);
-	std::vector<int64_t> entries(count+1);
+	std::vector<int64_t> entries(count+1), blocks(count);
 	for (int k = 0; k <= count; ++k) entries[k] = 4*node_offsets[k];
-	gmres_.SetSegments(entries);
+	const auto& rows = mesh_.pattern().row_offsets;
+	for (int k = 0; k < count; ++k) blocks[k] = (int64_t)rows[node_offsets[k+1]]-rows[node_offsets[k]];
+	gmres_.SetSegments(entries, blocks);
 	segment_entries_.Allocate(count+1);
 	segment_entries_.Upload(entries.data(), count+1, stream_);
 	segment_sq_.Allocate(count);
