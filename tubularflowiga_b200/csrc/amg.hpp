@@ -62,6 +62,8 @@ public:
 	// Block-Jacobi inverses (4x4 per node, FP64) of the fine level, current after Refresh.
 	const double* fine_inverse() const;
 	long long launches() const { return launches_; }
+	// launches replayed from a captured CUDA graph (counted as if launched)
+	void count_launches(long long n) { launches_ += n; }
 	void set_profiler(Profiler* p) { profiler_ = p; }
 
 private:

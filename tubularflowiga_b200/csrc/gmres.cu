@@ -463,6 +463,7 @@ Gmres::Gmres(int nodes, int restart, cudaStream_t stream, int fields)
 
 Gmres::~Gmres()
 {
+	ReleaseSegmentGraphs();
 	if (host_) cudaFreeHost(host_);
 }
 

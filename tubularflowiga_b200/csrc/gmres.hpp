@@ -106,6 +106,12 @@ private:
 		double* x, double rtol, int max_iterations, Amg& preconditioner, long long* launches);
 	template <class T, class B>
 	void SegFlexibleStep(const DevicePatternView& pattern, const T* values, int j, Amg& preconditioner);
+	// SegFlexibleStep through a CUDA graph captured on the step's first use (one graph per Arnoldi
+	// index j, replayed while the operator, preconditioner and vectors stay where they are); direct
+	// launches while profiling, with the outlet term or the learned stage, or if capture fails.
+	template <class T, class B>
+	void SegStep(const DevicePatternView& pattern, const T* values, int j, Amg& preconditioner);
+	void ReleaseSegmentGraphs();
 	// r = b - A x, segment norms into seg_host_beta_ / seg_beta_, r stored as basis vector 0
 	template <class T, class B>
 	void SegTrueResidual(const DevicePatternView& pattern, const T* values, const double* rhs, const double* x);
@@ -119,6 +125,11 @@ private:
 	std::vector<int> seg_host_flags_, seg_host_stop_;
 	std::vector<int64_t> seg_blocks_;    // matrix blocks per segment (byte accounting)
 	std::vector<int64_t> seg_len_;       // entries per segment
+	std::vector<cudaGraphExec_t> seg_graphs_;            // per Arnoldi index j
+	std::vector<long long> seg_graph_launches_, seg_graph_amg_launches_;
+	const void* seg_graph_values_ = nullptr;             // operator the graphs were captured with
+	const void* seg_graph_amg_ = nullptr;
+	bool seg_graphs_ok_ = true;
 
 	int nodes_, fields_, n_, restart_, blocks_;
 	unsigned singular_count_ = 0;     // singular diagonal blocks of the last block-inverse build

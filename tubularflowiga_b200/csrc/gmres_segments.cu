@@ -303,6 +303,7 @@ __global__ void SegStoreBasisKernel(long long n, const double* __restrict__ r, B
 
 void Gmres::SetSegments(const std::vector<int64_t>& entry_offsets, const std::vector<int64_t>& blocks)
 {
+	ReleaseSegmentGraphs();
 	const int count = (int)entry_offsets.size()-1;
 	if (count <= 0) { segments_ = 0; return; }
 	if (count > 1024) Fail(-7, "at most 1024 segments per flexible solve");
@@ -418,6 +419,68 @@ void Gmres::SegFlexibleStep(const DevicePatternView& pattern, const T* values, i
 	launches_ += 8;
 }
 
+void Gmres::ReleaseSegmentGraphs()
+{
+	for (auto& g : seg_graphs_)
+		if (g) cudaGraphExecDestroy(g);
+	seg_graphs_.clear();
+	seg_graph_launches_.clear();
+	seg_graph_amg_launches_.clear();
+	seg_graph_values_ = nullptr;
+	seg_graph_amg_ = nullptr;
+}
+
+template <class T, class B>
+void Gmres::SegStep(const DevicePatternView& pattern, const T* values, int j, Amg& M)
+{
+	const bool profiling = profiler_ != nullptr && profiler_->enabled();
+	if (!seg_graphs_ok_ || profiling || low_on_ || learned_ != nullptr) {
+		SegFlexibleStep<T, B>(pattern, values, j, M);
+		return;
+	}
+	if (seg_graph_values_ != static_cast<const void*>(values) || seg_graph_amg_ != static_cast<const void*>(&M))
+		ReleaseSegmentGraphs();
+	if ((int)seg_graphs_.size() < restart_) {
+		seg_graphs_.resize(restart_, nullptr);
+		seg_graph_launches_.resize(restart_, 0);
+		seg_graph_amg_launches_.resize(restart_, 0);
+	}
+	seg_graph_values_ = values;
+	seg_graph_amg_ = &M;
+	if (seg_graphs_[j] == nullptr) {
+		const long long own0 = launches_, amg0 = M.launches();
+		cudaGraph_t graph = nullptr;
+		if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+			(void)cudaGetLastError();
+			seg_graphs_ok_ = false;
+			SegFlexibleStep<T, B>(pattern, values, j, M);
+			return;
+		}
+		SegFlexibleStep<T, B>(pattern, values, j, M);
+		const cudaError_t end = cudaStreamEndCapture(stream_, &graph);
+		cudaGraphExec_t exec = nullptr;
+		const bool ok = end == cudaSuccess && graph != nullptr
+			&& cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+		if (graph) cudaGraphDestroy(graph);
+		if (!ok) {
+			// nothing of the step ran while it was being captured: run it directly from now on
+			(void)cudaGetLastError();
+			seg_graphs_ok_ = false;
+			launches_ = own0;
+			SegFlexibleStep<T, B>(pattern, values, j, M);
+			return;
+		}
+		seg_graphs_[j] = exec;
+		seg_graph_launches_[j] = launches_-own0;
+		seg_graph_amg_launches_[j] = M.launches()-amg0;
+		launches_ = own0;
+		M.count_launches(-seg_graph_amg_launches_[j]);
+	}
+	CudaCheck(cudaGraphLaunch(seg_graphs_[j], stream_), "segmented FGMRES step graph");
+	launches_ += seg_graph_launches_[j];
+	M.count_launches(seg_graph_amg_launches_[j]);
+}
+
 template <class T>
 GmresResult Gmres::SolveFlexibleSegments(const DevicePatternView& pattern, const T* values, const double* rhs,
 	double* x, double rtol, int max_iterations, Amg& M, long long* launches, bool fp64_basis)
@@ -471,7 +534,7 @@ GmresResult Gmres::SolveFlexibleSegmentsImpl(const DevicePatternView& pattern, c
 		int used = 0;
 		for (int j = 0; j < cap;) {
 			const int batch = std::min(kSegBatch, cap-j);
-			for (int b = 0; b < batch; ++b) SegFlexibleStep<T, B>(pattern, values, j+b, M);
+			for (int b = 0; b < batch; ++b) SegStep<T, B>(pattern, values, j+b, M);
 			seg_all_.Download(seg_host_flags_.data(), 3, stream_);
 			if (profiler_) seg_stop_.Download(seg_host_stop_.data(), segments_, stream_);
 			CudaCheck(cudaStreamSynchronize(stream_), "segmented FGMRES batch");
