@@ -325,7 +325,8 @@ int tfiga_ns_amg_info(tfiga_ns* ns, tfiga_amg_info* info);
  * test is then taken per tube, relative to the tube's own first residual of the step, and a tube that
  * passes is frozen for the rest of the step (its rows of the linear system carry a zero rhs); the
  * linear solves run one FGMRES per tube over shared launches (each tube its own Arnoldi process,
- * Hessenberg matrix and tolerance, stopping on its own; the AMG preconditioner only), each open
+ * Hessenberg matrix and tolerance, stopping on its own; the AMG preconditioner only; each Arnoldi step
+ * replayed from a CUDA graph captured on its first use, except while profiling), each open
  * tube's rhs scaled to unit norm and its update scaled back; the step converges when every tube has
  * passed. */
 int tfiga_ns_set_segments(tfiga_ns* ns, const int64_t* node_offsets, int32_t count);
