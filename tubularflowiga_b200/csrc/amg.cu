@@ -138,12 +138,14 @@ template <class A>
 __global__ void __launch_bounds__(256) CoarseCorrectionKernel(int nodes, const int32_t* __restrict__ agg,
 	const double* __restrict__ mask, const double* __restrict__ xc, const int32_t* __restrict__ ap_rows,
 	const int32_t* __restrict__ ap_cols, const A* __restrict__ ap, const double* __restrict__ b,
-	const double* __restrict__ inverse, double omega, double* __restrict__ z, const int* __restrict__ stop)
+	const double* __restrict__ inverse, double omega, double* __restrict__ z, const int* __restrict__ stop,
+	const int32_t* __restrict__ node_seg, const int* __restrict__ seg_stop)
 {
 	if (*stop) return;
 	const long long t = (long long)blockIdx.x*blockDim.x+threadIdx.x;
 	const int i = (int)(t >> 2), row = (int)(t & 3);
-	const bool active = i < nodes;
+	// a node of a stopped segment takes no work (the lane quad stays together for the shuffles)
+	const bool active = i < nodes && (seg_stop == nullptr || !seg_stop[node_seg[i]]);
 	double r = 0.0;
 	if (active) {
 		r = b[t];
@@ -167,10 +169,15 @@ __global__ void __launch_bounds__(256) CoarseCorrectionKernel(int nodes, const i
 // b_c[I,c] = sum_{i in I} mask_i[c] r[i,c]: one CTA per aggregate, fixed-order reduction.
 __global__ void __launch_bounds__(128) RestrictKernel(int coarse_nodes, const int32_t* __restrict__ order,
 	const int32_t* __restrict__ offsets, const double* __restrict__ mask, const double* __restrict__ r,
-	double* __restrict__ bc, const int* __restrict__ stop)
+	double* __restrict__ bc, const int* __restrict__ stop, const int32_t* __restrict__ agg_seg,
+	const int* __restrict__ seg_stop)
 {
 	if (*stop) return;
 	const int I = blockIdx.x;
+	if (seg_stop != nullptr && seg_stop[agg_seg[I]]) {
+		if (threadIdx.x < 4) bc[4*I+threadIdx.x] = 0.0;   // a stopped segment's coarse rows
+		return;
+	}
 	double acc[4] = {0.0, 0.0, 0.0, 0.0};
 	for (int k = offsets[I]+threadIdx.x; k < offsets[I+1]; k += blockDim.x) {
 		const size_t i = (size_t)order[k];
@@ -704,6 +711,7 @@ void Amg::BuildFromStrength(std::vector<double> s)
 	}
 	CudaCheck(cudaStreamSynchronize(stream_), "AMG setup");
 	built_ = true;
+	BuildSegmentMaps();
 	masks_dirty_ = true;
 }
 
@@ -823,32 +831,65 @@ template void Amg::Refresh<double>(const double*, bool);
 template void Amg::Refresh<float>(const float*, bool);
 
 template <class T>
-void Amg::Cycle(int l, const T* A, const double* b, double* x, const int* stop)
+void Amg::Cycle(int l, const T* A, const double* b, double* x, const int* stop, const int* seg_stop)
 {
 	// Two-level: x_c = Ac^{-1} P^T b, then x = P x_c + omega D^{-1} (b - (A P) x_c).
 	Level& L = *levels_[l];
 	Level& C = *levels_[l+1];
+	const bool masked = seg_stop != nullptr && segment_maps_ && l == 0;
 	RestrictKernel<<<C.nodes, 128, 0, stream_>>>(C.nodes, L.agg_order.get(), L.agg_offsets.get(),
-		L.mask.get(), b, C.b.get(), stop);
+		L.mask.get(), b, C.b.get(), stop, masked ? aggregate_segment_dev_.get() : nullptr, masked ? seg_stop : nullptr);
 	LaunchCheck("RestrictKernel");
 	DenseApplyKernel<<<Grid(C.dense_n, 8), 256, 0, stream_>>>(C.dense_n, C.dense.get(), C.b.get(), C.x.get(), stop);
 	LaunchCheck("DenseApplyKernel");
 	(void)A;      // the fine operator enters through A P, refreshed with it
 	CoarseCorrectionKernel<T><<<Grid(4LL*L.nodes, 256), 256, 0, stream_>>>(L.nodes, L.agg.get(), L.mask.get(),
-		C.x.get(), L.ap_rows.get(), L.ap_cols.get(), ApValues<T>(L), b, L.inverse.get(), options_.omega, x, stop);
+		C.x.get(), L.ap_rows.get(), L.ap_cols.get(), ApValues<T>(L), b, L.inverse.get(), options_.omega, x, stop,
+		masked ? node_segment_dev_.get() : nullptr, masked ? seg_stop : nullptr);
 	LaunchCheck("CoarseCorrectionKernel");
 	launches_ += 3;
 }
 
 template <class T>
-void Amg::Apply(const T* fine_values, const double* v, double* z, const int* stop)
+void Amg::Apply(const T* fine_values, const double* v, double* z, const int* stop, const int* seg_stop)
 {
 	if (profiler_) profiler_->Begin(Profiler::kOther, stream_);
-	Cycle<T>(0, fine_values, v, z, stop);
+	Cycle<T>(0, fine_values, v, z, stop, seg_stop);
 	if (profiler_) profiler_->End(stream_);
 }
 
-template void Amg::Apply<double>(const double*, const double*, double*, const int*);
-template void Amg::Apply<float>(const float*, const double*, double*, const int*);
+template void Amg::Apply<double>(const double*, const double*, double*, const int*, const int*);
+template void Amg::Apply<float>(const float*, const double*, double*, const int*, const int*);
+
+void Amg::SetSegments(const std::vector<int32_t>& node_segment)
+{
+	node_segment_ = node_segment;
+	segment_maps_ = false;
+	if (built_) BuildSegmentMaps();
+}
+
+// Device maps of the masked application: each fine node's segment, and each level-1 aggregate's
+// (taken from any of its nodes; aggregates never cross segments, the matrix having no coupling
+// between them).
+void Amg::BuildSegmentMaps()
+{
+	segment_maps_ = false;
+	if (node_segment_.empty() || levels_.size() < 2) return;
+	const Level& L = *levels_[0];
+	if ((int)node_segment_.size() != L.nodes) Fail(-1, "AMG segment map does not match the fine level");
+	std::vector<int32_t> agg_seg(levels_[1]->nodes, -1);
+	for (int i = 0; i < L.nodes; ++i) {
+		const int32_t I = L.h_agg[i];
+		if (agg_seg[I] < 0) agg_seg[I] = node_segment_[i];
+		else if (agg_seg[I] != node_segment_[i]) Fail(-1, "an AMG aggregate spans two segments");
+	}
+	for (auto& v : agg_seg) if (v < 0) v = 0;
+	node_segment_dev_.Allocate(node_segment_.size());
+	node_segment_dev_.Upload(node_segment_.data(), node_segment_.size(), stream_);
+	aggregate_segment_dev_.Allocate(agg_seg.size());
+	aggregate_segment_dev_.Upload(agg_seg.data(), agg_seg.size(), stream_);
+	CudaCheck(cudaStreamSynchronize(stream_), "AMG segment maps");
+	segment_maps_ = true;
+}
 
 } // namespace tfiga

@@ -52,8 +52,13 @@ public:
 	// Refresh from the fine values: A P and the fine block-Jacobi inverses always; the Galerkin
 	// coarse operator and its dense inverse when `coarse` (always on the first refresh).
 	template <class T> void Refresh(const T* values, bool coarse = true);
-	// z = M^{-1} v; kernels skip when *stop is set.
-	template <class T> void Apply(const T* fine_values, const double* v, double* z, const int* stop);
+	// z = M^{-1} v; kernels skip when *stop is set.  With seg_stop (after SetSegments): the fine
+	// nodes and aggregates of segments whose flag is set are skipped (their z is left as it was).
+	template <class T> void Apply(const T* fine_values, const double* v, double* z, const int* stop,
+		const int* seg_stop = nullptr);
+	// Segment of every fine node (independent blocks of the matrix; aggregates never cross them), for
+	// the masked Apply; empty: none.
+	void SetSegments(const std::vector<int32_t>& node_segment);
 	int levels() const { return (int)levels_.size(); }
 	std::vector<int> level_nodes() const;
 	const std::vector<int>& aggregation_rounds() const { return coarse_history_; }
@@ -68,7 +73,12 @@ public:
 
 private:
 	struct Level;
-	template <class T> void Cycle(int level, const T* fine, const double* b, double* x, const int* stop);
+	template <class T> void Cycle(int level, const T* fine, const double* b, double* x, const int* stop,
+		const int* seg_stop);
+	void BuildSegmentMaps();           // after the hierarchy exists (Build, or SetSegments once built)
+	std::vector<int32_t> node_segment_;                 // host copy until the hierarchy exists
+	DeviceArray<int32_t> node_segment_dev_, aggregate_segment_dev_;
+	bool segment_maps_ = false;
 	template <class T> T* ApValues(Level& level);   // A P blocks in the fine matrix's precision
 	void BuildFromStrength(std::vector<double> s);
 	std::vector<std::unique_ptr<Level>> levels_;

@@ -385,7 +385,7 @@ void Gmres::SegFlexibleStep(const DevicePatternView& pattern, const T* values, i
 	LaunchCheck("SegScaleCopyKernel");
 	if (profiler_) profiler_->End(stream_);
 	double* z = Z_.get()+(size_t)j*n_;
-	M.Apply(values, r_.get(), z, all);
+	M.Apply(values, r_.get(), z, all, seg_stop_.get());   // stopped tubes' nodes and aggregates skipped
 	if (profiler_) profiler_->Begin(Profiler::kSpmv, stream_);
 	// the rows of stopped segments are skipped: nothing reads their w again in this cycle
 	LaunchSpmvMasked<T>(pattern, values, z, w_.get(), all, seg_node_.get(), seg_stop_.get(), stream_);

@@ -1006,6 +1006,7 @@ void NsSolver::SetSegments(const int64_t* node_offsets, int count)
 	if (count == 0) {
 		segments_ = 0;
 		gmres_.SetSegments({});
+		if (amg_) amg_->SetSegments({});
 		return;
 	}
 	if (node_offsets == nullptr) Fail(-1, "null segment offsets");
@@ -1018,6 +1019,12 @@ void NsSolver::SetSegments(const int64_t* node_offsets, int count)
 	const auto& rows = mesh_.pattern().row_offsets;
 	for (int k = 0; k < count; ++k) blocks[k] = (int64_t)rows[node_offsets[k+1]]-rows[node_offsets[k]];
 	gmres_.SetSegments(entries, blocks);
+	if (amg_) {
+		std::vector<int32_t> node_segment((size_t)nodes());
+		for (int k = 0; k < count; ++k)
+			for (int64_t i = node_offsets[k]; i < node_offsets[k+1]; ++i) node_segment[i] = k;
+		amg_->SetSegments(node_segment);
+	}
 	segment_entries_.Allocate(count+1);
 	segment_entries_.Upload(entries.data(), count+1, stream_);
 	segment_sq_.Allocate(count);
