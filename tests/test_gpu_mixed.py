@@ -8,7 +8,7 @@ FP32 accumulation and stored in FP32; the residual stays FP64.  Tolerances:
   operand), and the blocks whose terms cancel lose a few bits more;
 * Newton: the mixed Newton iteration converges to the FP64 solution; after
   convergence to 1e-10 of the initial residual velocity and pressure agree to
-  1e-8 relative L2 with the FP64 path (the north star's bar; measured about
+  1e-8 relative L2 with the FP64 path (the accuracy bar of the mixed path; measured about
   2e-13 on the cylinder), and over several transient steps of the pulsatile
   section with the bench's solver settings every step stays within 1e-8
   (measured 3e-11 .. 7e-11).
