@@ -1189,7 +1189,7 @@ def main():
         "metric": METRIC, "value": steps_per_s, "unit": "time steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": ("tf32-tc/f32/f64" if args.precision == "tf32" else "bf16-tc/f32/f64") if mixed else "f64",
-        "data": "synthetic (seeded generator; BASELINE publishes no dataset)",
+        "data": "synthetic (seeded generator; the reference publishes no dataset for this metric)",
         "config": {"workload": desc, "elements": tube.mesh.elements, "nodes": n, "block_nonzeros": mesh.blocks,
                    "solver": (("mixed: tcgen05 %s tangent (FP32 accumulate), FP32 Jacobian, FP64 residual and "
                                "refinement; " % {"bf16x3": "split-BF16 (hi + lo, 3 products)", "tf32": "TF32",
